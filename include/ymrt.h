@@ -1,0 +1,153 @@
+/*
+ * ymrt.h -- C ABI of the ymrt_b200 wavefront path tracer (sm_100a).
+ *
+ * Plain C: opaque handles, plain pointers and sizes, int status codes
+ * (0 = YMRT_OK, negative = YMRT_ERR_*). No exception or C++ type crosses
+ * this boundary.
+ *
+ * What each entry point replaces in the YMRT reference (paths relative to
+ * the reference project):
+ *
+ *   ymrt_scene_load_ymtmp   SceneParser::parsing_scene          src/core/YMParser.cpp:2330
+ *                           + the scene preparation of
+ *                           GuiModule::UpdateScene (BVH build,
+ *                           shape-light table, camera)          src/core/GuiModule.cpp:116-282
+ *   ymrt_scene_upload       GuiModule::UpdateScene device upload src/core/GuiModule.cpp:173-272
+ *                           (UPLOAD_TO_GPU of every array)
+ *   ymrt_render_forward     one progressive frame of
+ *                           RenderModule::PathTracingExecuteTask src/core/RenderModule.cpp:494-653
+ *                           i.e. the stage launchers
+ *                           RayGenerationPathTracing            src/Shading.cu:1727
+ *                           RayTracePathTracing                 src/Shading.cu:1903
+ *                           RayShadingPathTracing               src/Shading.cu:2304
+ *                           into the frame's noise image
+ *   ymrt_accumulate         AccumulateImagePathTracing          src/Shading.cu:2375
+ *   ymrt_debug_trace        TraceRay                            src/ShadingUtilities.cuh:310
+ *   ymrt_debug_occluded     BVHTraverseShadow                   src/ShadingUtilities.cuh:563
+ *   ymrt_debug_halton       HaltonEnumerator::GetIndex +        src/HaltonEnumerator.h:43
+ *                           HaltonSampler::Random1D             src/RandomSampler.cuh:430
+ *
+ * Threading: a context owns one CUDA stream; use one context per host
+ * thread. Scenes belong to the context they were uploaded with.
+ */
+#ifndef YMRT_H_
+#define YMRT_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define YMRT_OK 0
+#define YMRT_ERR_INVALID (-1)     /* bad argument */
+#define YMRT_ERR_IO (-2)          /* file cannot be read */
+#define YMRT_ERR_FORMAT (-3)      /* malformed .ymtmp */
+#define YMRT_ERR_UNSUPPORTED (-4) /* valid input this build does not render */
+#define YMRT_ERR_CUDA (-5)        /* CUDA runtime error (see ymrt_last_error) */
+#define YMRT_ERR_OOM (-6)         /* device allocation failed */
+#define YMRT_ERR_TIMEOUT (-7)     /* a bounded device loop gave up */
+#define YMRT_ERR_OVERFLOW (-8)    /* a queue or stack limit was exceeded */
+#define YMRT_ERR_NO_DEVICE (-9)   /* no CUDA device, or the kernels are missing */
+
+typedef struct ymrt_context ymrt_context;
+typedef struct ymrt_host_scene ymrt_host_scene;
+typedef struct ymrt_scene ymrt_scene;
+
+/* Byte-compatible with the reference's RenderSetting (src/SceneDefines.h:17-40). */
+typedef struct ymrt_render_setting {
+  int ssp;                 /* samples per pixel per frame */
+  int ray_depth;           /* bounces before Russian roulette / termination */
+  float gamma;             /* unused on this path (display only) */
+  float exposure;          /* unused on this path (display only) */
+  int max_frame_count;
+  int sampler_type;        /* 0 PCG, 1 Halton, 2 Sobol (this build renders Halton) */
+  int enable_shape_light;
+  uint8_t enable_distant_light;
+  uint8_t enable_volume_scattering;
+  uint8_t enable_env_light;
+  uint8_t enable_russian_roulette;
+  uint8_t enable_indirect_clamp;
+  uint8_t pad_[3];
+  float indirect_limit;
+} ymrt_render_setting;
+
+/* Per-frame counters and timings filled by ymrt_render_forward. */
+typedef struct ymrt_stats {
+  uint64_t paths;            /* camera paths started */
+  uint64_t extension_rays;   /* closest-hit queries */
+  uint64_t shadow_rays;      /* any-hit (occlusion) queries */
+  uint64_t waves;            /* extend/shade iterations */
+  double ms_total;           /* device time of the frame (CUDA events) */
+  double ms_generate;
+  double ms_extend;
+  double ms_shade;
+  uint32_t device_errors;    /* bit set of YMRT_DEVERR_* raised on the device */
+  uint32_t reserved_;
+} ymrt_stats;
+
+#define YMRT_DEVERR_STACK 1u     /* a traversal stack overflowed (entries were dropped) */
+#define YMRT_DEVERR_QUEUE 2u     /* a path queue overflowed */
+#define YMRT_DEVERR_ITER 4u      /* a bounded loop hit its iteration cap */
+
+/* ---- contexts ---- */
+int ymrt_create(int device_ordinal, ymrt_context** out);
+void ymrt_destroy(ymrt_context* ctx);
+/* Last error message of the context (or of the library when ctx is NULL). */
+const char* ymrt_last_error(const ymrt_context* ctx);
+/* Largest number of paths in flight (queue slots); 0 keeps the default. */
+int ymrt_set_queue_capacity(ymrt_context* ctx, uint32_t paths);
+
+/* ---- scenes ---- */
+/* Parses and prepares a scene on the host (no GPU needed). err may be NULL. */
+int ymrt_scene_load_ymtmp(const char* path, int width, int height, ymrt_host_scene** out, char* err,
+                          size_t err_len);
+void ymrt_host_scene_free(ymrt_host_scene* scene);
+
+/* Host-scene queries (for parity checks against the reference's own scene
+ * preparation). Each copies into `out` (capacity `cap` elements) and returns
+ * the element count, or a negative YMRT_ERR_*. */
+#define YMRT_QUERY_COUNTS 0      /* uint64[8]: instances, meshes, triangles, instanced triangles, lights, blas nodes, tlas nodes, materials */
+#define YMRT_QUERY_INSTANCES 1   /* uint32[6*n]: geometry, transform, material, volume, boundary, file index */
+#define YMRT_QUERY_LIGHTS 2      /* float[4*n]: instance (bits), triangle (bits), power, area */
+#define YMRT_QUERY_LIGHT_TABLE 3 /* float[n] */
+#define YMRT_QUERY_TRANSFORMS 4  /* float[32*n]: object-to-world then world-to-object, column major */
+#define YMRT_QUERY_CAMERA 5      /* float[14]: position, u, v, w, aspect, tan(fov/2) */
+#define YMRT_QUERY_TRIANGLES 6   /* uint32[3*n] corner triples of mesh `index`, reference order */
+long long ymrt_host_scene_query(const ymrt_host_scene* scene, int what, int index, void* out, size_t cap);
+
+/* Uploads a prepared scene. halton_perm: the concatenated digit permutations
+ * of the first 1000 primes (3,682,913 uint32), the table the reference keeps
+ * in Scene::sampler_data.halton_permute_table. */
+int ymrt_scene_upload(ymrt_context* ctx, const ymrt_host_scene* scene, const uint32_t* halton_perm, size_t perm_len,
+                      ymrt_scene** out);
+void ymrt_scene_free(ymrt_scene* scene);
+
+/* ---- rendering ---- */
+/* Renders one progressive frame (frame_index >= 1) of every tile into
+ * out_rgba (width*height float4, linear radiance averaged over the frame's
+ * samples, alpha = 1), like the reference's noise image. out_rgba is a device
+ * pointer when out_on_device != 0, else host memory (copied back before
+ * returning). stats may be NULL. */
+int ymrt_render_forward(ymrt_scene* scene, const ymrt_render_setting* setting, int frame_index, float* out_rgba,
+                        int out_on_device, ymrt_stats* stats);
+/* Same, restricted to tiles [tile_begin, tile_end) of the 16x16 tiling. */
+int ymrt_render_tiles(ymrt_scene* scene, const ymrt_render_setting* setting, int frame_index, int tile_begin,
+                      int tile_end, float* out_rgba, int out_on_device, ymrt_stats* stats);
+/* Running mean over frames (device pointers): acc = (acc*(f-1) + noise) / f. */
+int ymrt_accumulate(ymrt_scene* scene, const float* noise_rgba, float* acc_rgba, int frame_index);
+
+/* ---- known-answer entry points (host buffers) ---- */
+int ymrt_debug_trace(ymrt_scene* scene, int n, const float* origin, const float* dir, const uint32_t* last_hit,
+                     uint32_t* inst, uint32_t* tri, float* t, float* bary, int* back, int* nearby);
+int ymrt_debug_occluded(ymrt_scene* scene, int n, const float* origin, const float* dir, const float* tmax,
+                        int* occluded);
+int ymrt_debug_halton(ymrt_scene* scene, int n, const int* px, const int* py, const int* sample, int n_dims,
+                      uint64_t* index, float* offset, float* dims);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* YMRT_H_ */

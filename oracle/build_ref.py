@@ -1,0 +1,196 @@
+"""Build recipe for the oracle: the YMRT reference compiled for the host.
+
+TEST INFRASTRUCTURE ONLY. Compiles the reference's own sources where they lie
+(``/root/reference/src``) with g++ into ``oracle/_ref/libymrt_ref.so``
+(git-ignored, but shipped with the repository snapshot to GPU machines). The
+reference's CMake build is not used: the hot-path sources compile directly
+once a few MSVC/CUDA-runtime stand-ins are provided (``oracle/shims``,
+``oracle/ref_stubs.cpp``). ``oracle/ref_harness.cpp`` is this project's
+headless driver around the reference's stage kernels.
+
+Floating point: ``-ffp-contract=off`` (no fused multiply-add), SSE2 scalar
+float, IEEE division and square root; glm is forced to its scalar code path.
+That is the same arithmetic the ymrt_b200 kernels use (they are built with
+``-fmad=false``), so both evaluate each reference expression in source order.
+
+Sampler argument order: where the reference passes several ``random()`` calls
+as arguments of one call (e.g. ``src/Shading.cu:325, 370``), C++ leaves their
+evaluation order unspecified. With ``arg_order="ltr"`` the build writes a copy
+of ``src/Shading.cu`` into ``oracle/_ref/gen/`` in which those argument lists
+are drawn left to right (the order nvcc's device front end uses); with
+``"native"`` the file is compiled unchanged (g++ on x86-64 evaluates them
+right to left). Nothing else in the file is changed.
+
+Usage: ``python oracle/build_ref.py [--arg-order ltr|native] [--force]``.
+"""
+from __future__ import annotations
+
+import argparse
+import hashlib
+import os
+import re
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF = os.environ.get("YMRT_REFERENCE_ROOT", "/root/reference")
+OUT = os.path.join(HERE, "_ref")
+LIB = os.path.join(OUT, "libymrt_ref.so")
+
+HOST_SOURCES = [
+    "src/BottomBVH.cpp",
+    "src/TopBVH.cpp",
+    "src/Camera.cpp",
+    "src/core/SceneModule.cpp",
+    "src/core/YMParser.cpp",
+    "src/FileIO.cpp",
+    "src/LowDiscrepancy.cpp",
+]
+
+CXXFLAGS = [
+    "-std=c++17", "-O2", "-ffp-contract=off", "-fno-fast-math", "-DNDEBUG", "-DGLM_FORCE_PURE",
+    "-fPIC", "-w", "-pthread",
+]
+
+
+def _includes():
+    return [
+        "-include", os.path.join(HERE, "shims", "ymrt_ref_prelude.h"),
+        "-I" + os.path.join(HERE, "shims"),
+        "-I" + REF, "-I" + os.path.join(REF, "src"), "-I" + os.path.join(REF, "src", "core"),
+        "-I" + os.path.join(REF, "external", "glm"),
+        "-I" + os.path.join(REF, "external", "glad", "include"),
+        "-I" + os.path.join(REF, "external", "image_lib"),
+        "-I" + os.path.join(REF, "external", "assimp-5.1.0", "include"),
+        "-I/usr/local/cuda/include",
+    ]
+
+
+# Call arguments made of several sampler draws, e.g. "random(), random()" or
+# "ray_sampler.Random1D(), ray_sampler.Random1D(), ray_sampler.Random1D()".
+_DRAW = r"(random\(\)|[A-Za-z_][A-Za-z_0-9]*\.Random1D\(\))"
+_RUN = re.compile(_DRAW + r"(?:\s*,\s*" + _DRAW + r")+")
+
+
+def _sequence_draws(text: str) -> tuple[str, int]:
+    """Rewrites each run of sampler draws inside an argument list so that the
+    draws happen left to right whatever order the compiler evaluates
+    arguments in: the first-evaluated draw of the run fills a small buffer in
+    source order, each argument then reads its own slot."""
+    count = 0
+
+    def repl(m: re.Match) -> str:
+        nonlocal count
+        parts = [p.strip() for p in m.group(0).split(",")]
+        n = len(parts)
+        if n < 2 or len(set(parts)) != 1:
+            return m.group(0)
+        count += 1
+        draw = parts[0]
+        fn = "[&]()->float{ return " + draw + "; }"
+        return ", ".join(f"ymrt_oracle_draw_in_order({fn}, {n}, {k})" for k in range(n))
+
+    return _RUN.sub(repl, text), count
+
+
+_HELPER = r'''
+// ---- inserted by oracle/build_ref.py: left-to-right sampler draws ----
+#include <cstddef>
+namespace {
+struct YmrtOracleDrawBuffer { float v[8]; int pending = 0; };
+thread_local YmrtOracleDrawBuffer ymrt_oracle_draw_buffer;
+template <typename Draw>
+inline float ymrt_oracle_draw_in_order(Draw draw, int n, int k) {
+  YmrtOracleDrawBuffer& b = ymrt_oracle_draw_buffer;
+  if (b.pending == 0) { for (int i = 0; i < n; ++i) b.v[i] = draw(); b.pending = n; }
+  --b.pending;
+  return b.v[k];
+}
+}  // namespace
+// ---- end of insertion ----
+'''
+
+
+def shading_source(arg_order: str) -> str:
+    src = os.path.join(REF, "src", "Shading.cu")
+    if arg_order == "native":
+        return src
+    with open(src, "r", encoding="utf-8", errors="replace") as f:
+        text = f.read()
+    body, n = _sequence_draws(text)
+    gen_dir = os.path.join(OUT, "gen")
+    os.makedirs(gen_dir, exist_ok=True)
+    dst = os.path.join(gen_dir, "Shading.cu")
+    out = _HELPER + f'#line 1 "{src}"\n' + body
+    with open(dst, "w") as f:
+        f.write(out)
+    with open(os.path.join(gen_dir, "Shading.cu.sites"), "w") as f:
+        f.write(f"{n} argument lists rewritten\n")
+    return dst
+
+
+def _stamp(arg_order: str) -> str:
+    h = hashlib.sha256()
+    h.update(arg_order.encode())
+    h.update(" ".join(CXXFLAGS).encode())
+    for rel in HOST_SOURCES + ["src/Shading.cu"]:
+        p = os.path.join(REF, rel)
+        h.update(str(os.path.getmtime(p)).encode())
+    for rel in ["ref_harness.cpp", "ref_stubs.cpp", "build_ref.py", "shims/ymrt_ref_prelude.h", "shims/ppl.h"]:
+        with open(os.path.join(HERE, rel), "rb") as f:
+            h.update(f.read())
+    return h.hexdigest()
+
+
+def build(arg_order: str = "ltr", force: bool = False, jobs: int = 8) -> str:
+    if not os.path.isdir(os.path.join(REF, "src")):
+        if os.path.exists(LIB):
+            return LIB
+        raise FileNotFoundError(f"reference sources not found at {REF} and no prebuilt {LIB}")
+    os.makedirs(OUT, exist_ok=True)
+    stamp_file = os.path.join(OUT, "stamp")
+    stamp = _stamp(arg_order)
+    if not force and os.path.exists(LIB) and os.path.exists(stamp_file):
+        with open(stamp_file) as f:
+            if f.read().strip() == stamp:
+                return LIB
+    objs = []
+    procs = []
+    obj_dir = os.path.join(OUT, "obj")
+    os.makedirs(obj_dir, exist_ok=True)
+    jobs_list = [(os.path.join(REF, s), os.path.join(obj_dir, os.path.basename(s) + ".o"), []) for s in HOST_SOURCES]
+    shading = shading_source(arg_order)
+    jobs_list.append((os.path.join(HERE, "ref_harness.cpp"), os.path.join(obj_dir, "ref_harness.o"),
+                      [f'-DYMRT_SHADING_SOURCE="{shading}"']))
+    jobs_list.append((os.path.join(HERE, "ref_stubs.cpp"), os.path.join(obj_dir, "ref_stubs.o"), []))
+    for src, obj, extra in jobs_list:
+        cmd = ["g++"] + CXXFLAGS + extra + _includes() + ["-c", src, "-o", obj]
+        procs.append((src, subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT)))
+        objs.append(obj)
+        while len([p for _, p in procs if p.poll() is None]) >= jobs:
+            procs[0][1].wait()
+    for src, p in procs:
+        out, _ = p.communicate()
+        if p.returncode != 0:
+            raise RuntimeError(f"oracle build failed for {src}:\n{out.decode(errors='replace')[-4000:]}")
+    tmp = LIB + ".tmp"
+    cmd = ["g++", "-shared", "-pthread", "-o", tmp] + objs + ["-Wl,--no-undefined"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("oracle link failed:\n" + r.stdout[-4000:] + r.stderr[-4000:])
+    os.replace(tmp, LIB)
+    with open(stamp_file, "w") as f:
+        f.write(stamp)
+    return LIB
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--arg-order", choices=["ltr", "native"], default="ltr")
+    ap.add_argument("--force", action="store_true")
+    a = ap.parse_args(argv)
+    print(build(a.arg_order, a.force))
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,181 @@
+"""ctypes front end of the oracle (the YMRT reference built for the host).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and
+bench.py's CPU-baseline / reference legs, never by the ymrt_b200 product.
+See oracle/build_ref.py for how the library is built and oracle/ref_harness.cpp
+for what each entry point runs in the reference.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_ref", "libymrt_ref.so")
+
+_lib = None
+
+
+class Settings(ctypes.Structure):
+    _fields_ = [
+        ("spp", ctypes.c_int), ("ray_depth", ctypes.c_int), ("sampler_type", ctypes.c_int),
+        ("enable_shape_light", ctypes.c_int), ("enable_distant_light", ctypes.c_int),
+        ("enable_volume_scattering", ctypes.c_int), ("enable_env_light", ctypes.c_int),
+        ("enable_russian_roulette", ctypes.c_int), ("enable_indirect_clamp", ctypes.c_int),
+        ("indirect_limit", ctypes.c_float),
+    ]
+
+
+def available() -> bool:
+    return os.path.exists(LIB_PATH)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            from . import build_ref  # noqa: F401  (only when sources are present)
+            build_ref.build()
+        L = ctypes.CDLL(LIB_PATH)
+        vp, i, u64 = ctypes.c_void_p, ctypes.c_int, ctypes.c_uint64
+        L.ymref_halton_table_size.restype = ctypes.c_size_t
+        L.ymref_scene_load.restype = vp
+        L.ymref_scene_load.argtypes = [ctypes.c_char_p, vp, ctypes.c_size_t, i, i]
+        L.ymref_scene_free.argtypes = [vp]
+        L.ymref_set_settings.argtypes = [vp, ctypes.POINTER(Settings)]
+        for name in ("ymref_scene_counts", "ymref_instances", "ymref_transforms"):
+            getattr(L, name).argtypes = [vp, vp] if name != "ymref_transforms" else [vp, vp, vp]
+        L.ymref_geometry_triangle_count.restype = ctypes.c_int64
+        L.ymref_geometry_triangle_count.argtypes = [vp, ctypes.c_uint32]
+        L.ymref_geometry_triangles.argtypes = [vp, ctypes.c_uint32, vp]
+        L.ymref_lights.argtypes = [vp, vp, vp, vp]
+        L.ymref_camera_bytes.argtypes = [vp, vp, i]
+        L.ymref_trace.argtypes = [vp, i, vp, vp, vp, vp, vp, vp, vp, vp, vp]
+        L.ymref_occluded.argtypes = [vp, i, vp, vp, vp, vp]
+        L.ymref_halton.argtypes = [vp, i, vp, vp, vp, i, vp, vp, vp]
+        L.ymref_render_frame.argtypes = [vp, i, i, i, i, i, vp]
+        L.ymref_last_render_seconds.restype = ctypes.c_double
+        L.ymref_last_render_seconds.argtypes = [vp]
+        L.ymref_accumulate.argtypes = [vp, vp, i, i, i]
+        _lib = L
+    return _lib
+
+
+def _p(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+class RefScene:
+    """One scene loaded and prepared by the reference's own scene module."""
+
+    def __init__(self, path: str, halton_perm: np.ndarray, width: int, height: int):
+        L = lib()
+        perm = np.ascontiguousarray(halton_perm, dtype=np.uint32)
+        self.width, self.height = width, height
+        self.h = L.ymref_scene_load(path.encode(), _p(perm), perm.size, width, height)
+        if not self.h:
+            raise RuntimeError(f"reference failed to load {path}")
+        self._perm = perm
+
+    def close(self):
+        if self.h:
+            lib().ymref_scene_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_settings(self, spp=1, ray_depth=8, sampler_type=1, shape_light=1, distant_light=0, volume=0,
+                     env_light=0, russian_roulette=0, indirect_clamp=0, indirect_limit=10.0):
+        s = Settings(spp, ray_depth, sampler_type, shape_light, distant_light, volume, env_light,
+                     russian_roulette, indirect_clamp, indirect_limit)
+        lib().ymref_set_settings(self.h, ctypes.byref(s))
+
+    def counts(self) -> dict:
+        out = np.zeros(5, np.uint32)
+        lib().ymref_scene_counts(self.h, _p(out))
+        return dict(zip(["instances", "geometries", "lights", "transforms", "materials"], out.tolist()))
+
+    def instances(self) -> np.ndarray:
+        n = self.counts()["instances"]
+        out = np.zeros((n, 6), np.uint32)
+        lib().ymref_instances(self.h, _p(out))
+        return out
+
+    def geometry_triangles(self, g: int) -> np.ndarray:
+        n = lib().ymref_geometry_triangle_count(self.h, g)
+        out = np.zeros((max(n, 0), 3), np.uint32)
+        if n > 0:
+            lib().ymref_geometry_triangles(self.h, g, _p(out))
+        return out
+
+    def lights(self):
+        n = self.counts()["lights"]
+        ids = np.zeros((n, 2), np.uint32)
+        pa = np.zeros((n, 2), np.float32)
+        tab = np.zeros(n, np.float32)
+        lib().ymref_lights(self.h, _p(ids), _p(pa), _p(tab))
+        return ids, pa, tab
+
+    def transforms(self):
+        n = self.counts()["transforms"]
+        fwd = np.zeros((n, 16), np.float32)
+        inv = np.zeros((n, 16), np.float32)
+        lib().ymref_transforms(self.h, _p(fwd), _p(inv))
+        return fwd, inv
+
+    def camera_bytes(self) -> bytes:
+        buf = np.zeros(512, np.uint8)
+        n = lib().ymref_camera_bytes(self.h, _p(buf), buf.size)
+        return buf[:n].tobytes()
+
+    def trace(self, origins, dirs, last_hit=None) -> dict:
+        o = np.ascontiguousarray(origins, np.float32)
+        d = np.ascontiguousarray(dirs, np.float32)
+        n = o.shape[0]
+        lh = None if last_hit is None else np.ascontiguousarray(last_hit, np.uint32)
+        inst = np.zeros(n, np.uint32)
+        tri = np.zeros(n, np.uint32)
+        t = np.zeros(n, np.float32)
+        bary = np.zeros((n, 3), np.float32)
+        back = np.zeros(n, np.int32)
+        nearby = np.zeros(n, np.int32)
+        lib().ymref_trace(self.h, n, _p(o), _p(d), None if lh is None else _p(lh), _p(inst), _p(tri), _p(t),
+                          _p(bary), _p(back), _p(nearby))
+        return {"inst": inst, "tri": tri, "t": t, "bary": bary, "back": back, "nearby": nearby}
+
+    def occluded(self, origins, dirs, tmax) -> np.ndarray:
+        o = np.ascontiguousarray(origins, np.float32)
+        d = np.ascontiguousarray(dirs, np.float32)
+        tm = np.ascontiguousarray(tmax, np.float32)
+        out = np.zeros(o.shape[0], np.int32)
+        lib().ymref_occluded(self.h, o.shape[0], _p(o), _p(d), _p(tm), _p(out))
+        return out
+
+    def halton(self, px, py, sample, n_dims: int):
+        px = np.ascontiguousarray(px, np.int32)
+        py = np.ascontiguousarray(py, np.int32)
+        sm = np.ascontiguousarray(sample, np.int32)
+        n = px.size
+        idx = np.zeros(n, np.uint64)
+        off = np.zeros((n, 2), np.float32)
+        dims = np.zeros((n, n_dims), np.float32)
+        lib().ymref_halton(self.h, n, _p(px), _p(py), _p(sm), n_dims, _p(idx), _p(off), _p(dims))
+        return idx, off, dims
+
+    def render_frame(self, frame_index: int = 1, tile_begin: int = 0, tile_end: int = 0,
+                     wave_capacity: int = 1 << 18, threads: int | None = None) -> np.ndarray:
+        out = np.zeros((self.height, self.width, 4), np.float32)
+        threads = threads or os.cpu_count() or 1
+        rc = lib().ymref_render_frame(self.h, frame_index, tile_begin, tile_end, wave_capacity, threads, _p(out))
+        if rc != 0:
+            raise RuntimeError(f"reference render failed ({rc})")
+        return out
+
+    def last_render_seconds(self) -> float:
+        return lib().ymref_last_render_seconds(self.h)

@@ -1,0 +1,463 @@
+// Headless host driver for the YMRT reference (the oracle).
+//
+// TEST INFRASTRUCTURE ONLY. Built by oracle/build_ref.py into
+// oracle/_ref/libymrt_ref.so from the reference sources where they lie; only
+// tests/, __graft_entry__.smoke() and bench.py's CPU-baseline/reference legs
+// load it. The ymrt_b200 product never links or calls it.
+//
+// What it does: loads a .ymtmp scene with the reference's own parser and scene
+// module (src/core/YMParser.cpp:2330 SceneParser::parsing_scene), prepares the
+// scene exactly as the reference editor does before rendering
+// (src/core/GuiModule.cpp:116-282 GuiModule::UpdateScene: top-level BVH build
+// with instance reordering, shape-light table, camera ray-transfer), and runs
+// the reference's three wavefront stage kernels (src/Shading.cu:1634
+// Ray_generation_path_tracing, :1765 Ray_trace_path_tracing, :1953
+// Ray_shading_path_tracing) as host functions with the wave protocol of
+// src/core/RenderModule.cpp:494-653 (PathTracingExecuteTask). Blocks of each
+// emulated launch are spread over host threads; threadIdx/blockIdx are
+// thread_local.
+//
+// The wave capacity is a parameter (the reference uses 1 Mi rays). Each
+// path's result is independent of how paths are packed into waves, so the
+// per-pixel output equals the reference's up to the order of the per-pixel
+// float additions when spp > 1.
+#include YMRT_SHADING_SOURCE
+
+#include "core/SceneModule.h"
+#include "core/YMParser.h"
+
+#include <atomic>
+#include <chrono>
+#include <thread>
+
+thread_local uint3 threadIdx;
+thread_local uint3 blockIdx;
+thread_local dim3 blockDim;
+thread_local dim3 gridDim;
+
+namespace YMRT {
+
+// SceneModule names GuiModule as a friend (src/core/SceneModule.h:87). The
+// oracle is not linked with the GUI, so this class stands in for the part of
+// GuiModule::UpdateScene that prepares a freshly parsed scene for rendering.
+class GuiModule {
+ public:
+  static bool PrepareScene(SceneModule& m, const uint32_t* halton_perm, size_t perm_len, int width,
+                           int height, std::vector<uint32_t>* instance_old_index) {
+    std::unordered_map<uint32_t, uint32_t> dst_indices_map;
+    TopBVHBuilder builder(m.primitive_instances.data(), (uint32_t)m.primitive_instances.size(),
+                          m.transforms.data(), m.geometries.data());
+    m.top_nodes.clear();
+    builder.BuildSceneBVH(m.top_nodes, nullptr, nullptr, &dst_indices_map);
+    for (auto& item : m.primitive_index_to_index_map) item.second = dst_indices_map[item.second];
+    instance_old_index->assign(m.primitive_instances.size(), EMPTY_UINT32);
+    for (auto& kv : dst_indices_map) (*instance_old_index)[kv.second] = kv.first;
+
+    m.shape_lights.clear();
+    m.shape_light_sample_table.clear();
+    m.LoadShapeLight();
+
+    m.permute_table.assign(halton_perm, halton_perm + perm_len);
+
+    m.camera[EDITOR_CAMERA_INDEX].InitCameraRayTransfer(m.GetHostSceneDataPointer());
+    std::memcpy(&m.camera[RENDERING_CAMERA_INDEX], &m.camera[EDITOR_CAMERA_INDEX], sizeof(Camera));
+    m.camera[RENDERING_CAMERA_INDEX].m_width = width;
+    m.camera[RENDERING_CAMERA_INDEX].m_height = height;
+    m.camera[RENDERING_CAMERA_INDEX].SetAspectRatio(float(width) / float(height));
+    return true;
+  }
+  static Scene HostScene(SceneModule& m) { return m.GetHostSceneDataPointer(); }
+  static std::vector<GeometryData>& Geometries(SceneModule& m) { return m.geometries; }
+  static std::vector<PrimitiveInstance>& Instances(SceneModule& m) { return m.primitive_instances; }
+  static std::vector<ShapeLight>& Lights(SceneModule& m) { return m.shape_lights; }
+  static std::vector<float>& LightTable(SceneModule& m) { return m.shape_light_sample_table; }
+  static std::vector<glm::mat4>& Transforms(SceneModule& m) { return m.transforms; }
+  static std::vector<glm::mat4>& InvTransforms(SceneModule& m) { return m.i_transforms; }
+  static std::vector<Material>& Materials(SceneModule& m) { return m.materials; }
+  static Camera* Cameras(SceneModule& m) { return m.camera; }
+};
+
+}  // namespace YMRT
+
+using namespace YMRT;
+
+namespace {
+
+struct Queues {
+  std::vector<Ray> s_ray;
+  std::vector<glm::vec3> s_light, s_tp;
+  std::vector<int> s_px, s_py, s_depth, s_never, s_cam, s_psi;
+  std::vector<RandomSampler> s_sampler;
+  std::vector<RayTransfer> s_transfer;
+
+  std::vector<HitRecord> h_rec;
+  std::vector<int> h_nearby_count;
+  std::vector<uint32_t> h_nearby_prim;
+  std::vector<float> h_nearby_t;
+  std::vector<int> h_nearby_back;
+  std::vector<float> h_vol_w;
+  std::vector<Ray> h_ray;
+  std::vector<glm::vec3> h_light, h_tp;
+  std::vector<int> h_px, h_py, h_depth, h_never, h_cam, h_psi;
+  std::vector<RandomSampler> h_sampler;
+  std::vector<RayTransfer> h_transfer;
+
+  void Resize(size_t n) {
+    const size_t nb = MAX_BOUNDARY_RECORD + 2;
+    s_ray.resize(n); s_light.resize(n); s_tp.resize(n); s_px.resize(n); s_py.resize(n);
+    s_depth.resize(n); s_never.resize(n); s_cam.resize(n); s_psi.resize(n);
+    s_sampler.resize(n); s_transfer.resize(n);
+    h_rec.resize(n); h_nearby_count.resize(n); h_nearby_prim.resize(n * nb); h_nearby_t.resize(n * nb);
+    h_nearby_back.resize(n * nb); h_vol_w.resize(n * MAX_BOUNDARY_RECORD);
+    h_ray.resize(n); h_light.resize(n); h_tp.resize(n); h_px.resize(n); h_py.resize(n);
+    h_depth.resize(n); h_never.resize(n); h_cam.resize(n); h_psi.resize(n);
+    h_sampler.resize(n); h_transfer.resize(n);
+  }
+};
+
+struct RefContext {
+  std::shared_ptr<SceneModule> module;
+  Scene scene{};
+  RenderSetting setting;
+  int width = 0, height = 0;
+  std::vector<uint32_t> instance_old_index;
+  Queues q;
+  size_t capacity = 0;
+  double last_render_seconds = 0.0;
+};
+
+// Runs `body` once per emulated CUDA thread of a 1-D launch of `count` threads
+// in blocks of `block`, spreading whole blocks over `n_threads` host threads.
+template <typename F>
+void Launch(uint32_t count, uint32_t block, int n_threads, const F& body) {
+  if (count == 0) return;
+  const uint32_t n_blocks = (count + block - 1) / block;
+  std::atomic<uint32_t> next_block(0);
+  auto worker = [&]() {
+    blockDim = dim3(block, 1, 1);
+    gridDim = dim3(n_blocks, 1, 1);
+    for (;;) {
+      const uint32_t b = next_block.fetch_add(1);
+      if (b >= n_blocks) break;
+      blockIdx = make_uint3(b, 0, 0);
+      for (uint32_t t = 0; t < block; ++t) {
+        threadIdx = make_uint3(t, 0, 0);
+        body();
+      }
+    }
+  };
+  if (n_threads <= 1 || n_blocks == 1) {
+    worker();
+    return;
+  }
+  std::vector<std::thread> pool;
+  const int n = std::min<int>(n_threads, (int)n_blocks);
+  for (int i = 0; i < n; ++i) pool.emplace_back(worker);
+  for (auto& th : pool) th.join();
+}
+
+}  // namespace
+
+extern "C" {
+
+// Settings block passed from Python; mirrors the fields of the reference's
+// RenderSetting (src/SceneDefines.h:17-40) that the stage kernels read.
+struct YmrefSettings {
+  int spp;
+  int ray_depth;
+  int sampler_type;
+  int enable_shape_light;
+  int enable_distant_light;
+  int enable_volume_scattering;
+  int enable_env_light;
+  int enable_russian_roulette;
+  int enable_indirect_clamp;
+  float indirect_limit;
+};
+
+size_t ymref_halton_table_size() {
+  size_t total = 0;
+  for (uint32_t i = 0; i < prime_count; ++i) total += primes[i];
+  return total;
+}
+
+void* ymref_scene_load(const char* path, const uint32_t* halton_perm, size_t perm_len, int width, int height) {
+  if (perm_len != ymref_halton_table_size() || width <= 0 || height <= 0) return nullptr;
+  auto ctx = new RefContext();
+  ctx->module = std::make_shared<SceneModule>();
+  SceneParser parser;
+  if (!parser.parsing_scene(path, ctx->module)) {
+    delete ctx;
+    return nullptr;
+  }
+  GuiModule::PrepareScene(*ctx->module, halton_perm, perm_len, width, height, &ctx->instance_old_index);
+  ctx->scene = GuiModule::HostScene(*ctx->module);
+  ctx->scene.render_setting = &ctx->setting;
+  ctx->width = width;
+  ctx->height = height;
+  return ctx;
+}
+
+void ymref_scene_free(void* handle) { delete static_cast<RefContext*>(handle); }
+
+void ymref_set_settings(void* handle, const YmrefSettings* s) {
+  auto ctx = static_cast<RefContext*>(handle);
+  RenderSetting& r = ctx->setting;
+  r.ssp = s->spp;
+  r.ray_depth = s->ray_depth;
+  r.sampler_type = s->sampler_type;
+  r.enable_shape_light = s->enable_shape_light;
+  r.enable_distant_light = s->enable_distant_light != 0;
+  r.enable_volume_scattering = s->enable_volume_scattering != 0;
+  r.enable_env_light = s->enable_env_light != 0;
+  r.enable_russian_roulette = s->enable_russian_roulette != 0;
+  r.enable_indirect_clamp = s->enable_indirect_clamp != 0;
+  r.indirect_limit = s->indirect_limit;
+}
+
+// Scene facts after the reference's preparation, for comparing host-side scene
+// preparation (instance order, triangle order, light table) with ymrt_b200.
+int ymref_scene_counts(void* handle, uint32_t* out /* [instances, geometries, lights, transforms, materials] */) {
+  auto ctx = static_cast<RefContext*>(handle);
+  out[0] = ctx->scene.primitive_instance_count;
+  out[1] = ctx->scene.geometry_count;
+  out[2] = ctx->scene.shape_light_count;
+  out[3] = ctx->scene.transform_count;
+  out[4] = ctx->scene.material_count;
+  return 0;
+}
+
+// Per instance (reference order): geometry, transform, material, volume,
+// boundary flag, and the instance's index in file order.
+int ymref_instances(void* handle, uint32_t* out /* 6 per instance */) {
+  auto ctx = static_cast<RefContext*>(handle);
+  auto& inst = GuiModule::Instances(*ctx->module);
+  for (size_t i = 0; i < inst.size(); ++i) {
+    out[6 * i + 0] = inst[i].geometry_idx;
+    out[6 * i + 1] = inst[i].transform_idx;
+    out[6 * i + 2] = inst[i].material_idx;
+    out[6 * i + 3] = (uint32_t)inst[i].inner_volume_idx;
+    out[6 * i + 4] = (uint32_t)inst[i].treat_as_boundary;
+    out[6 * i + 5] = ctx->instance_old_index[i];
+  }
+  return 0;
+}
+
+// Triangle count of a mesh geometry (or -1).
+int64_t ymref_geometry_triangle_count(void* handle, uint32_t g) {
+  auto ctx = static_cast<RefContext*>(handle);
+  auto& geo = GuiModule::Geometries(*ctx->module);
+  if (g >= geo.size() || geo[g].geometry_type != TRIANGLE_MESH) return -1;
+  return geo[g].triangle_mesh.triangle_count;
+}
+
+// The geometry's triangles after the reference's bottom-level BVH build
+// (src/BottomBVH.cpp:155-161 reorders them): three corner indices each.
+int ymref_geometry_triangles(void* handle, uint32_t g, uint32_t* out) {
+  auto ctx = static_cast<RefContext*>(handle);
+  auto& geo = GuiModule::Geometries(*ctx->module);
+  if (g >= geo.size() || geo[g].geometry_type != TRIANGLE_MESH) return -1;
+  const Triangle* tris = geo[g].triangle_mesh.GetTrianglesHost();
+  for (int64_t i = 0; i < geo[g].triangle_mesh.triangle_count; ++i) {
+    out[3 * i + 0] = tris[i].id0;
+    out[3 * i + 1] = tris[i].id1;
+    out[3 * i + 2] = tris[i].id2;
+  }
+  return 0;
+}
+
+// Shape lights (instance, triangle, power, area) and the power CDF table.
+int ymref_lights(void* handle, uint32_t* ids /* 2 per light */, float* power_area /* 2 per light */,
+                 float* table) {
+  auto ctx = static_cast<RefContext*>(handle);
+  auto& lights = GuiModule::Lights(*ctx->module);
+  auto& tab = GuiModule::LightTable(*ctx->module);
+  for (size_t i = 0; i < lights.size(); ++i) {
+    ids[2 * i] = lights[i].instance_idx;
+    ids[2 * i + 1] = lights[i].triangle_idx;
+    power_area[2 * i] = lights[i].power;
+    power_area[2 * i + 1] = lights[i].area;
+    table[i] = tab[i];
+  }
+  return 0;
+}
+
+// Object-to-world and world-to-object matrices, 16 floats each, column major.
+int ymref_transforms(void* handle, float* fwd, float* inv) {
+  auto ctx = static_cast<RefContext*>(handle);
+  auto& t = GuiModule::Transforms(*ctx->module);
+  auto& it = GuiModule::InvTransforms(*ctx->module);
+  std::memcpy(fwd, t.data(), t.size() * sizeof(glm::mat4));
+  std::memcpy(inv, it.data(), it.size() * sizeof(glm::mat4));
+  return 0;
+}
+
+// The rendering camera after preparation, as raw bytes of the reference's
+// Camera struct (176 bytes on x86-64).
+int ymref_camera_bytes(void* handle, uint8_t* out, int out_len) {
+  auto ctx = static_cast<RefContext*>(handle);
+  if (out_len < (int)sizeof(Camera)) return -(int)sizeof(Camera);
+  std::memcpy(out, &GuiModule::Cameras(*ctx->module)[RENDERING_CAMERA_INDEX], sizeof(Camera));
+  return (int)sizeof(Camera);
+}
+
+// Closest-hit queries through the reference's TraceRay
+// (src/ShadingUtilities.cuh:310). Rays are built with the reference's Ray
+// constructor (which normalises the direction). Outputs per ray: instance,
+// triangle, t, barycentrics (3), back-face flag, nearby-hit count.
+int ymref_trace(void* handle, int n, const float* origin, const float* dir, const uint32_t* last_hit /* 2 per ray or null */,
+                uint32_t* inst, uint32_t* tri, float* t, float* bary, int* back, int* nearby) {
+  auto ctx = static_cast<RefContext*>(handle);
+  for (int i = 0; i < n; ++i) {
+    Ray ray(glm::vec3(origin[3 * i], origin[3 * i + 1], origin[3 * i + 2]),
+            glm::vec3(dir[3 * i], dir[3 * i + 1], dir[3 * i + 2]),
+            last_hit ? last_hit[2 * i] : EMPTY_UINT32, last_hit ? last_hit[2 * i + 1] : EMPTY_UINT32);
+    HitRecord rec;
+    int nearby_count = 0;
+    NearbyHit nearby_hits[MAX_BOUNDARY_RECORD + 2];
+    const bool hit = TraceRay(ctx->scene, ray, &rec, &nearby_count, nearby_hits);
+    inst[i] = hit ? rec.hit_instance_idx : EMPTY_UINT32;
+    tri[i] = hit ? rec.hit_triangle_idx : EMPTY_UINT32;
+    t[i] = hit ? rec.hit_t : TMAX;
+    bary[3 * i] = rec.hit_barycentric.x;
+    bary[3 * i + 1] = rec.hit_barycentric.y;
+    bary[3 * i + 2] = rec.hit_barycentric.z;
+    back[i] = rec.hit_back;
+    nearby[i] = nearby_count;
+  }
+  return 0;
+}
+
+// Any-hit occlusion through the reference's BVHTraverseShadow
+// (src/ShadingUtilities.cuh:563) with ray.t = tmax.
+int ymref_occluded(void* handle, int n, const float* origin, const float* dir, const float* tmax, int* occluded) {
+  auto ctx = static_cast<RefContext*>(handle);
+  for (int i = 0; i < n; ++i) {
+    Ray ray(glm::vec3(origin[3 * i], origin[3 * i + 1], origin[3 * i + 2]),
+            glm::vec3(dir[3 * i], dir[3 * i + 1], dir[3 * i + 2]));
+    ray.t = tmax[i];
+    HitRecord rec;
+    occluded[i] = BVHTraverseShadow(ctx->scene, ray, &rec) ? 1 : 0;
+  }
+  return 0;
+}
+
+// Halton sampler known-answer values: for each (px, py, sample) the global
+// sample index (src/HaltonEnumerator.h:43 GetIndex), the pixel offset as the
+// ray-generation stage computes it (src/Shading.cu:1698-1704) and the first
+// n_dims scrambled dimensions starting at dimension 2
+// (src/RandomSampler.cuh:430 Random1D).
+int ymref_halton(void* handle, int n, const int* px, const int* py, const int* sample, int n_dims,
+                 uint64_t* index, float* offset, float* dims) {
+  auto ctx = static_cast<RefContext*>(handle);
+  HaltonEnumerator he(ctx->width, ctx->height);
+  for (int i = 0; i < n; ++i) {
+    const uint64_t sample_index = he.GetIndex(px[i], py[i], sample[i]);
+    index[i] = sample_index;
+    RandomSampler sampler;
+    sampler.InitHaltonSampler(sample_index, 2, ctx->scene.sampler_data.halton_permute_table);
+    glm::vec2 pixel_offset = sampler.SamplePixelOffset();
+    pixel_offset.x = he.ScaleX(pixel_offset.x) - float(px[i]);
+    pixel_offset.y = he.ScaleY(pixel_offset.y) - float(py[i]);
+    pixel_offset = glm::clamp(pixel_offset, glm::vec2(0.000001f), glm::vec2(0.999999f));
+    offset[2 * i] = pixel_offset.x;
+    offset[2 * i + 1] = pixel_offset.y;
+    for (int d = 0; d < n_dims; ++d) dims[(size_t)i * n_dims + d] = sampler.Random1D();
+  }
+  return 0;
+}
+
+// One progressive frame of the path-tracing view over tiles
+// [tile_begin, tile_end) (tile_end <= 0 means all tiles), accumulated into
+// out_rgba (width*height*4 floats, zeroed here) exactly as the reference's
+// noise image. Returns 0, or -1 on bad arguments.
+int ymref_render_frame(void* handle, int frame_index, int tile_begin, int tile_end, int wave_capacity,
+                       int n_threads, float* out_rgba) {
+  auto ctx = static_cast<RefContext*>(handle);
+  const RenderSetting& rs = ctx->setting;
+  const uint32_t spp = (uint32_t)std::max(rs.ssp, 1);
+  const uint32_t w = ctx->width, h = ctx->height;
+  const uint32_t tiles_x = (w + TILE_X_RES - 1) / TILE_X_RES;
+  const uint32_t tiles_y = (h + TILE_Y_RES - 1) / TILE_Y_RES;
+  const uint32_t total_tiles = tiles_x * tiles_y;
+  const uint32_t t_end = tile_end <= 0 ? total_tiles : std::min<uint32_t>(tile_end, total_tiles);
+  const uint32_t rays_per_tile = TILE_PIXEL_COUNT * spp;
+  if (frame_index < 1 || wave_capacity < (int)rays_per_tile || tile_begin < 0) return -1;
+  const size_t cap = (size_t)wave_capacity;
+  if (ctx->capacity < cap) {
+    ctx->q.Resize(cap);
+    ctx->capacity = cap;
+  }
+  Queues& q = ctx->q;
+  std::memset(out_rgba, 0, sizeof(float) * 4 * w * h);
+  glm::vec4* noise = reinterpret_cast<glm::vec4*>(out_rgba);
+  HaltonEnumerator halton(w, h);
+  RayCounter counter{0, 0, 0};
+  RayCounter host_counter{0, 0, 0};
+  const Scene* scene = &ctx->scene;
+  uint32_t next_tile = (uint32_t)tile_begin;
+  const auto t0 = std::chrono::steady_clock::now();
+
+  while (host_counter.shading_ray_counter > 0 || next_tile < t_end) {
+    const uint32_t tiles_this_batch =
+        std::min<uint32_t>((uint32_t)((cap - host_counter.shading_ray_counter) / rays_per_tile), t_end - next_tile);
+    const uint32_t gen_count = tiles_this_batch * rays_per_tile;
+    counter.shading_ray_counter = host_counter.shading_ray_counter;
+    Launch(gen_count, STAGE_RAY_GEN_BLOCK_SIZE, n_threads, [&]() {
+      Ray_generation_path_tracing(frame_index, scene, &halton, &counter, next_tile, gen_count, spp, w, h, tiles_x,
+                                  tiles_y, q.s_ray.data(), q.s_light.data(), q.s_tp.data(), q.s_px.data(),
+                                  q.s_py.data(), q.s_depth.data(), q.s_never.data(), q.s_cam.data(),
+                                  q.s_psi.data(), q.s_sampler.data(), q.s_transfer.data());
+    });
+    next_tile += tiles_this_batch;
+    host_counter.shading_ray_counter += gen_count;
+
+    counter = host_counter;
+    const uint32_t trace_count = host_counter.shading_ray_counter;
+    Launch(trace_count, STAGE_RAY_TRACE_BLOCK_SIZE, n_threads, [&]() {
+      Ray_trace_path_tracing(frame_index, scene, &counter, trace_count, w, h, noise, q.s_ray.data(), q.s_light.data(),
+                             q.s_tp.data(), q.s_px.data(), q.s_py.data(), q.s_depth.data(), q.s_never.data(),
+                             q.s_cam.data(), q.s_psi.data(), q.s_sampler.data(), q.s_transfer.data(), q.h_rec.data(),
+                             q.h_nearby_count.data(), q.h_nearby_prim.data(), q.h_nearby_t.data(),
+                             q.h_nearby_back.data(), q.h_vol_w.data(), q.h_ray.data(), q.h_light.data(),
+                             q.h_tp.data(), q.h_px.data(), q.h_py.data(), q.h_depth.data(), q.h_never.data(),
+                             q.h_cam.data(), q.h_psi.data(), q.h_sampler.data(), q.h_transfer.data());
+    });
+    host_counter = counter;
+    host_counter.shading_ray_counter = 0;
+
+    counter = host_counter;
+    const uint32_t shade_count = host_counter.hit_counter;
+    Launch(shade_count, STAGE_RAY_SHADING_BLOCK_SIZE, n_threads, [&]() {
+      Ray_shading_path_tracing(frame_index, scene, &counter, shade_count, w, h, noise, q.s_ray.data(),
+                               q.s_light.data(), q.s_tp.data(), q.s_px.data(), q.s_py.data(), q.s_depth.data(),
+                               q.s_never.data(), q.s_cam.data(), q.s_psi.data(), q.s_sampler.data(),
+                               q.s_transfer.data(), q.h_rec.data(), q.h_nearby_count.data(), q.h_nearby_prim.data(),
+                               q.h_nearby_t.data(), q.h_nearby_back.data(), q.h_vol_w.data(), q.h_ray.data(),
+                               q.h_light.data(), q.h_tp.data(), q.h_px.data(), q.h_py.data(), q.h_depth.data(),
+                               q.h_never.data(), q.h_cam.data(), q.h_psi.data(), q.h_sampler.data(),
+                               q.h_transfer.data());
+    });
+    host_counter = counter;
+    host_counter.hit_counter = 0;
+    if (host_counter.shading_ray_counter > cap) return -2;  // queue overflow
+  }
+  ctx->last_render_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  return 0;
+}
+
+double ymref_last_render_seconds(void* handle) { return static_cast<RefContext*>(handle)->last_render_seconds; }
+
+// Running mean over frames, src/Shading.cu:2354 Accumulate_image_path_tracing.
+void ymref_accumulate(const float* noise, float* acc, int width, int height, int frame_index) {
+  for (int y = 0; y < height; ++y)
+    for (int x = 0; x < width; ++x) {
+      blockIdx = make_uint3(0, 0, 0);
+      blockDim = dim3(1, 1, 1);
+      threadIdx = make_uint3(x, y, 0);
+      Accumulate_image_path_tracing(reinterpret_cast<const glm::vec4*>(noise), reinterpret_cast<glm::vec4*>(acc),
+                                    width, height, frame_index);
+    }
+}
+
+}  // extern "C"

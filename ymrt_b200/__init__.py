@@ -1,0 +1,277 @@
+"""ymrt_b200: a B200-native (sm_100a) wavefront path tracer behind YMRT's
+scene format and stage interface.
+
+Python front end over the C ABI in ``include/ymrt.h`` (``libymrt.so``, built
+in-tree by ``ymrt_b200.build``). It mirrors the reference's host side
+(src/core/RenderModule.cpp, src/core/SceneModule.cpp): load a ``.ymtmp``
+scene, upload it, render progressive frames into a float4 noise image and
+accumulate them. There is no CPU rendering path: without a CUDA device or
+without the built library every render call raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+__all__ = [
+    "RenderSetting", "Stats", "YmrtError", "Context", "HostScene", "Scene", "library", "default_setting",
+    "HALTON_TABLE_SIZE",
+]
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libymrt.so")
+HALTON_TABLE_SIZE = 3682913  # sum of the first 1000 primes
+
+YMRT_OK = 0
+ERRORS = {
+    -1: "invalid argument", -2: "i/o error", -3: "malformed scene", -4: "unsupported", -5: "CUDA error",
+    -6: "out of memory", -7: "timeout", -8: "overflow", -9: "no CUDA device",
+}
+
+QUERY_COUNTS, QUERY_INSTANCES, QUERY_LIGHTS, QUERY_LIGHT_TABLE = 0, 1, 2, 3
+QUERY_TRANSFORMS, QUERY_CAMERA, QUERY_TRIANGLES = 4, 5, 6
+
+
+class YmrtError(RuntimeError):
+    def __init__(self, code: int, message: str):
+        super().__init__(f"{ERRORS.get(code, 'error')} ({code}): {message}")
+        self.code = code
+
+
+class RenderSetting(ctypes.Structure):
+    """Byte-compatible with the reference's RenderSetting (src/SceneDefines.h:17-40)."""
+    _fields_ = [
+        ("ssp", ctypes.c_int), ("ray_depth", ctypes.c_int), ("gamma", ctypes.c_float),
+        ("exposure", ctypes.c_float), ("max_frame_count", ctypes.c_int), ("sampler_type", ctypes.c_int),
+        ("enable_shape_light", ctypes.c_int), ("enable_distant_light", ctypes.c_uint8),
+        ("enable_volume_scattering", ctypes.c_uint8), ("enable_env_light", ctypes.c_uint8),
+        ("enable_russian_roulette", ctypes.c_uint8), ("enable_indirect_clamp", ctypes.c_uint8),
+        ("pad_", ctypes.c_uint8 * 3), ("indirect_limit", ctypes.c_float),
+    ]
+
+
+assert ctypes.sizeof(RenderSetting) == 40
+
+
+def default_setting(spp=1, ray_depth=8, shape_light=True, distant_light=False, volume=False, env_light=False,
+                    russian_roulette=False, indirect_clamp=False, indirect_limit=10.0) -> RenderSetting:
+    s = RenderSetting()
+    s.ssp, s.ray_depth, s.gamma, s.exposure, s.max_frame_count, s.sampler_type = spp, ray_depth, 2.2, 1.0, -1, 1
+    s.enable_shape_light = int(shape_light)
+    s.enable_distant_light, s.enable_volume_scattering, s.enable_env_light = int(distant_light), int(volume), int(env_light)
+    s.enable_russian_roulette, s.enable_indirect_clamp, s.indirect_limit = int(russian_roulette), int(indirect_clamp), indirect_limit
+    return s
+
+
+class Stats(ctypes.Structure):
+    _fields_ = [
+        ("paths", ctypes.c_uint64), ("extension_rays", ctypes.c_uint64), ("shadow_rays", ctypes.c_uint64),
+        ("waves", ctypes.c_uint64), ("ms_total", ctypes.c_double), ("ms_generate", ctypes.c_double),
+        ("ms_extend", ctypes.c_double), ("ms_shade", ctypes.c_double), ("device_errors", ctypes.c_uint32),
+        ("reserved_", ctypes.c_uint32),
+    ]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_ if not k.endswith("_")}
+
+
+_lib = None
+
+
+def library():
+    """Loads libymrt.so (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise YmrtError(-9, f"{LIB_PATH} is missing; run `python -m ymrt_b200.build`")
+    L = ctypes.CDLL(LIB_PATH)
+    vp, i, sz = ctypes.c_void_p, ctypes.c_int, ctypes.c_size_t
+    L.ymrt_create.argtypes = [i, ctypes.POINTER(vp)]
+    L.ymrt_destroy.argtypes = [vp]
+    L.ymrt_last_error.restype = ctypes.c_char_p
+    L.ymrt_last_error.argtypes = [vp]
+    L.ymrt_set_queue_capacity.argtypes = [vp, ctypes.c_uint32]
+    L.ymrt_scene_load_ymtmp.argtypes = [ctypes.c_char_p, i, i, ctypes.POINTER(vp), ctypes.c_char_p, sz]
+    L.ymrt_host_scene_free.argtypes = [vp]
+    L.ymrt_host_scene_query.restype = ctypes.c_longlong
+    L.ymrt_host_scene_query.argtypes = [vp, i, i, vp, sz]
+    L.ymrt_scene_upload.argtypes = [vp, vp, vp, sz, ctypes.POINTER(vp)]
+    L.ymrt_scene_free.argtypes = [vp]
+    L.ymrt_render_forward.argtypes = [vp, ctypes.POINTER(RenderSetting), i, vp, i, ctypes.POINTER(Stats)]
+    L.ymrt_render_tiles.argtypes = [vp, ctypes.POINTER(RenderSetting), i, i, i, vp, i, ctypes.POINTER(Stats)]
+    L.ymrt_accumulate.argtypes = [vp, vp, vp, i]
+    L.ymrt_debug_trace.argtypes = [vp, i, vp, vp, vp, vp, vp, vp, vp, vp, vp]
+    L.ymrt_debug_occluded.argtypes = [vp, i, vp, vp, vp, vp]
+    L.ymrt_debug_halton.argtypes = [vp, i, vp, vp, vp, i, vp, vp, vp]
+    _lib = L
+    return L
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(ctypes.c_void_p)
+
+
+def _check(rc: int, ctx=None):
+    if rc != YMRT_OK:
+        msg = library().ymrt_last_error(ctx).decode(errors="replace")
+        raise YmrtError(rc, msg)
+
+
+class Context:
+    """One CUDA device + stream (the reference's RenderModule path-tracing stream)."""
+
+    def __init__(self, device: int = 0, queue_capacity: int = 0):
+        self.h = ctypes.c_void_p()
+        _check(library().ymrt_create(device, ctypes.byref(self.h)))
+        if queue_capacity:
+            library().ymrt_set_queue_capacity(self.h, queue_capacity)
+
+    def close(self):
+        if self.h:
+            library().ymrt_destroy(self.h)
+            self.h = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class HostScene:
+    """A parsed and prepared .ymtmp scene (no GPU involved)."""
+
+    def __init__(self, path: str, width: int, height: int):
+        self.h = ctypes.c_void_p()
+        err = ctypes.create_string_buffer(1024)
+        rc = library().ymrt_scene_load_ymtmp(path.encode(), width, height, ctypes.byref(self.h), err, len(err))
+        if rc != YMRT_OK:
+            raise YmrtError(rc, err.value.decode(errors="replace"))
+        self.width, self.height = width, height
+
+    def close(self):
+        if self.h:
+            library().ymrt_host_scene_free(self.h)
+            self.h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _query(self, what, dtype, index=0):
+        L = library()
+        n = L.ymrt_host_scene_query(self.h, what, index, None, 0)
+        if n < 0:
+            raise YmrtError(int(n), "query failed")
+        out = np.zeros(int(n), dtype=dtype)
+        if n:
+            L.ymrt_host_scene_query(self.h, what, index, _p(out), int(n))
+        return out
+
+    def counts(self) -> dict:
+        c = self._query(QUERY_COUNTS, np.uint64)
+        keys = ["instances", "meshes", "triangles", "instanced_triangles", "lights", "blas_nodes", "tlas_nodes", "materials"]
+        return dict(zip(keys, (int(x) for x in c)))
+
+    def instances(self) -> np.ndarray:
+        return self._query(QUERY_INSTANCES, np.uint32).reshape(-1, 6)
+
+    def lights(self):
+        raw = self._query(QUERY_LIGHTS, np.float32).reshape(-1, 4)
+        ids = raw[:, :2].copy().view(np.uint32)
+        return ids, raw[:, 2:].copy(), self._query(QUERY_LIGHT_TABLE, np.float32)
+
+    def transforms(self):
+        t = self._query(QUERY_TRANSFORMS, np.float32).reshape(-1, 32)
+        return t[:, :16].copy(), t[:, 16:].copy()
+
+    def camera(self) -> np.ndarray:
+        return self._query(QUERY_CAMERA, np.float32)
+
+    def triangles(self, mesh: int) -> np.ndarray:
+        return self._query(QUERY_TRIANGLES, np.uint32, mesh).reshape(-1, 3)
+
+
+class Scene:
+    """A scene resident on the device of a Context."""
+
+    def __init__(self, ctx: Context, host: HostScene, halton_perm: np.ndarray):
+        self.ctx = ctx
+        self.width, self.height = host.width, host.height
+        perm = np.ascontiguousarray(halton_perm, dtype=np.uint32)
+        self.h = ctypes.c_void_p()
+        _check(library().ymrt_scene_upload(ctx.h, host.h, _p(perm), perm.size, ctypes.byref(self.h)), ctx.h)
+        self.host = host
+
+    def close(self):
+        if self.h:
+            library().ymrt_scene_free(self.h)
+            self.h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def render(self, setting: RenderSetting, frame_index: int = 1, out=None, tile_begin: int = 0, tile_end: int = 0):
+        """Renders one frame. `out`: None (returns a new host array), a host
+        numpy float32 (H, W, 4) array, or a torch CUDA tensor of that shape."""
+        stats = Stats()
+        on_device = 0
+        if out is None:
+            out = np.zeros((self.height, self.width, 4), np.float32)
+        if isinstance(out, np.ndarray):
+            assert out.dtype == np.float32 and out.flags.c_contiguous and out.size == self.width * self.height * 4
+            ptr = _p(out)
+        else:  # torch tensor on the device
+            assert out.is_cuda and out.is_contiguous() and out.numel() == self.width * self.height * 4
+            ptr = ctypes.c_void_p(out.data_ptr())
+            on_device = 1
+        rc = library().ymrt_render_tiles(self.h, ctypes.byref(setting), frame_index, tile_begin, tile_end, ptr,
+                                         on_device, ctypes.byref(stats))
+        _check(rc, self.ctx.h)
+        return out, stats
+
+    def trace(self, origins, dirs, last_hit=None) -> dict:
+        o = np.ascontiguousarray(origins, np.float32)
+        d = np.ascontiguousarray(dirs, np.float32)
+        n = o.shape[0]
+        lh = None if last_hit is None else np.ascontiguousarray(last_hit, np.uint32)
+        inst, tri = np.zeros(n, np.uint32), np.zeros(n, np.uint32)
+        t, bary = np.zeros(n, np.float32), np.zeros((n, 3), np.float32)
+        back, nearby = np.zeros(n, np.int32), np.zeros(n, np.int32)
+        _check(library().ymrt_debug_trace(self.h, n, _p(o), _p(d), _p(lh), _p(inst), _p(tri), _p(t), _p(bary),
+                                          _p(back), _p(nearby)), self.ctx.h)
+        return {"inst": inst, "tri": tri, "t": t, "bary": bary, "back": back, "nearby": nearby}
+
+    def occluded(self, origins, dirs, tmax) -> np.ndarray:
+        o = np.ascontiguousarray(origins, np.float32)
+        d = np.ascontiguousarray(dirs, np.float32)
+        tm = np.ascontiguousarray(tmax, np.float32)
+        out = np.zeros(o.shape[0], np.int32)
+        _check(library().ymrt_debug_occluded(self.h, o.shape[0], _p(o), _p(d), _p(tm), _p(out)), self.ctx.h)
+        return out
+
+    def halton(self, px, py, sample, n_dims: int):
+        px = np.ascontiguousarray(px, np.int32)
+        py = np.ascontiguousarray(py, np.int32)
+        sm = np.ascontiguousarray(sample, np.int32)
+        n = px.size
+        idx = np.zeros(n, np.uint64)
+        off = np.zeros((n, 2), np.float32)
+        dims = np.zeros((n, max(n_dims, 1)), np.float32)
+        _check(library().ymrt_debug_halton(self.h, n, _p(px), _p(py), _p(sm), n_dims, _p(idx), _p(off), _p(dims)),
+               self.ctx.h)
+        return idx, off, dims[:, :n_dims]

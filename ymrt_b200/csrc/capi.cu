@@ -1,0 +1,616 @@
+// C ABI of ymrt_b200 (include/ymrt.h): contexts, scene upload, the frame
+// loop that drives the wavefront kernels, and the known-answer entry points.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <functional>
+#include <memory>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/ymrt.h"
+#include "kernels.h"
+#include "scene_host.h"
+
+using namespace ym;
+
+struct ymrt_host_scene {
+  HostScene s;
+};
+
+namespace {
+
+thread_local std::string g_last_error;
+
+struct DeviceBuffer {
+  void* ptr = nullptr;
+  size_t bytes = 0;
+  ~DeviceBuffer() { release(); }
+  void release() {
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    bytes = 0;
+  }
+  cudaError_t ensure(size_t n) {
+    if (n <= bytes && ptr) return cudaSuccess;
+    release();
+    cudaError_t e = cudaMalloc(&ptr, n ? n : 16);
+    if (e == cudaSuccess) bytes = n;
+    return e;
+  }
+  template <typename T>
+  T* as() const {
+    return static_cast<T*>(ptr);
+  }
+};
+
+std::vector<uint32_t> first_primes(int n) {
+  std::vector<uint32_t> p;
+  for (uint32_t c = 2; (int)p.size() < n; ++c) {
+    bool prime = true;
+    for (uint32_t q : p) {
+      if (q * q > c) break;
+      if (c % q == 0) {
+        prime = false;
+        break;
+      }
+    }
+    if (prime) p.push_back(c);
+  }
+  return p;
+}
+
+}  // namespace
+
+struct ymrt_context {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  std::string error;
+  uint32_t capacity = 1u << 21;
+  // two path pools (ping-pong), one hit pool, counters
+  DeviceBuffer pool_buf[2], hit_buf, counters_buf, image_buf;
+  PathPool pool[2]{};
+  HitPool hits{};
+  uint32_t pool_capacity = 0;
+  WaveCounters* counters_host = nullptr;  // pinned
+  cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
+  std::vector<uint32_t> primes, prime_sums;
+
+  int fail(int code, const std::string& msg) {
+    error = msg;
+    g_last_error = msg;
+    return code;
+  }
+  int cuda_fail(cudaError_t e, const char* what) {
+    return fail(e == cudaErrorMemoryAllocation ? YMRT_ERR_OOM : YMRT_ERR_CUDA,
+                std::string(what) + ": " + cudaGetErrorString(e));
+  }
+
+  int ensure_pools() {
+    if (pool_capacity == capacity) return YMRT_OK;
+    const size_t n = capacity;
+    const size_t pool_bytes = n * (4 * sizeof(float4) + 2 * sizeof(uint2) + sizeof(uint4) + sizeof(RayTransfer) + 16);
+    for (int k = 0; k < 2; ++k) {
+      cudaError_t e = pool_buf[k].ensure(pool_bytes);
+      if (e != cudaSuccess) return cuda_fail(e, "allocating path pool");
+      char* p = pool_buf[k].as<char>();
+      PathPool& P = pool[k];
+      P.ray_o = reinterpret_cast<float4*>(p); p += n * sizeof(float4);
+      P.ray_d = reinterpret_cast<float4*>(p); p += n * sizeof(float4);
+      P.throughput = reinterpret_cast<float4*>(p); p += n * sizeof(float4);
+      P.radiance = reinterpret_cast<float4*>(p); p += n * sizeof(float4);
+      P.sampler = reinterpret_cast<uint4*>(p); p += n * sizeof(uint4);
+      P.pixel_flags = reinterpret_cast<uint2*>(p); p += n * sizeof(uint2);
+      P.last_hit = reinterpret_cast<uint2*>(p); p += n * sizeof(uint2);
+      P.transfer = reinterpret_cast<RayTransfer*>(p); p += n * sizeof(RayTransfer);
+      p = reinterpret_cast<char*>((reinterpret_cast<uintptr_t>(p) + 15) & ~uintptr_t(15));
+      P.transfer_count = reinterpret_cast<uint8_t*>(p);
+      P.capacity = capacity;
+    }
+    const size_t hit_bytes = n * (sizeof(float4) + sizeof(uint4) + kMaxNearby * sizeof(uint4));
+    cudaError_t e = hit_buf.ensure(hit_bytes);
+    if (e != cudaSuccess) return cuda_fail(e, "allocating hit pool");
+    char* h = hit_buf.as<char>();
+    hits.bary_t = reinterpret_cast<float4*>(h); h += n * sizeof(float4);
+    hits.ids = reinterpret_cast<uint4*>(h); h += n * sizeof(uint4);
+    hits.nearby = reinterpret_cast<uint4*>(h);
+    pool_capacity = capacity;
+    return YMRT_OK;
+  }
+};
+
+struct ymrt_scene {
+  ymrt_context* ctx = nullptr;
+  DeviceScene dev{};
+  std::vector<std::unique_ptr<DeviceBuffer>> buffers;
+  int width = 0, height = 0;
+  uint64_t triangles = 0;
+
+  template <typename T>
+  cudaError_t upload(const std::vector<T>& v, const T** out) {
+    buffers.emplace_back(new DeviceBuffer());
+    DeviceBuffer& b = *buffers.back();
+    cudaError_t e = b.ensure(std::max<size_t>(v.size() * sizeof(T), 16));
+    if (e != cudaSuccess) return e;
+    if (!v.empty()) e = cudaMemcpyAsync(b.ptr, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, ctx->stream);
+    *out = b.as<T>();
+    return e;
+  }
+};
+
+extern "C" {
+
+int ymrt_create(int device_ordinal, ymrt_context** out) {
+  if (!out) return YMRT_ERR_INVALID;
+  *out = nullptr;
+  int n = 0;
+  cudaError_t e = cudaGetDeviceCount(&n);
+  if (e != cudaSuccess || n == 0) {
+    g_last_error = std::string("no CUDA device: ") + cudaGetErrorString(e);
+    return YMRT_ERR_NO_DEVICE;
+  }
+  if (device_ordinal < 0 || device_ordinal >= n) {
+    g_last_error = "device ordinal out of range";
+    return YMRT_ERR_INVALID;
+  }
+  std::unique_ptr<ymrt_context> ctx(new (std::nothrow) ymrt_context());
+  if (!ctx) return YMRT_ERR_OOM;
+  ctx->device = device_ordinal;
+  if ((e = cudaSetDevice(device_ordinal)) != cudaSuccess) return ctx->cuda_fail(e, "cudaSetDevice");
+  if ((e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking)) != cudaSuccess)
+    return ctx->cuda_fail(e, "cudaStreamCreate");
+  if ((e = cudaEventCreate(&ctx->ev_start)) != cudaSuccess || (e = cudaEventCreate(&ctx->ev_stop)) != cudaSuccess)
+    return ctx->cuda_fail(e, "cudaEventCreate");
+  if ((e = cudaMallocHost(&ctx->counters_host, sizeof(WaveCounters))) != cudaSuccess)
+    return ctx->cuda_fail(e, "cudaMallocHost");
+  if ((e = ctx->counters_buf.ensure(sizeof(WaveCounters))) != cudaSuccess) return ctx->cuda_fail(e, "cudaMalloc");
+  ctx->primes = first_primes(kHaltonDims);
+  ctx->prime_sums.resize(kHaltonDims);
+  uint32_t acc = 0;
+  for (int i = 0; i < kHaltonDims; ++i) {
+    ctx->prime_sums[i] = acc;
+    acc += ctx->primes[i];
+  }
+  *out = ctx.release();
+  return YMRT_OK;
+}
+
+void ymrt_destroy(ymrt_context* ctx) {
+  if (!ctx) return;
+  cudaSetDevice(ctx->device);
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  for (auto& b : ctx->pool_buf) b.release();
+  ctx->hit_buf.release();
+  ctx->counters_buf.release();
+  ctx->image_buf.release();
+  if (ctx->counters_host) cudaFreeHost(ctx->counters_host);
+  if (ctx->ev_start) cudaEventDestroy(ctx->ev_start);
+  if (ctx->ev_stop) cudaEventDestroy(ctx->ev_stop);
+  if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+}
+
+const char* ymrt_last_error(const ymrt_context* ctx) { return ctx ? ctx->error.c_str() : g_last_error.c_str(); }
+
+int ymrt_set_queue_capacity(ymrt_context* ctx, uint32_t paths) {
+  if (!ctx) return YMRT_ERR_INVALID;
+  ctx->capacity = paths ? paths : (1u << 21);
+  return YMRT_OK;
+}
+
+int ymrt_scene_load_ymtmp(const char* path, int width, int height, ymrt_host_scene** out, char* err, size_t err_len) {
+  auto report = [&](int code, const std::string& msg) {
+    g_last_error = msg;
+    if (err && err_len) {
+      std::strncpy(err, msg.c_str(), err_len - 1);
+      err[err_len - 1] = 0;
+    }
+    return code;
+  };
+  if (!path || !out) return report(YMRT_ERR_INVALID, "null argument");
+  *out = nullptr;
+  std::unique_ptr<ymrt_host_scene> hs(new (std::nothrow) ymrt_host_scene());
+  if (!hs) return report(YMRT_ERR_OOM, "out of host memory");
+  std::string msg;
+  int rc;
+  try {
+    rc = load_ymtmp(path, &hs->s, &msg);
+    if (rc == YMRT_OK) rc = prepare_scene(&hs->s, width, height, &msg);
+  } catch (const std::exception& ex) {
+    rc = YMRT_ERR_FORMAT;
+    msg = std::string("malformed value in ") + path + ": " + ex.what();
+  }
+  if (rc != YMRT_OK) return report(rc, msg);
+  *out = hs.release();
+  return YMRT_OK;
+}
+
+void ymrt_host_scene_free(ymrt_host_scene* scene) { delete scene; }
+
+long long ymrt_host_scene_query(const ymrt_host_scene* hs, int what, int index, void* out, size_t cap) {
+  if (!hs) return YMRT_ERR_INVALID;
+  const HostScene& s = hs->s;
+  auto copy = [&](const void* src, size_t count, size_t elem) -> long long {
+    if (out && cap < count) return YMRT_ERR_INVALID;
+    if (out && count) std::memcpy(out, src, count * elem);
+    return (long long)count;
+  };
+  switch (what) {
+    case YMRT_QUERY_COUNTS: {
+      uint64_t c[8] = {s.instances.size(), s.meshes.size(), s.tri_corners.size() / 3, s.triangle_count_instanced,
+                       s.shape_lights.size(), s.blas_nodes.size(), s.tlas_nodes.size(), s.materials.size()};
+      return copy(c, 8, sizeof(uint64_t));
+    }
+    case YMRT_QUERY_INSTANCES: {
+      std::vector<uint32_t> v;
+      for (size_t i = 0; i < s.instances.size(); ++i) {
+        const Instance& in = s.instances[i];
+        v.insert(v.end(), {in.geometry_idx, in.transform_idx, in.material_idx, (uint32_t)in.inner_volume_idx,
+                           (uint32_t)in.treat_as_boundary, s.instance_file_index[i]});
+      }
+      return copy(v.data(), v.size(), sizeof(uint32_t));
+    }
+    case YMRT_QUERY_LIGHTS: {
+      std::vector<float> v;
+      for (const ShapeLight& l : s.shape_lights) v.insert(v.end(), {u2f(l.instance_idx), u2f(l.triangle_idx), l.power, l.area});
+      return copy(v.data(), v.size(), sizeof(float));
+    }
+    case YMRT_QUERY_LIGHT_TABLE:
+      return copy(s.shape_light_table.data(), s.shape_light_table.size(), sizeof(float));
+    case YMRT_QUERY_TRANSFORMS: {
+      std::vector<float> v;
+      for (size_t i = 0; i < s.transforms.size(); ++i) {
+        const float* a = &s.transforms[i].m[0][0];
+        const float* b = &s.i_transforms[i].m[0][0];
+        v.insert(v.end(), a, a + 16);
+        v.insert(v.end(), b, b + 16);
+      }
+      return copy(v.data(), v.size(), sizeof(float));
+    }
+    case YMRT_QUERY_CAMERA: {
+      const CameraDesc& c = s.camera;
+      const float v[14] = {c.position.x, c.position.y, c.position.z, c.u.x, c.u.y, c.u.z, c.v.x,
+                           c.v.y,        c.v.z,        c.w.x,        c.w.y, c.w.z, c.aspect_ratio, c.tan_half_fov};
+      return copy(v, 14, sizeof(float));
+    }
+    case YMRT_QUERY_TRIANGLES: {
+      if (index < 0 || (size_t)index >= s.meshes.size()) return YMRT_ERR_INVALID;
+      const std::vector<uint32_t>& t = s.meshes[index].tris;
+      return copy(t.data(), t.size(), sizeof(uint32_t));
+    }
+    default:
+      return YMRT_ERR_INVALID;
+  }
+}
+
+int ymrt_scene_upload(ymrt_context* ctx, const ymrt_host_scene* hs, const uint32_t* halton_perm, size_t perm_len,
+                      ymrt_scene** out) {
+  if (!ctx || !hs || !out || !halton_perm) return YMRT_ERR_INVALID;
+  *out = nullptr;
+  size_t need = 0;
+  for (uint32_t p : ctx->primes) need += p;
+  if (perm_len != need)
+    return ctx->fail(YMRT_ERR_INVALID, "halton permutation table must hold " + std::to_string(need) + " entries");
+  const HostScene& s = hs->s;
+  for (const Material& m : s.materials) {
+    if (m.material_type != kDefaultMtl) continue;
+    const DefaultMtl& d = m.default_mtl;
+    const uint32_t tex[] = {d.diffuse_albedo_tex, d.alpha_x_tex, d.specular_albedo_tex, d.alpha_y_tex,
+                            d.specular_weight_tex, d.metalness_tex, d.transmission_weight_tex, d.normal_mapping_tex,
+                            d.bump_mapping_tex, d.coat_albedo_tex, d.coat_weight_tex, d.coat_thickness_tex,
+                            d.coat_roughness_x_tex, d.coat_roughness_y_tex};
+    for (uint32_t t : tex)
+      if (t != kEmpty) return ctx->fail(YMRT_ERR_UNSUPPORTED, "textured material parameters are not supported");
+  }
+  cudaSetDevice(ctx->device);
+  std::unique_ptr<ymrt_scene> sc(new (std::nothrow) ymrt_scene());
+  if (!sc) return YMRT_ERR_OOM;
+  sc->ctx = ctx;
+  sc->width = s.width;
+  sc->height = s.height;
+  sc->triangles = s.triangle_count_instanced;
+  DeviceScene& D = sc->dev;
+  cudaError_t e = cudaSuccess;
+#define UP(vec, field)                                          \
+  do {                                                          \
+    if (e == cudaSuccess) e = sc->upload(vec, &D.field);        \
+  } while (0)
+  UP(s.instances, instances);
+  UP(s.transforms, transforms);
+  UP(s.i_transforms, i_transforms);
+  UP(s.tlas_nodes, tlas_nodes);
+  UP(s.tlas_prims, tlas_prims);
+  UP(s.geo_desc, geometries);
+  UP(s.blas_nodes, blas_nodes);
+  UP(s.wtris, wtris);
+  UP(s.tri_corners, tri_corners);
+  UP(s.all_pos_idx, pos_idx);
+  UP(s.all_nrm_idx, nrm_idx);
+  UP(s.all_uv_idx, uv_idx);
+  UP(s.all_pos, positions);
+  UP(s.all_nrm, normals);
+  UP(s.all_uv, texcoords);
+  UP(s.materials, materials);
+  UP(s.shape_lights, shape_lights);
+  UP(s.shape_light_table, shape_light_table);
+  UP(s.volumes, volumes);
+  UP(s.textures, textures);
+#undef UP
+  if (e == cudaSuccess) {
+    std::vector<uint32_t> perm(halton_perm, halton_perm + perm_len);
+    e = sc->upload(perm, &D.halton_perm);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  }
+  if (e != cudaSuccess) return ctx->cuda_fail(e, "uploading scene");
+  D.instance_count = (uint32_t)s.instances.size();
+  D.transform_count = (uint32_t)s.transforms.size();
+  D.geometry_count = (uint32_t)s.geo_desc.size();
+  D.material_count = (uint32_t)s.materials.size();
+  D.shape_light_count = (uint32_t)s.shape_lights.size();
+  D.volume_count = (uint32_t)s.volumes.size();
+  D.texture_count = (uint32_t)s.textures.size();
+  D.camera = s.camera;
+  D.width = s.width;
+  D.height = s.height;
+  // HaltonEnumerator constructor (src/HaltonEnumerator.h:13-38).
+  {
+    int scale2 = 1, exp2 = 0, scale3 = 1, exp3 = 0;
+    while (scale2 < s.width) {
+      scale2 *= 2;
+      ++exp2;
+    }
+    while (scale3 < s.height) {
+      scale3 *= 3;
+      ++exp3;
+    }
+    struct MI {
+      int x, y;
+    };
+    std::function<MI(int, int)> ee = [&](int a, int b) -> MI {
+      if (b == 0) return MI{1, 0};
+      const MI lo = ee(b, a % b);
+      return MI{lo.y, lo.x - (a / b) * lo.y};
+    };
+    const int w = scale2, h = scale3;
+    const MI mi = ee(h, w);
+    const int inv2 = mi.x < 0 ? (mi.x + w) : (mi.x % w);
+    const int inv3 = mi.y < 0 ? (mi.y + h) : (mi.y % h);
+    D.halton_mx = h * inv2;
+    D.halton_my = w * inv3;
+    D.halton_increment = w * h;
+    D.halton_x_scale = float(scale2);
+    D.halton_y_scale = float(scale3);
+    D.halton_exp2 = exp2;
+    D.halton_exp3 = exp3;
+  }
+  *out = sc.release();
+  return YMRT_OK;
+}
+
+void ymrt_scene_free(ymrt_scene* scene) {
+  if (!scene) return;
+  cudaSetDevice(scene->ctx->device);
+  cudaStreamSynchronize(scene->ctx->stream);
+  delete scene;
+}
+
+int ymrt_render_tiles(ymrt_scene* sc, const ymrt_render_setting* setting, int frame_index, int tile_begin, int tile_end,
+                      float* out_rgba, int out_on_device, ymrt_stats* stats) {
+  if (!sc || !setting || !out_rgba) return YMRT_ERR_INVALID;
+  ymrt_context* ctx = sc->ctx;
+  static_assert(sizeof(ymrt_render_setting) == sizeof(RenderSetting), "render setting layout");
+  RenderSetting rs;
+  std::memcpy(&rs, setting, sizeof(rs));
+  if (frame_index < 1) return ctx->fail(YMRT_ERR_INVALID, "frame_index starts at 1");
+  if (rs.sampler_type != 1) return ctx->fail(YMRT_ERR_UNSUPPORTED, "only the Halton sampler (sampler_type 1) is supported");
+  if (rs.enable_distant_light) return ctx->fail(YMRT_ERR_UNSUPPORTED, "distant lights are not supported yet");
+  if (rs.enable_volume_scattering) return ctx->fail(YMRT_ERR_UNSUPPORTED, "volume scattering is not supported yet");
+  const uint32_t spp = (uint32_t)std::max(rs.ssp, 1);
+  const uint32_t per_tile = (uint32_t)kTilePixels * spp;
+  cudaSetDevice(ctx->device);
+  int rc = ctx->ensure_pools();
+  if (rc != YMRT_OK) return rc;
+  if (per_tile > ctx->capacity) return ctx->fail(YMRT_ERR_INVALID, "queue capacity smaller than one tile of samples");
+  const uint32_t W = sc->width, Hh = sc->height;
+  const uint32_t tiles_x = (W + kTileRes - 1) / kTileRes, tiles_y = (Hh + kTileRes - 1) / kTileRes;
+  const uint32_t total_tiles = tiles_x * tiles_y;
+  const uint32_t t_end = tile_end <= 0 ? total_tiles : std::min<uint32_t>((uint32_t)tile_end, total_tiles);
+  uint32_t cursor = (uint32_t)std::max(tile_begin, 0);
+  cudaStream_t st = ctx->stream;
+  cudaError_t e;
+  float4* image = reinterpret_cast<float4*>(out_rgba);
+  const size_t img_bytes = (size_t)W * Hh * sizeof(float4);
+  if (!out_on_device) {
+    if ((e = ctx->image_buf.ensure(img_bytes)) != cudaSuccess) return ctx->cuda_fail(e, "allocating image");
+    image = ctx->image_buf.as<float4>();
+  }
+  if ((e = upload_constants(sc->dev, ctx->primes.data(), ctx->prime_sums.data(), st)) != cudaSuccess)
+    return ctx->cuda_fail(e, "uploading constants");
+  if ((e = upload_setting(rs, st)) != cudaSuccess) return ctx->cuda_fail(e, "uploading render setting");
+  WaveCounters* dc = ctx->counters_buf.as<WaveCounters>();
+  cudaMemsetAsync(dc, 0, sizeof(WaveCounters), st);
+  cudaMemsetAsync(image, 0, img_bytes, st);
+  cudaEventRecord(ctx->ev_start, st);
+  uint32_t live = 0;
+  int a = 0;
+  uint64_t waves = 0, paths = 0;
+  while (live > 0 || cursor < t_end) {
+    const uint32_t n_tiles = std::min<uint32_t>((ctx->capacity - live) / per_tile, t_end - cursor);
+    const uint32_t gen = n_tiles * per_tile;
+    PathPool& A = ctx->pool[a];
+    PathPool& B = ctx->pool[a ^ 1];
+    launch_generate(A, live, gen, cursor, tiles_x, frame_index, spp, st);
+    const uint32_t total = live + gen;
+    launch_extend(A, total, ctx->hits, image, dc, st);
+    cudaMemsetAsync(&dc->next_count, 0, sizeof(uint32_t), st);
+    launch_shade(A, total, ctx->hits, B, image, dc, st);
+    if ((e = cudaMemcpyAsync(ctx->counters_host, dc, sizeof(WaveCounters), cudaMemcpyDeviceToHost, st)) != cudaSuccess)
+      return ctx->cuda_fail(e, "reading wave counters");
+    if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return ctx->cuda_fail(e, "wave");
+    live = ctx->counters_host->next_count;
+    if (live > ctx->capacity) return ctx->fail(YMRT_ERR_OVERFLOW, "path queue overflow");
+    a ^= 1;
+    cursor += n_tiles;
+    paths += gen;
+    ++waves;
+  }
+  cudaEventRecord(ctx->ev_stop, st);
+  if (!out_on_device) {
+    if ((e = cudaMemcpyAsync(out_rgba, image, img_bytes, cudaMemcpyDeviceToHost, st)) != cudaSuccess)
+      return ctx->cuda_fail(e, "copying image");
+  }
+  if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return ctx->cuda_fail(e, "frame");
+  if ((e = cudaMemcpy(ctx->counters_host, dc, sizeof(WaveCounters), cudaMemcpyDeviceToHost)) != cudaSuccess)
+    return ctx->cuda_fail(e, "reading counters");
+  float ms = 0.0f;
+  cudaEventElapsedTime(&ms, ctx->ev_start, ctx->ev_stop);
+  if (stats) {
+    std::memset(stats, 0, sizeof(*stats));
+    stats->paths = paths;
+    stats->extension_rays = ctx->counters_host->extension_rays;
+    stats->shadow_rays = ctx->counters_host->shadow_rays;
+    stats->waves = waves;
+    stats->ms_total = ms;
+    stats->device_errors = ctx->counters_host->errors;
+  }
+  if (ctx->counters_host->errors & kDevErrQueue) return ctx->fail(YMRT_ERR_OVERFLOW, "path queue overflow on the device");
+  if (ctx->counters_host->errors & kDevErrStack)
+    return ctx->fail(YMRT_ERR_OVERFLOW, "traversal or nested-media stack overflow on the device");
+  return YMRT_OK;
+}
+
+int ymrt_render_forward(ymrt_scene* sc, const ymrt_render_setting* setting, int frame_index, float* out_rgba,
+                        int out_on_device, ymrt_stats* stats) {
+  return ymrt_render_tiles(sc, setting, frame_index, 0, 0, out_rgba, out_on_device, stats);
+}
+
+int ymrt_accumulate(ymrt_scene* sc, const float* noise, float* acc, int frame_index) {
+  if (!sc || !noise || !acc || frame_index < 1) return YMRT_ERR_INVALID;
+  ymrt_context* ctx = sc->ctx;
+  cudaSetDevice(ctx->device);
+  launch_accumulate(reinterpret_cast<const float4*>(noise), reinterpret_cast<float4*>(acc),
+                    (uint32_t)sc->width * (uint32_t)sc->height, frame_index, ctx->stream);
+  cudaError_t e = cudaStreamSynchronize(ctx->stream);
+  return e == cudaSuccess ? YMRT_OK : ctx->cuda_fail(e, "accumulate");
+}
+
+}  // extern "C"
+
+namespace {
+// Stages host arrays on the device for the known-answer kernels.
+struct Staging {
+  ymrt_context* ctx;
+  std::vector<std::unique_ptr<DeviceBuffer>> bufs;
+  cudaError_t err = cudaSuccess;
+  template <typename T>
+  T* in(const T* host, size_t n) {
+    if (!host || err != cudaSuccess) return nullptr;
+    bufs.emplace_back(new DeviceBuffer());
+    if ((err = bufs.back()->ensure(n * sizeof(T))) != cudaSuccess) return nullptr;
+    err = cudaMemcpyAsync(bufs.back()->ptr, host, n * sizeof(T), cudaMemcpyHostToDevice, ctx->stream);
+    return bufs.back()->as<T>();
+  }
+  template <typename T>
+  T* out(size_t n) {
+    if (err != cudaSuccess) return nullptr;
+    bufs.emplace_back(new DeviceBuffer());
+    if ((err = bufs.back()->ensure(n * sizeof(T))) != cudaSuccess) return nullptr;
+    return bufs.back()->as<T>();
+  }
+  template <typename T>
+  void back(T* host, const T* dev, size_t n) {
+    if (err == cudaSuccess && host) err = cudaMemcpyAsync(host, dev, n * sizeof(T), cudaMemcpyDeviceToHost, ctx->stream);
+  }
+};
+}  // namespace
+
+extern "C" {
+
+int ymrt_debug_trace(ymrt_scene* sc, int n, const float* origin, const float* dir, const uint32_t* last_hit,
+                     uint32_t* inst, uint32_t* tri, float* t, float* bary, int* back, int* nearby) {
+  if (!sc || n < 0 || !origin || !dir || !inst || !tri || !t || !bary || !back || !nearby) return YMRT_ERR_INVALID;
+  if (n == 0) return YMRT_OK;
+  ymrt_context* ctx = sc->ctx;
+  cudaSetDevice(ctx->device);
+  Staging sg{ctx};
+  const float* d_o = sg.in(origin, 3 * (size_t)n);
+  const float* d_d = sg.in(dir, 3 * (size_t)n);
+  const uint32_t* d_lh = last_hit ? sg.in(last_hit, 2 * (size_t)n) : nullptr;
+  uint32_t* d_inst = sg.out<uint32_t>(n);
+  uint32_t* d_tri = sg.out<uint32_t>(n);
+  float* d_t = sg.out<float>(n);
+  float* d_b = sg.out<float>(3 * (size_t)n);
+  int* d_back = sg.out<int>(n);
+  int* d_nb = sg.out<int>(n);
+  uint32_t* d_err = sg.out<uint32_t>(1);
+  if (sg.err != cudaSuccess) return ctx->cuda_fail(sg.err, "staging");
+  cudaMemsetAsync(d_err, 0, sizeof(uint32_t), ctx->stream);
+  upload_constants(sc->dev, ctx->primes.data(), ctx->prime_sums.data(), ctx->stream);
+  launch_debug_trace(n, d_o, d_d, d_lh, d_inst, d_tri, d_t, d_b, d_back, d_nb, d_err, ctx->stream);
+  uint32_t errs = 0;
+  sg.back(inst, d_inst, n);
+  sg.back(tri, d_tri, n);
+  sg.back(t, d_t, n);
+  sg.back(bary, d_b, 3 * (size_t)n);
+  sg.back(back, d_back, n);
+  sg.back(nearby, d_nb, n);
+  sg.back(&errs, d_err, 1);
+  cudaError_t e = cudaStreamSynchronize(ctx->stream);
+  if (sg.err != cudaSuccess || e != cudaSuccess) return ctx->cuda_fail(sg.err != cudaSuccess ? sg.err : e, "debug trace");
+  if (errs) return ctx->fail(YMRT_ERR_OVERFLOW, "traversal stack overflow");
+  return YMRT_OK;
+}
+
+int ymrt_debug_occluded(ymrt_scene* sc, int n, const float* origin, const float* dir, const float* tmax, int* occluded) {
+  if (!sc || n < 0 || !origin || !dir || !tmax || !occluded) return YMRT_ERR_INVALID;
+  if (n == 0) return YMRT_OK;
+  ymrt_context* ctx = sc->ctx;
+  cudaSetDevice(ctx->device);
+  Staging sg{ctx};
+  const float* d_o = sg.in(origin, 3 * (size_t)n);
+  const float* d_d = sg.in(dir, 3 * (size_t)n);
+  const float* d_tm = sg.in(tmax, (size_t)n);
+  int* d_occ = sg.out<int>(n);
+  uint32_t* d_err = sg.out<uint32_t>(1);
+  if (sg.err != cudaSuccess) return ctx->cuda_fail(sg.err, "staging");
+  cudaMemsetAsync(d_err, 0, sizeof(uint32_t), ctx->stream);
+  upload_constants(sc->dev, ctx->primes.data(), ctx->prime_sums.data(), ctx->stream);
+  launch_debug_occluded(n, d_o, d_d, d_tm, d_occ, d_err, ctx->stream);
+  uint32_t errs = 0;
+  sg.back(occluded, d_occ, n);
+  sg.back(&errs, d_err, 1);
+  cudaError_t e = cudaStreamSynchronize(ctx->stream);
+  if (sg.err != cudaSuccess || e != cudaSuccess) return ctx->cuda_fail(sg.err != cudaSuccess ? sg.err : e, "debug occluded");
+  if (errs) return ctx->fail(YMRT_ERR_OVERFLOW, "traversal stack overflow");
+  return YMRT_OK;
+}
+
+int ymrt_debug_halton(ymrt_scene* sc, int n, const int* px, const int* py, const int* sample, int n_dims, uint64_t* index,
+                      float* offset, float* dims) {
+  if (!sc || n < 0 || n_dims < 0 || !px || !py || !sample || !index || !offset || (n_dims > 0 && !dims))
+    return YMRT_ERR_INVALID;
+  if (n == 0) return YMRT_OK;
+  ymrt_context* ctx = sc->ctx;
+  cudaSetDevice(ctx->device);
+  Staging sg{ctx};
+  const int* d_px = sg.in(px, n);
+  const int* d_py = sg.in(py, n);
+  const int* d_s = sg.in(sample, n);
+  uint64_t* d_idx = sg.out<uint64_t>(n);
+  float* d_off = sg.out<float>(2 * (size_t)n);
+  float* d_dims = sg.out<float>(std::max<size_t>((size_t)n * n_dims, 1));
+  if (sg.err != cudaSuccess) return ctx->cuda_fail(sg.err, "staging");
+  upload_constants(sc->dev, ctx->primes.data(), ctx->prime_sums.data(), ctx->stream);
+  launch_debug_halton(n, d_px, d_py, d_s, n_dims, d_idx, d_off, d_dims, ctx->stream);
+  sg.back(index, d_idx, n);
+  sg.back(offset, d_off, 2 * (size_t)n);
+  if (n_dims > 0) sg.back(dims, d_dims, (size_t)n * n_dims);
+  cudaError_t e = cudaStreamSynchronize(ctx->stream);
+  if (sg.err != cudaSuccess || e != cudaSuccess) return ctx->cuda_fail(sg.err != cudaSuccess ? sg.err : e, "debug halton");
+  return YMRT_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,420 @@
+// Two-level ray traversal over compressed 8-wide BVHs (sm_100a).
+//
+// Semantics follow the reference's TraceRay / IntersectMeshObject /
+// IntersectTri / BVHTraverseShadow (src/ShadingUtilities.cuh:54-217,
+// 310-431, 563-635): world rays are carried into each instance with the
+// instance's inverse transform (glm mat4*vec4 order), triangles are tested
+// with the watertight test in the reference's exact float order (so t and the
+// barycentrics are bit-identical), a hit is kept when TMIN <= t <= current t
+// (a later hit at an equal t replaces the earlier one), and the "nearby hits"
+// list for nested media records every instance whose hit lies within two
+// ulps of the final t.
+//
+// The acceleration structure is this project's: each node holds 8 child boxes
+// quantised to bytes on a per-node power-of-two grid (80-byte nodes, five
+// 128-bit read-only loads), leaves hold up to three triangles stored as three
+// float4 vertices (no index indirection), and the traversal stack lives in
+// shared memory (spilling to a short local-memory tail). Box tests use fused
+// multiply-adds and are widened by a few ulps so that they are conservative:
+// they only decide which triangles are tested, never the hit itself.
+#pragma once
+
+#include "ymrt_scene.h"
+
+namespace ym {
+
+constexpr int kStackShared = 40;  // entries per thread in shared memory
+constexpr int kStackLocal = 40;   // further entries per thread in local memory
+constexpr int kTraceBlock = 128;  // threads per block of the traversal kernels
+
+struct TraversalStack {
+  uint32_t* sh;  // shared-memory column of this thread (stride kTraceBlock)
+  uint32_t loc[kStackLocal];
+  int sp;
+  bool overflow;
+  __device__ __forceinline__ void push(uint32_t v) {
+    if (sp < kStackShared) sh[sp * kTraceBlock] = v;
+    else if (sp < kStackShared + kStackLocal) loc[sp - kStackShared] = v;
+    else {
+      overflow = true;
+      return;
+    }
+    ++sp;
+  }
+  __device__ __forceinline__ uint32_t pop() {
+    --sp;
+    return sp < kStackShared ? sh[sp * kTraceBlock] : loc[sp - kStackShared];
+  }
+};
+
+// Ray set-up shared by every triangle test of one object-space ray: the
+// reference recomputes these in each IntersectTri call; they are the same
+// numbers each time.
+struct TriRay {
+  vec3 o, d;
+  int kx, ky, kz;
+  float sx, sy, sz;
+};
+__device__ __forceinline__ TriRay make_tri_ray(vec3 o, vec3 d) {
+  TriRay r;
+  r.o = o;
+  r.d = d;
+  r.kz = max_dimension(vabs(d));
+  r.kx = r.kz + 1; if (r.kx == 3) r.kx = 0;
+  r.ky = r.kx + 1; if (r.ky == 3) r.ky = 0;
+  const vec3 dd(d[r.kx], d[r.ky], d[r.kz]);
+  r.sx = -dd.x / dd.z;
+  r.sy = -dd.y / dd.z;
+  r.sz = 1.f / dd.z;
+  return r;
+}
+
+// Watertight ray/triangle test, IntersectTri (src/ShadingUtilities.cuh:54-134).
+// Returns false when the edge tests fail; otherwise t (may be outside range)
+// and the three unnormalised edge values with 1/den.
+__device__ __forceinline__ bool tri_test(const TriRay& R, vec3 p0, vec3 p1, vec3 p2, float* t_out, float* e_out,
+                                         float* inv_den_out) {
+  p0 = p0 - R.o;
+  p1 = p1 - R.o;
+  p2 = p2 - R.o;
+  p0 = vec3(p0[R.kx], p0[R.ky], p0[R.kz]);
+  p1 = vec3(p1[R.kx], p1[R.ky], p1[R.kz]);
+  p2 = vec3(p2[R.kx], p2[R.ky], p2[R.kz]);
+  p0.x += R.sx * p0.z;
+  p0.y += R.sy * p0.z;
+  p1.x += R.sx * p1.z;
+  p1.y += R.sy * p1.z;
+  p2.x += R.sx * p2.z;
+  p2.y += R.sy * p2.z;
+  const float e0 = p1.x * p2.y - p1.y * p2.x;
+  const float e1 = p2.x * p0.y - p2.y * p0.x;
+  const float e2 = p0.x * p1.y - p0.y * p1.x;
+  if ((e0 < 0 || e1 < 0 || e2 < 0) && (e0 > 0 || e1 > 0 || e2 > 0)) return false;
+  const float den = e0 + e1 + e2;
+  if (den == 0) return false;
+  p0.z *= R.sz;
+  p1.z *= R.sz;
+  p2.z *= R.sz;
+  const float inv = 1.0f / den;
+  float t = e0 * p0.z + e1 * p1.z + e2 * p2.z;
+  t *= inv;
+  *t_out = t;
+  e_out[0] = e0;
+  e_out[1] = e1;
+  e_out[2] = e2;
+  *inv_den_out = inv;
+  return true;
+}
+
+__device__ __forceinline__ void load_tri(const float4* __restrict__ wtris, uint32_t i, vec3* p0, vec3* p1, vec3* p2,
+                                         uint32_t* id) {
+  const float4 a = __ldg(wtris + 3 * (size_t)i);
+  const float4 b = __ldg(wtris + 3 * (size_t)i + 1);
+  const float4 c = __ldg(wtris + 3 * (size_t)i + 2);
+  *p0 = vec3(a.x, a.y, a.z);
+  *p1 = vec3(b.x, b.y, b.z);
+  *p2 = vec3(c.x, c.y, c.z);
+  *id = __float_as_uint(a.w);
+}
+
+// Per-ray constants for box tests.
+struct BoxRay {
+  float ox, oy, oz, ix, iy, iz;
+};
+__device__ __forceinline__ BoxRay make_box_ray(vec3 o, vec3 d) {
+  BoxRay b;
+  b.ox = o.x; b.oy = o.y; b.oz = o.z;
+  b.ix = 1.0f / d.x; b.iy = 1.0f / d.y; b.iz = 1.0f / d.z;
+  return b;
+}
+
+__device__ __forceinline__ float byte_of(uint32_t w, int k) { return (float)((w >> (8 * k)) & 0xFFu); }
+
+// Tests the 8 child boxes of a node. Returns a mask of hit children; tnear
+// receives each hit child's entry distance.
+__device__ __forceinline__ uint32_t intersect_children(const uint4* __restrict__ nodes_u4, uint32_t node, const BoxRay& r,
+                                                       float tmax, float tnear_out[8], uint32_t* imask,
+                                                       uint32_t* child_base, uint32_t* prim_base, uint32_t meta[2]) {
+  const uint4* p = nodes_u4 + 5 * (size_t)node;
+  const uint4 w0 = __ldg(p), w1 = __ldg(p + 1), w2 = __ldg(p + 2), w3 = __ldg(p + 3), w4 = __ldg(p + 4);
+  const float nox = __uint_as_float(w0.x), noy = __uint_as_float(w0.y), noz = __uint_as_float(w0.z);
+  const float sx = __uint_as_float((w0.w & 0xFFu) << 23);
+  const float sy = __uint_as_float(((w0.w >> 8) & 0xFFu) << 23);
+  const float sz = __uint_as_float(((w0.w >> 16) & 0xFFu) << 23);
+  *imask = w0.w >> 24;
+  *child_base = w1.x;
+  *prim_base = w1.y;
+  meta[0] = w1.z;
+  meta[1] = w1.w;
+  // t = (origin + q * scale - o) * inv = q * (scale * inv) + (origin - o) * inv
+  const float ax = sx * r.ix, bx = (nox - r.ox) * r.ix;
+  const float ay = sy * r.iy, by = (noy - r.oy) * r.iy;
+  const float az = sz * r.iz, bz = (noz - r.oz) * r.iz;
+  // byte planes: w2 = qlo_x[0..7], qlo_y[0..7]; w3 = qlo_z, qhi_x; w4 = qhi_y, qhi_z
+  const bool negx = r.ix < 0.0f, negy = r.iy < 0.0f, negz = r.iz < 0.0f;
+  uint32_t hits = 0;
+#pragma unroll
+  for (int c = 0; c < 8; ++c) {
+    const int k = c & 3;
+    const uint32_t lox = c < 4 ? w2.x : w2.y, loy = c < 4 ? w2.z : w2.w;
+    const uint32_t loz = c < 4 ? w3.x : w3.y, hix = c < 4 ? w3.z : w3.w;
+    const uint32_t hiy = c < 4 ? w4.x : w4.y, hiz = c < 4 ? w4.z : w4.w;
+    const float qlx = byte_of(lox, k), qhx = byte_of(hix, k);
+    const float qly = byte_of(loy, k), qhy = byte_of(hiy, k);
+    const float qlz = byte_of(loz, k), qhz = byte_of(hiz, k);
+    const float t0x = __fmaf_rn(negx ? qhx : qlx, ax, bx), t1x = __fmaf_rn(negx ? qlx : qhx, ax, bx);
+    const float t0y = __fmaf_rn(negy ? qhy : qly, ay, by), t1y = __fmaf_rn(negy ? qly : qhy, ay, by);
+    const float t0z = __fmaf_rn(negz ? qhz : qlz, az, bz), t1z = __fmaf_rn(negz ? qlz : qhz, az, bz);
+    float tn = fmaxf(fmaxf(t0x, t0y), fmaxf(t0z, 0.0f));
+    float tf = fminf(fminf(t1x, t1y), fminf(t1z, tmax));
+    tn = __fmaf_rn(-fabsf(tn), 1e-6f, tn);
+    tf = __fmaf_rn(fabsf(tf), 1e-6f, tf);
+    const uint32_t m = (c < 4 ? meta[0] : meta[1]) >> (8 * k) & 0xFFu;
+    const bool occupied = ((*imask >> c) & 1u) || m != 0;
+    if (occupied && tn <= tf) {
+      hits |= 1u << c;
+      tnear_out[c] = tn;
+    }
+  }
+  return hits;
+}
+
+__device__ __forceinline__ uint32_t child_meta(const uint32_t meta[2], int c) {
+  return (c < 4 ? meta[0] : meta[1]) >> (8 * (c & 3)) & 0xFFu;
+}
+
+// Pushes the hit internal children far-to-near so the nearest is popped first.
+__device__ __forceinline__ void push_sorted(TraversalStack& st, uint32_t hits_internal, const float tnear[8],
+                                            const uint32_t meta[2], uint32_t child_base) {
+  uint32_t idx[8];
+  float key[8];
+  int n = 0;
+#pragma unroll
+  for (int c = 0; c < 8; ++c) {
+    if (hits_internal & (1u << c)) {
+      idx[n] = child_base + child_meta(meta, c);
+      key[n] = tnear[c];
+      ++n;
+    }
+  }
+  // insertion sort, descending distance
+  for (int i = 1; i < n; ++i) {
+    const float k = key[i];
+    const uint32_t v = idx[i];
+    int j = i - 1;
+    while (j >= 0 && key[j] < k) {
+      key[j + 1] = key[j];
+      idx[j + 1] = idx[j];
+      --j;
+    }
+    key[j + 1] = k;
+    idx[j + 1] = v;
+  }
+  for (int i = 0; i < n; ++i) st.push(idx[i]);
+}
+
+struct NearbyHit {
+  uint32_t prim;
+  float t;
+  int back;
+};
+
+struct ClosestHit {
+  float t;
+  float b0, b1, b2;
+  uint32_t inst, tri;
+  int back;
+  int nearby_count;
+  NearbyHit nearby[kMaxNearby];
+};
+
+// Closest hit of one world-space ray (TraceRay, src/ShadingUtilities.cuh:310-431).
+// `volume_only`: traverse only treat_as_boundary instances (TraceVolume, :434-561).
+__device__ __noinline__ bool trace_closest(const DeviceScene& S, TraversalStack& st, vec3 wo, vec3 wd, float tmax,
+                                           uint32_t last_inst, uint32_t last_tri, bool volume_only, ClosestHit* out,
+                                           uint32_t* tri_tests) {
+  const uint4* tlas = reinterpret_cast<const uint4*>(S.tlas_nodes);
+  const uint4* blas = reinterpret_cast<const uint4*>(S.blas_nodes);
+  const bool skip_enabled = last_inst != kEmpty && last_tri != kEmpty;
+  float t_ray = tmax;
+  bool hit = false;
+  float t_upper = 0.0f, t_lower = 0.0f;
+  int n_nearby = 0;
+  NearbyHit* nb = out->nearby;
+  const BoxRay wray = make_box_ray(wo, wd);
+  st.sp = 0;
+  st.push(0);
+  while (st.sp > 0) {
+    const uint32_t node = st.pop();
+    float tn[8];
+    uint32_t imask, cbase, pbase, meta[2];
+    const uint32_t hits = intersect_children(tlas, node, wray, t_ray, tn, &imask, &cbase, &pbase, meta);
+    // instance leaves
+    uint32_t leaves = hits & ~imask;
+    while (leaves) {
+      const int c = __ffs(leaves) - 1;
+      leaves &= leaves - 1;
+      const uint32_t m = child_meta(meta, c);
+      const uint32_t cnt = m >> 5, off = m & 31u;
+      for (uint32_t k = 0; k < cnt; ++k) {
+        const uint32_t inst_idx = __ldg(S.tlas_prims + pbase + off + k);
+        const Instance inst = S.instances[inst_idx];
+        if (volume_only && !inst.treat_as_boundary) continue;
+        const mat4& wto = S.i_transforms[inst.transform_idx];
+        const vec3 oo = xform_point_glm(wto, wo);
+        const vec3 od = xform_dir_glm(wto, wd);
+        const GeometryDesc& g = S.geometries[inst.geometry_idx];
+        const TriRay tr = make_tri_ray(oo, od);
+        const BoxRay br = make_box_ray(oo, od);
+        const bool skip_here = skip_enabled && inst_idx == last_inst;
+        bool inst_hit = false;
+        float inst_t = 0.0f, hb0 = 0.0f, hb1 = 0.0f, hb2 = 0.0f;
+        uint32_t hit_tri = kEmpty, hit_w = 0;
+        float extra_t = kTMax;
+        uint32_t extra_w = kEmpty;
+        const int base = st.sp;
+        st.push(g.node_offset);
+        while (st.sp > base) {
+          const uint32_t bn = st.pop();
+          float btn[8];
+          uint32_t bim, bcb, bpb, bmeta[2];
+          const uint32_t bh = intersect_children(blas, bn, br, t_ray, btn, &bim, &bcb, &bpb, bmeta);
+          uint32_t bl = bh & ~bim;
+          while (bl) {
+            const int bc = __ffs(bl) - 1;
+            bl &= bl - 1;
+            const uint32_t bm = child_meta(bmeta, bc);
+            const uint32_t bcnt = bm >> 5, boff = bm & 31u;
+            for (uint32_t q = 0; q < bcnt; ++q) {
+              const uint32_t wi = g.wtri_offset + bpb + boff + q;
+              vec3 p0, p1, p2;
+              uint32_t tid;
+              load_tri(S.wtris, wi, &p0, &p1, &p2, &tid);
+              if (skip_here && tid == last_tri) continue;
+              float t, e[3], inv;
+              ++*tri_tests;
+              if (!tri_test(tr, p0, p1, p2, &t, e, &inv)) continue;
+              if (t >= kTMin && t < extra_t) {
+                extra_t = t;
+                extra_w = wi;
+              }
+              if (t < kTMin || t > t_ray) continue;
+              t_ray = t;
+              inst_hit = true;
+              inst_t = t;
+              hb0 = e[0] * inv;
+              hb1 = e[1] * inv;
+              hb2 = e[2] * inv;
+              hit_tri = tid;
+              hit_w = wi;
+            }
+          }
+          push_sorted(st, bh & bim, btn, bmeta, bcb);
+        }
+        if (inst_hit) {
+          vec3 p0, p1, p2;
+          uint32_t tid;
+          load_tri(S.wtris, hit_w, &p0, &p1, &p2, &tid);
+          const vec3 ng = normalize(cross(p1 - p0, p2 - p0));
+          out->t = inst_t;
+          out->b0 = hb0;
+          out->b1 = hb1;
+          out->b2 = hb2;
+          out->inst = inst_idx;
+          out->tri = hit_tri;
+          out->back = dot(ng, od) > 0.0f;
+          hit = true;
+          t_upper = next_float_up(next_float_up(t_ray));
+          t_lower = next_float_down(next_float_down(t_ray));
+          int head = 0, tail = n_nearby - 1;
+          while (head <= tail) {
+            if (nb[head].t > t_lower && nb[head].t < t_upper) ++head;
+            else {
+              const NearbyHit tmp = nb[head];
+              nb[head] = nb[tail];
+              nb[tail] = tmp;
+              --tail;
+            }
+          }
+          n_nearby = head;
+          if (n_nearby < kMaxNearby) nb[n_nearby++] = NearbyHit{inst_idx, inst_t, out->back};
+        } else if (hit && extra_w != kEmpty && extra_t > t_lower && extra_t < t_upper) {
+          vec3 p0, p1, p2;
+          uint32_t tid;
+          load_tri(S.wtris, extra_w, &p0, &p1, &p2, &tid);
+          const vec3 ng = normalize(cross(p1 - p0, p2 - p0));
+          if (n_nearby < kMaxNearby) nb[n_nearby++] = NearbyHit{inst_idx, extra_t, dot(ng, od) > 0.0f};
+        }
+      }
+    }
+    push_sorted(st, hits & imask, tn, meta, cbase);
+  }
+  out->nearby_count = n_nearby;
+  return hit;
+}
+
+// Any hit within (TMIN, tmax] ignoring boundary-only instances
+// (BVHTraverseShadow, src/ShadingUtilities.cuh:563-635).
+__device__ __noinline__ bool trace_occluded(const DeviceScene& S, TraversalStack& st, vec3 wo, vec3 wd, float tmax,
+                                            uint32_t* tri_tests) {
+  const uint4* tlas = reinterpret_cast<const uint4*>(S.tlas_nodes);
+  const uint4* blas = reinterpret_cast<const uint4*>(S.blas_nodes);
+  const BoxRay wray = make_box_ray(wo, wd);
+  st.sp = 0;
+  st.push(0);
+  while (st.sp > 0) {
+    const uint32_t node = st.pop();
+    float tn[8];
+    uint32_t imask, cbase, pbase, meta[2];
+    const uint32_t hits = intersect_children(tlas, node, wray, tmax, tn, &imask, &cbase, &pbase, meta);
+    uint32_t leaves = hits & ~imask;
+    while (leaves) {
+      const int c = __ffs(leaves) - 1;
+      leaves &= leaves - 1;
+      const uint32_t m = child_meta(meta, c);
+      const uint32_t cnt = m >> 5, off = m & 31u;
+      for (uint32_t k = 0; k < cnt; ++k) {
+        const uint32_t inst_idx = __ldg(S.tlas_prims + pbase + off + k);
+        const Instance inst = S.instances[inst_idx];
+        if (inst.treat_as_boundary) continue;
+        const mat4& wto = S.i_transforms[inst.transform_idx];
+        const vec3 oo = xform_point_glm(wto, wo);
+        const vec3 od = xform_dir_glm(wto, wd);
+        const GeometryDesc& g = S.geometries[inst.geometry_idx];
+        const TriRay tr = make_tri_ray(oo, od);
+        const BoxRay br = make_box_ray(oo, od);
+        const int base = st.sp;
+        st.push(g.node_offset);
+        while (st.sp > base) {
+          const uint32_t bn = st.pop();
+          float btn[8];
+          uint32_t bim, bcb, bpb, bmeta[2];
+          const uint32_t bh = intersect_children(blas, bn, br, tmax, btn, &bim, &bcb, &bpb, bmeta);
+          uint32_t bl = bh & ~bim;
+          while (bl) {
+            const int bc = __ffs(bl) - 1;
+            bl &= bl - 1;
+            const uint32_t bm = child_meta(bmeta, bc);
+            const uint32_t bcnt = bm >> 5, boff = bm & 31u;
+            for (uint32_t q = 0; q < bcnt; ++q) {
+              vec3 p0, p1, p2;
+              uint32_t tid;
+              load_tri(S.wtris, g.wtri_offset + bpb + boff + q, &p0, &p1, &p2, &tid);
+              float t, e[3], inv;
+              ++*tri_tests;
+              if (!tri_test(tr, p0, p1, p2, &t, e, &inv)) continue;
+              if (t < kTMin || t > tmax) continue;
+              st.sp = 0;
+              return true;
+            }
+          }
+          push_sorted(st, bh & bim, btn, bmeta, bcb);
+        }
+      }
+    }
+    push_sorted(st, hits & imask, tn, meta, cbase);
+  }
+  return false;
+}
+
+}  // namespace ym

@@ -1,0 +1,617 @@
+// Wavefront path-tracing kernels for sm_100a.
+//
+// One frame is a sequence of waves over a fixed pool of path slots:
+//   generate -> camera paths for whole 16x16 tiles appended behind the paths
+//               still alive (Ray_generation_path_tracing, src/Shading.cu:1634);
+//   extend   -> closest hit for every live path; misses are accumulated and
+//               retired (Ray_trace_path_tracing, src/Shading.cu:1765);
+//   shade    -> hit reconstruction, next-event estimation with both shadow
+//               rays traced in place, BSDF continuation; surviving paths are
+//               compacted into the other pool with one atomic per warp
+//               (Ray_shading_path_tracing, src/Shading.cu:1953).
+// Path state is structure-of-arrays (float4 / uint2 per field) so every
+// field of a wave is read and written with coalesced 16-byte accesses.
+//
+// Per-path arithmetic follows the reference step for step (see dev_*.cuh),
+// so each path's radiance equals the reference's; only the per-pixel sum of
+// several samples depends on the order in which their atomics land.
+#include <cuda_runtime.h>
+
+#include "dev_sampler.cuh"
+#include "dev_shade.cuh"
+#include "dev_traverse.cuh"
+#include "kernels.h"
+
+namespace ym {
+
+__constant__ DeviceScene c_scene;
+__constant__ RenderSetting c_setting;
+
+// ---------------------------------------------------------------- paths ---
+
+__device__ __forceinline__ void store_path(const PathPool& P, uint32_t i, vec3 o, vec3 d, vec3 tp, vec3 rad, uint32_t pixel,
+                                           uint32_t flags, uint32_t last_inst, uint32_t last_tri, const HaltonState& hs) {
+  P.ray_o[i] = make_float4(o.x, o.y, o.z, 0.0f);
+  P.ray_d[i] = make_float4(d.x, d.y, d.z, 0.0f);
+  P.throughput[i] = make_float4(tp.x, tp.y, tp.z, 0.0f);
+  P.radiance[i] = make_float4(rad.x, rad.y, rad.z, 0.0f);
+  P.pixel_flags[i] = make_uint2(pixel, flags);
+  P.last_hit[i] = make_uint2(last_inst, last_tri);
+  P.sampler[i] = make_uint4((uint32_t)hs.index, (uint32_t)(hs.index >> 32), hs.dim, 0u);
+}
+
+__device__ __forceinline__ void accumulate_pixel(float4* image, uint32_t pixel, vec3 light, float inv_spp) {
+  float* p = reinterpret_cast<float*>(image + pixel);
+  atomicAdd(p + 0, light.x * inv_spp);
+  atomicAdd(p + 1, light.y * inv_spp);
+  atomicAdd(p + 2, light.z * inv_spp);
+  atomicAdd(p + 3, inv_spp);
+}
+
+// Warp-aggregated slot allocation in the output pool.
+__device__ __forceinline__ uint32_t warp_append(uint32_t* counter, bool want) {
+  const uint32_t mask = __ballot_sync(0xFFFFFFFFu, want);
+  if (!want) return kEmpty;
+  const int lane = threadIdx.x & 31;
+  const int leader = __ffs(mask) - 1;
+  uint32_t base = 0;
+  if (lane == leader) base = atomicAdd(counter, (uint32_t)__popc(mask));
+  base = __shfl_sync(mask, base, leader);
+  return base + (uint32_t)__popc(mask & ((1u << lane) - 1u));
+}
+
+__device__ __forceinline__ uint32_t flags_pack(int depth, bool never_scatter, bool camera_ray, int pixel_sample) {
+  return (uint32_t)depth | (never_scatter ? kFlagNeverScatter : 0u) | (camera_ray ? kFlagCameraRay : 0u) |
+         ((uint32_t)pixel_sample << kFlagSampleShift);
+}
+
+// ------------------------------------------------------------ generate ---
+
+__global__ void __launch_bounds__(256) k_generate(PathPool P, uint32_t base, uint32_t count, uint32_t next_tile,
+                                                  uint32_t tiles_x, int frame_index, uint32_t spp) {
+  const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
+  if (tid >= count) return;
+  const DeviceScene& S = c_scene;
+  const uint32_t i = base + tid;
+  const uint32_t per_tile = (uint32_t)kTilePixels * spp;
+  const uint32_t tile_in_batch = tid / per_tile;
+  const uint32_t tile_y = (tile_in_batch + next_tile) / tiles_x;
+  const uint32_t tile_x = (tile_in_batch + next_tile) - tiles_x * tile_y;
+  const uint32_t local = tid - tile_in_batch * per_tile;
+  const uint32_t tile_pixel = local / spp;
+  const uint32_t pixel_sample = local - tile_pixel * spp;
+  const uint32_t tpy = tile_pixel / kTileRes;
+  const uint32_t tpx = tile_pixel - tpy * kTileRes;
+  const uint32_t px = tile_x * kTileRes + tpx;
+  const uint32_t py = tile_y * kTileRes + tpy;
+  if (!(px < (uint32_t)S.width && py < (uint32_t)S.height)) {
+    P.pixel_flags[i] = make_uint2(kEmpty, kFlagDead);
+    return;
+  }
+  const uint32_t pixel = py * (uint32_t)S.width + px;
+  const uint64_t sample_index =
+      halton_index(S, (int)px, (int)py, (frame_index - 1) * c_setting.ssp + (int)pixel_sample);
+  HaltonState hs{sample_index, 2u};
+  float ox = radical_inverse_2(sample_index);
+  float oy = radical_inverse_3(sample_index);
+  ox = ox * S.halton_x_scale - float(px);
+  oy = oy * S.halton_y_scale - float(py);
+  ox = gmin(gmax(ox, 0.000001f), 0.999999f);
+  oy = gmin(gmax(oy, 0.000001f), 0.999999f);
+  // Camera::GenerateRay (src/Camera.h:164-170) + Ray's normalising constructor.
+  const CameraDesc& cam = S.camera;
+  const float ndc_x = float(px + ox) / float(S.width);
+  const float ndc_y = float(py + oy) / float(S.height);
+  const float h = 2.0f * cam.tan_half_fov;
+  const float w = h * cam.aspect_ratio;
+  const vec3 dir = normalize(-cam.w + (ndc_x - 0.5f) * w * cam.u + (ndc_y - 0.5f) * h * cam.v);
+  store_path(P, i, cam.position, dir, vec3(1.0f), vec3(0.0f), pixel, flags_pack(1, true, true, (int)pixel_sample), kEmpty,
+             kEmpty, hs);
+  if (cam.transfer.record_count > 0) P.transfer[i] = cam.transfer;
+  P.transfer_count[i] = (uint8_t)cam.transfer.record_count;
+}
+
+// -------------------------------------------------------------- extend ---
+
+__global__ void __launch_bounds__(kTraceBlock) k_extend(PathPool P, uint32_t count, HitPool H, float4* image,
+                                                        WaveCounters* counters) {
+  __shared__ uint32_t s_stack[kStackShared * kTraceBlock];
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  uint32_t tests = 0;
+  bool active = i < count;
+  uint2 pf = active ? P.pixel_flags[i] : make_uint2(kEmpty, kFlagDead);
+  if (active && (pf.y & kFlagDead)) active = false;
+  bool overflow = false;
+  if (active) {
+    const DeviceScene& S = c_scene;
+    const float4 o4 = P.ray_o[i], d4 = P.ray_d[i];
+    const vec3 o(o4.x, o4.y, o4.z), d(d4.x, d4.y, d4.z);
+    const uint2 lh = P.last_hit[i];
+    TraversalStack st;
+    st.sh = s_stack + threadIdx.x;
+    st.sp = 0;
+    st.overflow = false;
+    ClosestHit ch;
+    const bool hit = trace_closest(S, st, o, d, kTMax, lh.x, lh.y, false, &ch, &tests);
+    overflow = st.overflow;
+    if (!hit) {
+      // Ray_trace_path_tracing miss branch (src/Shading.cu:1855-1864).
+      const float4 r4 = P.radiance[i];
+      vec3 rad(r4.x, r4.y, r4.z);
+      if (c_setting.enable_env_light) {
+        const float4 t4 = P.throughput[i];
+        rad += indirect_clamp(c_setting, vec3(t4.x, t4.y, t4.z) * background(d), (int)(pf.y & kFlagDepthMask));
+      }
+      const float inv_spp = 1.0f / gmax(c_setting.ssp, 1);
+      accumulate_pixel(image, pf.x, rad, inv_spp);
+      P.pixel_flags[i] = make_uint2(pf.x, pf.y | kFlagDead);
+    } else {
+      H.bary_t[i] = make_float4(ch.b0, ch.b1, ch.b2, ch.t);
+      uint32_t nearby_word = (uint32_t)ch.nearby_count;
+      if (!(ch.nearby_count == 1 && ch.nearby[0].prim == ch.inst && ch.nearby[0].t == ch.t &&
+            ch.nearby[0].back == ch.back)) {
+        for (int k = 0; k < ch.nearby_count; ++k)
+          H.nearby[(size_t)i * kMaxNearby + k] =
+              make_uint4(ch.nearby[k].prim, __float_as_uint(ch.nearby[k].t), (uint32_t)ch.nearby[k].back, 0u);
+        nearby_word |= kNearbyExplicit;
+      }
+      H.ids[i] = make_uint4(ch.inst, ch.tri, (uint32_t)ch.back, nearby_word);
+    }
+  }
+  // counters: one atomic per warp
+  const uint32_t n_rays = __popc(__ballot_sync(0xFFFFFFFFu, active));
+  uint32_t t_sum = tests;
+  for (int off = 16; off > 0; off >>= 1) t_sum += __shfl_down_sync(0xFFFFFFFFu, t_sum, off);
+  if ((threadIdx.x & 31) == 0) {
+    if (n_rays) atomicAdd(&counters->extension_rays, (unsigned long long)n_rays);
+    if (t_sum) atomicAdd(&counters->tri_tests, (unsigned long long)t_sum);
+  }
+  if (overflow) atomicOr(&counters->errors, (uint32_t)kDevErrStack);
+}
+
+// --------------------------------------------------------------- shade ---
+
+__device__ __forceinline__ int find_record(const RayTransfer& rt, uint32_t prim) {
+  for (int r = rt.record_count - 1; r >= 0; --r)
+    if (rt.records[r].prim_idx == prim) return r;
+  return -1;
+}
+__device__ __forceinline__ int find_max_priority_record(const RayTransfer& rt) {
+  if (rt.record_count == 0) return -1;
+  uint32_t mp = rt.records[0].ior_priority;
+  int mi = 0;
+  for (int r = 1; r < rt.record_count; ++r)
+    if (rt.records[r].ior_priority >= mp) {
+      mp = rt.records[r].ior_priority;
+      mi = r;
+    }
+  return mi;
+}
+// RayTransfer::PushRecord / PopRecord (src/Ray.h:179-224).
+__device__ __forceinline__ bool push_record(RayTransfer& rt, uint32_t prim, float ior, uint32_t prio, int vol,
+                                            uint32_t* errors) {
+  if (rt.record_count == kMaxBoundaryRecord) {
+    atomicOr(errors, (uint32_t)kDevErrStack);
+    return false;
+  }
+  BoundaryRecord& r = rt.records[rt.record_count];
+  r.prim_idx = prim;
+  r.ior = ior;
+  r.ior_priority = prio;
+  r.vol_idx = vol;
+  ++rt.record_count;
+  if (rt.record_count == 1) {
+    rt.max_priority_record_index = 0;
+    return true;
+  }
+  if (prio >= rt.records[rt.max_priority_record_index].ior_priority) rt.max_priority_record_index = rt.record_count - 1;
+  return true;
+}
+__device__ __forceinline__ void pop_record(RayTransfer& rt, int idx) {
+  if (rt.record_count == 0 || !(idx >= 0 && idx < rt.record_count)) return;
+  for (int k = idx + 1; k < rt.record_count; ++k) rt.records[k - 1] = rt.records[k];
+  --rt.record_count;
+  rt.max_priority_record_index = find_max_priority_record(rt);
+}
+// Material::FetchIOR (src/Material.h:262-278); a light material reports ior 1
+// and priority 0.
+__device__ __forceinline__ float fetch_ior(const Material& m, uint32_t* prio) {
+  if (m.material_type == kDefaultMtl) {
+    *prio = m.default_mtl.ior_priority;
+    return m.default_mtl.ior_n;
+  }
+  *prio = 0;
+  return 1.0f;
+}
+// BoundaryTransitionBunch (src/ShadingUtilities.cuh:954-990).
+__device__ __forceinline__ void boundary_transition(const DeviceScene& S, RayTransfer& rt, const NearbyHit* nb, int n,
+                                                    uint32_t* errors) {
+  for (int k = 0; k < n; ++k) {
+    if (nb[k].back) continue;
+    const Instance inst = S.instances[nb[k].prim];
+    uint32_t prio;
+    const float ior = fetch_ior(S.materials[inst.material_idx], &prio);
+    if (find_record(rt, nb[k].prim) == -1) push_record(rt, nb[k].prim, ior, prio, inst.inner_volume_idx, errors);
+  }
+  for (int k = 0; k < n; ++k) {
+    if (!nb[k].back) continue;
+    const int r = find_record(rt, nb[k].prim);
+    if (r != -1) pop_record(rt, r);
+  }
+}
+// RayTransfer::GetRayIOR / GetExIOR (src/Ray.h:239-258).
+__device__ __forceinline__ float ray_ior(const RayTransfer& rt) {
+  return rt.record_count > 0 ? rt.records[rt.max_priority_record_index].ior : 1.0f;
+}
+__device__ __forceinline__ float ex_ior(const RayTransfer& rt, uint32_t hit_prim) {
+  uint32_t mp = 0;
+  int mi = -1;
+  for (int r = 0; r < rt.record_count; ++r) {
+    if (rt.records[r].prim_idx == hit_prim) continue;
+    if (rt.records[r].ior_priority >= mp) {
+      mp = rt.records[r].ior_priority;
+      mi = r;
+    }
+  }
+  return mi == -1 ? 1.0f : rt.records[mi].ior;
+}
+
+// EvalShapeLight (src/Shading.cu:294-417) for surfaces without media.
+__device__ __forceinline__ vec3 eval_shape_light(const DeviceScene& S, TraversalStack& st, const LayeredBsdf& B,
+                                                 vec3 ray_dir, vec3 p, vec3 p_err, vec3 ng, HaltonState& hs,
+                                                 uint32_t* shadow_rays, uint32_t* tests) {
+  if (S.shape_light_count == 0) return vec3(0.0f);
+  vec3 direct(0.0f);
+  const vec3 wo = B.to_local(-ray_dir);
+  float select_pdf = 0.0f;
+  const int li = sample_light_power(S, halton_next(hs, S.halton_perm), &select_pdf);
+  const ShapeLight L = S.shape_lights[li];
+  const LightTri lt = load_light_tri(S, L);
+  {
+    float u0, u1;
+    halton_next2(hs, S.halton_perm, &u0, &u1);
+    vec3 ldir(0.0f), lpos(0.0f), lerr(0.0f), lng(0.0f), Li(0.0f);
+    float lpdf = 0.0f;
+    const bool valid = light_sample_li(lt, L.area, p, u0, u1, &ldir, &lpos, &lerr, &lng, &Li, &lpdf);
+    const vec3 lwi = B.to_local(ldir);
+    float wpdf = 0.0f;
+    const vec3 f = bsdf_eval(B, wo, lwi, &wpdf);
+    if (max_component(f) > kMinColorEps && valid) {
+      const vec3 so = offset_ray_origin(p, p_err, ldir, ng);
+      const float maxd = length(offset_ray_origin(lpos, lerr, -ldir, lng) - p) * kShadowRayClamp;
+      const bool tb = dot(-ray_dir, ng) * dot(ldir, ng) < 0.0f;
+      const bool invalid = (!same_hemisphere(wo, lwi) && !tb) || (same_hemisphere(wo, lwi) && tb);
+      if (!invalid) {
+        ++*shadow_rays;
+        if (!trace_occluded(S, st, so, normalize(ldir), maxd, tests)) {
+          const float mis = power_heuristic(lpdf, wpdf);
+          direct += mis * 1.0f * vmin(f, vec3(kMaxColorClamp)) * vmin(Li, vec3(kMaxColorClamp));
+        }
+      }
+    }
+  }
+  {
+    float u0, u1, u2;
+    halton_next3(hs, S.halton_perm, &u0, &u1, &u2);
+    vec3 bw, bwi;
+    float bpdf = 0.0f;
+    if (bsdf_sample(B, wo, &bw, &bwi, &bpdf, u0, u1, u2)) {
+      const vec3 ldir = B.to_world(bwi);
+      vec3 lpos(0.0f), lerr(0.0f), lng(0.0f);
+      float wpdf = 0.0f;
+      const vec3 Li = light_eval_li(lt, L.area, p, ldir, &lpos, &lerr, &lng, &wpdf);
+      if (max_component(Li) > kMinColorEps) {
+        const vec3 so = offset_ray_origin(p, p_err, ldir, ng);
+        const float maxd = length(offset_ray_origin(lpos, lerr, -ldir, lng) - p) * kShadowRayClamp;
+        const bool tb = dot(-ray_dir, ng) * dot(ldir, ng) < 0.0f;
+        const bool invalid = (!same_hemisphere(wo, bwi) && !tb) || (same_hemisphere(wo, bwi) && tb);
+        if (!invalid) {
+          ++*shadow_rays;
+          if (!trace_occluded(S, st, so, normalize(ldir), maxd, tests)) {
+            const float mis = power_heuristic(bpdf, wpdf);
+            direct += mis * 1.0f * vmin(bw, vec3(kMaxColorClamp)) * vmin(Li, vec3(kMaxColorClamp));
+          }
+        }
+      }
+    }
+  }
+  return direct * safe_rcp(select_pdf);
+}
+
+__global__ void __launch_bounds__(kTraceBlock) k_shade(PathPool P, uint32_t count, HitPool H, PathPool Q, float4* image,
+                                                       WaveCounters* counters) {
+  __shared__ uint32_t s_stack[kStackShared * kTraceBlock];
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  uint32_t shadow_rays = 0, tests = 0;
+  bool alive = false;  // continues into Q
+  uint2 pf = i < count ? P.pixel_flags[i] : make_uint2(kEmpty, kFlagDead);
+  const bool active = i < count && !(pf.y & kFlagDead);
+
+  vec3 new_o, new_d, tp, rad;
+  uint32_t new_flags = 0, new_last_inst = kEmpty, new_last_tri = kEmpty;
+  HaltonState hs{0, 0};
+  RayTransfer rt;
+  rt.record_count = 0;
+  rt.max_priority_record_index = -1;
+  bool write_transfer = false;
+
+  if (active) {
+    const DeviceScene& S = c_scene;
+    const RenderSetting& rs = c_setting;
+    const float4 o4 = P.ray_o[i], d4 = P.ray_d[i], t4 = P.throughput[i], r4 = P.radiance[i];
+    const vec3 ro(o4.x, o4.y, o4.z), rd(d4.x, d4.y, d4.z);
+    tp = vec3(t4.x, t4.y, t4.z);
+    rad = vec3(r4.x, r4.y, r4.z);
+    const uint4 s4 = P.sampler[i];
+    hs.index = (uint64_t)s4.x | ((uint64_t)s4.y << 32);
+    hs.dim = s4.z;
+    int depth = (int)(pf.y & kFlagDepthMask);
+    bool never_scatter = (pf.y & kFlagNeverScatter) != 0;
+    const uint32_t sample_bits = pf.y & ~(kFlagDepthMask | kFlagNeverScatter | kFlagCameraRay | kFlagDead);
+    const int n_rec = P.transfer_count[i];
+    if (n_rec > 0) rt = P.transfer[i];
+    const float4 bt = H.bary_t[i];
+    const uint4 ids = H.ids[i];
+    const vec3 bary(bt.x, bt.y, bt.z);
+    const uint32_t inst_idx = ids.x, tri = ids.y;
+    const int hit_back = (int)ids.z;
+    NearbyHit nb[kMaxNearby];
+    const int n_nb = (int)(ids.w & 0xFFu);
+    if (ids.w & kNearbyExplicit) {
+      for (int k = 0; k < n_nb; ++k) {
+        const uint4 e = H.nearby[(size_t)i * kMaxNearby + k];
+        nb[k] = NearbyHit{e.x, __uint_as_float(e.y), (int)e.z};
+      }
+    } else {
+      nb[0] = NearbyHit{inst_idx, bt.w, hit_back};
+    }
+    const float inv_spp = 1.0f / gmax(rs.ssp, 1);
+    TraversalStack st;
+    st.sh = s_stack + threadIdx.x;
+    st.sp = 0;
+    st.overflow = false;
+
+    const SurfacePoint sp = fetch_surface(S, inst_idx, tri, bary);
+    const Instance inst = S.instances[inst_idx];
+    bool done = false;
+    if (!(inst.material_idx < S.material_count)) {
+      accumulate_pixel(image, pf.x, rad, inv_spp);
+      done = true;
+    }
+    const Material& mat = S.materials[done ? 0 : inst.material_idx];
+    uint32_t prio = 0;
+    if (!done) fetch_ior(mat, &prio);
+    if (!done && rt.record_count != 0 && prio < rt.records[rt.max_priority_record_index].ior_priority) {
+      // lower-priority boundary: pass straight through, no depth consumed
+      boundary_transition(S, rt, nb, n_nb, &counters->errors);
+      new_o = offset_ray_origin(sp.p, sp.p_err, rd, sp.ng);
+      new_d = normalize(rd);
+      new_flags = flags_pack(depth, never_scatter, false, 0) | sample_bits;
+      new_last_inst = inst_idx;
+      new_last_tri = tri;
+      alive = true;
+      done = true;
+    }
+    if (!done && inst.treat_as_boundary) {
+      boundary_transition(S, rt, nb, n_nb, &counters->errors);
+      new_o = offset_ray_origin(sp.p, sp.p_err, rd, sp.ng);
+      new_d = normalize(rd);
+      new_flags = flags_pack(depth, never_scatter, false, 0) | sample_bits;
+      new_last_inst = inst_idx;
+      new_last_tri = tri;
+      alive = true;
+      done = true;
+    }
+    if (!done && mat.material_type == kLightMtl) {
+      if (never_scatter) rad += indirect_clamp(rs, tp * mat.light_mtl.light_color * mat.light_mtl.intensity, depth);
+      accumulate_pixel(image, pf.x, rad, inv_spp);
+      done = true;
+    }
+    if (!done) {
+      LayeredBsdf B;
+      init_shading_frame(B, hit_back, rd, sp.ng, sp.ns, sp.dpdu, sp.dpdv);
+      init_layered_lobes(B, mat.default_mtl, rd, hit_back, ray_ior(rt), ex_ior(rt, inst_idx));
+      if (rs.enable_shape_light)
+        rad += indirect_clamp(rs, tp * eval_shape_light(S, st, B, rd, sp.p, sp.p_err, sp.ng, hs, &shadow_rays, &tests),
+                              depth);
+      const vec3 wo = B.to_local(-rd);
+      vec3 w, wi;
+      float pdf = 0.0f;
+      float u0, u1, u2;
+      halton_next3(hs, S.halton_perm, &u0, &u1, &u2);
+      const bool valid = bsdf_sample(B, wo, &w, &wi, &pdf, u0, u1, u2);
+      if (!valid) {
+        accumulate_pixel(image, pf.x, rad, inv_spp);
+      } else {
+        tp *= w;
+        float rr = gmax(tp.x, gmax(tp.y, tp.z));
+        rr = gmin(rr, 1.0f);
+        bool terminate = false;
+        if (depth + 1 > rs.ray_depth) {
+          if (rs.enable_russian_roulette && halton_next(hs, S.halton_perm) < rr) tp /= gmax(rr, kMinColorEps);
+          else terminate = true;
+        }
+        if (!terminate) {
+          const vec3 nd = B.to_world(wi);
+          const bool tb = dot(-rd, sp.ng) * dot(nd, sp.ng) < 0.0f;
+          const bool invalid = (!same_hemisphere(wo, wi) && !tb) || (same_hemisphere(wo, wi) && tb);
+          if (invalid) {
+            terminate = true;
+          } else {
+            if (tb) boundary_transition(S, rt, nb, n_nb, &counters->errors);
+            new_o = offset_ray_origin(sp.p, sp.p_err, nd, sp.ng);
+            new_d = normalize(nd);
+            never_scatter = false;
+            depth += 1;
+            if (depth > kMaxRayDepth) {
+              terminate = true;
+            } else {
+              new_flags = flags_pack(depth, false, false, 0) | sample_bits;
+              new_last_inst = inst_idx;
+              new_last_tri = tri;
+              alive = true;
+            }
+          }
+        }
+        if (terminate) accumulate_pixel(image, pf.x, rad, inv_spp);
+      }
+    }
+    write_transfer = rt.record_count > 0 || n_rec > 0;
+    if (st.overflow) atomicOr(&counters->errors, (uint32_t)kDevErrStack);
+  }
+  const uint32_t slot = warp_append(&counters->next_count, alive);
+  if (alive) {
+    if (slot < Q.capacity) {
+      store_path(Q, slot, new_o, new_d, tp, rad, pf.x, new_flags, new_last_inst, new_last_tri, hs);
+      Q.transfer_count[slot] = (uint8_t)rt.record_count;
+      if (write_transfer && rt.record_count > 0) Q.transfer[slot] = rt;
+    } else {
+      atomicOr(&counters->errors, (uint32_t)kDevErrQueue);
+    }
+  }
+  uint32_t s_sum = shadow_rays, t_sum = tests;
+  for (int off = 16; off > 0; off >>= 1) {
+    s_sum += __shfl_down_sync(0xFFFFFFFFu, s_sum, off);
+    t_sum += __shfl_down_sync(0xFFFFFFFFu, t_sum, off);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    if (s_sum) atomicAdd(&counters->shadow_rays, (unsigned long long)s_sum);
+    if (t_sum) atomicAdd(&counters->tri_tests, (unsigned long long)t_sum);
+  }
+}
+
+// ----------------------------------------------------------- accumulate ---
+
+__global__ void k_accumulate(const float4* noise, float4* acc, uint32_t n, int frame_index) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  if (frame_index == 1) {
+    acc[i] = noise[i];
+  } else {
+    const float4 a = acc[i], z = noise[i];
+    const float f1 = float(frame_index - 1), f = float(frame_index);
+    acc[i] = make_float4((a.x * f1 + z.x) / f, (a.y * f1 + z.y) / f, (a.z * f1 + z.z) / f, (a.w * f1 + z.w) / f);
+  }
+}
+
+// ---------------------------------------------------- known-answer tests ---
+
+__global__ void __launch_bounds__(kTraceBlock) k_debug_trace(int n, const float* origin, const float* dir,
+                                                             const uint32_t* last_hit, uint32_t* inst, uint32_t* tri,
+                                                             float* t, float* bary, int* back, int* nearby,
+                                                             uint32_t* errors) {
+  __shared__ uint32_t s_stack[kStackShared * kTraceBlock];
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  TraversalStack st;
+  st.sh = s_stack + threadIdx.x;
+  st.sp = 0;
+  st.overflow = false;
+  const vec3 o(origin[3 * i], origin[3 * i + 1], origin[3 * i + 2]);
+  const vec3 d = normalize(vec3(dir[3 * i], dir[3 * i + 1], dir[3 * i + 2]));
+  ClosestHit ch;
+  uint32_t tests = 0;
+  const bool hit = trace_closest(c_scene, st, o, d, kTMax, last_hit ? last_hit[2 * i] : kEmpty,
+                                 last_hit ? last_hit[2 * i + 1] : kEmpty, false, &ch, &tests);
+  inst[i] = hit ? ch.inst : kEmpty;
+  tri[i] = hit ? ch.tri : kEmpty;
+  t[i] = hit ? ch.t : kTMax;
+  bary[3 * i] = hit ? ch.b0 : 1.0f;
+  bary[3 * i + 1] = hit ? ch.b1 : 1.0f;
+  bary[3 * i + 2] = hit ? ch.b2 : 1.0f;
+  back[i] = hit ? ch.back : 0;
+  nearby[i] = hit ? ch.nearby_count : 0;
+  if (st.overflow) atomicOr(errors, (uint32_t)kDevErrStack);
+}
+
+__global__ void __launch_bounds__(kTraceBlock) k_debug_occluded(int n, const float* origin, const float* dir,
+                                                                const float* tmax, int* occluded, uint32_t* errors) {
+  __shared__ uint32_t s_stack[kStackShared * kTraceBlock];
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  TraversalStack st;
+  st.sh = s_stack + threadIdx.x;
+  st.sp = 0;
+  st.overflow = false;
+  const vec3 o(origin[3 * i], origin[3 * i + 1], origin[3 * i + 2]);
+  const vec3 d = normalize(vec3(dir[3 * i], dir[3 * i + 1], dir[3 * i + 2]));
+  uint32_t tests = 0;
+  occluded[i] = trace_occluded(c_scene, st, o, d, tmax[i], &tests) ? 1 : 0;
+  if (st.overflow) atomicOr(errors, (uint32_t)kDevErrStack);
+}
+
+__global__ void k_debug_halton(int n, const int* px, const int* py, const int* sample, int n_dims, uint64_t* index,
+                               float* offset, float* dims) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const DeviceScene& S = c_scene;
+  const uint64_t idx = halton_index(S, px[i], py[i], sample[i]);
+  index[i] = idx;
+  float ox = radical_inverse_2(idx), oy = radical_inverse_3(idx);
+  ox = ox * S.halton_x_scale - float(px[i]);
+  oy = oy * S.halton_y_scale - float(py[i]);
+  offset[2 * i] = gmin(gmax(ox, 0.000001f), 0.999999f);
+  offset[2 * i + 1] = gmin(gmax(oy, 0.000001f), 0.999999f);
+  HaltonState hs{idx, 2u};
+  for (int d = 0; d < n_dims; ++d) dims[(size_t)i * n_dims + d] = halton_next(hs, S.halton_perm);
+}
+
+// ------------------------------------------------------------ launchers ---
+
+cudaError_t upload_constants(const DeviceScene& scene, const uint32_t* primes, const uint32_t* prime_sums,
+                             cudaStream_t stream) {
+  cudaError_t e = cudaMemcpyToSymbolAsync(c_scene, &scene, sizeof(DeviceScene), 0, cudaMemcpyHostToDevice, stream);
+  if (e != cudaSuccess) return e;
+  e = cudaMemcpyToSymbolAsync(c_primes, primes, sizeof(uint32_t) * kHaltonDims, 0, cudaMemcpyHostToDevice, stream);
+  if (e != cudaSuccess) return e;
+  return cudaMemcpyToSymbolAsync(c_prime_sums, prime_sums, sizeof(uint32_t) * kHaltonDims, 0, cudaMemcpyHostToDevice,
+                                 stream);
+}
+
+cudaError_t upload_setting(const RenderSetting& rs, cudaStream_t stream) {
+  return cudaMemcpyToSymbolAsync(c_setting, &rs, sizeof(RenderSetting), 0, cudaMemcpyHostToDevice, stream);
+}
+
+void launch_generate(const PathPool& P, uint32_t base, uint32_t count, uint32_t next_tile, uint32_t tiles_x,
+                     int frame_index, uint32_t spp, cudaStream_t stream) {
+  if (count == 0) return;
+  k_generate<<<(count + 255) / 256, 256, 0, stream>>>(P, base, count, next_tile, tiles_x, frame_index, spp);
+}
+
+void launch_extend(const PathPool& P, uint32_t count, const HitPool& H, float4* image, WaveCounters* counters,
+                   cudaStream_t stream) {
+  if (count == 0) return;
+  k_extend<<<(count + kTraceBlock - 1) / kTraceBlock, kTraceBlock, 0, stream>>>(P, count, H, image, counters);
+}
+
+void launch_shade(const PathPool& P, uint32_t count, const HitPool& H, const PathPool& Q, float4* image,
+                  WaveCounters* counters, cudaStream_t stream) {
+  if (count == 0) return;
+  k_shade<<<(count + kTraceBlock - 1) / kTraceBlock, kTraceBlock, 0, stream>>>(P, count, H, Q, image, counters);
+}
+
+void launch_accumulate(const float4* noise, float4* acc, uint32_t n, int frame_index, cudaStream_t stream) {
+  if (n == 0) return;
+  k_accumulate<<<(n + 255) / 256, 256, 0, stream>>>(noise, acc, n, frame_index);
+}
+
+void launch_debug_trace(int n, const float* o, const float* d, const uint32_t* lh, uint32_t* inst, uint32_t* tri,
+                        float* t, float* bary, int* back, int* nearby, uint32_t* errors, cudaStream_t stream) {
+  if (n <= 0) return;
+  k_debug_trace<<<(n + kTraceBlock - 1) / kTraceBlock, kTraceBlock, 0, stream>>>(n, o, d, lh, inst, tri, t, bary, back,
+                                                                                 nearby, errors);
+}
+
+void launch_debug_occluded(int n, const float* o, const float* d, const float* tmax, int* occ, uint32_t* errors,
+                           cudaStream_t stream) {
+  if (n <= 0) return;
+  k_debug_occluded<<<(n + kTraceBlock - 1) / kTraceBlock, kTraceBlock, 0, stream>>>(n, o, d, tmax, occ, errors);
+}
+
+void launch_debug_halton(int n, const int* px, const int* py, const int* sample, int n_dims, uint64_t* index,
+                         float* offset, float* dims, cudaStream_t stream) {
+  if (n <= 0) return;
+  k_debug_halton<<<(n + 127) / 128, 128, 0, stream>>>(n, px, py, sample, n_dims, index, offset, dims);
+}
+
+}  // namespace ym

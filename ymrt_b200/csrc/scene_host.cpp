@@ -1,0 +1,1075 @@
+// Host-side scene preparation: .ymtmp loading, transforms, BVH ordering,
+// wide-BVH construction, shape-light table, camera. See scene_host.h.
+//
+// Built with -ffp-contract=off: the transform matrices, triangle boxes and
+// light powers are rounded exactly as the reference computes them, because
+// the kernels' intersection results depend on those bits.
+#include "scene_host.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <functional>
+#include <sstream>
+#include <unordered_map>
+
+#include "../../include/ymrt.h"
+
+namespace ym {
+
+// ------------------------------------------------------------- matrices ---
+// glm 0.9.8 operation order (glm/detail/type_mat4x4.inl, glm/gtc/matrix_transform.inl,
+// glm/detail/func_matrix.inl), as used by InitTransformMatrix (src/Transform.h:39-66).
+
+namespace {
+struct v4 {
+  float x, y, z, w;
+};
+inline v4 operator*(v4 a, float s) { return {a.x * s, a.y * s, a.z * s, a.w * s}; }
+inline v4 operator*(v4 a, v4 b) { return {a.x * b.x, a.y * b.y, a.z * b.z, a.w * b.w}; }
+inline v4 operator+(v4 a, v4 b) { return {a.x + b.x, a.y + b.y, a.z + b.z, a.w + b.w}; }
+inline v4 operator-(v4 a, v4 b) { return {a.x - b.x, a.y - b.y, a.z - b.z, a.w - b.w}; }
+inline v4 col(const mat4& m, int c) { return {m.m[c][0], m.m[c][1], m.m[c][2], m.m[c][3]}; }
+inline void set_col(mat4& m, int c, v4 v) {
+  m.m[c][0] = v.x; m.m[c][1] = v.y; m.m[c][2] = v.z; m.m[c][3] = v.w;
+}
+inline mat4 identity() {
+  mat4 r{};
+  for (int i = 0; i < 4; ++i) r.m[i][i] = 1.0f;
+  return r;
+}
+inline float radians(float deg) { return deg * static_cast<float>(0.01745329251994329576923690768489); }
+
+mat4 translate(const mat4& m, vec3 v) {
+  mat4 r = m;
+  set_col(r, 3, col(m, 0) * v.x + col(m, 1) * v.y + col(m, 2) * v.z + col(m, 3));
+  return r;
+}
+mat4 scale(const mat4& m, vec3 v) {
+  mat4 r;
+  set_col(r, 0, col(m, 0) * v.x);
+  set_col(r, 1, col(m, 1) * v.y);
+  set_col(r, 2, col(m, 2) * v.z);
+  set_col(r, 3, col(m, 3));
+  return r;
+}
+mat4 rotate(const mat4& m, float angle, vec3 axis_in) {
+  const float c = std::cos(angle);
+  const float s = std::sin(angle);
+  const vec3 axis = normalize(axis_in);
+  const vec3 temp = (1.0f - c) * axis;
+  float R[3][3];
+  R[0][0] = c + temp.x * axis.x;
+  R[0][1] = temp.x * axis.y + s * axis.z;
+  R[0][2] = temp.x * axis.z - s * axis.y;
+  R[1][0] = temp.y * axis.x - s * axis.z;
+  R[1][1] = c + temp.y * axis.y;
+  R[1][2] = temp.y * axis.z + s * axis.x;
+  R[2][0] = temp.z * axis.x + s * axis.y;
+  R[2][1] = temp.z * axis.y - s * axis.x;
+  R[2][2] = c + temp.z * axis.z;
+  mat4 r;
+  for (int i = 0; i < 3; ++i) set_col(r, i, col(m, 0) * R[i][0] + col(m, 1) * R[i][1] + col(m, 2) * R[i][2]);
+  set_col(r, 3, col(m, 3));
+  return r;
+}
+}  // namespace
+
+mat4 mat4_mul(const mat4& a, const mat4& b) {
+  mat4 r;
+  for (int j = 0; j < 4; ++j) {
+    const v4 bj = col(b, j);
+    set_col(r, j, col(a, 0) * bj.x + col(a, 1) * bj.y + col(a, 2) * bj.z + col(a, 3) * bj.w);
+  }
+  return r;
+}
+
+mat4 mat4_inverse(const mat4& M) {
+  const float (*m)[4] = M.m;
+  const float c00 = m[2][2] * m[3][3] - m[3][2] * m[2][3];
+  const float c02 = m[1][2] * m[3][3] - m[3][2] * m[1][3];
+  const float c03 = m[1][2] * m[2][3] - m[2][2] * m[1][3];
+  const float c04 = m[2][1] * m[3][3] - m[3][1] * m[2][3];
+  const float c06 = m[1][1] * m[3][3] - m[3][1] * m[1][3];
+  const float c07 = m[1][1] * m[2][3] - m[2][1] * m[1][3];
+  const float c08 = m[2][1] * m[3][2] - m[3][1] * m[2][2];
+  const float c10 = m[1][1] * m[3][2] - m[3][1] * m[1][2];
+  const float c11 = m[1][1] * m[2][2] - m[2][1] * m[1][2];
+  const float c12 = m[2][0] * m[3][3] - m[3][0] * m[2][3];
+  const float c14 = m[1][0] * m[3][3] - m[3][0] * m[1][3];
+  const float c15 = m[1][0] * m[2][3] - m[2][0] * m[1][3];
+  const float c16 = m[2][0] * m[3][2] - m[3][0] * m[2][2];
+  const float c18 = m[1][0] * m[3][2] - m[3][0] * m[1][2];
+  const float c19 = m[1][0] * m[2][2] - m[2][0] * m[1][2];
+  const float c20 = m[2][0] * m[3][1] - m[3][0] * m[2][1];
+  const float c22 = m[1][0] * m[3][1] - m[3][0] * m[1][1];
+  const float c23 = m[1][0] * m[2][1] - m[2][0] * m[1][1];
+  const v4 f0{c00, c00, c02, c03}, f1{c04, c04, c06, c07}, f2{c08, c08, c10, c11};
+  const v4 f3{c12, c12, c14, c15}, f4{c16, c16, c18, c19}, f5{c20, c20, c22, c23};
+  const v4 e0{m[1][0], m[0][0], m[0][0], m[0][0]};
+  const v4 e1{m[1][1], m[0][1], m[0][1], m[0][1]};
+  const v4 e2{m[1][2], m[0][2], m[0][2], m[0][2]};
+  const v4 e3{m[1][3], m[0][3], m[0][3], m[0][3]};
+  const v4 i0 = e1 * f0 - e2 * f1 + e3 * f2;
+  const v4 i1 = e0 * f0 - e2 * f3 + e3 * f4;
+  const v4 i2 = e0 * f1 - e1 * f3 + e3 * f5;
+  const v4 i3 = e0 * f2 - e1 * f4 + e2 * f5;
+  const v4 sa{+1, -1, +1, -1}, sb{-1, +1, -1, +1};
+  mat4 inv;
+  set_col(inv, 0, i0 * sa);
+  set_col(inv, 1, i1 * sb);
+  set_col(inv, 2, i2 * sa);
+  set_col(inv, 3, i3 * sb);
+  const v4 row0{inv.m[0][0], inv.m[1][0], inv.m[2][0], inv.m[3][0]};
+  const v4 d0 = col(M, 0) * row0;
+  const float d1 = (d0.x + d0.y) + (d0.z + d0.w);
+  const float one_over_det = 1.0f / d1;
+  mat4 r;
+  for (int c = 0; c < 4; ++c) set_col(r, c, col(inv, c) * one_over_det);
+  return r;
+}
+
+mat4 compose_transform(vec3 t, vec3 s, vec3 r_deg) {
+  const mat4 I = identity();
+  mat4 m = translate(I, t);
+  m = mat4_mul(m, rotate(I, radians(r_deg.z), vec3(0.0f, 0.0f, 1.0f)));
+  m = mat4_mul(m, rotate(I, radians(r_deg.y), vec3(0.0f, 1.0f, 0.0f)));
+  m = mat4_mul(m, rotate(I, radians(r_deg.x), vec3(1.0f, 0.0f, 0.0f)));
+  m = mat4_mul(m, scale(I, s));
+  return m;
+}
+
+// ------------------------------------------------------------ bounding ---
+// BBox3 helpers, src/BoundingBox.h:10-140.
+
+namespace {
+inline BBox box_extend(const BBox& b, vec3 p) {
+  BBox r;
+  r.pmin = vec3(gmin(b.pmin.x, p.x), gmin(b.pmin.y, p.y), gmin(b.pmin.z, p.z));
+  r.pmax = vec3(gmax(b.pmax.x, p.x), gmax(b.pmax.y, p.y), gmax(b.pmax.z, p.z));
+  return r;
+}
+inline BBox box_union(const BBox& a, const BBox& b) {
+  BBox r;
+  r.pmin = vec3(gmin(a.pmin.x, b.pmin.x), gmin(a.pmin.y, b.pmin.y), gmin(a.pmin.z, b.pmin.z));
+  r.pmax = vec3(gmax(a.pmax.x, b.pmax.x), gmax(a.pmax.y, b.pmax.y), gmax(a.pmax.z, b.pmax.z));
+  return r;
+}
+inline BBox bound_fix(const BBox& in) {
+  const float eps = 0.0005f;
+  BBox b = in;
+  for (int i = 0; i < 3; ++i) {
+    if (b.pmax[i] < b.pmin[i]) std::swap(b.pmax[i], b.pmin[i]);
+    if (std::fabs(b.pmax[i] - b.pmin[i]) < 2.0f * eps) {
+      b.pmax[i] += eps;
+      b.pmin[i] -= eps;
+    }
+  }
+  return b;
+}
+inline float box_area(const BBox& b) {
+  const vec3 e = b.pmax - b.pmin;
+  return 2.f * (e.x * e.y + e.y * e.z + e.x * e.z);
+}
+inline int box_longest_axis(const BBox& b) {
+  const vec3 d = b.pmax - b.pmin;
+  int a = 0;
+  if (d[1] > d[a]) a = 1;
+  if (d[2] > d[a]) a = 2;
+  return a;
+}
+inline vec3 box_center(const BBox& b) { return (b.pmax + b.pmin) * 0.5f; }
+inline BBox box_transform(const BBox& b, const mat4& M) {
+  BBox r;
+  for (int i = 0; i < 8; ++i) {
+    const vec3 c((i & 1) ? b.pmax.x : b.pmin.x, (i & 2) ? b.pmax.y : b.pmin.y, (i & 4) ? b.pmax.z : b.pmin.z);
+    r = box_extend(r, xform_point_glm(M, c));
+  }
+  return bound_fix(r);
+}
+
+// --------------------------------------------------- binary BVH (order) ---
+// The reference's top-down SAH builder (src/BottomBVH.cpp:34-166,
+// src/BottomBVH.h:40-190, src/TopBVH.cpp:34-198): 24 bins per axis, a
+// median split (heap selection) when SAH declines or partitioning fails,
+// one primitive per leaf, children flattened depth-first. Its partitioning
+// and selection steps are reproduced step for step, because the resulting
+// primitive order defines the triangle and instance indices (and the
+// shape-light order) that the rest of the pipeline reports.
+
+struct BuildItem {
+  BBox box;
+  vec3 center;
+  uint32_t idx;
+};
+
+struct BinNode {
+  BBox box;
+  uint32_t left = kEmpty, right = kEmpty;
+  uint32_t offset = 0, count = 0;
+};
+
+void heap_down(BuildItem* t, uint32_t i, uint32_t right, int axis) {
+  for (;;) {
+    const uint32_t lc = 2 * i + 1, rc = 2 * i + 2;
+    if (!(lc <= right)) return;
+    uint32_t target = lc;
+    if (rc <= right && t[rc].center[axis] > t[lc].center[axis]) target = rc;
+    if (t[i].center[axis] > t[target].center[axis]) return;
+    std::swap(t[i], t[target]);
+    i = target;
+  }
+}
+
+uint32_t find_mid_element(BuildItem* t, uint32_t count, int axis) {
+  const uint32_t n_th = (count - 1) / 2;
+  uint32_t n_pass = count - n_th;
+  for (uint32_t i = count / 2 - 1; i != kEmpty; --i) heap_down(t, i, count - 1, axis);
+  for (uint32_t i = count - 1; i > 0 && n_pass > 0; --i, --n_pass) {
+    std::swap(t[0], t[i]);
+    heap_down(t, 0, i - 1, axis);
+  }
+  return n_th;
+}
+
+uint32_t partition_items(BuildItem* t, uint32_t count, float pivot, int axis) {
+  uint32_t left = 0, right = count - 1;
+  while (left <= right && right != kEmpty) {
+    if (t[left].center[axis] <= pivot) ++left;
+    else std::swap(t[left], t[right--]);
+  }
+  return right;
+}
+
+bool eval_sah(const BuildItem* prims, uint32_t count, const BBox& cb, float parent_cost, float* split_pos,
+              int* split_axis) {
+  constexpr int kBins = 24;
+  int best_axis = -1;
+  float best_pos = 0.0f, best_cost = 1E36f;
+  struct Bin {
+    uint32_t count = 0;
+    BBox box;
+  };
+  bool valid[3] = {true, true, true};
+  vec3 ext = cb.pmax - cb.pmin;
+  for (int a = 0; a < 3; ++a)
+    if (ext[a] < kFloatEps) {
+      valid[a] = false;
+      ext[a] = kFloatEps;
+    }
+  Bin bins[kBins][3];
+  const vec3 i_ext = vec3(1.0f) / ext;
+  const vec3 bin_len = vmax(cb.pmax - cb.pmin, vec3(0.0f)) / float(kBins);
+  for (uint32_t i = 0; i < count; ++i) {
+    const vec3 ndc = (prims[i].center - cb.pmin) * i_ext;
+    for (int a = 0; a < 3; ++a) {
+      const int b = gmax(gmin((int)(ndc[a] * kBins), kBins - 1), 0);
+      bins[b][a].count++;
+      bins[b][a].box = box_union(bins[b][a].box, prims[i].box);
+    }
+  }
+  float la[kBins - 1][3], ra[kBins - 1][3];
+  uint32_t lc[kBins - 1][3], rc[kBins - 1][3];
+  for (int a = 0; a < 3; ++a) {
+    if (!valid[a]) continue;
+    BBox lb, rb;
+    uint32_t lcount = 0, rcount = 0;
+    for (int i = 0; i < kBins - 1; ++i) {
+      lcount += bins[i][a].count;
+      lb = box_union(lb, bins[i][a].box);
+      lc[i][a] = lcount;
+      la[i][a] = box_area(lb);
+      rcount += bins[kBins - 1 - i][a].count;
+      rb = box_union(rb, bins[kBins - 1 - i][a].box);
+      rc[kBins - 2 - i][a] = rcount;
+      ra[kBins - 2 - i][a] = box_area(rb);
+    }
+    for (int i = 0; i < kBins - 1; ++i) {
+      const float cost = lc[i][a] * la[i][a] + rc[i][a] * ra[i][a];
+      if (cost <= 0.0f) continue;
+      if (cost < best_cost) {
+        best_cost = cost;
+        best_axis = a;
+        best_pos = cb.pmin[a] + float(i + 1) * bin_len[a];
+      }
+    }
+  }
+  if (best_axis == -1 || best_cost >= parent_cost) return false;
+  *split_axis = best_axis;
+  *split_pos = best_pos;
+  return true;
+}
+
+// Builds the binary tree; reorders `items` in place. Returns the nodes in
+// build (breadth-first) order, root at 0.
+std::vector<BinNode> build_binary(std::vector<BuildItem>& items) {
+  const uint32_t n = (uint32_t)items.size();
+  std::vector<BinNode> nodes;
+  if (n == 0) return nodes;
+  nodes.resize(2 * n - 1);
+  std::vector<char> mid_split(2 * n - 1, 0);
+  nodes[0].offset = 0;
+  nodes[0].count = n;
+  uint32_t start = 0, total = 1;
+  while (total - start > 0) {
+    const uint32_t process = total - start;
+    for (uint32_t ni = start; ni < start + process; ++ni) {
+      BinNode& node = nodes[ni];
+      BuildItem* its = items.data() + node.offset;
+      BBox nb, cb;
+      for (uint32_t i = 0; i < node.count; ++i) {
+        nb = box_union(nb, its[i].box);
+        cb = box_extend(cb, its[i].center);
+      }
+      node.box = nb;
+      auto make_mid = [&]() {
+        const int axis = box_longest_axis(nb);
+        const uint32_t mid = find_mid_element(its, node.count, axis);
+        const uint32_t l = total;
+        total += 2;
+        node.left = l;
+        node.right = l + 1;
+        nodes[l].offset = node.offset;
+        nodes[l].count = mid + 1;
+        mid_split[l] = 1;
+        nodes[l + 1].offset = node.offset + mid + 1;
+        nodes[l + 1].count = node.count - 1 - mid;
+        mid_split[l + 1] = 1;
+      };
+      if (node.count <= 1) {
+        node.left = node.right = kEmpty;
+        continue;
+      }
+      if (mid_split[ni]) {
+        make_mid();
+        continue;
+      }
+      const float parent_cost = node.count * box_area(node.box);
+      int axis = 0;
+      float pos = 0.0f;
+      if (!eval_sah(its, node.count, cb, parent_cost, &pos, &axis)) {
+        make_mid();
+        continue;
+      }
+      const uint32_t split = partition_items(its, node.count, pos, axis);
+      if (split == kEmpty || split == node.count - 1) {
+        make_mid();
+        continue;
+      }
+      const uint32_t l = total;
+      total += 2;
+      node.left = l;
+      node.right = l + 1;
+      nodes[l].offset = node.offset;
+      nodes[l].count = split + 1;
+      nodes[l + 1].offset = node.offset + split + 1;
+      nodes[l + 1].count = node.count - 1 - split;
+    }
+    start += process;
+  }
+  nodes.resize(total);
+  return nodes;
+}
+
+// ------------------------------------------------------- wide BVH (8) ---
+
+constexpr int kWide = 8;
+constexpr uint32_t kMaxLeafPrims = 3;
+
+struct WideBuilder {
+  const std::vector<BinNode>* bin;
+  std::vector<WideNode>* out;
+  std::vector<uint32_t>* prim_order;  // primitive (item position) per wide-leaf slot
+
+  static uint8_t quant_exp(float extent) {
+    // smallest e with extent / 2^e <= 250 (margin for outward rounding)
+    int e = -126;
+    if (extent > 0.0f) e = (int)std::ceil(std::log2(extent / 250.0f));
+    e = std::max(-126, std::min(127, e));
+    return (uint8_t)(e + 127);
+  }
+  static float exp_scale(uint8_t be) { return u2f((uint32_t)be << 23); }
+
+  // Grows a box by a relative margin so float rounding in the slab test can
+  // never reject a ray that touches the exact box.
+  static BBox pad(const BBox& b) {
+    BBox r = b;
+    for (int a = 0; a < 3; ++a) {
+      const float m = 2e-6f * std::max(std::fabs(b.pmin[a]), std::fabs(b.pmax[a])) + 1e-30f;
+      r.pmin[a] = b.pmin[a] - m;
+      r.pmax[a] = b.pmax[a] + m;
+    }
+    return r;
+  }
+
+  uint32_t subtree_prims(uint32_t ni) const { return (*bin)[ni].count; }
+
+  // Fills node `slot` of `out` from binary node `root`.
+  void build(uint32_t root, uint32_t slot) {
+    const auto& B = *bin;
+    std::vector<uint32_t> cand;
+    if (B[root].left == kEmpty) {
+      cand.push_back(root);  // single-leaf tree
+    } else {
+      cand.push_back(B[root].left);
+      cand.push_back(B[root].right);
+      while ((int)cand.size() < kWide) {
+        int best = -1;
+        float best_area = -1.0f;
+        for (int i = 0; i < (int)cand.size(); ++i) {
+          const BinNode& c = B[cand[i]];
+          if (c.left == kEmpty || c.count <= kMaxLeafPrims) continue;
+          const float a = box_area(c.box);
+          if (a > best_area) {
+            best_area = a;
+            best = i;
+          }
+        }
+        if (best < 0) break;
+        const uint32_t e = cand[best];
+        cand[best] = B[e].left;
+        cand.insert(cand.begin() + best + 1, B[e].right);
+      }
+    }
+    WideNode node;
+    std::memset(&node, 0, sizeof(node));
+    BBox all;
+    std::vector<BBox> boxes;
+    for (uint32_t c : cand) {
+      boxes.push_back(pad(B[c].box));
+      all = box_union(all, boxes.back());
+    }
+    node.ox = all.pmin.x;
+    node.oy = all.pmin.y;
+    node.oz = all.pmin.z;
+    node.ex = quant_exp(all.pmax.x - all.pmin.x);
+    node.ey = quant_exp(all.pmax.y - all.pmin.y);
+    node.ez = quant_exp(all.pmax.z - all.pmin.z);
+    node.prim_base = (uint32_t)prim_order->size();
+    std::vector<uint32_t> internal;
+    for (size_t i = 0; i < cand.size(); ++i) {
+      const BinNode& c = B[cand[i]];
+      if (c.left == kEmpty || c.count <= kMaxLeafPrims) {
+        const uint32_t off = (uint32_t)prim_order->size() - node.prim_base;
+        for (uint32_t k = 0; k < c.count; ++k) prim_order->push_back(c.offset + k);
+        node.meta[i] = (uint8_t)((c.count << 5) | off);
+      } else {
+        node.imask |= (uint8_t)(1u << i);
+        node.meta[i] = (uint8_t)internal.size();
+        internal.push_back(cand[i]);
+      }
+    }
+    // Quantise every child box on the node grid origin + q * 2^e, decoding
+    // exactly as the kernel does (one fmaf) and rounding outwards; widen the
+    // grid step if a bound does not fit in 8 bits.
+    const float org[3] = {node.ox, node.oy, node.oz};
+    uint8_t* exps[3] = {&node.ex, &node.ey, &node.ez};
+    uint8_t* qlo[3] = {node.qlo_x, node.qlo_y, node.qlo_z};
+    uint8_t* qhi[3] = {node.qhi_x, node.qhi_y, node.qhi_z};
+    for (int a = 0; a < 3; ++a) {
+      for (;;) {
+        const float sc = exp_scale(*exps[a]);
+        bool ok = true;
+        for (size_t i = 0; i < cand.size() && ok; ++i) {
+          int lo = (int)std::floor((boxes[i].pmin[a] - org[a]) / sc);
+          int hi = (int)std::ceil((boxes[i].pmax[a] - org[a]) / sc);
+          lo = std::max(0, std::min(255, lo));
+          hi = std::max(0, std::min(255, hi));
+          while (lo > 0 && std::fma((float)lo, sc, org[a]) > boxes[i].pmin[a]) --lo;
+          while (hi < 255 && std::fma((float)hi, sc, org[a]) < boxes[i].pmax[a]) ++hi;
+          if (std::fma((float)lo, sc, org[a]) > boxes[i].pmin[a] || std::fma((float)hi, sc, org[a]) < boxes[i].pmax[a])
+            ok = false;
+          qlo[a][i] = (uint8_t)lo;
+          qhi[a][i] = (uint8_t)hi;
+        }
+        if (ok || *exps[a] >= 254) break;
+        ++*exps[a];
+      }
+    }
+    node.child_base = (uint32_t)out->size();
+    out->resize(out->size() + internal.size());
+    (*out)[slot] = node;
+    for (size_t k = 0; k < internal.size(); ++k) build(internal[k], node.child_base + (uint32_t)k);
+  }
+};
+
+// Builds the wide BVH for a binary tree; appends nodes to `out` (root first)
+// and the primitive order of the leaves to `prim_order`.
+uint32_t build_wide(const std::vector<BinNode>& bin, std::vector<WideNode>* out, std::vector<uint32_t>* prim_order) {
+  const uint32_t root = (uint32_t)out->size();
+  out->resize(out->size() + 1);
+  WideBuilder wb{&bin, out, prim_order};
+  wb.build(0, root);
+  return root;
+}
+
+// ------------------------------------------------------------- parsing ---
+
+struct Statement {
+  size_t line;
+  bool bracket;
+  std::string left, right;
+};
+
+bool valid_char(char c) {
+  return std::isalpha((unsigned char)c) || std::isdigit((unsigned char)c) || c == '=' || c == '<' || c == '>' ||
+         c == ',' || c == '.' || c == '"' || c == '(' || c == ')' || c == '#' || c == '_' || c == ';' || c == '[' ||
+         c == ']' || c == '+' || c == '-' || c == '\\' || c == '/' || c == ':';
+}
+
+bool parse_vec(const std::string& s, vec3* v) {
+  if (s.size() < 2 || s.front() != '<' || s.back() != '>') return false;
+  int n = 0;
+  size_t start = 1;
+  for (size_t end = 1; end < s.size(); ++end) {
+    if (s[end] != ',' && s[end] != '>') continue;
+    if (n >= 3) return false;
+    (*v)[n++] = std::stof(s.substr(start, end - start));
+    start = end + 1;
+  }
+  return n == 3;
+}
+template <typename T, typename F>
+bool parse_array(const std::string& s, std::vector<T>* out, F conv) {
+  if (s.size() < 2 || s.front() != '[' || s.back() != ']') return false;
+  size_t start = 1;
+  for (size_t end = 1; end < s.size(); ++end) {
+    if (s[end] != ',' && s[end] != ']') continue;
+    if (end > start) out->push_back(conv(s.substr(start, end - start)));
+    start = end + 1;
+  }
+  return true;
+}
+std::string unquote(const std::string& s) {
+  if (s.size() >= 2 && s.front() == '"' && s.back() == '"') return s.substr(1, s.size() - 2);
+  return s;
+}
+
+}  // namespace
+
+int load_ymtmp(const std::string& path, HostScene* scene, std::string* error) {
+  auto fail = [&](int code, const std::string& msg) {
+    if (error) *error = msg;
+    return code;
+  };
+  if (path.size() < 6 || path.substr(path.size() - 6) != ".ymtmp")
+    return fail(YMRT_ERR_FORMAT, "scene file must have the .ymtmp extension: " + path);
+  std::ifstream f(path, std::ios::binary);
+  if (!f) return fail(YMRT_ERR_IO, "cannot open " + path);
+  std::stringstream ss;
+  ss << f.rdbuf();
+  const std::string text = ss.str();
+
+  // Strip comments (to end of line) and characters the format ignores, then
+  // split into ';'-terminated statements.
+  std::vector<Statement> stmts;
+  {
+    std::string cur;
+    size_t line = 1, stmt_line = 1;
+    bool in_comment = false;
+    for (char c : text) {
+      if (c == '\n') {
+        ++line;
+        in_comment = false;
+        continue;
+      }
+      if (in_comment) continue;
+      if (c == '#') {
+        in_comment = true;
+        continue;
+      }
+      if (!valid_char(c)) continue;
+      if (cur.empty()) stmt_line = line;
+      if (c == ';') {
+        if (!cur.empty()) {
+          Statement st;
+          st.line = stmt_line;
+          const size_t eq = cur.find('=');
+          if (eq == std::string::npos) {
+            st.bracket = true;
+            st.left = cur;
+          } else {
+            st.bracket = false;
+            st.left = cur.substr(0, eq);
+            st.right = cur.substr(eq + 1);
+          }
+          stmts.push_back(std::move(st));
+        }
+        cur.clear();
+        continue;
+      }
+      cur.push_back(c);
+    }
+  }
+
+  std::unordered_map<std::string, uint32_t> names;
+  auto bad = [&](const Statement& st, const std::string& msg) {
+    return fail(YMRT_ERR_FORMAT, path + ":" + std::to_string(st.line) + ": " + msg);
+  };
+  auto lookup = [&](const std::string& v, uint32_t* idx) -> bool {
+    auto it = names.find(unquote(v));
+    if (it == names.end()) return false;
+    *idx = it->second;
+    return true;
+  };
+
+  size_t i = 0;
+  while (i < stmts.size()) {
+    const Statement& open = stmts[i];
+    if (!open.bracket || open.left.rfind("Begin(", 0) != 0 || open.left.back() != ')')
+      return bad(open, "expected Begin(Type)");
+    const std::string type = open.left.substr(6, open.left.size() - 7);
+    size_t j = i + 1;
+    while (j < stmts.size() && !(stmts[j].bracket && stmts[j].left == "End(" + type + ")")) {
+      if (stmts[j].bracket) return bad(stmts[j], "unexpected " + stmts[j].left + " inside " + type);
+      ++j;
+    }
+    if (j >= stmts.size()) return bad(open, "missing End(" + type + ")");
+    std::string name;
+    std::unordered_map<std::string, std::string> attrs;
+    for (size_t k = i + 1; k < j; ++k) {
+      if (stmts[k].left == "name") name = unquote(stmts[k].right);
+      else attrs[stmts[k].left] = stmts[k].right;
+    }
+    auto get_f = [&](const char* key, float def) { return attrs.count(key) ? std::stof(attrs[key]) : def; };
+    auto get_v = [&](const char* key, vec3 def) {
+      vec3 v = def;
+      if (attrs.count(key)) parse_vec(attrs[key], &v);
+      return v;
+    };
+    auto get_ref = [&](const char* key, uint32_t* idx) -> int {
+      *idx = kEmpty;
+      if (!attrs.count(key)) return 0;
+      if (!lookup(attrs[key], idx)) return bad(open, std::string("unknown name for ") + key + ": " + attrs[key]);
+      return 0;
+    };
+    if (type != "Camera") {
+      if (name.empty()) return bad(open, type + " requires a name");
+      if (names.count(name)) return bad(open, "name already declared: " + name);
+    }
+    int rc = 0;
+    if (type == "Camera") {
+      scene->cam_from = get_v("from", vec3(0.0f, 0.0f, 10.0f));
+      scene->cam_look = get_v("look", vec3(0.0f, 0.0f, 4.0f));
+      scene->cam_fov_deg = gmax(get_f("fov", 45.0f), 0.01f);
+    } else if (type == "Transform") {
+      const vec3 t = get_v("translate", vec3(0.0f));
+      const vec3 s = vmax(vec3(0.0001f), get_v("scale", vec3(1.0f)));
+      const vec3 r = vclamp(get_v("rotate", vec3(0.0f)), vec3(0.0f), vec3(360.0f));
+      uint32_t parent = kEmpty;
+      if ((rc = get_ref("parent_transform_index", &parent))) return rc;
+      mat4 m = compose_transform(t, s, r);
+      if (parent != kEmpty) m = mat4_mul(scene->transforms[parent], m);
+      names[name] = (uint32_t)scene->transforms.size();
+      scene->transforms.push_back(m);
+      scene->i_transforms.push_back(mat4_inverse(m));
+    } else if (type == "Mesh") {
+      HostMesh mesh;
+      mesh.name = name;
+      auto to_u = [](const std::string& s) { return (uint32_t)std::stoi(s); };
+      auto to_f = [](const std::string& s) { return std::stof(s); };
+      std::vector<uint32_t> tris;
+      if (attrs.count("mesh_triangles")) parse_array(attrs["mesh_triangles"], &tris, to_u);
+      if (attrs.count("mesh_position_indices")) parse_array(attrs["mesh_position_indices"], &mesh.pos_idx, to_u);
+      if (attrs.count("mesh_positions")) parse_array(attrs["mesh_positions"], &mesh.pos, to_f);
+      if (attrs.count("mesh_normal_indices")) parse_array(attrs["mesh_normal_indices"], &mesh.nrm_idx, to_u);
+      if (attrs.count("mesh_normals")) parse_array(attrs["mesh_normals"], &mesh.nrm, to_f);
+      if (attrs.count("mesh_texcoord_indices")) parse_array(attrs["mesh_texcoord_indices"], &mesh.uv_idx, to_u);
+      if (attrs.count("mesh_texcoords")) parse_array(attrs["mesh_texcoords"], &mesh.uv, to_f);
+      const size_t nt = tris.size() / 3;
+      tris.resize(nt * 3);
+      if (nt == 0) return bad(open, "mesh has no triangles");
+      if (mesh.pos_idx.size() != nt * 3) return bad(open, "mesh's position indices number is wrong");
+      if (mesh.nrm_idx.size() != nt * 3) return bad(open, "mesh's normal indices number is wrong");
+      if (!mesh.uv_idx.empty() && mesh.uv_idx.size() != nt * 3) return bad(open, "mesh's texcoord indices number is wrong");
+      if (mesh.nrm.empty() || mesh.pos.empty()) return bad(open, "mesh requires position and normal arrays");
+      if (mesh.uv_idx.empty() || mesh.uv.empty()) {
+        mesh.uv_idx.clear();
+        mesh.uv.clear();
+      }
+      const size_t np = mesh.pos.size() / 3, nn = mesh.nrm.size() / 3, nu = mesh.uv.size() / 2;
+      for (size_t k = 0; k < nt * 3; ++k) {
+        if (tris[k] >= nt * 3) return bad(open, "triangle corner index out of range");
+        if (mesh.pos_idx[k] >= np || mesh.nrm_idx[k] >= nn) return bad(open, "vertex index out of range");
+        if (!mesh.uv_idx.empty() && mesh.uv_idx[k] >= nu) return bad(open, "texcoord index out of range");
+      }
+      mesh.tris = std::move(tris);
+      names[name] = (uint32_t)scene->meshes.size();
+      scene->meshes.push_back(std::move(mesh));
+    } else if (type == "Cube" || type == "Sphere") {
+      return fail(YMRT_ERR_UNSUPPORTED, type + " geometry blocks are not supported; write the shape as a Mesh block");
+    } else if (type == "PrimitiveInstance") {
+      Instance inst{};
+      uint32_t g, t, m, v;
+      if ((rc = get_ref("geometry_index", &g)) || (rc = get_ref("transform_index", &t)) ||
+          (rc = get_ref("material_index", &m)) || (rc = get_ref("inner_volume_index", &v)))
+        return rc;
+      if (g == kEmpty) return bad(open, "primitive instance requires a geometry");
+      if (t == kEmpty) return bad(open, "primitive instance requires a transform");
+      if (m == kEmpty) return bad(open, "primitive instance requires a material");
+      inst.geometry_idx = g;
+      inst.transform_idx = t;
+      inst.transform_count = 1;
+      inst.material_idx = m;
+      inst.inner_volume_idx = (int)v;
+      inst.treat_as_boundary = attrs.count("treat_as_boundary") && attrs["treat_as_boundary"] == "true";
+      inst.unique_index = (uint32_t)scene->instances.size();
+      names[name] = inst.unique_index;
+      scene->instances.push_back(inst);
+    } else if (type == "DefaultMaterial") {
+      Material mat;
+      std::memset(&mat, 0, sizeof(mat));
+      mat.material_type = kDefaultMtl;
+      DefaultMtl& d = mat.default_mtl;
+      d.diffuse_albedo = vmax(get_v("diffuse_albedo", vec3(0.5f)), vec3(0.0f));
+      d.specular_albedo = vmax(get_v("specular_albedo", vec3(1.0f)), vec3(0.0f));
+      d.alpha_x = gclamp(get_f("roughness_x", 0.2f), 0.0f, 1.0f);
+      d.alpha_y = gclamp(get_f("roughness_y", 0.2f), 0.0f, 1.0f);
+      d.ior_n = gmax(0.0001f, get_f("ior_n", 1.3f));
+      d.metalness = gclamp(get_f("metalness", 0.0f), 0.0f, 1.0f);
+      d.specular_weight = gclamp(get_f("specular_weight", 1.0f), 0.0f, 1.0f);
+      d.transmission_weight = gclamp(get_f("transmission_weight", 0.0f), 0.0f, 1.0f);
+      d.ior_priority = attrs.count("ior_priority") ? (uint32_t)gmax(0, std::stoi(attrs["ior_priority"])) : 0u;
+      d.coat_albedo = vmax(get_v("coat_albedo", vec3(1.0f)), vec3(0.0f));
+      d.coat_weight = gclamp(get_f("coat_weight", 0.0f), 0.0f, 1.0f);
+      d.coat_thickness = gmax(get_f("coat_thickness", 1.0f), 0.0f);
+      d.coat_ior = gmax(get_f("coat_ior", 1.6f), 0.0001f);
+      d.coat_roughness_x = gclamp(get_f("coat_roughness_x", 0.2f), 0.0f, 1.0f);
+      d.coat_roughness_y = gclamp(get_f("coat_roughness_y", 0.2f), 0.0f, 1.0f);
+      const char* tex_keys[] = {"diffuse_albedo_tex", "alpha_x_tex", "specular_albedo_tex", "alpha_y_tex",
+                                "specular_weight_tex", "metalness_tex", "transmission_weight_tex",
+                                "normal_mapping_tex", "bump_mapping_tex", "coat_albedo_tex", "coat_weight_tex",
+                                "coat_thickness_tex", "coat_roughness_x_tex", "coat_roughness_y_tex",
+                                "coat_normal_tex"};
+      uint32_t* tex_fields[] = {&d.diffuse_albedo_tex, &d.alpha_x_tex, &d.specular_albedo_tex, &d.alpha_y_tex,
+                                &d.specular_weight_tex, &d.metalness_tex, &d.transmission_weight_tex,
+                                &d.normal_mapping_tex, &d.bump_mapping_tex, &d.coat_albedo_tex, &d.coat_weight_tex,
+                                &d.coat_thickness_tex, &d.coat_roughness_x_tex, &d.coat_roughness_y_tex,
+                                &d.coat_normal_tex};
+      for (int k = 0; k < 15; ++k)
+        if ((rc = get_ref(tex_keys[k], tex_fields[k]))) return rc;
+      d.coat_normal_tex_type = attrs.count("coat_normal_tex_type") ? (uint32_t)std::stoi(attrs["coat_normal_tex_type"]) : 1u;
+      names[name] = (uint32_t)scene->materials.size();
+      scene->materials.push_back(mat);
+    } else if (type == "LightMaterial") {
+      Material mat;
+      std::memset(&mat, 0, sizeof(mat));
+      mat.material_type = kLightMtl;
+      mat.light_mtl.light_color = vmax(get_v("light_color", vec3(1.0f)), vec3(0.0f));
+      mat.light_mtl.intensity = gmax(get_f("intensity", 1.0f), 0.0f);
+      names[name] = (uint32_t)scene->materials.size();
+      scene->materials.push_back(mat);
+    } else if (type == "ConstantTextureFloat" || type == "ConstantTextureRgb" || type == "NoiseTextureFBM") {
+      Texture tex;
+      std::memset(&tex, 0, sizeof(tex));
+      tex.child[0] = tex.child[1] = kEmpty;
+      if (type == "ConstantTextureFloat") {
+        tex.type = kTexConstFloat;
+        tex.value = get_f("value", 0.0f);
+      } else if (type == "ConstantTextureRgb") {
+        tex.type = kTexConstRgb;
+        tex.color = get_v("color", vec3(0.0f));
+      } else {
+        tex.type = kTexFbm;
+        if ((rc = get_ref("texture_black_idx", &tex.child[0])) || (rc = get_ref("texture_white_idx", &tex.child[1])))
+          return rc;
+        if (tex.child[0] == kEmpty || tex.child[1] == kEmpty) return bad(open, "fbm texture requires black and white inputs");
+        tex.frequency = gmax(0.001f, get_f("frequency", 16.0f));
+        tex.lacunarity = get_f("lacunarity", 2.0f);
+        tex.gain = get_f("gain", 0.5f);
+        tex.layer_count = attrs.count("layer_count") ? std::stoi(attrs["layer_count"]) : 4;
+        tex.amplitude = get_f("amplitude", 1.0f);
+        tex.offset = get_f("offset", 0.0f);
+      }
+      names[name] = (uint32_t)scene->textures.size();
+      scene->textures.push_back(tex);
+    } else if (type == "ImageTexture" || type == "CheckerBoardTexture" || type == "NoiseTexture" ||
+               type == "NoiseTextureTurbulence" || type == "NoiseTextureMarble" || type == "NoiseTextureWood" ||
+               type == "NoiseTexturePolkaDot" || type == "NoiseTextureWave") {
+      return fail(YMRT_ERR_UNSUPPORTED, type + " textures are not supported (constant and fBm textures are)");
+    } else if (type == "DistantLight") {
+      DistantLightRec dl{};
+      dl.light_color = vmax(get_v("light_color", vec3(1.0f)), vec3(0.0f));
+      if ((rc = get_ref("transform_index", &dl.transform_idx))) return rc;
+      if (dl.transform_idx == kEmpty) return bad(open, "distant light requires a transform");
+      dl.intensity = gmax(get_f("intensity", 1.0f), 0.0f);
+      dl.theta_max = get_f("theta_max", 5.0f);
+      dl.cos_theta_max = std::cos(dl.theta_max * static_cast<float>(0.01745329251994329576923690768489));
+      names[name] = (uint32_t)scene->distant_lights.size();
+      scene->distant_lights.push_back(dl);
+    } else if (type == "Volume") {
+      Volume vol{};
+      uint32_t t, tex;
+      if ((rc = get_ref("transform_index", &t)) || (rc = get_ref("density_texture_index", &tex))) return rc;
+      if (t == kEmpty) return bad(open, "volume requires a transform");
+      vol.transform_idx = t;
+      vol.sigma_t = vmax(vec3(0.0f), get_v("sigma_t", vec3(0.05f)));
+      vol.albedo = vmax(vec3(0.0f), get_v("albedo", vec3(1.0f)));
+      vol.g = gclamp(get_f("g", 0.0f), 0.0f, 1.0f);
+      vol.density_texture_idx = (int)tex;
+      names[name] = (uint32_t)scene->volumes.size();
+      scene->volumes.push_back(vol);
+    } else {
+      return bad(open, "unknown block type " + type);
+    }
+    i = j + 1;
+  }
+  for (const Instance& inst : scene->instances) {
+    if (inst.geometry_idx >= scene->meshes.size() || inst.transform_idx >= scene->transforms.size() ||
+        inst.material_idx >= scene->materials.size())
+      return fail(YMRT_ERR_FORMAT, "instance refers to an asset of the wrong type");
+    if (inst.inner_volume_idx != -1 && (uint32_t)inst.inner_volume_idx >= scene->volumes.size())
+      return fail(YMRT_ERR_FORMAT, "instance refers to an unknown volume");
+  }
+  return YMRT_OK;
+}
+
+// ---------------------------------------------------------- preparation ---
+
+namespace {
+
+// Watertight ray/triangle test, the reference's IntersectTri
+// (src/ShadingUtilities.cuh:54-134), host copy for camera set-up.
+bool host_intersect_tri(vec3 p0, vec3 p1, vec3 p2, vec3 o, vec3 d, float tmax, float* t_out) {
+  p0 = p0 - o;
+  p1 = p1 - o;
+  p2 = p2 - o;
+  const int kz = max_dimension(vabs(d));
+  int kx = kz + 1; if (kx == 3) kx = 0;
+  int ky = kx + 1; if (ky == 3) ky = 0;
+  const vec3 dd(d[kx], d[ky], d[kz]);
+  p0 = vec3(p0[kx], p0[ky], p0[kz]);
+  p1 = vec3(p1[kx], p1[ky], p1[kz]);
+  p2 = vec3(p2[kx], p2[ky], p2[kz]);
+  const float sx = -dd.x / dd.z, sy = -dd.y / dd.z, sz = 1.f / dd.z;
+  p0.x += sx * p0.z; p0.y += sy * p0.z;
+  p1.x += sx * p1.z; p1.y += sy * p1.z;
+  p2.x += sx * p2.z; p2.y += sy * p2.z;
+  const float e0 = p1.x * p2.y - p1.y * p2.x;
+  const float e1 = p2.x * p0.y - p2.y * p0.x;
+  const float e2 = p0.x * p1.y - p0.y * p1.x;
+  if ((e0 < 0 || e1 < 0 || e2 < 0) && (e0 > 0 || e1 > 0 || e2 > 0)) return false;
+  const float den = e0 + e1 + e2;
+  if (den == 0) return false;
+  p0.z *= sz; p1.z *= sz; p2.z *= sz;
+  const float inv = 1.0f / den;
+  float t = e0 * p0.z + e1 * p1.z + e2 * p2.z;
+  t *= inv;
+  if (t < kTMin || t > tmax) return false;
+  *t_out = t;
+  return true;
+}
+
+// Camera::InitCameraRayTransfer (src/Camera.cpp:15-78): instances the
+// camera sits inside (a ray from the camera hits them both forwards and
+// backwards) are pushed on the camera's ray-transfer stack.
+void init_camera_transfer(HostScene* s) {
+  RayTransfer& rt = s->camera.transfer;
+  rt.max_priority_record_index = -1;
+  rt.record_count = 0;
+  const CameraDesc& cam = s->camera;
+  const float height = 2.0f * cam.tan_half_fov;
+  const float width = height * cam.aspect_ratio;
+  vec3 dir = -cam.w + (0.5f - 0.5f) * width * cam.u + (0.5f - 0.5f) * height * cam.v;
+  dir = normalize(dir);
+  auto hits_geometry = [&](uint32_t inst_idx, vec3 o_world, vec3 d_world) {
+    const Instance& inst = s->instances[inst_idx];
+    const mat4& wto = s->i_transforms[inst.transform_idx];
+    const vec3 o = xform_point_glm(wto, o_world), d = xform_dir_glm(wto, d_world);
+    const HostMesh& m = s->meshes[inst.geometry_idx];
+    for (size_t t = 0; t < m.tris.size() / 3; ++t) {
+      vec3 p[3];
+      for (int k = 0; k < 3; ++k) {
+        const uint32_t vi = m.pos_idx[m.tris[3 * t + k]];
+        p[k] = vec3(m.pos[3 * vi], m.pos[3 * vi + 1], m.pos[3 * vi + 2]);
+      }
+      float th;
+      if (host_intersect_tri(p[0], p[1], p[2], o, d, kTMax, &th)) return true;
+    }
+    return false;
+  };
+  std::vector<uint32_t> inside;
+  for (uint32_t i = 0; i < s->instances.size(); ++i)
+    if (hits_geometry(i, cam.position, dir) && hits_geometry(i, cam.position, -dir)) inside.push_back(i);
+  for (uint32_t i : inside) {
+    if (rt.record_count == kMaxBoundaryRecord) break;
+    const Instance& inst = s->instances[i];
+    const Material& mat = s->materials[inst.material_idx];
+    const float ior = mat.material_type == kDefaultMtl ? mat.default_mtl.ior_n : 1.0f;
+    const uint32_t prio = mat.material_type == kDefaultMtl ? mat.default_mtl.ior_priority : 0u;
+    BoundaryRecord& r = rt.records[rt.record_count++];
+    r.prim_idx = i;
+    r.ior = ior;
+    r.ior_priority = prio;
+    r.vol_idx = inst.inner_volume_idx;
+    if (rt.record_count == 1 || prio >= rt.records[rt.max_priority_record_index].ior_priority)
+      rt.max_priority_record_index = rt.record_count - 1;
+  }
+}
+
+}  // namespace
+
+int prepare_scene(HostScene* s, int width, int height, std::string* error) {
+  if (width <= 0 || height <= 0) {
+    if (error) *error = "image size must be positive";
+    return YMRT_ERR_INVALID;
+  }
+  s->width = width;
+  s->height = height;
+
+  // Bottom level: per mesh, the reference's build order, then a wide BVH.
+  s->geo_desc.clear();
+  s->blas_nodes.clear();
+  s->wtris.clear();
+  s->tri_corners.clear();
+  s->all_pos_idx.clear(); s->all_nrm_idx.clear(); s->all_uv_idx.clear();
+  s->all_pos.clear(); s->all_nrm.clear(); s->all_uv.clear();
+  for (HostMesh& m : s->meshes) {
+    const uint32_t nt = (uint32_t)(m.tris.size() / 3);
+    auto P = [&](uint32_t corner) {
+      const uint32_t vi = m.pos_idx[corner];
+      return vec3(m.pos[3 * vi], m.pos[3 * vi + 1], m.pos[3 * vi + 2]);
+    };
+    std::vector<BuildItem> items(nt);
+    for (uint32_t t = 0; t < nt; ++t) {
+      const vec3 p0 = P(m.tris[3 * t]), p1 = P(m.tris[3 * t + 1]), p2 = P(m.tris[3 * t + 2]);
+      BBox b;
+      b = box_extend(b, p0);
+      b = box_extend(b, p1);
+      b = box_extend(b, p2);
+      items[t].box = bound_fix(b);
+      items[t].center = (p0 + p1 + p2) / 3.f;
+      items[t].idx = t;
+    }
+    std::vector<BinNode> bin = build_binary(items);
+    std::vector<uint32_t> reordered(nt * 3);
+    for (uint32_t t = 0; t < nt; ++t)
+      for (int k = 0; k < 3; ++k) reordered[3 * t + k] = m.tris[3 * items[t].idx + k];
+    m.tris.swap(reordered);
+    m.root_box = bin[0].box;
+
+    GeometryDesc gd{};
+    gd.tri_offset = (uint32_t)(s->tri_corners.size() / 3);
+    gd.tri_count = nt;
+    gd.corner_offset = (uint32_t)s->all_pos_idx.size();
+    gd.pos_offset = (uint32_t)(s->all_pos.size() / 3);
+    gd.nrm_offset = (uint32_t)(s->all_nrm.size() / 3);
+    gd.uv_offset = m.uv.empty() ? -1 : (int32_t)(s->all_uv.size() / 2);
+    gd.bbox_min = m.root_box.pmin;
+    gd.bbox_max = m.root_box.pmax;
+    s->tri_corners.insert(s->tri_corners.end(), m.tris.begin(), m.tris.end());
+    s->all_pos_idx.insert(s->all_pos_idx.end(), m.pos_idx.begin(), m.pos_idx.end());
+    s->all_nrm_idx.insert(s->all_nrm_idx.end(), m.nrm_idx.begin(), m.nrm_idx.end());
+    if (!m.uv.empty()) s->all_uv_idx.insert(s->all_uv_idx.end(), m.uv_idx.begin(), m.uv_idx.end());
+    else s->all_uv_idx.resize(s->all_pos_idx.size(), 0);
+    s->all_pos.insert(s->all_pos.end(), m.pos.begin(), m.pos.end());
+    s->all_nrm.insert(s->all_nrm.end(), m.nrm.begin(), m.nrm.end());
+    s->all_uv.insert(s->all_uv.end(), m.uv.begin(), m.uv.end());
+
+    std::vector<uint32_t> order;
+    gd.node_offset = build_wide(bin, &s->blas_nodes, &order);
+    // the wide builder numbered nodes relative to the whole array already;
+    // prim_base values are relative to this mesh's triangle block.
+    gd.wtri_offset = (uint32_t)(s->wtris.size() / 3);
+    for (uint32_t pos : order) {
+      // `pos` is a position in the reordered triangle array == triangle id
+      const vec3 p0 = P(m.tris[3 * pos]), p1 = P(m.tris[3 * pos + 1]), p2 = P(m.tris[3 * pos + 2]);
+      s->wtris.push_back(float4{p0.x, p0.y, p0.z, u2f(pos)});
+      s->wtris.push_back(float4{p1.x, p1.y, p1.z, 0.0f});
+      s->wtris.push_back(float4{p2.x, p2.y, p2.z, 0.0f});
+    }
+    s->geo_desc.push_back(gd);
+  }
+
+  // Top level: the reference's instance order, then a wide BVH.
+  const uint32_t ni = (uint32_t)s->instances.size();
+  if (ni == 0) {
+    if (error) *error = "scene has no instances";
+    return YMRT_ERR_INVALID;
+  }
+  std::vector<BuildItem> items(ni);
+  for (uint32_t i = 0; i < ni; ++i) {
+    const Instance& inst = s->instances[i];
+    items[i].box = box_transform(s->meshes[inst.geometry_idx].root_box, s->transforms[inst.transform_idx]);
+    items[i].center = box_center(items[i].box);
+    items[i].idx = i;
+  }
+  std::vector<BinNode> tbin = build_binary(items);
+  std::vector<Instance> reordered(ni);
+  s->instance_file_index.assign(ni, 0);
+  for (uint32_t i = 0; i < ni; ++i) {
+    reordered[i] = s->instances[items[i].idx];
+    s->instance_file_index[i] = items[i].idx;
+  }
+  s->instances.swap(reordered);
+  s->tlas_nodes.clear();
+  s->tlas_prims.clear();
+  build_wide(tbin, &s->tlas_nodes, &s->tlas_prims);
+  s->triangle_count_instanced = 0;
+  for (const Instance& inst : s->instances) s->triangle_count_instanced += s->meshes[inst.geometry_idx].tris.size() / 3;
+
+  // Shape lights: SceneModule::LoadShapeLight (src/core/SceneModule.cpp:1203-1304).
+  s->shape_lights.clear();
+  s->shape_light_table.clear();
+  for (uint32_t pi = 0; pi < ni; ++pi) {
+    const Instance& inst = s->instances[pi];
+    const Material& mat = s->materials[inst.material_idx];
+    if (mat.material_type != kLightMtl) continue;
+    const mat4& otw = s->transforms[inst.transform_idx];
+    const vec3 c = mat.light_mtl.light_color;
+    const float irradiance = (c.x + c.y + c.z) * mat.light_mtl.intensity * kPi;
+    const HostMesh& m = s->meshes[inst.geometry_idx];
+    for (uint32_t t = 0; t < m.tris.size() / 3; ++t) {
+      vec3 p[3];
+      for (int k = 0; k < 3; ++k) {
+        const uint32_t vi = m.pos_idx[m.tris[3 * t + k]];
+        p[k] = transform_position(otw, vec3(m.pos[3 * vi], m.pos[3 * vi + 1], m.pos[3 * vi + 2]));
+      }
+      const float area = length(cross(p[1] - p[0], p[2] - p[0]));
+      s->shape_lights.push_back(ShapeLight{pi, t, irradiance * area, 0.5f * area});
+    }
+  }
+  {
+    float total = 0.0f;
+    s->shape_light_table.resize(s->shape_lights.size());
+    for (size_t i = 0; i < s->shape_lights.size(); ++i) {
+      total += s->shape_lights[i].power;
+      s->shape_light_table[i] = total;
+    }
+    const float rcp = safe_rcp(total);
+    for (float& v : s->shape_light_table) v = total == 0.0f ? 0.0f : (v * rcp);
+  }
+
+  // Camera: SceneParser -> Camera::SetFov/SetPosition/SetDir (src/Camera.h:32,
+  // 235-238, 301-311), then the rendering camera's aspect ratio.
+  {
+    CameraDesc& cam = s->camera;
+    const float fov = s->cam_fov_deg * static_cast<float>(0.01745329251994329576923690768489);
+    cam.tan_half_fov = std::tan(0.5f * fov);
+    cam.position = s->cam_from;
+    vec3 w = s->cam_from - s->cam_look;
+    w = w * safe_rcp(length(w));
+    const vec3 up(0.0f, 1.0f, 0.0f);
+    double mu[3], mv[3];
+    mu[0] = (double)up.y * (double)w.z - (double)up.z * (double)w.y;
+    mu[1] = -((double)up.x * (double)w.z - (double)up.z * (double)w.x);
+    mu[2] = (double)up.x * (double)w.y - (double)up.y * (double)w.x;
+    const vec3 u = vec3((float)mu[0], (float)mu[1], (float)mu[2]) *
+                   safe_rcp((float)std::sqrt(mu[0] * mu[0] + mu[1] * mu[1] + mu[2] * mu[2]));
+    mv[0] = (double)w.y * (double)u.z - (double)w.z * (double)u.y;
+    mv[1] = -((double)w.x * (double)u.z - (double)w.z * (double)u.x);
+    mv[2] = (double)w.x * (double)u.y - (double)w.y * (double)u.x;
+    const vec3 v = vec3((float)mv[0], (float)mv[1], (float)mv[2]) *
+                   safe_rcp((float)std::sqrt(mv[0] * mv[0] + mv[1] * mv[1] + mv[2] * mv[2]));
+    cam.w = w;
+    cam.u = u;
+    cam.v = v;
+    cam.aspect_ratio = float(width) / float(height);
+    init_camera_transfer(s);
+  }
+  return YMRT_OK;
+}
+
+}  // namespace ym

@@ -1,0 +1,82 @@
+// Host-side scene preparation for ymrt_b200.
+//
+// Reads YMRT's .ymtmp text format, builds the transforms, orders triangles and
+// instances exactly as the reference's BVH builders do (so every triangle,
+// instance and shape-light index a kernel reports is the index the reference
+// reports), collapses those binary trees into compressed 8-wide BVHs, and
+// flattens everything into the arrays the kernels read.
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include <vector_types.h>
+
+#include "ymrt_scene.h"
+
+namespace ym {
+
+struct BBox {
+  vec3 pmax{kFloatMin, kFloatMin, kFloatMin};
+  vec3 pmin{kFloatMax, kFloatMax, kFloatMax};
+};
+
+struct HostMesh {
+  std::string name;
+  std::vector<uint32_t> tris;      // corner triples (id0, id1, id2), reference post-build order
+  std::vector<uint32_t> pos_idx, nrm_idx, uv_idx;
+  std::vector<float> pos, nrm, uv;
+  BBox root_box;                   // root box of the reference's mesh BVH
+};
+
+struct DistantLightRec {
+  vec3 light_color;
+  uint32_t transform_idx;
+  float intensity;
+  float cos_theta_max;
+  float theta_max;
+  float padding;
+};
+
+struct HostScene {
+  // camera as written in the file
+  vec3 cam_from{0.0f, 0.0f, 10.0f}, cam_look{0.0f, 0.0f, 4.0f};
+  float cam_fov_deg = 45.0f;
+
+  std::vector<mat4> transforms, i_transforms;
+  std::vector<HostMesh> meshes;
+  std::vector<Instance> instances;          // after prepare(): reference order
+  std::vector<uint32_t> instance_file_index;  // after prepare(): file index of each instance
+  std::vector<Material> materials;
+  std::vector<Texture> textures;
+  std::vector<Volume> volumes;
+  std::vector<DistantLightRec> distant_lights;
+  std::vector<ShapeLight> shape_lights;
+  std::vector<float> shape_light_table;
+  CameraDesc camera{};
+  int width = 0, height = 0;
+
+  // flattened device-side arrays (filled by prepare())
+  std::vector<GeometryDesc> geo_desc;
+  std::vector<WideNode> blas_nodes, tlas_nodes;
+  std::vector<float4> wtris;
+  std::vector<uint32_t> tlas_prims;
+  std::vector<uint32_t> tri_corners, all_pos_idx, all_nrm_idx, all_uv_idx;
+  std::vector<float> all_pos, all_nrm, all_uv;
+  size_t triangle_count_instanced = 0;
+};
+
+// Parses a .ymtmp file. Returns 0 or a negative YMRT_ERR_* code with a message.
+int load_ymtmp(const std::string& path, HostScene* scene, std::string* error);
+
+// Builds BVHs, orders instances/triangles/lights like the reference, sets up
+// the rendering camera for a width x height image and flattens the arrays.
+int prepare_scene(HostScene* scene, int width, int height, std::string* error);
+
+// glm-order transform helpers (exposed for tests through the C-ABI).
+mat4 compose_transform(vec3 translate, vec3 scale, vec3 rotate_deg);
+mat4 mat4_mul(const mat4& a, const mat4& b);
+mat4 mat4_inverse(const mat4& m);
+
+}  // namespace ym

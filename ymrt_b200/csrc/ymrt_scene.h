@@ -1,0 +1,229 @@
+// Scene data shared by the host-side scene preparation and the sm_100a kernels.
+//
+// Records that cross the drop-in boundary keep the YMRT reference's byte
+// layout (Material src/Material.h:9-359, Volume src/Volume.h:9-18,
+// ShapeLight src/Light.h:80-86, PrimitiveInstance src/PrimtiveInstance.h:9-22,
+// RenderSetting src/SceneDefines.h:17-40) so a caller holding the reference's
+// arrays can pass them through unchanged. Everything the kernels traverse is
+// this project's own layout: a compressed 8-wide BVH per mesh and one over the
+// instances, triangles stored as three float4 vertices, geometry tables
+// flattened into a few global arrays.
+#pragma once
+
+#include <cstdint>
+#include <cstddef>
+
+#include <vector_types.h>
+
+#include "ymrt_math.h"
+
+namespace ym {
+
+constexpr int kMaxBoundaryRecord = 6;         // MAX_BOUNDARY_RECORD, src/Ray.h:12
+constexpr int kMaxNearby = kMaxBoundaryRecord + 2;
+constexpr int kMaxRayDepth = 64;              // MAX_RAY_DEPTH, src/SceneDefines.h:9
+constexpr int kTileRes = 16;                  // TILE_X_RES / TILE_Y_RES
+constexpr int kTilePixels = 256;
+constexpr int kHaltonDims = 1000;             // PRIME_TABLE_SIZE, src/RandomSampler.cuh:12
+constexpr int kMaxFreePath = 2048;            // MAX_FREE_PATH_LENGTH, src/VolumeEval.cuh:16
+
+enum MaterialType : uint32_t { kDefaultMtl = 0, kLightMtl = 1 };
+
+// DefaultMtl, src/Material.h:21-60 (152 bytes).
+struct DefaultMtl {
+  vec3 diffuse_albedo; uint32_t diffuse_albedo_tex;
+  vec3 specular_albedo; uint32_t specular_albedo_tex;
+  float alpha_x; uint32_t alpha_x_tex;
+  float alpha_y; uint32_t alpha_y_tex;
+  float specular_weight; uint32_t specular_weight_tex;
+  float metalness; uint32_t metalness_tex;
+  float transmission_weight; uint32_t transmission_weight_tex;
+  float ior_n; uint32_t ior_priority;
+  vec3 coat_albedo; uint32_t coat_albedo_tex;
+  float coat_weight; uint32_t coat_weight_tex;
+  float coat_thickness; uint32_t coat_thickness_tex;
+  float coat_roughness_x; uint32_t coat_roughness_x_tex;
+  float coat_roughness_y; uint32_t coat_roughness_y_tex;
+  float coat_ior; uint32_t normal_mapping_tex;
+  uint32_t bump_mapping_tex; uint32_t padding;
+  uint32_t coat_normal_tex; uint32_t coat_normal_tex_type;
+};
+struct LightMtl {
+  vec3 light_color;
+  float intensity;
+};
+// Material, src/Material.h:200-207 (156 bytes).
+struct Material {
+  uint32_t material_type;
+  union {
+    DefaultMtl default_mtl;
+    LightMtl light_mtl;
+  };
+};
+static_assert(sizeof(DefaultMtl) == 152, "DefaultMtl layout");
+static_assert(sizeof(Material) == 156, "Material layout");
+
+// Volume, src/Volume.h:9-18 (36 bytes).
+struct Volume {
+  vec3 sigma_t;
+  vec3 albedo;
+  int density_texture_idx;
+  uint32_t transform_idx;
+  float g;
+};
+static_assert(sizeof(Volume) == 36, "Volume layout");
+
+// ShapeLight, src/Light.h:80-86 (16 bytes): triangle `triangle_idx` (in the
+// reference's post-build order) of instance `instance_idx`.
+struct ShapeLight {
+  uint32_t instance_idx;
+  uint32_t triangle_idx;
+  float power;
+  float area;
+};
+
+// PrimitiveInstance, src/PrimtiveInstance.h:9-22 (32 bytes).
+struct Instance {
+  uint32_t geometry_idx;
+  uint32_t transform_idx;
+  uint32_t transform_count;
+  uint32_t material_idx;
+  int inner_volume_idx;
+  int treat_as_boundary;
+  uint32_t unique_index;
+  int padding;
+};
+static_assert(sizeof(Instance) == 32, "Instance layout");
+
+// RenderSetting, src/SceneDefines.h:17-40 (40 bytes, x86-64 and device).
+struct RenderSetting {
+  int ssp;
+  int ray_depth;
+  float gamma;
+  float exposure;
+  int max_frame_count;
+  int sampler_type;
+  int enable_shape_light;
+  bool enable_distant_light;
+  bool enable_volume_scattering;
+  bool enable_env_light;
+  bool enable_russian_roulette;
+  bool enable_indirect_clamp;
+  float indirect_limit;
+};
+static_assert(sizeof(RenderSetting) == 40, "RenderSetting layout");
+
+// Texture subset used on the hot path: constants and the fBm noise node
+// (src/Texture.h:168-690 holds the full union). Children are texture indices.
+enum TextureType : uint32_t {
+  kTexImage = 0, kTexConstFloat = 1, kTexConstRgb = 2, kTexChecker = 3, kTexNoise = 4, kTexFbm = 5,
+  kTexTurbulence = 6, kTexMarble = 7, kTexWood = 8, kTexPolkaDot = 9, kTexWave = 10,
+};
+struct Texture {
+  uint32_t type;
+  uint32_t child[2];   // black / white inputs (kEmpty when absent)
+  float value;         // constant float
+  vec3 color;          // constant rgb
+  float frequency, lacunarity, gain, amplitude, offset;
+  int layer_count;
+  int normalized;
+};
+
+// Ray-transfer stack of nested media, src/Ray.h:106-260 (RayTransfer).
+struct BoundaryRecord {
+  uint32_t prim_idx;
+  float ior;
+  uint32_t ior_priority;
+  int vol_idx;
+};
+struct RayTransfer {
+  int max_priority_record_index;
+  int record_count;
+  BoundaryRecord records[kMaxBoundaryRecord];
+};
+
+// Pinhole camera (the reference's Camera, src/Camera.h:14-332, reduced to the
+// fields ray generation reads) plus the media the camera sits in.
+struct CameraDesc {
+  vec3 position, u, v, w;
+  float aspect_ratio;
+  float tan_half_fov;
+  RayTransfer transfer;
+};
+
+// ---- acceleration structures (this project's layout) ----
+
+// One node of the compressed 8-wide BVH: 80 bytes, read as five 16-byte
+// loads. Child boxes are quantised to 8 bits per bound on a per-node grid
+// origin + q * 2^e (rounded outwards, so every decoded box contains the
+// exact one). imask bit i set: child i is an internal node at
+// child_base + meta[i]. Otherwise meta[i] = (count << 5) | offset: a leaf of
+// `count` primitives at prim_base + offset (count 0: empty slot).
+struct alignas(16) WideNode {
+  float ox, oy, oz;
+  uint8_t ex, ey, ez, imask;
+  uint32_t child_base;
+  uint32_t prim_base;
+  uint8_t meta[8];
+  uint8_t qlo_x[8], qlo_y[8], qlo_z[8];
+  uint8_t qhi_x[8], qhi_y[8], qhi_z[8];
+};
+static_assert(sizeof(WideNode) == 80, "WideNode is five 16-byte words");
+
+// Per-mesh tables (offsets into the flattened global arrays).
+struct GeometryDesc {
+  uint32_t tri_offset;      // into tri_corners (reference post-build triangle order)
+  uint32_t tri_count;
+  uint32_t corner_offset;   // into pos_idx / nrm_idx / uv_idx
+  uint32_t pos_offset;      // into positions
+  uint32_t nrm_offset;      // into normals
+  int32_t uv_offset;        // into texcoords, -1 when the mesh has none
+  uint32_t node_offset;     // root of the mesh's wide BVH in blas_nodes
+  uint32_t wtri_offset;     // into wtris (wide-BVH triangle order)
+  vec3 bbox_min, bbox_max;  // root box (object space)
+};
+
+// Everything the kernels read, as device pointers.
+struct DeviceScene {
+  // instances
+  uint32_t instance_count;
+  const Instance* instances;
+  const mat4* transforms;
+  const mat4* i_transforms;
+  uint32_t transform_count;
+  // top-level BVH over instances
+  const WideNode* tlas_nodes;
+  const uint32_t* tlas_prims;   // instance index per TLAS leaf slot
+  // meshes
+  uint32_t geometry_count;
+  const GeometryDesc* geometries;
+  const WideNode* blas_nodes;
+  const float4* wtris;          // 3 per triangle: v0, v1, v2 (w of v0 = triangle id bits)
+  const uint32_t* tri_corners;  // 3 per triangle (Triangle id0,id1,id2)
+  const uint32_t* pos_idx;
+  const uint32_t* nrm_idx;
+  const uint32_t* uv_idx;
+  const float* positions;       // xyz
+  const float* normals;         // xyz
+  const float* texcoords;       // uv
+  // materials, lights, media
+  uint32_t material_count;
+  const Material* materials;
+  uint32_t shape_light_count;
+  const ShapeLight* shape_lights;
+  const float* shape_light_table;
+  uint32_t volume_count;
+  const Volume* volumes;
+  uint32_t texture_count;
+  const Texture* textures;
+  // sampler
+  const uint32_t* halton_perm;
+  // camera
+  CameraDesc camera;
+  int width, height;
+  // Halton enumerator (src/HaltonEnumerator.h:13-38)
+  float halton_x_scale, halton_y_scale;
+  int halton_mx, halton_my, halton_exp2, halton_exp3, halton_increment;
+};
+
+}  // namespace ym

@@ -1,0 +1,405 @@
+"""Seeded synthetic scenes in YMRT's ``.ymtmp`` text format.
+
+The reference publishes no benchmark scenes (its only scene file ships with
+meshes that are missing from the checkout), so the workloads are generated
+from seeds with numpy ``PCG64``:
+
+* ``cornell``  -- Cornell-box-like: 5 wall quads, 2 boxes rotated by U[0,45]
+  degrees about y, 1 emissive quad (radiance 15); Lambertian albedos
+  U[0.1,0.9] per channel; every object one instance.
+* ``instanced`` -- ~1.2 M instanced triangles: 64 instances of an icosphere
+  (subdivision 5, 20,480 triangles), a 256x256 fBm heightfield (131,072
+  triangles), a 64-segment torus and a box, each with a random affine
+  transform; 32 materials (GGX conductors with roughness U[0.05,0.8],
+  dielectrics with IOR 1.5 and roughness U[0,0.3], diffuse); 2 quad lights.
+* ``volumetric`` -- the Cornell scene plus a homogeneous fog box
+  (sigma_t 0.05, albedo 0.8, g 0.6) and a heterogeneous medium whose density is
+  a procedural fBm texture (the reference's ``NoiseTextureFBM``).
+
+The file layout follows the reference's parser (src/core/YMParser.cpp:2330,
+block types :57-92, attribute sets :94-372). Every float is written as the
+shortest decimal that round-trips its float32 value, so the reference parser
+(``std::stof``) and this project's loader read identical bits.
+
+The Halton permutation table (src/core/SceneModule.cpp:1412
+``InitHaltonPermuteTable``) is seeded by ``std::random_device`` in the
+reference; here it is an explicit seeded input shared by both sides.
+"""
+from __future__ import annotations
+
+import math
+import os
+
+import numpy as np
+
+__all__ = [
+    "first_primes", "halton_permutations", "cornell_scene", "instanced_scene", "volumetric_scene",
+    "write_scene", "SCENES",
+]
+
+
+def first_primes(n: int = 1000) -> np.ndarray:
+    """The first ``n`` primes (the reference tabulates 1000, 2..7919)."""
+    limit = 8000
+    sieve = np.ones(limit, dtype=bool)
+    sieve[:2] = False
+    for i in range(2, int(limit ** 0.5) + 1):
+        if sieve[i]:
+            sieve[i * i::i] = False
+    p = np.nonzero(sieve)[0][:n]
+    assert len(p) == n
+    return p.astype(np.uint32)
+
+
+def halton_permutations(seed: int = 0x594D5254) -> np.ndarray:
+    """Concatenated random digit permutations for the first 1000 primes, in
+    prime order (permutation k occupies ``sum(primes[:k])`` onwards), as the
+    reference's table is laid out."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    parts = [rng.permutation(int(p)).astype(np.uint32) for p in first_primes()]
+    return np.concatenate(parts)
+
+
+# ---------------------------------------------------------------- meshes ---
+
+class Mesh:
+    """Triangle mesh with one position index and one normal index per corner."""
+
+    def __init__(self, name, positions, pos_idx, normals, nrm_idx):
+        self.name = name
+        self.positions = np.asarray(positions, dtype=np.float32).reshape(-1, 3)
+        self.pos_idx = np.asarray(pos_idx, dtype=np.uint32).reshape(-1)
+        self.normals = np.asarray(normals, dtype=np.float32).reshape(-1, 3)
+        self.nrm_idx = np.asarray(nrm_idx, dtype=np.uint32).reshape(-1)
+        assert len(self.pos_idx) == len(self.nrm_idx) and len(self.pos_idx) % 3 == 0
+
+    @property
+    def triangle_count(self) -> int:
+        return len(self.pos_idx) // 3
+
+
+def quad_mesh(name="Geo_Quad") -> Mesh:
+    p = [[-0.5, 0, -0.5], [-0.5, 0, 0.5], [0.5, 0, 0.5], [0.5, 0, -0.5]]
+    idx = [0, 1, 2, 0, 2, 3]
+    return Mesh(name, p, idx, [[0, 1, 0]], [0] * 6)
+
+
+def box_mesh(name="Geo_Box") -> Mesh:
+    faces = []  # (normal, u axis, v axis)
+    for axis in range(3):
+        for sign in (1.0, -1.0):
+            n = np.zeros(3)
+            n[axis] = sign
+            u = np.zeros(3)
+            u[(axis + 1) % 3] = 1.0
+            v = np.cross(n, u)
+            faces.append((n, u, v))
+    pos, pidx, nrm, nidx = [], [], [], []
+    for fi, (n, u, v) in enumerate(faces):
+        c = 0.5 * n
+        corners = [c - 0.5 * u - 0.5 * v, c + 0.5 * u - 0.5 * v, c + 0.5 * u + 0.5 * v, c - 0.5 * u + 0.5 * v]
+        base = len(pos)
+        pos.extend(corners)
+        nrm.append(n)
+        for tri in ((0, 1, 2), (0, 2, 3)):
+            pidx.extend(base + k for k in tri)
+            nidx.extend([fi] * 3)
+    return Mesh(name, pos, pidx, nrm, nidx)
+
+
+def icosphere_mesh(subdivisions=5, name="Geo_Icosphere") -> Mesh:
+    t = (1.0 + 5.0 ** 0.5) / 2.0
+    verts = [[-1, t, 0], [1, t, 0], [-1, -t, 0], [1, -t, 0], [0, -1, t], [0, 1, t], [0, -1, -t], [0, 1, -t],
+             [t, 0, -1], [t, 0, 1], [-t, 0, -1], [-t, 0, 1]]
+    verts = [list(np.asarray(v) / np.linalg.norm(v)) for v in verts]
+    faces = [[0, 11, 5], [0, 5, 1], [0, 1, 7], [0, 7, 10], [0, 10, 11], [1, 5, 9], [5, 11, 4], [11, 10, 2],
+             [10, 7, 6], [7, 1, 8], [3, 9, 4], [3, 4, 2], [3, 2, 6], [3, 6, 8], [3, 8, 9], [4, 9, 5], [2, 4, 11],
+             [6, 2, 10], [8, 6, 7], [9, 8, 1]]
+    for _ in range(subdivisions):
+        cache = {}
+
+        def mid(a, b):
+            key = (min(a, b), max(a, b))
+            if key not in cache:
+                m = np.asarray(verts[a]) + np.asarray(verts[b])
+                verts.append(list(m / np.linalg.norm(m)))
+                cache[key] = len(verts) - 1
+            return cache[key]
+
+        nf = []
+        for a, b, c in faces:
+            ab, bc, ca = mid(a, b), mid(b, c), mid(c, a)
+            nf += [[a, ab, ca], [b, bc, ab], [c, ca, bc], [ab, bc, ca]]
+        faces = nf
+    v = np.asarray(verts, dtype=np.float64)
+    idx = np.asarray(faces, dtype=np.uint32).reshape(-1)
+    return Mesh(name, v, idx, v, idx)
+
+
+def _fbm2(x, y, rng_perm, octaves=5):
+    """Value-noise fBm on a 2-D grid (numpy), used for heightfield displacement."""
+    total = np.zeros_like(x)
+    amp, freq = 1.0, 1.0
+    for _ in range(octaves):
+        xi = np.floor(x * freq).astype(np.int64)
+        yi = np.floor(y * freq).astype(np.int64)
+        xf = x * freq - xi
+        yf = y * freq - yi
+
+        def h(ix, iy):
+            return rng_perm[(rng_perm[ix & 255] + iy) & 255] / 255.0
+
+        sx = xf * xf * (3 - 2 * xf)
+        sy = yf * yf * (3 - 2 * yf)
+        a = h(xi, yi) + sx * (h(xi + 1, yi) - h(xi, yi))
+        b = h(xi, yi + 1) + sx * (h(xi + 1, yi + 1) - h(xi, yi + 1))
+        total += amp * (a + sy * (b - a))
+        amp *= 0.5
+        freq *= 2.0
+    return total
+
+
+def heightfield_mesh(res=256, seed=1, name="Geo_Heightfield") -> Mesh:
+    rng = np.random.Generator(np.random.PCG64(seed))
+    perm = rng.permutation(256)
+    n = res + 1
+    g = np.linspace(-0.5, 0.5, n)
+    x, z = np.meshgrid(g, g, indexing="xy")
+    hgt = 0.25 * _fbm2((x + 0.5) * 6.0, (z + 0.5) * 6.0, perm)
+    pos = np.stack([x, hgt, z], axis=-1).reshape(-1, 3)
+    # smooth normals from central differences
+    dx = np.gradient(hgt, g, axis=1)
+    dz = np.gradient(hgt, g, axis=0)
+    nrm = np.stack([-dx, np.ones_like(hgt), -dz], axis=-1)
+    nrm /= np.linalg.norm(nrm, axis=-1, keepdims=True)
+    nrm = nrm.reshape(-1, 3)
+    i, j = np.meshgrid(np.arange(res), np.arange(res), indexing="xy")
+    v00 = (j * n + i).reshape(-1)
+    v10 = v00 + 1
+    v01 = v00 + n
+    v11 = v01 + 1
+    tris = np.stack([v00, v01, v11, v00, v11, v10], axis=-1).reshape(-1)  # +y facing
+    return Mesh(name, pos, tris, nrm, tris)
+
+
+def torus_mesh(major=64, minor=32, r_major=0.35, r_minor=0.15, name="Geo_Torus") -> Mesh:
+    u = np.arange(major) * (2 * math.pi / major)
+    v = np.arange(minor) * (2 * math.pi / minor)
+    uu, vv = np.meshgrid(u, v, indexing="ij")
+    cx, cz = np.cos(uu), np.sin(uu)
+    pos = np.stack([(r_major + r_minor * np.cos(vv)) * cx, r_minor * np.sin(vv),
+                    (r_major + r_minor * np.cos(vv)) * cz], axis=-1).reshape(-1, 3)
+    nrm = np.stack([np.cos(vv) * cx, np.sin(vv), np.cos(vv) * cz], axis=-1).reshape(-1, 3)
+    i, j = np.meshgrid(np.arange(major), np.arange(minor), indexing="ij")
+    a = (i * minor + j)
+    b = (((i + 1) % major) * minor + j)
+    c = (((i + 1) % major) * minor + (j + 1) % minor)
+    d = (i * minor + (j + 1) % minor)
+    tris = np.stack([a, d, c, a, c, b], axis=-1).reshape(-1)
+    return Mesh(name, pos, tris, nrm, tris)
+
+
+# ------------------------------------------------------------ scene model ---
+
+class Scene:
+    def __init__(self):
+        self.camera = None  # (from, look, fov)
+        self.meshes = []
+        self.transforms = []  # (name, translate, scale, rotate_deg)
+        self.materials = []   # (kind, name, dict)
+        self.textures = []    # (kind, name, dict)
+        self.volumes = []     # (name, transform, sigma_t, albedo, g, density_texture or None)
+        self.instances = []   # (name, geometry, transform, material, volume or None, boundary)
+
+    @property
+    def triangle_count(self) -> int:
+        by_name = {m.name: m.triangle_count for m in self.meshes}
+        return sum(by_name[i[1]] for i in self.instances)
+
+
+def _f(v) -> str:
+    # shortest positional decimal that reads back as the same float32 (the
+    # reference's parser accepts no exponent notation)
+    return np.format_float_positional(np.float32(v), unique=True, trim="-")
+
+
+def _vec(v) -> str:
+    return "<" + ",".join(_f(x) for x in v) + ">"
+
+
+def _arr(a, fmt) -> str:
+    return "[" + ",".join(fmt(x) for x in a) + "]"
+
+
+def write_scene(scene: Scene, path: str) -> str:
+    out = []
+    frm, look, fov = scene.camera
+    out.append(f"Begin(Camera);\n\tfov = {_f(fov)};\n\tfrom = {_vec(frm)};\n\tlook = {_vec(look)};\nEnd(Camera);\n")
+    for m in scene.meshes:
+        n = m.triangle_count
+        corners = np.arange(3 * n, dtype=np.uint32)
+        pos = m.positions.astype(np.float32).reshape(-1)
+        nrm = m.normals.astype(np.float32).reshape(-1)
+        out.append("Begin(Mesh);\n")
+        out.append(f'\tname = "{m.name}";\n')
+        out.append("\tmesh_triangles = " + _arr(corners.tolist(), str) + ";\n")
+        out.append("\tmesh_position_indices = " + _arr(m.pos_idx.tolist(), str) + ";\n")
+        out.append("\tmesh_positions = " + _arr(pos, _f) + ";\n")
+        out.append("\tmesh_normal_indices = " + _arr(m.nrm_idx.tolist(), str) + ";\n")
+        out.append("\tmesh_normals = " + _arr(nrm, _f) + ";\n")
+        out.append("End(Mesh);\n")
+    for name, t, s, r in scene.transforms:
+        out.append(f'Begin(Transform);\n\tname = "{name}";\n\ttranslate = {_vec(t)};\n\tscale = {_vec(s)};\n'
+                   f'\trotate = {_vec(r)};\nEnd(Transform);\n')
+    for kind, name, attrs in scene.textures:
+        out.append(f"Begin({kind});\n\tname = \"{name}\";\n")
+        for k, v in attrs.items():
+            if isinstance(v, str):
+                out.append(f'\t{k} = "{v}";\n')
+            elif isinstance(v, bool):
+                out.append(f"\t{k} = {'true' if v else 'false'};\n")
+            elif isinstance(v, int):
+                out.append(f"\t{k} = {v};\n")
+            else:
+                out.append(f"\t{k} = {_f(v)};\n")
+        out.append(f"End({kind});\n")
+    for kind, name, attrs in scene.materials:
+        out.append(f"Begin({kind});\n\tname = \"{name}\";\n")
+        for k, v in attrs.items():
+            if isinstance(v, (list, tuple, np.ndarray)):
+                out.append(f"\t{k} = {_vec(v)};\n")
+            elif isinstance(v, int):
+                out.append(f"\t{k} = {v};\n")
+            else:
+                out.append(f"\t{k} = {_f(v)};\n")
+        out.append(f"End({kind});\n")
+    for name, tr, sigma, albedo, g, dens in scene.volumes:
+        out.append(f'Begin(Volume);\n\tname = "{name}";\n\ttransform_index = "{tr}";\n\tsigma_t = {_vec(sigma)};\n'
+                   f"\talbedo = {_vec(albedo)};\n\tg = {_f(g)};\n")
+        if dens is not None:
+            out.append(f'\tdensity_texture_index = "{dens}";\n')
+        out.append("End(Volume);\n")
+    for name, geo, tr, mat, vol, boundary in scene.instances:
+        out.append(f'Begin(PrimitiveInstance);\n\tname = "{name}";\n\tgeometry_index = "{geo}";\n'
+                   f'\ttransform_index = "{tr}";\n\tmaterial_index = "{mat}";\n')
+        if vol is not None:
+            out.append(f'\tinner_volume_index = "{vol}";\n')
+        out.append(f"\ttreat_as_boundary = {'true' if boundary else 'false'};\nEnd(PrimitiveInstance);\n")
+    d = os.path.dirname(os.path.abspath(path))
+    os.makedirs(d, exist_ok=True)
+    tmp = path + ".tmp"
+    with open(tmp, "w") as f:
+        f.write("".join(out))
+    os.replace(tmp, path)
+    return path
+
+
+def _lambert(rgb) -> dict:
+    return {"diffuse_albedo": list(rgb), "specular_weight": 0.0, "metalness": 0.0, "transmission_weight": 0.0,
+            "coat_weight": 0.0}
+
+
+def cornell_scene(seed: int = 0) -> Scene:
+    rng = np.random.Generator(np.random.PCG64(seed))
+    s = Scene()
+    s.camera = ((0.0, 0.0, 3.4), (0.0, 0.0, 0.0), 40.0)
+    s.meshes = [quad_mesh(), box_mesh()]
+    walls = [("floor", (0, -1, 0), (0, 0, 0)), ("ceiling", (0, 1, 0), (180, 0, 0)),
+             ("back", (0, 0, -1), (90, 0, 0)), ("left", (-1, 0, 0), (0, 0, -90)),
+             ("right", (1, 0, 0), (0, 0, 90))]
+    for name, t, r in walls:
+        s.transforms.append((name + "_transform", t, (2, 1, 2), r))
+        s.materials.append(("DefaultMaterial", name + "_material", _lambert(rng.uniform(0.1, 0.9, 3))))
+        s.instances.append((name, "Geo_Quad", name + "_transform", name + "_material", None, False))
+    boxes = [("tall_box", (-0.35, -0.399, -0.3), (0.6, 1.2, 0.6)), ("short_box", (0.35, -0.699, 0.3), (0.6, 0.6, 0.6))]
+    for name, t, sc in boxes:
+        s.transforms.append((name + "_transform", t, sc, (0.0, float(rng.uniform(0, 45)), 0.0)))
+        s.materials.append(("DefaultMaterial", name + "_material", _lambert(rng.uniform(0.1, 0.9, 3))))
+        s.instances.append((name, "Geo_Box", name + "_transform", name + "_material", None, False))
+    s.transforms.append(("light_transform", (0, 0.995, 0), (0.5, 1, 0.5), (180, 0, 0)))
+    s.materials.append(("LightMaterial", "light_material", {"light_color": [1.0, 1.0, 1.0], "intensity": 15.0}))
+    s.instances.append(("light", "Geo_Quad", "light_transform", "light_material", None, False))
+    return s
+
+
+def instanced_scene(seed: int = 0) -> Scene:
+    rng = np.random.Generator(np.random.PCG64(seed))
+    s = Scene()
+    s.camera = ((0.0, 9.0, 24.0), (0.0, 1.5, 0.0), 45.0)
+    sphere, hfield, torus, box = icosphere_mesh(5), heightfield_mesh(256, seed + 1), torus_mesh(), box_mesh()
+    s.meshes = [sphere, hfield, torus, box, quad_mesh()]
+    # 7 heightfields + 12 spheres + 16 tori + 29 boxes = 1,229,148 triangles in 64 instances
+    kinds = ["Geo_Heightfield"] * 7 + ["Geo_Icosphere"] * 12 + ["Geo_Torus"] * 16 + ["Geo_Box"] * 29
+    order = rng.permutation(len(kinds))
+    closed = {"Geo_Icosphere", "Geo_Torus", "Geo_Box"}
+    for m in range(32):
+        kind = m % 3
+        if kind == 0:
+            r = float(rng.uniform(0.05, 0.8))
+            attrs = {"diffuse_albedo": list(rng.uniform(0.4, 0.95, 3)), "specular_albedo": list(rng.uniform(0.5, 1.0, 3)),
+                     "roughness_x": r, "roughness_y": r, "metalness": 1.0}
+        elif kind == 1:
+            r = float(rng.uniform(0.0, 0.3))
+            attrs = {"diffuse_albedo": [0.5, 0.5, 0.5], "specular_albedo": list(rng.uniform(0.85, 1.0, 3)),
+                     "roughness_x": r, "roughness_y": r, "ior_n": 1.5, "metalness": 0.0, "specular_weight": 1.0,
+                     "transmission_weight": 1.0}
+        else:
+            attrs = _lambert(rng.uniform(0.1, 0.9, 3))
+        s.materials.append(("DefaultMaterial", f"material_{m}", attrs))
+    diffuse = [m for m in range(32) if m % 3 == 2]
+    for i, k in enumerate(order):
+        geo = kinds[k]
+        if geo == "Geo_Heightfield":
+            sc = rng.uniform(5.0, 9.0)
+            scale = (sc, float(rng.uniform(2.0, 4.0)), sc)
+            t = (float(rng.uniform(-8, 8)), float(rng.uniform(-1.0, 0.0)), float(rng.uniform(-8, 8)))
+            rot = (0.0, float(rng.uniform(0, 360)), 0.0)
+        else:
+            sc = float(rng.uniform(0.6, 2.2))
+            scale = (sc * float(rng.uniform(0.8, 1.25)), sc * float(rng.uniform(0.8, 1.25)), sc * float(rng.uniform(0.8, 1.25)))
+            t = (float(rng.uniform(-9, 9)), float(rng.uniform(0.3, 4.0)), float(rng.uniform(-9, 9)))
+            rot = tuple(float(x) for x in rng.uniform(0, 360, 3))
+        mat = int(rng.integers(0, 32))
+        if mat % 3 == 1 and geo not in closed:
+            mat = diffuse[int(rng.integers(0, len(diffuse)))]
+        s.transforms.append((f"t_{i}", t, scale, rot))
+        s.instances.append((f"inst_{i}", geo, f"t_{i}", f"material_{mat}", None, False))
+    for li, (lt, rot) in enumerate((((-5.0, 14.0, 2.0), (180, 0, 15)), ((6.0, 12.0, -4.0), (180, 0, -20)))):
+        s.transforms.append((f"light_t_{li}", lt, (6.0, 1.0, 6.0), rot))
+        s.materials.append(("LightMaterial", f"light_material_{li}", {"light_color": [1.0, 0.95, 0.9], "intensity": 12.0}))
+        s.instances.append((f"light_{li}", "Geo_Quad", f"light_t_{li}", f"light_material_{li}", None, False))
+    return s
+
+
+def volumetric_scene(seed: int = 0) -> Scene:
+    s = cornell_scene(seed)
+    s.textures.append(("ConstantTextureFloat", "density_black", {"value": 0.0}))
+    s.textures.append(("ConstantTextureFloat", "density_white", {"value": 1.0}))
+    s.textures.append(("NoiseTextureFBM", "density_fbm", {
+        "texture_black_idx": "density_black", "texture_white_idx": "density_white", "frequency": 4.0,
+        "lacunarity": 2.0, "gain": 0.5, "layer_count": 4, "amplitude": 1.0, "offset": 0.0}))
+    s.transforms.append(("fog_transform", (0.0, 0.0, 0.0), (1.98, 1.98, 1.98), (0, 0, 0)))
+    s.volumes.append(("fog_volume", "fog_transform", (0.05, 0.05, 0.05), (0.8, 0.8, 0.8), 0.6, None))
+    s.materials.append(("DefaultMaterial", "boundary_material", {"ior_n": 1.0}))
+    s.instances.append(("fog_box", "Geo_Box", "fog_transform", "boundary_material", "fog_volume", True))
+    s.transforms.append(("smoke_transform", (0.3, 0.2, 0.0), (0.7, 0.7, 0.7), (0, 0, 0)))
+    s.volumes.append(("smoke_volume", "smoke_transform", (2.0, 2.0, 2.0), (0.9, 0.9, 0.9), 0.0, "density_fbm"))
+    s.materials.append(("DefaultMaterial", "smoke_boundary_material", {"ior_n": 1.0, "ior_priority": 1}))
+    s.instances.append(("smoke_box", "Geo_Box", "smoke_transform", "smoke_boundary_material", "smoke_volume", True))
+    return s
+
+
+SCENES = {
+    "cornell": cornell_scene,
+    "instanced": instanced_scene,
+    "volumetric": volumetric_scene,
+}
+
+
+def scene_path(name: str, seed: int = 0, cache_dir: str | None = None) -> str:
+    """Writes (once) and returns the path of a generated scene file."""
+    cache_dir = cache_dir or os.environ.get("YMRT_SCENE_CACHE", os.path.join(os.path.dirname(__file__), "_scenes"))
+    path = os.path.join(cache_dir, f"{name}_{seed}.ymtmp")
+    if not os.path.exists(path):
+        write_scene(SCENES[name](seed), path)
+    return path
