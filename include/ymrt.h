@@ -79,8 +79,11 @@ typedef struct ymrt_stats {
   uint64_t extension_rays;   /* closest-hit queries */
   uint64_t shadow_rays;      /* any-hit (occlusion) queries */
   uint64_t waves;            /* extend/shade iterations */
+  uint64_t node_visits;      /* wide-BVH nodes fetched by all queries */
+  uint64_t triangle_tests;   /* triangles fetched and tested by all queries */
+  uint64_t kernel_launches;  /* kernels launched for the frame */
   double ms_total;           /* device time of the frame (CUDA events) */
-  double ms_generate;
+  double ms_generate;        /* per-stage device time; filled when profiling is on */
   double ms_extend;
   double ms_shade;
   uint32_t device_errors;    /* bit set of YMRT_DEVERR_* raised on the device */
@@ -98,6 +101,9 @@ void ymrt_destroy(ymrt_context* ctx);
 const char* ymrt_last_error(const ymrt_context* ctx);
 /* Largest number of paths in flight (queue slots); 0 keeps the default. */
 int ymrt_set_queue_capacity(ymrt_context* ctx, uint32_t paths);
+/* When enabled, every stage launch is bracketed by CUDA events and the
+ * per-stage times are reported in ymrt_stats (costs a little host time). */
+int ymrt_set_profiling(ymrt_context* ctx, int enable);
 
 /* ---- scenes ---- */
 /* Parses and prepares a scene on the host (no GPU needed). err may be NULL. */

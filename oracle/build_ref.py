@@ -21,6 +21,11 @@ are drawn left to right (the order nvcc's device front end uses); with
 ``"native"`` the file is compiled unchanged (g++ on x86-64 evaluates them
 right to left). Nothing else in the file is changed.
 
+The same build-time copy also counts the stage kernels' closest-hit and
+occlusion queries, and reads the maximum-priority record of the nested-media
+stack directly where the reference reads it through a dangling reference
+(see ``_COUNTERS``).
+
 Usage: ``python oracle/build_ref.py [--arg-order ltr|native] [--force]``.
 """
 from __future__ import annotations
@@ -65,6 +70,10 @@ def _includes():
         "-I/usr/local/cuda/include",
     ]
 
+
+# The library binds its own symbols (-Bsymbolic): its CUDA-runtime stand-ins
+# must win over a real libcudart that the host process (e.g. torch) may have
+# loaded globally.
 
 # Call arguments made of several sampler draws, e.g. "random(), random()" or
 # "ray_sampler.Random1D(), ray_sampler.Random1D(), ray_sampler.Random1D()".
@@ -111,21 +120,61 @@ inline float ymrt_oracle_draw_in_order(Draw draw, int n, int k) {
 '''
 
 
+# Ray counting: the build-time copy routes the stage kernels' calls of the
+# reference's closest-hit and occlusion queries (TraceRay,
+# BVHTraverseShadow) through counting wrappers, so the reference's Mrays/s is
+# computed from the same query counts as ymrt_b200's.
+_COUNTERS = r'''
+// ---- inserted by oracle/build_ref.py: query counters ----
+#include <atomic>
+std::atomic<unsigned long long> ymrt_oracle_trace_queries{0};
+std::atomic<unsigned long long> ymrt_oracle_shadow_queries{0};
+template <typename... A>
+inline bool ymrt_oracle_counted_trace(A&&... a) {
+  ymrt_oracle_trace_queries.fetch_add(1, std::memory_order_relaxed);
+  return YMRT::TraceRay(std::forward<A>(a)...);
+}
+template <typename... A>
+inline bool ymrt_oracle_counted_shadow(A&&... a) {
+  ymrt_oracle_shadow_queries.fetch_add(1, std::memory_order_relaxed);
+  return YMRT::BVHTraverseShadow(std::forward<A>(a)...);
+}
+// RayTransfer::GetMaxPriorityRecord (src/Ray.h:148-151) returns a reference
+// bound to a temporary copy of the selected record (its conditional operator
+// has a prvalue branch); g++ compiles reading through that dangling reference
+// into a null dereference. The priority the expression copies is read here
+// directly, which is the value the device build reads.
+inline uint32_t ymrt_oracle_max_priority(const YMRT::RayTransfer& rt) {
+  return rt.max_priority_record_index != -1 ? rt.boundary_records[rt.max_priority_record_index].ior_priority
+                                            : YMRT::BoundaryRecord().ior_priority;
+}
+// ---- end of insertion ----
+'''
+
+
 def shading_source(arg_order: str) -> str:
     src = os.path.join(REF, "src", "Shading.cu")
-    if arg_order == "native":
-        return src
     with open(src, "r", encoding="utf-8", errors="replace") as f:
         text = f.read()
-    body, n = _sequence_draws(text)
+    n = 0
+    if arg_order == "ltr":
+        text, n = _sequence_draws(text)
+    # counting wrappers go after the includes, before the first namespace block
+    first_ns = text.index("namespace YMRT")
+    head, body = text[:first_ns], text[first_ns:]
+    body, n_trace = re.subn(r"\bTraceRay\(", "ymrt_oracle_counted_trace(", body)
+    body, n_shadow = re.subn(r"\bBVHTraverseShadow\(", "ymrt_oracle_counted_shadow(", body)
+    body, n_prio = re.subn(r"\b(\w+)\.GetMaxPriorityRecord\(\)\.ior_priority", r"ymrt_oracle_max_priority(\1)", body)
+    line_of_body = head.count("\n") + 1
     gen_dir = os.path.join(OUT, "gen")
     os.makedirs(gen_dir, exist_ok=True)
     dst = os.path.join(gen_dir, "Shading.cu")
-    out = _HELPER + f'#line 1 "{src}"\n' + body
+    out = (_HELPER + f'#line 1 "{src}"\n' + head + _COUNTERS + f'#line {line_of_body} "{src}"\n' + body)
     with open(dst, "w") as f:
         f.write(out)
     with open(os.path.join(gen_dir, "Shading.cu.sites"), "w") as f:
-        f.write(f"{n} argument lists rewritten\n")
+        f.write(f"{n} argument lists sequenced, {n_trace} TraceRay and {n_shadow} BVHTraverseShadow calls counted, "
+                f"{n_prio} GetMaxPriorityRecord reads made direct\n")
     return dst
 
 
@@ -174,7 +223,7 @@ def build(arg_order: str = "ltr", force: bool = False, jobs: int = 8) -> str:
         if p.returncode != 0:
             raise RuntimeError(f"oracle build failed for {src}:\n{out.decode(errors='replace')[-4000:]}")
     tmp = LIB + ".tmp"
-    cmd = ["g++", "-shared", "-pthread", "-o", tmp] + objs + ["-Wl,--no-undefined"]
+    cmd = ["g++", "-shared", "-pthread", "-o", tmp] + objs + ["-Wl,--no-undefined", "-Wl,-Bsymbolic"]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError("oracle link failed:\n" + r.stdout[-4000:] + r.stderr[-4000:])

@@ -59,6 +59,7 @@ def lib():
         L.ymref_last_render_seconds.restype = ctypes.c_double
         L.ymref_last_render_seconds.argtypes = [vp]
         L.ymref_accumulate.argtypes = [vp, vp, i, i, i]
+        L.ymref_query_counts.argtypes = [vp, i]
         _lib = L
     return _lib
 
@@ -179,3 +180,11 @@ class RefScene:
 
     def last_render_seconds(self) -> float:
         return lib().ymref_last_render_seconds(self.h)
+
+
+def query_counts(reset: bool = True) -> tuple[int, int]:
+    """(closest-hit queries, occlusion queries) made by the reference's stage
+    kernels since the last reset, across all scenes."""
+    out = np.zeros(2, np.uint64)
+    lib().ymref_query_counts(_p(out), int(reset))
+    return int(out[0]), int(out[1])

@@ -448,6 +448,17 @@ int ymref_render_frame(void* handle, int frame_index, int tile_begin, int tile_e
 
 double ymref_last_render_seconds(void* handle) { return static_cast<RefContext*>(handle)->last_render_seconds; }
 
+// Closest-hit (TraceRay) and occlusion (BVHTraverseShadow) queries made by the
+// stage kernels since the last reset (counted by oracle/build_ref.py's copy).
+void ymref_query_counts(unsigned long long* out, int reset) {
+  out[0] = ymrt_oracle_trace_queries.load();
+  out[1] = ymrt_oracle_shadow_queries.load();
+  if (reset) {
+    ymrt_oracle_trace_queries.store(0);
+    ymrt_oracle_shadow_queries.store(0);
+  }
+}
+
 // Running mean over frames, src/Shading.cu:2354 Accumulate_image_path_tracing.
 void ymref_accumulate(const float* noise, float* acc, int width, int height, int frame_index) {
   for (int y = 0; y < height; ++y)

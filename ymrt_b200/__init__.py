@@ -68,7 +68,8 @@ def default_setting(spp=1, ray_depth=8, shape_light=True, distant_light=False, v
 class Stats(ctypes.Structure):
     _fields_ = [
         ("paths", ctypes.c_uint64), ("extension_rays", ctypes.c_uint64), ("shadow_rays", ctypes.c_uint64),
-        ("waves", ctypes.c_uint64), ("ms_total", ctypes.c_double), ("ms_generate", ctypes.c_double),
+        ("waves", ctypes.c_uint64), ("node_visits", ctypes.c_uint64), ("triangle_tests", ctypes.c_uint64),
+        ("kernel_launches", ctypes.c_uint64), ("ms_total", ctypes.c_double), ("ms_generate", ctypes.c_double),
         ("ms_extend", ctypes.c_double), ("ms_shade", ctypes.c_double), ("device_errors", ctypes.c_uint32),
         ("reserved_", ctypes.c_uint32),
     ]
@@ -94,6 +95,7 @@ def library():
     L.ymrt_last_error.restype = ctypes.c_char_p
     L.ymrt_last_error.argtypes = [vp]
     L.ymrt_set_queue_capacity.argtypes = [vp, ctypes.c_uint32]
+    L.ymrt_set_profiling.argtypes = [vp, i]
     L.ymrt_scene_load_ymtmp.argtypes = [ctypes.c_char_p, i, i, ctypes.POINTER(vp), ctypes.c_char_p, sz]
     L.ymrt_host_scene_free.argtypes = [vp]
     L.ymrt_host_scene_query.restype = ctypes.c_longlong
@@ -123,11 +125,13 @@ def _check(rc: int, ctx=None):
 class Context:
     """One CUDA device + stream (the reference's RenderModule path-tracing stream)."""
 
-    def __init__(self, device: int = 0, queue_capacity: int = 0):
+    def __init__(self, device: int = 0, queue_capacity: int = 0, profiling: bool = False):
         self.h = ctypes.c_void_p()
         _check(library().ymrt_create(device, ctypes.byref(self.h)))
         if queue_capacity:
             library().ymrt_set_queue_capacity(self.h, queue_capacity)
+        if profiling:
+            library().ymrt_set_profiling(self.h, 1)
 
     def close(self):
         if self.h:

@@ -86,7 +86,14 @@ def build(force: bool = False, verbose: bool = False, ptxas_report: bool = False
         if verbose or ptxas_report:
             reports.append(out)
     tmp = LIB + ".tmp"
-    _run([NVCC] + ARCH + ["-shared", "-cudart", "static", "-o", tmp] + objs, verbose)
+    # Export only the C ABI and bind internal references locally, so the
+    # statically linked CUDA runtime never collides with another copy loaded
+    # by the host process (torch, the oracle).
+    vs = os.path.join(OUT_DIR, "exports.map")
+    with open(vs, "w") as f:
+        f.write("{ global: ymrt_*; local: *; };\n")
+    _run([NVCC] + ARCH + ["-shared", "-cudart", "static", "-o", tmp] + objs +
+         ["-Xlinker", "-Bsymbolic", "-Xlinker", "--version-script=" + vs], verbose)
     os.replace(tmp, LIB)
     with open(stamp_file, "w") as f:
         f.write(stamp)

@@ -77,6 +77,8 @@ struct ymrt_context {
   uint32_t pool_capacity = 0;
   WaveCounters* counters_host = nullptr;  // pinned
   cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
+  bool profiling = false;
+  cudaEvent_t ev_stage[4] = {nullptr, nullptr, nullptr, nullptr};
   std::vector<uint32_t> primes, prime_sums;
 
   int fail(int code, const std::string& msg) {
@@ -164,6 +166,8 @@ int ymrt_create(int device_ordinal, ymrt_context** out) {
     return ctx->cuda_fail(e, "cudaStreamCreate");
   if ((e = cudaEventCreate(&ctx->ev_start)) != cudaSuccess || (e = cudaEventCreate(&ctx->ev_stop)) != cudaSuccess)
     return ctx->cuda_fail(e, "cudaEventCreate");
+  for (auto& ev : ctx->ev_stage)
+    if ((e = cudaEventCreate(&ev)) != cudaSuccess) return ctx->cuda_fail(e, "cudaEventCreate");
   if ((e = cudaMallocHost(&ctx->counters_host, sizeof(WaveCounters))) != cudaSuccess)
     return ctx->cuda_fail(e, "cudaMallocHost");
   if ((e = ctx->counters_buf.ensure(sizeof(WaveCounters))) != cudaSuccess) return ctx->cuda_fail(e, "cudaMalloc");
@@ -189,6 +193,8 @@ void ymrt_destroy(ymrt_context* ctx) {
   if (ctx->counters_host) cudaFreeHost(ctx->counters_host);
   if (ctx->ev_start) cudaEventDestroy(ctx->ev_start);
   if (ctx->ev_stop) cudaEventDestroy(ctx->ev_stop);
+  for (auto& ev : ctx->ev_stage)
+    if (ev) cudaEventDestroy(ev);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
 }
@@ -198,6 +204,12 @@ const char* ymrt_last_error(const ymrt_context* ctx) { return ctx ? ctx->error.c
 int ymrt_set_queue_capacity(ymrt_context* ctx, uint32_t paths) {
   if (!ctx) return YMRT_ERR_INVALID;
   ctx->capacity = paths ? paths : (1u << 21);
+  return YMRT_OK;
+}
+
+int ymrt_set_profiling(ymrt_context* ctx, int enable) {
+  if (!ctx) return YMRT_ERR_INVALID;
+  ctx->profiling = enable != 0;
   return YMRT_OK;
 }
 
@@ -436,20 +448,33 @@ int ymrt_render_tiles(ymrt_scene* sc, const ymrt_render_setting* setting, int fr
   cudaEventRecord(ctx->ev_start, st);
   uint32_t live = 0;
   int a = 0;
-  uint64_t waves = 0, paths = 0;
+  uint64_t waves = 0, paths = 0, launches = 0;
+  double ms_stage[3] = {0.0, 0.0, 0.0};
   while (live > 0 || cursor < t_end) {
     const uint32_t n_tiles = std::min<uint32_t>((ctx->capacity - live) / per_tile, t_end - cursor);
     const uint32_t gen = n_tiles * per_tile;
     PathPool& A = ctx->pool[a];
     PathPool& B = ctx->pool[a ^ 1];
-    launch_generate(A, live, gen, cursor, tiles_x, frame_index, spp, st);
     const uint32_t total = live + gen;
+    if (ctx->profiling) cudaEventRecord(ctx->ev_stage[0], st);
+    launch_generate(A, live, gen, cursor, tiles_x, frame_index, spp, st);
+    if (ctx->profiling) cudaEventRecord(ctx->ev_stage[1], st);
     launch_extend(A, total, ctx->hits, image, dc, st);
+    if (ctx->profiling) cudaEventRecord(ctx->ev_stage[2], st);
     cudaMemsetAsync(&dc->next_count, 0, sizeof(uint32_t), st);
     launch_shade(A, total, ctx->hits, B, image, dc, st);
+    if (ctx->profiling) cudaEventRecord(ctx->ev_stage[3], st);
+    launches += (gen > 0 ? 1 : 0) + (total > 0 ? 2 : 0);
     if ((e = cudaMemcpyAsync(ctx->counters_host, dc, sizeof(WaveCounters), cudaMemcpyDeviceToHost, st)) != cudaSuccess)
       return ctx->cuda_fail(e, "reading wave counters");
     if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return ctx->cuda_fail(e, "wave");
+    if (ctx->profiling) {
+      for (int k = 0; k < 3; ++k) {
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, ctx->ev_stage[k], ctx->ev_stage[k + 1]);
+        ms_stage[k] += ms;
+      }
+    }
     live = ctx->counters_host->next_count;
     if (live > ctx->capacity) return ctx->fail(YMRT_ERR_OVERFLOW, "path queue overflow");
     a ^= 1;
@@ -473,7 +498,13 @@ int ymrt_render_tiles(ymrt_scene* sc, const ymrt_render_setting* setting, int fr
     stats->extension_rays = ctx->counters_host->extension_rays;
     stats->shadow_rays = ctx->counters_host->shadow_rays;
     stats->waves = waves;
+    stats->node_visits = ctx->counters_host->node_visits;
+    stats->triangle_tests = ctx->counters_host->tri_tests;
+    stats->kernel_launches = launches;
     stats->ms_total = ms;
+    stats->ms_generate = ms_stage[0];
+    stats->ms_extend = ms_stage[1];
+    stats->ms_shade = ms_stage[2];
     stats->device_errors = ctx->counters_host->errors;
   }
   if (ctx->counters_host->errors & kDevErrQueue) return ctx->fail(YMRT_ERR_OVERFLOW, "path queue overflow on the device");

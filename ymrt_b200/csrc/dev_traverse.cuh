@@ -232,7 +232,7 @@ struct ClosestHit {
 // `volume_only`: traverse only treat_as_boundary instances (TraceVolume, :434-561).
 __device__ __noinline__ bool trace_closest(const DeviceScene& S, TraversalStack& st, vec3 wo, vec3 wd, float tmax,
                                            uint32_t last_inst, uint32_t last_tri, bool volume_only, ClosestHit* out,
-                                           uint32_t* tri_tests) {
+                                           uint32_t* tri_tests, uint32_t* node_visits) {
   const uint4* tlas = reinterpret_cast<const uint4*>(S.tlas_nodes);
   const uint4* blas = reinterpret_cast<const uint4*>(S.blas_nodes);
   const bool skip_enabled = last_inst != kEmpty && last_tri != kEmpty;
@@ -246,6 +246,7 @@ __device__ __noinline__ bool trace_closest(const DeviceScene& S, TraversalStack&
   st.push(0);
   while (st.sp > 0) {
     const uint32_t node = st.pop();
+    ++*node_visits;
     float tn[8];
     uint32_t imask, cbase, pbase, meta[2];
     const uint32_t hits = intersect_children(tlas, node, wray, t_ray, tn, &imask, &cbase, &pbase, meta);
@@ -276,6 +277,7 @@ __device__ __noinline__ bool trace_closest(const DeviceScene& S, TraversalStack&
         st.push(g.node_offset);
         while (st.sp > base) {
           const uint32_t bn = st.pop();
+          ++*node_visits;
           float btn[8];
           uint32_t bim, bcb, bpb, bmeta[2];
           const uint32_t bh = intersect_children(blas, bn, br, t_ray, btn, &bim, &bcb, &bpb, bmeta);
@@ -356,7 +358,7 @@ __device__ __noinline__ bool trace_closest(const DeviceScene& S, TraversalStack&
 // Any hit within (TMIN, tmax] ignoring boundary-only instances
 // (BVHTraverseShadow, src/ShadingUtilities.cuh:563-635).
 __device__ __noinline__ bool trace_occluded(const DeviceScene& S, TraversalStack& st, vec3 wo, vec3 wd, float tmax,
-                                            uint32_t* tri_tests) {
+                                            uint32_t* tri_tests, uint32_t* node_visits) {
   const uint4* tlas = reinterpret_cast<const uint4*>(S.tlas_nodes);
   const uint4* blas = reinterpret_cast<const uint4*>(S.blas_nodes);
   const BoxRay wray = make_box_ray(wo, wd);
@@ -364,6 +366,7 @@ __device__ __noinline__ bool trace_occluded(const DeviceScene& S, TraversalStack
   st.push(0);
   while (st.sp > 0) {
     const uint32_t node = st.pop();
+    ++*node_visits;
     float tn[8];
     uint32_t imask, cbase, pbase, meta[2];
     const uint32_t hits = intersect_children(tlas, node, wray, tmax, tn, &imask, &cbase, &pbase, meta);
@@ -387,6 +390,7 @@ __device__ __noinline__ bool trace_occluded(const DeviceScene& S, TraversalStack
         st.push(g.node_offset);
         while (st.sp > base) {
           const uint32_t bn = st.pop();
+          ++*node_visits;
           float btn[8];
           uint32_t bim, bcb, bpb, bmeta[2];
           const uint32_t bh = intersect_children(blas, bn, br, tmax, btn, &bim, &bcb, &bpb, bmeta);

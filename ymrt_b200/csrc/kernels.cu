@@ -117,7 +117,7 @@ __global__ void __launch_bounds__(kTraceBlock) k_extend(PathPool P, uint32_t cou
                                                         WaveCounters* counters) {
   __shared__ uint32_t s_stack[kStackShared * kTraceBlock];
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  uint32_t tests = 0;
+  uint32_t tests = 0, nodes = 0;
   bool active = i < count;
   uint2 pf = active ? P.pixel_flags[i] : make_uint2(kEmpty, kFlagDead);
   if (active && (pf.y & kFlagDead)) active = false;
@@ -132,7 +132,7 @@ __global__ void __launch_bounds__(kTraceBlock) k_extend(PathPool P, uint32_t cou
     st.sp = 0;
     st.overflow = false;
     ClosestHit ch;
-    const bool hit = trace_closest(S, st, o, d, kTMax, lh.x, lh.y, false, &ch, &tests);
+    const bool hit = trace_closest(S, st, o, d, kTMax, lh.x, lh.y, false, &ch, &tests, &nodes);
     overflow = st.overflow;
     if (!hit) {
       // Ray_trace_path_tracing miss branch (src/Shading.cu:1855-1864).
@@ -160,11 +160,15 @@ __global__ void __launch_bounds__(kTraceBlock) k_extend(PathPool P, uint32_t cou
   }
   // counters: one atomic per warp
   const uint32_t n_rays = __popc(__ballot_sync(0xFFFFFFFFu, active));
-  uint32_t t_sum = tests;
-  for (int off = 16; off > 0; off >>= 1) t_sum += __shfl_down_sync(0xFFFFFFFFu, t_sum, off);
+  uint32_t t_sum = tests, n_sum = nodes;
+  for (int off = 16; off > 0; off >>= 1) {
+    t_sum += __shfl_down_sync(0xFFFFFFFFu, t_sum, off);
+    n_sum += __shfl_down_sync(0xFFFFFFFFu, n_sum, off);
+  }
   if ((threadIdx.x & 31) == 0) {
     if (n_rays) atomicAdd(&counters->extension_rays, (unsigned long long)n_rays);
     if (t_sum) atomicAdd(&counters->tri_tests, (unsigned long long)t_sum);
+    if (n_sum) atomicAdd(&counters->node_visits, (unsigned long long)n_sum);
   }
   if (overflow) atomicOr(&counters->errors, (uint32_t)kDevErrStack);
 }
@@ -259,7 +263,7 @@ __device__ __forceinline__ float ex_ior(const RayTransfer& rt, uint32_t hit_prim
 // EvalShapeLight (src/Shading.cu:294-417) for surfaces without media.
 __device__ __forceinline__ vec3 eval_shape_light(const DeviceScene& S, TraversalStack& st, const LayeredBsdf& B,
                                                  vec3 ray_dir, vec3 p, vec3 p_err, vec3 ng, HaltonState& hs,
-                                                 uint32_t* shadow_rays, uint32_t* tests) {
+                                                 uint32_t* shadow_rays, uint32_t* tests, uint32_t* nodes) {
   if (S.shape_light_count == 0) return vec3(0.0f);
   vec3 direct(0.0f);
   const vec3 wo = B.to_local(-ray_dir);
@@ -283,7 +287,7 @@ __device__ __forceinline__ vec3 eval_shape_light(const DeviceScene& S, Traversal
       const bool invalid = (!same_hemisphere(wo, lwi) && !tb) || (same_hemisphere(wo, lwi) && tb);
       if (!invalid) {
         ++*shadow_rays;
-        if (!trace_occluded(S, st, so, normalize(ldir), maxd, tests)) {
+        if (!trace_occluded(S, st, so, normalize(ldir), maxd, tests, nodes)) {
           const float mis = power_heuristic(lpdf, wpdf);
           direct += mis * 1.0f * vmin(f, vec3(kMaxColorClamp)) * vmin(Li, vec3(kMaxColorClamp));
         }
@@ -307,7 +311,7 @@ __device__ __forceinline__ vec3 eval_shape_light(const DeviceScene& S, Traversal
         const bool invalid = (!same_hemisphere(wo, bwi) && !tb) || (same_hemisphere(wo, bwi) && tb);
         if (!invalid) {
           ++*shadow_rays;
-          if (!trace_occluded(S, st, so, normalize(ldir), maxd, tests)) {
+          if (!trace_occluded(S, st, so, normalize(ldir), maxd, tests, nodes)) {
             const float mis = power_heuristic(bpdf, wpdf);
             direct += mis * 1.0f * vmin(bw, vec3(kMaxColorClamp)) * vmin(Li, vec3(kMaxColorClamp));
           }
@@ -322,7 +326,7 @@ __global__ void __launch_bounds__(kTraceBlock) k_shade(PathPool P, uint32_t coun
                                                        WaveCounters* counters) {
   __shared__ uint32_t s_stack[kStackShared * kTraceBlock];
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  uint32_t shadow_rays = 0, tests = 0;
+  uint32_t shadow_rays = 0, tests = 0, nodes = 0;
   bool alive = false;  // continues into Q
   uint2 pf = i < count ? P.pixel_flags[i] : make_uint2(kEmpty, kFlagDead);
   const bool active = i < count && !(pf.y & kFlagDead);
@@ -412,7 +416,7 @@ __global__ void __launch_bounds__(kTraceBlock) k_shade(PathPool P, uint32_t coun
       init_shading_frame(B, hit_back, rd, sp.ng, sp.ns, sp.dpdu, sp.dpdv);
       init_layered_lobes(B, mat.default_mtl, rd, hit_back, ray_ior(rt), ex_ior(rt, inst_idx));
       if (rs.enable_shape_light)
-        rad += indirect_clamp(rs, tp * eval_shape_light(S, st, B, rd, sp.p, sp.p_err, sp.ng, hs, &shadow_rays, &tests),
+        rad += indirect_clamp(rs, tp * eval_shape_light(S, st, B, rd, sp.p, sp.p_err, sp.ng, hs, &shadow_rays, &tests, &nodes),
                               depth);
       const vec3 wo = B.to_local(-rd);
       vec3 w, wi;
@@ -469,14 +473,16 @@ __global__ void __launch_bounds__(kTraceBlock) k_shade(PathPool P, uint32_t coun
       atomicOr(&counters->errors, (uint32_t)kDevErrQueue);
     }
   }
-  uint32_t s_sum = shadow_rays, t_sum = tests;
+  uint32_t s_sum = shadow_rays, t_sum = tests, n_sum = nodes;
   for (int off = 16; off > 0; off >>= 1) {
     s_sum += __shfl_down_sync(0xFFFFFFFFu, s_sum, off);
     t_sum += __shfl_down_sync(0xFFFFFFFFu, t_sum, off);
+    n_sum += __shfl_down_sync(0xFFFFFFFFu, n_sum, off);
   }
   if ((threadIdx.x & 31) == 0) {
     if (s_sum) atomicAdd(&counters->shadow_rays, (unsigned long long)s_sum);
     if (t_sum) atomicAdd(&counters->tri_tests, (unsigned long long)t_sum);
+    if (n_sum) atomicAdd(&counters->node_visits, (unsigned long long)n_sum);
   }
 }
 
@@ -510,9 +516,9 @@ __global__ void __launch_bounds__(kTraceBlock) k_debug_trace(int n, const float*
   const vec3 o(origin[3 * i], origin[3 * i + 1], origin[3 * i + 2]);
   const vec3 d = normalize(vec3(dir[3 * i], dir[3 * i + 1], dir[3 * i + 2]));
   ClosestHit ch;
-  uint32_t tests = 0;
+  uint32_t tests = 0, nodes = 0;
   const bool hit = trace_closest(c_scene, st, o, d, kTMax, last_hit ? last_hit[2 * i] : kEmpty,
-                                 last_hit ? last_hit[2 * i + 1] : kEmpty, false, &ch, &tests);
+                                 last_hit ? last_hit[2 * i + 1] : kEmpty, false, &ch, &tests, &nodes);
   inst[i] = hit ? ch.inst : kEmpty;
   tri[i] = hit ? ch.tri : kEmpty;
   t[i] = hit ? ch.t : kTMax;
@@ -535,8 +541,8 @@ __global__ void __launch_bounds__(kTraceBlock) k_debug_occluded(int n, const flo
   st.overflow = false;
   const vec3 o(origin[3 * i], origin[3 * i + 1], origin[3 * i + 2]);
   const vec3 d = normalize(vec3(dir[3 * i], dir[3 * i + 1], dir[3 * i + 2]));
-  uint32_t tests = 0;
-  occluded[i] = trace_occluded(c_scene, st, o, d, tmax[i], &tests) ? 1 : 0;
+  uint32_t tests = 0, nodes = 0;
+  occluded[i] = trace_occluded(c_scene, st, o, d, tmax[i], &tests, &nodes) ? 1 : 0;
   if (st.overflow) atomicOr(errors, (uint32_t)kDevErrStack);
 }
 

@@ -47,6 +47,7 @@ struct WaveCounters {
   unsigned long long extension_rays;
   unsigned long long shadow_rays;
   unsigned long long tri_tests;
+  unsigned long long node_visits;
 };
 
 cudaError_t upload_constants(const DeviceScene& scene, const uint32_t* primes, const uint32_t* prime_sums,
