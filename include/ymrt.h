@@ -141,6 +141,24 @@ int ymrt_render_forward(ymrt_scene* scene, const ymrt_render_setting* setting, i
 /* Same, restricted to tiles [tile_begin, tile_end) of the 16x16 tiling. */
 int ymrt_render_tiles(ymrt_scene* scene, const ymrt_render_setting* setting, int frame_index, int tile_begin,
                       int tile_end, float* out_rgba, int out_on_device, ymrt_stats* stats);
+/* Allocation-free variant of ymrt_render_tiles, for callers that cannot
+ * allocate device memory while rendering (a host with a fixed up-front
+ * memory budget or its own pool allocator, or code that must not let a
+ * cudaMalloc synchronise the device mid-frame). It has no counterpart in the
+ * reference. The path queues, hit records and counters live in one fixed
+ * 32 MiB array that every device holds while the library is loaded; the
+ * caller passes the scene and a device output image (width*height float4).
+ * Limits: 256 * spp paths (one tile) must fit in the array, i.e.
+ * spp <= ymrt_noalloc_max_paths() / 256; larger spp is rejected with
+ * YMRT_ERR_INVALID. The first call on a device looks up the array's device
+ * address (cudaGetSymbolAddress), so make that first call before any stream
+ * capture. All calls share the array: calls that overlap on the GPU race and
+ * must be serialised by the caller. */
+int ymrt_render_tiles_noalloc(ymrt_scene* scene, const ymrt_render_setting* setting, int frame_index, int tile_begin,
+                              int tile_end, float* out_rgba_device, ymrt_stats* stats);
+/* Path slots available to ymrt_render_tiles_noalloc. */
+uint32_t ymrt_noalloc_max_paths(void);
+
 /* Running mean over frames (device pointers): acc = (acc*(f-1) + noise) / f. */
 int ymrt_accumulate(ymrt_scene* scene, const float* noise_rgba, float* acc_rgba, int frame_index);
 

@@ -7,6 +7,7 @@
 #include <cstring>
 #include <functional>
 #include <memory>
+#include <mutex>
 #include <new>
 #include <string>
 #include <vector>
@@ -516,6 +517,184 @@ int ymrt_render_tiles(ymrt_scene* sc, const ymrt_render_setting* setting, int fr
 int ymrt_render_forward(ymrt_scene* sc, const ymrt_render_setting* setting, int frame_index, float* out_rgba,
                         int out_on_device, ymrt_stats* stats) {
   return ymrt_render_tiles(sc, setting, frame_index, 0, 0, out_rgba, out_on_device, stats);
+}
+
+}  // extern "C"
+
+// ------------------------------------------------- allocation-free render ---
+//
+// Some callers cannot allocate device memory while they render: a host that
+// hands the renderer a fixed memory budget up front (an embedding application
+// with its own pool allocator, or a process that must not grow its footprint
+// once its frame loop runs), or code that runs where a cudaMalloc would
+// synchronise the device and stall other work. ymrt_render_tiles_noalloc
+// serves them: instead of the context's path queues (allocated on first use)
+// it places the path queues, the hit records and the wave counters in the
+// fixed array below, which exists once per device for as long as the library
+// is loaded.
+//
+// Limits: the array holds kNoAllocScratchBytes; one wave holds as many
+// 16x16-pixel tiles of samples as fit (at least one tile of 256 * spp
+// paths must fit, so spp is bounded by the array size). All calls share the
+// array: calls that overlap on the GPU (from several host threads, or on
+// several contexts of one device) race on it and must be serialised by the
+// caller. The wave counters are cleared at the start of every call; the
+// queues need no clearing (every slot is written before it is read).
+
+namespace {
+
+constexpr size_t kNoAllocScratchBytes = size_t(32) << 20;  // 32 MiB per device
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+// Device address of g_noalloc_scratch per device ordinal, looked up once per
+// device (with that device current) and kept for the life of the process.
+std::mutex g_noalloc_mutex;
+void* g_noalloc_addr[128] = {};
+
+constexpr size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+
+// Bytes one path slot needs across both path pools and the hit pool.
+constexpr size_t kPoolSlotBytes = 4 * sizeof(float4) + sizeof(uint4) + 2 * sizeof(uint2) + sizeof(RayTransfer) + 1;
+constexpr size_t kHitSlotBytes = sizeof(float4) + sizeof(uint4) + kMaxNearby * sizeof(uint4);
+
+uint32_t noalloc_capacity() {
+  const size_t fixed = align256(sizeof(WaveCounters)) + 16 * 256;  // counters + alignment slack of the carved arrays
+  return (uint32_t)((kNoAllocScratchBytes - fixed) / (2 * kPoolSlotBytes + kHitSlotBytes));
+}
+
+// Carves the two path pools, the hit pool and the counters out of `base`;
+// returns the number of bytes used.
+size_t carve(unsigned char* base, uint32_t n, PathPool pools[2], HitPool* hits, WaveCounters** counters) {
+  size_t off = 0;
+  auto take = [&](size_t bytes) {
+    unsigned char* p = base + off;
+    off = align256(off + bytes);
+    return p;
+  };
+  *counters = reinterpret_cast<WaveCounters*>(take(sizeof(WaveCounters)));
+  for (int k = 0; k < 2; ++k) {
+    PathPool& P = pools[k];
+    P.ray_o = reinterpret_cast<float4*>(take(n * sizeof(float4)));
+    P.ray_d = reinterpret_cast<float4*>(P.ray_o + n);
+    P.throughput = P.ray_d + n;
+    P.radiance = P.throughput + n;
+    P.sampler = reinterpret_cast<uint4*>(P.radiance + n);
+    off = align256((reinterpret_cast<unsigned char*>(P.sampler + n)) - base);
+    P.pixel_flags = reinterpret_cast<uint2*>(take(n * sizeof(uint2)));
+    P.last_hit = reinterpret_cast<uint2*>(take(n * sizeof(uint2)));
+    P.transfer = reinterpret_cast<RayTransfer*>(take(n * sizeof(RayTransfer)));
+    P.transfer_count = reinterpret_cast<uint8_t*>(take(n));
+    P.capacity = n;
+  }
+  hits->bary_t = reinterpret_cast<float4*>(take(n * sizeof(float4)));
+  hits->ids = reinterpret_cast<uint4*>(take(n * sizeof(uint4)));
+  hits->nearby = reinterpret_cast<uint4*>(take(n * kMaxNearby * sizeof(uint4)));
+  return off;
+}
+
+}  // namespace
+
+extern "C" {
+
+uint32_t ymrt_noalloc_max_paths(void) { return noalloc_capacity(); }
+
+int ymrt_render_tiles_noalloc(ymrt_scene* sc, const ymrt_render_setting* setting, int frame_index, int tile_begin,
+                              int tile_end, float* out_rgba_device, ymrt_stats* stats) {
+  if (!sc || !setting || !out_rgba_device) return YMRT_ERR_INVALID;
+  ymrt_context* ctx = sc->ctx;
+  RenderSetting rs;
+  std::memcpy(&rs, setting, sizeof(rs));
+  if (frame_index < 1) return ctx->fail(YMRT_ERR_INVALID, "frame_index starts at 1");
+  if (rs.sampler_type != 1) return ctx->fail(YMRT_ERR_UNSUPPORTED, "only the Halton sampler (sampler_type 1) is supported");
+  if (rs.enable_distant_light) return ctx->fail(YMRT_ERR_UNSUPPORTED, "distant lights are not supported yet");
+  if (rs.enable_volume_scattering) return ctx->fail(YMRT_ERR_UNSUPPORTED, "volume scattering is not supported yet");
+  const uint32_t spp = (uint32_t)std::max(rs.ssp, 1);
+  const uint32_t per_tile = (uint32_t)kTilePixels * spp;
+  const uint32_t cap = noalloc_capacity();
+  if (per_tile > cap)
+    return ctx->fail(YMRT_ERR_INVALID, "ymrt_render_tiles_noalloc: one 16x16 tile at " + std::to_string(spp) +
+                                           " spp needs " + std::to_string(per_tile) + " path slots; the fixed " +
+                                           std::to_string(kNoAllocScratchBytes >> 20) + " MiB scratch array holds " +
+                                           std::to_string(cap) + " (at most " + std::to_string(cap / kTilePixels) +
+                                           " spp)");
+  cudaError_t e = cudaSetDevice(ctx->device);
+  if (e != cudaSuccess) return ctx->cuda_fail(e, "cudaSetDevice");
+  if (ctx->device < 0 || ctx->device >= 128) return ctx->fail(YMRT_ERR_INVALID, "device ordinal out of range");
+  unsigned char* base = nullptr;
+  {
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_addr[ctx->device]) {
+      void* ptr = nullptr;
+      e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+      if (e != cudaSuccess || !ptr) return ctx->cuda_fail(e, "cudaGetSymbolAddress(scratch)");
+      g_noalloc_addr[ctx->device] = ptr;
+    }
+    base = static_cast<unsigned char*>(g_noalloc_addr[ctx->device]);
+  }
+  PathPool pools[2];
+  HitPool hits;
+  WaveCounters* dc = nullptr;
+  if (carve(base, cap, pools, &hits, &dc) > kNoAllocScratchBytes)
+    return ctx->fail(YMRT_ERR_OVERFLOW, "scratch layout exceeds the fixed array");
+
+  const uint32_t W = sc->width, Hh = sc->height;
+  const uint32_t tiles_x = (W + kTileRes - 1) / kTileRes, tiles_y = (Hh + kTileRes - 1) / kTileRes;
+  const uint32_t total_tiles = tiles_x * tiles_y;
+  const uint32_t t_end = tile_end <= 0 ? total_tiles : std::min<uint32_t>((uint32_t)tile_end, total_tiles);
+  uint32_t cursor = (uint32_t)std::max(tile_begin, 0);
+  cudaStream_t st = ctx->stream;
+  float4* image = reinterpret_cast<float4*>(out_rgba_device);
+  const size_t img_bytes = (size_t)W * Hh * sizeof(float4);
+  if ((e = upload_constants(sc->dev, ctx->primes.data(), ctx->prime_sums.data(), st)) != cudaSuccess)
+    return ctx->cuda_fail(e, "uploading constants");
+  if ((e = upload_setting(rs, st)) != cudaSuccess) return ctx->cuda_fail(e, "uploading render setting");
+  cudaMemsetAsync(dc, 0, sizeof(WaveCounters), st);
+  cudaMemsetAsync(image, 0, img_bytes, st);
+  cudaEventRecord(ctx->ev_start, st);
+  uint32_t live = 0;
+  int a = 0;
+  uint64_t waves = 0, paths = 0, launches = 0;
+  while (live > 0 || cursor < t_end) {
+    const uint32_t n_tiles = std::min<uint32_t>((cap - live) / per_tile, t_end - cursor);
+    const uint32_t gen = n_tiles * per_tile;
+    const uint32_t total = live + gen;
+    launch_generate(pools[a], live, gen, cursor, tiles_x, frame_index, spp, st);
+    launch_extend(pools[a], total, hits, image, dc, st);
+    cudaMemsetAsync(&dc->next_count, 0, sizeof(uint32_t), st);
+    launch_shade(pools[a], total, hits, pools[a ^ 1], image, dc, st);
+    launches += (gen > 0 ? 1 : 0) + (total > 0 ? 2 : 0);
+    if ((e = cudaMemcpyAsync(ctx->counters_host, dc, sizeof(WaveCounters), cudaMemcpyDeviceToHost, st)) != cudaSuccess)
+      return ctx->cuda_fail(e, "reading wave counters");
+    if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return ctx->cuda_fail(e, "wave");
+    live = ctx->counters_host->next_count;
+    if (live > cap) return ctx->fail(YMRT_ERR_OVERFLOW, "path queue overflow");
+    a ^= 1;
+    cursor += n_tiles;
+    paths += gen;
+    ++waves;
+  }
+  cudaEventRecord(ctx->ev_stop, st);
+  if ((e = cudaMemcpyAsync(ctx->counters_host, dc, sizeof(WaveCounters), cudaMemcpyDeviceToHost, st)) != cudaSuccess)
+    return ctx->cuda_fail(e, "reading counters");
+  if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return ctx->cuda_fail(e, "frame");
+  float ms = 0.0f;
+  cudaEventElapsedTime(&ms, ctx->ev_start, ctx->ev_stop);
+  if (stats) {
+    std::memset(stats, 0, sizeof(*stats));
+    stats->paths = paths;
+    stats->extension_rays = ctx->counters_host->extension_rays;
+    stats->shadow_rays = ctx->counters_host->shadow_rays;
+    stats->waves = waves;
+    stats->node_visits = ctx->counters_host->node_visits;
+    stats->triangle_tests = ctx->counters_host->tri_tests;
+    stats->kernel_launches = launches;
+    stats->ms_total = ms;
+    stats->device_errors = ctx->counters_host->errors;
+  }
+  if (ctx->counters_host->errors & kDevErrQueue) return ctx->fail(YMRT_ERR_OVERFLOW, "path queue overflow on the device");
+  if (ctx->counters_host->errors & kDevErrStack)
+    return ctx->fail(YMRT_ERR_OVERFLOW, "traversal or nested-media stack overflow on the device");
+  return YMRT_OK;
 }
 
 int ymrt_accumulate(ymrt_scene* sc, const float* noise, float* acc, int frame_index) {
