@@ -121,6 +121,10 @@ void ymrt_host_scene_free(ymrt_host_scene* scene);
 #define YMRT_QUERY_TRANSFORMS 4  /* float[32*n]: object-to-world then world-to-object, column major */
 #define YMRT_QUERY_CAMERA 5      /* float[14]: position, u, v, w, aspect, tan(fov/2) */
 #define YMRT_QUERY_TRIANGLES 6   /* uint32[3*n] corner triples of mesh `index`, reference order */
+#define YMRT_QUERY_MATERIALS 7   /* uint32[39*n]: the reference's Material struct words */
+#define YMRT_QUERY_VOLUMES 8     /* uint32[9*n]: the reference's Volume struct words */
+#define YMRT_QUERY_DISTANT_LIGHTS 9 /* uint32[8*n]: the reference's DistantLight struct words */
+#define YMRT_QUERY_TEXTURES 10   /* uint32[13*n]: type, black/white inputs, value, rgb, frequency, lacunarity, gain, layers, amplitude, offset */
 long long ymrt_host_scene_query(const ymrt_host_scene* scene, int what, int index, void* out, size_t cap);
 
 /* Uploads a prepared scene. halton_perm: the concatenated digit permutations

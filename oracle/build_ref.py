@@ -178,6 +178,136 @@ def shading_source(arg_order: str) -> str:
     return dst
 
 
+# ---------------------------------------------------------------------------
+# The reference's own kernels built for the device (sm_100a), as a baseline.
+
+GPU_LIB = os.path.join(OUT, "libymrt_refgpu.so")
+# Same kernels compiled without FMA contraction and with IEEE division and
+# square root (the flags ymrt_b200 is built with), for per-sample comparison.
+GPU_LIB_EXACT = os.path.join(OUT, "libymrt_refgpu_exact.so")
+EXACT_FLAGS = ["-fmad=false", "-prec-div=true", "-prec-sqrt=true", "-ftz=false"]
+
+_GPU_FIX = r'''
+// ---- inserted by oracle/build_ref.py: direct priority read ----
+// RayTransfer::GetMaxPriorityRecord (src/Ray.h:148-151) returns a reference
+// bound to a temporary copy of the selected record; the priority it yields is
+// read here directly instead of through that reference.
+__host__ __device__ inline uint32_t ymrt_oracle_max_priority(const YMRT::RayTransfer& rt) {
+  return rt.max_priority_record_index != -1 ? rt.boundary_records[rt.max_priority_record_index].ior_priority
+                                            : YMRT::BoundaryRecord().ior_priority;
+}
+// ---- end of insertion ----
+'''
+
+
+def shading_source_gpu() -> str:
+    """Build-time copy of src/Shading.cu for the device build: only the
+    GetMaxPriorityRecord reads are rewritten; argument order and everything
+    else stay as the reference wrote them."""
+    src = os.path.join(REF, "src", "Shading.cu")
+    with open(src, "r", encoding="utf-8", errors="replace") as f:
+        text = f.read()
+    first_ns = text.index("namespace YMRT")
+    head, body = text[:first_ns], text[first_ns:]
+    body, n_prio = re.subn(r"\b(\w+)\.GetMaxPriorityRecord\(\)\.ior_priority", r"ymrt_oracle_max_priority(\1)", body)
+    # nvcc does not macro-expand the argument of "#pragma unroll" (MSVC's
+    # conforming preprocessor does): write the values, MAX_BOUNDARY_RECORD = 6.
+    body, n_unroll = re.subn(r"#pragma unroll \(MAX_BOUNDARY_RECORD \+ 2\)", "#pragma unroll 8", body)
+    body, n_unroll6 = re.subn(r"#pragma unroll MAX_BOUNDARY_RECORD\b", "#pragma unroll 6", body)
+    n_unroll += n_unroll6
+    line_of_body = head.count("\n") + 1
+    gen_dir = os.path.join(OUT, "gen")
+    os.makedirs(gen_dir, exist_ok=True)
+    dst = os.path.join(gen_dir, "Shading_gpu.cu")
+    with open(dst, "w") as f:
+        f.write(f'#line 1 "{src}"\n' + head + _GPU_FIX + f'#line {line_of_body} "{src}"\n' + body)
+    with open(os.path.join(gen_dir, "Shading_gpu.cu.sites"), "w") as f:
+        f.write(f"{n_prio} GetMaxPriorityRecord reads made direct, {n_unroll} unroll counts written as literals\n")
+    return dst
+
+
+NVCC_GPU_FLAGS = [
+    "-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-std=c++17", "-DNDEBUG", "-DGLM_FORCE_PURE",
+    "--expt-relaxed-constexpr", "-Xcompiler", "-fPIC", "-w", "-lineinfo",
+]
+
+
+def _gpu_includes():
+    inc = _includes()
+    inc[1] = os.path.join(HERE, "shims", "ymrt_ref_gpu_prelude.h")  # replace the host prelude
+    return inc
+
+
+def _gpu_stamp(exact: bool) -> str:
+    h = hashlib.sha256()
+    h.update(" ".join(CXXFLAGS + NVCC_GPU_FLAGS + (EXACT_FLAGS if exact else [])).encode())
+    for rel in HOST_SOURCES + ["src/Shading.cu"]:
+        h.update(str(os.path.getmtime(os.path.join(REF, rel))).encode())
+    for rel in ["ref_gpu_harness.cu", "ref_prepare.h", "ref_stubs.cpp", "build_ref.py", "shims/ymrt_ref_gpu_prelude.h",
+                "shims/ppl.h"]:
+        with open(os.path.join(HERE, rel), "rb") as f:
+            h.update(f.read())
+    return h.hexdigest()
+
+
+def build_gpu(force: bool = False, jobs: int = 8, exact: bool = False) -> str:
+    """Builds oracle/_ref/libymrt_refgpu.so: the reference's stage kernels for
+    sm_100a (nvcc's default floating-point flags, as the reference's CMake
+    build uses) plus its host-side scene module, driven by ref_gpu_harness.cu.
+    exact=True builds libymrt_refgpu_exact.so with EXACT_FLAGS instead."""
+    lib = GPU_LIB_EXACT if exact else GPU_LIB
+    if not os.path.isdir(os.path.join(REF, "src")):
+        if os.path.exists(lib):
+            return lib
+        raise FileNotFoundError(f"reference sources not found at {REF} and no prebuilt {lib}")
+    os.makedirs(OUT, exist_ok=True)
+    stamp_file = os.path.join(OUT, "stamp_gpu_exact" if exact else "stamp_gpu")
+    stamp = _gpu_stamp(exact)
+    if not force and os.path.exists(lib) and os.path.exists(stamp_file):
+        with open(stamp_file) as f:
+            if f.read().strip() == stamp:
+                return lib
+    obj_dir = os.path.join(OUT, "obj_gpu_exact" if exact else "obj_gpu")
+    os.makedirs(obj_dir, exist_ok=True)
+    shading = shading_source_gpu()
+    cmds, objs = [], []
+    for rel in HOST_SOURCES:
+        obj = os.path.join(obj_dir, os.path.basename(rel) + ".o")
+        cmds.append(["g++"] + CXXFLAGS + _gpu_includes() + ["-c", os.path.join(REF, rel), "-o", obj])
+        objs.append(obj)
+    obj = os.path.join(obj_dir, "ref_stubs.o")
+    cmds.append(["g++"] + CXXFLAGS + ["-DYMRT_ORACLE_REAL_CUDA"] + _gpu_includes() +
+                ["-c", os.path.join(HERE, "ref_stubs.cpp"), "-o", obj])
+    objs.append(obj)
+    obj = os.path.join(obj_dir, "ref_gpu_harness.o")
+    cmds.append(["nvcc"] + NVCC_GPU_FLAGS + (EXACT_FLAGS if exact else []) +
+                [f'-DYMRT_SHADING_SOURCE="{shading}"'] + _gpu_includes() +
+                ["-c", os.path.join(HERE, "ref_gpu_harness.cu"), "-o", obj])
+    objs.append(obj)
+    procs = []
+    for cmd in cmds:
+        procs.append((cmd[-3], subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT)))
+        while len([p for _, p in procs if p.poll() is None]) >= jobs:
+            procs[0][1].wait()
+    for src, p in procs:
+        out, _ = p.communicate()
+        if p.returncode != 0:
+            raise RuntimeError(f"device oracle build failed for {src}:\n{out.decode(errors='replace')[-4000:]}")
+    vs = os.path.join(obj_dir, "exports.map")
+    with open(vs, "w") as f:
+        f.write("{ global: ymrefgpu_*; local: *; };\n")
+    tmp = lib + ".tmp"
+    cmd = ["nvcc", "-shared", "-cudart", "static", "-gencode", "arch=compute_100a,code=sm_100a", "-o", tmp] + objs + [
+        "-Xlinker", "-Bsymbolic", "-Xlinker", "--version-script=" + vs, "-Xlinker", "--no-undefined", "-lpthread"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("device oracle link failed:\n" + r.stdout[-4000:] + r.stderr[-4000:])
+    os.replace(tmp, lib)
+    with open(stamp_file, "w") as f:
+        f.write(stamp)
+    return lib
+
+
 def _stamp(arg_order: str) -> str:
     h = hashlib.sha256()
     h.update(arg_order.encode())
@@ -185,7 +315,8 @@ def _stamp(arg_order: str) -> str:
     for rel in HOST_SOURCES + ["src/Shading.cu"]:
         p = os.path.join(REF, rel)
         h.update(str(os.path.getmtime(p)).encode())
-    for rel in ["ref_harness.cpp", "ref_stubs.cpp", "build_ref.py", "shims/ymrt_ref_prelude.h", "shims/ppl.h"]:
+    for rel in ["ref_harness.cpp", "ref_prepare.h", "ref_stubs.cpp", "build_ref.py", "shims/ymrt_ref_prelude.h",
+                "shims/ppl.h"]:
         with open(os.path.join(HERE, rel), "rb") as f:
             h.update(f.read())
     return h.hexdigest()
@@ -237,8 +368,12 @@ def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--arg-order", choices=["ltr", "native"], default="ltr")
     ap.add_argument("--force", action="store_true")
+    ap.add_argument("--gpu", action="store_true", help="also build the reference's kernels for sm_100a")
     a = ap.parse_args(argv)
     print(build(a.arg_order, a.force))
+    if a.gpu:
+        print(build_gpu(a.force))
+        print(build_gpu(a.force, exact=True))
 
 
 if __name__ == "__main__":

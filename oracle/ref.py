@@ -52,6 +52,7 @@ def lib():
         L.ymref_geometry_triangles.argtypes = [vp, ctypes.c_uint32, vp]
         L.ymref_lights.argtypes = [vp, vp, vp, vp]
         L.ymref_camera_bytes.argtypes = [vp, vp, i]
+        L.ymref_scene_records.argtypes = [vp, i, vp, i]
         L.ymref_trace.argtypes = [vp, i, vp, vp, vp, vp, vp, vp, vp, vp, vp]
         L.ymref_occluded.argtypes = [vp, i, vp, vp, vp, vp]
         L.ymref_halton.argtypes = [vp, i, vp, vp, vp, i, vp, vp, vp]
@@ -135,6 +136,17 @@ class RefScene:
         n = lib().ymref_camera_bytes(self.h, _p(buf), buf.size)
         return buf[:n].tobytes()
 
+    def records(self, kind: str) -> np.ndarray:
+        """Materials, volumes, distant lights (raw 32-bit words of the
+        reference structs) or textures (13 words each), one row per record."""
+        what = {"materials": 0, "volumes": 1, "distant_lights": 2, "textures": 3}[kind]
+        width = {"materials": 39, "volumes": 9, "distant_lights": 8, "textures": 13}[kind]
+        n = lib().ymref_scene_records(self.h, what, None, 0)
+        out = np.zeros(max(n, 0), np.uint32)
+        if n > 0:
+            lib().ymref_scene_records(self.h, what, _p(out), out.size)
+        return out.reshape(-1, width)
+
     def trace(self, origins, dirs, last_hit=None) -> dict:
         o = np.ascontiguousarray(origins, np.float32)
         d = np.ascontiguousarray(dirs, np.float32)
@@ -188,3 +200,86 @@ def query_counts(reset: bool = True) -> tuple[int, int]:
     out = np.zeros(2, np.uint64)
     lib().ymref_query_counts(_p(out), int(reset))
     return int(out[0]), int(out[1])
+
+
+# ---------------------------------------------------------------------------
+# The reference's own wavefront kernels rebuilt for the device (sm_100a),
+# driven by oracle/ref_gpu_harness.cu. Two builds: nvcc's default
+# floating-point flags (the reference's own build; the timing baseline) and
+# "exact" (no FMA contraction, IEEE division/square root -- the flags
+# ymrt_b200 uses), for per-sample comparison.
+
+GPU_LIB_PATHS = {False: os.path.join(HERE, "_ref", "libymrt_refgpu.so"),
+                 True: os.path.join(HERE, "_ref", "libymrt_refgpu_exact.so")}
+_gpu_libs = {}
+
+
+def gpu_available(exact: bool = False) -> bool:
+    return os.path.exists(GPU_LIB_PATHS[exact])
+
+
+def gpu_lib(exact: bool = False):
+    if exact not in _gpu_libs:
+        path = GPU_LIB_PATHS[exact]
+        if not os.path.exists(path):
+            from . import build_ref
+            build_ref.build_gpu(exact=exact)
+        L = ctypes.CDLL(path)
+        vp, i = ctypes.c_void_p, ctypes.c_int
+        L.ymrefgpu_scene_load.restype = vp
+        L.ymrefgpu_scene_load.argtypes = [ctypes.c_char_p, vp, ctypes.c_size_t, i, i, i]
+        L.ymrefgpu_scene_free.argtypes = [vp]
+        L.ymrefgpu_set_settings.argtypes = [vp, ctypes.POINTER(Settings)]
+        L.ymrefgpu_render_frame.argtypes = [vp, i, i, i, vp]
+        L.ymrefgpu_last_error.restype = ctypes.c_char_p
+        L.ymrefgpu_last_error.argtypes = [vp]
+        for name in ("ymrefgpu_last_render_ms", "ymrefgpu_last_wall_ms"):
+            getattr(L, name).restype = ctypes.c_double
+            getattr(L, name).argtypes = [vp]
+        _gpu_libs[exact] = L
+    return _gpu_libs[exact]
+
+
+class RefGpuScene:
+    """A scene rendered by the reference's own CUDA kernels on `device`."""
+
+    def __init__(self, path: str, halton_perm: np.ndarray, width: int, height: int, device: int = 0,
+                 exact: bool = False):
+        self.L = gpu_lib(exact)
+        perm = np.ascontiguousarray(halton_perm, dtype=np.uint32)
+        self.width, self.height = width, height
+        self.h = self.L.ymrefgpu_scene_load(path.encode(), _p(perm), perm.size, width, height, device)
+        if not self.h:
+            raise RuntimeError(f"reference (device build) failed to load {path}")
+
+    def set_settings(self, spp=1, ray_depth=8, sampler_type=1, shape_light=1, distant_light=0, volume=0,
+                     env_light=0, russian_roulette=0, indirect_clamp=0, indirect_limit=10.0):
+        s = Settings(spp, ray_depth, sampler_type, shape_light, distant_light, volume, env_light,
+                     russian_roulette, indirect_clamp, indirect_limit)
+        if self.L.ymrefgpu_set_settings(self.h, ctypes.byref(s)) != 0:
+            raise RuntimeError("ymrefgpu_set_settings failed")
+
+    def render_frame(self, frame_index: int, tile_begin: int = 0, tile_end: int = 0, copy_out: bool = True):
+        out = np.zeros((self.height, self.width, 4), np.float32) if copy_out else None
+        rc = self.L.ymrefgpu_render_frame(self.h, frame_index, tile_begin, tile_end,
+                                          _p(out) if copy_out else None)
+        if rc != 0:
+            raise RuntimeError("reference device render failed: " + self.L.ymrefgpu_last_error(self.h).decode())
+        return out
+
+    def last_render_ms(self) -> float:
+        return self.L.ymrefgpu_last_render_ms(self.h)
+
+    def last_wall_ms(self) -> float:
+        return self.L.ymrefgpu_last_wall_ms(self.h)
+
+    def close(self):
+        if self.h:
+            self.L.ymrefgpu_scene_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

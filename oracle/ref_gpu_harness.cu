@@ -1,0 +1,288 @@
+// Headless device driver for the YMRT reference's own wavefront kernels,
+// rebuilt for sm_100a (the "reference CUDA" baseline).
+//
+// TEST AND BASELINE INFRASTRUCTURE ONLY. Built by oracle/build_ref.py
+// (build_gpu) into oracle/_ref/libymrt_refgpu.so from the reference sources
+// where they lie; only tests/ and bench.py load it, to time the reference's
+// kernels beside ymrt_b200's and to compare their outputs. The ymrt_b200
+// product never links or calls it.
+//
+// What it does, in the reference's own terms:
+//  * loads a .ymtmp scene with the reference's parser and scene module
+//    (src/core/YMParser.cpp:2330), which uploads each mesh to the device as it
+//    is created (src/GeometryDefines.h:171-174 TriangleMesh::Upload);
+//  * prepares it as GuiModule::UpdateScene does (shared with the host oracle,
+//    oracle/ref_prepare.h) and copies every scene array to the device the way
+//    UpdateScene's device block does (src/core/GuiModule.cpp:173-272);
+//  * allocates the wave queues with the reference's own AllocateRayCounter /
+//    AllocateShadingRayData / AllocateHitData / AllocateShadowRayData
+//    (src/Shading.cu:1067-1163, MAX_RAY_COUNT = 1 Mi rays);
+//  * renders a frame with the wave loop of RenderModule::PathTracingExecuteTask
+//    (src/core/RenderModule.cpp:494-653), calling the reference's stage
+//    launchers RayGenerationPathTracing, RayTracePathTracing and
+//    RayShadingPathTracing (src/Shading.cu:1727, 1903, 2304) on one stream,
+//    with the same host synchronisation after each stage.
+//
+// The kernels are the reference's, compiled from a build-time copy of
+// src/Shading.cu with one read rewritten (RayTransfer::GetMaxPriorityRecord
+// returns a reference to a temporary; the copy reads the priority directly).
+// Device time is taken with CUDA events around the wave loop.
+#include YMRT_SHADING_SOURCE
+
+#include "core/SceneModule.h"
+#include "core/YMParser.h"
+
+#include "ref_prepare.h"
+
+#include <chrono>
+#include <cstring>
+#include <string>
+
+using namespace YMRT;
+
+namespace {
+
+struct GpuContext {
+  std::shared_ptr<SceneModule> module;
+  std::vector<uint32_t> instance_old_index;
+  Scene device_scene{};  // host copy of the Scene struct, its arrays on the device
+  std::vector<void*> owned;
+  RenderSetting setting{};
+  int width = 0, height = 0;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  RayCounterData counters{};
+  ShadingRayData shading{};
+  HitData hits{};
+  ShadowRayData shadow{};
+  glm::vec4* image = nullptr;
+  double last_ms = 0.0, last_wall_ms = 0.0;
+  std::string error;
+};
+
+template <typename T>
+bool upload(GpuContext* c, T** dst, const T* src, size_t count) {
+  *dst = nullptr;
+  if (count == 0) return true;
+  void* p = nullptr;
+  if (cudaMalloc(&p, sizeof(T) * count) != cudaSuccess) return false;
+  c->owned.push_back(p);
+  if (cudaMemcpy(p, src, sizeof(T) * count, cudaMemcpyHostToDevice) != cudaSuccess) return false;
+  *dst = static_cast<T*>(p);
+  return true;
+}
+
+}  // namespace
+
+extern "C" {
+
+// Same settings block as the host oracle's (oracle/ref_harness.cpp).
+struct YmrefGpuSettings {
+  int spp;
+  int ray_depth;
+  int sampler_type;
+  int enable_shape_light;
+  int enable_distant_light;
+  int enable_volume_scattering;
+  int enable_env_light;
+  int enable_russian_roulette;
+  int enable_indirect_clamp;
+  float indirect_limit;
+};
+
+const char* ymrefgpu_last_error(void* handle) { return static_cast<GpuContext*>(handle)->error.c_str(); }
+
+void* ymrefgpu_scene_load(const char* path, const uint32_t* halton_perm, size_t perm_len, int width, int height,
+                          int device) {
+  size_t table = 0;
+  for (uint32_t i = 0; i < prime_count; ++i) table += primes[i];
+  if (perm_len != table || width <= 0 || height <= 0) return nullptr;
+  if (cudaSetDevice(device) != cudaSuccess) return nullptr;
+  auto c = new GpuContext();
+  c->device = device;
+  c->width = width;
+  c->height = height;
+  try {
+    c->module = std::make_shared<SceneModule>();
+    SceneParser parser;
+    if (!parser.parsing_scene(path, c->module)) {
+      delete c;
+      return nullptr;
+    }
+    SceneModule& m = *c->module;
+    GuiModule::PrepareScene(m, halton_perm, perm_len, width, height, &c->instance_old_index);
+    Scene host = GuiModule::HostScene(m);
+    Scene& d = c->device_scene;
+    ImageTileCache empty_cache;
+    std::memset(&empty_cache, 0, sizeof(empty_cache));
+    bool ok = upload(c, &d.camera, host.camera, CAMERA_COUNT) &&
+              upload(c, &d.geometries, host.geometries, host.geometry_count) &&
+              upload(c, &d.primitive_instances, host.primitive_instances, host.primitive_instance_count) &&
+              upload(c, &d.top_nodes, host.top_nodes, host.top_node_count) &&
+              upload(c, &d.transforms, host.transforms, host.transform_count) &&
+              upload(c, &d.i_transforms, host.i_transforms, host.transform_count) &&
+              upload(c, &d.materials, host.materials, host.material_count) &&
+              upload(c, &d.distant_lights, host.distant_lights, host.distant_light_count) &&
+              upload(c, &d.shape_lights, host.shape_lights, host.shape_light_count) &&
+              upload(c, &d.shape_light_sample_table, host.shape_light_sample_table, host.shape_light_count) &&
+              upload(c, &d.volumes, host.volumes, host.volume_count) &&
+              upload(c, &d.textures, host.textures, host.texture_count) &&
+              upload(c, &d.image_tile_cache, &empty_cache, 1) &&
+              upload(c, &d.sampler_data.halton_permute_table, halton_perm, perm_len) &&
+              upload(c, &d.sampler_data.sobol_matrices, (const uint32_t*)sobol_matrices32, (size_t)4096 * 32) &&
+              upload(c, &d.render_setting, &c->setting, 1);
+    d.camera_count = CAMERA_COUNT;
+    d.geometry_count = host.geometry_count;
+    d.primitive_instance_count = host.primitive_instance_count;
+    d.top_node_count = host.top_node_count;
+    d.transform_count = host.transform_count;
+    d.material_count = host.material_count;
+    d.distant_light_count = host.distant_light_count;
+    d.shape_light_count = host.shape_light_count;
+    d.volume_count = host.volume_count;
+    d.texture_count = host.texture_count;
+    if (!ok) throw std::runtime_error("scene upload failed");
+    AllocateRayCounter(c->counters);
+    AllocateShadingRayData(c->shading);
+    AllocateHitData(c->hits);
+    AllocateShadowRayData(c->shadow);
+    CUDA_CHECK(cudaStreamCreate(&c->stream));
+    CUDA_CHECK(cudaEventCreate(&c->ev0));
+    CUDA_CHECK(cudaEventCreate(&c->ev1));
+    CUDA_CHECK(cudaMalloc(&c->image, sizeof(glm::vec4) * (size_t)width * height));
+  } catch (const std::exception& e) {
+    fprintf(stderr, "ymrefgpu_scene_load: %s\n", e.what());
+    delete c;
+    return nullptr;
+  }
+  return c;
+}
+
+void ymrefgpu_scene_free(void* handle) {
+  auto c = static_cast<GpuContext*>(handle);
+  if (!c) return;
+  cudaSetDevice(c->device);
+  cudaDeviceSynchronize();
+  try {
+    ReleaseRayCounter(c->counters);
+    ReleaseShadingRayData(c->shading);
+    ReleaseHitData(c->hits);
+    ReleaseShadowRayData(c->shadow);
+  } catch (...) {
+  }
+  for (void* p : c->owned) cudaFree(p);
+  if (c->image) cudaFree(c->image);
+  if (c->ev0) cudaEventDestroy(c->ev0);
+  if (c->ev1) cudaEventDestroy(c->ev1);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  c->module.reset();  // frees the meshes' device copies
+  delete c;
+}
+
+int ymrefgpu_set_settings(void* handle, const YmrefGpuSettings* s) {
+  auto c = static_cast<GpuContext*>(handle);
+  RenderSetting& r = c->setting;
+  r.ssp = s->spp;
+  r.ray_depth = s->ray_depth;
+  r.sampler_type = s->sampler_type;
+  r.enable_shape_light = s->enable_shape_light;
+  r.enable_distant_light = s->enable_distant_light != 0;
+  r.enable_volume_scattering = s->enable_volume_scattering != 0;
+  r.enable_env_light = s->enable_env_light != 0;
+  r.enable_russian_roulette = s->enable_russian_roulette != 0;
+  r.enable_indirect_clamp = s->enable_indirect_clamp != 0;
+  r.indirect_limit = s->indirect_limit;
+  cudaSetDevice(c->device);
+  return cudaMemcpy(c->device_scene.render_setting, &r, sizeof(RenderSetting), cudaMemcpyHostToDevice) == cudaSuccess
+             ? 0
+             : -1;
+}
+
+// Renders one frame (tiles [tile_begin, tile_end), 0/0 = all) into the
+// context's device image and copies it to out_rgba when that is not null.
+// Returns 0, or -1 on a CUDA error (message in ymrefgpu_last_error).
+int ymrefgpu_render_frame(void* handle, int frame_index, int tile_begin, int tile_end, float* out_rgba) {
+  auto c = static_cast<GpuContext*>(handle);
+  if (frame_index < 1 || tile_begin < 0) return -1;
+  try {
+    CUDA_CHECK(cudaSetDevice(c->device));
+    const RenderSetting& rs = c->setting;
+    const uint32_t w = c->width, h = c->height;
+    const uint32_t tiles_x = (w + TILE_X_RES - 1) / TILE_X_RES;
+    const uint32_t tiles_y = (h + TILE_Y_RES - 1) / TILE_Y_RES;
+    const uint32_t total = tiles_x * tiles_y;
+    const uint32_t t_end = tile_end <= 0 ? total : std::min<uint32_t>((uint32_t)tile_end, total);
+    const bool partial = tile_begin > 0 || t_end < total;
+    const uint32_t spp = (uint32_t)rs.ssp;
+    if (spp == 0 || spp * TILE_PIXEL_COUNT > MAX_RAY_COUNT) return -1;
+
+    CUDA_CHECK(cudaMemsetAsync(c->image, 0, sizeof(glm::vec4) * (size_t)w * h, c->stream));
+    Scene* scene_device = nullptr;
+    HaltonEnumerator* halton_device = nullptr;
+    CUDA_CHECK(cudaMalloc(&scene_device, sizeof(Scene)));
+    CUDA_CHECK(cudaMemcpyAsync(scene_device, &c->device_scene, sizeof(Scene), cudaMemcpyHostToDevice, c->stream));
+    HaltonEnumerator halton(w, h);
+    CUDA_CHECK(cudaMalloc(&halton_device, sizeof(HaltonEnumerator)));
+    CUDA_CHECK(cudaMemcpyAsync(halton_device, &halton, sizeof(HaltonEnumerator), cudaMemcpyHostToDevice, c->stream));
+    RayCounter* counter_host = c->counters.ray_counter_host;
+    RayCounter* counter_device = c->counters.ray_counter_device;
+    counter_host->hit_counter = 0;
+    counter_host->shading_ray_counter = 0;
+    counter_host->shadow_ray_counter = 0;
+    CUDA_CHECK(cudaMemcpyAsync(counter_device, counter_host, sizeof(RayCounter), cudaMemcpyHostToDevice, c->stream));
+    CUDA_CHECK(cudaStreamSynchronize(c->stream));
+
+    const auto wall0 = std::chrono::steady_clock::now();
+    CUDA_CHECK(cudaEventRecord(c->ev0, c->stream));
+    uint32_t next_tile = (uint32_t)tile_begin;
+    while (counter_host->shading_ray_counter > 0 || next_tile < t_end) {
+      uint32_t batch = (MAX_RAY_COUNT - counter_host->shading_ray_counter) / (TILE_PIXEL_COUNT * spp);
+      if (partial) batch = std::min(batch, t_end - next_tile);  // the full-frame loop is the reference's, uncapped
+      RayGenerationPathTracing(frame_index, rs, scene_device, halton_device, counter_device, next_tile, batch, w, h,
+                               tiles_x, tiles_y, c->shading, c->stream);
+      next_tile += batch;
+      counter_host->shading_ray_counter += batch * spp * TILE_PIXEL_COUNT;
+      CUDA_CHECK(cudaMemcpyAsync(counter_device, counter_host, sizeof(RayCounter), cudaMemcpyHostToDevice, c->stream));
+      CUDA_CHECK(cudaStreamSynchronize(c->stream));
+
+      RayTracePathTracing(frame_index, rs, scene_device, counter_device, counter_host, w, h, c->image, c->shading,
+                          c->hits, c->stream);
+      CUDA_CHECK(cudaMemcpyAsync(counter_host, counter_device, sizeof(RayCounter), cudaMemcpyDeviceToHost, c->stream));
+      CUDA_CHECK(cudaStreamSynchronize(c->stream));
+      counter_host->shading_ray_counter = 0;
+      CUDA_CHECK(cudaMemcpyAsync(counter_device, counter_host, sizeof(RayCounter), cudaMemcpyHostToDevice, c->stream));
+      CUDA_CHECK(cudaStreamSynchronize(c->stream));
+
+      RayShadingPathTracing(frame_index, rs, scene_device, counter_device, counter_host, w, h, c->image, c->shading,
+                            c->hits, c->shadow, c->stream);
+      CUDA_CHECK(cudaMemcpyAsync(counter_host, counter_device, sizeof(RayCounter), cudaMemcpyDeviceToHost, c->stream));
+      CUDA_CHECK(cudaStreamSynchronize(c->stream));
+      counter_host->hit_counter = 0;
+      CUDA_CHECK(cudaMemcpyAsync(counter_device, counter_host, sizeof(RayCounter), cudaMemcpyHostToDevice, c->stream));
+      CUDA_CHECK(cudaStreamSynchronize(c->stream));
+      if (counter_host->shading_ray_counter > MAX_RAY_COUNT) throw std::runtime_error("wave queue overflow");
+    }
+    CUDA_CHECK(cudaEventRecord(c->ev1, c->stream));
+    CUDA_CHECK(cudaEventSynchronize(c->ev1));
+    c->last_wall_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - wall0).count();
+    float ms = 0.0f;
+    CUDA_CHECK(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+    c->last_ms = ms;
+    CUDA_CHECK(cudaFree(scene_device));
+    CUDA_CHECK(cudaFree(halton_device));
+    if (out_rgba)
+      CUDA_CHECK(cudaMemcpy(out_rgba, c->image, sizeof(glm::vec4) * (size_t)w * h, cudaMemcpyDeviceToHost));
+  } catch (const std::exception& e) {
+    c->error = e.what();
+    return -1;
+  }
+  return 0;
+}
+
+// Device time (CUDA events on the render stream) and host wall time of the
+// last frame's wave loop, in milliseconds.
+double ymrefgpu_last_render_ms(void* handle) { return static_cast<GpuContext*>(handle)->last_ms; }
+double ymrefgpu_last_wall_ms(void* handle) { return static_cast<GpuContext*>(handle)->last_wall_ms; }
+
+}  // extern "C"

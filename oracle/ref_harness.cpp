@@ -35,49 +35,7 @@ thread_local uint3 blockIdx;
 thread_local dim3 blockDim;
 thread_local dim3 gridDim;
 
-namespace YMRT {
-
-// SceneModule names GuiModule as a friend (src/core/SceneModule.h:87). The
-// oracle is not linked with the GUI, so this class stands in for the part of
-// GuiModule::UpdateScene that prepares a freshly parsed scene for rendering.
-class GuiModule {
- public:
-  static bool PrepareScene(SceneModule& m, const uint32_t* halton_perm, size_t perm_len, int width,
-                           int height, std::vector<uint32_t>* instance_old_index) {
-    std::unordered_map<uint32_t, uint32_t> dst_indices_map;
-    TopBVHBuilder builder(m.primitive_instances.data(), (uint32_t)m.primitive_instances.size(),
-                          m.transforms.data(), m.geometries.data());
-    m.top_nodes.clear();
-    builder.BuildSceneBVH(m.top_nodes, nullptr, nullptr, &dst_indices_map);
-    for (auto& item : m.primitive_index_to_index_map) item.second = dst_indices_map[item.second];
-    instance_old_index->assign(m.primitive_instances.size(), EMPTY_UINT32);
-    for (auto& kv : dst_indices_map) (*instance_old_index)[kv.second] = kv.first;
-
-    m.shape_lights.clear();
-    m.shape_light_sample_table.clear();
-    m.LoadShapeLight();
-
-    m.permute_table.assign(halton_perm, halton_perm + perm_len);
-
-    m.camera[EDITOR_CAMERA_INDEX].InitCameraRayTransfer(m.GetHostSceneDataPointer());
-    std::memcpy(&m.camera[RENDERING_CAMERA_INDEX], &m.camera[EDITOR_CAMERA_INDEX], sizeof(Camera));
-    m.camera[RENDERING_CAMERA_INDEX].m_width = width;
-    m.camera[RENDERING_CAMERA_INDEX].m_height = height;
-    m.camera[RENDERING_CAMERA_INDEX].SetAspectRatio(float(width) / float(height));
-    return true;
-  }
-  static Scene HostScene(SceneModule& m) { return m.GetHostSceneDataPointer(); }
-  static std::vector<GeometryData>& Geometries(SceneModule& m) { return m.geometries; }
-  static std::vector<PrimitiveInstance>& Instances(SceneModule& m) { return m.primitive_instances; }
-  static std::vector<ShapeLight>& Lights(SceneModule& m) { return m.shape_lights; }
-  static std::vector<float>& LightTable(SceneModule& m) { return m.shape_light_sample_table; }
-  static std::vector<glm::mat4>& Transforms(SceneModule& m) { return m.transforms; }
-  static std::vector<glm::mat4>& InvTransforms(SceneModule& m) { return m.i_transforms; }
-  static std::vector<Material>& Materials(SceneModule& m) { return m.materials; }
-  static Camera* Cameras(SceneModule& m) { return m.camera; }
-};
-
-}  // namespace YMRT
+#include "ref_prepare.h"
 
 using namespace YMRT;
 
@@ -290,6 +248,47 @@ int ymref_transforms(void* handle, float* fwd, float* inv) {
   std::memcpy(fwd, t.data(), t.size() * sizeof(glm::mat4));
   std::memcpy(inv, it.data(), it.size() * sizeof(glm::mat4));
   return 0;
+}
+
+// Scene records as the reference's scene module holds them. what: 0 materials
+// (raw Material words), 1 volumes (raw Volume words), 2 distant lights (raw
+// DistantLight words), 3 textures (13 words: type, black/white inputs, constant
+// value, constant rgb, fBm frequency, lacunarity, gain, layer count, amplitude,
+// offset). Returns the number of 32-bit words (written when out has room).
+int ymref_scene_records(void* handle, int what, uint32_t* out, int cap) {
+  auto ctx = static_cast<RefContext*>(handle);
+  std::vector<uint32_t> w;
+  auto raw = [&](const void* p, size_t bytes) {
+    const size_t n = bytes / 4;
+    const size_t at = w.size();
+    w.resize(at + n);
+    std::memcpy(w.data() + at, p, n * 4);
+  };
+  auto f = [](float v) { uint32_t u; std::memcpy(&u, &v, 4); return u; };
+  switch (what) {
+    case 0: for (auto& m : GuiModule::Materials(*ctx->module)) raw(&m, sizeof(m)); break;
+    case 1: for (auto& v : GuiModule::Volumes(*ctx->module)) raw(&v, sizeof(v)); break;
+    case 2: for (auto& d : GuiModule::DistantLights(*ctx->module)) raw(&d, sizeof(d)); break;
+    case 3:
+      for (auto& t : GuiModule::Textures(*ctx->module)) {
+        uint32_t r[13] = {t.texture_type, EMPTY_UINT32, EMPTY_UINT32, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+        if (t.texture_type == CONSTANT_TEXTURE_FLOAT) {
+          r[3] = f(t.constant_texture_float.value);
+        } else if (t.texture_type == CONSTANT_TEXTURE_RGB) {
+          r[4] = f(t.constant_texture_rgb.color.x); r[5] = f(t.constant_texture_rgb.color.y); r[6] = f(t.constant_texture_rgb.color.z);
+        } else if (t.texture_type == SOLID_TEXTURE_FBM) {
+          const auto& n = t.noise_texture_fbm;
+          r[1] = n.indices[0]; r[2] = n.indices[1];
+          r[7] = f(n.frequency); r[8] = f(n.lacunarity); r[9] = f(n.gain); r[10] = (uint32_t)n.layer_count;
+          r[11] = f(n.amplitude); r[12] = f(n.offset);
+        }
+        w.insert(w.end(), r, r + 13);
+      }
+      break;
+    default: return -1;
+  }
+  if (out && cap >= (int)w.size()) std::memcpy(out, w.data(), w.size() * 4);
+  return (int)w.size();
 }
 
 // The rendering camera after preparation, as raw bytes of the reference's

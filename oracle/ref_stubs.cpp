@@ -9,6 +9,9 @@
 //   as host functions itself.
 // * assimp: model import is outside the hot path; the importer entry points
 //   the scene module references fail cleanly.
+// The device build of the reference (oracle/ref_gpu_harness.cu) compiles this
+// file with YMRT_ORACLE_REAL_CUDA defined: it keeps only the assimp stand-ins
+// and links the real CUDA runtime.
 #include <cstdlib>
 #include <cstring>
 #include <cuda_runtime_api.h>
@@ -17,6 +20,7 @@
 
 extern "C" {
 
+#ifndef YMRT_ORACLE_REAL_CUDA
 cudaError_t CUDARTAPI cudaMalloc(void** ptr, size_t size) {
   *ptr = std::malloc(size ? size : 1);
   return *ptr ? cudaSuccess : cudaErrorMemoryAllocation;
@@ -44,6 +48,7 @@ cudaError_t CUDARTAPI cudaLaunchKernel(const void*, dim3, dim3, void**, size_t, 
 const char* CUDARTAPI cudaGetErrorString(cudaError_t error) {
   return error == cudaSuccess ? "no error" : "oracle host stand-in: operation not supported";
 }
+#endif  // YMRT_ORACLE_REAL_CUDA
 
 aiReturn aiGetMaterialFloatArray(const aiMaterial*, const char*, unsigned int, unsigned int, ai_real*,
                                  unsigned int*) {

@@ -58,6 +58,12 @@ def instanced_path(scene_dir):
 
 
 @pytest.fixture(scope="session")
+def volumetric_path(scene_dir):
+    from ymrt_b200 import scenes
+    return scenes.scene_path("volumetric", 0, scene_dir)
+
+
+@pytest.fixture(scope="session")
 def oracle():
     """The reference built for the host (oracle/_ref); skips when absent."""
     from oracle import ref

@@ -32,6 +32,7 @@ ERRORS = {
 
 QUERY_COUNTS, QUERY_INSTANCES, QUERY_LIGHTS, QUERY_LIGHT_TABLE = 0, 1, 2, 3
 QUERY_TRANSFORMS, QUERY_CAMERA, QUERY_TRIANGLES = 4, 5, 6
+QUERY_MATERIALS, QUERY_VOLUMES, QUERY_DISTANT_LIGHTS, QUERY_TEXTURES = 7, 8, 9, 10
 
 
 class YmrtError(RuntimeError):
@@ -205,6 +206,13 @@ class HostScene:
 
     def triangles(self, mesh: int) -> np.ndarray:
         return self._query(QUERY_TRIANGLES, np.uint32, mesh).reshape(-1, 3)
+
+    def records(self, kind: str) -> np.ndarray:
+        """Materials, volumes, distant lights (32-bit words of the reference's
+        structs) or textures (13 words each), one row per record."""
+        what, width = {"materials": (QUERY_MATERIALS, 39), "volumes": (QUERY_VOLUMES, 9),
+                       "distant_lights": (QUERY_DISTANT_LIGHTS, 8), "textures": (QUERY_TEXTURES, 13)}[kind]
+        return self._query(what, np.uint32).reshape(-1, width)
 
 
 class Scene:

@@ -113,13 +113,14 @@ struct ymrt_context {
       P.transfer_count = reinterpret_cast<uint8_t*>(p);
       P.capacity = capacity;
     }
-    const size_t hit_bytes = n * (sizeof(float4) + sizeof(uint4) + kMaxNearby * sizeof(uint4));
+    const size_t hit_bytes = n * (sizeof(float4) + sizeof(uint4) + kMaxNearby * sizeof(uint4) + kMaxBoundaryRecord * sizeof(float));
     cudaError_t e = hit_buf.ensure(hit_bytes);
     if (e != cudaSuccess) return cuda_fail(e, "allocating hit pool");
     char* h = hit_buf.as<char>();
     hits.bary_t = reinterpret_cast<float4*>(h); h += n * sizeof(float4);
     hits.ids = reinterpret_cast<uint4*>(h); h += n * sizeof(uint4);
-    hits.nearby = reinterpret_cast<uint4*>(h);
+    hits.nearby = reinterpret_cast<uint4*>(h); h += n * kMaxNearby * sizeof(uint4);
+    hits.vol_w = reinterpret_cast<float*>(h);
     pool_capacity = capacity;
     return YMRT_OK;
   }
@@ -289,6 +290,29 @@ long long ymrt_host_scene_query(const ymrt_host_scene* hs, int what, int index, 
                            c.v.y,        c.v.z,        c.w.x,        c.w.y, c.w.z, c.aspect_ratio, c.tan_half_fov};
       return copy(v, 14, sizeof(float));
     }
+    case YMRT_QUERY_MATERIALS:
+      return copy(s.materials.data(), s.materials.size() * (sizeof(Material) / 4), 4);
+    case YMRT_QUERY_VOLUMES:
+      return copy(s.volumes.data(), s.volumes.size() * (sizeof(Volume) / 4), 4);
+    case YMRT_QUERY_DISTANT_LIGHTS:
+      return copy(s.distant_lights.data(), s.distant_lights.size() * (sizeof(DistantLight) / 4), 4);
+    case YMRT_QUERY_TEXTURES: {
+      std::vector<uint32_t> v;
+      for (const Texture& t : s.textures) {
+        uint32_t r[13] = {t.type, kEmpty, kEmpty, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+        if (t.type == kTexConstFloat) {
+          r[3] = f2u(t.value);
+        } else if (t.type == kTexConstRgb) {
+          r[4] = f2u(t.color.x); r[5] = f2u(t.color.y); r[6] = f2u(t.color.z);
+        } else if (t.type == kTexFbm) {
+          r[1] = t.child[0]; r[2] = t.child[1];
+          r[7] = f2u(t.frequency); r[8] = f2u(t.lacunarity); r[9] = f2u(t.gain); r[10] = (uint32_t)t.layer_count;
+          r[11] = f2u(t.amplitude); r[12] = f2u(t.offset);
+        }
+        v.insert(v.end(), r, r + 13);
+      }
+      return copy(v.data(), v.size(), sizeof(uint32_t));
+    }
     case YMRT_QUERY_TRIANGLES: {
       if (index < 0 || (size_t)index >= s.meshes.size()) return YMRT_ERR_INVALID;
       const std::vector<uint32_t>& t = s.meshes[index].tris;
@@ -347,6 +371,7 @@ int ymrt_scene_upload(ymrt_context* ctx, const ymrt_host_scene* hs, const uint32
   UP(s.all_nrm, normals);
   UP(s.all_uv, texcoords);
   UP(s.materials, materials);
+  UP(s.distant_lights, distant_lights);
   UP(s.shape_lights, shape_lights);
   UP(s.shape_light_table, shape_light_table);
   UP(s.volumes, volumes);
@@ -362,6 +387,7 @@ int ymrt_scene_upload(ymrt_context* ctx, const ymrt_host_scene* hs, const uint32
   D.transform_count = (uint32_t)s.transforms.size();
   D.geometry_count = (uint32_t)s.geo_desc.size();
   D.material_count = (uint32_t)s.materials.size();
+  D.distant_light_count = (uint32_t)s.distant_lights.size();
   D.shape_light_count = (uint32_t)s.shape_lights.size();
   D.volume_count = (uint32_t)s.volumes.size();
   D.texture_count = (uint32_t)s.textures.size();
@@ -419,8 +445,7 @@ int ymrt_render_tiles(ymrt_scene* sc, const ymrt_render_setting* setting, int fr
   std::memcpy(&rs, setting, sizeof(rs));
   if (frame_index < 1) return ctx->fail(YMRT_ERR_INVALID, "frame_index starts at 1");
   if (rs.sampler_type != 1) return ctx->fail(YMRT_ERR_UNSUPPORTED, "only the Halton sampler (sampler_type 1) is supported");
-  if (rs.enable_distant_light) return ctx->fail(YMRT_ERR_UNSUPPORTED, "distant lights are not supported yet");
-  if (rs.enable_volume_scattering) return ctx->fail(YMRT_ERR_UNSUPPORTED, "volume scattering is not supported yet");
+  const bool volumes = rs.enable_volume_scattering && sc->dev.volume_count > 0;
   const uint32_t spp = (uint32_t)std::max(rs.ssp, 1);
   const uint32_t per_tile = (uint32_t)kTilePixels * spp;
   cudaSetDevice(ctx->device);
@@ -460,10 +485,10 @@ int ymrt_render_tiles(ymrt_scene* sc, const ymrt_render_setting* setting, int fr
     if (ctx->profiling) cudaEventRecord(ctx->ev_stage[0], st);
     launch_generate(A, live, gen, cursor, tiles_x, frame_index, spp, st);
     if (ctx->profiling) cudaEventRecord(ctx->ev_stage[1], st);
-    launch_extend(A, total, ctx->hits, image, dc, st);
+    launch_extend(A, total, ctx->hits, image, dc, volumes, st);
     if (ctx->profiling) cudaEventRecord(ctx->ev_stage[2], st);
     cudaMemsetAsync(&dc->next_count, 0, sizeof(uint32_t), st);
-    launch_shade(A, total, ctx->hits, B, image, dc, st);
+    launch_shade(A, total, ctx->hits, B, image, dc, volumes, st);
     if (ctx->profiling) cudaEventRecord(ctx->ev_stage[3], st);
     launches += (gen > 0 ? 1 : 0) + (total > 0 ? 2 : 0);
     if ((e = cudaMemcpyAsync(ctx->counters_host, dc, sizeof(WaveCounters), cudaMemcpyDeviceToHost, st)) != cudaSuccess)
@@ -589,6 +614,7 @@ size_t carve(unsigned char* base, uint32_t n, PathPool pools[2], HitPool* hits, 
   hits->bary_t = reinterpret_cast<float4*>(take(n * sizeof(float4)));
   hits->ids = reinterpret_cast<uint4*>(take(n * sizeof(uint4)));
   hits->nearby = reinterpret_cast<uint4*>(take(n * kMaxNearby * sizeof(uint4)));
+  hits->vol_w = nullptr;  // volume scattering is not rendered by this entry point
   return off;
 }
 
@@ -659,9 +685,9 @@ int ymrt_render_tiles_noalloc(ymrt_scene* sc, const ymrt_render_setting* setting
     const uint32_t gen = n_tiles * per_tile;
     const uint32_t total = live + gen;
     launch_generate(pools[a], live, gen, cursor, tiles_x, frame_index, spp, st);
-    launch_extend(pools[a], total, hits, image, dc, st);
+    launch_extend(pools[a], total, hits, image, dc, false, st);
     cudaMemsetAsync(&dc->next_count, 0, sizeof(uint32_t), st);
-    launch_shade(pools[a], total, hits, pools[a ^ 1], image, dc, st);
+    launch_shade(pools[a], total, hits, pools[a ^ 1], image, dc, false, st);
     launches += (gen > 0 ? 1 : 0) + (total > 0 ? 2 : 0);
     if ((e = cudaMemcpyAsync(ctx->counters_host, dc, sizeof(WaveCounters), cudaMemcpyDeviceToHost, st)) != cudaSuccess)
       return ctx->cuda_fail(e, "reading wave counters");

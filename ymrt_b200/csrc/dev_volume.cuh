@@ -1,0 +1,492 @@
+// Volume media on the device: delta tracking through overlapping media,
+// transmittance along shadow rays through medium boundaries, Henyey-Greenstein
+// phase functions, and the procedural fBm density the reference's media use.
+//
+// Follows src/VolumeEval.cuh (SampleTrHomogeneous :18-78,
+// SampleTrHeterogeneous :80-214, EvalTrHomogeneous :253-267,
+// EvalTrHeterogeneous :269-386, TraceTr :420-468, SampleMixedPhases
+// :470-516, EvalMixedPhases :518-538), src/Volume.h (EvalPhase, SamplePhase),
+// src/TextureEval.cuh (PerlinNoiseEval :55-132, PerlinNoiseFBM :134-145,
+// TextureEval :419-481) and src/Texture.h (GetUpperBound :1181-1251), in
+// the reference's operand order.
+#pragma once
+
+#include "ymrt_scene.h"
+#include "dev_sampler.cuh"
+
+namespace ym {
+
+// Lattice permutation of the reference's Perlin noise (src/TextureEval.cuh:19);
+// kept identical so that procedural densities match the reference's value for
+// value. Indexed modulo 256 (the reference stores it twice in a row).
+__constant__ uint8_t c_perlin_perm[256] = {
+    172, 142, 240, 182, 179, 214,  29, 111, 156,   3, 131, 161, 164, 194, 243, 124,
+    127, 236,  88, 166,  83, 134,  71, 183, 227, 235, 106, 226, 216,  99, 149, 241,
+    206,  63,  48,  31,  20, 171,  46, 185,   6, 125, 184, 133, 199, 201,  58,  81,
+    177, 174,  92,  78,  32, 190,  89, 229,  14, 159, 196,  69, 242, 222,  13,  54,
+    200,  50,  26, 218,   5, 101,  18,  72, 203, 191, 104, 141, 252,  65, 139, 210,
+     22, 180, 113, 253,  27, 102,  25, 169,  56, 110, 178, 105, 254,  80,  73,   4,
+     90, 155,  91, 120, 181,   9, 123, 198, 193, 118, 146,  44, 247, 162, 231, 143,
+    153, 160,  57, 112, 238,  77,  95,  34, 168, 195, 126, 224, 213, 187,  41,  42,
+    152, 219, 220,  39,  53, 138, 239, 157,  12,  38,  24, 188,  76,   7, 103,   1,
+     33, 130,  74, 189,  79, 232,  96,  86, 135,  35, 234, 205, 150, 165,  30, 109,
+    212,  66,   0, 228, 129,  23,  97,   8, 107, 209, 192, 175,  11,  52,  16, 248,
+     55,  28, 173, 115,  51, 163, 197,   2, 208,  64, 148,  37,  19, 167,  84,  61,
+    176, 211,  17,  93, 108, 121, 116,  87,  43, 249, 147, 122,  21, 117, 136, 233,
+    145,  15, 245,  59,  75, 137, 151, 255, 154, 204, 244,  98,  40,  70,  10,  85,
+    225, 223, 251, 158, 132,  45, 119, 114,  60,  67, 140, 144, 207, 215,  47, 246,
+    230, 186, 250, 100,  36, 221, 217,  68, 128,  49,  62, 237,  82,  94, 170, 202,
+};
+
+__device__ __forceinline__ int perlin_hash(int x, int y, int z) {
+  return c_perlin_perm[(c_perlin_perm[(c_perlin_perm[x] + y) & 255] + z) & 255];
+}
+
+// Gradient dot products of the 16 lattice directions (PerlinNoiseEval).
+__device__ __forceinline__ float perlin_grad(int h, float x, float y, float z) {
+  switch (h & 15) {
+    case 0: return x + y;
+    case 1: return -x + y;
+    case 2: return x - y;
+    case 3: return -x - y;
+    case 4: return x + z;
+    case 5: return -x + z;
+    case 6: return x - z;
+    case 7: return -x - z;
+    case 8: return y + z;
+    case 9: return -y + z;
+    case 10: return y - z;
+    case 11: return -y - z;
+    case 12: return y + x;
+    case 13: return -x + y;
+    case 14: return -y + z;
+    default: return -y - z;
+  }
+}
+
+__device__ __forceinline__ float perlin_fade(float t) { return t * t * t * (t * (t * 6.0f - 15.0f) + 10.0f); }
+
+// PerlinNoiseEval (src/TextureEval.cuh:55-132).
+__device__ __forceinline__ float perlin_noise(vec3 p) {
+  int x0 = (int)floorf(p.x), y0 = (int)floorf(p.y), z0 = (int)floorf(p.z);
+  const float tx = p.x - (float)x0, ty = p.y - (float)y0, tz = p.z - (float)z0;
+  const int x1 = (x0 + 1) & 255, y1 = (y0 + 1) & 255, z1 = (z0 + 1) & 255;
+  x0 &= 255;
+  y0 &= 255;
+  z0 &= 255;
+  const float v000 = perlin_grad(perlin_hash(x0, y0, z0), tx, ty, tz);
+  const float v100 = perlin_grad(perlin_hash(x1, y0, z0), tx - 1, ty, tz);
+  const float v010 = perlin_grad(perlin_hash(x0, y1, z0), tx, ty - 1, tz);
+  const float v001 = perlin_grad(perlin_hash(x0, y0, z1), tx, ty, tz - 1);
+  const float v110 = perlin_grad(perlin_hash(x1, y1, z0), tx - 1, ty - 1, tz);
+  const float v011 = perlin_grad(perlin_hash(x0, y1, z1), tx, ty - 1, tz - 1);
+  const float v101 = perlin_grad(perlin_hash(x1, y0, z1), tx - 1, ty, tz - 1);
+  const float v111 = perlin_grad(perlin_hash(x1, y1, z1), tx - 1, ty - 1, tz - 1);
+  const float ix = perlin_fade(tx), iy = perlin_fade(ty), iz = perlin_fade(tz);
+  const float v00 = v000 + ix * (v100 - v000);
+  const float v01 = v001 + ix * (v101 - v001);
+  const float v10 = v010 + ix * (v110 - v010);
+  const float v11 = v011 + ix * (v111 - v011);
+  const float v0 = v00 + iy * (v10 - v00);
+  const float v1 = v01 + iy * (v11 - v01);
+  return v0 + iz * (v1 - v0);
+}
+
+// PerlinNoiseFBM (src/TextureEval.cuh:134-145).
+__device__ __forceinline__ float perlin_fbm(vec3 p, float lacunarity, float gain, int layers, float amplitude,
+                                            float offset) {
+  float r = 0.0f, freq = 1.0f;
+  for (int i = 0; i < layers; ++i) {
+    r += amplitude * perlin_noise(freq * p) + offset;
+    amplitude *= gain;
+    offset *= gain;
+    freq *= lacunarity;
+  }
+  return r;
+}
+
+// TextureEval for constant and fBm nodes (src/TextureEval.cuh:419-481): a
+// post-order walk with an explicit stack of eight nodes, as the reference.
+__device__ __forceinline__ vec3 texture_eval(const Texture* __restrict__ tex, uint32_t root, vec3 p_object,
+                                             uint32_t* errors) {
+  struct Frame {
+    uint32_t idx;
+    int parent, slot, next;
+    vec3 child[2];
+  };
+  Frame st[8];
+  int top = 0;
+  st[0].idx = root;
+  st[0].parent = -1;
+  st[0].slot = -1;
+  st[0].next = 0;
+  for (int guard = 0; guard < 64; ++guard) {
+    Frame& f = st[top];
+    const Texture& t = tex[f.idx];
+    const int n_child = t.type == kTexFbm ? 2 : 0;
+    if (f.next < n_child) {
+      const uint32_t c = t.child[f.next];
+      if (c == kEmpty) {
+        f.child[f.next] = vec3(0.0f);
+        ++f.next;
+        continue;
+      }
+      if (top + 1 >= 8) {
+        atomicOr(errors, 1u);
+        return vec3(0.0f);
+      }
+      Frame& g = st[++top];
+      g.idx = c;
+      g.parent = top - 1;
+      g.slot = f.next;
+      g.next = 0;
+      continue;
+    }
+    vec3 r(0.0f);
+    if (t.type == kTexConstFloat) {
+      r = vec3(t.value);
+    } else if (t.type == kTexConstRgb) {
+      r = t.color;
+    } else if (t.type == kTexFbm) {
+      const float fbm = perlin_fbm(t.frequency * p_object, t.lacunarity, t.gain, t.layer_count, t.amplitude, t.offset);
+      r = f.child[0] + fbm * (f.child[1] - f.child[0]);
+    }
+    if (f.parent < 0) return r;
+    Frame& par = st[f.parent];
+    par.child[f.slot] = r;
+    ++par.next;
+    --top;
+  }
+  atomicOr(errors, 4u);
+  return vec3(0.0f);
+}
+
+// Texture::GetUpperBound for the supported node types (src/Texture.h:1181-1251).
+__device__ __forceinline__ float texture_upper_bound(const Texture& t) {
+  if (t.type == kTexConstFloat) return t.value;
+  if (t.type == kTexConstRgb) return gmax(t.color.x, gmax(t.color.y, t.color.z));
+  if (t.type == kTexFbm) {
+    float r = 0.0f, a = t.amplitude, o = t.offset;
+    for (int i = 0; i < t.layer_count; ++i) {
+      r += a + o;
+      a *= t.gain;
+      o *= t.gain;
+    }
+    return r;
+  }
+  return 0.0f;
+}
+
+__device__ __forceinline__ bool has_density(const DeviceScene& S, const Volume& v) {
+  return v.density_texture_idx >= 0 && (uint32_t)v.density_texture_idx < S.texture_count;
+}
+
+// RayTransfer::GetCurrentVolumeIndices (src/Ray.h:131-145).
+__device__ __forceinline__ int current_volumes(const RayTransfer& rt, uint32_t volume_count, int idx[kMaxBoundaryRecord]) {
+  if (rt.record_count == 0 || rt.max_priority_record_index == -1) return 0;
+  const uint32_t mp = rt.records[rt.max_priority_record_index].ior_priority;
+  int n = 0;
+  for (int r = rt.record_count - 1; r >= 0; --r)
+    if (rt.records[r].ior_priority == mp && rt.records[r].vol_idx >= 0 && (uint32_t)rt.records[r].vol_idx < volume_count)
+      idx[n++] = rt.records[r].vol_idx;
+  return n;
+}
+
+// -------------------------------------------------------------- phases ---
+
+// EvalPhase (src/Volume.h:21-27).
+__device__ __forceinline__ float eval_phase(float g, vec3 wo, vec3 wi, float* pdf) {
+  const float c = dot(wo, wi);
+  const float t = 1.f + g * g + 2.f * g * c;
+  *pdf = 0.25f * kInvPi * (1.f - g * g) * safe_rcp((t * sqrtf(gmax(t, 0.0f))));
+  return *pdf;
+}
+
+// SamplePhase (src/Volume.h:28-47).
+__device__ __forceinline__ void sample_phase(float g, float u0, float u1, vec3 wo, float* weight, vec3* wi, float* pdf) {
+  float c;
+  if (fabsf(g) < 1e-4f) {
+    c = 1.f - 2.f * u0;
+  } else {
+    const float t = (1.f - g * g) * safe_rcp(1.f - g + 2.f * g * u0);
+    c = (1.f + g * g - t * t) / (2.f * g);
+  }
+  const float s = sqrtf(gmax(0.0f, 1.0f - c * c));
+  const float phi = 2.f * kPi * u1;
+  vec3 w = wo, u, v;
+  orthogonal_basis(w, u, v);
+  *wi = u * s * cosf(phi) + v * s * sinf(phi) + w * c;
+  eval_phase(g, wo, *wi, pdf);
+  *weight = 1.0f;
+}
+
+// SampleMixedPhases (src/VolumeEval.cuh:470-516).
+__device__ __forceinline__ bool sample_mixed_phases(const float* w, const float* gs, int n, float u0, float u1, vec3 wo,
+                                                    float* weight, vec3* wi, float* pdf) {
+  if (n == 0) return false;
+  float cdf = 0.0f;
+  int sel = -1;
+  for (int i = 0; i < n; ++i) {
+    if (u0 < cdf + w[i]) {
+      sel = i;
+      u0 = (u0 - cdf) * safe_rcp(w[i]);
+      break;
+    }
+    cdf += w[i];
+  }
+  if (sel == -1) sel = n - 1;
+  float ppdf = 0.0f;
+  sample_phase(gs[sel], u0, u1, wo, weight, wi, &ppdf);
+  float mixed_pdf = ppdf * w[sel];
+  float mixed_g = (*weight) * ppdf * w[sel];
+  for (int i = 0; i < n; ++i) {
+    if (i == sel) continue;
+    float p;
+    mixed_g += w[i] * eval_phase(gs[i], wo, *wi, &p);
+    mixed_pdf += w[i] * p;
+  }
+  *pdf = mixed_pdf;
+  *weight = mixed_g * safe_rcp(mixed_pdf);
+  return true;
+}
+
+// EvalMixedPhases (src/VolumeEval.cuh:518-538).
+__device__ __forceinline__ float eval_mixed_phases(const float* w, const float* gs, int n, vec3 wo, vec3 wi, float* pdf) {
+  if (n == 0) {
+    *pdf = 0.0f;
+    return 0.0f;
+  }
+  float mg = 0.0f, mp = 0.0f;
+  for (int i = 0; i < n; ++i) {
+    float sp = 0.0f;
+    const float sg = eval_phase(gs[i], wo, wi, &sp);
+    mg += w[i] * sg;
+    mp += w[i] * sp;
+  }
+  *pdf = mp;
+  return mg;
+}
+
+// ------------------------------------------------------- free flights ---
+
+// SampleTrHomogeneous (src/VolumeEval.cuh:18-78).
+__device__ __forceinline__ bool sample_tr_homogeneous(const DeviceScene& S, int n, const int* vidx, float t_max,
+                                                      vec3* tr_weight, float* dist, float* vw, HaltonState& hs) {
+  *tr_weight = vec3(1.0f);
+  *dist = kFloatMax;
+  vec3 m(0.0f), ms(0.0f);
+  for (int i = 0; i < n; ++i) {
+    const Volume& v = S.volumes[vidx[i]];
+    m += v.sigma_t;
+    ms += v.sigma_t * v.albedo;
+  }
+  const float csum = m.x + m.y + m.z;
+  const vec3 cw = csum > 0.0f ? (m / csum) : vec3(1.0f / 3.0f);
+  float u0 = halton_next(hs, S.halton_perm);
+  int ch = 0;
+  if (u0 < cw[0]) {
+    ch = 0;
+    u0 = u0 * safe_rcp(cw[0]);
+  } else if (u0 < cw[0] + cw[1]) {
+    ch = 1;
+    u0 = (u0 - cw[0]) * safe_rcp(cw[1]);
+  } else {
+    ch = 2;
+    u0 = (u0 - cw[0] - cw[1]) * safe_rcp(cw[2]);
+  }
+  const float fpl = m[ch] > 0.0f ? (-logf(1.0f - u0) / m[ch]) : kFloatMax;
+  const bool scatter = fpl < t_max;
+  const vec3 tr = vexp(-m * gmin(t_max, fpl));
+  const float pdf = scatter ? (cw.x * m.x * tr.x + cw.y * m.y * tr.y + cw.z * m.z * tr.z)
+                            : (cw.x * tr.x + cw.y * tr.y + cw.z * tr.z);
+  if (!(fabsf(pdf) > 0.0f)) return false;
+  const float vwt = 1.0f / float(n);
+  for (int i = 0; i < n; ++i) vw[i] = vwt;
+  *tr_weight = scatter ? (tr * ms / pdf) : (tr / pdf);
+  *dist = fpl;
+  return scatter;
+}
+
+// Majorant set-up shared by the heterogeneous estimators.
+struct Majorant {
+  vec3 m, cw, nf, mrcp;
+  vec3 ro[kMaxBoundaryRecord], rd[kMaxBoundaryRecord];
+  int ch;
+};
+__device__ __forceinline__ void volume_space_rays(const DeviceScene& S, int n, const int* vidx, vec3 o, vec3 d, float t_max,
+                                                  Majorant& M) {
+  M.m = vec3(0.0f);
+  for (int i = 0; i < n; ++i) {
+    const Volume& v = S.volumes[vidx[i]];
+    float ub = 1.0f;
+    if (has_density(S, v)) {
+      const mat4& it = S.i_transforms[v.transform_idx];
+      M.ro[i] = xform_point_glm(it, o);
+      M.rd[i] = xform_dir_glm(it, d);
+      ub = texture_upper_bound(S.textures[v.density_texture_idx]);
+    }
+    M.m += v.sigma_t * ub;
+  }
+  const float csum = M.m.x + M.m.y + M.m.z;
+  M.cw = csum > 0.0f ? (M.m / csum) : vec3(1.0f / 3.0f);
+}
+__device__ __forceinline__ void densities(const DeviceScene& S, int n, const int* vidx, const Majorant& M, float acc,
+                                          vec3* mst, vec3* mss, uint32_t* errors) {
+  *mst = vec3(0.0f);
+  if (mss) *mss = vec3(0.0f);
+  for (int i = 0; i < n; ++i) {
+    const Volume& v = S.volumes[vidx[i]];
+    float density = 1.0f;
+    if (has_density(S, v))
+      density = gmax(texture_eval(S.textures, (uint32_t)v.density_texture_idx, M.ro[i] + M.rd[i] * acc, errors).x, 0.0f);
+    *mst += v.sigma_t * density;
+    if (mss) *mss += v.sigma_t * v.albedo * density;
+  }
+}
+
+// SampleTrHeterogeneous (src/VolumeEval.cuh:80-214): delta tracking against
+// the summed majorant with channel-wise real / null collision probabilities.
+__device__ __noinline__ bool sample_tr_heterogeneous(const DeviceScene& S, int n, const int* vidx, vec3 o, vec3 d,
+                                                     float t_max, vec3* tr_weight, float* dist, float* vw,
+                                                     HaltonState& hs, uint32_t* errors) {
+  *tr_weight = vec3(1.0f);
+  *dist = kFloatMax;
+  Majorant M;
+  volume_space_rays(S, n, vidx, o, d, t_max, M);
+  const float u0 = halton_next(hs, S.halton_perm);
+  int ch = 0;
+  if (u0 < M.cw[0]) ch = 0;
+  else if (u0 < M.cw[0] + M.cw[1]) ch = 1;
+  else ch = 2;
+  if (!(M.m[ch] > 0.0f)) return false;
+  const vec3 nf(safe_rcp(M.m.x + 1.0f), safe_rcp(M.m.y + 1.0f), safe_rcp(M.m.z + 1.0f));
+  const vec3 mrcp(safe_rcp(M.m.x), safe_rcp(M.m.y), safe_rcp(M.m.z));
+  vec3 tr(1.0f), pdf(1.0f);
+  float acc = 0.0f;
+  int it = 0;
+  while (true) {
+    if (it >= kMaxFreePath) {
+      atomicOr(errors, 4u);
+      break;
+    }
+    const float fpl = -logf(1.0f - halton_next(hs, S.halton_perm)) / M.m[ch];
+    if (acc + fpl > t_max) {
+      const vec3 ptr = vexp(-M.m * (t_max - acc));
+      tr *= ptr * nf;
+      pdf *= ptr * nf;
+      acc += fpl;
+      break;
+    }
+    acc += fpl;
+    vec3 mst, mss;
+    densities(S, n, vidx, M, acc, &mst, &mss, errors);
+    vec3 real;
+    real.x = gmin(M.m.x > 0.0f ? mst.x * mrcp.x : 0.0f, 1.0f);
+    real.y = gmin(M.m.y > 0.0f ? mst.y * mrcp.y : 0.0f, 1.0f);
+    real.z = gmin(M.m.z > 0.0f ? mst.z * mrcp.z : 0.0f, 1.0f);
+    const vec3 fake = vec3(1.0f) - real;
+    const vec3 ptr = vexp(-M.m * fpl);
+    if (halton_next(hs, S.halton_perm) < real[ch]) {
+      tr *= ptr * mss * nf;
+      pdf *= ptr * M.m * real * nf;
+      break;
+    } else {
+      tr *= ptr * M.m * fake * nf;
+      pdf *= ptr * M.m * fake * nf;
+    }
+    ++it;
+  }
+  const float vwt = 1.0f / float(n);
+  for (int i = 0; i < n; ++i) vw[i] = vwt;
+  *tr_weight = tr * safe_rcp(dot(M.cw, pdf));
+  *dist = acc;
+  return acc > t_max || it >= kMaxFreePath ? false : true;
+}
+
+// SampleVolumeScattering (src/VolumeEval.cuh:217-251).
+__device__ __forceinline__ bool sample_volume_scattering(const DeviceScene& S, vec3 o, vec3 d, int n, const int* vidx,
+                                                         float t_max, vec3* tr_weight, float* dist, float* vw,
+                                                         HaltonState& hs, uint32_t* errors) {
+  if (S.volume_count == 0 || n == 0) return false;
+  bool het = false;
+  for (int i = 0; i < n; ++i)
+    if (has_density(S, S.volumes[vidx[i]])) {
+      het = true;
+      break;
+    }
+  if (het) return sample_tr_heterogeneous(S, n, vidx, o, d, t_max, tr_weight, dist, vw, hs, errors);
+  return sample_tr_homogeneous(S, n, vidx, t_max, tr_weight, dist, vw, hs);
+}
+
+// EvalTrHeterogeneous (src/VolumeEval.cuh:269-386): ratio-tracking style
+// transmittance with Russian roulette after 32 steps.
+__device__ __noinline__ vec3 eval_tr_heterogeneous(const DeviceScene& S, int n, const int* vidx, vec3 o, vec3 d,
+                                                   float t_max, HaltonState& hs, uint32_t* errors) {
+  Majorant M;
+  volume_space_rays(S, n, vidx, o, d, t_max, M);
+  const float u0 = halton_next(hs, S.halton_perm);
+  int ch = 0;
+  if (u0 < M.cw[0]) ch = 0;
+  else if (u0 < M.cw[0] + M.cw[1]) ch = 1;
+  else ch = 2;
+  if (!(M.m[ch] > 0.0f)) return vec3(1.0f);
+  const vec3 nf(safe_rcp(M.m.x + 1.0f), safe_rcp(M.m.y + 1.0f), safe_rcp(M.m.z + 1.0f));
+  const vec3 mrcp(safe_rcp(M.m.x), safe_rcp(M.m.y), safe_rcp(M.m.z));
+  vec3 tr(1.0f), pdf(1.0f);
+  float acc = 0.0f;
+  int it = 0;
+  while (true) {
+    if (it >= kMaxFreePath) {
+      atomicOr(errors, 4u);
+      break;
+    }
+    const float fpl = -logf(1.0f - halton_next(hs, S.halton_perm)) / M.m[ch];
+    if (acc + fpl > t_max) {
+      const vec3 ptr = vexp(-M.m * (t_max - acc));
+      tr *= ptr * nf;
+      pdf *= ptr * nf;
+      break;
+    }
+    acc += fpl;
+    vec3 mst;
+    densities(S, n, vidx, M, acc, &mst, nullptr, errors);
+    vec3 real;
+    real.x = gmin(M.m.x > 0.0f ? mst.x * mrcp.x : 0.0f, 1.0f);
+    real.y = gmin(M.m.y > 0.0f ? mst.y * mrcp.y : 0.0f, 1.0f);
+    real.z = gmin(M.m.z > 0.0f ? mst.z * mrcp.z : 0.0f, 1.0f);
+    const vec3 fake = vec3(1.0f) - real;
+    const vec3 ptr = vexp(-M.m * fpl);
+    tr *= ptr * M.m * fake * nf;
+    pdf *= ptr * M.m * nf;
+    if (it + 1 > 32) {
+      const vec3 pt = tr * safe_rcp(dot(M.cw, pdf));
+      float rr = gmax(pt.x, gmax(pt.y, pt.z));
+      rr = gmin(rr, 1.0f);
+      if (halton_next(hs, S.halton_perm) < rr) tr /= gmax(rr, kMinColorEps);
+      else break;
+    }
+    ++it;
+  }
+  return tr * safe_rcp(dot(M.cw, pdf));
+}
+
+// EvalTr (src/VolumeEval.cuh:388-418).
+__device__ __forceinline__ vec3 eval_tr(const DeviceScene& S, vec3 o, vec3 d, const RayTransfer& rt, float t_max,
+                                        HaltonState& hs, uint32_t* errors) {
+  if (S.volume_count == 0) return vec3(1.0f);
+  int vidx[kMaxBoundaryRecord];
+  const int n = current_volumes(rt, S.volume_count, vidx);
+  if (n == 0) return vec3(1.0f);
+  bool het = false;
+  for (int i = 0; i < n; ++i)
+    if (has_density(S, S.volumes[vidx[i]])) {
+      het = true;
+      break;
+    }
+  if (het) return eval_tr_heterogeneous(S, n, vidx, o, d, t_max, hs, errors);
+  vec3 m(0.0f);
+  for (int i = 0; i < n; ++i) m += S.volumes[vidx[i]].sigma_t;
+  return vexp(-m * t_max);
+}
+
+}  // namespace ym

@@ -20,6 +20,7 @@
 #include "dev_sampler.cuh"
 #include "dev_shade.cuh"
 #include "dev_traverse.cuh"
+#include "dev_volume.cuh"
 #include "kernels.h"
 
 namespace ym {
@@ -113,6 +114,7 @@ __global__ void __launch_bounds__(256) k_generate(PathPool P, uint32_t base, uin
 
 // -------------------------------------------------------------- extend ---
 
+template <bool kVol>
 __global__ void __launch_bounds__(kTraceBlock) k_extend(PathPool P, uint32_t count, HitPool H, float4* image,
                                                         WaveCounters* counters) {
   __shared__ uint32_t s_stack[kStackShared * kTraceBlock];
@@ -132,21 +134,56 @@ __global__ void __launch_bounds__(kTraceBlock) k_extend(PathPool P, uint32_t cou
     st.sp = 0;
     st.overflow = false;
     ClosestHit ch;
-    const bool hit = trace_closest(S, st, o, d, kTMax, lh.x, lh.y, false, &ch, &tests, &nodes);
+    bool hit = trace_closest(S, st, o, d, kTMax, lh.x, lh.y, false, &ch, &tests, &nodes);
     overflow = st.overflow;
+    bool volume_hit = false;
+    float4 t4 = P.throughput[i];
+    vec3 tp(t4.x, t4.y, t4.z);
+    vec3 vol_pos(0.0f);
+    if (kVol) {
+      // volume free flight before the surface (src/Shading.cu:1828-1853)
+      RayTransfer rt;
+      rt.record_count = P.transfer_count[i];
+      rt.max_priority_record_index = -1;
+      if (rt.record_count > 0) rt = P.transfer[i];
+      const uint4 s4 = P.sampler[i];
+      HaltonState hs{(uint64_t)s4.x | ((uint64_t)s4.y << 32), s4.z};
+      int vidx[kMaxBoundaryRecord];
+      const int n = current_volumes(rt, S.volume_count, vidx);
+      vec3 trw(1.0f);
+      float dist = 0.0f;
+      float vw[kMaxBoundaryRecord];
+      const bool hv = sample_volume_scattering(S, o, d, n, vidx, hit ? ch.t : kTMax, &trw, &dist, vw, hs,
+                                               &counters->errors);
+      tp *= trw;
+      P.throughput[i] = make_float4(tp.x, tp.y, tp.z, 0.0f);
+      P.sampler[i] = make_uint4((uint32_t)hs.index, (uint32_t)(hs.index >> 32), hs.dim, 0u);
+      if (hv) {
+        volume_hit = true;
+        vol_pos = o + d * dist;
+        for (int k = 0; k < n; ++k) H.vol_w[(size_t)i * kMaxBoundaryRecord + k] = vw[k];
+        if (!hit) {
+          ch.inst = kEmpty;
+          ch.tri = kEmpty;
+          ch.back = 0;
+          ch.t = kTMax;
+          ch.nearby_count = 0;
+        }
+      }
+      hit = hit || hv;
+    }
     if (!hit) {
       // Ray_trace_path_tracing miss branch (src/Shading.cu:1855-1864).
       const float4 r4 = P.radiance[i];
       vec3 rad(r4.x, r4.y, r4.z);
-      if (c_setting.enable_env_light) {
-        const float4 t4 = P.throughput[i];
-        rad += indirect_clamp(c_setting, vec3(t4.x, t4.y, t4.z) * background(d), (int)(pf.y & kFlagDepthMask));
-      }
+      if (c_setting.enable_env_light)
+        rad += indirect_clamp(c_setting, tp * background(d), (int)(pf.y & kFlagDepthMask));
       const float inv_spp = 1.0f / gmax(c_setting.ssp, 1);
       accumulate_pixel(image, pf.x, rad, inv_spp);
       P.pixel_flags[i] = make_uint2(pf.x, pf.y | kFlagDead);
     } else {
-      H.bary_t[i] = make_float4(ch.b0, ch.b1, ch.b2, ch.t);
+      if (volume_hit) H.bary_t[i] = make_float4(vol_pos.x, vol_pos.y, vol_pos.z, ch.t);
+      else H.bary_t[i] = make_float4(ch.b0, ch.b1, ch.b2, ch.t);
       uint32_t nearby_word = (uint32_t)ch.nearby_count;
       if (!(ch.nearby_count == 1 && ch.nearby[0].prim == ch.inst && ch.nearby[0].t == ch.t &&
             ch.nearby[0].back == ch.back)) {
@@ -155,7 +192,7 @@ __global__ void __launch_bounds__(kTraceBlock) k_extend(PathPool P, uint32_t cou
               make_uint4(ch.nearby[k].prim, __float_as_uint(ch.nearby[k].t), (uint32_t)ch.nearby[k].back, 0u);
         nearby_word |= kNearbyExplicit;
       }
-      H.ids[i] = make_uint4(ch.inst, ch.tri, (uint32_t)ch.back, nearby_word);
+      H.ids[i] = make_uint4(ch.inst, ch.tri, (uint32_t)ch.back | (volume_hit ? 2u : 0u), nearby_word);
     }
   }
   // counters: one atomic per warp
@@ -260,13 +297,104 @@ __device__ __forceinline__ float ex_ior(const RayTransfer& rt, uint32_t hit_prim
   return mi == -1 ? 1.0f : rt.records[mi].ior;
 }
 
-// EvalShapeLight (src/Shading.cu:294-417) for surfaces without media.
+// Closest boundary crossing of a ray (TraceVolume, src/ShadingUtilities.cuh:434-561)
+// and the transmittance along a shadow ray through every medium it crosses
+// (TraceTr, src/VolumeEval.cuh:420-468). `rt` is the shadow ray's own copy of
+// the nested-media stack; `o`/`d`/`tmax` and the last hit are the shadow ray.
+__device__ __noinline__ vec3 trace_tr(const DeviceScene& S, TraversalStack& st, vec3 o, vec3 d, float tmax,
+                                      uint32_t last_inst, uint32_t last_tri, RayTransfer& rt, HaltonState& hs,
+                                      uint32_t* errors, uint32_t* tests, uint32_t* nodes) {
+  if (S.volume_count == 0) return vec3(1.0f);
+  vec3 tr(1.0f);
+  const float max_d = tmax;
+  float traced = kTMin;
+  float ray_t = tmax;
+  int guard = 0;
+  while (traced < max_d) {
+    if (++guard > 4 * kMaxRayDepth) {
+      atomicOr(errors, (uint32_t)kDevErrIter);
+      break;
+    }
+    ClosestHit ch;
+    const bool hit = trace_closest(S, st, o, d, ray_t, last_inst, last_tri, true, &ch, tests, nodes);
+    if (!hit) {
+      tr *= eval_tr(S, o, d, rt, gmax(max_d - traced, 0.0f), hs, errors);
+      break;
+    }
+    tr *= eval_tr(S, o, d, rt, ch.t, hs, errors);
+    traced += ch.t;
+    vec3 hp, herr, hng;
+    fetch_geometry_normal(S, ch.inst, ch.tri, vec3(ch.b0, ch.b1, ch.b2), &hp, &herr, &hng);
+    boundary_transition(S, rt, ch.nearby, ch.nearby_count, errors);
+    o = offset_ray_origin(hp, herr, d, hng);
+    d = normalize(d);
+    last_inst = ch.inst;
+    last_tri = ch.tri;
+    ray_t = kTMax;
+  }
+  return tr;
+}
+
+// DistantLight::SampleLi / EvalLi (src/Light.h:343-386).
+__device__ __forceinline__ void distant_sample_li(const DeviceScene& S, const DistantLight& L, float u0, float u1, vec3* wi,
+                                                  vec3* Li, float* pdf) {
+  const mat4& otw = S.transforms[L.transform_idx];
+  const float cone = 2.0f * kPi * (1.0f - L.cos_theta_max);
+  vec3 cs(0.0f);
+  if (cone < 1E-10f) {
+    cs = vec3(0.0f, 1.0f, 0.0f);
+  } else {
+    const float c = (1.0f - u0) + u0 * L.cos_theta_max;
+    const float sn = sqrtf(gmax(0.0f, 1.0f - c * c));
+    const float phi = u1 * 2.0f * kPi;
+    cs = vec3(cosf(phi) * sn, sinf(phi) * sn, c);
+    cs = vec3(cs.x, cs.z, cs.y);
+  }
+  *wi = -normalize(transform_vector(otw, cs));
+  *pdf = 1.0f / gmax(cone, 1E-10f);
+  *Li = L.light_color * L.intensity;
+}
+__device__ __forceinline__ vec3 distant_eval_li(const DeviceScene& S, const DistantLight& L, vec3 wi, float* pdf) {
+  const vec3 lwi = transform_vector(S.i_transforms[L.transform_idx], wi);
+  const float c = -lwi.y;
+  if (c < L.cos_theta_max) {
+    *pdf = 0.0f;
+    return vec3(0.0f);
+  }
+  const float cone = 2.0f * kPi * (1.0f - L.cos_theta_max);
+  *pdf = 1.0f / cone;
+  return L.light_color * L.intensity * (*pdf);
+}
+
+// Shading-point context the light estimators share.
+struct SurfaceNee {
+  vec3 ray_dir, p, p_err, ng;
+  uint32_t inst, tri;
+  const RayTransfer* rt;
+  const NearbyHit* nb;
+  int n_nb;
+};
+
+// Transmittance of an unoccluded surface shadow ray (the volume part of the
+// reference's EvalShapeLight / EvalDistantLight).
+template <bool kVol>
+__device__ __forceinline__ vec3 surface_shadow_tr(const DeviceScene& S, TraversalStack& st, const SurfaceNee& c, vec3 so,
+                                                  vec3 ldir, float maxd, bool tb, HaltonState& hs, uint32_t* errors,
+                                                  uint32_t* tests, uint32_t* nodes) {
+  if (!kVol) return vec3(1.0f);
+  RayTransfer srt = *c.rt;
+  if (tb) boundary_transition(S, srt, c.nb, c.n_nb, errors);
+  return trace_tr(S, st, so, normalize(ldir), maxd, c.inst, c.tri, srt, hs, errors, tests, nodes);
+}
+
+// EvalShapeLight (src/Shading.cu:294-417).
+template <bool kVol>
 __device__ __forceinline__ vec3 eval_shape_light(const DeviceScene& S, TraversalStack& st, const LayeredBsdf& B,
-                                                 vec3 ray_dir, vec3 p, vec3 p_err, vec3 ng, HaltonState& hs,
-                                                 uint32_t* shadow_rays, uint32_t* tests, uint32_t* nodes) {
+                                                 const SurfaceNee& c, HaltonState& hs, uint32_t* shadow_rays,
+                                                 uint32_t* tests, uint32_t* nodes, uint32_t* errors) {
   if (S.shape_light_count == 0) return vec3(0.0f);
   vec3 direct(0.0f);
-  const vec3 wo = B.to_local(-ray_dir);
+  const vec3 wo = B.to_local(-c.ray_dir);
   float select_pdf = 0.0f;
   const int li = sample_light_power(S, halton_next(hs, S.halton_perm), &select_pdf);
   const ShapeLight L = S.shape_lights[li];
@@ -276,20 +404,21 @@ __device__ __forceinline__ vec3 eval_shape_light(const DeviceScene& S, Traversal
     halton_next2(hs, S.halton_perm, &u0, &u1);
     vec3 ldir(0.0f), lpos(0.0f), lerr(0.0f), lng(0.0f), Li(0.0f);
     float lpdf = 0.0f;
-    const bool valid = light_sample_li(lt, L.area, p, u0, u1, &ldir, &lpos, &lerr, &lng, &Li, &lpdf);
+    const bool valid = light_sample_li(lt, L.area, c.p, u0, u1, &ldir, &lpos, &lerr, &lng, &Li, &lpdf);
     const vec3 lwi = B.to_local(ldir);
     float wpdf = 0.0f;
     const vec3 f = bsdf_eval(B, wo, lwi, &wpdf);
     if (max_component(f) > kMinColorEps && valid) {
-      const vec3 so = offset_ray_origin(p, p_err, ldir, ng);
-      const float maxd = length(offset_ray_origin(lpos, lerr, -ldir, lng) - p) * kShadowRayClamp;
-      const bool tb = dot(-ray_dir, ng) * dot(ldir, ng) < 0.0f;
+      const vec3 so = offset_ray_origin(c.p, c.p_err, ldir, c.ng);
+      const float maxd = length(offset_ray_origin(lpos, lerr, -ldir, lng) - c.p) * kShadowRayClamp;
+      const bool tb = dot(-c.ray_dir, c.ng) * dot(ldir, c.ng) < 0.0f;
       const bool invalid = (!same_hemisphere(wo, lwi) && !tb) || (same_hemisphere(wo, lwi) && tb);
       if (!invalid) {
         ++*shadow_rays;
         if (!trace_occluded(S, st, so, normalize(ldir), maxd, tests, nodes)) {
+          const vec3 tr = surface_shadow_tr<kVol>(S, st, c, so, ldir, maxd, tb, hs, errors, tests, nodes);
           const float mis = power_heuristic(lpdf, wpdf);
-          direct += mis * 1.0f * vmin(f, vec3(kMaxColorClamp)) * vmin(Li, vec3(kMaxColorClamp));
+          direct += mis * tr * vmin(f, vec3(kMaxColorClamp)) * vmin(Li, vec3(kMaxColorClamp));
         }
       }
     }
@@ -303,17 +432,18 @@ __device__ __forceinline__ vec3 eval_shape_light(const DeviceScene& S, Traversal
       const vec3 ldir = B.to_world(bwi);
       vec3 lpos(0.0f), lerr(0.0f), lng(0.0f);
       float wpdf = 0.0f;
-      const vec3 Li = light_eval_li(lt, L.area, p, ldir, &lpos, &lerr, &lng, &wpdf);
+      const vec3 Li = light_eval_li(lt, L.area, c.p, ldir, &lpos, &lerr, &lng, &wpdf);
       if (max_component(Li) > kMinColorEps) {
-        const vec3 so = offset_ray_origin(p, p_err, ldir, ng);
-        const float maxd = length(offset_ray_origin(lpos, lerr, -ldir, lng) - p) * kShadowRayClamp;
-        const bool tb = dot(-ray_dir, ng) * dot(ldir, ng) < 0.0f;
+        const vec3 so = offset_ray_origin(c.p, c.p_err, ldir, c.ng);
+        const float maxd = length(offset_ray_origin(lpos, lerr, -ldir, lng) - c.p) * kShadowRayClamp;
+        const bool tb = dot(-c.ray_dir, c.ng) * dot(ldir, c.ng) < 0.0f;
         const bool invalid = (!same_hemisphere(wo, bwi) && !tb) || (same_hemisphere(wo, bwi) && tb);
         if (!invalid) {
           ++*shadow_rays;
           if (!trace_occluded(S, st, so, normalize(ldir), maxd, tests, nodes)) {
+            const vec3 tr = surface_shadow_tr<kVol>(S, st, c, so, ldir, maxd, tb, hs, errors, tests, nodes);
             const float mis = power_heuristic(bpdf, wpdf);
-            direct += mis * 1.0f * vmin(bw, vec3(kMaxColorClamp)) * vmin(Li, vec3(kMaxColorClamp));
+            direct += mis * tr * vmin(bw, vec3(kMaxColorClamp)) * vmin(Li, vec3(kMaxColorClamp));
           }
         }
       }
@@ -322,6 +452,167 @@ __device__ __forceinline__ vec3 eval_shape_light(const DeviceScene& S, Traversal
   return direct * safe_rcp(select_pdf);
 }
 
+// EvalDistantLight (src/Shading.cu:83-198).
+template <bool kVol>
+__device__ __forceinline__ vec3 eval_distant_light(const DeviceScene& S, TraversalStack& st, const LayeredBsdf& B,
+                                                   const SurfaceNee& c, HaltonState& hs, uint32_t* shadow_rays,
+                                                   uint32_t* tests, uint32_t* nodes, uint32_t* errors) {
+  if (S.distant_light_count == 0) return vec3(0.0f);
+  vec3 direct(0.0f);
+  const vec3 wo = B.to_local(-c.ray_dir);
+  const float select_pdf = 1.0f / float(S.distant_light_count);
+  const int li = gmax(gmin((int)(halton_next(hs, S.halton_perm) * S.distant_light_count), (int)S.distant_light_count - 1), 0);
+  const DistantLight L = S.distant_lights[li];
+  {
+    float u0, u1;
+    halton_next2(hs, S.halton_perm, &u0, &u1);
+    vec3 ldir(0.0f), Li(0.0f);
+    float lpdf = 0.0f;
+    distant_sample_li(S, L, u0, u1, &ldir, &Li, &lpdf);
+    const vec3 lwi = B.to_local(ldir);
+    float wpdf = 0.0f;
+    const vec3 f = bsdf_eval(B, wo, lwi, &wpdf);
+    if (max_component(f) > kMinColorEps) {
+      const vec3 so = offset_ray_origin(c.p, c.p_err, ldir, c.ng);
+      const bool tb = dot(-c.ray_dir, c.ng) * dot(ldir, c.ng) < 0.0f;
+      const bool invalid = (!same_hemisphere(wo, lwi) && !tb) || (same_hemisphere(wo, lwi) && tb);
+      if (!invalid) {
+        ++*shadow_rays;
+        if (!trace_occluded(S, st, so, normalize(ldir), kTMax, tests, nodes)) {
+          const vec3 tr = surface_shadow_tr<kVol>(S, st, c, so, ldir, kTMax, tb, hs, errors, tests, nodes);
+          const float mis = power_heuristic(lpdf, wpdf);
+          direct += mis * tr * vmin(f, vec3(kMaxColorClamp)) * vmin(Li, vec3(kMaxColorClamp));
+        }
+      }
+    }
+  }
+  {
+    float u0, u1, u2;
+    halton_next3(hs, S.halton_perm, &u0, &u1, &u2);
+    vec3 bw, bwi;
+    float bpdf = 0.0f;
+    if (bsdf_sample(B, wo, &bw, &bwi, &bpdf, u0, u1, u2)) {
+      const vec3 ldir = B.to_world(bwi);
+      float wpdf = 0.0f;
+      const vec3 Li = distant_eval_li(S, L, ldir, &wpdf);
+      if (max_component(Li) > kMinColorEps) {
+        const vec3 so = offset_ray_origin(c.p, c.p_err, ldir, c.ng);
+        const bool tb = dot(-c.ray_dir, c.ng) * dot(ldir, c.ng) < 0.0f;
+        const bool invalid = (!same_hemisphere(wo, bwi) && !tb) || (same_hemisphere(wo, bwi) && tb);
+        if (!invalid) {
+          ++*shadow_rays;
+          if (!trace_occluded(S, st, so, normalize(ldir), kTMax, tests, nodes)) {
+            const vec3 tr = surface_shadow_tr<kVol>(S, st, c, so, ldir, kTMax, tb, hs, errors, tests, nodes);
+            const float mis = power_heuristic(bpdf, wpdf);
+            direct += mis * tr * vmin(bw, vec3(kMaxColorClamp)) * vmin(Li, vec3(kMaxColorClamp));
+          }
+        }
+      }
+    }
+  }
+  return direct / select_pdf;
+}
+
+// EvalVolumeShapeLight / EvalVolumeDistantLight (src/Shading.cu:202-291, 419-513):
+// next-event estimation at a scattering point inside the media.
+__device__ __noinline__ vec3 eval_volume_lights(const DeviceScene& S, TraversalStack& st, bool distant, int n,
+                                                const float* gs, const float* vw, vec3 ray_dir, const RayTransfer& rt,
+                                                vec3 pos, HaltonState& hs, uint32_t* shadow_rays, uint32_t* tests,
+                                                uint32_t* nodes, uint32_t* errors) {
+  vec3 direct(0.0f);
+  if (distant) {
+    if (S.distant_light_count == 0 || n == 0) return vec3(0.0f);
+    const float select_pdf = 1.0f / float(S.distant_light_count);
+    const int li = gmax(gmin((int)(halton_next(hs, S.halton_perm) * S.distant_light_count), (int)S.distant_light_count - 1), 0);
+    const DistantLight L = S.distant_lights[li];
+    {
+      float u0, u1;
+      halton_next2(hs, S.halton_perm, &u0, &u1);
+      vec3 ldir(0.0f), Li(0.0f);
+      float lpdf = 0.0f;
+      distant_sample_li(S, L, u0, u1, &ldir, &Li, &lpdf);
+      float wpdf = 0.0f;
+      const float pw = eval_mixed_phases(vw, gs, n, -ray_dir, ldir, &wpdf);
+      if (pw > kMinColorEps) {
+        ++*shadow_rays;
+        if (!trace_occluded(S, st, pos, normalize(ldir), kTMax, tests, nodes)) {
+          RayTransfer srt = rt;
+          const vec3 tr = trace_tr(S, st, pos, normalize(ldir), kTMax, kEmpty, kEmpty, srt, hs, errors, tests, nodes);
+          const float mis = power_heuristic(lpdf, wpdf);
+          direct += mis * tr * gmin(pw, kMaxColorClamp) * vmin(Li, vec3(kMaxColorClamp));
+        }
+      }
+    }
+    {
+      float u0, u1;
+      halton_next2(hs, S.halton_perm, &u0, &u1);
+      vec3 pwi;
+      float pspdf = 0.0f, pw = 0.0f;
+      if (sample_mixed_phases(vw, gs, n, u0, u1, -ray_dir, &pw, &pwi, &pspdf)) {
+        float wpdf = 0.0f;
+        const vec3 Li = distant_eval_li(S, L, pwi, &wpdf);
+        if (max_component(Li) > kMinColorEps) {
+          ++*shadow_rays;
+          if (!trace_occluded(S, st, pos, normalize(pwi), kTMax, tests, nodes)) {
+            RayTransfer srt = rt;
+            const vec3 tr = trace_tr(S, st, pos, normalize(pwi), kTMax, kEmpty, kEmpty, srt, hs, errors, tests, nodes);
+            const float mis = power_heuristic(pspdf, wpdf);
+            direct += mis * tr * gmin(pw, kMaxColorClamp) * vmin(Li, vec3(kMaxColorClamp));
+          }
+        }
+      }
+    }
+    return direct / select_pdf;
+  }
+  if (S.shape_light_count == 0 || n == 0) return vec3(0.0f);
+  float select_pdf = 0.0f;
+  const int li = sample_light_power(S, halton_next(hs, S.halton_perm), &select_pdf);
+  const ShapeLight L = S.shape_lights[li];
+  const LightTri lt = load_light_tri(S, L);
+  {
+    float u0, u1;
+    halton_next2(hs, S.halton_perm, &u0, &u1);
+    vec3 ldir(0.0f), lpos(0.0f), lerr(0.0f), lng(0.0f), Li(0.0f);
+    float lpdf = 0.0f;
+    const bool valid = light_sample_li(lt, L.area, pos, u0, u1, &ldir, &lpos, &lerr, &lng, &Li, &lpdf);
+    float wpdf = 0.0f;
+    const float pw = eval_mixed_phases(vw, gs, n, -ray_dir, ldir, &wpdf);
+    if (pw > kMinColorEps && valid) {
+      const float maxd = length(offset_ray_origin(lpos, lerr, -ldir, lng) - pos) * kShadowRayClamp;
+      ++*shadow_rays;
+      if (!trace_occluded(S, st, pos, normalize(ldir), maxd, tests, nodes)) {
+        RayTransfer srt = rt;
+        const vec3 tr = trace_tr(S, st, pos, normalize(ldir), maxd, kEmpty, kEmpty, srt, hs, errors, tests, nodes);
+        const float mis = power_heuristic(lpdf, wpdf);
+        direct += mis * tr * gmin(pw, kMaxColorClamp) * vmin(Li, vec3(kMaxColorClamp));
+      }
+    }
+  }
+  {
+    float u0, u1;
+    halton_next2(hs, S.halton_perm, &u0, &u1);
+    vec3 pwi;
+    float pspdf = 0.0f, pw = 0.0f;
+    if (sample_mixed_phases(vw, gs, n, u0, u1, -ray_dir, &pw, &pwi, &pspdf)) {
+      vec3 lpos(0.0f), lerr(0.0f), lng(0.0f);
+      float wpdf = 0.0f;
+      const vec3 Li = light_eval_li(lt, L.area, pos, pwi, &lpos, &lerr, &lng, &wpdf);
+      if (max_component(Li) > kMinColorEps) {
+        const float maxd = length(offset_ray_origin(lpos, lerr, -pwi, lng) - pos) * kShadowRayClamp;
+        ++*shadow_rays;
+        if (!trace_occluded(S, st, pos, normalize(pwi), maxd, tests, nodes)) {
+          RayTransfer srt = rt;
+          const vec3 tr = trace_tr(S, st, pos, normalize(pwi), maxd, kEmpty, kEmpty, srt, hs, errors, tests, nodes);
+          const float mis = power_heuristic(pspdf, wpdf);
+          direct += mis * tr * gmin(pw, kMaxColorClamp) * vmin(Li, vec3(kMaxColorClamp));
+        }
+      }
+    }
+  }
+  return select_pdf > 0.0f ? (direct / select_pdf) : vec3(0.0f);
+}
+
+template <bool kVol>
 __global__ void __launch_bounds__(kTraceBlock) k_shade(PathPool P, uint32_t count, HitPool H, PathPool Q, float4* image,
                                                        WaveCounters* counters) {
   __shared__ uint32_t s_stack[kStackShared * kTraceBlock];
@@ -337,13 +628,14 @@ __global__ void __launch_bounds__(kTraceBlock) k_shade(PathPool P, uint32_t coun
   RayTransfer rt;
   rt.record_count = 0;
   rt.max_priority_record_index = -1;
-  bool write_transfer = false;
 
   if (active) {
     const DeviceScene& S = c_scene;
     const RenderSetting& rs = c_setting;
+    uint32_t* errors = &counters->errors;
     const float4 o4 = P.ray_o[i], d4 = P.ray_d[i], t4 = P.throughput[i], r4 = P.radiance[i];
-    const vec3 ro(o4.x, o4.y, o4.z), rd(d4.x, d4.y, d4.z);
+    const vec3 rd(d4.x, d4.y, d4.z);
+    (void)o4;
     tp = vec3(t4.x, t4.y, t4.z);
     rad = vec3(r4.x, r4.y, r4.z);
     const uint4 s4 = P.sampler[i];
@@ -358,109 +650,159 @@ __global__ void __launch_bounds__(kTraceBlock) k_shade(PathPool P, uint32_t coun
     const uint4 ids = H.ids[i];
     const vec3 bary(bt.x, bt.y, bt.z);
     const uint32_t inst_idx = ids.x, tri = ids.y;
-    const int hit_back = (int)ids.z;
-    NearbyHit nb[kMaxNearby];
-    const int n_nb = (int)(ids.w & 0xFFu);
-    if (ids.w & kNearbyExplicit) {
-      for (int k = 0; k < n_nb; ++k) {
-        const uint4 e = H.nearby[(size_t)i * kMaxNearby + k];
-        nb[k] = NearbyHit{e.x, __uint_as_float(e.y), (int)e.z};
-      }
-    } else {
-      nb[0] = NearbyHit{inst_idx, bt.w, hit_back};
-    }
+    const int hit_back = (int)(ids.z & 1u);
+    const bool volume_hit = kVol && (ids.z & 2u);
     const float inv_spp = 1.0f / gmax(rs.ssp, 1);
     TraversalStack st;
     st.sh = s_stack + threadIdx.x;
     st.sp = 0;
     st.overflow = false;
 
-    const SurfacePoint sp = fetch_surface(S, inst_idx, tri, bary);
-    const Instance inst = S.instances[inst_idx];
-    bool done = false;
-    if (!(inst.material_idx < S.material_count)) {
-      accumulate_pixel(image, pf.x, rad, inv_spp);
-      done = true;
-    }
-    const Material& mat = S.materials[done ? 0 : inst.material_idx];
-    uint32_t prio = 0;
-    if (!done) fetch_ior(mat, &prio);
-    if (!done && rt.record_count != 0 && prio < rt.records[rt.max_priority_record_index].ior_priority) {
-      // lower-priority boundary: pass straight through, no depth consumed
-      boundary_transition(S, rt, nb, n_nb, &counters->errors);
-      new_o = offset_ray_origin(sp.p, sp.p_err, rd, sp.ng);
-      new_d = normalize(rd);
-      new_flags = flags_pack(depth, never_scatter, false, 0) | sample_bits;
-      new_last_inst = inst_idx;
-      new_last_tri = tri;
-      alive = true;
-      done = true;
-    }
-    if (!done && inst.treat_as_boundary) {
-      boundary_transition(S, rt, nb, n_nb, &counters->errors);
-      new_o = offset_ray_origin(sp.p, sp.p_err, rd, sp.ng);
-      new_d = normalize(rd);
-      new_flags = flags_pack(depth, never_scatter, false, 0) | sample_bits;
-      new_last_inst = inst_idx;
-      new_last_tri = tri;
-      alive = true;
-      done = true;
-    }
-    if (!done && mat.material_type == kLightMtl) {
-      if (never_scatter) rad += indirect_clamp(rs, tp * mat.light_mtl.light_color * mat.light_mtl.intensity, depth);
-      accumulate_pixel(image, pf.x, rad, inv_spp);
-      done = true;
-    }
-    if (!done) {
-      LayeredBsdf B;
-      init_shading_frame(B, hit_back, rd, sp.ng, sp.ns, sp.dpdu, sp.dpdv);
-      init_layered_lobes(B, mat.default_mtl, rd, hit_back, ray_ior(rt), ex_ior(rt, inst_idx));
+    if (volume_hit) {
+      // Ray_shading_path_tracing volume branch (src/Shading.cu:2066-2126).
+      float vw[kMaxBoundaryRecord], gs[kMaxBoundaryRecord];
+      int vidx[kMaxBoundaryRecord];
+      const int n = current_volumes(rt, S.volume_count, vidx);
+      for (int k = 0; k < n; ++k) {
+        gs[k] = S.volumes[vidx[k]].g;
+        vw[k] = H.vol_w[(size_t)i * kMaxBoundaryRecord + k];
+      }
+      const vec3 pos = bary;
+      if (rs.enable_distant_light)
+        rad += indirect_clamp(rs, tp * eval_volume_lights(S, st, true, n, gs, vw, rd, rt, pos, hs, &shadow_rays, &tests,
+                                                          &nodes, errors), depth);
       if (rs.enable_shape_light)
-        rad += indirect_clamp(rs, tp * eval_shape_light(S, st, B, rd, sp.p, sp.p_err, sp.ng, hs, &shadow_rays, &tests, &nodes),
-                              depth);
-      const vec3 wo = B.to_local(-rd);
-      vec3 w, wi;
-      float pdf = 0.0f;
-      float u0, u1, u2;
-      halton_next3(hs, S.halton_perm, &u0, &u1, &u2);
-      const bool valid = bsdf_sample(B, wo, &w, &wi, &pdf, u0, u1, u2);
-      if (!valid) {
-        accumulate_pixel(image, pf.x, rad, inv_spp);
-      } else {
-        tp *= w;
+        rad += indirect_clamp(rs, tp * eval_volume_lights(S, st, false, n, gs, vw, rd, rt, pos, hs, &shadow_rays,
+                                                          &tests, &nodes, errors), depth);
+      vec3 wi;
+      float pdf = 0.0f, pw = 0.0f;
+      float u0, u1;
+      halton_next2(hs, S.halton_perm, &u0, &u1);
+      bool terminate = !sample_mixed_phases(vw, gs, n, u0, u1, -rd, &pw, &wi, &pdf);
+      if (!terminate) {
+        tp *= pw;
         float rr = gmax(tp.x, gmax(tp.y, tp.z));
         rr = gmin(rr, 1.0f);
-        bool terminate = false;
         if (depth + 1 > rs.ray_depth) {
           if (rs.enable_russian_roulette && halton_next(hs, S.halton_perm) < rr) tp /= gmax(rr, kMinColorEps);
           else terminate = true;
         }
-        if (!terminate) {
-          const vec3 nd = B.to_world(wi);
-          const bool tb = dot(-rd, sp.ng) * dot(nd, sp.ng) < 0.0f;
-          const bool invalid = (!same_hemisphere(wo, wi) && !tb) || (same_hemisphere(wo, wi) && tb);
-          if (invalid) {
-            terminate = true;
-          } else {
-            if (tb) boundary_transition(S, rt, nb, n_nb, &counters->errors);
-            new_o = offset_ray_origin(sp.p, sp.p_err, nd, sp.ng);
-            new_d = normalize(nd);
-            never_scatter = false;
-            depth += 1;
-            if (depth > kMaxRayDepth) {
+      }
+      if (!terminate) {
+        new_o = pos;
+        new_d = normalize(wi);
+        depth += 1;
+        if (depth > kMaxRayDepth) {
+          terminate = true;
+        } else {
+          new_flags = flags_pack(depth, false, false, 0) | sample_bits;
+          new_last_inst = kEmpty;
+          new_last_tri = kEmpty;
+          alive = true;
+        }
+      }
+      if (terminate) accumulate_pixel(image, pf.x, rad, inv_spp);
+    } else {
+      NearbyHit nb[kMaxNearby];
+      const int n_nb = (int)(ids.w & 0xFFu);
+      if (ids.w & kNearbyExplicit) {
+        for (int k = 0; k < n_nb; ++k) {
+          const uint4 e = H.nearby[(size_t)i * kMaxNearby + k];
+          nb[k] = NearbyHit{e.x, __uint_as_float(e.y), (int)e.z};
+        }
+      } else {
+        nb[0] = NearbyHit{inst_idx, bt.w, hit_back};
+      }
+      const SurfacePoint sp = fetch_surface(S, inst_idx, tri, bary);
+      const Instance inst = S.instances[inst_idx];
+      bool done = false;
+      if (!(inst.material_idx < S.material_count)) {
+        accumulate_pixel(image, pf.x, rad, inv_spp);
+        done = true;
+      }
+      const Material& mat = S.materials[done ? 0 : inst.material_idx];
+      uint32_t prio = 0;
+      if (!done) fetch_ior(mat, &prio);
+      if (!done && rt.record_count != 0 && prio < rt.records[rt.max_priority_record_index].ior_priority) {
+        // lower-priority boundary: pass straight through, no depth consumed
+        boundary_transition(S, rt, nb, n_nb, errors);
+        new_o = offset_ray_origin(sp.p, sp.p_err, rd, sp.ng);
+        new_d = normalize(rd);
+        new_flags = flags_pack(depth, never_scatter, false, 0) | sample_bits;
+        new_last_inst = inst_idx;
+        new_last_tri = tri;
+        alive = true;
+        done = true;
+      }
+      if (!done && inst.treat_as_boundary) {
+        boundary_transition(S, rt, nb, n_nb, errors);
+        new_o = offset_ray_origin(sp.p, sp.p_err, rd, sp.ng);
+        new_d = normalize(rd);
+        new_flags = flags_pack(depth, never_scatter, false, 0) | sample_bits;
+        new_last_inst = inst_idx;
+        new_last_tri = tri;
+        alive = true;
+        done = true;
+      }
+      if (!done && mat.material_type == kLightMtl) {
+        if (never_scatter) rad += indirect_clamp(rs, tp * mat.light_mtl.light_color * mat.light_mtl.intensity, depth);
+        accumulate_pixel(image, pf.x, rad, inv_spp);
+        done = true;
+      }
+      if (!done) {
+        LayeredBsdf B;
+        init_shading_frame(B, hit_back, rd, sp.ng, sp.ns, sp.dpdu, sp.dpdv);
+        init_layered_lobes(B, mat.default_mtl, rd, hit_back, ray_ior(rt), ex_ior(rt, inst_idx));
+        const SurfaceNee nc{rd, sp.p, sp.p_err, sp.ng, inst_idx, tri, &rt, nb, n_nb};
+        if (rs.enable_distant_light)
+          rad += indirect_clamp(rs, tp * eval_distant_light<kVol>(S, st, B, nc, hs, &shadow_rays, &tests, &nodes, errors),
+                                depth);
+        if (rs.enable_shape_light)
+          rad += indirect_clamp(rs, tp * eval_shape_light<kVol>(S, st, B, nc, hs, &shadow_rays, &tests, &nodes, errors),
+                                depth);
+        const vec3 wo = B.to_local(-rd);
+        vec3 w, wi;
+        float pdf = 0.0f;
+        float u0, u1, u2;
+        halton_next3(hs, S.halton_perm, &u0, &u1, &u2);
+        const bool valid = bsdf_sample(B, wo, &w, &wi, &pdf, u0, u1, u2);
+        if (!valid) {
+          accumulate_pixel(image, pf.x, rad, inv_spp);
+        } else {
+          tp *= w;
+          float rr = gmax(tp.x, gmax(tp.y, tp.z));
+          rr = gmin(rr, 1.0f);
+          bool terminate = false;
+          if (depth + 1 > rs.ray_depth) {
+            if (rs.enable_russian_roulette && halton_next(hs, S.halton_perm) < rr) tp /= gmax(rr, kMinColorEps);
+            else terminate = true;
+          }
+          if (!terminate) {
+            const vec3 nd = B.to_world(wi);
+            const bool tb = dot(-rd, sp.ng) * dot(nd, sp.ng) < 0.0f;
+            const bool invalid = (!same_hemisphere(wo, wi) && !tb) || (same_hemisphere(wo, wi) && tb);
+            if (invalid) {
               terminate = true;
             } else {
-              new_flags = flags_pack(depth, false, false, 0) | sample_bits;
-              new_last_inst = inst_idx;
-              new_last_tri = tri;
-              alive = true;
+              if (tb) boundary_transition(S, rt, nb, n_nb, errors);
+              new_o = offset_ray_origin(sp.p, sp.p_err, nd, sp.ng);
+              new_d = normalize(nd);
+              never_scatter = false;
+              depth += 1;
+              if (depth > kMaxRayDepth) {
+                terminate = true;
+              } else {
+                new_flags = flags_pack(depth, false, false, 0) | sample_bits;
+                new_last_inst = inst_idx;
+                new_last_tri = tri;
+                alive = true;
+              }
             }
           }
+          if (terminate) accumulate_pixel(image, pf.x, rad, inv_spp);
         }
-        if (terminate) accumulate_pixel(image, pf.x, rad, inv_spp);
       }
     }
-    write_transfer = rt.record_count > 0 || n_rec > 0;
     if (st.overflow) atomicOr(&counters->errors, (uint32_t)kDevErrStack);
   }
   const uint32_t slot = warp_append(&counters->next_count, alive);
@@ -468,7 +810,7 @@ __global__ void __launch_bounds__(kTraceBlock) k_shade(PathPool P, uint32_t coun
     if (slot < Q.capacity) {
       store_path(Q, slot, new_o, new_d, tp, rad, pf.x, new_flags, new_last_inst, new_last_tri, hs);
       Q.transfer_count[slot] = (uint8_t)rt.record_count;
-      if (write_transfer && rt.record_count > 0) Q.transfer[slot] = rt;
+      if (rt.record_count > 0) Q.transfer[slot] = rt;
     } else {
       atomicOr(&counters->errors, (uint32_t)kDevErrQueue);
     }
@@ -585,15 +927,19 @@ void launch_generate(const PathPool& P, uint32_t base, uint32_t count, uint32_t 
 }
 
 void launch_extend(const PathPool& P, uint32_t count, const HitPool& H, float4* image, WaveCounters* counters,
-                   cudaStream_t stream) {
+                   bool volumes, cudaStream_t stream) {
   if (count == 0) return;
-  k_extend<<<(count + kTraceBlock - 1) / kTraceBlock, kTraceBlock, 0, stream>>>(P, count, H, image, counters);
+  const uint32_t blocks = (count + kTraceBlock - 1) / kTraceBlock;
+  if (volumes) k_extend<true><<<blocks, kTraceBlock, 0, stream>>>(P, count, H, image, counters);
+  else k_extend<false><<<blocks, kTraceBlock, 0, stream>>>(P, count, H, image, counters);
 }
 
 void launch_shade(const PathPool& P, uint32_t count, const HitPool& H, const PathPool& Q, float4* image,
-                  WaveCounters* counters, cudaStream_t stream) {
+                  WaveCounters* counters, bool volumes, cudaStream_t stream) {
   if (count == 0) return;
-  k_shade<<<(count + kTraceBlock - 1) / kTraceBlock, kTraceBlock, 0, stream>>>(P, count, H, Q, image, counters);
+  const uint32_t blocks = (count + kTraceBlock - 1) / kTraceBlock;
+  if (volumes) k_shade<true><<<blocks, kTraceBlock, 0, stream>>>(P, count, H, Q, image, counters);
+  else k_shade<false><<<blocks, kTraceBlock, 0, stream>>>(P, count, H, Q, image, counters);
 }
 
 void launch_accumulate(const float4* noise, float4* acc, uint32_t n, int frame_index, cudaStream_t stream) {

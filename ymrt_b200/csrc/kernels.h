@@ -36,9 +36,10 @@ struct PathPool {
 
 // Closest-hit results of one wave, indexed like the path pool.
 struct HitPool {
-  float4* bary_t;   // barycentrics, t
-  uint4* ids;       // instance, triangle, back face, nearby count | kNearbyExplicit
+  float4* bary_t;   // barycentrics (or the scattering position of a volume hit), t
+  uint4* ids;       // instance, triangle, back face | volume hit << 1, nearby count | kNearbyExplicit
   uint4* nearby;    // kMaxNearby entries per slot: prim, t bits, back
+  float* vol_w;     // kMaxBoundaryRecord medium-selection weights per slot (volume hits only)
 };
 
 struct WaveCounters {
@@ -56,9 +57,9 @@ cudaError_t upload_setting(const RenderSetting& rs, cudaStream_t stream);
 void launch_generate(const PathPool& P, uint32_t base, uint32_t count, uint32_t next_tile, uint32_t tiles_x,
                      int frame_index, uint32_t spp, cudaStream_t stream);
 void launch_extend(const PathPool& P, uint32_t count, const HitPool& H, float4* image, WaveCounters* counters,
-                   cudaStream_t stream);
+                   bool volumes, cudaStream_t stream);
 void launch_shade(const PathPool& P, uint32_t count, const HitPool& H, const PathPool& Q, float4* image,
-                  WaveCounters* counters, cudaStream_t stream);
+                  WaveCounters* counters, bool volumes, cudaStream_t stream);
 void launch_accumulate(const float4* noise, float4* acc, uint32_t n, int frame_index, cudaStream_t stream);
 void launch_debug_trace(int n, const float* o, const float* d, const uint32_t* lh, uint32_t* inst, uint32_t* tri,
                         float* t, float* bary, int* back, int* nearby, uint32_t* errors, cudaStream_t stream);

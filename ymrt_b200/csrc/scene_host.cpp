@@ -777,7 +777,9 @@ int load_ymtmp(const std::string& path, HostScene* scene, std::string* error) {
           return rc;
         if (tex.child[0] == kEmpty || tex.child[1] == kEmpty) return bad(open, "fbm texture requires black and white inputs");
         tex.frequency = gmax(0.001f, get_f("frequency", 16.0f));
-        tex.lacunarity = get_f("lacunarity", 2.0f);
+        // The reference's reader has no case for "lacunarity" (the attribute is
+        // accepted and dropped, src/core/YMParser.cpp:1741-1780), so it is always 2.
+        tex.lacunarity = 2.0f;
         tex.gain = get_f("gain", 0.5f);
         tex.layer_count = attrs.count("layer_count") ? std::stoi(attrs["layer_count"]) : 4;
         tex.amplitude = get_f("amplitude", 1.0f);
@@ -790,12 +792,12 @@ int load_ymtmp(const std::string& path, HostScene* scene, std::string* error) {
                type == "NoiseTexturePolkaDot" || type == "NoiseTextureWave") {
       return fail(YMRT_ERR_UNSUPPORTED, type + " textures are not supported (constant and fBm textures are)");
     } else if (type == "DistantLight") {
-      DistantLightRec dl{};
+      DistantLight dl{};
       dl.light_color = vmax(get_v("light_color", vec3(1.0f)), vec3(0.0f));
       if ((rc = get_ref("transform_index", &dl.transform_idx))) return rc;
       if (dl.transform_idx == kEmpty) return bad(open, "distant light requires a transform");
       dl.intensity = gmax(get_f("intensity", 1.0f), 0.0f);
-      dl.theta_max = get_f("theta_max", 5.0f);
+      dl.theta_max = gmax(0.0f, get_f("theta_max", 5.0f));
       dl.cos_theta_max = std::cos(dl.theta_max * static_cast<float>(0.01745329251994329576923690768489));
       names[name] = (uint32_t)scene->distant_lights.size();
       scene->distant_lights.push_back(dl);

@@ -30,15 +30,6 @@ struct HostMesh {
   BBox root_box;                   // root box of the reference's mesh BVH
 };
 
-struct DistantLightRec {
-  vec3 light_color;
-  uint32_t transform_idx;
-  float intensity;
-  float cos_theta_max;
-  float theta_max;
-  float padding;
-};
-
 struct HostScene {
   // camera as written in the file
   vec3 cam_from{0.0f, 0.0f, 10.0f}, cam_look{0.0f, 0.0f, 4.0f};
@@ -51,7 +42,7 @@ struct HostScene {
   std::vector<Material> materials;
   std::vector<Texture> textures;
   std::vector<Volume> volumes;
-  std::vector<DistantLightRec> distant_lights;
+  std::vector<DistantLight> distant_lights;
   std::vector<ShapeLight> shape_lights;
   std::vector<float> shape_light_table;
   CameraDesc camera{};

@@ -82,6 +82,18 @@ struct ShapeLight {
   float area;
 };
 
+// DistantLight, src/Light.h:324-388 (32 bytes): a cone of directions around
+// the light transform's -y axis.
+struct DistantLight {
+  vec3 light_color;
+  uint32_t transform_idx;
+  float intensity;
+  float cos_theta_max;
+  float theta_max;
+  float padding;
+};
+static_assert(sizeof(DistantLight) == 32, "DistantLight layout");
+
 // PrimitiveInstance, src/PrimtiveInstance.h:9-22 (32 bytes).
 struct Instance {
   uint32_t geometry_idx;
@@ -209,6 +221,8 @@ struct DeviceScene {
   // materials, lights, media
   uint32_t material_count;
   const Material* materials;
+  uint32_t distant_light_count;
+  const DistantLight* distant_lights;
   uint32_t shape_light_count;
   const ShapeLight* shape_lights;
   const float* shape_light_table;

@@ -210,6 +210,7 @@ class Scene:
         self.textures = []    # (kind, name, dict)
         self.volumes = []     # (name, transform, sigma_t, albedo, g, density_texture or None)
         self.instances = []   # (name, geometry, transform, material, volume or None, boundary)
+        self.distant_lights = []  # (name, transform, color, intensity, theta_max_deg)
 
     @property
     def triangle_count(self) -> int:
@@ -251,6 +252,10 @@ def write_scene(scene: Scene, path: str) -> str:
     for name, t, s, r in scene.transforms:
         out.append(f'Begin(Transform);\n\tname = "{name}";\n\ttranslate = {_vec(t)};\n\tscale = {_vec(s)};\n'
                    f'\trotate = {_vec(r)};\nEnd(Transform);\n')
+    for name, tr, color, intensity, theta_max in scene.distant_lights:
+        out.append(f'Begin(DistantLight);\n\tname = "{name}";\n\ttransform_index = "{tr}";\n'
+                   f"\tlight_color = {_vec(color)};\n\tintensity = {_f(intensity)};\n\ttheta_max = {_f(theta_max)};\n"
+                   "End(DistantLight);\n")
     for kind, name, attrs in scene.textures:
         out.append(f"Begin({kind});\n\tname = \"{name}\";\n")
         for k, v in attrs.items():
@@ -386,6 +391,10 @@ def volumetric_scene(seed: int = 0) -> Scene:
     s.volumes.append(("smoke_volume", "smoke_transform", (2.0, 2.0, 2.0), (0.9, 0.9, 0.9), 0.0, "density_fbm"))
     s.materials.append(("DefaultMaterial", "smoke_boundary_material", {"ior_n": 1.0, "ior_priority": 1}))
     s.instances.append(("smoke_box", "Geo_Box", "smoke_transform", "smoke_boundary_material", "smoke_volume", True))
+    # a sun shining in through the open front of the box: the light's +y axis
+    # maps to the direction light travels, so rotate it to point back into the box
+    s.transforms.append(("sun_transform", (0.0, 0.0, 0.0), (1.0, 1.0, 1.0), (-110.0, 15.0, 0.0)))
+    s.distant_lights.append(("sun", "sun_transform", (1.0, 0.95, 0.85), 3.0, 5.0))
     return s
 
 
