@@ -53,6 +53,7 @@ def lib():
         L.ymref_lights.argtypes = [vp, vp, vp, vp]
         L.ymref_camera_bytes.argtypes = [vp, vp, i]
         L.ymref_scene_records.argtypes = [vp, i, vp, i]
+        L.ymref_bvh_depths.argtypes = [vp, vp]
         L.ymref_trace.argtypes = [vp, i, vp, vp, vp, vp, vp, vp, vp, vp, vp]
         L.ymref_occluded.argtypes = [vp, i, vp, vp, vp, vp]
         L.ymref_halton.argtypes = [vp, i, vp, vp, vp, i, vp, vp, vp]
@@ -135,6 +136,12 @@ class RefScene:
         buf = np.zeros(512, np.uint8)
         n = lib().ymref_camera_bytes(self.h, _p(buf), buf.size)
         return buf[:n].tobytes()
+
+    def bvh_depths(self) -> np.ndarray:
+        """Depth of each mesh's binary BVH, then of the top-level BVH."""
+        out = np.zeros(self.counts()["geometries"] + 1, np.uint32)
+        lib().ymref_bvh_depths(self.h, _p(out))
+        return out
 
     def records(self, kind: str) -> np.ndarray:
         """Materials, volumes, distant lights (raw 32-bit words of the
@@ -233,6 +240,9 @@ def gpu_lib(exact: bool = False):
         L.ymrefgpu_render_frame.argtypes = [vp, i, i, i, vp]
         L.ymrefgpu_last_error.restype = ctypes.c_char_p
         L.ymrefgpu_last_error.argtypes = [vp]
+        L.ymrefgpu_set_profiling.argtypes = [vp, i]
+        L.ymrefgpu_last_stage_ms.restype = ctypes.c_uint32
+        L.ymrefgpu_last_stage_ms.argtypes = [vp, vp]
         for name in ("ymrefgpu_last_render_ms", "ymrefgpu_last_wall_ms"):
             getattr(L, name).restype = ctypes.c_double
             getattr(L, name).argtypes = [vp]
@@ -272,6 +282,14 @@ class RefGpuScene:
 
     def last_wall_ms(self) -> float:
         return self.L.ymrefgpu_last_wall_ms(self.h)
+
+    def set_profiling(self, on: bool):
+        self.L.ymrefgpu_set_profiling(self.h, int(on))
+
+    def last_stage_ms(self) -> dict:
+        out = np.zeros(3, np.float64)
+        waves = self.L.ymrefgpu_last_stage_ms(self.h, _p(out))
+        return {"generate": float(out[0]), "trace": float(out[1]), "shade": float(out[2]), "waves": int(waves)}
 
     def close(self):
         if self.h:

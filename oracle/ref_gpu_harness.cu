@@ -58,6 +58,10 @@ struct GpuContext {
   ShadowRayData shadow{};
   glm::vec4* image = nullptr;
   double last_ms = 0.0, last_wall_ms = 0.0;
+  bool profile_stages = false;
+  cudaEvent_t st0 = nullptr, st1 = nullptr;
+  double stage_ms[3] = {0.0, 0.0, 0.0};  // generation, trace, shading (profiled frames only)
+  uint32_t waves = 0;
   std::string error;
 };
 
@@ -150,6 +154,8 @@ void* ymrefgpu_scene_load(const char* path, const uint32_t* halton_perm, size_t 
     CUDA_CHECK(cudaStreamCreate(&c->stream));
     CUDA_CHECK(cudaEventCreate(&c->ev0));
     CUDA_CHECK(cudaEventCreate(&c->ev1));
+    CUDA_CHECK(cudaEventCreate(&c->st0));
+    CUDA_CHECK(cudaEventCreate(&c->st1));
     CUDA_CHECK(cudaMalloc(&c->image, sizeof(glm::vec4) * (size_t)width * height));
   } catch (const std::exception& e) {
     fprintf(stderr, "ymrefgpu_scene_load: %s\n", e.what());
@@ -175,6 +181,8 @@ void ymrefgpu_scene_free(void* handle) {
   if (c->image) cudaFree(c->image);
   if (c->ev0) cudaEventDestroy(c->ev0);
   if (c->ev1) cudaEventDestroy(c->ev1);
+  if (c->st0) cudaEventDestroy(c->st0);
+  if (c->st1) cudaEventDestroy(c->st1);
   if (c->stream) cudaStreamDestroy(c->stream);
   c->module.reset();  // frees the meshes' device copies
   delete c;
@@ -236,26 +244,48 @@ int ymrefgpu_render_frame(void* handle, int frame_index, int tile_begin, int til
     const auto wall0 = std::chrono::steady_clock::now();
     CUDA_CHECK(cudaEventRecord(c->ev0, c->stream));
     uint32_t next_tile = (uint32_t)tile_begin;
+    c->stage_ms[0] = c->stage_ms[1] = c->stage_ms[2] = 0.0;
+    c->waves = 0;
+    // Optional per-stage device times (events around each stage launcher; the
+    // loop synchronises after every stage anyway).
+    auto stage_begin = [&]() {
+      if (c->profile_stages) CUDA_CHECK(cudaEventRecord(c->st0, c->stream));
+    };
+    auto stage_end = [&](int k) {
+      if (!c->profile_stages) return;
+      CUDA_CHECK(cudaEventRecord(c->st1, c->stream));
+      CUDA_CHECK(cudaEventSynchronize(c->st1));
+      float ms = 0.0f;
+      CUDA_CHECK(cudaEventElapsedTime(&ms, c->st0, c->st1));
+      c->stage_ms[k] += ms;
+    };
     while (counter_host->shading_ray_counter > 0 || next_tile < t_end) {
       uint32_t batch = (MAX_RAY_COUNT - counter_host->shading_ray_counter) / (TILE_PIXEL_COUNT * spp);
       if (partial) batch = std::min(batch, t_end - next_tile);  // the full-frame loop is the reference's, uncapped
+      ++c->waves;
+      stage_begin();
       RayGenerationPathTracing(frame_index, rs, scene_device, halton_device, counter_device, next_tile, batch, w, h,
                                tiles_x, tiles_y, c->shading, c->stream);
+      stage_end(0);
       next_tile += batch;
       counter_host->shading_ray_counter += batch * spp * TILE_PIXEL_COUNT;
       CUDA_CHECK(cudaMemcpyAsync(counter_device, counter_host, sizeof(RayCounter), cudaMemcpyHostToDevice, c->stream));
       CUDA_CHECK(cudaStreamSynchronize(c->stream));
 
+      stage_begin();
       RayTracePathTracing(frame_index, rs, scene_device, counter_device, counter_host, w, h, c->image, c->shading,
                           c->hits, c->stream);
+      stage_end(1);
       CUDA_CHECK(cudaMemcpyAsync(counter_host, counter_device, sizeof(RayCounter), cudaMemcpyDeviceToHost, c->stream));
       CUDA_CHECK(cudaStreamSynchronize(c->stream));
       counter_host->shading_ray_counter = 0;
       CUDA_CHECK(cudaMemcpyAsync(counter_device, counter_host, sizeof(RayCounter), cudaMemcpyHostToDevice, c->stream));
       CUDA_CHECK(cudaStreamSynchronize(c->stream));
 
+      stage_begin();
       RayShadingPathTracing(frame_index, rs, scene_device, counter_device, counter_host, w, h, c->image, c->shading,
                             c->hits, c->shadow, c->stream);
+      stage_end(2);
       CUDA_CHECK(cudaMemcpyAsync(counter_host, counter_device, sizeof(RayCounter), cudaMemcpyDeviceToHost, c->stream));
       CUDA_CHECK(cudaStreamSynchronize(c->stream));
       counter_host->hit_counter = 0;
@@ -284,5 +314,14 @@ int ymrefgpu_render_frame(void* handle, int frame_index, int tile_begin, int til
 // last frame's wave loop, in milliseconds.
 double ymrefgpu_last_render_ms(void* handle) { return static_cast<GpuContext*>(handle)->last_ms; }
 double ymrefgpu_last_wall_ms(void* handle) { return static_cast<GpuContext*>(handle)->last_wall_ms; }
+
+// Per-stage device times of the last frame rendered with profiling on
+// (generation, trace, shading, in ms) and its wave count.
+void ymrefgpu_set_profiling(void* handle, int on) { static_cast<GpuContext*>(handle)->profile_stages = on != 0; }
+uint32_t ymrefgpu_last_stage_ms(void* handle, double* out3) {
+  auto c = static_cast<GpuContext*>(handle);
+  for (int k = 0; k < 3; ++k) out3[k] = c->stage_ms[k];
+  return c->waves;
+}
 
 }  // extern "C"

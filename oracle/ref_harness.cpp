@@ -291,6 +291,45 @@ int ymref_scene_records(void* handle, int what, uint32_t* out, int cap) {
   return (int)w.size();
 }
 
+// Depth (root = 1) of the reference's binary BVHs: out[g] for mesh g, then
+// out[geometry_count] for the top-level tree. The reference's traversals keep
+// at most depth + 1 entries on a 32-entry stack (src/ShadingUtilities.cuh:147).
+}  // extern "C"
+namespace {
+template <typename Node>
+uint32_t binary_depth(const Node* nodes, size_t count) {
+  if (!nodes || count == 0) return 0;
+  std::vector<std::pair<uint32_t, uint32_t>> todo{{0u, 1u}};
+  uint32_t best = 0;
+  while (!todo.empty()) {
+    auto [n, d] = todo.back();
+    todo.pop_back();
+    best = std::max(best, d);
+    if (n >= count) return 0xFFFFFFFFu;
+    if (nodes[n].internal.left != EMPTY_UINT32) continue;  // leaf
+    todo.push_back({n + 1, d + 1});
+    todo.push_back({nodes[n].internal.right, d + 1});
+  }
+  return best;
+}
+}  // namespace
+extern "C" {
+
+int ymref_bvh_depths(void* handle, uint32_t* out) {
+  auto ctx = static_cast<RefContext*>(handle);
+  auto& geo = GuiModule::Geometries(*ctx->module);
+  for (size_t g = 0; g < geo.size(); ++g) {
+    out[g] = 0;
+    if (geo[g].geometry_type != TRIANGLE_MESH) continue;
+    const auto& tm = geo[g].triangle_mesh;
+    const size_t n = (size_t)std::max<int64_t>(2 * tm.triangle_count - 1, 1);
+    out[g] = binary_depth(tm.GetNodesHost(), n);
+  }
+  auto& top = GuiModule::TopNodes(*ctx->module);
+  out[geo.size()] = binary_depth(top.data(), top.size());
+  return (int)geo.size() + 1;
+}
+
 // The rendering camera after preparation, as raw bytes of the reference's
 // Camera struct (176 bytes on x86-64).
 int ymref_camera_bytes(void* handle, uint8_t* out, int out_len) {

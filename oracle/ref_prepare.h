@@ -48,6 +48,7 @@ class GuiModule {
   static std::vector<DistantLight>& DistantLights(SceneModule& m) { return m.distant_lights; }
   static std::vector<Texture>& Textures(SceneModule& m) { return m.textures; }
   static Camera* Cameras(SceneModule& m) { return m.camera; }
+  static std::vector<TopNode>& TopNodes(SceneModule& m) { return m.top_nodes; }
 };
 
 }  // namespace YMRT

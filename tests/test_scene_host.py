@@ -88,3 +88,15 @@ def test_loader_rejects_bad_input(tmp_path):
     with pytest.raises(Y.YmrtError) as e:  # scene without instances
         Y.HostScene(write(tmp_path, "Begin(Camera);\n\tfov = 30;\nEnd(Camera);\n"), 8, 8)
     assert e.value.code == -1
+
+
+@pytest.mark.parametrize("name", ["cornell", "instanced", "volumetric"])
+def test_reference_bvh_depth_fits_its_stack(name, scene_dir, halton_perm, oracle):
+    """The reference's traversals keep at most depth + 1 node indices on a
+    32-entry stack with no bounds check in release builds
+    (src/ShadingUtilities.cuh:147-212): its device kernels are only run on
+    scenes whose binary BVHs are shallower than that."""
+    from ymrt_b200 import scenes
+    ref = oracle.RefScene(scenes.scene_path(name, 0, scene_dir), halton_perm, 64, 64)
+    depths = ref.bvh_depths()
+    assert depths.max() + 1 <= 32, depths

@@ -23,29 +23,61 @@
 
 namespace ym {
 
-constexpr int kStackShared = 40;  // entries per thread in shared memory
-constexpr int kStackLocal = 40;   // further entries per thread in local memory
+constexpr int kStackShared = 32;  // entries per thread in shared memory
+constexpr int kStackLocal = 64;   // further entries per thread in local memory
 constexpr int kTraceBlock = 128;  // threads per block of the traversal kernels
 
+// Stack entries carry the entry distance of the box that produced them, so a
+// pop can drop entries that lie beyond the current closest hit. An entry with
+// kInstanceEntry set names a top-level instance to enter.
+constexpr uint32_t kInstanceEntry = 0x80000000u;
+
 struct TraversalStack {
-  uint32_t* sh;  // shared-memory column of this thread (stride kTraceBlock)
+  uint32_t* sh;   // shared-memory column of this thread: entries (stride kTraceBlock)
+  float* sht;     // shared-memory column of this thread: entry distances
   uint32_t loc[kStackLocal];
+  float loct[kStackLocal];
   int sp;
   bool overflow;
-  __device__ __forceinline__ void push(uint32_t v) {
-    if (sp < kStackShared) sh[sp * kTraceBlock] = v;
-    else if (sp < kStackShared + kStackLocal) loc[sp - kStackShared] = v;
-    else {
+  __device__ __forceinline__ void bind(uint32_t* shared_entries, float* shared_t) {
+    sh = shared_entries + threadIdx.x;
+    sht = shared_t + threadIdx.x;
+    sp = 0;
+    overflow = false;
+  }
+  __device__ __forceinline__ void push(uint32_t v, float t = 0.0f) {
+    if (sp < kStackShared) {
+      sh[sp * kTraceBlock] = v;
+      sht[sp * kTraceBlock] = t;
+    } else if (sp < kStackShared + kStackLocal) {
+      loc[sp - kStackShared] = v;
+      loct[sp - kStackShared] = t;
+    } else {
       overflow = true;
       return;
     }
     ++sp;
   }
-  __device__ __forceinline__ uint32_t pop() {
+  __device__ __forceinline__ uint32_t pop(float* t) {
     --sp;
-    return sp < kStackShared ? sh[sp * kTraceBlock] : loc[sp - kStackShared];
+    if (sp < kStackShared) {
+      *t = sht[sp * kTraceBlock];
+      return sh[sp * kTraceBlock];
+    }
+    *t = loct[sp - kStackShared];
+    return loc[sp - kStackShared];
   }
 };
+
+// Shared-memory backing of the traversal stacks of one kTraceBlock block.
+#define YM_TRAVERSAL_SHARED(name)                                      \
+  __shared__ uint32_t name##_entries[kStackShared * kTraceBlock];      \
+  __shared__ float name##_t[kStackShared * kTraceBlock]
+
+// The far end of the box-test interval for a ray whose closest hit so far is
+// at t: boxes are widened by 1e-6 relative, and so is this bound, so a box
+// entered beyond it cannot hold a hit at or near t.
+__device__ __forceinline__ float widened_tmax(float t) { return __fmaf_rn(fabsf(t), 1e-6f, t); }
 
 // Ray set-up shared by every triangle test of one object-space ray: the
 // reference recomputes these in each IntersectTri call; they are the same
@@ -183,34 +215,66 @@ __device__ __forceinline__ uint32_t child_meta(const uint32_t meta[2], int c) {
   return (c < 4 ? meta[0] : meta[1]) >> (8 * (c & 3)) & 0xFFu;
 }
 
-// Pushes the hit internal children far-to-near so the nearest is popped first.
-__device__ __forceinline__ void push_sorted(TraversalStack& st, uint32_t hits_internal, const float tnear[8],
-                                            const uint32_t meta[2], uint32_t child_base) {
-  uint32_t idx[8];
-  float key[8];
-  int n = 0;
+// Branch-free ordering of the hit children of one node: keys hold the entry
+// distance (non-negative, so its bits order like the float) with the child
+// slot in the low three bits, misses sort last. The 19-comparator network is
+// the optimal sorting network for 8 keys.
+__device__ __forceinline__ void sort8(uint32_t k[8]) {
+#define YM_CS(a, b)                         \
+  {                                         \
+    const uint32_t lo = min(k[a], k[b]);    \
+    const uint32_t hi = max(k[a], k[b]);    \
+    k[a] = lo;                              \
+    k[b] = hi;                              \
+  }
+  YM_CS(0, 1) YM_CS(2, 3) YM_CS(4, 5) YM_CS(6, 7)
+  YM_CS(0, 2) YM_CS(1, 3) YM_CS(4, 6) YM_CS(5, 7)
+  YM_CS(1, 2) YM_CS(5, 6) YM_CS(0, 4) YM_CS(3, 7)
+  YM_CS(1, 5) YM_CS(2, 6)
+  YM_CS(1, 4) YM_CS(3, 6)
+  YM_CS(2, 4) YM_CS(3, 5)
+  YM_CS(3, 4)
+#undef YM_CS
+}
+
+__device__ __forceinline__ uint32_t child_key(uint32_t mask, const float tnear[8], int c) {
+  return ((mask >> c) & 1u) ? ((__float_as_uint(tnear[c]) & ~7u) | (uint32_t)c) : 0xFFFFFFFFu;
+}
+
+// Pushes the children in `mask` far-to-near (so the nearest pops first), each
+// with its entry distance. Internal children push their node; in a top-level
+// node, leaf children push their instances (tlas_prims) as instance entries.
+__device__ __forceinline__ void push_children(TraversalStack& st, uint32_t internal, uint32_t leaves,
+                                              const float tnear[8], const uint32_t meta[2], uint32_t child_base,
+                                              uint32_t prim_base, const uint32_t* __restrict__ tlas_prims) {
+  const uint32_t mask = internal | leaves;
+  if (mask == 0) return;
+  if ((mask & (mask - 1)) == 0) {  // one child: no ordering needed
+    const int c = __ffs(mask) - 1;
+    const uint32_t m = child_meta(meta, c);
+    if (internal) {
+      st.push(child_base + m, tnear[c]);
+    } else {
+      for (uint32_t k = 0; k < (m >> 5); ++k) st.push(kInstanceEntry | __ldg(tlas_prims + prim_base + (m & 31u) + k), tnear[c]);
+    }
+    return;
+  }
+  uint32_t key[8];
 #pragma unroll
-  for (int c = 0; c < 8; ++c) {
-    if (hits_internal & (1u << c)) {
-      idx[n] = child_base + child_meta(meta, c);
-      key[n] = tnear[c];
-      ++n;
+  for (int c = 0; c < 8; ++c) key[c] = child_key(mask, tnear, c);
+  sort8(key);
+#pragma unroll
+  for (int j = 7; j >= 0; --j) {
+    if (key[j] == 0xFFFFFFFFu) continue;
+    const int c = (int)(key[j] & 7u);
+    const float t = __uint_as_float(key[j] & ~7u);
+    const uint32_t m = child_meta(meta, c);
+    if ((internal >> c) & 1u) {
+      st.push(child_base + m, t);
+    } else {
+      for (uint32_t k = 0; k < (m >> 5); ++k) st.push(kInstanceEntry | __ldg(tlas_prims + prim_base + (m & 31u) + k), t);
     }
   }
-  // insertion sort, descending distance
-  for (int i = 1; i < n; ++i) {
-    const float k = key[i];
-    const uint32_t v = idx[i];
-    int j = i - 1;
-    while (j >= 0 && key[j] < k) {
-      key[j + 1] = key[j];
-      idx[j + 1] = idx[j];
-      --j;
-    }
-    key[j + 1] = k;
-    idx[j + 1] = v;
-  }
-  for (int i = 0; i < n; ++i) st.push(idx[i]);
 }
 
 struct NearbyHit {
@@ -230,6 +294,13 @@ struct ClosestHit {
 
 // Closest hit of one world-space ray (TraceRay, src/ShadingUtilities.cuh:310-431).
 // `volume_only`: traverse only treat_as_boundary instances (TraceVolume, :434-561).
+//
+// One loop serves both levels: each iteration pops one entry -- a top-level
+// node, an instance to enter, or a bottom-level node of the current instance
+// -- so the lanes of a warp run the same node code whatever level they are
+// in. Instance leaves are pushed in distance order with the internal nodes,
+// bottom-level leaves are tested at once, and entries whose box begins
+// beyond the closest hit so far are dropped when popped.
 __device__ __noinline__ bool trace_closest(const DeviceScene& S, TraversalStack& st, vec3 wo, vec3 wd, float tmax,
                                            uint32_t last_inst, uint32_t last_tri, bool volume_only, ClosestHit* out,
                                            uint32_t* tri_tests, uint32_t* node_visits) {
@@ -242,181 +313,192 @@ __device__ __noinline__ bool trace_closest(const DeviceScene& S, TraversalStack&
   int n_nearby = 0;
   NearbyHit* nb = out->nearby;
   const BoxRay wray = make_box_ray(wo, wd);
+
+  // the instance being traversed (inst_base < 0: none)
+  int inst_base = -1;
+  uint32_t inst_idx = 0, wtri_offset = 0;
+  vec3 od(0.0f);
+  TriRay tr;
+  BoxRay br = wray;
+  bool skip_here = false, inst_hit = false;
+  float inst_t = 0.0f, hb0 = 0.0f, hb1 = 0.0f, hb2 = 0.0f, extra_t = kTMax;
+  uint32_t hit_tri = kEmpty, hit_w = 0, extra_w = kEmpty;
+
   st.sp = 0;
-  st.push(0);
-  while (st.sp > 0) {
-    const uint32_t node = st.pop();
+  st.push(0, 0.0f);
+  for (;;) {
+    if (inst_base >= 0 && st.sp == inst_base) {
+      // leaving the instance: record its hit (and the nearby-hit list)
+      if (inst_hit) {
+        vec3 p0, p1, p2;
+        uint32_t tid;
+        load_tri(S.wtris, hit_w, &p0, &p1, &p2, &tid);
+        const vec3 ng = normalize(cross(p1 - p0, p2 - p0));
+        out->t = inst_t;
+        out->b0 = hb0;
+        out->b1 = hb1;
+        out->b2 = hb2;
+        out->inst = inst_idx;
+        out->tri = hit_tri;
+        out->back = dot(ng, od) > 0.0f;
+        hit = true;
+        t_upper = next_float_up(next_float_up(t_ray));
+        t_lower = next_float_down(next_float_down(t_ray));
+        int head = 0, tail = n_nearby - 1;
+        while (head <= tail) {
+          if (nb[head].t > t_lower && nb[head].t < t_upper) ++head;
+          else {
+            const NearbyHit tmp = nb[head];
+            nb[head] = nb[tail];
+            nb[tail] = tmp;
+            --tail;
+          }
+        }
+        n_nearby = head;
+        if (n_nearby < kMaxNearby) nb[n_nearby++] = NearbyHit{inst_idx, inst_t, out->back};
+      } else if (hit && extra_w != kEmpty && extra_t > t_lower && extra_t < t_upper) {
+        vec3 p0, p1, p2;
+        uint32_t tid;
+        load_tri(S.wtris, extra_w, &p0, &p1, &p2, &tid);
+        const vec3 ng = normalize(cross(p1 - p0, p2 - p0));
+        if (n_nearby < kMaxNearby) nb[n_nearby++] = NearbyHit{inst_idx, extra_t, dot(ng, od) > 0.0f};
+      }
+      inst_base = -1;
+    }
+    if (st.sp == 0) break;
+    float etn;
+    uint32_t e = st.pop(&etn);
+    if (etn > widened_tmax(t_ray)) continue;
+    if (e & kInstanceEntry) {
+      inst_idx = e & ~kInstanceEntry;
+      const Instance inst = S.instances[inst_idx];
+      if (volume_only && !inst.treat_as_boundary) continue;
+      const mat4& wto = S.i_transforms[inst.transform_idx];
+      const vec3 oo = xform_point_glm(wto, wo);
+      od = xform_dir_glm(wto, wd);
+      const GeometryDesc& g = S.geometries[inst.geometry_idx];
+      tr = make_tri_ray(oo, od);
+      br = make_box_ray(oo, od);
+      wtri_offset = g.wtri_offset;
+      skip_here = skip_enabled && inst_idx == last_inst;
+      inst_hit = false;
+      extra_t = kTMax;
+      extra_w = kEmpty;
+      inst_base = st.sp;
+      e = g.node_offset;  // continue with the instance's root in this iteration
+    }
+    const bool in_blas = inst_base >= 0;
     ++*node_visits;
     float tn[8];
     uint32_t imask, cbase, pbase, meta[2];
-    const uint32_t hits = intersect_children(tlas, node, wray, t_ray, tn, &imask, &cbase, &pbase, meta);
-    // instance leaves
+    const uint32_t hits =
+        intersect_children(in_blas ? blas : tlas, e, in_blas ? br : wray, t_ray, tn, &imask, &cbase, &pbase, meta);
     uint32_t leaves = hits & ~imask;
-    while (leaves) {
-      const int c = __ffs(leaves) - 1;
-      leaves &= leaves - 1;
-      const uint32_t m = child_meta(meta, c);
-      const uint32_t cnt = m >> 5, off = m & 31u;
-      for (uint32_t k = 0; k < cnt; ++k) {
-        const uint32_t inst_idx = __ldg(S.tlas_prims + pbase + off + k);
-        const Instance inst = S.instances[inst_idx];
-        if (volume_only && !inst.treat_as_boundary) continue;
-        const mat4& wto = S.i_transforms[inst.transform_idx];
-        const vec3 oo = xform_point_glm(wto, wo);
-        const vec3 od = xform_dir_glm(wto, wd);
-        const GeometryDesc& g = S.geometries[inst.geometry_idx];
-        const TriRay tr = make_tri_ray(oo, od);
-        const BoxRay br = make_box_ray(oo, od);
-        const bool skip_here = skip_enabled && inst_idx == last_inst;
-        bool inst_hit = false;
-        float inst_t = 0.0f, hb0 = 0.0f, hb1 = 0.0f, hb2 = 0.0f;
-        uint32_t hit_tri = kEmpty, hit_w = 0;
-        float extra_t = kTMax;
-        uint32_t extra_w = kEmpty;
-        const int base = st.sp;
-        st.push(g.node_offset);
-        while (st.sp > base) {
-          const uint32_t bn = st.pop();
-          ++*node_visits;
-          float btn[8];
-          uint32_t bim, bcb, bpb, bmeta[2];
-          const uint32_t bh = intersect_children(blas, bn, br, t_ray, btn, &bim, &bcb, &bpb, bmeta);
-          uint32_t bl = bh & ~bim;
-          while (bl) {
-            const int bc = __ffs(bl) - 1;
-            bl &= bl - 1;
-            const uint32_t bm = child_meta(bmeta, bc);
-            const uint32_t bcnt = bm >> 5, boff = bm & 31u;
-            for (uint32_t q = 0; q < bcnt; ++q) {
-              const uint32_t wi = g.wtri_offset + bpb + boff + q;
-              vec3 p0, p1, p2;
-              uint32_t tid;
-              load_tri(S.wtris, wi, &p0, &p1, &p2, &tid);
-              if (skip_here && tid == last_tri) continue;
-              float t, e[3], inv;
-              ++*tri_tests;
-              if (!tri_test(tr, p0, p1, p2, &t, e, &inv)) continue;
-              if (t >= kTMin && t < extra_t) {
-                extra_t = t;
-                extra_w = wi;
-              }
-              if (t < kTMin || t > t_ray) continue;
-              t_ray = t;
-              inst_hit = true;
-              inst_t = t;
-              hb0 = e[0] * inv;
-              hb1 = e[1] * inv;
-              hb2 = e[2] * inv;
-              hit_tri = tid;
-              hit_w = wi;
-            }
-          }
-          push_sorted(st, bh & bim, btn, bmeta, bcb);
-        }
-        if (inst_hit) {
+    if (in_blas) {
+      while (leaves) {
+        const int c = __ffs(leaves) - 1;
+        leaves &= leaves - 1;
+        const uint32_t m = child_meta(meta, c);
+        const uint32_t cnt = m >> 5, off = m & 31u;
+        for (uint32_t q = 0; q < cnt; ++q) {
+          const uint32_t wi = wtri_offset + pbase + off + q;
           vec3 p0, p1, p2;
           uint32_t tid;
-          load_tri(S.wtris, hit_w, &p0, &p1, &p2, &tid);
-          const vec3 ng = normalize(cross(p1 - p0, p2 - p0));
-          out->t = inst_t;
-          out->b0 = hb0;
-          out->b1 = hb1;
-          out->b2 = hb2;
-          out->inst = inst_idx;
-          out->tri = hit_tri;
-          out->back = dot(ng, od) > 0.0f;
-          hit = true;
-          t_upper = next_float_up(next_float_up(t_ray));
-          t_lower = next_float_down(next_float_down(t_ray));
-          int head = 0, tail = n_nearby - 1;
-          while (head <= tail) {
-            if (nb[head].t > t_lower && nb[head].t < t_upper) ++head;
-            else {
-              const NearbyHit tmp = nb[head];
-              nb[head] = nb[tail];
-              nb[tail] = tmp;
-              --tail;
-            }
+          load_tri(S.wtris, wi, &p0, &p1, &p2, &tid);
+          if (skip_here && tid == last_tri) continue;
+          float t, ev[3], inv;
+          ++*tri_tests;
+          if (!tri_test(tr, p0, p1, p2, &t, ev, &inv)) continue;
+          if (t >= kTMin && t < extra_t) {
+            extra_t = t;
+            extra_w = wi;
           }
-          n_nearby = head;
-          if (n_nearby < kMaxNearby) nb[n_nearby++] = NearbyHit{inst_idx, inst_t, out->back};
-        } else if (hit && extra_w != kEmpty && extra_t > t_lower && extra_t < t_upper) {
-          vec3 p0, p1, p2;
-          uint32_t tid;
-          load_tri(S.wtris, extra_w, &p0, &p1, &p2, &tid);
-          const vec3 ng = normalize(cross(p1 - p0, p2 - p0));
-          if (n_nearby < kMaxNearby) nb[n_nearby++] = NearbyHit{inst_idx, extra_t, dot(ng, od) > 0.0f};
+          if (t < kTMin || t > t_ray) continue;
+          t_ray = t;
+          inst_hit = true;
+          inst_t = t;
+          hb0 = ev[0] * inv;
+          hb1 = ev[1] * inv;
+          hb2 = ev[2] * inv;
+          hit_tri = tid;
+          hit_w = wi;
         }
       }
+      push_children(st, hits & imask, 0u, tn, meta, cbase, pbase, S.tlas_prims);
+    } else {
+      push_children(st, hits & imask, leaves, tn, meta, cbase, pbase, S.tlas_prims);
     }
-    push_sorted(st, hits & imask, tn, meta, cbase);
   }
   out->nearby_count = n_nearby;
   return hit;
 }
 
 // Any hit within (TMIN, tmax] ignoring boundary-only instances
-// (BVHTraverseShadow, src/ShadingUtilities.cuh:563-635).
+// (BVHTraverseShadow, src/ShadingUtilities.cuh:563-635). Same single loop as
+// trace_closest; children are pushed unordered and the first hit ends it.
 __device__ __noinline__ bool trace_occluded(const DeviceScene& S, TraversalStack& st, vec3 wo, vec3 wd, float tmax,
                                             uint32_t* tri_tests, uint32_t* node_visits) {
   const uint4* tlas = reinterpret_cast<const uint4*>(S.tlas_nodes);
   const uint4* blas = reinterpret_cast<const uint4*>(S.blas_nodes);
   const BoxRay wray = make_box_ray(wo, wd);
+  int inst_base = -1;
+  uint32_t wtri_offset = 0;
+  TriRay tr;
+  BoxRay br = wray;
   st.sp = 0;
-  st.push(0);
-  while (st.sp > 0) {
-    const uint32_t node = st.pop();
+  st.push(0, 0.0f);
+  for (;;) {
+    if (inst_base >= 0 && st.sp == inst_base) inst_base = -1;
+    if (st.sp == 0) break;
+    float etn;
+    uint32_t e = st.pop(&etn);
+    if (e & kInstanceEntry) {
+      const Instance inst = S.instances[e & ~kInstanceEntry];
+      if (inst.treat_as_boundary) continue;
+      const mat4& wto = S.i_transforms[inst.transform_idx];
+      const vec3 oo = xform_point_glm(wto, wo);
+      const vec3 od = xform_dir_glm(wto, wd);
+      const GeometryDesc& g = S.geometries[inst.geometry_idx];
+      tr = make_tri_ray(oo, od);
+      br = make_box_ray(oo, od);
+      wtri_offset = g.wtri_offset;
+      inst_base = st.sp;
+      e = g.node_offset;
+    }
+    const bool in_blas = inst_base >= 0;
     ++*node_visits;
     float tn[8];
     uint32_t imask, cbase, pbase, meta[2];
-    const uint32_t hits = intersect_children(tlas, node, wray, tmax, tn, &imask, &cbase, &pbase, meta);
+    const uint32_t hits =
+        intersect_children(in_blas ? blas : tlas, e, in_blas ? br : wray, tmax, tn, &imask, &cbase, &pbase, meta);
     uint32_t leaves = hits & ~imask;
+    uint32_t internal = hits & imask;
+    while (internal) {
+      const int c = __ffs(internal) - 1;
+      internal &= internal - 1;
+      st.push(cbase + child_meta(meta, c), tn[c]);
+    }
     while (leaves) {
       const int c = __ffs(leaves) - 1;
       leaves &= leaves - 1;
       const uint32_t m = child_meta(meta, c);
       const uint32_t cnt = m >> 5, off = m & 31u;
-      for (uint32_t k = 0; k < cnt; ++k) {
-        const uint32_t inst_idx = __ldg(S.tlas_prims + pbase + off + k);
-        const Instance inst = S.instances[inst_idx];
-        if (inst.treat_as_boundary) continue;
-        const mat4& wto = S.i_transforms[inst.transform_idx];
-        const vec3 oo = xform_point_glm(wto, wo);
-        const vec3 od = xform_dir_glm(wto, wd);
-        const GeometryDesc& g = S.geometries[inst.geometry_idx];
-        const TriRay tr = make_tri_ray(oo, od);
-        const BoxRay br = make_box_ray(oo, od);
-        const int base = st.sp;
-        st.push(g.node_offset);
-        while (st.sp > base) {
-          const uint32_t bn = st.pop();
-          ++*node_visits;
-          float btn[8];
-          uint32_t bim, bcb, bpb, bmeta[2];
-          const uint32_t bh = intersect_children(blas, bn, br, tmax, btn, &bim, &bcb, &bpb, bmeta);
-          uint32_t bl = bh & ~bim;
-          while (bl) {
-            const int bc = __ffs(bl) - 1;
-            bl &= bl - 1;
-            const uint32_t bm = child_meta(bmeta, bc);
-            const uint32_t bcnt = bm >> 5, boff = bm & 31u;
-            for (uint32_t q = 0; q < bcnt; ++q) {
-              vec3 p0, p1, p2;
-              uint32_t tid;
-              load_tri(S.wtris, g.wtri_offset + bpb + boff + q, &p0, &p1, &p2, &tid);
-              float t, e[3], inv;
-              ++*tri_tests;
-              if (!tri_test(tr, p0, p1, p2, &t, e, &inv)) continue;
-              if (t < kTMin || t > tmax) continue;
-              st.sp = 0;
-              return true;
-            }
-          }
-          push_sorted(st, bh & bim, btn, bmeta, bcb);
-        }
+      if (!in_blas) {
+        for (uint32_t k = 0; k < cnt; ++k) st.push(kInstanceEntry | __ldg(S.tlas_prims + pbase + off + k), tn[c]);
+        continue;
+      }
+      for (uint32_t q = 0; q < cnt; ++q) {
+        vec3 p0, p1, p2;
+        uint32_t tid;
+        load_tri(S.wtris, wtri_offset + pbase + off + q, &p0, &p1, &p2, &tid);
+        float t, ev[3], inv;
+        ++*tri_tests;
+        if (!tri_test(tr, p0, p1, p2, &t, ev, &inv)) continue;
+        if (t < kTMin || t > tmax) continue;
+        st.sp = 0;
+        return true;
       }
     }
-    push_sorted(st, hits & imask, tn, meta, cbase);
   }
   return false;
 }

@@ -117,7 +117,7 @@ __global__ void __launch_bounds__(256) k_generate(PathPool P, uint32_t base, uin
 template <bool kVol>
 __global__ void __launch_bounds__(kTraceBlock) k_extend(PathPool P, uint32_t count, HitPool H, float4* image,
                                                         WaveCounters* counters) {
-  __shared__ uint32_t s_stack[kStackShared * kTraceBlock];
+  YM_TRAVERSAL_SHARED(s_stack);
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   uint32_t tests = 0, nodes = 0;
   bool active = i < count;
@@ -130,9 +130,7 @@ __global__ void __launch_bounds__(kTraceBlock) k_extend(PathPool P, uint32_t cou
     const vec3 o(o4.x, o4.y, o4.z), d(d4.x, d4.y, d4.z);
     const uint2 lh = P.last_hit[i];
     TraversalStack st;
-    st.sh = s_stack + threadIdx.x;
-    st.sp = 0;
-    st.overflow = false;
+    st.bind(s_stack_entries, s_stack_t);
     ClosestHit ch;
     bool hit = trace_closest(S, st, o, d, kTMax, lh.x, lh.y, false, &ch, &tests, &nodes);
     overflow = st.overflow;
@@ -615,7 +613,7 @@ __device__ __noinline__ vec3 eval_volume_lights(const DeviceScene& S, TraversalS
 template <bool kVol>
 __global__ void __launch_bounds__(kTraceBlock) k_shade(PathPool P, uint32_t count, HitPool H, PathPool Q, float4* image,
                                                        WaveCounters* counters) {
-  __shared__ uint32_t s_stack[kStackShared * kTraceBlock];
+  YM_TRAVERSAL_SHARED(s_stack);
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   uint32_t shadow_rays = 0, tests = 0, nodes = 0;
   bool alive = false;  // continues into Q
@@ -654,9 +652,7 @@ __global__ void __launch_bounds__(kTraceBlock) k_shade(PathPool P, uint32_t coun
     const bool volume_hit = kVol && (ids.z & 2u);
     const float inv_spp = 1.0f / gmax(rs.ssp, 1);
     TraversalStack st;
-    st.sh = s_stack + threadIdx.x;
-    st.sp = 0;
-    st.overflow = false;
+    st.bind(s_stack_entries, s_stack_t);
 
     if (volume_hit) {
       // Ray_shading_path_tracing volume branch (src/Shading.cu:2066-2126).
@@ -848,13 +844,11 @@ __global__ void __launch_bounds__(kTraceBlock) k_debug_trace(int n, const float*
                                                              const uint32_t* last_hit, uint32_t* inst, uint32_t* tri,
                                                              float* t, float* bary, int* back, int* nearby,
                                                              uint32_t* errors) {
-  __shared__ uint32_t s_stack[kStackShared * kTraceBlock];
+  YM_TRAVERSAL_SHARED(s_stack);
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   TraversalStack st;
-  st.sh = s_stack + threadIdx.x;
-  st.sp = 0;
-  st.overflow = false;
+  st.bind(s_stack_entries, s_stack_t);
   const vec3 o(origin[3 * i], origin[3 * i + 1], origin[3 * i + 2]);
   const vec3 d = normalize(vec3(dir[3 * i], dir[3 * i + 1], dir[3 * i + 2]));
   ClosestHit ch;
@@ -874,13 +868,11 @@ __global__ void __launch_bounds__(kTraceBlock) k_debug_trace(int n, const float*
 
 __global__ void __launch_bounds__(kTraceBlock) k_debug_occluded(int n, const float* origin, const float* dir,
                                                                 const float* tmax, int* occluded, uint32_t* errors) {
-  __shared__ uint32_t s_stack[kStackShared * kTraceBlock];
+  YM_TRAVERSAL_SHARED(s_stack);
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   TraversalStack st;
-  st.sh = s_stack + threadIdx.x;
-  st.sp = 0;
-  st.overflow = false;
+  st.bind(s_stack_entries, s_stack_t);
   const vec3 o(origin[3 * i], origin[3 * i + 1], origin[3 * i + 2]);
   const vec3 d = normalize(vec3(dir[3 * i], dir[3 * i + 1], dir[3 * i + 2]));
   uint32_t tests = 0, nodes = 0;
