@@ -104,6 +104,17 @@ int ymrt_set_queue_capacity(ymrt_context* ctx, uint32_t paths);
 /* When enabled, every stage launch is bracketed by CUDA events and the
  * per-stage times are reported in ymrt_stats (costs a little host time). */
 int ymrt_set_profiling(ymrt_context* ctx, int enable);
+/* Wave-loop options (no counterpart in the reference, whose stages have one
+ * fixed form; results are the same either way up to the order of per-pixel
+ * float additions):
+ *   YMRT_OPT_SORT_HITS     (default 1) shade hits grouped by material lobes
+ *   YMRT_OPT_DEFER_SHADOWS (default 1) queue surface shadow rays and trace
+ *                          them in a separate kernel (not used with volume
+ *                          scattering or the indirect clamp) */
+#define YMRT_OPT_SORT_HITS 1
+#define YMRT_OPT_DEFER_SHADOWS 2
+int ymrt_set_option(ymrt_context* ctx, int option, int value);
+int ymrt_get_option(const ymrt_context* ctx, int option, int* value);
 
 /* ---- scenes ---- */
 /* Parses and prepares a scene on the host (no GPU needed). err may be NULL. */

@@ -174,3 +174,25 @@ def test_converged_cornell_16spp(cornell):
     rmse = float(np.sqrt(np.mean((a[..., :3] - b[..., :3]) ** 2)))
     assert rmse <= 1e-3, rmse
     assert np.allclose(a[..., 3], 1.0, atol=1e-6)
+
+
+@pytest.mark.parametrize("sort_hits,defer_shadows", [(0, 0), (1, 0), (0, 1), (1, 1)])
+def test_wave_options_keep_per_sample_radiance(ctx, cornell, sort_hits, defer_shadows):
+    """Listing hits by shading bucket and deferring shadow rays to their own
+    kernel change only the order of per-pixel float additions."""
+    ours, ref = cornell
+    before = {k: ctx.get_option(k) for k in ("sort_hits", "defer_shadows")}
+    try:
+        ctx.set_option("sort_hits", sort_hits)
+        ctx.set_option("defer_shadows", defer_shadows)
+        s = Y.default_setting(spp=1, ray_depth=8)
+        ref.set_settings(spp=1, ray_depth=8)
+        a, stats = ours.render(s, 4)
+        b = ref.render_frame(4)
+        assert np.array_equal(a[..., 3], b[..., 3])
+        bad = _compare_radiance(a, b)
+        assert bad.mean() <= 2e-3, f"{bad.sum()} of {bad.size} pixels differ beyond 1e-5 relative"
+        assert stats.device_errors == 0
+    finally:
+        for k, v in before.items():
+            ctx.set_option(k, v)

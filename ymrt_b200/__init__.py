@@ -97,6 +97,8 @@ def library():
     L.ymrt_last_error.argtypes = [vp]
     L.ymrt_set_queue_capacity.argtypes = [vp, ctypes.c_uint32]
     L.ymrt_set_profiling.argtypes = [vp, i]
+    L.ymrt_set_option.argtypes = [vp, i, i]
+    L.ymrt_get_option.argtypes = [vp, i, ctypes.POINTER(i)]
     L.ymrt_scene_load_ymtmp.argtypes = [ctypes.c_char_p, i, i, ctypes.POINTER(vp), ctypes.c_char_p, sz]
     L.ymrt_host_scene_free.argtypes = [vp]
     L.ymrt_host_scene_query.restype = ctypes.c_longlong
@@ -123,16 +125,30 @@ def _check(rc: int, ctx=None):
         raise YmrtError(rc, msg)
 
 
+OPTIONS = {"sort_hits": 1, "defer_shadows": 2}
+
+
 class Context:
     """One CUDA device + stream (the reference's RenderModule path-tracing stream)."""
 
-    def __init__(self, device: int = 0, queue_capacity: int = 0, profiling: bool = False):
+    def __init__(self, device: int = 0, queue_capacity: int = 0, profiling: bool = False, **options):
         self.h = ctypes.c_void_p()
         _check(library().ymrt_create(device, ctypes.byref(self.h)))
         if queue_capacity:
             library().ymrt_set_queue_capacity(self.h, queue_capacity)
         if profiling:
             library().ymrt_set_profiling(self.h, 1)
+        for name, value in options.items():
+            self.set_option(name, value)
+
+    def set_option(self, name: str, value) -> None:
+        """Wave-loop options: sort_hits, defer_shadows (see include/ymrt.h)."""
+        _check(library().ymrt_set_option(self.h, OPTIONS[name], int(value)))
+
+    def get_option(self, name: str) -> int:
+        v = ctypes.c_int()
+        _check(library().ymrt_get_option(self.h, OPTIONS[name], ctypes.byref(v)))
+        return v.value
 
     def close(self):
         if self.h:

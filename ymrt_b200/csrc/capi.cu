@@ -81,6 +81,11 @@ struct ymrt_context {
   bool profiling = false;
   cudaEvent_t ev_stage[4] = {nullptr, nullptr, nullptr, nullptr};
   std::vector<uint32_t> primes, prime_sums;
+  // wave options (ymrt_set_option)
+  bool sort_hits = true;
+  bool defer_shadows = true;
+  DeviceBuffer shadow_buf;
+  ShadowQueue shadow_queue{};
 
   int fail(int code, const std::string& msg) {
     error = msg;
@@ -113,18 +118,57 @@ struct ymrt_context {
       P.transfer_count = reinterpret_cast<uint8_t*>(p);
       P.capacity = capacity;
     }
-    const size_t hit_bytes = n * (sizeof(float4) + sizeof(uint4) + kMaxNearby * sizeof(uint4) + kMaxBoundaryRecord * sizeof(float));
+    const size_t hit_bytes = n * (sizeof(float4) + sizeof(uint4) + kMaxNearby * sizeof(uint4) +
+                                  kMaxBoundaryRecord * sizeof(float) + sizeof(uint32_t) + 1);
     cudaError_t e = hit_buf.ensure(hit_bytes);
     if (e != cudaSuccess) return cuda_fail(e, "allocating hit pool");
     char* h = hit_buf.as<char>();
     hits.bary_t = reinterpret_cast<float4*>(h); h += n * sizeof(float4);
     hits.ids = reinterpret_cast<uint4*>(h); h += n * sizeof(uint4);
     hits.nearby = reinterpret_cast<uint4*>(h); h += n * kMaxNearby * sizeof(uint4);
-    hits.vol_w = reinterpret_cast<float*>(h);
+    hits.vol_w = reinterpret_cast<float*>(h); h += n * kMaxBoundaryRecord * sizeof(float);
+    hits.order = reinterpret_cast<uint32_t*>(h); h += n * sizeof(uint32_t);
+    hits.bucket = reinterpret_cast<uint8_t*>(h);
     pool_capacity = capacity;
+    shadow_queue = ShadowQueue{};
+    return YMRT_OK;
+  }
+
+  // Deferred shadow rays: at most kShadowRaysPerVertex per shaded path.
+  static constexpr uint32_t kShadowRaysPerVertex = 4;
+  int ensure_shadow_queue() {
+    const size_t n = (size_t)pool_capacity * kShadowRaysPerVertex;
+    if (shadow_queue.capacity == n) return YMRT_OK;
+    cudaError_t e = shadow_buf.ensure(n * 3 * sizeof(float4));
+    if (e != cudaSuccess) return cuda_fail(e, "allocating shadow-ray queue");
+    float4* q = shadow_buf.as<float4>();
+    shadow_queue = ShadowQueue{q, q + n, q + 2 * n, (uint32_t)n};
     return YMRT_OK;
   }
 };
+
+namespace {
+
+// Shading bucket of a hit on `inst`: pass-through boundaries, lights and
+// invalid materials share the cheap bucket; a default material's bucket is
+// the set of lobes its constant parameters switch on (the lobes
+// init_layered_lobes builds), so hits in one bucket run the same BSDF code.
+uint32_t shading_bucket(const HostScene& s, const Instance& inst) {
+  if (inst.treat_as_boundary || inst.material_idx >= s.materials.size()) return kBucketCheap;
+  const Material& m = s.materials[inst.material_idx];
+  if (m.material_type != kDefaultMtl) return kBucketCheap;
+  const DefaultMtl& d = m.default_mtl;
+  const bool not_metal = d.metalness < 1.0f;
+  uint32_t mask = 0;
+  if (d.coat_weight > 0.0f) mask |= 1u;
+  if (d.metalness > 0.0f) mask |= 2u;
+  if (not_metal && d.specular_weight > 0.0f) mask |= 4u;
+  if (not_metal && d.transmission_weight > 0.0f) mask |= 8u;
+  if (not_metal && d.transmission_weight < 1.0f) mask |= 16u;
+  return kBucketLobes + mask;
+}
+
+}  // namespace
 
 struct ymrt_scene {
   ymrt_context* ctx = nullptr;
@@ -213,6 +257,24 @@ int ymrt_set_profiling(ymrt_context* ctx, int enable) {
   if (!ctx) return YMRT_ERR_INVALID;
   ctx->profiling = enable != 0;
   return YMRT_OK;
+}
+
+int ymrt_set_option(ymrt_context* ctx, int option, int value) {
+  if (!ctx) return YMRT_ERR_INVALID;
+  switch (option) {
+    case YMRT_OPT_SORT_HITS: ctx->sort_hits = value != 0; return YMRT_OK;
+    case YMRT_OPT_DEFER_SHADOWS: ctx->defer_shadows = value != 0; return YMRT_OK;
+    default: return ctx->fail(YMRT_ERR_INVALID, "unknown option " + std::to_string(option));
+  }
+}
+
+int ymrt_get_option(const ymrt_context* ctx, int option, int* value) {
+  if (!ctx || !value) return YMRT_ERR_INVALID;
+  switch (option) {
+    case YMRT_OPT_SORT_HITS: *value = ctx->sort_hits ? 1 : 0; return YMRT_OK;
+    case YMRT_OPT_DEFER_SHADOWS: *value = ctx->defer_shadows ? 1 : 0; return YMRT_OK;
+    default: return YMRT_ERR_INVALID;
+  }
 }
 
 int ymrt_scene_load_ymtmp(const char* path, int width, int height, ymrt_host_scene** out, char* err, size_t err_len) {
@@ -376,6 +438,11 @@ int ymrt_scene_upload(ymrt_context* ctx, const ymrt_host_scene* hs, const uint32
   UP(s.shape_light_table, shape_light_table);
   UP(s.volumes, volumes);
   UP(s.textures, textures);
+  {
+    std::vector<uint8_t> buckets(s.instances.size());
+    for (size_t i = 0; i < s.instances.size(); ++i) buckets[i] = (uint8_t)shading_bucket(s, s.instances[i]);
+    UP(buckets, inst_bucket);
+  }
 #undef UP
   if (e == cudaSuccess) {
     std::vector<uint32_t> perm(halton_perm, halton_perm + perm_len);
@@ -452,6 +519,14 @@ int ymrt_render_tiles(ymrt_scene* sc, const ymrt_render_setting* setting, int fr
   int rc = ctx->ensure_pools();
   if (rc != YMRT_OK) return rc;
   if (per_tile > ctx->capacity) return ctx->fail(YMRT_ERR_INVALID, "queue capacity smaller than one tile of samples");
+  WaveOptions opt;
+  opt.volumes = volumes;
+  opt.sort_hits = ctx->sort_hits;
+  opt.defer_shadows = ctx->defer_shadows && !volumes && !rs.enable_indirect_clamp;
+  if (opt.defer_shadows) {
+    if ((rc = ctx->ensure_shadow_queue()) != YMRT_OK) return rc;
+    opt.shadow_queue = ctx->shadow_queue;
+  }
   const uint32_t W = sc->width, Hh = sc->height;
   const uint32_t tiles_x = (W + kTileRes - 1) / kTileRes, tiles_y = (Hh + kTileRes - 1) / kTileRes;
   const uint32_t total_tiles = tiles_x * tiles_y;
@@ -481,16 +556,8 @@ int ymrt_render_tiles(ymrt_scene* sc, const ymrt_render_setting* setting, int fr
     const uint32_t gen = n_tiles * per_tile;
     PathPool& A = ctx->pool[a];
     PathPool& B = ctx->pool[a ^ 1];
-    const uint32_t total = live + gen;
-    if (ctx->profiling) cudaEventRecord(ctx->ev_stage[0], st);
-    launch_generate(A, live, gen, cursor, tiles_x, frame_index, spp, st);
-    if (ctx->profiling) cudaEventRecord(ctx->ev_stage[1], st);
-    launch_extend(A, total, ctx->hits, image, dc, volumes, st);
-    if (ctx->profiling) cudaEventRecord(ctx->ev_stage[2], st);
-    cudaMemsetAsync(&dc->next_count, 0, sizeof(uint32_t), st);
-    launch_shade(A, total, ctx->hits, B, image, dc, volumes, st);
-    if (ctx->profiling) cudaEventRecord(ctx->ev_stage[3], st);
-    launches += (gen > 0 ? 1 : 0) + (total > 0 ? 2 : 0);
+    launches += launch_wave(A, B, ctx->hits, live, gen, cursor, tiles_x, frame_index, spp, image, dc, opt,
+                            ctx->profiling ? ctx->ev_stage : nullptr, st);
     if ((e = cudaMemcpyAsync(ctx->counters_host, dc, sizeof(WaveCounters), cudaMemcpyDeviceToHost, st)) != cudaSuccess)
       return ctx->cuda_fail(e, "reading wave counters");
     if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return ctx->cuda_fail(e, "wave");
@@ -580,10 +647,10 @@ constexpr size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 
 // Bytes one path slot needs across both path pools and the hit pool.
 constexpr size_t kPoolSlotBytes = 4 * sizeof(float4) + sizeof(uint4) + 2 * sizeof(uint2) + sizeof(RayTransfer) + 1;
-constexpr size_t kHitSlotBytes = sizeof(float4) + sizeof(uint4) + kMaxNearby * sizeof(uint4);
+constexpr size_t kHitSlotBytes = sizeof(float4) + sizeof(uint4) + kMaxNearby * sizeof(uint4) + sizeof(uint32_t) + 1;
 
 uint32_t noalloc_capacity() {
-  const size_t fixed = align256(sizeof(WaveCounters)) + 16 * 256;  // counters + alignment slack of the carved arrays
+  const size_t fixed = align256(sizeof(WaveCounters)) + 18 * 256;  // counters + alignment slack of the carved arrays
   return (uint32_t)((kNoAllocScratchBytes - fixed) / (2 * kPoolSlotBytes + kHitSlotBytes));
 }
 
@@ -615,6 +682,8 @@ size_t carve(unsigned char* base, uint32_t n, PathPool pools[2], HitPool* hits, 
   hits->ids = reinterpret_cast<uint4*>(take(n * sizeof(uint4)));
   hits->nearby = reinterpret_cast<uint4*>(take(n * kMaxNearby * sizeof(uint4)));
   hits->vol_w = nullptr;  // volume scattering is not rendered by this entry point
+  hits->order = reinterpret_cast<uint32_t*>(take(n * sizeof(uint32_t)));
+  hits->bucket = reinterpret_cast<uint8_t*>(take(n));
   return off;
 }
 
@@ -683,12 +752,8 @@ int ymrt_render_tiles_noalloc(ymrt_scene* sc, const ymrt_render_setting* setting
   while (live > 0 || cursor < t_end) {
     const uint32_t n_tiles = std::min<uint32_t>((cap - live) / per_tile, t_end - cursor);
     const uint32_t gen = n_tiles * per_tile;
-    const uint32_t total = live + gen;
-    launch_generate(pools[a], live, gen, cursor, tiles_x, frame_index, spp, st);
-    launch_extend(pools[a], total, hits, image, dc, false, st);
-    cudaMemsetAsync(&dc->next_count, 0, sizeof(uint32_t), st);
-    launch_shade(pools[a], total, hits, pools[a ^ 1], image, dc, false, st);
-    launches += (gen > 0 ? 1 : 0) + (total > 0 ? 2 : 0);
+    launches += launch_wave(pools[a], pools[a ^ 1], hits, live, gen, cursor, tiles_x, frame_index, spp, image, dc,
+                            WaveOptions{}, nullptr, st);
     if ((e = cudaMemcpyAsync(ctx->counters_host, dc, sizeof(WaveCounters), cudaMemcpyDeviceToHost, st)) != cudaSuccess)
       return ctx->cuda_fail(e, "reading wave counters");
     if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return ctx->cuda_fail(e, "wave");

@@ -19,11 +19,16 @@
 
 #include "dev_sampler.cuh"
 #include "dev_shade.cuh"
+#include <cooperative_groups.h>
+
 #include "dev_traverse.cuh"
 #include "dev_volume.cuh"
 #include "kernels.h"
 
 namespace ym {
+
+namespace cg = cooperative_groups;
+
 
 __constant__ DeviceScene c_scene;
 __constant__ RenderSetting c_setting;
@@ -114,8 +119,46 @@ __global__ void __launch_bounds__(256) k_generate(PathPool P, uint32_t base, uin
 
 // -------------------------------------------------------------- extend ---
 
+// Counts this lane's hit under its shading bucket (kBucketNone: no hit), one
+// atomic per bucket present in the warp, and the warp's hits in hit_count.
+__device__ __forceinline__ void file_bucket(WaveCounters* counters, uint32_t bucket) {
+  const bool has = bucket != kBucketNone;
+  const uint32_t act = __ballot_sync(0xFFFFFFFFu, has);
+  const int lane = threadIdx.x & 31;
+  if (lane == 0 && act) atomicAdd(&counters->hit_count, (uint32_t)__popc(act));
+  if (!has) return;
+  const uint32_t peers = __match_any_sync(act, bucket);
+  if (lane == __ffs(peers) - 1) atomicAdd(&counters->bucket_count[bucket], (uint32_t)__popc(peers));
+}
+
+// Lists the slots holding hits bucket by bucket (a counting sort: the
+// buckets' counts from k_extend give each bucket's start).
+__global__ void __launch_bounds__(256) k_sort_hits(uint32_t count, HitPool H, WaveCounters* counters) {
+  __shared__ uint32_t s_start[kShadeBuckets];
+  if (threadIdx.x == 0) {
+    uint32_t acc = 0;
+    for (int b = 0; b < kShadeBuckets; ++b) {
+      s_start[b] = acc;
+      acc += counters->bucket_count[b];
+    }
+  }
+  __syncthreads();
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t b = i < count ? (uint32_t)H.bucket[i] : (uint32_t)kBucketNone;
+  const bool has = b != kBucketNone;
+  const uint32_t act = __ballot_sync(0xFFFFFFFFu, has);
+  if (!has) return;
+  const int lane = threadIdx.x & 31;
+  const uint32_t peers = __match_any_sync(act, b);
+  const int leader = __ffs(peers) - 1;
+  uint32_t base = 0;
+  if (lane == leader) base = atomicAdd(&counters->bucket_fill[b], (uint32_t)__popc(peers));
+  base = __shfl_sync(peers, base, leader);
+  H.order[s_start[b] + base + (uint32_t)__popc(peers & ((1u << lane) - 1u))] = i;
+}
+
 template <bool kVol>
-__global__ void __launch_bounds__(kTraceBlock) k_extend(PathPool P, uint32_t count, HitPool H, float4* image,
+__global__ void __launch_bounds__(kTraceBlock, 5) k_extend(PathPool P, uint32_t count, HitPool H, float4* image,
                                                         WaveCounters* counters) {
   YM_TRAVERSAL_SHARED(s_stack);
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -124,6 +167,7 @@ __global__ void __launch_bounds__(kTraceBlock) k_extend(PathPool P, uint32_t cou
   uint2 pf = active ? P.pixel_flags[i] : make_uint2(kEmpty, kFlagDead);
   if (active && (pf.y & kFlagDead)) active = false;
   bool overflow = false;
+  uint32_t bucket = kBucketNone;
   if (active) {
     const DeviceScene& S = c_scene;
     const float4 o4 = P.ray_o[i], d4 = P.ray_d[i];
@@ -191,8 +235,11 @@ __global__ void __launch_bounds__(kTraceBlock) k_extend(PathPool P, uint32_t cou
         nearby_word |= kNearbyExplicit;
       }
       H.ids[i] = make_uint4(ch.inst, ch.tri, (uint32_t)ch.back | (volume_hit ? 2u : 0u), nearby_word);
+      bucket = volume_hit ? kBucketVolume : (uint32_t)S.inst_bucket[ch.inst];
     }
   }
+  if (i < count) H.bucket[i] = (uint8_t)bucket;
+  file_bucket(counters, bucket);
   // counters: one atomic per warp
   const uint32_t n_rays = __popc(__ballot_sync(0xFFFFFFFFu, active));
   uint32_t t_sum = tests, n_sum = nodes;
@@ -385,11 +432,62 @@ __device__ __forceinline__ vec3 surface_shadow_tr(const DeviceScene& S, Traversa
   return trace_tr(S, st, so, normalize(ldir), maxd, c.inst, c.tri, srt, hs, errors, tests, nodes);
 }
 
+// Where a surface shadow ray goes when shadow rays are deferred: the queue
+// k_connect traces, the pixel it lights and the path's weight on it
+// (throughput / spp).
+struct ShadowEmit {
+  ShadowQueue q;
+  uint32_t* count;
+  uint32_t* errors;
+  uint32_t pixel;
+  vec3 weight;
+};
+
+// Queues one shadow ray with its contribution (warp-aggregated slot claim
+// over the lanes that reach this point together).
+__device__ __forceinline__ void emit_shadow_ray(const ShadowEmit& em, vec3 o, vec3 d, float maxd, vec3 contribution) {
+  cg::coalesced_group g = cg::coalesced_threads();
+  uint32_t base = 0;
+  if (g.thread_rank() == 0) base = atomicAdd(em.count, g.size());
+  const uint32_t slot = g.shfl(base, 0) + g.thread_rank();
+  if (slot >= em.q.capacity) {
+    atomicOr(em.errors, kDevErrQueue);
+    return;
+  }
+  const vec3 w = em.weight * contribution;
+  em.q.o[slot] = make_float4(o.x, o.y, o.z, maxd);
+  em.q.d[slot] = make_float4(d.x, d.y, d.z, __uint_as_float(em.pixel));
+  em.q.c[slot] = make_float4(w.x, w.y, w.z, 0.0f);
+}
+
+// One next-event shadow ray of a surface vertex toward a light, with MIS
+// weight `mis`, clamped BSDF value fc and radiance Lc; the light-selection
+// pdf enters as (x * mul) / div, the form each estimator uses. Traced here
+// (direct += its unoccluded contribution, times the media transmittance)
+// or, with kDefer, queued for k_connect.
+template <bool kVol, bool kDefer>
+__device__ __forceinline__ void nee_shadow_ray(const DeviceScene& S, TraversalStack& st, const SurfaceNee& c,
+                                               const ShadowEmit& em, vec3 so, vec3 ldir, float maxd, bool tb,
+                                               float mis, vec3 fc, vec3 Lc, float mul, float div, vec3* direct,
+                                               HaltonState& hs, uint32_t* shadow_rays, uint32_t* tests,
+                                               uint32_t* nodes, uint32_t* errors) {
+  ++*shadow_rays;
+  if (kDefer) {
+    emit_shadow_ray(em, so, normalize(ldir), maxd, ((mis * vec3(1.0f) * fc * Lc) * mul) / div);
+    return;
+  }
+  if (!trace_occluded(S, st, so, normalize(ldir), maxd, tests, nodes)) {
+    const vec3 tr = surface_shadow_tr<kVol>(S, st, c, so, ldir, maxd, tb, hs, errors, tests, nodes);
+    *direct += mis * tr * fc * Lc;
+  }
+}
+
 // EvalShapeLight (src/Shading.cu:294-417).
-template <bool kVol>
+template <bool kVol, bool kDefer>
 __device__ __forceinline__ vec3 eval_shape_light(const DeviceScene& S, TraversalStack& st, const LayeredBsdf& B,
-                                                 const SurfaceNee& c, HaltonState& hs, uint32_t* shadow_rays,
-                                                 uint32_t* tests, uint32_t* nodes, uint32_t* errors) {
+                                                 const SurfaceNee& c, const ShadowEmit& em, HaltonState& hs,
+                                                 uint32_t* shadow_rays, uint32_t* tests, uint32_t* nodes,
+                                                 uint32_t* errors) {
   if (S.shape_light_count == 0) return vec3(0.0f);
   vec3 direct(0.0f);
   const vec3 wo = B.to_local(-c.ray_dir);
@@ -411,14 +509,10 @@ __device__ __forceinline__ vec3 eval_shape_light(const DeviceScene& S, Traversal
       const float maxd = length(offset_ray_origin(lpos, lerr, -ldir, lng) - c.p) * kShadowRayClamp;
       const bool tb = dot(-c.ray_dir, c.ng) * dot(ldir, c.ng) < 0.0f;
       const bool invalid = (!same_hemisphere(wo, lwi) && !tb) || (same_hemisphere(wo, lwi) && tb);
-      if (!invalid) {
-        ++*shadow_rays;
-        if (!trace_occluded(S, st, so, normalize(ldir), maxd, tests, nodes)) {
-          const vec3 tr = surface_shadow_tr<kVol>(S, st, c, so, ldir, maxd, tb, hs, errors, tests, nodes);
-          const float mis = power_heuristic(lpdf, wpdf);
-          direct += mis * tr * vmin(f, vec3(kMaxColorClamp)) * vmin(Li, vec3(kMaxColorClamp));
-        }
-      }
+      if (!invalid)
+        nee_shadow_ray<kVol, kDefer>(S, st, c, em, so, ldir, maxd, tb, power_heuristic(lpdf, wpdf),
+                                     vmin(f, vec3(kMaxColorClamp)), vmin(Li, vec3(kMaxColorClamp)),
+                                     safe_rcp(select_pdf), 1.0f, &direct, hs, shadow_rays, tests, nodes, errors);
     }
   }
   {
@@ -436,14 +530,10 @@ __device__ __forceinline__ vec3 eval_shape_light(const DeviceScene& S, Traversal
         const float maxd = length(offset_ray_origin(lpos, lerr, -ldir, lng) - c.p) * kShadowRayClamp;
         const bool tb = dot(-c.ray_dir, c.ng) * dot(ldir, c.ng) < 0.0f;
         const bool invalid = (!same_hemisphere(wo, bwi) && !tb) || (same_hemisphere(wo, bwi) && tb);
-        if (!invalid) {
-          ++*shadow_rays;
-          if (!trace_occluded(S, st, so, normalize(ldir), maxd, tests, nodes)) {
-            const vec3 tr = surface_shadow_tr<kVol>(S, st, c, so, ldir, maxd, tb, hs, errors, tests, nodes);
-            const float mis = power_heuristic(bpdf, wpdf);
-            direct += mis * tr * vmin(bw, vec3(kMaxColorClamp)) * vmin(Li, vec3(kMaxColorClamp));
-          }
-        }
+        if (!invalid)
+          nee_shadow_ray<kVol, kDefer>(S, st, c, em, so, ldir, maxd, tb, power_heuristic(bpdf, wpdf),
+                                       vmin(bw, vec3(kMaxColorClamp)), vmin(Li, vec3(kMaxColorClamp)),
+                                       safe_rcp(select_pdf), 1.0f, &direct, hs, shadow_rays, tests, nodes, errors);
       }
     }
   }
@@ -451,10 +541,11 @@ __device__ __forceinline__ vec3 eval_shape_light(const DeviceScene& S, Traversal
 }
 
 // EvalDistantLight (src/Shading.cu:83-198).
-template <bool kVol>
+template <bool kVol, bool kDefer>
 __device__ __forceinline__ vec3 eval_distant_light(const DeviceScene& S, TraversalStack& st, const LayeredBsdf& B,
-                                                   const SurfaceNee& c, HaltonState& hs, uint32_t* shadow_rays,
-                                                   uint32_t* tests, uint32_t* nodes, uint32_t* errors) {
+                                                   const SurfaceNee& c, const ShadowEmit& em, HaltonState& hs,
+                                                   uint32_t* shadow_rays, uint32_t* tests, uint32_t* nodes,
+                                                   uint32_t* errors) {
   if (S.distant_light_count == 0) return vec3(0.0f);
   vec3 direct(0.0f);
   const vec3 wo = B.to_local(-c.ray_dir);
@@ -474,14 +565,10 @@ __device__ __forceinline__ vec3 eval_distant_light(const DeviceScene& S, Travers
       const vec3 so = offset_ray_origin(c.p, c.p_err, ldir, c.ng);
       const bool tb = dot(-c.ray_dir, c.ng) * dot(ldir, c.ng) < 0.0f;
       const bool invalid = (!same_hemisphere(wo, lwi) && !tb) || (same_hemisphere(wo, lwi) && tb);
-      if (!invalid) {
-        ++*shadow_rays;
-        if (!trace_occluded(S, st, so, normalize(ldir), kTMax, tests, nodes)) {
-          const vec3 tr = surface_shadow_tr<kVol>(S, st, c, so, ldir, kTMax, tb, hs, errors, tests, nodes);
-          const float mis = power_heuristic(lpdf, wpdf);
-          direct += mis * tr * vmin(f, vec3(kMaxColorClamp)) * vmin(Li, vec3(kMaxColorClamp));
-        }
-      }
+      if (!invalid)
+        nee_shadow_ray<kVol, kDefer>(S, st, c, em, so, ldir, kTMax, tb, power_heuristic(lpdf, wpdf),
+                                     vmin(f, vec3(kMaxColorClamp)), vmin(Li, vec3(kMaxColorClamp)), 1.0f,
+                                     select_pdf, &direct, hs, shadow_rays, tests, nodes, errors);
     }
   }
   {
@@ -497,14 +584,10 @@ __device__ __forceinline__ vec3 eval_distant_light(const DeviceScene& S, Travers
         const vec3 so = offset_ray_origin(c.p, c.p_err, ldir, c.ng);
         const bool tb = dot(-c.ray_dir, c.ng) * dot(ldir, c.ng) < 0.0f;
         const bool invalid = (!same_hemisphere(wo, bwi) && !tb) || (same_hemisphere(wo, bwi) && tb);
-        if (!invalid) {
-          ++*shadow_rays;
-          if (!trace_occluded(S, st, so, normalize(ldir), kTMax, tests, nodes)) {
-            const vec3 tr = surface_shadow_tr<kVol>(S, st, c, so, ldir, kTMax, tb, hs, errors, tests, nodes);
-            const float mis = power_heuristic(bpdf, wpdf);
-            direct += mis * tr * vmin(bw, vec3(kMaxColorClamp)) * vmin(Li, vec3(kMaxColorClamp));
-          }
-        }
+        if (!invalid)
+          nee_shadow_ray<kVol, kDefer>(S, st, c, em, so, ldir, kTMax, tb, power_heuristic(bpdf, wpdf),
+                                       vmin(bw, vec3(kMaxColorClamp)), vmin(Li, vec3(kMaxColorClamp)), 1.0f,
+                                       select_pdf, &direct, hs, shadow_rays, tests, nodes, errors);
       }
     }
   }
@@ -610,15 +693,23 @@ __device__ __noinline__ vec3 eval_volume_lights(const DeviceScene& S, TraversalS
   return select_pdf > 0.0f ? (direct / select_pdf) : vec3(0.0f);
 }
 
-template <bool kVol>
+// kDefer (surfaces only, no indirect clamp): next-event shadow rays are queued
+// for k_connect instead of traced here, which keeps traversal out of this
+// kernel.
+template <bool kVol, bool kDefer>
 __global__ void __launch_bounds__(kTraceBlock) k_shade(PathPool P, uint32_t count, HitPool H, PathPool Q, float4* image,
-                                                       WaveCounters* counters) {
-  YM_TRAVERSAL_SHARED(s_stack);
-  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+                                                       WaveCounters* counters, ShadowQueue shadow_q) {
+  static_assert(!(kVol && kDefer), "volume transmittance needs the path's sampler: shadow rays are traced inline");
+  // The path slot this thread shades: the t-th listed hit, or (hits not
+  // listed by bucket) slot t itself when it holds a hit.
+  const uint32_t t_idx = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool listed = H.order != nullptr;
+  bool active = t_idx < count && (!listed || t_idx < counters->hit_count);
+  const uint32_t i = active ? (listed ? H.order[t_idx] : t_idx) : 0u;
   uint32_t shadow_rays = 0, tests = 0, nodes = 0;
   bool alive = false;  // continues into Q
-  uint2 pf = i < count ? P.pixel_flags[i] : make_uint2(kEmpty, kFlagDead);
-  const bool active = i < count && !(pf.y & kFlagDead);
+  const uint2 pf = active ? P.pixel_flags[i] : make_uint2(kEmpty, kFlagDead);
+  if (pf.y & kFlagDead) active = false;  // a miss (already accumulated) or an empty slot
 
   vec3 new_o, new_d, tp, rad;
   uint32_t new_flags = 0, new_last_inst = kEmpty, new_last_tri = kEmpty;
@@ -652,7 +743,13 @@ __global__ void __launch_bounds__(kTraceBlock) k_shade(PathPool P, uint32_t coun
     const bool volume_hit = kVol && (ids.z & 2u);
     const float inv_spp = 1.0f / gmax(rs.ssp, 1);
     TraversalStack st;
-    st.bind(s_stack_entries, s_stack_t);
+    if constexpr (!kDefer) {
+      YM_TRAVERSAL_SHARED(s_stack);
+      st.bind(s_stack_entries, s_stack_t);
+    } else {
+      st.sp = 0;
+      st.overflow = false;
+    }
 
     if (volume_hit) {
       // Ray_shading_path_tracing volume branch (src/Shading.cu:2066-2126).
@@ -750,12 +847,15 @@ __global__ void __launch_bounds__(kTraceBlock) k_shade(PathPool P, uint32_t coun
         init_shading_frame(B, hit_back, rd, sp.ng, sp.ns, sp.dpdu, sp.dpdv);
         init_layered_lobes(B, mat.default_mtl, rd, hit_back, ray_ior(rt), ex_ior(rt, inst_idx));
         const SurfaceNee nc{rd, sp.p, sp.p_err, sp.ng, inst_idx, tri, &rt, nb, n_nb};
+        const ShadowEmit em{shadow_q, &counters->shadow_count, errors, pf.x, tp * inv_spp};
         if (rs.enable_distant_light)
-          rad += indirect_clamp(rs, tp * eval_distant_light<kVol>(S, st, B, nc, hs, &shadow_rays, &tests, &nodes, errors),
-                                depth);
+          rad += indirect_clamp(
+              rs, tp * eval_distant_light<kVol, kDefer>(S, st, B, nc, em, hs, &shadow_rays, &tests, &nodes, errors),
+              depth);
         if (rs.enable_shape_light)
-          rad += indirect_clamp(rs, tp * eval_shape_light<kVol>(S, st, B, nc, hs, &shadow_rays, &tests, &nodes, errors),
-                                depth);
+          rad += indirect_clamp(
+              rs, tp * eval_shape_light<kVol, kDefer>(S, st, B, nc, em, hs, &shadow_rays, &tests, &nodes, errors),
+              depth);
         const vec3 wo = B.to_local(-rd);
         vec3 w, wi;
         float pdf = 0.0f;
@@ -822,6 +922,37 @@ __global__ void __launch_bounds__(kTraceBlock) k_shade(PathPool P, uint32_t coun
     if (t_sum) atomicAdd(&counters->tri_tests, (unsigned long long)t_sum);
     if (n_sum) atomicAdd(&counters->node_visits, (unsigned long long)n_sum);
   }
+}
+
+// ------------------------------------------------------------- connect ---
+// Traces the wave's queued shadow rays (grid-stride over the queue, so the
+// grid is sized to the GPU, not to the queue) and adds each unoccluded ray's
+// contribution to its pixel.
+__global__ void __launch_bounds__(kTraceBlock, 5) k_connect(ShadowQueue Q, float4* image, WaveCounters* counters) {
+  YM_TRAVERSAL_SHARED(s_stack);
+  TraversalStack st;
+  st.bind(s_stack_entries, s_stack_t);
+  const uint32_t n = min(counters->shadow_count, Q.capacity);
+  uint32_t tests = 0, nodes = 0;
+  for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+    const float4 o = Q.o[t], d = Q.d[t];
+    if (!trace_occluded(c_scene, st, vec3(o.x, o.y, o.z), vec3(d.x, d.y, d.z), o.w, &tests, &nodes)) {
+      const float4 c = Q.c[t];
+      float* p = reinterpret_cast<float*>(image + __float_as_uint(d.w));
+      atomicAdd(p + 0, c.x);
+      atomicAdd(p + 1, c.y);
+      atomicAdd(p + 2, c.z);
+    }
+  }
+  for (int off = 16; off > 0; off >>= 1) {
+    tests += __shfl_down_sync(0xFFFFFFFFu, tests, off);
+    nodes += __shfl_down_sync(0xFFFFFFFFu, nodes, off);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    if (tests) atomicAdd(&counters->tri_tests, (unsigned long long)tests);
+    if (nodes) atomicAdd(&counters->node_visits, (unsigned long long)nodes);
+  }
+  if (st.overflow) atomicOr(&counters->errors, (uint32_t)kDevErrStack);
 }
 
 // ----------------------------------------------------------- accumulate ---
@@ -926,12 +1057,47 @@ void launch_extend(const PathPool& P, uint32_t count, const HitPool& H, float4* 
   else k_extend<false><<<blocks, kTraceBlock, 0, stream>>>(P, count, H, image, counters);
 }
 
+void launch_sort_hits(uint32_t count, const HitPool& H, WaveCounters* counters, cudaStream_t stream) {
+  if (count == 0) return;
+  k_sort_hits<<<(count + 255) / 256, 256, 0, stream>>>(count, H, counters);
+}
+
+uint32_t launch_wave(const PathPool& A, const PathPool& B, const HitPool& H, uint32_t live, uint32_t gen,
+                     uint32_t next_tile, uint32_t tiles_x, int frame_index, uint32_t spp, float4* image,
+                     WaveCounters* counters, const WaveOptions& opt, cudaEvent_t* ev, cudaStream_t stream) {
+  const uint32_t total = live + gen;
+  const ShadowQueue* defer = (!opt.volumes && opt.defer_shadows) ? &opt.shadow_queue : nullptr;
+  HitPool Hs = H;
+  if (!opt.sort_hits) Hs.order = nullptr;
+  cudaMemsetAsync(counters, 0, kWaveClearBytes, stream);
+  if (ev) cudaEventRecord(ev[0], stream);
+  launch_generate(A, live, gen, next_tile, tiles_x, frame_index, spp, stream);
+  if (ev) cudaEventRecord(ev[1], stream);
+  launch_extend(A, total, Hs, image, counters, opt.volumes, stream);
+  if (opt.sort_hits) launch_sort_hits(total, Hs, counters, stream);
+  if (ev) cudaEventRecord(ev[2], stream);
+  launch_shade(A, total, Hs, B, image, counters, opt.volumes, defer, stream);
+  if (defer && total > 0) launch_connect(*defer, image, counters, stream);
+  if (ev) cudaEventRecord(ev[3], stream);
+  if (total == 0) return gen > 0 ? 1u : 0u;
+  return (gen > 0 ? 1u : 0u) + 2u + (opt.sort_hits ? 1u : 0u) + (defer ? 1u : 0u);
+}
+
 void launch_shade(const PathPool& P, uint32_t count, const HitPool& H, const PathPool& Q, float4* image,
-                  WaveCounters* counters, bool volumes, cudaStream_t stream) {
+                  WaveCounters* counters, bool volumes, const ShadowQueue* defer, cudaStream_t stream) {
   if (count == 0) return;
   const uint32_t blocks = (count + kTraceBlock - 1) / kTraceBlock;
-  if (volumes) k_shade<true><<<blocks, kTraceBlock, 0, stream>>>(P, count, H, Q, image, counters);
-  else k_shade<false><<<blocks, kTraceBlock, 0, stream>>>(P, count, H, Q, image, counters);
+  const ShadowQueue none{};
+  if (volumes) k_shade<true, false><<<blocks, kTraceBlock, 0, stream>>>(P, count, H, Q, image, counters, none);
+  else if (defer) k_shade<false, true><<<blocks, kTraceBlock, 0, stream>>>(P, count, H, Q, image, counters, *defer);
+  else k_shade<false, false><<<blocks, kTraceBlock, 0, stream>>>(P, count, H, Q, image, counters, none);
+}
+
+void launch_connect(const ShadowQueue& Q, float4* image, WaveCounters* counters, cudaStream_t stream) {
+  int sms = 148;
+  int dev = 0;
+  if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  k_connect<<<sms * 5, kTraceBlock, 0, stream>>>(Q, image, counters);
 }
 
 void launch_accumulate(const float4* noise, float4* acc, uint32_t n, int frame_index, cudaStream_t stream) {

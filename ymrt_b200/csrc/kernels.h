@@ -1,6 +1,8 @@
 // Device-side buffers of one wave and the kernel launchers (kernels.cu).
 #pragma once
 
+#include <cstddef>
+
 #include <cuda_runtime.h>
 
 #include "ymrt_scene.h"
@@ -15,6 +17,16 @@ constexpr uint32_t kFlagDead = 1u << 10;          // slot holds no live path
 constexpr uint32_t kFlagSampleShift = 11;         // sample index within the pixel (for non-Halton samplers)
 
 constexpr uint32_t kNearbyExplicit = 1u << 31;    // hit ids.w: nearby list stored in HitPool::nearby
+
+// Shading buckets: k_extend files every hit under a bucket, a sort pass lists
+// the hits bucket by bucket, and k_shade runs over that list, so each warp
+// shades hits that take the same code path (lights and pass-through
+// boundaries, volume scattering, or one combination of material lobes).
+constexpr int kShadeBuckets = 34;
+constexpr uint32_t kBucketCheap = 0;    // light, boundary pass-through, invalid material
+constexpr uint32_t kBucketVolume = 1;   // scattering inside a medium
+constexpr uint32_t kBucketLobes = 2;    // + bit mask of the material's lobes (coat, metal, specular, transmission, diffuse)
+constexpr uint8_t kBucketNone = 0xFF;   // no hit (or no path) in this slot
 
 constexpr uint32_t kDevErrStack = 1u;
 constexpr uint32_t kDevErrQueue = 2u;
@@ -40,16 +52,35 @@ struct HitPool {
   uint4* ids;       // instance, triangle, back face | volume hit << 1, nearby count | kNearbyExplicit
   uint4* nearby;    // kMaxNearby entries per slot: prim, t bits, back
   float* vol_w;     // kMaxBoundaryRecord medium-selection weights per slot (volume hits only)
+  uint8_t* bucket;  // shading bucket per slot (kBucketNone: nothing to shade)
+  uint32_t* order;  // slots to shade, bucket by bucket
+};
+
+// Deferred next-event shadow rays of one wave (traced by k_connect).
+struct ShadowQueue {
+  float4* o;   // origin xyz, maximum distance
+  float4* d;   // normalised direction xyz, pixel index (bits)
+  float4* c;   // contribution rgb, already weighted by throughput / spp
+  uint32_t capacity;
 };
 
 struct WaveCounters {
+  // cleared at the start of every wave (the first kWaveClearBytes bytes)
   uint32_t next_count;             // paths written to the next pool
+  uint32_t hit_count;              // slots listed in HitPool::order
+  uint32_t shadow_count;           // rays written to the ShadowQueue
+  uint32_t bucket_count[kShadeBuckets];
+  uint32_t bucket_fill[kShadeBuckets];
+  // cleared once per frame
   uint32_t errors;                 // kDevErr* bits
+  uint32_t reserved;
   unsigned long long extension_rays;
   unsigned long long shadow_rays;
   unsigned long long tri_tests;
   unsigned long long node_visits;
 };
+
+constexpr size_t kWaveClearBytes = offsetof(WaveCounters, errors);
 
 cudaError_t upload_constants(const DeviceScene& scene, const uint32_t* primes, const uint32_t* prime_sums,
                              cudaStream_t stream);
@@ -58,8 +89,27 @@ void launch_generate(const PathPool& P, uint32_t base, uint32_t count, uint32_t 
                      int frame_index, uint32_t spp, cudaStream_t stream);
 void launch_extend(const PathPool& P, uint32_t count, const HitPool& H, float4* image, WaveCounters* counters,
                    bool volumes, cudaStream_t stream);
+void launch_sort_hits(uint32_t count, const HitPool& H, WaveCounters* counters, cudaStream_t stream);
 void launch_shade(const PathPool& P, uint32_t count, const HitPool& H, const PathPool& Q, float4* image,
-                  WaveCounters* counters, bool volumes, cudaStream_t stream);
+                  WaveCounters* counters, bool volumes, const ShadowQueue* defer, cudaStream_t stream);
+void launch_connect(const ShadowQueue& Q, float4* image, WaveCounters* counters, cudaStream_t stream);
+// One wave: generates `gen` camera paths after the `live` continuing ones in
+// A, traces them, lists the hits by shading bucket and shades them, writing
+// continuing paths to B. With opt.defer_shadows (surfaces only; the caller
+// turns it off for the indirect clamp, which needs a vertex's whole direct
+// light at once) the shading kernel queues its shadow rays and k_connect
+// traces them.
+// ev (optional, 4 events) is recorded before generate, extend and shade and
+// after shade (and connect). Returns the number of kernels launched.
+struct WaveOptions {
+  bool volumes = false;        // volume scattering kernels
+  bool sort_hits = true;       // shade hits listed by shading bucket
+  bool defer_shadows = false;  // queue surface shadow rays for k_connect (ignored with volumes)
+  ShadowQueue shadow_queue{};
+};
+uint32_t launch_wave(const PathPool& A, const PathPool& B, const HitPool& H, uint32_t live, uint32_t gen,
+                     uint32_t next_tile, uint32_t tiles_x, int frame_index, uint32_t spp, float4* image,
+                     WaveCounters* counters, const WaveOptions& opt, cudaEvent_t* ev, cudaStream_t stream);
 void launch_accumulate(const float4* noise, float4* acc, uint32_t n, int frame_index, cudaStream_t stream);
 void launch_debug_trace(int n, const float* o, const float* d, const uint32_t* lh, uint32_t* inst, uint32_t* tri,
                         float* t, float* bary, int* back, int* nearby, uint32_t* errors, cudaStream_t stream);

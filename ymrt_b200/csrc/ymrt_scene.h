@@ -203,6 +203,7 @@ struct DeviceScene {
   const mat4* transforms;
   const mat4* i_transforms;
   uint32_t transform_count;
+  const uint8_t* inst_bucket;   // shading bucket of a hit on each instance
   // top-level BVH over instances
   const WideNode* tlas_nodes;
   const uint32_t* tlas_prims;   // instance index per TLAS leaf slot
