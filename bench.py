@@ -6,14 +6,19 @@ fBm heightfield, a torus and a box; 32 GGX conductor / dielectric / diffuse
 materials; 2 quad lights), 1920x1080, 64 samples per pixel, maximum depth 12,
 Halton sampler, shape-light next-event estimation. One step = one full frame.
 
-Metric: Mrays/s = (closest-hit queries + occlusion queries) / frame time; the
-reference performs the same queries on the same paths (its counts are taken
-from the instrumented oracle build in the reference arm).
+Metric: Mrays/s = (closest-hit queries + occlusion queries) / time; the
+reference performs the same queries on the same paths.
 
 Arms:
-  (default)          ymrt_b200 kernels; `value` timed on the device with the
-                     scene resident; `e2e` through the C ABI with the scene
-                     uploaded from host memory and the image read back every step.
+  (default)          ymrt_b200 kernels. `value`: K frames with the scene
+                     resident, timed with CUDA events between a barrier and a
+                     synchronize on each side (max over ranks). `e2e`: through
+                     the C ABI with the scene uploaded from host memory and the
+                     image read back every step. `kernels` / `roofline`: one
+                     profiled frame with events around every launch.
+                     `ref_cuda`: the reference's own stage kernels rebuilt for
+                     sm_100a on the same frame. `cpu_baseline`: the reference
+                     built for the host on a bounded tile sample.
   --impl reference   the reference's own path tracer compiled for the host
                      (oracle/_ref), all host threads, on a bounded tile
                      sample of the same frame.
@@ -43,6 +48,25 @@ WORKLOADS = {
     "instanced": dict(scene="instanced", width=1920, height=1080, spp=64, depth=12),
     "cornell": dict(scene="cornell", width=256, height=256, spp=16, depth=8),
 }
+
+
+class quiet_stdout:
+    """Sends file descriptor 1 to /dev/null while the reference's own code
+    runs (its scene loader reports progress on stdout), so that stdout
+    carries only the one JSON line."""
+
+    def __enter__(self):
+        sys.stdout.flush()
+        self.saved = os.dup(1)
+        devnull = os.open(os.devnull, os.O_WRONLY)
+        os.dup2(devnull, 1)
+        os.close(devnull)
+        return self
+
+    def __exit__(self, *exc):
+        sys.stdout.flush()
+        os.dup2(self.saved, 1)
+        os.close(self.saved)
 
 
 def dist_env():
@@ -112,6 +136,45 @@ def flush_l2(torch_mod, buf):
     buf.add_(1.0)  # writes 256 MB (> 126 MB L2)
 
 
+# Algorithmic bytes per unit (the path state each kernel must move; BVH nodes
+# and triangles are counted separately: the unique scene geometry is a few MB
+# and stays resident in L2).
+EXT_STATE_BYTES_PER_RAY = 81       # reads ray o/d 32, pixel+flags 8, last hit 8; writes hit 16+16+1 (a miss: 40)
+SHADE_STATE_BYTES_PER_HIT = 222    # reads path+hit state 125 B; writes the continuation 97 B
+SHADOW_QUEUE_BYTES_PER_RAY = 48    # written by k_shade, read by k_connect
+NODE_BYTES, TRI_BYTES = 80, 48     # one wide node; one triangle (3 float4)
+
+
+def kernel_table(pst):
+    """Per-kernel device time of the profiled frame with the algorithmic
+    bytes of each launch (averaged over the frame's waves)."""
+    waves = max(int(pst.waves), 1)
+    ext_nodes = pst.node_visits - pst.shadow_node_visits
+    ext_tris = pst.triangle_tests - pst.shadow_triangle_tests
+    k = {
+        "k_extend": dict(ms=pst.ms_extend, state=pst.extension_rays * EXT_STATE_BYTES_PER_RAY,
+                         bvh=ext_nodes * NODE_BYTES + ext_tris * TRI_BYTES, units=pst.extension_rays, unit="rays"),
+        "k_shade": dict(ms=pst.ms_shade, state=pst.shaded_hits * SHADE_STATE_BYTES_PER_HIT +
+                        pst.shadow_rays * SHADOW_QUEUE_BYTES_PER_RAY, bvh=0, units=pst.shaded_hits, unit="hits"),
+        "k_connect": dict(ms=pst.ms_connect, state=pst.shadow_rays * SHADOW_QUEUE_BYTES_PER_RAY,
+                          bvh=pst.shadow_node_visits * NODE_BYTES + pst.shadow_triangle_tests * TRI_BYTES,
+                          units=pst.shadow_rays, unit="shadow rays"),
+        "k_sort_hits": dict(ms=pst.ms_sort, state=pst.extension_rays * 1 + pst.shaded_hits * 4, bvh=0,
+                            units=pst.extension_rays, unit="slots"),
+        "k_generate": dict(ms=pst.ms_generate, state=pst.paths * 97, bvh=0, units=pst.paths, unit="paths"),
+    }
+    out = {}
+    for name, v in k.items():
+        ms_launch = v["ms"] / waves
+        out[name] = {"ms_per_frame": round(v["ms"], 3), "launches": waves, "ms_per_launch": round(ms_launch, 4),
+                     "alg_state_bytes_per_launch": int(v["state"] / waves),
+                     "bvh_bytes_per_launch": int(v["bvh"] / waves),
+                     "units_per_launch": int(v["units"] / waves), "unit": v["unit"],
+                     "state_gbs": round(v["state"] / waves / (ms_launch * 1e-3) / 1e9, 1) if ms_launch > 0 else None,
+                     "bvh_l2_gbs": round(v["bvh"] / waves / (ms_launch * 1e-3) / 1e9, 1) if ms_launch > 0 else None}
+    return out
+
+
 def run_ours(args):
     import torch
     import ymrt_b200 as Y
@@ -150,32 +213,34 @@ def run_ours(args):
 
     for i in range(args.warmup):
         step(i)
+
+    # Timed region: K steps between a barrier + synchronize on each side,
+    # timed with CUDA events on this stream (render() returns after its own
+    # stream finished, so the events bracket every kernel of the K frames).
     torch.cuda.synchronize()
     barrier()
     clocks = ClockSampler(local_rank)
     clocks.start()
-    t0 = time.perf_counter()
-    rays = 0
-    dev_ms = 0.0
-    launches = 0
-    node_visits = tri_tests = ext = shadow = 0
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record()
+    rays = ext = shadow = launches = 0
+    frame_ms = 0.0
     errors = 0
     for i in range(args.steps):
         st = step(args.warmup + i)
         rays += st.extension_rays + st.shadow_rays
         ext += st.extension_rays
         shadow += st.shadow_rays
-        node_visits += st.node_visits
-        tri_tests += st.triangle_tests
-        dev_ms += st.ms_total
+        frame_ms += st.ms_total
         launches += st.kernel_launches
         errors |= st.device_errors
+    ev1.record()
     torch.cuda.synchronize()
     barrier()
-    wall = time.perf_counter() - t0
     clk = clocks.stop()
+    elapsed_ms = ev0.elapsed_time(ev1)
 
-    # Per-stage device times from one profiled frame (events around each launch).
+    # Per-kernel device times from one profiled frame (events around each launch).
     lib = Y.library()
     lib.ymrt_set_profiling(ctx.h, 1)
     _, pst = scene.render(setting, frame_index=10_000 + rank, out=image)
@@ -185,7 +250,6 @@ def run_ours(args):
     # read the image back -- every step.
     host_img = np.zeros((H, W, 4), np.float32)
     e2e_rays, e2e_wall = 0, 0.0
-    h2d = None
     for i in range(max(1, min(args.steps, 3))):
         torch.cuda.synchronize()
         t = time.perf_counter()
@@ -194,66 +258,60 @@ def run_ours(args):
         e2e_wall += time.perf_counter() - t
         e2e_rays += st.extension_rays + st.shadow_rays
         sc2.close()
-        if h2d is None:
-            c = host.counts()
-            h2d = None
     scene_bytes = scene_upload_bytes(host, perm)
 
-    out = {"rays": rays, "dev_ms": dev_ms, "wall": wall, "ext": ext, "shadow": shadow}
     if world > 1:
         import torch.distributed as dist
-        t = torch.tensor([rays, dev_ms, wall, e2e_rays, e2e_wall], dtype=torch.float64, device="cuda")
+        t = torch.tensor([rays, elapsed_ms, e2e_rays, e2e_wall], dtype=torch.float64, device="cuda")
         tmax = t.clone()
         dist.all_reduce(t, op=dist.ReduceOp.SUM)
         dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
-        rays_all, dev_ms_max, wall_max = t[0].item(), tmax[1].item(), tmax[2].item()
-        e2e_rays_all, e2e_wall_max = t[3].item(), tmax[4].item()
+        rays_all, ms_max = t[0].item(), tmax[1].item()
+        e2e_rays_all, e2e_wall_max = t[2].item(), tmax[3].item()
     else:
-        rays_all, dev_ms_max, wall_max = rays, dev_ms, wall
+        rays_all, ms_max = rays, elapsed_ms
         e2e_rays_all, e2e_wall_max = e2e_rays, e2e_wall
 
     result = None
     if rank == 0:
         hbm_peak, peak_kind = read_peaks()
-        # Roofline of the dominant kernel (the shade stage: next-event shadow
-        # traversals plus BSDF work). Algorithmic bytes per path-vertex:
-        # traversal fetches (80 B per wide node, 48 B per triangle) plus the
-        # path/hit state the stage reads and writes.
-        dominant = "k_shade" if pst.ms_shade >= pst.ms_extend else "k_extend"
-        frac_nodes = 1.0
-        state_ext = 32 + 8 + 8 + 16 + 32  # ray, pixel/flags, last hit, sampler; hit record written
-        state_shade = 32 + 32 + 8 + 8 + 16 + 32 + 104 * 0  # path state read + hit read (+ continuation write below)
-        alg_bytes = pst.node_visits * 80 + pst.triangle_tests * 48 + pst.extension_rays * (state_ext + state_shade + 96)
-        ms_kernels = pst.ms_extend + pst.ms_shade + pst.ms_generate
-        achieved = alg_bytes / (ms_kernels * 1e-3) / 1e9 if ms_kernels > 0 else 0.0
-        value = rays_all / (dev_ms_max * 1e-3) / 1e6
+        kernels = kernel_table(pst)
+        dominant = max(kernels, key=lambda n: kernels[n]["ms_per_frame"])
+        dk = kernels[dominant]
+        achieved = dk["state_gbs"] or 0.0
+        value = rays_all / (ms_max * 1e-3) / 1e6
         result = {
             "metric": "Mrays/s", "value": round(value, 2), "unit": "Mrays/s", "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": round(dev_ms_max / args.steps, 3), "higher_is_better": True,
+            "warmup": args.warmup, "ms_per_step": round(ms_max / args.steps, 3), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded .ymtmp scene generated by ymrt_b200.scenes)",
-            "config": {"workload": f"{wl['scene']} {W}x{H} {spp}spp depth {wl['depth']} (~1.2M instanced triangles)"
-                       if wl["scene"] == "instanced" else f"{wl['scene']} {W}x{H} {spp}spp depth {wl['depth']}",
+            "config": {"workload": f"{wl['scene']} {W}x{H} {spp}spp depth {wl['depth']}" +
+                       (" (~1.2M instanced triangles)" if wl["scene"] == "instanced" else ""),
                        "sampler": "halton", "lights": "shape lights, NEE with MIS",
                        "parallelism": f"replica x{world}" + (" + allreduce of frames" if world > 1 else ""),
-                       "l2": "256 MB buffer written between steps; path queues (>1 GB) exceed L2"},
-            "spp_per_s": round(W * H * spp * world / (dev_ms_max * 1e-3 / args.steps) / args.steps * args.steps, 1),
+                       "l2": "256 MB buffer written between steps; path queues (>1 GB) exceed L2",
+                       "options": {"sort_hits": ctx.get_option("sort_hits"),
+                                   "defer_shadows": ctx.get_option("defer_shadows")}},
+            "spp_per_s": round(W * H * spp * world * args.steps / (ms_max * 1e-3), 1),
             "rays": {"extension": ext, "shadow": shadow, "per_step": rays // max(args.steps, 1)},
-            "wall_s": round(wall_max, 3),
+            "frame_ms_device": round(frame_ms / args.steps, 3),
             "gpu_launches": int(launches),
             "device_errors": int(errors),
-            "stage_ms": {"generate": round(pst.ms_generate, 2), "extend": round(pst.ms_extend, 2),
-                         "shade": round(pst.ms_shade, 2), "frame": round(pst.ms_total, 2), "waves": int(pst.waves)},
-            "roofline": {"bound": "hbm", "kernels": "k_extend+k_shade+k_generate", "dominant": dominant,
-                         "achieved": round(achieved, 1), "peak": hbm_peak, "peak_kind": peak_kind, "unit": "GB/s",
-                         "frac": round(achieved / hbm_peak, 4), "traffic": read_traffic(pst),
-                         "alg_bytes_per_frame": int(alg_bytes)},
+            "kernels": kernels,
+            "roofline": {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": hbm_peak,
+                         "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / hbm_peak, 4),
+                         "traffic": read_traffic(dominant, dk),
+                         "alg_bytes_per_launch": dk["alg_state_bytes_per_launch"],
+                         "l2_bvh_gbs": dk["bvh_l2_gbs"]},
             "e2e": {"value": round(e2e_rays_all / e2e_wall_max / 1e6, 2) if e2e_wall_max > 0 else None,
                     "unit": "Mrays/s", "h2d_bytes_per_step": int(scene_bytes), "d2h_bytes_per_step": int(W * H * 16)},
             "clocks": clk,
         }
-        if not args.no_cpu_baseline:
-            result["cpu_baseline"] = cpu_baseline(path, perm, W, H, spp, wl["depth"], budget_s=args.cpu_budget)
+        with quiet_stdout():
+            if not args.no_ref_cuda:
+                result["ref_cuda"] = ref_cuda_timing(path, perm, W, H, spp, wl["depth"], pst)
+            if not args.no_cpu_baseline:
+                result["cpu_baseline"] = cpu_baseline(path, perm, W, H, spp, wl["depth"], budget_s=args.cpu_budget)
     if world > 1:
         import torch.distributed as dist
         dist.barrier()
@@ -263,14 +321,46 @@ def run_ours(args):
     return result
 
 
-def read_traffic(pst):
-    """DRAM bytes per frame from the committed ncu summary, scaled to this frame."""
+def ref_cuda_timing(path, perm, W, H, spp, depth, pst, frames=2):
+    """The reference's own wavefront kernels rebuilt for sm_100a
+    (oracle/_ref/libymrt_refgpu.so, nvcc default floating-point flags), on
+    the same frame: device time of its wave loop. Its paths are the same
+    samples, so its query count is ours for the same frame index."""
+    try:
+        from oracle import ref
+        if not ref.gpu_available(exact=False):
+            return {"unavailable": "oracle/_ref/libymrt_refgpu.so not built"}
+        rg = ref.RefGpuScene(path, perm, W, H)
+        rg.set_settings(spp=spp, ray_depth=depth)
+        rg.render_frame(10_000, copy_out=False)  # warm-up (same frame as the profiled one)
+        ms = []
+        for _ in range(frames):
+            rg.render_frame(10_000, copy_out=False)
+            ms.append(rg.last_render_ms())
+        rg.set_profiling(True)
+        rg.render_frame(10_000, copy_out=False)
+        stages = rg.last_stage_ms()
+        rg.close()
+    except Exception as e:  # noqa: BLE001 - reported, not fatal for our own measurement
+        return {"unavailable": f"{type(e).__name__}: {e}"}
+    rays = pst.extension_rays + pst.shadow_rays
+    best = min(ms)
+    return {"value": round(rays / (best * 1e-3) / 1e6, 2), "unit": "Mrays/s", "ms_per_frame": round(best, 2),
+            "frames": frames, "stage_ms": {k: round(v, 2) if isinstance(v, float) else v for k, v in stages.items()},
+            "build": "reference src/Shading.cu stage kernels, nvcc -O3 sm_100a default FP flags, MAX_RAY_COUNT 1Mi",
+            "rays_per_frame": int(rays)}
+
+
+def read_traffic(kernel, dk):
+    """DRAM bytes per launch of `kernel` from the committed ncu summary
+    (profiles/traffic.json: bytes per unit from one capture), scaled to this
+    frame's units per launch."""
     p = os.path.join(ROOT, "profiles", "traffic.json")
     try:
         with open(p) as f:
-            t = json.load(f)
-        return {"bytes_per_path_vertex": t["bytes_per_path_vertex"],
-                "bytes_per_frame": int(t["bytes_per_path_vertex"] * pst.extension_rays), "source": t["source"]}
+            t = json.load(f)[kernel]
+        return {"bytes_per_launch": int(t["dram_bytes_per_unit"] * dk["units_per_launch"]),
+                "dram_bytes_per_unit": t["dram_bytes_per_unit"], "unit": t["unit"], "source": t["source"]}
     except Exception:
         return None
 
@@ -365,10 +455,15 @@ def main(argv=None):
     ap.add_argument("--queue", type=int, default=0, help="path queue capacity (0 = library default)")
     ap.add_argument("--cpu-budget", type=float, default=12.0, help="seconds of CPU work per reference sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-ref-cuda", action="store_true", help="skip timing the reference's own CUDA kernels")
     args = ap.parse_args(argv)
     if args.warmup < 3:
         args.warmup = 3
-    res = run_reference(args) if args.impl == "reference" else run_ours(args)
+    if args.impl == "reference":
+        with quiet_stdout():
+            res = run_reference(args)
+    else:
+        res = run_ours(args)
     if res is not None:
         print(json.dumps(res), flush=True)
 

@@ -83,11 +83,16 @@ typedef struct ymrt_stats {
   uint64_t triangle_tests;   /* triangles fetched and tested by all queries */
   uint64_t kernel_launches;  /* kernels launched for the frame */
   double ms_total;           /* device time of the frame (CUDA events) */
-  double ms_generate;        /* per-stage device time; filled when profiling is on */
-  double ms_extend;
-  double ms_shade;
+  double ms_generate;        /* per-kernel device time; filled when profiling is on */
+  double ms_extend;          /* closest-hit kernel */
+  double ms_shade;           /* shading kernel */
   uint32_t device_errors;    /* bit set of YMRT_DEVERR_* raised on the device */
   uint32_t reserved_;
+  uint64_t shadow_node_visits;     /* the part of node_visits made by occlusion queries */
+  uint64_t shadow_triangle_tests;  /* the part of triangle_tests made by occlusion queries */
+  double ms_sort;            /* hit listing by shading bucket (profiling on) */
+  double ms_connect;         /* deferred shadow-ray kernel (profiling on) */
+  uint64_t shaded_hits;      /* path vertices shaded (extension rays that hit) */
 } ymrt_stats;
 
 #define YMRT_DEVERR_STACK 1u     /* a traversal stack overflowed (entries were dropped) */

@@ -72,7 +72,9 @@ class Stats(ctypes.Structure):
         ("waves", ctypes.c_uint64), ("node_visits", ctypes.c_uint64), ("triangle_tests", ctypes.c_uint64),
         ("kernel_launches", ctypes.c_uint64), ("ms_total", ctypes.c_double), ("ms_generate", ctypes.c_double),
         ("ms_extend", ctypes.c_double), ("ms_shade", ctypes.c_double), ("device_errors", ctypes.c_uint32),
-        ("reserved_", ctypes.c_uint32),
+        ("reserved_", ctypes.c_uint32), ("shadow_node_visits", ctypes.c_uint64),
+        ("shadow_triangle_tests", ctypes.c_uint64), ("ms_sort", ctypes.c_double), ("ms_connect", ctypes.c_double),
+        ("shaded_hits", ctypes.c_uint64),
     ]
 
     def as_dict(self) -> dict:

@@ -79,7 +79,7 @@ struct ymrt_context {
   WaveCounters* counters_host = nullptr;  // pinned
   cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
   bool profiling = false;
-  cudaEvent_t ev_stage[4] = {nullptr, nullptr, nullptr, nullptr};
+  cudaEvent_t ev_stage[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
   std::vector<uint32_t> primes, prime_sums;
   // wave options (ymrt_set_option)
   bool sort_hits = true;
@@ -549,8 +549,8 @@ int ymrt_render_tiles(ymrt_scene* sc, const ymrt_render_setting* setting, int fr
   cudaEventRecord(ctx->ev_start, st);
   uint32_t live = 0;
   int a = 0;
-  uint64_t waves = 0, paths = 0, launches = 0;
-  double ms_stage[3] = {0.0, 0.0, 0.0};
+  uint64_t waves = 0, paths = 0, launches = 0, hits = 0;
+  double ms_stage[5] = {0.0, 0.0, 0.0, 0.0, 0.0};  // generate, extend, sort, shade, connect
   while (live > 0 || cursor < t_end) {
     const uint32_t n_tiles = std::min<uint32_t>((ctx->capacity - live) / per_tile, t_end - cursor);
     const uint32_t gen = n_tiles * per_tile;
@@ -562,13 +562,14 @@ int ymrt_render_tiles(ymrt_scene* sc, const ymrt_render_setting* setting, int fr
       return ctx->cuda_fail(e, "reading wave counters");
     if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return ctx->cuda_fail(e, "wave");
     if (ctx->profiling) {
-      for (int k = 0; k < 3; ++k) {
+      for (int k = 0; k < 5; ++k) {
         float ms = 0.0f;
         cudaEventElapsedTime(&ms, ctx->ev_stage[k], ctx->ev_stage[k + 1]);
         ms_stage[k] += ms;
       }
     }
     live = ctx->counters_host->next_count;
+    hits += ctx->counters_host->hit_count;
     if (live > ctx->capacity) return ctx->fail(YMRT_ERR_OVERFLOW, "path queue overflow");
     a ^= 1;
     cursor += n_tiles;
@@ -591,13 +592,18 @@ int ymrt_render_tiles(ymrt_scene* sc, const ymrt_render_setting* setting, int fr
     stats->extension_rays = ctx->counters_host->extension_rays;
     stats->shadow_rays = ctx->counters_host->shadow_rays;
     stats->waves = waves;
-    stats->node_visits = ctx->counters_host->node_visits;
-    stats->triangle_tests = ctx->counters_host->tri_tests;
+    stats->shaded_hits = hits;
+    stats->node_visits = ctx->counters_host->node_visits + ctx->counters_host->shadow_node_visits;
+    stats->triangle_tests = ctx->counters_host->tri_tests + ctx->counters_host->shadow_tri_tests;
+    stats->shadow_node_visits = ctx->counters_host->shadow_node_visits;
+    stats->shadow_triangle_tests = ctx->counters_host->shadow_tri_tests;
     stats->kernel_launches = launches;
     stats->ms_total = ms;
     stats->ms_generate = ms_stage[0];
     stats->ms_extend = ms_stage[1];
-    stats->ms_shade = ms_stage[2];
+    stats->ms_sort = ms_stage[2];
+    stats->ms_shade = ms_stage[3];
+    stats->ms_connect = ms_stage[4];
     stats->device_errors = ctx->counters_host->errors;
   }
   if (ctx->counters_host->errors & kDevErrQueue) return ctx->fail(YMRT_ERR_OVERFLOW, "path queue overflow on the device");
@@ -748,7 +754,7 @@ int ymrt_render_tiles_noalloc(ymrt_scene* sc, const ymrt_render_setting* setting
   cudaEventRecord(ctx->ev_start, st);
   uint32_t live = 0;
   int a = 0;
-  uint64_t waves = 0, paths = 0, launches = 0;
+  uint64_t waves = 0, paths = 0, launches = 0, hits = 0;
   while (live > 0 || cursor < t_end) {
     const uint32_t n_tiles = std::min<uint32_t>((cap - live) / per_tile, t_end - cursor);
     const uint32_t gen = n_tiles * per_tile;
@@ -758,6 +764,7 @@ int ymrt_render_tiles_noalloc(ymrt_scene* sc, const ymrt_render_setting* setting
       return ctx->cuda_fail(e, "reading wave counters");
     if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return ctx->cuda_fail(e, "wave");
     live = ctx->counters_host->next_count;
+    hits += ctx->counters_host->hit_count;
     if (live > cap) return ctx->fail(YMRT_ERR_OVERFLOW, "path queue overflow");
     a ^= 1;
     cursor += n_tiles;
@@ -776,8 +783,11 @@ int ymrt_render_tiles_noalloc(ymrt_scene* sc, const ymrt_render_setting* setting
     stats->extension_rays = ctx->counters_host->extension_rays;
     stats->shadow_rays = ctx->counters_host->shadow_rays;
     stats->waves = waves;
-    stats->node_visits = ctx->counters_host->node_visits;
-    stats->triangle_tests = ctx->counters_host->tri_tests;
+    stats->shaded_hits = hits;
+    stats->node_visits = ctx->counters_host->node_visits + ctx->counters_host->shadow_node_visits;
+    stats->triangle_tests = ctx->counters_host->tri_tests + ctx->counters_host->shadow_tri_tests;
+    stats->shadow_node_visits = ctx->counters_host->shadow_node_visits;
+    stats->shadow_triangle_tests = ctx->counters_host->shadow_tri_tests;
     stats->kernel_launches = launches;
     stats->ms_total = ms;
     stats->device_errors = ctx->counters_host->errors;

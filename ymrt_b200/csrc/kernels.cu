@@ -919,8 +919,8 @@ __global__ void __launch_bounds__(kTraceBlock) k_shade(PathPool P, uint32_t coun
   }
   if ((threadIdx.x & 31) == 0) {
     if (s_sum) atomicAdd(&counters->shadow_rays, (unsigned long long)s_sum);
-    if (t_sum) atomicAdd(&counters->tri_tests, (unsigned long long)t_sum);
-    if (n_sum) atomicAdd(&counters->node_visits, (unsigned long long)n_sum);
+    if (t_sum) atomicAdd(&counters->shadow_tri_tests, (unsigned long long)t_sum);
+    if (n_sum) atomicAdd(&counters->shadow_node_visits, (unsigned long long)n_sum);
   }
 }
 
@@ -949,8 +949,8 @@ __global__ void __launch_bounds__(kTraceBlock, 5) k_connect(ShadowQueue Q, float
     nodes += __shfl_down_sync(0xFFFFFFFFu, nodes, off);
   }
   if ((threadIdx.x & 31) == 0) {
-    if (tests) atomicAdd(&counters->tri_tests, (unsigned long long)tests);
-    if (nodes) atomicAdd(&counters->node_visits, (unsigned long long)nodes);
+    if (tests) atomicAdd(&counters->shadow_tri_tests, (unsigned long long)tests);
+    if (nodes) atomicAdd(&counters->shadow_node_visits, (unsigned long long)nodes);
   }
   if (st.overflow) atomicOr(&counters->errors, (uint32_t)kDevErrStack);
 }
@@ -1074,11 +1074,13 @@ uint32_t launch_wave(const PathPool& A, const PathPool& B, const HitPool& H, uin
   launch_generate(A, live, gen, next_tile, tiles_x, frame_index, spp, stream);
   if (ev) cudaEventRecord(ev[1], stream);
   launch_extend(A, total, Hs, image, counters, opt.volumes, stream);
-  if (opt.sort_hits) launch_sort_hits(total, Hs, counters, stream);
   if (ev) cudaEventRecord(ev[2], stream);
-  launch_shade(A, total, Hs, B, image, counters, opt.volumes, defer, stream);
-  if (defer && total > 0) launch_connect(*defer, image, counters, stream);
+  if (opt.sort_hits) launch_sort_hits(total, Hs, counters, stream);
   if (ev) cudaEventRecord(ev[3], stream);
+  launch_shade(A, total, Hs, B, image, counters, opt.volumes, defer, stream);
+  if (ev) cudaEventRecord(ev[4], stream);
+  if (defer && total > 0) launch_connect(*defer, image, counters, stream);
+  if (ev) cudaEventRecord(ev[5], stream);
   if (total == 0) return gen > 0 ? 1u : 0u;
   return (gen > 0 ? 1u : 0u) + 2u + (opt.sort_hits ? 1u : 0u) + (defer ? 1u : 0u);
 }

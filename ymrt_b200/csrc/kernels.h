@@ -76,8 +76,10 @@ struct WaveCounters {
   uint32_t reserved;
   unsigned long long extension_rays;
   unsigned long long shadow_rays;
-  unsigned long long tri_tests;
+  unsigned long long tri_tests;     // closest-hit queries
   unsigned long long node_visits;
+  unsigned long long shadow_tri_tests;   // occlusion (and transmittance) queries
+  unsigned long long shadow_node_visits;
 };
 
 constexpr size_t kWaveClearBytes = offsetof(WaveCounters, errors);
@@ -99,8 +101,8 @@ void launch_connect(const ShadowQueue& Q, float4* image, WaveCounters* counters,
 // turns it off for the indirect clamp, which needs a vertex's whole direct
 // light at once) the shading kernel queues its shadow rays and k_connect
 // traces them.
-// ev (optional, 4 events) is recorded before generate, extend and shade and
-// after shade (and connect). Returns the number of kernels launched.
+// ev (optional, 6 events) is recorded before generate, extend, sort, shade and
+// connect and at the end. Returns the number of kernels launched.
 struct WaveOptions {
   bool volumes = false;        // volume scattering kernels
   bool sort_hits = true;       // shade hits listed by shading bucket
