@@ -47,6 +47,9 @@ sys.path.insert(0, ROOT)
 WORKLOADS = {
     "instanced": dict(scene="instanced", width=1920, height=1080, spp=64, depth=12),
     "cornell": dict(scene="cornell", width=256, height=256, spp=16, depth=8),
+    # the Cornell-like scene with a homogeneous fog box and a procedural fBm
+    # smoke box (the density-texture form the reference renders), delta tracking
+    "volumetric": dict(scene="volumetric", width=1280, height=720, spp=32, depth=16, volume=True),
 }
 
 
@@ -194,7 +197,7 @@ def run_ours(args):
     ctx = Y.Context(local_rank, queue_capacity=args.queue, profiling=False)
     host = Y.HostScene(path, W, H)
     scene = Y.Scene(ctx, host, perm)
-    setting = Y.default_setting(spp=spp, ray_depth=wl["depth"])
+    setting = Y.default_setting(spp=spp, ray_depth=wl["depth"], volume=wl.get("volume", False))
     image = torch.zeros((H, W, 4), dtype=torch.float32, device="cuda")
     flush = torch.zeros(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
 
@@ -288,6 +291,7 @@ def run_ours(args):
             "config": {"workload": f"{wl['scene']} {W}x{H} {spp}spp depth {wl['depth']}" +
                        (" (~1.2M instanced triangles)" if wl["scene"] == "instanced" else ""),
                        "sampler": "halton", "lights": "shape lights, NEE with MIS",
+                       "media": "fog box + fBm smoke box, delta tracking" if wl.get("volume") else "none",
                        "parallelism": f"replica x{world}" + (" + allreduce of frames" if world > 1 else ""),
                        "l2": "256 MB buffer written between steps; path queues (>1 GB) exceed L2",
                        "options": {"sort_hits": ctx.get_option("sort_hits"),
@@ -309,9 +313,10 @@ def run_ours(args):
         }
         with quiet_stdout():
             if not args.no_ref_cuda:
-                result["ref_cuda"] = ref_cuda_timing(path, perm, W, H, spp, wl["depth"], pst)
+                result["ref_cuda"] = ref_cuda_timing(path, perm, W, H, spp, wl["depth"], pst, volume=wl.get("volume", False))
             if not args.no_cpu_baseline:
-                result["cpu_baseline"] = cpu_baseline(path, perm, W, H, spp, wl["depth"], budget_s=args.cpu_budget)
+                result["cpu_baseline"] = cpu_baseline(path, perm, W, H, spp, wl["depth"], budget_s=args.cpu_budget,
+                                                      volume=wl.get("volume", False))
     if world > 1:
         import torch.distributed as dist
         dist.barrier()
@@ -321,7 +326,7 @@ def run_ours(args):
     return result
 
 
-def ref_cuda_timing(path, perm, W, H, spp, depth, pst, frames=2):
+def ref_cuda_timing(path, perm, W, H, spp, depth, pst, frames=2, volume=False):
     """The reference's own wavefront kernels rebuilt for sm_100a
     (oracle/_ref/libymrt_refgpu.so, nvcc default floating-point flags), on
     the same frame: device time of its wave loop. Its paths are the same
@@ -331,7 +336,7 @@ def ref_cuda_timing(path, perm, W, H, spp, depth, pst, frames=2):
         if not ref.gpu_available(exact=False):
             return {"unavailable": "oracle/_ref/libymrt_refgpu.so not built"}
         rg = ref.RefGpuScene(path, perm, W, H)
-        rg.set_settings(spp=spp, ray_depth=depth)
+        rg.set_settings(spp=spp, ray_depth=depth, volume=int(volume))
         rg.render_frame(10_000, copy_out=False)  # warm-up (same frame as the profiled one)
         ms = []
         for _ in range(frames):
@@ -372,13 +377,13 @@ def scene_upload_bytes(host, perm) -> int:
                + perm.nbytes)
 
 
-def cpu_baseline(path, perm, W, H, spp, depth, budget_s=15.0, threads=None):
+def cpu_baseline(path, perm, W, H, spp, depth, budget_s=15.0, threads=None, volume=False):
     """The reference's own path tracer built for the host, on a bounded tile
     sample of the same frame (all host threads)."""
     from oracle import ref
     threads = threads or os.cpu_count() or 1
     rs = ref.RefScene(path, perm, W, H)
-    rs.set_settings(spp=spp, ray_depth=depth)
+    rs.set_settings(spp=spp, ray_depth=depth, volume=int(volume))
     tiles_x, tiles_y = (W + 15) // 16, (H + 15) // 16
     mid = (tiles_y // 2) * tiles_x
     # calibrate on a few tiles, then size the sample to the budget
@@ -410,7 +415,7 @@ def run_reference(args):
     from oracle import ref
     threads = os.cpu_count() or 1
     rs = ref.RefScene(path, perm, W, H)
-    rs.set_settings(spp=spp, ray_depth=wl["depth"])
+    rs.set_settings(spp=spp, ray_depth=wl["depth"], volume=int(wl.get("volume", False)))
     tiles_x, tiles_y = (W + 15) // 16, (H + 15) // 16
     total_tiles = tiles_x * tiles_y
     mid = (tiles_y // 2) * tiles_x

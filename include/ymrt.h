@@ -148,6 +148,11 @@ long long ymrt_host_scene_query(const ymrt_host_scene* scene, int what, int inde
  * in Scene::sampler_data.halton_permute_table. */
 int ymrt_scene_upload(ymrt_context* ctx, const ymrt_host_scene* scene, const uint32_t* halton_perm, size_t perm_len,
                       ymrt_scene** out);
+/* Generator matrices of the Sobol sampler (RenderSetting::sampler_type 2):
+ * 4096 dimensions x 32 columns, the reference's sobol_matrices32 table
+ * (src/LowDiscrepancy.cpp:179), which its GuiModule::UpdateScene uploads
+ * (src/core/GuiModule.cpp:256). Needed only for Sobol renders. */
+int ymrt_scene_set_sobol_matrices(ymrt_scene* scene, const uint32_t* matrices, size_t count);
 void ymrt_scene_free(ymrt_scene* scene);
 
 /* ---- rendering ---- */

@@ -54,6 +54,8 @@ def lib():
         L.ymref_camera_bytes.argtypes = [vp, vp, i]
         L.ymref_scene_records.argtypes = [vp, i, vp, i]
         L.ymref_bvh_depths.argtypes = [vp, vp]
+        L.ymref_sobol_matrices.restype = ctypes.c_size_t
+        L.ymref_sobol_matrices.argtypes = [vp, ctypes.c_size_t]
         L.ymref_trace.argtypes = [vp, i, vp, vp, vp, vp, vp, vp, vp, vp, vp]
         L.ymref_occluded.argtypes = [vp, i, vp, vp, vp, vp]
         L.ymref_halton.argtypes = [vp, i, vp, vp, vp, i, vp, vp, vp]
@@ -68,6 +70,14 @@ def lib():
 
 def _p(a: np.ndarray):
     return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def sobol_matrices() -> np.ndarray:
+    """The reference's Sobol generator matrices (4096 x 32 uint32)."""
+    n = lib().ymref_sobol_matrices(None, 0)
+    out = np.zeros(n, np.uint32)
+    lib().ymref_sobol_matrices(_p(out), n)
+    return out
 
 
 class RefScene:

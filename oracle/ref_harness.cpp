@@ -330,6 +330,14 @@ int ymref_bvh_depths(void* handle, uint32_t* out) {
   return (int)geo.size() + 1;
 }
 
+// The Sobol generator matrices the reference links (src/LowDiscrepancy.cpp:179,
+// 4096 dimensions x 32 columns); returns the word count.
+size_t ymref_sobol_matrices(uint32_t* out, size_t cap) {
+  const size_t n = (size_t)4096 * 32;
+  if (out && cap >= n) std::memcpy(out, sobol_matrices32, n * sizeof(uint32_t));
+  return n;
+}
+
 // The rendering camera after preparation, as raw bytes of the reference's
 // Camera struct (176 bytes on x86-64).
 int ymref_camera_bytes(void* handle, uint8_t* out, int out_len) {

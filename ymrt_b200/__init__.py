@@ -57,9 +57,10 @@ assert ctypes.sizeof(RenderSetting) == 40
 
 
 def default_setting(spp=1, ray_depth=8, shape_light=True, distant_light=False, volume=False, env_light=False,
-                    russian_roulette=False, indirect_clamp=False, indirect_limit=10.0) -> RenderSetting:
+                    russian_roulette=False, indirect_clamp=False, indirect_limit=10.0, sampler_type=1) -> RenderSetting:
     s = RenderSetting()
-    s.ssp, s.ray_depth, s.gamma, s.exposure, s.max_frame_count, s.sampler_type = spp, ray_depth, 2.2, 1.0, -1, 1
+    s.ssp, s.ray_depth, s.gamma, s.exposure, s.max_frame_count = spp, ray_depth, 2.2, 1.0, -1
+    s.sampler_type = sampler_type
     s.enable_shape_light = int(shape_light)
     s.enable_distant_light, s.enable_volume_scattering, s.enable_env_light = int(distant_light), int(volume), int(env_light)
     s.enable_russian_roulette, s.enable_indirect_clamp, s.indirect_limit = int(russian_roulette), int(indirect_clamp), indirect_limit
@@ -107,6 +108,7 @@ def library():
     L.ymrt_host_scene_query.argtypes = [vp, i, i, vp, sz]
     L.ymrt_scene_upload.argtypes = [vp, vp, vp, sz, ctypes.POINTER(vp)]
     L.ymrt_scene_free.argtypes = [vp]
+    L.ymrt_scene_set_sobol_matrices.argtypes = [vp, vp, sz]
     L.ymrt_render_forward.argtypes = [vp, ctypes.POINTER(RenderSetting), i, vp, i, ctypes.POINTER(Stats)]
     L.ymrt_render_tiles.argtypes = [vp, ctypes.POINTER(RenderSetting), i, i, i, vp, i, ctypes.POINTER(Stats)]
     L.ymrt_accumulate.argtypes = [vp, vp, vp, i]
@@ -243,6 +245,11 @@ class Scene:
         self.h = ctypes.c_void_p()
         _check(library().ymrt_scene_upload(ctx.h, host.h, _p(perm), perm.size, ctypes.byref(self.h)), ctx.h)
         self.host = host
+
+    def set_sobol_matrices(self, matrices: np.ndarray) -> None:
+        """Generator matrices for the Sobol sampler (4096 x 32 uint32)."""
+        m = np.ascontiguousarray(matrices, dtype=np.uint32)
+        _check(library().ymrt_scene_set_sobol_matrices(self.h, _p(m), m.size), self.ctx.h)
 
     def close(self):
         if self.h:

@@ -450,6 +450,7 @@ int ymrt_scene_upload(ymrt_context* ctx, const ymrt_host_scene* hs, const uint32
     if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
   }
   if (e != cudaSuccess) return ctx->cuda_fail(e, "uploading scene");
+  D.sampler_type = kSamplerHalton;
   D.instance_count = (uint32_t)s.instances.size();
   D.transform_count = (uint32_t)s.transforms.size();
   D.geometry_count = (uint32_t)s.geo_desc.size();
@@ -496,6 +497,18 @@ int ymrt_scene_upload(ymrt_context* ctx, const ymrt_host_scene* hs, const uint32
   return YMRT_OK;
 }
 
+int ymrt_scene_set_sobol_matrices(ymrt_scene* scene, const uint32_t* matrices, size_t count) {
+  if (!scene || !matrices) return YMRT_ERR_INVALID;
+  if (count != (size_t)4096 * 32)
+    return scene->ctx->fail(YMRT_ERR_INVALID, "Sobol generator matrices: expected 4096 x 32 words");
+  cudaSetDevice(scene->ctx->device);
+  std::vector<uint32_t> m(matrices, matrices + count);
+  cudaError_t e = scene->upload(m, &scene->dev.sobol_matrices);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(scene->ctx->stream);
+  if (e != cudaSuccess) return scene->ctx->cuda_fail(e, "uploading Sobol matrices");
+  return YMRT_OK;
+}
+
 void ymrt_scene_free(ymrt_scene* scene) {
   if (!scene) return;
   cudaSetDevice(scene->ctx->device);
@@ -511,7 +524,12 @@ int ymrt_render_tiles(ymrt_scene* sc, const ymrt_render_setting* setting, int fr
   RenderSetting rs;
   std::memcpy(&rs, setting, sizeof(rs));
   if (frame_index < 1) return ctx->fail(YMRT_ERR_INVALID, "frame_index starts at 1");
-  if (rs.sampler_type != 1) return ctx->fail(YMRT_ERR_UNSUPPORTED, "only the Halton sampler (sampler_type 1) is supported");
+  if (rs.sampler_type > 2u)
+    return ctx->fail(YMRT_ERR_UNSUPPORTED, "sampler_type must be 0 (PCG), 1 (Halton) or 2 (Sobol)");
+  if (rs.sampler_type == 2u && !sc->dev.sobol_matrices)
+    return ctx->fail(YMRT_ERR_INVALID, "the Sobol sampler needs its generator matrices (ymrt_scene_set_sobol_matrices)");
+  DeviceScene dev = sc->dev;
+  dev.sampler_type = rs.sampler_type;
   const bool volumes = rs.enable_volume_scattering && sc->dev.volume_count > 0;
   const uint32_t spp = (uint32_t)std::max(rs.ssp, 1);
   const uint32_t per_tile = (uint32_t)kTilePixels * spp;
@@ -540,7 +558,7 @@ int ymrt_render_tiles(ymrt_scene* sc, const ymrt_render_setting* setting, int fr
     if ((e = ctx->image_buf.ensure(img_bytes)) != cudaSuccess) return ctx->cuda_fail(e, "allocating image");
     image = ctx->image_buf.as<float4>();
   }
-  if ((e = upload_constants(sc->dev, ctx->primes.data(), ctx->prime_sums.data(), st)) != cudaSuccess)
+  if ((e = upload_constants(dev, ctx->primes.data(), ctx->prime_sums.data(), st)) != cudaSuccess)
     return ctx->cuda_fail(e, "uploading constants");
   if ((e = upload_setting(rs, st)) != cudaSuccess) return ctx->cuda_fail(e, "uploading render setting");
   WaveCounters* dc = ctx->counters_buf.as<WaveCounters>();
@@ -706,7 +724,12 @@ int ymrt_render_tiles_noalloc(ymrt_scene* sc, const ymrt_render_setting* setting
   RenderSetting rs;
   std::memcpy(&rs, setting, sizeof(rs));
   if (frame_index < 1) return ctx->fail(YMRT_ERR_INVALID, "frame_index starts at 1");
-  if (rs.sampler_type != 1) return ctx->fail(YMRT_ERR_UNSUPPORTED, "only the Halton sampler (sampler_type 1) is supported");
+  if (rs.sampler_type > 2u)
+    return ctx->fail(YMRT_ERR_UNSUPPORTED, "sampler_type must be 0 (PCG), 1 (Halton) or 2 (Sobol)");
+  if (rs.sampler_type == 2u && !sc->dev.sobol_matrices)
+    return ctx->fail(YMRT_ERR_INVALID, "the Sobol sampler needs its generator matrices (ymrt_scene_set_sobol_matrices)");
+  DeviceScene dev = sc->dev;
+  dev.sampler_type = rs.sampler_type;
   if (rs.enable_distant_light) return ctx->fail(YMRT_ERR_UNSUPPORTED, "distant lights are not supported yet");
   if (rs.enable_volume_scattering) return ctx->fail(YMRT_ERR_UNSUPPORTED, "volume scattering is not supported yet");
   const uint32_t spp = (uint32_t)std::max(rs.ssp, 1);
@@ -746,7 +769,7 @@ int ymrt_render_tiles_noalloc(ymrt_scene* sc, const ymrt_render_setting* setting
   cudaStream_t st = ctx->stream;
   float4* image = reinterpret_cast<float4*>(out_rgba_device);
   const size_t img_bytes = (size_t)W * Hh * sizeof(float4);
-  if ((e = upload_constants(sc->dev, ctx->primes.data(), ctx->prime_sums.data(), st)) != cudaSuccess)
+  if ((e = upload_constants(dev, ctx->primes.data(), ctx->prime_sums.data(), st)) != cudaSuccess)
     return ctx->cuda_fail(e, "uploading constants");
   if ((e = upload_setting(rs, st)) != cudaSuccess) return ctx->cuda_fail(e, "uploading render setting");
   cudaMemsetAsync(dc, 0, sizeof(WaveCounters), st);
@@ -754,7 +777,7 @@ int ymrt_render_tiles_noalloc(ymrt_scene* sc, const ymrt_render_setting* setting
   cudaEventRecord(ctx->ev_start, st);
   uint32_t live = 0;
   int a = 0;
-  uint64_t waves = 0, paths = 0, launches = 0, hits = 0;
+  uint64_t waves = 0, paths = 0, launches = 0, shaded = 0;
   while (live > 0 || cursor < t_end) {
     const uint32_t n_tiles = std::min<uint32_t>((cap - live) / per_tile, t_end - cursor);
     const uint32_t gen = n_tiles * per_tile;
@@ -764,7 +787,7 @@ int ymrt_render_tiles_noalloc(ymrt_scene* sc, const ymrt_render_setting* setting
       return ctx->cuda_fail(e, "reading wave counters");
     if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return ctx->cuda_fail(e, "wave");
     live = ctx->counters_host->next_count;
-    hits += ctx->counters_host->hit_count;
+    shaded += ctx->counters_host->hit_count;
     if (live > cap) return ctx->fail(YMRT_ERR_OVERFLOW, "path queue overflow");
     a ^= 1;
     cursor += n_tiles;
@@ -783,7 +806,7 @@ int ymrt_render_tiles_noalloc(ymrt_scene* sc, const ymrt_render_setting* setting
     stats->extension_rays = ctx->counters_host->extension_rays;
     stats->shadow_rays = ctx->counters_host->shadow_rays;
     stats->waves = waves;
-    stats->shaded_hits = hits;
+    stats->shaded_hits = shaded;
     stats->node_visits = ctx->counters_host->node_visits + ctx->counters_host->shadow_node_visits;
     stats->triangle_tests = ctx->counters_host->tri_tests + ctx->counters_host->shadow_tri_tests;
     stats->shadow_node_visits = ctx->counters_host->shadow_node_visits;

@@ -271,7 +271,7 @@ __device__ __forceinline__ float eval_mixed_phases(const float* w, const float* 
 
 // SampleTrHomogeneous (src/VolumeEval.cuh:18-78).
 __device__ __forceinline__ bool sample_tr_homogeneous(const DeviceScene& S, int n, const int* vidx, float t_max,
-                                                      vec3* tr_weight, float* dist, float* vw, HaltonState& hs) {
+                                                      vec3* tr_weight, float* dist, float* vw, PathSampler& hs) {
   *tr_weight = vec3(1.0f);
   *dist = kFloatMax;
   vec3 m(0.0f), ms(0.0f);
@@ -282,7 +282,7 @@ __device__ __forceinline__ bool sample_tr_homogeneous(const DeviceScene& S, int 
   }
   const float csum = m.x + m.y + m.z;
   const vec3 cw = csum > 0.0f ? (m / csum) : vec3(1.0f / 3.0f);
-  float u0 = halton_next(hs, S.halton_perm);
+  float u0 = sample1d(hs, S);
   int ch = 0;
   if (u0 < cw[0]) {
     ch = 0;
@@ -348,12 +348,12 @@ __device__ __forceinline__ void densities(const DeviceScene& S, int n, const int
 // the summed majorant with channel-wise real / null collision probabilities.
 __device__ __noinline__ bool sample_tr_heterogeneous(const DeviceScene& S, int n, const int* vidx, vec3 o, vec3 d,
                                                      float t_max, vec3* tr_weight, float* dist, float* vw,
-                                                     HaltonState& hs, uint32_t* errors) {
+                                                     PathSampler& hs, uint32_t* errors) {
   *tr_weight = vec3(1.0f);
   *dist = kFloatMax;
   Majorant M;
   volume_space_rays(S, n, vidx, o, d, t_max, M);
-  const float u0 = halton_next(hs, S.halton_perm);
+  const float u0 = sample1d(hs, S);
   int ch = 0;
   if (u0 < M.cw[0]) ch = 0;
   else if (u0 < M.cw[0] + M.cw[1]) ch = 1;
@@ -369,7 +369,7 @@ __device__ __noinline__ bool sample_tr_heterogeneous(const DeviceScene& S, int n
       atomicOr(errors, 4u);
       break;
     }
-    const float fpl = -logf(1.0f - halton_next(hs, S.halton_perm)) / M.m[ch];
+    const float fpl = -logf(1.0f - sample1d(hs, S)) / M.m[ch];
     if (acc + fpl > t_max) {
       const vec3 ptr = vexp(-M.m * (t_max - acc));
       tr *= ptr * nf;
@@ -386,7 +386,7 @@ __device__ __noinline__ bool sample_tr_heterogeneous(const DeviceScene& S, int n
     real.z = gmin(M.m.z > 0.0f ? mst.z * mrcp.z : 0.0f, 1.0f);
     const vec3 fake = vec3(1.0f) - real;
     const vec3 ptr = vexp(-M.m * fpl);
-    if (halton_next(hs, S.halton_perm) < real[ch]) {
+    if (sample1d(hs, S) < real[ch]) {
       tr *= ptr * mss * nf;
       pdf *= ptr * M.m * real * nf;
       break;
@@ -406,7 +406,7 @@ __device__ __noinline__ bool sample_tr_heterogeneous(const DeviceScene& S, int n
 // SampleVolumeScattering (src/VolumeEval.cuh:217-251).
 __device__ __forceinline__ bool sample_volume_scattering(const DeviceScene& S, vec3 o, vec3 d, int n, const int* vidx,
                                                          float t_max, vec3* tr_weight, float* dist, float* vw,
-                                                         HaltonState& hs, uint32_t* errors) {
+                                                         PathSampler& hs, uint32_t* errors) {
   if (S.volume_count == 0 || n == 0) return false;
   bool het = false;
   for (int i = 0; i < n; ++i)
@@ -421,10 +421,10 @@ __device__ __forceinline__ bool sample_volume_scattering(const DeviceScene& S, v
 // EvalTrHeterogeneous (src/VolumeEval.cuh:269-386): ratio-tracking style
 // transmittance with Russian roulette after 32 steps.
 __device__ __noinline__ vec3 eval_tr_heterogeneous(const DeviceScene& S, int n, const int* vidx, vec3 o, vec3 d,
-                                                   float t_max, HaltonState& hs, uint32_t* errors) {
+                                                   float t_max, PathSampler& hs, uint32_t* errors) {
   Majorant M;
   volume_space_rays(S, n, vidx, o, d, t_max, M);
-  const float u0 = halton_next(hs, S.halton_perm);
+  const float u0 = sample1d(hs, S);
   int ch = 0;
   if (u0 < M.cw[0]) ch = 0;
   else if (u0 < M.cw[0] + M.cw[1]) ch = 1;
@@ -440,7 +440,7 @@ __device__ __noinline__ vec3 eval_tr_heterogeneous(const DeviceScene& S, int n, 
       atomicOr(errors, 4u);
       break;
     }
-    const float fpl = -logf(1.0f - halton_next(hs, S.halton_perm)) / M.m[ch];
+    const float fpl = -logf(1.0f - sample1d(hs, S)) / M.m[ch];
     if (acc + fpl > t_max) {
       const vec3 ptr = vexp(-M.m * (t_max - acc));
       tr *= ptr * nf;
@@ -462,7 +462,7 @@ __device__ __noinline__ vec3 eval_tr_heterogeneous(const DeviceScene& S, int n, 
       const vec3 pt = tr * safe_rcp(dot(M.cw, pdf));
       float rr = gmax(pt.x, gmax(pt.y, pt.z));
       rr = gmin(rr, 1.0f);
-      if (halton_next(hs, S.halton_perm) < rr) tr /= gmax(rr, kMinColorEps);
+      if (sample1d(hs, S) < rr) tr /= gmax(rr, kMinColorEps);
       else break;
     }
     ++it;
@@ -472,7 +472,7 @@ __device__ __noinline__ vec3 eval_tr_heterogeneous(const DeviceScene& S, int n, 
 
 // EvalTr (src/VolumeEval.cuh:388-418).
 __device__ __forceinline__ vec3 eval_tr(const DeviceScene& S, vec3 o, vec3 d, const RayTransfer& rt, float t_max,
-                                        HaltonState& hs, uint32_t* errors) {
+                                        PathSampler& hs, uint32_t* errors) {
   if (S.volume_count == 0) return vec3(1.0f);
   int vidx[kMaxBoundaryRecord];
   const int n = current_volumes(rt, S.volume_count, vidx);

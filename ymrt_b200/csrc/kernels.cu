@@ -36,14 +36,14 @@ __constant__ RenderSetting c_setting;
 // ---------------------------------------------------------------- paths ---
 
 __device__ __forceinline__ void store_path(const PathPool& P, uint32_t i, vec3 o, vec3 d, vec3 tp, vec3 rad, uint32_t pixel,
-                                           uint32_t flags, uint32_t last_inst, uint32_t last_tri, const HaltonState& hs) {
+                                           uint32_t flags, uint32_t last_inst, uint32_t last_tri, const PathSampler& hs) {
   P.ray_o[i] = make_float4(o.x, o.y, o.z, 0.0f);
   P.ray_d[i] = make_float4(d.x, d.y, d.z, 0.0f);
   P.throughput[i] = make_float4(tp.x, tp.y, tp.z, 0.0f);
   P.radiance[i] = make_float4(rad.x, rad.y, rad.z, 0.0f);
   P.pixel_flags[i] = make_uint2(pixel, flags);
   P.last_hit[i] = make_uint2(last_inst, last_tri);
-  P.sampler[i] = make_uint4((uint32_t)hs.index, (uint32_t)(hs.index >> 32), hs.dim, 0u);
+  P.sampler[i] = make_uint4((uint32_t)hs.index, (uint32_t)(hs.index >> 32), hs.dim, hs.aux);
 }
 
 __device__ __forceinline__ void accumulate_pixel(float4* image, uint32_t pixel, vec3 light, float inv_spp) {
@@ -95,15 +95,27 @@ __global__ void __launch_bounds__(256) k_generate(PathPool P, uint32_t base, uin
     return;
   }
   const uint32_t pixel = py * (uint32_t)S.width + px;
-  const uint64_t sample_index =
-      halton_index(S, (int)px, (int)py, (frame_index - 1) * c_setting.ssp + (int)pixel_sample);
-  HaltonState hs{sample_index, 2u};
-  float ox = radical_inverse_2(sample_index);
-  float oy = radical_inverse_3(sample_index);
-  ox = ox * S.halton_x_scale - float(px);
-  oy = oy * S.halton_y_scale - float(py);
-  ox = gmin(gmax(ox, 0.000001f), 0.999999f);
-  oy = gmin(gmax(oy, 0.000001f), 0.999999f);
+  // Sampler set-up and pixel jitter, src/Shading.cu:1690-1711.
+  PathSampler hs{0, 0u, 0u};
+  float ox = 0.5f, oy = 0.5f;
+  if (S.sampler_type == kSamplerHalton) {
+    const uint64_t sample_index =
+        halton_index(S, (int)px, (int)py, (frame_index - 1) * c_setting.ssp + (int)pixel_sample);
+    hs = PathSampler{sample_index, 2u, 0u};
+    ox = radical_inverse_2(sample_index);
+    oy = radical_inverse_3(sample_index);
+    ox = ox * S.halton_x_scale - float(px);
+    oy = oy * S.halton_y_scale - float(py);
+    ox = gmin(gmax(ox, 0.000001f), 0.999999f);
+    oy = gmin(gmax(oy, 0.000001f), 0.999999f);
+  } else if (S.sampler_type == kSamplerPcg) {
+    hs = PathSampler{(uint64_t)pixel | ((uint64_t)pixel_sample << 32), 0u, (uint32_t)(frame_index - 1)};
+    sample2d(hs, S, &ox, &oy);
+  } else {
+    const uint32_t sample = (uint32_t)(frame_index - 1) * (uint32_t)c_setting.ssp + pixel_sample;
+    hs = PathSampler{(uint64_t)sample | ((uint64_t)pixel << 32), 1u, 0u};
+    sample2d(hs, S, &ox, &oy);
+  }
   // Camera::GenerateRay (src/Camera.h:164-170) + Ray's normalising constructor.
   const CameraDesc& cam = S.camera;
   const float ndc_x = float(px + ox) / float(S.width);
@@ -189,7 +201,7 @@ __global__ void __launch_bounds__(kTraceBlock, 5) k_extend(PathPool P, uint32_t 
       rt.max_priority_record_index = -1;
       if (rt.record_count > 0) rt = P.transfer[i];
       const uint4 s4 = P.sampler[i];
-      HaltonState hs{(uint64_t)s4.x | ((uint64_t)s4.y << 32), s4.z};
+      PathSampler hs{(uint64_t)s4.x | ((uint64_t)s4.y << 32), s4.z, s4.w};
       int vidx[kMaxBoundaryRecord];
       const int n = current_volumes(rt, S.volume_count, vidx);
       vec3 trw(1.0f);
@@ -199,7 +211,7 @@ __global__ void __launch_bounds__(kTraceBlock, 5) k_extend(PathPool P, uint32_t 
                                                &counters->errors);
       tp *= trw;
       P.throughput[i] = make_float4(tp.x, tp.y, tp.z, 0.0f);
-      P.sampler[i] = make_uint4((uint32_t)hs.index, (uint32_t)(hs.index >> 32), hs.dim, 0u);
+      P.sampler[i] = make_uint4((uint32_t)hs.index, (uint32_t)(hs.index >> 32), hs.dim, hs.aux);
       if (hv) {
         volume_hit = true;
         vol_pos = o + d * dist;
@@ -347,7 +359,7 @@ __device__ __forceinline__ float ex_ior(const RayTransfer& rt, uint32_t hit_prim
 // (TraceTr, src/VolumeEval.cuh:420-468). `rt` is the shadow ray's own copy of
 // the nested-media stack; `o`/`d`/`tmax` and the last hit are the shadow ray.
 __device__ __noinline__ vec3 trace_tr(const DeviceScene& S, TraversalStack& st, vec3 o, vec3 d, float tmax,
-                                      uint32_t last_inst, uint32_t last_tri, RayTransfer& rt, HaltonState& hs,
+                                      uint32_t last_inst, uint32_t last_tri, RayTransfer& rt, PathSampler& hs,
                                       uint32_t* errors, uint32_t* tests, uint32_t* nodes) {
   if (S.volume_count == 0) return vec3(1.0f);
   vec3 tr(1.0f);
@@ -424,7 +436,7 @@ struct SurfaceNee {
 // reference's EvalShapeLight / EvalDistantLight).
 template <bool kVol>
 __device__ __forceinline__ vec3 surface_shadow_tr(const DeviceScene& S, TraversalStack& st, const SurfaceNee& c, vec3 so,
-                                                  vec3 ldir, float maxd, bool tb, HaltonState& hs, uint32_t* errors,
+                                                  vec3 ldir, float maxd, bool tb, PathSampler& hs, uint32_t* errors,
                                                   uint32_t* tests, uint32_t* nodes) {
   if (!kVol) return vec3(1.0f);
   RayTransfer srt = *c.rt;
@@ -469,7 +481,7 @@ template <bool kVol, bool kDefer>
 __device__ __forceinline__ void nee_shadow_ray(const DeviceScene& S, TraversalStack& st, const SurfaceNee& c,
                                                const ShadowEmit& em, vec3 so, vec3 ldir, float maxd, bool tb,
                                                float mis, vec3 fc, vec3 Lc, float mul, float div, vec3* direct,
-                                               HaltonState& hs, uint32_t* shadow_rays, uint32_t* tests,
+                                               PathSampler& hs, uint32_t* shadow_rays, uint32_t* tests,
                                                uint32_t* nodes, uint32_t* errors) {
   ++*shadow_rays;
   if (kDefer) {
@@ -485,19 +497,19 @@ __device__ __forceinline__ void nee_shadow_ray(const DeviceScene& S, TraversalSt
 // EvalShapeLight (src/Shading.cu:294-417).
 template <bool kVol, bool kDefer>
 __device__ __forceinline__ vec3 eval_shape_light(const DeviceScene& S, TraversalStack& st, const LayeredBsdf& B,
-                                                 const SurfaceNee& c, const ShadowEmit& em, HaltonState& hs,
+                                                 const SurfaceNee& c, const ShadowEmit& em, PathSampler& hs,
                                                  uint32_t* shadow_rays, uint32_t* tests, uint32_t* nodes,
                                                  uint32_t* errors) {
   if (S.shape_light_count == 0) return vec3(0.0f);
   vec3 direct(0.0f);
   const vec3 wo = B.to_local(-c.ray_dir);
   float select_pdf = 0.0f;
-  const int li = sample_light_power(S, halton_next(hs, S.halton_perm), &select_pdf);
+  const int li = sample_light_power(S, sample1d(hs, S), &select_pdf);
   const ShapeLight L = S.shape_lights[li];
   const LightTri lt = load_light_tri(S, L);
   {
     float u0, u1;
-    halton_next2(hs, S.halton_perm, &u0, &u1);
+    sample2d(hs, S, &u0, &u1);
     vec3 ldir(0.0f), lpos(0.0f), lerr(0.0f), lng(0.0f), Li(0.0f);
     float lpdf = 0.0f;
     const bool valid = light_sample_li(lt, L.area, c.p, u0, u1, &ldir, &lpos, &lerr, &lng, &Li, &lpdf);
@@ -517,7 +529,7 @@ __device__ __forceinline__ vec3 eval_shape_light(const DeviceScene& S, Traversal
   }
   {
     float u0, u1, u2;
-    halton_next3(hs, S.halton_perm, &u0, &u1, &u2);
+    sample3d(hs, S, &u0, &u1, &u2);
     vec3 bw, bwi;
     float bpdf = 0.0f;
     if (bsdf_sample(B, wo, &bw, &bwi, &bpdf, u0, u1, u2)) {
@@ -543,18 +555,18 @@ __device__ __forceinline__ vec3 eval_shape_light(const DeviceScene& S, Traversal
 // EvalDistantLight (src/Shading.cu:83-198).
 template <bool kVol, bool kDefer>
 __device__ __forceinline__ vec3 eval_distant_light(const DeviceScene& S, TraversalStack& st, const LayeredBsdf& B,
-                                                   const SurfaceNee& c, const ShadowEmit& em, HaltonState& hs,
+                                                   const SurfaceNee& c, const ShadowEmit& em, PathSampler& hs,
                                                    uint32_t* shadow_rays, uint32_t* tests, uint32_t* nodes,
                                                    uint32_t* errors) {
   if (S.distant_light_count == 0) return vec3(0.0f);
   vec3 direct(0.0f);
   const vec3 wo = B.to_local(-c.ray_dir);
   const float select_pdf = 1.0f / float(S.distant_light_count);
-  const int li = gmax(gmin((int)(halton_next(hs, S.halton_perm) * S.distant_light_count), (int)S.distant_light_count - 1), 0);
+  const int li = gmax(gmin((int)(sample1d(hs, S) * S.distant_light_count), (int)S.distant_light_count - 1), 0);
   const DistantLight L = S.distant_lights[li];
   {
     float u0, u1;
-    halton_next2(hs, S.halton_perm, &u0, &u1);
+    sample2d(hs, S, &u0, &u1);
     vec3 ldir(0.0f), Li(0.0f);
     float lpdf = 0.0f;
     distant_sample_li(S, L, u0, u1, &ldir, &Li, &lpdf);
@@ -573,7 +585,7 @@ __device__ __forceinline__ vec3 eval_distant_light(const DeviceScene& S, Travers
   }
   {
     float u0, u1, u2;
-    halton_next3(hs, S.halton_perm, &u0, &u1, &u2);
+    sample3d(hs, S, &u0, &u1, &u2);
     vec3 bw, bwi;
     float bpdf = 0.0f;
     if (bsdf_sample(B, wo, &bw, &bwi, &bpdf, u0, u1, u2)) {
@@ -598,17 +610,17 @@ __device__ __forceinline__ vec3 eval_distant_light(const DeviceScene& S, Travers
 // next-event estimation at a scattering point inside the media.
 __device__ __noinline__ vec3 eval_volume_lights(const DeviceScene& S, TraversalStack& st, bool distant, int n,
                                                 const float* gs, const float* vw, vec3 ray_dir, const RayTransfer& rt,
-                                                vec3 pos, HaltonState& hs, uint32_t* shadow_rays, uint32_t* tests,
+                                                vec3 pos, PathSampler& hs, uint32_t* shadow_rays, uint32_t* tests,
                                                 uint32_t* nodes, uint32_t* errors) {
   vec3 direct(0.0f);
   if (distant) {
     if (S.distant_light_count == 0 || n == 0) return vec3(0.0f);
     const float select_pdf = 1.0f / float(S.distant_light_count);
-    const int li = gmax(gmin((int)(halton_next(hs, S.halton_perm) * S.distant_light_count), (int)S.distant_light_count - 1), 0);
+    const int li = gmax(gmin((int)(sample1d(hs, S) * S.distant_light_count), (int)S.distant_light_count - 1), 0);
     const DistantLight L = S.distant_lights[li];
     {
       float u0, u1;
-      halton_next2(hs, S.halton_perm, &u0, &u1);
+      sample2d(hs, S, &u0, &u1);
       vec3 ldir(0.0f), Li(0.0f);
       float lpdf = 0.0f;
       distant_sample_li(S, L, u0, u1, &ldir, &Li, &lpdf);
@@ -626,7 +638,7 @@ __device__ __noinline__ vec3 eval_volume_lights(const DeviceScene& S, TraversalS
     }
     {
       float u0, u1;
-      halton_next2(hs, S.halton_perm, &u0, &u1);
+      sample2d(hs, S, &u0, &u1);
       vec3 pwi;
       float pspdf = 0.0f, pw = 0.0f;
       if (sample_mixed_phases(vw, gs, n, u0, u1, -ray_dir, &pw, &pwi, &pspdf)) {
@@ -647,12 +659,12 @@ __device__ __noinline__ vec3 eval_volume_lights(const DeviceScene& S, TraversalS
   }
   if (S.shape_light_count == 0 || n == 0) return vec3(0.0f);
   float select_pdf = 0.0f;
-  const int li = sample_light_power(S, halton_next(hs, S.halton_perm), &select_pdf);
+  const int li = sample_light_power(S, sample1d(hs, S), &select_pdf);
   const ShapeLight L = S.shape_lights[li];
   const LightTri lt = load_light_tri(S, L);
   {
     float u0, u1;
-    halton_next2(hs, S.halton_perm, &u0, &u1);
+    sample2d(hs, S, &u0, &u1);
     vec3 ldir(0.0f), lpos(0.0f), lerr(0.0f), lng(0.0f), Li(0.0f);
     float lpdf = 0.0f;
     const bool valid = light_sample_li(lt, L.area, pos, u0, u1, &ldir, &lpos, &lerr, &lng, &Li, &lpdf);
@@ -671,7 +683,7 @@ __device__ __noinline__ vec3 eval_volume_lights(const DeviceScene& S, TraversalS
   }
   {
     float u0, u1;
-    halton_next2(hs, S.halton_perm, &u0, &u1);
+    sample2d(hs, S, &u0, &u1);
     vec3 pwi;
     float pspdf = 0.0f, pw = 0.0f;
     if (sample_mixed_phases(vw, gs, n, u0, u1, -ray_dir, &pw, &pwi, &pspdf)) {
@@ -713,7 +725,7 @@ __global__ void __launch_bounds__(kTraceBlock) k_shade(PathPool P, uint32_t coun
 
   vec3 new_o, new_d, tp, rad;
   uint32_t new_flags = 0, new_last_inst = kEmpty, new_last_tri = kEmpty;
-  HaltonState hs{0, 0};
+  PathSampler hs{0, 0u, 0u};
   RayTransfer rt;
   rt.record_count = 0;
   rt.max_priority_record_index = -1;
@@ -730,6 +742,7 @@ __global__ void __launch_bounds__(kTraceBlock) k_shade(PathPool P, uint32_t coun
     const uint4 s4 = P.sampler[i];
     hs.index = (uint64_t)s4.x | ((uint64_t)s4.y << 32);
     hs.dim = s4.z;
+    hs.aux = s4.w;
     int depth = (int)(pf.y & kFlagDepthMask);
     bool never_scatter = (pf.y & kFlagNeverScatter) != 0;
     const uint32_t sample_bits = pf.y & ~(kFlagDepthMask | kFlagNeverScatter | kFlagCameraRay | kFlagDead);
@@ -770,14 +783,14 @@ __global__ void __launch_bounds__(kTraceBlock) k_shade(PathPool P, uint32_t coun
       vec3 wi;
       float pdf = 0.0f, pw = 0.0f;
       float u0, u1;
-      halton_next2(hs, S.halton_perm, &u0, &u1);
+      sample2d(hs, S, &u0, &u1);
       bool terminate = !sample_mixed_phases(vw, gs, n, u0, u1, -rd, &pw, &wi, &pdf);
       if (!terminate) {
         tp *= pw;
         float rr = gmax(tp.x, gmax(tp.y, tp.z));
         rr = gmin(rr, 1.0f);
         if (depth + 1 > rs.ray_depth) {
-          if (rs.enable_russian_roulette && halton_next(hs, S.halton_perm) < rr) tp /= gmax(rr, kMinColorEps);
+          if (rs.enable_russian_roulette && sample1d(hs, S) < rr) tp /= gmax(rr, kMinColorEps);
           else terminate = true;
         }
       }
@@ -860,7 +873,7 @@ __global__ void __launch_bounds__(kTraceBlock) k_shade(PathPool P, uint32_t coun
         vec3 w, wi;
         float pdf = 0.0f;
         float u0, u1, u2;
-        halton_next3(hs, S.halton_perm, &u0, &u1, &u2);
+        sample3d(hs, S, &u0, &u1, &u2);
         const bool valid = bsdf_sample(B, wo, &w, &wi, &pdf, u0, u1, u2);
         if (!valid) {
           accumulate_pixel(image, pf.x, rad, inv_spp);
@@ -870,7 +883,7 @@ __global__ void __launch_bounds__(kTraceBlock) k_shade(PathPool P, uint32_t coun
           rr = gmin(rr, 1.0f);
           bool terminate = false;
           if (depth + 1 > rs.ray_depth) {
-            if (rs.enable_russian_roulette && halton_next(hs, S.halton_perm) < rr) tp /= gmax(rr, kMinColorEps);
+            if (rs.enable_russian_roulette && sample1d(hs, S) < rr) tp /= gmax(rr, kMinColorEps);
             else terminate = true;
           }
           if (!terminate) {
@@ -1023,8 +1036,8 @@ __global__ void k_debug_halton(int n, const int* px, const int* py, const int* s
   oy = oy * S.halton_y_scale - float(py[i]);
   offset[2 * i] = gmin(gmax(ox, 0.000001f), 0.999999f);
   offset[2 * i + 1] = gmin(gmax(oy, 0.000001f), 0.999999f);
-  HaltonState hs{idx, 2u};
-  for (int d = 0; d < n_dims; ++d) dims[(size_t)i * n_dims + d] = halton_next(hs, S.halton_perm);
+  PathSampler hs{idx, 2u, 0u};
+  for (int d = 0; d < n_dims; ++d) dims[(size_t)i * n_dims + d] = halton_draw(hs, S.halton_perm);
 }
 
 // ------------------------------------------------------------ launchers ---

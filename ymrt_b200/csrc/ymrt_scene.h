@@ -196,6 +196,9 @@ struct GeometryDesc {
 };
 
 // Everything the kernels read, as device pointers.
+// RenderSetting::sampler_type values (src/RandomSampler.cuh:617-620).
+constexpr uint32_t kSamplerPcg = 0, kSamplerHalton = 1, kSamplerSobol = 2;
+
 struct DeviceScene {
   // instances
   uint32_t instance_count;
@@ -232,7 +235,9 @@ struct DeviceScene {
   uint32_t texture_count;
   const Texture* textures;
   // sampler
+  uint32_t sampler_type;            // RenderSetting::sampler_type of the current render
   const uint32_t* halton_perm;
+  const uint32_t* sobol_matrices;   // 4096 dimensions x 32 columns (input; null until set)
   // camera
   CameraDesc camera;
   int width, height;
