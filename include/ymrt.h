@@ -166,6 +166,22 @@ int ymrt_render_forward(ymrt_scene* scene, const ymrt_render_setting* setting, i
 /* Same, restricted to tiles [tile_begin, tile_end) of the 16x16 tiling. */
 int ymrt_render_tiles(ymrt_scene* scene, const ymrt_render_setting* setting, int frame_index, int tile_begin,
                       int tile_end, float* out_rgba, int out_on_device, ymrt_stats* stats);
+
+/* One render of a batch. */
+typedef struct ymrt_job {
+  ymrt_scene* scene;             /* uploaded scene (its resolution and camera) */
+  ymrt_render_setting setting;
+  int frame_index;               /* >= 1 */
+  int tile_begin, tile_end;      /* 16x16 tiles to render; 0, 0 = all */
+  float* out_rgba_device;        /* width*height*4 floats of device memory, overwritten */
+} ymrt_job;
+
+/* Renders n_jobs renders (scenes, resolutions, spp and settings may all
+ * differ; scenes must belong to ctx) together: their paths share the wave
+ * queues, so small renders keep the GPU full. Same results as rendering each
+ * job with ymrt_render_tiles. No counterpart in the reference, which renders
+ * one frame per PathTracingExecuteTask. */
+int ymrt_render_batch(ymrt_context* ctx, const ymrt_job* jobs, int n_jobs, ymrt_stats* stats);
 /* Allocation-free variant of ymrt_render_tiles, for callers that cannot
  * allocate device memory while rendering (a host with a fixed up-front
  * memory budget or its own pool allocator, or code that must not let a

@@ -172,10 +172,37 @@ def shading_source(arg_order: str) -> str:
     out = (_HELPER + f'#line 1 "{src}"\n' + head + _COUNTERS + f'#line {line_of_body} "{src}"\n' + body)
     with open(dst, "w") as f:
         f.write(out)
+    n_pairs = _sampler_headers(arg_order, gen_dir)
     with open(os.path.join(gen_dir, "Shading.cu.sites"), "w") as f:
         f.write(f"{n} argument lists sequenced, {n_trace} TraceRay and {n_shadow} BVHTraverseShadow calls counted, "
-                f"{n_prio} GetMaxPriorityRecord reads made direct\n")
+                f"{n_prio} GetMaxPriorityRecord reads made direct, {n_pairs} two-draw constructors in "
+                f"RandomSampler.cuh sequenced\n")
     return dst
+
+
+_PAIR = re.compile(r"return glm::vec2\(Random1D\(\), Random1D\(\)\);")
+
+
+def _sampler_headers(arg_order: str, gen_dir: str) -> int:
+    """The PCG and Sobol samplers' Random2D / SamplePixelOffset build a vec2
+    from two Random1D() calls (src/RandomSampler.cuh:401-405, 544-548); the
+    build-time copy of the header draws them first then second, as the
+    device build evaluates them. VolumeEval.cuh, the header's only other
+    includer, is copied beside it so that it picks the copy up."""
+    src_dir = os.path.join(REF, "src")
+    with open(os.path.join(src_dir, "RandomSampler.cuh"), "r", encoding="utf-8", errors="replace") as f:
+        text = f.read()
+    n = 0
+    if arg_order == "ltr":
+        text, n = _PAIR.subn("{ const float ymrt_first = Random1D(); const float ymrt_second = Random1D(); "
+                             "return glm::vec2(ymrt_first, ymrt_second); }", text)
+    with open(os.path.join(gen_dir, "RandomSampler.cuh"), "w") as f:
+        f.write(f'#line 1 "{os.path.join(src_dir, "RandomSampler.cuh")}"\n' + text)
+    with open(os.path.join(src_dir, "VolumeEval.cuh"), "r", encoding="utf-8", errors="replace") as f:
+        vol = f.read()
+    with open(os.path.join(gen_dir, "VolumeEval.cuh"), "w") as f:
+        f.write(f'#line 1 "{os.path.join(src_dir, "VolumeEval.cuh")}"\n' + vol)
+    return n
 
 
 # ---------------------------------------------------------------------------

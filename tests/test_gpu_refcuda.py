@@ -100,3 +100,18 @@ def test_converged_cornell_vs_reference_default_build(ctx, refgpu, cornell_path,
     assert rmse <= 1e-3, rmse
     ours.close()
     ref.close()
+
+
+@pytest.mark.parametrize("sampler_type", [0, 2])
+def test_pcg_and_sobol_vs_reference_cuda(ctx, refgpu, cornell_path, halton_perm, sampler_type):
+    ours, ref = _pair(ctx, refgpu, cornell_path, halton_perm, 256, 256, exact=True)
+    if sampler_type == 2:
+        ours.set_sobol_matrices(refgpu.sobol_matrices())
+    ref.set_settings(spp=1, ray_depth=8, sampler_type=sampler_type)
+    a, _ = ours.render(Y.default_setting(spp=1, ray_depth=8, sampler_type=sampler_type), 2)
+    b = ref.render_frame(2)
+    assert np.array_equal(a[..., 3], b[..., 3])
+    bad = _bad(a, b)
+    assert bad.mean() <= 1e-3, f"{bad.sum()} of {bad.size} pixels differ beyond 1e-5 relative"
+    ours.close()
+    ref.close()

@@ -67,6 +67,11 @@ def default_setting(spp=1, ray_depth=8, shape_light=True, distant_light=False, v
     return s
 
 
+class Job(ctypes.Structure):
+    _fields_ = [("scene", ctypes.c_void_p), ("setting", RenderSetting), ("frame_index", ctypes.c_int),
+                ("tile_begin", ctypes.c_int), ("tile_end", ctypes.c_int), ("out_rgba_device", ctypes.c_void_p)]
+
+
 class Stats(ctypes.Structure):
     _fields_ = [
         ("paths", ctypes.c_uint64), ("extension_rays", ctypes.c_uint64), ("shadow_rays", ctypes.c_uint64),
@@ -109,6 +114,7 @@ def library():
     L.ymrt_scene_upload.argtypes = [vp, vp, vp, sz, ctypes.POINTER(vp)]
     L.ymrt_scene_free.argtypes = [vp]
     L.ymrt_scene_set_sobol_matrices.argtypes = [vp, vp, sz]
+    L.ymrt_render_batch.argtypes = [vp, ctypes.POINTER(Job), i, ctypes.POINTER(Stats)]
     L.ymrt_render_forward.argtypes = [vp, ctypes.POINTER(RenderSetting), i, vp, i, ctypes.POINTER(Stats)]
     L.ymrt_render_tiles.argtypes = [vp, ctypes.POINTER(RenderSetting), i, i, i, vp, i, ctypes.POINTER(Stats)]
     L.ymrt_accumulate.argtypes = [vp, vp, vp, i]
@@ -312,3 +318,24 @@ class Scene:
         _check(library().ymrt_debug_halton(self.h, n, _p(px), _p(py), _p(sm), n_dims, _p(idx), _p(off), _p(dims)),
                self.ctx.h)
         return idx, off, dims[:, :n_dims]
+
+
+def render_batch(ctx: Context, renders) -> Stats:
+    """Renders several (scene, setting, frame_index, out, tile_begin, tile_end)
+    tuples in one batch; each `out` is a torch CUDA float32 tensor of its
+    scene's (H, W, 4) shape and receives that render."""
+    jobs = (Job * len(renders))()
+    for k, r in enumerate(renders):
+        scene, setting, frame, out = r[:4]
+        tb, te = (r[4], r[5]) if len(r) > 4 else (0, 0)
+        assert out.is_cuda and out.dtype.is_floating_point and out.is_contiguous()
+        assert out.numel() == scene.width * scene.height * 4
+        jobs[k].scene = scene.h.value if isinstance(scene.h, ctypes.c_void_p) else scene.h
+        jobs[k].setting = setting
+        jobs[k].frame_index = frame
+        jobs[k].tile_begin, jobs[k].tile_end = tb, te
+        jobs[k].out_rgba_device = out.data_ptr()
+    stats = Stats()
+    _check(library().ymrt_render_batch(ctx.h, jobs, len(renders), ctypes.byref(stats)), ctx.h)
+    return stats
+

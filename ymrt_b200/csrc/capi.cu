@@ -72,7 +72,7 @@ struct ymrt_context {
   std::string error;
   uint32_t capacity = 1u << 21;
   // two path pools (ping-pong), one hit pool, counters
-  DeviceBuffer pool_buf[2], hit_buf, counters_buf, image_buf;
+  DeviceBuffer pool_buf[2], hit_buf, counters_buf, image_buf, jobs_buf;
   PathPool pool[2]{};
   HitPool hits{};
   uint32_t pool_capacity = 0;
@@ -235,6 +235,7 @@ void ymrt_destroy(ymrt_context* ctx) {
   for (auto& b : ctx->pool_buf) b.release();
   ctx->hit_buf.release();
   ctx->counters_buf.release();
+  ctx->jobs_buf.release();
   ctx->image_buf.release();
   if (ctx->counters_host) cudaFreeHost(ctx->counters_host);
   if (ctx->ev_start) cudaEventDestroy(ctx->ev_start);
@@ -516,11 +517,32 @@ void ymrt_scene_free(ymrt_scene* scene) {
   delete scene;
 }
 
-int ymrt_render_tiles(ymrt_scene* sc, const ymrt_render_setting* setting, int frame_index, int tile_begin, int tile_end,
-                      float* out_rgba, int out_on_device, ymrt_stats* stats) {
-  if (!sc || !setting || !out_rgba) return YMRT_ERR_INVALID;
-  ymrt_context* ctx = sc->ctx;
+}  // extern "C"
+
+namespace {
+
+// Device memory one batch renders with: the context's queues, or the fixed
+// array of the allocation-free entry point.
+struct BatchMemory {
+  PathPool pool[2];
+  HitPool hits;
+  WaveCounters* counters = nullptr;
+  JobDesc* jobs = nullptr;  // device job table
+  uint32_t capacity = 0;
+};
+
+struct BatchResult {
+  uint64_t paths = 0, waves = 0, launches = 0, hits = 0;
+  double ms = 0.0;
+  double stage_ms[5] = {0.0, 0.0, 0.0, 0.0, 0.0};  // generate, extend, sort, shade, connect
+};
+
+// Checks one render's arguments and fills its job (path range left at 0).
+int make_job(ymrt_context* ctx, ymrt_scene* sc, const ymrt_render_setting* setting, int frame_index, int tile_begin,
+             int tile_end, float4* image, JobDesc* job) {
   static_assert(sizeof(ymrt_render_setting) == sizeof(RenderSetting), "render setting layout");
+  if (!sc || !setting || !image) return ctx->fail(YMRT_ERR_INVALID, "null scene, setting or output");
+  if (sc->ctx != ctx) return ctx->fail(YMRT_ERR_INVALID, "scene belongs to another context");
   RenderSetting rs;
   std::memcpy(&rs, setting, sizeof(rs));
   if (frame_index < 1) return ctx->fail(YMRT_ERR_INVALID, "frame_index starts at 1");
@@ -528,106 +550,209 @@ int ymrt_render_tiles(ymrt_scene* sc, const ymrt_render_setting* setting, int fr
     return ctx->fail(YMRT_ERR_UNSUPPORTED, "sampler_type must be 0 (PCG), 1 (Halton) or 2 (Sobol)");
   if (rs.sampler_type == 2u && !sc->dev.sobol_matrices)
     return ctx->fail(YMRT_ERR_INVALID, "the Sobol sampler needs its generator matrices (ymrt_scene_set_sobol_matrices)");
-  DeviceScene dev = sc->dev;
-  dev.sampler_type = rs.sampler_type;
-  const bool volumes = rs.enable_volume_scattering && sc->dev.volume_count > 0;
-  const uint32_t spp = (uint32_t)std::max(rs.ssp, 1);
-  const uint32_t per_tile = (uint32_t)kTilePixels * spp;
-  cudaSetDevice(ctx->device);
-  int rc = ctx->ensure_pools();
-  if (rc != YMRT_OK) return rc;
-  if (per_tile > ctx->capacity) return ctx->fail(YMRT_ERR_INVALID, "queue capacity smaller than one tile of samples");
-  WaveOptions opt;
-  opt.volumes = volumes;
-  opt.sort_hits = ctx->sort_hits;
-  opt.defer_shadows = ctx->defer_shadows && !volumes && !rs.enable_indirect_clamp;
-  if (opt.defer_shadows) {
-    if ((rc = ctx->ensure_shadow_queue()) != YMRT_OK) return rc;
-    opt.shadow_queue = ctx->shadow_queue;
-  }
-  const uint32_t W = sc->width, Hh = sc->height;
-  const uint32_t tiles_x = (W + kTileRes - 1) / kTileRes, tiles_y = (Hh + kTileRes - 1) / kTileRes;
+  if (tile_begin < 0) return ctx->fail(YMRT_ERR_INVALID, "tile_begin < 0");
+  const uint32_t tiles_x = (sc->width + kTileRes - 1) / kTileRes, tiles_y = (sc->height + kTileRes - 1) / kTileRes;
   const uint32_t total_tiles = tiles_x * tiles_y;
   const uint32_t t_end = tile_end <= 0 ? total_tiles : std::min<uint32_t>((uint32_t)tile_end, total_tiles);
-  uint32_t cursor = (uint32_t)std::max(tile_begin, 0);
+  const uint32_t t_begin = std::min<uint32_t>((uint32_t)tile_begin, t_end);
+  std::memset(job, 0, sizeof(*job));
+  job->scene = sc->dev;
+  job->scene.sampler_type = rs.sampler_type;
+  if (rs.enable_volume_scattering && sc->dev.volume_count == 0) rs.enable_volume_scattering = false;
+  job->setting = rs;
+  job->image = image;
+  job->frame_index = frame_index;
+  job->spp = (uint32_t)std::max(rs.ssp, 1);
+  job->tiles_x = tiles_x;
+  job->tile_begin = t_begin;
+  job->path_count = (unsigned long long)(t_end - t_begin) * kTilePixels * job->spp;
+  return YMRT_OK;
+}
+
+// Renders a batch of jobs (paths numbered job after job) with the
+// host-driven wave loop: one synchronisation per wave to read the number of
+// continuing paths. The job images must be zeroed by the caller.
+int run_batch(ymrt_context* ctx, const BatchMemory& M, std::vector<JobDesc>& jobs, const WaveOptions& opt,
+              bool profiling, BatchResult* r) {
+  cudaStream_t st = ctx->stream;
+  cudaError_t e;
+  unsigned long long total = 0;
+  for (JobDesc& j : jobs) {
+    j.path_begin = total;
+    total += j.path_count;
+  }
+  if ((e = cudaMemcpyAsync(M.jobs, jobs.data(), sizeof(JobDesc) * jobs.size(), cudaMemcpyHostToDevice, st)) !=
+      cudaSuccess)
+    return ctx->cuda_fail(e, "uploading the job table");
+  cudaMemsetAsync(M.counters, 0, sizeof(WaveCounters), st);
+  cudaEventRecord(ctx->ev_start, st);
+  uint32_t live = 0;
+  unsigned long long cursor = 0;
+  int a = 0;
+  while (live > 0 || cursor < total) {
+    const uint32_t gen = (uint32_t)std::min<unsigned long long>(M.capacity - live, total - cursor);
+    r->launches += launch_wave(M.pool[a], M.pool[a ^ 1], M.hits, live, gen, cursor, M.jobs, (uint32_t)jobs.size(),
+                               M.counters, opt, profiling ? ctx->ev_stage : nullptr, st);
+    if ((e = cudaMemcpyAsync(ctx->counters_host, M.counters, sizeof(WaveCounters), cudaMemcpyDeviceToHost, st)) !=
+        cudaSuccess)
+      return ctx->cuda_fail(e, "reading wave counters");
+    if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return ctx->cuda_fail(e, "wave");
+    if (profiling) {
+      for (int k = 0; k < 5; ++k) {
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, ctx->ev_stage[k], ctx->ev_stage[k + 1]);
+        r->stage_ms[k] += ms;
+      }
+    }
+    live = ctx->counters_host->next_count;
+    r->hits += ctx->counters_host->hit_count;
+    if (live > M.capacity) return ctx->fail(YMRT_ERR_OVERFLOW, "path queue overflow");
+    a ^= 1;
+    cursor += gen;
+    r->paths += gen;
+    ++r->waves;
+  }
+  cudaEventRecord(ctx->ev_stop, st);
+  if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return ctx->cuda_fail(e, "frame");
+  float ms = 0.0f;
+  cudaEventElapsedTime(&ms, ctx->ev_start, ctx->ev_stop);
+  r->ms = ms;
+  return YMRT_OK;
+}
+
+// Fills ymrt_stats from the frame's counters and turns device error flags
+// into a status.
+int finish_batch(ymrt_context* ctx, const BatchResult& r, ymrt_stats* stats) {
+  const WaveCounters& c = *ctx->counters_host;
+  if (stats) {
+    std::memset(stats, 0, sizeof(*stats));
+    stats->paths = r.paths;
+    stats->extension_rays = c.extension_rays;
+    stats->shadow_rays = c.shadow_rays;
+    stats->waves = r.waves;
+    stats->shaded_hits = r.hits;
+    stats->node_visits = c.node_visits + c.shadow_node_visits;
+    stats->triangle_tests = c.tri_tests + c.shadow_tri_tests;
+    stats->shadow_node_visits = c.shadow_node_visits;
+    stats->shadow_triangle_tests = c.shadow_tri_tests;
+    stats->kernel_launches = r.launches;
+    stats->ms_total = r.ms;
+    stats->ms_generate = r.stage_ms[0];
+    stats->ms_extend = r.stage_ms[1];
+    stats->ms_sort = r.stage_ms[2];
+    stats->ms_shade = r.stage_ms[3];
+    stats->ms_connect = r.stage_ms[4];
+    stats->device_errors = c.errors;
+  }
+  if (c.errors & kDevErrQueue) return ctx->fail(YMRT_ERR_OVERFLOW, "path queue overflow on the device");
+  if (c.errors & kDevErrStack) return ctx->fail(YMRT_ERR_OVERFLOW, "traversal or nested-media stack overflow on the device");
+  return YMRT_OK;
+}
+
+// Wave options for a batch: media kernels when any job scatters in media;
+// shadow rays deferred unless a job clamps indirect light.
+int batch_options(ymrt_context* ctx, const std::vector<JobDesc>& jobs, WaveOptions* opt) {
+  opt->volumes = false;
+  bool clamp = false;
+  for (const JobDesc& j : jobs) {
+    opt->volumes = opt->volumes || j.setting.enable_volume_scattering;
+    clamp = clamp || j.setting.enable_indirect_clamp;
+  }
+  opt->sort_hits = ctx->sort_hits;
+  opt->defer_shadows = ctx->defer_shadows && !opt->volumes && !clamp;
+  if (opt->defer_shadows) {
+    int rc = ctx->ensure_shadow_queue();
+    if (rc != YMRT_OK) return rc;
+    opt->shadow_queue = ctx->shadow_queue;
+  }
+  return YMRT_OK;
+}
+
+// The context's queues as batch memory, with room for n_jobs jobs.
+int context_memory(ymrt_context* ctx, size_t n_jobs, BatchMemory* M) {
+  int rc = ctx->ensure_pools();
+  if (rc != YMRT_OK) return rc;
+  cudaError_t e = ctx->counters_buf.ensure(sizeof(WaveCounters));
+  if (e == cudaSuccess) e = ctx->jobs_buf.ensure(sizeof(JobDesc) * std::max<size_t>(n_jobs, 1));
+  if (e != cudaSuccess) return ctx->cuda_fail(e, "allocating the job table");
+  M->pool[0] = ctx->pool[0];
+  M->pool[1] = ctx->pool[1];
+  M->hits = ctx->hits;
+  M->counters = ctx->counters_buf.as<WaveCounters>();
+  M->jobs = ctx->jobs_buf.as<JobDesc>();
+  M->capacity = ctx->capacity;
+  return YMRT_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int ymrt_render_tiles(ymrt_scene* sc, const ymrt_render_setting* setting, int frame_index, int tile_begin, int tile_end,
+                      float* out_rgba, int out_on_device, ymrt_stats* stats) {
+  if (!sc || !setting || !out_rgba) return YMRT_ERR_INVALID;
+  ymrt_context* ctx = sc->ctx;
+  cudaSetDevice(ctx->device);
   cudaStream_t st = ctx->stream;
   cudaError_t e;
   float4* image = reinterpret_cast<float4*>(out_rgba);
-  const size_t img_bytes = (size_t)W * Hh * sizeof(float4);
+  const size_t img_bytes = (size_t)sc->width * sc->height * sizeof(float4);
   if (!out_on_device) {
     if ((e = ctx->image_buf.ensure(img_bytes)) != cudaSuccess) return ctx->cuda_fail(e, "allocating image");
     image = ctx->image_buf.as<float4>();
   }
-  if ((e = upload_constants(dev, ctx->primes.data(), ctx->prime_sums.data(), st)) != cudaSuccess)
+  std::vector<JobDesc> jobs(1);
+  int rc = make_job(ctx, sc, setting, frame_index, tile_begin, tile_end, image, &jobs[0]);
+  if (rc != YMRT_OK) return rc;
+  BatchMemory M;
+  if ((rc = context_memory(ctx, 1, &M)) != YMRT_OK) return rc;
+  WaveOptions opt;
+  if ((rc = batch_options(ctx, jobs, &opt)) != YMRT_OK) return rc;
+  if ((e = upload_constants(jobs[0].scene, ctx->primes.data(), ctx->prime_sums.data(), st)) != cudaSuccess)
     return ctx->cuda_fail(e, "uploading constants");
-  if ((e = upload_setting(rs, st)) != cudaSuccess) return ctx->cuda_fail(e, "uploading render setting");
-  WaveCounters* dc = ctx->counters_buf.as<WaveCounters>();
-  cudaMemsetAsync(dc, 0, sizeof(WaveCounters), st);
   cudaMemsetAsync(image, 0, img_bytes, st);
-  cudaEventRecord(ctx->ev_start, st);
-  uint32_t live = 0;
-  int a = 0;
-  uint64_t waves = 0, paths = 0, launches = 0, hits = 0;
-  double ms_stage[5] = {0.0, 0.0, 0.0, 0.0, 0.0};  // generate, extend, sort, shade, connect
-  while (live > 0 || cursor < t_end) {
-    const uint32_t n_tiles = std::min<uint32_t>((ctx->capacity - live) / per_tile, t_end - cursor);
-    const uint32_t gen = n_tiles * per_tile;
-    PathPool& A = ctx->pool[a];
-    PathPool& B = ctx->pool[a ^ 1];
-    launches += launch_wave(A, B, ctx->hits, live, gen, cursor, tiles_x, frame_index, spp, image, dc, opt,
-                            ctx->profiling ? ctx->ev_stage : nullptr, st);
-    if ((e = cudaMemcpyAsync(ctx->counters_host, dc, sizeof(WaveCounters), cudaMemcpyDeviceToHost, st)) != cudaSuccess)
-      return ctx->cuda_fail(e, "reading wave counters");
-    if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return ctx->cuda_fail(e, "wave");
-    if (ctx->profiling) {
-      for (int k = 0; k < 5; ++k) {
-        float ms = 0.0f;
-        cudaEventElapsedTime(&ms, ctx->ev_stage[k], ctx->ev_stage[k + 1]);
-        ms_stage[k] += ms;
-      }
-    }
-    live = ctx->counters_host->next_count;
-    hits += ctx->counters_host->hit_count;
-    if (live > ctx->capacity) return ctx->fail(YMRT_ERR_OVERFLOW, "path queue overflow");
-    a ^= 1;
-    cursor += n_tiles;
-    paths += gen;
-    ++waves;
-  }
-  cudaEventRecord(ctx->ev_stop, st);
+  BatchResult r;
+  if ((rc = run_batch(ctx, M, jobs, opt, ctx->profiling, &r)) != YMRT_OK) return rc;
   if (!out_on_device) {
     if ((e = cudaMemcpyAsync(out_rgba, image, img_bytes, cudaMemcpyDeviceToHost, st)) != cudaSuccess)
       return ctx->cuda_fail(e, "copying image");
   }
-  if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return ctx->cuda_fail(e, "frame");
-  if ((e = cudaMemcpy(ctx->counters_host, dc, sizeof(WaveCounters), cudaMemcpyDeviceToHost)) != cudaSuccess)
+  if ((e = cudaMemcpyAsync(ctx->counters_host, M.counters, sizeof(WaveCounters), cudaMemcpyDeviceToHost, st)) !=
+      cudaSuccess)
     return ctx->cuda_fail(e, "reading counters");
-  float ms = 0.0f;
-  cudaEventElapsedTime(&ms, ctx->ev_start, ctx->ev_stop);
-  if (stats) {
-    std::memset(stats, 0, sizeof(*stats));
-    stats->paths = paths;
-    stats->extension_rays = ctx->counters_host->extension_rays;
-    stats->shadow_rays = ctx->counters_host->shadow_rays;
-    stats->waves = waves;
-    stats->shaded_hits = hits;
-    stats->node_visits = ctx->counters_host->node_visits + ctx->counters_host->shadow_node_visits;
-    stats->triangle_tests = ctx->counters_host->tri_tests + ctx->counters_host->shadow_tri_tests;
-    stats->shadow_node_visits = ctx->counters_host->shadow_node_visits;
-    stats->shadow_triangle_tests = ctx->counters_host->shadow_tri_tests;
-    stats->kernel_launches = launches;
-    stats->ms_total = ms;
-    stats->ms_generate = ms_stage[0];
-    stats->ms_extend = ms_stage[1];
-    stats->ms_sort = ms_stage[2];
-    stats->ms_shade = ms_stage[3];
-    stats->ms_connect = ms_stage[4];
-    stats->device_errors = ctx->counters_host->errors;
+  if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return ctx->cuda_fail(e, "frame");
+  return finish_batch(ctx, r, stats);
+}
+
+int ymrt_render_batch(ymrt_context* ctx, const ymrt_job* jobs_in, int n_jobs, ymrt_stats* stats) {
+  if (!ctx || !jobs_in || n_jobs <= 0) return YMRT_ERR_INVALID;
+  if (n_jobs > (1 << 21)) return ctx->fail(YMRT_ERR_INVALID, "too many jobs in one batch (at most 2^21)");
+  cudaSetDevice(ctx->device);
+  cudaStream_t st = ctx->stream;
+  cudaError_t e;
+  std::vector<JobDesc> jobs((size_t)n_jobs);
+  for (int k = 0; k < n_jobs; ++k) {
+    const ymrt_job& in = jobs_in[k];
+    int rc = make_job(ctx, in.scene, &in.setting, in.frame_index, in.tile_begin, in.tile_end,
+                      reinterpret_cast<float4*>(in.out_rgba_device), &jobs[k]);
+    if (rc != YMRT_OK) return rc;
   }
-  if (ctx->counters_host->errors & kDevErrQueue) return ctx->fail(YMRT_ERR_OVERFLOW, "path queue overflow on the device");
-  if (ctx->counters_host->errors & kDevErrStack)
-    return ctx->fail(YMRT_ERR_OVERFLOW, "traversal or nested-media stack overflow on the device");
-  return YMRT_OK;
+  BatchMemory M;
+  int rc = context_memory(ctx, jobs.size(), &M);
+  if (rc != YMRT_OK) return rc;
+  WaveOptions opt;
+  if ((rc = batch_options(ctx, jobs, &opt)) != YMRT_OK) return rc;
+  if ((e = upload_constants(jobs[0].scene, ctx->primes.data(), ctx->prime_sums.data(), st)) != cudaSuccess)
+    return ctx->cuda_fail(e, "uploading constants");
+  for (int k = 0; k < n_jobs; ++k)
+    cudaMemsetAsync(jobs[k].image, 0, (size_t)jobs[k].scene.width * jobs[k].scene.height * sizeof(float4), st);
+  BatchResult r;
+  if ((rc = run_batch(ctx, M, jobs, opt, ctx->profiling, &r)) != YMRT_OK) return rc;
+  if ((e = cudaMemcpyAsync(ctx->counters_host, M.counters, sizeof(WaveCounters), cudaMemcpyDeviceToHost, st)) !=
+      cudaSuccess)
+    return ctx->cuda_fail(e, "reading counters");
+  if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return ctx->cuda_fail(e, "batch");
+  return finish_batch(ctx, r, stats);
 }
 
 int ymrt_render_forward(ymrt_scene* sc, const ymrt_render_setting* setting, int frame_index, float* out_rgba,
@@ -674,13 +799,15 @@ constexpr size_t kPoolSlotBytes = 4 * sizeof(float4) + sizeof(uint4) + 2 * sizeo
 constexpr size_t kHitSlotBytes = sizeof(float4) + sizeof(uint4) + kMaxNearby * sizeof(uint4) + sizeof(uint32_t) + 1;
 
 uint32_t noalloc_capacity() {
-  const size_t fixed = align256(sizeof(WaveCounters)) + 18 * 256;  // counters + alignment slack of the carved arrays
+  // counters, one job, and the alignment slack of the carved arrays
+  const size_t fixed = align256(sizeof(WaveCounters)) + align256(sizeof(JobDesc)) + 18 * 256;
   return (uint32_t)((kNoAllocScratchBytes - fixed) / (2 * kPoolSlotBytes + kHitSlotBytes));
 }
 
 // Carves the two path pools, the hit pool and the counters out of `base`;
 // returns the number of bytes used.
-size_t carve(unsigned char* base, uint32_t n, PathPool pools[2], HitPool* hits, WaveCounters** counters) {
+size_t carve(unsigned char* base, uint32_t n, PathPool pools[2], HitPool* hits, WaveCounters** counters,
+             JobDesc** job) {
   size_t off = 0;
   auto take = [&](size_t bytes) {
     unsigned char* p = base + off;
@@ -688,6 +815,7 @@ size_t carve(unsigned char* base, uint32_t n, PathPool pools[2], HitPool* hits, 
     return p;
   };
   *counters = reinterpret_cast<WaveCounters*>(take(sizeof(WaveCounters)));
+  *job = reinterpret_cast<JobDesc*>(take(sizeof(JobDesc)));
   for (int k = 0; k < 2; ++k) {
     PathPool& P = pools[k];
     P.ray_o = reinterpret_cast<float4*>(take(n * sizeof(float4)));
@@ -721,18 +849,13 @@ int ymrt_render_tiles_noalloc(ymrt_scene* sc, const ymrt_render_setting* setting
                               int tile_end, float* out_rgba_device, ymrt_stats* stats) {
   if (!sc || !setting || !out_rgba_device) return YMRT_ERR_INVALID;
   ymrt_context* ctx = sc->ctx;
-  RenderSetting rs;
-  std::memcpy(&rs, setting, sizeof(rs));
-  if (frame_index < 1) return ctx->fail(YMRT_ERR_INVALID, "frame_index starts at 1");
-  if (rs.sampler_type > 2u)
-    return ctx->fail(YMRT_ERR_UNSUPPORTED, "sampler_type must be 0 (PCG), 1 (Halton) or 2 (Sobol)");
-  if (rs.sampler_type == 2u && !sc->dev.sobol_matrices)
-    return ctx->fail(YMRT_ERR_INVALID, "the Sobol sampler needs its generator matrices (ymrt_scene_set_sobol_matrices)");
-  DeviceScene dev = sc->dev;
-  dev.sampler_type = rs.sampler_type;
-  if (rs.enable_distant_light) return ctx->fail(YMRT_ERR_UNSUPPORTED, "distant lights are not supported yet");
-  if (rs.enable_volume_scattering) return ctx->fail(YMRT_ERR_UNSUPPORTED, "volume scattering is not supported yet");
-  const uint32_t spp = (uint32_t)std::max(rs.ssp, 1);
+  if (setting->enable_distant_light) return ctx->fail(YMRT_ERR_UNSUPPORTED, "distant lights are not supported yet");
+  if (setting->enable_volume_scattering) return ctx->fail(YMRT_ERR_UNSUPPORTED, "volume scattering is not supported yet");
+  std::vector<JobDesc> jobs(1);
+  int rc = make_job(ctx, sc, setting, frame_index, tile_begin, tile_end, reinterpret_cast<float4*>(out_rgba_device),
+                    &jobs[0]);
+  if (rc != YMRT_OK) return rc;
+  const uint32_t spp = jobs[0].spp;
   const uint32_t per_tile = (uint32_t)kTilePixels * spp;
   const uint32_t cap = noalloc_capacity();
   if (per_tile > cap)
@@ -755,70 +878,21 @@ int ymrt_render_tiles_noalloc(ymrt_scene* sc, const ymrt_render_setting* setting
     }
     base = static_cast<unsigned char*>(g_noalloc_addr[ctx->device]);
   }
-  PathPool pools[2];
-  HitPool hits;
-  WaveCounters* dc = nullptr;
-  if (carve(base, cap, pools, &hits, &dc) > kNoAllocScratchBytes)
+  BatchMemory M;
+  if (carve(base, cap, M.pool, &M.hits, &M.counters, &M.jobs) > kNoAllocScratchBytes)
     return ctx->fail(YMRT_ERR_OVERFLOW, "scratch layout exceeds the fixed array");
-
-  const uint32_t W = sc->width, Hh = sc->height;
-  const uint32_t tiles_x = (W + kTileRes - 1) / kTileRes, tiles_y = (Hh + kTileRes - 1) / kTileRes;
-  const uint32_t total_tiles = tiles_x * tiles_y;
-  const uint32_t t_end = tile_end <= 0 ? total_tiles : std::min<uint32_t>((uint32_t)tile_end, total_tiles);
-  uint32_t cursor = (uint32_t)std::max(tile_begin, 0);
+  M.capacity = cap;
   cudaStream_t st = ctx->stream;
-  float4* image = reinterpret_cast<float4*>(out_rgba_device);
-  const size_t img_bytes = (size_t)W * Hh * sizeof(float4);
-  if ((e = upload_constants(dev, ctx->primes.data(), ctx->prime_sums.data(), st)) != cudaSuccess)
+  if ((e = upload_constants(jobs[0].scene, ctx->primes.data(), ctx->prime_sums.data(), st)) != cudaSuccess)
     return ctx->cuda_fail(e, "uploading constants");
-  if ((e = upload_setting(rs, st)) != cudaSuccess) return ctx->cuda_fail(e, "uploading render setting");
-  cudaMemsetAsync(dc, 0, sizeof(WaveCounters), st);
-  cudaMemsetAsync(image, 0, img_bytes, st);
-  cudaEventRecord(ctx->ev_start, st);
-  uint32_t live = 0;
-  int a = 0;
-  uint64_t waves = 0, paths = 0, launches = 0, shaded = 0;
-  while (live > 0 || cursor < t_end) {
-    const uint32_t n_tiles = std::min<uint32_t>((cap - live) / per_tile, t_end - cursor);
-    const uint32_t gen = n_tiles * per_tile;
-    launches += launch_wave(pools[a], pools[a ^ 1], hits, live, gen, cursor, tiles_x, frame_index, spp, image, dc,
-                            WaveOptions{}, nullptr, st);
-    if ((e = cudaMemcpyAsync(ctx->counters_host, dc, sizeof(WaveCounters), cudaMemcpyDeviceToHost, st)) != cudaSuccess)
-      return ctx->cuda_fail(e, "reading wave counters");
-    if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return ctx->cuda_fail(e, "wave");
-    live = ctx->counters_host->next_count;
-    shaded += ctx->counters_host->hit_count;
-    if (live > cap) return ctx->fail(YMRT_ERR_OVERFLOW, "path queue overflow");
-    a ^= 1;
-    cursor += n_tiles;
-    paths += gen;
-    ++waves;
-  }
-  cudaEventRecord(ctx->ev_stop, st);
-  if ((e = cudaMemcpyAsync(ctx->counters_host, dc, sizeof(WaveCounters), cudaMemcpyDeviceToHost, st)) != cudaSuccess)
+  cudaMemsetAsync(out_rgba_device, 0, (size_t)sc->width * sc->height * sizeof(float4), st);
+  BatchResult r;
+  if ((rc = run_batch(ctx, M, jobs, WaveOptions{}, false, &r)) != YMRT_OK) return rc;
+  if ((e = cudaMemcpyAsync(ctx->counters_host, M.counters, sizeof(WaveCounters), cudaMemcpyDeviceToHost, st)) !=
+      cudaSuccess)
     return ctx->cuda_fail(e, "reading counters");
   if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return ctx->cuda_fail(e, "frame");
-  float ms = 0.0f;
-  cudaEventElapsedTime(&ms, ctx->ev_start, ctx->ev_stop);
-  if (stats) {
-    std::memset(stats, 0, sizeof(*stats));
-    stats->paths = paths;
-    stats->extension_rays = ctx->counters_host->extension_rays;
-    stats->shadow_rays = ctx->counters_host->shadow_rays;
-    stats->waves = waves;
-    stats->shaded_hits = shaded;
-    stats->node_visits = ctx->counters_host->node_visits + ctx->counters_host->shadow_node_visits;
-    stats->triangle_tests = ctx->counters_host->tri_tests + ctx->counters_host->shadow_tri_tests;
-    stats->shadow_node_visits = ctx->counters_host->shadow_node_visits;
-    stats->shadow_triangle_tests = ctx->counters_host->shadow_tri_tests;
-    stats->kernel_launches = launches;
-    stats->ms_total = ms;
-    stats->device_errors = ctx->counters_host->errors;
-  }
-  if (ctx->counters_host->errors & kDevErrQueue) return ctx->fail(YMRT_ERR_OVERFLOW, "path queue overflow on the device");
-  if (ctx->counters_host->errors & kDevErrStack)
-    return ctx->fail(YMRT_ERR_OVERFLOW, "traversal or nested-media stack overflow on the device");
-  return YMRT_OK;
+  return finish_batch(ctx, r, stats);
 }
 
 int ymrt_accumulate(ymrt_scene* sc, const float* noise, float* acc, int frame_index) {

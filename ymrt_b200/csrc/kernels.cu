@@ -31,7 +31,6 @@ namespace cg = cooperative_groups;
 
 
 __constant__ DeviceScene c_scene;
-__constant__ RenderSetting c_setting;
 
 // ---------------------------------------------------------------- paths ---
 
@@ -66,24 +65,43 @@ __device__ __forceinline__ uint32_t warp_append(uint32_t* counter, bool want) {
   return base + (uint32_t)__popc(mask & ((1u << lane) - 1u));
 }
 
-__device__ __forceinline__ uint32_t flags_pack(int depth, bool never_scatter, bool camera_ray, int pixel_sample) {
+__device__ __forceinline__ uint32_t flags_pack(int depth, bool never_scatter, bool camera_ray, uint32_t job) {
   return (uint32_t)depth | (never_scatter ? kFlagNeverScatter : 0u) | (camera_ray ? kFlagCameraRay : 0u) |
-         ((uint32_t)pixel_sample << kFlagSampleShift);
+         (job << kFlagJobShift);
 }
 
 // ------------------------------------------------------------ generate ---
 
-__global__ void __launch_bounds__(256) k_generate(PathPool P, uint32_t base, uint32_t count, uint32_t next_tile,
-                                                  uint32_t tiles_x, int frame_index, uint32_t spp) {
+// The job holding path g of the batch's path space (binary search; jobs are
+// in path order).
+__device__ __forceinline__ uint32_t find_job(const JobDesc* __restrict__ jobs, uint32_t n_jobs, unsigned long long g) {
+  uint32_t lo = 0, hi = n_jobs;
+  while (hi - lo > 1) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (jobs[mid].path_begin <= g) lo = mid;
+    else hi = mid;
+  }
+  return lo;
+}
+
+__global__ void __launch_bounds__(256) k_generate(PathPool P, uint32_t base, uint32_t count,
+                                                  unsigned long long path_cursor, const JobDesc* __restrict__ jobs,
+                                                  uint32_t n_jobs) {
   const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
   if (tid >= count) return;
-  const DeviceScene& S = c_scene;
   const uint32_t i = base + tid;
+  const unsigned long long g = path_cursor + tid;
+  const uint32_t job = find_job(jobs, n_jobs, g);
+  const JobDesc& J = jobs[job];
+  const DeviceScene& S = J.scene;
+  const uint32_t spp = J.spp;
+  const int frame_index = J.frame_index;
+  const uint32_t local_path = (uint32_t)(g - J.path_begin);
   const uint32_t per_tile = (uint32_t)kTilePixels * spp;
-  const uint32_t tile_in_batch = tid / per_tile;
-  const uint32_t tile_y = (tile_in_batch + next_tile) / tiles_x;
-  const uint32_t tile_x = (tile_in_batch + next_tile) - tiles_x * tile_y;
-  const uint32_t local = tid - tile_in_batch * per_tile;
+  const uint32_t tile = local_path / per_tile + J.tile_begin;
+  const uint32_t tile_y = tile / J.tiles_x;
+  const uint32_t tile_x = tile - J.tiles_x * tile_y;
+  const uint32_t local = local_path - (tile - J.tile_begin) * per_tile;
   const uint32_t tile_pixel = local / spp;
   const uint32_t pixel_sample = local - tile_pixel * spp;
   const uint32_t tpy = tile_pixel / kTileRes;
@@ -100,7 +118,7 @@ __global__ void __launch_bounds__(256) k_generate(PathPool P, uint32_t base, uin
   float ox = 0.5f, oy = 0.5f;
   if (S.sampler_type == kSamplerHalton) {
     const uint64_t sample_index =
-        halton_index(S, (int)px, (int)py, (frame_index - 1) * c_setting.ssp + (int)pixel_sample);
+        halton_index(S, (int)px, (int)py, (frame_index - 1) * J.setting.ssp + (int)pixel_sample);
     hs = PathSampler{sample_index, 2u, 0u};
     ox = radical_inverse_2(sample_index);
     oy = radical_inverse_3(sample_index);
@@ -112,7 +130,7 @@ __global__ void __launch_bounds__(256) k_generate(PathPool P, uint32_t base, uin
     hs = PathSampler{(uint64_t)pixel | ((uint64_t)pixel_sample << 32), 0u, (uint32_t)(frame_index - 1)};
     sample2d(hs, S, &ox, &oy);
   } else {
-    const uint32_t sample = (uint32_t)(frame_index - 1) * (uint32_t)c_setting.ssp + pixel_sample;
+    const uint32_t sample = (uint32_t)(frame_index - 1) * (uint32_t)J.setting.ssp + pixel_sample;
     hs = PathSampler{(uint64_t)sample | ((uint64_t)pixel << 32), 1u, 0u};
     sample2d(hs, S, &ox, &oy);
   }
@@ -123,8 +141,8 @@ __global__ void __launch_bounds__(256) k_generate(PathPool P, uint32_t base, uin
   const float h = 2.0f * cam.tan_half_fov;
   const float w = h * cam.aspect_ratio;
   const vec3 dir = normalize(-cam.w + (ndc_x - 0.5f) * w * cam.u + (ndc_y - 0.5f) * h * cam.v);
-  store_path(P, i, cam.position, dir, vec3(1.0f), vec3(0.0f), pixel, flags_pack(1, true, true, (int)pixel_sample), kEmpty,
-             kEmpty, hs);
+  store_path(P, i, cam.position, dir, vec3(1.0f), vec3(0.0f), pixel, flags_pack(1, true, true, job), kEmpty, kEmpty,
+             hs);
   if (cam.transfer.record_count > 0) P.transfer[i] = cam.transfer;
   P.transfer_count[i] = (uint8_t)cam.transfer.record_count;
 }
@@ -170,8 +188,8 @@ __global__ void __launch_bounds__(256) k_sort_hits(uint32_t count, HitPool H, Wa
 }
 
 template <bool kVol>
-__global__ void __launch_bounds__(kTraceBlock, 5) k_extend(PathPool P, uint32_t count, HitPool H, float4* image,
-                                                        WaveCounters* counters) {
+__global__ void __launch_bounds__(kTraceBlock, 5) k_extend(PathPool P, uint32_t count, HitPool H,
+                                                           const JobDesc* __restrict__ jobs, WaveCounters* counters) {
   YM_TRAVERSAL_SHARED(s_stack);
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   uint32_t tests = 0, nodes = 0;
@@ -181,7 +199,8 @@ __global__ void __launch_bounds__(kTraceBlock, 5) k_extend(PathPool P, uint32_t 
   bool overflow = false;
   uint32_t bucket = kBucketNone;
   if (active) {
-    const DeviceScene& S = c_scene;
+    const JobDesc& J = jobs[pf.y >> kFlagJobShift];
+    const DeviceScene& S = J.scene;
     const float4 o4 = P.ray_o[i], d4 = P.ray_d[i];
     const vec3 o(o4.x, o4.y, o4.z), d(d4.x, d4.y, d4.z);
     const uint2 lh = P.last_hit[i];
@@ -194,7 +213,7 @@ __global__ void __launch_bounds__(kTraceBlock, 5) k_extend(PathPool P, uint32_t 
     float4 t4 = P.throughput[i];
     vec3 tp(t4.x, t4.y, t4.z);
     vec3 vol_pos(0.0f);
-    if (kVol) {
+    if (kVol && J.setting.enable_volume_scattering) {
       // volume free flight before the surface (src/Shading.cu:1828-1853)
       RayTransfer rt;
       rt.record_count = P.transfer_count[i];
@@ -230,10 +249,10 @@ __global__ void __launch_bounds__(kTraceBlock, 5) k_extend(PathPool P, uint32_t 
       // Ray_trace_path_tracing miss branch (src/Shading.cu:1855-1864).
       const float4 r4 = P.radiance[i];
       vec3 rad(r4.x, r4.y, r4.z);
-      if (c_setting.enable_env_light)
-        rad += indirect_clamp(c_setting, tp * background(d), (int)(pf.y & kFlagDepthMask));
-      const float inv_spp = 1.0f / gmax(c_setting.ssp, 1);
-      accumulate_pixel(image, pf.x, rad, inv_spp);
+      if (J.setting.enable_env_light)
+        rad += indirect_clamp(J.setting, tp * background(d), (int)(pf.y & kFlagDepthMask));
+      const float inv_spp = 1.0f / gmax(J.setting.ssp, 1);
+      accumulate_pixel(J.image, pf.x, rad, inv_spp);
       P.pixel_flags[i] = make_uint2(pf.x, pf.y | kFlagDead);
     } else {
       if (volume_hit) H.bary_t[i] = make_float4(vol_pos.x, vol_pos.y, vol_pos.z, ch.t);
@@ -430,6 +449,7 @@ struct SurfaceNee {
   const RayTransfer* rt;
   const NearbyHit* nb;
   int n_nb;
+  bool media;  // the render's enable_volume_scattering
 };
 
 // Transmittance of an unoccluded surface shadow ray (the volume part of the
@@ -438,7 +458,7 @@ template <bool kVol>
 __device__ __forceinline__ vec3 surface_shadow_tr(const DeviceScene& S, TraversalStack& st, const SurfaceNee& c, vec3 so,
                                                   vec3 ldir, float maxd, bool tb, PathSampler& hs, uint32_t* errors,
                                                   uint32_t* tests, uint32_t* nodes) {
-  if (!kVol) return vec3(1.0f);
+  if (!kVol || !c.media) return vec3(1.0f);
   RayTransfer srt = *c.rt;
   if (tb) boundary_transition(S, srt, c.nb, c.n_nb, errors);
   return trace_tr(S, st, so, normalize(ldir), maxd, c.inst, c.tri, srt, hs, errors, tests, nodes);
@@ -452,6 +472,7 @@ struct ShadowEmit {
   uint32_t* count;
   uint32_t* errors;
   uint32_t pixel;
+  uint32_t job;
   vec3 weight;
 };
 
@@ -469,7 +490,7 @@ __device__ __forceinline__ void emit_shadow_ray(const ShadowEmit& em, vec3 o, ve
   const vec3 w = em.weight * contribution;
   em.q.o[slot] = make_float4(o.x, o.y, o.z, maxd);
   em.q.d[slot] = make_float4(d.x, d.y, d.z, __uint_as_float(em.pixel));
-  em.q.c[slot] = make_float4(w.x, w.y, w.z, 0.0f);
+  em.q.c[slot] = make_float4(w.x, w.y, w.z, __uint_as_float(em.job));
 }
 
 // One next-event shadow ray of a surface vertex toward a light, with MIS
@@ -709,8 +730,9 @@ __device__ __noinline__ vec3 eval_volume_lights(const DeviceScene& S, TraversalS
 // for k_connect instead of traced here, which keeps traversal out of this
 // kernel.
 template <bool kVol, bool kDefer>
-__global__ void __launch_bounds__(kTraceBlock) k_shade(PathPool P, uint32_t count, HitPool H, PathPool Q, float4* image,
-                                                       WaveCounters* counters, ShadowQueue shadow_q) {
+__global__ void __launch_bounds__(kTraceBlock) k_shade(PathPool P, uint32_t count, HitPool H, PathPool Q,
+                                                       const JobDesc* __restrict__ jobs, WaveCounters* counters,
+                                                       ShadowQueue shadow_q) {
   static_assert(!(kVol && kDefer), "volume transmittance needs the path's sampler: shadow rays are traced inline");
   // The path slot this thread shades: the t-th listed hit, or (hits not
   // listed by bucket) slot t itself when it holds a hit.
@@ -731,8 +753,11 @@ __global__ void __launch_bounds__(kTraceBlock) k_shade(PathPool P, uint32_t coun
   rt.max_priority_record_index = -1;
 
   if (active) {
-    const DeviceScene& S = c_scene;
-    const RenderSetting& rs = c_setting;
+    const uint32_t job = pf.y >> kFlagJobShift;
+    const JobDesc& J = jobs[job];
+    const DeviceScene& S = J.scene;
+    const RenderSetting& rs = J.setting;
+    float4* image = J.image;
     uint32_t* errors = &counters->errors;
     const float4 o4 = P.ray_o[i], d4 = P.ray_d[i], t4 = P.throughput[i], r4 = P.radiance[i];
     const vec3 rd(d4.x, d4.y, d4.z);
@@ -745,7 +770,7 @@ __global__ void __launch_bounds__(kTraceBlock) k_shade(PathPool P, uint32_t coun
     hs.aux = s4.w;
     int depth = (int)(pf.y & kFlagDepthMask);
     bool never_scatter = (pf.y & kFlagNeverScatter) != 0;
-    const uint32_t sample_bits = pf.y & ~(kFlagDepthMask | kFlagNeverScatter | kFlagCameraRay | kFlagDead);
+    const uint32_t sample_bits = pf.y & ~(kFlagDepthMask | kFlagNeverScatter | kFlagCameraRay | kFlagDead);  // job
     const int n_rec = P.transfer_count[i];
     if (n_rec > 0) rt = P.transfer[i];
     const float4 bt = H.bary_t[i];
@@ -859,8 +884,8 @@ __global__ void __launch_bounds__(kTraceBlock) k_shade(PathPool P, uint32_t coun
         LayeredBsdf B;
         init_shading_frame(B, hit_back, rd, sp.ng, sp.ns, sp.dpdu, sp.dpdv);
         init_layered_lobes(B, mat.default_mtl, rd, hit_back, ray_ior(rt), ex_ior(rt, inst_idx));
-        const SurfaceNee nc{rd, sp.p, sp.p_err, sp.ng, inst_idx, tri, &rt, nb, n_nb};
-        const ShadowEmit em{shadow_q, &counters->shadow_count, errors, pf.x, tp * inv_spp};
+        const SurfaceNee nc{rd, sp.p, sp.p_err, sp.ng, inst_idx, tri, &rt, nb, n_nb, rs.enable_volume_scattering != 0};
+        const ShadowEmit em{shadow_q, &counters->shadow_count, errors, pf.x, job, tp * inv_spp};
         if (rs.enable_distant_light)
           rad += indirect_clamp(
               rs, tp * eval_distant_light<kVol, kDefer>(S, st, B, nc, em, hs, &shadow_rays, &tests, &nodes, errors),
@@ -941,17 +966,18 @@ __global__ void __launch_bounds__(kTraceBlock) k_shade(PathPool P, uint32_t coun
 // Traces the wave's queued shadow rays (grid-stride over the queue, so the
 // grid is sized to the GPU, not to the queue) and adds each unoccluded ray's
 // contribution to its pixel.
-__global__ void __launch_bounds__(kTraceBlock, 5) k_connect(ShadowQueue Q, float4* image, WaveCounters* counters) {
+__global__ void __launch_bounds__(kTraceBlock, 5) k_connect(ShadowQueue Q, const JobDesc* __restrict__ jobs,
+                                                            WaveCounters* counters) {
   YM_TRAVERSAL_SHARED(s_stack);
   TraversalStack st;
   st.bind(s_stack_entries, s_stack_t);
   const uint32_t n = min(counters->shadow_count, Q.capacity);
   uint32_t tests = 0, nodes = 0;
   for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
-    const float4 o = Q.o[t], d = Q.d[t];
-    if (!trace_occluded(c_scene, st, vec3(o.x, o.y, o.z), vec3(d.x, d.y, d.z), o.w, &tests, &nodes)) {
-      const float4 c = Q.c[t];
-      float* p = reinterpret_cast<float*>(image + __float_as_uint(d.w));
+    const float4 o = Q.o[t], d = Q.d[t], c = Q.c[t];
+    const JobDesc& J = jobs[__float_as_uint(c.w)];
+    if (!trace_occluded(J.scene, st, vec3(o.x, o.y, o.z), vec3(d.x, d.y, d.z), o.w, &tests, &nodes)) {
+      float* p = reinterpret_cast<float*>(J.image + __float_as_uint(d.w));
       atomicAdd(p + 0, c.x);
       atomicAdd(p + 1, c.y);
       atomicAdd(p + 2, c.z);
@@ -1052,22 +1078,18 @@ cudaError_t upload_constants(const DeviceScene& scene, const uint32_t* primes, c
                                  stream);
 }
 
-cudaError_t upload_setting(const RenderSetting& rs, cudaStream_t stream) {
-  return cudaMemcpyToSymbolAsync(c_setting, &rs, sizeof(RenderSetting), 0, cudaMemcpyHostToDevice, stream);
-}
-
-void launch_generate(const PathPool& P, uint32_t base, uint32_t count, uint32_t next_tile, uint32_t tiles_x,
-                     int frame_index, uint32_t spp, cudaStream_t stream) {
+void launch_generate(const PathPool& P, uint32_t base, uint32_t count, unsigned long long path_cursor,
+                     const JobDesc* jobs, uint32_t n_jobs, cudaStream_t stream) {
   if (count == 0) return;
-  k_generate<<<(count + 255) / 256, 256, 0, stream>>>(P, base, count, next_tile, tiles_x, frame_index, spp);
+  k_generate<<<(count + 255) / 256, 256, 0, stream>>>(P, base, count, path_cursor, jobs, n_jobs);
 }
 
-void launch_extend(const PathPool& P, uint32_t count, const HitPool& H, float4* image, WaveCounters* counters,
+void launch_extend(const PathPool& P, uint32_t count, const HitPool& H, const JobDesc* jobs, WaveCounters* counters,
                    bool volumes, cudaStream_t stream) {
   if (count == 0) return;
   const uint32_t blocks = (count + kTraceBlock - 1) / kTraceBlock;
-  if (volumes) k_extend<true><<<blocks, kTraceBlock, 0, stream>>>(P, count, H, image, counters);
-  else k_extend<false><<<blocks, kTraceBlock, 0, stream>>>(P, count, H, image, counters);
+  if (volumes) k_extend<true><<<blocks, kTraceBlock, 0, stream>>>(P, count, H, jobs, counters);
+  else k_extend<false><<<blocks, kTraceBlock, 0, stream>>>(P, count, H, jobs, counters);
 }
 
 void launch_sort_hits(uint32_t count, const HitPool& H, WaveCounters* counters, cudaStream_t stream) {
@@ -1076,43 +1098,43 @@ void launch_sort_hits(uint32_t count, const HitPool& H, WaveCounters* counters, 
 }
 
 uint32_t launch_wave(const PathPool& A, const PathPool& B, const HitPool& H, uint32_t live, uint32_t gen,
-                     uint32_t next_tile, uint32_t tiles_x, int frame_index, uint32_t spp, float4* image,
-                     WaveCounters* counters, const WaveOptions& opt, cudaEvent_t* ev, cudaStream_t stream) {
+                     unsigned long long path_cursor, const JobDesc* jobs, uint32_t n_jobs, WaveCounters* counters,
+                     const WaveOptions& opt, cudaEvent_t* ev, cudaStream_t stream) {
   const uint32_t total = live + gen;
   const ShadowQueue* defer = (!opt.volumes && opt.defer_shadows) ? &opt.shadow_queue : nullptr;
   HitPool Hs = H;
   if (!opt.sort_hits) Hs.order = nullptr;
   cudaMemsetAsync(counters, 0, kWaveClearBytes, stream);
   if (ev) cudaEventRecord(ev[0], stream);
-  launch_generate(A, live, gen, next_tile, tiles_x, frame_index, spp, stream);
+  launch_generate(A, live, gen, path_cursor, jobs, n_jobs, stream);
   if (ev) cudaEventRecord(ev[1], stream);
-  launch_extend(A, total, Hs, image, counters, opt.volumes, stream);
+  launch_extend(A, total, Hs, jobs, counters, opt.volumes, stream);
   if (ev) cudaEventRecord(ev[2], stream);
   if (opt.sort_hits) launch_sort_hits(total, Hs, counters, stream);
   if (ev) cudaEventRecord(ev[3], stream);
-  launch_shade(A, total, Hs, B, image, counters, opt.volumes, defer, stream);
+  launch_shade(A, total, Hs, B, jobs, counters, opt.volumes, defer, stream);
   if (ev) cudaEventRecord(ev[4], stream);
-  if (defer && total > 0) launch_connect(*defer, image, counters, stream);
+  if (defer && total > 0) launch_connect(*defer, jobs, counters, stream);
   if (ev) cudaEventRecord(ev[5], stream);
   if (total == 0) return gen > 0 ? 1u : 0u;
   return (gen > 0 ? 1u : 0u) + 2u + (opt.sort_hits ? 1u : 0u) + (defer ? 1u : 0u);
 }
 
-void launch_shade(const PathPool& P, uint32_t count, const HitPool& H, const PathPool& Q, float4* image,
+void launch_shade(const PathPool& P, uint32_t count, const HitPool& H, const PathPool& Q, const JobDesc* jobs,
                   WaveCounters* counters, bool volumes, const ShadowQueue* defer, cudaStream_t stream) {
   if (count == 0) return;
   const uint32_t blocks = (count + kTraceBlock - 1) / kTraceBlock;
   const ShadowQueue none{};
-  if (volumes) k_shade<true, false><<<blocks, kTraceBlock, 0, stream>>>(P, count, H, Q, image, counters, none);
-  else if (defer) k_shade<false, true><<<blocks, kTraceBlock, 0, stream>>>(P, count, H, Q, image, counters, *defer);
-  else k_shade<false, false><<<blocks, kTraceBlock, 0, stream>>>(P, count, H, Q, image, counters, none);
+  if (volumes) k_shade<true, false><<<blocks, kTraceBlock, 0, stream>>>(P, count, H, Q, jobs, counters, none);
+  else if (defer) k_shade<false, true><<<blocks, kTraceBlock, 0, stream>>>(P, count, H, Q, jobs, counters, *defer);
+  else k_shade<false, false><<<blocks, kTraceBlock, 0, stream>>>(P, count, H, Q, jobs, counters, none);
 }
 
-void launch_connect(const ShadowQueue& Q, float4* image, WaveCounters* counters, cudaStream_t stream) {
+void launch_connect(const ShadowQueue& Q, const JobDesc* jobs, WaveCounters* counters, cudaStream_t stream) {
   int sms = 148;
   int dev = 0;
   if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  k_connect<<<sms * 5, kTraceBlock, 0, stream>>>(Q, image, counters);
+  k_connect<<<sms * 5, kTraceBlock, 0, stream>>>(Q, jobs, counters);
 }
 
 void launch_accumulate(const float4* noise, float4* acc, uint32_t n, int frame_index, cudaStream_t stream) {

@@ -14,7 +14,7 @@ constexpr uint32_t kFlagDepthMask = 0xFFu;        // path depth (1 = camera ray)
 constexpr uint32_t kFlagNeverScatter = 1u << 8;
 constexpr uint32_t kFlagCameraRay = 1u << 9;
 constexpr uint32_t kFlagDead = 1u << 10;          // slot holds no live path
-constexpr uint32_t kFlagSampleShift = 11;         // sample index within the pixel (for non-Halton samplers)
+constexpr uint32_t kFlagJobShift = 11;            // render (job) of the batch the path belongs to (21 bits)
 
 constexpr uint32_t kNearbyExplicit = 1u << 31;    // hit ids.w: nearby list stored in HitPool::nearby
 
@@ -56,11 +56,26 @@ struct HitPool {
   uint32_t* order;  // slots to shade, bucket by bucket
 };
 
+// One render of a batch (a single render is a batch of one): its scene,
+// settings, output image and its range in the batch's path space (paths are
+// numbered tile by tile, 256 * spp per 16x16 tile, job after job).
+struct JobDesc {
+  DeviceScene scene;
+  RenderSetting setting;
+  float4* image;                  // width * height float4, accumulated with atomics
+  int frame_index;
+  uint32_t spp;
+  uint32_t tiles_x;
+  uint32_t tile_begin;            // first tile rendered
+  unsigned long long path_begin;  // first path of this job in the batch's path space
+  unsigned long long path_count;  // tiles rendered * 256 * spp
+};
+
 // Deferred next-event shadow rays of one wave (traced by k_connect).
 struct ShadowQueue {
   float4* o;   // origin xyz, maximum distance
   float4* d;   // normalised direction xyz, pixel index (bits)
-  float4* c;   // contribution rgb, already weighted by throughput / spp
+  float4* c;   // contribution rgb, already weighted by throughput / spp; job index (bits)
   uint32_t capacity;
 };
 
@@ -86,17 +101,16 @@ constexpr size_t kWaveClearBytes = offsetof(WaveCounters, errors);
 
 cudaError_t upload_constants(const DeviceScene& scene, const uint32_t* primes, const uint32_t* prime_sums,
                              cudaStream_t stream);
-cudaError_t upload_setting(const RenderSetting& rs, cudaStream_t stream);
-void launch_generate(const PathPool& P, uint32_t base, uint32_t count, uint32_t next_tile, uint32_t tiles_x,
-                     int frame_index, uint32_t spp, cudaStream_t stream);
-void launch_extend(const PathPool& P, uint32_t count, const HitPool& H, float4* image, WaveCounters* counters,
+void launch_generate(const PathPool& P, uint32_t base, uint32_t count, unsigned long long path_cursor,
+                     const JobDesc* jobs, uint32_t n_jobs, cudaStream_t stream);
+void launch_extend(const PathPool& P, uint32_t count, const HitPool& H, const JobDesc* jobs, WaveCounters* counters,
                    bool volumes, cudaStream_t stream);
 void launch_sort_hits(uint32_t count, const HitPool& H, WaveCounters* counters, cudaStream_t stream);
-void launch_shade(const PathPool& P, uint32_t count, const HitPool& H, const PathPool& Q, float4* image,
+void launch_shade(const PathPool& P, uint32_t count, const HitPool& H, const PathPool& Q, const JobDesc* jobs,
                   WaveCounters* counters, bool volumes, const ShadowQueue* defer, cudaStream_t stream);
-void launch_connect(const ShadowQueue& Q, float4* image, WaveCounters* counters, cudaStream_t stream);
-// One wave: generates `gen` camera paths after the `live` continuing ones in
-// A, traces them, lists the hits by shading bucket and shades them, writing
+void launch_connect(const ShadowQueue& Q, const JobDesc* jobs, WaveCounters* counters, cudaStream_t stream);
+// One wave: generates `gen` camera paths (the batch's paths from
+// path_cursor on) after the `live` continuing ones in A, traces them, lists the hits by shading bucket and shades them, writing
 // continuing paths to B. With opt.defer_shadows (surfaces only; the caller
 // turns it off for the indirect clamp, which needs a vertex's whole direct
 // light at once) the shading kernel queues its shadow rays and k_connect
@@ -110,8 +124,8 @@ struct WaveOptions {
   ShadowQueue shadow_queue{};
 };
 uint32_t launch_wave(const PathPool& A, const PathPool& B, const HitPool& H, uint32_t live, uint32_t gen,
-                     uint32_t next_tile, uint32_t tiles_x, int frame_index, uint32_t spp, float4* image,
-                     WaveCounters* counters, const WaveOptions& opt, cudaEvent_t* ev, cudaStream_t stream);
+                     unsigned long long path_cursor, const JobDesc* jobs, uint32_t n_jobs, WaveCounters* counters,
+                     const WaveOptions& opt, cudaEvent_t* ev, cudaStream_t stream);
 void launch_accumulate(const float4* noise, float4* acc, uint32_t n, int frame_index, cudaStream_t stream);
 void launch_debug_trace(int n, const float* o, const float* d, const uint32_t* lh, uint32_t* inst, uint32_t* tri,
                         float* t, float* bary, int* back, int* nearby, uint32_t* errors, cudaStream_t stream);
