@@ -81,6 +81,7 @@ struct ymrt_context {
   bool profiling = false;
   cudaEvent_t ev_stage[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
   std::vector<uint32_t> primes, prime_sums;
+  WaveCounters batch_counters{};  // frame totals across the launch groups of one batch
   // wave options (ymrt_set_option)
   bool sort_hits = true;
   bool defer_shadows = true;
@@ -539,7 +540,7 @@ struct BatchResult {
 
 // Checks one render's arguments and fills its job (path range left at 0).
 int make_job(ymrt_context* ctx, ymrt_scene* sc, const ymrt_render_setting* setting, int frame_index, int tile_begin,
-             int tile_end, float4* image, JobDesc* job) {
+             int tile_end, float4* image, JobDesc* job, DeviceScene* scene) {
   static_assert(sizeof(ymrt_render_setting) == sizeof(RenderSetting), "render setting layout");
   if (!sc || !setting || !image) return ctx->fail(YMRT_ERR_INVALID, "null scene, setting or output");
   if (sc->ctx != ctx) return ctx->fail(YMRT_ERR_INVALID, "scene belongs to another context");
@@ -556,8 +557,10 @@ int make_job(ymrt_context* ctx, ymrt_scene* sc, const ymrt_render_setting* setti
   const uint32_t t_end = tile_end <= 0 ? total_tiles : std::min<uint32_t>((uint32_t)tile_end, total_tiles);
   const uint32_t t_begin = std::min<uint32_t>((uint32_t)tile_begin, t_end);
   std::memset(job, 0, sizeof(*job));
-  job->scene = sc->dev;
-  job->scene.sampler_type = rs.sampler_type;
+  *scene = sc->dev;
+  scene->sampler_type = rs.sampler_type;
+  job->width = (uint32_t)sc->width;
+  job->height = (uint32_t)sc->height;
   if (rs.enable_volume_scattering && sc->dev.volume_count == 0) rs.enable_volume_scattering = false;
   job->setting = rs;
   job->image = image;
@@ -567,6 +570,26 @@ int make_job(ymrt_context* ctx, ymrt_scene* sc, const ymrt_render_setting* setti
   job->tile_begin = t_begin;
   job->path_count = (unsigned long long)(t_end - t_begin) * kTilePixels * job->spp;
   return YMRT_OK;
+}
+
+// Gives every job the constant-memory slot of its (scene, sampler) pair;
+// returns the slots' scenes.
+std::vector<DeviceScene> assign_slots(std::vector<JobDesc>& jobs, const std::vector<DeviceScene>& job_scenes,
+                                      const std::vector<const void*>& keys) {
+  std::vector<DeviceScene> slots;
+  std::vector<std::pair<const void*, uint32_t>> seen;
+  for (size_t k = 0; k < jobs.size(); ++k) {
+    const auto key = std::make_pair(keys[k], job_scenes[k].sampler_type);
+    uint32_t slot = (uint32_t)seen.size();
+    for (uint32_t q = 0; q < seen.size(); ++q)
+      if (seen[q] == key) slot = q;
+    if (slot == seen.size()) {
+      seen.push_back(key);
+      slots.push_back(job_scenes[k]);
+    }
+    jobs[k].scene_slot = slot;
+  }
+  return slots;
 }
 
 // Renders a batch of jobs (paths numbered job after job) with the
@@ -618,6 +641,20 @@ int run_batch(ymrt_context* ctx, const BatchMemory& M, std::vector<JobDesc>& job
   cudaEventElapsedTime(&ms, ctx->ev_start, ctx->ev_stop);
   r->ms = ms;
   return YMRT_OK;
+}
+
+// Adds the last group's frame counters (in counters_host) to batch_counters.
+void total_counters_add(ymrt_context* ctx, bool first) {
+  WaveCounters& t = ctx->batch_counters;
+  const WaveCounters& c = *ctx->counters_host;
+  if (first) t = WaveCounters{};
+  t.errors |= c.errors;
+  t.extension_rays += c.extension_rays;
+  t.shadow_rays += c.shadow_rays;
+  t.tri_tests += c.tri_tests;
+  t.node_visits += c.node_visits;
+  t.shadow_tri_tests += c.shadow_tri_tests;
+  t.shadow_node_visits += c.shadow_node_visits;
 }
 
 // Fills ymrt_stats from the frame's counters and turns device error flags
@@ -702,13 +739,15 @@ int ymrt_render_tiles(ymrt_scene* sc, const ymrt_render_setting* setting, int fr
     image = ctx->image_buf.as<float4>();
   }
   std::vector<JobDesc> jobs(1);
-  int rc = make_job(ctx, sc, setting, frame_index, tile_begin, tile_end, image, &jobs[0]);
+  DeviceScene scene;
+  int rc = make_job(ctx, sc, setting, frame_index, tile_begin, tile_end, image, &jobs[0], &scene);
   if (rc != YMRT_OK) return rc;
   BatchMemory M;
   if ((rc = context_memory(ctx, 1, &M)) != YMRT_OK) return rc;
   WaveOptions opt;
   if ((rc = batch_options(ctx, jobs, &opt)) != YMRT_OK) return rc;
-  if ((e = upload_constants(jobs[0].scene, ctx->primes.data(), ctx->prime_sums.data(), st)) != cudaSuccess)
+  jobs[0].scene_slot = 0;
+  if ((e = upload_constants(&scene, 1, ctx->primes.data(), ctx->prime_sums.data(), st)) != cudaSuccess)
     return ctx->cuda_fail(e, "uploading constants");
   cudaMemsetAsync(image, 0, img_bytes, st);
   BatchResult r;
@@ -730,29 +769,63 @@ int ymrt_render_batch(ymrt_context* ctx, const ymrt_job* jobs_in, int n_jobs, ym
   cudaSetDevice(ctx->device);
   cudaStream_t st = ctx->stream;
   cudaError_t e;
-  std::vector<JobDesc> jobs((size_t)n_jobs);
+  std::vector<JobDesc> all((size_t)n_jobs);
+  std::vector<DeviceScene> scenes((size_t)n_jobs);
+  std::vector<const void*> keys((size_t)n_jobs);
   for (int k = 0; k < n_jobs; ++k) {
     const ymrt_job& in = jobs_in[k];
     int rc = make_job(ctx, in.scene, &in.setting, in.frame_index, in.tile_begin, in.tile_end,
-                      reinterpret_cast<float4*>(in.out_rgba_device), &jobs[k]);
+                      reinterpret_cast<float4*>(in.out_rgba_device), &all[k], &scenes[k]);
     if (rc != YMRT_OK) return rc;
+    keys[k] = in.scene;
   }
   BatchMemory M;
-  int rc = context_memory(ctx, jobs.size(), &M);
+  int rc = context_memory(ctx, all.size(), &M);
   if (rc != YMRT_OK) return rc;
-  WaveOptions opt;
-  if ((rc = batch_options(ctx, jobs, &opt)) != YMRT_OK) return rc;
-  if ((e = upload_constants(jobs[0].scene, ctx->primes.data(), ctx->prime_sums.data(), st)) != cudaSuccess)
-    return ctx->cuda_fail(e, "uploading constants");
-  for (int k = 0; k < n_jobs; ++k)
-    cudaMemsetAsync(jobs[k].image, 0, (size_t)jobs[k].scene.width * jobs[k].scene.height * sizeof(float4), st);
-  BatchResult r;
-  if ((rc = run_batch(ctx, M, jobs, opt, ctx->profiling, &r)) != YMRT_OK) return rc;
-  if ((e = cudaMemcpyAsync(ctx->counters_host, M.counters, sizeof(WaveCounters), cudaMemcpyDeviceToHost, st)) !=
-      cudaSuccess)
-    return ctx->cuda_fail(e, "reading counters");
-  if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return ctx->cuda_fail(e, "batch");
-  return finish_batch(ctx, r, stats);
+  for (const JobDesc& j : all) cudaMemsetAsync(j.image, 0, (size_t)j.width * j.height * sizeof(float4), st);
+  // Launch groups of jobs whose (scene, sampler) pairs fit the constant-memory slots.
+  BatchResult total;
+  size_t k0 = 0;
+  while (k0 < all.size()) {
+    size_t k1 = k0;
+    std::vector<std::pair<const void*, uint32_t>> seen;
+    while (k1 < all.size()) {
+      const auto key = std::make_pair(keys[k1], scenes[k1].sampler_type);
+      bool found = false;
+      for (const auto& q : seen) found = found || q == key;
+      if (!found) {
+        if (seen.size() == kMaxSceneSlots) break;
+        seen.push_back(key);
+      }
+      ++k1;
+    }
+    std::vector<JobDesc> jobs(all.begin() + k0, all.begin() + k1);
+    std::vector<DeviceScene> js(scenes.begin() + k0, scenes.begin() + k1);
+    std::vector<const void*> ks(keys.begin() + k0, keys.begin() + k1);
+    const std::vector<DeviceScene> slots = assign_slots(jobs, js, ks);
+    WaveOptions opt;
+    if ((rc = batch_options(ctx, jobs, &opt)) != YMRT_OK) return rc;
+    if ((e = upload_constants(slots.data(), (uint32_t)slots.size(), ctx->primes.data(), ctx->prime_sums.data(), st)) !=
+        cudaSuccess)
+      return ctx->cuda_fail(e, "uploading constants");
+    BatchResult r;
+    if ((rc = run_batch(ctx, M, jobs, opt, ctx->profiling, &r)) != YMRT_OK) return rc;
+    total.paths += r.paths;
+    total.waves += r.waves;
+    total.launches += r.launches;
+    total.hits += r.hits;
+    total.ms += r.ms;
+    for (int q = 0; q < 5; ++q) total.stage_ms[q] += r.stage_ms[q];
+    // counters are cleared per group: keep this group's totals
+    if ((e = cudaMemcpyAsync(ctx->counters_host, M.counters, sizeof(WaveCounters), cudaMemcpyDeviceToHost, st)) !=
+        cudaSuccess)
+      return ctx->cuda_fail(e, "reading counters");
+    if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return ctx->cuda_fail(e, "batch");
+    total_counters_add(ctx, k0 == 0);
+    k0 = k1;
+  }
+  *ctx->counters_host = ctx->batch_counters;
+  return finish_batch(ctx, total, stats);
 }
 
 int ymrt_render_forward(ymrt_scene* sc, const ymrt_render_setting* setting, int frame_index, float* out_rgba,
@@ -852,9 +925,11 @@ int ymrt_render_tiles_noalloc(ymrt_scene* sc, const ymrt_render_setting* setting
   if (setting->enable_distant_light) return ctx->fail(YMRT_ERR_UNSUPPORTED, "distant lights are not supported yet");
   if (setting->enable_volume_scattering) return ctx->fail(YMRT_ERR_UNSUPPORTED, "volume scattering is not supported yet");
   std::vector<JobDesc> jobs(1);
+  DeviceScene scene;
   int rc = make_job(ctx, sc, setting, frame_index, tile_begin, tile_end, reinterpret_cast<float4*>(out_rgba_device),
-                    &jobs[0]);
+                    &jobs[0], &scene);
   if (rc != YMRT_OK) return rc;
+  jobs[0].scene_slot = 0;
   const uint32_t spp = jobs[0].spp;
   const uint32_t per_tile = (uint32_t)kTilePixels * spp;
   const uint32_t cap = noalloc_capacity();
@@ -883,7 +958,7 @@ int ymrt_render_tiles_noalloc(ymrt_scene* sc, const ymrt_render_setting* setting
     return ctx->fail(YMRT_ERR_OVERFLOW, "scratch layout exceeds the fixed array");
   M.capacity = cap;
   cudaStream_t st = ctx->stream;
-  if ((e = upload_constants(jobs[0].scene, ctx->primes.data(), ctx->prime_sums.data(), st)) != cudaSuccess)
+  if ((e = upload_constants(&scene, 1, ctx->primes.data(), ctx->prime_sums.data(), st)) != cudaSuccess)
     return ctx->cuda_fail(e, "uploading constants");
   cudaMemsetAsync(out_rgba_device, 0, (size_t)sc->width * sc->height * sizeof(float4), st);
   BatchResult r;
@@ -956,7 +1031,7 @@ int ymrt_debug_trace(ymrt_scene* sc, int n, const float* origin, const float* di
   uint32_t* d_err = sg.out<uint32_t>(1);
   if (sg.err != cudaSuccess) return ctx->cuda_fail(sg.err, "staging");
   cudaMemsetAsync(d_err, 0, sizeof(uint32_t), ctx->stream);
-  upload_constants(sc->dev, ctx->primes.data(), ctx->prime_sums.data(), ctx->stream);
+  upload_constants(&sc->dev, 1, ctx->primes.data(), ctx->prime_sums.data(), ctx->stream);
   launch_debug_trace(n, d_o, d_d, d_lh, d_inst, d_tri, d_t, d_b, d_back, d_nb, d_err, ctx->stream);
   uint32_t errs = 0;
   sg.back(inst, d_inst, n);
@@ -985,7 +1060,7 @@ int ymrt_debug_occluded(ymrt_scene* sc, int n, const float* origin, const float*
   uint32_t* d_err = sg.out<uint32_t>(1);
   if (sg.err != cudaSuccess) return ctx->cuda_fail(sg.err, "staging");
   cudaMemsetAsync(d_err, 0, sizeof(uint32_t), ctx->stream);
-  upload_constants(sc->dev, ctx->primes.data(), ctx->prime_sums.data(), ctx->stream);
+  upload_constants(&sc->dev, 1, ctx->primes.data(), ctx->prime_sums.data(), ctx->stream);
   launch_debug_occluded(n, d_o, d_d, d_tm, d_occ, d_err, ctx->stream);
   uint32_t errs = 0;
   sg.back(occluded, d_occ, n);
@@ -1011,7 +1086,7 @@ int ymrt_debug_halton(ymrt_scene* sc, int n, const int* px, const int* py, const
   float* d_off = sg.out<float>(2 * (size_t)n);
   float* d_dims = sg.out<float>(std::max<size_t>((size_t)n * n_dims, 1));
   if (sg.err != cudaSuccess) return ctx->cuda_fail(sg.err, "staging");
-  upload_constants(sc->dev, ctx->primes.data(), ctx->prime_sums.data(), ctx->stream);
+  upload_constants(&sc->dev, 1, ctx->primes.data(), ctx->prime_sums.data(), ctx->stream);
   launch_debug_halton(n, d_px, d_py, d_s, n_dims, d_idx, d_off, d_dims, ctx->stream);
   sg.back(index, d_idx, n);
   sg.back(offset, d_off, 2 * (size_t)n);

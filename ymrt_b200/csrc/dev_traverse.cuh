@@ -19,6 +19,7 @@
 // they only decide which triangles are tested, never the hit itself.
 #pragma once
 
+#include "dev_constants.cuh"
 #include "ymrt_scene.h"
 
 namespace ym {
@@ -292,7 +293,8 @@ struct ClosestHit {
   NearbyHit nearby[kMaxNearby];
 };
 
-// Closest hit of one world-space ray (TraceRay, src/ShadingUtilities.cuh:310-431).
+// Closest hit of one world-space ray (TraceRay, src/ShadingUtilities.cuh:310-431)
+// in the scene of constant-memory slot `scene`.
 // `volume_only`: traverse only treat_as_boundary instances (TraceVolume, :434-561).
 //
 // One loop serves both levels: each iteration pops one entry -- a top-level
@@ -301,9 +303,10 @@ struct ClosestHit {
 // in. Instance leaves are pushed in distance order with the internal nodes,
 // bottom-level leaves are tested at once, and entries whose box begins
 // beyond the closest hit so far are dropped when popped.
-__device__ __noinline__ bool trace_closest(const DeviceScene& S, TraversalStack& st, vec3 wo, vec3 wd, float tmax,
+__device__ __noinline__ bool trace_closest(uint32_t scene, TraversalStack& st, vec3 wo, vec3 wd, float tmax,
                                            uint32_t last_inst, uint32_t last_tri, bool volume_only, ClosestHit* out,
                                            uint32_t* tri_tests, uint32_t* node_visits) {
+  const DeviceScene& S = c_scenes[scene];
   const uint4* tlas = reinterpret_cast<const uint4*>(S.tlas_nodes);
   const uint4* blas = reinterpret_cast<const uint4*>(S.blas_nodes);
   const bool skip_enabled = last_inst != kEmpty && last_tri != kEmpty;
@@ -436,8 +439,9 @@ __device__ __noinline__ bool trace_closest(const DeviceScene& S, TraversalStack&
 // Any hit within (TMIN, tmax] ignoring boundary-only instances
 // (BVHTraverseShadow, src/ShadingUtilities.cuh:563-635). Same single loop as
 // trace_closest; children are pushed unordered and the first hit ends it.
-__device__ __noinline__ bool trace_occluded(const DeviceScene& S, TraversalStack& st, vec3 wo, vec3 wd, float tmax,
+__device__ __noinline__ bool trace_occluded(uint32_t scene, TraversalStack& st, vec3 wo, vec3 wd, float tmax,
                                             uint32_t* tri_tests, uint32_t* node_visits) {
+  const DeviceScene& S = c_scenes[scene];
   const uint4* tlas = reinterpret_cast<const uint4*>(S.tlas_nodes);
   const uint4* blas = reinterpret_cast<const uint4*>(S.blas_nodes);
   const BoxRay wray = make_box_ray(wo, wd);

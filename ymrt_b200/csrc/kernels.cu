@@ -30,7 +30,6 @@ namespace ym {
 namespace cg = cooperative_groups;
 
 
-__constant__ DeviceScene c_scene;
 
 // ---------------------------------------------------------------- paths ---
 
@@ -45,12 +44,11 @@ __device__ __forceinline__ void store_path(const PathPool& P, uint32_t i, vec3 o
   P.sampler[i] = make_uint4((uint32_t)hs.index, (uint32_t)(hs.index >> 32), hs.dim, hs.aux);
 }
 
+// Per-pixel accumulation (the reference adds the four channels with four
+// float atomics, src/Shading.cu:1859-1862): one vector atomic that adds each
+// channel atomically.
 __device__ __forceinline__ void accumulate_pixel(float4* image, uint32_t pixel, vec3 light, float inv_spp) {
-  float* p = reinterpret_cast<float*>(image + pixel);
-  atomicAdd(p + 0, light.x * inv_spp);
-  atomicAdd(p + 1, light.y * inv_spp);
-  atomicAdd(p + 2, light.z * inv_spp);
-  atomicAdd(p + 3, inv_spp);
+  atomicAdd(image + pixel, make_float4(light.x * inv_spp, light.y * inv_spp, light.z * inv_spp, inv_spp));
 }
 
 // Warp-aggregated slot allocation in the output pool.
@@ -93,7 +91,7 @@ __global__ void __launch_bounds__(256) k_generate(PathPool P, uint32_t base, uin
   const unsigned long long g = path_cursor + tid;
   const uint32_t job = find_job(jobs, n_jobs, g);
   const JobDesc& J = jobs[job];
-  const DeviceScene& S = J.scene;
+  const DeviceScene& S = c_scenes[J.scene_slot];
   const uint32_t spp = J.spp;
   const int frame_index = J.frame_index;
   const uint32_t local_path = (uint32_t)(g - J.path_begin);
@@ -154,16 +152,21 @@ __global__ void __launch_bounds__(256) k_generate(PathPool P, uint32_t base, uin
 __device__ __forceinline__ void file_bucket(WaveCounters* counters, uint32_t bucket) {
   const bool has = bucket != kBucketNone;
   const uint32_t act = __ballot_sync(0xFFFFFFFFu, has);
+  const uint32_t hits = __ballot_sync(0xFFFFFFFFu, has && bucket != kBucketMiss);
   const int lane = threadIdx.x & 31;
-  if (lane == 0 && act) atomicAdd(&counters->hit_count, (uint32_t)__popc(act));
+  if (lane == 0 && hits) atomicAdd(&counters->hit_count, (uint32_t)__popc(hits));
   if (!has) return;
   const uint32_t peers = __match_any_sync(act, bucket);
   if (lane == __ffs(peers) - 1) atomicAdd(&counters->bucket_count[bucket], (uint32_t)__popc(peers));
 }
 
 // Lists the slots holding hits bucket by bucket (a counting sort: the
-// buckets' counts from k_extend give each bucket's start).
-__global__ void __launch_bounds__(256) k_sort_hits(uint32_t count, HitPool H, WaveCounters* counters) {
+// buckets' counts from k_extend give each bucket's start) and ends the paths
+// whose ray left the scene: the background when the environment light is on
+// (the miss branch of Ray_trace_path_tracing, src/Shading.cu:1855-1864), then
+// the path's radiance into its pixel. Misses are not listed.
+__global__ void __launch_bounds__(256) k_sort_hits(uint32_t count, HitPool H, PathPool P,
+                                                   const JobDesc* __restrict__ jobs, WaveCounters* counters) {
   __shared__ uint32_t s_start[kShadeBuckets];
   if (threadIdx.x == 0) {
     uint32_t acc = 0;
@@ -174,7 +177,20 @@ __global__ void __launch_bounds__(256) k_sort_hits(uint32_t count, HitPool H, Wa
   }
   __syncthreads();
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  const uint32_t b = i < count ? (uint32_t)H.bucket[i] : (uint32_t)kBucketNone;
+  uint32_t b = i < count ? (uint32_t)H.bucket[i] : (uint32_t)kBucketNone;
+  if (b == kBucketMiss) {
+    const uint2 pf = P.pixel_flags[i];
+    const JobDesc& J = jobs[pf.y >> kFlagJobShift];
+    const float4 r4 = P.radiance[i];
+    vec3 rad(r4.x, r4.y, r4.z);
+    if (J.setting.enable_env_light) {
+      const float4 t4 = P.throughput[i], d4 = P.ray_d[i];
+      rad += indirect_clamp(J.setting, vec3(t4.x, t4.y, t4.z) * background(vec3(d4.x, d4.y, d4.z)),
+                            (int)(pf.y & kFlagDepthMask));
+    }
+    accumulate_pixel(J.image, pf.x, rad, 1.0f / gmax(J.setting.ssp, 1));
+    b = kBucketNone;
+  }
   const bool has = b != kBucketNone;
   const uint32_t act = __ballot_sync(0xFFFFFFFFu, has);
   if (!has) return;
@@ -200,18 +216,18 @@ __global__ void __launch_bounds__(kTraceBlock, 5) k_extend(PathPool P, uint32_t 
   uint32_t bucket = kBucketNone;
   if (active) {
     const JobDesc& J = jobs[pf.y >> kFlagJobShift];
-    const DeviceScene& S = J.scene;
+    const uint32_t slot = J.scene_slot;
+    const DeviceScene& S = c_scenes[slot];
     const float4 o4 = P.ray_o[i], d4 = P.ray_d[i];
+    (void)J;
     const vec3 o(o4.x, o4.y, o4.z), d(d4.x, d4.y, d4.z);
     const uint2 lh = P.last_hit[i];
     TraversalStack st;
     st.bind(s_stack_entries, s_stack_t);
     ClosestHit ch;
-    bool hit = trace_closest(S, st, o, d, kTMax, lh.x, lh.y, false, &ch, &tests, &nodes);
+    bool hit = trace_closest(slot, st, o, d, kTMax, lh.x, lh.y, false, &ch, &tests, &nodes);
     overflow = st.overflow;
     bool volume_hit = false;
-    float4 t4 = P.throughput[i];
-    vec3 tp(t4.x, t4.y, t4.z);
     vec3 vol_pos(0.0f);
     if (kVol && J.setting.enable_volume_scattering) {
       // volume free flight before the surface (src/Shading.cu:1828-1853)
@@ -228,6 +244,8 @@ __global__ void __launch_bounds__(kTraceBlock, 5) k_extend(PathPool P, uint32_t 
       float vw[kMaxBoundaryRecord];
       const bool hv = sample_volume_scattering(S, o, d, n, vidx, hit ? ch.t : kTMax, &trw, &dist, vw, hs,
                                                &counters->errors);
+      const float4 t4 = P.throughput[i];
+      vec3 tp(t4.x, t4.y, t4.z);
       tp *= trw;
       P.throughput[i] = make_float4(tp.x, tp.y, tp.z, 0.0f);
       P.sampler[i] = make_uint4((uint32_t)hs.index, (uint32_t)(hs.index >> 32), hs.dim, hs.aux);
@@ -246,14 +264,11 @@ __global__ void __launch_bounds__(kTraceBlock, 5) k_extend(PathPool P, uint32_t 
       hit = hit || hv;
     }
     if (!hit) {
-      // Ray_trace_path_tracing miss branch (src/Shading.cu:1855-1864).
-      const float4 r4 = P.radiance[i];
-      vec3 rad(r4.x, r4.y, r4.z);
-      if (J.setting.enable_env_light)
-        rad += indirect_clamp(J.setting, tp * background(d), (int)(pf.y & kFlagDepthMask));
-      const float inv_spp = 1.0f / gmax(J.setting.ssp, 1);
-      accumulate_pixel(J.image, pf.x, rad, inv_spp);
-      P.pixel_flags[i] = make_uint2(pf.x, pf.y | kFlagDead);
+      // a miss: listed in its own bucket; k_shade adds the background and
+      // ends the path (the miss branch of Ray_trace_path_tracing,
+      // src/Shading.cu:1855-1864)
+      H.ids[i] = make_uint4(kEmpty, kEmpty, 0u, 0u);
+      bucket = kBucketMiss;
     } else {
       if (volume_hit) H.bary_t[i] = make_float4(vol_pos.x, vol_pos.y, vol_pos.z, ch.t);
       else H.bary_t[i] = make_float4(ch.b0, ch.b1, ch.b2, ch.t);
@@ -377,9 +392,10 @@ __device__ __forceinline__ float ex_ior(const RayTransfer& rt, uint32_t hit_prim
 // and the transmittance along a shadow ray through every medium it crosses
 // (TraceTr, src/VolumeEval.cuh:420-468). `rt` is the shadow ray's own copy of
 // the nested-media stack; `o`/`d`/`tmax` and the last hit are the shadow ray.
-__device__ __noinline__ vec3 trace_tr(const DeviceScene& S, TraversalStack& st, vec3 o, vec3 d, float tmax,
+__device__ __noinline__ vec3 trace_tr(uint32_t scene, TraversalStack& st, vec3 o, vec3 d, float tmax,
                                       uint32_t last_inst, uint32_t last_tri, RayTransfer& rt, PathSampler& hs,
                                       uint32_t* errors, uint32_t* tests, uint32_t* nodes) {
+  const DeviceScene& S = c_scenes[scene];
   if (S.volume_count == 0) return vec3(1.0f);
   vec3 tr(1.0f);
   const float max_d = tmax;
@@ -392,7 +408,7 @@ __device__ __noinline__ vec3 trace_tr(const DeviceScene& S, TraversalStack& st, 
       break;
     }
     ClosestHit ch;
-    const bool hit = trace_closest(S, st, o, d, ray_t, last_inst, last_tri, true, &ch, tests, nodes);
+    const bool hit = trace_closest(scene, st, o, d, ray_t, last_inst, last_tri, true, &ch, tests, nodes);
     if (!hit) {
       tr *= eval_tr(S, o, d, rt, gmax(max_d - traced, 0.0f), hs, errors);
       break;
@@ -450,6 +466,7 @@ struct SurfaceNee {
   const NearbyHit* nb;
   int n_nb;
   bool media;  // the render's enable_volume_scattering
+  uint32_t slot;  // scene slot
 };
 
 // Transmittance of an unoccluded surface shadow ray (the volume part of the
@@ -461,7 +478,7 @@ __device__ __forceinline__ vec3 surface_shadow_tr(const DeviceScene& S, Traversa
   if (!kVol || !c.media) return vec3(1.0f);
   RayTransfer srt = *c.rt;
   if (tb) boundary_transition(S, srt, c.nb, c.n_nb, errors);
-  return trace_tr(S, st, so, normalize(ldir), maxd, c.inst, c.tri, srt, hs, errors, tests, nodes);
+  return trace_tr(c.slot, st, so, normalize(ldir), maxd, c.inst, c.tri, srt, hs, errors, tests, nodes);
 }
 
 // Where a surface shadow ray goes when shadow rays are deferred: the queue
@@ -509,7 +526,7 @@ __device__ __forceinline__ void nee_shadow_ray(const DeviceScene& S, TraversalSt
     emit_shadow_ray(em, so, normalize(ldir), maxd, ((mis * vec3(1.0f) * fc * Lc) * mul) / div);
     return;
   }
-  if (!trace_occluded(S, st, so, normalize(ldir), maxd, tests, nodes)) {
+  if (!trace_occluded(c.slot, st, so, normalize(ldir), maxd, tests, nodes)) {
     const vec3 tr = surface_shadow_tr<kVol>(S, st, c, so, ldir, maxd, tb, hs, errors, tests, nodes);
     *direct += mis * tr * fc * Lc;
   }
@@ -629,10 +646,11 @@ __device__ __forceinline__ vec3 eval_distant_light(const DeviceScene& S, Travers
 
 // EvalVolumeShapeLight / EvalVolumeDistantLight (src/Shading.cu:202-291, 419-513):
 // next-event estimation at a scattering point inside the media.
-__device__ __noinline__ vec3 eval_volume_lights(const DeviceScene& S, TraversalStack& st, bool distant, int n,
+__device__ __noinline__ vec3 eval_volume_lights(uint32_t slot, TraversalStack& st, bool distant, int n,
                                                 const float* gs, const float* vw, vec3 ray_dir, const RayTransfer& rt,
                                                 vec3 pos, PathSampler& hs, uint32_t* shadow_rays, uint32_t* tests,
                                                 uint32_t* nodes, uint32_t* errors) {
+  const DeviceScene& S = c_scenes[slot];
   vec3 direct(0.0f);
   if (distant) {
     if (S.distant_light_count == 0 || n == 0) return vec3(0.0f);
@@ -649,9 +667,9 @@ __device__ __noinline__ vec3 eval_volume_lights(const DeviceScene& S, TraversalS
       const float pw = eval_mixed_phases(vw, gs, n, -ray_dir, ldir, &wpdf);
       if (pw > kMinColorEps) {
         ++*shadow_rays;
-        if (!trace_occluded(S, st, pos, normalize(ldir), kTMax, tests, nodes)) {
+        if (!trace_occluded(slot, st, pos, normalize(ldir), kTMax, tests, nodes)) {
           RayTransfer srt = rt;
-          const vec3 tr = trace_tr(S, st, pos, normalize(ldir), kTMax, kEmpty, kEmpty, srt, hs, errors, tests, nodes);
+          const vec3 tr = trace_tr(slot, st, pos, normalize(ldir), kTMax, kEmpty, kEmpty, srt, hs, errors, tests, nodes);
           const float mis = power_heuristic(lpdf, wpdf);
           direct += mis * tr * gmin(pw, kMaxColorClamp) * vmin(Li, vec3(kMaxColorClamp));
         }
@@ -667,9 +685,9 @@ __device__ __noinline__ vec3 eval_volume_lights(const DeviceScene& S, TraversalS
         const vec3 Li = distant_eval_li(S, L, pwi, &wpdf);
         if (max_component(Li) > kMinColorEps) {
           ++*shadow_rays;
-          if (!trace_occluded(S, st, pos, normalize(pwi), kTMax, tests, nodes)) {
+          if (!trace_occluded(slot, st, pos, normalize(pwi), kTMax, tests, nodes)) {
             RayTransfer srt = rt;
-            const vec3 tr = trace_tr(S, st, pos, normalize(pwi), kTMax, kEmpty, kEmpty, srt, hs, errors, tests, nodes);
+            const vec3 tr = trace_tr(slot, st, pos, normalize(pwi), kTMax, kEmpty, kEmpty, srt, hs, errors, tests, nodes);
             const float mis = power_heuristic(pspdf, wpdf);
             direct += mis * tr * gmin(pw, kMaxColorClamp) * vmin(Li, vec3(kMaxColorClamp));
           }
@@ -694,9 +712,9 @@ __device__ __noinline__ vec3 eval_volume_lights(const DeviceScene& S, TraversalS
     if (pw > kMinColorEps && valid) {
       const float maxd = length(offset_ray_origin(lpos, lerr, -ldir, lng) - pos) * kShadowRayClamp;
       ++*shadow_rays;
-      if (!trace_occluded(S, st, pos, normalize(ldir), maxd, tests, nodes)) {
+      if (!trace_occluded(slot, st, pos, normalize(ldir), maxd, tests, nodes)) {
         RayTransfer srt = rt;
-        const vec3 tr = trace_tr(S, st, pos, normalize(ldir), maxd, kEmpty, kEmpty, srt, hs, errors, tests, nodes);
+        const vec3 tr = trace_tr(slot, st, pos, normalize(ldir), maxd, kEmpty, kEmpty, srt, hs, errors, tests, nodes);
         const float mis = power_heuristic(lpdf, wpdf);
         direct += mis * tr * gmin(pw, kMaxColorClamp) * vmin(Li, vec3(kMaxColorClamp));
       }
@@ -714,9 +732,9 @@ __device__ __noinline__ vec3 eval_volume_lights(const DeviceScene& S, TraversalS
       if (max_component(Li) > kMinColorEps) {
         const float maxd = length(offset_ray_origin(lpos, lerr, -pwi, lng) - pos) * kShadowRayClamp;
         ++*shadow_rays;
-        if (!trace_occluded(S, st, pos, normalize(pwi), maxd, tests, nodes)) {
+        if (!trace_occluded(slot, st, pos, normalize(pwi), maxd, tests, nodes)) {
           RayTransfer srt = rt;
-          const vec3 tr = trace_tr(S, st, pos, normalize(pwi), maxd, kEmpty, kEmpty, srt, hs, errors, tests, nodes);
+          const vec3 tr = trace_tr(slot, st, pos, normalize(pwi), maxd, kEmpty, kEmpty, srt, hs, errors, tests, nodes);
           const float mis = power_heuristic(pspdf, wpdf);
           direct += mis * tr * gmin(pw, kMaxColorClamp) * vmin(Li, vec3(kMaxColorClamp));
         }
@@ -755,7 +773,8 @@ __global__ void __launch_bounds__(kTraceBlock) k_shade(PathPool P, uint32_t coun
   if (active) {
     const uint32_t job = pf.y >> kFlagJobShift;
     const JobDesc& J = jobs[job];
-    const DeviceScene& S = J.scene;
+    const uint32_t slot = J.scene_slot;
+    const DeviceScene& S = c_scenes[slot];
     const RenderSetting& rs = J.setting;
     float4* image = J.image;
     uint32_t* errors = &counters->errors;
@@ -789,7 +808,12 @@ __global__ void __launch_bounds__(kTraceBlock) k_shade(PathPool P, uint32_t coun
       st.overflow = false;
     }
 
-    if (volume_hit) {
+    if (inst_idx == kEmpty && !volume_hit) {
+      // a miss (Ray_trace_path_tracing, src/Shading.cu:1855-1864): the
+      // background when the environment light is on, then the path ends
+      if (rs.enable_env_light) rad += indirect_clamp(rs, tp * background(rd), depth);
+      accumulate_pixel(image, pf.x, rad, inv_spp);
+    } else if (volume_hit) {
       // Ray_shading_path_tracing volume branch (src/Shading.cu:2066-2126).
       float vw[kMaxBoundaryRecord], gs[kMaxBoundaryRecord];
       int vidx[kMaxBoundaryRecord];
@@ -800,10 +824,10 @@ __global__ void __launch_bounds__(kTraceBlock) k_shade(PathPool P, uint32_t coun
       }
       const vec3 pos = bary;
       if (rs.enable_distant_light)
-        rad += indirect_clamp(rs, tp * eval_volume_lights(S, st, true, n, gs, vw, rd, rt, pos, hs, &shadow_rays, &tests,
+        rad += indirect_clamp(rs, tp * eval_volume_lights(slot, st, true, n, gs, vw, rd, rt, pos, hs, &shadow_rays, &tests,
                                                           &nodes, errors), depth);
       if (rs.enable_shape_light)
-        rad += indirect_clamp(rs, tp * eval_volume_lights(S, st, false, n, gs, vw, rd, rt, pos, hs, &shadow_rays,
+        rad += indirect_clamp(rs, tp * eval_volume_lights(slot, st, false, n, gs, vw, rd, rt, pos, hs, &shadow_rays,
                                                           &tests, &nodes, errors), depth);
       vec3 wi;
       float pdf = 0.0f, pw = 0.0f;
@@ -884,7 +908,8 @@ __global__ void __launch_bounds__(kTraceBlock) k_shade(PathPool P, uint32_t coun
         LayeredBsdf B;
         init_shading_frame(B, hit_back, rd, sp.ng, sp.ns, sp.dpdu, sp.dpdv);
         init_layered_lobes(B, mat.default_mtl, rd, hit_back, ray_ior(rt), ex_ior(rt, inst_idx));
-        const SurfaceNee nc{rd, sp.p, sp.p_err, sp.ng, inst_idx, tri, &rt, nb, n_nb, rs.enable_volume_scattering != 0};
+        const SurfaceNee nc{rd, sp.p, sp.p_err, sp.ng, inst_idx, tri, &rt, nb, n_nb, rs.enable_volume_scattering != 0,
+                            slot};
         const ShadowEmit em{shadow_q, &counters->shadow_count, errors, pf.x, job, tp * inv_spp};
         if (rs.enable_distant_light)
           rad += indirect_clamp(
@@ -976,11 +1001,8 @@ __global__ void __launch_bounds__(kTraceBlock, 5) k_connect(ShadowQueue Q, const
   for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
     const float4 o = Q.o[t], d = Q.d[t], c = Q.c[t];
     const JobDesc& J = jobs[__float_as_uint(c.w)];
-    if (!trace_occluded(J.scene, st, vec3(o.x, o.y, o.z), vec3(d.x, d.y, d.z), o.w, &tests, &nodes)) {
-      float* p = reinterpret_cast<float*>(J.image + __float_as_uint(d.w));
-      atomicAdd(p + 0, c.x);
-      atomicAdd(p + 1, c.y);
-      atomicAdd(p + 2, c.z);
+    if (!trace_occluded(J.scene_slot, st, vec3(o.x, o.y, o.z), vec3(d.x, d.y, d.z), o.w, &tests, &nodes)) {
+      atomicAdd(J.image + __float_as_uint(d.w), make_float4(c.x, c.y, c.z, 0.0f));
     }
   }
   for (int off = 16; off > 0; off >>= 1) {
@@ -1023,7 +1045,7 @@ __global__ void __launch_bounds__(kTraceBlock) k_debug_trace(int n, const float*
   const vec3 d = normalize(vec3(dir[3 * i], dir[3 * i + 1], dir[3 * i + 2]));
   ClosestHit ch;
   uint32_t tests = 0, nodes = 0;
-  const bool hit = trace_closest(c_scene, st, o, d, kTMax, last_hit ? last_hit[2 * i] : kEmpty,
+  const bool hit = trace_closest(0, st, o, d, kTMax, last_hit ? last_hit[2 * i] : kEmpty,
                                  last_hit ? last_hit[2 * i + 1] : kEmpty, false, &ch, &tests, &nodes);
   inst[i] = hit ? ch.inst : kEmpty;
   tri[i] = hit ? ch.tri : kEmpty;
@@ -1046,7 +1068,7 @@ __global__ void __launch_bounds__(kTraceBlock) k_debug_occluded(int n, const flo
   const vec3 o(origin[3 * i], origin[3 * i + 1], origin[3 * i + 2]);
   const vec3 d = normalize(vec3(dir[3 * i], dir[3 * i + 1], dir[3 * i + 2]));
   uint32_t tests = 0, nodes = 0;
-  occluded[i] = trace_occluded(c_scene, st, o, d, tmax[i], &tests, &nodes) ? 1 : 0;
+  occluded[i] = trace_occluded(0, st, o, d, tmax[i], &tests, &nodes) ? 1 : 0;
   if (st.overflow) atomicOr(errors, (uint32_t)kDevErrStack);
 }
 
@@ -1054,7 +1076,7 @@ __global__ void k_debug_halton(int n, const int* px, const int* py, const int* s
                                float* offset, float* dims) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  const DeviceScene& S = c_scene;
+  const DeviceScene& S = c_scenes[0];
   const uint64_t idx = halton_index(S, px[i], py[i], sample[i]);
   index[i] = idx;
   float ox = radical_inverse_2(idx), oy = radical_inverse_3(idx);
@@ -1068,9 +1090,11 @@ __global__ void k_debug_halton(int n, const int* px, const int* py, const int* s
 
 // ------------------------------------------------------------ launchers ---
 
-cudaError_t upload_constants(const DeviceScene& scene, const uint32_t* primes, const uint32_t* prime_sums,
+cudaError_t upload_constants(const DeviceScene* scenes, uint32_t n, const uint32_t* primes, const uint32_t* prime_sums,
                              cudaStream_t stream) {
-  cudaError_t e = cudaMemcpyToSymbolAsync(c_scene, &scene, sizeof(DeviceScene), 0, cudaMemcpyHostToDevice, stream);
+  static_assert(kMaxSceneSlots == (uint32_t)kMaxBatchScenes, "slot count");
+  if (n == 0 || n > kMaxSceneSlots) return cudaErrorInvalidValue;
+  cudaError_t e = cudaMemcpyToSymbolAsync(c_scenes, scenes, sizeof(DeviceScene) * n, 0, cudaMemcpyHostToDevice, stream);
   if (e != cudaSuccess) return e;
   e = cudaMemcpyToSymbolAsync(c_primes, primes, sizeof(uint32_t) * kHaltonDims, 0, cudaMemcpyHostToDevice, stream);
   if (e != cudaSuccess) return e;
@@ -1092,9 +1116,10 @@ void launch_extend(const PathPool& P, uint32_t count, const HitPool& H, const Jo
   else k_extend<false><<<blocks, kTraceBlock, 0, stream>>>(P, count, H, jobs, counters);
 }
 
-void launch_sort_hits(uint32_t count, const HitPool& H, WaveCounters* counters, cudaStream_t stream) {
+void launch_sort_hits(uint32_t count, const HitPool& H, const PathPool& P, const JobDesc* jobs, WaveCounters* counters,
+                      cudaStream_t stream) {
   if (count == 0) return;
-  k_sort_hits<<<(count + 255) / 256, 256, 0, stream>>>(count, H, counters);
+  k_sort_hits<<<(count + 255) / 256, 256, 0, stream>>>(count, H, P, jobs, counters);
 }
 
 uint32_t launch_wave(const PathPool& A, const PathPool& B, const HitPool& H, uint32_t live, uint32_t gen,
@@ -1110,7 +1135,7 @@ uint32_t launch_wave(const PathPool& A, const PathPool& B, const HitPool& H, uin
   if (ev) cudaEventRecord(ev[1], stream);
   launch_extend(A, total, Hs, jobs, counters, opt.volumes, stream);
   if (ev) cudaEventRecord(ev[2], stream);
-  if (opt.sort_hits) launch_sort_hits(total, Hs, counters, stream);
+  if (opt.sort_hits) launch_sort_hits(total, Hs, A, jobs, counters, stream);
   if (ev) cudaEventRecord(ev[3], stream);
   launch_shade(A, total, Hs, B, jobs, counters, opt.volumes, defer, stream);
   if (ev) cudaEventRecord(ev[4], stream);

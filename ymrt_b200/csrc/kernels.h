@@ -22,11 +22,12 @@ constexpr uint32_t kNearbyExplicit = 1u << 31;    // hit ids.w: nearby list stor
 // the hits bucket by bucket, and k_shade runs over that list, so each warp
 // shades hits that take the same code path (lights and pass-through
 // boundaries, volume scattering, or one combination of material lobes).
-constexpr int kShadeBuckets = 34;
+constexpr int kShadeBuckets = 35;
 constexpr uint32_t kBucketCheap = 0;    // light, boundary pass-through, invalid material
 constexpr uint32_t kBucketVolume = 1;   // scattering inside a medium
 constexpr uint32_t kBucketLobes = 2;    // + bit mask of the material's lobes (coat, metal, specular, transmission, diffuse)
-constexpr uint8_t kBucketNone = 0xFF;   // no hit (or no path) in this slot
+constexpr uint32_t kBucketMiss = 34;    // the ray left the scene: background, then the path ends
+constexpr uint8_t kBucketNone = 0xFF;   // no path in this slot
 
 constexpr uint32_t kDevErrStack = 1u;
 constexpr uint32_t kDevErrQueue = 2u;
@@ -60,7 +61,8 @@ struct HitPool {
 // settings, output image and its range in the batch's path space (paths are
 // numbered tile by tile, 256 * spp per 16x16 tile, job after job).
 struct JobDesc {
-  DeviceScene scene;
+  uint32_t scene_slot;            // c_scenes slot of the job's scene (with its sampler type)
+  uint32_t width, height;
   RenderSetting setting;
   float4* image;                  // width * height float4, accumulated with atomics
   int frame_index;
@@ -82,7 +84,7 @@ struct ShadowQueue {
 struct WaveCounters {
   // cleared at the start of every wave (the first kWaveClearBytes bytes)
   uint32_t next_count;             // paths written to the next pool
-  uint32_t hit_count;              // slots listed in HitPool::order
+  uint32_t hit_count;              // hits (slots listed in HitPool::order when sorting)
   uint32_t shadow_count;           // rays written to the ShadowQueue
   uint32_t bucket_count[kShadeBuckets];
   uint32_t bucket_fill[kShadeBuckets];
@@ -99,13 +101,16 @@ struct WaveCounters {
 
 constexpr size_t kWaveClearBytes = offsetof(WaveCounters, errors);
 
-cudaError_t upload_constants(const DeviceScene& scene, const uint32_t* primes, const uint32_t* prime_sums,
+// Uploads `n` scenes into constant-memory slots 0..n-1 and the prime tables.
+cudaError_t upload_constants(const DeviceScene* scenes, uint32_t n, const uint32_t* primes, const uint32_t* prime_sums,
                              cudaStream_t stream);
+constexpr uint32_t kMaxSceneSlots = 64;
 void launch_generate(const PathPool& P, uint32_t base, uint32_t count, unsigned long long path_cursor,
                      const JobDesc* jobs, uint32_t n_jobs, cudaStream_t stream);
 void launch_extend(const PathPool& P, uint32_t count, const HitPool& H, const JobDesc* jobs, WaveCounters* counters,
                    bool volumes, cudaStream_t stream);
-void launch_sort_hits(uint32_t count, const HitPool& H, WaveCounters* counters, cudaStream_t stream);
+void launch_sort_hits(uint32_t count, const HitPool& H, const PathPool& P, const JobDesc* jobs, WaveCounters* counters,
+                      cudaStream_t stream);
 void launch_shade(const PathPool& P, uint32_t count, const HitPool& H, const PathPool& Q, const JobDesc* jobs,
                   WaveCounters* counters, bool volumes, const ShadowQueue* defer, cudaStream_t stream);
 void launch_connect(const ShadowQueue& Q, const JobDesc* jobs, WaveCounters* counters, cudaStream_t stream);
