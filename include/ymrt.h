@@ -115,9 +115,13 @@ int ymrt_set_profiling(ymrt_context* ctx, int enable);
  *   YMRT_OPT_SORT_HITS     (default 1) shade hits grouped by material lobes
  *   YMRT_OPT_DEFER_SHADOWS (default 1) queue surface shadow rays and trace
  *                          them in a separate kernel (not used with volume
- *                          scattering or the indirect clamp) */
+ *                          scattering or the indirect clamp)
+ *   YMRT_OPT_GRAPH_LOOP    (default 1) run the whole wave loop as one CUDA
+ *                          graph (a device-side while loop) instead of one
+ *                          host round trip per wave; off while profiling */
 #define YMRT_OPT_SORT_HITS 1
 #define YMRT_OPT_DEFER_SHADOWS 2
+#define YMRT_OPT_GRAPH_LOOP 3
 int ymrt_set_option(ymrt_context* ctx, int option, int value);
 int ymrt_get_option(const ymrt_context* ctx, int option, int* value);
 

@@ -135,7 +135,7 @@ def _check(rc: int, ctx=None):
         raise YmrtError(rc, msg)
 
 
-OPTIONS = {"sort_hits": 1, "defer_shadows": 2}
+OPTIONS = {"sort_hits": 1, "defer_shadows": 2, "graph_loop": 3}
 
 
 class Context:
@@ -152,7 +152,7 @@ class Context:
             self.set_option(name, value)
 
     def set_option(self, name: str, value) -> None:
-        """Wave-loop options: sort_hits, defer_shadows (see include/ymrt.h)."""
+        """Wave-loop options: sort_hits, defer_shadows, graph_loop (see include/ymrt.h)."""
         _check(library().ymrt_set_option(self.h, OPTIONS[name], int(value)))
 
     def get_option(self, name: str) -> int:

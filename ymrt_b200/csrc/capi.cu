@@ -77,6 +77,21 @@ struct ymrt_context {
   HitPool hits{};
   uint32_t pool_capacity = 0;
   WaveCounters* counters_host = nullptr;  // pinned
+  WaveControl* ctl_host = nullptr;        // pinned
+  DeviceBuffer ctl_buf;
+  // CUDA graph of the wave loop (a while-loop node around two waves), cached
+  // for the memory and options it was captured with
+  bool graph_loop = true;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t graph_exec = nullptr;
+  std::vector<uintptr_t> graph_key;
+  void drop_graph() {
+    if (graph_exec) cudaGraphExecDestroy(graph_exec);
+    if (graph) cudaGraphDestroy(graph);
+    graph_exec = nullptr;
+    graph = nullptr;
+    graph_key.clear();
+  }
   cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
   bool profiling = false;
   cudaEvent_t ev_stage[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
@@ -217,6 +232,8 @@ int ymrt_create(int device_ordinal, ymrt_context** out) {
     if ((e = cudaEventCreate(&ev)) != cudaSuccess) return ctx->cuda_fail(e, "cudaEventCreate");
   if ((e = cudaMallocHost(&ctx->counters_host, sizeof(WaveCounters))) != cudaSuccess)
     return ctx->cuda_fail(e, "cudaMallocHost");
+  if ((e = cudaMallocHost(&ctx->ctl_host, sizeof(WaveControl))) != cudaSuccess)
+    return ctx->cuda_fail(e, "cudaMallocHost");
   if ((e = ctx->counters_buf.ensure(sizeof(WaveCounters))) != cudaSuccess) return ctx->cuda_fail(e, "cudaMalloc");
   ctx->primes = first_primes(kHaltonDims);
   ctx->prime_sums.resize(kHaltonDims);
@@ -238,7 +255,10 @@ void ymrt_destroy(ymrt_context* ctx) {
   ctx->counters_buf.release();
   ctx->jobs_buf.release();
   ctx->image_buf.release();
+  ctx->drop_graph();
   if (ctx->counters_host) cudaFreeHost(ctx->counters_host);
+  if (ctx->ctl_host) cudaFreeHost(ctx->ctl_host);
+  ctx->ctl_buf.release();
   if (ctx->ev_start) cudaEventDestroy(ctx->ev_start);
   if (ctx->ev_stop) cudaEventDestroy(ctx->ev_stop);
   for (auto& ev : ctx->ev_stage)
@@ -266,6 +286,7 @@ int ymrt_set_option(ymrt_context* ctx, int option, int value) {
   switch (option) {
     case YMRT_OPT_SORT_HITS: ctx->sort_hits = value != 0; return YMRT_OK;
     case YMRT_OPT_DEFER_SHADOWS: ctx->defer_shadows = value != 0; return YMRT_OK;
+    case YMRT_OPT_GRAPH_LOOP: ctx->graph_loop = value != 0; return YMRT_OK;
     default: return ctx->fail(YMRT_ERR_INVALID, "unknown option " + std::to_string(option));
   }
 }
@@ -275,6 +296,7 @@ int ymrt_get_option(const ymrt_context* ctx, int option, int* value) {
   switch (option) {
     case YMRT_OPT_SORT_HITS: *value = ctx->sort_hits ? 1 : 0; return YMRT_OK;
     case YMRT_OPT_DEFER_SHADOWS: *value = ctx->defer_shadows ? 1 : 0; return YMRT_OK;
+    case YMRT_OPT_GRAPH_LOOP: *value = ctx->graph_loop ? 1 : 0; return YMRT_OK;
     default: return YMRT_ERR_INVALID;
   }
 }
@@ -528,6 +550,7 @@ struct BatchMemory {
   PathPool pool[2];
   HitPool hits;
   WaveCounters* counters = nullptr;
+  WaveControl* ctl = nullptr;
   JobDesc* jobs = nullptr;  // device job table
   uint32_t capacity = 0;
 };
@@ -592,11 +615,14 @@ std::vector<DeviceScene> assign_slots(std::vector<JobDesc>& jobs, const std::vec
   return slots;
 }
 
-// Renders a batch of jobs (paths numbered job after job) with the
-// host-driven wave loop: one synchronisation per wave to read the number of
-// continuing paths. The job images must be zeroed by the caller.
+// Renders a batch of jobs (paths numbered job after job). The wave loop is
+// planned on the device (k_plan / k_finish); the host either launches the
+// whole loop as one CUDA graph (a while-loop node around two waves, captured
+// once and reused while memory and options stay the same), or, with
+// per-kernel profiling or graph_loop off, launches wave after wave and reads
+// the loop condition after each. The job images must be zeroed by the caller.
 int run_batch(ymrt_context* ctx, const BatchMemory& M, std::vector<JobDesc>& jobs, const WaveOptions& opt,
-              bool profiling, BatchResult* r) {
+              bool profiling, bool use_graph, BatchResult* r) {
   cudaStream_t st = ctx->stream;
   cudaError_t e;
   unsigned long long total = 0;
@@ -607,39 +633,95 @@ int run_batch(ymrt_context* ctx, const BatchMemory& M, std::vector<JobDesc>& job
   if ((e = cudaMemcpyAsync(M.jobs, jobs.data(), sizeof(JobDesc) * jobs.size(), cudaMemcpyHostToDevice, st)) !=
       cudaSuccess)
     return ctx->cuda_fail(e, "uploading the job table");
+  WaveControl& c = *ctx->ctl_host;
+  std::memset(&c, 0, sizeof(c));
+  c.total = total;
+  c.capacity = M.capacity;
+  c.more = 1;
+  // a path lives at most kMaxRayDepth scattering vertices plus its boundary
+  // crossings: a generous bound on waves, reached only by a fault
+  const unsigned long long bound = total / std::max<uint32_t>(M.capacity, 1u) * 80ull + 4096ull;
+  c.max_waves = (uint32_t)std::min<unsigned long long>(bound, 1ull << 30);
+  if ((e = cudaMemcpyAsync(M.ctl, &c, sizeof(c), cudaMemcpyHostToDevice, st)) != cudaSuccess)
+    return ctx->cuda_fail(e, "uploading the wave control");
+  WaveOptions o = opt;
+  o.capacity = M.capacity;
   cudaMemsetAsync(M.counters, 0, sizeof(WaveCounters), st);
+  prepare_persistent_grids();
   cudaEventRecord(ctx->ev_start, st);
-  uint32_t live = 0;
-  unsigned long long cursor = 0;
-  int a = 0;
-  while (live > 0 || cursor < total) {
-    const uint32_t gen = (uint32_t)std::min<unsigned long long>(M.capacity - live, total - cursor);
-    r->launches += launch_wave(M.pool[a], M.pool[a ^ 1], M.hits, live, gen, cursor, M.jobs, (uint32_t)jobs.size(),
-                               M.counters, opt, profiling ? ctx->ev_stage : nullptr, st);
-    if ((e = cudaMemcpyAsync(ctx->counters_host, M.counters, sizeof(WaveCounters), cudaMemcpyDeviceToHost, st)) !=
-        cudaSuccess)
-      return ctx->cuda_fail(e, "reading wave counters");
-    if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return ctx->cuda_fail(e, "wave");
-    if (profiling) {
-      for (int k = 0; k < 5; ++k) {
-        float ms = 0.0f;
-        cudaEventElapsedTime(&ms, ctx->ev_stage[k], ctx->ev_stage[k + 1]);
-        r->stage_ms[k] += ms;
+  if (use_graph && !profiling) {
+    const std::vector<uintptr_t> key = {
+        (uintptr_t)M.pool[0].ray_o, (uintptr_t)M.pool[1].ray_o, (uintptr_t)M.hits.bary_t, (uintptr_t)M.ctl,
+        (uintptr_t)M.jobs, (uintptr_t)M.counters, (uintptr_t)jobs.size(), (uintptr_t)o.volumes,
+        (uintptr_t)o.sort_hits, (uintptr_t)o.defer_shadows, (uintptr_t)o.shadow_queue.o, M.capacity};
+    if (ctx->graph_key != key) {
+      ctx->drop_graph();
+      cudaGraph_t g = nullptr;
+      if ((e = cudaGraphCreate(&g, 0)) != cudaSuccess) return ctx->cuda_fail(e, "cudaGraphCreate");
+      cudaGraphConditionalHandle cond;
+      e = cudaGraphConditionalHandleCreate(&cond, g, 1, cudaGraphCondAssignDefault);
+      cudaGraphNodeParams params{};
+      params.type = cudaGraphNodeTypeConditional;
+      params.conditional.handle = cond;
+      params.conditional.type = cudaGraphCondTypeWhile;
+      params.conditional.size = 1;
+      cudaGraphNode_t node;
+      if (e == cudaSuccess) e = cudaGraphAddNode(&node, g, nullptr, 0, &params);
+      if (e != cudaSuccess) {
+        cudaGraphDestroy(g);
+        return ctx->cuda_fail(e, "building the wave-loop graph");
       }
+      cudaGraph_t body = params.conditional.phGraph_out[0];
+      e = cudaStreamBeginCaptureToGraph(st, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed);
+      if (e == cudaSuccess) {
+        launch_wave(M.pool[0], M.pool[1], M.hits, M.ctl, M.jobs, (uint32_t)jobs.size(), M.counters, o, nullptr, st,
+                    (unsigned long long)cond);
+        launch_wave(M.pool[1], M.pool[0], M.hits, M.ctl, M.jobs, (uint32_t)jobs.size(), M.counters, o, nullptr, st,
+                    (unsigned long long)cond);
+        e = cudaStreamEndCapture(st, &body);
+      }
+      cudaGraphExec_t exec = nullptr;
+      if (e == cudaSuccess) e = cudaGraphInstantiate(&exec, g, 0);
+      if (e != cudaSuccess) {
+        cudaGraphDestroy(g);
+        return ctx->cuda_fail(e, "capturing the wave-loop graph");
+      }
+      ctx->graph = g;
+      ctx->graph_exec = exec;
+      ctx->graph_key = key;
     }
-    live = ctx->counters_host->next_count;
-    r->hits += ctx->counters_host->hit_count;
-    if (live > M.capacity) return ctx->fail(YMRT_ERR_OVERFLOW, "path queue overflow");
-    a ^= 1;
-    cursor += gen;
-    r->paths += gen;
-    ++r->waves;
+    if ((e = cudaGraphLaunch(ctx->graph_exec, st)) != cudaSuccess) return ctx->cuda_fail(e, "launching the wave loop");
+    if ((e = cudaMemcpyAsync(&c, M.ctl, sizeof(c), cudaMemcpyDeviceToHost, st)) != cudaSuccess)
+      return ctx->cuda_fail(e, "reading the wave control");
+    if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return ctx->cuda_fail(e, "wave loop");
+    r->launches += 1;
+  } else {
+    int a = 0;
+    for (;;) {
+      r->launches += launch_wave(M.pool[a], M.pool[a ^ 1], M.hits, M.ctl, M.jobs, (uint32_t)jobs.size(), M.counters,
+                                 o, profiling ? ctx->ev_stage : nullptr, st);
+      if ((e = cudaMemcpyAsync(&c, M.ctl, sizeof(c), cudaMemcpyDeviceToHost, st)) != cudaSuccess)
+        return ctx->cuda_fail(e, "reading the wave control");
+      if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return ctx->cuda_fail(e, "wave");
+      if (profiling) {
+        for (int k = 0; k < 5; ++k) {
+          float ms = 0.0f;
+          cudaEventElapsedTime(&ms, ctx->ev_stage[k], ctx->ev_stage[k + 1]);
+          r->stage_ms[k] += ms;
+        }
+      }
+      if (!c.more) break;
+      a ^= 1;
+    }
   }
   cudaEventRecord(ctx->ev_stop, st);
   if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return ctx->cuda_fail(e, "frame");
   float ms = 0.0f;
   cudaEventElapsedTime(&ms, ctx->ev_start, ctx->ev_stop);
   r->ms = ms;
+  r->paths = c.cursor;
+  r->waves = c.waves;
+  r->hits = c.hits;
   return YMRT_OK;
 }
 
@@ -710,12 +792,14 @@ int context_memory(ymrt_context* ctx, size_t n_jobs, BatchMemory* M) {
   int rc = ctx->ensure_pools();
   if (rc != YMRT_OK) return rc;
   cudaError_t e = ctx->counters_buf.ensure(sizeof(WaveCounters));
+  if (e == cudaSuccess) e = ctx->ctl_buf.ensure(sizeof(WaveControl));
   if (e == cudaSuccess) e = ctx->jobs_buf.ensure(sizeof(JobDesc) * std::max<size_t>(n_jobs, 1));
   if (e != cudaSuccess) return ctx->cuda_fail(e, "allocating the job table");
   M->pool[0] = ctx->pool[0];
   M->pool[1] = ctx->pool[1];
   M->hits = ctx->hits;
   M->counters = ctx->counters_buf.as<WaveCounters>();
+  M->ctl = ctx->ctl_buf.as<WaveControl>();
   M->jobs = ctx->jobs_buf.as<JobDesc>();
   M->capacity = ctx->capacity;
   return YMRT_OK;
@@ -751,7 +835,7 @@ int ymrt_render_tiles(ymrt_scene* sc, const ymrt_render_setting* setting, int fr
     return ctx->cuda_fail(e, "uploading constants");
   cudaMemsetAsync(image, 0, img_bytes, st);
   BatchResult r;
-  if ((rc = run_batch(ctx, M, jobs, opt, ctx->profiling, &r)) != YMRT_OK) return rc;
+  if ((rc = run_batch(ctx, M, jobs, opt, ctx->profiling, ctx->graph_loop, &r)) != YMRT_OK) return rc;
   if (!out_on_device) {
     if ((e = cudaMemcpyAsync(out_rgba, image, img_bytes, cudaMemcpyDeviceToHost, st)) != cudaSuccess)
       return ctx->cuda_fail(e, "copying image");
@@ -809,7 +893,7 @@ int ymrt_render_batch(ymrt_context* ctx, const ymrt_job* jobs_in, int n_jobs, ym
         cudaSuccess)
       return ctx->cuda_fail(e, "uploading constants");
     BatchResult r;
-    if ((rc = run_batch(ctx, M, jobs, opt, ctx->profiling, &r)) != YMRT_OK) return rc;
+    if ((rc = run_batch(ctx, M, jobs, opt, ctx->profiling, ctx->graph_loop, &r)) != YMRT_OK) return rc;
     total.paths += r.paths;
     total.waves += r.waves;
     total.launches += r.launches;
@@ -873,14 +957,14 @@ constexpr size_t kHitSlotBytes = sizeof(float4) + sizeof(uint4) + kMaxNearby * s
 
 uint32_t noalloc_capacity() {
   // counters, one job, and the alignment slack of the carved arrays
-  const size_t fixed = align256(sizeof(WaveCounters)) + align256(sizeof(JobDesc)) + 18 * 256;
+  const size_t fixed = align256(sizeof(WaveCounters)) + align256(sizeof(WaveControl)) + align256(sizeof(JobDesc)) + 18 * 256;
   return (uint32_t)((kNoAllocScratchBytes - fixed) / (2 * kPoolSlotBytes + kHitSlotBytes));
 }
 
 // Carves the two path pools, the hit pool and the counters out of `base`;
 // returns the number of bytes used.
 size_t carve(unsigned char* base, uint32_t n, PathPool pools[2], HitPool* hits, WaveCounters** counters,
-             JobDesc** job) {
+             WaveControl** ctl, JobDesc** job) {
   size_t off = 0;
   auto take = [&](size_t bytes) {
     unsigned char* p = base + off;
@@ -888,6 +972,7 @@ size_t carve(unsigned char* base, uint32_t n, PathPool pools[2], HitPool* hits, 
     return p;
   };
   *counters = reinterpret_cast<WaveCounters*>(take(sizeof(WaveCounters)));
+  *ctl = reinterpret_cast<WaveControl*>(take(sizeof(WaveControl)));
   *job = reinterpret_cast<JobDesc*>(take(sizeof(JobDesc)));
   for (int k = 0; k < 2; ++k) {
     PathPool& P = pools[k];
@@ -954,7 +1039,7 @@ int ymrt_render_tiles_noalloc(ymrt_scene* sc, const ymrt_render_setting* setting
     base = static_cast<unsigned char*>(g_noalloc_addr[ctx->device]);
   }
   BatchMemory M;
-  if (carve(base, cap, M.pool, &M.hits, &M.counters, &M.jobs) > kNoAllocScratchBytes)
+  if (carve(base, cap, M.pool, &M.hits, &M.counters, &M.ctl, &M.jobs) > kNoAllocScratchBytes)
     return ctx->fail(YMRT_ERR_OVERFLOW, "scratch layout exceeds the fixed array");
   M.capacity = cap;
   cudaStream_t st = ctx->stream;
@@ -962,7 +1047,7 @@ int ymrt_render_tiles_noalloc(ymrt_scene* sc, const ymrt_render_setting* setting
     return ctx->cuda_fail(e, "uploading constants");
   cudaMemsetAsync(out_rgba_device, 0, (size_t)sc->width * sc->height * sizeof(float4), st);
   BatchResult r;
-  if ((rc = run_batch(ctx, M, jobs, WaveOptions{}, false, &r)) != YMRT_OK) return rc;
+  if ((rc = run_batch(ctx, M, jobs, WaveOptions{}, false, false, &r)) != YMRT_OK) return rc;
   if ((e = cudaMemcpyAsync(ctx->counters_host, M.counters, sizeof(WaveCounters), cudaMemcpyDeviceToHost, st)) !=
       cudaSuccess)
     return ctx->cuda_fail(e, "reading counters");

@@ -82,11 +82,23 @@ __device__ __forceinline__ uint32_t find_job(const JobDesc* __restrict__ jobs, u
   return lo;
 }
 
-__global__ void __launch_bounds__(256) k_generate(PathPool P, uint32_t base, uint32_t count,
-                                                  unsigned long long path_cursor, const JobDesc* __restrict__ jobs,
-                                                  uint32_t n_jobs) {
-  const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
-  if (tid >= count) return;
+__device__ __forceinline__ void generate_path(const PathPool& P, uint32_t base, uint32_t tid,
+                                              unsigned long long path_cursor, const JobDesc* __restrict__ jobs,
+                                              uint32_t n_jobs);
+
+// Walks the wave's new paths (ctl->gen of them, written after the ctl->live
+// continuing ones) with a grid-stride loop.
+__global__ void __launch_bounds__(256) k_generate(PathPool P, const WaveControl* __restrict__ ctl,
+                                                  const JobDesc* __restrict__ jobs, uint32_t n_jobs) {
+  const uint32_t gen = ctl->gen, live = ctl->live;
+  const unsigned long long cursor = ctl->gen_cursor;
+  for (uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x; tid < gen; tid += gridDim.x * blockDim.x)
+    generate_path(P, live, tid, cursor, jobs, n_jobs);
+}
+
+__device__ __forceinline__ void generate_path(const PathPool& P, uint32_t base, uint32_t tid,
+                                              unsigned long long path_cursor, const JobDesc* __restrict__ jobs,
+                                              uint32_t n_jobs) {
   const uint32_t i = base + tid;
   const unsigned long long g = path_cursor + tid;
   const uint32_t job = find_job(jobs, n_jobs, g);
@@ -165,9 +177,11 @@ __device__ __forceinline__ void file_bucket(WaveCounters* counters, uint32_t buc
 // whose ray left the scene: the background when the environment light is on
 // (the miss branch of Ray_trace_path_tracing, src/Shading.cu:1855-1864), then
 // the path's radiance into its pixel. Misses are not listed.
-__global__ void __launch_bounds__(256) k_sort_hits(uint32_t count, HitPool H, PathPool P,
+__global__ void __launch_bounds__(256) k_sort_hits(const WaveControl* __restrict__ ctl, HitPool H, PathPool P,
                                                    const JobDesc* __restrict__ jobs, WaveCounters* counters) {
   __shared__ uint32_t s_start[kShadeBuckets];
+  const uint32_t count = ctl->count;
+  if (blockIdx.x * blockDim.x >= count) return;  // (uniform per block)
   if (threadIdx.x == 0) {
     uint32_t acc = 0;
     for (int b = 0; b < kShadeBuckets; ++b) {
@@ -176,7 +190,9 @@ __global__ void __launch_bounds__(256) k_sort_hits(uint32_t count, HitPool H, Pa
     }
   }
   __syncthreads();
-  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  for (uint32_t warp_base = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); warp_base < count;
+       warp_base += gridDim.x * blockDim.x) {
+  const uint32_t i = warp_base + (threadIdx.x & 31u);
   uint32_t b = i < count ? (uint32_t)H.bucket[i] : (uint32_t)kBucketNone;
   if (b == kBucketMiss) {
     const uint2 pf = P.pixel_flags[i];
@@ -193,26 +209,35 @@ __global__ void __launch_bounds__(256) k_sort_hits(uint32_t count, HitPool H, Pa
   }
   const bool has = b != kBucketNone;
   const uint32_t act = __ballot_sync(0xFFFFFFFFu, has);
-  if (!has) return;
-  const int lane = threadIdx.x & 31;
-  const uint32_t peers = __match_any_sync(act, b);
-  const int leader = __ffs(peers) - 1;
-  uint32_t base = 0;
-  if (lane == leader) base = atomicAdd(&counters->bucket_fill[b], (uint32_t)__popc(peers));
-  base = __shfl_sync(peers, base, leader);
-  H.order[s_start[b] + base + (uint32_t)__popc(peers & ((1u << lane) - 1u))] = i;
+  if (has) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t peers = __match_any_sync(act, b);
+    const int leader = __ffs(peers) - 1;
+    uint32_t base = 0;
+    if (lane == leader) base = atomicAdd(&counters->bucket_fill[b], (uint32_t)__popc(peers));
+    base = __shfl_sync(peers, base, leader);
+    H.order[s_start[b] + base + (uint32_t)__popc(peers & ((1u << lane) - 1u))] = i;
+  }
+  }
 }
 
+// Walks the wave's paths warp by warp (every lane of a warp takes part in each
+// iteration, for the warp-collective bucket filing); the wave's size comes
+// from the wave-control block, so any grid works (launched with one thread
+// per pool slot, each thread takes at most one path).
 template <bool kVol>
-__global__ void __launch_bounds__(kTraceBlock, 5) k_extend(PathPool P, uint32_t count, HitPool H,
+__global__ void __launch_bounds__(kTraceBlock, 5) k_extend(PathPool P, const WaveControl* __restrict__ ctl, HitPool H,
                                                            const JobDesc* __restrict__ jobs, WaveCounters* counters) {
   YM_TRAVERSAL_SHARED(s_stack);
-  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  uint32_t tests = 0, nodes = 0;
+  const uint32_t count = ctl->count;
+  uint32_t tests = 0, nodes = 0, n_rays = 0;
+  bool overflow = false;
+  for (uint32_t warp_base = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); warp_base < count;
+       warp_base += gridDim.x * blockDim.x) {
+  const uint32_t i = warp_base + (threadIdx.x & 31u);
   bool active = i < count;
   uint2 pf = active ? P.pixel_flags[i] : make_uint2(kEmpty, kFlagDead);
   if (active && (pf.y & kFlagDead)) active = false;
-  bool overflow = false;
   uint32_t bucket = kBucketNone;
   if (active) {
     const JobDesc& J = jobs[pf.y >> kFlagJobShift];
@@ -226,7 +251,7 @@ __global__ void __launch_bounds__(kTraceBlock, 5) k_extend(PathPool P, uint32_t 
     st.bind(s_stack_entries, s_stack_t);
     ClosestHit ch;
     bool hit = trace_closest(slot, st, o, d, kTMax, lh.x, lh.y, false, &ch, &tests, &nodes);
-    overflow = st.overflow;
+    overflow = overflow || st.overflow;
     bool volume_hit = false;
     vec3 vol_pos(0.0f);
     if (kVol && J.setting.enable_volume_scattering) {
@@ -286,8 +311,9 @@ __global__ void __launch_bounds__(kTraceBlock, 5) k_extend(PathPool P, uint32_t 
   }
   if (i < count) H.bucket[i] = (uint8_t)bucket;
   file_bucket(counters, bucket);
+  n_rays += __popc(__ballot_sync(0xFFFFFFFFu, active));
+  }
   // counters: one atomic per warp
-  const uint32_t n_rays = __popc(__ballot_sync(0xFFFFFFFFu, active));
   uint32_t t_sum = tests, n_sum = nodes;
   for (int off = 16; off > 0; off >>= 1) {
     t_sum += __shfl_down_sync(0xFFFFFFFFu, t_sum, off);
@@ -748,17 +774,21 @@ __device__ __noinline__ vec3 eval_volume_lights(uint32_t slot, TraversalStack& s
 // for k_connect instead of traced here, which keeps traversal out of this
 // kernel.
 template <bool kVol, bool kDefer>
-__global__ void __launch_bounds__(kTraceBlock) k_shade(PathPool P, uint32_t count, HitPool H, PathPool Q,
-                                                       const JobDesc* __restrict__ jobs, WaveCounters* counters,
-                                                       ShadowQueue shadow_q) {
+__global__ void __launch_bounds__(kTraceBlock) k_shade(PathPool P, const WaveControl* __restrict__ ctl, HitPool H,
+                                                       PathPool Q, const JobDesc* __restrict__ jobs,
+                                                       WaveCounters* counters, ShadowQueue shadow_q) {
   static_assert(!(kVol && kDefer), "volume transmittance needs the path's sampler: shadow rays are traced inline");
-  // The path slot this thread shades: the t-th listed hit, or (hits not
-  // listed by bucket) slot t itself when it holds a hit.
-  const uint32_t t_idx = blockIdx.x * blockDim.x + threadIdx.x;
   const bool listed = H.order != nullptr;
-  bool active = t_idx < count && (!listed || t_idx < counters->hit_count);
-  const uint32_t i = active ? (listed ? H.order[t_idx] : t_idx) : 0u;
+  const uint32_t count = listed ? min(ctl->count, counters->hit_count) : ctl->count;
   uint32_t shadow_rays = 0, tests = 0, nodes = 0;
+  bool overflow = false;
+  for (uint32_t warp_base = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); warp_base < count;
+       warp_base += gridDim.x * blockDim.x) {
+  // The path slot this lane shades: the t-th listed hit, or (hits not listed
+  // by bucket) slot t itself when it holds a live path.
+  const uint32_t t_idx = warp_base + (threadIdx.x & 31u);
+  bool active = t_idx < count;
+  const uint32_t i = active ? (listed ? H.order[t_idx] : t_idx) : 0u;
   bool alive = false;  // continues into Q
   const uint2 pf = active ? P.pixel_flags[i] : make_uint2(kEmpty, kFlagDead);
   if (pf.y & kFlagDead) active = false;  // a miss (already accumulated) or an empty slot
@@ -962,7 +992,7 @@ __global__ void __launch_bounds__(kTraceBlock) k_shade(PathPool P, uint32_t coun
         }
       }
     }
-    if (st.overflow) atomicOr(&counters->errors, (uint32_t)kDevErrStack);
+    overflow = overflow || st.overflow;
   }
   const uint32_t slot = warp_append(&counters->next_count, alive);
   if (alive) {
@@ -974,6 +1004,8 @@ __global__ void __launch_bounds__(kTraceBlock) k_shade(PathPool P, uint32_t coun
       atomicOr(&counters->errors, (uint32_t)kDevErrQueue);
     }
   }
+  }
+  if (overflow) atomicOr(&counters->errors, (uint32_t)kDevErrStack);
   uint32_t s_sum = shadow_rays, t_sum = tests, n_sum = nodes;
   for (int off = 16; off > 0; off >>= 1) {
     s_sum += __shfl_down_sync(0xFFFFFFFFu, s_sum, off);
@@ -1102,64 +1134,120 @@ cudaError_t upload_constants(const DeviceScene* scenes, uint32_t n, const uint32
                                  stream);
 }
 
-void launch_generate(const PathPool& P, uint32_t base, uint32_t count, unsigned long long path_cursor,
-                     const JobDesc* jobs, uint32_t n_jobs, cudaStream_t stream) {
-  if (count == 0) return;
-  k_generate<<<(count + 255) / 256, 256, 0, stream>>>(P, base, count, path_cursor, jobs, n_jobs);
+// ---------------------------------------------------------- wave control ---
+
+// Start of a wave: the continuing paths left by the previous wave, the new
+// paths to generate (as many as fit), and the per-wave counters cleared.
+__global__ void k_plan(WaveControl* ctl, WaveCounters* counters) {
+  __shared__ uint32_t s_live;
+  if (threadIdx.x == 0) s_live = counters->next_count;
+  __syncthreads();
+  uint32_t* words = reinterpret_cast<uint32_t*>(counters);
+  for (uint32_t k = threadIdx.x; k < (uint32_t)(kWaveClearBytes / sizeof(uint32_t)); k += blockDim.x) words[k] = 0u;
+  if (threadIdx.x == 0) {
+    const uint32_t live = ctl->more ? s_live : 0u;
+    const unsigned long long left = ctl->more ? ctl->total - ctl->cursor : 0ull;
+    const uint32_t room = ctl->capacity > live ? ctl->capacity - live : 0u;
+    const uint32_t gen = (uint32_t)(left < (unsigned long long)room ? left : (unsigned long long)room);
+    ctl->live = live;
+    ctl->gen = gen;
+    ctl->count = live + gen;
+    ctl->gen_cursor = ctl->cursor;
+    ctl->cursor += gen;
+  }
 }
 
-void launch_extend(const PathPool& P, uint32_t count, const HitPool& H, const JobDesc* jobs, WaveCounters* counters,
-                   bool volumes, cudaStream_t stream) {
-  if (count == 0) return;
-  const uint32_t blocks = (count + kTraceBlock - 1) / kTraceBlock;
-  if (volumes) k_extend<true><<<blocks, kTraceBlock, 0, stream>>>(P, count, H, jobs, counters);
-  else k_extend<false><<<blocks, kTraceBlock, 0, stream>>>(P, count, H, jobs, counters);
+// End of a wave: totals, and whether another wave is needed (the loop is
+// bounded by max_waves, after which YMRT_DEVERR_ITER is raised).
+__global__ void k_finish(WaveControl* ctl, WaveCounters* counters, unsigned long long graph_condition) {
+  if (threadIdx.x != 0) return;
+  if (!ctl->more) {
+    if (graph_condition) cudaGraphSetConditional((cudaGraphConditionalHandle)graph_condition, 0u);
+    return;
+  }
+  ctl->hits += counters->hit_count;
+  ctl->waves += 1;
+  bool more = counters->next_count > 0 || ctl->cursor < ctl->total;
+  if (more && ctl->waves >= ctl->max_waves) {
+    atomicOr(&counters->errors, (uint32_t)kDevErrIter);
+    more = false;
+  }
+  if (!more) counters->next_count = 0;
+  ctl->more = more ? 1u : 0u;
+  if (graph_condition) cudaGraphSetConditional((cudaGraphConditionalHandle)graph_condition, more ? 1u : 0u);
 }
 
-void launch_sort_hits(uint32_t count, const HitPool& H, const PathPool& P, const JobDesc* jobs, WaveCounters* counters,
-                      cudaStream_t stream) {
-  if (count == 0) return;
-  k_sort_hits<<<(count + 255) / 256, 256, 0, stream>>>(count, H, P, jobs, counters);
+namespace {
+
+// Persistent grid sizes: resident blocks per SM x SMs, per kernel.
+struct PersistentGrids {
+  int device = -1;
+  uint32_t generate = 0, extend[2] = {0, 0}, sort = 0, shade[3] = {0, 0, 0}, connect = 0;
+};
+PersistentGrids g_grids;
+
+template <typename K>
+uint32_t grid_for(K kernel, int block, int sms) {
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, block, 0) != cudaSuccess || per_sm < 1) per_sm = 1;
+  return (uint32_t)(per_sm * sms);
 }
 
-uint32_t launch_wave(const PathPool& A, const PathPool& B, const HitPool& H, uint32_t live, uint32_t gen,
-                     unsigned long long path_cursor, const JobDesc* jobs, uint32_t n_jobs, WaveCounters* counters,
-                     const WaveOptions& opt, cudaEvent_t* ev, cudaStream_t stream) {
-  const uint32_t total = live + gen;
+}  // namespace
+
+void prepare_persistent_grids() {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (g_grids.device == dev) return;
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  PersistentGrids g;
+  g.device = dev;
+  g.generate = grid_for(k_generate, 256, sms);
+  g.extend[0] = grid_for(k_extend<false>, kTraceBlock, sms);
+  g.extend[1] = grid_for(k_extend<true>, kTraceBlock, sms);
+  g.sort = grid_for(k_sort_hits, 256, sms);
+  g.shade[0] = grid_for(k_shade<false, false>, kTraceBlock, sms);
+  g.shade[1] = grid_for(k_shade<false, true>, kTraceBlock, sms);
+  g.shade[2] = grid_for(k_shade<true, false>, kTraceBlock, sms);
+  g.connect = grid_for(k_connect, kTraceBlock, sms);
+  g_grids = g;
+}
+
+uint32_t launch_wave(const PathPool& A, const PathPool& B, const HitPool& H, WaveControl* ctl, const JobDesc* jobs,
+                     uint32_t n_jobs, WaveCounters* counters, const WaveOptions& opt, cudaEvent_t* ev,
+                     cudaStream_t stream, unsigned long long graph_condition) {
+  prepare_persistent_grids();
+  const PersistentGrids& g = g_grids;
   const ShadowQueue* defer = (!opt.volumes && opt.defer_shadows) ? &opt.shadow_queue : nullptr;
   HitPool Hs = H;
   if (!opt.sort_hits) Hs.order = nullptr;
-  cudaMemsetAsync(counters, 0, kWaveClearBytes, stream);
-  if (ev) cudaEventRecord(ev[0], stream);
-  launch_generate(A, live, gen, path_cursor, jobs, n_jobs, stream);
-  if (ev) cudaEventRecord(ev[1], stream);
-  launch_extend(A, total, Hs, jobs, counters, opt.volumes, stream);
-  if (ev) cudaEventRecord(ev[2], stream);
-  if (opt.sort_hits) launch_sort_hits(total, Hs, A, jobs, counters, stream);
-  if (ev) cudaEventRecord(ev[3], stream);
-  launch_shade(A, total, Hs, B, jobs, counters, opt.volumes, defer, stream);
-  if (ev) cudaEventRecord(ev[4], stream);
-  if (defer && total > 0) launch_connect(*defer, jobs, counters, stream);
-  if (ev) cudaEventRecord(ev[5], stream);
-  if (total == 0) return gen > 0 ? 1u : 0u;
-  return (gen > 0 ? 1u : 0u) + 2u + (opt.sort_hits ? 1u : 0u) + (defer ? 1u : 0u);
-}
-
-void launch_shade(const PathPool& P, uint32_t count, const HitPool& H, const PathPool& Q, const JobDesc* jobs,
-                  WaveCounters* counters, bool volumes, const ShadowQueue* defer, cudaStream_t stream) {
-  if (count == 0) return;
-  const uint32_t blocks = (count + kTraceBlock - 1) / kTraceBlock;
   const ShadowQueue none{};
-  if (volumes) k_shade<true, false><<<blocks, kTraceBlock, 0, stream>>>(P, count, H, Q, jobs, counters, none);
-  else if (defer) k_shade<false, true><<<blocks, kTraceBlock, 0, stream>>>(P, count, H, Q, jobs, counters, *defer);
-  else k_shade<false, false><<<blocks, kTraceBlock, 0, stream>>>(P, count, H, Q, jobs, counters, none);
-}
-
-void launch_connect(const ShadowQueue& Q, const JobDesc* jobs, WaveCounters* counters, cudaStream_t stream) {
-  int sms = 148;
-  int dev = 0;
-  if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  k_connect<<<sms * 5, kTraceBlock, 0, stream>>>(Q, jobs, counters);
+  // The per-path kernels get one thread per pool slot (blocks past the
+  // wave's count return at once), so the hardware block scheduler balances
+  // the uneven per-ray work; k_connect walks its queue with a GPU-sized grid.
+  const uint32_t cap = std::max(opt.capacity, 1u);
+  const uint32_t blocks_256 = (cap + 255) / 256, blocks_trace = (cap + kTraceBlock - 1) / kTraceBlock;
+  k_plan<<<1, 128, 0, stream>>>(ctl, counters);
+  if (ev) cudaEventRecord(ev[0], stream);
+  k_generate<<<blocks_256, 256, 0, stream>>>(A, ctl, jobs, n_jobs);
+  if (ev) cudaEventRecord(ev[1], stream);
+  if (opt.volumes) k_extend<true><<<blocks_trace, kTraceBlock, 0, stream>>>(A, ctl, Hs, jobs, counters);
+  else k_extend<false><<<blocks_trace, kTraceBlock, 0, stream>>>(A, ctl, Hs, jobs, counters);
+  if (ev) cudaEventRecord(ev[2], stream);
+  if (opt.sort_hits) k_sort_hits<<<blocks_256, 256, 0, stream>>>(ctl, Hs, A, jobs, counters);
+  if (ev) cudaEventRecord(ev[3], stream);
+  if (opt.volumes)
+    k_shade<true, false><<<blocks_trace, kTraceBlock, 0, stream>>>(A, ctl, Hs, B, jobs, counters, none);
+  else if (defer)
+    k_shade<false, true><<<blocks_trace, kTraceBlock, 0, stream>>>(A, ctl, Hs, B, jobs, counters, *defer);
+  else
+    k_shade<false, false><<<blocks_trace, kTraceBlock, 0, stream>>>(A, ctl, Hs, B, jobs, counters, none);
+  if (ev) cudaEventRecord(ev[4], stream);
+  if (defer) k_connect<<<g.connect, kTraceBlock, 0, stream>>>(*defer, jobs, counters);
+  if (ev) cudaEventRecord(ev[5], stream);
+  k_finish<<<1, 32, 0, stream>>>(ctl, counters, graph_condition);
+  return 5u + (opt.sort_hits ? 1u : 0u) + (defer ? 1u : 0u);
 }
 
 void launch_accumulate(const float4* noise, float4* acc, uint32_t n, int frame_index, cudaStream_t stream) {

@@ -105,32 +105,50 @@ constexpr size_t kWaveClearBytes = offsetof(WaveCounters, errors);
 cudaError_t upload_constants(const DeviceScene* scenes, uint32_t n, const uint32_t* primes, const uint32_t* prime_sums,
                              cudaStream_t stream);
 constexpr uint32_t kMaxSceneSlots = 64;
-void launch_generate(const PathPool& P, uint32_t base, uint32_t count, unsigned long long path_cursor,
-                     const JobDesc* jobs, uint32_t n_jobs, cudaStream_t stream);
-void launch_extend(const PathPool& P, uint32_t count, const HitPool& H, const JobDesc* jobs, WaveCounters* counters,
-                   bool volumes, cudaStream_t stream);
-void launch_sort_hits(uint32_t count, const HitPool& H, const PathPool& P, const JobDesc* jobs, WaveCounters* counters,
-                      cudaStream_t stream);
-void launch_shade(const PathPool& P, uint32_t count, const HitPool& H, const PathPool& Q, const JobDesc* jobs,
-                  WaveCounters* counters, bool volumes, const ShadowQueue* defer, cudaStream_t stream);
-void launch_connect(const ShadowQueue& Q, const JobDesc* jobs, WaveCounters* counters, cudaStream_t stream);
-// One wave: generates `gen` camera paths (the batch's paths from
-// path_cursor on) after the `live` continuing ones in A, traces them, lists the hits by shading bucket and shades them, writing
+
+
+
+// One wave: plans it on the device (k_plan: continuing paths, new paths to
+// generate), generates the new camera paths after the continuing ones in A,
+// traces them, lists the hits by shading bucket and shades them, writing
 // continuing paths to B. With opt.defer_shadows (surfaces only; the caller
 // turns it off for the indirect clamp, which needs a vertex's whole direct
 // light at once) the shading kernel queues its shadow rays and k_connect
 // traces them.
 // ev (optional, 6 events) is recorded before generate, extend, sort, shade and
-// connect and at the end. Returns the number of kernels launched.
+// connect and at the end. graph_condition: the handle of the CUDA graph's
+// while-loop condition when the wave runs inside one (k_finish sets it).
+// Returns the number of kernels launched.
+// Wave control of one batch in device memory: k_plan fills it at the start
+// of every wave and every kernel of the wave reads its sizes from it, so the
+// wave loop takes no host decisions and can run as a CUDA graph.
+struct WaveControl {
+  unsigned long long cursor;      // next path of the batch to generate
+  unsigned long long total;       // paths in the batch
+  unsigned long long gen_cursor;  // first path generated in this wave
+  unsigned long long hits;        // hits shaded so far
+  uint32_t capacity;              // path slots per pool
+  uint32_t live;                  // continuing paths at the start of this wave
+  uint32_t gen;                   // paths generated in this wave
+  uint32_t count;                 // live + gen
+  uint32_t waves;                 // waves finished
+  uint32_t max_waves;             // bound on waves (then YMRT_DEVERR_ITER)
+  uint32_t more;                  // 1 while paths remain
+  uint32_t reserved;
+};
+
 struct WaveOptions {
+  uint32_t capacity = 0;       // path slots per pool (sizes the grids)
   bool volumes = false;        // volume scattering kernels
   bool sort_hits = true;       // shade hits listed by shading bucket
   bool defer_shadows = false;  // queue surface shadow rays for k_connect (ignored with volumes)
   ShadowQueue shadow_queue{};
 };
-uint32_t launch_wave(const PathPool& A, const PathPool& B, const HitPool& H, uint32_t live, uint32_t gen,
-                     unsigned long long path_cursor, const JobDesc* jobs, uint32_t n_jobs, WaveCounters* counters,
-                     const WaveOptions& opt, cudaEvent_t* ev, cudaStream_t stream);
+uint32_t launch_wave(const PathPool& A, const PathPool& B, const HitPool& H, WaveControl* ctl, const JobDesc* jobs,
+                     uint32_t n_jobs, WaveCounters* counters, const WaveOptions& opt, cudaEvent_t* ev,
+                     cudaStream_t stream, unsigned long long graph_condition = 0);
+// Grid sizes of the persistent kernels for the current device (computed once).
+void prepare_persistent_grids();
 void launch_accumulate(const float4* noise, float4* acc, uint32_t n, int frame_index, cudaStream_t stream);
 void launch_debug_trace(int n, const float* o, const float* d, const uint32_t* lh, uint32_t* inst, uint32_t* tri,
                         float* t, float* bary, int* back, int* nearby, uint32_t* errors, cudaStream_t stream);
