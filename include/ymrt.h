@@ -129,6 +129,14 @@ int ymrt_get_option(const ymrt_context* ctx, int option, int* value);
 /* Parses and prepares a scene on the host (no GPU needed). err may be NULL. */
 int ymrt_scene_load_ymtmp(const char* path, int width, int height, ymrt_host_scene** out, char* err,
                           size_t err_len);
+/* Scene build options (no counterpart in the reference, whose binary BVH has
+ * one primitive per leaf). */
+typedef struct ymrt_load_options {
+  uint32_t max_leaf_triangles; /* wide-BVH leaf size, 1..4 (default 3); also instances per top-level leaf */
+  uint32_t reserved[7];
+} ymrt_load_options;
+int ymrt_scene_load_ymtmp_ex(const char* path, int width, int height, const ymrt_load_options* options,
+                             ymrt_host_scene** out, char* err, size_t err_len);
 void ymrt_host_scene_free(ymrt_host_scene* scene);
 
 /* Host-scene queries (for parity checks against the reference's own scene

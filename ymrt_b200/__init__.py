@@ -67,6 +67,10 @@ def default_setting(spp=1, ray_depth=8, shape_light=True, distant_light=False, v
     return s
 
 
+class LoadOptions(ctypes.Structure):
+    _fields_ = [("max_leaf_triangles", ctypes.c_uint32), ("reserved", ctypes.c_uint32 * 7)]
+
+
 class Job(ctypes.Structure):
     _fields_ = [("scene", ctypes.c_void_p), ("setting", RenderSetting), ("frame_index", ctypes.c_int),
                 ("tile_begin", ctypes.c_int), ("tile_end", ctypes.c_int), ("out_rgba_device", ctypes.c_void_p)]
@@ -108,6 +112,8 @@ def library():
     L.ymrt_set_option.argtypes = [vp, i, i]
     L.ymrt_get_option.argtypes = [vp, i, ctypes.POINTER(i)]
     L.ymrt_scene_load_ymtmp.argtypes = [ctypes.c_char_p, i, i, ctypes.POINTER(vp), ctypes.c_char_p, sz]
+    L.ymrt_scene_load_ymtmp_ex.argtypes = [ctypes.c_char_p, i, i, ctypes.POINTER(LoadOptions), ctypes.POINTER(vp),
+                                           ctypes.c_char_p, sz]
     L.ymrt_host_scene_free.argtypes = [vp]
     L.ymrt_host_scene_query.restype = ctypes.c_longlong
     L.ymrt_host_scene_query.argtypes = [vp, i, i, vp, sz]
@@ -181,10 +187,13 @@ class Context:
 class HostScene:
     """A parsed and prepared .ymtmp scene (no GPU involved)."""
 
-    def __init__(self, path: str, width: int, height: int):
+    def __init__(self, path: str, width: int, height: int, max_leaf_triangles: int = 3):
         self.h = ctypes.c_void_p()
         err = ctypes.create_string_buffer(1024)
-        rc = library().ymrt_scene_load_ymtmp(path.encode(), width, height, ctypes.byref(self.h), err, len(err))
+        opts = LoadOptions()
+        opts.max_leaf_triangles = max_leaf_triangles
+        rc = library().ymrt_scene_load_ymtmp_ex(path.encode(), width, height, ctypes.byref(opts), ctypes.byref(self.h),
+                                                err, len(err))
         if rc != YMRT_OK:
             raise YmrtError(rc, err.value.decode(errors="replace"))
         self.width, self.height = width, height

@@ -302,6 +302,11 @@ int ymrt_get_option(const ymrt_context* ctx, int option, int* value) {
 }
 
 int ymrt_scene_load_ymtmp(const char* path, int width, int height, ymrt_host_scene** out, char* err, size_t err_len) {
+  return ymrt_scene_load_ymtmp_ex(path, width, height, nullptr, out, err, err_len);
+}
+
+int ymrt_scene_load_ymtmp_ex(const char* path, int width, int height, const ymrt_load_options* options,
+                             ymrt_host_scene** out, char* err, size_t err_len) {
   auto report = [&](int code, const std::string& msg) {
     g_last_error = msg;
     if (err && err_len) {
@@ -316,6 +321,11 @@ int ymrt_scene_load_ymtmp(const char* path, int width, int height, ymrt_host_sce
   if (!hs) return report(YMRT_ERR_OOM, "out of host memory");
   std::string msg;
   int rc;
+  if (options) {
+    if (options->max_leaf_triangles < 1 || options->max_leaf_triangles > 4)
+      return report(YMRT_ERR_INVALID, "max_leaf_triangles must be 1..4");
+    hs->s.max_leaf_prims = options->max_leaf_triangles;
+  }
   try {
     rc = load_ymtmp(path, &hs->s, &msg);
     if (rc == YMRT_OK) rc = prepare_scene(&hs->s, width, height, &msg);

@@ -376,12 +376,12 @@ std::vector<BinNode> build_binary(std::vector<BuildItem>& items) {
 // ------------------------------------------------------- wide BVH (8) ---
 
 constexpr int kWide = 8;
-constexpr uint32_t kMaxLeafPrims = 3;
 
 struct WideBuilder {
   const std::vector<BinNode>* bin;
   std::vector<WideNode>* out;
   std::vector<uint32_t>* prim_order;  // primitive (item position) per wide-leaf slot
+  uint32_t max_leaf;                  // a subtree of at most this many primitives becomes a leaf
 
   static uint8_t quant_exp(float extent) {
     // smallest e with extent / 2^e <= 250 (margin for outward rounding)
@@ -420,7 +420,7 @@ struct WideBuilder {
         float best_area = -1.0f;
         for (int i = 0; i < (int)cand.size(); ++i) {
           const BinNode& c = B[cand[i]];
-          if (c.left == kEmpty || c.count <= kMaxLeafPrims) continue;
+          if (c.left == kEmpty || c.count <= max_leaf) continue;
           const float a = box_area(c.box);
           if (a > best_area) {
             best_area = a;
@@ -451,7 +451,7 @@ struct WideBuilder {
     std::vector<uint32_t> internal;
     for (size_t i = 0; i < cand.size(); ++i) {
       const BinNode& c = B[cand[i]];
-      if (c.left == kEmpty || c.count <= kMaxLeafPrims) {
+      if (c.left == kEmpty || c.count <= max_leaf) {
         const uint32_t off = (uint32_t)prim_order->size() - node.prim_base;
         for (uint32_t k = 0; k < c.count; ++k) prim_order->push_back(c.offset + k);
         node.meta[i] = (uint8_t)((c.count << 5) | off);
@@ -497,10 +497,11 @@ struct WideBuilder {
 
 // Builds the wide BVH for a binary tree; appends nodes to `out` (root first)
 // and the primitive order of the leaves to `prim_order`.
-uint32_t build_wide(const std::vector<BinNode>& bin, std::vector<WideNode>* out, std::vector<uint32_t>* prim_order) {
+uint32_t build_wide(const std::vector<BinNode>& bin, std::vector<WideNode>* out, std::vector<uint32_t>* prim_order,
+                    uint32_t max_leaf) {
   const uint32_t root = (uint32_t)out->size();
   out->resize(out->size() + 1);
-  WideBuilder wb{&bin, out, prim_order};
+  WideBuilder wb{&bin, out, prim_order, max_leaf};
   wb.build(0, root);
   return root;
 }
@@ -971,7 +972,7 @@ int prepare_scene(HostScene* s, int width, int height, std::string* error) {
     s->all_uv.insert(s->all_uv.end(), m.uv.begin(), m.uv.end());
 
     std::vector<uint32_t> order;
-    gd.node_offset = build_wide(bin, &s->blas_nodes, &order);
+    gd.node_offset = build_wide(bin, &s->blas_nodes, &order, s->max_leaf_prims);
     // the wide builder numbered nodes relative to the whole array already;
     // prim_base values are relative to this mesh's triangle block.
     gd.wtri_offset = (uint32_t)(s->wtris.size() / 3);
@@ -1008,7 +1009,7 @@ int prepare_scene(HostScene* s, int width, int height, std::string* error) {
   s->instances.swap(reordered);
   s->tlas_nodes.clear();
   s->tlas_prims.clear();
-  build_wide(tbin, &s->tlas_nodes, &s->tlas_prims);
+  build_wide(tbin, &s->tlas_nodes, &s->tlas_prims, s->max_leaf_prims);
   s->triangle_count_instanced = 0;
   for (const Instance& inst : s->instances) s->triangle_count_instanced += s->meshes[inst.geometry_idx].tris.size() / 3;
 

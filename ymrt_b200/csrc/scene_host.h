@@ -47,6 +47,7 @@ struct HostScene {
   std::vector<float> shape_light_table;
   CameraDesc camera{};
   int width = 0, height = 0;
+  uint32_t max_leaf_prims = 3;  // wide-BVH leaf size (1..4), a build option
 
   // flattened device-side arrays (filled by prepare())
   std::vector<GeometryDesc> geo_desc;
