@@ -178,6 +178,105 @@ def kernel_table(pst):
     return out
 
 
+def batch_renders(seed: int = 0, n: int = 64):
+    """The batched workload: n renders, each a Cornell-like or instanced
+    scene variant (per-render scene seed), at a resolution drawn from
+    {256x256, 512x512, 640x480, 1024x1024} and U{4..64} spp, all seeded.
+    Instanced variants use two scene seeds (their BVH build dominates set-up)."""
+    rng = np.random.default_rng(seed)
+    res = [(256, 256), (512, 512), (640, 480), (1024, 1024)]
+    out = []
+    for k in range(n):
+        kind = "instanced" if rng.random() < 0.25 else "cornell"
+        scene_seed = int(rng.integers(0, 2)) if kind == "instanced" else k
+        W, H = res[int(rng.integers(0, len(res)))]
+        spp = int(rng.integers(4, 65))
+        out.append({"scene": kind, "seed": scene_seed, "width": W, "height": H, "spp": spp,
+                    "depth": 12 if kind == "instanced" else 8})
+    return out
+
+
+def run_batch_workload(args):
+    """64 renders in one batch (one CUDA-graph wave loop over all of them)
+    against the same renders made one after another."""
+    import torch
+    import ymrt_b200 as Y
+    from ymrt_b200 import scenes
+
+    rank, world, local_rank = dist_env()
+    torch.cuda.set_device(local_rank)
+    perm = scenes.halton_permutations()
+    specs = batch_renders(seed=rank)
+    ctx = Y.Context(local_rank)
+    hosts, renders = {}, []
+    for sp in specs:
+        key = (sp["scene"], sp["seed"], sp["width"], sp["height"])
+        if key not in hosts:
+            hosts[key] = Y.Scene(ctx, Y.HostScene(scenes.scene_path(sp["scene"], sp["seed"]), sp["width"], sp["height"]),
+                                 perm)
+        out = torch.zeros((sp["height"], sp["width"], 4), dtype=torch.float32, device="cuda")
+        renders.append([hosts[key], Y.default_setting(spp=sp["spp"], ray_depth=sp["depth"]), 1, out])
+    flush = torch.zeros(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
+
+    def step(i):
+        for r in renders:
+            r[2] = i + 1
+        st = Y.render_batch(ctx, renders)
+        flush.add_(1.0)
+        return st
+
+    tuned = None
+    if args.autotune:
+        from ymrt_b200 import autotune
+        r = autotune.tune_batch(ctx, renders, space={"queue_capacity": [1 << 21, 1 << 22], "sort_hits": [0, 1]},
+                                repeats=1)
+        tuned = {"best": r["best"], "table": [{"config": t["config"], "ms": t["ms"]} for t in r["table"]]}
+    for i in range(args.warmup):
+        step(i)
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record()
+    rays = launches = errors = 0
+    for i in range(args.steps):
+        st = step(args.warmup + i)
+        rays += st.extension_rays + st.shadow_rays
+        launches += st.kernel_launches
+        errors |= st.device_errors
+    ev1.record()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    elapsed = ev0.elapsed_time(ev1)
+    # the same renders one after another (frame 1 of each)
+    seq_ms, seq_rays = 0.0, 0
+    for sc, setting, _, out in renders:
+        _, s1 = sc.render(setting, 1, out=out)
+        seq_ms += s1.ms_total
+        seq_rays += s1.extension_rays + s1.shadow_rays
+    batch_ms = elapsed / args.steps
+    paths = sum(sp["width"] * sp["height"] * sp["spp"] for sp in specs)
+    result = {
+        "metric": "Mrays/s", "value": round(rays / (elapsed * 1e-3) / 1e6, 2), "unit": "Mrays/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(batch_ms, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded .ymtmp scenes generated by ymrt_b200.scenes)",
+        "config": {"workload": f"batch of {len(specs)} renders (Cornell-like and instanced variants, "
+                               "256x256..1024x1024, 4-64 spp)", "paths_per_step": paths,
+                   "l2": "256 MB buffer written between steps"},
+        "spp_per_s": round(paths / (batch_ms * 1e-3), 1),
+        "sequential": {"ms": round(seq_ms, 3), "mrays_s": round(seq_rays / (seq_ms * 1e-3) / 1e6, 2),
+                       "batch_speedup": round(seq_ms / batch_ms, 3)},
+        "gpu_launches": int(launches), "device_errors": int(errors), "clocks": clk,
+        "autotuned": tuned,
+        "renders": specs,
+    }
+    for sc in hosts.values():
+        sc.close()
+    ctx.close()
+    return result if rank == 0 else None
+
+
 def run_ours(args):
     import torch
     import ymrt_b200 as Y
@@ -455,18 +554,21 @@ def main(argv=None):
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="instanced")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["batch"], default="instanced")
     ap.add_argument("--spp", type=int, default=0)
     ap.add_argument("--queue", type=int, default=0, help="path queue capacity (0 = library default)")
     ap.add_argument("--cpu-budget", type=float, default=12.0, help="seconds of CPU work per reference sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-ref-cuda", action="store_true", help="skip timing the reference's own CUDA kernels")
+    ap.add_argument("--autotune", action="store_true", help="batch workload: tune the wave options first")
     args = ap.parse_args(argv)
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
         with quiet_stdout():
             res = run_reference(args)
+    elif args.workload == "batch":
+        res = run_batch_workload(args)
     else:
         res = run_ours(args)
     if res is not None:
