@@ -165,6 +165,7 @@ int ymrt_scene_upload(ymrt_context* ctx, const ymrt_host_scene* scene, const uin
  * (src/LowDiscrepancy.cpp:179), which its GuiModule::UpdateScene uploads
  * (src/core/GuiModule.cpp:256). Needed only for Sobol renders. */
 int ymrt_scene_set_sobol_matrices(ymrt_scene* scene, const uint32_t* matrices, size_t count);
+/* Scenes must be freed before the context they were uploaded to. */
 void ymrt_scene_free(ymrt_scene* scene);
 
 /* ---- rendering ---- */
@@ -186,7 +187,30 @@ typedef struct ymrt_job {
   int frame_index;               /* >= 1 */
   int tile_begin, tile_end;      /* 16x16 tiles to render; 0, 0 = all */
   float* out_rgba_device;        /* width*height*4 floats of device memory, overwritten */
+  /* differentiable rendering (NULL otherwise): */
+  float* path_radiance_device;   /* forward: receives each path's radiance (ymrt_job_path_count * 4 floats) */
+  const float* dloss_device;     /* backward: dLoss/dImage, width*height*4 floats */
 } ymrt_job;
+
+/* Paths a job renders: tiles * 256 * spp (sizes path_radiance_device). */
+unsigned long long ymrt_job_path_count(const ymrt_job* job);
+
+/* Path-replay adjoint (no counterpart in the reference, which has no
+ * backward pass): gradients of a loss with respect to every material's
+ * diffuse albedo (rgb) and roughness (alpha_x = alpha_y), given dLoss/dImage
+ * per job. The jobs must be the ones rendered (by ymrt_render_batch) with
+ * path_radiance_device set, with unchanged scenes and settings: every path is
+ * re-traced with its own samples. grads_device receives 4 floats per material
+ * (n_materials materials, in the scene's material order), overwritten.
+ * Surfaces only: volume scattering and the indirect clamp are rejected. */
+int ymrt_render_backward(ymrt_context* ctx, const ymrt_job* jobs, int n_jobs, float* grads_device,
+                         uint32_t n_materials, ymrt_stats* stats);
+
+/* Material parameters a backward pass differentiates, 4 floats per material:
+ * diffuse albedo r, g, b and roughness (stored as alpha_x and alpha_y). Light
+ * materials are skipped (set) or read as zeros (get). */
+int ymrt_scene_set_material_params(ymrt_scene* scene, uint32_t first, uint32_t count, const float* params);
+int ymrt_scene_get_material_params(const ymrt_scene* scene, uint32_t first, uint32_t count, float* params);
 
 /* Renders n_jobs renders (scenes, resolutions, spp and settings may all
  * differ; scenes must belong to ctx) together: their paths share the wave

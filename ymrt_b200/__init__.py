@@ -73,7 +73,8 @@ class LoadOptions(ctypes.Structure):
 
 class Job(ctypes.Structure):
     _fields_ = [("scene", ctypes.c_void_p), ("setting", RenderSetting), ("frame_index", ctypes.c_int),
-                ("tile_begin", ctypes.c_int), ("tile_end", ctypes.c_int), ("out_rgba_device", ctypes.c_void_p)]
+                ("tile_begin", ctypes.c_int), ("tile_end", ctypes.c_int), ("out_rgba_device", ctypes.c_void_p),
+                ("path_radiance_device", ctypes.c_void_p), ("dloss_device", ctypes.c_void_p)]
 
 
 class Stats(ctypes.Structure):
@@ -121,6 +122,11 @@ def library():
     L.ymrt_scene_free.argtypes = [vp]
     L.ymrt_scene_set_sobol_matrices.argtypes = [vp, vp, sz]
     L.ymrt_render_batch.argtypes = [vp, ctypes.POINTER(Job), i, ctypes.POINTER(Stats)]
+    L.ymrt_render_backward.argtypes = [vp, ctypes.POINTER(Job), i, vp, ctypes.c_uint32, ctypes.POINTER(Stats)]
+    L.ymrt_job_path_count.restype = ctypes.c_ulonglong
+    L.ymrt_job_path_count.argtypes = [ctypes.POINTER(Job)]
+    L.ymrt_scene_set_material_params.argtypes = [vp, ctypes.c_uint32, ctypes.c_uint32, vp]
+    L.ymrt_scene_get_material_params.argtypes = [vp, ctypes.c_uint32, ctypes.c_uint32, vp]
     L.ymrt_render_forward.argtypes = [vp, ctypes.POINTER(RenderSetting), i, vp, i, ctypes.POINTER(Stats)]
     L.ymrt_render_tiles.argtypes = [vp, ctypes.POINTER(RenderSetting), i, i, i, vp, i, ctypes.POINTER(Stats)]
     L.ymrt_accumulate.argtypes = [vp, vp, vp, i]
@@ -148,7 +154,9 @@ class Context:
     """One CUDA device + stream (the reference's RenderModule path-tracing stream)."""
 
     def __init__(self, device: int = 0, queue_capacity: int = 0, profiling: bool = False, **options):
+        import weakref
         self.h = ctypes.c_void_p()
+        self._scenes = weakref.WeakSet()  # scenes made on this context: freed before it
         _check(library().ymrt_create(device, ctypes.byref(self.h)))
         if queue_capacity:
             library().ymrt_set_queue_capacity(self.h, queue_capacity)
@@ -168,6 +176,8 @@ class Context:
 
     def close(self):
         if self.h:
+            for sc in list(self._scenes):
+                sc.close()
             library().ymrt_destroy(self.h)
             self.h = ctypes.c_void_p()
 
@@ -260,6 +270,19 @@ class Scene:
         self.h = ctypes.c_void_p()
         _check(library().ymrt_scene_upload(ctx.h, host.h, _p(perm), perm.size, ctypes.byref(self.h)), ctx.h)
         self.host = host
+        ctx._scenes.add(self)
+
+    def material_params(self) -> np.ndarray:
+        """(materials, 4) float32: diffuse albedo r, g, b and roughness per
+        material (zeros for light materials)."""
+        n = int(self.host.counts()["materials"])
+        out = np.zeros((n, 4), np.float32)
+        _check(library().ymrt_scene_get_material_params(self.h, 0, n, _p(out)), self.ctx.h)
+        return out
+
+    def set_material_params(self, params: np.ndarray, first: int = 0) -> None:
+        p = np.ascontiguousarray(params, dtype=np.float32).reshape(-1, 4)
+        _check(library().ymrt_scene_set_material_params(self.h, first, p.shape[0], _p(p)), self.ctx.h)
 
     def set_sobol_matrices(self, matrices: np.ndarray) -> None:
         """Generator matrices for the Sobol sampler (4096 x 32 uint32)."""
@@ -267,9 +290,11 @@ class Scene:
         _check(library().ymrt_scene_set_sobol_matrices(self.h, _p(m), m.size), self.ctx.h)
 
     def close(self):
-        if self.h:
+        # a scene outlives its context only as a handle: the context's close()
+        # freed it already
+        if self.h and self.ctx.h:
             library().ymrt_scene_free(self.h)
-            self.h = ctypes.c_void_p()
+        self.h = ctypes.c_void_p()
 
     def __del__(self):
         try:
@@ -329,10 +354,7 @@ class Scene:
         return idx, off, dims[:, :n_dims]
 
 
-def render_batch(ctx: Context, renders) -> Stats:
-    """Renders several (scene, setting, frame_index, out, tile_begin, tile_end)
-    tuples in one batch; each `out` is a torch CUDA float32 tensor of its
-    scene's (H, W, 4) shape and receives that render."""
+def _jobs(renders, records=None, dlosses=None):
     jobs = (Job * len(renders))()
     for k, r in enumerate(renders):
         scene, setting, frame, out = r[:4]
@@ -344,7 +366,39 @@ def render_batch(ctx: Context, renders) -> Stats:
         jobs[k].frame_index = frame
         jobs[k].tile_begin, jobs[k].tile_end = tb, te
         jobs[k].out_rgba_device = out.data_ptr()
+        if records is not None:
+            jobs[k].path_radiance_device = records[k].data_ptr()
+        if dlosses is not None:
+            jobs[k].dloss_device = dlosses[k].data_ptr()
+    return jobs
+
+
+def render_batch(ctx: Context, renders, records=None) -> Stats:
+    """Renders several (scene, setting, frame_index, out, tile_begin, tile_end)
+    tuples in one batch; each `out` is a torch CUDA float32 tensor of its
+    scene's (H, W, 4) shape and receives that render. `records` (optional,
+    one CUDA float32 tensor of path_count(render) x 4 per render) receive
+    each path's radiance, for a later backward pass."""
+    jobs = _jobs(renders, records)
     stats = Stats()
     _check(library().ymrt_render_batch(ctx.h, jobs, len(renders), ctypes.byref(stats)), ctx.h)
+    return stats
+
+
+def path_count(render) -> int:
+    """Paths the render (as render_batch takes it) traces."""
+    return int(library().ymrt_job_path_count(ctypes.byref(_jobs([render])[0])))
+
+
+def render_backward(ctx: Context, renders, records, dlosses, grads) -> Stats:
+    """Path-replay adjoint of render_batch(ctx, renders, records): `dlosses`
+    holds dLoss/dImage per render (CUDA float32, (H, W, 4)); `grads` (CUDA
+    float32, (materials, 4)) receives dLoss/d(albedo rgb, roughness) per
+    material."""
+    jobs = _jobs(renders, records, dlosses)
+    stats = Stats()
+    assert grads.is_cuda and grads.dtype.is_floating_point and grads.is_contiguous()
+    _check(library().ymrt_render_backward(ctx.h, jobs, len(renders), grads.data_ptr(), grads.shape[0],
+                                          ctypes.byref(stats)), ctx.h)
     return stats
 

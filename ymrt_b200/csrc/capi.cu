@@ -116,7 +116,8 @@ struct ymrt_context {
   int ensure_pools() {
     if (pool_capacity == capacity) return YMRT_OK;
     const size_t n = capacity;
-    const size_t pool_bytes = n * (4 * sizeof(float4) + 2 * sizeof(uint2) + sizeof(uint4) + sizeof(RayTransfer) + 16);
+    const size_t pool_bytes =
+        n * (4 * sizeof(float4) + 2 * sizeof(uint2) + sizeof(uint4) + sizeof(RayTransfer) + sizeof(uint32_t) + 1) + 64;
     for (int k = 0; k < 2; ++k) {
       cudaError_t e = pool_buf[k].ensure(pool_bytes);
       if (e != cudaSuccess) return cuda_fail(e, "allocating path pool");
@@ -131,6 +132,7 @@ struct ymrt_context {
       P.last_hit = reinterpret_cast<uint2*>(p); p += n * sizeof(uint2);
       P.transfer = reinterpret_cast<RayTransfer*>(p); p += n * sizeof(RayTransfer);
       p = reinterpret_cast<char*>((reinterpret_cast<uintptr_t>(p) + 15) & ~uintptr_t(15));
+      P.path_id = reinterpret_cast<uint32_t*>(p); p += n * sizeof(uint32_t);
       P.transfer_count = reinterpret_cast<uint8_t*>(p);
       P.capacity = capacity;
     }
@@ -189,6 +191,7 @@ uint32_t shading_bucket(const HostScene& s, const Instance& inst) {
 struct ymrt_scene {
   ymrt_context* ctx = nullptr;
   DeviceScene dev{};
+  std::vector<Material> materials;  // host copy (material parameters can be updated)
   std::vector<std::unique_ptr<DeviceBuffer>> buffers;
   int width = 0, height = 0;
   uint64_t triangles = 0;
@@ -467,6 +470,7 @@ int ymrt_scene_upload(ymrt_context* ctx, const ymrt_host_scene* hs, const uint32
   UP(s.all_nrm, normals);
   UP(s.all_uv, texcoords);
   UP(s.materials, materials);
+  sc->materials = s.materials;
   UP(s.distant_lights, distant_lights);
   UP(s.shape_lights, shape_lights);
   UP(s.shape_light_table, shape_light_table);
@@ -573,7 +577,8 @@ struct BatchResult {
 
 // Checks one render's arguments and fills its job (path range left at 0).
 int make_job(ymrt_context* ctx, ymrt_scene* sc, const ymrt_render_setting* setting, int frame_index, int tile_begin,
-             int tile_end, float4* image, JobDesc* job, DeviceScene* scene) {
+             int tile_end, float4* image, JobDesc* job, DeviceScene* scene, float* record = nullptr,
+             const float* dloss = nullptr) {
   static_assert(sizeof(ymrt_render_setting) == sizeof(RenderSetting), "render setting layout");
   if (!sc || !setting || !image) return ctx->fail(YMRT_ERR_INVALID, "null scene, setting or output");
   if (sc->ctx != ctx) return ctx->fail(YMRT_ERR_INVALID, "scene belongs to another context");
@@ -602,6 +607,9 @@ int make_job(ymrt_context* ctx, ymrt_scene* sc, const ymrt_render_setting* setti
   job->tiles_x = tiles_x;
   job->tile_begin = t_begin;
   job->path_count = (unsigned long long)(t_end - t_begin) * kTilePixels * job->spp;
+  if (job->path_count > 0xFFFFFFFFull) return ctx->fail(YMRT_ERR_INVALID, "a render of more than 2^32 paths");
+  job->path_radiance = reinterpret_cast<float4*>(record);
+  job->dloss = reinterpret_cast<const float4*>(dloss);
   return YMRT_OK;
 }
 
@@ -663,7 +671,8 @@ int run_batch(ymrt_context* ctx, const BatchMemory& M, std::vector<JobDesc>& job
     const std::vector<uintptr_t> key = {
         (uintptr_t)M.pool[0].ray_o, (uintptr_t)M.pool[1].ray_o, (uintptr_t)M.hits.bary_t, (uintptr_t)M.ctl,
         (uintptr_t)M.jobs, (uintptr_t)M.counters, (uintptr_t)jobs.size(), (uintptr_t)o.volumes,
-        (uintptr_t)o.sort_hits, (uintptr_t)o.defer_shadows, (uintptr_t)o.shadow_queue.o, M.capacity};
+        (uintptr_t)o.sort_hits, (uintptr_t)o.defer_shadows, (uintptr_t)o.shadow_queue.o, M.capacity,
+        (uintptr_t)o.adjoint, (uintptr_t)o.grads, o.grad_materials};
     if (ctx->graph_key != key) {
       ctx->drop_graph();
       cudaGraph_t g = nullptr;
@@ -787,8 +796,11 @@ int batch_options(ymrt_context* ctx, const std::vector<JobDesc>& jobs, WaveOptio
     opt->volumes = opt->volumes || j.setting.enable_volume_scattering;
     clamp = clamp || j.setting.enable_indirect_clamp;
   }
+  bool record = false;
+  for (const JobDesc& j : jobs) record = record || j.path_radiance != nullptr;
   opt->sort_hits = ctx->sort_hits;
-  opt->defer_shadows = ctx->defer_shadows && !opt->volumes && !clamp;
+  // a recorded path's radiance must include its shadow rays: trace them inline
+  opt->defer_shadows = ctx->defer_shadows && !opt->volumes && !clamp && !record;
   if (opt->defer_shadows) {
     int rc = ctx->ensure_shadow_queue();
     if (rc != YMRT_OK) return rc;
@@ -869,7 +881,7 @@ int ymrt_render_batch(ymrt_context* ctx, const ymrt_job* jobs_in, int n_jobs, ym
   for (int k = 0; k < n_jobs; ++k) {
     const ymrt_job& in = jobs_in[k];
     int rc = make_job(ctx, in.scene, &in.setting, in.frame_index, in.tile_begin, in.tile_end,
-                      reinterpret_cast<float4*>(in.out_rgba_device), &all[k], &scenes[k]);
+                      reinterpret_cast<float4*>(in.out_rgba_device), &all[k], &scenes[k], in.path_radiance_device);
     if (rc != YMRT_OK) return rc;
     keys[k] = in.scene;
   }
@@ -922,6 +934,98 @@ int ymrt_render_batch(ymrt_context* ctx, const ymrt_job* jobs_in, int n_jobs, ym
   return finish_batch(ctx, total, stats);
 }
 
+unsigned long long ymrt_job_path_count(const ymrt_job* job) {
+  if (!job || !job->scene) return 0;
+  const ymrt_scene* sc = job->scene;
+  const uint32_t tiles_x = (sc->width + kTileRes - 1) / kTileRes, tiles_y = (sc->height + kTileRes - 1) / kTileRes;
+  const uint32_t total = tiles_x * tiles_y;
+  const uint32_t t_end = job->tile_end <= 0 ? total : std::min<uint32_t>((uint32_t)job->tile_end, total);
+  const uint32_t t_begin = std::min<uint32_t>((uint32_t)std::max(job->tile_begin, 0), t_end);
+  return (unsigned long long)(t_end - t_begin) * kTilePixels * (uint32_t)std::max(job->setting.ssp, 1);
+}
+
+int ymrt_render_backward(ymrt_context* ctx, const ymrt_job* jobs_in, int n_jobs, float* grads_device,
+                         uint32_t n_materials, ymrt_stats* stats) {
+  if (!ctx || !jobs_in || n_jobs <= 0 || !grads_device || n_materials == 0) return YMRT_ERR_INVALID;
+  cudaSetDevice(ctx->device);
+  cudaStream_t st = ctx->stream;
+  cudaError_t e;
+  std::vector<JobDesc> jobs((size_t)n_jobs);
+  std::vector<DeviceScene> scenes((size_t)n_jobs);
+  std::vector<const void*> keys((size_t)n_jobs);
+  for (int k = 0; k < n_jobs; ++k) {
+    const ymrt_job& in = jobs_in[k];
+    if (!in.path_radiance_device || !in.dloss_device)
+      return ctx->fail(YMRT_ERR_INVALID, "backward: every job needs its recorded path radiance and dLoss/dImage");
+    if (in.setting.enable_volume_scattering)
+      return ctx->fail(YMRT_ERR_UNSUPPORTED, "backward: volume scattering is not differentiated");
+    if (in.setting.enable_indirect_clamp)
+      return ctx->fail(YMRT_ERR_UNSUPPORTED, "backward: the indirect clamp is not differentiated");
+    int rc = make_job(ctx, in.scene, &in.setting, in.frame_index, in.tile_begin, in.tile_end,
+                      reinterpret_cast<float4*>(in.out_rgba_device), &jobs[k], &scenes[k], in.path_radiance_device,
+                      in.dloss_device);
+    if (rc != YMRT_OK) return rc;
+    keys[k] = in.scene;
+  }
+  const std::vector<DeviceScene> slots = assign_slots(jobs, scenes, keys);
+  if (slots.size() > kMaxSceneSlots) return ctx->fail(YMRT_ERR_INVALID, "backward: too many distinct scenes in one call");
+  BatchMemory M;
+  int rc = context_memory(ctx, jobs.size(), &M);
+  if (rc != YMRT_OK) return rc;
+  WaveOptions opt;
+  opt.adjoint = true;
+  opt.grads = grads_device;
+  opt.grad_materials = n_materials;
+  if ((e = upload_constants(slots.data(), (uint32_t)slots.size(), ctx->primes.data(), ctx->prime_sums.data(), st)) !=
+      cudaSuccess)
+    return ctx->cuda_fail(e, "uploading constants");
+  cudaMemsetAsync(grads_device, 0, sizeof(float) * kGradParams * n_materials, st);
+  BatchResult r;
+  if ((rc = run_batch(ctx, M, jobs, opt, ctx->profiling, ctx->graph_loop, &r)) != YMRT_OK) return rc;
+  if ((e = cudaMemcpyAsync(ctx->counters_host, M.counters, sizeof(WaveCounters), cudaMemcpyDeviceToHost, st)) !=
+      cudaSuccess)
+    return ctx->cuda_fail(e, "reading counters");
+  if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return ctx->cuda_fail(e, "backward");
+  return finish_batch(ctx, r, stats);
+}
+
+int ymrt_scene_set_material_params(ymrt_scene* scene, uint32_t first, uint32_t count, const float* params) {
+  if (!scene || !params) return YMRT_ERR_INVALID;
+  if ((size_t)first + count > scene->materials.size())
+    return scene->ctx->fail(YMRT_ERR_INVALID, "material range out of bounds");
+  for (uint32_t k = 0; k < count; ++k) {
+    Material& m = scene->materials[first + k];
+    if (m.material_type != kDefaultMtl) continue;
+    const float* q = params + 4 * k;
+    m.default_mtl.diffuse_albedo = vec3(q[0], q[1], q[2]);
+    m.default_mtl.alpha_x = q[3];
+    m.default_mtl.alpha_y = q[3];
+  }
+  cudaSetDevice(scene->ctx->device);
+  cudaError_t e = cudaMemcpyAsync(const_cast<Material*>(scene->dev.materials) + first, scene->materials.data() + first,
+                                  sizeof(Material) * count, cudaMemcpyHostToDevice, scene->ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(scene->ctx->stream);
+  if (e != cudaSuccess) return scene->ctx->cuda_fail(e, "updating materials");
+  return YMRT_OK;
+}
+
+int ymrt_scene_get_material_params(const ymrt_scene* scene, uint32_t first, uint32_t count, float* params) {
+  if (!scene || !params || (size_t)first + count > scene->materials.size()) return YMRT_ERR_INVALID;
+  for (uint32_t k = 0; k < count; ++k) {
+    const Material& m = scene->materials[first + k];
+    float* q = params + 4 * k;
+    if (m.material_type != kDefaultMtl) {
+      q[0] = q[1] = q[2] = q[3] = 0.0f;
+      continue;
+    }
+    q[0] = m.default_mtl.diffuse_albedo.x;
+    q[1] = m.default_mtl.diffuse_albedo.y;
+    q[2] = m.default_mtl.diffuse_albedo.z;
+    q[3] = m.default_mtl.alpha_x;
+  }
+  return YMRT_OK;
+}
+
 int ymrt_render_forward(ymrt_scene* sc, const ymrt_render_setting* setting, int frame_index, float* out_rgba,
                         int out_on_device, ymrt_stats* stats) {
   return ymrt_render_tiles(sc, setting, frame_index, 0, 0, out_rgba, out_on_device, stats);
@@ -962,12 +1066,13 @@ void* g_noalloc_addr[128] = {};
 constexpr size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 
 // Bytes one path slot needs across both path pools and the hit pool.
-constexpr size_t kPoolSlotBytes = 4 * sizeof(float4) + sizeof(uint4) + 2 * sizeof(uint2) + sizeof(RayTransfer) + 1;
+constexpr size_t kPoolSlotBytes =
+    4 * sizeof(float4) + sizeof(uint4) + 2 * sizeof(uint2) + sizeof(RayTransfer) + sizeof(uint32_t) + 1;
 constexpr size_t kHitSlotBytes = sizeof(float4) + sizeof(uint4) + kMaxNearby * sizeof(uint4) + sizeof(uint32_t) + 1;
 
 uint32_t noalloc_capacity() {
   // counters, one job, and the alignment slack of the carved arrays
-  const size_t fixed = align256(sizeof(WaveCounters)) + align256(sizeof(WaveControl)) + align256(sizeof(JobDesc)) + 18 * 256;
+  const size_t fixed = align256(sizeof(WaveCounters)) + align256(sizeof(WaveControl)) + align256(sizeof(JobDesc)) + 20 * 256;
   return (uint32_t)((kNoAllocScratchBytes - fixed) / (2 * kPoolSlotBytes + kHitSlotBytes));
 }
 
@@ -995,6 +1100,7 @@ size_t carve(unsigned char* base, uint32_t n, PathPool pools[2], HitPool* hits, 
     P.pixel_flags = reinterpret_cast<uint2*>(take(n * sizeof(uint2)));
     P.last_hit = reinterpret_cast<uint2*>(take(n * sizeof(uint2)));
     P.transfer = reinterpret_cast<RayTransfer*>(take(n * sizeof(RayTransfer)));
+    P.path_id = reinterpret_cast<uint32_t*>(take(n * sizeof(uint32_t)));
     P.transfer_count = reinterpret_cast<uint8_t*>(take(n));
     P.capacity = n;
   }

@@ -34,7 +34,9 @@ namespace cg = cooperative_groups;
 // ---------------------------------------------------------------- paths ---
 
 __device__ __forceinline__ void store_path(const PathPool& P, uint32_t i, vec3 o, vec3 d, vec3 tp, vec3 rad, uint32_t pixel,
-                                           uint32_t flags, uint32_t last_inst, uint32_t last_tri, const PathSampler& hs) {
+                                           uint32_t flags, uint32_t last_inst, uint32_t last_tri, const PathSampler& hs,
+                                           uint32_t path_id) {
+  P.path_id[i] = path_id;
   P.ray_o[i] = make_float4(o.x, o.y, o.z, 0.0f);
   P.ray_d[i] = make_float4(d.x, d.y, d.z, 0.0f);
   P.throughput[i] = make_float4(tp.x, tp.y, tp.z, 0.0f);
@@ -49,6 +51,19 @@ __device__ __forceinline__ void store_path(const PathPool& P, uint32_t i, vec3 o
 // channel atomically.
 __device__ __forceinline__ void accumulate_pixel(float4* image, uint32_t pixel, vec3 light, float inv_spp) {
   atomicAdd(image + pixel, make_float4(light.x * inv_spp, light.y * inv_spp, light.z * inv_spp, inv_spp));
+}
+
+// A path ends: its radiance into its pixel, and (differentiable renders)
+// into the job's per-path record.
+__device__ __forceinline__ void finish_path(const JobDesc& J, uint32_t pixel, uint32_t path_id, vec3 rad,
+                                            float inv_spp) {
+  accumulate_pixel(J.image, pixel, rad, inv_spp);
+  if (J.path_radiance) J.path_radiance[path_id] = make_float4(rad.x, rad.y, rad.z, 0.0f);
+}
+
+template <bool kAdj>
+__device__ __forceinline__ void end_path(const JobDesc& J, uint32_t pixel, uint32_t path_id, vec3 rad, float inv_spp) {
+  if (!kAdj) finish_path(J, pixel, path_id, rad, inv_spp);
 }
 
 // Warp-aggregated slot allocation in the output pool.
@@ -152,7 +167,7 @@ __device__ __forceinline__ void generate_path(const PathPool& P, uint32_t base, 
   const float w = h * cam.aspect_ratio;
   const vec3 dir = normalize(-cam.w + (ndc_x - 0.5f) * w * cam.u + (ndc_y - 0.5f) * h * cam.v);
   store_path(P, i, cam.position, dir, vec3(1.0f), vec3(0.0f), pixel, flags_pack(1, true, true, job), kEmpty, kEmpty,
-             hs);
+             hs, local_path);
   if (cam.transfer.record_count > 0) P.transfer[i] = cam.transfer;
   P.transfer_count[i] = (uint8_t)cam.transfer.record_count;
 }
@@ -204,7 +219,7 @@ __global__ void __launch_bounds__(256) k_sort_hits(const WaveControl* __restrict
       rad += indirect_clamp(J.setting, vec3(t4.x, t4.y, t4.z) * background(vec3(d4.x, d4.y, d4.z)),
                             (int)(pf.y & kFlagDepthMask));
     }
-    accumulate_pixel(J.image, pf.x, rad, 1.0f / gmax(J.setting.ssp, 1));
+    finish_path(J, pf.x, P.path_id[i], rad, 1.0f / gmax(J.setting.ssp, 1));
     b = kBucketNone;
   }
   const bool has = b != kBucketNone;
@@ -507,6 +522,67 @@ __device__ __forceinline__ vec3 surface_shadow_tr(const DeviceScene& S, Traversa
   return trace_tr(c.slot, st, so, normalize(ldir), maxd, c.inst, c.tri, srt, hs, errors, tests, nodes);
 }
 
+// ------------------------------------------------- path-replay adjoint ---
+//
+// Gradients of an image loss with respect to each material's diffuse albedo
+// (rgb) and roughness (alpha_x and alpha_y together), by path replay: the
+// adjoint pass re-traces every path with its own sampler (same directions as
+// the forward pass, which recorded each path's radiance), and at every
+// surface vertex adds, for each parameter p of the vertex's material,
+//   dLoss/dI . ( tp * dNEE/dp  +  L_after * (df/dp) / f )
+// where L_after is the radiance the path gathers after the vertex (its
+// recorded total minus what it gathered so far). Sampling and MIS weights are
+// held fixed (detached), so only BSDF values are differentiated; df/dp is the
+// central difference of the closed-form layered BSDF at the vertex's fixed
+// directions.
+
+constexpr int kMaxGradMaterials = 64;     // materials with shared-memory gradient slots per block
+constexpr float kParamStep = 1e-3f;       // central-difference step of df/dp
+
+struct AdjCtx {
+  const DefaultMtl* mtl;                  // the vertex's material
+  int hit_back;
+  vec3 ray_dir;
+  float ray_ior, ex_ior;
+  vec3 weight;                            // dLoss/dI (per path) * throughput: the weight of this vertex's NEE
+  float g[kGradParams];                   // accumulated dLoss/dp
+};
+
+__device__ __forceinline__ void perturb(DefaultMtl& m, int k, float h) {
+  if (k < 3) {
+    m.diffuse_albedo[k] += h;
+  } else {
+    m.alpha_x += h;
+    m.alpha_y += h;
+  }
+}
+
+// df/dp_k at fixed (wo, wi) in the frame of B (central difference).
+__device__ __noinline__ vec3 dfdparam(const AdjCtx& a, const LayeredBsdf& B, int k, vec3 wo, vec3 wi) {
+  DefaultMtl mp = *a.mtl, mm = *a.mtl;
+  perturb(mp, k, kParamStep);
+  perturb(mm, k, -kParamStep);
+  LayeredBsdf Bp = B, Bm = B;
+  init_layered_lobes(Bp, mp, a.ray_dir, a.hit_back, a.ray_ior, a.ex_ior);
+  init_layered_lobes(Bm, mm, a.ray_dir, a.hit_back, a.ray_ior, a.ex_ior);
+  float pdf;
+  const vec3 fp = bsdf_eval(Bp, wo, wi, &pdf), fm = bsdf_eval(Bm, wo, wi, &pdf);
+  return (fp - fm) * (0.5f / kParamStep);
+}
+
+// Adds weight . (c * (df/dp_k) / f) for every parameter, f = the BSDF at (wo, wi).
+__device__ __forceinline__ void add_relative_grads(AdjCtx* a, const LayeredBsdf& B, vec3 wo, vec3 wi, vec3 weight, vec3 c) {
+  float pdf;
+  const vec3 f = bsdf_eval(B, wo, wi, &pdf);
+  for (int k = 0; k < kGradParams; ++k) {
+    const vec3 d = dfdparam(*a, B, k, wo, wi);
+    float acc = 0.0f;
+    for (int ch = 0; ch < 3; ++ch)
+      if (f[ch] > 0.0f) acc += weight[ch] * c[ch] * d[ch] / f[ch];
+    a->g[k] += acc;
+  }
+}
+
 // Where a surface shadow ray goes when shadow rays are deferred: the queue
 // k_connect traces, the pixel it lights and the path's weight on it
 // (throughput / spp).
@@ -546,7 +622,8 @@ __device__ __forceinline__ void nee_shadow_ray(const DeviceScene& S, TraversalSt
                                                const ShadowEmit& em, vec3 so, vec3 ldir, float maxd, bool tb,
                                                float mis, vec3 fc, vec3 Lc, float mul, float div, vec3* direct,
                                                PathSampler& hs, uint32_t* shadow_rays, uint32_t* tests,
-                                               uint32_t* nodes, uint32_t* errors) {
+                                               uint32_t* nodes, uint32_t* errors, AdjCtx* adj = nullptr,
+                                               const LayeredBsdf* B = nullptr) {
   ++*shadow_rays;
   if (kDefer) {
     emit_shadow_ray(em, so, normalize(ldir), maxd, ((mis * vec3(1.0f) * fc * Lc) * mul) / div);
@@ -555,6 +632,11 @@ __device__ __forceinline__ void nee_shadow_ray(const DeviceScene& S, TraversalSt
   if (!trace_occluded(c.slot, st, so, normalize(ldir), maxd, tests, nodes)) {
     const vec3 tr = surface_shadow_tr<kVol>(S, st, c, so, ldir, maxd, tb, hs, errors, tests, nodes);
     *direct += mis * tr * fc * Lc;
+    if (adj) {
+      // d(direct)/dp = mis * tr * fc * (df/dp)/f * Lc, scaled like the estimator
+      const vec3 wo = B->to_local(-c.ray_dir), wi = B->to_local(ldir);
+      add_relative_grads(adj, *B, wo, wi, adj->weight * (mul / div), mis * tr * fc * Lc);
+    }
   }
 }
 
@@ -563,7 +645,7 @@ template <bool kVol, bool kDefer>
 __device__ __forceinline__ vec3 eval_shape_light(const DeviceScene& S, TraversalStack& st, const LayeredBsdf& B,
                                                  const SurfaceNee& c, const ShadowEmit& em, PathSampler& hs,
                                                  uint32_t* shadow_rays, uint32_t* tests, uint32_t* nodes,
-                                                 uint32_t* errors) {
+                                                 uint32_t* errors, AdjCtx* adj = nullptr) {
   if (S.shape_light_count == 0) return vec3(0.0f);
   vec3 direct(0.0f);
   const vec3 wo = B.to_local(-c.ray_dir);
@@ -588,7 +670,7 @@ __device__ __forceinline__ vec3 eval_shape_light(const DeviceScene& S, Traversal
       if (!invalid)
         nee_shadow_ray<kVol, kDefer>(S, st, c, em, so, ldir, maxd, tb, power_heuristic(lpdf, wpdf),
                                      vmin(f, vec3(kMaxColorClamp)), vmin(Li, vec3(kMaxColorClamp)),
-                                     safe_rcp(select_pdf), 1.0f, &direct, hs, shadow_rays, tests, nodes, errors);
+                                     safe_rcp(select_pdf), 1.0f, &direct, hs, shadow_rays, tests, nodes, errors, adj, &B);
     }
   }
   {
@@ -609,7 +691,7 @@ __device__ __forceinline__ vec3 eval_shape_light(const DeviceScene& S, Traversal
         if (!invalid)
           nee_shadow_ray<kVol, kDefer>(S, st, c, em, so, ldir, maxd, tb, power_heuristic(bpdf, wpdf),
                                        vmin(bw, vec3(kMaxColorClamp)), vmin(Li, vec3(kMaxColorClamp)),
-                                       safe_rcp(select_pdf), 1.0f, &direct, hs, shadow_rays, tests, nodes, errors);
+                                       safe_rcp(select_pdf), 1.0f, &direct, hs, shadow_rays, tests, nodes, errors, adj, &B);
       }
     }
   }
@@ -621,7 +703,7 @@ template <bool kVol, bool kDefer>
 __device__ __forceinline__ vec3 eval_distant_light(const DeviceScene& S, TraversalStack& st, const LayeredBsdf& B,
                                                    const SurfaceNee& c, const ShadowEmit& em, PathSampler& hs,
                                                    uint32_t* shadow_rays, uint32_t* tests, uint32_t* nodes,
-                                                   uint32_t* errors) {
+                                                   uint32_t* errors, AdjCtx* adj = nullptr) {
   if (S.distant_light_count == 0) return vec3(0.0f);
   vec3 direct(0.0f);
   const vec3 wo = B.to_local(-c.ray_dir);
@@ -644,7 +726,7 @@ __device__ __forceinline__ vec3 eval_distant_light(const DeviceScene& S, Travers
       if (!invalid)
         nee_shadow_ray<kVol, kDefer>(S, st, c, em, so, ldir, kTMax, tb, power_heuristic(lpdf, wpdf),
                                      vmin(f, vec3(kMaxColorClamp)), vmin(Li, vec3(kMaxColorClamp)), 1.0f,
-                                     select_pdf, &direct, hs, shadow_rays, tests, nodes, errors);
+                                     select_pdf, &direct, hs, shadow_rays, tests, nodes, errors, adj, &B);
     }
   }
   {
@@ -663,7 +745,7 @@ __device__ __forceinline__ vec3 eval_distant_light(const DeviceScene& S, Travers
         if (!invalid)
           nee_shadow_ray<kVol, kDefer>(S, st, c, em, so, ldir, kTMax, tb, power_heuristic(bpdf, wpdf),
                                        vmin(bw, vec3(kMaxColorClamp)), vmin(Li, vec3(kMaxColorClamp)), 1.0f,
-                                       select_pdf, &direct, hs, shadow_rays, tests, nodes, errors);
+                                       select_pdf, &direct, hs, shadow_rays, tests, nodes, errors, adj, &B);
       }
     }
   }
@@ -773,11 +855,26 @@ __device__ __noinline__ vec3 eval_volume_lights(uint32_t slot, TraversalStack& s
 // kDefer (surfaces only, no indirect clamp): next-event shadow rays are queued
 // for k_connect instead of traced here, which keeps traversal out of this
 // kernel.
-template <bool kVol, bool kDefer>
+//
+// kAdj (surfaces, inline shadow rays): the path-replay adjoint pass. Paths
+// are shaded exactly as in the forward pass, nothing is added to the image,
+// and each material vertex adds its terms of dLoss/dParam (see AdjCtx) to
+// `grads` (per-block sums in shared memory, then one atomic per touched slot).
+template <bool kVol, bool kDefer, bool kAdj = false>
 __global__ void __launch_bounds__(kTraceBlock) k_shade(PathPool P, const WaveControl* __restrict__ ctl, HitPool H,
                                                        PathPool Q, const JobDesc* __restrict__ jobs,
-                                                       WaveCounters* counters, ShadowQueue shadow_q) {
+                                                       WaveCounters* counters, ShadowQueue shadow_q,
+                                                       float* grads = nullptr, uint32_t grad_materials = 0) {
   static_assert(!(kVol && kDefer), "volume transmittance needs the path's sampler: shadow rays are traced inline");
+  static_assert(!(kAdj && (kVol || kDefer)), "the adjoint pass shades surfaces with inline shadow rays");
+  float* s_grad = nullptr;
+  const uint32_t n_slots = min(grad_materials, (uint32_t)kMaxGradMaterials) * kGradParams;
+  if constexpr (kAdj) {
+    __shared__ float s_grad_buf[kMaxGradMaterials * kGradParams];
+    s_grad = s_grad_buf;
+    for (uint32_t k = threadIdx.x; k < n_slots; k += blockDim.x) s_grad[k] = 0.0f;
+    __syncthreads();
+  }
   const bool listed = H.order != nullptr;
   const uint32_t count = listed ? min(ctl->count, counters->hit_count) : ctl->count;
   uint32_t shadow_rays = 0, tests = 0, nodes = 0;
@@ -806,7 +903,6 @@ __global__ void __launch_bounds__(kTraceBlock) k_shade(PathPool P, const WaveCon
     const uint32_t slot = J.scene_slot;
     const DeviceScene& S = c_scenes[slot];
     const RenderSetting& rs = J.setting;
-    float4* image = J.image;
     uint32_t* errors = &counters->errors;
     const float4 o4 = P.ray_o[i], d4 = P.ray_d[i], t4 = P.throughput[i], r4 = P.radiance[i];
     const vec3 rd(d4.x, d4.y, d4.z);
@@ -842,7 +938,7 @@ __global__ void __launch_bounds__(kTraceBlock) k_shade(PathPool P, const WaveCon
       // a miss (Ray_trace_path_tracing, src/Shading.cu:1855-1864): the
       // background when the environment light is on, then the path ends
       if (rs.enable_env_light) rad += indirect_clamp(rs, tp * background(rd), depth);
-      accumulate_pixel(image, pf.x, rad, inv_spp);
+      end_path<kAdj>(J, pf.x, P.path_id[i], rad, inv_spp);
     } else if (volume_hit) {
       // Ray_shading_path_tracing volume branch (src/Shading.cu:2066-2126).
       float vw[kMaxBoundaryRecord], gs[kMaxBoundaryRecord];
@@ -886,7 +982,7 @@ __global__ void __launch_bounds__(kTraceBlock) k_shade(PathPool P, const WaveCon
           alive = true;
         }
       }
-      if (terminate) accumulate_pixel(image, pf.x, rad, inv_spp);
+      if (terminate) end_path<kAdj>(J, pf.x, P.path_id[i], rad, inv_spp);
     } else {
       NearbyHit nb[kMaxNearby];
       const int n_nb = (int)(ids.w & 0xFFu);
@@ -902,7 +998,7 @@ __global__ void __launch_bounds__(kTraceBlock) k_shade(PathPool P, const WaveCon
       const Instance inst = S.instances[inst_idx];
       bool done = false;
       if (!(inst.material_idx < S.material_count)) {
-        accumulate_pixel(image, pf.x, rad, inv_spp);
+        end_path<kAdj>(J, pf.x, P.path_id[i], rad, inv_spp);
         done = true;
       }
       const Material& mat = S.materials[done ? 0 : inst.material_idx];
@@ -931,7 +1027,7 @@ __global__ void __launch_bounds__(kTraceBlock) k_shade(PathPool P, const WaveCon
       }
       if (!done && mat.material_type == kLightMtl) {
         if (never_scatter) rad += indirect_clamp(rs, tp * mat.light_mtl.light_color * mat.light_mtl.intensity, depth);
-        accumulate_pixel(image, pf.x, rad, inv_spp);
+        end_path<kAdj>(J, pf.x, P.path_id[i], rad, inv_spp);
         done = true;
       }
       if (!done) {
@@ -941,13 +1037,30 @@ __global__ void __launch_bounds__(kTraceBlock) k_shade(PathPool P, const WaveCon
         const SurfaceNee nc{rd, sp.p, sp.p_err, sp.ng, inst_idx, tri, &rt, nb, n_nb, rs.enable_volume_scattering != 0,
                             slot};
         const ShadowEmit em{shadow_q, &counters->shadow_count, errors, pf.x, job, tp * inv_spp};
+        AdjCtx adj_ctx;
+        AdjCtx* adj = nullptr;
+        vec3 delta(0.0f), l_total(0.0f);
+        if constexpr (kAdj) {
+          const float4 dl = J.dloss[pf.x];
+          const float4 lt = J.path_radiance[P.path_id[i]];
+          delta = vec3(dl.x, dl.y, dl.z) * inv_spp;  // dLoss/d(this path's radiance)
+          l_total = vec3(lt.x, lt.y, lt.z);
+          adj_ctx.mtl = &mat.default_mtl;
+          adj_ctx.hit_back = hit_back;
+          adj_ctx.ray_dir = rd;
+          adj_ctx.ray_ior = ray_ior(rt);
+          adj_ctx.ex_ior = ex_ior(rt, inst_idx);
+          adj_ctx.weight = delta * tp;
+          for (int k = 0; k < kGradParams; ++k) adj_ctx.g[k] = 0.0f;
+          adj = &adj_ctx;
+        }
         if (rs.enable_distant_light)
           rad += indirect_clamp(
-              rs, tp * eval_distant_light<kVol, kDefer>(S, st, B, nc, em, hs, &shadow_rays, &tests, &nodes, errors),
+              rs, tp * eval_distant_light<kVol, kDefer>(S, st, B, nc, em, hs, &shadow_rays, &tests, &nodes, errors, adj),
               depth);
         if (rs.enable_shape_light)
           rad += indirect_clamp(
-              rs, tp * eval_shape_light<kVol, kDefer>(S, st, B, nc, em, hs, &shadow_rays, &tests, &nodes, errors),
+              rs, tp * eval_shape_light<kVol, kDefer>(S, st, B, nc, em, hs, &shadow_rays, &tests, &nodes, errors, adj),
               depth);
         const vec3 wo = B.to_local(-rd);
         vec3 w, wi;
@@ -955,8 +1068,18 @@ __global__ void __launch_bounds__(kTraceBlock) k_shade(PathPool P, const WaveCon
         float u0, u1, u2;
         sample3d(hs, S, &u0, &u1, &u2);
         const bool valid = bsdf_sample(B, wo, &w, &wi, &pdf, u0, u1, u2);
+        if constexpr (kAdj) {
+          // the radiance gathered after this vertex, through the sampled BSDF value
+          if (valid) add_relative_grads(&adj_ctx, B, wo, wi, delta, l_total - rad);
+          const uint32_t m = inst.material_idx;
+          for (int k = 0; k < kGradParams; ++k) {
+            if (adj_ctx.g[k] == 0.0f) continue;
+            if (m * kGradParams + k < n_slots) atomicAdd(&s_grad[m * kGradParams + k], adj_ctx.g[k]);
+            else if (m < grad_materials) atomicAdd(&grads[m * kGradParams + k], adj_ctx.g[k]);
+          }
+        }
         if (!valid) {
-          accumulate_pixel(image, pf.x, rad, inv_spp);
+          end_path<kAdj>(J, pf.x, P.path_id[i], rad, inv_spp);
         } else {
           tp *= w;
           float rr = gmax(tp.x, gmax(tp.y, tp.z));
@@ -988,7 +1111,7 @@ __global__ void __launch_bounds__(kTraceBlock) k_shade(PathPool P, const WaveCon
               }
             }
           }
-          if (terminate) accumulate_pixel(image, pf.x, rad, inv_spp);
+          if (terminate) end_path<kAdj>(J, pf.x, P.path_id[i], rad, inv_spp);
         }
       }
     }
@@ -997,7 +1120,7 @@ __global__ void __launch_bounds__(kTraceBlock) k_shade(PathPool P, const WaveCon
   const uint32_t slot = warp_append(&counters->next_count, alive);
   if (alive) {
     if (slot < Q.capacity) {
-      store_path(Q, slot, new_o, new_d, tp, rad, pf.x, new_flags, new_last_inst, new_last_tri, hs);
+      store_path(Q, slot, new_o, new_d, tp, rad, pf.x, new_flags, new_last_inst, new_last_tri, hs, P.path_id[i]);
       Q.transfer_count[slot] = (uint8_t)rt.record_count;
       if (rt.record_count > 0) Q.transfer[slot] = rt;
     } else {
@@ -1016,6 +1139,11 @@ __global__ void __launch_bounds__(kTraceBlock) k_shade(PathPool P, const WaveCon
     if (s_sum) atomicAdd(&counters->shadow_rays, (unsigned long long)s_sum);
     if (t_sum) atomicAdd(&counters->shadow_tri_tests, (unsigned long long)t_sum);
     if (n_sum) atomicAdd(&counters->shadow_node_visits, (unsigned long long)n_sum);
+  }
+  if constexpr (kAdj) {
+    __syncthreads();
+    for (uint32_t k = threadIdx.x; k < n_slots; k += blockDim.x)
+      if (s_grad[k] != 0.0f) atomicAdd(&grads[k], s_grad[k]);
   }
 }
 
@@ -1219,9 +1347,11 @@ uint32_t launch_wave(const PathPool& A, const PathPool& B, const HitPool& H, Wav
                      cudaStream_t stream, unsigned long long graph_condition) {
   prepare_persistent_grids();
   const PersistentGrids& g = g_grids;
-  const ShadowQueue* defer = (!opt.volumes && opt.defer_shadows) ? &opt.shadow_queue : nullptr;
+  const bool adjoint = opt.adjoint && !opt.volumes;
+  const ShadowQueue* defer = (!opt.volumes && opt.defer_shadows && !adjoint) ? &opt.shadow_queue : nullptr;
+  const bool sort_hits = opt.sort_hits && !adjoint;
   HitPool Hs = H;
-  if (!opt.sort_hits) Hs.order = nullptr;
+  if (!sort_hits) Hs.order = nullptr;
   const ShadowQueue none{};
   // The per-path kernels get one thread per pool slot (blocks past the
   // wave's count return at once), so the hardware block scheduler balances
@@ -1235,9 +1365,12 @@ uint32_t launch_wave(const PathPool& A, const PathPool& B, const HitPool& H, Wav
   if (opt.volumes) k_extend<true><<<blocks_trace, kTraceBlock, 0, stream>>>(A, ctl, Hs, jobs, counters);
   else k_extend<false><<<blocks_trace, kTraceBlock, 0, stream>>>(A, ctl, Hs, jobs, counters);
   if (ev) cudaEventRecord(ev[2], stream);
-  if (opt.sort_hits) k_sort_hits<<<blocks_256, 256, 0, stream>>>(ctl, Hs, A, jobs, counters);
+  if (sort_hits) k_sort_hits<<<blocks_256, 256, 0, stream>>>(ctl, Hs, A, jobs, counters);
   if (ev) cudaEventRecord(ev[3], stream);
-  if (opt.volumes)
+  if (adjoint)
+    k_shade<false, false, true><<<blocks_trace, kTraceBlock, 0, stream>>>(A, ctl, Hs, B, jobs, counters, none,
+                                                                         opt.grads, opt.grad_materials);
+  else if (opt.volumes)
     k_shade<true, false><<<blocks_trace, kTraceBlock, 0, stream>>>(A, ctl, Hs, B, jobs, counters, none);
   else if (defer)
     k_shade<false, true><<<blocks_trace, kTraceBlock, 0, stream>>>(A, ctl, Hs, B, jobs, counters, *defer);
@@ -1247,7 +1380,7 @@ uint32_t launch_wave(const PathPool& A, const PathPool& B, const HitPool& H, Wav
   if (defer) k_connect<<<g.connect, kTraceBlock, 0, stream>>>(*defer, jobs, counters);
   if (ev) cudaEventRecord(ev[5], stream);
   k_finish<<<1, 32, 0, stream>>>(ctl, counters, graph_condition);
-  return 5u + (opt.sort_hits ? 1u : 0u) + (defer ? 1u : 0u);
+  return 5u + (sort_hits ? 1u : 0u) + (defer ? 1u : 0u);
 }
 
 void launch_accumulate(const float4* noise, float4* acc, uint32_t n, int frame_index, cudaStream_t stream) {

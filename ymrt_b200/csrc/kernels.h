@@ -44,6 +44,7 @@ struct PathPool {
   uint4* sampler;       // Halton sample index (lo, hi), dimension
   uint8_t* transfer_count;  // records in the nested-media stack
   RayTransfer* transfer;    // nested-media stack (read only when count > 0)
+  uint32_t* path_id;        // the path's index within its job (for recording and replay)
   uint32_t capacity;
 };
 
@@ -71,6 +72,11 @@ struct JobDesc {
   uint32_t tile_begin;            // first tile rendered
   unsigned long long path_begin;  // first path of this job in the batch's path space
   unsigned long long path_count;  // tiles rendered * 256 * spp
+  // differentiable rendering (null when unused)
+  float4* path_radiance;          // forward: each path's radiance, by path index
+  const float4* dloss;            // adjoint: dLoss/dImage per pixel
+  float* grads;                   // adjoint: dLoss/dParam, 4 per material (albedo rgb, roughness)
+  uint32_t grad_materials;        // materials with gradient slots
 };
 
 // Deferred next-event shadow rays of one wave (traced by k_connect).
@@ -137,12 +143,17 @@ struct WaveControl {
   uint32_t reserved;
 };
 
+constexpr int kGradParams = 4;  // differentiated parameters per material: albedo r, g, b, roughness
+
 struct WaveOptions {
   uint32_t capacity = 0;       // path slots per pool (sizes the grids)
   bool volumes = false;        // volume scattering kernels
   bool sort_hits = true;       // shade hits listed by shading bucket
   bool defer_shadows = false;  // queue surface shadow rays for k_connect (ignored with volumes)
   ShadowQueue shadow_queue{};
+  bool adjoint = false;        // path-replay adjoint pass (surfaces; no sorting, no deferral)
+  float* grads = nullptr;      // adjoint: dLoss/dParam, kGradParams per material
+  uint32_t grad_materials = 0;
 };
 uint32_t launch_wave(const PathPool& A, const PathPool& B, const HitPool& H, WaveControl* ctl, const JobDesc* jobs,
                      uint32_t n_jobs, WaveCounters* counters, const WaveOptions& opt, cudaEvent_t* ev,

@@ -398,17 +398,54 @@ def volumetric_scene(seed: int = 0) -> Scene:
     return s
 
 
+def glossy_scene(seed: int = 0) -> Scene:
+    """The Cornell-like scene with a rough GGX conductor tall box and a
+    rough plastic-like (diffuse + specular) short box: every differentiated
+    material parameter (albedo, roughness) affects the image."""
+    s = cornell_scene(seed)
+    rng = np.random.Generator(np.random.PCG64(seed + 1000))
+    mats = dict((name, i) for i, (_, name, _) in enumerate(s.materials))
+    s.materials[mats["tall_box_material"]] = ("DefaultMaterial", "tall_box_material", {
+        "diffuse_albedo": list(rng.uniform(0.5, 0.9, 3)), "specular_albedo": list(rng.uniform(0.6, 1.0, 3)),
+        "roughness_x": 0.35, "roughness_y": 0.35, "metalness": 1.0})
+    s.materials[mats["short_box_material"]] = ("DefaultMaterial", "short_box_material", {
+        "diffuse_albedo": list(rng.uniform(0.2, 0.8, 3)), "specular_albedo": [1.0, 1.0, 1.0],
+        "roughness_x": 0.3, "roughness_y": 0.3, "metalness": 0.0, "specular_weight": 1.0, "ior_n": 1.5,
+        "transmission_weight": 0.0})
+    return s
+
+
+def orbit_camera(scene: Scene, k: int, n: int) -> Scene:
+    """A copy of the scene viewed from the k-th of n cameras on a circle
+    around its current look-at point (same height and distance)."""
+    import copy
+    frm, look, fov = scene.camera
+    dx, dz = frm[0] - look[0], frm[2] - look[2]
+    r = float(np.hypot(dx, dz))
+    a0 = float(np.arctan2(dx, dz))
+    a = a0 + 2.0 * np.pi * k / n * 0.25 - np.pi * 0.125  # a 90-degree arc centred on the original view
+    out = copy.copy(scene)
+    out.camera = ((look[0] + r * np.sin(a), frm[1], look[2] + r * np.cos(a)), look, fov)
+    return out
+
+
 SCENES = {
     "cornell": cornell_scene,
+    "glossy": glossy_scene,
     "instanced": instanced_scene,
     "volumetric": volumetric_scene,
 }
 
 
-def scene_path(name: str, seed: int = 0, cache_dir: str | None = None) -> str:
-    """Writes (once) and returns the path of a generated scene file."""
+def scene_path(name: str, seed: int = 0, cache_dir: str | None = None, view: int = 0, views: int = 1) -> str:
+    """Writes (once) and returns the path of a generated scene file; `view`
+    of `views` > 1 selects an orbit camera (orbit_camera)."""
     cache_dir = cache_dir or os.environ.get("YMRT_SCENE_CACHE", os.path.join(os.path.dirname(__file__), "_scenes"))
-    path = os.path.join(cache_dir, f"{name}_{seed}.ymtmp")
+    suffix = f"_v{view}of{views}" if views > 1 else ""
+    path = os.path.join(cache_dir, f"{name}_{seed}{suffix}.ymtmp")
     if not os.path.exists(path):
-        write_scene(SCENES[name](seed), path)
+        scene = SCENES[name](seed)
+        if views > 1:
+            scene = orbit_camera(scene, view, views)
+        write_scene(scene, path)
     return path
