@@ -277,6 +277,75 @@ def run_batch_workload(args):
     return result if rank == 0 else None
 
 
+def run_diff_workload(args):
+    """Differentiable batched render: 16 views of the instanced scene (32
+    materials) at 512x512, 16 spp, forward with path records and the
+    path-replay backward of an L2 loss against a target rendered with
+    perturbed albedos and roughnesses. Reports the forward and backward
+    device times and their ratio."""
+    import torch
+    import ymrt_b200 as Y
+    from ymrt_b200 import scenes
+
+    rank, world, local_rank = dist_env()
+    torch.cuda.set_device(local_rank)
+    perm = scenes.halton_permutations()
+    n_views, size, spp = 16, 512, 16
+    ctx = Y.Context(local_rank)
+    path = scenes.scene_path("instanced", 0)
+    views = [Y.Scene(ctx, Y.HostScene(path, size, size, camera=scenes.orbit_view("instanced", 0, v, n_views)), perm)
+             for v in range(n_views)]
+    setting = Y.default_setting(spp=spp, ray_depth=12)
+    images = [torch.zeros((size, size, 4), dtype=torch.float32, device="cuda") for _ in views]
+    renders = [[v, setting, 1, img] for v, img in zip(views, images)]
+    records = [torch.zeros((Y.path_count(r), 4), dtype=torch.float32, device="cuda") for r in renders]
+    params = views[0].material_params()
+    rng = np.random.default_rng(3)
+    target_params = params.copy()
+    live = params.sum(1) > 0
+    target_params[live, :3] = np.clip(params[live, :3] + rng.uniform(-0.2, 0.2, (live.sum(), 3)), 0.0, 1.0)
+    target_params[live, 3] = np.clip(params[live, 3] + rng.uniform(-0.1, 0.1, live.sum()), 0.01, 0.99)
+    for v in views:
+        v.set_material_params(target_params)
+    Y.render_batch(ctx, renders)
+    targets = [img.clone() for img in images]
+    for v in views:
+        v.set_material_params(params)
+    grads = torch.zeros((params.shape[0], 4), dtype=torch.float32, device="cuda")
+    fwd_ms, bwd_ms, plain_ms = [], [], []
+    for i in range(args.warmup + args.steps):
+        for r in renders:
+            r[2] = i + 1
+        st_plain = Y.render_batch(ctx, renders)  # the plain forward (no records, deferred shadow rays)
+        st_f = Y.render_batch(ctx, renders, records)
+        dl = [2.0 * (img - t) for img, t in zip(images, targets)]
+        st_b = Y.render_backward(ctx, renders, records, dl, grads)
+        if i >= args.warmup:
+            plain_ms.append(st_plain.ms_total)
+            fwd_ms.append(st_f.ms_total)
+            bwd_ms.append(st_b.ms_total)
+        errors = st_f.device_errors | st_b.device_errors
+    g = grads.cpu().numpy()
+    plain, fwd, bwd = float(np.mean(plain_ms)), float(np.mean(fwd_ms)), float(np.mean(bwd_ms))
+    rays = st_f.extension_rays + st_f.shadow_rays
+    result = {
+        "metric": "Mrays/s", "value": round(rays / (fwd * 1e-3) / 1e6, 2), "unit": "Mrays/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(fwd + bwd, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded .ymtmp scene generated by ymrt_b200.scenes, 16 orbit views)",
+        "config": {"workload": f"differentiable: {n_views} views {size}x{size} {spp}spp depth 12 of the instanced "
+                               "scene, L2 loss against perturbed-parameter target",
+                   "params": "32 materials x (albedo rgb, roughness)"},
+        "forward_plain_ms": round(plain, 3), "forward_recorded_ms": round(fwd, 3), "backward_ms": round(bwd, 3),
+        "backward_over_plain_forward": round(bwd / plain, 3),
+        "grad_norm": float(np.linalg.norm(g)), "device_errors": int(errors),
+    }
+    for v in views:
+        v.close()
+    ctx.close()
+    return result if rank == 0 else None
+
+
 def run_ours(args):
     import torch
     import ymrt_b200 as Y
@@ -554,7 +623,7 @@ def main(argv=None):
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["batch"], default="instanced")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["batch", "diff"], default="instanced")
     ap.add_argument("--spp", type=int, default=0)
     ap.add_argument("--queue", type=int, default=0, help="path queue capacity (0 = library default)")
     ap.add_argument("--cpu-budget", type=float, default=12.0, help="seconds of CPU work per reference sample")
@@ -569,6 +638,8 @@ def main(argv=None):
             res = run_reference(args)
     elif args.workload == "batch":
         res = run_batch_workload(args)
+    elif args.workload == "diff":
+        res = run_diff_workload(args)
     else:
         res = run_ours(args)
     if res is not None:

@@ -133,6 +133,8 @@ int ymrt_scene_load_ymtmp(const char* path, int width, int height, ymrt_host_sce
  * one primitive per leaf). */
 typedef struct ymrt_load_options {
   uint32_t max_leaf_triangles; /* wide-BVH leaf size, 1..4 (default 3); also instances per top-level leaf */
+  uint32_t override_camera;    /* nonzero: the camera below replaces the file's Camera block (other views) */
+  float camera_from[3], camera_look[3], camera_fov_deg;
   uint32_t reserved[7];
 } ymrt_load_options;
 int ymrt_scene_load_ymtmp_ex(const char* path, int width, int height, const ymrt_load_options* options,

@@ -125,8 +125,8 @@ def test_roughness_gradients_match_finite_differences(ctx, scene_dir, halton_per
 def test_autograd_function_two_views(ctx, cornell_path, halton_perm):
     import torch
     from ymrt_b200 import scenes
-    paths = [scenes.scene_path("cornell", 0, view=v, views=4) for v in (0, 3)]
-    views = [Y.Scene(ctx, Y.HostScene(p, 64, 64), halton_perm) for p in paths]
+    views = [Y.Scene(ctx, Y.HostScene(cornell_path, 64, 64, camera=scenes.orbit_view("cornell", 0, v, 4)), halton_perm)
+             for v in (0, 3)]
     r = MultiViewRenderer(ctx, views, Y.default_setting(spp=8, ray_depth=8))
     base = views[0].material_params()
     target_params = base.copy()

@@ -68,7 +68,9 @@ def default_setting(spp=1, ray_depth=8, shape_light=True, distant_light=False, v
 
 
 class LoadOptions(ctypes.Structure):
-    _fields_ = [("max_leaf_triangles", ctypes.c_uint32), ("reserved", ctypes.c_uint32 * 7)]
+    _fields_ = [("max_leaf_triangles", ctypes.c_uint32), ("override_camera", ctypes.c_uint32),
+                ("camera_from", ctypes.c_float * 3), ("camera_look", ctypes.c_float * 3),
+                ("camera_fov_deg", ctypes.c_float), ("reserved", ctypes.c_uint32 * 7)]
 
 
 class Job(ctypes.Structure):
@@ -197,11 +199,18 @@ class Context:
 class HostScene:
     """A parsed and prepared .ymtmp scene (no GPU involved)."""
 
-    def __init__(self, path: str, width: int, height: int, max_leaf_triangles: int = 3):
+    def __init__(self, path: str, width: int, height: int, max_leaf_triangles: int = 3, camera=None):
+        """camera: optional (from, look, fov_degrees) replacing the file's camera."""
         self.h = ctypes.c_void_p()
         err = ctypes.create_string_buffer(1024)
         opts = LoadOptions()
         opts.max_leaf_triangles = max_leaf_triangles
+        if camera is not None:
+            frm, look, fov = camera
+            opts.override_camera = 1
+            opts.camera_from[:] = [float(x) for x in frm]
+            opts.camera_look[:] = [float(x) for x in look]
+            opts.camera_fov_deg = float(fov)
         rc = library().ymrt_scene_load_ymtmp_ex(path.encode(), width, height, ctypes.byref(opts), ctypes.byref(self.h),
                                                 err, len(err))
         if rc != YMRT_OK:

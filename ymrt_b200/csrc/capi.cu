@@ -157,10 +157,10 @@ struct ymrt_context {
   int ensure_shadow_queue() {
     const size_t n = (size_t)pool_capacity * kShadowRaysPerVertex;
     if (shadow_queue.capacity == n) return YMRT_OK;
-    cudaError_t e = shadow_buf.ensure(n * 3 * sizeof(float4));
+    cudaError_t e = shadow_buf.ensure(n * (3 * sizeof(float4) + sizeof(uint32_t)));
     if (e != cudaSuccess) return cuda_fail(e, "allocating shadow-ray queue");
     float4* q = shadow_buf.as<float4>();
-    shadow_queue = ShadowQueue{q, q + n, q + 2 * n, (uint32_t)n};
+    shadow_queue = ShadowQueue{q, q + n, q + 2 * n, reinterpret_cast<uint32_t*>(q + 3 * n), (uint32_t)n};
     return YMRT_OK;
   }
 };
@@ -331,6 +331,11 @@ int ymrt_scene_load_ymtmp_ex(const char* path, int width, int height, const ymrt
   }
   try {
     rc = load_ymtmp(path, &hs->s, &msg);
+    if (rc == YMRT_OK && options && options->override_camera) {
+      hs->s.cam_from = vec3(options->camera_from[0], options->camera_from[1], options->camera_from[2]);
+      hs->s.cam_look = vec3(options->camera_look[0], options->camera_look[1], options->camera_look[2]);
+      hs->s.cam_fov_deg = gmax(options->camera_fov_deg, 0.01f);
+    }
     if (rc == YMRT_OK) rc = prepare_scene(&hs->s, width, height, &msg);
   } catch (const std::exception& ex) {
     rc = YMRT_ERR_FORMAT;
@@ -796,11 +801,8 @@ int batch_options(ymrt_context* ctx, const std::vector<JobDesc>& jobs, WaveOptio
     opt->volumes = opt->volumes || j.setting.enable_volume_scattering;
     clamp = clamp || j.setting.enable_indirect_clamp;
   }
-  bool record = false;
-  for (const JobDesc& j : jobs) record = record || j.path_radiance != nullptr;
   opt->sort_hits = ctx->sort_hits;
-  // a recorded path's radiance must include its shadow rays: trace them inline
-  opt->defer_shadows = ctx->defer_shadows && !opt->volumes && !clamp && !record;
+  opt->defer_shadows = ctx->defer_shadows && !opt->volumes && !clamp;
   if (opt->defer_shadows) {
     int rc = ctx->ensure_shadow_queue();
     if (rc != YMRT_OK) return rc;
@@ -888,7 +890,10 @@ int ymrt_render_batch(ymrt_context* ctx, const ymrt_job* jobs_in, int n_jobs, ym
   BatchMemory M;
   int rc = context_memory(ctx, all.size(), &M);
   if (rc != YMRT_OK) return rc;
-  for (const JobDesc& j : all) cudaMemsetAsync(j.image, 0, (size_t)j.width * j.height * sizeof(float4), st);
+  for (const JobDesc& j : all) {
+    cudaMemsetAsync(j.image, 0, (size_t)j.width * j.height * sizeof(float4), st);
+    if (j.path_radiance) cudaMemsetAsync(j.path_radiance, 0, (size_t)j.path_count * sizeof(float4), st);
+  }
   // Launch groups of jobs whose (scene, sampler) pairs fit the constant-memory slots.
   BatchResult total;
   size_t k0 = 0;

@@ -198,6 +198,9 @@ __device__ __forceinline__ vec3 sample_wh(vec3 wo, float u0, float u1, float ax,
 
 enum LobeType : int { kLambert = 0, kReflect = 1, kTransmit = 2 };
 
+// Which layer of DefaultMtl a lobe models (used by the adjoint pass).
+constexpr int kRoleCoat = 0, kRoleMetal = 1, kRoleSpecular = 2, kRoleTransmission = 3, kRoleDiffuse = 4;
+
 struct Lobe {
   int type;
   vec3 albedo;        // diffuse / specular / transmission albedo
@@ -205,6 +208,7 @@ struct Lobe {
   float ni;
   float ax, ay;
   int is_metal;
+  int role;           // kRole*
 };
 
 constexpr int kMaxLobes = 5;
@@ -389,6 +393,7 @@ __device__ __forceinline__ void init_layered_lobes(LayeredBsdf& B, const Default
     L.kt = vec3(0.0f);
     L.ni = ior_in;
     L.is_metal = 0;
+    L.role = kRoleCoat;
     B.w[n] = coat_lum;
     wsum += coat_lum;
     ++n;
@@ -408,6 +413,7 @@ __device__ __forceinline__ void init_layered_lobes(LayeredBsdf& B, const Default
     L.kt = mk;
     L.ni = ior_in;
     L.is_metal = 1;
+    L.role = kRoleMetal;
     B.w[n] = metal_lum;
     wsum += metal_lum;
     ++n;
@@ -425,6 +431,7 @@ __device__ __forceinline__ void init_layered_lobes(LayeredBsdf& B, const Default
     L.kt = vec3(0.0f);
     L.ni = ior_in;
     L.is_metal = 0;
+    L.role = kRoleSpecular;
     B.w[n] = spec_lum;
     wsum += spec_lum;
     ++n;
@@ -441,6 +448,7 @@ __device__ __forceinline__ void init_layered_lobes(LayeredBsdf& B, const Default
     L.nt = vec3(ior_out);
     L.kt = vec3(0.0f);
     L.is_metal = 0;
+    L.role = kRoleTransmission;
     B.w[n] = trans_lum;
     wsum += trans_lum;
     ++n;
@@ -456,6 +464,7 @@ __device__ __forceinline__ void init_layered_lobes(LayeredBsdf& B, const Default
     L.ni = 1.0f;
     L.nt = L.kt = vec3(0.0f);
     L.is_metal = 0;
+    L.role = kRoleDiffuse;
     B.w[n] = diff_lum;
     wsum += diff_lum;
     ++n;

@@ -58,7 +58,8 @@ __device__ __forceinline__ void accumulate_pixel(float4* image, uint32_t pixel, 
 __device__ __forceinline__ void finish_path(const JobDesc& J, uint32_t pixel, uint32_t path_id, vec3 rad,
                                             float inv_spp) {
   accumulate_pixel(J.image, pixel, rad, inv_spp);
-  if (J.path_radiance) J.path_radiance[path_id] = make_float4(rad.x, rad.y, rad.z, 0.0f);
+  // added, not stored: deferred shadow rays of the path add to the same record
+  if (J.path_radiance) atomicAdd(J.path_radiance + path_id, make_float4(rad.x, rad.y, rad.z, 0.0f));
 }
 
 template <bool kAdj>
@@ -540,47 +541,73 @@ constexpr int kMaxGradMaterials = 64;     // materials with shared-memory gradie
 constexpr float kParamStep = 1e-3f;       // central-difference step of df/dp
 
 struct AdjCtx {
-  const DefaultMtl* mtl;                  // the vertex's material
-  int hit_back;
-  vec3 ray_dir;
-  float ray_ior, ex_ior;
   vec3 weight;                            // dLoss/dI (per path) * throughput: the weight of this vertex's NEE
   float g[kGradParams];                   // accumulated dLoss/dp
+  // Per-lobe derivative data of the vertex's layered BSDF (channel-diagonal
+  // in albedo: each channel's albedo moves only that channel of f):
+  vec3 lambert_coeff;                     // the diffuse lobe's colour per unit albedo
+  vec3 metal_n[2], metal_k[2];            // the conductor's complex IOR at albedo +-h
+  float ax[2], ay[2];                     // the microfacet lobes' alpha at roughness +-h
 };
 
-__device__ __forceinline__ void perturb(DefaultMtl& m, int k, float h) {
-  if (k < 3) {
-    m.diffuse_albedo[k] += h;
-  } else {
-    m.alpha_x += h;
-    m.alpha_y += h;
-  }
+__device__ __noinline__ void init_adjoint(AdjCtx& a, const LayeredBsdf& B, const DefaultMtl& m) {
+  a.lambert_coeff = vec3(0.0f);
+  for (int i = 0; i < B.count; ++i)
+    if (B.lobe[i].role == kRoleDiffuse)
+      for (int c = 0; c < 3; ++c)
+        a.lambert_coeff[c] = m.diffuse_albedo[c] > 0.0f ? B.lobe[i].albedo[c] / m.diffuse_albedo[c] : 0.0f;
+  edge_tint_to_conductor(m.diffuse_albedo + vec3(kParamStep), m.specular_albedo, &a.metal_n[0], &a.metal_k[0]);
+  edge_tint_to_conductor(m.diffuse_albedo - vec3(kParamStep), m.specular_albedo, &a.metal_n[1], &a.metal_k[1]);
+  a.ax[0] = sqr(gclamp(m.alpha_x + kParamStep, 0.001f, 0.999f));
+  a.ax[1] = sqr(gclamp(m.alpha_x - kParamStep, 0.001f, 0.999f));
+  a.ay[0] = sqr(gclamp(m.alpha_y + kParamStep, 0.001f, 0.999f));
+  a.ay[1] = sqr(gclamp(m.alpha_y - kParamStep, 0.001f, 0.999f));
+  for (int k = 0; k < kGradParams; ++k) a.g[k] = 0.0f;
 }
 
-// df/dp_k at fixed (wo, wi) in the frame of B (central difference).
-__device__ __noinline__ vec3 dfdparam(const AdjCtx& a, const LayeredBsdf& B, int k, vec3 wo, vec3 wi) {
-  DefaultMtl mp = *a.mtl, mm = *a.mtl;
-  perturb(mp, k, kParamStep);
-  perturb(mm, k, -kParamStep);
-  LayeredBsdf Bp = B, Bm = B;
-  init_layered_lobes(Bp, mp, a.ray_dir, a.hit_back, a.ray_ior, a.ex_ior);
-  init_layered_lobes(Bm, mm, a.ray_dir, a.hit_back, a.ray_ior, a.ex_ior);
+// Adds weight . (c * (df/dp) / f) for every parameter at the fixed
+// directions (wo, wi) in the frame of B. df/d(albedo): exact for the diffuse
+// lobe (linear), a central difference of the conductor's Fresnel term
+// through its edge-tint IOR; df/d(roughness): central differences of the
+// metal, specular and transmission lobes (the coat has its own roughness).
+__device__ __noinline__ void add_relative_grads(AdjCtx* a, const LayeredBsdf& B, vec3 wo, vec3 wi, vec3 weight,
+                                                vec3 c) {
   float pdf;
-  const vec3 fp = bsdf_eval(Bp, wo, wi, &pdf), fm = bsdf_eval(Bm, wo, wi, &pdf);
-  return (fp - fm) * (0.5f / kParamStep);
-}
-
-// Adds weight . (c * (df/dp_k) / f) for every parameter, f = the BSDF at (wo, wi).
-__device__ __forceinline__ void add_relative_grads(AdjCtx* a, const LayeredBsdf& B, vec3 wo, vec3 wi, vec3 weight, vec3 c) {
-  float pdf;
-  const vec3 f = bsdf_eval(B, wo, wi, &pdf);
-  for (int k = 0; k < kGradParams; ++k) {
-    const vec3 d = dfdparam(*a, B, k, wo, wi);
-    float acc = 0.0f;
-    for (int ch = 0; ch < 3; ++ch)
-      if (f[ch] > 0.0f) acc += weight[ch] * c[ch] * d[ch] / f[ch];
-    a->g[k] += acc;
+  const float inv2h = 0.5f / kParamStep;
+  vec3 f(0.0f), da(0.0f), dr(0.0f);
+  for (int i = 0; i < B.count; ++i) {
+    const Lobe& L = B.lobe[i];
+    f += lobe_eval(L, wo, wi, &pdf);
+    if (L.role == kRoleDiffuse) {
+      Lobe u = L;
+      u.albedo = a->lambert_coeff;
+      da += lobe_eval(u, wo, wi, &pdf);
+    }
+    if (L.role == kRoleMetal) {
+      Lobe hi = L, lo = L;
+      hi.nt = a->metal_n[0];
+      hi.kt = a->metal_k[0];
+      lo.nt = a->metal_n[1];
+      lo.kt = a->metal_k[1];
+      da += (lobe_eval(hi, wo, wi, &pdf) - lobe_eval(lo, wo, wi, &pdf)) * inv2h;
+    }
+    if (L.role == kRoleMetal || L.role == kRoleSpecular || L.role == kRoleTransmission) {
+      Lobe hi = L, lo = L;
+      hi.ax = a->ax[0];
+      hi.ay = a->ay[0];
+      lo.ax = a->ax[1];
+      lo.ay = a->ay[1];
+      dr += (lobe_eval(hi, wo, wi, &pdf) - lobe_eval(lo, wo, wi, &pdf)) * inv2h;
+    }
   }
+  float rough = 0.0f;
+  for (int ch = 0; ch < 3; ++ch) {
+    if (!(f[ch] > 0.0f)) continue;
+    const float s = weight[ch] * c[ch] / f[ch];
+    a->g[ch] += s * da[ch];
+    rough += s * dr[ch];
+  }
+  a->g[3] += rough;
 }
 
 // Where a surface shadow ray goes when shadow rays are deferred: the queue
@@ -592,6 +619,7 @@ struct ShadowEmit {
   uint32_t* errors;
   uint32_t pixel;
   uint32_t job;
+  uint32_t path;
   vec3 weight;
 };
 
@@ -610,6 +638,7 @@ __device__ __forceinline__ void emit_shadow_ray(const ShadowEmit& em, vec3 o, ve
   em.q.o[slot] = make_float4(o.x, o.y, o.z, maxd);
   em.q.d[slot] = make_float4(d.x, d.y, d.z, __uint_as_float(em.pixel));
   em.q.c[slot] = make_float4(w.x, w.y, w.z, __uint_as_float(em.job));
+  em.q.path[slot] = em.path;
 }
 
 // One next-event shadow ray of a surface vertex toward a light, with MIS
@@ -1036,7 +1065,7 @@ __global__ void __launch_bounds__(kTraceBlock) k_shade(PathPool P, const WaveCon
         init_layered_lobes(B, mat.default_mtl, rd, hit_back, ray_ior(rt), ex_ior(rt, inst_idx));
         const SurfaceNee nc{rd, sp.p, sp.p_err, sp.ng, inst_idx, tri, &rt, nb, n_nb, rs.enable_volume_scattering != 0,
                             slot};
-        const ShadowEmit em{shadow_q, &counters->shadow_count, errors, pf.x, job, tp * inv_spp};
+        const ShadowEmit em{shadow_q, &counters->shadow_count, errors, pf.x, job, P.path_id[i], tp * inv_spp};
         AdjCtx adj_ctx;
         AdjCtx* adj = nullptr;
         vec3 delta(0.0f), l_total(0.0f);
@@ -1045,13 +1074,8 @@ __global__ void __launch_bounds__(kTraceBlock) k_shade(PathPool P, const WaveCon
           const float4 lt = J.path_radiance[P.path_id[i]];
           delta = vec3(dl.x, dl.y, dl.z) * inv_spp;  // dLoss/d(this path's radiance)
           l_total = vec3(lt.x, lt.y, lt.z);
-          adj_ctx.mtl = &mat.default_mtl;
-          adj_ctx.hit_back = hit_back;
-          adj_ctx.ray_dir = rd;
-          adj_ctx.ray_ior = ray_ior(rt);
-          adj_ctx.ex_ior = ex_ior(rt, inst_idx);
+          init_adjoint(adj_ctx, B, mat.default_mtl);
           adj_ctx.weight = delta * tp;
-          for (int k = 0; k < kGradParams; ++k) adj_ctx.g[k] = 0.0f;
           adj = &adj_ctx;
         }
         if (rs.enable_distant_light)
@@ -1163,6 +1187,11 @@ __global__ void __launch_bounds__(kTraceBlock, 5) k_connect(ShadowQueue Q, const
     const JobDesc& J = jobs[__float_as_uint(c.w)];
     if (!trace_occluded(J.scene_slot, st, vec3(o.x, o.y, o.z), vec3(d.x, d.y, d.z), o.w, &tests, &nodes)) {
       atomicAdd(J.image + __float_as_uint(d.w), make_float4(c.x, c.y, c.z, 0.0f));
+      if (J.path_radiance) {
+        // the record holds radiance, the contribution is weighted by 1/spp
+        const float spp = (float)gmax(J.setting.ssp, 1);
+        atomicAdd(J.path_radiance + Q.path[t], make_float4(c.x * spp, c.y * spp, c.z * spp, 0.0f));
+      }
     }
   }
   for (int off = 16; off > 0; off >>= 1) {

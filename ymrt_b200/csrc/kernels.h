@@ -73,7 +73,7 @@ struct JobDesc {
   unsigned long long path_begin;  // first path of this job in the batch's path space
   unsigned long long path_count;  // tiles rendered * 256 * spp
   // differentiable rendering (null when unused)
-  float4* path_radiance;          // forward: each path's radiance, by path index
+  float4* path_radiance;          // forward: each path's radiance, by path index (accumulated: zero it first)
   const float4* dloss;            // adjoint: dLoss/dImage per pixel
   float* grads;                   // adjoint: dLoss/dParam, 4 per material (albedo rgb, roughness)
   uint32_t grad_materials;        // materials with gradient slots
@@ -84,6 +84,7 @@ struct ShadowQueue {
   float4* o;   // origin xyz, maximum distance
   float4* d;   // normalised direction xyz, pixel index (bits)
   float4* c;   // contribution rgb, already weighted by throughput / spp; job index (bits)
+  uint32_t* path;  // path index within the job (for per-path records)
   uint32_t capacity;
 };
 

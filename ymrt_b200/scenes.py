@@ -415,18 +415,16 @@ def glossy_scene(seed: int = 0) -> Scene:
     return s
 
 
-def orbit_camera(scene: Scene, k: int, n: int) -> Scene:
-    """A copy of the scene viewed from the k-th of n cameras on a circle
-    around its current look-at point (same height and distance)."""
-    import copy
-    frm, look, fov = scene.camera
+def orbit_view(name: str, seed: int, k: int, n: int):
+    """The k-th of n cameras (from, look, fov) on a 90-degree arc around the
+    scene's look-at point, at the original camera's height and distance and
+    centred on it (for HostScene(..., camera=...))."""
+    frm, look, fov = SCENES[name](seed).camera
     dx, dz = frm[0] - look[0], frm[2] - look[2]
     r = float(np.hypot(dx, dz))
     a0 = float(np.arctan2(dx, dz))
-    a = a0 + 2.0 * np.pi * k / n * 0.25 - np.pi * 0.125  # a 90-degree arc centred on the original view
-    out = copy.copy(scene)
-    out.camera = ((look[0] + r * np.sin(a), frm[1], look[2] + r * np.cos(a)), look, fov)
-    return out
+    a = a0 + (k / max(n - 1, 1) - 0.5) * (np.pi / 2)
+    return (float(look[0] + r * np.sin(a)), float(frm[1]), float(look[2] + r * np.cos(a))), tuple(look), fov
 
 
 SCENES = {
@@ -437,15 +435,10 @@ SCENES = {
 }
 
 
-def scene_path(name: str, seed: int = 0, cache_dir: str | None = None, view: int = 0, views: int = 1) -> str:
-    """Writes (once) and returns the path of a generated scene file; `view`
-    of `views` > 1 selects an orbit camera (orbit_camera)."""
+def scene_path(name: str, seed: int = 0, cache_dir: str | None = None) -> str:
+    """Writes (once) and returns the path of a generated scene file."""
     cache_dir = cache_dir or os.environ.get("YMRT_SCENE_CACHE", os.path.join(os.path.dirname(__file__), "_scenes"))
-    suffix = f"_v{view}of{views}" if views > 1 else ""
-    path = os.path.join(cache_dir, f"{name}_{seed}{suffix}.ymtmp")
+    path = os.path.join(cache_dir, f"{name}_{seed}.ymtmp")
     if not os.path.exists(path):
-        scene = SCENES[name](seed)
-        if views > 1:
-            scene = orbit_camera(scene, view, views)
-        write_scene(scene, path)
+        write_scene(SCENES[name](seed), path)
     return path
