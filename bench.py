@@ -351,12 +351,11 @@ def run_ours(args):
     import ymrt_b200 as Y
     from ymrt_b200 import scenes
 
+    from ymrt_b200 import distributed as D
     rank, world, local_rank = dist_env()
     torch.cuda.set_device(local_rank)
     if world > 1:
-        import torch.distributed as dist
-        from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+        D.init("nccl", timeout_s=120)
     wl = WORKLOADS[args.workload]
     W, H = wl["width"], wl["height"]
     spp = args.spp or wl["spp"]
@@ -375,10 +374,8 @@ def run_ours(args):
             dist.barrier()
 
     def step(i):
-        _, st = scene.render(setting, frame_index=i * world + rank + 1, out=image)
-        if world > 1:
-            import torch.distributed as dist
-            dist.all_reduce(image)
+        _, st = scene.render(setting, frame_index=D.frame_index(i, rank, world), out=image)
+        D.combine_frames(image, world, mean=False)  # one all-reduce of the ranks' frames per step
         flush_l2(torch, flush)
         return st
 
