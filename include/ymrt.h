@@ -155,6 +155,8 @@ void ymrt_host_scene_free(ymrt_host_scene* scene);
 #define YMRT_QUERY_VOLUMES 8     /* uint32[9*n]: the reference's Volume struct words */
 #define YMRT_QUERY_DISTANT_LIGHTS 9 /* uint32[8*n]: the reference's DistantLight struct words */
 #define YMRT_QUERY_TEXTURES 10   /* uint32[13*n]: type, black/white inputs, value, rgb, frequency, lacunarity, gain, layers, amplitude, offset */
+#define YMRT_QUERY_GEOMETRIES 11 /* uint32[2*n]: kind (0 triangle mesh, 1 sphere), sphere radius (float bits) */
+#define YMRT_QUERY_MESH_CORNERS 12 /* float[8*c] of mesh `index`, by corner: position, normal, uv (0 without texcoords) */
 long long ymrt_host_scene_query(const ymrt_host_scene* scene, int what, int index, void* out, size_t cap);
 
 /* Uploads a prepared scene. halton_perm: the concatenated digit permutations

@@ -50,6 +50,8 @@ def lib():
         L.ymref_geometry_triangle_count.restype = ctypes.c_int64
         L.ymref_geometry_triangle_count.argtypes = [vp, ctypes.c_uint32]
         L.ymref_geometry_triangles.argtypes = [vp, ctypes.c_uint32, vp]
+        L.ymref_geometry_kind.argtypes = [vp, ctypes.c_uint32, vp]
+        L.ymref_mesh_corners.argtypes = [vp, ctypes.c_uint32, vp]
         L.ymref_lights.argtypes = [vp, vp, vp, vp]
         L.ymref_camera_bytes.argtypes = [vp, vp, i]
         L.ymref_scene_records.argtypes = [vp, i, vp, i]
@@ -125,6 +127,23 @@ class RefScene:
         out = np.zeros((max(n, 0), 3), np.uint32)
         if n > 0:
             lib().ymref_geometry_triangles(self.h, g, _p(out))
+        return out
+
+    def geometries(self) -> np.ndarray:
+        """(type, radius) per geometry: type 0 a triangle mesh, 1 a sphere."""
+        n = self.counts()["geometries"]
+        out = np.zeros((n, 2), np.float32)
+        r = np.zeros(1, np.float32)
+        for g in range(n):
+            out[g, 0] = lib().ymref_geometry_kind(self.h, g, _p(r))
+            out[g, 1] = r[0]
+        return out
+
+    def mesh_corners(self, g: int) -> np.ndarray:
+        n = lib().ymref_geometry_triangle_count(self.h, g)
+        out = np.zeros((3 * max(n, 0), 8), np.float32)
+        if n > 0:
+            lib().ymref_mesh_corners(self.h, g, _p(out))
         return out
 
     def lights(self):

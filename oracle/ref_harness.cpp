@@ -224,6 +224,41 @@ int ymref_geometry_triangles(void* handle, uint32_t g, uint32_t* out) {
   return 0;
 }
 
+// Geometry type (GEOMETRY_TYPE: 0 triangle mesh, 1 sphere) and, for a
+// sphere, its radius; -1 for an index out of range.
+int ymref_geometry_kind(void* handle, uint32_t g, float* radius) {
+  auto ctx = static_cast<RefContext*>(handle);
+  auto& geo = GuiModule::Geometries(*ctx->module);
+  if (g >= geo.size()) return -1;
+  *radius = geo[g].geometry_type == SPHERE ? geo[g].sphere.radius : 0.0f;
+  return (int)geo[g].geometry_type;
+}
+
+// Per corner of a mesh geometry (3 per triangle, corner-index order):
+// position, normal and texcoord (0, 0 when the mesh has none), 8 floats.
+int ymref_mesh_corners(void* handle, uint32_t g, float* out) {
+  auto ctx = static_cast<RefContext*>(handle);
+  auto& geo = GuiModule::Geometries(*ctx->module);
+  if (g >= geo.size() || geo[g].geometry_type != TRIANGLE_MESH) return -1;
+  const TriangleMesh& m = geo[g].triangle_mesh;
+  const uint32_t* pi = m.GetPositionIndicesHost();
+  const glm::vec3* p = m.GetPositionsHost();
+  const uint32_t* ni = m.GetNormalIndicesHost();
+  const glm::vec3* n = m.GetNormalsHost();
+  const bool has_uv = m.texcoord_idx_offset != -1 && m.texcoord_offset != -1;
+  const uint32_t* ti = has_uv ? m.GetTexcoordIndicesHost() : nullptr;
+  const glm::vec2* t = has_uv ? m.GetTexcoordsHost() : nullptr;
+  for (int64_t c = 0; c < 3 * m.triangle_count; ++c) {
+    float* o = out + 8 * c;
+    const glm::vec3 q = p[pi[c]], r = n[ni[c]];
+    o[0] = q.x; o[1] = q.y; o[2] = q.z;
+    o[3] = r.x; o[4] = r.y; o[5] = r.z;
+    o[6] = has_uv ? t[ti[c]].x : 0.0f;
+    o[7] = has_uv ? t[ti[c]].y : 0.0f;
+  }
+  return 0;
+}
+
 // Shape lights (instance, triangle, power, area) and the power CDF table.
 int ymref_lights(void* handle, uint32_t* ids /* 2 per light */, float* power_area /* 2 per light */,
                  float* table) {

@@ -91,6 +91,23 @@ def test_per_sample_volumetric_vs_reference_cuda(ctx, refgpu, volumetric_path, h
     ref.close()
 
 
+@pytest.mark.parametrize("volume", [0, 1])
+def test_per_sample_spheres_vs_reference_cuda(ctx, refgpu, scene_dir, halton_perm, volume):
+    """Sphere and Cube blocks: a glass and a metal sphere, a sphere light, a
+    medium-filled boundary sphere around the camera and the built-in cube."""
+    from ymrt_b200 import scenes
+    path = scenes.scene_path("spheres", 0, scene_dir)
+    ours, ref = _pair(ctx, refgpu, path, halton_perm, 256, 256, exact=True)
+    ref.set_settings(spp=1, ray_depth=8, volume=volume)
+    a, _ = ours.render(Y.default_setting(spp=1, ray_depth=8, volume=bool(volume)), 2)
+    b = ref.render_frame(2)
+    assert np.array_equal(a[..., 3], b[..., 3])
+    bad = _bad(a, b)
+    assert bad.mean() <= 2e-3, f"{bad.sum()} of {bad.size} pixels differ beyond 1e-5 relative"
+    ours.close()
+    ref.close()
+
+
 def test_converged_cornell_vs_reference_default_build(ctx, refgpu, cornell_path, halton_perm):
     ours, ref = _pair(ctx, refgpu, cornell_path, halton_perm, 256, 256, exact=False)
     ref.set_settings(spp=16, ray_depth=8)

@@ -27,7 +27,7 @@ def _meaningful(kind, rec):
 
 
 @pytest.mark.parametrize("name,size", [("cornell", (256, 256)), ("instanced", (1920, 1080)),
-                                       ("volumetric", (256, 256))])
+                                       ("volumetric", (256, 256)), ("spheres", (256, 256))])
 def test_scene_preparation_matches_reference(name, size, scene_dir, halton_perm, oracle):
     from ymrt_b200 import scenes
     path = scenes.scene_path(name, 0, scene_dir)
@@ -45,8 +45,10 @@ def test_scene_preparation_matches_reference(name, size, scene_dir, halton_perm,
     for kind in ("materials", "volumes", "distant_lights", "textures"):
         a, b = _meaningful(kind, ours.records(kind)), _meaningful(kind, ref.records(kind))
         assert np.array_equal(a, b), kind
+    assert np.array_equal(ours.geometries().view(np.uint32), ref.geometries().view(np.uint32))
     for g in range(ref.counts()["geometries"]):
         assert np.array_equal(ours.triangles(g), ref.geometry_triangles(g)), f"mesh {g}"
+        assert np.array_equal(ours.mesh_corners(g).view(np.uint32), ref.mesh_corners(g).view(np.uint32)), f"mesh {g}"
     # camera: position, u, v, w, aspect, tan(fov/2) against the reference Camera bytes
     cam = np.frombuffer(ref.camera_bytes(), dtype=np.float32)
     # Camera layout: m_width, m_height (ints), position, u, v, w, aspect, fov, lens, tan_half_fov
@@ -80,7 +82,7 @@ def test_loader_rejects_bad_input(tmp_path):
         Y.HostScene(write(tmp_path, "Begin(Transform);\n\ttranslate = <0,0,0>;\n"), 8, 8)
     assert e.value.code == -3  # missing End
     with pytest.raises(Y.YmrtError) as e:
-        Y.HostScene(write(tmp_path, 'Begin(Sphere);\n\tname = "s";\nEnd(Sphere);\n'), 8, 8)
+        Y.HostScene(write(tmp_path, 'Begin(CheckerBoardTexture);\n\tname = "t";\nEnd(CheckerBoardTexture);\n'), 8, 8)
     assert e.value.code == -4
     with pytest.raises(Y.YmrtError) as e:  # instance referring to an undeclared name
         Y.HostScene(write(tmp_path, 'Begin(PrimitiveInstance);\n\tname = "i";\n\tgeometry_index = "g";\nEnd(PrimitiveInstance);\n'), 8, 8)
@@ -90,7 +92,7 @@ def test_loader_rejects_bad_input(tmp_path):
     assert e.value.code == -1
 
 
-@pytest.mark.parametrize("name", ["cornell", "instanced", "volumetric"])
+@pytest.mark.parametrize("name", ["cornell", "instanced", "volumetric", "spheres"])
 def test_reference_bvh_depth_fits_its_stack(name, scene_dir, halton_perm, oracle):
     """The reference's traversals keep at most depth + 1 node indices on a
     32-entry stack with no bounds check in release builds

@@ -33,6 +33,7 @@ ERRORS = {
 QUERY_COUNTS, QUERY_INSTANCES, QUERY_LIGHTS, QUERY_LIGHT_TABLE = 0, 1, 2, 3
 QUERY_TRANSFORMS, QUERY_CAMERA, QUERY_TRIANGLES = 4, 5, 6
 QUERY_MATERIALS, QUERY_VOLUMES, QUERY_DISTANT_LIGHTS, QUERY_TEXTURES = 7, 8, 9, 10
+QUERY_GEOMETRIES, QUERY_MESH_CORNERS = 11, 12
 
 
 class YmrtError(RuntimeError):
@@ -260,6 +261,15 @@ class HostScene:
 
     def triangles(self, mesh: int) -> np.ndarray:
         return self._query(QUERY_TRIANGLES, np.uint32, mesh).reshape(-1, 3)
+
+    def geometries(self) -> np.ndarray:
+        """(kind, radius) per geometry: kind 0 a triangle mesh, 1 a sphere."""
+        g = self._query(QUERY_GEOMETRIES, np.uint32).reshape(-1, 2)
+        return np.stack([g[:, 0].astype(np.float32), g[:, 1].view(np.float32)], axis=1)
+
+    def mesh_corners(self, mesh: int) -> np.ndarray:
+        """Per corner of a mesh: position, normal, uv (8 floats; uv 0 without texcoords)."""
+        return self._query(QUERY_MESH_CORNERS, np.float32, mesh).reshape(-1, 8)
 
     def records(self, kind: str) -> np.ndarray:
         """Materials, volumes, distant lights (32-bit words of the reference's

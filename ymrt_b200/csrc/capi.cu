@@ -422,6 +422,28 @@ long long ymrt_host_scene_query(const ymrt_host_scene* hs, int what, int index, 
       const std::vector<uint32_t>& t = s.meshes[index].tris;
       return copy(t.data(), t.size(), sizeof(uint32_t));
     }
+    case YMRT_QUERY_GEOMETRIES: {
+      std::vector<uint32_t> v;
+      for (const HostMesh& m : s.meshes) v.insert(v.end(), {m.kind, f2u(m.radius)});
+      return copy(v.data(), v.size(), sizeof(uint32_t));
+    }
+    case YMRT_QUERY_MESH_CORNERS: {
+      if (index < 0 || (size_t)index >= s.meshes.size()) return YMRT_ERR_INVALID;
+      const HostMesh& m = s.meshes[index];
+      std::vector<float> v;
+      for (size_t c = 0; c < m.pos_idx.size(); ++c) {
+        const uint32_t pi = m.pos_idx[c], ni = m.nrm_idx[c];
+        v.insert(v.end(), {m.pos[3 * pi], m.pos[3 * pi + 1], m.pos[3 * pi + 2], m.nrm[3 * ni], m.nrm[3 * ni + 1],
+                           m.nrm[3 * ni + 2]});
+        if (m.uv_idx.empty()) {
+          v.insert(v.end(), {0.0f, 0.0f});
+        } else {
+          const uint32_t ti = m.uv_idx[c];
+          v.insert(v.end(), {m.uv[2 * ti], m.uv[2 * ti + 1]});
+        }
+      }
+      return copy(v.data(), v.size(), sizeof(float));
+    }
     default:
       return YMRT_ERR_INVALID;
   }
@@ -497,6 +519,8 @@ int ymrt_scene_upload(ymrt_context* ctx, const ymrt_host_scene* hs, const uint32
   D.instance_count = (uint32_t)s.instances.size();
   D.transform_count = (uint32_t)s.transforms.size();
   D.geometry_count = (uint32_t)s.geo_desc.size();
+  D.sphere_count = 0;
+  for (const GeometryDesc& g : s.geo_desc) D.sphere_count += g.kind == kGeoSphere ? 1u : 0u;
   D.material_count = (uint32_t)s.materials.size();
   D.distant_light_count = (uint32_t)s.distant_lights.size();
   D.shape_light_count = (uint32_t)s.shape_lights.size();
@@ -677,6 +701,7 @@ int run_batch(ymrt_context* ctx, const BatchMemory& M, std::vector<JobDesc>& job
         (uintptr_t)M.pool[0].ray_o, (uintptr_t)M.pool[1].ray_o, (uintptr_t)M.hits.bary_t, (uintptr_t)M.ctl,
         (uintptr_t)M.jobs, (uintptr_t)M.counters, (uintptr_t)jobs.size(), (uintptr_t)o.volumes,
         (uintptr_t)o.sort_hits, (uintptr_t)o.defer_shadows, (uintptr_t)o.shadow_queue.o, M.capacity,
+        (uintptr_t)o.spheres,
         (uintptr_t)o.adjoint, (uintptr_t)o.grads, o.grad_materials};
     if (ctx->graph_key != key) {
       ctx->drop_graph();
@@ -792,6 +817,13 @@ int finish_batch(ymrt_context* ctx, const BatchResult& r, ymrt_stats* stats) {
   return YMRT_OK;
 }
 
+// Whether any of the batch's scenes holds sphere geometry.
+bool any_spheres(const DeviceScene* scenes, size_t n) {
+  for (size_t i = 0; i < n; ++i)
+    if (scenes[i].sphere_count != 0) return true;
+  return false;
+}
+
 // Wave options for a batch: media kernels when any job scatters in media;
 // shadow rays deferred unless a job clamps indirect light.
 int batch_options(ymrt_context* ctx, const std::vector<JobDesc>& jobs, WaveOptions* opt) {
@@ -854,6 +886,7 @@ int ymrt_render_tiles(ymrt_scene* sc, const ymrt_render_setting* setting, int fr
   if ((rc = context_memory(ctx, 1, &M)) != YMRT_OK) return rc;
   WaveOptions opt;
   if ((rc = batch_options(ctx, jobs, &opt)) != YMRT_OK) return rc;
+  opt.spheres = any_spheres(&scene, 1);
   jobs[0].scene_slot = 0;
   if ((e = upload_constants(&scene, 1, ctx->primes.data(), ctx->prime_sums.data(), st)) != cudaSuccess)
     return ctx->cuda_fail(e, "uploading constants");
@@ -916,6 +949,7 @@ int ymrt_render_batch(ymrt_context* ctx, const ymrt_job* jobs_in, int n_jobs, ym
     const std::vector<DeviceScene> slots = assign_slots(jobs, js, ks);
     WaveOptions opt;
     if ((rc = batch_options(ctx, jobs, &opt)) != YMRT_OK) return rc;
+    opt.spheres = any_spheres(slots.data(), slots.size());
     if ((e = upload_constants(slots.data(), (uint32_t)slots.size(), ctx->primes.data(), ctx->prime_sums.data(), st)) !=
         cudaSuccess)
       return ctx->cuda_fail(e, "uploading constants");
@@ -979,6 +1013,7 @@ int ymrt_render_backward(ymrt_context* ctx, const ymrt_job* jobs_in, int n_jobs,
   if (rc != YMRT_OK) return rc;
   WaveOptions opt;
   opt.adjoint = true;
+  opt.spheres = any_spheres(slots.data(), slots.size());
   opt.grads = grads_device;
   opt.grad_materials = n_materials;
   if ((e = upload_constants(slots.data(), (uint32_t)slots.size(), ctx->primes.data(), ctx->prime_sums.data(), st)) !=

@@ -8,6 +8,7 @@
 // places where the reference mixes in double-precision literals.
 #pragma once
 
+#include "sphere.h"
 #include "ymrt_scene.h"
 
 namespace ym {
@@ -18,11 +19,50 @@ struct SurfacePoint {
   vec3 p, p_err, p_obj, ns, ng, dpdu, dpdv;
 };
 
-// FetchShadingData + FetchMeshShadingData (src/ShadingUtilities.cuh:713-875).
+// FetchSphereShadingData (src/ShadingUtilities.cuh:639-711) in object space:
+// `p` is the hit point the sphere test projected onto the sphere. The
+// texture coordinates are not formed: no texture here reads them.
+__device__ __forceinline__ void sphere_surface(float sphere_radius, vec3 p, SurfacePoint* sp) {
+  const float radius = gmax(sphere_radius, kFloatEps);
+  const vec3 n = p / radius;
+  sp->p = p;
+  sp->p_err = error_gamma(5) * vabs(p);
+  sp->ns = n;
+  sp->ng = n;
+  float sin_theta = 0.0f;
+  if (1.0f - n.y * n.y > 0.0f) sin_theta = sqrtf(1.0f - n.y * n.y);
+  float cos_phi, sin_phi;
+  if (sin_theta > 0.0f) {
+    cos_phi = n.x / sin_theta;
+    sin_phi = n.z / sin_theta;
+  } else {
+    cos_phi = 1.0f;
+    sin_phi = 0.0f;
+  }
+  sp->dpdu = vec3(-p.z, 0.0f, p.x) * kTwoPi;
+  sp->dpdv = vec3(p.y * cos_phi, -radius * sin_theta, sin_phi * p.y) * kPi;
+}
+
+// FetchShadingData + FetchMeshShadingData / FetchSphereShadingData
+// (src/ShadingUtilities.cuh:639-875). For a sphere `bary` is the object-space
+// hit point and `tri` is EMPTY.
 __device__ __forceinline__ SurfacePoint fetch_surface(const DeviceScene& S, uint32_t inst_idx, uint32_t tri,
                                                       vec3 bary) {
   const Instance inst = S.instances[inst_idx];
   const GeometryDesc& g = S.geometries[inst.geometry_idx];
+  if (g.kind == kGeoSphere) {
+    SurfacePoint sp;
+    sphere_surface(g.radius, bary, &sp);
+    const mat4& otw = S.transforms[inst.transform_idx];
+    const mat4& wto = S.i_transforms[inst.transform_idx];
+    sp.p_obj = sp.p;
+    sp.p = transform_position(otw, sp.p, &sp.p_err);
+    sp.ns = normalize(transpose_transform_vector(wto, sp.ns));
+    sp.ng = normalize(transpose_transform_vector(wto, sp.ng));
+    sp.dpdu = transform_vector(otw, sp.dpdu);
+    sp.dpdv = transform_vector(otw, sp.dpdv);
+    return sp;
+  }
   const uint32_t* tc = S.tri_corners + 3 * (size_t)(g.tri_offset + tri);
   const uint32_t c0 = tc[0], c1 = tc[1], c2 = tc[2];
   auto P = [&](uint32_t c) {
@@ -77,25 +117,33 @@ __device__ __forceinline__ SurfacePoint fetch_surface(const DeviceScene& S, uint
   return sp;
 }
 
-// FetchGeometryNormal (src/ShadingUtilities.cuh:923-952): position, error and
-// normalised geometric normal only.
+// FetchGeometryNormal with FetchMeshGeometryNormal / FetchSphereGeometryNormal
+// (src/ShadingUtilities.cuh:877-952): position, error and normalised
+// geometric normal only.
 __device__ __forceinline__ void fetch_geometry_normal(const DeviceScene& S, uint32_t inst_idx, uint32_t tri, vec3 bary,
                                                       vec3* p, vec3* p_err, vec3* ng) {
   const Instance inst = S.instances[inst_idx];
   const GeometryDesc& g = S.geometries[inst.geometry_idx];
-  const uint32_t* tc = S.tri_corners + 3 * (size_t)(g.tri_offset + tri);
-  vec3 q[3];
-  for (int k = 0; k < 3; ++k) {
-    const uint32_t vi = S.pos_idx[g.corner_offset + tc[k]];
-    const float* a = S.positions + 3 * (size_t)(g.pos_offset + vi);
-    q[k] = vec3(a[0], a[1], a[2]);
+  if (g.kind == kGeoSphere) {
+    const float radius = gmax(g.radius, kFloatEps);
+    *p = bary;
+    *p_err = error_gamma(5) * vabs(bary);
+    *ng = bary / radius;
+  } else {
+    const uint32_t* tc = S.tri_corners + 3 * (size_t)(g.tri_offset + tri);
+    vec3 q[3];
+    for (int k = 0; k < 3; ++k) {
+      const uint32_t vi = S.pos_idx[g.corner_offset + tc[k]];
+      const float* a = S.positions + 3 * (size_t)(g.pos_offset + vi);
+      q[k] = vec3(a[0], a[1], a[2]);
+    }
+    const float xs = fabsf(q[0].x * bary.x) + fabsf(q[1].x * bary.y) + fabsf(q[2].x * bary.z);
+    const float ys = fabsf(q[0].y * bary.x) + fabsf(q[1].y * bary.y) + fabsf(q[2].y * bary.z);
+    const float zs = fabsf(q[0].z * bary.x) + fabsf(q[1].z * bary.y) + fabsf(q[2].z * bary.z);
+    *p = q[0] * bary.x + q[1] * bary.y + q[2] * bary.z;
+    *p_err = error_gamma(7) * vec3(xs, ys, zs);
+    *ng = cross(q[1] - q[0], q[2] - q[0]);
   }
-  const float xs = fabsf(q[0].x * bary.x) + fabsf(q[1].x * bary.y) + fabsf(q[2].x * bary.z);
-  const float ys = fabsf(q[0].y * bary.x) + fabsf(q[1].y * bary.y) + fabsf(q[2].y * bary.z);
-  const float zs = fabsf(q[0].z * bary.x) + fabsf(q[1].z * bary.y) + fabsf(q[2].z * bary.z);
-  *p = q[0] * bary.x + q[1] * bary.y + q[2] * bary.z;
-  *p_err = error_gamma(7) * vec3(xs, ys, zs);
-  *ng = cross(q[1] - q[0], q[2] - q[0]);
   const mat4& otw = S.transforms[inst.transform_idx];
   const mat4& wto = S.i_transforms[inst.transform_idx];
   *p = transform_position(otw, *p, p_err);
@@ -542,17 +590,27 @@ __device__ __forceinline__ int sample_light_power(const DeviceScene& S, float u0
   return idx;
 }
 
+// One shape light: a triangle of a mesh instance, or a whole sphere.
 struct LightTri {
   vec3 p0, p1, p2, n0, n1, n2, color;
   float intensity;
   const mat4* otw;
   const mat4* wto;
+  bool sphere;
+  float radius;
 };
 __device__ __forceinline__ LightTri load_light_tri(const DeviceScene& S, const ShapeLight& L) {
   LightTri lt;
   const Instance inst = S.instances[L.instance_idx];
   const Material& mat = S.materials[inst.material_idx];
   const GeometryDesc& g = S.geometries[inst.geometry_idx];
+  lt.color = mat.light_mtl.light_color;
+  lt.intensity = mat.light_mtl.intensity;
+  lt.otw = &S.transforms[inst.transform_idx];
+  lt.wto = &S.i_transforms[inst.transform_idx];
+  lt.sphere = g.kind == kGeoSphere;
+  lt.radius = g.radius;
+  if (lt.sphere) return lt;
   const uint32_t* tc = S.tri_corners + 3 * (size_t)(g.tri_offset + L.triangle_idx);
   vec3* P[3] = {&lt.p0, &lt.p1, &lt.p2};
   vec3* N[3] = {&lt.n0, &lt.n1, &lt.n2};
@@ -564,16 +622,87 @@ __device__ __forceinline__ LightTri load_light_tri(const DeviceScene& S, const S
     const float* b = S.normals + 3 * (size_t)(g.nrm_offset + ni);
     *N[k] = vec3(b[0], b[1], b[2]);
   }
-  lt.color = mat.light_mtl.light_color;
-  lt.intensity = mat.light_mtl.intensity;
-  lt.otw = &S.transforms[inst.transform_idx];
-  lt.wto = &S.i_transforms[inst.transform_idx];
   return lt;
 }
 
-// ShapeLight::SampleLi, triangle meshes (src/Light.h:207-264).
+// SampleCone (src/SampleUtilities.h:33-39).
+__device__ __forceinline__ vec3 sample_cone(float u0, float u1, float cos_theta_max) {
+  const float c = (1.0f - u0) + u0 * cos_theta_max;
+  const float sn = sqrtf(gmax(0.0f, 1.0f - c * c));
+  const float phi = u1 * 2.0f * kPi;
+  return vec3(cosf(phi) * sn, sinf(phi) * sn, c);
+}
+
+// ShapeLight::SampleLi, spheres (src/Light.h:282-314): a direction in the
+// cone the sphere subtends, solid-angle pdf.
+__device__ __forceinline__ bool sphere_light_sample_li(const LightTri& lt, vec3 position, float u0, float u1, vec3* wi,
+                                                       vec3* lpos, vec3* lpos_err, vec3* lng, vec3* Li, float* pdf) {
+  const vec3 op = transform_position(*lt.wto, position);
+  const float lpo = length(op);
+  const float r = lt.radius;
+  if (lpo < r) {
+    *pdf = 0.0f;
+    return false;
+  }
+  const float ctm = sqrtf(gmax(sqr(lpo) - sqr(r), 0.0f)) / lpo;
+  const float cone = 2.0f * kPi * (1.0f - ctm);
+  vec3 cs = sample_cone(u0, u1, ctm);
+  vec3 w = -op, u, v;
+  orthogonal_basis(w, u, v);
+  cs = cs.x * u + cs.y * v + cs.z * w;
+  float t0, t1;
+  sphere_solve(op, cs, r, &t0, &t1);
+  vec3 ip = op + cs * t0;
+  const float lio = length(ip);
+  ip *= r * safe_rcp(lio);
+  vec3 err = error_gamma(5) * vabs(ip);
+  *lpos = transform_position(*lt.otw, ip, &err);
+  *lpos_err = err;
+  *lng = normalize(*lpos - get_translate(*lt.otw));
+  *wi = normalize(transform_vector(*lt.otw, cs));
+  *pdf = 1.0f / cone;
+  *Li = lt.color * lt.intensity * cone;
+  return true;
+}
+
+// ShapeLight::EvalLi, spheres (src/Light.h:163-200).
+__device__ __forceinline__ vec3 sphere_light_eval_li(const LightTri& lt, vec3 position, vec3 wi, vec3* lpos,
+                                                     vec3* lpos_err, vec3* lng, float* pdf) {
+  const vec3 owi = transform_vector(*lt.wto, wi);
+  const vec3 op = transform_position(*lt.wto, position);
+  const float lpo = length(op);
+  const float r = lt.radius;
+  if (lpo < r) {
+    *pdf = 0.0f;
+    return vec3(0.0f);
+  }
+  float t0, t1;
+  if (!sphere_solve(op, owi, r, &t0, &t1)) {
+    *pdf = 0.0f;
+    return vec3(0.0f);
+  }
+  const float ctm = sqrtf(gmax(sqr(lpo) - sqr(r), 0.0f)) / lpo;
+  const float cone = 2.0f * kPi * (1.0f - ctm);
+  const float ct = dot(normalize(owi), -op / lpo);
+  if (ct < ctm) {
+    *pdf = 0.0f;
+    return vec3(0.0f);
+  }
+  vec3 ip = op + owi * t0;
+  const float lio = length(ip);
+  ip *= r * safe_rcp(lio);
+  vec3 err = error_gamma(5) * vabs(ip);
+  *lpos = transform_position(*lt.otw, ip, &err);
+  *lpos_err = err;
+  *lng = normalize(*lpos - get_translate(*lt.otw));
+  *pdf = 1.0f / cone;
+  return lt.color * lt.intensity;
+}
+
+// ShapeLight::SampleLi, triangle meshes (src/Light.h:207-264), and spheres.
 __device__ __forceinline__ bool light_sample_li(const LightTri& lt, float area, vec3 position, float u0, float u1, vec3* wi,
                                                 vec3* lpos, vec3* lpos_err, vec3* lng, vec3* Li, float* pdf) {
+  if (lt.sphere) return sphere_light_sample_li(lt, position, u0, u1, wi, lpos, lpos_err, lng, Li, pdf);
   const vec3 geo_n = cross(lt.p1 - lt.p0, lt.p2 - lt.p0);
   const float su = sqrtf(gmax(0.0f, u0));
   const float bu = 1.0f - su;
@@ -605,6 +734,7 @@ __device__ __forceinline__ bool light_sample_li(const LightTri& lt, float area, 
 // RayIntersectTriangle's glm 3x3 inverse (src/Light.h:14-40).
 __device__ __forceinline__ vec3 light_eval_li(const LightTri& lt, float area, vec3 position, vec3 wi, vec3* lpos,
                                               vec3* lpos_err, vec3* lng, float* pdf) {
+  if (lt.sphere) return sphere_light_eval_li(lt, position, wi, lpos, lpos_err, lng, pdf);
   const vec3 geo_n = cross(lt.p1 - lt.p0, lt.p2 - lt.p0);
   const vec3 owi = transform_vector(*lt.wto, wi);
   const vec3 opos = transform_position(*lt.wto, position);

@@ -1,8 +1,8 @@
 // Two-level ray traversal over compressed 8-wide BVHs (sm_100a).
 //
 // Semantics follow the reference's TraceRay / IntersectMeshObject /
-// IntersectTri / BVHTraverseShadow (src/ShadingUtilities.cuh:54-217,
-// 310-431, 563-635): world rays are carried into each instance with the
+// IntersectTri / IntersectSphereObject / BVHTraverseShadow
+// (src/ShadingUtilities.cuh:54-276, 310-431, 563-635): world rays are carried into each instance with the
 // instance's inverse transform (glm mat4*vec4 order), triangles are tested
 // with the watertight test in the reference's exact float order (so t and the
 // barycentrics are bit-identical), a hit is kept when TMIN <= t <= current t
@@ -20,6 +20,7 @@
 #pragma once
 
 #include "dev_constants.cuh"
+#include "sphere.h"
 #include "ymrt_scene.h"
 
 namespace ym {
@@ -278,6 +279,34 @@ __device__ __forceinline__ void push_children(TraversalStack& st, uint32_t inter
   }
 }
 
+// Sphere tests of the traversals, kept out of line so that their registers do
+// not weigh on the triangle loop that surrounds them.
+struct SphereTest {
+  float t, px, py, pz;  // the hit, when hit != 0
+  float xt;             // the extra crossing, when xhit != 0
+  int hit, back, xhit, xback;
+};
+__device__ __noinline__ SphereTest sphere_instance_test(float radius, vec3 o, vec3 d, float t_max) {
+  SphereHit h{0.0f, vec3(0.0f), 0};
+  SphereExtra x{false, kTMax, 0};
+  SphereTest r;
+  r.hit = sphere_intersect(radius, o, d, t_max, &h, &x);
+  r.t = h.t;
+  r.px = h.p.x;
+  r.py = h.p.y;
+  r.pz = h.p.z;
+  r.back = h.back;
+  r.xhit = x.hit;
+  r.xt = x.t;
+  r.xback = x.back;
+  return r;
+}
+__device__ __noinline__ bool sphere_occludes(float radius, vec3 o, vec3 d, float t_max) {
+  SphereHit h;
+  SphereExtra x;
+  return sphere_intersect(radius, o, d, t_max, &h, &x);
+}
+
 struct NearbyHit {
   uint32_t prim;
   float t;
@@ -303,9 +332,14 @@ struct ClosestHit {
 // in. Instance leaves are pushed in distance order with the internal nodes,
 // bottom-level leaves are tested at once, and entries whose box begins
 // beyond the closest hit so far are dropped when popped.
-__device__ __noinline__ bool trace_closest(uint32_t scene, TraversalStack& st, vec3 wo, vec3 wd, float tmax,
-                                           uint32_t last_inst, uint32_t last_tri, bool volume_only, ClosestHit* out,
-                                           uint32_t* tri_tests, uint32_t* node_visits) {
+//
+// kSpheres: the scene holds sphere geometry. The loop without sphere code is
+// a separate function, so scenes of meshes alone keep its register
+// allocation (the sphere branch costs the triangle loop about 5%).
+template <bool kSpheres>
+__device__ __noinline__ bool trace_closest_impl(uint32_t scene, TraversalStack& st, vec3 wo, vec3 wd, float tmax,
+                                                uint32_t last_inst, uint32_t last_tri, bool volume_only,
+                                                ClosestHit* out, uint32_t* tri_tests, uint32_t* node_visits) {
   const DeviceScene& S = c_scenes[scene];
   const uint4* tlas = reinterpret_cast<const uint4*>(S.tlas_nodes);
   const uint4* blas = reinterpret_cast<const uint4*>(S.blas_nodes);
@@ -325,7 +359,10 @@ __device__ __noinline__ bool trace_closest(uint32_t scene, TraversalStack& st, v
   BoxRay br = wray;
   bool skip_here = false, inst_hit = false;
   float inst_t = 0.0f, hb0 = 0.0f, hb1 = 0.0f, hb2 = 0.0f, extra_t = kTMax;
+  // hit_w / extra_w: the wide-BVH slot of the hit / extra triangle, or for a
+  // sphere (inst_sphere) the back-face flag of its hit / extra crossing
   uint32_t hit_tri = kEmpty, hit_w = 0, extra_w = kEmpty;
+  bool inst_sphere = false;
 
   st.sp = 0;
   st.push(0, 0.0f);
@@ -333,17 +370,23 @@ __device__ __noinline__ bool trace_closest(uint32_t scene, TraversalStack& st, v
     if (inst_base >= 0 && st.sp == inst_base) {
       // leaving the instance: record its hit (and the nearby-hit list)
       if (inst_hit) {
-        vec3 p0, p1, p2;
-        uint32_t tid;
-        load_tri(S.wtris, hit_w, &p0, &p1, &p2, &tid);
-        const vec3 ng = normalize(cross(p1 - p0, p2 - p0));
+        int back;
+        if (kSpheres && inst_sphere) {
+          back = (int)hit_w;
+        } else {
+          vec3 p0, p1, p2;
+          uint32_t tid;
+          load_tri(S.wtris, hit_w, &p0, &p1, &p2, &tid);
+          const vec3 ng = normalize(cross(p1 - p0, p2 - p0));
+          back = dot(ng, od) > 0.0f;
+        }
         out->t = inst_t;
         out->b0 = hb0;
         out->b1 = hb1;
         out->b2 = hb2;
         out->inst = inst_idx;
         out->tri = hit_tri;
-        out->back = dot(ng, od) > 0.0f;
+        out->back = back;
         hit = true;
         t_upper = next_float_up(next_float_up(t_ray));
         t_lower = next_float_down(next_float_down(t_ray));
@@ -358,13 +401,19 @@ __device__ __noinline__ bool trace_closest(uint32_t scene, TraversalStack& st, v
           }
         }
         n_nearby = head;
-        if (n_nearby < kMaxNearby) nb[n_nearby++] = NearbyHit{inst_idx, inst_t, out->back};
+        if (n_nearby < kMaxNearby) nb[n_nearby++] = NearbyHit{inst_idx, inst_t, back};
       } else if (hit && extra_w != kEmpty && extra_t > t_lower && extra_t < t_upper) {
-        vec3 p0, p1, p2;
-        uint32_t tid;
-        load_tri(S.wtris, extra_w, &p0, &p1, &p2, &tid);
-        const vec3 ng = normalize(cross(p1 - p0, p2 - p0));
-        if (n_nearby < kMaxNearby) nb[n_nearby++] = NearbyHit{inst_idx, extra_t, dot(ng, od) > 0.0f};
+        int back;
+        if (kSpheres && inst_sphere) {
+          back = (int)extra_w;
+        } else {
+          vec3 p0, p1, p2;
+          uint32_t tid;
+          load_tri(S.wtris, extra_w, &p0, &p1, &p2, &tid);
+          const vec3 ng = normalize(cross(p1 - p0, p2 - p0));
+          back = dot(ng, od) > 0.0f;
+        }
+        if (n_nearby < kMaxNearby) nb[n_nearby++] = NearbyHit{inst_idx, extra_t, back};
       }
       inst_base = -1;
     }
@@ -380,6 +429,28 @@ __device__ __noinline__ bool trace_closest(uint32_t scene, TraversalStack& st, v
       const vec3 oo = xform_point_glm(wto, wo);
       od = xform_dir_glm(wto, wd);
       const GeometryDesc& g = S.geometries[inst.geometry_idx];
+      if (kSpheres && g.kind == kGeoSphere) {
+        // a sphere is tested at once and left at the next iteration; its hit
+        // point travels in the barycentric slots and its triangle is EMPTY
+        ++*tri_tests;
+        const SphereTest q = sphere_instance_test(g.radius, oo, od, t_ray);
+        inst_sphere = true;
+        inst_hit = q.hit != 0;
+        if (inst_hit) {
+          t_ray = q.t;
+          inst_t = q.t;
+          hb0 = q.px;
+          hb1 = q.py;
+          hb2 = q.pz;
+          hit_tri = kEmpty;
+          hit_w = (uint32_t)q.back;
+        }
+        extra_t = q.xhit ? q.xt : kTMax;
+        extra_w = q.xhit ? (uint32_t)q.xback : kEmpty;
+        inst_base = st.sp;
+        continue;
+      }
+      inst_sphere = false;
       tr = make_tri_ray(oo, od);
       br = make_box_ray(oo, od);
       wtri_offset = g.wtri_offset;
@@ -436,11 +507,24 @@ __device__ __noinline__ bool trace_closest(uint32_t scene, TraversalStack& st, v
   return hit;
 }
 
+// Closest hit of one world-space ray in the scene of constant-memory slot
+// `scene` (see trace_closest_impl).
+__device__ __forceinline__ bool trace_closest(uint32_t scene, TraversalStack& st, vec3 wo, vec3 wd, float tmax,
+                                              uint32_t last_inst, uint32_t last_tri, bool volume_only,
+                                              ClosestHit* out, uint32_t* tri_tests, uint32_t* node_visits) {
+  if (c_scenes[scene].sphere_count != 0)
+    return trace_closest_impl<true>(scene, st, wo, wd, tmax, last_inst, last_tri, volume_only, out, tri_tests,
+                                    node_visits);
+  return trace_closest_impl<false>(scene, st, wo, wd, tmax, last_inst, last_tri, volume_only, out, tri_tests,
+                                   node_visits);
+}
+
 // Any hit within (TMIN, tmax] ignoring boundary-only instances
 // (BVHTraverseShadow, src/ShadingUtilities.cuh:563-635). Same single loop as
 // trace_closest; children are pushed unordered and the first hit ends it.
-__device__ __noinline__ bool trace_occluded(uint32_t scene, TraversalStack& st, vec3 wo, vec3 wd, float tmax,
-                                            uint32_t* tri_tests, uint32_t* node_visits) {
+template <bool kSpheres>
+__device__ __noinline__ bool trace_occluded_impl(uint32_t scene, TraversalStack& st, vec3 wo, vec3 wd, float tmax,
+                                                 uint32_t* tri_tests, uint32_t* node_visits) {
   const DeviceScene& S = c_scenes[scene];
   const uint4* tlas = reinterpret_cast<const uint4*>(S.tlas_nodes);
   const uint4* blas = reinterpret_cast<const uint4*>(S.blas_nodes);
@@ -463,6 +547,14 @@ __device__ __noinline__ bool trace_occluded(uint32_t scene, TraversalStack& st, 
       const vec3 oo = xform_point_glm(wto, wo);
       const vec3 od = xform_dir_glm(wto, wd);
       const GeometryDesc& g = S.geometries[inst.geometry_idx];
+      if (kSpheres && g.kind == kGeoSphere) {
+        ++*tri_tests;
+        if (sphere_occludes(g.radius, oo, od, tmax)) {
+          st.sp = 0;
+          return true;
+        }
+        continue;
+      }
       tr = make_tri_ray(oo, od);
       br = make_box_ray(oo, od);
       wtri_offset = g.wtri_offset;
@@ -505,6 +597,12 @@ __device__ __noinline__ bool trace_occluded(uint32_t scene, TraversalStack& st, 
     }
   }
   return false;
+}
+
+__device__ __forceinline__ bool trace_occluded(uint32_t scene, TraversalStack& st, vec3 wo, vec3 wd, float tmax,
+                                               uint32_t* tri_tests, uint32_t* node_visits) {
+  if (c_scenes[scene].sphere_count != 0) return trace_occluded_impl<true>(scene, st, wo, wd, tmax, tri_tests, node_visits);
+  return trace_occluded_impl<false>(scene, st, wo, wd, tmax, tri_tests, node_visits);
 }
 
 }  // namespace ym

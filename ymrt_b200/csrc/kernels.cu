@@ -241,7 +241,10 @@ __global__ void __launch_bounds__(256) k_sort_hits(const WaveControl* __restrict
 // iteration, for the warp-collective bucket filing); the wave's size comes
 // from the wave-control block, so any grid works (launched with one thread
 // per pool slot, each thread takes at most one path).
-template <bool kVol>
+//
+// kSph: some scene of the batch holds spheres (the traversal without sphere
+// tests is a separate instantiation; see trace_closest_impl).
+template <bool kVol, bool kSph>
 __global__ void __launch_bounds__(kTraceBlock, 5) k_extend(PathPool P, const WaveControl* __restrict__ ctl, HitPool H,
                                                            const JobDesc* __restrict__ jobs, WaveCounters* counters) {
   YM_TRAVERSAL_SHARED(s_stack);
@@ -266,7 +269,7 @@ __global__ void __launch_bounds__(kTraceBlock, 5) k_extend(PathPool P, const Wav
     TraversalStack st;
     st.bind(s_stack_entries, s_stack_t);
     ClosestHit ch;
-    bool hit = trace_closest(slot, st, o, d, kTMax, lh.x, lh.y, false, &ch, &tests, &nodes);
+    bool hit = trace_closest_impl<kSph>(slot, st, o, d, kTMax, lh.x, lh.y, false, &ch, &tests, &nodes);
     overflow = overflow || st.overflow;
     bool volume_hit = false;
     vec3 vol_pos(0.0f);
@@ -1175,6 +1178,7 @@ __global__ void __launch_bounds__(kTraceBlock) k_shade(PathPool P, const WaveCon
 // Traces the wave's queued shadow rays (grid-stride over the queue, so the
 // grid is sized to the GPU, not to the queue) and adds each unoccluded ray's
 // contribution to its pixel.
+template <bool kSph>
 __global__ void __launch_bounds__(kTraceBlock, 5) k_connect(ShadowQueue Q, const JobDesc* __restrict__ jobs,
                                                             WaveCounters* counters) {
   YM_TRAVERSAL_SHARED(s_stack);
@@ -1185,7 +1189,8 @@ __global__ void __launch_bounds__(kTraceBlock, 5) k_connect(ShadowQueue Q, const
   for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
     const float4 o = Q.o[t], d = Q.d[t], c = Q.c[t];
     const JobDesc& J = jobs[__float_as_uint(c.w)];
-    if (!trace_occluded(J.scene_slot, st, vec3(o.x, o.y, o.z), vec3(d.x, d.y, d.z), o.w, &tests, &nodes)) {
+    if (!trace_occluded_impl<kSph>(J.scene_slot, st, vec3(o.x, o.y, o.z), vec3(d.x, d.y, d.z), o.w, &tests,
+                                   &nodes)) {
       atomicAdd(J.image + __float_as_uint(d.w), make_float4(c.x, c.y, c.z, 0.0f));
       if (J.path_radiance) {
         // the record holds radiance, the contribution is weighted by 1/spp
@@ -1361,13 +1366,13 @@ void prepare_persistent_grids() {
   PersistentGrids g;
   g.device = dev;
   g.generate = grid_for(k_generate, 256, sms);
-  g.extend[0] = grid_for(k_extend<false>, kTraceBlock, sms);
-  g.extend[1] = grid_for(k_extend<true>, kTraceBlock, sms);
+  g.extend[0] = grid_for(k_extend<false, false>, kTraceBlock, sms);
+  g.extend[1] = grid_for(k_extend<true, false>, kTraceBlock, sms);
   g.sort = grid_for(k_sort_hits, 256, sms);
   g.shade[0] = grid_for(k_shade<false, false>, kTraceBlock, sms);
   g.shade[1] = grid_for(k_shade<false, true>, kTraceBlock, sms);
   g.shade[2] = grid_for(k_shade<true, false>, kTraceBlock, sms);
-  g.connect = grid_for(k_connect, kTraceBlock, sms);
+  g.connect = grid_for(k_connect<false>, kTraceBlock, sms);
   g_grids = g;
 }
 
@@ -1391,8 +1396,10 @@ uint32_t launch_wave(const PathPool& A, const PathPool& B, const HitPool& H, Wav
   if (ev) cudaEventRecord(ev[0], stream);
   k_generate<<<blocks_256, 256, 0, stream>>>(A, ctl, jobs, n_jobs);
   if (ev) cudaEventRecord(ev[1], stream);
-  if (opt.volumes) k_extend<true><<<blocks_trace, kTraceBlock, 0, stream>>>(A, ctl, Hs, jobs, counters);
-  else k_extend<false><<<blocks_trace, kTraceBlock, 0, stream>>>(A, ctl, Hs, jobs, counters);
+  if (opt.volumes && opt.spheres) k_extend<true, true><<<blocks_trace, kTraceBlock, 0, stream>>>(A, ctl, Hs, jobs, counters);
+  else if (opt.volumes) k_extend<true, false><<<blocks_trace, kTraceBlock, 0, stream>>>(A, ctl, Hs, jobs, counters);
+  else if (opt.spheres) k_extend<false, true><<<blocks_trace, kTraceBlock, 0, stream>>>(A, ctl, Hs, jobs, counters);
+  else k_extend<false, false><<<blocks_trace, kTraceBlock, 0, stream>>>(A, ctl, Hs, jobs, counters);
   if (ev) cudaEventRecord(ev[2], stream);
   if (sort_hits) k_sort_hits<<<blocks_256, 256, 0, stream>>>(ctl, Hs, A, jobs, counters);
   if (ev) cudaEventRecord(ev[3], stream);
@@ -1406,7 +1413,8 @@ uint32_t launch_wave(const PathPool& A, const PathPool& B, const HitPool& H, Wav
   else
     k_shade<false, false><<<blocks_trace, kTraceBlock, 0, stream>>>(A, ctl, Hs, B, jobs, counters, none);
   if (ev) cudaEventRecord(ev[4], stream);
-  if (defer) k_connect<<<g.connect, kTraceBlock, 0, stream>>>(*defer, jobs, counters);
+  if (defer && opt.spheres) k_connect<true><<<g.connect, kTraceBlock, 0, stream>>>(*defer, jobs, counters);
+  else if (defer) k_connect<false><<<g.connect, kTraceBlock, 0, stream>>>(*defer, jobs, counters);
   if (ev) cudaEventRecord(ev[5], stream);
   k_finish<<<1, 32, 0, stream>>>(ctl, counters, graph_condition);
   return 5u + (sort_hits ? 1u : 0u) + (defer ? 1u : 0u);

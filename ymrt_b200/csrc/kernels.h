@@ -151,6 +151,7 @@ struct WaveOptions {
   bool volumes = false;        // volume scattering kernels
   bool sort_hits = true;       // shade hits listed by shading bucket
   bool defer_shadows = false;  // queue surface shadow rays for k_connect (ignored with volumes)
+  bool spheres = true;         // some scene holds sphere geometry (false selects the mesh-only traversal)
   ShadowQueue shadow_queue{};
   bool adjoint = false;        // path-replay adjoint pass (surfaces; no sorting, no deferral)
   float* grads = nullptr;      // adjoint: dLoss/dParam, kGradParams per material

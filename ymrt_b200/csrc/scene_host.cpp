@@ -16,6 +16,7 @@
 #include <unordered_map>
 
 #include "../../include/ymrt.h"
+#include "sphere.h"
 
 namespace ym {
 
@@ -548,6 +549,50 @@ std::string unquote(const std::string& s) {
   return s;
 }
 
+// The built-in unit cube of a Cube block (GeometryData::InitCube,
+// src/GeometryDefines.h:274-520): [-0.5, 0.5]^3 as 12 triangles over 36
+// unshared corners, faces in the order -z, +z, -x, +x, -y, +y. Each face lists
+// its six corners by the signs of its two in-plane coordinates, in the order
+// the reference writes them (the bottom-level build orders triangles from
+// these, so the order is part of the format); the normal is the face's, and
+// uv = (first in-plane coordinate > 0, second > 0, each flipped as marked).
+HostMesh make_unit_cube(const std::string& name) {
+  struct Face {
+    int axis;           // normal axis
+    float sign;         // normal direction
+    int a, b;           // in-plane axes
+    const char* corners;  // six sign pairs of (a, b)
+    bool flip_v;        // v = (b < 0) instead of (b > 0)
+  };
+  static const Face faces[6] = {
+      {2, -1.0f, 0, 1, "--+++-++---+", true},     {2, 1.0f, 0, 1, "--+-++++-+--", false},
+      {0, -1.0f, 1, 2, "+++------+++", true},     {0, 1.0f, 1, 2, "++--+---++-+", false},
+      {1, -1.0f, 0, 2, "--+-++++-+--", false},    {1, 1.0f, 0, 2, "--+++-++---+", true},
+  };
+  HostMesh m;
+  m.name = name;
+  for (const Face& f : faces) {
+    for (int k = 0; k < 6; ++k) {
+      const bool pa = f.corners[2 * k] == '+', pb = f.corners[2 * k + 1] == '+';
+      float p[3], n[3] = {0.0f, 0.0f, 0.0f};
+      p[f.axis] = 0.5f * f.sign;
+      p[f.a] = pa ? 0.5f : -0.5f;
+      p[f.b] = pb ? 0.5f : -0.5f;
+      n[f.axis] = f.sign;
+      const uint32_t c = (uint32_t)m.pos.size() / 3;
+      m.pos.insert(m.pos.end(), p, p + 3);
+      m.nrm.insert(m.nrm.end(), n, n + 3);
+      m.uv.push_back(pa ? 1.0f : 0.0f);
+      m.uv.push_back((pb != f.flip_v) ? 1.0f : 0.0f);
+      m.tris.push_back(c);
+      m.pos_idx.push_back(c);
+      m.nrm_idx.push_back(c);
+      m.uv_idx.push_back(c);
+    }
+  }
+  return m;
+}
+
 }  // namespace
 
 int load_ymtmp(const std::string& path, HostScene* scene, std::string* error) {
@@ -666,6 +711,7 @@ int load_ymtmp(const std::string& path, HostScene* scene, std::string* error) {
       names[name] = (uint32_t)scene->transforms.size();
       scene->transforms.push_back(m);
       scene->i_transforms.push_back(mat4_inverse(m));
+      scene->transform_scales.push_back(s);
     } else if (type == "Mesh") {
       HostMesh mesh;
       mesh.name = name;
@@ -699,8 +745,19 @@ int load_ymtmp(const std::string& path, HostScene* scene, std::string* error) {
       mesh.tris = std::move(tris);
       names[name] = (uint32_t)scene->meshes.size();
       scene->meshes.push_back(std::move(mesh));
-    } else if (type == "Cube" || type == "Sphere") {
-      return fail(YMRT_ERR_UNSUPPORTED, type + " geometry blocks are not supported; write the shape as a Mesh block");
+    } else if (type == "Cube") {
+      // CreateCube (src/core/SceneModule.cpp:263-277)
+      names[name] = (uint32_t)scene->meshes.size();
+      scene->meshes.push_back(make_unit_cube(name));
+    } else if (type == "Sphere") {
+      // read_sphere_attributes / CreateSphere (src/core/YMParser.cpp:1155-1187,
+      // src/core/SceneModule.cpp:278-292)
+      HostMesh sphere;
+      sphere.name = name;
+      sphere.kind = kGeoSphere;
+      sphere.radius = attrs.count("radius") ? gmax(0.0001f, std::stof(attrs["radius"])) : 1.0f;
+      names[name] = (uint32_t)scene->meshes.size();
+      scene->meshes.push_back(std::move(sphere));
     } else if (type == "PrimitiveInstance") {
       Instance inst{};
       uint32_t g, t, m, v;
@@ -882,6 +939,11 @@ void init_camera_transfer(HostScene* s) {
     const mat4& wto = s->i_transforms[inst.transform_idx];
     const vec3 o = xform_point_glm(wto, o_world), d = xform_dir_glm(wto, d_world);
     const HostMesh& m = s->meshes[inst.geometry_idx];
+    if (m.kind == kGeoSphere) {
+      SphereHit h;
+      SphereExtra x;
+      return sphere_intersect(m.radius, o, d, kTMax, &h, &x);
+    }
     for (size_t t = 0; t < m.tris.size() / 3; ++t) {
       vec3 p[3];
       for (int k = 0; k < 3; ++k) {
@@ -930,6 +992,26 @@ int prepare_scene(HostScene* s, int width, int height, std::string* error) {
   s->all_pos_idx.clear(); s->all_nrm_idx.clear(); s->all_uv_idx.clear();
   s->all_pos.clear(); s->all_nrm.clear(); s->all_uv.clear();
   for (HostMesh& m : s->meshes) {
+    if (m.kind == kGeoSphere) {
+      // GetSphereObjectBound (src/GeometryUtilities.h:19-25); no triangles
+      BBox b;
+      b.pmin = vec3(-m.radius);
+      b.pmax = vec3(m.radius);
+      m.root_box = bound_fix(b);
+      GeometryDesc gd{};
+      gd.tri_offset = (uint32_t)(s->tri_corners.size() / 3);
+      gd.corner_offset = (uint32_t)s->all_pos_idx.size();
+      gd.pos_offset = (uint32_t)(s->all_pos.size() / 3);
+      gd.nrm_offset = (uint32_t)(s->all_nrm.size() / 3);
+      gd.uv_offset = -1;
+      gd.wtri_offset = (uint32_t)(s->wtris.size() / 3);
+      gd.bbox_min = m.root_box.pmin;
+      gd.bbox_max = m.root_box.pmax;
+      gd.kind = kGeoSphere;
+      gd.radius = m.radius;
+      s->geo_desc.push_back(gd);
+      continue;
+    }
     const uint32_t nt = (uint32_t)(m.tris.size() / 3);
     auto P = [&](uint32_t corner) {
       const uint32_t vi = m.pos_idx[corner];
@@ -962,6 +1044,7 @@ int prepare_scene(HostScene* s, int width, int height, std::string* error) {
     gd.uv_offset = m.uv.empty() ? -1 : (int32_t)(s->all_uv.size() / 2);
     gd.bbox_min = m.root_box.pmin;
     gd.bbox_max = m.root_box.pmax;
+    gd.kind = kGeoMesh;
     s->tri_corners.insert(s->tri_corners.end(), m.tris.begin(), m.tris.end());
     s->all_pos_idx.insert(s->all_pos_idx.end(), m.pos_idx.begin(), m.pos_idx.end());
     s->all_nrm_idx.insert(s->all_nrm_idx.end(), m.nrm_idx.begin(), m.nrm_idx.end());
@@ -1024,6 +1107,15 @@ int prepare_scene(HostScene* s, int width, int height, std::string* error) {
     const vec3 c = mat.light_mtl.light_color;
     const float irradiance = (c.x + c.y + c.z) * mat.light_mtl.intensity * kPi;
     const HostMesh& m = s->meshes[inst.geometry_idx];
+    if (m.kind == kGeoSphere) {
+      // the transform's own scale stretches the sphere into an ellipsoid;
+      // its area is approximated as (4/3) pi (ab + bc + ca)
+      const vec3 sc = s->transform_scales[inst.transform_idx];
+      const float a = m.radius * sc.x, b = m.radius * sc.y, c3 = m.radius * sc.z;
+      const float area = (4.0f / 3.0f) * kPi * (a * b + b * c3 + c3 * a);
+      s->shape_lights.push_back(ShapeLight{pi, kEmpty, irradiance * area, area});
+      continue;
+    }
     for (uint32_t t = 0; t < m.tris.size() / 3; ++t) {
       vec3 p[3];
       for (int k = 0; k < 3; ++k) {

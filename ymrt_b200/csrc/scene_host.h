@@ -22,8 +22,12 @@ struct BBox {
   vec3 pmin{kFloatMax, kFloatMax, kFloatMax};
 };
 
+// One geometry: a triangle mesh, or (kind kGeoSphere) an analytic sphere of
+// `radius` with no triangles.
 struct HostMesh {
   std::string name;
+  uint32_t kind = kGeoMesh;
+  float radius = 0.0f;
   std::vector<uint32_t> tris;      // corner triples (id0, id1, id2), reference post-build order
   std::vector<uint32_t> pos_idx, nrm_idx, uv_idx;
   std::vector<float> pos, nrm, uv;
@@ -36,6 +40,7 @@ struct HostScene {
   float cam_fov_deg = 45.0f;
 
   std::vector<mat4> transforms, i_transforms;
+  std::vector<vec3> transform_scales;       // each Transform block's own (clamped) scale
   std::vector<HostMesh> meshes;
   std::vector<Instance> instances;          // after prepare(): reference order
   std::vector<uint32_t> instance_file_index;  // after prepare(): file index of each instance

@@ -74,7 +74,8 @@ struct Volume {
 static_assert(sizeof(Volume) == 36, "Volume layout");
 
 // ShapeLight, src/Light.h:80-86 (16 bytes): triangle `triangle_idx` (in the
-// reference's post-build order) of instance `instance_idx`.
+// reference's post-build order) of instance `instance_idx`, or the whole
+// sphere of a sphere instance (triangle_idx = EMPTY).
 struct ShapeLight {
   uint32_t instance_idx;
   uint32_t triangle_idx;
@@ -182,7 +183,12 @@ struct alignas(16) WideNode {
 };
 static_assert(sizeof(WideNode) == 80, "WideNode is five 16-byte words");
 
-// Per-mesh tables (offsets into the flattened global arrays).
+// GeometryData::geometry_type (src/GeometryDefines.h:10-14).
+constexpr uint32_t kGeoMesh = 0, kGeoSphere = 1;
+
+// Per-geometry tables (offsets into the flattened global arrays). A sphere
+// (kind kGeoSphere) is centred on its object-space origin and has no
+// triangles or bottom-level nodes.
 struct GeometryDesc {
   uint32_t tri_offset;      // into tri_corners (reference post-build triangle order)
   uint32_t tri_count;
@@ -193,6 +199,8 @@ struct GeometryDesc {
   uint32_t node_offset;     // root of the mesh's wide BVH in blas_nodes
   uint32_t wtri_offset;     // into wtris (wide-BVH triangle order)
   vec3 bbox_min, bbox_max;  // root box (object space)
+  uint32_t kind;            // kGeoMesh or kGeoSphere
+  float radius;             // sphere radius (Sphere::radius)
 };
 
 // Everything the kernels read, as device pointers.
@@ -213,6 +221,7 @@ struct DeviceScene {
   // meshes
   uint32_t geometry_count;
   const GeometryDesc* geometries;
+  uint32_t sphere_count;        // sphere geometries (0: the traversal skips sphere tests)
   const WideNode* blas_nodes;
   const float4* wtris;          // 3 per triangle: v0, v1, v2 (w of v0 = triangle id bits)
   const uint32_t* tri_corners;  // 3 per triangle (Triangle id0,id1,id2)

@@ -15,6 +15,11 @@ from seeds with numpy ``PCG64``:
 * ``volumetric`` -- the Cornell scene plus a homogeneous fog box
   (sigma_t 0.05, albedo 0.8, g 0.6) and a heterogeneous medium whose density is
   a procedural fBm texture (the reference's ``NoiseTextureFBM``).
+* ``spheres`` -- the Cornell walls with the analytic shapes of the format: a
+  built-in ``Cube`` block (rotated, diffuse), ``Sphere`` blocks as a smooth
+  dielectric (IOR 1.55), a rough conductor, a small emissive sphere beside the
+  ceiling quad light, and a medium-filled boundary sphere (sigma_t 0.02) large
+  enough to enclose the camera.
 
 The file layout follows the reference's parser (src/core/YMParser.cpp:2330,
 block types :57-92, attribute sets :94-372). Every float is written as the
@@ -33,7 +38,7 @@ import os
 import numpy as np
 
 __all__ = [
-    "first_primes", "halton_permutations", "cornell_scene", "instanced_scene", "volumetric_scene",
+    "first_primes", "halton_permutations", "cornell_scene", "instanced_scene", "volumetric_scene", "spheres_scene",
     "write_scene", "SCENES",
 ]
 
@@ -205,6 +210,8 @@ class Scene:
     def __init__(self):
         self.camera = None  # (from, look, fov)
         self.meshes = []
+        self.cubes = []       # names of built-in unit cubes (Cube blocks)
+        self.spheres = []     # (name, radius) of analytic spheres (Sphere blocks)
         self.transforms = []  # (name, translate, scale, rotate_deg)
         self.materials = []   # (kind, name, dict)
         self.textures = []    # (kind, name, dict)
@@ -215,6 +222,8 @@ class Scene:
     @property
     def triangle_count(self) -> int:
         by_name = {m.name: m.triangle_count for m in self.meshes}
+        by_name.update({c: 12 for c in self.cubes})
+        by_name.update({n: 0 for n, _ in self.spheres})
         return sum(by_name[i[1]] for i in self.instances)
 
 
@@ -249,6 +258,10 @@ def write_scene(scene: Scene, path: str) -> str:
         out.append("\tmesh_normal_indices = " + _arr(m.nrm_idx.tolist(), str) + ";\n")
         out.append("\tmesh_normals = " + _arr(nrm, _f) + ";\n")
         out.append("End(Mesh);\n")
+    for name in scene.cubes:
+        out.append(f'Begin(Cube);\n\tname = "{name}";\nEnd(Cube);\n')
+    for name, radius in scene.spheres:
+        out.append(f'Begin(Sphere);\n\tname = "{name}";\n\tradius = {_f(radius)};\nEnd(Sphere);\n')
     for name, t, s, r in scene.transforms:
         out.append(f'Begin(Transform);\n\tname = "{name}";\n\ttranslate = {_vec(t)};\n\tscale = {_vec(s)};\n'
                    f'\trotate = {_vec(r)};\nEnd(Transform);\n')
@@ -398,6 +411,36 @@ def volumetric_scene(seed: int = 0) -> Scene:
     return s
 
 
+def spheres_scene(seed: int = 0) -> Scene:
+    rng = np.random.Generator(np.random.PCG64(seed))
+    s = cornell_scene(seed)
+    keep = {"tall_box", "short_box"}
+    s.instances = [i for i in s.instances if i[0] not in keep]
+    s.cubes = ["Geo_UnitCube"]
+    s.spheres = [("Geo_Sphere", 1.0), ("Geo_SmallSphere", 0.5)]
+    s.transforms.append(("cube_transform", (-0.4, -0.6, -0.35), (0.55, 0.8, 0.55), (0.0, float(rng.uniform(10, 40)), 0.0)))
+    s.materials.append(("DefaultMaterial", "cube_material", _lambert(rng.uniform(0.2, 0.9, 3))))
+    s.instances.append(("cube", "Geo_UnitCube", "cube_transform", "cube_material", None, False))
+    s.transforms.append(("glass_transform", (0.4, -0.62, 0.25), (0.38, 0.38, 0.38), (0, 0, 0)))
+    s.materials.append(("DefaultMaterial", "glass_material", {
+        "diffuse_albedo": [0.5, 0.5, 0.5], "specular_albedo": [1.0, 1.0, 1.0], "roughness_x": 0.031,
+        "roughness_y": 0.035, "ior_n": 1.55, "metalness": 0.0, "specular_weight": 1.0, "transmission_weight": 1.0}))
+    s.instances.append(("glass_sphere", "Geo_Sphere", "glass_transform", "glass_material", None, False))
+    s.transforms.append(("metal_transform", (-0.45, 0.45, -0.5), (0.5, 0.5, 0.5), (0, 30, 0)))
+    s.materials.append(("DefaultMaterial", "metal_material", {
+        "diffuse_albedo": list(rng.uniform(0.5, 0.95, 3)), "specular_albedo": [1.0, 1.0, 1.0],
+        "roughness_x": 0.2, "roughness_y": 0.2, "metalness": 1.0}))
+    s.instances.append(("metal_sphere", "Geo_SmallSphere", "metal_transform", "metal_material", None, False))
+    s.transforms.append(("bulb_transform", (0.55, 0.7, -0.45), (0.12, 0.12, 0.12), (0, 0, 0)))
+    s.materials.append(("LightMaterial", "bulb_material", {"light_color": [1.0, 0.8, 0.6], "intensity": 20.0}))
+    s.instances.append(("bulb", "Geo_Sphere", "bulb_transform", "bulb_material", None, False))
+    s.transforms.append(("air_transform", (0.0, 0.0, 0.5), (3.5, 3.5, 3.5), (0, 0, 0)))
+    s.volumes.append(("air_volume", "air_transform", (0.02, 0.02, 0.02), (0.9, 0.9, 0.9), 0.3, None))
+    s.materials.append(("DefaultMaterial", "air_boundary_material", {"ior_n": 1.0}))
+    s.instances.append(("air", "Geo_Sphere", "air_transform", "air_boundary_material", "air_volume", True))
+    return s
+
+
 def glossy_scene(seed: int = 0) -> Scene:
     """The Cornell-like scene with a rough GGX conductor tall box and a
     rough plastic-like (diffuse + specular) short box: every differentiated
@@ -431,6 +474,7 @@ SCENES = {
     "cornell": cornell_scene,
     "glossy": glossy_scene,
     "instanced": instanced_scene,
+    "spheres": spheres_scene,
     "volumetric": volumetric_scene,
 }
 
