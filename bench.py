@@ -19,6 +19,9 @@ Arms:
                      `ref_cuda`: the reference's own stage kernels rebuilt for
                      sm_100a on the same frame. `cpu_baseline`: the reference
                      built for the host on a bounded tile sample.
+                     `rmse_vs_fp64`: the profiled frame against the FP64
+                     oracle on a band of tiles, beside the reference's own
+                     float error there.
   --impl reference   the reference's own path tracer compiled for the host
                      (oracle/_ref), all host threads, on a bounded tile
                      sample of the same frame.
@@ -413,6 +416,7 @@ def run_ours(args):
     lib.ymrt_set_profiling(ctx.h, 1)
     _, pst = scene.render(setting, frame_index=10_000 + rank, out=image)
     lib.ymrt_set_profiling(ctx.h, 0)
+    profiled_image = image.cpu().numpy() if rank == 0 else None
 
     # End to end through the C ABI: upload the scene from host memory, render,
     # read the image back -- every step.
@@ -482,6 +486,9 @@ def run_ours(args):
             if not args.no_cpu_baseline:
                 result["cpu_baseline"] = cpu_baseline(path, perm, W, H, spp, wl["depth"], budget_s=args.cpu_budget,
                                                       volume=wl.get("volume", False))
+            if not args.no_fp64:
+                result["rmse_vs_fp64"] = fp64_check(path, perm, W, H, spp, wl["depth"], 10_000, profiled_image,
+                                                    volume=wl.get("volume", False))
     if world > 1:
         import torch.distributed as dist
         dist.barrier()
@@ -489,6 +496,35 @@ def run_ours(args):
     scene.close()
     ctx.close()
     return result
+
+
+def fp64_check(path, perm, W, H, spp, depth, frame, image, volume=False, n_tiles=40):
+    """Image error of the profiled frame against the FP64 oracle (the
+    reference's algorithm computed in double, oracle/_ref/libymrt_ref64.so)
+    on the same samples, over a band of tiles through the middle of the frame,
+    beside the error of the reference's own float arithmetic (the float
+    oracle) on the same band."""
+    try:
+        from oracle import ref
+        if not (ref.available() and ref.available64()):
+            return {"unavailable": "oracle/_ref/libymrt_ref64.so not built"}
+        total = ((W + 15) // 16) * ((H + 15) // 16)
+        tb = max(0, total // 2 - n_tiles // 2)
+        te = min(total, tb + n_tiles)
+        imgs = []
+        for fp64 in (True, False):
+            r = ref.RefScene(path, perm, W, H, fp64=fp64)
+            r.set_settings(spp=spp, ray_depth=depth, volume=int(volume))
+            imgs.append(r.render_frame(frame, tb, te))
+            r.close()
+        c, b = imgs
+        cov = c[..., 3] > 0
+        ours = np.sqrt(np.mean((image[..., :3][cov].astype(np.float64) - c[..., :3][cov]) ** 2))
+        theirs = np.sqrt(np.mean((b[..., :3][cov].astype(np.float64) - c[..., :3][cov]) ** 2))
+    except Exception as e:  # noqa: BLE001 - reported, not fatal for our own measurement
+        return {"unavailable": f"{type(e).__name__}: {e}"}
+    return {"rmse": float(f"{ours:.4g}"), "rmse_reference_float": float(f"{theirs:.4g}"), "pixels": int(cov.sum()),
+            "spp": spp, "sample": f"tiles {tb}..{te - 1} (16x16 each) of frame {frame}, same samples on all three"}
 
 
 def ref_cuda_timing(path, perm, W, H, spp, depth, pst, frames=2, volume=False):
@@ -626,6 +662,7 @@ def main(argv=None):
     ap.add_argument("--cpu-budget", type=float, default=12.0, help="seconds of CPU work per reference sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-ref-cuda", action="store_true", help="skip timing the reference's own CUDA kernels")
+    ap.add_argument("--no-fp64", action="store_true", help="skip the image check against the FP64 oracle")
     ap.add_argument("--autotune", action="store_true", help="batch workload: tune the wave options first")
     args = ap.parse_args(argv)
     if args.warmup < 3:

@@ -391,6 +391,145 @@ def build(arg_order: str = "ltr", force: bool = False, jobs: int = 8) -> str:
     return LIB
 
 
+# ---------------------------------------------------------------------------
+# FP64 oracle: the same reference sources and harness with every float
+# computation done in double precision, for the converged-image error of the
+# float renderers (the reference's and ymrt_b200's) at equal spp.
+#
+# The build-time copy (oracle/_ref/gen64) is made by rewriting tokens, not by
+# editing the algorithm: ``float`` becomes ``double``; glm's float vector and
+# matrix types become their double counterparts; float literals lose their
+# ``f`` suffix (so glm's templates see one scalar type); the two places that
+# reinterpret a float's bits (NextFloatUp/NextFloatDown, src/MathCommon.h:263-
+# 297, and Ray::SetInvalid/Invalid, src/Ray.h:36-52) are rewritten for a
+# 64-bit double (std::nextafter, an all-ones 64-bit pattern). The scene is
+# still parsed with std::stof, so both precisions see the same geometry. The
+# sampler draws, the light selection and every estimator step are the
+# reference's; only rounding differs.
+
+LIB64 = os.path.join(OUT, "libymrt_ref64.so")
+_CODE_EXT = (".h", ".cuh", ".cu", ".cpp", ".hpp")
+_FLOAT_LIT = re.compile(r"(?<![\w.])((?:\d+\.\d*|\.\d+)(?:[eE][+-]?\d+)?|\d+[eE][+-]?\d+)[fF](?![\w.])")
+_NEXT_UP = re.compile(r"inline double NextFloatUp\(double f\)\s*\{.*?return UintToFloat\(ui\);\s*\}", re.S)
+_NEXT_DOWN = re.compile(r"inline double NextFloatDown\(double f\)\s*\{.*?return UintToFloat\(ui\);\s*\}", re.S)
+_BITS32 = re.compile(r"uint32_t& ui = \*\(\(uint32_t\*\)\(&f\)\);(\s*)ui = 0xFFFFFFFF;")
+_CHECK32 = re.compile(r"uint32_t& ui = \*\(\(uint32_t\*\)\(&f\)\);(\s*)return ui == 0xFFFFFFFF;")
+
+
+def to_fp64(text: str) -> tuple[str, dict]:
+    """The token rewrite described above; returns the text and per-rule counts."""
+    n = {}
+    text, n["float"] = re.subn(r"\bfloat\b", "double", text)
+    text, n["glm types"] = re.subn(r"\bglm::(vec|mat)([234])\b", r"glm::d\1\2", text)
+    text, n["literals"] = _FLOAT_LIT.subn(r"\1", text)
+    text, a = _NEXT_UP.subn("inline double NextFloatUp(double f) { return std::isinf(f) && f > 0.0 ? f : "
+                            "std::nextafter(f == -0.0 ? 0.0 : f, INFINITY); }", text)
+    text, b = _NEXT_DOWN.subn("inline double NextFloatDown(double f) { return std::isinf(f) && f < 0.0 ? f : "
+                              "std::nextafter(f == 0.0 ? -0.0 : f, -INFINITY); }", text)
+    n["next float"] = a + b
+    text, a = _BITS32.subn(r"uint64_t& ui = *((uint64_t*)(&f));\1ui = 0xFFFFFFFFFFFFFFFFull;", text)
+    text, b = _CHECK32.subn(r"uint64_t& ui = *((uint64_t*)(&f));\1return ui == 0xFFFFFFFFFFFFFFFFull;", text)
+    n["invalid bits"] = a + b
+    return text, n
+
+
+def _fp64_tree() -> str:
+    """Writes oracle/_ref/gen64: the rewritten reference src/ tree (with the
+    sequenced Shading.cu / RandomSampler.cuh / VolumeEval.cuh of the float
+    oracle in place of the originals), the harness and its shims."""
+    shading_source("ltr")  # the float oracle's sequenced copies, rewritten below
+    gen = os.path.join(OUT, "gen")
+    root = os.path.join(OUT, "gen64")
+    src_root = os.path.join(REF, "src")
+    totals = {}
+    for d, _, files in os.walk(src_root):
+        for name in files:
+            if not name.endswith(_CODE_EXT):
+                continue
+            rel = os.path.relpath(os.path.join(d, name), src_root)
+            origin = os.path.join(d, name)
+            if rel in ("Shading.cu", "RandomSampler.cuh", "VolumeEval.cuh"):
+                origin = os.path.join(gen, rel)
+            with open(origin, "r", encoding="utf-8", errors="replace") as f:
+                text, n = to_fp64(f.read())
+            for k, v in n.items():
+                totals[k] = totals.get(k, 0) + v
+            dst = os.path.join(root, "src", rel)
+            os.makedirs(os.path.dirname(dst), exist_ok=True)
+            with open(dst, "w") as f:
+                f.write(text)
+    for rel in ("ref_harness.cpp", "ref_prepare.h", "ref_stubs.cpp", os.path.join("shims", "ymrt_ref_prelude.h"),
+                os.path.join("shims", "ppl.h")):
+        with open(os.path.join(HERE, rel)) as f:
+            text, _ = to_fp64(f.read())
+        dst = os.path.join(root, rel)
+        os.makedirs(os.path.dirname(dst), exist_ok=True)
+        with open(dst, "w") as f:
+            f.write(text)
+    with open(os.path.join(root, "rewrites.txt"), "w") as f:
+        f.write(", ".join(f"{k}: {v}" for k, v in sorted(totals.items())) + "\n")
+    return root
+
+
+def _fp64_includes(root: str):
+    return [
+        "-include", os.path.join(root, "shims", "ymrt_ref_prelude.h"),
+        "-I" + os.path.join(root, "shims"), "-I" + os.path.join(HERE, "shims"),
+        "-I" + root, "-I" + os.path.join(root, "src"), "-I" + os.path.join(root, "src", "core"),
+        "-I" + os.path.join(REF, "external", "glm"),
+        "-I" + os.path.join(REF, "external", "glad", "include"),
+        "-I" + os.path.join(REF, "external", "image_lib"),
+        "-I" + os.path.join(REF, "external", "assimp-5.1.0", "include"),
+        "-I/usr/local/cuda/include",
+    ]
+
+
+def build_fp64(force: bool = False, jobs: int = 8) -> str:
+    """Builds oracle/_ref/libymrt_ref64.so (exports ymref_*, with double in
+    place of float in every signature)."""
+    if not os.path.isdir(os.path.join(REF, "src")):
+        if os.path.exists(LIB64):
+            return LIB64
+        raise FileNotFoundError(f"reference sources not found at {REF} and no prebuilt {LIB64}")
+    os.makedirs(OUT, exist_ok=True)
+    stamp_file = os.path.join(OUT, "stamp64")
+    stamp = _stamp("fp64")
+    if not force and os.path.exists(LIB64) and os.path.exists(stamp_file):
+        with open(stamp_file) as f:
+            if f.read().strip() == stamp:
+                return LIB64
+    root = _fp64_tree()
+    obj_dir = os.path.join(OUT, "obj64")
+    os.makedirs(obj_dir, exist_ok=True)
+    inc = _fp64_includes(root)
+    jobs_list = [(os.path.join(root, s), os.path.join(obj_dir, os.path.basename(s) + ".o"), []) for s in HOST_SOURCES]
+    jobs_list.append((os.path.join(root, "ref_harness.cpp"), os.path.join(obj_dir, "ref_harness.o"),
+                      [f'-DYMRT_SHADING_SOURCE="{os.path.join(root, "src", "Shading.cu")}"']))
+    jobs_list.append((os.path.join(root, "ref_stubs.cpp"), os.path.join(obj_dir, "ref_stubs.o"), []))
+    procs, objs = [], []
+    for src, obj, extra in jobs_list:
+        # assimp's material getters are called with the (now double) colour
+        # arrays of the model importer; its double-precision mode types them
+        cmd = ["g++"] + CXXFLAGS + ["-DASSIMP_DOUBLE_PRECISION"] + extra + inc + ["-c", src, "-o", obj]
+        procs.append((src, subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT)))
+        objs.append(obj)
+        while len([p for _, p in procs if p.poll() is None]) >= jobs:
+            procs[0][1].wait()
+    for src, p in procs:
+        out, _ = p.communicate()
+        if p.returncode != 0:
+            raise RuntimeError(f"fp64 oracle build failed for {src}:\n{out.decode(errors='replace')[-6000:]}")
+    tmp = LIB64 + ".tmp"
+    cmd = ["g++", "-shared", "-pthread", "-o", tmp] + objs + ["-Wl,--no-undefined", "-Wl,-Bsymbolic"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("fp64 oracle link failed:\n" + r.stdout[-4000:] + r.stderr[-4000:])
+    os.replace(tmp, LIB64)
+    with open(stamp_file, "w") as f:
+        f.write(stamp)
+    return LIB64
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--arg-order", choices=["ltr", "native"], default="ltr")
@@ -398,6 +537,7 @@ def main(argv=None):
     ap.add_argument("--gpu", action="store_true", help="also build the reference's kernels for sm_100a")
     a = ap.parse_args(argv)
     print(build(a.arg_order, a.force))
+    print(build_fp64(a.force))
     if a.gpu:
         print(build_gpu(a.force))
         print(build_gpu(a.force, exact=True))

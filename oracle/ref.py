@@ -14,8 +14,10 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_ref", "libymrt_ref.so")
+LIB64_PATH = os.path.join(HERE, "_ref", "libymrt_ref64.so")
 
 _lib = None
+_lib64 = None
 
 
 class Settings(ctypes.Structure):
@@ -28,8 +30,42 @@ class Settings(ctypes.Structure):
     ]
 
 
+class Settings64(ctypes.Structure):
+    _fields_ = [(n, t) for n, t in Settings._fields_[:-1]] + [("indirect_limit", ctypes.c_double)]
+
+
 def available() -> bool:
     return os.path.exists(LIB_PATH)
+
+
+def _bind(L, settings_type):
+    vp, i, u64 = ctypes.c_void_p, ctypes.c_int, ctypes.c_uint64
+    L.ymref_halton_table_size.restype = ctypes.c_size_t
+    L.ymref_scene_load.restype = vp
+    L.ymref_scene_load.argtypes = [ctypes.c_char_p, vp, ctypes.c_size_t, i, i]
+    L.ymref_scene_free.argtypes = [vp]
+    L.ymref_set_settings.argtypes = [vp, ctypes.POINTER(settings_type)]
+    for name in ("ymref_scene_counts", "ymref_instances", "ymref_transforms"):
+        getattr(L, name).argtypes = [vp, vp] if name != "ymref_transforms" else [vp, vp, vp]
+    L.ymref_geometry_triangle_count.restype = ctypes.c_int64
+    L.ymref_geometry_triangle_count.argtypes = [vp, ctypes.c_uint32]
+    L.ymref_geometry_triangles.argtypes = [vp, ctypes.c_uint32, vp]
+    L.ymref_geometry_kind.argtypes = [vp, ctypes.c_uint32, vp]
+    L.ymref_mesh_corners.argtypes = [vp, ctypes.c_uint32, vp]
+    L.ymref_lights.argtypes = [vp, vp, vp, vp]
+    L.ymref_camera_bytes.argtypes = [vp, vp, i]
+    L.ymref_scene_records.argtypes = [vp, i, vp, i]
+    L.ymref_bvh_depths.argtypes = [vp, vp]
+    L.ymref_sobol_matrices.restype = ctypes.c_size_t
+    L.ymref_sobol_matrices.argtypes = [vp, ctypes.c_size_t]
+    L.ymref_trace.argtypes = [vp, i, vp, vp, vp, vp, vp, vp, vp, vp, vp]
+    L.ymref_occluded.argtypes = [vp, i, vp, vp, vp, vp]
+    L.ymref_halton.argtypes = [vp, i, vp, vp, vp, i, vp, vp, vp]
+    L.ymref_render_frame.argtypes = [vp, i, i, i, i, i, vp]
+    L.ymref_last_render_seconds.restype = ctypes.c_double
+    L.ymref_last_render_seconds.argtypes = [vp]
+    L.ymref_accumulate.argtypes = [vp, vp, i, i, i]
+    L.ymref_query_counts.argtypes = [vp, i]
 
 
 def lib():
@@ -39,35 +75,27 @@ def lib():
             from . import build_ref  # noqa: F401  (only when sources are present)
             build_ref.build()
         L = ctypes.CDLL(LIB_PATH)
-        vp, i, u64 = ctypes.c_void_p, ctypes.c_int, ctypes.c_uint64
-        L.ymref_halton_table_size.restype = ctypes.c_size_t
-        L.ymref_scene_load.restype = vp
-        L.ymref_scene_load.argtypes = [ctypes.c_char_p, vp, ctypes.c_size_t, i, i]
-        L.ymref_scene_free.argtypes = [vp]
-        L.ymref_set_settings.argtypes = [vp, ctypes.POINTER(Settings)]
-        for name in ("ymref_scene_counts", "ymref_instances", "ymref_transforms"):
-            getattr(L, name).argtypes = [vp, vp] if name != "ymref_transforms" else [vp, vp, vp]
-        L.ymref_geometry_triangle_count.restype = ctypes.c_int64
-        L.ymref_geometry_triangle_count.argtypes = [vp, ctypes.c_uint32]
-        L.ymref_geometry_triangles.argtypes = [vp, ctypes.c_uint32, vp]
-        L.ymref_geometry_kind.argtypes = [vp, ctypes.c_uint32, vp]
-        L.ymref_mesh_corners.argtypes = [vp, ctypes.c_uint32, vp]
-        L.ymref_lights.argtypes = [vp, vp, vp, vp]
-        L.ymref_camera_bytes.argtypes = [vp, vp, i]
-        L.ymref_scene_records.argtypes = [vp, i, vp, i]
-        L.ymref_bvh_depths.argtypes = [vp, vp]
-        L.ymref_sobol_matrices.restype = ctypes.c_size_t
-        L.ymref_sobol_matrices.argtypes = [vp, ctypes.c_size_t]
-        L.ymref_trace.argtypes = [vp, i, vp, vp, vp, vp, vp, vp, vp, vp, vp]
-        L.ymref_occluded.argtypes = [vp, i, vp, vp, vp, vp]
-        L.ymref_halton.argtypes = [vp, i, vp, vp, vp, i, vp, vp, vp]
-        L.ymref_render_frame.argtypes = [vp, i, i, i, i, i, vp]
-        L.ymref_last_render_seconds.restype = ctypes.c_double
-        L.ymref_last_render_seconds.argtypes = [vp]
-        L.ymref_accumulate.argtypes = [vp, vp, i, i, i]
-        L.ymref_query_counts.argtypes = [vp, i]
+        _bind(L, Settings)
         _lib = L
     return _lib
+
+
+def available64() -> bool:
+    return os.path.exists(LIB64_PATH)
+
+
+def lib64():
+    """The FP64 build of the oracle (every float of the reference and the
+    harness computed in double; see build_ref.build_fp64)."""
+    global _lib64
+    if _lib64 is None:
+        if not os.path.exists(LIB64_PATH):
+            from . import build_ref  # noqa: F401  (only when sources are present)
+            build_ref.build_fp64()
+        L = ctypes.CDLL(LIB64_PATH)
+        _bind(L, Settings64)
+        _lib64 = L
+    return _lib64
 
 
 def _p(a: np.ndarray):
@@ -85,8 +113,12 @@ def sobol_matrices() -> np.ndarray:
 class RefScene:
     """One scene loaded and prepared by the reference's own scene module."""
 
-    def __init__(self, path: str, halton_perm: np.ndarray, width: int, height: int):
-        L = lib()
+    def __init__(self, path: str, halton_perm: np.ndarray, width: int, height: int, fp64: bool = False):
+        """fp64: load it into the FP64 build (renders return float64 images)."""
+        L = lib64() if fp64 else lib()
+        self._L = L
+        self._f = np.float64 if fp64 else np.float32
+        self._settings = Settings64 if fp64 else Settings
         perm = np.ascontiguousarray(halton_perm, dtype=np.uint32)
         self.width, self.height = width, height
         self.h = L.ymref_scene_load(path.encode(), _p(perm), perm.size, width, height)
@@ -96,7 +128,7 @@ class RefScene:
 
     def close(self):
         if self.h:
-            lib().ymref_scene_free(self.h)
+            self._L.ymref_scene_free(self.h)
             self.h = None
 
     def __del__(self):
@@ -107,69 +139,69 @@ class RefScene:
 
     def set_settings(self, spp=1, ray_depth=8, sampler_type=1, shape_light=1, distant_light=0, volume=0,
                      env_light=0, russian_roulette=0, indirect_clamp=0, indirect_limit=10.0):
-        s = Settings(spp, ray_depth, sampler_type, shape_light, distant_light, volume, env_light,
+        s = self._settings(spp, ray_depth, sampler_type, shape_light, distant_light, volume, env_light,
                      russian_roulette, indirect_clamp, indirect_limit)
-        lib().ymref_set_settings(self.h, ctypes.byref(s))
+        self._L.ymref_set_settings(self.h, ctypes.byref(s))
 
     def counts(self) -> dict:
         out = np.zeros(5, np.uint32)
-        lib().ymref_scene_counts(self.h, _p(out))
+        self._L.ymref_scene_counts(self.h, _p(out))
         return dict(zip(["instances", "geometries", "lights", "transforms", "materials"], out.tolist()))
 
     def instances(self) -> np.ndarray:
         n = self.counts()["instances"]
         out = np.zeros((n, 6), np.uint32)
-        lib().ymref_instances(self.h, _p(out))
+        self._L.ymref_instances(self.h, _p(out))
         return out
 
     def geometry_triangles(self, g: int) -> np.ndarray:
-        n = lib().ymref_geometry_triangle_count(self.h, g)
+        n = self._L.ymref_geometry_triangle_count(self.h, g)
         out = np.zeros((max(n, 0), 3), np.uint32)
         if n > 0:
-            lib().ymref_geometry_triangles(self.h, g, _p(out))
+            self._L.ymref_geometry_triangles(self.h, g, _p(out))
         return out
 
     def geometries(self) -> np.ndarray:
         """(type, radius) per geometry: type 0 a triangle mesh, 1 a sphere."""
         n = self.counts()["geometries"]
-        out = np.zeros((n, 2), np.float32)
-        r = np.zeros(1, np.float32)
+        out = np.zeros((n, 2), self._f)
+        r = np.zeros(1, self._f)
         for g in range(n):
-            out[g, 0] = lib().ymref_geometry_kind(self.h, g, _p(r))
+            out[g, 0] = self._L.ymref_geometry_kind(self.h, g, _p(r))
             out[g, 1] = r[0]
         return out
 
     def mesh_corners(self, g: int) -> np.ndarray:
-        n = lib().ymref_geometry_triangle_count(self.h, g)
-        out = np.zeros((3 * max(n, 0), 8), np.float32)
+        n = self._L.ymref_geometry_triangle_count(self.h, g)
+        out = np.zeros((3 * max(n, 0), 8), self._f)
         if n > 0:
-            lib().ymref_mesh_corners(self.h, g, _p(out))
+            self._L.ymref_mesh_corners(self.h, g, _p(out))
         return out
 
     def lights(self):
         n = self.counts()["lights"]
         ids = np.zeros((n, 2), np.uint32)
-        pa = np.zeros((n, 2), np.float32)
-        tab = np.zeros(n, np.float32)
-        lib().ymref_lights(self.h, _p(ids), _p(pa), _p(tab))
+        pa = np.zeros((n, 2), self._f)
+        tab = np.zeros(n, self._f)
+        self._L.ymref_lights(self.h, _p(ids), _p(pa), _p(tab))
         return ids, pa, tab
 
     def transforms(self):
         n = self.counts()["transforms"]
-        fwd = np.zeros((n, 16), np.float32)
-        inv = np.zeros((n, 16), np.float32)
-        lib().ymref_transforms(self.h, _p(fwd), _p(inv))
+        fwd = np.zeros((n, 16), self._f)
+        inv = np.zeros((n, 16), self._f)
+        self._L.ymref_transforms(self.h, _p(fwd), _p(inv))
         return fwd, inv
 
     def camera_bytes(self) -> bytes:
         buf = np.zeros(512, np.uint8)
-        n = lib().ymref_camera_bytes(self.h, _p(buf), buf.size)
+        n = self._L.ymref_camera_bytes(self.h, _p(buf), buf.size)
         return buf[:n].tobytes()
 
     def bvh_depths(self) -> np.ndarray:
         """Depth of each mesh's binary BVH, then of the top-level BVH."""
         out = np.zeros(self.counts()["geometries"] + 1, np.uint32)
-        lib().ymref_bvh_depths(self.h, _p(out))
+        self._L.ymref_bvh_depths(self.h, _p(out))
         return out
 
     def records(self, kind: str) -> np.ndarray:
@@ -177,33 +209,33 @@ class RefScene:
         reference structs) or textures (13 words each), one row per record."""
         what = {"materials": 0, "volumes": 1, "distant_lights": 2, "textures": 3}[kind]
         width = {"materials": 39, "volumes": 9, "distant_lights": 8, "textures": 13}[kind]
-        n = lib().ymref_scene_records(self.h, what, None, 0)
+        n = self._L.ymref_scene_records(self.h, what, None, 0)
         out = np.zeros(max(n, 0), np.uint32)
         if n > 0:
-            lib().ymref_scene_records(self.h, what, _p(out), out.size)
+            self._L.ymref_scene_records(self.h, what, _p(out), out.size)
         return out.reshape(-1, width)
 
     def trace(self, origins, dirs, last_hit=None) -> dict:
-        o = np.ascontiguousarray(origins, np.float32)
-        d = np.ascontiguousarray(dirs, np.float32)
+        o = np.ascontiguousarray(origins, self._f)
+        d = np.ascontiguousarray(dirs, self._f)
         n = o.shape[0]
         lh = None if last_hit is None else np.ascontiguousarray(last_hit, np.uint32)
         inst = np.zeros(n, np.uint32)
         tri = np.zeros(n, np.uint32)
-        t = np.zeros(n, np.float32)
-        bary = np.zeros((n, 3), np.float32)
+        t = np.zeros(n, self._f)
+        bary = np.zeros((n, 3), self._f)
         back = np.zeros(n, np.int32)
         nearby = np.zeros(n, np.int32)
-        lib().ymref_trace(self.h, n, _p(o), _p(d), None if lh is None else _p(lh), _p(inst), _p(tri), _p(t),
+        self._L.ymref_trace(self.h, n, _p(o), _p(d), None if lh is None else _p(lh), _p(inst), _p(tri), _p(t),
                           _p(bary), _p(back), _p(nearby))
         return {"inst": inst, "tri": tri, "t": t, "bary": bary, "back": back, "nearby": nearby}
 
     def occluded(self, origins, dirs, tmax) -> np.ndarray:
-        o = np.ascontiguousarray(origins, np.float32)
-        d = np.ascontiguousarray(dirs, np.float32)
-        tm = np.ascontiguousarray(tmax, np.float32)
+        o = np.ascontiguousarray(origins, self._f)
+        d = np.ascontiguousarray(dirs, self._f)
+        tm = np.ascontiguousarray(tmax, self._f)
         out = np.zeros(o.shape[0], np.int32)
-        lib().ymref_occluded(self.h, o.shape[0], _p(o), _p(d), _p(tm), _p(out))
+        self._L.ymref_occluded(self.h, o.shape[0], _p(o), _p(d), _p(tm), _p(out))
         return out
 
     def halton(self, px, py, sample, n_dims: int):
@@ -212,22 +244,22 @@ class RefScene:
         sm = np.ascontiguousarray(sample, np.int32)
         n = px.size
         idx = np.zeros(n, np.uint64)
-        off = np.zeros((n, 2), np.float32)
-        dims = np.zeros((n, n_dims), np.float32)
-        lib().ymref_halton(self.h, n, _p(px), _p(py), _p(sm), n_dims, _p(idx), _p(off), _p(dims))
+        off = np.zeros((n, 2), self._f)
+        dims = np.zeros((n, n_dims), self._f)
+        self._L.ymref_halton(self.h, n, _p(px), _p(py), _p(sm), n_dims, _p(idx), _p(off), _p(dims))
         return idx, off, dims
 
     def render_frame(self, frame_index: int = 1, tile_begin: int = 0, tile_end: int = 0,
                      wave_capacity: int = 1 << 18, threads: int | None = None) -> np.ndarray:
-        out = np.zeros((self.height, self.width, 4), np.float32)
+        out = np.zeros((self.height, self.width, 4), self._f)
         threads = threads or os.cpu_count() or 1
-        rc = lib().ymref_render_frame(self.h, frame_index, tile_begin, tile_end, wave_capacity, threads, _p(out))
+        rc = self._L.ymref_render_frame(self.h, frame_index, tile_begin, tile_end, wave_capacity, threads, _p(out))
         if rc != 0:
             raise RuntimeError(f"reference render failed ({rc})")
         return out
 
     def last_render_seconds(self) -> float:
-        return lib().ymref_last_render_seconds(self.h)
+        return self._L.ymref_last_render_seconds(self.h)
 
 
 def query_counts(reset: bool = True) -> tuple[int, int]:
