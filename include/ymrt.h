@@ -214,6 +214,17 @@ int ymrt_render_backward(ymrt_context* ctx, const ymrt_job* jobs, int n_jobs, fl
  * diffuse albedo r, g, b and roughness (stored as alpha_x and alpha_y). Light
  * materials are skipped (set) or read as zeros (get). */
 int ymrt_scene_set_material_params(ymrt_scene* scene, uint32_t first, uint32_t count, const float* params);
+/* Attaches a density grid to texture node `texture_index` (replacing that
+ * node; no counterpart in the reference, whose texture graph has no grid): a
+ * volume whose density texture is that node then reads the grid. values holds
+ * nx*ny*nz floats in host memory, x fastest, sampled at cell centres of the
+ * volume's object-space box [-0.5, 0.5]^3, read trilinearly with clamped
+ * edges; store_half != 0 keeps them as float16 (rounded to nearest). The
+ * node's upper bound, which sets the delta-tracking majorant, is the grid's
+ * maximum. Values must be finite; calling it again replaces the grid. */
+int ymrt_scene_set_density_grid(ymrt_scene* scene, uint32_t texture_index, int nx, int ny, int nz,
+                                const float* values, int store_half);
+
 int ymrt_scene_get_material_params(const ymrt_scene* scene, uint32_t first, uint32_t count, float* params);
 
 /* Renders n_jobs renders (scenes, resolutions, spp and settings may all
@@ -246,6 +257,10 @@ int ymrt_accumulate(ymrt_scene* scene, const float* noise_rgba, float* acc_rgba,
 /* ---- known-answer entry points (host buffers) ---- */
 int ymrt_debug_trace(ymrt_scene* scene, int n, const float* origin, const float* dir, const uint32_t* last_hit,
                      uint32_t* inst, uint32_t* tri, float* t, float* bary, int* back, int* nearby);
+/* Value of texture node `texture_index` at n object-space points (3 floats
+ * each; host buffers), as the media read it: known-answer checks of grid and
+ * fBm nodes. */
+int ymrt_debug_density(ymrt_scene* scene, uint32_t texture_index, int n, const float* points, float* out);
 int ymrt_debug_occluded(ymrt_scene* scene, int n, const float* origin, const float* dir, const float* tmax,
                         int* occluded);
 int ymrt_debug_halton(ymrt_scene* scene, int n, const int* px, const int* py, const int* sample, int n_dims,

@@ -130,6 +130,8 @@ def library():
     L.ymrt_job_path_count.argtypes = [ctypes.POINTER(Job)]
     L.ymrt_scene_set_material_params.argtypes = [vp, ctypes.c_uint32, ctypes.c_uint32, vp]
     L.ymrt_scene_get_material_params.argtypes = [vp, ctypes.c_uint32, ctypes.c_uint32, vp]
+    L.ymrt_scene_set_density_grid.argtypes = [vp, ctypes.c_uint32, i, i, i, vp, i]
+    L.ymrt_debug_density.argtypes = [vp, ctypes.c_uint32, i, vp, vp]
     L.ymrt_render_forward.argtypes = [vp, ctypes.POINTER(RenderSetting), i, vp, i, ctypes.POINTER(Stats)]
     L.ymrt_render_tiles.argtypes = [vp, ctypes.POINTER(RenderSetting), i, i, i, vp, i, ctypes.POINTER(Stats)]
     L.ymrt_accumulate.argtypes = [vp, vp, vp, i]
@@ -302,6 +304,22 @@ class Scene:
     def set_material_params(self, params: np.ndarray, first: int = 0) -> None:
         p = np.ascontiguousarray(params, dtype=np.float32).reshape(-1, 4)
         _check(library().ymrt_scene_set_material_params(self.h, first, p.shape[0], _p(p)), self.ctx.h)
+
+    def set_density_grid(self, texture_index: int, values: np.ndarray, half: bool = False) -> None:
+        """Attaches a density grid to texture node `texture_index`: values has
+        shape (nz, ny, nx) over the volume's object-space box [-0.5, 0.5]^3."""
+        v = np.ascontiguousarray(values, dtype=np.float32)
+        if v.ndim != 3:
+            raise ValueError("density grid must be a (nz, ny, nx) array")
+        nz, ny, nx = v.shape
+        _check(library().ymrt_scene_set_density_grid(self.h, texture_index, nx, ny, nz, _p(v), int(half)), self.ctx.h)
+
+    def density(self, texture_index: int, points) -> np.ndarray:
+        """Texture node `texture_index` at object-space points (n, 3), on the device."""
+        p = np.ascontiguousarray(points, np.float32).reshape(-1, 3)
+        out = np.zeros(p.shape[0], np.float32)
+        _check(library().ymrt_debug_density(self.h, texture_index, p.shape[0], _p(p), _p(out)), self.ctx.h)
+        return out
 
     def set_sobol_matrices(self, matrices: np.ndarray) -> None:
         """Generator matrices for the Sobol sampler (4096 x 32 uint32)."""

@@ -1,11 +1,14 @@
 // C ABI of ymrt_b200 (include/ymrt.h): contexts, scene upload, the frame
 // loop that drives the wavefront kernels, and the known-answer entry points.
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <functional>
+#include <map>
 #include <memory>
 #include <mutex>
 #include <new>
@@ -192,6 +195,8 @@ struct ymrt_scene {
   ymrt_context* ctx = nullptr;
   DeviceScene dev{};
   std::vector<Material> materials;  // host copy (material parameters can be updated)
+  std::vector<Texture> textures;    // host copy (grid nodes can be attached)
+  std::map<uint32_t, std::unique_ptr<DeviceBuffer>> grids;  // grid values per texture node
   std::vector<std::unique_ptr<DeviceBuffer>> buffers;
   int width = 0, height = 0;
   uint64_t triangles = 0;
@@ -503,6 +508,7 @@ int ymrt_scene_upload(ymrt_context* ctx, const ymrt_host_scene* hs, const uint32
   UP(s.shape_light_table, shape_light_table);
   UP(s.volumes, volumes);
   UP(s.textures, textures);
+  sc->textures = s.textures;
   {
     std::vector<uint8_t> buckets(s.instances.size());
     for (size_t i = 0; i < s.instances.size(); ++i) buckets[i] = (uint8_t)shading_bucket(s, s.instances[i]);
@@ -701,7 +707,7 @@ int run_batch(ymrt_context* ctx, const BatchMemory& M, std::vector<JobDesc>& job
         (uintptr_t)M.pool[0].ray_o, (uintptr_t)M.pool[1].ray_o, (uintptr_t)M.hits.bary_t, (uintptr_t)M.ctl,
         (uintptr_t)M.jobs, (uintptr_t)M.counters, (uintptr_t)jobs.size(), (uintptr_t)o.volumes,
         (uintptr_t)o.sort_hits, (uintptr_t)o.defer_shadows, (uintptr_t)o.shadow_queue.o, M.capacity,
-        (uintptr_t)o.spheres,
+        (uintptr_t)o.features,
         (uintptr_t)o.adjoint, (uintptr_t)o.grads, o.grad_materials};
     if (ctx->graph_key != key) {
       ctx->drop_graph();
@@ -817,11 +823,14 @@ int finish_batch(ymrt_context* ctx, const BatchResult& r, ymrt_stats* stats) {
   return YMRT_OK;
 }
 
-// Whether any of the batch's scenes holds sphere geometry.
-bool any_spheres(const DeviceScene* scenes, size_t n) {
-  for (size_t i = 0; i < n; ++i)
-    if (scenes[i].sphere_count != 0) return true;
-  return false;
+// The features (kFeatSpheres, kFeatGrids) any of the batch's scenes uses.
+uint32_t batch_features(const DeviceScene* scenes, size_t n) {
+  uint32_t f = 0;
+  for (size_t i = 0; i < n; ++i) {
+    if (scenes[i].sphere_count != 0) f |= kFeatSpheres;
+    if (scenes[i].grid_count != 0) f |= kFeatGrids;
+  }
+  return f;
 }
 
 // Wave options for a batch: media kernels when any job scatters in media;
@@ -886,7 +895,7 @@ int ymrt_render_tiles(ymrt_scene* sc, const ymrt_render_setting* setting, int fr
   if ((rc = context_memory(ctx, 1, &M)) != YMRT_OK) return rc;
   WaveOptions opt;
   if ((rc = batch_options(ctx, jobs, &opt)) != YMRT_OK) return rc;
-  opt.spheres = any_spheres(&scene, 1);
+  opt.features = batch_features(&scene, 1);
   jobs[0].scene_slot = 0;
   if ((e = upload_constants(&scene, 1, ctx->primes.data(), ctx->prime_sums.data(), st)) != cudaSuccess)
     return ctx->cuda_fail(e, "uploading constants");
@@ -949,7 +958,7 @@ int ymrt_render_batch(ymrt_context* ctx, const ymrt_job* jobs_in, int n_jobs, ym
     const std::vector<DeviceScene> slots = assign_slots(jobs, js, ks);
     WaveOptions opt;
     if ((rc = batch_options(ctx, jobs, &opt)) != YMRT_OK) return rc;
-    opt.spheres = any_spheres(slots.data(), slots.size());
+    opt.features = batch_features(slots.data(), slots.size());
     if ((e = upload_constants(slots.data(), (uint32_t)slots.size(), ctx->primes.data(), ctx->prime_sums.data(), st)) !=
         cudaSuccess)
       return ctx->cuda_fail(e, "uploading constants");
@@ -1013,7 +1022,7 @@ int ymrt_render_backward(ymrt_context* ctx, const ymrt_job* jobs_in, int n_jobs,
   if (rc != YMRT_OK) return rc;
   WaveOptions opt;
   opt.adjoint = true;
-  opt.spheres = any_spheres(slots.data(), slots.size());
+  opt.features = batch_features(slots.data(), slots.size());
   opt.grads = grads_device;
   opt.grad_materials = n_materials;
   if ((e = upload_constants(slots.data(), (uint32_t)slots.size(), ctx->primes.data(), ctx->prime_sums.data(), st)) !=
@@ -1046,6 +1055,53 @@ int ymrt_scene_set_material_params(ymrt_scene* scene, uint32_t first, uint32_t c
                                   sizeof(Material) * count, cudaMemcpyHostToDevice, scene->ctx->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(scene->ctx->stream);
   if (e != cudaSuccess) return scene->ctx->cuda_fail(e, "updating materials");
+  return YMRT_OK;
+}
+
+int ymrt_scene_set_density_grid(ymrt_scene* scene, uint32_t texture_index, int nx, int ny, int nz,
+                                const float* values, int store_half) {
+  if (!scene || !values || nx < 1 || ny < 1 || nz < 1) return YMRT_ERR_INVALID;
+  ymrt_context* ctx = scene->ctx;
+  if (texture_index >= scene->textures.size()) return ctx->fail(YMRT_ERR_INVALID, "texture index out of range");
+  const size_t n = (size_t)nx * (size_t)ny * (size_t)nz;
+  if (n > (size_t)1 << 30) return ctx->fail(YMRT_ERR_INVALID, "grid larger than 2^30 values");
+  float vmax = 0.0f;
+  std::vector<uint16_t> half;
+  if (store_half) half.resize(n);
+  for (size_t i = 0; i < n; ++i) {
+    float v = values[i];
+    if (!std::isfinite(v)) return ctx->fail(YMRT_ERR_INVALID, "grid values must be finite");
+    if (store_half) {
+      half[i] = __half_as_ushort(__float2half_rn(v));
+      v = __half2float(__ushort_as_half(half[i]));
+    }
+    vmax = std::max(vmax, v);
+  }
+  cudaSetDevice(ctx->device);
+  std::unique_ptr<DeviceBuffer>& buf = scene->grids[texture_index];
+  if (!buf) buf.reset(new DeviceBuffer());
+  const size_t bytes = n * (store_half ? sizeof(uint16_t) : sizeof(float));
+  cudaError_t e = buf->ensure(bytes);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(buf->ptr, store_half ? static_cast<const void*>(half.data()) : static_cast<const void*>(values),
+                        bytes, cudaMemcpyHostToDevice, ctx->stream);
+  Texture& t = scene->textures[texture_index];
+  t = Texture{};
+  t.type = kTexGrid;
+  t.child[0] = t.child[1] = kEmpty;
+  t.value = vmax;
+  t.grid_n[0] = nx;
+  t.grid_n[1] = ny;
+  t.grid_n[2] = nz;
+  t.grid_half = store_half ? 1 : 0;
+  t.grid = buf->ptr;
+  scene->dev.grid_count = 0;
+  for (const Texture& x : scene->textures) scene->dev.grid_count += x.type == kTexGrid ? 1u : 0u;
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(const_cast<Texture*>(scene->dev.textures) + texture_index, &t, sizeof(Texture),
+                        cudaMemcpyHostToDevice, ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  if (e != cudaSuccess) return ctx->cuda_fail(e, "uploading the density grid");
   return YMRT_OK;
 }
 
@@ -1285,6 +1341,29 @@ int ymrt_debug_trace(ymrt_scene* sc, int n, const float* origin, const float* di
   cudaError_t e = cudaStreamSynchronize(ctx->stream);
   if (sg.err != cudaSuccess || e != cudaSuccess) return ctx->cuda_fail(sg.err != cudaSuccess ? sg.err : e, "debug trace");
   if (errs) return ctx->fail(YMRT_ERR_OVERFLOW, "traversal stack overflow");
+  return YMRT_OK;
+}
+
+int ymrt_debug_density(ymrt_scene* sc, uint32_t texture_index, int n, const float* points, float* out) {
+  if (!sc || n < 0 || !points || !out) return YMRT_ERR_INVALID;
+  if (texture_index >= sc->textures.size()) return sc->ctx->fail(YMRT_ERR_INVALID, "texture index out of range");
+  if (n == 0) return YMRT_OK;
+  ymrt_context* ctx = sc->ctx;
+  cudaSetDevice(ctx->device);
+  Staging sg{ctx};
+  const float* d_p = sg.in(points, 3 * (size_t)n);
+  float* d_out = sg.out<float>(n);
+  uint32_t* d_err = sg.out<uint32_t>(1);
+  if (sg.err != cudaSuccess) return ctx->cuda_fail(sg.err, "staging");
+  cudaMemsetAsync(d_err, 0, sizeof(uint32_t), ctx->stream);
+  upload_constants(&sc->dev, 1, ctx->primes.data(), ctx->prime_sums.data(), ctx->stream);
+  launch_debug_density(n, texture_index, d_p, d_out, d_err, ctx->stream);
+  uint32_t errs = 0;
+  sg.back(out, d_out, n);
+  sg.back(&errs, d_err, 1);
+  cudaError_t e = cudaStreamSynchronize(ctx->stream);
+  if (sg.err != cudaSuccess || e != cudaSuccess) return ctx->cuda_fail(sg.err != cudaSuccess ? sg.err : e, "debug density");
+  if (errs) return ctx->fail(YMRT_ERR_OVERFLOW, "texture graph too deep");
   return YMRT_OK;
 }
 

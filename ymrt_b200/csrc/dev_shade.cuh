@@ -46,11 +46,12 @@ __device__ __forceinline__ void sphere_surface(float sphere_radius, vec3 p, Surf
 // FetchShadingData + FetchMeshShadingData / FetchSphereShadingData
 // (src/ShadingUtilities.cuh:639-875). For a sphere `bary` is the object-space
 // hit point and `tri` is EMPTY.
+template <uint32_t kF = kFeatAll>
 __device__ __forceinline__ SurfacePoint fetch_surface(const DeviceScene& S, uint32_t inst_idx, uint32_t tri,
                                                       vec3 bary) {
   const Instance inst = S.instances[inst_idx];
   const GeometryDesc& g = S.geometries[inst.geometry_idx];
-  if (g.kind == kGeoSphere) {
+  if ((kF & kFeatSpheres) && g.kind == kGeoSphere) {
     SurfacePoint sp;
     sphere_surface(g.radius, bary, &sp);
     const mat4& otw = S.transforms[inst.transform_idx];
@@ -120,11 +121,12 @@ __device__ __forceinline__ SurfacePoint fetch_surface(const DeviceScene& S, uint
 // FetchGeometryNormal with FetchMeshGeometryNormal / FetchSphereGeometryNormal
 // (src/ShadingUtilities.cuh:877-952): position, error and normalised
 // geometric normal only.
+template <uint32_t kF = kFeatAll>
 __device__ __forceinline__ void fetch_geometry_normal(const DeviceScene& S, uint32_t inst_idx, uint32_t tri, vec3 bary,
                                                       vec3* p, vec3* p_err, vec3* ng) {
   const Instance inst = S.instances[inst_idx];
   const GeometryDesc& g = S.geometries[inst.geometry_idx];
-  if (g.kind == kGeoSphere) {
+  if ((kF & kFeatSpheres) && g.kind == kGeoSphere) {
     const float radius = gmax(g.radius, kFloatEps);
     *p = bary;
     *p_err = error_gamma(5) * vabs(bary);
@@ -599,6 +601,7 @@ struct LightTri {
   bool sphere;
   float radius;
 };
+template <uint32_t kF = kFeatAll>
 __device__ __forceinline__ LightTri load_light_tri(const DeviceScene& S, const ShapeLight& L) {
   LightTri lt;
   const Instance inst = S.instances[L.instance_idx];
@@ -608,7 +611,7 @@ __device__ __forceinline__ LightTri load_light_tri(const DeviceScene& S, const S
   lt.intensity = mat.light_mtl.intensity;
   lt.otw = &S.transforms[inst.transform_idx];
   lt.wto = &S.i_transforms[inst.transform_idx];
-  lt.sphere = g.kind == kGeoSphere;
+  lt.sphere = (kF & kFeatSpheres) && g.kind == kGeoSphere;
   lt.radius = g.radius;
   if (lt.sphere) return lt;
   const uint32_t* tc = S.tri_corners + 3 * (size_t)(g.tri_offset + L.triangle_idx);
@@ -634,8 +637,10 @@ __device__ __forceinline__ vec3 sample_cone(float u0, float u1, float cos_theta_
 }
 
 // ShapeLight::SampleLi, spheres (src/Light.h:282-314): a direction in the
-// cone the sphere subtends, solid-angle pdf.
-__device__ __forceinline__ bool sphere_light_sample_li(const LightTri& lt, vec3 position, float u0, float u1, vec3* wi,
+// cone the sphere subtends, solid-angle pdf. Both sphere-light functions are
+// out of line: they run only for sphere lights, and inlined they would add
+// registers to every light evaluation.
+__device__ __noinline__ bool sphere_light_sample_li(const LightTri& lt, vec3 position, float u0, float u1, vec3* wi,
                                                        vec3* lpos, vec3* lpos_err, vec3* lng, vec3* Li, float* pdf) {
   const vec3 op = transform_position(*lt.wto, position);
   const float lpo = length(op);
@@ -666,7 +671,7 @@ __device__ __forceinline__ bool sphere_light_sample_li(const LightTri& lt, vec3 
 }
 
 // ShapeLight::EvalLi, spheres (src/Light.h:163-200).
-__device__ __forceinline__ vec3 sphere_light_eval_li(const LightTri& lt, vec3 position, vec3 wi, vec3* lpos,
+__device__ __noinline__ vec3 sphere_light_eval_li(const LightTri& lt, vec3 position, vec3 wi, vec3* lpos,
                                                      vec3* lpos_err, vec3* lng, float* pdf) {
   const vec3 owi = transform_vector(*lt.wto, wi);
   const vec3 op = transform_position(*lt.wto, position);
@@ -700,9 +705,10 @@ __device__ __forceinline__ vec3 sphere_light_eval_li(const LightTri& lt, vec3 po
 }
 
 // ShapeLight::SampleLi, triangle meshes (src/Light.h:207-264), and spheres.
+template <uint32_t kF = kFeatAll>
 __device__ __forceinline__ bool light_sample_li(const LightTri& lt, float area, vec3 position, float u0, float u1, vec3* wi,
                                                 vec3* lpos, vec3* lpos_err, vec3* lng, vec3* Li, float* pdf) {
-  if (lt.sphere) return sphere_light_sample_li(lt, position, u0, u1, wi, lpos, lpos_err, lng, Li, pdf);
+  if ((kF & kFeatSpheres) && lt.sphere) return sphere_light_sample_li(lt, position, u0, u1, wi, lpos, lpos_err, lng, Li, pdf);
   const vec3 geo_n = cross(lt.p1 - lt.p0, lt.p2 - lt.p0);
   const float su = sqrtf(gmax(0.0f, u0));
   const float bu = 1.0f - su;
@@ -732,9 +738,10 @@ __device__ __forceinline__ bool light_sample_li(const LightTri& lt, float area, 
 
 // ShapeLight::EvalLi, triangle meshes (src/Light.h:97-155), with
 // RayIntersectTriangle's glm 3x3 inverse (src/Light.h:14-40).
+template <uint32_t kF = kFeatAll>
 __device__ __forceinline__ vec3 light_eval_li(const LightTri& lt, float area, vec3 position, vec3 wi, vec3* lpos,
                                               vec3* lpos_err, vec3* lng, float* pdf) {
-  if (lt.sphere) return sphere_light_eval_li(lt, position, wi, lpos, lpos_err, lng, pdf);
+  if ((kF & kFeatSpheres) && lt.sphere) return sphere_light_eval_li(lt, position, wi, lpos, lpos_err, lng, pdf);
   const vec3 geo_n = cross(lt.p1 - lt.p0, lt.p2 - lt.p0);
   const vec3 owi = transform_vector(*lt.wto, wi);
   const vec3 opos = transform_position(*lt.wto, position);

@@ -508,8 +508,9 @@ __device__ __noinline__ bool trace_closest_impl(uint32_t scene, TraversalStack& 
 }
 
 // Closest hit of one world-space ray in the scene of constant-memory slot
-// `scene` (see trace_closest_impl).
-__device__ __forceinline__ bool trace_closest(uint32_t scene, TraversalStack& st, vec3 wo, vec3 wd, float tmax,
+// `scene` (see trace_closest_impl). Out of line, so that its callers keep one
+// call site whichever instantiation runs.
+__device__ __noinline__ bool trace_closest(uint32_t scene, TraversalStack& st, vec3 wo, vec3 wd, float tmax,
                                               uint32_t last_inst, uint32_t last_tri, bool volume_only,
                                               ClosestHit* out, uint32_t* tri_tests, uint32_t* node_visits) {
   if (c_scenes[scene].sphere_count != 0)
@@ -599,7 +600,7 @@ __device__ __noinline__ bool trace_occluded_impl(uint32_t scene, TraversalStack&
   return false;
 }
 
-__device__ __forceinline__ bool trace_occluded(uint32_t scene, TraversalStack& st, vec3 wo, vec3 wd, float tmax,
+__device__ __noinline__ bool trace_occluded(uint32_t scene, TraversalStack& st, vec3 wo, vec3 wd, float tmax,
                                                uint32_t* tri_tests, uint32_t* node_visits) {
   if (c_scenes[scene].sphere_count != 0) return trace_occluded_impl<true>(scene, st, wo, wd, tmax, tri_tests, node_visits);
   return trace_occluded_impl<false>(scene, st, wo, wd, tmax, tri_tests, node_visits);

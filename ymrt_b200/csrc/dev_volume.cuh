@@ -11,6 +11,8 @@
 // the reference's operand order.
 #pragma once
 
+#include <cuda_fp16.h>
+
 #include "ymrt_scene.h"
 #include "dev_sampler.cuh"
 
@@ -105,8 +107,55 @@ __device__ __forceinline__ float perlin_fbm(vec3 p, float lacunarity, float gain
   return r;
 }
 
+// ---- density grids (kTexGrid) ----
+
+// The lattice cell of an object-space point along one axis: lower and upper
+// sample index and the upper sample's weight, clamped to the edge samples
+// outside [0.5/n, 1 - 0.5/n] (and for a NaN coordinate).
+__device__ __forceinline__ void grid_axis(float p, int n, int* i0, int* i1, float* w) {
+  const float g = (p + 0.5f) * (float)n - 0.5f;
+  if (!(g > 0.0f)) {
+    *i0 = *i1 = 0;
+    *w = 0.0f;
+  } else if (!(g < (float)(n - 1))) {
+    *i0 = *i1 = n - 1;
+    *w = 0.0f;
+  } else {
+    const float fl = floorf(g);
+    *i0 = (int)fl;
+    *i1 = *i0 + 1;
+    *w = g - fl;
+  }
+}
+
+__device__ __forceinline__ float grid_at(const Texture& t, int x, int y, int z) {
+  const size_t k = ((size_t)z * (size_t)t.grid_n[1] + (size_t)y) * (size_t)t.grid_n[0] + (size_t)x;
+  if (t.grid_half) return __half2float(__ushort_as_half(__ldg(static_cast<const unsigned short*>(t.grid) + k)));
+  return __ldg(static_cast<const float*>(t.grid) + k);
+}
+
+__device__ __forceinline__ float lerp1(float a, float b, float w) { return a + w * (b - a); }
+
+// Trilinear read of a grid node at an object-space point. A constant grid
+// reads back its value exactly (a + w * 0 == a). Out of line, so that the
+// procedural nodes' tracking loops do not carry its registers.
+__device__ __noinline__ float grid_eval(const Texture& t, vec3 p) {
+  int x0, x1, y0, y1, z0, z1;
+  float wx, wy, wz;
+  grid_axis(p.x, t.grid_n[0], &x0, &x1, &wx);
+  grid_axis(p.y, t.grid_n[1], &y0, &y1, &wy);
+  grid_axis(p.z, t.grid_n[2], &z0, &z1, &wz);
+  const float c00 = lerp1(grid_at(t, x0, y0, z0), grid_at(t, x1, y0, z0), wx);
+  const float c10 = lerp1(grid_at(t, x0, y1, z0), grid_at(t, x1, y1, z0), wx);
+  const float c01 = lerp1(grid_at(t, x0, y0, z1), grid_at(t, x1, y0, z1), wx);
+  const float c11 = lerp1(grid_at(t, x0, y1, z1), grid_at(t, x1, y1, z1), wx);
+  return lerp1(lerp1(c00, c10, wy), lerp1(c01, c11, wy), wz);
+}
+
 // TextureEval for constant and fBm nodes (src/TextureEval.cuh:419-481): a
-// post-order walk with an explicit stack of eight nodes, as the reference.
+// post-order walk with an explicit stack of eight nodes, as the reference;
+// grid nodes are leaves.
+template <uint32_t kF = kFeatAll>
 __device__ __forceinline__ vec3 texture_eval(const Texture* __restrict__ tex, uint32_t root, vec3 p_object,
                                              uint32_t* errors) {
   struct Frame {
@@ -150,6 +199,8 @@ __device__ __forceinline__ vec3 texture_eval(const Texture* __restrict__ tex, ui
     } else if (t.type == kTexFbm) {
       const float fbm = perlin_fbm(t.frequency * p_object, t.lacunarity, t.gain, t.layer_count, t.amplitude, t.offset);
       r = f.child[0] + fbm * (f.child[1] - f.child[0]);
+    } else if ((kF & kFeatGrids) && t.type == kTexGrid) {
+      r = vec3(grid_eval(t, p_object));
     }
     if (f.parent < 0) return r;
     Frame& par = st[f.parent];
@@ -163,7 +214,7 @@ __device__ __forceinline__ vec3 texture_eval(const Texture* __restrict__ tex, ui
 
 // Texture::GetUpperBound for the supported node types (src/Texture.h:1181-1251).
 __device__ __forceinline__ float texture_upper_bound(const Texture& t) {
-  if (t.type == kTexConstFloat) return t.value;
+  if (t.type == kTexConstFloat || t.type == kTexGrid) return t.value;
   if (t.type == kTexConstRgb) return gmax(t.color.x, gmax(t.color.y, t.color.z));
   if (t.type == kTexFbm) {
     float r = 0.0f, a = t.amplitude, o = t.offset;
@@ -330,6 +381,7 @@ __device__ __forceinline__ void volume_space_rays(const DeviceScene& S, int n, c
   const float csum = M.m.x + M.m.y + M.m.z;
   M.cw = csum > 0.0f ? (M.m / csum) : vec3(1.0f / 3.0f);
 }
+template <uint32_t kF>
 __device__ __forceinline__ void densities(const DeviceScene& S, int n, const int* vidx, const Majorant& M, float acc,
                                           vec3* mst, vec3* mss, uint32_t* errors) {
   *mst = vec3(0.0f);
@@ -338,7 +390,7 @@ __device__ __forceinline__ void densities(const DeviceScene& S, int n, const int
     const Volume& v = S.volumes[vidx[i]];
     float density = 1.0f;
     if (has_density(S, v))
-      density = gmax(texture_eval(S.textures, (uint32_t)v.density_texture_idx, M.ro[i] + M.rd[i] * acc, errors).x, 0.0f);
+      density = gmax(texture_eval<kF>(S.textures, (uint32_t)v.density_texture_idx, M.ro[i] + M.rd[i] * acc, errors).x, 0.0f);
     *mst += v.sigma_t * density;
     if (mss) *mss += v.sigma_t * v.albedo * density;
   }
@@ -346,6 +398,7 @@ __device__ __forceinline__ void densities(const DeviceScene& S, int n, const int
 
 // SampleTrHeterogeneous (src/VolumeEval.cuh:80-214): delta tracking against
 // the summed majorant with channel-wise real / null collision probabilities.
+template <uint32_t kF>
 __device__ __noinline__ bool sample_tr_heterogeneous(const DeviceScene& S, int n, const int* vidx, vec3 o, vec3 d,
                                                      float t_max, vec3* tr_weight, float* dist, float* vw,
                                                      PathSampler& hs, uint32_t* errors) {
@@ -379,7 +432,7 @@ __device__ __noinline__ bool sample_tr_heterogeneous(const DeviceScene& S, int n
     }
     acc += fpl;
     vec3 mst, mss;
-    densities(S, n, vidx, M, acc, &mst, &mss, errors);
+    densities<kF>(S, n, vidx, M, acc, &mst, &mss, errors);
     vec3 real;
     real.x = gmin(M.m.x > 0.0f ? mst.x * mrcp.x : 0.0f, 1.0f);
     real.y = gmin(M.m.y > 0.0f ? mst.y * mrcp.y : 0.0f, 1.0f);
@@ -404,6 +457,7 @@ __device__ __noinline__ bool sample_tr_heterogeneous(const DeviceScene& S, int n
 }
 
 // SampleVolumeScattering (src/VolumeEval.cuh:217-251).
+template <uint32_t kF>
 __device__ __forceinline__ bool sample_volume_scattering(const DeviceScene& S, vec3 o, vec3 d, int n, const int* vidx,
                                                          float t_max, vec3* tr_weight, float* dist, float* vw,
                                                          PathSampler& hs, uint32_t* errors) {
@@ -414,12 +468,13 @@ __device__ __forceinline__ bool sample_volume_scattering(const DeviceScene& S, v
       het = true;
       break;
     }
-  if (het) return sample_tr_heterogeneous(S, n, vidx, o, d, t_max, tr_weight, dist, vw, hs, errors);
+  if (het) return sample_tr_heterogeneous<kF>(S, n, vidx, o, d, t_max, tr_weight, dist, vw, hs, errors);
   return sample_tr_homogeneous(S, n, vidx, t_max, tr_weight, dist, vw, hs);
 }
 
 // EvalTrHeterogeneous (src/VolumeEval.cuh:269-386): ratio-tracking style
 // transmittance with Russian roulette after 32 steps.
+template <uint32_t kF>
 __device__ __noinline__ vec3 eval_tr_heterogeneous(const DeviceScene& S, int n, const int* vidx, vec3 o, vec3 d,
                                                    float t_max, PathSampler& hs, uint32_t* errors) {
   Majorant M;
@@ -449,7 +504,7 @@ __device__ __noinline__ vec3 eval_tr_heterogeneous(const DeviceScene& S, int n, 
     }
     acc += fpl;
     vec3 mst;
-    densities(S, n, vidx, M, acc, &mst, nullptr, errors);
+    densities<kF>(S, n, vidx, M, acc, &mst, nullptr, errors);
     vec3 real;
     real.x = gmin(M.m.x > 0.0f ? mst.x * mrcp.x : 0.0f, 1.0f);
     real.y = gmin(M.m.y > 0.0f ? mst.y * mrcp.y : 0.0f, 1.0f);
@@ -471,6 +526,7 @@ __device__ __noinline__ vec3 eval_tr_heterogeneous(const DeviceScene& S, int n, 
 }
 
 // EvalTr (src/VolumeEval.cuh:388-418).
+template <uint32_t kF>
 __device__ __forceinline__ vec3 eval_tr(const DeviceScene& S, vec3 o, vec3 d, const RayTransfer& rt, float t_max,
                                         PathSampler& hs, uint32_t* errors) {
   if (S.volume_count == 0) return vec3(1.0f);
@@ -483,7 +539,7 @@ __device__ __forceinline__ vec3 eval_tr(const DeviceScene& S, vec3 o, vec3 d, co
       het = true;
       break;
     }
-  if (het) return eval_tr_heterogeneous(S, n, vidx, o, d, t_max, hs, errors);
+  if (het) return eval_tr_heterogeneous<kF>(S, n, vidx, o, d, t_max, hs, errors);
   vec3 m(0.0f);
   for (int i = 0; i < n; ++i) m += S.volumes[vidx[i]].sigma_t;
   return vexp(-m * t_max);

@@ -242,9 +242,9 @@ __global__ void __launch_bounds__(256) k_sort_hits(const WaveControl* __restrict
 // from the wave-control block, so any grid works (launched with one thread
 // per pool slot, each thread takes at most one path).
 //
-// kSph: some scene of the batch holds spheres (the traversal without sphere
-// tests is a separate instantiation; see trace_closest_impl).
-template <bool kVol, bool kSph>
+// kF: the batch's scene features (kFeatSpheres, kFeatGrids); a batch without
+// spheres or grids runs the instantiation without their code.
+template <bool kVol, uint32_t kF>
 __global__ void __launch_bounds__(kTraceBlock, 5) k_extend(PathPool P, const WaveControl* __restrict__ ctl, HitPool H,
                                                            const JobDesc* __restrict__ jobs, WaveCounters* counters) {
   YM_TRAVERSAL_SHARED(s_stack);
@@ -269,7 +269,7 @@ __global__ void __launch_bounds__(kTraceBlock, 5) k_extend(PathPool P, const Wav
     TraversalStack st;
     st.bind(s_stack_entries, s_stack_t);
     ClosestHit ch;
-    bool hit = trace_closest_impl<kSph>(slot, st, o, d, kTMax, lh.x, lh.y, false, &ch, &tests, &nodes);
+    bool hit = trace_closest_impl<(kF & kFeatSpheres) != 0>(slot, st, o, d, kTMax, lh.x, lh.y, false, &ch, &tests, &nodes);
     overflow = overflow || st.overflow;
     bool volume_hit = false;
     vec3 vol_pos(0.0f);
@@ -286,7 +286,7 @@ __global__ void __launch_bounds__(kTraceBlock, 5) k_extend(PathPool P, const Wav
       vec3 trw(1.0f);
       float dist = 0.0f;
       float vw[kMaxBoundaryRecord];
-      const bool hv = sample_volume_scattering(S, o, d, n, vidx, hit ? ch.t : kTMax, &trw, &dist, vw, hs,
+      const bool hv = sample_volume_scattering<kF>(S, o, d, n, vidx, hit ? ch.t : kTMax, &trw, &dist, vw, hs,
                                                &counters->errors);
       const float4 t4 = P.throughput[i];
       vec3 tp(t4.x, t4.y, t4.z);
@@ -437,6 +437,7 @@ __device__ __forceinline__ float ex_ior(const RayTransfer& rt, uint32_t hit_prim
 // and the transmittance along a shadow ray through every medium it crosses
 // (TraceTr, src/VolumeEval.cuh:420-468). `rt` is the shadow ray's own copy of
 // the nested-media stack; `o`/`d`/`tmax` and the last hit are the shadow ray.
+template <uint32_t kF>
 __device__ __noinline__ vec3 trace_tr(uint32_t scene, TraversalStack& st, vec3 o, vec3 d, float tmax,
                                       uint32_t last_inst, uint32_t last_tri, RayTransfer& rt, PathSampler& hs,
                                       uint32_t* errors, uint32_t* tests, uint32_t* nodes) {
@@ -453,15 +454,15 @@ __device__ __noinline__ vec3 trace_tr(uint32_t scene, TraversalStack& st, vec3 o
       break;
     }
     ClosestHit ch;
-    const bool hit = trace_closest(scene, st, o, d, ray_t, last_inst, last_tri, true, &ch, tests, nodes);
+    const bool hit = trace_closest_impl<(kF & kFeatSpheres) != 0>(scene, st, o, d, ray_t, last_inst, last_tri, true, &ch, tests, nodes);
     if (!hit) {
-      tr *= eval_tr(S, o, d, rt, gmax(max_d - traced, 0.0f), hs, errors);
+      tr *= eval_tr<kF>(S, o, d, rt, gmax(max_d - traced, 0.0f), hs, errors);
       break;
     }
-    tr *= eval_tr(S, o, d, rt, ch.t, hs, errors);
+    tr *= eval_tr<kF>(S, o, d, rt, ch.t, hs, errors);
     traced += ch.t;
     vec3 hp, herr, hng;
-    fetch_geometry_normal(S, ch.inst, ch.tri, vec3(ch.b0, ch.b1, ch.b2), &hp, &herr, &hng);
+    fetch_geometry_normal<kF>(S, ch.inst, ch.tri, vec3(ch.b0, ch.b1, ch.b2), &hp, &herr, &hng);
     boundary_transition(S, rt, ch.nearby, ch.nearby_count, errors);
     o = offset_ray_origin(hp, herr, d, hng);
     d = normalize(d);
@@ -516,14 +517,14 @@ struct SurfaceNee {
 
 // Transmittance of an unoccluded surface shadow ray (the volume part of the
 // reference's EvalShapeLight / EvalDistantLight).
-template <bool kVol>
+template <bool kVol, uint32_t kF>
 __device__ __forceinline__ vec3 surface_shadow_tr(const DeviceScene& S, TraversalStack& st, const SurfaceNee& c, vec3 so,
                                                   vec3 ldir, float maxd, bool tb, PathSampler& hs, uint32_t* errors,
                                                   uint32_t* tests, uint32_t* nodes) {
   if (!kVol || !c.media) return vec3(1.0f);
   RayTransfer srt = *c.rt;
   if (tb) boundary_transition(S, srt, c.nb, c.n_nb, errors);
-  return trace_tr(c.slot, st, so, normalize(ldir), maxd, c.inst, c.tri, srt, hs, errors, tests, nodes);
+  return trace_tr<kF>(c.slot, st, so, normalize(ldir), maxd, c.inst, c.tri, srt, hs, errors, tests, nodes);
 }
 
 // ------------------------------------------------- path-replay adjoint ---
@@ -649,7 +650,7 @@ __device__ __forceinline__ void emit_shadow_ray(const ShadowEmit& em, vec3 o, ve
 // pdf enters as (x * mul) / div, the form each estimator uses. Traced here
 // (direct += its unoccluded contribution, times the media transmittance)
 // or, with kDefer, queued for k_connect.
-template <bool kVol, bool kDefer>
+template <bool kVol, bool kDefer, uint32_t kF>
 __device__ __forceinline__ void nee_shadow_ray(const DeviceScene& S, TraversalStack& st, const SurfaceNee& c,
                                                const ShadowEmit& em, vec3 so, vec3 ldir, float maxd, bool tb,
                                                float mis, vec3 fc, vec3 Lc, float mul, float div, vec3* direct,
@@ -661,8 +662,8 @@ __device__ __forceinline__ void nee_shadow_ray(const DeviceScene& S, TraversalSt
     emit_shadow_ray(em, so, normalize(ldir), maxd, ((mis * vec3(1.0f) * fc * Lc) * mul) / div);
     return;
   }
-  if (!trace_occluded(c.slot, st, so, normalize(ldir), maxd, tests, nodes)) {
-    const vec3 tr = surface_shadow_tr<kVol>(S, st, c, so, ldir, maxd, tb, hs, errors, tests, nodes);
+  if (!trace_occluded_impl<(kF & kFeatSpheres) != 0>(c.slot, st, so, normalize(ldir), maxd, tests, nodes)) {
+    const vec3 tr = surface_shadow_tr<kVol, kF>(S, st, c, so, ldir, maxd, tb, hs, errors, tests, nodes);
     *direct += mis * tr * fc * Lc;
     if (adj) {
       // d(direct)/dp = mis * tr * fc * (df/dp)/f * Lc, scaled like the estimator
@@ -673,7 +674,7 @@ __device__ __forceinline__ void nee_shadow_ray(const DeviceScene& S, TraversalSt
 }
 
 // EvalShapeLight (src/Shading.cu:294-417).
-template <bool kVol, bool kDefer>
+template <bool kVol, bool kDefer, uint32_t kF>
 __device__ __forceinline__ vec3 eval_shape_light(const DeviceScene& S, TraversalStack& st, const LayeredBsdf& B,
                                                  const SurfaceNee& c, const ShadowEmit& em, PathSampler& hs,
                                                  uint32_t* shadow_rays, uint32_t* tests, uint32_t* nodes,
@@ -684,13 +685,13 @@ __device__ __forceinline__ vec3 eval_shape_light(const DeviceScene& S, Traversal
   float select_pdf = 0.0f;
   const int li = sample_light_power(S, sample1d(hs, S), &select_pdf);
   const ShapeLight L = S.shape_lights[li];
-  const LightTri lt = load_light_tri(S, L);
+  const LightTri lt = load_light_tri<kF>(S, L);
   {
     float u0, u1;
     sample2d(hs, S, &u0, &u1);
     vec3 ldir(0.0f), lpos(0.0f), lerr(0.0f), lng(0.0f), Li(0.0f);
     float lpdf = 0.0f;
-    const bool valid = light_sample_li(lt, L.area, c.p, u0, u1, &ldir, &lpos, &lerr, &lng, &Li, &lpdf);
+    const bool valid = light_sample_li<kF>(lt, L.area, c.p, u0, u1, &ldir, &lpos, &lerr, &lng, &Li, &lpdf);
     const vec3 lwi = B.to_local(ldir);
     float wpdf = 0.0f;
     const vec3 f = bsdf_eval(B, wo, lwi, &wpdf);
@@ -700,7 +701,7 @@ __device__ __forceinline__ vec3 eval_shape_light(const DeviceScene& S, Traversal
       const bool tb = dot(-c.ray_dir, c.ng) * dot(ldir, c.ng) < 0.0f;
       const bool invalid = (!same_hemisphere(wo, lwi) && !tb) || (same_hemisphere(wo, lwi) && tb);
       if (!invalid)
-        nee_shadow_ray<kVol, kDefer>(S, st, c, em, so, ldir, maxd, tb, power_heuristic(lpdf, wpdf),
+        nee_shadow_ray<kVol, kDefer, kF>(S, st, c, em, so, ldir, maxd, tb, power_heuristic(lpdf, wpdf),
                                      vmin(f, vec3(kMaxColorClamp)), vmin(Li, vec3(kMaxColorClamp)),
                                      safe_rcp(select_pdf), 1.0f, &direct, hs, shadow_rays, tests, nodes, errors, adj, &B);
     }
@@ -714,14 +715,14 @@ __device__ __forceinline__ vec3 eval_shape_light(const DeviceScene& S, Traversal
       const vec3 ldir = B.to_world(bwi);
       vec3 lpos(0.0f), lerr(0.0f), lng(0.0f);
       float wpdf = 0.0f;
-      const vec3 Li = light_eval_li(lt, L.area, c.p, ldir, &lpos, &lerr, &lng, &wpdf);
+      const vec3 Li = light_eval_li<kF>(lt, L.area, c.p, ldir, &lpos, &lerr, &lng, &wpdf);
       if (max_component(Li) > kMinColorEps) {
         const vec3 so = offset_ray_origin(c.p, c.p_err, ldir, c.ng);
         const float maxd = length(offset_ray_origin(lpos, lerr, -ldir, lng) - c.p) * kShadowRayClamp;
         const bool tb = dot(-c.ray_dir, c.ng) * dot(ldir, c.ng) < 0.0f;
         const bool invalid = (!same_hemisphere(wo, bwi) && !tb) || (same_hemisphere(wo, bwi) && tb);
         if (!invalid)
-          nee_shadow_ray<kVol, kDefer>(S, st, c, em, so, ldir, maxd, tb, power_heuristic(bpdf, wpdf),
+          nee_shadow_ray<kVol, kDefer, kF>(S, st, c, em, so, ldir, maxd, tb, power_heuristic(bpdf, wpdf),
                                        vmin(bw, vec3(kMaxColorClamp)), vmin(Li, vec3(kMaxColorClamp)),
                                        safe_rcp(select_pdf), 1.0f, &direct, hs, shadow_rays, tests, nodes, errors, adj, &B);
       }
@@ -731,7 +732,7 @@ __device__ __forceinline__ vec3 eval_shape_light(const DeviceScene& S, Traversal
 }
 
 // EvalDistantLight (src/Shading.cu:83-198).
-template <bool kVol, bool kDefer>
+template <bool kVol, bool kDefer, uint32_t kF>
 __device__ __forceinline__ vec3 eval_distant_light(const DeviceScene& S, TraversalStack& st, const LayeredBsdf& B,
                                                    const SurfaceNee& c, const ShadowEmit& em, PathSampler& hs,
                                                    uint32_t* shadow_rays, uint32_t* tests, uint32_t* nodes,
@@ -756,7 +757,7 @@ __device__ __forceinline__ vec3 eval_distant_light(const DeviceScene& S, Travers
       const bool tb = dot(-c.ray_dir, c.ng) * dot(ldir, c.ng) < 0.0f;
       const bool invalid = (!same_hemisphere(wo, lwi) && !tb) || (same_hemisphere(wo, lwi) && tb);
       if (!invalid)
-        nee_shadow_ray<kVol, kDefer>(S, st, c, em, so, ldir, kTMax, tb, power_heuristic(lpdf, wpdf),
+        nee_shadow_ray<kVol, kDefer, kF>(S, st, c, em, so, ldir, kTMax, tb, power_heuristic(lpdf, wpdf),
                                      vmin(f, vec3(kMaxColorClamp)), vmin(Li, vec3(kMaxColorClamp)), 1.0f,
                                      select_pdf, &direct, hs, shadow_rays, tests, nodes, errors, adj, &B);
     }
@@ -775,7 +776,7 @@ __device__ __forceinline__ vec3 eval_distant_light(const DeviceScene& S, Travers
         const bool tb = dot(-c.ray_dir, c.ng) * dot(ldir, c.ng) < 0.0f;
         const bool invalid = (!same_hemisphere(wo, bwi) && !tb) || (same_hemisphere(wo, bwi) && tb);
         if (!invalid)
-          nee_shadow_ray<kVol, kDefer>(S, st, c, em, so, ldir, kTMax, tb, power_heuristic(bpdf, wpdf),
+          nee_shadow_ray<kVol, kDefer, kF>(S, st, c, em, so, ldir, kTMax, tb, power_heuristic(bpdf, wpdf),
                                        vmin(bw, vec3(kMaxColorClamp)), vmin(Li, vec3(kMaxColorClamp)), 1.0f,
                                        select_pdf, &direct, hs, shadow_rays, tests, nodes, errors, adj, &B);
       }
@@ -786,6 +787,7 @@ __device__ __forceinline__ vec3 eval_distant_light(const DeviceScene& S, Travers
 
 // EvalVolumeShapeLight / EvalVolumeDistantLight (src/Shading.cu:202-291, 419-513):
 // next-event estimation at a scattering point inside the media.
+template <uint32_t kF>
 __device__ __noinline__ vec3 eval_volume_lights(uint32_t slot, TraversalStack& st, bool distant, int n,
                                                 const float* gs, const float* vw, vec3 ray_dir, const RayTransfer& rt,
                                                 vec3 pos, PathSampler& hs, uint32_t* shadow_rays, uint32_t* tests,
@@ -807,9 +809,9 @@ __device__ __noinline__ vec3 eval_volume_lights(uint32_t slot, TraversalStack& s
       const float pw = eval_mixed_phases(vw, gs, n, -ray_dir, ldir, &wpdf);
       if (pw > kMinColorEps) {
         ++*shadow_rays;
-        if (!trace_occluded(slot, st, pos, normalize(ldir), kTMax, tests, nodes)) {
+        if (!trace_occluded_impl<(kF & kFeatSpheres) != 0>(slot, st, pos, normalize(ldir), kTMax, tests, nodes)) {
           RayTransfer srt = rt;
-          const vec3 tr = trace_tr(slot, st, pos, normalize(ldir), kTMax, kEmpty, kEmpty, srt, hs, errors, tests, nodes);
+          const vec3 tr = trace_tr<kF>(slot, st, pos, normalize(ldir), kTMax, kEmpty, kEmpty, srt, hs, errors, tests, nodes);
           const float mis = power_heuristic(lpdf, wpdf);
           direct += mis * tr * gmin(pw, kMaxColorClamp) * vmin(Li, vec3(kMaxColorClamp));
         }
@@ -825,9 +827,9 @@ __device__ __noinline__ vec3 eval_volume_lights(uint32_t slot, TraversalStack& s
         const vec3 Li = distant_eval_li(S, L, pwi, &wpdf);
         if (max_component(Li) > kMinColorEps) {
           ++*shadow_rays;
-          if (!trace_occluded(slot, st, pos, normalize(pwi), kTMax, tests, nodes)) {
+          if (!trace_occluded_impl<(kF & kFeatSpheres) != 0>(slot, st, pos, normalize(pwi), kTMax, tests, nodes)) {
             RayTransfer srt = rt;
-            const vec3 tr = trace_tr(slot, st, pos, normalize(pwi), kTMax, kEmpty, kEmpty, srt, hs, errors, tests, nodes);
+            const vec3 tr = trace_tr<kF>(slot, st, pos, normalize(pwi), kTMax, kEmpty, kEmpty, srt, hs, errors, tests, nodes);
             const float mis = power_heuristic(pspdf, wpdf);
             direct += mis * tr * gmin(pw, kMaxColorClamp) * vmin(Li, vec3(kMaxColorClamp));
           }
@@ -840,21 +842,21 @@ __device__ __noinline__ vec3 eval_volume_lights(uint32_t slot, TraversalStack& s
   float select_pdf = 0.0f;
   const int li = sample_light_power(S, sample1d(hs, S), &select_pdf);
   const ShapeLight L = S.shape_lights[li];
-  const LightTri lt = load_light_tri(S, L);
+  const LightTri lt = load_light_tri<kF>(S, L);
   {
     float u0, u1;
     sample2d(hs, S, &u0, &u1);
     vec3 ldir(0.0f), lpos(0.0f), lerr(0.0f), lng(0.0f), Li(0.0f);
     float lpdf = 0.0f;
-    const bool valid = light_sample_li(lt, L.area, pos, u0, u1, &ldir, &lpos, &lerr, &lng, &Li, &lpdf);
+    const bool valid = light_sample_li<kF>(lt, L.area, pos, u0, u1, &ldir, &lpos, &lerr, &lng, &Li, &lpdf);
     float wpdf = 0.0f;
     const float pw = eval_mixed_phases(vw, gs, n, -ray_dir, ldir, &wpdf);
     if (pw > kMinColorEps && valid) {
       const float maxd = length(offset_ray_origin(lpos, lerr, -ldir, lng) - pos) * kShadowRayClamp;
       ++*shadow_rays;
-      if (!trace_occluded(slot, st, pos, normalize(ldir), maxd, tests, nodes)) {
+      if (!trace_occluded_impl<(kF & kFeatSpheres) != 0>(slot, st, pos, normalize(ldir), maxd, tests, nodes)) {
         RayTransfer srt = rt;
-        const vec3 tr = trace_tr(slot, st, pos, normalize(ldir), maxd, kEmpty, kEmpty, srt, hs, errors, tests, nodes);
+        const vec3 tr = trace_tr<kF>(slot, st, pos, normalize(ldir), maxd, kEmpty, kEmpty, srt, hs, errors, tests, nodes);
         const float mis = power_heuristic(lpdf, wpdf);
         direct += mis * tr * gmin(pw, kMaxColorClamp) * vmin(Li, vec3(kMaxColorClamp));
       }
@@ -868,13 +870,13 @@ __device__ __noinline__ vec3 eval_volume_lights(uint32_t slot, TraversalStack& s
     if (sample_mixed_phases(vw, gs, n, u0, u1, -ray_dir, &pw, &pwi, &pspdf)) {
       vec3 lpos(0.0f), lerr(0.0f), lng(0.0f);
       float wpdf = 0.0f;
-      const vec3 Li = light_eval_li(lt, L.area, pos, pwi, &lpos, &lerr, &lng, &wpdf);
+      const vec3 Li = light_eval_li<kF>(lt, L.area, pos, pwi, &lpos, &lerr, &lng, &wpdf);
       if (max_component(Li) > kMinColorEps) {
         const float maxd = length(offset_ray_origin(lpos, lerr, -pwi, lng) - pos) * kShadowRayClamp;
         ++*shadow_rays;
-        if (!trace_occluded(slot, st, pos, normalize(pwi), maxd, tests, nodes)) {
+        if (!trace_occluded_impl<(kF & kFeatSpheres) != 0>(slot, st, pos, normalize(pwi), maxd, tests, nodes)) {
           RayTransfer srt = rt;
-          const vec3 tr = trace_tr(slot, st, pos, normalize(pwi), maxd, kEmpty, kEmpty, srt, hs, errors, tests, nodes);
+          const vec3 tr = trace_tr<kF>(slot, st, pos, normalize(pwi), maxd, kEmpty, kEmpty, srt, hs, errors, tests, nodes);
           const float mis = power_heuristic(pspdf, wpdf);
           direct += mis * tr * gmin(pw, kMaxColorClamp) * vmin(Li, vec3(kMaxColorClamp));
         }
@@ -892,7 +894,7 @@ __device__ __noinline__ vec3 eval_volume_lights(uint32_t slot, TraversalStack& s
 // are shaded exactly as in the forward pass, nothing is added to the image,
 // and each material vertex adds its terms of dLoss/dParam (see AdjCtx) to
 // `grads` (per-block sums in shared memory, then one atomic per touched slot).
-template <bool kVol, bool kDefer, bool kAdj = false>
+template <bool kVol, bool kDefer, bool kAdj, uint32_t kF>
 __global__ void __launch_bounds__(kTraceBlock) k_shade(PathPool P, const WaveControl* __restrict__ ctl, HitPool H,
                                                        PathPool Q, const JobDesc* __restrict__ jobs,
                                                        WaveCounters* counters, ShadowQueue shadow_q,
@@ -982,10 +984,10 @@ __global__ void __launch_bounds__(kTraceBlock) k_shade(PathPool P, const WaveCon
       }
       const vec3 pos = bary;
       if (rs.enable_distant_light)
-        rad += indirect_clamp(rs, tp * eval_volume_lights(slot, st, true, n, gs, vw, rd, rt, pos, hs, &shadow_rays, &tests,
+        rad += indirect_clamp(rs, tp * eval_volume_lights<kF>(slot, st, true, n, gs, vw, rd, rt, pos, hs, &shadow_rays, &tests,
                                                           &nodes, errors), depth);
       if (rs.enable_shape_light)
-        rad += indirect_clamp(rs, tp * eval_volume_lights(slot, st, false, n, gs, vw, rd, rt, pos, hs, &shadow_rays,
+        rad += indirect_clamp(rs, tp * eval_volume_lights<kF>(slot, st, false, n, gs, vw, rd, rt, pos, hs, &shadow_rays,
                                                           &tests, &nodes, errors), depth);
       vec3 wi;
       float pdf = 0.0f, pw = 0.0f;
@@ -1026,7 +1028,7 @@ __global__ void __launch_bounds__(kTraceBlock) k_shade(PathPool P, const WaveCon
       } else {
         nb[0] = NearbyHit{inst_idx, bt.w, hit_back};
       }
-      const SurfacePoint sp = fetch_surface(S, inst_idx, tri, bary);
+      const SurfacePoint sp = fetch_surface<kF>(S, inst_idx, tri, bary);
       const Instance inst = S.instances[inst_idx];
       bool done = false;
       if (!(inst.material_idx < S.material_count)) {
@@ -1083,11 +1085,11 @@ __global__ void __launch_bounds__(kTraceBlock) k_shade(PathPool P, const WaveCon
         }
         if (rs.enable_distant_light)
           rad += indirect_clamp(
-              rs, tp * eval_distant_light<kVol, kDefer>(S, st, B, nc, em, hs, &shadow_rays, &tests, &nodes, errors, adj),
+              rs, tp * eval_distant_light<kVol, kDefer, kF>(S, st, B, nc, em, hs, &shadow_rays, &tests, &nodes, errors, adj),
               depth);
         if (rs.enable_shape_light)
           rad += indirect_clamp(
-              rs, tp * eval_shape_light<kVol, kDefer>(S, st, B, nc, em, hs, &shadow_rays, &tests, &nodes, errors, adj),
+              rs, tp * eval_shape_light<kVol, kDefer, kF>(S, st, B, nc, em, hs, &shadow_rays, &tests, &nodes, errors, adj),
               depth);
         const vec3 wo = B.to_local(-rd);
         vec3 w, wi;
@@ -1178,7 +1180,7 @@ __global__ void __launch_bounds__(kTraceBlock) k_shade(PathPool P, const WaveCon
 // Traces the wave's queued shadow rays (grid-stride over the queue, so the
 // grid is sized to the GPU, not to the queue) and adds each unoccluded ray's
 // contribution to its pixel.
-template <bool kSph>
+template <uint32_t kF>
 __global__ void __launch_bounds__(kTraceBlock, 5) k_connect(ShadowQueue Q, const JobDesc* __restrict__ jobs,
                                                             WaveCounters* counters) {
   YM_TRAVERSAL_SHARED(s_stack);
@@ -1189,7 +1191,7 @@ __global__ void __launch_bounds__(kTraceBlock, 5) k_connect(ShadowQueue Q, const
   for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
     const float4 o = Q.o[t], d = Q.d[t], c = Q.c[t];
     const JobDesc& J = jobs[__float_as_uint(c.w)];
-    if (!trace_occluded_impl<kSph>(J.scene_slot, st, vec3(o.x, o.y, o.z), vec3(d.x, d.y, d.z), o.w, &tests,
+    if (!trace_occluded_impl<(kF & kFeatSpheres) != 0>(J.scene_slot, st, vec3(o.x, o.y, o.z), vec3(d.x, d.y, d.z), o.w, &tests,
                                    &nodes)) {
       atomicAdd(J.image + __float_as_uint(d.w), make_float4(c.x, c.y, c.z, 0.0f));
       if (J.path_radiance) {
@@ -1264,6 +1266,13 @@ __global__ void __launch_bounds__(kTraceBlock) k_debug_occluded(int n, const flo
   uint32_t tests = 0, nodes = 0;
   occluded[i] = trace_occluded(0, st, o, d, tmax[i], &tests, &nodes) ? 1 : 0;
   if (st.overflow) atomicOr(errors, (uint32_t)kDevErrStack);
+}
+
+__global__ void k_debug_density(int n, uint32_t tex, const float* p, float* out, uint32_t* errors) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const DeviceScene& S = c_scenes[0];
+  out[i] = texture_eval(S.textures, tex, vec3(p[3 * i], p[3 * i + 1], p[3 * i + 2]), errors).x;
 }
 
 __global__ void k_debug_halton(int n, const int* px, const int* py, const int* sample, int n_dims, uint64_t* index,
@@ -1341,10 +1350,11 @@ __global__ void k_finish(WaveControl* ctl, WaveCounters* counters, unsigned long
 
 namespace {
 
-// Persistent grid sizes: resident blocks per SM x SMs, per kernel.
+// Persistent grid size (resident blocks per SM x SMs) of k_connect, which
+// walks its queue grid-stride; the per-path kernels get one thread per slot.
 struct PersistentGrids {
   int device = -1;
-  uint32_t generate = 0, extend[2] = {0, 0}, sort = 0, shade[3] = {0, 0, 0}, connect = 0;
+  uint32_t connect = 0;
 };
 PersistentGrids g_grids;
 
@@ -1353,6 +1363,34 @@ uint32_t grid_for(K kernel, int block, int sms) {
   int per_sm = 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, block, 0) != cudaSuccess || per_sm < 1) per_sm = 1;
   return (uint32_t)(per_sm * sms);
+}
+
+// The wave's extend, shade and connect launches for scene features kF. The
+// surface kernels depend on the sphere bit only (grids are media), so they
+// are instantiated for kF & kFeatSpheres.
+template <uint32_t kF>
+void launch_extend(bool volumes, uint32_t blocks, const PathPool& A, const WaveControl* ctl, const HitPool& Hs,
+                   const JobDesc* jobs, WaveCounters* counters, cudaStream_t stream) {
+  constexpr uint32_t kS = kF & kFeatSpheres;
+  if (volumes) k_extend<true, kF><<<blocks, kTraceBlock, 0, stream>>>(A, ctl, Hs, jobs, counters);
+  else k_extend<false, kS><<<blocks, kTraceBlock, 0, stream>>>(A, ctl, Hs, jobs, counters);
+}
+
+template <uint32_t kF>
+void launch_shade(bool adjoint, bool volumes, const ShadowQueue* defer, uint32_t blocks, const PathPool& A,
+                  const WaveControl* ctl, const HitPool& Hs, const PathPool& B, const JobDesc* jobs,
+                  WaveCounters* counters, const WaveOptions& opt, cudaStream_t stream) {
+  constexpr uint32_t kS = kF & kFeatSpheres;
+  const ShadowQueue none{};
+  if (adjoint)
+    k_shade<false, false, true, kS><<<blocks, kTraceBlock, 0, stream>>>(A, ctl, Hs, B, jobs, counters, none, opt.grads,
+                                                                        opt.grad_materials);
+  else if (volumes)
+    k_shade<true, false, false, kF><<<blocks, kTraceBlock, 0, stream>>>(A, ctl, Hs, B, jobs, counters, none);
+  else if (defer)
+    k_shade<false, true, false, kS><<<blocks, kTraceBlock, 0, stream>>>(A, ctl, Hs, B, jobs, counters, *defer);
+  else
+    k_shade<false, false, false, kS><<<blocks, kTraceBlock, 0, stream>>>(A, ctl, Hs, B, jobs, counters, none);
 }
 
 }  // namespace
@@ -1365,14 +1403,7 @@ void prepare_persistent_grids() {
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   PersistentGrids g;
   g.device = dev;
-  g.generate = grid_for(k_generate, 256, sms);
-  g.extend[0] = grid_for(k_extend<false, false>, kTraceBlock, sms);
-  g.extend[1] = grid_for(k_extend<true, false>, kTraceBlock, sms);
-  g.sort = grid_for(k_sort_hits, 256, sms);
-  g.shade[0] = grid_for(k_shade<false, false>, kTraceBlock, sms);
-  g.shade[1] = grid_for(k_shade<false, true>, kTraceBlock, sms);
-  g.shade[2] = grid_for(k_shade<true, false>, kTraceBlock, sms);
-  g.connect = grid_for(k_connect<false>, kTraceBlock, sms);
+  g.connect = grid_for(k_connect<0>, kTraceBlock, sms);
   g_grids = g;
 }
 
@@ -1386,7 +1417,7 @@ uint32_t launch_wave(const PathPool& A, const PathPool& B, const HitPool& H, Wav
   const bool sort_hits = opt.sort_hits && !adjoint;
   HitPool Hs = H;
   if (!sort_hits) Hs.order = nullptr;
-  const ShadowQueue none{};
+  const uint32_t feat = opt.features & kFeatAll;
   // The per-path kernels get one thread per pool slot (blocks past the
   // wave's count return at once), so the hardware block scheduler balances
   // the uneven per-ray work; k_connect walks its queue with a GPU-sized grid.
@@ -1396,25 +1427,24 @@ uint32_t launch_wave(const PathPool& A, const PathPool& B, const HitPool& H, Wav
   if (ev) cudaEventRecord(ev[0], stream);
   k_generate<<<blocks_256, 256, 0, stream>>>(A, ctl, jobs, n_jobs);
   if (ev) cudaEventRecord(ev[1], stream);
-  if (opt.volumes && opt.spheres) k_extend<true, true><<<blocks_trace, kTraceBlock, 0, stream>>>(A, ctl, Hs, jobs, counters);
-  else if (opt.volumes) k_extend<true, false><<<blocks_trace, kTraceBlock, 0, stream>>>(A, ctl, Hs, jobs, counters);
-  else if (opt.spheres) k_extend<false, true><<<blocks_trace, kTraceBlock, 0, stream>>>(A, ctl, Hs, jobs, counters);
-  else k_extend<false, false><<<blocks_trace, kTraceBlock, 0, stream>>>(A, ctl, Hs, jobs, counters);
+  switch (feat) {
+    case 0: launch_extend<0>(opt.volumes, blocks_trace, A, ctl, Hs, jobs, counters, stream); break;
+    case 1: launch_extend<1>(opt.volumes, blocks_trace, A, ctl, Hs, jobs, counters, stream); break;
+    case 2: launch_extend<2>(opt.volumes, blocks_trace, A, ctl, Hs, jobs, counters, stream); break;
+    default: launch_extend<3>(opt.volumes, blocks_trace, A, ctl, Hs, jobs, counters, stream); break;
+  }
   if (ev) cudaEventRecord(ev[2], stream);
   if (sort_hits) k_sort_hits<<<blocks_256, 256, 0, stream>>>(ctl, Hs, A, jobs, counters);
   if (ev) cudaEventRecord(ev[3], stream);
-  if (adjoint)
-    k_shade<false, false, true><<<blocks_trace, kTraceBlock, 0, stream>>>(A, ctl, Hs, B, jobs, counters, none,
-                                                                         opt.grads, opt.grad_materials);
-  else if (opt.volumes)
-    k_shade<true, false><<<blocks_trace, kTraceBlock, 0, stream>>>(A, ctl, Hs, B, jobs, counters, none);
-  else if (defer)
-    k_shade<false, true><<<blocks_trace, kTraceBlock, 0, stream>>>(A, ctl, Hs, B, jobs, counters, *defer);
-  else
-    k_shade<false, false><<<blocks_trace, kTraceBlock, 0, stream>>>(A, ctl, Hs, B, jobs, counters, none);
+  switch (feat) {
+    case 0: launch_shade<0>(adjoint, opt.volumes, defer, blocks_trace, A, ctl, Hs, B, jobs, counters, opt, stream); break;
+    case 1: launch_shade<1>(adjoint, opt.volumes, defer, blocks_trace, A, ctl, Hs, B, jobs, counters, opt, stream); break;
+    case 2: launch_shade<2>(adjoint, opt.volumes, defer, blocks_trace, A, ctl, Hs, B, jobs, counters, opt, stream); break;
+    default: launch_shade<3>(adjoint, opt.volumes, defer, blocks_trace, A, ctl, Hs, B, jobs, counters, opt, stream); break;
+  }
   if (ev) cudaEventRecord(ev[4], stream);
-  if (defer && opt.spheres) k_connect<true><<<g.connect, kTraceBlock, 0, stream>>>(*defer, jobs, counters);
-  else if (defer) k_connect<false><<<g.connect, kTraceBlock, 0, stream>>>(*defer, jobs, counters);
+  if (defer && (feat & kFeatSpheres)) k_connect<kFeatSpheres><<<g.connect, kTraceBlock, 0, stream>>>(*defer, jobs, counters);
+  else if (defer) k_connect<0><<<g.connect, kTraceBlock, 0, stream>>>(*defer, jobs, counters);
   if (ev) cudaEventRecord(ev[5], stream);
   k_finish<<<1, 32, 0, stream>>>(ctl, counters, graph_condition);
   return 5u + (sort_hits ? 1u : 0u) + (defer ? 1u : 0u);
@@ -1430,6 +1460,11 @@ void launch_debug_trace(int n, const float* o, const float* d, const uint32_t* l
   if (n <= 0) return;
   k_debug_trace<<<(n + kTraceBlock - 1) / kTraceBlock, kTraceBlock, 0, stream>>>(n, o, d, lh, inst, tri, t, bary, back,
                                                                                  nearby, errors);
+}
+
+void launch_debug_density(int n, uint32_t tex, const float* p, float* out, uint32_t* err, cudaStream_t stream) {
+  if (n <= 0) return;
+  k_debug_density<<<(n + 255) / 256, 256, 0, stream>>>(n, tex, p, out, err);
 }
 
 void launch_debug_occluded(int n, const float* o, const float* d, const float* tmax, int* occ, uint32_t* errors,

@@ -128,18 +128,29 @@ static_assert(sizeof(RenderSetting) == 40, "RenderSetting layout");
 
 // Texture subset used on the hot path: constants and the fBm noise node
 // (src/Texture.h:168-690 holds the full union). Children are texture indices.
+//
+// kTexGrid is this project's density grid (the reference's texture graph has
+// no grid node; a caller attaches one with ymrt_scene_set_density_grid): an
+// nx x ny x nz lattice of values spanning the volume's object-space box
+// [-0.5, 0.5]^3 with samples at cell centres, read trilinearly with clamped
+// edges, stored as float32 or float16. `value` holds its maximum (the node's
+// upper bound).
 enum TextureType : uint32_t {
   kTexImage = 0, kTexConstFloat = 1, kTexConstRgb = 2, kTexChecker = 3, kTexNoise = 4, kTexFbm = 5,
   kTexTurbulence = 6, kTexMarble = 7, kTexWood = 8, kTexPolkaDot = 9, kTexWave = 10,
+  kTexGrid = 64,
 };
 struct Texture {
   uint32_t type;
   uint32_t child[2];   // black / white inputs (kEmpty when absent)
-  float value;         // constant float
+  float value;         // constant float (grid: the maximum value)
   vec3 color;          // constant rgb
   float frequency, lacunarity, gain, amplitude, offset;
   int layer_count;
   int normalized;
+  int grid_n[3];       // grid: lattice size x, y, z
+  int grid_half;       // grid: values are float16 (else float32)
+  const void* grid;    // grid: device values, x fastest
 };
 
 // Ray-transfer stack of nested media, src/Ray.h:106-260 (RayTransfer).
@@ -186,6 +197,12 @@ static_assert(sizeof(WideNode) == 80, "WideNode is five 16-byte words");
 // GeometryData::geometry_type (src/GeometryDefines.h:10-14).
 constexpr uint32_t kGeoMesh = 0, kGeoSphere = 1;
 
+// Scene features the kernels are specialised on (template argument kF): a
+// batch whose scenes hold no sphere geometry or no density grid runs
+// instantiations without that code, so its register allocation is the same
+// as if the feature did not exist.
+constexpr uint32_t kFeatSpheres = 1, kFeatGrids = 2, kFeatAll = 3;
+
 // Per-geometry tables (offsets into the flattened global arrays). A sphere
 // (kind kGeoSphere) is centred on its object-space origin and has no
 // triangles or bottom-level nodes.
@@ -222,6 +239,7 @@ struct DeviceScene {
   uint32_t geometry_count;
   const GeometryDesc* geometries;
   uint32_t sphere_count;        // sphere geometries (0: the traversal skips sphere tests)
+  uint32_t grid_count;          // density-grid texture nodes
   const WideNode* blas_nodes;
   const float4* wtris;          // 3 per triangle: v0, v1, v2 (w of v0 = triangle id bits)
   const uint32_t* tri_corners;  // 3 per triangle (Triangle id0,id1,id2)

@@ -441,6 +441,16 @@ def spheres_scene(seed: int = 0) -> Scene:
     return s
 
 
+def volumetric_const_scene(seed: int = 0) -> Scene:
+    """The volumetric scene with the smoke's fBm density replaced by the
+    constant 0.5 (same node name and index): a density grid of 0.5s attached
+    to that node must render exactly as this constant."""
+    s = volumetric_scene(seed)
+    s.textures = [t if t[1] != "density_fbm" else ("ConstantTextureFloat", "density_fbm", {"value": 0.5})
+                  for t in s.textures]
+    return s
+
+
 def glossy_scene(seed: int = 0) -> Scene:
     """The Cornell-like scene with a rough GGX conductor tall box and a
     rough plastic-like (diffuse + specular) short box: every differentiated
@@ -476,7 +486,22 @@ SCENES = {
     "instanced": instanced_scene,
     "spheres": spheres_scene,
     "volumetric": volumetric_scene,
+    "volumetric_const": volumetric_const_scene,
 }
+
+
+def fbm_grid(scene, texture_index: int, n: int = 128) -> np.ndarray:
+    """An n^3 lattice (cell centres of the object-space box [-0.5, 0.5]^3)
+    of texture node `texture_index` of an uploaded scene (ymrt_b200.Scene),
+    evaluated on the device and scaled so that its maximum is 1: the density
+    grid of the media workload, whose volume's sigma_t is then the maximum
+    extinction."""
+    c = (np.arange(n, dtype=np.float32) + np.float32(0.5)) / np.float32(n) - np.float32(0.5)
+    z, y, x = np.meshgrid(c, c, c, indexing="ij")
+    pts = np.stack([x, y, z], axis=-1).reshape(-1, 3)
+    v = scene.density(texture_index, pts).reshape(n, n, n)
+    v = np.maximum(v, 0.0)
+    return (v / max(float(v.max()), 1e-12)).astype(np.float32)
 
 
 def scene_path(name: str, seed: int = 0, cache_dir: str | None = None) -> str:
