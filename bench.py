@@ -284,12 +284,14 @@ def run_batch_workload(args):
     return result if rank == 0 else None
 
 
-def run_diff_workload(args):
+def run_diff_workload(args, media=False):
     """Differentiable batched render: 16 views of the instanced scene (32
     materials) at 512x512, 16 spp, forward with path records and the
     path-replay backward of an L2 loss against a target rendered with
     perturbed albedos and roughnesses. Reports the forward and backward
-    device times and their ratio."""
+    device times and their ratio. media=True: the scene sits in a box of fog
+    whose density is a 64^3 float32 grid, the target's grid is scaled per cell
+    by U[0.5, 1.5], and the backward pass also returns dLoss/d(grid)."""
     import torch
     import ymrt_b200 as Y
     from ymrt_b200 import scenes
@@ -299,10 +301,17 @@ def run_diff_workload(args):
     perm = scenes.halton_permutations()
     n_views, size, spp = 16, 512, 16
     ctx = Y.Context(local_rank)
-    path = scenes.scene_path("instanced", 0)
-    views = [Y.Scene(ctx, Y.HostScene(path, size, size, camera=scenes.orbit_view("instanced", 0, v, n_views)), perm)
+    name = "instanced_fog" if media else "instanced"
+    path = scenes.scene_path(name, 0)
+    views = [Y.Scene(ctx, Y.HostScene(path, size, size, camera=scenes.orbit_view(name, 0, v, n_views)), perm)
              for v in range(n_views)]
-    setting = Y.default_setting(spp=spp, ray_depth=12)
+    setting = Y.default_setting(spp=spp, ray_depth=12, volume=media)
+    grid_n, fog_tex = 64, 0
+    grid = scenes.smooth_grid(grid_n, 5) if media else None
+    if media:
+        target_grid = (grid * np.random.default_rng(4).uniform(0.5, 1.5, grid.shape)).astype(np.float32)
+        for v in views:
+            v.set_density_grid(fog_tex, target_grid)
     images = [torch.zeros((size, size, 4), dtype=torch.float32, device="cuda") for _ in views]
     renders = [[v, setting, 1, img] for v, img in zip(views, images)]
     records = [torch.zeros((Y.path_count(r), 4), dtype=torch.float32, device="cuda") for r in renders]
@@ -318,7 +327,10 @@ def run_diff_workload(args):
     targets = [img.clone() for img in images]
     for v in views:
         v.set_material_params(params)
+        if media:
+            v.set_density_grid(fog_tex, grid)
     grads = torch.zeros((params.shape[0], 4), dtype=torch.float32, device="cuda")
+    grid_grads = torch.zeros(grid_n ** 3, dtype=torch.float32, device="cuda") if media else None
     fwd_ms, bwd_ms, plain_ms = [], [], []
     for i in range(args.warmup + args.steps):
         for r in renders:
@@ -326,12 +338,29 @@ def run_diff_workload(args):
         st_plain = Y.render_batch(ctx, renders)  # the plain forward (no records, deferred shadow rays)
         st_f = Y.render_batch(ctx, renders, records)
         dl = [2.0 * (img - t) for img, t in zip(images, targets)]
-        st_b = Y.render_backward(ctx, renders, records, dl, grads)
+        if media:
+            st_b = Y.render_backward_ex(ctx, renders, records, dl, material_grads=grads, grid_texture=fog_tex,
+                                        grid_grads=grid_grads)
+        else:
+            st_b = Y.render_backward(ctx, renders, records, dl, grads)
         if i >= args.warmup:
             plain_ms.append(st_plain.ms_total)
             fwd_ms.append(st_f.ms_total)
             bwd_ms.append(st_b.ms_total)
         errors = st_f.device_errors | st_b.device_errors
+    # per-stage device times of one profiled forward (recorded) and backward
+    Y.library().ymrt_set_profiling(ctx.h, 1)
+    st_pf = Y.render_batch(ctx, renders, records)
+    if media:
+        st_pb = Y.render_backward_ex(ctx, renders, records, dl, material_grads=grads, grid_texture=fog_tex,
+                                     grid_grads=grid_grads)
+    else:
+        st_pb = Y.render_backward(ctx, renders, records, dl, grads)
+    Y.library().ymrt_set_profiling(ctx.h, 0)
+
+    def stages(st):
+        return {k: round(getattr(st, "ms_" + k), 2) for k in ("generate", "extend", "sort", "shade", "connect")}
+
     g = grads.cpu().numpy()
     plain, fwd, bwd = float(np.mean(plain_ms)), float(np.mean(fwd_ms)), float(np.mean(bwd_ms))
     rays = st_f.extension_rays + st_f.shadow_rays
@@ -341,12 +370,16 @@ def run_diff_workload(args):
         "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded .ymtmp scene generated by ymrt_b200.scenes, 16 orbit views)",
         "config": {"workload": f"differentiable: {n_views} views {size}x{size} {spp}spp depth 12 of the instanced "
-                               "scene, L2 loss against perturbed-parameter target",
-                   "params": "32 materials x (albedo rgb, roughness)"},
+                               "scene" + (" in a fog box with a 64^3 float32 density grid" if media else "") +
+                               ", L2 loss against perturbed-parameter target",
+                   "params": "32 materials x (albedo rgb, roughness)" + (" + 64^3 density grid" if media else "")},
         "forward_plain_ms": round(plain, 3), "forward_recorded_ms": round(fwd, 3), "backward_ms": round(bwd, 3),
         "backward_over_plain_forward": round(bwd / plain, 3),
+        "stage_ms": {"forward_recorded": stages(st_pf), "backward": stages(st_pb)},
         "grad_norm": float(np.linalg.norm(g)), "device_errors": int(errors),
     }
+    if media:
+        result["grid_grad_norm"] = float(torch.linalg.vector_norm(grid_grads).item())
     for v in views:
         v.close()
     ctx.close()
@@ -668,7 +701,7 @@ def main(argv=None):
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["batch", "diff"], default="instanced")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["batch", "diff", "diff_media"], default="instanced")
     ap.add_argument("--spp", type=int, default=0)
     ap.add_argument("--queue", type=int, default=0, help="path queue capacity (0 = library default)")
     ap.add_argument("--cpu-budget", type=float, default=12.0, help="seconds of CPU work per reference sample")
@@ -684,8 +717,8 @@ def main(argv=None):
             res = run_reference(args)
     elif args.workload == "batch":
         res = run_batch_workload(args)
-    elif args.workload == "diff":
-        res = run_diff_workload(args)
+    elif args.workload in ("diff", "diff_media"):
+        res = run_diff_workload(args, media=args.workload == "diff_media")
     else:
         res = run_ours(args)
     if res is not None:

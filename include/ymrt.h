@@ -206,9 +206,32 @@ unsigned long long ymrt_job_path_count(const ymrt_job* job);
  * path_radiance_device set, with unchanged scenes and settings: every path is
  * re-traced with its own samples. grads_device receives 4 floats per material
  * (n_materials materials, in the scene's material order), overwritten.
- * Surfaces only: volume scattering and the indirect clamp are rejected. */
+ * The indirect clamp is rejected. */
 int ymrt_render_backward(ymrt_context* ctx, const ymrt_job* jobs, int n_jobs, float* grads_device,
                          uint32_t n_materials, ymrt_stats* stats);
+
+/* What ymrt_render_backward_ex differentiates. Either target may be absent
+ * (NULL). Material gradients: 4 floats per material as ymrt_render_backward.
+ * Density-grid gradients (no counterpart in the reference): dLoss/d(value)
+ * of the grid attached to texture node grid_texture
+ * (ymrt_scene_set_density_grid), one float per grid value in the grid's
+ * order, summed over every job; each job's scene must hold a grid of
+ * grid_values values at that node, and the jobs must scatter in media. */
+typedef struct ymrt_backward_targets {
+  float* material_grads_device;
+  uint32_t n_materials;
+  uint32_t grid_texture;
+  float* grid_grads_device;
+  uint64_t grid_values;
+  uint32_t reserved[4];
+} ymrt_backward_targets;
+
+/* ymrt_render_backward with material and/or density-grid targets; media
+ * (volume scattering) are differentiated too: free-flight sampling and
+ * shadow-ray transmittance contribute the grid's terms, with the tracking
+ * decisions and the majorant held fixed. The outputs are overwritten. */
+int ymrt_render_backward_ex(ymrt_context* ctx, const ymrt_job* jobs, int n_jobs, const ymrt_backward_targets* targets,
+                            ymrt_stats* stats);
 
 /* Material parameters a backward pass differentiates, 4 floats per material:
  * diffuse albedo r, g, b and roughness (stored as alpha_x and alpha_y). Light

@@ -126,6 +126,8 @@ def library():
     L.ymrt_scene_set_sobol_matrices.argtypes = [vp, vp, sz]
     L.ymrt_render_batch.argtypes = [vp, ctypes.POINTER(Job), i, ctypes.POINTER(Stats)]
     L.ymrt_render_backward.argtypes = [vp, ctypes.POINTER(Job), i, vp, ctypes.c_uint32, ctypes.POINTER(Stats)]
+    L.ymrt_render_backward_ex.argtypes = [vp, ctypes.POINTER(Job), i, ctypes.POINTER(BackwardTargets),
+                                          ctypes.POINTER(Stats)]
     L.ymrt_job_path_count.restype = ctypes.c_ulonglong
     L.ymrt_job_path_count.argtypes = [ctypes.POINTER(Job)]
     L.ymrt_scene_set_material_params.argtypes = [vp, ctypes.c_uint32, ctypes.c_uint32, vp]
@@ -425,6 +427,32 @@ def render_batch(ctx: Context, renders, records=None) -> Stats:
 def path_count(render) -> int:
     """Paths the render (as render_batch takes it) traces."""
     return int(library().ymrt_job_path_count(ctypes.byref(_jobs([render])[0])))
+
+
+class BackwardTargets(ctypes.Structure):
+    _fields_ = [("material_grads_device", ctypes.c_void_p), ("n_materials", ctypes.c_uint32),
+                ("grid_texture", ctypes.c_uint32), ("grid_grads_device", ctypes.c_void_p),
+                ("grid_values", ctypes.c_uint64), ("reserved", ctypes.c_uint32 * 4)]
+
+
+def render_backward_ex(ctx: Context, renders, records, dlosses, material_grads=None, grid_texture=None,
+                       grid_grads=None) -> Stats:
+    """render_backward with optional targets: `material_grads` (CUDA float32,
+    (materials, 4)) and/or `grid_grads` (CUDA float32, one value per value of
+    the density grid attached to texture node `grid_texture`, in the grid's
+    (nz, ny, nx) order). Media are differentiated."""
+    jobs = _jobs(renders, records, dlosses)
+    t = BackwardTargets()
+    t.grid_texture = 0xFFFFFFFF
+    if material_grads is not None:
+        assert material_grads.is_cuda and material_grads.dtype.is_floating_point and material_grads.is_contiguous()
+        t.material_grads_device, t.n_materials = material_grads.data_ptr(), material_grads.shape[0]
+    if grid_grads is not None:
+        assert grid_grads.is_cuda and grid_grads.is_contiguous() and grid_texture is not None
+        t.grid_texture, t.grid_grads_device, t.grid_values = grid_texture, grid_grads.data_ptr(), grid_grads.numel()
+    stats = Stats()
+    _check(library().ymrt_render_backward_ex(ctx.h, jobs, len(renders), ctypes.byref(t), ctypes.byref(stats)), ctx.h)
+    return stats
 
 
 def render_backward(ctx: Context, renders, records, dlosses, grads) -> Stats:

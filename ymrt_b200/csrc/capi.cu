@@ -707,7 +707,7 @@ int run_batch(ymrt_context* ctx, const BatchMemory& M, std::vector<JobDesc>& job
         (uintptr_t)M.pool[0].ray_o, (uintptr_t)M.pool[1].ray_o, (uintptr_t)M.hits.bary_t, (uintptr_t)M.ctl,
         (uintptr_t)M.jobs, (uintptr_t)M.counters, (uintptr_t)jobs.size(), (uintptr_t)o.volumes,
         (uintptr_t)o.sort_hits, (uintptr_t)o.defer_shadows, (uintptr_t)o.shadow_queue.o, M.capacity,
-        (uintptr_t)o.features,
+        (uintptr_t)o.features, (uintptr_t)o.grid_grads, (uintptr_t)o.grid_tex,
         (uintptr_t)o.adjoint, (uintptr_t)o.grads, o.grad_materials};
     if (ctx->graph_key != key) {
       ctx->drop_graph();
@@ -992,29 +992,41 @@ unsigned long long ymrt_job_path_count(const ymrt_job* job) {
   return (unsigned long long)(t_end - t_begin) * kTilePixels * (uint32_t)std::max(job->setting.ssp, 1);
 }
 
-int ymrt_render_backward(ymrt_context* ctx, const ymrt_job* jobs_in, int n_jobs, float* grads_device,
-                         uint32_t n_materials, ymrt_stats* stats) {
-  if (!ctx || !jobs_in || n_jobs <= 0 || !grads_device || n_materials == 0) return YMRT_ERR_INVALID;
+int ymrt_render_backward_ex(ymrt_context* ctx, const ymrt_job* jobs_in, int n_jobs, const ymrt_backward_targets* tg,
+                            ymrt_stats* stats) {
+  if (!ctx || !jobs_in || n_jobs <= 0 || !tg) return YMRT_ERR_INVALID;
+  const bool materials = tg->material_grads_device && tg->n_materials > 0;
+  const bool grid = tg->grid_grads_device != nullptr;
+  if (!materials && !grid) return ctx->fail(YMRT_ERR_INVALID, "backward: no gradient requested");
   cudaSetDevice(ctx->device);
   cudaStream_t st = ctx->stream;
   cudaError_t e;
   std::vector<JobDesc> jobs((size_t)n_jobs);
   std::vector<DeviceScene> scenes((size_t)n_jobs);
   std::vector<const void*> keys((size_t)n_jobs);
+  bool volumes = false;
   for (int k = 0; k < n_jobs; ++k) {
     const ymrt_job& in = jobs_in[k];
     if (!in.path_radiance_device || !in.dloss_device)
       return ctx->fail(YMRT_ERR_INVALID, "backward: every job needs its recorded path radiance and dLoss/dImage");
-    if (in.setting.enable_volume_scattering)
-      return ctx->fail(YMRT_ERR_UNSUPPORTED, "backward: volume scattering is not differentiated");
     if (in.setting.enable_indirect_clamp)
       return ctx->fail(YMRT_ERR_UNSUPPORTED, "backward: the indirect clamp is not differentiated");
+    if (grid) {
+      if (!in.scene || tg->grid_texture >= in.scene->textures.size())
+        return ctx->fail(YMRT_ERR_INVALID, "backward: grid texture index out of range");
+      const Texture& t = in.scene->textures[tg->grid_texture];
+      if (t.type != kTexGrid ||
+          (uint64_t)t.grid_n[0] * (uint64_t)t.grid_n[1] * (uint64_t)t.grid_n[2] != tg->grid_values)
+        return ctx->fail(YMRT_ERR_INVALID, "backward: the grid texture node is not a grid of grid_values values");
+    }
+    volumes = volumes || in.setting.enable_volume_scattering;
     int rc = make_job(ctx, in.scene, &in.setting, in.frame_index, in.tile_begin, in.tile_end,
                       reinterpret_cast<float4*>(in.out_rgba_device), &jobs[k], &scenes[k], in.path_radiance_device,
                       in.dloss_device);
     if (rc != YMRT_OK) return rc;
     keys[k] = in.scene;
   }
+  if (grid && !volumes) return ctx->fail(YMRT_ERR_INVALID, "backward: grid gradients need volume scattering on");
   const std::vector<DeviceScene> slots = assign_slots(jobs, scenes, keys);
   if (slots.size() > kMaxSceneSlots) return ctx->fail(YMRT_ERR_INVALID, "backward: too many distinct scenes in one call");
   BatchMemory M;
@@ -1022,13 +1034,17 @@ int ymrt_render_backward(ymrt_context* ctx, const ymrt_job* jobs_in, int n_jobs,
   if (rc != YMRT_OK) return rc;
   WaveOptions opt;
   opt.adjoint = true;
+  opt.volumes = volumes;
   opt.features = batch_features(slots.data(), slots.size());
-  opt.grads = grads_device;
-  opt.grad_materials = n_materials;
+  opt.grads = materials ? tg->material_grads_device : nullptr;
+  opt.grad_materials = materials ? tg->n_materials : 0;
+  opt.grid_grads = grid ? tg->grid_grads_device : nullptr;
+  opt.grid_tex = grid ? tg->grid_texture : kEmpty;
   if ((e = upload_constants(slots.data(), (uint32_t)slots.size(), ctx->primes.data(), ctx->prime_sums.data(), st)) !=
       cudaSuccess)
     return ctx->cuda_fail(e, "uploading constants");
-  cudaMemsetAsync(grads_device, 0, sizeof(float) * kGradParams * n_materials, st);
+  if (materials) cudaMemsetAsync(tg->material_grads_device, 0, sizeof(float) * kGradParams * tg->n_materials, st);
+  if (grid) cudaMemsetAsync(tg->grid_grads_device, 0, sizeof(float) * tg->grid_values, st);
   BatchResult r;
   if ((rc = run_batch(ctx, M, jobs, opt, ctx->profiling, ctx->graph_loop, &r)) != YMRT_OK) return rc;
   if ((e = cudaMemcpyAsync(ctx->counters_host, M.counters, sizeof(WaveCounters), cudaMemcpyDeviceToHost, st)) !=
@@ -1036,6 +1052,16 @@ int ymrt_render_backward(ymrt_context* ctx, const ymrt_job* jobs_in, int n_jobs,
     return ctx->cuda_fail(e, "reading counters");
   if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return ctx->cuda_fail(e, "backward");
   return finish_batch(ctx, r, stats);
+}
+
+int ymrt_render_backward(ymrt_context* ctx, const ymrt_job* jobs_in, int n_jobs, float* grads_device,
+                         uint32_t n_materials, ymrt_stats* stats) {
+  if (!ctx || !jobs_in || n_jobs <= 0 || !grads_device || n_materials == 0) return YMRT_ERR_INVALID;
+  ymrt_backward_targets tg{};
+  tg.material_grads_device = grads_device;
+  tg.n_materials = n_materials;
+  tg.grid_texture = kEmpty;
+  return ymrt_render_backward_ex(ctx, jobs_in, n_jobs, &tg, stats);
 }
 
 int ymrt_scene_set_material_params(ymrt_scene* scene, uint32_t first, uint32_t count, const float* params) {

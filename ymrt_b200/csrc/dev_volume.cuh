@@ -396,12 +396,68 @@ __device__ __forceinline__ void densities(const DeviceScene& S, int n, const int
   }
 }
 
+// ---- density-grid gradients (the adjoint pass) ----
+//
+// A tracking estimator's value is f / p with f the product, over its
+// tentative collisions x_j, of exp(-m * step) and
+//   null collision:  m - sigma_t(x_j)           (delta and ratio tracking)
+//   real collision:  sigma_s(x_j)               (delta tracking's last one)
+// and p the sampling pdf. With the samples (and the majorant m, which the
+// estimator's expectation does not depend on) held fixed, d(f/p)/d(g_k) for
+// a grid value g_k is (f/p) times the sum over collisions of
+//   null:  -d sigma_t(x_j)/d g_k / (m - sigma_t(x_j))
+//   real:   d sigma_s(x_j)/d g_k / sigma_s(x_j)
+// per colour channel, where sigma_t = sigma_t,vol * density and density is
+// the grid's trilinear read, linear in g_k with weight w_k(x_j). `scale` is
+// dLoss/d(radiance) times the radiance the estimator multiplies, per
+// channel; each collision adds its terms to the eight grid cells it reads.
+struct MediumAdj {
+  vec3 scale;
+  uint32_t grid_tex;   // the differentiated grid node
+  float* grads;        // dLoss/d(grid value), x fastest
+};
+
+// grads += g * (trilinear weight of each of the eight cells read at p).
+__device__ __forceinline__ void grid_scatter(const Texture& t, vec3 p, float g, float* grads) {
+  int x[2], y[2], z[2];
+  float wx, wy, wz;
+  grid_axis(p.x, t.grid_n[0], &x[0], &x[1], &wx);
+  grid_axis(p.y, t.grid_n[1], &y[0], &y[1], &wy);
+  grid_axis(p.z, t.grid_n[2], &z[0], &z[1], &wz);
+  const float fx[2] = {1.0f - wx, wx}, fy[2] = {1.0f - wy, wy}, fz[2] = {1.0f - wz, wz};
+  for (int c = 0; c < 8; ++c) {
+    const float w = fx[c & 1] * fy[(c >> 1) & 1] * fz[c >> 2];
+    if (w == 0.0f) continue;
+    const size_t k = ((size_t)z[c >> 2] * (size_t)t.grid_n[1] + (size_t)y[(c >> 1) & 1]) * (size_t)t.grid_n[0] +
+                     (size_t)x[c & 1];
+    atomicAdd(grads + k, g * w);
+  }
+}
+
+// One tentative collision's terms: coef_t (per channel) multiplies
+// d sigma_t / d density of each medium, coef_s multiplies d sigma_s / d density.
+__device__ __noinline__ void medium_grad(const DeviceScene& S, int n, const int* vidx, const vec3* ro, const vec3* rd,
+                                         float acc, vec3 coef_t, vec3 coef_s, const MediumAdj& am) {
+  for (int i = 0; i < n; ++i) {
+    const Volume& v = S.volumes[vidx[i]];
+    if (v.density_texture_idx != (int)am.grid_tex || !has_density(S, v)) continue;
+    const Texture& t = S.textures[am.grid_tex];
+    if (t.type != kTexGrid) continue;
+    const vec3 p = ro[i] + rd[i] * acc;
+    if (!(grid_eval(t, p) > 0.0f)) continue;  // the density is clamped at zero
+    const float g = dot(coef_t, v.sigma_t) + dot(coef_s, v.sigma_t * v.albedo);
+    if (g != 0.0f) grid_scatter(t, p, g, am.grads);
+  }
+}
+
 // SampleTrHeterogeneous (src/VolumeEval.cuh:80-214): delta tracking against
 // the summed majorant with channel-wise real / null collision probabilities.
-template <uint32_t kF>
+// kAdj: also adds the segment's density-grid gradient terms (MediumAdj).
+template <uint32_t kF, bool kAdj = false>
 __device__ __noinline__ bool sample_tr_heterogeneous(const DeviceScene& S, int n, const int* vidx, vec3 o, vec3 d,
                                                      float t_max, vec3* tr_weight, float* dist, float* vw,
-                                                     PathSampler& hs, uint32_t* errors) {
+                                                     PathSampler& hs, uint32_t* errors,
+                                                     const MediumAdj* am = nullptr) {
   *tr_weight = vec3(1.0f);
   *dist = kFloatMax;
   Majorant M;
@@ -442,10 +498,20 @@ __device__ __noinline__ bool sample_tr_heterogeneous(const DeviceScene& S, int n
     if (sample1d(hs, S) < real[ch]) {
       tr *= ptr * mss * nf;
       pdf *= ptr * M.m * real * nf;
+      if constexpr (kAdj) {
+        vec3 cs(0.0f);
+        for (int c = 0; c < 3; ++c) cs[c] = mss[c] > 0.0f ? am->scale[c] / mss[c] : 0.0f;
+        medium_grad(S, n, vidx, M.ro, M.rd, acc, vec3(0.0f), cs, *am);
+      }
       break;
     } else {
       tr *= ptr * M.m * fake * nf;
       pdf *= ptr * M.m * fake * nf;
+      if constexpr (kAdj) {
+        vec3 ct(0.0f);
+        for (int c = 0; c < 3; ++c) ct[c] = M.m[c] - mst[c] > 0.0f ? -am->scale[c] / (M.m[c] - mst[c]) : 0.0f;
+        medium_grad(S, n, vidx, M.ro, M.rd, acc, ct, vec3(0.0f), *am);
+      }
     }
     ++it;
   }
@@ -457,10 +523,11 @@ __device__ __noinline__ bool sample_tr_heterogeneous(const DeviceScene& S, int n
 }
 
 // SampleVolumeScattering (src/VolumeEval.cuh:217-251).
-template <uint32_t kF>
+template <uint32_t kF, bool kAdj = false>
 __device__ __forceinline__ bool sample_volume_scattering(const DeviceScene& S, vec3 o, vec3 d, int n, const int* vidx,
                                                          float t_max, vec3* tr_weight, float* dist, float* vw,
-                                                         PathSampler& hs, uint32_t* errors) {
+                                                         PathSampler& hs, uint32_t* errors,
+                                                         const MediumAdj* am = nullptr) {
   if (S.volume_count == 0 || n == 0) return false;
   bool het = false;
   for (int i = 0; i < n; ++i)
@@ -468,15 +535,17 @@ __device__ __forceinline__ bool sample_volume_scattering(const DeviceScene& S, v
       het = true;
       break;
     }
-  if (het) return sample_tr_heterogeneous<kF>(S, n, vidx, o, d, t_max, tr_weight, dist, vw, hs, errors);
+  if (het) return sample_tr_heterogeneous<kF, kAdj>(S, n, vidx, o, d, t_max, tr_weight, dist, vw, hs, errors, am);
   return sample_tr_homogeneous(S, n, vidx, t_max, tr_weight, dist, vw, hs);
 }
 
 // EvalTrHeterogeneous (src/VolumeEval.cuh:269-386): ratio-tracking style
-// transmittance with Russian roulette after 32 steps.
-template <uint32_t kF>
+// transmittance with Russian roulette after 32 steps. kAdj: also adds the
+// density-grid gradient terms of its collisions (MediumAdj).
+template <uint32_t kF, bool kAdj = false>
 __device__ __noinline__ vec3 eval_tr_heterogeneous(const DeviceScene& S, int n, const int* vidx, vec3 o, vec3 d,
-                                                   float t_max, PathSampler& hs, uint32_t* errors) {
+                                                   float t_max, PathSampler& hs, uint32_t* errors,
+                                                   const MediumAdj* am = nullptr) {
   Majorant M;
   volume_space_rays(S, n, vidx, o, d, t_max, M);
   const float u0 = sample1d(hs, S);
@@ -513,6 +582,11 @@ __device__ __noinline__ vec3 eval_tr_heterogeneous(const DeviceScene& S, int n, 
     const vec3 ptr = vexp(-M.m * fpl);
     tr *= ptr * M.m * fake * nf;
     pdf *= ptr * M.m * nf;
+    if constexpr (kAdj) {
+      vec3 ct(0.0f);
+      for (int c = 0; c < 3; ++c) ct[c] = M.m[c] - mst[c] > 0.0f ? -am->scale[c] / (M.m[c] - mst[c]) : 0.0f;
+      medium_grad(S, n, vidx, M.ro, M.rd, acc, ct, vec3(0.0f), *am);
+    }
     if (it + 1 > 32) {
       const vec3 pt = tr * safe_rcp(dot(M.cw, pdf));
       float rr = gmax(pt.x, gmax(pt.y, pt.z));
@@ -526,9 +600,9 @@ __device__ __noinline__ vec3 eval_tr_heterogeneous(const DeviceScene& S, int n, 
 }
 
 // EvalTr (src/VolumeEval.cuh:388-418).
-template <uint32_t kF>
+template <uint32_t kF, bool kAdj = false>
 __device__ __forceinline__ vec3 eval_tr(const DeviceScene& S, vec3 o, vec3 d, const RayTransfer& rt, float t_max,
-                                        PathSampler& hs, uint32_t* errors) {
+                                        PathSampler& hs, uint32_t* errors, const MediumAdj* am = nullptr) {
   if (S.volume_count == 0) return vec3(1.0f);
   int vidx[kMaxBoundaryRecord];
   const int n = current_volumes(rt, S.volume_count, vidx);
@@ -539,7 +613,7 @@ __device__ __forceinline__ vec3 eval_tr(const DeviceScene& S, vec3 o, vec3 d, co
       het = true;
       break;
     }
-  if (het) return eval_tr_heterogeneous<kF>(S, n, vidx, o, d, t_max, hs, errors);
+  if (het) return eval_tr_heterogeneous<kF, kAdj>(S, n, vidx, o, d, t_max, hs, errors, am);
   vec3 m(0.0f);
   for (int i = 0; i < n; ++i) m += S.volumes[vidx[i]].sigma_t;
   return vexp(-m * t_max);

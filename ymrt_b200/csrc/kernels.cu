@@ -192,7 +192,8 @@ __device__ __forceinline__ void file_bucket(WaveCounters* counters, uint32_t buc
 // buckets' counts from k_extend give each bucket's start) and ends the paths
 // whose ray left the scene: the background when the environment light is on
 // (the miss branch of Ray_trace_path_tracing, src/Shading.cu:1855-1864), then
-// the path's radiance into its pixel. Misses are not listed.
+// the path's radiance into its pixel (not in the adjoint pass, whose jobs
+// carry dLoss/dImage and only replay their paths). Misses are not listed.
 __global__ void __launch_bounds__(256) k_sort_hits(const WaveControl* __restrict__ ctl, HitPool H, PathPool P,
                                                    const JobDesc* __restrict__ jobs, WaveCounters* counters) {
   __shared__ uint32_t s_start[kShadeBuckets];
@@ -220,7 +221,7 @@ __global__ void __launch_bounds__(256) k_sort_hits(const WaveControl* __restrict
       rad += indirect_clamp(J.setting, vec3(t4.x, t4.y, t4.z) * background(vec3(d4.x, d4.y, d4.z)),
                             (int)(pf.y & kFlagDepthMask));
     }
-    finish_path(J, pf.x, P.path_id[i], rad, 1.0f / gmax(J.setting.ssp, 1));
+    if (!J.dloss) finish_path(J, pf.x, P.path_id[i], rad, 1.0f / gmax(J.setting.ssp, 1));  // (adjoint: replayed only)
     b = kBucketNone;
   }
   const bool has = b != kBucketNone;
@@ -244,9 +245,15 @@ __global__ void __launch_bounds__(256) k_sort_hits(const WaveControl* __restrict
 //
 // kF: the batch's scene features (kFeatSpheres, kFeatGrids); a batch without
 // spheres or grids runs the instantiation without their code.
-template <bool kVol, uint32_t kF>
+//
+// kAdj (with kVol): the adjoint pass; each free-flight segment also adds its
+// density-grid gradient terms to grid_grads, weighted by dLoss/dI times the
+// radiance the path gathers after the segment (its recorded total minus what
+// it gathered so far).
+template <bool kVol, uint32_t kF, bool kAdj = false>
 __global__ void __launch_bounds__(kTraceBlock, 5) k_extend(PathPool P, const WaveControl* __restrict__ ctl, HitPool H,
-                                                           const JobDesc* __restrict__ jobs, WaveCounters* counters) {
+                                                           const JobDesc* __restrict__ jobs, WaveCounters* counters,
+                                                           float* grid_grads = nullptr, uint32_t grid_tex = kEmpty) {
   YM_TRAVERSAL_SHARED(s_stack);
   const uint32_t count = ctl->count;
   uint32_t tests = 0, nodes = 0, n_rays = 0;
@@ -286,8 +293,20 @@ __global__ void __launch_bounds__(kTraceBlock, 5) k_extend(PathPool P, const Wav
       vec3 trw(1.0f);
       float dist = 0.0f;
       float vw[kMaxBoundaryRecord];
-      const bool hv = sample_volume_scattering<kF>(S, o, d, n, vidx, hit ? ch.t : kTMax, &trw, &dist, vw, hs,
-                                               &counters->errors);
+      bool hv;
+      if constexpr (kAdj) {
+        MediumAdj am{vec3(0.0f), grid_tex, grid_grads};
+        if (grid_grads && J.dloss) {
+          const float4 dl = J.dloss[pf.x], lt = J.path_radiance[P.path_id[i]], r4 = P.radiance[i];
+          const float inv_spp = 1.0f / gmax(J.setting.ssp, 1);
+          am.scale = vec3(dl.x, dl.y, dl.z) * inv_spp * (vec3(lt.x, lt.y, lt.z) - vec3(r4.x, r4.y, r4.z));
+        }
+        hv = sample_volume_scattering<kF, true>(S, o, d, n, vidx, hit ? ch.t : kTMax, &trw, &dist, vw, hs,
+                                                &counters->errors, &am);
+      } else {
+        hv = sample_volume_scattering<kF>(S, o, d, n, vidx, hit ? ch.t : kTMax, &trw, &dist, vw, hs,
+                                          &counters->errors);
+      }
       const float4 t4 = P.throughput[i];
       vec3 tp(t4.x, t4.y, t4.z);
       tp *= trw;
@@ -437,10 +456,11 @@ __device__ __forceinline__ float ex_ior(const RayTransfer& rt, uint32_t hit_prim
 // and the transmittance along a shadow ray through every medium it crosses
 // (TraceTr, src/VolumeEval.cuh:420-468). `rt` is the shadow ray's own copy of
 // the nested-media stack; `o`/`d`/`tmax` and the last hit are the shadow ray.
-template <uint32_t kF>
+template <uint32_t kF, bool kAdj = false>
 __device__ __noinline__ vec3 trace_tr(uint32_t scene, TraversalStack& st, vec3 o, vec3 d, float tmax,
                                       uint32_t last_inst, uint32_t last_tri, RayTransfer& rt, PathSampler& hs,
-                                      uint32_t* errors, uint32_t* tests, uint32_t* nodes) {
+                                      uint32_t* errors, uint32_t* tests, uint32_t* nodes,
+                                      const MediumAdj* am = nullptr) {
   const DeviceScene& S = c_scenes[scene];
   if (S.volume_count == 0) return vec3(1.0f);
   vec3 tr(1.0f);
@@ -456,10 +476,10 @@ __device__ __noinline__ vec3 trace_tr(uint32_t scene, TraversalStack& st, vec3 o
     ClosestHit ch;
     const bool hit = trace_closest_impl<(kF & kFeatSpheres) != 0>(scene, st, o, d, ray_t, last_inst, last_tri, true, &ch, tests, nodes);
     if (!hit) {
-      tr *= eval_tr<kF>(S, o, d, rt, gmax(max_d - traced, 0.0f), hs, errors);
+      tr *= eval_tr<kF, kAdj>(S, o, d, rt, gmax(max_d - traced, 0.0f), hs, errors, am);
       break;
     }
-    tr *= eval_tr<kF>(S, o, d, rt, ch.t, hs, errors);
+    tr *= eval_tr<kF, kAdj>(S, o, d, rt, ch.t, hs, errors, am);
     traced += ch.t;
     vec3 hp, herr, hng;
     fetch_geometry_normal<kF>(S, ch.inst, ch.tri, vec3(ch.b0, ch.b1, ch.b2), &hp, &herr, &hng);
@@ -517,14 +537,14 @@ struct SurfaceNee {
 
 // Transmittance of an unoccluded surface shadow ray (the volume part of the
 // reference's EvalShapeLight / EvalDistantLight).
-template <bool kVol, uint32_t kF>
+template <bool kVol, uint32_t kF, bool kAdj = false>
 __device__ __forceinline__ vec3 surface_shadow_tr(const DeviceScene& S, TraversalStack& st, const SurfaceNee& c, vec3 so,
                                                   vec3 ldir, float maxd, bool tb, PathSampler& hs, uint32_t* errors,
-                                                  uint32_t* tests, uint32_t* nodes) {
+                                                  uint32_t* tests, uint32_t* nodes, const MediumAdj* am = nullptr) {
   if (!kVol || !c.media) return vec3(1.0f);
   RayTransfer srt = *c.rt;
   if (tb) boundary_transition(S, srt, c.nb, c.n_nb, errors);
-  return trace_tr<kF>(c.slot, st, so, normalize(ldir), maxd, c.inst, c.tri, srt, hs, errors, tests, nodes);
+  return trace_tr<kF, kAdj>(c.slot, st, so, normalize(ldir), maxd, c.inst, c.tri, srt, hs, errors, tests, nodes, am);
 }
 
 // ------------------------------------------------- path-replay adjoint ---
@@ -547,6 +567,8 @@ constexpr float kParamStep = 1e-3f;       // central-difference step of df/dp
 struct AdjCtx {
   vec3 weight;                            // dLoss/dI (per path) * throughput: the weight of this vertex's NEE
   float g[kGradParams];                   // accumulated dLoss/dp
+  float* grid_grads;                      // dLoss/d(density-grid value), or null
+  uint32_t grid_tex;                      // the differentiated grid node
   // Per-lobe derivative data of the vertex's layered BSDF (channel-diagonal
   // in albedo: each channel's albedo moves only that channel of f):
   vec3 lambert_coeff;                     // the diffuse lobe's colour per unit albedo
@@ -663,8 +685,20 @@ __device__ __forceinline__ void nee_shadow_ray(const DeviceScene& S, TraversalSt
     return;
   }
   if (!trace_occluded_impl<(kF & kFeatSpheres) != 0>(c.slot, st, so, normalize(ldir), maxd, tests, nodes)) {
+    const PathSampler hs0 = hs;
     const vec3 tr = surface_shadow_tr<kVol, kF>(S, st, c, so, ldir, maxd, tb, hs, errors, tests, nodes);
     *direct += mis * tr * fc * Lc;
+    if constexpr (kVol) {
+      if (adj && adj->grid_grads && c.media) {
+        // the transmittance's density-grid terms: replay its tracking with the
+        // same samples, weighted by this ray's share of dLoss
+        const MediumAdj am{adj->weight * (mul / div) * (mis * tr * fc * Lc), adj->grid_tex, adj->grid_grads};
+        if (max_component(vabs(am.scale)) > 0.0f) {
+          PathSampler h2 = hs0;
+          surface_shadow_tr<kVol, kF, true>(S, st, c, so, ldir, maxd, tb, h2, errors, tests, nodes, &am);
+        }
+      }
+    }
     if (adj) {
       // d(direct)/dp = mis * tr * fc * (df/dp)/f * Lc, scaled like the estimator
       const vec3 wo = B->to_local(-c.ray_dir), wi = B->to_local(ldir);
@@ -785,13 +819,30 @@ __device__ __forceinline__ vec3 eval_distant_light(const DeviceScene& S, Travers
   return direct / select_pdf;
 }
 
-// EvalVolumeShapeLight / EvalVolumeDistantLight (src/Shading.cu:202-291, 419-513):
-// next-event estimation at a scattering point inside the media.
+// Density-grid terms of one volume shadow ray's transmittance (the adjoint
+// pass): its tracking replayed from the sampler state `hs` it started from,
+// weighted by av->scale (dLoss/dI times throughput) times the ray's
+// contribution to the estimate (contrib / select_pdf).
 template <uint32_t kF>
+__device__ __noinline__ void volume_shadow_grad(uint32_t slot, TraversalStack& st, vec3 pos, vec3 dir, float maxd,
+                                                const RayTransfer& rt, PathSampler hs, vec3 contrib, float select_pdf,
+                                                const MediumAdj* av, uint32_t* errors, uint32_t* tests,
+                                                uint32_t* nodes) {
+  if (!av || !av->grads || !(select_pdf > 0.0f)) return;
+  const MediumAdj am{av->scale * contrib / select_pdf, av->grid_tex, av->grads};
+  if (!(max_component(vabs(am.scale)) > 0.0f)) return;
+  RayTransfer srt = rt;
+  trace_tr<kF, true>(slot, st, pos, dir, maxd, kEmpty, kEmpty, srt, hs, errors, tests, nodes, &am);
+}
+
+// EvalVolumeShapeLight / EvalVolumeDistantLight (src/Shading.cu:202-291, 419-513):
+// next-event estimation at a scattering point inside the media. kAdj: the
+// adjoint pass, which also adds each shadow ray's density-grid terms (av).
+template <uint32_t kF, bool kAdj = false>
 __device__ __noinline__ vec3 eval_volume_lights(uint32_t slot, TraversalStack& st, bool distant, int n,
                                                 const float* gs, const float* vw, vec3 ray_dir, const RayTransfer& rt,
                                                 vec3 pos, PathSampler& hs, uint32_t* shadow_rays, uint32_t* tests,
-                                                uint32_t* nodes, uint32_t* errors) {
+                                                uint32_t* nodes, uint32_t* errors, const MediumAdj* av = nullptr) {
   const DeviceScene& S = c_scenes[slot];
   vec3 direct(0.0f);
   if (distant) {
@@ -811,9 +862,14 @@ __device__ __noinline__ vec3 eval_volume_lights(uint32_t slot, TraversalStack& s
         ++*shadow_rays;
         if (!trace_occluded_impl<(kF & kFeatSpheres) != 0>(slot, st, pos, normalize(ldir), kTMax, tests, nodes)) {
           RayTransfer srt = rt;
+          const PathSampler hs0 = hs;
           const vec3 tr = trace_tr<kF>(slot, st, pos, normalize(ldir), kTMax, kEmpty, kEmpty, srt, hs, errors, tests, nodes);
           const float mis = power_heuristic(lpdf, wpdf);
-          direct += mis * tr * gmin(pw, kMaxColorClamp) * vmin(Li, vec3(kMaxColorClamp));
+          const vec3 contrib = mis * tr * gmin(pw, kMaxColorClamp) * vmin(Li, vec3(kMaxColorClamp));
+          direct += contrib;
+          if constexpr (kAdj)
+            volume_shadow_grad<kF>(slot, st, pos, normalize(ldir), kTMax, rt, hs0, contrib, select_pdf, av, errors,
+                                   tests, nodes);
         }
       }
     }
@@ -829,9 +885,14 @@ __device__ __noinline__ vec3 eval_volume_lights(uint32_t slot, TraversalStack& s
           ++*shadow_rays;
           if (!trace_occluded_impl<(kF & kFeatSpheres) != 0>(slot, st, pos, normalize(pwi), kTMax, tests, nodes)) {
             RayTransfer srt = rt;
+            const PathSampler hs0 = hs;
             const vec3 tr = trace_tr<kF>(slot, st, pos, normalize(pwi), kTMax, kEmpty, kEmpty, srt, hs, errors, tests, nodes);
             const float mis = power_heuristic(pspdf, wpdf);
-            direct += mis * tr * gmin(pw, kMaxColorClamp) * vmin(Li, vec3(kMaxColorClamp));
+            const vec3 contrib = mis * tr * gmin(pw, kMaxColorClamp) * vmin(Li, vec3(kMaxColorClamp));
+            direct += contrib;
+            if constexpr (kAdj)
+              volume_shadow_grad<kF>(slot, st, pos, normalize(pwi), kTMax, rt, hs0, contrib, select_pdf, av, errors,
+                                     tests, nodes);
           }
         }
       }
@@ -856,9 +917,14 @@ __device__ __noinline__ vec3 eval_volume_lights(uint32_t slot, TraversalStack& s
       ++*shadow_rays;
       if (!trace_occluded_impl<(kF & kFeatSpheres) != 0>(slot, st, pos, normalize(ldir), maxd, tests, nodes)) {
         RayTransfer srt = rt;
+        const PathSampler hs0 = hs;
         const vec3 tr = trace_tr<kF>(slot, st, pos, normalize(ldir), maxd, kEmpty, kEmpty, srt, hs, errors, tests, nodes);
         const float mis = power_heuristic(lpdf, wpdf);
-        direct += mis * tr * gmin(pw, kMaxColorClamp) * vmin(Li, vec3(kMaxColorClamp));
+        const vec3 contrib = mis * tr * gmin(pw, kMaxColorClamp) * vmin(Li, vec3(kMaxColorClamp));
+        direct += contrib;
+        if constexpr (kAdj)
+          volume_shadow_grad<kF>(slot, st, pos, normalize(ldir), maxd, rt, hs0, contrib, select_pdf, av, errors,
+                                 tests, nodes);
       }
     }
   }
@@ -876,9 +942,14 @@ __device__ __noinline__ vec3 eval_volume_lights(uint32_t slot, TraversalStack& s
         ++*shadow_rays;
         if (!trace_occluded_impl<(kF & kFeatSpheres) != 0>(slot, st, pos, normalize(pwi), maxd, tests, nodes)) {
           RayTransfer srt = rt;
+          const PathSampler hs0 = hs;
           const vec3 tr = trace_tr<kF>(slot, st, pos, normalize(pwi), maxd, kEmpty, kEmpty, srt, hs, errors, tests, nodes);
           const float mis = power_heuristic(pspdf, wpdf);
-          direct += mis * tr * gmin(pw, kMaxColorClamp) * vmin(Li, vec3(kMaxColorClamp));
+          const vec3 contrib = mis * tr * gmin(pw, kMaxColorClamp) * vmin(Li, vec3(kMaxColorClamp));
+          direct += contrib;
+          if constexpr (kAdj)
+            volume_shadow_grad<kF>(slot, st, pos, normalize(pwi), maxd, rt, hs0, contrib, select_pdf, av, errors,
+                                   tests, nodes);
         }
       }
     }
@@ -898,9 +969,10 @@ template <bool kVol, bool kDefer, bool kAdj, uint32_t kF>
 __global__ void __launch_bounds__(kTraceBlock) k_shade(PathPool P, const WaveControl* __restrict__ ctl, HitPool H,
                                                        PathPool Q, const JobDesc* __restrict__ jobs,
                                                        WaveCounters* counters, ShadowQueue shadow_q,
-                                                       float* grads = nullptr, uint32_t grad_materials = 0) {
+                                                       float* grads = nullptr, uint32_t grad_materials = 0,
+                                                       float* grid_grads = nullptr, uint32_t grid_tex = kEmpty) {
   static_assert(!(kVol && kDefer), "volume transmittance needs the path's sampler: shadow rays are traced inline");
-  static_assert(!(kAdj && (kVol || kDefer)), "the adjoint pass shades surfaces with inline shadow rays");
+  static_assert(!(kAdj && kDefer), "the adjoint pass traces its shadow rays inline");
   float* s_grad = nullptr;
   const uint32_t n_slots = min(grad_materials, (uint32_t)kMaxGradMaterials) * kGradParams;
   if constexpr (kAdj) {
@@ -983,12 +1055,19 @@ __global__ void __launch_bounds__(kTraceBlock) k_shade(PathPool P, const WaveCon
         vw[k] = H.vol_w[(size_t)i * kMaxBoundaryRecord + k];
       }
       const vec3 pos = bary;
+      MediumAdj av{vec3(0.0f), grid_tex, grid_grads};
+      if constexpr (kAdj) {
+        const float4 dl = J.dloss[pf.x];
+        av.scale = vec3(dl.x, dl.y, dl.z) * inv_spp * tp;  // dLoss/d(this vertex's light), before 1/select_pdf
+      }
       if (rs.enable_distant_light)
-        rad += indirect_clamp(rs, tp * eval_volume_lights<kF>(slot, st, true, n, gs, vw, rd, rt, pos, hs, &shadow_rays, &tests,
-                                                          &nodes, errors), depth);
+        rad += indirect_clamp(rs, tp * eval_volume_lights<kF, kAdj>(slot, st, true, n, gs, vw, rd, rt, pos, hs,
+                                                                    &shadow_rays, &tests, &nodes, errors,
+                                                                    kAdj ? &av : nullptr), depth);
       if (rs.enable_shape_light)
-        rad += indirect_clamp(rs, tp * eval_volume_lights<kF>(slot, st, false, n, gs, vw, rd, rt, pos, hs, &shadow_rays,
-                                                          &tests, &nodes, errors), depth);
+        rad += indirect_clamp(rs, tp * eval_volume_lights<kF, kAdj>(slot, st, false, n, gs, vw, rd, rt, pos, hs,
+                                                                    &shadow_rays, &tests, &nodes, errors,
+                                                                    kAdj ? &av : nullptr), depth);
       vec3 wi;
       float pdf = 0.0f, pw = 0.0f;
       float u0, u1;
@@ -1081,6 +1160,8 @@ __global__ void __launch_bounds__(kTraceBlock) k_shade(PathPool P, const WaveCon
           l_total = vec3(lt.x, lt.y, lt.z);
           init_adjoint(adj_ctx, B, mat.default_mtl);
           adj_ctx.weight = delta * tp;
+          adj_ctx.grid_grads = grid_grads;
+          adj_ctx.grid_tex = grid_tex;
           adj = &adj_ctx;
         }
         if (rs.enable_distant_light)
@@ -1382,7 +1463,10 @@ void launch_shade(bool adjoint, bool volumes, const ShadowQueue* defer, uint32_t
                   WaveCounters* counters, const WaveOptions& opt, cudaStream_t stream) {
   constexpr uint32_t kS = kF & kFeatSpheres;
   const ShadowQueue none{};
-  if (adjoint)
+  if (adjoint && volumes)  // one instantiation (all features) for the media adjoint
+    k_shade<true, false, true, kFeatAll><<<blocks, kTraceBlock, 0, stream>>>(
+        A, ctl, Hs, B, jobs, counters, none, opt.grads, opt.grad_materials, opt.grid_grads, opt.grid_tex);
+  else if (adjoint)
     k_shade<false, false, true, kS><<<blocks, kTraceBlock, 0, stream>>>(A, ctl, Hs, B, jobs, counters, none, opt.grads,
                                                                         opt.grad_materials);
   else if (volumes)
@@ -1412,9 +1496,9 @@ uint32_t launch_wave(const PathPool& A, const PathPool& B, const HitPool& H, Wav
                      cudaStream_t stream, unsigned long long graph_condition) {
   prepare_persistent_grids();
   const PersistentGrids& g = g_grids;
-  const bool adjoint = opt.adjoint && !opt.volumes;
+  const bool adjoint = opt.adjoint;
   const ShadowQueue* defer = (!opt.volumes && opt.defer_shadows && !adjoint) ? &opt.shadow_queue : nullptr;
-  const bool sort_hits = opt.sort_hits && !adjoint;
+  const bool sort_hits = opt.sort_hits;
   HitPool Hs = H;
   if (!sort_hits) Hs.order = nullptr;
   const uint32_t feat = opt.features & kFeatAll;
@@ -1427,7 +1511,10 @@ uint32_t launch_wave(const PathPool& A, const PathPool& B, const HitPool& H, Wav
   if (ev) cudaEventRecord(ev[0], stream);
   k_generate<<<blocks_256, 256, 0, stream>>>(A, ctl, jobs, n_jobs);
   if (ev) cudaEventRecord(ev[1], stream);
-  switch (feat) {
+  if (adjoint && opt.volumes)  // free flight with density-grid terms (one instantiation, all features)
+    k_extend<true, kFeatAll, true><<<blocks_trace, kTraceBlock, 0, stream>>>(A, ctl, Hs, jobs, counters, opt.grid_grads,
+                                                                           opt.grid_tex);
+  else switch (feat) {
     case 0: launch_extend<0>(opt.volumes, blocks_trace, A, ctl, Hs, jobs, counters, stream); break;
     case 1: launch_extend<1>(opt.volumes, blocks_trace, A, ctl, Hs, jobs, counters, stream); break;
     case 2: launch_extend<2>(opt.volumes, blocks_trace, A, ctl, Hs, jobs, counters, stream); break;

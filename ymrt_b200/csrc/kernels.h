@@ -153,9 +153,11 @@ struct WaveOptions {
   bool defer_shadows = false;  // queue surface shadow rays for k_connect (ignored with volumes)
   uint32_t features = kFeatAll;  // scene features of the batch (kFeatSpheres | kFeatGrids)
   ShadowQueue shadow_queue{};
-  bool adjoint = false;        // path-replay adjoint pass (surfaces; no sorting, no deferral)
+  bool adjoint = false;        // path-replay adjoint pass (no deferral)
   float* grads = nullptr;      // adjoint: dLoss/dParam, kGradParams per material
   uint32_t grad_materials = 0;
+  float* grid_grads = nullptr; // adjoint: dLoss/d(value) of the density grid at texture node grid_tex
+  uint32_t grid_tex = 0xFFFFFFFFu;
 };
 uint32_t launch_wave(const PathPool& A, const PathPool& B, const HitPool& H, WaveControl* ctl, const JobDesc* jobs,
                      uint32_t n_jobs, WaveCounters* counters, const WaveOptions& opt, cudaEvent_t* ev,

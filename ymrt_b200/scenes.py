@@ -441,6 +441,34 @@ def spheres_scene(seed: int = 0) -> Scene:
     return s
 
 
+def instanced_fog_scene(seed: int = 0) -> Scene:
+    """The instanced scene inside a box of heterogeneous fog (sigma_t 0.15,
+    albedo 0.8, g 0.3) whose density node (texture 0, a constant 1 in the
+    file) takes a density grid at run time: the differentiable media workload."""
+    s = instanced_scene(seed)
+    s.meshes = s.meshes + [box_mesh("Geo_FogBox")]
+    s.textures.append(("ConstantTextureFloat", "fog_density", {"value": 1.0}))
+    s.transforms.append(("fog_transform", (0.0, 2.0, 0.0), (20.0, 6.0, 20.0), (0, 0, 0)))
+    s.volumes.append(("fog_volume", "fog_transform", (0.15, 0.15, 0.15), (0.8, 0.8, 0.8), 0.3, "fog_density"))
+    s.materials.append(("DefaultMaterial", "fog_boundary_material", {"ior_n": 1.0}))
+    s.instances.append(("fog_box", "Geo_FogBox", "fog_transform", "fog_boundary_material", "fog_volume", True))
+    return s
+
+
+def smooth_grid(n: int, seed: int = 0, lo: float = 0.2, hi: float = 1.0) -> np.ndarray:
+    """A seeded smooth density grid of n^3 values in [lo, hi]: a sum of a few
+    random low-frequency sinusoids, rescaled."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    c = (np.arange(n) + 0.5) / n
+    z, y, x = np.meshgrid(c, c, c, indexing="ij")
+    v = np.zeros((n, n, n))
+    for _ in range(6):
+        k = rng.uniform(1.0, 4.0, 3) * 2 * np.pi
+        v += rng.uniform(0.5, 1.0) * np.sin(k[0] * x + k[1] * y + k[2] * z + rng.uniform(0, 2 * np.pi))
+    v = (v - v.min()) / max(v.max() - v.min(), 1e-12)
+    return (lo + (hi - lo) * v).astype(np.float32)
+
+
 def volumetric_const_scene(seed: int = 0) -> Scene:
     """The volumetric scene with the smoke's fBm density replaced by the
     constant 0.5 (same node name and index): a density grid of 0.5s attached
@@ -484,6 +512,7 @@ SCENES = {
     "cornell": cornell_scene,
     "glossy": glossy_scene,
     "instanced": instanced_scene,
+    "instanced_fog": instanced_fog_scene,
     "spheres": spheres_scene,
     "volumetric": volumetric_scene,
     "volumetric_const": volumetric_const_scene,
