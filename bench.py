@@ -402,6 +402,8 @@ def run_ours(args):
     perm = scenes.halton_permutations()
     path = scenes.scene_path(wl["scene"], 0)
     ctx = Y.Context(local_rank, queue_capacity=args.queue, profiling=False)
+    if args.no_graph_loop:
+        ctx.set_option("graph_loop", 0)
     host = Y.HostScene(path, W, H)
     scene = Y.Scene(ctx, host, perm)
     grid = None
@@ -462,15 +464,19 @@ def run_ours(args):
     # End to end through the C ABI: upload the scene from host memory, render,
     # read the image back -- every step.
     host_img = np.zeros((H, W, 4), np.float32)
-    e2e_rays, e2e_wall = 0, 0.0
+    e2e_rays, e2e_wall, e2e_upload, e2e_render_dev = 0, 0.0, 0.0, 0.0
     for i in range(max(1, min(args.steps, 3))):
         torch.cuda.synchronize()
         t = time.perf_counter()
         sc2 = Y.Scene(ctx, host, perm)
         if grid is not None:
             sc2.set_density_grid(2, grid, half=True)
+        t_up = time.perf_counter()
         _, st = sc2.render(setting, frame_index=20_000 + i * world + rank, out=host_img)
-        e2e_wall += time.perf_counter() - t
+        t_end = time.perf_counter()
+        e2e_wall += t_end - t
+        e2e_upload += t_up - t
+        e2e_render_dev += st.ms_total * 1e-3
         e2e_rays += st.extension_rays + st.shadow_rays
         sc2.close()
     scene_bytes = scene_upload_bytes(host, perm) + (grid.size * 2 if grid is not None else 0)
@@ -509,7 +515,8 @@ def run_ours(args):
                        "parallelism": f"replica x{world}" + (" + allreduce of frames" if world > 1 else ""),
                        "l2": "256 MB buffer written between steps; path queues (>1 GB) exceed L2",
                        "options": {"sort_hits": ctx.get_option("sort_hits"),
-                                   "defer_shadows": ctx.get_option("defer_shadows")}},
+                                   "defer_shadows": ctx.get_option("defer_shadows"),
+                                   "graph_loop": ctx.get_option("graph_loop")}},
             "spp_per_s": round(W * H * spp * world * args.steps / (ms_max * 1e-3), 1),
             "rays": {"extension": ext, "shadow": shadow, "per_step": rays // max(args.steps, 1)},
             "frame_ms_device": round(frame_ms / args.steps, 3),
@@ -522,7 +529,10 @@ def run_ours(args):
                          "alg_bytes_per_launch": dk["alg_state_bytes_per_launch"],
                          "l2_bvh_gbs": dk["bvh_l2_gbs"]},
             "e2e": {"value": round(e2e_rays_all / e2e_wall_max / 1e6, 2) if e2e_wall_max > 0 else None,
-                    "unit": "Mrays/s", "h2d_bytes_per_step": int(scene_bytes), "d2h_bytes_per_step": int(W * H * 16)},
+                    "unit": "Mrays/s", "h2d_bytes_per_step": int(scene_bytes), "d2h_bytes_per_step": int(W * H * 16),
+                    "ms_per_step": {"scene_upload": round(e2e_upload * 1e3 / max(1, min(args.steps, 3)), 2),
+                                    "render_device": round(e2e_render_dev * 1e3 / max(1, min(args.steps, 3)), 2),
+                                    "total": round(e2e_wall * 1e3 / max(1, min(args.steps, 3)), 2)}},
             "clocks": clk,
         }
         with quiet_stdout():
@@ -708,6 +718,8 @@ def main(argv=None):
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-ref-cuda", action="store_true", help="skip timing the reference's own CUDA kernels")
     ap.add_argument("--no-fp64", action="store_true", help="skip the image check against the FP64 oracle")
+    ap.add_argument("--no-graph-loop", action="store_true",
+                    help="launch the wave loop from the host instead of as one CUDA graph (for per-kernel profilers)")
     ap.add_argument("--autotune", action="store_true", help="batch workload: tune the wave options first")
     args = ap.parse_args(argv)
     if args.warmup < 3:
