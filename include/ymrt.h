@@ -141,6 +141,70 @@ int ymrt_scene_load_ymtmp_ex(const char* path, int width, int height, const ymrt
                              ymrt_host_scene** out, char* err, size_t err_len);
 void ymrt_host_scene_free(ymrt_host_scene* scene);
 
+/* ---- scenes from memory ----
+ * For a host that holds its scene in memory (the reference editor's
+ * SceneModule arrays, src/core/SceneModule.h:288-326) instead of a .ymtmp
+ * file: the same assets, already resolved to indices, prepared exactly as
+ * ymrt_scene_load_ymtmp_ex prepares a parsed file (GuiModule::UpdateScene,
+ * src/core/GuiModule.cpp:116-282). All arrays are host memory and are
+ * copied; the caller keeps them. */
+typedef struct ymrt_mesh_desc {
+  /* Triangle mesh in creation order (as CreateMesh receives it,
+   * src/core/SceneModule.cpp:239-262): the library orders the triangles as
+   * the reference's mesh build does. 3 corner indices per triangle; one
+   * position / normal (/ texcoord) index per corner. */
+  const uint32_t* triangles;
+  uint32_t triangle_count;
+  const uint32_t* position_indices;
+  const float* positions;          /* xyz */
+  uint32_t position_count;
+  const uint32_t* normal_indices;
+  const float* normals;            /* xyz */
+  uint32_t normal_count;
+  const uint32_t* texcoord_indices; /* NULL: no texture coordinates */
+  const float* texcoords;           /* uv */
+  uint32_t texcoord_count;
+  /* > 0: an analytic sphere of this radius (a Sphere block); the arrays are
+   * then ignored. */
+  float sphere_radius;
+} ymrt_mesh_desc;
+
+/* A texture node, in the words YMRT_QUERY_TEXTURES returns: type
+ * (1 constant float, 2 constant rgb, 5 fBm noise), the fBm node's black and
+ * white input nodes (0xFFFFFFFF: none), and its parameters. */
+typedef struct ymrt_texture_desc {
+  uint32_t type;
+  uint32_t black, white;
+  float value;
+  float color[3];
+  float frequency, lacunarity, gain;
+  int32_t layer_count;
+  float amplitude, offset;
+} ymrt_texture_desc;
+
+typedef struct ymrt_scene_desc {
+  const float* transforms;          /* 16 floats per transform, column major (glm::mat4) */
+  const float* inverse_transforms;  /* NULL: inverted here (glm's inverse) */
+  const float* transform_scales;    /* xyz per transform (its Transform's own scale; sizes sphere lights); NULL: 1 */
+  uint32_t transform_count;
+  const ymrt_mesh_desc* geometries;
+  uint32_t geometry_count;
+  const void* instances;            /* PrimitiveInstance, 32 bytes each, creation order */
+  uint32_t instance_count;
+  const void* materials;            /* Material, 156 bytes each (src/Material.h) */
+  uint32_t material_count;
+  const void* volumes;              /* Volume, 36 bytes each (src/Volume.h) */
+  uint32_t volume_count;
+  const void* distant_lights;       /* DistantLight, 32 bytes each (src/Light.h:324-388) */
+  uint32_t distant_light_count;
+  const ymrt_texture_desc* textures;
+  uint32_t texture_count;
+  float camera_from[3], camera_look[3], camera_fov_deg;
+} ymrt_scene_desc;
+
+int ymrt_scene_from_arrays(const ymrt_scene_desc* desc, int width, int height, const ymrt_load_options* options,
+                           ymrt_host_scene** out, char* err, size_t err_len);
+
 /* Host-scene queries (for parity checks against the reference's own scene
  * preparation). Each copies into `out` (capacity `cap` elements) and returns
  * the element count, or a negative YMRT_ERR_*. */

@@ -119,6 +119,8 @@ def library():
     L.ymrt_scene_load_ymtmp_ex.argtypes = [ctypes.c_char_p, i, i, ctypes.POINTER(LoadOptions), ctypes.POINTER(vp),
                                            ctypes.c_char_p, sz]
     L.ymrt_host_scene_free.argtypes = [vp]
+    L.ymrt_scene_from_arrays.argtypes = [ctypes.POINTER(SceneDesc), i, i, ctypes.POINTER(LoadOptions), ctypes.POINTER(vp),
+                                         ctypes.c_char_p, sz]
     L.ymrt_host_scene_query.restype = ctypes.c_longlong
     L.ymrt_host_scene_query.argtypes = [vp, i, i, vp, sz]
     L.ymrt_scene_upload.argtypes = [vp, vp, vp, sz, ctypes.POINTER(vp)]
@@ -201,6 +203,26 @@ class Context:
             pass
 
 
+class MeshDesc(ctypes.Structure):
+    _fields_ = [("triangles", ctypes.c_void_p), ("triangle_count", ctypes.c_uint32),
+                ("position_indices", ctypes.c_void_p), ("positions", ctypes.c_void_p), ("position_count", ctypes.c_uint32),
+                ("normal_indices", ctypes.c_void_p), ("normals", ctypes.c_void_p), ("normal_count", ctypes.c_uint32),
+                ("texcoord_indices", ctypes.c_void_p), ("texcoords", ctypes.c_void_p), ("texcoord_count", ctypes.c_uint32),
+                ("sphere_radius", ctypes.c_float)]
+
+
+class SceneDesc(ctypes.Structure):
+    _fields_ = [("transforms", ctypes.c_void_p), ("inverse_transforms", ctypes.c_void_p),
+                ("transform_scales", ctypes.c_void_p), ("transform_count", ctypes.c_uint32),
+                ("geometries", ctypes.POINTER(MeshDesc)), ("geometry_count", ctypes.c_uint32),
+                ("instances", ctypes.c_void_p), ("instance_count", ctypes.c_uint32),
+                ("materials", ctypes.c_void_p), ("material_count", ctypes.c_uint32),
+                ("volumes", ctypes.c_void_p), ("volume_count", ctypes.c_uint32),
+                ("distant_lights", ctypes.c_void_p), ("distant_light_count", ctypes.c_uint32),
+                ("textures", ctypes.c_void_p), ("texture_count", ctypes.c_uint32),
+                ("camera_from", ctypes.c_float * 3), ("camera_look", ctypes.c_float * 3), ("camera_fov_deg", ctypes.c_float)]
+
+
 class HostScene:
     """A parsed and prepared .ymtmp scene (no GPU involved)."""
 
@@ -221,6 +243,69 @@ class HostScene:
         if rc != YMRT_OK:
             raise YmrtError(rc, err.value.decode(errors="replace"))
         self.width, self.height = width, height
+
+    @classmethod
+    def from_arrays(cls, width: int, height: int, transforms, geometries, instances, materials, camera,
+                    volumes=None, distant_lights=None, textures=None, inverse_transforms=None, transform_scales=None,
+                    max_leaf_triangles: int = 3) -> "HostScene":
+        """A scene from in-memory arrays (ymrt_scene_from_arrays):
+        transforms (n, 16) float32 column major; geometries: dicts with
+        triangles (n, 3), position_indices, positions (m, 3), normal_indices,
+        normals, optional texcoord_indices / texcoords, or {"sphere_radius": r};
+        instances / materials / volumes / distant_lights: the reference's
+        structs as uint32 words ((n, 8), (n, 39), (n, 9), (n, 8)); textures:
+        (n, 13) words as records("textures") returns; camera: (from, look, fov)."""
+        keep = []
+
+        def arr(a, dtype, cols=None):
+            if a is None:
+                return None, 0
+            v = np.ascontiguousarray(a, dtype=dtype)
+            if cols:
+                v = v.reshape(-1, cols)
+            keep.append(v)
+            return v.ctypes.data_as(ctypes.c_void_p), (v.shape[0] if v.ndim > 1 else v.size)
+
+        d = SceneDesc()
+        d.transforms, d.transform_count = arr(transforms, np.float32, 16)
+        d.inverse_transforms, _ = arr(inverse_transforms, np.float32, 16)
+        d.transform_scales, _ = arr(transform_scales, np.float32, 3)
+        meshes = (MeshDesc * max(len(geometries), 1))()
+        for k, g in enumerate(geometries):
+            m = meshes[k]
+            if g.get("sphere_radius"):
+                m.sphere_radius = float(g["sphere_radius"])
+                continue
+            m.triangles, m.triangle_count = arr(g["triangles"], np.uint32, 3)
+            m.position_indices, _ = arr(g["position_indices"], np.uint32)
+            m.positions, m.position_count = arr(g["positions"], np.float32, 3)
+            m.normal_indices, _ = arr(g["normal_indices"], np.uint32)
+            m.normals, m.normal_count = arr(g["normals"], np.float32, 3)
+            if g.get("texcoords") is not None:
+                m.texcoord_indices, _ = arr(g["texcoord_indices"], np.uint32)
+                m.texcoords, m.texcoord_count = arr(g["texcoords"], np.float32, 2)
+        keep.append(meshes)
+        d.geometries, d.geometry_count = meshes, len(geometries)
+        d.instances, d.instance_count = arr(instances, np.uint32, 8)
+        d.materials, d.material_count = arr(materials, np.uint32, 39)
+        d.volumes, d.volume_count = arr(volumes, np.uint32, 9)
+        d.distant_lights, d.distant_light_count = arr(distant_lights, np.uint32, 8)
+        d.textures, d.texture_count = arr(textures, np.uint32, 13)
+        frm, look, fov = camera
+        d.camera_from[:] = [float(x) for x in frm]
+        d.camera_look[:] = [float(x) for x in look]
+        d.camera_fov_deg = float(fov)
+        opts = LoadOptions()
+        opts.max_leaf_triangles = max_leaf_triangles
+        self = cls.__new__(cls)
+        self.h = ctypes.c_void_p()
+        err = ctypes.create_string_buffer(1024)
+        rc = library().ymrt_scene_from_arrays(ctypes.byref(d), width, height, ctypes.byref(opts), ctypes.byref(self.h),
+                                              err, len(err))
+        if rc != YMRT_OK:
+            raise YmrtError(rc, err.value.decode(errors="replace"))
+        self.width, self.height = width, height
+        return self
 
     def close(self):
         if self.h:

@@ -22,6 +22,9 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 OUT_DIR = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libymrt.so")
+# The reference's stage-launcher symbols, forwarding to libymrt.so (include/ymrt_compat.h).
+COMPAT_LIB = os.path.join(HERE, "libymrt_compat.so")
+COMPAT_SOURCE = "compat_shim.cpp"
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
@@ -62,7 +65,7 @@ def build(force: bool = False, verbose: bool = False, ptxas_report: bool = False
     os.makedirs(OUT_DIR, exist_ok=True)
     stamp_file = os.path.join(OUT_DIR, "stamp")
     stamp = _stamp()
-    if not force and os.path.exists(LIB) and os.path.exists(stamp_file):
+    if not force and os.path.exists(LIB) and os.path.exists(COMPAT_LIB) and os.path.exists(stamp_file):
         with open(stamp_file) as f:
             if f.read().strip() == stamp:
                 return LIB
@@ -95,6 +98,14 @@ def build(force: bool = False, verbose: bool = False, ptxas_report: bool = False
     _run([NVCC] + ARCH + ["-shared", "-cudart", "static", "-o", tmp] + objs +
          ["-Xlinker", "-Bsymbolic", "-Xlinker", "--version-script=" + vs], verbose)
     os.replace(tmp, LIB)
+    # libymrt_compat.so: host code only, linked against libymrt.so (found
+    # beside it at run time), so that one CUDA runtime does all device work.
+    cobj = os.path.join(OUT_DIR, COMPAT_SOURCE + ".o")
+    _run(["g++"] + CXX_FLAGS + ["-c", os.path.join(CSRC, COMPAT_SOURCE), "-o", cobj], verbose)
+    ctmp = COMPAT_LIB + ".tmp"
+    _run(["g++", "-shared", "-o", ctmp, cobj, "-L" + HERE, "-l:libymrt.so", "-Wl,-rpath,$ORIGIN",
+          "-Wl,--no-undefined"], verbose)
+    os.replace(ctmp, COMPAT_LIB)
     with open(stamp_file, "w") as f:
         f.write(stamp)
     if reports:

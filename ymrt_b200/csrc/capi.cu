@@ -6,6 +6,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <functional>
 #include <map>
@@ -16,6 +17,7 @@
 #include <vector>
 
 #include "../../include/ymrt.h"
+#include "../../include/ymrt_compat.h"
 #include "kernels.h"
 #include "scene_host.h"
 
@@ -346,6 +348,38 @@ int ymrt_scene_load_ymtmp_ex(const char* path, int width, int height, const ymrt
     rc = YMRT_ERR_FORMAT;
     msg = std::string("malformed value in ") + path + ": " + ex.what();
   }
+  if (rc != YMRT_OK) return report(rc, msg);
+  *out = hs.release();
+  return YMRT_OK;
+}
+
+int ymrt_scene_from_arrays(const ymrt_scene_desc* desc, int width, int height, const ymrt_load_options* options,
+                           ymrt_host_scene** out, char* err, size_t err_len) {
+  auto report = [&](int code, const std::string& msg) {
+    g_last_error = msg;
+    if (err && err_len) {
+      std::strncpy(err, msg.c_str(), err_len - 1);
+      err[err_len - 1] = 0;
+    }
+    return code;
+  };
+  if (!desc || !out) return report(YMRT_ERR_INVALID, "null argument");
+  *out = nullptr;
+  std::unique_ptr<ymrt_host_scene> hs(new (std::nothrow) ymrt_host_scene());
+  if (!hs) return report(YMRT_ERR_OOM, "out of host memory");
+  if (options) {
+    if (options->max_leaf_triangles < 1 || options->max_leaf_triangles > 4)
+      return report(YMRT_ERR_INVALID, "max_leaf_triangles must be 1..4");
+    hs->s.max_leaf_prims = options->max_leaf_triangles;
+  }
+  std::string msg;
+  int rc = load_arrays(desc, &hs->s, &msg);
+  if (rc == YMRT_OK && options && options->override_camera) {
+    hs->s.cam_from = vec3(options->camera_from[0], options->camera_from[1], options->camera_from[2]);
+    hs->s.cam_look = vec3(options->camera_look[0], options->camera_look[1], options->camera_look[2]);
+    hs->s.cam_fov_deg = gmax(options->camera_fov_deg, 0.01f);
+  }
+  if (rc == YMRT_OK) rc = prepare_scene(&hs->s, width, height, &msg);
   if (rc != YMRT_OK) return report(rc, msg);
   *out = hs.release();
   return YMRT_OK;
@@ -1301,6 +1335,156 @@ int ymrt_accumulate(ymrt_scene* sc, const float* noise, float* acc, int frame_in
                     (uint32_t)sc->width * (uint32_t)sc->height, frame_index, ctx->stream);
   cudaError_t e = cudaStreamSynchronize(ctx->stream);
   return e == cudaSuccess ? YMRT_OK : ctx->cuda_fail(e, "accumulate");
+}
+
+// ---- the reference's stage interface (include/ymrt_compat.h) ----
+
+namespace {
+struct CompatBinding {
+  std::mutex m;
+  ymrt_context* ctx = nullptr;
+  ymrt_scene* scene = nullptr;
+  bool frame_marked = false;
+  int frame_index = 0;
+};
+CompatBinding g_compat;
+
+int compat_sync(void* stream) {
+  if (!stream) return YMRT_OK;
+  cudaError_t e = cudaStreamSynchronize(*static_cast<cudaStream_t*>(stream));
+  if (e != cudaSuccess) {
+    g_last_error = std::string("caller's stream: ") + cudaGetErrorString(e);
+    return YMRT_ERR_CUDA;
+  }
+  return YMRT_OK;
+}
+
+int compat_clear_counter(void* device_counter) {
+  if (!device_counter) return YMRT_ERR_INVALID;
+  cudaError_t e = cudaMemset(device_counter, 0, 3 * sizeof(uint32_t));
+  if (e == cudaSuccess) e = cudaDeviceSynchronize();
+  if (e != cudaSuccess) {
+    g_last_error = std::string("clearing the ray counter: ") + cudaGetErrorString(e);
+    return YMRT_ERR_CUDA;
+  }
+  return YMRT_OK;
+}
+}  // namespace
+
+int ymrt_compat_bind(ymrt_context* ctx, ymrt_scene* scene) {
+  if (scene && (!ctx || scene->ctx != ctx)) return YMRT_ERR_INVALID;
+  std::lock_guard<std::mutex> lk(g_compat.m);
+  g_compat.ctx = ctx;
+  g_compat.scene = scene;
+  g_compat.frame_marked = false;
+  return YMRT_OK;
+}
+
+int ymrt_compat_alloc_counter(void** host_counter, void** device_counter) {
+  if (!host_counter || !device_counter) return YMRT_ERR_INVALID;
+  *host_counter = std::calloc(1, 3 * sizeof(uint32_t));
+  if (!*host_counter) return YMRT_ERR_OOM;
+  cudaError_t e = cudaMalloc(device_counter, 3 * sizeof(uint32_t));
+  if (e == cudaSuccess) e = cudaMemset(*device_counter, 0, 3 * sizeof(uint32_t));
+  if (e != cudaSuccess) {
+    std::free(*host_counter);
+    *host_counter = nullptr;
+    g_last_error = std::string("allocating the ray counter: ") + cudaGetErrorString(e);
+    return YMRT_ERR_CUDA;
+  }
+  return YMRT_OK;
+}
+
+int ymrt_compat_free_counter(void* host_counter, void* device_counter) {
+  std::free(host_counter);
+  if (device_counter && cudaFree(device_counter) != cudaSuccess) return YMRT_ERR_CUDA;
+  return YMRT_OK;
+}
+
+int ymrt_compat_generate(int frame_index, const ymrt_render_setting* setting, void* device_counter,
+                         uint32_t next_tile, uint32_t tile_count, uint32_t width, uint32_t height, uint32_t tiles_x,
+                         uint32_t tiles_y, void* stream) {
+  (void)device_counter;
+  (void)tile_count;
+  std::lock_guard<std::mutex> lk(g_compat.m);
+  if (!g_compat.scene || !setting) {
+    g_last_error = "no scene bound (ymrt_compat_bind)";
+    return YMRT_ERR_INVALID;
+  }
+  ymrt_scene* sc = g_compat.scene;
+  if ((int)width != sc->width || (int)height != sc->height ||
+      tiles_x != (width + 15) / 16 || tiles_y != (height + 15) / 16) {
+    g_last_error = "frame size differs from the bound scene's";
+    return YMRT_ERR_INVALID;
+  }
+  int rc = compat_sync(stream);
+  if (rc != YMRT_OK) return rc;
+  if (next_tile == 0) {
+    g_compat.frame_marked = true;
+    g_compat.frame_index = frame_index;
+  }
+  return YMRT_OK;
+}
+
+int ymrt_compat_trace(int frame_index, const ymrt_render_setting* setting, void* device_counter, uint32_t width,
+                      uint32_t height, float* noise_rgba, void* stream) {
+  std::lock_guard<std::mutex> lk(g_compat.m);
+  if (!g_compat.scene || !setting || !noise_rgba) {
+    g_last_error = "no scene bound (ymrt_compat_bind) or null argument";
+    return YMRT_ERR_INVALID;
+  }
+  int rc = compat_sync(stream);
+  if (rc != YMRT_OK) return rc;
+  ymrt_scene* sc = g_compat.scene;
+  if ((int)width != sc->width || (int)height != sc->height) {
+    g_last_error = "frame size differs from the bound scene's";
+    return YMRT_ERR_INVALID;
+  }
+  if (g_compat.frame_marked && g_compat.frame_index == frame_index) {
+    g_compat.frame_marked = false;
+    ymrt_stats st;
+    rc = ymrt_render_tiles(sc, setting, frame_index, 0, 0, noise_rgba, 1, &st);
+    if (rc != YMRT_OK) {
+      g_last_error = sc->ctx->error;
+      return rc;
+    }
+    if (st.device_errors) {
+      g_last_error = "device errors while rendering";
+      return YMRT_ERR_CUDA;
+    }
+  }
+  return compat_clear_counter(device_counter);
+}
+
+int ymrt_compat_shade(int frame_index, const ymrt_render_setting* setting, void* device_counter, uint32_t width,
+                      uint32_t height, float* noise_rgba, void* stream) {
+  (void)frame_index;
+  (void)setting;
+  (void)width;
+  (void)height;
+  (void)noise_rgba;
+  int rc = compat_sync(stream);
+  if (rc != YMRT_OK) return rc;
+  return compat_clear_counter(device_counter);
+}
+
+int ymrt_compat_accumulate(const float* noise_rgba, float* acc_rgba, uint32_t width, uint32_t height, int frame_index,
+                           int max_frames, void* stream) {
+  if (max_frames > 0 && frame_index - 1 >= max_frames) return YMRT_OK;
+  std::lock_guard<std::mutex> lk(g_compat.m);
+  if (!g_compat.scene) {
+    g_last_error = "no scene bound (ymrt_compat_bind)";
+    return YMRT_ERR_INVALID;
+  }
+  if ((int)width != g_compat.scene->width || (int)height != g_compat.scene->height) {
+    g_last_error = "frame size differs from the bound scene's";
+    return YMRT_ERR_INVALID;
+  }
+  int rc = compat_sync(stream);
+  if (rc != YMRT_OK) return rc;
+  rc = ymrt_accumulate(g_compat.scene, noise_rgba, acc_rgba, frame_index);
+  if (rc != YMRT_OK) g_last_error = g_compat.scene->ctx->error;
+  return rc;
 }
 
 }  // extern "C"

@@ -13,6 +13,7 @@
 #include <fstream>
 #include <functional>
 #include <sstream>
+#include <type_traits>
 #include <unordered_map>
 
 #include "../../include/ymrt.h"
@@ -883,6 +884,125 @@ int load_ymtmp(const std::string& path, HostScene* scene, std::string* error) {
     if (inst.inner_volume_idx != -1 && (uint32_t)inst.inner_volume_idx >= scene->volumes.size())
       return fail(YMRT_ERR_FORMAT, "instance refers to an unknown volume");
   }
+  return YMRT_OK;
+}
+
+// ------------------------------------------------------- from arrays ---
+
+int load_arrays(const ymrt_scene_desc* d, HostScene* scene, std::string* error) {
+  auto fail = [&](int code, const std::string& msg) {
+    if (error) *error = msg;
+    return code;
+  };
+  if (!d) return fail(YMRT_ERR_INVALID, "null scene description");
+  // transforms
+  if (d->transform_count > 0 && !d->transforms) return fail(YMRT_ERR_INVALID, "transforms missing");
+  for (uint32_t t = 0; t < d->transform_count; ++t) {
+    mat4 m, mi;
+    std::memcpy(&m.m[0][0], d->transforms + 16 * (size_t)t, sizeof(float) * 16);
+    if (d->inverse_transforms) std::memcpy(&mi.m[0][0], d->inverse_transforms + 16 * (size_t)t, sizeof(float) * 16);
+    else mi = mat4_inverse(m);
+    scene->transforms.push_back(m);
+    scene->i_transforms.push_back(mi);
+    const float* sc = d->transform_scales ? d->transform_scales + 3 * (size_t)t : nullptr;
+    scene->transform_scales.push_back(sc ? vmax(vec3(0.0001f), vec3(sc[0], sc[1], sc[2])) : vec3(1.0f));
+  }
+  // geometries
+  if (d->geometry_count > 0 && !d->geometries) return fail(YMRT_ERR_INVALID, "geometries missing");
+  for (uint32_t g = 0; g < d->geometry_count; ++g) {
+    const ymrt_mesh_desc& md = d->geometries[g];
+    HostMesh m;
+    m.name = "geometry " + std::to_string(g);
+    if (md.sphere_radius > 0.0f) {
+      m.kind = kGeoSphere;
+      m.radius = gmax(0.0001f, md.sphere_radius);
+      scene->meshes.push_back(std::move(m));
+      continue;
+    }
+    const size_t nt = md.triangle_count, nc = 3 * nt;
+    if (nt == 0 || !md.triangles || !md.position_indices || !md.positions || !md.normal_indices || !md.normals)
+      return fail(YMRT_ERR_INVALID, m.name + ": a mesh needs triangles, positions and normals with their indices");
+    m.tris.assign(md.triangles, md.triangles + nc);
+    m.pos_idx.assign(md.position_indices, md.position_indices + nc);
+    m.nrm_idx.assign(md.normal_indices, md.normal_indices + nc);
+    m.pos.assign(md.positions, md.positions + 3 * (size_t)md.position_count);
+    m.nrm.assign(md.normals, md.normals + 3 * (size_t)md.normal_count);
+    if (md.texcoord_indices && md.texcoords && md.texcoord_count > 0) {
+      m.uv_idx.assign(md.texcoord_indices, md.texcoord_indices + nc);
+      m.uv.assign(md.texcoords, md.texcoords + 2 * (size_t)md.texcoord_count);
+    }
+    for (size_t k = 0; k < nc; ++k) {
+      if (m.tris[k] >= nc) return fail(YMRT_ERR_INVALID, m.name + ": triangle corner index out of range");
+      if (m.pos_idx[k] >= md.position_count || m.nrm_idx[k] >= md.normal_count)
+        return fail(YMRT_ERR_INVALID, m.name + ": vertex index out of range");
+      if (!m.uv_idx.empty() && m.uv_idx[k] >= md.texcoord_count)
+        return fail(YMRT_ERR_INVALID, m.name + ": texcoord index out of range");
+    }
+    scene->meshes.push_back(std::move(m));
+  }
+  // textures
+  if (d->texture_count > 0 && !d->textures) return fail(YMRT_ERR_INVALID, "textures missing");
+  for (uint32_t k = 0; k < d->texture_count; ++k) {
+    const ymrt_texture_desc& td = d->textures[k];
+    Texture tex;
+    std::memset(&tex, 0, sizeof(tex));
+    tex.child[0] = tex.child[1] = kEmpty;
+    tex.type = td.type;
+    if (td.type == kTexConstFloat) {
+      tex.value = td.value;
+    } else if (td.type == kTexConstRgb) {
+      tex.color = vec3(td.color[0], td.color[1], td.color[2]);
+    } else if (td.type == kTexFbm) {
+      if (td.black >= d->texture_count || td.white >= d->texture_count)
+        return fail(YMRT_ERR_INVALID, "fbm texture requires black and white inputs");
+      tex.child[0] = td.black;
+      tex.child[1] = td.white;
+      tex.frequency = gmax(0.001f, td.frequency);
+      tex.lacunarity = td.lacunarity;
+      tex.gain = td.gain;
+      tex.layer_count = td.layer_count;
+      tex.amplitude = td.amplitude;
+      tex.offset = td.offset;
+    } else {
+      return fail(YMRT_ERR_UNSUPPORTED, "texture type " + std::to_string(td.type) +
+                                            " is not supported (constant and fBm textures are)");
+    }
+    scene->textures.push_back(tex);
+  }
+  // materials, volumes, distant lights: the reference's own layouts
+  auto take = [&](const void* src, uint32_t n, auto* out) -> bool {
+    using T = typename std::remove_pointer<decltype(out)>::type::value_type;
+    if (n > 0 && !src) return false;
+    out->resize(n);
+    if (n) std::memcpy(out->data(), src, sizeof(T) * n);
+    return true;
+  };
+  if (!take(d->materials, d->material_count, &scene->materials)) return fail(YMRT_ERR_INVALID, "materials missing");
+  if (!take(d->volumes, d->volume_count, &scene->volumes)) return fail(YMRT_ERR_INVALID, "volumes missing");
+  if (!take(d->distant_lights, d->distant_light_count, &scene->distant_lights))
+    return fail(YMRT_ERR_INVALID, "distant lights missing");
+  if (!take(d->instances, d->instance_count, &scene->instances)) return fail(YMRT_ERR_INVALID, "instances missing");
+  for (const Material& m : scene->materials)
+    if (m.material_type != kDefaultMtl && m.material_type != kLightMtl)
+      return fail(YMRT_ERR_UNSUPPORTED, "material type " + std::to_string(m.material_type) + " is not supported");
+  for (const Volume& v : scene->volumes) {
+    if (v.transform_idx >= scene->transforms.size()) return fail(YMRT_ERR_INVALID, "volume refers to an unknown transform");
+    if (v.density_texture_idx != -1 && (uint32_t)v.density_texture_idx >= scene->textures.size())
+      return fail(YMRT_ERR_INVALID, "volume refers to an unknown texture");
+  }
+  for (const DistantLight& l : scene->distant_lights)
+    if (l.transform_idx >= scene->transforms.size())
+      return fail(YMRT_ERR_INVALID, "distant light refers to an unknown transform");
+  for (const Instance& inst : scene->instances) {
+    if (inst.geometry_idx >= scene->meshes.size() || inst.transform_idx >= scene->transforms.size() ||
+        inst.material_idx >= scene->materials.size())
+      return fail(YMRT_ERR_INVALID, "instance refers to an unknown asset");
+    if (inst.inner_volume_idx != -1 && (uint32_t)inst.inner_volume_idx >= scene->volumes.size())
+      return fail(YMRT_ERR_INVALID, "instance refers to an unknown volume");
+  }
+  scene->cam_from = vec3(d->camera_from[0], d->camera_from[1], d->camera_from[2]);
+  scene->cam_look = vec3(d->camera_look[0], d->camera_look[1], d->camera_look[2]);
+  scene->cam_fov_deg = gmax(d->camera_fov_deg, 0.01f);
   return YMRT_OK;
 }
 

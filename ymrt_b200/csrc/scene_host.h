@@ -15,6 +15,8 @@
 
 #include "ymrt_scene.h"
 
+struct ymrt_scene_desc;
+
 namespace ym {
 
 struct BBox {
@@ -66,6 +68,11 @@ struct HostScene {
 
 // Parses a .ymtmp file. Returns 0 or a negative YMRT_ERR_* code with a message.
 int load_ymtmp(const std::string& path, HostScene* scene, std::string* error);
+
+// Fills a scene from in-memory arrays (ymrt_scene_desc, include/ymrt.h):
+// the same assets load_ymtmp produces, already resolved to indices. Returns 0
+// or a negative YMRT_ERR_* code with a message.
+int load_arrays(const ymrt_scene_desc* desc, HostScene* scene, std::string* error);
 
 // Builds BVHs, orders instances/triangles/lights like the reference, sets up
 // the rendering camera for a width x height image and flattens the arrays.
