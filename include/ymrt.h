@@ -169,9 +169,21 @@ typedef struct ymrt_mesh_desc {
   float sphere_radius;
 } ymrt_mesh_desc;
 
-/* A texture node, in the words YMRT_QUERY_TEXTURES returns: type
- * (1 constant float, 2 constant rgb, 5 fBm noise), the fBm node's black and
- * white input nodes (0xFFFFFFFF: none), and its parameters. */
+/* A texture node, in the words YMRT_QUERY_TEXTURES returns (20 per node):
+ * type (src/Texture.h:16-28: 1 constant float, 2 constant rgb,
+ * 3 checkerboard, 4 noise, 5 fBm, 6 turbulence, 7 marble, 8 wood,
+ * 9 polka dot, 10 wave; 64 a density grid, which only
+ * ymrt_scene_set_density_grid makes), the black and white input nodes
+ * (0xFFFFFFFF: none; the solid nodes 3-10 require both), and the node's
+ * parameters. Unused words are 0. Fields per type:
+ *   constant float: value;  constant rgb: color;
+ *   checkerboard: frequency;  noise: frequency, flags bit 0 (normalized);
+ *   fBm, turbulence: frequency, lacunarity, gain, layer_count, amplitude, offset;
+ *   marble: frequency, lacunarity, gain, layer_count, variation,
+ *           flags bits 1-3 (x, y, z coordinate added to the phase);
+ *   wood: frequency, variation;  polka dot: frequency, radius;
+ *   wave: frequency, lacunarity, gain, layer_count (first fBm),
+ *         frequency1, lacunarity1, gain1, layer_count1 (second fBm). */
 typedef struct ymrt_texture_desc {
   uint32_t type;
   uint32_t black, white;
@@ -180,6 +192,10 @@ typedef struct ymrt_texture_desc {
   float frequency, lacunarity, gain;
   int32_t layer_count;
   float amplitude, offset;
+  float variation, radius;
+  uint32_t flags;
+  float frequency1, lacunarity1, gain1;
+  int32_t layer_count1;
 } ymrt_texture_desc;
 
 typedef struct ymrt_scene_desc {
@@ -218,7 +234,7 @@ int ymrt_scene_from_arrays(const ymrt_scene_desc* desc, int width, int height, c
 #define YMRT_QUERY_MATERIALS 7   /* uint32[39*n]: the reference's Material struct words */
 #define YMRT_QUERY_VOLUMES 8     /* uint32[9*n]: the reference's Volume struct words */
 #define YMRT_QUERY_DISTANT_LIGHTS 9 /* uint32[8*n]: the reference's DistantLight struct words */
-#define YMRT_QUERY_TEXTURES 10   /* uint32[13*n]: type, black/white inputs, value, rgb, frequency, lacunarity, gain, layers, amplitude, offset */
+#define YMRT_QUERY_TEXTURES 10   /* uint32[20*n]: ymrt_texture_desc words per node */
 #define YMRT_QUERY_GEOMETRIES 11 /* uint32[2*n]: kind (0 triangle mesh, 1 sphere), sphere radius (float bits) */
 #define YMRT_QUERY_MESH_CORNERS 12 /* float[8*c] of mesh `index`, by corner: position, normal, uv (0 without texcoords) */
 long long ymrt_host_scene_query(const ymrt_host_scene* scene, int what, int index, void* out, size_t cap);
@@ -348,6 +364,10 @@ int ymrt_debug_trace(ymrt_scene* scene, int n, const float* origin, const float*
  * each; host buffers), as the media read it: known-answer checks of grid and
  * fBm nodes. */
 int ymrt_debug_density(ymrt_scene* scene, uint32_t texture_index, int n, const float* points, float* out);
+/* Value (rgb) of texture node `texture_index` as a surface reads it, at n
+ * points of 5 floats each: texture coordinates s, t and the object-space
+ * position x, y, z (host buffers): known-answer checks of every node type. */
+int ymrt_debug_texture(ymrt_scene* scene, uint32_t texture_index, int n, const float* coords, float* rgb);
 int ymrt_debug_occluded(ymrt_scene* scene, int n, const float* origin, const float* dir, const float* tmax,
                         int* occluded);
 int ymrt_debug_halton(ymrt_scene* scene, int n, const int* px, const int* py, const int* sample, int n_dims,

@@ -55,6 +55,7 @@ def _bind(L, settings_type):
     L.ymref_lights.argtypes = [vp, vp, vp, vp]
     L.ymref_camera_bytes.argtypes = [vp, vp, i]
     L.ymref_scene_records.argtypes = [vp, i, vp, i]
+    L.ymref_texture_eval.argtypes = [vp, ctypes.c_uint32, i, vp, vp]
     L.ymref_bvh_depths.argtypes = [vp, vp]
     L.ymref_sobol_matrices.restype = ctypes.c_size_t
     L.ymref_sobol_matrices.argtypes = [vp, ctypes.c_size_t]
@@ -206,14 +207,26 @@ class RefScene:
 
     def records(self, kind: str) -> np.ndarray:
         """Materials, volumes, distant lights (raw 32-bit words of the
-        reference structs) or textures (13 words each), one row per record."""
+        reference structs) or textures (20 words each, the layout of
+        ymrt_texture_desc), one row per record."""
         what = {"materials": 0, "volumes": 1, "distant_lights": 2, "textures": 3}[kind]
-        width = {"materials": 39, "volumes": 9, "distant_lights": 8, "textures": 13}[kind]
+        width = {"materials": 39, "volumes": 9, "distant_lights": 8, "textures": 20}[kind]
         n = self._L.ymref_scene_records(self.h, what, None, 0)
         out = np.zeros(max(n, 0), np.uint32)
         if n > 0:
             self._L.ymref_scene_records(self.h, what, _p(out), out.size)
         return out.reshape(-1, width)
+
+    def texture(self, tex: int, st, points) -> np.ndarray:
+        """The reference's TextureEval of node `tex` at texture coordinates
+        st (n, 2) and object-space points (n, 3): rgb (n, 3)."""
+        st = np.asarray(st, self._f).reshape(-1, 2)
+        p = np.asarray(points, self._f).reshape(-1, 3)
+        c = np.ascontiguousarray(np.concatenate([st, p], axis=1), self._f)
+        out = np.zeros((c.shape[0], 3), self._f)
+        if self._L.ymref_texture_eval(self.h, tex, c.shape[0], _p(c), _p(out)) != 0:
+            raise ValueError("unknown texture node")
+        return out
 
     def trace(self, origins, dirs, last_hit=None) -> dict:
         o = np.ascontiguousarray(origins, self._f)

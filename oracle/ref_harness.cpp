@@ -287,9 +287,12 @@ int ymref_transforms(void* handle, float* fwd, float* inv) {
 
 // Scene records as the reference's scene module holds them. what: 0 materials
 // (raw Material words), 1 volumes (raw Volume words), 2 distant lights (raw
-// DistantLight words), 3 textures (13 words: type, black/white inputs, constant
-// value, constant rgb, fBm frequency, lacunarity, gain, layer count, amplitude,
-// offset). Returns the number of 32-bit words (written when out has room).
+// DistantLight words), 3 textures (20 words per node, the layout of
+// ymrt_texture_desc: type, black/white inputs, constant value, constant rgb,
+// frequency, lacunarity, gain, layer count, amplitude, offset, variation,
+// radius, flags (1 normalized, 2/4/8 marble x/y/z), and the wave's second
+// frequency, lacunarity, gain, layer count). Returns the number of 32-bit
+// words (written when out has room).
 int ymref_scene_records(void* handle, int what, uint32_t* out, int cap) {
   auto ctx = static_cast<RefContext*>(handle);
   std::vector<uint32_t> w;
@@ -306,24 +309,86 @@ int ymref_scene_records(void* handle, int what, uint32_t* out, int cap) {
     case 2: for (auto& d : GuiModule::DistantLights(*ctx->module)) raw(&d, sizeof(d)); break;
     case 3:
       for (auto& t : GuiModule::Textures(*ctx->module)) {
-        uint32_t r[13] = {t.texture_type, EMPTY_UINT32, EMPTY_UINT32, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
-        if (t.texture_type == CONSTANT_TEXTURE_FLOAT) {
-          r[3] = f(t.constant_texture_float.value);
-        } else if (t.texture_type == CONSTANT_TEXTURE_RGB) {
-          r[4] = f(t.constant_texture_rgb.color.x); r[5] = f(t.constant_texture_rgb.color.y); r[6] = f(t.constant_texture_rgb.color.z);
-        } else if (t.texture_type == SOLID_TEXTURE_FBM) {
-          const auto& n = t.noise_texture_fbm;
-          r[1] = n.indices[0]; r[2] = n.indices[1];
-          r[7] = f(n.frequency); r[8] = f(n.lacunarity); r[9] = f(n.gain); r[10] = (uint32_t)n.layer_count;
-          r[11] = f(n.amplitude); r[12] = f(n.offset);
+        uint32_t r[20] = {t.texture_type, EMPTY_UINT32, EMPTY_UINT32};
+        if (t.GetChildCount() == 2) {
+          r[1] = t.GetChildTextureIndex(0);
+          r[2] = t.GetChildTextureIndex(1);
         }
-        w.insert(w.end(), r, r + 13);
+        auto fbm = [&](float freq, float lac, float gain, int layers) {
+          r[7] = f(freq); r[8] = f(lac); r[9] = f(gain); r[10] = (uint32_t)layers;
+        };
+        switch (t.texture_type) {
+          case CONSTANT_TEXTURE_FLOAT: r[3] = f(t.constant_texture_float.value); break;
+          case CONSTANT_TEXTURE_RGB:
+            r[4] = f(t.constant_texture_rgb.color.x); r[5] = f(t.constant_texture_rgb.color.y);
+            r[6] = f(t.constant_texture_rgb.color.z);
+            break;
+          case SOLID_TEXTURE_CHECKERBOARD: r[7] = f(t.checker_board_texture.frequency); break;
+          case SOLID_TEXTURE_NOISE:
+            r[7] = f(t.noise_texture.frequency);
+            r[15] = t.noise_texture.normalized ? 1u : 0u;
+            break;
+          case SOLID_TEXTURE_FBM: {
+            const auto& n = t.noise_texture_fbm;
+            fbm(n.frequency, n.lacunarity, n.gain, n.layer_count);
+            r[11] = f(n.amplitude); r[12] = f(n.offset);
+            break;
+          }
+          case SOLID_TEXTURE_TURBULENCE: {
+            const auto& n = t.noise_texture_turbulence;
+            fbm(n.frequency, n.lacunarity, n.gain, n.layer_count);
+            r[11] = f(n.amplitude); r[12] = f(n.offset);
+            break;
+          }
+          case SOLID_TEXTURE_MARBLE: {
+            const auto& n = t.noise_texture_marble;
+            fbm(n.frequency, n.lacunarity, n.gain, n.layer_count);
+            r[13] = f(n.variation);
+            r[15] = (n.x_turb ? 2u : 0u) | (n.y_turb ? 4u : 0u) | (n.z_turb ? 8u : 0u);
+            break;
+          }
+          case SOLID_TEXTURE_WOOD:
+            r[7] = f(t.noise_texture_wood.frequency); r[13] = f(t.noise_texture_wood.variation);
+            break;
+          case SOLID_TEXTURE_POLKA_DOT:
+            r[7] = f(t.noise_texture_polka_dot.frequency); r[14] = f(t.noise_texture_polka_dot.radius);
+            break;
+          case SOLID_TEXTURE_WAVE: {
+            const auto& n = t.noise_texture_wave;
+            fbm(n.freq_0, n.lacunarity_0, n.gain_0, n.layer_count_0);
+            r[16] = f(n.freq_1); r[17] = f(n.lacunarity_1); r[18] = f(n.gain_1); r[19] = (uint32_t)n.layer_count_1;
+            break;
+          }
+          default: break;
+        }
+        w.insert(w.end(), r, r + 20);
       }
       break;
     default: return -1;
   }
   if (out && cap >= (int)w.size()) std::memcpy(out, w.data(), w.size() * 4);
   return (int)w.size();
+}
+
+// TextureEval (src/TextureEval.cuh:419-481) of texture node `tex` at n
+// points of 5 floats (texture coordinates s, t, object-space x, y, z; the
+// world position is set to the object position, which no procedural node
+// reads): rgb out. Returns 0, or -1 for an unknown node.
+int ymref_texture_eval(void* handle, uint32_t tex, int n, const float* coords, float* rgb) {
+  auto ctx = static_cast<RefContext*>(handle);
+  const auto& textures = GuiModule::Textures(*ctx->module);
+  if (tex >= textures.size()) return -1;
+  ImageTileCache cache;
+  for (int i = 0; i < n; ++i) {
+    const float* c = coords + 5 * (size_t)i;
+    const glm::vec3 p(c[2], c[3], c[4]);
+    const TextureCoordinate tc(glm::vec2(c[0], c[1]), p, p);
+    const glm::vec3 v = TextureEval(textures[tex], textures.data(), cache, tc);
+    rgb[3 * i] = v.x;
+    rgb[3 * i + 1] = v.y;
+    rgb[3 * i + 2] = v.z;
+  }
+  return 0;
 }
 
 // Depth (root = 1) of the reference's binary BVHs: out[g] for mesh g, then

@@ -36,7 +36,7 @@ def arrays_of(name, scene_dir, width, height):
         ident = np.arange(n, dtype=np.uint32)
         mesh = {"triangles": ident.reshape(-1, 3), "position_indices": ident, "positions": corners[:, 0:3],
                 "normal_indices": ident, "normals": corners[:, 3:6]}
-        if g >= len(model.meshes):  # the built-in cube has texture coordinates; the Mesh blocks have none
+        if g >= len(model.meshes) or model.meshes[g].uv_idx is not None:  # meshes with texture coordinates
             mesh.update(texcoord_indices=ident, texcoords=corners[:, 6:8])
         geometries.append(mesh)
     inst = hs.instances()  # prepared order: geometry, transform, material, volume, boundary, file index
@@ -56,7 +56,7 @@ def arrays_of(name, scene_dir, width, height):
 
 
 @pytest.mark.parametrize("name,size", [("cornell", (256, 256)), ("spheres", (256, 256)),
-                                       ("volumetric", (128, 128))])
+                                       ("volumetric", (128, 128)), ("textured", (128, 128))])
 def test_arrays_prepare_like_the_file(name, size, scene_dir):
     hs, kw = arrays_of(name, scene_dir, *size)
     ha = Y.HostScene.from_arrays(size[0], size[1], **kw)
@@ -85,8 +85,8 @@ def test_arrays_reject_bad_input(scene_dir):
         Y.HostScene.from_arrays(64, 64, **bad)
     assert e.value.code == -1
     bad = dict(kw)
-    tex = np.zeros((1, 13), np.uint32)
-    tex[0, 0] = 3  # a checkerboard node
+    tex = np.zeros((1, Y.TEXTURE_WORDS), np.uint32)
+    tex[0, 0] = 0  # an image node
     bad["textures"] = tex
     with pytest.raises(Y.YmrtError) as e:
         Y.HostScene.from_arrays(64, 64, **bad)

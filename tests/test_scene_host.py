@@ -27,7 +27,7 @@ def _meaningful(kind, rec):
 
 
 @pytest.mark.parametrize("name,size", [("cornell", (256, 256)), ("instanced", (1920, 1080)),
-                                       ("volumetric", (256, 256)), ("spheres", (256, 256))])
+                                       ("volumetric", (256, 256)), ("spheres", (256, 256)), ("textured", (256, 256))])
 def test_scene_preparation_matches_reference(name, size, scene_dir, halton_perm, oracle):
     from ymrt_b200 import scenes
     path = scenes.scene_path(name, 0, scene_dir)
@@ -81,9 +81,12 @@ def test_loader_rejects_bad_input(tmp_path):
     with pytest.raises(Y.YmrtError) as e:
         Y.HostScene(write(tmp_path, "Begin(Transform);\n\ttranslate = <0,0,0>;\n"), 8, 8)
     assert e.value.code == -3  # missing End
-    with pytest.raises(Y.YmrtError) as e:
-        Y.HostScene(write(tmp_path, 'Begin(CheckerBoardTexture);\n\tname = "t";\nEnd(CheckerBoardTexture);\n'), 8, 8)
+    with pytest.raises(Y.YmrtError) as e:  # image textures are not supported
+        Y.HostScene(write(tmp_path, 'Begin(ImageTexture);\n\tname = "t";\nEnd(ImageTexture);\n'), 8, 8)
     assert e.value.code == -4
+    with pytest.raises(Y.YmrtError) as e:  # a solid node needs both inputs (the reference's reader too)
+        Y.HostScene(write(tmp_path, 'Begin(CheckerBoardTexture);\n\tname = "t";\nEnd(CheckerBoardTexture);\n'), 8, 8)
+    assert e.value.code == -3
     with pytest.raises(Y.YmrtError) as e:  # instance referring to an undeclared name
         Y.HostScene(write(tmp_path, 'Begin(PrimitiveInstance);\n\tname = "i";\n\tgeometry_index = "g";\nEnd(PrimitiveInstance);\n'), 8, 8)
     assert e.value.code == -3

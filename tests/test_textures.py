@@ -1,0 +1,136 @@
+"""Texture nodes on the host: the solid (procedural) node types of the
+format, textured material parameters and normal / bump maps as the loader
+reads them, against the reference's own scene module.
+
+The generated ``textured`` scene holds every solid node type on material
+parameters and a medium density; the reference's own test scene
+(src/model/CornellBox_Test.ymtmp: checkerboard albedo, metalness and bump map
+on its ground) is checked too where the reference checkout is present. Node
+records (the 20 words of ymrt_texture_desc), materials, volumes and instances
+must equal the reference's bit for bit. The texture-graph checks (missing
+inputs, cycles, graphs deeper than the evaluation stack, image nodes) and the
+reference parser's attribute-name rule are exercised on small inputs.
+"""
+import os
+
+import numpy as np
+import pytest
+
+import ymrt_b200 as Y
+from ymrt_b200 import scenes
+from test_scene_arrays import arrays_of
+from test_scene_host import _meaningful
+
+
+def _compare_prepared(ours, ref):
+    assert np.array_equal(ours.instances(), ref.instances())
+    for kind in ("materials", "volumes", "distant_lights", "textures"):
+        a, b = _meaningful(kind, ours.records(kind)), _meaningful(kind, ref.records(kind))
+        assert np.array_equal(a, b), kind
+    la, lb = ours.lights(), ref.lights()
+    assert np.array_equal(la[0], lb[0])
+    assert np.array_equal(la[1].view(np.uint32), lb[1].view(np.uint32))
+    for g in range(ref.counts()["geometries"]):
+        assert np.array_equal(ours.triangles(g), ref.geometry_triangles(g)), f"mesh {g}"
+        assert np.array_equal(ours.mesh_corners(g).view(np.uint32), ref.mesh_corners(g).view(np.uint32)), f"mesh {g}"
+
+
+def test_textured_scene_covers_every_solid_node(scene_dir):
+    hs = Y.HostScene(scenes.scene_path("textured", 0, scene_dir), 64, 64)
+    types = set(hs.records("textures")[:, 0].tolist())
+    assert set(range(1, 11)) <= types, types
+    mats = hs.records("materials")
+    default = mats[mats[:, 0] == 0]
+    # every texture reference of DefaultMtl is used by some material: the words of diffuse_albedo_tex,
+    # specular_albedo_tex, alpha_x/y_tex, specular_weight_tex, metalness_tex, transmission_weight_tex,
+    # coat_albedo_tex, coat_weight_tex, coat_thickness_tex, coat_roughness_x/y_tex, normal and bump maps
+    slots = [4, 8, 10, 12, 14, 16, 18, 24, 26, 28, 30, 32, 34, 35]
+    assert all((default[:, w] != 0xFFFFFFFF).any() for w in slots), [w for w in slots if (default[:, w] == 0xFFFFFFFF).all()]
+
+
+def test_textured_scene_prepares_like_the_reference(scene_dir, halton_perm, oracle):
+    path = scenes.scene_path("textured", 0, scene_dir)
+    _compare_prepared(Y.HostScene(path, 256, 256), oracle.RefScene(path, halton_perm, 256, 256))
+
+
+def test_reference_test_scene_prepares_like_the_reference(halton_perm, oracle):
+    """src/model/CornellBox_Test.ymtmp, read where the reference checkout is."""
+    from oracle import build_ref
+    path = os.path.join(build_ref.REF, "src", "model", "CornellBox_Test.ymtmp")
+    if not os.path.exists(path):
+        pytest.skip("reference checkout absent")
+    ours = Y.HostScene(path, 320, 240)
+    ref = oracle.RefScene(path, halton_perm, 320, 240)
+    _compare_prepared(ours, ref)
+    tex = ours.records("textures")
+    assert (tex[:, 0] == 3).sum() == 3  # the checkerboard albedo, metalness and bump nodes
+
+
+def test_texture_nodes_from_arrays(scene_dir):
+    hs, kw = arrays_of("textured", scene_dir, 64, 64)
+    ha = Y.HostScene.from_arrays(64, 64, **kw)
+    assert np.array_equal(ha.records("textures"), hs.records("textures"))
+    assert np.array_equal(ha.records("materials"), hs.records("materials"))
+
+
+def _bad_textures(kw, textures, materials=None):
+    bad = dict(kw)
+    bad["textures"] = np.asarray(textures, np.uint32)
+    if materials is not None:
+        bad["materials"] = materials
+    with pytest.raises(Y.YmrtError) as e:
+        Y.HostScene.from_arrays(64, 64, **bad)
+    return e.value.code
+
+
+def _node(kind, black=0xFFFFFFFF, white=0xFFFFFFFF, freq=1.0):
+    r = np.zeros(Y.TEXTURE_WORDS, np.uint32)
+    r[0], r[1], r[2] = kind, black, white
+    r[7] = np.float32(freq).view(np.uint32)
+    return r
+
+
+def test_texture_graph_checks(scene_dir):
+    hs, kw = arrays_of("cornell", scene_dir, 64, 64)
+    const = _node(1)
+    # an image node is not supported
+    assert _bad_textures(kw, [_node(0)]) == -4
+    # a solid node needs both inputs
+    assert _bad_textures(kw, [const, _node(3, 0)]) == -1
+    # a graph read by a material: a cycle, and a chain deeper than the 8-node evaluation stack
+    mats = kw["materials"].copy()
+    mats[0, 4] = 0  # DefaultMtl.diffuse_albedo_tex of material 0 (after the type word and the rgb albedo)
+    cyc = [_node(3, 1, 1), _node(3, 0, 0)]
+    assert _bad_textures(kw, cyc, mats) == -1
+    deep = [_node(3, k + 1, k + 1) for k in range(8)] + [const]  # 9 nodes on the path from node 0
+    assert _bad_textures(kw, deep, mats) == -1
+    ok = dict(kw)
+    ok["textures"] = np.asarray(deep[1:], np.uint32)  # 8 nodes (renumbered): accepted
+    ok["textures"][:, 1:3] = np.where(ok["textures"][:, 1:3] != 0xFFFFFFFF, ok["textures"][:, 1:3] - 1, 0xFFFFFFFF)
+    ok["materials"] = mats
+    Y.HostScene.from_arrays(64, 64, **ok)
+    # deep graphs nothing reads are accepted
+    unused = dict(kw)
+    unused["textures"] = np.asarray(deep, np.uint32)
+    Y.HostScene.from_arrays(64, 64, **unused)
+    # a material referring to a node that does not exist
+    mats2 = kw["materials"].copy()
+    mats2[0, 4] = 5
+    assert _bad_textures(kw, [const], mats2) == -1
+
+
+def test_wave_parameters_are_illegal_statements(tmp_path, halton_perm, oracle):
+    """The reference's statement check allows letters and '_' in attribute
+    names only (src/core/YMParser.cpp:700-705), so NoiseTextureWave's
+    freq_0 .. layer_count_1 make a file unreadable; ours reads it the same."""
+    s = scenes.cornell_scene(0)
+    s.textures.append(("ConstantTextureFloat", "w0", {"value": 0.0}))
+    s.textures.append(("ConstantTextureFloat", "w1", {"value": 1.0}))
+    s.textures.append(("NoiseTextureWave", "wave", {"texture_black_idx": "w0", "texture_white_idx": "w1",
+                                                    "freq_0": 0.5}))
+    path = scenes.write_scene(s, str(tmp_path / "wave_params.ymtmp"))
+    with pytest.raises(Y.YmrtError) as e:
+        Y.HostScene(path, 32, 32)
+    assert e.value.code == -3
+    with pytest.raises(RuntimeError):
+        oracle.RefScene(path, halton_perm, 32, 32)

@@ -23,6 +23,7 @@ __all__ = [
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libymrt.so")
 HALTON_TABLE_SIZE = 3682913  # sum of the first 1000 primes
+TEXTURE_WORDS = 20  # 32-bit words of a ymrt_texture_desc
 
 YMRT_OK = 0
 ERRORS = {
@@ -136,6 +137,7 @@ def library():
     L.ymrt_scene_get_material_params.argtypes = [vp, ctypes.c_uint32, ctypes.c_uint32, vp]
     L.ymrt_scene_set_density_grid.argtypes = [vp, ctypes.c_uint32, i, i, i, vp, i]
     L.ymrt_debug_density.argtypes = [vp, ctypes.c_uint32, i, vp, vp]
+    L.ymrt_debug_texture.argtypes = [vp, ctypes.c_uint32, i, vp, vp]
     L.ymrt_render_forward.argtypes = [vp, ctypes.POINTER(RenderSetting), i, vp, i, ctypes.POINTER(Stats)]
     L.ymrt_render_tiles.argtypes = [vp, ctypes.POINTER(RenderSetting), i, i, i, vp, i, ctypes.POINTER(Stats)]
     L.ymrt_accumulate.argtypes = [vp, vp, vp, i]
@@ -254,7 +256,8 @@ class HostScene:
         normals, optional texcoord_indices / texcoords, or {"sphere_radius": r};
         instances / materials / volumes / distant_lights: the reference's
         structs as uint32 words ((n, 8), (n, 39), (n, 9), (n, 8)); textures:
-        (n, 13) words as records("textures") returns; camera: (from, look, fov)."""
+        (n, 20) words as records("textures") returns (ymrt_texture_desc); camera:
+        (from, look, fov)."""
         keep = []
 
         def arr(a, dtype, cols=None):
@@ -290,7 +293,7 @@ class HostScene:
         d.materials, d.material_count = arr(materials, np.uint32, 39)
         d.volumes, d.volume_count = arr(volumes, np.uint32, 9)
         d.distant_lights, d.distant_light_count = arr(distant_lights, np.uint32, 8)
-        d.textures, d.texture_count = arr(textures, np.uint32, 13)
+        d.textures, d.texture_count = arr(textures, np.uint32, TEXTURE_WORDS)
         frm, look, fov = camera
         d.camera_from[:] = [float(x) for x in frm]
         d.camera_look[:] = [float(x) for x in look]
@@ -362,9 +365,10 @@ class HostScene:
 
     def records(self, kind: str) -> np.ndarray:
         """Materials, volumes, distant lights (32-bit words of the reference's
-        structs) or textures (13 words each), one row per record."""
+        structs) or textures (TEXTURE_WORDS words each: ymrt_texture_desc), one
+        row per record."""
         what, width = {"materials": (QUERY_MATERIALS, 39), "volumes": (QUERY_VOLUMES, 9),
-                       "distant_lights": (QUERY_DISTANT_LIGHTS, 8), "textures": (QUERY_TEXTURES, 13)}[kind]
+                       "distant_lights": (QUERY_DISTANT_LIGHTS, 8), "textures": (QUERY_TEXTURES, TEXTURE_WORDS)}[kind]
         return self._query(what, np.uint32).reshape(-1, width)
 
 
@@ -400,6 +404,18 @@ class Scene:
             raise ValueError("density grid must be a (nz, ny, nx) array")
         nz, ny, nx = v.shape
         _check(library().ymrt_scene_set_density_grid(self.h, texture_index, nx, ny, nz, _p(v), int(half)), self.ctx.h)
+
+    def texture(self, texture_index: int, st, points) -> np.ndarray:
+        """rgb of texture node `texture_index` as a surface reads it, at
+        texture coordinates st (n, 2) and object-space points (n, 3)."""
+        st = np.asarray(st, np.float32).reshape(-1, 2)
+        p = np.asarray(points, np.float32).reshape(-1, 3)
+        if st.shape[0] != p.shape[0]:
+            raise ValueError("st and points must have the same length")
+        c = np.ascontiguousarray(np.concatenate([st, p], axis=1), np.float32)
+        out = np.zeros((c.shape[0], 3), np.float32)
+        _check(library().ymrt_debug_texture(self.h, texture_index, c.shape[0], _p(c), _p(out)), self.ctx.h)
+        return out
 
     def density(self, texture_index: int, points) -> np.ndarray:
         """Texture node `texture_index` at object-space points (n, 3), on the device."""

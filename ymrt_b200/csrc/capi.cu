@@ -172,6 +172,27 @@ struct ymrt_context {
 
 namespace {
 
+// Whether a default material reads any texture (parameters, normal or bump map).
+bool material_textures(const DefaultMtl& d) {
+  const uint32_t tex[] = {d.diffuse_albedo_tex, d.alpha_x_tex, d.specular_albedo_tex, d.alpha_y_tex,
+                          d.specular_weight_tex, d.metalness_tex, d.transmission_weight_tex, d.normal_mapping_tex,
+                          d.bump_mapping_tex, d.coat_albedo_tex, d.coat_weight_tex, d.coat_thickness_tex,
+                          d.coat_roughness_x_tex, d.coat_roughness_y_tex};
+  for (uint32_t t : tex)
+    if (t != kEmpty) return true;
+  return false;
+}
+
+// DeviceScene::textured: a material reads textures, or a medium's density
+// graph holds a solid node beyond fBm (both need the full node set).
+bool uses_textures(const std::vector<Material>& materials, const std::vector<Texture>& textures) {
+  for (const Material& m : materials)
+    if (m.material_type == kDefaultMtl && material_textures(m.default_mtl)) return true;
+  for (const Texture& t : textures)
+    if (t.type >= kTexChecker && t.type <= kTexWave && t.type != kTexFbm) return true;
+  return false;
+}
+
 // Shading bucket of a hit on `inst`: pass-through boundaries, lights and
 // invalid materials share the cheap bucket; a default material's bucket is
 // the set of lobes its constant parameters switch on (the lobes
@@ -181,6 +202,7 @@ uint32_t shading_bucket(const HostScene& s, const Instance& inst) {
   const Material& m = s.materials[inst.material_idx];
   if (m.material_type != kDefaultMtl) return kBucketCheap;
   const DefaultMtl& d = m.default_mtl;
+  if (material_textures(d)) return kBucketLobes + 31u;  // lobes vary over the surface
   const bool not_metal = d.metalness < 1.0f;
   uint32_t mask = 0;
   if (d.coat_weight > 0.0f) mask |= 1u;
@@ -442,17 +464,9 @@ long long ymrt_host_scene_query(const ymrt_host_scene* hs, int what, int index, 
     case YMRT_QUERY_TEXTURES: {
       std::vector<uint32_t> v;
       for (const Texture& t : s.textures) {
-        uint32_t r[13] = {t.type, kEmpty, kEmpty, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
-        if (t.type == kTexConstFloat) {
-          r[3] = f2u(t.value);
-        } else if (t.type == kTexConstRgb) {
-          r[4] = f2u(t.color.x); r[5] = f2u(t.color.y); r[6] = f2u(t.color.z);
-        } else if (t.type == kTexFbm) {
-          r[1] = t.child[0]; r[2] = t.child[1];
-          r[7] = f2u(t.frequency); r[8] = f2u(t.lacunarity); r[9] = f2u(t.gain); r[10] = (uint32_t)t.layer_count;
-          r[11] = f2u(t.amplitude); r[12] = f2u(t.offset);
-        }
-        v.insert(v.end(), r, r + 13);
+        uint32_t r[kTextureWords];
+        texture_words(t, r);
+        v.insert(v.end(), r, r + kTextureWords);
       }
       return copy(v.data(), v.size(), sizeof(uint32_t));
     }
@@ -497,16 +511,6 @@ int ymrt_scene_upload(ymrt_context* ctx, const ymrt_host_scene* hs, const uint32
   if (perm_len != need)
     return ctx->fail(YMRT_ERR_INVALID, "halton permutation table must hold " + std::to_string(need) + " entries");
   const HostScene& s = hs->s;
-  for (const Material& m : s.materials) {
-    if (m.material_type != kDefaultMtl) continue;
-    const DefaultMtl& d = m.default_mtl;
-    const uint32_t tex[] = {d.diffuse_albedo_tex, d.alpha_x_tex, d.specular_albedo_tex, d.alpha_y_tex,
-                            d.specular_weight_tex, d.metalness_tex, d.transmission_weight_tex, d.normal_mapping_tex,
-                            d.bump_mapping_tex, d.coat_albedo_tex, d.coat_weight_tex, d.coat_thickness_tex,
-                            d.coat_roughness_x_tex, d.coat_roughness_y_tex};
-    for (uint32_t t : tex)
-      if (t != kEmpty) return ctx->fail(YMRT_ERR_UNSUPPORTED, "textured material parameters are not supported");
-  }
   cudaSetDevice(ctx->device);
   std::unique_ptr<ymrt_scene> sc(new (std::nothrow) ymrt_scene());
   if (!sc) return YMRT_ERR_OOM;
@@ -566,6 +570,7 @@ int ymrt_scene_upload(ymrt_context* ctx, const ymrt_host_scene* hs, const uint32
   D.shape_light_count = (uint32_t)s.shape_lights.size();
   D.volume_count = (uint32_t)s.volumes.size();
   D.texture_count = (uint32_t)s.textures.size();
+  D.textured = uses_textures(s.materials, s.textures) ? 1u : 0u;
   D.camera = s.camera;
   D.width = s.width;
   D.height = s.height;
@@ -857,12 +862,14 @@ int finish_batch(ymrt_context* ctx, const BatchResult& r, ymrt_stats* stats) {
   return YMRT_OK;
 }
 
-// The features (kFeatSpheres, kFeatGrids) any of the batch's scenes uses.
+// The features (kFeatSpheres, kFeatGrids, kFeatTextures) any of the batch's
+// scenes uses.
 uint32_t batch_features(const DeviceScene* scenes, size_t n) {
   uint32_t f = 0;
   for (size_t i = 0; i < n; ++i) {
     if (scenes[i].sphere_count != 0) f |= kFeatSpheres;
     if (scenes[i].grid_count != 0) f |= kFeatGrids;
+    if (scenes[i].textured != 0) f |= kFeatTextures;
   }
   return f;
 }
@@ -1157,6 +1164,7 @@ int ymrt_scene_set_density_grid(ymrt_scene* scene, uint32_t texture_index, int n
   t.grid = buf->ptr;
   scene->dev.grid_count = 0;
   for (const Texture& x : scene->textures) scene->dev.grid_count += x.type == kTexGrid ? 1u : 0u;
+  scene->dev.textured = uses_textures(scene->materials, scene->textures) ? 1u : 0u;
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(const_cast<Texture*>(scene->dev.textures) + texture_index, &t, sizeof(Texture),
                         cudaMemcpyHostToDevice, ctx->stream);
@@ -1573,6 +1581,29 @@ int ymrt_debug_density(ymrt_scene* sc, uint32_t texture_index, int n, const floa
   sg.back(&errs, d_err, 1);
   cudaError_t e = cudaStreamSynchronize(ctx->stream);
   if (sg.err != cudaSuccess || e != cudaSuccess) return ctx->cuda_fail(sg.err != cudaSuccess ? sg.err : e, "debug density");
+  if (errs) return ctx->fail(YMRT_ERR_OVERFLOW, "texture graph too deep");
+  return YMRT_OK;
+}
+
+int ymrt_debug_texture(ymrt_scene* sc, uint32_t texture_index, int n, const float* coords, float* rgb) {
+  if (!sc || n < 0 || !coords || !rgb) return YMRT_ERR_INVALID;
+  if (texture_index >= sc->textures.size()) return sc->ctx->fail(YMRT_ERR_INVALID, "texture index out of range");
+  if (n == 0) return YMRT_OK;
+  ymrt_context* ctx = sc->ctx;
+  cudaSetDevice(ctx->device);
+  Staging sg{ctx};
+  const float* d_c = sg.in(coords, 5 * (size_t)n);
+  float* d_out = sg.out<float>(3 * (size_t)n);
+  uint32_t* d_err = sg.out<uint32_t>(1);
+  if (sg.err != cudaSuccess) return ctx->cuda_fail(sg.err, "staging");
+  cudaMemsetAsync(d_err, 0, sizeof(uint32_t), ctx->stream);
+  upload_constants(&sc->dev, 1, ctx->primes.data(), ctx->prime_sums.data(), ctx->stream);
+  launch_debug_texture(n, texture_index, d_c, d_out, d_err, ctx->stream);
+  uint32_t errs = 0;
+  sg.back(rgb, d_out, 3 * (size_t)n);
+  sg.back(&errs, d_err, 1);
+  cudaError_t e = cudaStreamSynchronize(ctx->stream);
+  if (sg.err != cudaSuccess || e != cudaSuccess) return ctx->cuda_fail(sg.err != cudaSuccess ? sg.err : e, "debug texture");
   if (errs) return ctx->fail(YMRT_ERR_OVERFLOW, "texture graph too deep");
   return YMRT_OK;
 }

@@ -8,6 +8,7 @@
 // places where the reference mixes in double-precision literals.
 #pragma once
 
+#include "dev_texture.cuh"
 #include "sphere.h"
 #include "ymrt_scene.h"
 
@@ -17,11 +18,11 @@ namespace ym {
 
 struct SurfacePoint {
   vec3 p, p_err, p_obj, ns, ng, dpdu, dpdv;
+  float u, v;  // texture coordinates
 };
 
 // FetchSphereShadingData (src/ShadingUtilities.cuh:639-711) in object space:
-// `p` is the hit point the sphere test projected onto the sphere. The
-// texture coordinates are not formed: no texture here reads them.
+// `p` is the hit point the sphere test projected onto the sphere.
 __device__ __forceinline__ void sphere_surface(float sphere_radius, vec3 p, SurfacePoint* sp) {
   const float radius = gmax(sphere_radius, kFloatEps);
   const vec3 n = p / radius;
@@ -29,6 +30,11 @@ __device__ __forceinline__ void sphere_surface(float sphere_radius, vec3 p, Surf
   sp->p_err = error_gamma(5) * vabs(p);
   sp->ns = n;
   sp->ng = n;
+  const float theta = acosf(n.y);
+  float phi = atan2f(n.z, n.x);
+  if (phi < 0.0f) phi += kTwoPi;
+  sp->u = 0.5f * phi * kInvPi;
+  sp->v = theta * kInvPi;
   float sin_theta = 0.0f;
   if (1.0f - n.y * n.y > 0.0f) sin_theta = sqrtf(1.0f - n.y * n.y);
   float cos_phi, sin_phi;
@@ -95,6 +101,8 @@ __device__ __forceinline__ SurfacePoint fetch_surface(const DeviceScene& S, uint
     u1x = uvb[2 * t1]; u1y = uvb[2 * t1 + 1];
     u2x = uvb[2 * t2]; u2y = uvb[2 * t2 + 1];
   }
+  sp.u = u0x * bary.x + u1x * bary.y + u2x * bary.z;
+  sp.v = u0y * bary.x + u1y * bary.y + u2y * bary.z;
   float du01 = u1x - u0x, dv01 = u1y - u0y;
   float du02 = u2x - u0x, dv02 = u2y - u0y;
   float det = du01 * dv02 - dv01 * du02;
@@ -155,7 +163,6 @@ __device__ __forceinline__ void fetch_geometry_normal(const DeviceScene& S, uint
 // ---------------------------------------------------------- microfacet ---
 // src/BSDF.cuh:19-176.
 
-__device__ __forceinline__ float sqr(float x) { return x * x; }
 
 __device__ __forceinline__ vec3 reflect(vec3 wo, vec3 n) { return -wo + 2.0f * n * dot(n, wo); }
 
@@ -400,6 +407,159 @@ __device__ __forceinline__ void init_shading_frame(LayeredBsdf& B, int hit_back,
     B.t = normalize(B.t - B.n * dot(B.t, B.n));
     B.b = hit_back ? -cross(B.n, B.t) : cross(B.n, B.t);
   }
+}
+
+// ------------------------------------------------------ textured surfaces ---
+
+// A material texture read at a surface point: every node type (grids
+// included), one out-of-line copy for all callers.
+__device__ __noinline__ vec3 surface_texture(const Texture* __restrict__ tex, uint32_t root, const TexCoord& tc,
+                                             uint32_t* errors) {
+  return texture_eval<kFeatGrids | kFeatTextures>(tex, root, tc, errors);
+}
+
+// Camera::TextureCoordinatesDifferential (src/Camera.h:56-140) with the
+// reference's pixel-footprint scales (0.25, 0.25): the texture-coordinate
+// footprint (du/dx, dv/dx, du/dy, dv/dy) of a pixel at a hit, from the
+// offset camera rays' intersections with the hit's tangent plane (the
+// offsets are added to the local -z axis in world-space directions, as the
+// reference does). Zero when dp/du, dp/dv are degenerate in the plane the
+// geometric normal selects.
+__device__ __forceinline__ void tex_differentials(const CameraDesc& cam, vec3 p, vec3 ns, vec3 ng, vec3 dpdu, vec3 dpdv,
+                                                  int width, int height, float sx, float sy, float d[4]) {
+  vec3 look = cam.position - p;
+  const float dist = length(look);
+  look *= safe_rcp(dist);
+  const vec3 right = normalize(cam.u - look * dot(cam.u, look));
+  const vec3 up = cross(look, right);
+  const float plane_h = 2.0f * cam.tan_half_fov;
+  const float y_off = plane_h * sy / (float)height;
+  const float plane_w = plane_h * cam.aspect_ratio;
+  const float x_off = plane_w * sx / (float)width;
+  auto min_abs = [](float f, float th) { return fabsf(f) < th ? (f > 0.0f ? th : -th) : f; };
+  const vec3 dxd = normalize(vec3(0.0f, 0.0f, -1.0f) + right * x_off);
+  const vec3 dyd = normalize(vec3(0.0f, 0.0f, -1.0f) + up * y_off);
+  const vec3 ln(dot(ns, right), dot(ns, up), dot(ns, look));
+  const vec3 lp(0.0f, 0.0f, -dist);
+  const float tx = dot(ln, lp) / min_abs(dot(ln, dxd), 1E-4f);
+  vec3 dpdx = (dxd * tx - lp) * safe_rcp(sx);
+  const float ty = dot(ln, lp) / min_abs(dot(ln, dyd), 1E-4f);
+  vec3 dpdy = (dyd * ty - lp) * safe_rcp(sy);
+  dpdx = dpdx.x * right + dpdx.y * up + dpdx.z * look;
+  dpdy = dpdy.x * right + dpdy.y * up + dpdy.z * look;
+  const vec3 an = vabs(ng);
+  int a0, a1;
+  if (an.z > an.y && an.z > an.x) {
+    a0 = 0;
+    a1 = 1;
+  } else if (an.y > an.x) {
+    a0 = 0;
+    a1 = 2;
+  } else {
+    a0 = 1;
+    a1 = 2;
+  }
+  const float m00 = dpdu[a0], m01 = dpdv[a0], m10 = dpdu[a1], m11 = dpdv[a1];
+  const float det = m00 * m11 - m10 * m01;
+  if (fabsf(det) < 1E-7f) {
+    d[0] = d[1] = d[2] = d[3] = 0.0f;
+    return;
+  }
+  const float idet = 1.0f / det;
+  d[0] = (m11 * dpdx[a0] - m01 * dpdx[a1]) * idet;
+  d[1] = (-m10 * dpdx[a0] + m00 * dpdx[a1]) * idet;
+  d[2] = (m11 * dpdy[a0] - m01 * dpdy[a1]) * idet;
+  d[3] = (-m10 * dpdy[a0] + m00 * dpdy[a1]) * idet;
+}
+
+// MaterialBSDF::InitShadingSpace (src/BSDF.cuh:694-807) with normal mapping
+// (the node's rgb * 2 - 1 as tangent-space normal) or bump mapping (the
+// height node's first channel, differenced over the pixel's texture
+// footprint, at least 0.0005, along the tangents).
+__device__ __noinline__ void init_shading_frame_mapped(LayeredBsdf& B, const DefaultMtl& m, int hit_back, vec3 ray_dir,
+                                                       const SurfacePoint& sp, const mat4& wto, const DeviceScene& S,
+                                                       const TexCoord& tc, uint32_t* errors) {
+  vec3 sn = sp.ns;
+  if (dot(sp.ns, sp.ng) < 0.0f) sn = -sp.ns;
+  vec3 su = sp.dpdu;
+  if (dot(cross(sp.dpdu, sp.dpdv), sp.ng) < 0.0f) su = -sp.dpdu;
+  vec3 sv = sp.dpdv;
+  su = su - sn * dot(su, sn);
+  sv = sv - sn * dot(sv, sn);
+  auto frame = [&](vec3 n, vec3 du) {
+    if (!hit_back) {
+      B.n = n;
+      B.t = normalize(du);
+      B.b = cross(B.n, B.t);
+    } else {
+      B.n = -n;
+      B.t = -normalize(du);
+      B.b = -cross(B.n, B.t);
+    }
+  };
+  if (m.normal_mapping_tex != kEmpty) {
+    frame(sn, su);
+    const vec3 tn = normalize(surface_texture(S.textures, m.normal_mapping_tex, tc, errors) * 2.0f - vec3(1.0f));
+    B.n = tn.x * B.t + tn.y * B.b + tn.z * B.n;
+    B.t = normalize(B.t - B.n * dot(B.t, B.n));
+    B.b = hit_back ? -cross(B.n, B.t) : cross(B.n, B.t);
+  } else if (m.bump_mapping_tex != kEmpty) {
+    float d[4];
+    tex_differentials(S.camera, sp.p, sp.ns, sp.ng, sp.dpdu, sp.dpdv, S.width, S.height, 0.25f, 0.25f, d);
+    const vec3 ou = transform_vector(wto, su), ov = transform_vector(wto, sv);
+    float du = gmax((fabsf(d[0]) + fabsf(d[2])) * 0.5f, 0.0005f);
+    if (!(du > 0.0f)) du = 0.0005f;
+    TexCoord bc{tc.s + du, tc.t, tc.p + ou * du};
+    const float hu = surface_texture(S.textures, m.bump_mapping_tex, bc, errors).x;
+    float dv = gmax((fabsf(d[1]) + fabsf(d[3])) * 0.5f, 0.0005f);
+    if (!(dv > 0.0f)) dv = 0.0005f;
+    bc = TexCoord{tc.s, tc.t + dv, tc.p + ov * dv};
+    const float hv = surface_texture(S.textures, m.bump_mapping_tex, bc, errors).x;
+    const float h = surface_texture(S.textures, m.bump_mapping_tex, tc, errors).x;
+    su = su + (hu - h) * safe_rcp(du) * sn;
+    sv = sv + (hv - h) * safe_rcp(dv) * sn;
+    sn = normalize(cross(su, sv));
+    frame(sn, su);
+  } else {
+    frame(sn, su);
+  }
+  if (dot(-ray_dir, B.n) < 0.0f) {
+    B.n = reflect(B.n, dot(B.n, sp.ng) > 0.0f ? sp.ng : -sp.ng);
+    B.t = normalize(B.t - B.n * dot(B.t, B.n));
+    B.b = hit_back ? -cross(B.n, B.t) : cross(B.n, B.t);
+  }
+}
+
+// The textured parameters of a default material, read at the hit
+// (DefaultMtlBSDF::InitBSDFSettings' fetch_float / fetch_color,
+// src/BSDF.cuh:463-498): a float parameter takes its node's first channel.
+// Unlike the constants, the values are not clamped at load.
+__device__ __noinline__ void resolve_material_textures(DefaultMtl& m, const Texture* __restrict__ tex,
+                                                       const TexCoord& tc, uint32_t* errors) {
+  auto f = [&](uint32_t t, float* v) {
+    if (t != kEmpty) *v = surface_texture(tex, t, tc, errors).x;
+  };
+  auto c = [&](uint32_t t, vec3* v) {
+    if (t != kEmpty) *v = surface_texture(tex, t, tc, errors);
+  };
+  f(m.coat_weight_tex, &m.coat_weight);
+  f(m.metalness_tex, &m.metalness);
+  f(m.alpha_x_tex, &m.alpha_x);
+  f(m.alpha_y_tex, &m.alpha_y);
+  f(m.specular_weight_tex, &m.specular_weight);
+  f(m.transmission_weight_tex, &m.transmission_weight);
+  c(m.diffuse_albedo_tex, &m.diffuse_albedo);
+  c(m.specular_albedo_tex, &m.specular_albedo);
+  f(m.coat_thickness_tex, &m.coat_thickness);
+  f(m.coat_roughness_x_tex, &m.coat_roughness_x);
+  f(m.coat_roughness_y_tex, &m.coat_roughness_y);
+  c(m.coat_albedo_tex, &m.coat_albedo);
+}
+
+__device__ __forceinline__ bool material_textured(const DefaultMtl& m) {
+  return (m.diffuse_albedo_tex & m.specular_albedo_tex & m.alpha_x_tex & m.alpha_y_tex & m.specular_weight_tex &
+          m.metalness_tex & m.transmission_weight_tex & m.coat_albedo_tex & m.coat_weight_tex & m.coat_thickness_tex &
+          m.coat_roughness_x_tex & m.coat_roughness_y_tex & m.normal_mapping_tex & m.bump_mapping_tex) != kEmpty;
 }
 
 // DefaultMtlBSDF::InitBSDFSettings with constant parameters (src/BSDF.cuh:453-618).

@@ -580,18 +580,24 @@ struct AdjCtx {
   float ax[2], ay[2];                     // the microfacet lobes' alpha at roughness +-h
 };
 
+// m: the material's parameters as read at the vertex. A parameter a texture
+// supplies does not depend on the material's constant: its derivative is 0.
 __device__ __noinline__ void init_adjoint(AdjCtx& a, const LayeredBsdf& B, const DefaultMtl& m) {
+  const bool albedo_const = m.diffuse_albedo_tex == kEmpty;
+  const float ha = albedo_const ? kParamStep : 0.0f;
+  const float hx = m.alpha_x_tex == kEmpty ? kParamStep : 0.0f;
+  const float hy = m.alpha_y_tex == kEmpty ? kParamStep : 0.0f;
   a.lambert_coeff = vec3(0.0f);
   for (int i = 0; i < B.count; ++i)
-    if (B.lobe[i].role == kRoleDiffuse)
+    if (B.lobe[i].role == kRoleDiffuse && albedo_const)
       for (int c = 0; c < 3; ++c)
         a.lambert_coeff[c] = m.diffuse_albedo[c] > 0.0f ? B.lobe[i].albedo[c] / m.diffuse_albedo[c] : 0.0f;
-  edge_tint_to_conductor(m.diffuse_albedo + vec3(kParamStep), m.specular_albedo, &a.metal_n[0], &a.metal_k[0]);
-  edge_tint_to_conductor(m.diffuse_albedo - vec3(kParamStep), m.specular_albedo, &a.metal_n[1], &a.metal_k[1]);
-  a.ax[0] = sqr(gclamp(m.alpha_x + kParamStep, 0.001f, 0.999f));
-  a.ax[1] = sqr(gclamp(m.alpha_x - kParamStep, 0.001f, 0.999f));
-  a.ay[0] = sqr(gclamp(m.alpha_y + kParamStep, 0.001f, 0.999f));
-  a.ay[1] = sqr(gclamp(m.alpha_y - kParamStep, 0.001f, 0.999f));
+  edge_tint_to_conductor(m.diffuse_albedo + vec3(ha), m.specular_albedo, &a.metal_n[0], &a.metal_k[0]);
+  edge_tint_to_conductor(m.diffuse_albedo - vec3(ha), m.specular_albedo, &a.metal_n[1], &a.metal_k[1]);
+  a.ax[0] = sqr(gclamp(m.alpha_x + hx, 0.001f, 0.999f));
+  a.ax[1] = sqr(gclamp(m.alpha_x - hx, 0.001f, 0.999f));
+  a.ay[0] = sqr(gclamp(m.alpha_y + hy, 0.001f, 0.999f));
+  a.ay[1] = sqr(gclamp(m.alpha_y - hy, 0.001f, 0.999f));
   for (int k = 0; k < kGradParams; ++k) a.g[k] = 0.0f;
 }
 
@@ -1149,8 +1155,23 @@ __global__ void __launch_bounds__(kTraceBlock) k_shade(PathPool P, const WaveCon
       }
       if (!done) {
         LayeredBsdf B;
-        init_shading_frame(B, hit_back, rd, sp.ng, sp.ns, sp.dpdu, sp.dpdv);
-        init_layered_lobes(B, mat.default_mtl, rd, hit_back, ray_ior(rt), ex_ior(rt, inst_idx));
+        const DefaultMtl* mp = &mat.default_mtl;
+        DefaultMtl mt;
+        if constexpr ((kF & kFeatTextures) != 0) {
+          if (material_textured(mat.default_mtl)) {
+            // textured parameters, normal or bump mapping: read at the hit
+            mt = mat.default_mtl;
+            const TexCoord tc{sp.u, sp.v, sp.p_obj};
+            init_shading_frame_mapped(B, mt, hit_back, rd, sp, S.i_transforms[inst.transform_idx], S, tc, errors);
+            resolve_material_textures(mt, S.textures, tc, errors);
+            mp = &mt;
+          } else {
+            init_shading_frame(B, hit_back, rd, sp.ng, sp.ns, sp.dpdu, sp.dpdv);
+          }
+        } else {
+          init_shading_frame(B, hit_back, rd, sp.ng, sp.ns, sp.dpdu, sp.dpdv);
+        }
+        init_layered_lobes(B, *mp, rd, hit_back, ray_ior(rt), ex_ior(rt, inst_idx));
         const SurfaceNee nc{rd, sp.p, sp.p_err, sp.ng, inst_idx, tri, &rt, nb, n_nb, rs.enable_volume_scattering != 0,
                             slot};
         const ShadowEmit em{shadow_q, &counters->shadow_count, errors, pf.x, job, P.path_id[i], tp * inv_spp};
@@ -1162,7 +1183,7 @@ __global__ void __launch_bounds__(kTraceBlock) k_shade(PathPool P, const WaveCon
           const float4 lt = J.path_radiance[P.path_id[i]];
           delta = vec3(dl.x, dl.y, dl.z) * inv_spp;  // dLoss/d(this path's radiance)
           l_total = vec3(lt.x, lt.y, lt.z);
-          init_adjoint(adj_ctx, B, mat.default_mtl);
+          init_adjoint(adj_ctx, B, *mp);
           adj_ctx.weight = delta * tp;
           adj_ctx.grid_grads = grid_grads;
           adj_ctx.grid_tex = grid_tex;
@@ -1360,6 +1381,18 @@ __global__ void k_debug_density(int n, uint32_t tex, const float* p, float* out,
   out[i] = texture_eval(S.textures, tex, vec3(p[3 * i], p[3 * i + 1], p[3 * i + 2]), errors).x;
 }
 
+// Texture node `tex` of scene slot 0 at points (s, t, x, y, z): rgb out.
+__global__ void k_debug_texture(int n, uint32_t tex, const float* c, float* out, uint32_t* errors) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const DeviceScene& S = c_scenes[0];
+  const TexCoord tc{c[5 * i], c[5 * i + 1], vec3(c[5 * i + 2], c[5 * i + 3], c[5 * i + 4])};
+  const vec3 r = surface_texture(S.textures, tex, tc, errors);
+  out[3 * i] = r.x;
+  out[3 * i + 1] = r.y;
+  out[3 * i + 2] = r.z;
+}
+
 __global__ void k_debug_halton(int n, const int* px, const int* py, const int* sample, int n_dims, uint64_t* index,
                                float* offset, float* dims) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1450,22 +1483,32 @@ uint32_t grid_for(K kernel, int block, int sms) {
   return (uint32_t)(per_sm * sms);
 }
 
-// The wave's extend, shade and connect launches for scene features kF. The
-// surface kernels depend on the sphere bit only (grids are media), so they
-// are instantiated for kF & kFeatSpheres.
+// The wave's extend, shade and connect launches for scene features kF.
+// Surface kernels are instantiated on the sphere and texture bits (grids are
+// media); media kernels on the sphere bit and one bit for the full texture
+// node set (grids or the solid nodes beyond fBm switch on both), so a batch
+// runs one of four instantiations of each.
+template <uint32_t kF>
+constexpr uint32_t surface_features() {
+  return kF & (kFeatSpheres | kFeatTextures);
+}
+template <uint32_t kF>
+constexpr uint32_t media_features() {
+  return (kF & (kFeatGrids | kFeatTextures)) ? (kF | kFeatGrids | kFeatTextures) : kF;
+}
+
 template <uint32_t kF>
 void launch_extend(bool volumes, uint32_t blocks, const PathPool& A, const WaveControl* ctl, const HitPool& Hs,
                    const JobDesc* jobs, WaveCounters* counters, cudaStream_t stream) {
-  constexpr uint32_t kS = kF & kFeatSpheres;
-  if (volumes) k_extend<true, kF><<<blocks, kTraceBlock, 0, stream>>>(A, ctl, Hs, jobs, counters);
-  else k_extend<false, kS><<<blocks, kTraceBlock, 0, stream>>>(A, ctl, Hs, jobs, counters);
+  if (volumes) k_extend<true, media_features<kF>()><<<blocks, kTraceBlock, 0, stream>>>(A, ctl, Hs, jobs, counters);
+  else k_extend<false, kF & kFeatSpheres><<<blocks, kTraceBlock, 0, stream>>>(A, ctl, Hs, jobs, counters);
 }
 
 template <uint32_t kF>
 void launch_shade(bool adjoint, bool volumes, const ShadowQueue* defer, uint32_t blocks, const PathPool& A,
                   const WaveControl* ctl, const HitPool& Hs, const PathPool& B, const JobDesc* jobs,
                   WaveCounters* counters, const WaveOptions& opt, cudaStream_t stream) {
-  constexpr uint32_t kS = kF & kFeatSpheres;
+  constexpr uint32_t kS = surface_features<kF>();
   const ShadowQueue none{};
   if (adjoint && volumes)  // one instantiation (all features) for the media adjoint
     k_shade<true, false, true, kFeatAll><<<blocks, kTraceBlock, 0, stream>>>(
@@ -1474,7 +1517,8 @@ void launch_shade(bool adjoint, bool volumes, const ShadowQueue* defer, uint32_t
     k_shade<false, false, true, kS><<<blocks, kTraceBlock, 0, stream>>>(A, ctl, Hs, B, jobs, counters, none, opt.grads,
                                                                         opt.grad_materials);
   else if (volumes)
-    k_shade<true, false, false, kF><<<blocks, kTraceBlock, 0, stream>>>(A, ctl, Hs, B, jobs, counters, none);
+    k_shade<true, false, false, media_features<kF>()><<<blocks, kTraceBlock, 0, stream>>>(A, ctl, Hs, B, jobs,
+                                                                                         counters, none);
   else if (defer)
     k_shade<false, true, false, kS><<<blocks, kTraceBlock, 0, stream>>>(A, ctl, Hs, B, jobs, counters, *defer);
   else
@@ -1522,7 +1566,11 @@ uint32_t launch_wave(const PathPool& A, const PathPool& B, const HitPool& H, Wav
     case 0: launch_extend<0>(opt.volumes, blocks_trace, A, ctl, Hs, jobs, counters, stream); break;
     case 1: launch_extend<1>(opt.volumes, blocks_trace, A, ctl, Hs, jobs, counters, stream); break;
     case 2: launch_extend<2>(opt.volumes, blocks_trace, A, ctl, Hs, jobs, counters, stream); break;
-    default: launch_extend<3>(opt.volumes, blocks_trace, A, ctl, Hs, jobs, counters, stream); break;
+    case 3: launch_extend<3>(opt.volumes, blocks_trace, A, ctl, Hs, jobs, counters, stream); break;
+    case 4: launch_extend<4>(opt.volumes, blocks_trace, A, ctl, Hs, jobs, counters, stream); break;
+    case 5: launch_extend<5>(opt.volumes, blocks_trace, A, ctl, Hs, jobs, counters, stream); break;
+    case 6: launch_extend<6>(opt.volumes, blocks_trace, A, ctl, Hs, jobs, counters, stream); break;
+    default: launch_extend<7>(opt.volumes, blocks_trace, A, ctl, Hs, jobs, counters, stream); break;
   }
   if (ev) cudaEventRecord(ev[2], stream);
   if (sort_hits) k_sort_hits<<<blocks_256, 256, 0, stream>>>(ctl, Hs, A, jobs, counters);
@@ -1531,7 +1579,11 @@ uint32_t launch_wave(const PathPool& A, const PathPool& B, const HitPool& H, Wav
     case 0: launch_shade<0>(adjoint, opt.volumes, defer, blocks_trace, A, ctl, Hs, B, jobs, counters, opt, stream); break;
     case 1: launch_shade<1>(adjoint, opt.volumes, defer, blocks_trace, A, ctl, Hs, B, jobs, counters, opt, stream); break;
     case 2: launch_shade<2>(adjoint, opt.volumes, defer, blocks_trace, A, ctl, Hs, B, jobs, counters, opt, stream); break;
-    default: launch_shade<3>(adjoint, opt.volumes, defer, blocks_trace, A, ctl, Hs, B, jobs, counters, opt, stream); break;
+    case 3: launch_shade<3>(adjoint, opt.volumes, defer, blocks_trace, A, ctl, Hs, B, jobs, counters, opt, stream); break;
+    case 4: launch_shade<4>(adjoint, opt.volumes, defer, blocks_trace, A, ctl, Hs, B, jobs, counters, opt, stream); break;
+    case 5: launch_shade<5>(adjoint, opt.volumes, defer, blocks_trace, A, ctl, Hs, B, jobs, counters, opt, stream); break;
+    case 6: launch_shade<6>(adjoint, opt.volumes, defer, blocks_trace, A, ctl, Hs, B, jobs, counters, opt, stream); break;
+    default: launch_shade<7>(adjoint, opt.volumes, defer, blocks_trace, A, ctl, Hs, B, jobs, counters, opt, stream); break;
   }
   if (ev) cudaEventRecord(ev[4], stream);
   if (defer && (feat & kFeatSpheres)) k_connect<kFeatSpheres><<<g.connect, kTraceBlock, 0, stream>>>(*defer, jobs, counters);
@@ -1556,6 +1608,11 @@ void launch_debug_trace(int n, const float* o, const float* d, const uint32_t* l
 void launch_debug_density(int n, uint32_t tex, const float* p, float* out, uint32_t* err, cudaStream_t stream) {
   if (n <= 0) return;
   k_debug_density<<<(n + 255) / 256, 256, 0, stream>>>(n, tex, p, out, err);
+}
+
+void launch_debug_texture(int n, uint32_t tex, const float* c, float* out, uint32_t* err, cudaStream_t stream) {
+  if (n <= 0) return;
+  k_debug_texture<<<(n + 255) / 256, 256, 0, stream>>>(n, tex, c, out, err);
 }
 
 void launch_debug_occluded(int n, const float* o, const float* d, const float* tmax, int* occ, uint32_t* errors,

@@ -151,7 +151,7 @@ struct WaveOptions {
   bool volumes = false;        // volume scattering kernels
   bool sort_hits = true;       // shade hits listed by shading bucket
   bool defer_shadows = false;  // queue surface shadow rays for k_connect (ignored with volumes)
-  uint32_t features = kFeatAll;  // scene features of the batch (kFeatSpheres | kFeatGrids)
+  uint32_t features = kFeatAll;  // scene features of the batch (kFeatSpheres | kFeatGrids | kFeatTextures)
   ShadowQueue shadow_queue{};
   bool adjoint = false;        // path-replay adjoint pass (no deferral)
   float* grads = nullptr;      // adjoint: dLoss/dParam, kGradParams per material
@@ -167,6 +167,7 @@ void prepare_persistent_grids();
 void launch_accumulate(const float4* noise, float4* acc, uint32_t n, int frame_index, cudaStream_t stream);
 // Density of texture node `tex` at object-space points (3 floats each), scene slot 0.
 void launch_debug_density(int n, uint32_t tex, const float* p, float* out, uint32_t* err, cudaStream_t stream);
+void launch_debug_texture(int n, uint32_t tex, const float* c, float* out, uint32_t* err, cudaStream_t stream);
 void launch_debug_trace(int n, const float* o, const float* d, const uint32_t* lh, uint32_t* inst, uint32_t* tri,
                         float* t, float* bary, int* back, int* nearby, uint32_t* errors, cudaStream_t stream);
 void launch_debug_occluded(int n, const float* o, const float* d, const float* tmax, int* occ, uint32_t* errors,

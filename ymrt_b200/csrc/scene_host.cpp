@@ -677,6 +677,11 @@ int load_ymtmp(const std::string& path, HostScene* scene, std::string* error) {
     std::string name;
     std::unordered_map<std::string, std::string> attrs;
     for (size_t k = i + 1; k < j; ++k) {
+      // is_valid_statement (src/core/YMParser.cpp:680-720): attribute names
+      // are letters and '_' only (so NoiseTextureWave's freq_0 .. layer_count_1
+      // can never be given in a file)
+      for (char c : stmts[k].left)
+        if (!(std::isalpha((unsigned char)c) || c == '_')) return bad(stmts[k], "illegal statement " + stmts[k].left);
       if (stmts[k].left == "name") name = unquote(stmts[k].right);
       else attrs[stmts[k].left] = stmts[k].right;
     }
@@ -820,10 +825,19 @@ int load_ymtmp(const std::string& path, HostScene* scene, std::string* error) {
       mat.light_mtl.intensity = gmax(get_f("intensity", 1.0f), 0.0f);
       names[name] = (uint32_t)scene->materials.size();
       scene->materials.push_back(mat);
-    } else if (type == "ConstantTextureFloat" || type == "ConstantTextureRgb" || type == "NoiseTextureFBM") {
+    } else if (type == "ConstantTextureFloat" || type == "ConstantTextureRgb" || type == "CheckerBoardTexture" ||
+               type == "NoiseTexture" || type == "NoiseTextureFBM" || type == "NoiseTextureTurbulence" ||
+               type == "NoiseTextureMarble" || type == "NoiseTextureWood" || type == "NoiseTexturePolkaDot" ||
+               type == "NoiseTextureWave") {
+      // read_*_texture_attributes (src/core/YMParser.cpp:1560-2118): the
+      // readers' defaults and clamps. Attributes a reader has no case for
+      // are dropped (the fBm, turbulence and marble readers have none for
+      // "lacunarity", so theirs stays 2).
       Texture tex;
       std::memset(&tex, 0, sizeof(tex));
       tex.child[0] = tex.child[1] = kEmpty;
+      auto get_i = [&](const char* k, int def) { return attrs.count(k) ? std::stoi(attrs[k]) : def; };
+      auto get_b = [&](const char* k, bool def) { return attrs.count(k) ? attrs[k] == "true" : def; };
       if (type == "ConstantTextureFloat") {
         tex.type = kTexConstFloat;
         tex.value = get_f("value", 0.0f);
@@ -831,25 +845,58 @@ int load_ymtmp(const std::string& path, HostScene* scene, std::string* error) {
         tex.type = kTexConstRgb;
         tex.color = get_v("color", vec3(0.0f));
       } else {
-        tex.type = kTexFbm;
         if ((rc = get_ref("texture_black_idx", &tex.child[0])) || (rc = get_ref("texture_white_idx", &tex.child[1])))
           return rc;
-        if (tex.child[0] == kEmpty || tex.child[1] == kEmpty) return bad(open, "fbm texture requires black and white inputs");
-        tex.frequency = gmax(0.001f, get_f("frequency", 16.0f));
-        // The reference's reader has no case for "lacunarity" (the attribute is
-        // accepted and dropped, src/core/YMParser.cpp:1741-1780), so it is always 2.
-        tex.lacunarity = 2.0f;
-        tex.gain = get_f("gain", 0.5f);
-        tex.layer_count = attrs.count("layer_count") ? std::stoi(attrs["layer_count"]) : 4;
-        tex.amplitude = get_f("amplitude", 1.0f);
-        tex.offset = get_f("offset", 0.0f);
+        if (tex.child[0] == kEmpty || tex.child[1] == kEmpty) return bad(open, type + " requires black and white inputs");
+        if (type == "CheckerBoardTexture") {
+          tex.type = kTexChecker;
+          tex.frequency = gmax(get_f("frequency", 4.0f), 0.001f);
+        } else if (type == "NoiseTexture") {
+          tex.type = kTexNoise;
+          tex.frequency = gmax(get_f("frequency", 1.0f), 0.001f);
+          tex.flags = get_b("normalized", true) ? kTexNormalized : 0u;
+        } else if (type == "NoiseTextureFBM" || type == "NoiseTextureTurbulence") {
+          tex.type = type == "NoiseTextureFBM" ? kTexFbm : kTexTurbulence;
+          tex.frequency = gmax(0.001f, get_f("frequency", 16.0f));
+          tex.lacunarity = 2.0f;
+          tex.gain = get_f("gain", 0.5f);
+          tex.layer_count = get_i("layer_count", 4);
+          tex.amplitude = get_f("amplitude", 1.0f);
+          tex.offset = get_f("offset", 0.0f);
+        } else if (type == "NoiseTextureMarble") {
+          tex.type = kTexMarble;
+          tex.frequency = get_f("frequency", 16.0f);
+          tex.lacunarity = 2.0f;
+          tex.gain = get_f("gain", 0.5f);
+          tex.layer_count = get_i("layer_count", 4);
+          tex.variation = get_f("variation", 10.0f);
+          tex.flags = (get_b("x_turb", true) ? kTexTurbX : 0u) | (get_b("y_turb", true) ? kTexTurbY : 0u) |
+                      (get_b("z_turb", true) ? kTexTurbZ : 0u);
+        } else if (type == "NoiseTextureWood") {
+          tex.type = kTexWood;
+          tex.frequency = gmax(0.001f, get_f("frequency", 2.0f));
+          tex.variation = get_f("variation", 10.0f);
+        } else if (type == "NoiseTexturePolkaDot") {
+          tex.type = kTexPolkaDot;
+          tex.frequency = get_f("frequency", 8.0f);
+          tex.radius = get_f("radius", 0.35f);
+        } else {
+          // the reader's defaults (its numbered attributes are illegal statements)
+          tex.type = kTexWave;
+          tex.frequency = 0.1f;
+          tex.lacunarity = 2.0f;
+          tex.gain = 0.5f;
+          tex.layer_count = 2;
+          tex.frequency1 = 2.0f;
+          tex.lacunarity1 = 2.0f;
+          tex.gain1 = 0.5f;
+          tex.layer_count1 = 4;
+        }
       }
       names[name] = (uint32_t)scene->textures.size();
       scene->textures.push_back(tex);
-    } else if (type == "ImageTexture" || type == "CheckerBoardTexture" || type == "NoiseTexture" ||
-               type == "NoiseTextureTurbulence" || type == "NoiseTextureMarble" || type == "NoiseTextureWood" ||
-               type == "NoiseTexturePolkaDot" || type == "NoiseTextureWave") {
-      return fail(YMRT_ERR_UNSUPPORTED, type + " textures are not supported (constant and fBm textures are)");
+    } else if (type == "ImageTexture") {
+      return fail(YMRT_ERR_UNSUPPORTED, "image textures are not supported (constant and solid textures are)");
     } else if (type == "DistantLight") {
       DistantLight dl{};
       dl.light_color = vmax(get_v("light_color", vec3(1.0f)), vec3(0.0f));
@@ -884,6 +931,129 @@ int load_ymtmp(const std::string& path, HostScene* scene, std::string* error) {
     if (inst.inner_volume_idx != -1 && (uint32_t)inst.inner_volume_idx >= scene->volumes.size())
       return fail(YMRT_ERR_FORMAT, "instance refers to an unknown volume");
   }
+  std::string why;
+  if (const int rc = check_textures(*scene, YMRT_ERR_FORMAT, &why)) return fail(rc, why);
+  return YMRT_OK;
+}
+
+// ------------------------------------------------------- texture nodes ---
+
+void texture_words(const Texture& t, uint32_t r[kTextureWords]) {
+  for (int k = 0; k < kTextureWords; ++k) r[k] = 0;
+  r[0] = t.type;
+  r[1] = t.child[0];
+  r[2] = t.child[1];
+  r[3] = f2u(t.value);
+  r[4] = f2u(t.color.x);
+  r[5] = f2u(t.color.y);
+  r[6] = f2u(t.color.z);
+  r[7] = f2u(t.frequency);
+  r[8] = f2u(t.lacunarity);
+  r[9] = f2u(t.gain);
+  r[10] = (uint32_t)t.layer_count;
+  r[11] = f2u(t.amplitude);
+  r[12] = f2u(t.offset);
+  r[13] = f2u(t.variation);
+  r[14] = f2u(t.radius);
+  r[15] = t.flags;
+  r[16] = f2u(t.frequency1);
+  r[17] = f2u(t.lacunarity1);
+  r[18] = f2u(t.gain1);
+  r[19] = (uint32_t)t.layer_count1;
+  if (t.type == kTexGrid) {  // the lattice is not part of the node's words
+    r[1] = r[2] = kEmpty;
+  }
+}
+
+int texture_from_desc(const ymrt_texture_desc& d, Texture* t, std::string* error) {
+  std::memset(t, 0, sizeof(*t));
+  t->type = d.type;
+  t->child[0] = t->child[1] = kEmpty;
+  if (d.type == kTexConstFloat) {
+    t->value = d.value;
+    return YMRT_OK;
+  }
+  if (d.type == kTexConstRgb) {
+    t->color = vec3(d.color[0], d.color[1], d.color[2]);
+    return YMRT_OK;
+  }
+  if (d.type < kTexChecker || d.type > kTexWave) {
+    if (error) *error = "node type " + std::to_string(d.type) + " is not supported (constant and solid nodes are)";
+    return YMRT_ERR_UNSUPPORTED;
+  }
+  t->child[0] = d.black;
+  t->child[1] = d.white;
+  t->frequency = d.frequency;
+  t->lacunarity = d.lacunarity;
+  t->gain = d.gain;
+  t->layer_count = d.layer_count;
+  t->amplitude = d.amplitude;
+  t->offset = d.offset;
+  t->variation = d.variation;
+  t->radius = d.radius;
+  t->flags = d.flags & (kTexNormalized | kTexTurbX | kTexTurbY | kTexTurbZ);
+  t->frequency1 = d.frequency1;
+  t->lacunarity1 = d.lacunarity1;
+  t->gain1 = d.gain1;
+  t->layer_count1 = d.layer_count1;
+  return YMRT_OK;
+}
+
+int check_textures(const HostScene& s, int code, std::string* error) {
+  const size_t n = s.textures.size();
+  auto fail = [&](const std::string& msg) {
+    if (error) *error = msg;
+    return code;
+  };
+  for (size_t k = 0; k < n; ++k) {
+    const Texture& t = s.textures[k];
+    if (t.type < kTexChecker || t.type > kTexWave) continue;
+    if (t.child[0] >= n || t.child[1] >= n)
+      return fail("texture " + std::to_string(k) + " requires black and white inputs");
+  }
+  // longest path (in nodes) from each node; 0 = not yet visited, -1 = on the path
+  std::vector<int> depth(n, 0);
+  std::function<int(uint32_t)> walk = [&](uint32_t k) -> int {
+    if (depth[k] > 0) return depth[k];
+    if (depth[k] < 0) return -1;
+    depth[k] = -1;
+    int d = 1;
+    const Texture& t = s.textures[k];
+    if (t.type >= kTexChecker && t.type <= kTexWave)
+      for (int c = 0; c < 2; ++c) {
+        const int dc = walk(t.child[c]);
+        if (dc < 0) return -1;
+        d = std::max(d, dc + 1);
+      }
+    depth[k] = d;
+    return d;
+  };
+  // the graphs the renderer evaluates: from material references and media densities
+  auto root = [&](uint32_t k) -> int {
+    const int d = walk(k);
+    if (d < 0) return fail("the texture graph has a cycle through node " + std::to_string(k));
+    if (d > kTextureStack)
+      return fail("texture " + std::to_string(k) + " is " + std::to_string(d) + " nodes deep (at most " +
+                  std::to_string(kTextureStack) + " are evaluated)");
+    return YMRT_OK;
+  };
+  for (size_t m = 0; m < s.materials.size(); ++m) {
+    const Material& mat = s.materials[m];
+    if (mat.material_type != kDefaultMtl) continue;
+    const DefaultMtl& d = mat.default_mtl;
+    const uint32_t refs[] = {d.diffuse_albedo_tex, d.alpha_x_tex, d.specular_albedo_tex, d.alpha_y_tex,
+                             d.specular_weight_tex, d.metalness_tex, d.transmission_weight_tex, d.normal_mapping_tex,
+                             d.bump_mapping_tex, d.coat_albedo_tex, d.coat_weight_tex, d.coat_thickness_tex,
+                             d.coat_roughness_x_tex, d.coat_roughness_y_tex};
+    for (uint32_t r : refs) {
+      if (r == kEmpty) continue;
+      if (r >= n) return fail("material " + std::to_string(m) + " refers to an unknown texture");
+      if (const int rc = root(r)) return rc;
+    }
+  }
+  for (const Volume& v : s.volumes)
+    if (v.density_texture_idx >= 0 && (size_t)v.density_texture_idx < n)
+      if (const int rc = root((uint32_t)v.density_texture_idx)) return rc;
   return YMRT_OK;
 }
 
@@ -943,30 +1113,10 @@ int load_arrays(const ymrt_scene_desc* d, HostScene* scene, std::string* error) 
   // textures
   if (d->texture_count > 0 && !d->textures) return fail(YMRT_ERR_INVALID, "textures missing");
   for (uint32_t k = 0; k < d->texture_count; ++k) {
-    const ymrt_texture_desc& td = d->textures[k];
     Texture tex;
-    std::memset(&tex, 0, sizeof(tex));
-    tex.child[0] = tex.child[1] = kEmpty;
-    tex.type = td.type;
-    if (td.type == kTexConstFloat) {
-      tex.value = td.value;
-    } else if (td.type == kTexConstRgb) {
-      tex.color = vec3(td.color[0], td.color[1], td.color[2]);
-    } else if (td.type == kTexFbm) {
-      if (td.black >= d->texture_count || td.white >= d->texture_count)
-        return fail(YMRT_ERR_INVALID, "fbm texture requires black and white inputs");
-      tex.child[0] = td.black;
-      tex.child[1] = td.white;
-      tex.frequency = gmax(0.001f, td.frequency);
-      tex.lacunarity = td.lacunarity;
-      tex.gain = td.gain;
-      tex.layer_count = td.layer_count;
-      tex.amplitude = td.amplitude;
-      tex.offset = td.offset;
-    } else {
-      return fail(YMRT_ERR_UNSUPPORTED, "texture type " + std::to_string(td.type) +
-                                            " is not supported (constant and fBm textures are)");
-    }
+    std::string why;
+    const int rc = texture_from_desc(d->textures[k], &tex, &why);
+    if (rc) return fail(rc, "texture " + std::to_string(k) + ": " + why);
     scene->textures.push_back(tex);
   }
   // materials, volumes, distant lights: the reference's own layouts
@@ -999,6 +1149,11 @@ int load_arrays(const ymrt_scene_desc* d, HostScene* scene, std::string* error) 
       return fail(YMRT_ERR_INVALID, "instance refers to an unknown asset");
     if (inst.inner_volume_idx != -1 && (uint32_t)inst.inner_volume_idx >= scene->volumes.size())
       return fail(YMRT_ERR_INVALID, "instance refers to an unknown volume");
+  }
+  {
+    std::string why;
+    const int rc = check_textures(*scene, YMRT_ERR_INVALID, &why);
+    if (rc) return fail(rc, why);
   }
   scene->cam_from = vec3(d->camera_from[0], d->camera_from[1], d->camera_from[2]);
   scene->cam_look = vec3(d->camera_look[0], d->camera_look[1], d->camera_look[2]);

@@ -16,6 +16,7 @@
 #include "ymrt_scene.h"
 
 struct ymrt_scene_desc;
+struct ymrt_texture_desc;
 
 namespace ym {
 
@@ -77,6 +78,17 @@ int load_arrays(const ymrt_scene_desc* desc, HostScene* scene, std::string* erro
 // Builds BVHs, orders instances/triangles/lights like the reference, sets up
 // the rendering camera for a width x height image and flattens the arrays.
 int prepare_scene(HostScene* scene, int width, int height, std::string* error);
+
+// Texture nodes in the words of ymrt_texture_desc (include/ymrt.h).
+constexpr int kTextureWords = 20;
+void texture_words(const Texture& t, uint32_t words[kTextureWords]);
+int texture_from_desc(const ymrt_texture_desc& desc, Texture* t, std::string* error);
+
+// Checks the texture graph a scene's materials and media read: indices in
+// range, both inputs of every solid node present, no cycle, and no path of
+// more than kTextureStack nodes (the evaluation stack). Returns 0 or
+// `code` with a message.
+int check_textures(const HostScene& scene, int code, std::string* error);
 
 // glm-order transform helpers (exposed for tests through the C-ABI).
 mat4 compose_transform(vec3 translate, vec3 scale, vec3 rotate_deg);

@@ -45,6 +45,8 @@ YM_HD float gclamp(float x, float lo, float hi) { return gmin(gmax(x, lo), hi); 
 
 YM_HD float error_gamma(int n) { return (n * kFloatEps) / (1.0f - n * kFloatEps); }
 
+YM_HD float sqr(float x) { return x * x; }
+
 YM_HD float safe_rcp(float f) { return fabsf(f) < 1E-30f ? (f > 0.0f ? 1E30f : -1E30f) : (1.0f / f); }
 
 YM_HD uint32_t f2u(float f) {

@@ -126,8 +126,10 @@ struct RenderSetting {
 };
 static_assert(sizeof(RenderSetting) == 40, "RenderSetting layout");
 
-// Texture subset used on the hot path: constants and the fBm noise node
-// (src/Texture.h:168-690 holds the full union). Children are texture indices.
+// Texture nodes (src/Texture.h:16-28, 168-690): constants and the solid
+// (procedural) nodes, each with a black and a white input node whose results
+// it blends or selects. Children are texture indices (kEmpty: absent, reads
+// as black). The image node (type 0) is not supported.
 //
 // kTexGrid is this project's density grid (the reference's texture graph has
 // no grid node; a caller attaches one with ymrt_scene_set_density_grid): an
@@ -140,14 +142,22 @@ enum TextureType : uint32_t {
   kTexTurbulence = 6, kTexMarble = 7, kTexWood = 8, kTexPolkaDot = 9, kTexWave = 10,
   kTexGrid = 64,
 };
+// Texture::flags bits.
+constexpr uint32_t kTexNormalized = 1;  // noise: remapped from [-1, 1] to [0, 1]
+constexpr uint32_t kTexTurbX = 2, kTexTurbY = 4, kTexTurbZ = 8;  // marble: coordinates added to the phase
+constexpr int kTextureStack = 8;         // nodes on one evaluation path (the reference's texture_stack_size)
 struct Texture {
   uint32_t type;
   uint32_t child[2];   // black / white inputs (kEmpty when absent)
   float value;         // constant float (grid: the maximum value)
   vec3 color;          // constant rgb
-  float frequency, lacunarity, gain, amplitude, offset;
+  float frequency, lacunarity, gain, amplitude, offset;  // checker .. wave (wave: its first fBm)
   int layer_count;
-  int normalized;
+  uint32_t flags;      // kTexNormalized, kTexTurb*
+  float variation;     // marble, wood
+  float radius;        // polka dot
+  float frequency1, lacunarity1, gain1;                  // wave: its second fBm
+  int layer_count1;
   int grid_n[3];       // grid: lattice size x, y, z
   int grid_half;       // grid: values are float16 (else float32)
   const void* grid;    // grid: device values, x fastest
@@ -198,10 +208,11 @@ static_assert(sizeof(WideNode) == 80, "WideNode is five 16-byte words");
 constexpr uint32_t kGeoMesh = 0, kGeoSphere = 1;
 
 // Scene features the kernels are specialised on (template argument kF): a
-// batch whose scenes hold no sphere geometry or no density grid runs
+// batch whose scenes hold no sphere geometry, no density grid or no textured
+// surface (and no solid texture node beyond constants and fBm) runs
 // instantiations without that code, so its register allocation is the same
 // as if the feature did not exist.
-constexpr uint32_t kFeatSpheres = 1, kFeatGrids = 2, kFeatAll = 3;
+constexpr uint32_t kFeatSpheres = 1, kFeatGrids = 2, kFeatTextures = 4, kFeatAll = 7;
 
 // Per-geometry tables (offsets into the flattened global arrays). A sphere
 // (kind kGeoSphere) is centred on its object-space origin and has no
@@ -240,6 +251,7 @@ struct DeviceScene {
   const GeometryDesc* geometries;
   uint32_t sphere_count;        // sphere geometries (0: the traversal skips sphere tests)
   uint32_t grid_count;          // density-grid texture nodes
+  uint32_t textured;            // materials read textures, or solid nodes beyond constants and fBm exist
   const WideNode* blas_nodes;
   const float4* wtris;          // 3 per triangle: v0, v1, v2 (w of v0 = triangle id bits)
   const uint32_t* tri_corners;  // 3 per triangle (Triangle id0,id1,id2)

@@ -68,15 +68,19 @@ def halton_permutations(seed: int = 0x594D5254) -> np.ndarray:
 # ---------------------------------------------------------------- meshes ---
 
 class Mesh:
-    """Triangle mesh with one position index and one normal index per corner."""
+    """Triangle mesh with one position index and one normal index per corner
+    (and optionally one texture-coordinate index)."""
 
-    def __init__(self, name, positions, pos_idx, normals, nrm_idx):
+    def __init__(self, name, positions, pos_idx, normals, nrm_idx, uvs=None, uv_idx=None):
         self.name = name
         self.positions = np.asarray(positions, dtype=np.float32).reshape(-1, 3)
         self.pos_idx = np.asarray(pos_idx, dtype=np.uint32).reshape(-1)
         self.normals = np.asarray(normals, dtype=np.float32).reshape(-1, 3)
         self.nrm_idx = np.asarray(nrm_idx, dtype=np.uint32).reshape(-1)
+        self.uvs = None if uvs is None else np.asarray(uvs, dtype=np.float32).reshape(-1, 2)
+        self.uv_idx = None if uv_idx is None else np.asarray(uv_idx, dtype=np.uint32).reshape(-1)
         assert len(self.pos_idx) == len(self.nrm_idx) and len(self.pos_idx) % 3 == 0
+        assert self.uv_idx is None or len(self.uv_idx) == len(self.pos_idx)
 
     @property
     def triangle_count(self) -> int:
@@ -87,6 +91,14 @@ def quad_mesh(name="Geo_Quad") -> Mesh:
     p = [[-0.5, 0, -0.5], [-0.5, 0, 0.5], [0.5, 0, 0.5], [0.5, 0, -0.5]]
     idx = [0, 1, 2, 0, 2, 3]
     return Mesh(name, p, idx, [[0, 1, 0]], [0] * 6)
+
+
+def uv_quad_mesh(name="Geo_UVQuad", repeat=1.0) -> Mesh:
+    """The quad with texture coordinates [0, repeat]^2 over its corners."""
+    p = [[-0.5, 0, -0.5], [-0.5, 0, 0.5], [0.5, 0, 0.5], [0.5, 0, -0.5]]
+    idx = [0, 1, 2, 0, 2, 3]
+    uv = [[0, 0], [0, repeat], [repeat, repeat], [repeat, 0]]
+    return Mesh(name, p, idx, [[0, 1, 0]], [0] * 6, uv, idx)
 
 
 def box_mesh(name="Geo_Box") -> Mesh:
@@ -257,6 +269,9 @@ def write_scene(scene: Scene, path: str) -> str:
         out.append("\tmesh_positions = " + _arr(pos, _f) + ";\n")
         out.append("\tmesh_normal_indices = " + _arr(m.nrm_idx.tolist(), str) + ";\n")
         out.append("\tmesh_normals = " + _arr(nrm, _f) + ";\n")
+        if m.uv_idx is not None:
+            out.append("\tmesh_texcoord_indices = " + _arr(m.uv_idx.tolist(), str) + ";\n")
+            out.append("\tmesh_texcoords = " + _arr(m.uvs.reshape(-1), _f) + ";\n")
         out.append("End(Mesh);\n")
     for name in scene.cubes:
         out.append(f'Begin(Cube);\n\tname = "{name}";\nEnd(Cube);\n')
@@ -274,6 +289,8 @@ def write_scene(scene: Scene, path: str) -> str:
         for k, v in attrs.items():
             if isinstance(v, str):
                 out.append(f'\t{k} = "{v}";\n')
+            elif isinstance(v, (list, tuple, np.ndarray)):
+                out.append(f"\t{k} = {_vec(v)};\n")
             elif isinstance(v, bool):
                 out.append(f"\t{k} = {'true' if v else 'false'};\n")
             elif isinstance(v, int):
@@ -284,7 +301,9 @@ def write_scene(scene: Scene, path: str) -> str:
     for kind, name, attrs in scene.materials:
         out.append(f"Begin({kind});\n\tname = \"{name}\";\n")
         for k, v in attrs.items():
-            if isinstance(v, (list, tuple, np.ndarray)):
+            if isinstance(v, str):  # a texture node's name
+                out.append(f'\t{k} = "{v}";\n')
+            elif isinstance(v, (list, tuple, np.ndarray)):
                 out.append(f"\t{k} = {_vec(v)};\n")
             elif isinstance(v, int):
                 out.append(f"\t{k} = {v};\n")
@@ -496,6 +515,138 @@ def glossy_scene(seed: int = 0) -> Scene:
     return s
 
 
+def _const(s, name, v):
+    if np.ndim(v) == 0:
+        s.textures.append(("ConstantTextureFloat", name, {"value": float(v)}))
+    else:
+        s.textures.append(("ConstantTextureRgb", name, {"color": tuple(float(x) for x in v)}))
+    return name
+
+
+def _solid(s, kind, name, black, white, **attrs):
+    s.textures.append((kind, name, {"texture_black_idx": black, "texture_white_idx": white, **attrs}))
+    return name
+
+
+def textured_scene(seed: int = 0) -> Scene:
+    """The Cornell-like room with every solid texture node of the format on
+    material parameters: a checkerboard floor (albedo, metalness and a bump
+    map, as the reference's own test scene has), a marble back wall with
+    noise-driven roughness, wood and wave side walls, a turbulence box with a
+    normal map from rgb noise, a polka-dot unit cube (texture coordinates of
+    the built-in cube), a coated sphere whose coat weight, thickness, albedo
+    and roughness are textured, a polka-dot sphere (spherical texture
+    coordinates), a textured-transmission glass sphere, a quad with its own
+    texture coordinates and a three-level node graph, and a medium sphere
+    whose density is normalised noise."""
+    rng = np.random.Generator(np.random.PCG64(seed + 77))
+    s = cornell_scene(seed)
+    s.meshes.append(uv_quad_mesh(repeat=3.0))
+    s.cubes = ["Geo_UnitCube"]
+    s.spheres = [("Geo_Sphere", 1.0)]
+    mats = dict((name, i) for i, (_, name, _) in enumerate(s.materials))
+
+    def set_mat(name, attrs):
+        s.materials[mats[name]] = ("DefaultMaterial", name, attrs)
+
+    # floor: checkerboard albedo, metalness and bump (CornellBox_Test's ground)
+    _solid(s, "CheckerBoardTexture", "floor_albedo", _const(s, "floor_dark", (0.1, 0.12, 0.15)),
+           _const(s, "floor_light", (0.8, 0.75, 0.6)), frequency=12.0)
+    _solid(s, "CheckerBoardTexture", "floor_metal", _const(s, "floor_metal_0", 0.0), _const(s, "floor_metal_1", 1.0),
+           frequency=12.0)
+    _solid(s, "CheckerBoardTexture", "floor_bump", _const(s, "floor_bump_0", 0.15), _const(s, "floor_bump_1", 0.35),
+           frequency=40.0)
+    set_mat("floor_material", {"diffuse_albedo": [0.5, 0.5, 0.5], "specular_albedo": [1.0, 1.0, 1.0],
+                               "roughness_x": 0.25, "roughness_y": 0.25, "ior_n": 1.65, "metalness": 0.0,
+                               "specular_weight": 1.0, "transmission_weight": 0.0,
+                               "diffuse_albedo_tex": "floor_albedo", "metalness_tex": "floor_metal",
+                               "bump_mapping_tex": "floor_bump"})
+    # back wall: marble albedo, noise roughness (x and y), specular albedo from fBm
+    _solid(s, "NoiseTextureMarble", "back_marble", _const(s, "marble_vein", (0.25, 0.2, 0.2)),
+           _const(s, "marble_base", (0.9, 0.88, 0.85)), frequency=2.5, gain=0.55, layer_count=5, variation=6.0,
+           x_turb=True, y_turb=False, z_turb=True)
+    _solid(s, "NoiseTexture", "back_rough", _const(s, "rough_lo", 0.1), _const(s, "rough_hi", 0.6), frequency=5.0,
+           normalized=True)
+    _solid(s, "NoiseTextureFBM", "back_spec", _const(s, "spec_lo", (0.6, 0.6, 0.6)), _const(s, "spec_hi", (1, 1, 1)),
+           frequency=3.0, gain=0.5, layer_count=3, amplitude=0.5, offset=0.5)
+    set_mat("back_material", {"diffuse_albedo": [0.5, 0.5, 0.5], "roughness_x": 0.3, "roughness_y": 0.3,
+                              "ior_n": 1.5, "specular_weight": 1.0, "diffuse_albedo_tex": "back_marble",
+                              "alpha_x_tex": "back_rough", "alpha_y_tex": "back_rough",
+                              "specular_albedo_tex": "back_spec"})
+    # side walls: wood and wave albedo
+    _solid(s, "NoiseTextureWood", "left_wood", _const(s, "wood_dark", (0.35, 0.2, 0.1)),
+           _const(s, "wood_light", (0.75, 0.55, 0.3)), frequency=1.5, variation=8.0)
+    set_mat("left_material", {**_lambert((0.5, 0.5, 0.5)), "diffuse_albedo_tex": "left_wood"})
+    # (the reference's parser accepts no wave parameters: attribute names with digits are illegal)
+    _solid(s, "NoiseTextureWave", "right_wave", _const(s, "wave_a", (0.1, 0.3, 0.6)), _const(s, "wave_b", (0.9, 0.8, 0.3)))
+    set_mat("right_material", {**_lambert((0.5, 0.5, 0.5)), "diffuse_albedo_tex": "right_wave"})
+    # tall box: turbulence albedo and a normal map from rgb noise
+    _solid(s, "NoiseTextureTurbulence", "box_turb", _const(s, "turb_a", (0.2, 0.5, 0.3)),
+           _const(s, "turb_b", (0.9, 0.9, 0.7)), frequency=4.0, gain=0.5, layer_count=4, amplitude=1.0, offset=0.0)
+    _solid(s, "NoiseTexture", "box_normal", _const(s, "nrm_a", (0.4, 0.45, 1.0)), _const(s, "nrm_b", (0.6, 0.55, 1.0)),
+           frequency=9.0, normalized=True)
+    set_mat("tall_box_material", {**_lambert((0.5, 0.5, 0.5)), "specular_weight": 0.5, "roughness_x": 0.4,
+                                  "roughness_y": 0.4, "diffuse_albedo_tex": "box_turb",
+                                  "normal_mapping_tex": "box_normal"})
+    # short box: metalness and specular weight from a three-level graph (checker of marble and wood)
+    _solid(s, "NoiseTextureMarble", "graph_marble", _const(s, "g_m0", 0.0), _const(s, "g_m1", 1.0), frequency=4.0)
+    _solid(s, "NoiseTextureWood", "graph_wood", _const(s, "g_w0", 0.2), _const(s, "g_w1", 0.9), frequency=3.0,
+           variation=4.0)
+    _solid(s, "CheckerBoardTexture", "graph_checker", "graph_marble", "graph_wood", frequency=9.0)
+    set_mat("short_box_material", {"diffuse_albedo": [0.7, 0.5, 0.3], "specular_albedo": [1.0, 0.9, 0.8],
+                                   "roughness_x": 0.3, "roughness_y": 0.3, "metalness_tex": "graph_checker",
+                                   "specular_weight_tex": "graph_checker"})
+    # the built-in cube: polka dots over its texture coordinates
+    _solid(s, "NoiseTexturePolkaDot", "cube_dots", _const(s, "dots_bg", (0.85, 0.85, 0.8)),
+           _const(s, "dots_fg", (0.7, 0.1, 0.1)), frequency=4.0, radius=0.3)
+    s.transforms.append(("cube_transform", (0.55, 0.1, -0.55), (0.3, 0.3, 0.3), (20.0, 30.0, 0.0)))
+    s.materials.append(("DefaultMaterial", "cube_material", {**_lambert((0.5, 0.5, 0.5)),
+                                                             "diffuse_albedo_tex": "cube_dots"}))
+    s.instances.append(("cube", "Geo_UnitCube", "cube_transform", "cube_material", None, False))
+    # a quad with its own texture coordinates (3x repeat): polka dots and checker coat on the ceiling side
+    _solid(s, "NoiseTexturePolkaDot", "quad_dots", _const(s, "qd_bg", (0.2, 0.6, 0.3)), _const(s, "qd_fg", (0.9, 0.9, 0.2)),
+           frequency=2.0, radius=0.2)
+    s.transforms.append(("uvquad_transform", (-0.6, 0.3, -0.8), (0.6, 1.0, 0.6), (70.0, 25.0, 0.0)))
+    s.materials.append(("DefaultMaterial", "uvquad_material", {**_lambert((0.5, 0.5, 0.5)),
+                                                               "diffuse_albedo_tex": "quad_dots"}))
+    s.instances.append(("uvquad", "Geo_UVQuad", "uvquad_transform", "uvquad_material", None, False))
+    # coated sphere: coat weight, thickness, albedo and roughness textured
+    _solid(s, "CheckerBoardTexture", "coat_w", _const(s, "coat_w0", 0.2), _const(s, "coat_w1", 1.0), frequency=10.0)
+    _solid(s, "NoiseTexture", "coat_t", _const(s, "coat_t0", 0.5), _const(s, "coat_t1", 2.0), frequency=3.0)
+    _solid(s, "NoiseTextureFBM", "coat_a", _const(s, "coat_a0", (0.9, 0.5, 0.3)), _const(s, "coat_a1", (0.4, 0.6, 0.9)),
+           frequency=2.0, gain=0.5, layer_count=2)
+    _solid(s, "NoiseTexture", "coat_r", _const(s, "coat_r0", 0.05), _const(s, "coat_r1", 0.4), frequency=6.0,
+           normalized=False)
+    s.transforms.append(("coated_transform", (-0.1, -0.75, 0.45), (0.25, 0.25, 0.25), (0.0, 40.0, 0.0)))
+    s.materials.append(("DefaultMaterial", "coated_material", {
+        "diffuse_albedo": list(rng.uniform(0.3, 0.8, 3)), "roughness_x": 0.5, "roughness_y": 0.5, "ior_n": 1.5,
+        "specular_weight": 0.0, "coat_ior": 1.6, "coat_weight_tex": "coat_w", "coat_thickness_tex": "coat_t",
+        "coat_albedo_tex": "coat_a", "coat_roughness_x_tex": "coat_r", "coat_roughness_y_tex": "coat_r"}))
+    s.instances.append(("coated_sphere", "Geo_Sphere", "coated_transform", "coated_material", None, False))
+    # polka-dot sphere (texture coordinates from the sphere's angles)
+    _solid(s, "NoiseTexturePolkaDot", "sphere_dots", _const(s, "sd_bg", (0.9, 0.9, 0.9)), _const(s, "sd_fg", (0.1, 0.2, 0.7)),
+           frequency=6.0, radius=0.25)
+    s.transforms.append(("dots_transform", (0.45, 0.55, 0.3), (0.2, 0.2, 0.2), (30.0, 0.0, 0.0)))
+    s.materials.append(("DefaultMaterial", "dots_material", {**_lambert((0.5, 0.5, 0.5)),
+                                                             "diffuse_albedo_tex": "sphere_dots"}))
+    s.instances.append(("dots_sphere", "Geo_Sphere", "dots_transform", "dots_material", None, False))
+    # glass sphere with textured transmission weight
+    _solid(s, "CheckerBoardTexture", "glass_tw", _const(s, "glass_tw0", 0.3), _const(s, "glass_tw1", 1.0), frequency=8.0)
+    s.transforms.append(("glass_transform", (0.35, -0.8, 0.55), (0.18, 0.18, 0.18), (0, 0, 0)))
+    s.materials.append(("DefaultMaterial", "glass_material", {
+        "diffuse_albedo": [0.6, 0.6, 0.6], "specular_albedo": [1.0, 1.0, 1.0], "roughness_x": 0.05,
+        "roughness_y": 0.05, "ior_n": 1.5, "metalness": 0.0, "specular_weight": 1.0,
+        "transmission_weight_tex": "glass_tw"}))
+    s.instances.append(("glass_sphere", "Geo_Sphere", "glass_transform", "glass_material", None, False))
+    # a medium sphere with normalised-noise density
+    _solid(s, "NoiseTexture", "haze_density", _const(s, "haze_0", 0.0), _const(s, "haze_1", 1.0), frequency=3.0)
+    s.transforms.append(("haze_transform", (-0.45, 0.45, 0.2), (0.35, 0.35, 0.35), (0, 0, 0)))
+    s.volumes.append(("haze_volume", "haze_transform", (2.0, 2.0, 2.0), (0.8, 0.8, 0.8), 0.2, "haze_density"))
+    s.materials.append(("DefaultMaterial", "haze_boundary_material", {"ior_n": 1.0}))
+    s.instances.append(("haze", "Geo_Sphere", "haze_transform", "haze_boundary_material", "haze_volume", True))
+    return s
+
+
 def orbit_view(name: str, seed: int, k: int, n: int):
     """The k-th of n cameras (from, look, fov) on a 90-degree arc around the
     scene's look-at point, at the original camera's height and distance and
@@ -514,6 +665,7 @@ SCENES = {
     "instanced": instanced_scene,
     "instanced_fog": instanced_fog_scene,
     "spheres": spheres_scene,
+    "textured": textured_scene,
     "volumetric": volumetric_scene,
     "volumetric_const": volumetric_const_scene,
 }
