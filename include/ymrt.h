@@ -183,7 +183,12 @@ typedef struct ymrt_mesh_desc {
  *           flags bits 1-3 (x, y, z coordinate added to the phase);
  *   wood: frequency, variation;  polka dot: frequency, radius;
  *   wave: frequency, lacunarity, gain, layer_count (first fBm),
- *         frequency1, lacunarity1, gain1, layer_count1 (second fBm). */
+ *         frequency1, lacunarity1, gain1, layer_count1 (second fBm);
+ *   image (type 0; ImageTexture, src/Texture.h:84-166): words 3-6 are
+ *         int32 width, height, channels (1-4), wrap (0 repeat, 1 clamp);
+ *         words 7-10 float scale_u, scale_v, offset_u, offset_v; word 15 the
+ *         colour space its pixels were decoded from (0 sRGB, 1 linear). Its
+ *         pixels are given with ymrt_host_scene_set_image. */
 typedef struct ymrt_texture_desc {
   uint32_t type;
   uint32_t black, white;
@@ -237,6 +242,7 @@ int ymrt_scene_from_arrays(const ymrt_scene_desc* desc, int width, int height, c
 #define YMRT_QUERY_TEXTURES 10   /* uint32[20*n]: ymrt_texture_desc words per node */
 #define YMRT_QUERY_GEOMETRIES 11 /* uint32[2*n]: kind (0 triangle mesh, 1 sphere), sphere radius (float bits) */
 #define YMRT_QUERY_MESH_CORNERS 12 /* float[8*c] of mesh `index`, by corner: position, normal, uv (0 without texcoords) */
+#define YMRT_QUERY_IMAGE_PIXELS 13 /* float[w*h*channels] of image node `index`: linear samples, bottom row first */
 long long ymrt_host_scene_query(const ymrt_host_scene* scene, int what, int index, void* out, size_t cap);
 
 /* Uploads a prepared scene. halton_perm: the concatenated digit permutations
@@ -364,6 +370,22 @@ int ymrt_debug_trace(ymrt_scene* scene, int n, const float* origin, const float*
  * each; host buffers), as the media read it: known-answer checks of grid and
  * fBm nodes. */
 int ymrt_debug_density(ymrt_scene* scene, uint32_t texture_index, int n, const float* points, float* out);
+/* The shading frame at n given hits (instance, triangle, barycentrics (3),
+ * back flag, ray direction (3); host buffers): out 22 floats per hit --
+ * normal, tangent, bitangent, texture footprint du/dx dv/dx du/dy dv/dy, uv,
+ * object-space position, dp/du, material index -- as the shade stage builds
+ * it (FetchShadingData, Camera::TextureCoordinatesDifferential,
+ * MaterialBSDF::InitShadingSpace): a known-answer check of normal and bump
+ * mapping. */
+int ymrt_debug_frame(ymrt_scene* scene, int n, const uint32_t* inst, const uint32_t* tri, const float* bary,
+                     const int* back, const float* dir, float* out);
+
+/* Pixels of image node `texture_index` of a host scene (from
+ * ymrt_scene_from_arrays, or replacing a loaded image): count =
+ * width * height * channels linear floats, channels interleaved, bottom row
+ * first (the layout the reference's loader produces, src/FileIO.cpp:77-172). */
+int ymrt_host_scene_set_image(ymrt_host_scene* scene, uint32_t texture_index, const float* pixels, size_t count);
+
 /* Value (rgb) of texture node `texture_index` as a surface reads it, at n
  * points of 5 floats each: texture coordinates s, t and the object-space
  * position x, y, z (host buffers): known-answer checks of every node type. */

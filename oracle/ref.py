@@ -56,6 +56,9 @@ def _bind(L, settings_type):
     L.ymref_camera_bytes.argtypes = [vp, vp, i]
     L.ymref_scene_records.argtypes = [vp, i, vp, i]
     L.ymref_texture_eval.argtypes = [vp, ctypes.c_uint32, i, vp, vp]
+    L.ymref_shading_frame.argtypes = [vp, i, vp, vp, vp, vp, vp, vp]
+    L.ymref_image_pixels.restype = ctypes.c_longlong
+    L.ymref_image_pixels.argtypes = [vp, ctypes.c_uint32, vp, ctypes.c_longlong]
     L.ymref_bvh_depths.argtypes = [vp, vp]
     L.ymref_sobol_matrices.restype = ctypes.c_size_t
     L.ymref_sobol_matrices.argtypes = [vp, ctypes.c_size_t]
@@ -216,6 +219,28 @@ class RefScene:
         if n > 0:
             self._L.ymref_scene_records(self.h, what, _p(out), out.size)
         return out.reshape(-1, width)
+
+    def shading_frame(self, inst, tri, bary, back, dirs) -> np.ndarray:
+        """The reference's shading frame at given hits: (n, 22) floats (normal,
+        tangent, bitangent, texture footprint du/dx dv/dx du/dy dv/dy, uv,
+        object-space position, dp/du, material index)."""
+        n = len(inst)
+        out = np.zeros((n, 22), self._f)
+        self._L.ymref_shading_frame(self.h, n, _p(np.ascontiguousarray(inst, np.uint32)),
+                                    _p(np.ascontiguousarray(tri, np.uint32)), _p(np.ascontiguousarray(bary, self._f)),
+                                    _p(np.ascontiguousarray(back, np.int32)), _p(np.ascontiguousarray(dirs, self._f)),
+                                    _p(out))
+        return out
+
+    def image_pixels(self, tex: int) -> np.ndarray:
+        """Pixels of image node `tex` as the reference loaded them (linear
+        samples, bottom row first, channels interleaved), flat."""
+        n = self._L.ymref_image_pixels(self.h, tex, None, 0)
+        if n < 0:
+            raise ValueError("not an image node")
+        out = np.zeros(n, self._f)
+        self._L.ymref_image_pixels(self.h, tex, _p(out), n)
+        return out
 
     def texture(self, tex: int, st, points) -> np.ndarray:
         """The reference's TextureEval of node `tex` at texture coordinates

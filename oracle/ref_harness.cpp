@@ -318,6 +318,14 @@ int ymref_scene_records(void* handle, int what, uint32_t* out, int cap) {
           r[7] = f(freq); r[8] = f(lac); r[9] = f(gain); r[10] = (uint32_t)layers;
         };
         switch (t.texture_type) {
+          case IMAGE_TEXTURE: {
+            const auto& im = t.image_texture;
+            r[3] = (uint32_t)im.width; r[4] = (uint32_t)im.height; r[5] = (uint32_t)im.channel_count;
+            r[6] = (uint32_t)im.warp_mode;
+            r[7] = f(im.scale_u); r[8] = f(im.scale_v); r[9] = f(im.offset_u); r[10] = f(im.offset_v);
+            r[15] = (uint32_t)im.color_space;
+            break;
+          }
           case CONSTANT_TEXTURE_FLOAT: r[3] = f(t.constant_texture_float.value); break;
           case CONSTANT_TEXTURE_RGB:
             r[4] = f(t.constant_texture_rgb.color.x); r[5] = f(t.constant_texture_rgb.color.y);
@@ -370,6 +378,28 @@ int ymref_scene_records(void* handle, int what, uint32_t* out, int cap) {
   return (int)w.size();
 }
 
+// Pixels of image node `tex` as the reference holds them (32x32 tiles,
+// src/FileIO.cpp:126-171), reassembled into rows (bottom row first, as
+// loaded): width * height * channels floats. Returns the count, or -1.
+long long ymref_image_pixels(void* handle, uint32_t tex, float* out, long long cap) {
+  auto ctx = static_cast<RefContext*>(handle);
+  const auto& textures = GuiModule::Textures(*ctx->module);
+  if (tex >= textures.size() || textures[tex].texture_type != IMAGE_TEXTURE) return -1;
+  const ImageTexture& im = textures[tex].image_texture;
+  const long long n = (long long)im.width * im.height * im.channel_count;
+  if (!out || cap < n) return n;
+  const auto& tiles = GuiModule::ImageTiles(*ctx->module);
+  const int tiles_x = (im.width + TEX_TILE_RES_X - 1) / TEX_TILE_RES_X;
+  for (int y = 0; y < im.height; ++y)
+    for (int x = 0; x < im.width; ++x) {
+      const ImageTile& tile = tiles[im.tile_offset + (y / TEX_TILE_RES_Y) * tiles_x + x / TEX_TILE_RES_X];
+      const float* d = static_cast<const float*>(tile.host_data) +
+                       ((y % TEX_TILE_RES_Y) * TEX_TILE_RES_X + x % TEX_TILE_RES_X) * im.channel_count;
+      for (int c = 0; c < im.channel_count; ++c) out[((long long)y * im.width + x) * im.channel_count + c] = d[c];
+    }
+  return n;
+}
+
 // TextureEval (src/TextureEval.cuh:419-481) of texture node `tex` at n
 // points of 5 floats (texture coordinates s, t, object-space x, y, z; the
 // world position is set to the object position, which no procedural node
@@ -379,6 +409,7 @@ int ymref_texture_eval(void* handle, uint32_t tex, int n, const float* coords, f
   const auto& textures = GuiModule::Textures(*ctx->module);
   if (tex >= textures.size()) return -1;
   ImageTileCache cache;
+  cache.image_tiles_host = GuiModule::ImageTiles(*ctx->module).data();
   for (int i = 0; i < n; ++i) {
     const float* c = coords + 5 * (size_t)i;
     const glm::vec3 p(c[2], c[3], c[4]);
@@ -470,6 +501,47 @@ int ymref_trace(void* handle, int n, const float* origin, const float* dir, cons
     bary[3 * i + 2] = rec.hit_barycentric.z;
     back[i] = rec.hit_back;
     nearby[i] = nearby_count;
+  }
+  return 0;
+}
+
+// The shading frame the reference's shade stage builds at a hit
+// (src/Shading.cu:2128-2188: FetchShadingData, the pixel's texture-coordinate
+// footprint, MaterialBSDF::InitShadingSpace with normal / bump maps). Per
+// hit: instance, triangle, barycentrics (3), back flag and ray direction (3)
+// in; out 22 floats: normal, tangent, bitangent (9), du/dx, dv/dx, du/dy,
+// dv/dy (4), uv (2), object-space position (3), shading dp/du (3) and the
+// hit's material index as a float (1).
+int ymref_shading_frame(void* handle, int n, const uint32_t* inst, const uint32_t* tri, const float* bary,
+                        const int* back, const float* dir, float* out) {
+  auto ctx = static_cast<RefContext*>(handle);
+  const Scene& scene = ctx->scene;
+  ImageTileCache cache;
+  cache.image_tiles_host = GuiModule::ImageTiles(*ctx->module).data();
+  for (int i = 0; i < n; ++i) {
+    float* o = out + 22 * (size_t)i;
+    for (int k = 0; k < 22; ++k) o[k] = 0.0f;
+    HitRecord rec;
+    rec.hit_instance_idx = inst[i];
+    rec.hit_triangle_idx = tri[i];
+    rec.hit_barycentric = glm::vec3(bary[3 * i], bary[3 * i + 1], bary[3 * i + 2]);
+    rec.hit_back = back[i];
+    Ray ray(glm::vec3(0.0f), glm::vec3(dir[3 * i], dir[3 * i + 1], dir[3 * i + 2]));
+    glm::vec3 p(0.0f), perr(0.0f), pobj(0.0f), ns(0.0f), ng(0.0f), dpdu(0.0f), dpdv(0.0f);
+    glm::vec2 uv(0.0f);
+    FetchShadingData(scene, rec, &p, &perr, &pobj, &ns, &ng, &uv, &dpdu, &dpdv);
+    const glm::vec4 d = scene.camera->TextureCoordinatesDifferential(ray, p, ns, ng, dpdu, dpdv, ctx->width,
+                                                                     ctx->height, 0.25f, 0.25f);
+    const auto& prim = scene.primitive_instances[rec.hit_instance_idx];
+    const auto& material = scene.materials[prim.material_idx];
+    MaterialBSDF bsdf;
+    const TextureCoordinate tc(uv, p, pobj, d);
+    bsdf.InitShadingSpace(material, rec.hit_back, ray, ng, ns, dpdu, dpdv, scene.transforms[prim.transform_idx],
+                          scene.i_transforms[prim.transform_idx], scene.textures, cache, tc);
+    const float v[22] = {bsdf.normal.x, bsdf.normal.y, bsdf.normal.z, bsdf.tangent.x, bsdf.tangent.y,
+                         bsdf.tangent.z, bsdf.bitangent.x, bsdf.bitangent.y, bsdf.bitangent.z, d.x, d.y, d.z, d.w,
+                         uv.x, uv.y, pobj.x, pobj.y, pobj.z, dpdu.x, dpdu.y, dpdu.z, (float)prim.material_idx};
+    for (int k = 0; k < 22; ++k) o[k] = v[k];
   }
   return 0;
 }

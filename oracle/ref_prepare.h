@@ -29,6 +29,9 @@ class GuiModule {
 
     m.permute_table.assign(halton_perm, halton_perm + perm_len);
 
+    // the image tiles the host-side texture fetch reads (GuiModule::UpdateScene, src/core/GuiModule.cpp:237)
+    m.image_tile_cache.image_tiles_host = m.image_texture_tiles.data();
+
     m.camera[EDITOR_CAMERA_INDEX].InitCameraRayTransfer(m.GetHostSceneDataPointer());
     std::memcpy(&m.camera[RENDERING_CAMERA_INDEX], &m.camera[EDITOR_CAMERA_INDEX], sizeof(Camera));
     m.camera[RENDERING_CAMERA_INDEX].m_width = width;
@@ -47,6 +50,7 @@ class GuiModule {
   static std::vector<Volume>& Volumes(SceneModule& m) { return m.volumes; }
   static std::vector<DistantLight>& DistantLights(SceneModule& m) { return m.distant_lights; }
   static std::vector<Texture>& Textures(SceneModule& m) { return m.textures; }
+  static std::vector<ImageTile>& ImageTiles(SceneModule& m) { return m.image_texture_tiles; }
   static Camera* Cameras(SceneModule& m) { return m.camera; }
   static std::vector<TopNode>& TopNodes(SceneModule& m) { return m.top_nodes; }
 };

@@ -110,3 +110,91 @@ def test_textured_parameters_get_no_gradient(ctx, textured_path, halton_perm):
     assert g[back, 3] == 0.0
     assert np.any(g[ceiling, :3] != 0.0)
     scene.close()
+
+
+@pytest.fixture(scope="module")
+def imaged(ctx, scene_dir, halton_perm, oracle):
+    from ymrt_b200 import scenes
+    path = scenes.scene_path("imaged", 0, scene_dir)
+    ours = Y.Scene(ctx, Y.HostScene(path, W, H), halton_perm)
+    ref = oracle.RefScene(path, halton_perm, W, H)
+    yield ours, ref, Y.HostScene(path, 16, 16).records("textures")
+    ours.close()
+    ref.close()
+
+
+def test_image_nodes_match_reference(imaged):
+    """Bilinear image fetches (repeat wrap, negative and >1 coordinates,
+    1-4 channels) equal the reference's EvalTexImage bit for bit."""
+    ours, ref, rec = imaged
+    rng = np.random.default_rng(31)
+    n = 20000
+    st = rng.uniform(-3.0, 4.0, (n, 2)).astype(np.float32)
+    p = rng.uniform(-1.0, 1.0, (n, 3)).astype(np.float32)
+    for k in range(rec.shape[0]):
+        a, b = ours.texture(k, st, p), ref.texture(k, st, p)
+        if rec[k, 0] == 3:  # the checkerboard of two images: its selection may flip where the sines' product is ~0
+            assert np.mean(np.any(a != b, axis=1)) <= 1e-4, k
+        else:
+            assert np.array_equal(a.view(np.uint32), b.view(np.uint32)), (k, np.abs(a - b).max())
+
+
+@pytest.mark.parametrize("frame", [1, 2])
+def test_per_sample_radiance_imaged(imaged, oracle, frame):
+    """One-sample frames of the image scene. Its bump map (a 2-bit image
+    differenced over a 0.0005 texture-coordinate step) turns last-place
+    differences of a path's earlier directions (sampling's sinf / cosf on the
+    device against the host's) into larger normal differences, so more
+    pixels pass 1e-5 than in the other scenes, and a few paths take another
+    branch (the frames themselves are pinned bit for bit by
+    test_shading_frames_match_reference): at most 2% of the pixels beyond
+    1e-5 relative, 0.2% beyond 1e-3, and the image means within 2e-4."""
+    ours, ref, _ = imaged
+    s = Y.default_setting(spp=1, ray_depth=8)
+    ref.set_settings(spp=1, ray_depth=8)
+    oracle.query_counts(reset=True)
+    a, stats = ours.render(s, frame)
+    b = ref.render_frame(frame)
+    ext, shadow = oracle.query_counts(reset=True)
+    assert np.array_equal(a[..., 3], b[..., 3])
+    assert a[..., :3].mean() > 0.01
+    bad = _bad(a, b)
+    assert bad.mean() <= 2e-2, f"{bad.sum()} of {bad.size} pixels differ beyond 1e-5 relative"
+    diff = np.abs(a[..., :3] - b[..., :3]) / np.maximum(np.maximum(np.abs(a[..., :3]), np.abs(b[..., :3])), 1e-6)
+    assert np.mean(np.any(diff > 1e-3, axis=-1)) <= 2e-3
+    assert abs(float(a[..., :3].mean()) - float(b[..., :3].mean())) <= 2e-4 * float(b[..., :3].mean())
+    assert stats.device_errors == 0
+    assert abs(int(stats.extension_rays) - ext) <= 0.01 * ext
+    assert abs(int(stats.shadow_rays) - shadow) <= 0.01 * shadow
+
+
+@pytest.mark.parametrize("scene_name", ["imaged", "textured"])
+def test_shading_frames_match_reference(ctx, scene_dir, halton_perm, oracle, scene_name):
+    """Normal, tangent and bitangent after normal / bump mapping, the texture
+    footprint, object-space position and dp/du at 20,000 hits: equal to the
+    reference's FetchShadingData + TextureCoordinatesDifferential +
+    InitShadingSpace bit for bit. Texture coordinates too, except on spheres,
+    whose angles come from acosf / atan2f (CUDA's and the host's may differ in
+    the last place)."""
+    from ymrt_b200 import scenes
+    path = scenes.scene_path(scene_name, 0, scene_dir)
+    ours = Y.Scene(ctx, Y.HostScene(path, W, H), halton_perm)
+    ref = oracle.RefScene(path, halton_perm, W, H)
+    rng = np.random.default_rng(41)
+    n = 20000
+    o = rng.uniform(-0.9, 0.9, (n, 3)).astype(np.float32)
+    d = rng.normal(size=(n, 3)).astype(np.float32)
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    hit = ref.trace(o, d)
+    m = hit["inst"] != 0xFFFFFFFF
+    args = (hit["inst"][m], hit["tri"][m], hit["bary"][m], hit["back"][m], d[m])
+    a = ours.shading_frame(*args)
+    b = ref.shading_frame(*args)
+    names = ["n"] * 3 + ["t"] * 3 + ["b"] * 3 + ["footprint"] * 4 + ["uv"] * 2 + ["p_obj"] * 3 + ["dpdu"] * 3 + ["mat"]
+    for c in range(22):
+        bad = a[:, c].view(np.uint32) != b[:, c].view(np.uint32)
+        if names[c] == "uv":
+            bad &= ~np.isclose(a[:, c], b[:, c], rtol=1e-6, atol=1e-7)
+        assert not bad.any(), (names[c], c, int(bad.sum()), a[bad][:3, c], b[bad][:3, c], a[bad][:3, 21])
+    ours.close()
+    ref.close()

@@ -86,7 +86,7 @@ def test_arrays_reject_bad_input(scene_dir):
     assert e.value.code == -1
     bad = dict(kw)
     tex = np.zeros((1, Y.TEXTURE_WORDS), np.uint32)
-    tex[0, 0] = 0  # an image node
+    tex[0, 0] = 11  # an unknown node type
     bad["textures"] = tex
     with pytest.raises(Y.YmrtError) as e:
         Y.HostScene.from_arrays(64, 64, **bad)

@@ -81,9 +81,9 @@ def test_loader_rejects_bad_input(tmp_path):
     with pytest.raises(Y.YmrtError) as e:
         Y.HostScene(write(tmp_path, "Begin(Transform);\n\ttranslate = <0,0,0>;\n"), 8, 8)
     assert e.value.code == -3  # missing End
-    with pytest.raises(Y.YmrtError) as e:  # image textures are not supported
+    with pytest.raises(Y.YmrtError) as e:  # an image texture needs a file name
         Y.HostScene(write(tmp_path, 'Begin(ImageTexture);\n\tname = "t";\nEnd(ImageTexture);\n'), 8, 8)
-    assert e.value.code == -4
+    assert e.value.code == -3
     with pytest.raises(Y.YmrtError) as e:  # a solid node needs both inputs (the reference's reader too)
         Y.HostScene(write(tmp_path, 'Begin(CheckerBoardTexture);\n\tname = "t";\nEnd(CheckerBoardTexture);\n'), 8, 8)
     assert e.value.code == -3

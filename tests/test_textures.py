@@ -93,8 +93,9 @@ def _node(kind, black=0xFFFFFFFF, white=0xFFFFFFFF, freq=1.0):
 def test_texture_graph_checks(scene_dir):
     hs, kw = arrays_of("cornell", scene_dir, 64, 64)
     const = _node(1)
-    # an image node is not supported
-    assert _bad_textures(kw, [_node(0)]) == -4
+    # an unknown node type is not supported; an image node needs a size, 1-4 channels and a wrap mode
+    assert _bad_textures(kw, [_node(11)]) == -4
+    assert _bad_textures(kw, [_node(0)]) == -1
     # a solid node needs both inputs
     assert _bad_textures(kw, [const, _node(3, 0)]) == -1
     # a graph read by a material: a cycle, and a chain deeper than the 8-node evaluation stack
@@ -134,3 +135,96 @@ def test_wave_parameters_are_illegal_statements(tmp_path, halton_perm, oracle):
     assert e.value.code == -3
     with pytest.raises(RuntimeError):
         oracle.RefScene(path, halton_perm, 32, 32)
+
+
+# ---- image textures ----
+
+def test_image_scene_prepares_like_the_reference(scene_dir, halton_perm, oracle):
+    """PNG files of every kind the scene uses (8-bit RGB / RGBA interlaced,
+    16-bit grey, 4-bit palette with transparency, 2-bit grey): node records
+    and decoded pixels equal the reference's (its image library plus its
+    sRGB decode) bit for bit; the image whose file is missing is left out
+    as the reference leaves it out."""
+    path = scenes.scene_path("imaged", 0, scene_dir)
+    ours, ref = Y.HostScene(path, 128, 128), oracle.RefScene(path, halton_perm, 128, 128)
+    _compare_prepared(ours, ref)
+    tex = ours.records("textures")
+    images = np.flatnonzero(tex[:, 0] == 0)
+    assert len(images) == 10
+    for k in images:
+        assert np.array_equal(ours.image_pixels(int(k)).view(np.uint32), ref.image_pixels(int(k)).view(np.uint32)), k
+    mats = ours.records("materials")
+    assert mats[1, 4] == 0xFFFFFFFF  # the ceiling's image did not load: its albedo stays constant
+
+
+def _png_cases():
+    rng = np.random.default_rng(99)
+    cases = []
+    for ctype, depths in ((0, (1, 2, 4, 8, 16)), (2, (8, 16)), (3, (1, 2, 4, 8)), (4, (8, 16)), (6, (8, 16))):
+        n = {0: 1, 2: 3, 3: 1, 4: 2, 6: 4}[ctype]
+        for depth in depths:
+            for interlace in (False, True):
+                h, w = 13, 19
+                top = (1 << depth) - 1 if ctype != 3 else min(15, (1 << depth) - 1)
+                img = rng.integers(0, top + 1, (h, w, n)).astype(np.uint16)
+                kw = dict(depth=depth, color_type=ctype, interlace=interlace, first_filter=depth % 5)
+                if ctype == 3:
+                    kw["palette"] = rng.integers(0, 256, (top + 1, 3))
+                    kw["trns"] = bytes(rng.integers(0, 256, top + 1 - 1).tolist()) if interlace else None
+                if ctype == 0 and depth == 8 and interlace:
+                    kw["trns"] = bytes([0, int(img[0, 0, 0])])  # a grey colour key present in the image
+                if ctype == 2 and depth == 16 and not interlace:
+                    v = img[1, 2]
+                    kw["trns"] = b"".join(int(x).to_bytes(2, "big") for x in v)
+                cases.append((f"c{ctype}d{depth}{'i' if interlace else ''}", img, kw))
+    return cases
+
+
+@pytest.mark.parametrize("case", _png_cases(), ids=lambda c: c[0])
+def test_png_decoding_matches_the_reference(case, tmp_path, halton_perm, oracle):
+    name, img, kw = case
+    s = scenes.cornell_scene(0)
+    s.image_files["img.png"] = (img, kw)
+    for cs in ("SRGB", "Linear"):
+        s.textures.append(("ImageTexture", "img_" + cs, {"texture_file_name": "img.png", "color_space": cs}))
+    path = scenes.write_scene(s, str(tmp_path / "png_case.ymtmp"))
+    ours, ref = Y.HostScene(path, 32, 32), oracle.RefScene(path, halton_perm, 32, 32)
+    assert np.array_equal(ours.records("textures"), ref.records("textures"))
+    for k in (0, 1):
+        a, b = ours.image_pixels(k), ref.image_pixels(k)
+        assert a.size == b.size and np.array_equal(a.view(np.uint32), b.view(np.uint32)), (name, k)
+
+
+def test_non_png_images_are_unsupported(tmp_path):
+    s = scenes.cornell_scene(0)
+    s.textures.append(("ImageTexture", "jpg", {"texture_file_name": "photo.jpg", "color_space": "SRGB"}))
+    path = scenes.write_scene(s, str(tmp_path / "jpg_case.ymtmp"))
+    folder = scenes.texture_folder(path)
+    os.makedirs(folder, exist_ok=True)
+    with open(os.path.join(folder, "photo.jpg"), "wb") as f:
+        f.write(b"\xff\xd8\xff\xe0" + bytes(64))
+    with pytest.raises(Y.YmrtError) as e:
+        Y.HostScene(path, 32, 32)
+    assert e.value.code == -4
+
+
+def test_image_nodes_from_arrays(scene_dir):
+    path = scenes.scene_path("imaged", 0, scene_dir)
+    hs = Y.HostScene(path, 64, 64)
+    _, kw = arrays_of("cornell", scene_dir, 64, 64)
+    tex = hs.records("textures")
+    k = int(np.flatnonzero(tex[:, 0] == 0)[0])
+    kw = dict(kw)
+    kw["textures"] = tex[k:k + 1]
+    ha = Y.HostScene.from_arrays(64, 64, **kw)
+    assert np.array_equal(ha.records("textures"), tex[k:k + 1])
+    with pytest.raises(Y.YmrtError):
+        ha.set_image(0, np.zeros(5, np.float32))  # wrong sample count
+    ha.set_image(0, hs.image_pixels(k))
+    assert np.array_equal(ha.image_pixels(0), hs.image_pixels(k))
+    bad = tex[k:k + 1].copy()
+    bad[0, 5] = 7  # seven channels
+    kw["textures"] = bad
+    with pytest.raises(Y.YmrtError) as e:
+        Y.HostScene.from_arrays(64, 64, **kw)
+    assert e.value.code == -1

@@ -34,7 +34,7 @@ ERRORS = {
 QUERY_COUNTS, QUERY_INSTANCES, QUERY_LIGHTS, QUERY_LIGHT_TABLE = 0, 1, 2, 3
 QUERY_TRANSFORMS, QUERY_CAMERA, QUERY_TRIANGLES = 4, 5, 6
 QUERY_MATERIALS, QUERY_VOLUMES, QUERY_DISTANT_LIGHTS, QUERY_TEXTURES = 7, 8, 9, 10
-QUERY_GEOMETRIES, QUERY_MESH_CORNERS = 11, 12
+QUERY_GEOMETRIES, QUERY_MESH_CORNERS, QUERY_IMAGE_PIXELS = 11, 12, 13
 
 
 class YmrtError(RuntimeError):
@@ -138,6 +138,8 @@ def library():
     L.ymrt_scene_set_density_grid.argtypes = [vp, ctypes.c_uint32, i, i, i, vp, i]
     L.ymrt_debug_density.argtypes = [vp, ctypes.c_uint32, i, vp, vp]
     L.ymrt_debug_texture.argtypes = [vp, ctypes.c_uint32, i, vp, vp]
+    L.ymrt_host_scene_set_image.argtypes = [vp, ctypes.c_uint32, vp, ctypes.c_size_t]
+    L.ymrt_debug_frame.argtypes = [vp, i, vp, vp, vp, vp, vp, vp]
     L.ymrt_render_forward.argtypes = [vp, ctypes.POINTER(RenderSetting), i, vp, i, ctypes.POINTER(Stats)]
     L.ymrt_render_tiles.argtypes = [vp, ctypes.POINTER(RenderSetting), i, i, i, vp, i, ctypes.POINTER(Stats)]
     L.ymrt_accumulate.argtypes = [vp, vp, vp, i]
@@ -363,6 +365,16 @@ class HostScene:
         """Per corner of a mesh: position, normal, uv (8 floats; uv 0 without texcoords)."""
         return self._query(QUERY_MESH_CORNERS, np.float32, mesh).reshape(-1, 8)
 
+    def image_pixels(self, texture_index: int) -> np.ndarray:
+        """Pixels of an image node: linear samples, bottom row first, channels interleaved (flat)."""
+        return self._query(QUERY_IMAGE_PIXELS, np.float32, texture_index)
+
+    def set_image(self, texture_index: int, pixels) -> None:
+        """Pixels of image node `texture_index` (width * height * channels
+        linear floats, bottom row first): for scenes from arrays."""
+        p = np.ascontiguousarray(pixels, np.float32).reshape(-1)
+        _check(library().ymrt_host_scene_set_image(self.h, texture_index, _p(p), p.size))
+
     def records(self, kind: str) -> np.ndarray:
         """Materials, volumes, distant lights (32-bit words of the reference's
         structs) or textures (TEXTURE_WORDS words each: ymrt_texture_desc), one
@@ -404,6 +416,18 @@ class Scene:
             raise ValueError("density grid must be a (nz, ny, nx) array")
         nz, ny, nx = v.shape
         _check(library().ymrt_scene_set_density_grid(self.h, texture_index, nx, ny, nz, _p(v), int(half)), self.ctx.h)
+
+    def shading_frame(self, inst, tri, bary, back, dirs) -> np.ndarray:
+        """The shading frame at given hits: (n, 22) floats (normal, tangent,
+        bitangent, texture footprint, uv, object-space position, dp/du,
+        material index)."""
+        n = len(inst)
+        out = np.zeros((n, 22), np.float32)
+        args = [np.ascontiguousarray(inst, np.uint32), np.ascontiguousarray(tri, np.uint32),
+                np.ascontiguousarray(bary, np.float32), np.ascontiguousarray(back, np.int32),
+                np.ascontiguousarray(dirs, np.float32)]
+        _check(library().ymrt_debug_frame(self.h, n, *[_p(a) for a in args], _p(out)), self.ctx.h)
+        return out
 
     def texture(self, texture_index: int, st, points) -> np.ndarray:
         """rgb of texture node `texture_index` as a surface reads it, at

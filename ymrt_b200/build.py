@@ -36,7 +36,7 @@ CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-fno-fast-math"
              "-I" + os.path.join(ROOT, "include")]
 
 CU_SOURCES = ["kernels.cu", "capi.cu"]
-CXX_SOURCES = ["scene_host.cpp"]
+CXX_SOURCES = ["scene_host.cpp", "png_decode.cpp"]
 
 
 def _stamp() -> str:
@@ -96,7 +96,7 @@ def build(force: bool = False, verbose: bool = False, ptxas_report: bool = False
     with open(vs, "w") as f:
         f.write("{ global: ymrt_*; local: *; };\n")
     _run([NVCC] + ARCH + ["-shared", "-cudart", "static", "-o", tmp] + objs +
-         ["-Xlinker", "-Bsymbolic", "-Xlinker", "--version-script=" + vs], verbose)
+         ["-lz", "-Xlinker", "-Bsymbolic", "-Xlinker", "--version-script=" + vs], verbose)
     os.replace(tmp, LIB)
     # libymrt_compat.so: host code only, linked against libymrt.so (found
     # beside it at run time), so that one CUDA runtime does all device work.

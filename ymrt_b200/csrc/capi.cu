@@ -189,7 +189,7 @@ bool uses_textures(const std::vector<Material>& materials, const std::vector<Tex
   for (const Material& m : materials)
     if (m.material_type == kDefaultMtl && material_textures(m.default_mtl)) return true;
   for (const Texture& t : textures)
-    if (t.type >= kTexChecker && t.type <= kTexWave && t.type != kTexFbm) return true;
+    if ((t.type >= kTexChecker && t.type <= kTexWave && t.type != kTexFbm) || t.type == kTexImage) return true;
   return false;
 }
 
@@ -480,6 +480,12 @@ long long ymrt_host_scene_query(const ymrt_host_scene* hs, int what, int index, 
       for (const HostMesh& m : s.meshes) v.insert(v.end(), {m.kind, f2u(m.radius)});
       return copy(v.data(), v.size(), sizeof(uint32_t));
     }
+    case YMRT_QUERY_IMAGE_PIXELS: {
+      if (index < 0) return YMRT_ERR_INVALID;
+      auto it = s.images.find((uint32_t)index);
+      if (it == s.images.end()) return YMRT_ERR_INVALID;
+      return copy(it->second.data(), it->second.size(), sizeof(float));
+    }
     case YMRT_QUERY_MESH_CORNERS: {
       if (index < 0 || (size_t)index >= s.meshes.size()) return YMRT_ERR_INVALID;
       const HostMesh& m = s.meshes[index];
@@ -545,8 +551,22 @@ int ymrt_scene_upload(ymrt_context* ctx, const ymrt_host_scene* hs, const uint32
   UP(s.shape_lights, shape_lights);
   UP(s.shape_light_table, shape_light_table);
   UP(s.volumes, volumes);
-  UP(s.textures, textures);
-  sc->textures = s.textures;
+  {
+    // image nodes: pixels into device buffers, the node pointing at them
+    std::vector<Texture> tex = s.textures;
+    for (size_t k = 0; k < tex.size() && e == cudaSuccess; ++k) {
+      if (tex[k].type != kTexImage) continue;
+      auto it = s.images.find((uint32_t)k);
+      const size_t n = (size_t)tex[k].width * tex[k].height * tex[k].channels;
+      if (it == s.images.end() || it->second.size() != n)
+        return ctx->fail(YMRT_ERR_INVALID, "image node " + std::to_string(k) + " has no pixels (ymrt_host_scene_set_image)");
+      const float* dev = nullptr;
+      e = sc->upload(it->second, &dev);
+      tex[k].image = dev;
+    }
+    UP(tex, textures);
+    sc->textures = tex;
+  }
   {
     std::vector<uint8_t> buckets(s.instances.size());
     for (size_t i = 0; i < s.instances.size(); ++i) buckets[i] = (uint8_t)shading_bucket(s, s.instances[i]);
@@ -1582,6 +1602,47 @@ int ymrt_debug_density(ymrt_scene* sc, uint32_t texture_index, int n, const floa
   cudaError_t e = cudaStreamSynchronize(ctx->stream);
   if (sg.err != cudaSuccess || e != cudaSuccess) return ctx->cuda_fail(sg.err != cudaSuccess ? sg.err : e, "debug density");
   if (errs) return ctx->fail(YMRT_ERR_OVERFLOW, "texture graph too deep");
+  return YMRT_OK;
+}
+
+int ymrt_host_scene_set_image(ymrt_host_scene* hs, uint32_t texture_index, const float* pixels, size_t count) {
+  if (!hs || !pixels) return YMRT_ERR_INVALID;
+  HostScene& s = hs->s;
+  if (texture_index >= s.textures.size() || s.textures[texture_index].type != kTexImage) {
+    g_last_error = "texture " + std::to_string(texture_index) + " is not an image node";
+    return YMRT_ERR_INVALID;
+  }
+  const Texture& t = s.textures[texture_index];
+  if (count != (size_t)t.width * t.height * t.channels) {
+    g_last_error = "image node " + std::to_string(texture_index) + " holds " +
+                   std::to_string((size_t)t.width * t.height * t.channels) + " samples";
+    return YMRT_ERR_INVALID;
+  }
+  s.images[texture_index].assign(pixels, pixels + count);
+  return YMRT_OK;
+}
+
+int ymrt_debug_frame(ymrt_scene* sc, int n, const uint32_t* inst, const uint32_t* tri, const float* bary,
+                     const int* back, const float* dir, float* out) {
+  if (!sc || n < 0 || !inst || !tri || !bary || !back || !dir || !out) return YMRT_ERR_INVALID;
+  if (n == 0) return YMRT_OK;
+  ymrt_context* ctx = sc->ctx;
+  cudaSetDevice(ctx->device);
+  Staging sg{ctx};
+  const uint32_t* d_i = sg.in(inst, (size_t)n);
+  const uint32_t* d_t = sg.in(tri, (size_t)n);
+  const float* d_b = sg.in(bary, 3 * (size_t)n);
+  const int* d_k = sg.in(back, (size_t)n);
+  const float* d_d = sg.in(dir, 3 * (size_t)n);
+  float* d_out = sg.out<float>(22 * (size_t)n);
+  uint32_t* d_err = sg.out<uint32_t>(1);
+  if (sg.err != cudaSuccess) return ctx->cuda_fail(sg.err, "staging");
+  cudaMemsetAsync(d_err, 0, sizeof(uint32_t), ctx->stream);
+  upload_constants(&sc->dev, 1, ctx->primes.data(), ctx->prime_sums.data(), ctx->stream);
+  launch_debug_frame(n, d_i, d_t, d_b, d_k, d_d, d_out, d_err, ctx->stream);
+  sg.back(out, d_out, 22 * (size_t)n);
+  cudaError_t e = cudaStreamSynchronize(ctx->stream);
+  if (sg.err != cudaSuccess || e != cudaSuccess) return ctx->cuda_fail(sg.err != cudaSuccess ? sg.err : e, "debug frame");
   return YMRT_OK;
 }
 

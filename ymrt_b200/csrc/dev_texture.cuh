@@ -229,6 +229,39 @@ __device__ __noinline__ vec3 solid_node(const Texture& t, vec3 black, vec3 white
   }
 }
 
+// EvalTexImage (src/TextureEval.cuh:162-237): the image's texture
+// coordinates (scaled, offset, negative ones moved up by whole periods),
+// bilinear between the four texels around them (texel centres at
+// half-integers), each fetched with the node's wrap mode; one channel reads
+// as grey, more give their first three.
+__device__ __noinline__ vec3 image_node(const Texture& t, const TexCoord& tc) {
+  if (!t.image) return vec3(0.0f);
+  float u = tc.s * t.scale_u + t.offset_u;
+  if (u < 0.0f) u = gmax(0.0f, u + fabsf(floorf(u)));
+  float v = tc.t * t.scale_v + t.offset_v;
+  if (v < 0.0f) v = gmax(0.0f, v + fabsf(floorf(v)));
+  const float px = u * (float)t.width - 0.5f, py = v * (float)t.height - 0.5f;
+  const int x0 = (int)floorf(px), y0 = (int)floorf(py);
+  const float fx = px - (float)x0, fy = py - (float)y0;
+  const int w = t.width, h = t.height, n = t.channels;
+  auto texel = [&](int x, int y) {
+    if (t.wrap == kWrapClamp) {
+      x = x < 0 ? 0 : (x > w - 1 ? w - 1 : x);
+      y = y < 0 ? 0 : (y > h - 1 ? h - 1 : y);
+    } else {
+      x = ((x % w) + w) % w;
+      y = ((y % h) + h) % h;
+    }
+    const float* p = t.image + ((size_t)y * (size_t)w + (size_t)x) * (size_t)n;
+    if (n == 1) return vec3(__ldg(p));
+    vec3 r(0.0f);
+    for (int c = 0; c < 3 && c < n; ++c) r[c] = __ldg(p + c);
+    return r;
+  };
+  return (1.0f - fx) * (1.0f - fy) * texel(x0, y0) + fx * (1.0f - fy) * texel(x0 + 1, y0) +
+         (1.0f - fx) * fy * texel(x0, y0 + 1) + fx * fy * texel(x0 + 1, y0 + 1);
+}
+
 // The inputs a node reads: two for the solid nodes, none for constants,
 // grids and unknown types.
 __device__ __forceinline__ int texture_inputs(uint32_t type) {
@@ -290,6 +323,8 @@ __device__ __forceinline__ vec3 texture_eval(const Texture* __restrict__ tex, ui
       r = vec3(grid_eval(t, tc.p));
     } else if ((kF & kFeatTextures) && n_in == 2) {
       r = solid_node(t, f.in[0], f.in[1], tc);
+    } else if ((kF & kFeatTextures) && t.type == kTexImage) {
+      r = image_node(t, tc);
     }
     if (f.parent < 0) return r;
     Frame& par = st[f.parent];

@@ -1381,6 +1381,36 @@ __global__ void k_debug_density(int n, uint32_t tex, const float* p, float* out,
   out[i] = texture_eval(S.textures, tex, vec3(p[3 * i], p[3 * i + 1], p[3 * i + 2]), errors).x;
 }
 
+// The shading frame k_shade builds at given hits of scene slot 0 (the
+// layout of the oracle's shading-frame probe): normal, tangent, bitangent,
+// texture footprint, uv, object-space position, dp/du, material index.
+__global__ void k_debug_frame(int n, const uint32_t* inst, const uint32_t* tri, const float* bary, const int* back,
+                              const float* dir, float* out, uint32_t* errors) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const DeviceScene& S = c_scenes[0];
+  float* o = out + 22 * (size_t)i;
+  for (int k = 0; k < 22; ++k) o[k] = 0.0f;
+  if (inst[i] >= S.instance_count) return;
+  const vec3 rd(dir[3 * i], dir[3 * i + 1], dir[3 * i + 2]);
+  const SurfacePoint sp = fetch_surface<kFeatAll>(S, inst[i], tri[i], vec3(bary[3 * i], bary[3 * i + 1], bary[3 * i + 2]));
+  const Instance in = S.instances[inst[i]];
+  if (in.material_idx >= S.material_count) return;
+  const Material& mat = S.materials[in.material_idx];
+  float d[4];
+  tex_differentials(S.camera, sp.p, sp.ns, sp.ng, sp.dpdu, sp.dpdv, S.width, S.height, 0.25f, 0.25f, d);
+  LayeredBsdf B;
+  const TexCoord tc{sp.u, sp.v, sp.p_obj};
+  if (mat.material_type == kDefaultMtl && material_textured(mat.default_mtl))
+    init_shading_frame_mapped(B, mat.default_mtl, back[i], rd, sp, S.i_transforms[in.transform_idx], S, tc, errors);
+  else
+    init_shading_frame(B, back[i], rd, sp.ng, sp.ns, sp.dpdu, sp.dpdv);
+  const float v[22] = {B.n.x, B.n.y, B.n.z, B.t.x, B.t.y, B.t.z, B.b.x, B.b.y, B.b.z, d[0], d[1], d[2], d[3],
+                       sp.u, sp.v, sp.p_obj.x, sp.p_obj.y, sp.p_obj.z, sp.dpdu.x, sp.dpdu.y, sp.dpdu.z,
+                       (float)in.material_idx};
+  for (int k = 0; k < 22; ++k) o[k] = v[k];
+}
+
 // Texture node `tex` of scene slot 0 at points (s, t, x, y, z): rgb out.
 __global__ void k_debug_texture(int n, uint32_t tex, const float* c, float* out, uint32_t* errors) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1608,6 +1638,12 @@ void launch_debug_trace(int n, const float* o, const float* d, const uint32_t* l
 void launch_debug_density(int n, uint32_t tex, const float* p, float* out, uint32_t* err, cudaStream_t stream) {
   if (n <= 0) return;
   k_debug_density<<<(n + 255) / 256, 256, 0, stream>>>(n, tex, p, out, err);
+}
+
+void launch_debug_frame(int n, const uint32_t* inst, const uint32_t* tri, const float* bary, const int* back,
+                        const float* dir, float* out, uint32_t* err, cudaStream_t stream) {
+  if (n <= 0) return;
+  k_debug_frame<<<(n + 127) / 128, 128, 0, stream>>>(n, inst, tri, bary, back, dir, out, err);
 }
 
 void launch_debug_texture(int n, uint32_t tex, const float* c, float* out, uint32_t* err, cudaStream_t stream) {

@@ -17,6 +17,7 @@
 #include <unordered_map>
 
 #include "../../include/ymrt.h"
+#include "png_decode.h"
 #include "sphere.h"
 
 namespace ym {
@@ -896,7 +897,31 @@ int load_ymtmp(const std::string& path, HostScene* scene, std::string* error) {
       names[name] = (uint32_t)scene->textures.size();
       scene->textures.push_back(tex);
     } else if (type == "ImageTexture") {
-      return fail(YMRT_ERR_UNSUPPORTED, "image textures are not supported (constant and solid textures are)");
+      // read_image_texture_attributes (src/core/YMParser.cpp:1509-1557): the
+      // file lies in the folder texture_<stem>_<extension> beside the scene
+      // file; a file that does not load leaves the name without a node
+      // (CreateImageTexture returns EMPTY, src/core/SceneModule.cpp:665-670).
+      const std::string file = attrs.count("texture_file_name") ? unquote(attrs["texture_file_name"]) : "";
+      const std::string cs = attrs.count("color_space") ? unquote(attrs["color_space"]) : "";
+      if (file.empty()) return bad(open, "image texture requires a file name");
+      const size_t slash = path.find_last_of('/');
+      const std::string dir = slash == std::string::npos ? "" : path.substr(0, slash + 1);
+      const std::string fname = slash == std::string::npos ? path : path.substr(slash + 1);
+      const size_t dot = fname.find_last_of('.');
+      const std::string folder = dir + "texture_" + fname.substr(0, dot) + "_" + fname.substr(dot + 1);
+      Texture tex;
+      std::vector<float> pixels;
+      std::string why;
+      const int irc = load_image_texture(folder + "/" + file, (cs.empty() || cs == "SRGB") ? kImageSrgb : kImageLinear,
+                                         &tex, &pixels, &why);
+      if (irc == YMRT_ERR_UNSUPPORTED) return fail(irc, why);
+      if (irc != YMRT_OK) {
+        names[name] = kEmpty;
+      } else {
+        names[name] = (uint32_t)scene->textures.size();
+        scene->images[(uint32_t)scene->textures.size()] = std::move(pixels);
+        scene->textures.push_back(tex);
+      }
     } else if (type == "DistantLight") {
       DistantLight dl{};
       dl.light_color = vmax(get_v("light_color", vec3(1.0f)), vec3(0.0f));
@@ -938,6 +963,49 @@ int load_ymtmp(const std::string& path, HostScene* scene, std::string* error) {
 
 // ------------------------------------------------------- texture nodes ---
 
+static_assert(sizeof(ymrt_texture_desc) == kTextureWords * 4, "ymrt_texture_desc is 20 words");
+
+float srgb_to_linear(float s) {
+  return s > 0.04045 ? (float)std::pow((s + 0.055) / 1.055, (double)2.4f) : (s / 12.92f);
+}
+
+int load_image_texture(const std::string& path, uint32_t color_space, Texture* t, std::vector<float>* pixels,
+                       std::string* error) {
+  {
+    std::ifstream f(path, std::ios::binary);
+    if (!f) {
+      if (error) *error = "cannot open " + path;
+      return YMRT_ERR_IO;
+    }
+    char sig[8] = {0};
+    f.read(sig, 8);
+    static const unsigned char kPng[8] = {137, 80, 78, 71, 13, 10, 26, 10};
+    if (f.gcount() == 8 && std::memcmp(sig, kPng, 8) != 0) {
+      if (error) *error = path + ": only PNG images are supported";
+      return YMRT_ERR_UNSUPPORTED;
+    }
+  }
+  PngImage img;
+  if (!decode_png_file(path, &img, error)) return YMRT_ERR_IO;
+  std::memset(t, 0, sizeof(*t));
+  t->type = kTexImage;
+  t->child[0] = t->child[1] = kEmpty;
+  t->width = img.width;
+  t->height = img.height;
+  t->channels = img.channels;
+  t->wrap = kWrapRepeat;
+  t->scale_u = t->scale_v = 1.0f;
+  t->offset_u = t->offset_v = 0.0f;
+  t->color_space = color_space;
+  const float inv = img.sixteen ? 1.0f / 65535.0f : 1.0f / 255.0f;
+  pixels->resize(img.samples.size());
+  for (size_t i = 0; i < img.samples.size(); ++i) {
+    const float v = float((int)img.samples[i]) * inv;
+    (*pixels)[i] = color_space == kImageSrgb ? srgb_to_linear(v) : v;
+  }
+  return YMRT_OK;
+}
+
 void texture_words(const Texture& t, uint32_t r[kTextureWords]) {
   for (int k = 0; k < kTextureWords; ++k) r[k] = 0;
   r[0] = t.type;
@@ -963,6 +1031,18 @@ void texture_words(const Texture& t, uint32_t r[kTextureWords]) {
   if (t.type == kTexGrid) {  // the lattice is not part of the node's words
     r[1] = r[2] = kEmpty;
   }
+  if (t.type == kTexImage) {
+    for (int k = 3; k < kTextureWords; ++k) r[k] = 0;
+    r[3] = (uint32_t)t.width;
+    r[4] = (uint32_t)t.height;
+    r[5] = (uint32_t)t.channels;
+    r[6] = (uint32_t)t.wrap;
+    r[7] = f2u(t.scale_u);
+    r[8] = f2u(t.scale_v);
+    r[9] = f2u(t.offset_u);
+    r[10] = f2u(t.offset_v);
+    r[15] = t.color_space;
+  }
 }
 
 int texture_from_desc(const ymrt_texture_desc& d, Texture* t, std::string* error) {
@@ -976,6 +1056,25 @@ int texture_from_desc(const ymrt_texture_desc& d, Texture* t, std::string* error
   if (d.type == kTexConstRgb) {
     t->color = vec3(d.color[0], d.color[1], d.color[2]);
     return YMRT_OK;
+  }
+  if (d.type == kTexImage) {  // words: width, height, channels, wrap, scale u/v, offset u/v, colour space
+    uint32_t w[kTextureWords];
+    std::memcpy(w, &d, sizeof(w));
+    t->width = (int)w[3];
+    t->height = (int)w[4];
+    t->channels = (int)w[5];
+    t->wrap = (int)w[6];
+    std::memcpy(&t->scale_u, &w[7], 4);
+    std::memcpy(&t->scale_v, &w[8], 4);
+    std::memcpy(&t->offset_u, &w[9], 4);
+    std::memcpy(&t->offset_v, &w[10], 4);
+    t->color_space = w[15];
+    if (t->width < 1 || t->height < 1 || t->channels < 1 || t->channels > 4 ||
+        (t->wrap != kWrapRepeat && t->wrap != kWrapClamp)) {
+      if (error) *error = "image node: size, channel count (1-4) or wrap mode (0 repeat, 1 clamp) out of range";
+      return YMRT_ERR_INVALID;
+    }
+    return YMRT_OK;  // pixels: ymrt_host_scene_set_image
   }
   if (d.type < kTexChecker || d.type > kTexWave) {
     if (error) *error = "node type " + std::to_string(d.type) + " is not supported (constant and solid nodes are)";

@@ -8,6 +8,7 @@
 #pragma once
 
 #include <cstdint>
+#include <map>
 #include <string>
 #include <vector>
 
@@ -49,6 +50,7 @@ struct HostScene {
   std::vector<uint32_t> instance_file_index;  // after prepare(): file index of each instance
   std::vector<Material> materials;
   std::vector<Texture> textures;
+  std::map<uint32_t, std::vector<float>> images;  // pixels of each image node (Texture::image is set at upload)
   std::vector<Volume> volumes;
   std::vector<DistantLight> distant_lights;
   std::vector<ShapeLight> shape_lights;
@@ -89,6 +91,18 @@ int texture_from_desc(const ymrt_texture_desc& desc, Texture* t, std::string* er
 // more than kTextureStack nodes (the evaluation stack). Returns 0 or
 // `code` with a message.
 int check_textures(const HostScene& scene, int code, std::string* error);
+
+// Loads a PNG as the pixels of an image node (LoadImageTexture,
+// src/FileIO.cpp:77-172: samples scaled by 1/255 or 1/65535, then decoded
+// from sRGB unless the colour space is linear; mip 0 only; repeat wrap,
+// unit scale, zero offset). Returns 0; YMRT_ERR_IO when the file cannot be
+// read or decoded (the reference then leaves the node out); or
+// YMRT_ERR_UNSUPPORTED for an image format other than PNG.
+int load_image_texture(const std::string& path, uint32_t color_space, Texture* t, std::vector<float>* pixels,
+                       std::string* error);
+
+// The reference's sRGB decode of one sample (SRGBToLinear, src/MathCommon.h:136-139).
+float srgb_to_linear(float s);
 
 // glm-order transform helpers (exposed for tests through the C-ABI).
 mat4 compose_transform(vec3 translate, vec3 scale, vec3 rotate_deg);

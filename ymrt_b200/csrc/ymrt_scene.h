@@ -126,10 +126,12 @@ struct RenderSetting {
 };
 static_assert(sizeof(RenderSetting) == 40, "RenderSetting layout");
 
-// Texture nodes (src/Texture.h:16-28, 168-690): constants and the solid
-// (procedural) nodes, each with a black and a white input node whose results
-// it blends or selects. Children are texture indices (kEmpty: absent, reads
-// as black). The image node (type 0) is not supported.
+// Texture nodes (src/Texture.h:16-28, 84-690): images, constants and the
+// solid (procedural) nodes, each solid node with a black and a white input
+// node whose results it blends or selects. Children are texture indices
+// (kEmpty: absent, reads as black). An image node holds its pixels (mip 0
+// only, as the reference loads them) as floats, rows bottom-up, channels
+// interleaved.
 //
 // kTexGrid is this project's density grid (the reference's texture graph has
 // no grid node; a caller attaches one with ymrt_scene_set_density_grid): an
@@ -161,7 +163,13 @@ struct Texture {
   int grid_n[3];       // grid: lattice size x, y, z
   int grid_half;       // grid: values are float16 (else float32)
   const void* grid;    // grid: device values, x fastest
+  int width, height, channels, wrap;             // image: size, samples per pixel, kWrap*
+  float scale_u, scale_v, offset_u, offset_v;    // image: texture-coordinate transform
+  uint32_t color_space;                          // image: kImageSrgb / kImageLinear (applied at load)
+  const float* image;                            // image: device pixels
 };
+constexpr int kWrapRepeat = 0, kWrapClamp = 1;      // WARP_MODE_*, src/Texture.h:30-34
+constexpr uint32_t kImageSrgb = 0, kImageLinear = 1;  // src/Texture.h:36-41
 
 // Ray-transfer stack of nested media, src/Ray.h:106-260 (RayTransfer).
 struct BoundaryRecord {

@@ -230,6 +230,7 @@ class Scene:
         self.volumes = []     # (name, transform, sigma_t, albedo, g, density_texture or None)
         self.instances = []   # (name, geometry, transform, material, volume or None, boundary)
         self.distant_lights = []  # (name, transform, color, intensity, theta_max_deg)
+        self.image_files = {}  # file name -> (samples, write_png keyword arguments), written beside the scene
 
     @property
     def triangle_count(self) -> int:
@@ -253,8 +254,102 @@ def _arr(a, fmt) -> str:
     return "[" + ",".join(fmt(x) for x in a) + "]"
 
 
+_ADAM7 = ((0, 0, 8, 8), (4, 0, 8, 8), (0, 4, 4, 8), (2, 0, 4, 4), (0, 2, 2, 4), (1, 0, 2, 2), (0, 1, 1, 2))
+
+
+def _png_rows(img: np.ndarray, depth: int) -> np.ndarray:
+    """Samples (h, w, n) packed into scanline bytes (h, row bytes), big-endian."""
+    h, w, n = img.shape
+    if depth == 16:
+        return img.astype(">u2").reshape(h, w * n).view(np.uint8).reshape(h, -1)
+    if depth == 8:
+        return img.astype(np.uint8).reshape(h, w * n)
+    per = 8 // depth
+    flat = img.reshape(h, w * n).astype(np.uint8)
+    pad = (-flat.shape[1]) % per
+    flat = np.pad(flat, ((0, 0), (0, pad)))
+    flat = flat.reshape(h, -1, per)
+    shifts = (8 - depth * (np.arange(per) + 1)).astype(np.uint8)
+    return np.bitwise_or.reduce(flat << shifts, axis=2).astype(np.uint8)
+
+
+def _png_filter(rows: np.ndarray, bpp: int, first_filter: int) -> bytes:
+    """Filters each scanline (types cycling from first_filter) and prefixes
+    its filter byte."""
+    out = bytearray()
+    prev = np.zeros(rows.shape[1], np.int32)
+    for y in range(rows.shape[0]):
+        x = rows[y].astype(np.int32)
+        a = np.concatenate([np.zeros(bpp, np.int32), x[:-bpp]]) if x.size > bpp else np.zeros_like(x)
+        c = np.concatenate([np.zeros(bpp, np.int32), prev[:-bpp]]) if x.size > bpp else np.zeros_like(x)
+        b = prev
+        t = (first_filter + y) % 5
+        if t == 0:
+            f = x
+        elif t == 1:
+            f = x - a
+        elif t == 2:
+            f = x - b
+        elif t == 3:
+            f = x - (a + b) // 2
+        else:
+            p = a + b - c
+            pa, pb, pc = np.abs(p - a), np.abs(p - b), np.abs(p - c)
+            f = x - np.where((pa <= pb) & (pa <= pc), a, np.where(pb <= pc, b, c))
+        out.append(t)
+        out += (f & 255).astype(np.uint8).tobytes()
+        prev = x
+    return bytes(out)
+
+
+def write_png(path: str, samples, depth: int = 8, color_type: int = 2, palette=None, trns: bytes | None = None,
+              interlace: bool = False, first_filter: int = 0) -> str:
+    """Writes a PNG (this project's encoder, for test images): samples
+    (h, w, n) in file order (top row first; palette images hold indices in
+    one channel), any bit depth the colour type allows, optional Adam7
+    interlacing, scanline filters cycling through all five types."""
+    import struct
+    import zlib
+    img = np.asarray(samples)
+    if img.ndim == 2:
+        img = img[..., None]
+    h, w, n = img.shape
+    bpp = max(1, n * depth // 8)
+    if interlace:
+        data = b"".join(_png_filter(_png_rows(img[y0::dy, x0::dx], depth), bpp, first_filter)
+                        for x0, y0, dx, dy in _ADAM7 if x0 < w and y0 < h)
+    else:
+        data = _png_filter(_png_rows(img, depth), bpp, first_filter)
+
+    def chunk(kind: bytes, body: bytes) -> bytes:
+        return struct.pack(">I", len(body)) + kind + body + struct.pack(">I", zlib.crc32(kind + body) & 0xFFFFFFFF)
+
+    png = b"\x89PNG\r\n\x1a\n" + chunk(b"IHDR", struct.pack(">IIBBBBB", w, h, depth, color_type, 0, 0, int(interlace)))
+    if palette is not None:
+        png += chunk(b"PLTE", np.asarray(palette, np.uint8).tobytes())
+    if trns is not None:
+        png += chunk(b"tRNS", bytes(trns))
+    png += chunk(b"IDAT", zlib.compress(data, 6)) + chunk(b"IEND", b"")
+    with open(path, "wb") as f:
+        f.write(png)
+    return path
+
+
+def texture_folder(path: str) -> str:
+    """Where a scene file's image textures lie: texture_<stem>_<extension>
+    beside it (get_texture_folder_from_scene_file, src/core/YMParser.cpp:20-30)."""
+    d, name = os.path.split(os.path.abspath(path))
+    stem, ext = os.path.splitext(name)
+    return os.path.join(d, f"texture_{stem}_{ext[1:]}")
+
+
 def write_scene(scene: Scene, path: str) -> str:
     out = []
+    if scene.image_files:
+        folder = texture_folder(path)
+        os.makedirs(folder, exist_ok=True)
+        for fname, (samples, kw) in scene.image_files.items():
+            write_png(os.path.join(folder, fname), samples, **kw)
     frm, look, fov = scene.camera
     out.append(f"Begin(Camera);\n\tfov = {_f(fov)};\n\tfrom = {_vec(frm)};\n\tlook = {_vec(look)};\nEnd(Camera);\n")
     for m in scene.meshes:
@@ -647,6 +742,80 @@ def textured_scene(seed: int = 0) -> Scene:
     return s
 
 
+def imaged_scene(seed: int = 0) -> Scene:
+    """The Cornell-like room with image textures (PNG files in the scene's
+    texture folder): an 8-bit sRGB RGB back wall, a floor whose albedo is an
+    interlaced 8-bit RGBA image and whose roughness and metalness come from a
+    16-bit linear grey image, a 4-bit palette image with transparency on the
+    left wall, a 2-bit grey bump map on the right wall, an 8-bit linear
+    normal map on the tall box, a checkerboard of two images on the short
+    box, an image over the built-in cube's and a sphere's texture
+    coordinates, a quad with 3x-repeating texture coordinates, and an image
+    whose file is missing (its material keeps its constant albedo, as in the
+    reference)."""
+    rng = np.random.Generator(np.random.PCG64(seed + 4242))
+    s = cornell_scene(seed)
+    s.meshes.append(uv_quad_mesh(repeat=3.0))
+    s.cubes = ["Geo_UnitCube"]
+    s.spheres = [("Geo_Sphere", 1.0)]
+    mats = dict((name, i) for i, (_, name, _) in enumerate(s.materials))
+
+    def set_mat(name, attrs):
+        s.materials[mats[name]] = ("DefaultMaterial", name, attrs)
+
+    def image(name, fname, samples, color_space="SRGB", **png):
+        s.image_files[fname] = (samples, png)
+        s.textures.append(("ImageTexture", name, {"texture_file_name": fname, "color_space": color_space}))
+        return name
+
+    def smooth(h, w, n, scale=255):
+        y, x = np.mgrid[0:h, 0:w]
+        base = [np.sin(x * (0.21 + 0.05 * k) + y * (0.13 - 0.03 * k) + k) for k in range(n)]
+        img = (np.stack(base, -1) * 0.35 + 0.5 + rng.uniform(-0.15, 0.15, (h, w, n)))
+        return np.clip(np.rint(img * scale), 0, scale).astype(np.uint16)
+
+    image("back_img", "back_wall.png", smooth(48, 64, 3), depth=8, color_type=2, first_filter=0)
+    set_mat("back_material", {**_lambert((0.5, 0.5, 0.5)), "diffuse_albedo_tex": "back_img"})
+    image("floor_albedo_img", "floor_albedo.png", smooth(40, 40, 4), depth=8, color_type=6, interlace=True,
+          first_filter=2)
+    image("floor_gray16", "floor_rough.png", smooth(33, 27, 1, 65535), color_space="Linear", depth=16,
+          color_type=0, first_filter=4)
+    set_mat("floor_material", {"diffuse_albedo": [0.5, 0.5, 0.5], "specular_albedo": [1.0, 1.0, 1.0],
+                               "roughness_x": 0.3, "roughness_y": 0.3, "ior_n": 1.5, "specular_weight": 1.0,
+                               "diffuse_albedo_tex": "floor_albedo_img", "alpha_x_tex": "floor_gray16",
+                               "alpha_y_tex": "floor_gray16", "metalness_tex": "floor_gray16"})
+    pal = rng.integers(20, 235, (16, 3))
+    idx = (np.add.outer(np.arange(30) // 3, np.arange(50) // 5) % 16).astype(np.uint16)
+    image("left_img", "left_palette.png", idx, depth=4, color_type=3, palette=pal,
+          trns=bytes(rng.integers(0, 256, 10).tolist()), first_filter=1)
+    set_mat("left_material", {**_lambert((0.5, 0.5, 0.5)), "diffuse_albedo_tex": "left_img"})
+    image("right_bump", "right_bump.png", (smooth(32, 32, 1, 3)).astype(np.uint16), depth=2, color_type=0,
+          first_filter=3)
+    set_mat("right_material", {**_lambert((0.6, 0.6, 0.6)), "bump_mapping_tex": "right_bump"})
+    nrm = np.stack([smooth(24, 24, 1, 255)[..., 0] // 4 + 96, smooth(24, 24, 1, 255)[..., 0] // 4 + 96,
+                    np.full((24, 24), 250)], -1).astype(np.uint16)
+    image("box_normal", "box_normal.png", nrm, color_space="Linear", depth=8, color_type=2, first_filter=2)
+    set_mat("tall_box_material", {**_lambert((0.7, 0.6, 0.5)), "normal_mapping_tex": "box_normal"})
+    image("chk_a", "checker_a.png", smooth(16, 16, 3), depth=8, color_type=2)
+    image("chk_b", "checker_b.png", smooth(8, 12, 1), depth=8, color_type=0, first_filter=1)
+    _solid(s, "CheckerBoardTexture", "short_checker", "chk_a", "chk_b", frequency=10.0)
+    set_mat("short_box_material", {**_lambert((0.5, 0.5, 0.5)), "diffuse_albedo_tex": "short_checker"})
+    image("cube_img", "cube.png", smooth(20, 30, 3), depth=8, color_type=2, first_filter=3)
+    s.transforms.append(("cube_transform", (0.55, 0.1, -0.55), (0.3, 0.3, 0.3), (20.0, 30.0, 0.0)))
+    s.materials.append(("DefaultMaterial", "cube_material", {**_lambert((0.5, 0.5, 0.5)), "diffuse_albedo_tex": "cube_img"}))
+    s.instances.append(("cube", "Geo_UnitCube", "cube_transform", "cube_material", None, False))
+    s.transforms.append(("ball_transform", (-0.45, 0.5, 0.2), (0.25, 0.25, 0.25), (30.0, 0.0, 0.0)))
+    s.materials.append(("DefaultMaterial", "ball_material", {**_lambert((0.5, 0.5, 0.5)), "diffuse_albedo_tex": "cube_img"}))
+    s.instances.append(("ball", "Geo_Sphere", "ball_transform", "ball_material", None, False))
+    image("quad_img", "quad.png", smooth(10, 14, 3), depth=8, color_type=2, interlace=True)
+    s.transforms.append(("uvquad_transform", (-0.6, 0.3, -0.8), (0.6, 1.0, 0.6), (70.0, 25.0, 0.0)))
+    s.materials.append(("DefaultMaterial", "uvquad_material", {**_lambert((0.5, 0.5, 0.5)), "diffuse_albedo_tex": "quad_img"}))
+    s.instances.append(("uvquad", "Geo_UVQuad", "uvquad_transform", "uvquad_material", None, False))
+    s.textures.append(("ImageTexture", "missing_img", {"texture_file_name": "missing.png", "color_space": "SRGB"}))
+    set_mat("ceiling_material", {**_lambert((0.7, 0.7, 0.7)), "diffuse_albedo_tex": "missing_img"})
+    return s
+
+
 def orbit_view(name: str, seed: int, k: int, n: int):
     """The k-th of n cameras (from, look, fov) on a 90-degree arc around the
     scene's look-at point, at the original camera's height and distance and
@@ -666,6 +835,7 @@ SCENES = {
     "instanced_fog": instanced_fog_scene,
     "spheres": spheres_scene,
     "textured": textured_scene,
+    "imaged": imaged_scene,
     "volumetric": volumetric_scene,
     "volumetric_const": volumetric_const_scene,
 }
