@@ -380,6 +380,30 @@ int ymrt_debug_density(ymrt_scene* scene, uint32_t texture_index, int n, const f
 int ymrt_debug_frame(ymrt_scene* scene, int n, const uint32_t* inst, const uint32_t* tri, const float* bary,
                      const int* back, const float* dir, float* out);
 
+/* ---- editor view and post-processing ---- */
+
+/* The editor's albedo / picking view (Ray_generation_editor_view,
+ * Ray_trace_editor_view, Ray_shading_editor_view, src/Shading.cu:1276-1594)
+ * of a width x height image from the scene's camera (aspect width/height):
+ * per pixel one ray through the pixel centre, followed through pass-through
+ * boundaries; the surface colour (diffuse albedo or its texture, a light's
+ * colour x intensity, black for an invalid material) or, on a miss, the
+ * background when setting->enable_env_light (else black) is ADDED to
+ * beauty_rgba with alpha 1, and the first hit's instance unique_index is
+ * written to primitive_index (a miss leaves it). device_buffers: 1 when both
+ * buffers are device memory, 0 for host memory. */
+int ymrt_render_editor_view(ymrt_scene* scene, const ymrt_render_setting* setting, uint32_t width, uint32_t height,
+                            float* beauty_rgba, uint32_t* primitive_index, int device_buffers);
+
+/* PostProcessingPathTracing / PostProcessingEditorView (src/Shading.cu:
+ * 2396-2516): ACES tone mapping of exposure x colour, then 1/gamma, alpha 1;
+ * with outline != 0 and selected != 0xFFFFFFFF, pixels whose 3x3
+ * neighbourhood shows instance `selected` (primitive_index) partly turn red
+ * and wholly get a 60% red tint. In place. */
+int ymrt_post_process(ymrt_context* ctx, float* image_rgba, const uint32_t* primitive_index, uint32_t width,
+                      uint32_t height, uint32_t selected, float gamma, float exposure, int outline,
+                      int device_buffers);
+
 /* Pixels of image node `texture_index` of a host scene (from
  * ymrt_scene_from_arrays, or replacing a loaded image): count =
  * width * height * channels linear floats, channels interleaved, bottom row

@@ -1,11 +1,12 @@
 /* ymrt_compat.h -- the reference's stage interface on top of ymrt_b200.
  *
- * The YMRT editor drives path tracing through twelve functions (four
- * Allocate / Release pairs and four stage launchers)
+ * The YMRT editor drives rendering through seventeen functions (four
+ * Allocate / Release pairs, four path-tracing stage launchers, three
+ * editor-view stage launchers and two post-processing calls)
  * declared in src/core/RenderModule.cpp:14-28, 36-42 and defined in src/Shading.cu
  * (AllocateRayCounter ... AccumulateImagePathTracing), called by the wave
  * loop of RenderModule::PathTracingExecuteTask
- * (src/core/RenderModule.cpp:494-653). libymrt_compat.so exports those twelve
+ * (src/core/RenderModule.cpp:494-653). libymrt_compat.so exports those seventeen
  * symbols with the same names and argument lists, so that RenderModule links
  * against it unchanged; each forwards to the entry points below (in
  * libymrt.so), which render with ymrt_b200's kernels.
@@ -60,6 +61,22 @@ int ymrt_compat_trace(int frame_index, const ymrt_render_setting* setting, void*
 /* RayShadingPathTracing (src/Shading.cu:2304): clears the device counter. */
 int ymrt_compat_shade(int frame_index, const ymrt_render_setting* setting, void* device_counter, uint32_t width,
                       uint32_t height, float* noise_rgba, void* stream);
+
+/* RayGenerationEditorView / RayTraceEditorView / RayShadingEditorView
+ * (src/Shading.cu:1333, 1442, 1596): the same protocol for the editor view
+ * (the first generation call marks the frame, the trace call renders the
+ * whole view with ymrt_render_editor_view into the caller's beauty and
+ * primitive-index buffers and clears the device counter). */
+int ymrt_compat_editor_generate(int frame_index, void* device_counter, uint32_t next_tile, uint32_t width,
+                                uint32_t height, void* stream);
+int ymrt_compat_editor_trace(int frame_index, const ymrt_render_setting* setting, void* device_counter, uint32_t width,
+                             uint32_t height, float* beauty_rgba, uint32_t* primitive_index, void* stream);
+int ymrt_compat_editor_shade(void* device_counter, void* stream);
+
+/* PostProcessingEditorView / PostProcessingPathTracing (src/Shading.cu:
+ * 2467-2515), with ymrt_post_process on device buffers. */
+int ymrt_compat_post_process(float* image_rgba, const uint32_t* primitive_index, uint32_t width, uint32_t height,
+                             uint32_t selected, float gamma, float exposure, int outline, void* stream);
 
 /* AccumulateImagePathTracing (src/Shading.cu:2375): the running mean, skipped
  * once max_frames (> 0) frames have been accumulated, as the reference. */

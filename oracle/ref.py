@@ -56,6 +56,8 @@ def _bind(L, settings_type):
     L.ymref_camera_bytes.argtypes = [vp, vp, i]
     L.ymref_scene_records.argtypes = [vp, i, vp, i]
     L.ymref_texture_eval.argtypes = [vp, ctypes.c_uint32, i, vp, vp]
+    L.ymref_render_editor_view.argtypes = [vp, i, i, vp, vp]
+    L.ymref_post_process.argtypes = [vp, vp, i, i, ctypes.c_uint32, ctypes.c_float, ctypes.c_float, i]
     L.ymref_shading_frame.argtypes = [vp, i, vp, vp, vp, vp, vp, vp]
     L.ymref_image_pixels.restype = ctypes.c_longlong
     L.ymref_image_pixels.argtypes = [vp, ctypes.c_uint32, vp, ctypes.c_longlong]
@@ -232,6 +234,17 @@ class RefScene:
                                     _p(out))
         return out
 
+    def editor_view(self, wave_capacity: int = 1 << 20, threads: int = 0):
+        """The reference's editor view: (beauty (H, W, 4), primitive index (H, W))
+        from zeroed beauty and an all-EMPTY primitive index."""
+        beauty = np.zeros((self.height, self.width, 4), self._f)
+        prim = np.full((self.height, self.width), 0xFFFFFFFF, np.uint32)
+        rc = self._L.ymref_render_editor_view(self.h, wave_capacity, threads or (os.cpu_count() or 1), _p(beauty),
+                                              _p(prim))
+        if rc != 0:
+            raise RuntimeError(f"ymref_render_editor_view failed ({rc})")
+        return beauty, prim
+
     def image_pixels(self, tex: int) -> np.ndarray:
         """Pixels of image node `tex` as the reference loaded them (linear
         samples, bottom row first, channels interleaved), flat."""
@@ -298,6 +311,15 @@ class RefScene:
 
     def last_render_seconds(self) -> float:
         return self._L.ymref_last_render_seconds(self.h)
+
+
+def post_process(image, primitive_index, selected: int, gamma: float, exposure: float, outline: bool):
+    """The reference's tone mapping (and outline) of an (H, W, 4) float32
+    image, returned as a new array."""
+    img = np.ascontiguousarray(image, np.float32).copy()
+    prim = np.ascontiguousarray(primitive_index, np.uint32)
+    lib().ymref_post_process(_p(img), _p(prim), img.shape[1], img.shape[0], selected, gamma, exposure, int(outline))
+    return img
 
 
 def query_counts(reset: bool = True) -> tuple[int, int]:

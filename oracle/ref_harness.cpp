@@ -664,6 +664,90 @@ int ymref_render_frame(void* handle, int frame_index, int tile_begin, int tile_e
   return 0;
 }
 
+// The editor view (src/Shading.cu:1276-1594) over all tiles with the
+// stages' own queue protocol, the editor camera set to the rendering camera
+// (as the editor sizes it to its viewport). Adds into beauty (width*height*4)
+// and writes primitive_index (width*height) as the stages do; neither is
+// cleared here. Returns 0, or -1 / -2 on bad arguments / queue overflow.
+int ymref_render_editor_view(void* handle, int wave_capacity, int n_threads, float* beauty, uint32_t* primitive_index) {
+  auto ctx = static_cast<RefContext*>(handle);
+  const uint32_t w = ctx->width, h = ctx->height;
+  const uint32_t tiles_x = (w + TILE_X_RES - 1) / TILE_X_RES;
+  const uint32_t tiles_y = (h + TILE_Y_RES - 1) / TILE_Y_RES;
+  const uint32_t total_tiles = tiles_x * tiles_y;
+  if (wave_capacity < (int)TILE_PIXEL_COUNT) return -1;
+  const size_t cap = (size_t)wave_capacity;
+  if (ctx->capacity < cap) {
+    ctx->q.Resize(cap);
+    ctx->capacity = cap;
+  }
+  Camera* cams = GuiModule::Cameras(*ctx->module);
+  std::memcpy(&cams[EDITOR_CAMERA_INDEX], &cams[RENDERING_CAMERA_INDEX], sizeof(Camera));
+  Queues& q = ctx->q;
+  glm::vec4* img = reinterpret_cast<glm::vec4*>(beauty);
+  RayCounter counter{0, 0, 0}, host_counter{0, 0, 0};
+  const Scene* scene = &ctx->scene;
+  uint32_t next_tile = 0;
+  while (host_counter.shading_ray_counter > 0 || next_tile < total_tiles) {
+    const uint32_t tiles_this_batch = std::min<uint32_t>(
+        (uint32_t)((cap - host_counter.shading_ray_counter) / TILE_PIXEL_COUNT), total_tiles - next_tile);
+    const uint32_t gen_count = tiles_this_batch * TILE_PIXEL_COUNT;
+    counter.shading_ray_counter = host_counter.shading_ray_counter;
+    Launch(gen_count, STAGE_RAY_GEN_BLOCK_SIZE, n_threads, [&]() {
+      Ray_generation_editor_view(1, scene, &counter, next_tile, gen_count, w, h, tiles_x, tiles_y, q.s_ray.data(),
+                                 q.s_px.data(), q.s_py.data(), q.s_cam.data(), q.s_transfer.data());
+    });
+    next_tile += tiles_this_batch;
+    host_counter.shading_ray_counter += gen_count;
+    counter = host_counter;
+    const uint32_t trace_count = host_counter.shading_ray_counter;
+    Launch(trace_count, STAGE_RAY_TRACE_BLOCK_SIZE, n_threads, [&]() {
+      Ray_trace_editor_view(1, scene, &counter, trace_count, w, h, img, primitive_index, q.s_ray.data(), q.s_px.data(),
+                            q.s_py.data(), q.s_cam.data(), q.s_transfer.data(), q.h_rec.data(),
+                            q.h_nearby_count.data(), q.h_nearby_prim.data(), q.h_nearby_t.data(),
+                            q.h_nearby_back.data(), q.h_ray.data(), q.h_px.data(), q.h_py.data(), q.h_cam.data(),
+                            q.h_transfer.data());
+    });
+    host_counter = counter;
+    host_counter.shading_ray_counter = 0;
+    counter = host_counter;
+    const uint32_t shade_count = host_counter.hit_counter;
+    Launch(shade_count, STAGE_RAY_SHADING_BLOCK_SIZE, n_threads, [&]() {
+      Ray_shading_editor_view(1, scene, &counter, shade_count, w, h, img, primitive_index, q.s_ray.data(),
+                              q.s_px.data(), q.s_py.data(), q.s_cam.data(), q.s_transfer.data(), q.h_rec.data(),
+                              q.h_nearby_count.data(), q.h_nearby_prim.data(), q.h_nearby_t.data(),
+                              q.h_nearby_back.data(), q.h_ray.data(), q.h_px.data(), q.h_py.data(), q.h_cam.data(),
+                              q.h_transfer.data());
+    });
+    host_counter = counter;
+    host_counter.hit_counter = 0;
+    if (host_counter.shading_ray_counter > cap) return -2;
+  }
+  return 0;
+}
+
+// Gamma_correction_common and Draw_outline (src/Shading.cu:2396-2466) over
+// an image in place, as PostProcessingEditorView runs them.
+void ymref_post_process(float* image, const uint32_t* primitive_index, int width, int height, uint32_t selected,
+                        float gamma, float exposure, int outline) {
+  glm::vec4* img = reinterpret_cast<glm::vec4*>(image);
+  auto grid = [&](auto body) {
+    blockDim = dim3(32, 32, 1);
+    gridDim = dim3((width + 31) / 32, (height + 31) / 32, 1);
+    for (uint32_t by = 0; by < gridDim.y; ++by)
+      for (uint32_t bx = 0; bx < gridDim.x; ++bx)
+        for (uint32_t ty = 0; ty < 32; ++ty)
+          for (uint32_t tx = 0; tx < 32; ++tx) {
+            blockIdx = make_uint3(bx, by, 0);
+            threadIdx = make_uint3(tx, ty, 0);
+            body();
+          }
+  };
+  grid([&]() { Gamma_correction_common(img, gamma, exposure, (uint32_t)width, (uint32_t)height); });
+  if (outline && selected != EMPTY_UINT32)
+    grid([&]() { Draw_outline(img, primitive_index, (uint32_t)width, (uint32_t)height, selected); });
+}
+
 double ymref_last_render_seconds(void* handle) { return static_cast<RefContext*>(handle)->last_render_seconds; }
 
 // Closest-hit (TraceRay) and occlusion (BVHTraverseShadow) queries made by the

@@ -41,3 +41,20 @@ def test_no_device_is_an_error_not_a_fallback():
     with pytest.raises(Y.YmrtError) as e:
         Y.Context(0)
     assert e.value.code == -9
+
+
+def test_compat_library_exports_the_reference_launchers():
+    """libymrt_compat.so exports the seventeen extern "C" launchers the
+    reference's RenderModule declares (src/core/RenderModule.cpp:14-46,
+    without its two ImGui test hooks), so that module links against it."""
+    import ctypes
+    import ymrt_b200 as Y
+    Y.library()
+    names = ["AllocateRayCounter", "ReleaseRayCounter", "AllocateShadingRayData", "ReleaseShadingRayData",
+             "AllocateHitData", "ReleaseHitData", "AllocateShadowRayData", "ReleaseShadowRayData",
+             "RayGenerationEditorView", "RayTraceEditorView", "RayShadingEditorView", "RayGenerationPathTracing",
+             "RayTracePathTracing", "RayShadingPathTracing", "AccumulateImagePathTracing", "PostProcessingEditorView",
+             "PostProcessingPathTracing"]
+    lib = ctypes.CDLL(os.path.join(ROOT, "ymrt_b200", "libymrt_compat.so"))
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing

@@ -140,6 +140,9 @@ def library():
     L.ymrt_debug_texture.argtypes = [vp, ctypes.c_uint32, i, vp, vp]
     L.ymrt_host_scene_set_image.argtypes = [vp, ctypes.c_uint32, vp, ctypes.c_size_t]
     L.ymrt_debug_frame.argtypes = [vp, i, vp, vp, vp, vp, vp, vp]
+    L.ymrt_render_editor_view.argtypes = [vp, ctypes.POINTER(RenderSetting), ctypes.c_uint32, ctypes.c_uint32, vp, vp, i]
+    L.ymrt_post_process.argtypes = [vp, vp, vp, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_float,
+                                    ctypes.c_float, i, i]
     L.ymrt_render_forward.argtypes = [vp, ctypes.POINTER(RenderSetting), i, vp, i, ctypes.POINTER(Stats)]
     L.ymrt_render_tiles.argtypes = [vp, ctypes.POINTER(RenderSetting), i, i, i, vp, i, ctypes.POINTER(Stats)]
     L.ymrt_accumulate.argtypes = [vp, vp, vp, i]
@@ -417,6 +420,15 @@ class Scene:
         nz, ny, nx = v.shape
         _check(library().ymrt_scene_set_density_grid(self.h, texture_index, nx, ny, nz, _p(v), int(half)), self.ctx.h)
 
+    def editor_view(self, setting: "RenderSetting"):
+        """The editor's albedo / picking view at the scene's size: (beauty
+        (H, W, 4), primitive index (H, W), 0xFFFFFFFF where nothing was hit)."""
+        beauty = np.zeros((self.height, self.width, 4), np.float32)
+        prim = np.full((self.height, self.width), 0xFFFFFFFF, np.uint32)
+        _check(library().ymrt_render_editor_view(self.h, ctypes.byref(setting), self.width, self.height, _p(beauty),
+                                                 _p(prim), 0), self.ctx.h)
+        return beauty, prim
+
     def shading_frame(self, inst, tri, bary, back, dirs) -> np.ndarray:
         """The shading frame at given hits: (n, 22) floats (normal, tangent,
         bitangent, texture footprint, uv, object-space position, dp/du,
@@ -558,6 +570,17 @@ class BackwardTargets(ctypes.Structure):
     _fields_ = [("material_grads_device", ctypes.c_void_p), ("n_materials", ctypes.c_uint32),
                 ("grid_texture", ctypes.c_uint32), ("grid_grads_device", ctypes.c_void_p),
                 ("grid_values", ctypes.c_uint64), ("reserved", ctypes.c_uint32 * 4)]
+
+
+def post_process(ctx: Context, image, primitive_index=None, selected: int = 0xFFFFFFFF, gamma: float = 2.2,
+                 exposure: float = 1.0, outline: bool = False) -> np.ndarray:
+    """ACES tone mapping and gamma (and the selection outline) of an (H, W, 4)
+    float32 host image; returns a new array."""
+    img = np.ascontiguousarray(image, np.float32).copy()
+    prim = None if primitive_index is None else np.ascontiguousarray(primitive_index, np.uint32)
+    _check(library().ymrt_post_process(ctx.h, _p(img), None if prim is None else _p(prim), img.shape[1], img.shape[0],
+                                       selected, gamma, exposure, int(outline), 0), ctx.h)
+    return img
 
 
 def render_backward_ex(ctx: Context, renders, records, dlosses, material_grads=None, grid_texture=None,

@@ -1374,6 +1374,8 @@ struct CompatBinding {
   ymrt_scene* scene = nullptr;
   bool frame_marked = false;
   int frame_index = 0;
+  bool editor_marked = false;  // the editor view's current frame, as frame_marked
+  int editor_frame = 0;
 };
 CompatBinding g_compat;
 
@@ -1494,6 +1496,64 @@ int ymrt_compat_shade(int frame_index, const ymrt_render_setting* setting, void*
   int rc = compat_sync(stream);
   if (rc != YMRT_OK) return rc;
   return compat_clear_counter(device_counter);
+}
+
+int ymrt_compat_editor_generate(int frame_index, void* device_counter, uint32_t next_tile, uint32_t width,
+                                uint32_t height, void* stream) {
+  (void)device_counter;
+  std::lock_guard<std::mutex> lk(g_compat.m);
+  if (!g_compat.scene) {
+    g_last_error = "no scene bound (ymrt_compat_bind)";
+    return YMRT_ERR_INVALID;
+  }
+  if (width == 0 || height == 0) return YMRT_ERR_INVALID;
+  int rc = compat_sync(stream);
+  if (rc != YMRT_OK) return rc;
+  if (next_tile == 0) {
+    g_compat.editor_marked = true;
+    g_compat.editor_frame = frame_index;
+  }
+  return YMRT_OK;
+}
+
+int ymrt_compat_editor_trace(int frame_index, const ymrt_render_setting* setting, void* device_counter, uint32_t width,
+                             uint32_t height, float* beauty_rgba, uint32_t* primitive_index, void* stream) {
+  std::lock_guard<std::mutex> lk(g_compat.m);
+  if (!g_compat.scene || !setting || !beauty_rgba || !primitive_index) {
+    g_last_error = "no scene bound (ymrt_compat_bind) or null argument";
+    return YMRT_ERR_INVALID;
+  }
+  int rc = compat_sync(stream);
+  if (rc != YMRT_OK) return rc;
+  if (g_compat.editor_marked && g_compat.editor_frame == frame_index) {
+    g_compat.editor_marked = false;
+    rc = ymrt_render_editor_view(g_compat.scene, setting, width, height, beauty_rgba, primitive_index, 1);
+    if (rc != YMRT_OK) {
+      g_last_error = g_compat.scene->ctx->error;
+      return rc;
+    }
+  }
+  return compat_clear_counter(device_counter);
+}
+
+int ymrt_compat_editor_shade(void* device_counter, void* stream) {
+  int rc = compat_sync(stream);
+  if (rc != YMRT_OK) return rc;
+  return compat_clear_counter(device_counter);
+}
+
+int ymrt_compat_post_process(float* image_rgba, const uint32_t* primitive_index, uint32_t width, uint32_t height,
+                             uint32_t selected, float gamma, float exposure, int outline, void* stream) {
+  std::lock_guard<std::mutex> lk(g_compat.m);
+  if (!g_compat.ctx) {
+    g_last_error = "no context bound (ymrt_compat_bind)";
+    return YMRT_ERR_INVALID;
+  }
+  int rc = compat_sync(stream);
+  if (rc != YMRT_OK) return rc;
+  rc = ymrt_post_process(g_compat.ctx, image_rgba, primitive_index, width, height, selected, gamma, exposure, outline, 1);
+  if (rc != YMRT_OK) g_last_error = g_compat.ctx->error;
+  return rc;
 }
 
 int ymrt_compat_accumulate(const float* noise_rgba, float* acc_rgba, uint32_t width, uint32_t height, int frame_index,
@@ -1619,6 +1679,60 @@ int ymrt_host_scene_set_image(ymrt_host_scene* hs, uint32_t texture_index, const
     return YMRT_ERR_INVALID;
   }
   s.images[texture_index].assign(pixels, pixels + count);
+  return YMRT_OK;
+}
+
+int ymrt_render_editor_view(ymrt_scene* sc, const ymrt_render_setting* setting, uint32_t width, uint32_t height,
+                            float* beauty_rgba, uint32_t* primitive_index, int device_buffers) {
+  if (!sc || !setting || !beauty_rgba || !primitive_index || width == 0 || height == 0) return YMRT_ERR_INVALID;
+  ymrt_context* ctx = sc->ctx;
+  cudaSetDevice(ctx->device);
+  const size_t n = (size_t)width * height;
+  Staging sg{ctx};
+  float* d_b = beauty_rgba;
+  uint32_t* d_p = primitive_index;
+  if (!device_buffers) {
+    d_b = const_cast<float*>(sg.in(beauty_rgba, 4 * n));
+    d_p = const_cast<uint32_t*>(sg.in(primitive_index, n));
+  }
+  uint32_t* d_err = sg.out<uint32_t>(1);
+  if (sg.err != cudaSuccess) return ctx->cuda_fail(sg.err, "staging");
+  cudaMemsetAsync(d_err, 0, sizeof(uint32_t), ctx->stream);
+  upload_constants(&sc->dev, 1, ctx->primes.data(), ctx->prime_sums.data(), ctx->stream);
+  launch_editor_view(0, (int)width, (int)height, setting->enable_env_light ? 1 : 0, reinterpret_cast<float4*>(d_b), d_p,
+                     d_err, ctx->stream);
+  uint32_t errs = 0;
+  if (!device_buffers) {
+    sg.back(beauty_rgba, d_b, 4 * n);
+    sg.back(primitive_index, d_p, n);
+  }
+  sg.back(&errs, d_err, 1);
+  cudaError_t e = cudaStreamSynchronize(ctx->stream);
+  if (sg.err != cudaSuccess || e != cudaSuccess) return ctx->cuda_fail(sg.err != cudaSuccess ? sg.err : e, "editor view");
+  if (errs & kDevErrStack) return ctx->fail(YMRT_ERR_OVERFLOW, "traversal or nested-media stack overflow on the device");
+  if (errs & kDevErrIter) return ctx->fail(YMRT_ERR_OVERFLOW, "a camera ray passed through too many boundaries");
+  return YMRT_OK;
+}
+
+int ymrt_post_process(ymrt_context* ctx, float* image_rgba, const uint32_t* primitive_index, uint32_t width,
+                      uint32_t height, uint32_t selected, float gamma, float exposure, int outline,
+                      int device_buffers) {
+  if (!ctx || !image_rgba || width == 0 || height == 0 || (outline && !primitive_index)) return YMRT_ERR_INVALID;
+  cudaSetDevice(ctx->device);
+  const size_t n = (size_t)width * height;
+  Staging sg{ctx};
+  float* d_i = image_rgba;
+  const uint32_t* d_p = primitive_index;
+  if (!device_buffers) {
+    d_i = const_cast<float*>(sg.in(image_rgba, 4 * n));
+    if (outline) d_p = sg.in(primitive_index, n);
+  }
+  if (sg.err != cudaSuccess) return ctx->cuda_fail(sg.err, "staging");
+  launch_post_process(reinterpret_cast<float4*>(d_i), d_p, (int)width, (int)height, selected, gamma, exposure,
+                      outline != 0 && selected != kEmpty, ctx->stream);
+  if (!device_buffers) sg.back(image_rgba, d_i, 4 * n);
+  cudaError_t e = cudaStreamSynchronize(ctx->stream);
+  if (sg.err != cudaSuccess || e != cudaSuccess) return ctx->cuda_fail(sg.err != cudaSuccess ? sg.err : e, "post process");
   return YMRT_OK;
 }
 

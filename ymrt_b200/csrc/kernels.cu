@@ -1381,6 +1381,131 @@ __global__ void k_debug_density(int n, uint32_t tex, const float* p, float* out,
   out[i] = texture_eval(S.textures, tex, vec3(p[3 * i], p[3 * i + 1], p[3 * i + 2]), errors).x;
 }
 
+// ---------------------------------------------------------- editor view ---
+//
+// The editor's picking / albedo view (Ray_generation_editor_view,
+// Ray_trace_editor_view, Ray_shading_editor_view, src/Shading.cu:1276-1594)
+// fused into one thread per pixel: a camera ray through the pixel centre,
+// closest hits followed through pass-through boundaries (medium stack
+// updated as the shade stage does), then the hit surface's colour
+// (MaterialSurfaceCol, src/BSDF.cuh:883-898: diffuse albedo or its texture;
+// a light's colour times intensity; black for an invalid material) or the
+// background (environment light on) / black on a miss, added to `beauty`
+// with alpha 1. The camera ray's first hit writes the instance's
+// unique_index into `primitive_index` (a miss leaves it). At most
+// kEditorPassThroughs boundaries are followed; a ray still passing after
+// that sets kDevErrIter and adds nothing.
+constexpr int kEditorPassThroughs = 64;
+
+__global__ void __launch_bounds__(kTraceBlock) k_editor_view(int slot, int width, int height, float aspect,
+                                                             int env_light, float4* beauty, uint32_t* primitive_index,
+                                                             uint32_t* errors) {
+  YM_TRAVERSAL_SHARED(s_stack);
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= width * height) return;
+  const int px = i % width, py = i / width;
+  const DeviceScene& S = c_scenes[slot];
+  const CameraDesc& cam = S.camera;
+  const float ndc_x = float(px + 0.5f) / float(width);
+  const float ndc_y = float(py + 0.5f) / float(height);
+  const float h = 2.0f * cam.tan_half_fov;
+  const float w = h * aspect;
+  vec3 o = cam.position;
+  vec3 d = normalize(-cam.w + (ndc_x - 0.5f) * w * cam.u + (ndc_y - 0.5f) * h * cam.v);
+  RayTransfer rt = cam.transfer;
+  uint32_t last_inst = kEmpty, last_tri = kEmpty;
+  TraversalStack st;
+  st.bind(s_stack_entries, s_stack_t);
+  uint32_t tests = 0, nodes = 0;
+  vec3 col(0.0f);
+  bool done = false;
+  for (int pass = 0; pass <= kEditorPassThroughs && !done; ++pass) {
+    ClosestHit ch;
+    if (!trace_closest(slot, st, o, d, kTMax, last_inst, last_tri, false, &ch, &tests, &nodes)) {
+      col = env_light ? background(d) : vec3(0.0f);
+      done = true;
+      break;
+    }
+    if (pass == 0) atomicExch(&primitive_index[i], S.instances[ch.inst].unique_index);
+    const vec3 bary(ch.b0, ch.b1, ch.b2);
+    const Instance inst = S.instances[ch.inst];
+    if (!(inst.material_idx < S.material_count)) {
+      done = true;
+      break;
+    }
+    if (inst.treat_as_boundary) {
+      if (pass == kEditorPassThroughs) break;
+      vec3 p, p_err, ng;
+      fetch_geometry_normal<kFeatAll>(S, ch.inst, ch.tri, bary, &p, &p_err, &ng);
+      boundary_transition(S, rt, ch.nearby, ch.nearby_count, errors);
+      o = offset_ray_origin(p, p_err, d, ng);
+      d = normalize(d);  // the reference's Ray constructor normalises again
+      last_inst = ch.inst;
+      last_tri = ch.tri;
+      continue;
+    }
+    const Material& mat = S.materials[inst.material_idx];
+    if (mat.material_type == kLightMtl) {
+      col = mat.light_mtl.light_color * mat.light_mtl.intensity;
+    } else if (mat.material_type == kDefaultMtl) {
+      const DefaultMtl& m = mat.default_mtl;
+      if (m.diffuse_albedo_tex != kEmpty) {
+        const SurfacePoint sp = fetch_surface<kFeatAll>(S, ch.inst, ch.tri, bary);
+        col = surface_texture(S.textures, m.diffuse_albedo_tex, TexCoord{sp.u, sp.v, sp.p_obj}, errors);
+      } else {
+        col = m.diffuse_albedo;
+      }
+    }
+    done = true;
+  }
+  if (st.overflow) atomicOr(errors, (uint32_t)kDevErrStack);
+  if (!done) {
+    atomicOr(errors, (uint32_t)kDevErrIter);
+    return;
+  }
+  atomicAdd(&beauty[i].x, col.x);
+  atomicAdd(&beauty[i].y, col.y);
+  atomicAdd(&beauty[i].z, col.z);
+  atomicAdd(&beauty[i].w, 1.0f);
+}
+
+// Gamma_correction_common (src/Shading.cu:2396-2425): ACES tone mapping of
+// the exposed colour, then 1/gamma, alpha 1.
+__global__ void k_tonemap(float4* image, int width, int height, float gamma, float exposure) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+  if (x >= width || y >= height) return;
+  const size_t k = (size_t)y * width + x;
+  const float4 c = image[k];
+  vec3 col(c.x, c.y, c.z);
+  const float a = 2.51f, b = 0.03f, cc = 2.43f, dd = 0.59f, e = 0.14f;
+  col *= exposure;
+  col = (col * (a * col + b)) / (col * (cc * col + dd) + e);
+  const float g = 1.0f / gamma;
+  image[k] = make_float4(powf(col.x, g), powf(col.y, g), powf(col.z, g), 1.0f);
+}
+
+// Draw_outline (src/Shading.cu:2426-2466): pixels whose 3x3 neighbourhood
+// (clipped to the image) shows the selected instance partly become red,
+// wholly a 60% tint towards (0.9, 0.2, 0.2); alpha 1.
+__global__ void k_outline(float4* image, const uint32_t* primitive_index, int width, int height, uint32_t selected) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+  if (x >= width || y >= height) return;
+  int hits = 0, total = 0;
+  for (int dx = -1; dx <= 1; ++dx)
+    for (int dy = -1; dy <= 1; ++dy) {
+      const int sx = x + dx, sy = y + dy;
+      if (sx < 0 || sx >= width || sy < 0 || sy >= height) continue;
+      ++total;
+      if (primitive_index[(size_t)sy * width + sx] == selected) ++hits;
+    }
+  const size_t k = (size_t)y * width + x;
+  const float4 c = image[k];
+  vec3 r(c.x, c.y, c.z);
+  if (hits == total) r = mix(r, vec3(0.9f, 0.2f, 0.2f), 0.6f);
+  else if (hits != 0) r = vec3(1.0f, 0.0f, 0.0f);
+  image[k] = make_float4(r.x, r.y, r.z, 1.0f);
+}
+
 // The shading frame k_shade builds at given hits of scene slot 0 (the
 // layout of the oracle's shading-frame probe): normal, tangent, bitangent,
 // texture footprint, uv, object-space position, dp/du, material index.
@@ -1638,6 +1763,22 @@ void launch_debug_trace(int n, const float* o, const float* d, const uint32_t* l
 void launch_debug_density(int n, uint32_t tex, const float* p, float* out, uint32_t* err, cudaStream_t stream) {
   if (n <= 0) return;
   k_debug_density<<<(n + 255) / 256, 256, 0, stream>>>(n, tex, p, out, err);
+}
+
+void launch_editor_view(int slot, int width, int height, int env_light, float4* beauty, uint32_t* primitive_index,
+                        uint32_t* errors, cudaStream_t stream) {
+  const int n = width * height;
+  if (n <= 0) return;
+  k_editor_view<<<(n + kTraceBlock - 1) / kTraceBlock, kTraceBlock, 0, stream>>>(
+      slot, width, height, float(width) / float(height), env_light, beauty, primitive_index, errors);
+}
+
+void launch_post_process(float4* image, const uint32_t* primitive_index, int width, int height, uint32_t selected,
+                         float gamma, float exposure, bool outline, cudaStream_t stream) {
+  if (width <= 0 || height <= 0) return;
+  const dim3 block(32, 8), grid((width + 31) / 32, (height + 7) / 8);
+  k_tonemap<<<grid, block, 0, stream>>>(image, width, height, gamma, exposure);
+  if (outline) k_outline<<<grid, block, 0, stream>>>(image, primitive_index, width, height, selected);
 }
 
 void launch_debug_frame(int n, const uint32_t* inst, const uint32_t* tri, const float* bary, const int* back,

@@ -168,6 +168,10 @@ void launch_accumulate(const float4* noise, float4* acc, uint32_t n, int frame_i
 // Density of texture node `tex` at object-space points (3 floats each), scene slot 0.
 void launch_debug_density(int n, uint32_t tex, const float* p, float* out, uint32_t* err, cudaStream_t stream);
 void launch_debug_texture(int n, uint32_t tex, const float* c, float* out, uint32_t* err, cudaStream_t stream);
+void launch_editor_view(int slot, int width, int height, int env_light, float4* beauty, uint32_t* primitive_index,
+                        uint32_t* errors, cudaStream_t stream);
+void launch_post_process(float4* image, const uint32_t* primitive_index, int width, int height, uint32_t selected,
+                         float gamma, float exposure, bool outline, cudaStream_t stream);
 void launch_debug_frame(int n, const uint32_t* inst, const uint32_t* tri, const float* bary, const int* back,
                         const float* dir, float* out, uint32_t* err, cudaStream_t stream);
 void launch_debug_trace(int n, const float* o, const float* d, const uint32_t* lh, uint32_t* inst, uint32_t* tri,
