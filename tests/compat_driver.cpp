@@ -16,6 +16,11 @@
 // are in flight, copying the counters between host and device in between.
 //
 // usage: compat_driver <scene.ymtmp> <halton_perm.u32> <width> <height> <spp> <frames> <max_frames> <out_compat> <out_direct>
+//        [<editor_compat> <editor_direct>]
+// The optional outputs hold, per side: the editor view's beauty (float4 per
+// pixel) and primitive index (uint32 per pixel), the editor view after
+// PostProcessingEditorView (outline of the instance at the image centre),
+// and the accumulated image after PostProcessingPathTracing.
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -69,6 +74,23 @@ void RayShadingPathTracing(int current_frame_index, const RenderSetting& render_
                            ShadowRayData& shadow_ray_data, cudaStream_t& stream);
 void AccumulateImagePathTracing(const vec4* noise_image, vec4* accumulated_image, uint32_t width, uint32_t height,
                                 int frame_index, const int max_accumulate_frame, cudaStream_t& stream);
+void RayGenerationEditorView(int current_frame_index, const RenderSetting& render_setting, Scene* scene_device,
+                             RayCounter* ray_counter_device, uint32_t next_tile_index, uint32_t tile_count_this_batch,
+                             uint32_t width, uint32_t height, uint32_t tile_count_x, uint32_t tile_count_y,
+                             ShadingRayData& shading_ray_data, cudaStream_t& stream);
+void RayTraceEditorView(int current_frame_index, const RenderSetting& render_setting, Scene* scene_device,
+                        RayCounter* ray_counter_device, RayCounter* ray_counter_host, uint32_t width, uint32_t height,
+                        vec4* beauty, uint32_t* primitive_index, ShadingRayData& shading_ray_data, HitData& hit_data,
+                        cudaStream_t& stream);
+void RayShadingEditorView(int current_frame_index, const RenderSetting& render_setting, Scene* scene_device,
+                          RayCounter* ray_counter_device, RayCounter* ray_counter_host, uint32_t width, uint32_t height,
+                          vec4* beauty, uint32_t* primitive_index, ShadingRayData& shading_ray_data,
+                          HitData& hit_data, ShadowRayData& shadow_ray_data, cudaStream_t& stream);
+void PostProcessingEditorView(vec4* image, uint32_t* primitive_index, uint32_t width, uint32_t height,
+                              uint32_t clicked_primitive_index, float gamma, float exposure, bool draw_selected_effect,
+                              cudaStream_t& stream);
+void PostProcessingPathTracing(vec4* image, uint32_t width, uint32_t height, float gamma, float exposure,
+                               cudaStream_t& stream);
 }
 
 namespace {
@@ -117,6 +139,46 @@ void run_frame(int frame, const RenderSetting& rs, RayCounterData& counters, Sha
   }
 }
 
+// RenderModule::EditorViewExecuteTask's loop (src/core/RenderModule.cpp:366-492):
+// batches of MAX_RAY_COUNT rays, re-queued pass-through rays, counters
+// copied between host and device around every stage.
+void run_editor_frame(int frame, const RenderSetting& rs, RayCounterData& counters, ShadingRayData& srd, HitData& hd,
+                      ShadowRayData& sd, uint32_t w, uint32_t h, vec4* beauty, uint32_t* prim, cudaStream_t& stream) {
+  const uint32_t tiles_x = (w + 15) / 16, tiles_y = (h + 15) / 16, total = tiles_x * tiles_y;
+  uint32_t next_tile = 0;
+  RayCounter* host = counters.ray_counter_host;
+  RayCounter* dev = counters.ray_counter_device;
+  host->hit_counter = host->shading_ray_counter = host->shadow_ray_counter = 0;
+  cuda(cudaMemcpyAsync(dev, host, sizeof(RayCounter), cudaMemcpyHostToDevice, stream), "counter");
+  cuda(cudaStreamSynchronize(stream), "sync");
+  while (host->shading_ray_counter > 0 || next_tile < total) {
+    const uint32_t batch = (kMaxRayCount - host->shading_ray_counter) / kTilePixels;
+    RayGenerationEditorView(frame, rs, nullptr, dev, next_tile, batch, w, h, tiles_x, tiles_y, srd, stream);
+    next_tile += batch;
+    host->shading_ray_counter += batch * kTilePixels;
+    cuda(cudaMemcpyAsync(dev, host, sizeof(RayCounter), cudaMemcpyHostToDevice, stream), "counter");
+    cuda(cudaStreamSynchronize(stream), "sync");
+    RayTraceEditorView(frame, rs, nullptr, dev, host, w, h, beauty, prim, srd, hd, stream);
+    cuda(cudaMemcpyAsync(host, dev, sizeof(RayCounter), cudaMemcpyDeviceToHost, stream), "counter");
+    cuda(cudaStreamSynchronize(stream), "sync");
+    host->shading_ray_counter = 0;
+    cuda(cudaMemcpyAsync(dev, host, sizeof(RayCounter), cudaMemcpyHostToDevice, stream), "counter");
+    cuda(cudaStreamSynchronize(stream), "sync");
+    RayShadingEditorView(frame, rs, nullptr, dev, host, w, h, beauty, prim, srd, hd, sd, stream);
+    cuda(cudaMemcpyAsync(host, dev, sizeof(RayCounter), cudaMemcpyDeviceToHost, stream), "counter");
+    cuda(cudaStreamSynchronize(stream), "sync");
+    host->hit_counter = 0;
+    cuda(cudaMemcpyAsync(dev, host, sizeof(RayCounter), cudaMemcpyHostToDevice, stream), "counter");
+    cuda(cudaStreamSynchronize(stream), "sync");
+  }
+}
+
+void save_raw(FILE* f, const void* dev, size_t bytes) {
+  std::vector<unsigned char> h(bytes);
+  cuda(cudaMemcpy(h.data(), dev, bytes, cudaMemcpyDeviceToHost), "read back");
+  if (std::fwrite(h.data(), 1, bytes, f) != bytes) throw std::runtime_error("writing");
+}
+
 void save(const char* path, const vec4* dev, size_t n) {
   std::vector<vec4> h(n);
   cuda(cudaMemcpy(h.data(), dev, sizeof(vec4) * n, cudaMemcpyDeviceToHost), "read back");
@@ -128,7 +190,7 @@ void save(const char* path, const vec4* dev, size_t n) {
 }  // namespace
 
 int main(int argc, char** argv) {
-  if (argc != 10) {
+  if (argc != 10 && argc != 12) {
     std::fprintf(stderr, "usage: %s scene perm width height spp frames max_frames out_compat out_direct\n", argv[0]);
     return 2;
   }
@@ -194,6 +256,49 @@ int main(int argc, char** argv) {
     }
     save(argv[8], acc, n);
     save(argv[9], acc2, n);
+    if (argc == 12) {
+      // the editor view through the launchers and directly, then post-processing
+      vec4 *eb, *eb2;
+      uint32_t *ep, *ep2;
+      cuda(cudaMalloc(&eb, sizeof(vec4) * n), "alloc");
+      cuda(cudaMalloc(&eb2, sizeof(vec4) * n), "alloc");
+      cuda(cudaMalloc(&ep, sizeof(uint32_t) * n), "alloc");
+      cuda(cudaMalloc(&ep2, sizeof(uint32_t) * n), "alloc");
+      cuda(cudaMemset(eb, 0, sizeof(vec4) * n), "clear");
+      cuda(cudaMemset(eb2, 0, sizeof(vec4) * n), "clear");
+      cuda(cudaMemset(ep, 0xFF, sizeof(uint32_t) * n), "clear");
+      cuda(cudaMemset(ep2, 0xFF, sizeof(uint32_t) * n), "clear");
+      RayCounterData ec{};
+      AllocateRayCounter(ec);
+      run_editor_frame(1, rs, ec, srd, hd, sd, (uint32_t)w, (uint32_t)h, eb, ep, stream);
+      ReleaseRayCounter(ec);
+      if (ymrt_render_editor_view(scene, &rs, (uint32_t)w, (uint32_t)h, reinterpret_cast<float*>(eb2), ep2, 1) != YMRT_OK)
+        throw std::runtime_error(ymrt_last_error(ctx));
+      uint32_t centre = 0;
+      cuda(cudaMemcpy(&centre, ep + (size_t)(h / 2) * w + w / 2, sizeof(uint32_t), cudaMemcpyDeviceToHost), "read");
+      FILE* fa = std::fopen(argv[10], "wb");
+      FILE* fb = std::fopen(argv[11], "wb");
+      if (!fa || !fb) throw std::runtime_error("opening the editor outputs");
+      save_raw(fa, eb, sizeof(vec4) * n);
+      save_raw(fa, ep, sizeof(uint32_t) * n);
+      save_raw(fb, eb2, sizeof(vec4) * n);
+      save_raw(fb, ep2, sizeof(uint32_t) * n);
+      PostProcessingEditorView(eb, ep, (uint32_t)w, (uint32_t)h, centre, 2.2f, 1.0f, true, stream);
+      if (ymrt_post_process(ctx, reinterpret_cast<float*>(eb2), ep2, (uint32_t)w, (uint32_t)h, centre, 2.2f, 1.0f, 1, 1) !=
+          YMRT_OK)
+        throw std::runtime_error(ymrt_last_error(ctx));
+      save_raw(fa, eb, sizeof(vec4) * n);
+      save_raw(fb, eb2, sizeof(vec4) * n);
+      PostProcessingPathTracing(acc, (uint32_t)w, (uint32_t)h, 2.2f, 1.0f, stream);
+      if (ymrt_post_process(ctx, reinterpret_cast<float*>(acc2), nullptr, (uint32_t)w, (uint32_t)h, 0xFFFFFFFFu, 2.2f,
+                            1.0f, 0, 1) != YMRT_OK)
+        throw std::runtime_error(ymrt_last_error(ctx));
+      save_raw(fa, acc, sizeof(vec4) * n);
+      save_raw(fb, acc2, sizeof(vec4) * n);
+      std::fclose(fa);
+      std::fclose(fb);
+      std::printf("editor_centre %u\n", centre);
+    }
     ReleaseRayCounter(counters);
     ReleaseShadingRayData(srd);
     ReleaseHitData(hd);

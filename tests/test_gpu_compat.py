@@ -7,7 +7,9 @@ batches of MAX_RAY_COUNT rays, counters copied between host and device)
 for several frames with accumulation; it also renders the same frames
 through the C ABI directly. The two accumulated images must agree within
 the per-sample tolerance (the renders differ only in the order of
-per-pixel float additions).
+per-pixel float additions). The driver also runs the editor view through
+the three editor-view launchers with the editor's own loop and both
+post-processing launchers, against the direct C-ABI calls.
 """
 import os
 import shutil
@@ -47,11 +49,22 @@ def test_reference_stage_protocol_matches_direct_render(driver, cornell_path, ha
     perm_file = tmp_path / "perm.u32"
     np.ascontiguousarray(halton_perm, np.uint32).tofile(perm_file)
     a_file, b_file = tmp_path / "compat.f32", tmp_path / "direct.f32"
+    ea_file, eb_file = tmp_path / "editor_compat.bin", tmp_path / "editor_direct.bin"
     r = subprocess.run([driver, cornell_path, str(perm_file), str(w), str(h), "16", str(frames), str(max_frames),
-                        str(a_file), str(b_file)], capture_output=True, text=True, timeout=600)
+                        str(a_file), str(b_file), str(ea_file), str(eb_file)], capture_output=True, text=True,
+                       timeout=600)
     assert r.returncode == 0, r.stderr[-3000:]
     assert "generation_calls %d" % (4 * frames) in r.stdout, r.stdout
     a = np.fromfile(a_file, np.float32).reshape(h, w, 4)
     b = np.fromfile(b_file, np.float32).reshape(h, w, 4)
     assert a[..., :3].mean() > 0.01
     assert np.allclose(a, b, rtol=1e-5, atol=1e-6), np.abs(a - b).max()
+    # the editor view and post-processing through the reference-named launchers equal the direct calls
+    n = w * h
+    ea, eb = np.fromfile(ea_file, np.uint8), np.fromfile(eb_file, np.uint8)
+    assert ea.size == eb.size == n * (16 + 4 + 16 + 16)
+    assert np.array_equal(ea[:n * 20], eb[:n * 20])  # beauty and primitive index, bit for bit
+    assert (ea[n * 16:n * 20].view(np.uint32) != 0xFFFFFFFF).mean() > 0.5
+    assert np.array_equal(ea[n * 20:n * 36], eb[n * 20:n * 36])  # editor post-processing with the outline
+    pa, pb = ea[n * 36:].view(np.float32), eb[n * 36:].view(np.float32)
+    assert np.allclose(pa, pb, rtol=1e-5, atol=1e-6)  # path-traced image after tone mapping
