@@ -57,6 +57,10 @@ WORKLOADS = {
     # from its fBm node (maximum sigma_t 2.0); the reference has no grid node,
     # so its arms render the procedural form of the same medium
     "volumetric_grid": dict(scene="volumetric", width=1280, height=720, spp=32, depth=16, volume=True, grid=128),
+    # the Cornell-like scene with every solid texture node on material
+    # parameters, a checkerboard bump map, an rgb-noise normal map and a
+    # noise-density medium (the texture graph the reference evaluates per hit)
+    "textured": dict(scene="textured", width=1280, height=720, spp=32, depth=12, volume=True),
 }
 
 
@@ -511,7 +515,8 @@ def run_ours(args):
                        "sampler": "halton", "lights": "shape lights, NEE with MIS",
                        "media": (("fog box + smoke box with a 128^3 fp16 density grid (fBm, 4 octaves, max "
                                   "sigma_t 2.0), delta tracking") if wl.get("grid") else
-                                 "fog box + fBm smoke box, delta tracking") if wl.get("volume") else "none",
+                                 ("noise-density medium sphere, delta tracking" if wl["scene"] == "textured" else
+                                  "fog box + fBm smoke box, delta tracking")) if wl.get("volume") else "none",
                        "parallelism": f"replica x{world}" + (" + allreduce of frames" if world > 1 else ""),
                        "l2": "256 MB buffer written between steps; path queues (>1 GB) exceed L2",
                        "options": {"sort_hits": ctx.get_option("sort_hits"),
