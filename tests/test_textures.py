@@ -228,3 +228,23 @@ def test_image_nodes_from_arrays(scene_dir):
     with pytest.raises(Y.YmrtError) as e:
         Y.HostScene.from_arrays(64, 64, **kw)
     assert e.value.code == -1
+
+
+def test_corrupt_png_is_left_out_like_the_reference(tmp_path, halton_perm, oracle):
+    """A truncated PNG fails to decode in both loaders; the node is left out
+    and the material that names it keeps its constant albedo."""
+    s = scenes.cornell_scene(0)
+    s.image_files["broken.png"] = (np.full((8, 8, 3), 128, np.uint16), dict(depth=8, color_type=2))
+    s.textures.append(("ImageTexture", "broken", {"texture_file_name": "broken.png", "color_space": "SRGB"}))
+    mats = dict((name, i) for i, (_, name, _) in enumerate(s.materials))
+    kind, name, attrs = s.materials[mats["back_material"]]
+    s.materials[mats["back_material"]] = (kind, name, {**attrs, "diffuse_albedo_tex": "broken"})
+    path = scenes.write_scene(s, str(tmp_path / "broken_png.ymtmp"))
+    png = os.path.join(scenes.texture_folder(path), "broken.png")
+    data = open(png, "rb").read()
+    with open(png, "wb") as f:
+        f.write(data[: len(data) // 2])
+    ours, ref = Y.HostScene(path, 32, 32), oracle.RefScene(path, halton_perm, 32, 32)
+    assert ours.records("textures").shape[0] == 0 == ref.records("textures").shape[0]
+    assert np.array_equal(_meaningful("materials", ours.records("materials")),
+                          _meaningful("materials", ref.records("materials")))
