@@ -248,3 +248,30 @@ def test_corrupt_png_is_left_out_like_the_reference(tmp_path, halton_perm, oracl
     assert ours.records("textures").shape[0] == 0 == ref.records("textures").shape[0]
     assert np.array_equal(_meaningful("materials", ours.records("materials")),
                           _meaningful("materials", ref.records("materials")))
+
+
+def test_malformed_pngs_are_left_out(tmp_path, halton_perm, oracle):
+    """PNGs the reference's image library refuses (a tRNS chunk on an image
+    with alpha, a palette tRNS longer than the palette, an oversized header)
+    leave the node out here too."""
+    import struct
+    import zlib
+    s = scenes.cornell_scene(0)
+    cases = {"alpha_trns.png": (np.full((4, 4, 4), 9, np.uint16), dict(depth=8, color_type=6, trns=b"\0\1\0\2\0\3")),
+             "long_trns.png": (np.zeros((4, 4), np.uint16), dict(depth=8, color_type=3, palette=[[1, 2, 3]],
+                                                                  trns=b"\1\2"))}
+    for fname, img in cases.items():
+        s.image_files[fname] = img
+        s.textures.append(("ImageTexture", fname[:-4], {"texture_file_name": fname, "color_space": "Linear"}))
+    s.textures.append(("ImageTexture", "huge", {"texture_file_name": "huge.png", "color_space": "Linear"}))
+    path = scenes.write_scene(s, str(tmp_path / "bad_pngs.ymtmp"))
+
+    def chunk(kind, body):
+        return struct.pack(">I", len(body)) + kind + body + struct.pack(">I", zlib.crc32(kind + body) & 0xFFFFFFFF)
+
+    huge = b"\x89PNG\r\n\x1a\n" + chunk(b"IHDR", struct.pack(">IIBBBBB", 1 << 24, 1 << 24, 8, 2, 0, 0, 0))
+    huge += chunk(b"IDAT", zlib.compress(b"\0" * 64)) + chunk(b"IEND", b"")
+    with open(os.path.join(scenes.texture_folder(path), "huge.png"), "wb") as f:
+        f.write(huge)
+    assert Y.HostScene(path, 32, 32).records("textures").shape[0] == 0
+    assert oracle.RefScene(path, halton_perm, 32, 32).records("textures").shape[0] == 0

@@ -110,7 +110,8 @@ bool decode_png(const uint8_t* d, size_t size, PngImage* out, std::string* error
     at += 12 + (size_t)len;
   }
   if (ctype < 0) return fail(error, "missing IHDR");
-  if (w == 0 || h == 0 || w > (1u << 24) || h > (1u << 24)) return fail(error, "bad PNG size");
+  if (w == 0 || h == 0 || w > (1u << 24) || h > (1u << 24) || (uint64_t)w * h > (1ull << 28))
+    return fail(error, "bad PNG size");
   int file_n;
   switch (ctype) {
     case 0: file_n = 1; break;
@@ -125,6 +126,8 @@ bool decode_png(const uint8_t* d, size_t size, PngImage* out, std::string* error
                         ((ctype == 2 || ctype == 4 || ctype == 6) && (depth == 8 || depth == 16));
   if (!depth_ok) return fail(error, "bad PNG bit depth");
   if (ctype == 3 && (palette.empty() || palette.size() % 3 != 0)) return fail(error, "missing PNG palette");
+  if (have_trns && (ctype == 4 || ctype == 6)) return fail(error, "PNG tRNS chunk on an image with alpha");
+  if (have_trns && ctype == 3 && trns.size() > palette.size() / 3) return fail(error, "PNG tRNS chunk longer than the palette");
 
   // passes: x0, y0, dx, dy (Adam7, or one pass)
   static const int kAdam7[7][4] = {{0, 0, 8, 8}, {4, 0, 8, 8}, {0, 4, 4, 8}, {2, 0, 4, 4},

@@ -12,6 +12,7 @@
 #include <cstring>
 #include <fstream>
 #include <functional>
+#include <new>
 #include <sstream>
 #include <type_traits>
 #include <unordered_map>
@@ -986,7 +987,12 @@ int load_image_texture(const std::string& path, uint32_t color_space, Texture* t
     }
   }
   PngImage img;
-  if (!decode_png_file(path, &img, error)) return YMRT_ERR_IO;
+  try {
+    if (!decode_png_file(path, &img, error)) return YMRT_ERR_IO;
+  } catch (const std::bad_alloc&) {
+    if (error) *error = path + ": out of memory decoding the image";
+    return YMRT_ERR_IO;
+  }
   std::memset(t, 0, sizeof(*t));
   t->type = kTexImage;
   t->child[0] = t->child[1] = kEmpty;
