@@ -87,7 +87,9 @@ typedef struct ymrt_stats {
   double ms_extend;          /* closest-hit kernel */
   double ms_shade;           /* shading kernel */
   uint32_t device_errors;    /* bit set of YMRT_DEVERR_* raised on the device */
-  uint32_t reserved_;
+  uint32_t tracking_bound_hits; /* delta / ratio tracking loops that stopped at the reference's
+                                   MAX_FREE_PATH_LENGTH (2048 steps, src/VolumeEval.cuh:16, :144,
+                                   :328), as the reference's do: not an error */
   uint64_t shadow_node_visits;     /* the part of node_visits made by occlusion queries */
   uint64_t shadow_triangle_tests;  /* the part of triangle_tests made by occlusion queries */
   double ms_sort;            /* hit listing by shading bucket (profiling on) */
@@ -97,7 +99,9 @@ typedef struct ymrt_stats {
 
 #define YMRT_DEVERR_STACK 1u     /* a traversal stack overflowed (entries were dropped) */
 #define YMRT_DEVERR_QUEUE 2u     /* a path queue overflowed */
-#define YMRT_DEVERR_ITER 4u      /* a bounded loop hit its iteration cap */
+#define YMRT_DEVERR_ITER 4u      /* a bound of this library's own (shadow-ray boundary crossings, waves of a
+                                    frame, editor-view boundaries) was reached; the render returns
+                                    YMRT_ERR_OVERFLOW */
 
 /* ---- contexts ---- */
 int ymrt_create(int device_ordinal, ymrt_context** out);
@@ -414,6 +418,18 @@ int ymrt_host_scene_set_image(ymrt_host_scene* scene, uint32_t texture_index, co
  * points of 5 floats each: texture coordinates s, t and the object-space
  * position x, y, z (host buffers): known-answer checks of every node type. */
 int ymrt_debug_texture(ymrt_scene* scene, uint32_t texture_index, int n, const float* coords, float* rgb);
+/* Where a bounded device loop last gave up (the event behind
+ * YMRT_DEVERR_ITER; no counterpart in the reference, whose loops have no
+ * bound): the first such event on the context's device since the record was
+ * last cleared, as 32-bit words -- taken (0: none, 1: written), site
+ * (1 shadow-ray boundary crossings, 2 delta-tracking steps, 3 ratio-tracking
+ * steps, 4 waves of a frame, 5 editor-view boundaries, 6 texture-graph walk),
+ * the iteration count, the ray's last instance and triangle, origin (3
+ * floats), direction (3), remaining length, the tracking majorant (3) and
+ * channel, then its nested-media stack (max-priority index, record count,
+ * 6 records of prim, ior, priority, volume). words receives up to n_words
+ * words (42 in all); clear != 0 resets the record afterwards. */
+int ymrt_debug_bound_record(ymrt_context* ctx, uint32_t* words, size_t n_words, int clear);
 int ymrt_debug_occluded(ymrt_scene* scene, int n, const float* origin, const float* dir, const float* tmax,
                         int* occluded);
 int ymrt_debug_halton(ymrt_scene* scene, int n, const int* px, const int* py, const int* sample, int n_dims,

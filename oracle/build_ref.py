@@ -200,9 +200,87 @@ def _sampler_headers(arg_order: str, gen_dir: str) -> int:
         f.write(f'#line 1 "{os.path.join(src_dir, "RandomSampler.cuh")}"\n' + text)
     with open(os.path.join(src_dir, "VolumeEval.cuh"), "r", encoding="utf-8", errors="replace") as f:
         vol = f.read()
+    vol = _media_hooks(vol)
     with open(os.path.join(gen_dir, "VolumeEval.cuh"), "w") as f:
         f.write(f'#line 1 "{os.path.join(src_dir, "VolumeEval.cuh")}"\n' + vol)
     return n
+
+
+# Media hooks in the build-time copy of VolumeEval.cuh (no change to the
+# estimators): a medium's density node may be replaced by a 3-D density grid
+# (this project's grid node, which the reference lacks: trilinear over cell
+# centres of the object-space box [-0.5, 0.5]^3 with clamped edges, upper
+# bound = the grid's maximum, in the same operand order as ymrt_b200's
+# grid_eval), and the two "Max iteration reached" messages of the tracking
+# loops (MAX_FREE_PATH_LENGTH steps, src/VolumeEval.cuh:144, 328) are counted
+# instead of printed, so tests can compare how often each side reaches that
+# bound.
+_MEDIA_HOOKS = r'''
+// ---- inserted by oracle/build_ref.py: density grids, tracking-bound counts ----
+struct YmrtOracleGrid {
+  const Texture* node;
+  int n[3];
+  std::vector<float> v;
+  float vmax;
+};
+inline std::vector<YmrtOracleGrid>& ymrt_oracle_grids() {
+  static std::vector<YmrtOracleGrid> g;
+  return g;
+}
+inline std::atomic<unsigned long long>& ymrt_oracle_tracking_caps() {
+  static std::atomic<unsigned long long> c{0};
+  return c;
+}
+inline const YmrtOracleGrid* ymrt_oracle_find_grid(const Texture& t) {
+  for (const YmrtOracleGrid& g : ymrt_oracle_grids())
+    if (g.node == &t) return &g;
+  return nullptr;
+}
+inline void ymrt_oracle_grid_axis(float p, int n, int* i0, int* i1, float* w) {
+  const float g = (p + 0.5f) * (float)n - 0.5f;
+  if (!(g > 0.0f)) { *i0 = *i1 = 0; *w = 0.0f; }
+  else if (!(g < (float)(n - 1))) { *i0 = *i1 = n - 1; *w = 0.0f; }
+  else { const float fl = std::floor(g); *i0 = (int)fl; *i1 = *i0 + 1; *w = g - fl; }
+}
+inline float ymrt_oracle_lerp(float a, float b, float w) { return a + w * (b - a); }
+inline float ymrt_oracle_grid_eval(const YmrtOracleGrid& G, const glm::vec3& p) {
+  int x0, x1, y0, y1, z0, z1;
+  float wx, wy, wz;
+  ymrt_oracle_grid_axis(p.x, G.n[0], &x0, &x1, &wx);
+  ymrt_oracle_grid_axis(p.y, G.n[1], &y0, &y1, &wy);
+  ymrt_oracle_grid_axis(p.z, G.n[2], &z0, &z1, &wz);
+  auto at = [&](int x, int y, int z) { return G.v[((size_t)z * G.n[1] + y) * G.n[0] + x]; };
+  const float c00 = ymrt_oracle_lerp(at(x0, y0, z0), at(x1, y0, z0), wx);
+  const float c10 = ymrt_oracle_lerp(at(x0, y1, z0), at(x1, y1, z0), wx);
+  const float c01 = ymrt_oracle_lerp(at(x0, y0, z1), at(x1, y0, z1), wx);
+  const float c11 = ymrt_oracle_lerp(at(x0, y1, z1), at(x1, y1, z1), wx);
+  return ymrt_oracle_lerp(ymrt_oracle_lerp(c00, c10, wy), ymrt_oracle_lerp(c01, c11, wy), wz);
+}
+inline glm::vec3 ymrt_oracle_density(const Texture& t, const Texture* textures, const ImageTileCache& cache,
+                                     const TextureCoordinate& tc) {
+  if (const YmrtOracleGrid* g = ymrt_oracle_find_grid(t)) return glm::vec3(ymrt_oracle_grid_eval(*g, tc.p_object));
+  return TextureEval(t, textures, cache, tc);
+}
+inline float ymrt_oracle_upper_bound(const Texture& t, const glm::vec3& o, const glm::vec3& d, float t_max) {
+  if (const YmrtOracleGrid* g = ymrt_oracle_find_grid(t)) return g->vmax;
+  return t.GetUpperBound(o, d, t_max);
+}
+// ---- end of insertion ----
+'''
+
+
+def _media_hooks(text: str) -> str:
+    i = text.index("namespace YMRT {") + len("namespace YMRT {")
+    line = text[:i].count("\n") + 2
+    text = (text[:i] + _MEDIA_HOOKS + f'#line {line}\n' + text[i:])
+    text, a = re.subn(r"\bTextureEval\(density_texture,", "ymrt_oracle_density(density_texture,", text)
+    text, b = re.subn(r"scene\.textures\[vol\.density_texture_idx\]\.GetUpperBound\(",
+                      "ymrt_oracle_upper_bound(scene.textures[vol.density_texture_idx], ", text)
+    text, c = re.subn(r'printf\("Max iteration reached at (SampleTrHeterogeneous|EvalTrHeterogeneous)!\\n"\);',
+                      "ymrt_oracle_tracking_caps().fetch_add(1, std::memory_order_relaxed);", text)
+    if (a, b, c) != (2, 2, 2):
+        raise RuntimeError(f"VolumeEval.cuh hooks: {a} density, {b} bound, {c} cap sites (expected 2 each)")
+    return "#include <atomic>\n#include <cmath>\n#include <vector>\n" + text
 
 
 # ---------------------------------------------------------------------------
@@ -510,7 +588,7 @@ def build_fp64(force: bool = False, jobs: int = 8) -> str:
     for src, obj, extra in jobs_list:
         # assimp's material getters are called with the (now double) colour
         # arrays of the model importer; its double-precision mode types them
-        cmd = ["g++"] + CXXFLAGS + ["-DASSIMP_DOUBLE_PRECISION"] + extra + inc + ["-c", src, "-o", obj]
+        cmd = ["g++"] + CXXFLAGS + ["-DASSIMP_DOUBLE_PRECISION", "-DYMREF_FP64"] + extra + inc + ["-c", src, "-o", obj]
         procs.append((src, subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT)))
         objs.append(obj)
         while len([p for _, p in procs if p.poll() is None]) >= jobs:

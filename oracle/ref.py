@@ -66,6 +66,12 @@ def _bind(L, settings_type):
     L.ymref_sobol_matrices.argtypes = [vp, ctypes.c_size_t]
     L.ymref_trace.argtypes = [vp, i, vp, vp, vp, vp, vp, vp, vp, vp, vp]
     L.ymref_occluded.argtypes = [vp, i, vp, vp, vp, vp]
+    L.ymref_set_density_grid.argtypes = [vp, ctypes.c_uint32, i, i, i, vp]
+    L.ymref_density.argtypes = [vp, ctypes.c_uint32, i, vp, vp]
+    L.ymref_tracking_caps.restype = ctypes.c_ulonglong
+    L.ymref_tracking_caps.argtypes = [i]
+    if hasattr(L, "ymref_boundary_walk"):
+        L.ymref_boundary_walk.argtypes = [vp, vp, vp, ctypes.c_float, ctypes.c_uint32, ctypes.c_uint32, vp, i, vp]
     L.ymref_halton.argtypes = [vp, i, vp, vp, vp, i, vp, vp, vp]
     L.ymref_render_frame.argtypes = [vp, i, i, i, i, i, vp]
     L.ymref_last_render_seconds.restype = ctypes.c_double
@@ -288,6 +294,39 @@ class RefScene:
         out = np.zeros(o.shape[0], np.int32)
         self._L.ymref_occluded(self.h, o.shape[0], _p(o), _p(d), _p(tm), _p(out))
         return out
+
+    def set_density_grid(self, texture_index: int, values) -> None:
+        """Replaces density node `texture_index` with a 3-D grid (values of
+        shape (nz, ny, nx), x fastest), as ymrt_scene_set_density_grid does;
+        pass the values the device stores (float16-rounded for a half grid)."""
+        v = np.ascontiguousarray(values, self._f)
+        nz, ny, nx = v.shape
+        assert self._L.ymref_set_density_grid(self.h, texture_index, nx, ny, nz, _p(v)) == 0
+
+    def density(self, texture_index: int, points) -> np.ndarray:
+        """A medium's density node (or attached grid) at object-space points
+        (n, 3), as the tracking loops read it."""
+        p = np.ascontiguousarray(points, self._f).reshape(-1, 3)
+        out = np.zeros(p.shape[0], self._f)
+        assert self._L.ymref_density(self.h, texture_index, p.shape[0], _p(p), _p(out)) == 0
+        return out
+
+    def tracking_caps(self, reset: bool = True) -> int:
+        """Tracking loops that reached MAX_FREE_PATH_LENGTH steps (all scenes
+        of this library) since the last reset."""
+        return int(self._L.ymref_tracking_caps(int(reset)))
+
+    def boundary_walk(self, origin, direction, tmax, last_inst, last_tri, transfer_words, max_steps=1024) -> np.ndarray:
+        """Boundary crossings of one shadow ray as the reference's TraceTr
+        follows them: one row per crossing (instance, triangle, t, back,
+        nearby count, stack records after it, distance traced)."""
+        o = np.ascontiguousarray(origin, np.float32)
+        d = np.ascontiguousarray(direction, np.float32)
+        tw = np.ascontiguousarray(transfer_words, np.uint32)
+        out = np.zeros((max_steps, 8), np.uint32)
+        n = self._L.ymref_boundary_walk(self.h, _p(o), _p(d), float(tmax), last_inst, last_tri, _p(tw), max_steps,
+                                        _p(out))
+        return out[:n]
 
     def halton(self, px, py, sample, n_dims: int):
         px = np.ascontiguousarray(px, np.int32)

@@ -27,6 +27,7 @@
 #include "core/YMParser.h"
 
 #include <atomic>
+#include <cstring>
 #include <chrono>
 #include <thread>
 
@@ -156,7 +157,14 @@ void* ymref_scene_load(const char* path, const uint32_t* halton_perm, size_t per
   return ctx;
 }
 
-void ymref_scene_free(void* handle) { delete static_cast<RefContext*>(handle); }
+void ymref_scene_free(void* handle) {
+  auto ctx = static_cast<RefContext*>(handle);
+  auto& grids = ymrt_oracle_grids();
+  for (size_t i = grids.size(); i-- > 0;)
+    if (grids[i].node >= ctx->scene.textures && grids[i].node < ctx->scene.textures + ctx->scene.texture_count)
+      grids.erase(grids.begin() + i);
+  delete ctx;
+}
 
 void ymref_set_settings(void* handle, const YmrefSettings* s) {
   auto ctx = static_cast<RefContext*>(handle);
@@ -558,6 +566,111 @@ int ymref_occluded(void* handle, int n, const float* origin, const float* dir, c
     occluded[i] = BVHTraverseShadow(ctx->scene, ray, &rec) ? 1 : 0;
   }
   return 0;
+}
+
+// The boundary crossings of one shadow ray as the reference's TraceTr
+// follows them (src/VolumeEval.cuh:420-468: TraceVolume, the nested-media
+// update BoundaryTransitionBunch and OffsetRayOrigin), without the
+// transmittance estimates, which do not move the ray. The ray starts at
+// origin / dir (already offset) leaving last_inst / last_tri, with `tmax` of
+// its length left and the nested-media stack `transfer` (the reference's
+// RayTransfer as 32-bit words: max-priority index, record count, then 6
+// records of prim, ior bits, priority, volume). At most max_steps crossings;
+// per crossing 8 words: instance, triangle, t bits, back flag, nearby count,
+// stack record count after it, and the distance traced so far (bits).
+// Returns the number of crossings (the walk ends when the ray passes tmax or
+// hits nothing). Float build only.
+#ifndef YMREF_FP64
+int ymref_boundary_walk(void* handle, const float* origin, const float* dir, float tmax, uint32_t last_inst,
+                        uint32_t last_tri, const uint32_t* transfer, int max_steps, uint32_t* out) {
+  auto ctx = static_cast<RefContext*>(handle);
+  const Scene& scene = ctx->scene;
+  RayTransfer rt;
+  rt.max_priority_record_index = (int)transfer[0];
+  rt.record_count = (int)transfer[1];
+  for (int r = 0; r < rt.record_count && r < MAX_BOUNDARY_RECORD; ++r) {
+    const uint32_t* w = transfer + 2 + 4 * r;
+    float ior;
+    std::memcpy(&ior, w + 1, 4);
+    rt.boundary_records[r] = BoundaryRecord(w[0], ior, w[2], (int)w[3]);
+  }
+  Ray tr_ray(glm::vec3(origin[0], origin[1], origin[2]), glm::vec3(dir[0], dir[1], dir[2]), last_inst, last_tri);
+  float traced = TMIN;
+  int n = 0;
+  while (traced < tmax && n < max_steps) {
+    HitRecord rec;
+    int nearby_count = 0;
+    NearbyHit nearby[MAX_BOUNDARY_RECORD + 2];
+    if (!TraceVolume(scene, tr_ray, &rec, &nearby_count, nearby)) break;
+    traced += rec.hit_t;
+    glm::vec3 p(0.0f), perr(0.0f), ng(0.0f);
+    FetchGeometryNormal(scene, rec, &p, &perr, &ng);
+    BoundaryTransitionBunch(rt, scene.primitive_instances, scene.materials, nearby, nearby_count);
+    tr_ray = Ray(OffsetRayOrigin(p, perr, tr_ray.direction, ng), tr_ray.direction, rec.hit_instance_idx,
+                 rec.hit_triangle_idx);
+    uint32_t* o = out + 8 * (size_t)n;
+    o[0] = rec.hit_instance_idx;
+    o[1] = rec.hit_triangle_idx;
+    std::memcpy(o + 2, &rec.hit_t, 4);
+    o[3] = rec.hit_back ? 1u : 0u;
+    o[4] = (uint32_t)nearby_count;
+    o[5] = (uint32_t)rt.record_count;
+    std::memcpy(o + 6, &traced, 4);
+    o[7] = 0;
+    ++n;
+  }
+  return n;
+}
+#endif
+
+// Replaces the density node `tex` of the scene with a 3-D grid of nx*ny*nz
+// values (x fastest) over the object-space box [-0.5, 0.5]^3 (this project's
+// grid node; the reference has none): media read it trilinearly with clamped
+// edges and track against its maximum (oracle/build_ref.py, _MEDIA_HOOKS).
+// Calling it again for the same node replaces the grid.
+int ymref_set_density_grid(void* handle, uint32_t tex, int nx, int ny, int nz, const float* values) {
+  auto ctx = static_cast<RefContext*>(handle);
+  if (tex >= ctx->scene.texture_count || nx < 1 || ny < 1 || nz < 1) return -1;
+  const Texture* node = &ctx->scene.textures[tex];
+  auto& grids = ymrt_oracle_grids();
+  for (size_t i = 0; i < grids.size(); ++i)
+    if (grids[i].node == node) {
+      grids.erase(grids.begin() + i);
+      break;
+    }
+  YmrtOracleGrid g;
+  g.node = node;
+  g.n[0] = nx;
+  g.n[1] = ny;
+  g.n[2] = nz;
+  g.v.assign(values, values + (size_t)nx * ny * nz);
+  g.vmax = 0.0f;
+  for (const auto v : g.v) g.vmax = std::max(g.vmax, v);
+  grids.push_back(std::move(g));
+  return 0;
+}
+
+// A medium's density as the build-time copy of VolumeEval.cuh reads it
+// (the grid node when one is attached to `tex`, else the reference's
+// TextureEval), at n object-space points (3 floats each).
+int ymref_density(void* handle, uint32_t tex, int n, const float* points, float* out) {
+  auto ctx = static_cast<RefContext*>(handle);
+  if (tex >= ctx->scene.texture_count) return -1;
+  ImageTileCache cache;
+  cache.image_tiles_host = GuiModule::ImageTiles(*ctx->module).data();
+  const Texture& t = ctx->scene.textures[tex];
+  for (int i = 0; i < n; ++i) {
+    const glm::vec3 p(points[3 * i], points[3 * i + 1], points[3 * i + 2]);
+    const TextureCoordinate tc(glm::vec2(0.0f), p, p);
+    out[i] = ymrt_oracle_density(t, ctx->scene.textures, cache, tc).x;
+  }
+  return 0;
+}
+
+// Tracking loops (delta and ratio tracking) that reached the reference's
+// MAX_FREE_PATH_LENGTH bound since the last reset, over every render.
+unsigned long long ymref_tracking_caps(int reset) {
+  return reset ? ymrt_oracle_tracking_caps().exchange(0) : ymrt_oracle_tracking_caps().load();
 }
 
 // Halton sampler known-answer values: for each (px, py, sample) the global

@@ -87,7 +87,7 @@ class Stats(ctypes.Structure):
         ("waves", ctypes.c_uint64), ("node_visits", ctypes.c_uint64), ("triangle_tests", ctypes.c_uint64),
         ("kernel_launches", ctypes.c_uint64), ("ms_total", ctypes.c_double), ("ms_generate", ctypes.c_double),
         ("ms_extend", ctypes.c_double), ("ms_shade", ctypes.c_double), ("device_errors", ctypes.c_uint32),
-        ("reserved_", ctypes.c_uint32), ("shadow_node_visits", ctypes.c_uint64),
+        ("tracking_bound_hits", ctypes.c_uint32), ("shadow_node_visits", ctypes.c_uint64),
         ("shadow_triangle_tests", ctypes.c_uint64), ("ms_sort", ctypes.c_double), ("ms_connect", ctypes.c_double),
         ("shaded_hits", ctypes.c_uint64),
     ]
@@ -149,6 +149,7 @@ def library():
     L.ymrt_debug_trace.argtypes = [vp, i, vp, vp, vp, vp, vp, vp, vp, vp, vp]
     L.ymrt_debug_occluded.argtypes = [vp, i, vp, vp, vp, vp]
     L.ymrt_debug_halton.argtypes = [vp, i, vp, vp, vp, i, vp, vp, vp]
+    L.ymrt_debug_bound_record.argtypes = [vp, vp, sz, i]
     _lib = L
     return L
 
@@ -189,6 +190,25 @@ class Context:
         v = ctypes.c_int()
         _check(library().ymrt_get_option(self.h, OPTIONS[name], ctypes.byref(v)))
         return v.value
+
+    BOUND_SITES = {1: "shadow-ray boundary crossings", 2: "delta-tracking steps", 3: "ratio-tracking steps",
+                   4: "waves of a frame", 5: "editor-view boundaries", 6: "texture-graph walk"}
+
+    def bound_record(self, clear: bool = True) -> dict | None:
+        """Where a bounded device loop last gave up (YMRT_DEVERR_ITER) on this
+        context's device, with the ray it was following; None when none did."""
+        w = np.zeros(64, np.uint32)
+        _check(library().ymrt_debug_bound_record(self.h, _p(w), w.size, int(clear)), self.h)
+        if w[0] == 0:
+            return None
+        f = w.view(np.float32)
+        rec = np.array(w[18:18 + 24]).reshape(6, 4)
+        return {"site": int(w[1]), "what": self.BOUND_SITES.get(int(w[1]), "?"), "count": int(w[2]),
+                "last_inst": int(w[3]), "last_tri": int(w[4]), "o": f[5:8].copy(), "d": f[8:11].copy(),
+                "tmax": float(f[11]), "majorant": f[12:15].copy(), "channel": float(f[15]),
+                "max_priority_index": int(w[16].view(np.int32)), "record_count": int(w[17].view(np.int32)),
+                "records": [(int(r[0]), float(r[1:2].view(np.float32)[0]), int(r[2]), int(r[3:4].view(np.int32)[0]))
+                            for r in rec[:max(0, min(6, int(w[17].view(np.int32))))]]}
 
     def close(self):
         if self.h:

@@ -11,6 +11,7 @@
 #include <functional>
 #include <map>
 #include <memory>
+#include <condition_variable>
 #include <mutex>
 #include <new>
 #include <string>
@@ -215,6 +216,43 @@ uint32_t shading_bucket(const HostScene& s, const Instance& inst) {
 
 }  // namespace
 
+namespace {
+
+// Constant-memory scene slots (kMaxSceneSlots per device) are shared by every
+// context on a device. A call leases the slots it uploads scenes into for as
+// long as its kernels may read them, so that calls from several contexts on
+// one device (one context per host thread) never overwrite each other's
+// scenes; it waits while another call holds too many. The lease ends after
+// the call's stream is synchronised.
+struct DeviceSlots {
+  std::mutex m;
+  std::condition_variable cv;
+  uint64_t used = 0;  // bit k: slot k leased
+};
+DeviceSlots g_device_slots[128];
+
+class SlotLease {
+ public:
+  SlotLease(ymrt_context* ctx, uint32_t n);
+  ~SlotLease();
+  SlotLease(const SlotLease&) = delete;
+  SlotLease& operator=(const SlotLease&) = delete;
+  bool ok() const { return ok_; }
+  const uint32_t* slots() const { return slots_; }
+  uint32_t slot(size_t k) const { return slots_[k]; }
+  // Uploads scenes[k] into the k-th leased slot (and the prime tables).
+  cudaError_t upload(const DeviceScene* scenes, uint32_t n) const;
+
+ private:
+  ymrt_context* ctx_;
+  uint64_t mask_ = 0;
+  uint32_t slots_[kMaxSceneSlots] = {};
+  uint32_t n_ = 0;
+  bool ok_ = false;
+};
+
+}  // namespace
+
 struct ymrt_scene {
   ymrt_context* ctx = nullptr;
   DeviceScene dev{};
@@ -236,6 +274,40 @@ struct ymrt_scene {
     return e;
   }
 };
+
+namespace {
+
+SlotLease::SlotLease(ymrt_context* ctx, uint32_t n) : ctx_(ctx) {
+  if (n == 0 || n > kMaxSceneSlots || ctx->device < 0 || ctx->device >= 128) return;
+  DeviceSlots& d = g_device_slots[ctx->device];
+  std::unique_lock<std::mutex> lk(d.m);
+  d.cv.wait(lk, [&] { return (uint32_t)__builtin_popcountll(~d.used) >= n; });
+  for (uint32_t k = 0; k < kMaxSceneSlots && n_ < n; ++k)
+    if (!((d.used >> k) & 1ull)) {
+      slots_[n_++] = k;
+      mask_ |= 1ull << k;
+    }
+  d.used |= mask_;
+  ok_ = true;
+}
+
+SlotLease::~SlotLease() {
+  if (!mask_) return;
+  cudaStreamSynchronize(ctx_->stream);  // no kernel of this call reads the slots any more
+  DeviceSlots& d = g_device_slots[ctx_->device];
+  {
+    std::lock_guard<std::mutex> lk(d.m);
+    d.used &= ~mask_;
+  }
+  d.cv.notify_all();
+}
+
+cudaError_t SlotLease::upload(const DeviceScene* scenes, uint32_t n) const {
+  if (!ok_ || n > n_) return cudaErrorInvalidValue;
+  return upload_constants(scenes, slots_, n, ctx_->primes.data(), ctx_->prime_sums.data(), ctx_->stream);
+}
+
+}  // namespace
 
 extern "C" {
 
@@ -845,6 +917,7 @@ void total_counters_add(ymrt_context* ctx, bool first) {
   const WaveCounters& c = *ctx->counters_host;
   if (first) t = WaveCounters{};
   t.errors |= c.errors;
+  t.tracking_caps += c.tracking_caps;
   t.extension_rays += c.extension_rays;
   t.shadow_rays += c.shadow_rays;
   t.tri_tests += c.tri_tests;
@@ -876,9 +949,13 @@ int finish_batch(ymrt_context* ctx, const BatchResult& r, ymrt_stats* stats) {
     stats->ms_shade = r.stage_ms[3];
     stats->ms_connect = r.stage_ms[4];
     stats->device_errors = c.errors;
+    stats->tracking_bound_hits = c.tracking_caps;
   }
   if (c.errors & kDevErrQueue) return ctx->fail(YMRT_ERR_OVERFLOW, "path queue overflow on the device");
   if (c.errors & kDevErrStack) return ctx->fail(YMRT_ERR_OVERFLOW, "traversal or nested-media stack overflow on the device");
+  if (c.errors & kDevErrIter)
+    return ctx->fail(YMRT_ERR_OVERFLOW, "a bounded device loop reached its limit (shadow-ray boundary crossings or "
+                                        "waves of a frame; ymrt_debug_bound_record tells which)");
   return YMRT_OK;
 }
 
@@ -957,10 +1034,11 @@ int ymrt_render_tiles(ymrt_scene* sc, const ymrt_render_setting* setting, int fr
   WaveOptions opt;
   if ((rc = batch_options(ctx, jobs, &opt)) != YMRT_OK) return rc;
   opt.features = batch_features(&scene, 1);
-  jobs[0].scene_slot = 0;
-  if ((e = upload_constants(&scene, 1, ctx->primes.data(), ctx->prime_sums.data(), st)) != cudaSuccess)
-    return ctx->cuda_fail(e, "uploading constants");
-  cudaMemsetAsync(image, 0, img_bytes, st);
+  SlotLease lease(ctx, 1);
+  if (!lease.ok()) return ctx->fail(YMRT_ERR_INVALID, "no constant-memory scene slot for this device");
+  jobs[0].scene_slot = lease.slot(0);
+  if ((e = lease.upload(&scene, 1)) != cudaSuccess) return ctx->cuda_fail(e, "uploading constants");
+  if ((e = cudaMemsetAsync(image, 0, img_bytes, st)) != cudaSuccess) return ctx->cuda_fail(e, "clearing the image");
   BatchResult r;
   if ((rc = run_batch(ctx, M, jobs, opt, ctx->profiling, ctx->graph_loop, &r)) != YMRT_OK) return rc;
   if (!out_on_device) {
@@ -1020,8 +1098,10 @@ int ymrt_render_batch(ymrt_context* ctx, const ymrt_job* jobs_in, int n_jobs, ym
     WaveOptions opt;
     if ((rc = batch_options(ctx, jobs, &opt)) != YMRT_OK) return rc;
     opt.features = batch_features(slots.data(), slots.size());
-    if ((e = upload_constants(slots.data(), (uint32_t)slots.size(), ctx->primes.data(), ctx->prime_sums.data(), st)) !=
-        cudaSuccess)
+    SlotLease lease(ctx, (uint32_t)slots.size());
+    if (!lease.ok()) return ctx->fail(YMRT_ERR_INVALID, "no constant-memory scene slots for this device");
+    for (JobDesc& j : jobs) j.scene_slot = lease.slot(j.scene_slot);
+    if ((e = lease.upload(slots.data(), (uint32_t)slots.size())) != cudaSuccess)
       return ctx->cuda_fail(e, "uploading constants");
     BatchResult r;
     if ((rc = run_batch(ctx, M, jobs, opt, ctx->profiling, ctx->graph_loop, &r)) != YMRT_OK) return rc;
@@ -1101,8 +1181,10 @@ int ymrt_render_backward_ex(ymrt_context* ctx, const ymrt_job* jobs_in, int n_jo
   opt.grad_materials = materials ? tg->n_materials : 0;
   opt.grid_grads = grid ? tg->grid_grads_device : nullptr;
   opt.grid_tex = grid ? tg->grid_texture : kEmpty;
-  if ((e = upload_constants(slots.data(), (uint32_t)slots.size(), ctx->primes.data(), ctx->prime_sums.data(), st)) !=
-      cudaSuccess)
+  SlotLease lease(ctx, (uint32_t)slots.size());
+  if (!lease.ok()) return ctx->fail(YMRT_ERR_INVALID, "no constant-memory scene slots for this device");
+  for (JobDesc& j : jobs) j.scene_slot = lease.slot(j.scene_slot);
+  if ((e = lease.upload(slots.data(), (uint32_t)slots.size())) != cudaSuccess)
     return ctx->cuda_fail(e, "uploading constants");
   if (materials) cudaMemsetAsync(tg->material_grads_device, 0, sizeof(float) * kGradParams * tg->n_materials, st);
   if (grid) cudaMemsetAsync(tg->grid_grads_device, 0, sizeof(float) * tg->grid_values, st);
@@ -1307,14 +1389,16 @@ int ymrt_render_tiles_noalloc(ymrt_scene* sc, const ymrt_render_setting* setting
                               int tile_end, float* out_rgba_device, ymrt_stats* stats) {
   if (!sc || !setting || !out_rgba_device) return YMRT_ERR_INVALID;
   ymrt_context* ctx = sc->ctx;
-  if (setting->enable_distant_light) return ctx->fail(YMRT_ERR_UNSUPPORTED, "distant lights are not supported yet");
-  if (setting->enable_volume_scattering) return ctx->fail(YMRT_ERR_UNSUPPORTED, "volume scattering is not supported yet");
   std::vector<JobDesc> jobs(1);
   DeviceScene scene;
   int rc = make_job(ctx, sc, setting, frame_index, tile_begin, tile_end, reinterpret_cast<float4*>(out_rgba_device),
                     &jobs[0], &scene);
   if (rc != YMRT_OK) return rc;
-  jobs[0].scene_slot = 0;
+  // (make_job has already turned off what the scene lacks, as for ymrt_render_tiles)
+  if (jobs[0].setting.enable_distant_light)
+    return ctx->fail(YMRT_ERR_UNSUPPORTED, "ymrt_render_tiles_noalloc: distant lights are not rendered by this entry point");
+  if (jobs[0].setting.enable_volume_scattering)
+    return ctx->fail(YMRT_ERR_UNSUPPORTED, "ymrt_render_tiles_noalloc: volume scattering is not rendered by this entry point");
   const uint32_t spp = jobs[0].spp;
   const uint32_t per_tile = (uint32_t)kTilePixels * spp;
   const uint32_t cap = noalloc_capacity();
@@ -1343,11 +1427,16 @@ int ymrt_render_tiles_noalloc(ymrt_scene* sc, const ymrt_render_setting* setting
     return ctx->fail(YMRT_ERR_OVERFLOW, "scratch layout exceeds the fixed array");
   M.capacity = cap;
   cudaStream_t st = ctx->stream;
-  if ((e = upload_constants(&scene, 1, ctx->primes.data(), ctx->prime_sums.data(), st)) != cudaSuccess)
-    return ctx->cuda_fail(e, "uploading constants");
-  cudaMemsetAsync(out_rgba_device, 0, (size_t)sc->width * sc->height * sizeof(float4), st);
+  SlotLease lease(ctx, 1);
+  if (!lease.ok()) return ctx->fail(YMRT_ERR_INVALID, "no constant-memory scene slot for this device");
+  jobs[0].scene_slot = lease.slot(0);
+  if ((e = lease.upload(&scene, 1)) != cudaSuccess) return ctx->cuda_fail(e, "uploading constants");
+  if ((e = cudaMemsetAsync(out_rgba_device, 0, (size_t)sc->width * sc->height * sizeof(float4), st)) != cudaSuccess)
+    return ctx->cuda_fail(e, "clearing the image");
+  WaveOptions opt;
+  opt.features = batch_features(&scene, 1);
   BatchResult r;
-  if ((rc = run_batch(ctx, M, jobs, WaveOptions{}, false, false, &r)) != YMRT_OK) return rc;
+  if ((rc = run_batch(ctx, M, jobs, opt, false, false, &r)) != YMRT_OK) return rc;
   if ((e = cudaMemcpyAsync(ctx->counters_host, M.counters, sizeof(WaveCounters), cudaMemcpyDeviceToHost, st)) !=
       cudaSuccess)
     return ctx->cuda_fail(e, "reading counters");
@@ -1626,8 +1715,10 @@ int ymrt_debug_trace(ymrt_scene* sc, int n, const float* origin, const float* di
   uint32_t* d_err = sg.out<uint32_t>(1);
   if (sg.err != cudaSuccess) return ctx->cuda_fail(sg.err, "staging");
   cudaMemsetAsync(d_err, 0, sizeof(uint32_t), ctx->stream);
-  upload_constants(&sc->dev, 1, ctx->primes.data(), ctx->prime_sums.data(), ctx->stream);
-  launch_debug_trace(n, d_o, d_d, d_lh, d_inst, d_tri, d_t, d_b, d_back, d_nb, d_err, ctx->stream);
+  SlotLease lease(ctx, 1);
+  if (!lease.ok()) return ctx->fail(YMRT_ERR_INVALID, "no constant-memory scene slot for this device");
+  if (const cudaError_t e0 = lease.upload(&sc->dev, 1); e0 != cudaSuccess) return ctx->cuda_fail(e0, "uploading constants");
+  launch_debug_trace(lease.slot(0), n, d_o, d_d, d_lh, d_inst, d_tri, d_t, d_b, d_back, d_nb, d_err, ctx->stream);
   uint32_t errs = 0;
   sg.back(inst, d_inst, n);
   sg.back(tri, d_tri, n);
@@ -1654,8 +1745,10 @@ int ymrt_debug_density(ymrt_scene* sc, uint32_t texture_index, int n, const floa
   uint32_t* d_err = sg.out<uint32_t>(1);
   if (sg.err != cudaSuccess) return ctx->cuda_fail(sg.err, "staging");
   cudaMemsetAsync(d_err, 0, sizeof(uint32_t), ctx->stream);
-  upload_constants(&sc->dev, 1, ctx->primes.data(), ctx->prime_sums.data(), ctx->stream);
-  launch_debug_density(n, texture_index, d_p, d_out, d_err, ctx->stream);
+  SlotLease lease(ctx, 1);
+  if (!lease.ok()) return ctx->fail(YMRT_ERR_INVALID, "no constant-memory scene slot for this device");
+  if (const cudaError_t e0 = lease.upload(&sc->dev, 1); e0 != cudaSuccess) return ctx->cuda_fail(e0, "uploading constants");
+  launch_debug_density(lease.slot(0), n, texture_index, d_p, d_out, d_err, ctx->stream);
   uint32_t errs = 0;
   sg.back(out, d_out, n);
   sg.back(&errs, d_err, 1);
@@ -1698,8 +1791,10 @@ int ymrt_render_editor_view(ymrt_scene* sc, const ymrt_render_setting* setting, 
   uint32_t* d_err = sg.out<uint32_t>(1);
   if (sg.err != cudaSuccess) return ctx->cuda_fail(sg.err, "staging");
   cudaMemsetAsync(d_err, 0, sizeof(uint32_t), ctx->stream);
-  upload_constants(&sc->dev, 1, ctx->primes.data(), ctx->prime_sums.data(), ctx->stream);
-  launch_editor_view(0, (int)width, (int)height, setting->enable_env_light ? 1 : 0, reinterpret_cast<float4*>(d_b), d_p,
+  SlotLease lease(ctx, 1);
+  if (!lease.ok()) return ctx->fail(YMRT_ERR_INVALID, "no constant-memory scene slot for this device");
+  if (const cudaError_t e0 = lease.upload(&sc->dev, 1); e0 != cudaSuccess) return ctx->cuda_fail(e0, "uploading constants");
+  launch_editor_view((int)lease.slot(0), (int)width, (int)height, setting->enable_env_light ? 1 : 0, reinterpret_cast<float4*>(d_b), d_p,
                      d_err, ctx->stream);
   uint32_t errs = 0;
   if (!device_buffers) {
@@ -1752,8 +1847,10 @@ int ymrt_debug_frame(ymrt_scene* sc, int n, const uint32_t* inst, const uint32_t
   uint32_t* d_err = sg.out<uint32_t>(1);
   if (sg.err != cudaSuccess) return ctx->cuda_fail(sg.err, "staging");
   cudaMemsetAsync(d_err, 0, sizeof(uint32_t), ctx->stream);
-  upload_constants(&sc->dev, 1, ctx->primes.data(), ctx->prime_sums.data(), ctx->stream);
-  launch_debug_frame(n, d_i, d_t, d_b, d_k, d_d, d_out, d_err, ctx->stream);
+  SlotLease lease(ctx, 1);
+  if (!lease.ok()) return ctx->fail(YMRT_ERR_INVALID, "no constant-memory scene slot for this device");
+  if (const cudaError_t e0 = lease.upload(&sc->dev, 1); e0 != cudaSuccess) return ctx->cuda_fail(e0, "uploading constants");
+  launch_debug_frame(lease.slot(0), n, d_i, d_t, d_b, d_k, d_d, d_out, d_err, ctx->stream);
   sg.back(out, d_out, 22 * (size_t)n);
   cudaError_t e = cudaStreamSynchronize(ctx->stream);
   if (sg.err != cudaSuccess || e != cudaSuccess) return ctx->cuda_fail(sg.err != cudaSuccess ? sg.err : e, "debug frame");
@@ -1772,8 +1869,10 @@ int ymrt_debug_texture(ymrt_scene* sc, uint32_t texture_index, int n, const floa
   uint32_t* d_err = sg.out<uint32_t>(1);
   if (sg.err != cudaSuccess) return ctx->cuda_fail(sg.err, "staging");
   cudaMemsetAsync(d_err, 0, sizeof(uint32_t), ctx->stream);
-  upload_constants(&sc->dev, 1, ctx->primes.data(), ctx->prime_sums.data(), ctx->stream);
-  launch_debug_texture(n, texture_index, d_c, d_out, d_err, ctx->stream);
+  SlotLease lease(ctx, 1);
+  if (!lease.ok()) return ctx->fail(YMRT_ERR_INVALID, "no constant-memory scene slot for this device");
+  if (const cudaError_t e0 = lease.upload(&sc->dev, 1); e0 != cudaSuccess) return ctx->cuda_fail(e0, "uploading constants");
+  launch_debug_texture(lease.slot(0), n, texture_index, d_c, d_out, d_err, ctx->stream);
   uint32_t errs = 0;
   sg.back(rgb, d_out, 3 * (size_t)n);
   sg.back(&errs, d_err, 1);
@@ -1796,14 +1895,26 @@ int ymrt_debug_occluded(ymrt_scene* sc, int n, const float* origin, const float*
   uint32_t* d_err = sg.out<uint32_t>(1);
   if (sg.err != cudaSuccess) return ctx->cuda_fail(sg.err, "staging");
   cudaMemsetAsync(d_err, 0, sizeof(uint32_t), ctx->stream);
-  upload_constants(&sc->dev, 1, ctx->primes.data(), ctx->prime_sums.data(), ctx->stream);
-  launch_debug_occluded(n, d_o, d_d, d_tm, d_occ, d_err, ctx->stream);
+  SlotLease lease(ctx, 1);
+  if (!lease.ok()) return ctx->fail(YMRT_ERR_INVALID, "no constant-memory scene slot for this device");
+  if (const cudaError_t e0 = lease.upload(&sc->dev, 1); e0 != cudaSuccess) return ctx->cuda_fail(e0, "uploading constants");
+  launch_debug_occluded(lease.slot(0), n, d_o, d_d, d_tm, d_occ, d_err, ctx->stream);
   uint32_t errs = 0;
   sg.back(occluded, d_occ, n);
   sg.back(&errs, d_err, 1);
   cudaError_t e = cudaStreamSynchronize(ctx->stream);
   if (sg.err != cudaSuccess || e != cudaSuccess) return ctx->cuda_fail(sg.err != cudaSuccess ? sg.err : e, "debug occluded");
   if (errs) return ctx->fail(YMRT_ERR_OVERFLOW, "traversal stack overflow");
+  return YMRT_OK;
+}
+
+int ymrt_debug_bound_record(ymrt_context* ctx, uint32_t* words, size_t n_words, int clear) {
+  if (!ctx || (!words && n_words > 0)) return YMRT_ERR_INVALID;
+  cudaSetDevice(ctx->device);
+  std::vector<uint32_t> tmp(64, 0u);
+  const cudaError_t e = read_bound_record(tmp.data(), (int)tmp.size(), clear != 0, ctx->stream);
+  if (e != cudaSuccess) return ctx->cuda_fail(e, "reading the bound record");
+  std::memcpy(words, tmp.data(), sizeof(uint32_t) * std::min<size_t>(n_words, tmp.size()));
   return YMRT_OK;
 }
 
@@ -1822,8 +1933,10 @@ int ymrt_debug_halton(ymrt_scene* sc, int n, const int* px, const int* py, const
   float* d_off = sg.out<float>(2 * (size_t)n);
   float* d_dims = sg.out<float>(std::max<size_t>((size_t)n * n_dims, 1));
   if (sg.err != cudaSuccess) return ctx->cuda_fail(sg.err, "staging");
-  upload_constants(&sc->dev, 1, ctx->primes.data(), ctx->prime_sums.data(), ctx->stream);
-  launch_debug_halton(n, d_px, d_py, d_s, n_dims, d_idx, d_off, d_dims, ctx->stream);
+  SlotLease lease(ctx, 1);
+  if (!lease.ok()) return ctx->fail(YMRT_ERR_INVALID, "no constant-memory scene slot for this device");
+  if (const cudaError_t e0 = lease.upload(&sc->dev, 1); e0 != cudaSuccess) return ctx->cuda_fail(e0, "uploading constants");
+  launch_debug_halton(lease.slot(0), n, d_px, d_py, d_s, n_dims, d_idx, d_off, d_dims, ctx->stream);
   sg.back(index, d_idx, n);
   sg.back(offset, d_off, 2 * (size_t)n);
   if (n_dims > 0) sg.back(dims, d_dims, (size_t)n * n_dims);

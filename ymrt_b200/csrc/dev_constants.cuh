@@ -9,6 +9,6 @@
 namespace ym {
 
 constexpr int kMaxBatchScenes = 64;  // distinct (scene, sampler) pairs per batch launch
-__constant__ DeviceScene c_scenes[kMaxBatchScenes];
+static __constant__ DeviceScene c_scenes[kMaxBatchScenes];
 
 }  // namespace ym

@@ -11,8 +11,8 @@ namespace ym {
 
 // First 1000 primes and their prefix sums (offset of each prime's digit
 // permutation in the table), uploaded before each launch sequence.
-__constant__ uint32_t c_primes[kHaltonDims];
-__constant__ uint32_t c_prime_sums[kHaltonDims];
+static __constant__ uint32_t c_primes[kHaltonDims];
+static __constant__ uint32_t c_prime_sums[kHaltonDims];
 
 // Evaluation order of the reference's multi-draw argument lists
 // (e.g. SampleLi(..., random(), random(), ...) at src/Shading.cu:325): the

@@ -413,7 +413,7 @@ __device__ __forceinline__ void init_shading_frame(LayeredBsdf& B, int hit_back,
 
 // A material texture read at a surface point: every node type (grids
 // included), one out-of-line copy for all callers.
-__device__ __noinline__ vec3 surface_texture(const Texture* __restrict__ tex, uint32_t root, const TexCoord& tc,
+static __device__ __noinline__ vec3 surface_texture(const Texture* __restrict__ tex, uint32_t root, const TexCoord& tc,
                                              uint32_t* errors) {
   return texture_eval<kFeatGrids | kFeatTextures>(tex, root, tc, errors);
 }
@@ -476,7 +476,7 @@ __device__ __forceinline__ void tex_differentials(const CameraDesc& cam, vec3 p,
 // (the node's rgb * 2 - 1 as tangent-space normal) or bump mapping (the
 // height node's first channel, differenced over the pixel's texture
 // footprint, at least 0.0005, along the tangents).
-__device__ __noinline__ void init_shading_frame_mapped(LayeredBsdf& B, const DefaultMtl& m, int hit_back, vec3 ray_dir,
+static __device__ __noinline__ void init_shading_frame_mapped(LayeredBsdf& B, const DefaultMtl& m, int hit_back, vec3 ray_dir,
                                                        const SurfacePoint& sp, const mat4& wto, const DeviceScene& S,
                                                        const TexCoord& tc, uint32_t* errors) {
   vec3 sn = sp.ns;
@@ -534,7 +534,7 @@ __device__ __noinline__ void init_shading_frame_mapped(LayeredBsdf& B, const Def
 // (DefaultMtlBSDF::InitBSDFSettings' fetch_float / fetch_color,
 // src/BSDF.cuh:463-498): a float parameter takes its node's first channel.
 // Unlike the constants, the values are not clamped at load.
-__device__ __noinline__ void resolve_material_textures(DefaultMtl& m, const Texture* __restrict__ tex,
+static __device__ __noinline__ void resolve_material_textures(DefaultMtl& m, const Texture* __restrict__ tex,
                                                        const TexCoord& tc, uint32_t* errors) {
   auto f = [&](uint32_t t, float* v) {
     if (t != kEmpty) *v = surface_texture(tex, t, tc, errors).x;
@@ -800,7 +800,7 @@ __device__ __forceinline__ vec3 sample_cone(float u0, float u1, float cos_theta_
 // cone the sphere subtends, solid-angle pdf. Both sphere-light functions are
 // out of line: they run only for sphere lights, and inlined they would add
 // registers to every light evaluation.
-__device__ __noinline__ bool sphere_light_sample_li(const LightTri& lt, vec3 position, float u0, float u1, vec3* wi,
+static __device__ __noinline__ bool sphere_light_sample_li(const LightTri& lt, vec3 position, float u0, float u1, vec3* wi,
                                                        vec3* lpos, vec3* lpos_err, vec3* lng, vec3* Li, float* pdf) {
   const vec3 op = transform_position(*lt.wto, position);
   const float lpo = length(op);
@@ -831,7 +831,7 @@ __device__ __noinline__ bool sphere_light_sample_li(const LightTri& lt, vec3 pos
 }
 
 // ShapeLight::EvalLi, spheres (src/Light.h:163-200).
-__device__ __noinline__ vec3 sphere_light_eval_li(const LightTri& lt, vec3 position, vec3 wi, vec3* lpos,
+static __device__ __noinline__ vec3 sphere_light_eval_li(const LightTri& lt, vec3 position, vec3 wi, vec3* lpos,
                                                      vec3* lpos_err, vec3* lng, float* pdf) {
   const vec3 owi = transform_vector(*lt.wto, wi);
   const vec3 op = transform_position(*lt.wto, position);

@@ -11,6 +11,7 @@
 
 #include <cuda_fp16.h>
 
+#include "dev_bound.cuh"
 #include "ymrt_scene.h"
 
 namespace ym {
@@ -18,7 +19,7 @@ namespace ym {
 // Lattice permutation of the reference's Perlin noise (src/TextureEval.cuh:19);
 // kept identical so that procedural densities match the reference's value for
 // value. Indexed modulo 256 (the reference stores it twice in a row).
-__constant__ uint8_t c_perlin_perm[256] = {
+static __constant__ uint8_t c_perlin_perm[256] = {
     172, 142, 240, 182, 179, 214,  29, 111, 156,   3, 131, 161, 164, 194, 243, 124,
     127, 236,  88, 166,  83, 134,  71, 183, 227, 235, 106, 226, 216,  99, 149, 241,
     206,  63,  48,  31,  20, 171,  46, 185,   6, 125, 184, 133, 199, 201,  58,  81,
@@ -151,7 +152,7 @@ __device__ __forceinline__ float lerp1(float a, float b, float w) { return a + w
 // Trilinear read of a grid node at an object-space point. A constant grid
 // reads back its value exactly (a + w * 0 == a). Out of line, so that the
 // procedural nodes' tracking loops do not carry its registers.
-__device__ __noinline__ float grid_eval(const Texture& t, vec3 p) {
+static __device__ __noinline__ float grid_eval(const Texture& t, vec3 p) {
   int x0, x1, y0, y1, z0, z1;
   float wx, wy, wz;
   grid_axis(p.x, t.grid_n[0], &x0, &x1, &wx);
@@ -182,7 +183,7 @@ __device__ __forceinline__ float polka_hash(float x, float m) {
 
 // The solid nodes (EvalTexCheckerBoard .. EvalTexPerlinNoiseWave,
 // src/TextureEval.cuh:246-391), given their inputs' results.
-__device__ __noinline__ vec3 solid_node(const Texture& t, vec3 black, vec3 white, const TexCoord& tc) {
+static __device__ __noinline__ vec3 solid_node(const Texture& t, vec3 black, vec3 white, const TexCoord& tc) {
   switch (t.type) {
     case kTexChecker: {
       const float x = sinf(tc.p.x * t.frequency), y = sinf(tc.p.y * t.frequency), z = sinf(tc.p.z * t.frequency);
@@ -234,7 +235,7 @@ __device__ __noinline__ vec3 solid_node(const Texture& t, vec3 black, vec3 white
 // bilinear between the four texels around them (texel centres at
 // half-integers), each fetched with the node's wrap mode; one channel reads
 // as grey, more give their first three.
-__device__ __noinline__ vec3 image_node(const Texture& t, const TexCoord& tc) {
+static __device__ __noinline__ vec3 image_node(const Texture& t, const TexCoord& tc) {
   if (!t.image) return vec3(0.0f);
   float u = tc.s * t.scale_u + t.offset_u;
   if (u < 0.0f) u = gmax(0.0f, u + fabsf(floorf(u)));
@@ -333,6 +334,7 @@ __device__ __forceinline__ vec3 texture_eval(const Texture* __restrict__ tex, ui
     --top;
   }
   atomicOr(errors, 4u);
+  note_bound(kBoundTextureWalk, 3u << kTextureStack, tc.p, vec3(0.0f), 0.0f, kEmpty, root, nullptr);
   return vec3(0.0f);
 }
 

@@ -286,7 +286,7 @@ struct SphereTest {
   float xt;             // the extra crossing, when xhit != 0
   int hit, back, xhit, xback;
 };
-__device__ __noinline__ SphereTest sphere_instance_test(float radius, vec3 o, vec3 d, float t_max) {
+static __device__ __noinline__ SphereTest sphere_instance_test(float radius, vec3 o, vec3 d, float t_max) {
   SphereHit h{0.0f, vec3(0.0f), 0};
   SphereExtra x{false, kTMax, 0};
   SphereTest r;
@@ -301,7 +301,7 @@ __device__ __noinline__ SphereTest sphere_instance_test(float radius, vec3 o, ve
   r.xback = x.back;
   return r;
 }
-__device__ __noinline__ bool sphere_occludes(float radius, vec3 o, vec3 d, float t_max) {
+static __device__ __noinline__ bool sphere_occludes(float radius, vec3 o, vec3 d, float t_max) {
   SphereHit h;
   SphereExtra x;
   return sphere_intersect(radius, o, d, t_max, &h, &x);
@@ -510,7 +510,7 @@ __device__ __noinline__ bool trace_closest_impl(uint32_t scene, TraversalStack& 
 // Closest hit of one world-space ray in the scene of constant-memory slot
 // `scene` (see trace_closest_impl). Out of line, so that its callers keep one
 // call site whichever instantiation runs.
-__device__ __noinline__ bool trace_closest(uint32_t scene, TraversalStack& st, vec3 wo, vec3 wd, float tmax,
+static __device__ __noinline__ bool trace_closest(uint32_t scene, TraversalStack& st, vec3 wo, vec3 wd, float tmax,
                                               uint32_t last_inst, uint32_t last_tri, bool volume_only,
                                               ClosestHit* out, uint32_t* tri_tests, uint32_t* node_visits) {
   if (c_scenes[scene].sphere_count != 0)
@@ -600,7 +600,7 @@ __device__ __noinline__ bool trace_occluded_impl(uint32_t scene, TraversalStack&
   return false;
 }
 
-__device__ __noinline__ bool trace_occluded(uint32_t scene, TraversalStack& st, vec3 wo, vec3 wd, float tmax,
+static __device__ __noinline__ bool trace_occluded(uint32_t scene, TraversalStack& st, vec3 wo, vec3 wd, float tmax,
                                                uint32_t* tri_tests, uint32_t* node_visits) {
   if (c_scenes[scene].sphere_count != 0) return trace_occluded_impl<true>(scene, st, wo, wd, tmax, tri_tests, node_visits);
   return trace_occluded_impl<false>(scene, st, wo, wd, tmax, tri_tests, node_visits);

@@ -226,7 +226,7 @@ __device__ __forceinline__ void grid_scatter(const Texture& t, vec3 p, float g, 
 
 // One tentative collision's terms: coef_t (per channel) multiplies
 // d sigma_t / d density of each medium, coef_s multiplies d sigma_s / d density.
-__device__ __noinline__ void medium_grad(const DeviceScene& S, int n, const int* vidx, const vec3* ro, const vec3* rd,
+static __device__ __noinline__ void medium_grad(const DeviceScene& S, int n, const int* vidx, const vec3* ro, const vec3* rd,
                                          float acc, vec3 coef_t, vec3 coef_s, const MediumAdj& am) {
   for (int i = 0; i < n; ++i) {
     const Volume& v = S.volumes[vidx[i]];
@@ -243,6 +243,9 @@ __device__ __noinline__ void medium_grad(const DeviceScene& S, int n, const int*
 // SampleTrHeterogeneous (src/VolumeEval.cuh:80-214): delta tracking against
 // the summed majorant with channel-wise real / null collision probabilities.
 // kAdj: also adds the segment's density-grid gradient terms (MediumAdj).
+// `errors` is the frame's WaveCounters::errors: a loop that reaches
+// kMaxFreePath steps stops there as the reference's does (a failed sample)
+// and is counted in the word after it (WaveCounters::tracking_caps).
 template <uint32_t kF, bool kAdj = false>
 __device__ __noinline__ bool sample_tr_heterogeneous(const DeviceScene& S, int n, const int* vidx, vec3 o, vec3 d,
                                                      float t_max, vec3* tr_weight, float* dist, float* vw,
@@ -265,7 +268,8 @@ __device__ __noinline__ bool sample_tr_heterogeneous(const DeviceScene& S, int n
   int it = 0;
   while (true) {
     if (it >= kMaxFreePath) {
-      atomicOr(errors, 4u);
+      atomicAdd(errors + 1, 1u);  // WaveCounters::tracking_caps
+      note_bound(kBoundDeltaTracking, (uint32_t)it, o, d, t_max - acc, kEmpty, kEmpty, nullptr, M.m, ch);
       break;
     }
     const float fpl = -logf(1.0f - sample1d(hs, S)) / M.m[ch];
@@ -331,7 +335,8 @@ __device__ __forceinline__ bool sample_volume_scattering(const DeviceScene& S, v
 
 // EvalTrHeterogeneous (src/VolumeEval.cuh:269-386): ratio-tracking style
 // transmittance with Russian roulette after 32 steps. kAdj: also adds the
-// density-grid gradient terms of its collisions (MediumAdj).
+// density-grid gradient terms of its collisions (MediumAdj). The
+// kMaxFreePath bound is counted as in sample_tr_heterogeneous.
 template <uint32_t kF, bool kAdj = false>
 __device__ __noinline__ vec3 eval_tr_heterogeneous(const DeviceScene& S, int n, const int* vidx, vec3 o, vec3 d,
                                                    float t_max, PathSampler& hs, uint32_t* errors,
@@ -351,7 +356,8 @@ __device__ __noinline__ vec3 eval_tr_heterogeneous(const DeviceScene& S, int n, 
   int it = 0;
   while (true) {
     if (it >= kMaxFreePath) {
-      atomicOr(errors, 4u);
+      atomicAdd(errors + 1, 1u);  // WaveCounters::tracking_caps
+      note_bound(kBoundRatioTracking, (uint32_t)it, o, d, t_max - acc, kEmpty, kEmpty, nullptr, M.m, ch);
       break;
     }
     const float fpl = -logf(1.0f - sample1d(hs, S)) / M.m[ch];

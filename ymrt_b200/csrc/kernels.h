@@ -97,7 +97,11 @@ struct WaveCounters {
   uint32_t bucket_fill[kShadeBuckets];
   // cleared once per frame
   uint32_t errors;                 // kDevErr* bits
-  uint32_t reserved;
+  // delta / ratio tracking loops that reached kMaxFreePath steps (the
+  // reference's MAX_FREE_PATH_LENGTH, after which its loop stops and reports
+  // a failed sample): reference behaviour, counted rather than raised. The
+  // tracking functions reach it as the word after `errors`.
+  uint32_t tracking_caps;
   unsigned long long extension_rays;
   unsigned long long shadow_rays;
   unsigned long long tri_tests;     // closest-hit queries
@@ -107,10 +111,14 @@ struct WaveCounters {
 };
 
 constexpr size_t kWaveClearBytes = offsetof(WaveCounters, errors);
+static_assert(offsetof(WaveCounters, tracking_caps) == offsetof(WaveCounters, errors) + sizeof(uint32_t),
+              "the tracking functions count through errors + 1");
 
-// Uploads `n` scenes into constant-memory slots 0..n-1 and the prime tables.
-cudaError_t upload_constants(const DeviceScene* scenes, uint32_t n, const uint32_t* primes, const uint32_t* prime_sums,
-                             cudaStream_t stream);
+// Uploads scenes[k] into constant-memory slot slots[k] (k < n; slots ==
+// nullptr: slot k) and the prime tables, in every translation unit that holds
+// wave kernels (each has its own copy of the table).
+cudaError_t upload_constants(const DeviceScene* scenes, const uint32_t* slots, uint32_t n, const uint32_t* primes,
+                             const uint32_t* prime_sums, cudaStream_t stream);
 constexpr uint32_t kMaxSceneSlots = 64;
 
 
@@ -159,26 +167,53 @@ struct WaveOptions {
   float* grid_grads = nullptr; // adjoint: dLoss/d(value) of the density grid at texture node grid_tex
   uint32_t grid_tex = 0xFFFFFFFFu;
 };
+// One wave's pools, control block, jobs and launch shape, for the launchers
+// of the media (wave_media.cu) and adjoint (wave_adjoint.cu) kernels.
+struct WaveArgs {
+  PathPool A, B;
+  HitPool H;
+  WaveControl* ctl;
+  const JobDesc* jobs;
+  WaveCounters* counters;
+  uint32_t blocks;  // kTraceBlock-thread blocks (one thread per pool slot)
+  cudaStream_t stream;
+};
+void launch_media_extend(uint32_t features, const WaveArgs& w);
+void launch_media_shade(uint32_t features, const WaveArgs& w);
+void launch_adjoint_extend_media(const WaveArgs& w, const WaveOptions& opt);
+void launch_adjoint_shade(bool volumes, uint32_t features, const WaveArgs& w, const WaveOptions& opt);
+cudaError_t upload_slots_media(const DeviceScene* scenes, const uint32_t* slots, uint32_t n, const uint32_t* primes,
+                               const uint32_t* prime_sums, cudaStream_t stream);
+cudaError_t upload_slots_adjoint(const DeviceScene* scenes, const uint32_t* slots, uint32_t n, const uint32_t* primes,
+                                 const uint32_t* prime_sums, cudaStream_t stream);
+struct BoundRecord;
+cudaError_t read_bound_media(BoundRecord* out, bool clear, cudaStream_t stream);
+cudaError_t read_bound_adjoint(BoundRecord* out, bool clear, cudaStream_t stream);
+
 uint32_t launch_wave(const PathPool& A, const PathPool& B, const HitPool& H, WaveControl* ctl, const JobDesc* jobs,
                      uint32_t n_jobs, WaveCounters* counters, const WaveOptions& opt, cudaEvent_t* ev,
                      cudaStream_t stream, unsigned long long graph_condition = 0);
 // Grid sizes of the persistent kernels for the current device (computed once).
 void prepare_persistent_grids();
 void launch_accumulate(const float4* noise, float4* acc, uint32_t n, int frame_index, cudaStream_t stream);
-// Density of texture node `tex` at object-space points (3 floats each), scene slot 0.
-void launch_debug_density(int n, uint32_t tex, const float* p, float* out, uint32_t* err, cudaStream_t stream);
-void launch_debug_texture(int n, uint32_t tex, const float* c, float* out, uint32_t* err, cudaStream_t stream);
+// Copies the device's bound record (dev_bound.cuh) into `words` (at most
+// n_words 32-bit words) and optionally clears it.
+cudaError_t read_bound_record(uint32_t* words, int n_words, bool clear, cudaStream_t stream);
+// Known-answer launchers: each reads the scene in constant-memory slot `slot`.
+// Density of texture node `tex` at object-space points (3 floats each).
+void launch_debug_density(uint32_t slot, int n, uint32_t tex, const float* p, float* out, uint32_t* err, cudaStream_t stream);
+void launch_debug_texture(uint32_t slot, int n, uint32_t tex, const float* c, float* out, uint32_t* err, cudaStream_t stream);
 void launch_editor_view(int slot, int width, int height, int env_light, float4* beauty, uint32_t* primitive_index,
                         uint32_t* errors, cudaStream_t stream);
 void launch_post_process(float4* image, const uint32_t* primitive_index, int width, int height, uint32_t selected,
                          float gamma, float exposure, bool outline, cudaStream_t stream);
-void launch_debug_frame(int n, const uint32_t* inst, const uint32_t* tri, const float* bary, const int* back,
+void launch_debug_frame(uint32_t slot, int n, const uint32_t* inst, const uint32_t* tri, const float* bary, const int* back,
                         const float* dir, float* out, uint32_t* err, cudaStream_t stream);
-void launch_debug_trace(int n, const float* o, const float* d, const uint32_t* lh, uint32_t* inst, uint32_t* tri,
+void launch_debug_trace(uint32_t slot, int n, const float* o, const float* d, const uint32_t* lh, uint32_t* inst, uint32_t* tri,
                         float* t, float* bary, int* back, int* nearby, uint32_t* errors, cudaStream_t stream);
-void launch_debug_occluded(int n, const float* o, const float* d, const float* tmax, int* occ, uint32_t* errors,
+void launch_debug_occluded(uint32_t slot, int n, const float* o, const float* d, const float* tmax, int* occ, uint32_t* errors,
                            cudaStream_t stream);
-void launch_debug_halton(int n, const int* px, const int* py, const int* sample, int n_dims, uint64_t* index,
+void launch_debug_halton(uint32_t slot, int n, const int* px, const int* py, const int* sample, int n_dims, uint64_t* index,
                          float* offset, float* dims, cudaStream_t stream);
 
 }  // namespace ym
