@@ -251,32 +251,37 @@ __device__ __forceinline__ void push_children(TraversalStack& st, uint32_t inter
                                               uint32_t prim_base, const uint32_t* __restrict__ tlas_prims) {
   const uint32_t mask = internal | leaves;
   if (mask == 0) return;
-  if ((mask & (mask - 1)) == 0) {  // one child: no ordering needed
-    const int c = __ffs(mask) - 1;
-    const uint32_t m = child_meta(meta, c);
-    if (internal) {
-      st.push(child_base + m, tnear[c]);
-    } else {
-      for (uint32_t k = 0; k < (m >> 5); ++k) st.push(kInstanceEntry | __ldg(tlas_prims + prim_base + (m & 31u) + k), tnear[c]);
-    }
-    return;
-  }
-  uint32_t key[8];
-#pragma unroll
-  for (int c = 0; c < 8; ++c) key[c] = child_key(mask, tnear, c);
-  sort8(key);
-#pragma unroll
-  for (int j = 7; j >= 0; --j) {
-    if (key[j] == 0xFFFFFFFFu) continue;
-    const int c = (int)(key[j] & 7u);
-    const float t = __uint_as_float(key[j] & ~7u);
+  // one child's entries (a node, or the instances of a top-level leaf)
+  auto push_one = [&](uint32_t key) {
+    const int c = (int)(key & 7u);
+    const float t = __uint_as_float(key & ~7u);
     const uint32_t m = child_meta(meta, c);
     if ((internal >> c) & 1u) {
       st.push(child_base + m, t);
     } else {
       for (uint32_t k = 0; k < (m >> 5); ++k) st.push(kInstanceEntry | __ldg(tlas_prims + prim_base + (m & 31u) + k), t);
     }
+  };
+  uint32_t key[8];
+#pragma unroll
+  for (int c = 0; c < 8; ++c) key[c] = child_key(mask, tnear, c);
+  const int n = __popc(mask);
+  if (n <= 2) {
+    // one or two children: the nearest key is the least, the other the
+    // greatest below 0xFFFFFFFF (the order the network gives)
+    uint32_t lo = key[0], hi = 0u;
+#pragma unroll
+    for (int c = 1; c < 8; ++c) lo = min(lo, key[c]);
+#pragma unroll
+    for (int c = 0; c < 8; ++c) hi = max(hi, key[c] == 0xFFFFFFFFu ? 0u : key[c]);
+    if (n == 2) push_one(hi);
+    push_one(lo);
+    return;
   }
+  sort8(key);
+#pragma unroll
+  for (int j = 7; j >= 0; --j)
+    if (key[j] != 0xFFFFFFFFu) push_one(key[j]);
 }
 
 // Sphere tests of the traversals, kept out of line so that their registers do
@@ -307,6 +312,9 @@ static __device__ __noinline__ bool sphere_occludes(float radius, vec3 o, vec3 d
   return sphere_intersect(radius, o, d, t_max, &h, &x);
 }
 
+// Results of one step of a resumable walk (ClosestWalk, occluded_step).
+constexpr int kWalkGoing = 0, kWalkOccluded = 1, kWalkClear = 2;
+
 struct NearbyHit {
   uint32_t prim;
   float t;
@@ -323,114 +331,146 @@ struct ClosestHit {
 };
 
 // Closest hit of one world-space ray (TraceRay, src/ShadingUtilities.cuh:310-431)
-// in the scene of constant-memory slot `scene`.
+// in the scene of constant-memory slot `scene`, as a resumable walk: one
+// step() visits one node or enters one instance, so a persistent kernel can
+// advance the lanes of a warp on different rays (k_extend); trace_closest_impl
+// runs the steps to the end.
 // `volume_only`: traverse only treat_as_boundary instances (TraceVolume, :434-561).
 //
-// One loop serves both levels: each iteration pops one entry -- a top-level
-// node, an instance to enter, or a bottom-level node of the current instance
-// -- so the lanes of a warp run the same node code whatever level they are
-// in. Instance leaves are pushed in distance order with the internal nodes,
-// bottom-level leaves are tested at once, and entries whose box begins
-// beyond the closest hit so far are dropped when popped.
+// One loop serves both levels: each step pops one entry -- a top-level node,
+// an instance to enter, or a bottom-level node of the current instance -- so
+// the lanes of a warp run the same node code whatever level they are in.
+// Instance leaves are pushed in distance order with the internal nodes,
+// bottom-level leaves are tested at once, and entries whose box begins beyond
+// the closest hit so far are dropped when popped.
 //
-// kSpheres: the scene holds sphere geometry. The loop without sphere code is
-// a separate function, so scenes of meshes alone keep its register
+// kSpheres: the scene holds sphere geometry. The walk without sphere code is a
+// separate instantiation, so scenes of meshes alone keep its register
 // allocation (the sphere branch costs the triangle loop about 5%).
 template <bool kSpheres>
-__device__ __noinline__ bool trace_closest_impl(uint32_t scene, TraversalStack& st, vec3 wo, vec3 wd, float tmax,
-                                                uint32_t last_inst, uint32_t last_tri, bool volume_only,
-                                                ClosestHit* out, uint32_t* tri_tests, uint32_t* node_visits) {
-  const DeviceScene& S = c_scenes[scene];
-  const uint4* tlas = reinterpret_cast<const uint4*>(S.tlas_nodes);
-  const uint4* blas = reinterpret_cast<const uint4*>(S.blas_nodes);
-  const bool skip_enabled = last_inst != kEmpty && last_tri != kEmpty;
-  float t_ray = tmax;
-  bool hit = false;
-  float t_upper = 0.0f, t_lower = 0.0f;
-  int n_nearby = 0;
-  NearbyHit* nb = out->nearby;
-  const BoxRay wray = make_box_ray(wo, wd);
-
+struct ClosestWalk {
+  uint32_t slot;
+  vec3 wo, wd;
+  BoxRay wray;
+  uint32_t last_inst, last_tri;
+  bool skip_enabled, volume_only, hit;
+  float t_ray, t_upper, t_lower;
+  int n_nearby;
   // the instance being traversed (inst_base < 0: none)
-  int inst_base = -1;
-  uint32_t inst_idx = 0, wtri_offset = 0;
-  vec3 od(0.0f);
+  int inst_base;
+  uint32_t inst_idx, wtri_offset;
+  vec3 od;
   TriRay tr;
-  BoxRay br = wray;
-  bool skip_here = false, inst_hit = false;
-  float inst_t = 0.0f, hb0 = 0.0f, hb1 = 0.0f, hb2 = 0.0f, extra_t = kTMax;
+  BoxRay br;
+  bool skip_here, inst_hit, inst_sphere;
+  float inst_t, hb0, hb1, hb2, extra_t;
   // hit_w / extra_w: the wide-BVH slot of the hit / extra triangle, or for a
   // sphere (inst_sphere) the back-face flag of its hit / extra crossing
-  uint32_t hit_tri = kEmpty, hit_w = 0, extra_w = kEmpty;
-  bool inst_sphere = false;
+  uint32_t hit_tri, hit_w, extra_w;
 
-  st.sp = 0;
-  st.push(0, 0.0f);
-  for (;;) {
-    if (inst_base >= 0 && st.sp == inst_base) {
-      // leaving the instance: record its hit (and the nearby-hit list)
-      if (inst_hit) {
-        int back;
-        if (kSpheres && inst_sphere) {
-          back = (int)hit_w;
-        } else {
-          vec3 p0, p1, p2;
-          uint32_t tid;
-          load_tri(S.wtris, hit_w, &p0, &p1, &p2, &tid);
-          const vec3 ng = normalize(cross(p1 - p0, p2 - p0));
-          back = dot(ng, od) > 0.0f;
-        }
-        out->t = inst_t;
-        out->b0 = hb0;
-        out->b1 = hb1;
-        out->b2 = hb2;
-        out->inst = inst_idx;
-        out->tri = hit_tri;
-        out->back = back;
-        hit = true;
-        t_upper = next_float_up(next_float_up(t_ray));
-        t_lower = next_float_down(next_float_down(t_ray));
-        int head = 0, tail = n_nearby - 1;
-        while (head <= tail) {
-          if (nb[head].t > t_lower && nb[head].t < t_upper) ++head;
-          else {
-            const NearbyHit tmp = nb[head];
-            nb[head] = nb[tail];
-            nb[tail] = tmp;
-            --tail;
-          }
-        }
-        n_nearby = head;
-        if (n_nearby < kMaxNearby) nb[n_nearby++] = NearbyHit{inst_idx, inst_t, back};
-      } else if (hit && extra_w != kEmpty && extra_t > t_lower && extra_t < t_upper) {
-        int back;
-        if (kSpheres && inst_sphere) {
-          back = (int)extra_w;
-        } else {
-          vec3 p0, p1, p2;
-          uint32_t tid;
-          load_tri(S.wtris, extra_w, &p0, &p1, &p2, &tid);
-          const vec3 ng = normalize(cross(p1 - p0, p2 - p0));
-          back = dot(ng, od) > 0.0f;
-        }
-        if (n_nearby < kMaxNearby) nb[n_nearby++] = NearbyHit{inst_idx, extra_t, back};
+  __device__ __forceinline__ void begin(uint32_t scene, TraversalStack& st, vec3 o, vec3 d, float tmax,
+                                        uint32_t li, uint32_t lt, bool vol_only) {
+    slot = scene;
+    wo = o;
+    wd = d;
+    wray = make_box_ray(o, d);
+    last_inst = li;
+    last_tri = lt;
+    skip_enabled = li != kEmpty && lt != kEmpty;
+    volume_only = vol_only;
+    hit = false;
+    t_ray = tmax;
+    t_upper = t_lower = 0.0f;
+    n_nearby = 0;
+    inst_base = -1;
+    inst_idx = wtri_offset = 0;
+    od = vec3(0.0f);
+    br = wray;
+    skip_here = inst_hit = inst_sphere = false;
+    inst_t = hb0 = hb1 = hb2 = 0.0f;
+    extra_t = kTMax;
+    hit_tri = kEmpty;
+    hit_w = 0;
+    extra_w = kEmpty;
+    st.sp = 0;
+    st.push(0, 0.0f);
+  }
+
+  // Leaving the instance: its hit (and the nearby-hit list) into `out`.
+  __device__ __forceinline__ void leave_instance(const DeviceScene& S, ClosestHit* out) {
+    NearbyHit* nb = out->nearby;
+    if (inst_hit) {
+      int back;
+      if (kSpheres && inst_sphere) {
+        back = (int)hit_w;
+      } else {
+        vec3 p0, p1, p2;
+        uint32_t tid;
+        load_tri(S.wtris, hit_w, &p0, &p1, &p2, &tid);
+        const vec3 ng = normalize(cross(p1 - p0, p2 - p0));
+        back = dot(ng, od) > 0.0f;
       }
-      inst_base = -1;
+      out->t = inst_t;
+      out->b0 = hb0;
+      out->b1 = hb1;
+      out->b2 = hb2;
+      out->inst = inst_idx;
+      out->tri = hit_tri;
+      out->back = back;
+      hit = true;
+      t_upper = next_float_up(next_float_up(t_ray));
+      t_lower = next_float_down(next_float_down(t_ray));
+      int head = 0, tail = n_nearby - 1;
+      while (head <= tail) {
+        if (nb[head].t > t_lower && nb[head].t < t_upper) ++head;
+        else {
+          const NearbyHit tmp = nb[head];
+          nb[head] = nb[tail];
+          nb[tail] = tmp;
+          --tail;
+        }
+      }
+      n_nearby = head;
+      if (n_nearby < kMaxNearby) nb[n_nearby++] = NearbyHit{inst_idx, inst_t, back};
+    } else if (hit && extra_w != kEmpty && extra_t > t_lower && extra_t < t_upper) {
+      int back;
+      if (kSpheres && inst_sphere) {
+        back = (int)extra_w;
+      } else {
+        vec3 p0, p1, p2;
+        uint32_t tid;
+        load_tri(S.wtris, extra_w, &p0, &p1, &p2, &tid);
+        const vec3 ng = normalize(cross(p1 - p0, p2 - p0));
+        back = dot(ng, od) > 0.0f;
+      }
+      if (n_nearby < kMaxNearby) nb[n_nearby++] = NearbyHit{inst_idx, extra_t, back};
     }
-    if (st.sp == 0) break;
+    inst_base = -1;
+  }
+
+  // One step; kWalkGoing while entries remain, else kWalkClear (the walk is
+  // over: `hit` says whether `out` holds a hit; out->nearby_count is set).
+  __device__ __forceinline__ int step(TraversalStack& st, ClosestHit* out, uint32_t* tri_tests,
+                                      uint32_t* node_visits) {
+    const DeviceScene& S = c_scenes[slot];
+    if (inst_base >= 0 && st.sp == inst_base) leave_instance(S, out);
+    if (st.sp == 0) {
+      out->nearby_count = n_nearby;
+      return kWalkClear;
+    }
     float etn;
     uint32_t e = st.pop(&etn);
-    if (etn > widened_tmax(t_ray)) continue;
+    if (etn > widened_tmax(t_ray)) return kWalkGoing;
     if (e & kInstanceEntry) {
       inst_idx = e & ~kInstanceEntry;
       const Instance inst = S.instances[inst_idx];
-      if (volume_only && !inst.treat_as_boundary) continue;
+      if (volume_only && !inst.treat_as_boundary) return kWalkGoing;
       const mat4& wto = S.i_transforms[inst.transform_idx];
       const vec3 oo = xform_point_glm(wto, wo);
       od = xform_dir_glm(wto, wd);
       const GeometryDesc& g = S.geometries[inst.geometry_idx];
       if (kSpheres && g.kind == kGeoSphere) {
-        // a sphere is tested at once and left at the next iteration; its hit
+        // a sphere is tested at once and left at the next step; its hit
         // point travels in the barycentric slots and its triangle is EMPTY
         ++*tri_tests;
         const SphereTest q = sphere_instance_test(g.radius, oo, od, t_ray);
@@ -448,7 +488,7 @@ __device__ __noinline__ bool trace_closest_impl(uint32_t scene, TraversalStack& 
         extra_t = q.xhit ? q.xt : kTMax;
         extra_w = q.xhit ? (uint32_t)q.xback : kEmpty;
         inst_base = st.sp;
-        continue;
+        return kWalkGoing;
       }
       inst_sphere = false;
       tr = make_tri_ray(oo, od);
@@ -459,14 +499,14 @@ __device__ __noinline__ bool trace_closest_impl(uint32_t scene, TraversalStack& 
       extra_t = kTMax;
       extra_w = kEmpty;
       inst_base = st.sp;
-      e = g.node_offset;  // continue with the instance's root in this iteration
+      e = g.node_offset;  // continue with the instance's root in this step
     }
     const bool in_blas = inst_base >= 0;
     ++*node_visits;
     float tn[8];
     uint32_t imask, cbase, pbase, meta[2];
-    const uint32_t hits =
-        intersect_children(in_blas ? blas : tlas, e, in_blas ? br : wray, t_ray, tn, &imask, &cbase, &pbase, meta);
+    const uint32_t hits = intersect_children(reinterpret_cast<const uint4*>(in_blas ? S.blas_nodes : S.tlas_nodes), e,
+                                             in_blas ? br : wray, t_ray, tn, &imask, &cbase, &pbase, meta);
     uint32_t leaves = hits & ~imask;
     if (in_blas) {
       while (leaves) {
@@ -502,9 +542,21 @@ __device__ __noinline__ bool trace_closest_impl(uint32_t scene, TraversalStack& 
     } else {
       push_children(st, hits & imask, leaves, tn, meta, cbase, pbase, S.tlas_prims);
     }
+    return kWalkGoing;
   }
-  out->nearby_count = n_nearby;
-  return hit;
+};
+
+// The whole walk of one ray (see ClosestWalk).
+template <bool kSpheres>
+static __device__ __noinline__ bool trace_closest_impl(uint32_t scene, TraversalStack& st, vec3 wo, vec3 wd,
+                                                       float tmax, uint32_t last_inst, uint32_t last_tri,
+                                                       bool volume_only, ClosestHit* out, uint32_t* tri_tests,
+                                                       uint32_t* node_visits) {
+  ClosestWalk<kSpheres> w;
+  w.begin(scene, st, wo, wd, tmax, last_inst, last_tri, volume_only);
+  while (w.step(st, out, tri_tests, node_visits) == kWalkGoing) {
+  }
+  return w.hit;
 }
 
 // Closest hit of one world-space ray in the scene of constant-memory slot
@@ -598,6 +650,123 @@ __device__ __noinline__ bool trace_occluded_impl(uint32_t scene, TraversalStack&
     }
   }
   return false;
+}
+
+// ------------------------------------------------ resumable occlusion walk ---
+//
+// The any-hit query of trace_occluded_impl cut into steps, so that a
+// persistent kernel can advance the lanes of a warp on different rays and
+// hand a finished lane its next ray at once (k_connect). One step enters an
+// instance and visits its root, or visits one node: its child boxes are
+// tested, internal children pushed (unordered: any hit ends the query) and
+// the triangles of its leaf children tested. Stack entries need no entry
+// distance here, so the stack is entries only.
+constexpr int kOccStackShared = 32;  // entries per thread in shared memory
+constexpr int kConnectBlocksPerSm = 8;
+
+struct OccStack {
+  uint32_t* sh;  // shared-memory column of this thread (stride kTraceBlock)
+  uint32_t loc[kStackLocal];
+  int sp;
+  bool overflow;
+  __device__ __forceinline__ void bind(uint32_t* shared_entries) {
+    sh = shared_entries + threadIdx.x;
+    sp = 0;
+    overflow = false;
+  }
+  __device__ __forceinline__ void push(uint32_t v) {
+    if (sp < kOccStackShared) sh[sp * kTraceBlock] = v;
+    else if (sp < kOccStackShared + kStackLocal) loc[sp - kOccStackShared] = v;
+    else {
+      overflow = true;
+      return;
+    }
+    ++sp;
+  }
+  __device__ __forceinline__ uint32_t pop() {
+    --sp;
+    return sp < kOccStackShared ? sh[sp * kTraceBlock] : loc[sp - kOccStackShared];
+  }
+};
+
+struct OccWalk {
+  uint32_t slot;       // scene slot
+  vec3 wo, wd;         // world ray
+  float tmax;
+  BoxRay wray;
+  int inst_base;       // stack depth below the current instance's entries (-1: top level)
+  uint32_t wtri_offset;
+  TriRay tr;           // the current instance's object-space ray
+  BoxRay br;
+  __device__ __forceinline__ void begin(uint32_t scene, vec3 o, vec3 d, float t_max, OccStack& st) {
+    slot = scene;
+    wo = o;
+    wd = d;
+    tmax = t_max;
+    wray = make_box_ray(o, d);
+    inst_base = -1;
+    st.sp = 0;
+    st.push(0);
+  }
+};
+
+template <bool kSpheres>
+__device__ __forceinline__ int occluded_step(OccWalk& w, OccStack& st, uint32_t* tri_tests, uint32_t* node_visits) {
+  const DeviceScene& S = c_scenes[w.slot];
+  if (w.inst_base >= 0 && st.sp == w.inst_base) w.inst_base = -1;
+  if (st.sp == 0) return kWalkClear;
+  uint32_t e = st.pop();
+  if (e & kInstanceEntry) {
+    const Instance inst = S.instances[e & ~kInstanceEntry];
+    if (inst.treat_as_boundary) return kWalkGoing;
+    const mat4& wto = S.i_transforms[inst.transform_idx];
+    const vec3 oo = xform_point_glm(wto, w.wo);
+    const vec3 od = xform_dir_glm(wto, w.wd);
+    const GeometryDesc& g = S.geometries[inst.geometry_idx];
+    if (kSpheres && g.kind == kGeoSphere) {
+      ++*tri_tests;
+      return sphere_occludes(g.radius, oo, od, w.tmax) ? kWalkOccluded : kWalkGoing;
+    }
+    w.tr = make_tri_ray(oo, od);
+    w.br = make_box_ray(oo, od);
+    w.wtri_offset = g.wtri_offset;
+    w.inst_base = st.sp;
+    e = g.node_offset;
+  }
+  const bool in_blas = w.inst_base >= 0;
+  ++*node_visits;
+  float tn[8];
+  uint32_t imask, cbase, pbase, meta[2];
+  const uint32_t hits = intersect_children(reinterpret_cast<const uint4*>(in_blas ? S.blas_nodes : S.tlas_nodes), e,
+                                           in_blas ? w.br : w.wray, w.tmax, tn, &imask, &cbase, &pbase, meta);
+  uint32_t leaves = hits & ~imask;
+  uint32_t internal = hits & imask;
+  while (internal) {
+    const int c = __ffs(internal) - 1;
+    internal &= internal - 1;
+    st.push(cbase + child_meta(meta, c));
+  }
+  while (leaves) {
+    const int c = __ffs(leaves) - 1;
+    leaves &= leaves - 1;
+    const uint32_t m = child_meta(meta, c);
+    const uint32_t cnt = m >> 5, off = m & 31u;
+    if (!in_blas) {
+      for (uint32_t k = 0; k < cnt; ++k) st.push(kInstanceEntry | __ldg(S.tlas_prims + pbase + off + k));
+      continue;
+    }
+    for (uint32_t q = 0; q < cnt; ++q) {
+      vec3 p0, p1, p2;
+      uint32_t tid;
+      load_tri(S.wtris, w.wtri_offset + pbase + off + q, &p0, &p1, &p2, &tid);
+      float t, ev[3], inv;
+      ++*tri_tests;
+      if (!tri_test(w.tr, p0, p1, p2, &t, ev, &inv)) continue;
+      if (t < kTMin || t > w.tmax) continue;
+      return kWalkOccluded;
+    }
+  }
+  return kWalkGoing;
 }
 
 static __device__ __noinline__ bool trace_occluded(uint32_t scene, TraversalStack& st, vec3 wo, vec3 wd, float tmax,

@@ -472,7 +472,9 @@ uint32_t grid_for(K kernel, int block, int sms) {
 // kernels are instantiated in wave_media.cu and wave_adjoint.cu.
 template <uint32_t kF>
 void launch_extend_surface(const WaveArgs& w) {
-  k_extend<false, kF & kFeatSpheres><<<w.blocks, kTraceBlock, 0, w.stream>>>(w.A, w.ctl, w.H, w.jobs, w.counters);
+  const auto k = k_extend<false, kF & kFeatSpheres>;
+  k<<<w.blocks, kTraceBlock, 0, w.stream>>>(w.A, w.ctl, w.H, w.jobs, w.counters, nullptr,
+                                                                   kEmpty);
 }
 
 template <uint32_t kF>

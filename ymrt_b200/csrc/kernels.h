@@ -93,6 +93,7 @@ struct WaveCounters {
   uint32_t next_count;             // paths written to the next pool
   uint32_t hit_count;              // hits (slots listed in HitPool::order when sorting)
   uint32_t shadow_count;           // rays written to the ShadowQueue
+  uint32_t shadow_cursor;          // next ShadowQueue ray k_connect hands out
   uint32_t bucket_count[kShadeBuckets];
   uint32_t bucket_fill[kShadeBuckets];
   // cleared once per frame

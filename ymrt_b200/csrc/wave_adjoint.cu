@@ -21,8 +21,9 @@ void surface_adjoint_shade(const WaveArgs& w, const WaveOptions& opt) {
 
 void launch_adjoint_extend_media(const WaveArgs& w, const WaveOptions& opt) {
   // free flight with the density-grid terms (one instantiation, all features)
-  k_extend<true, kFeatAll, true><<<w.blocks, kTraceBlock, 0, w.stream>>>(w.A, w.ctl, w.H, w.jobs, w.counters,
-                                                                       opt.grid_grads, opt.grid_tex);
+  const auto k = k_extend<true, kFeatAll, true>;
+  k<<<w.blocks, kTraceBlock, 0, w.stream>>>(w.A, w.ctl, w.H, w.jobs, w.counters,
+                                                                           opt.grid_grads, opt.grid_tex);
 }
 
 void launch_adjoint_shade(bool volumes, uint32_t features, const WaveArgs& w, const WaveOptions& opt) {

@@ -1156,27 +1156,61 @@ __global__ void __launch_bounds__(kTraceBlock) k_shade(PathPool P, const WaveCon
 }
 
 // ------------------------------------------------------------- connect ---
-// Traces the wave's queued shadow rays (grid-stride over the queue, so the
-// grid is sized to the GPU, not to the queue) and adds each unoccluded ray's
-// contribution to its pixel.
+//
+// Traces the wave's queued shadow rays and adds each unoccluded ray's
+// contribution to its pixel. Persistent (a GPU-sized grid) with warp-level
+// work fetch (Aila & Laine, HPG 2009): a lane whose ray is done takes the next
+// queued ray at once, one atomic per warp for all its idle lanes, instead of
+// waiting for the warp's slowest ray; each loop iteration advances every busy
+// lane by one step of its own walk (occluded_step).
 template <uint32_t kF>
-__global__ void __launch_bounds__(kTraceBlock, 5) k_connect(ShadowQueue Q, const JobDesc* __restrict__ jobs,
-                                                            WaveCounters* counters) {
-  YM_TRAVERSAL_SHARED(s_stack);
-  TraversalStack st;
-  st.bind(s_stack_entries, s_stack_t);
+__global__ void __launch_bounds__(kTraceBlock, kConnectBlocksPerSm) k_connect(ShadowQueue Q,
+                                                                             const JobDesc* __restrict__ jobs,
+                                                                             WaveCounters* counters) {
+  __shared__ uint32_t s_stack[kOccStackShared * kTraceBlock];
+  OccStack st;
+  st.bind(s_stack);
+  OccWalk w;
   const uint32_t n = min(counters->shadow_count, Q.capacity);
+  const int lane = threadIdx.x & 31;
+  uint32_t ray = kEmpty;   // queue index of this lane's ray (kEmpty: idle)
+  bool exhausted = false;  // the queue has been handed out (warp-uniform)
   uint32_t tests = 0, nodes = 0;
-  for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
-    const float4 o = Q.o[t], d = Q.d[t], c = Q.c[t];
-    const JobDesc& J = jobs[__float_as_uint(c.w)];
-    if (!trace_occluded_impl<(kF & kFeatSpheres) != 0>(J.scene_slot, st, vec3(o.x, o.y, o.z), vec3(d.x, d.y, d.z), o.w, &tests,
-                                   &nodes)) {
-      atomicAdd(J.image + __float_as_uint(d.w), make_float4(c.x, c.y, c.z, 0.0f));
-      if (J.path_radiance) {
-        // the record holds radiance, the contribution is weighted by 1/spp
-        const float spp = (float)gmax(J.setting.ssp, 1);
-        atomicAdd(J.path_radiance + Q.path[t], make_float4(c.x * spp, c.y * spp, c.z * spp, 0.0f));
+  for (;;) {
+    if (!exhausted) {
+      const uint32_t idle = __ballot_sync(0xFFFFFFFFu, ray == kEmpty);
+      if (idle) {
+        const int leader = __ffs(idle) - 1;
+        uint32_t base = 0;
+        if (lane == leader) base = atomicAdd(&counters->shadow_cursor, (uint32_t)__popc(idle));
+        base = __shfl_sync(0xFFFFFFFFu, base, leader);
+        if (base + (uint32_t)__popc(idle) >= n) exhausted = true;
+        if (ray == kEmpty) {
+          const uint32_t t = base + (uint32_t)__popc(idle & ((1u << lane) - 1u));
+          if (t < n) {
+            const float4 o = Q.o[t], d = Q.d[t];
+            const uint32_t job = __float_as_uint(Q.c[t].w);
+            w.begin(jobs[job].scene_slot, vec3(o.x, o.y, o.z), vec3(d.x, d.y, d.z), o.w, st);
+            ray = t;
+          }
+        }
+      }
+    }
+    if (__ballot_sync(0xFFFFFFFFu, ray != kEmpty) == 0) break;
+    if (ray != kEmpty) {
+      const int r = occluded_step<(kF & kFeatSpheres) != 0>(w, st, &tests, &nodes);
+      if (r != kWalkGoing) {
+        if (r == kWalkClear) {
+          const float4 c = Q.c[ray];
+          const JobDesc& J = jobs[__float_as_uint(c.w)];
+          atomicAdd(J.image + __float_as_uint(Q.d[ray].w), make_float4(c.x, c.y, c.z, 0.0f));
+          if (J.path_radiance) {
+            // the record holds radiance, the contribution is weighted by 1/spp
+            const float spp = (float)gmax(J.setting.ssp, 1);
+            atomicAdd(J.path_radiance + Q.path[ray], make_float4(c.x * spp, c.y * spp, c.z * spp, 0.0f));
+          }
+        }
+        ray = kEmpty;
       }
     }
   }
@@ -1184,7 +1218,7 @@ __global__ void __launch_bounds__(kTraceBlock, 5) k_connect(ShadowQueue Q, const
     tests += __shfl_down_sync(0xFFFFFFFFu, tests, off);
     nodes += __shfl_down_sync(0xFFFFFFFFu, nodes, off);
   }
-  if ((threadIdx.x & 31) == 0) {
+  if (lane == 0) {
     if (tests) atomicAdd(&counters->shadow_tri_tests, (unsigned long long)tests);
     if (nodes) atomicAdd(&counters->shadow_node_visits, (unsigned long long)nodes);
   }

@@ -11,7 +11,9 @@ namespace {
 
 template <uint32_t kF>
 void media_extend(const WaveArgs& w) {
-  k_extend<true, kF><<<w.blocks, kTraceBlock, 0, w.stream>>>(w.A, w.ctl, w.H, w.jobs, w.counters);
+  const auto k = k_extend<true, kF>;
+  k<<<w.blocks, kTraceBlock, 0, w.stream>>>(w.A, w.ctl, w.H, w.jobs, w.counters, nullptr,
+                                                                   kEmpty);
 }
 
 template <uint32_t kF>
