@@ -83,6 +83,19 @@ class quiet_stdout:
         os.close(self.saved)
 
 
+def workload_config(wl, W, H, spp, world) -> dict:
+    """The `config` both arms print (identical, so that their lines compare)."""
+    return {"workload": f"{wl['scene']} {W}x{H} {spp}spp depth {wl['depth']}" +
+                        (" (~1.2M instanced triangles)" if wl["scene"] == "instanced" else ""),
+            "sampler": "halton", "lights": "shape lights, NEE with MIS",
+            "media": (("fog box + smoke box with a 128^3 fp16 density grid (fBm, 4 octaves, max "
+                       "sigma_t 2.0), delta tracking") if wl.get("grid") else
+                      ("noise-density medium sphere, delta tracking" if wl["scene"] == "textured" else
+                       "fog box + fBm smoke box, delta tracking")) if wl.get("volume") else "none",
+            "parallelism": f"replica x{world}" + (" + allreduce of frames" if world > 1 else ""),
+            "l2": "256 MB buffer written between steps; path queues (>1 GB) exceed L2"}
+
+
 def dist_env():
     return int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("LOCAL_RANK", "0"))
 
@@ -408,7 +421,12 @@ def run_ours(args):
     ctx = Y.Context(local_rank, queue_capacity=args.queue, profiling=False)
     if args.no_graph_loop:
         ctx.set_option("graph_loop", 0)
+    # host scene preparation (parse, the reference's binary SAH builds, wide
+    # collapse, light table), timed apart from the frames: the reference's
+    # editor does it once per scene edit, not per frame
+    t_prep = time.perf_counter()
     host = Y.HostScene(path, W, H)
+    prep_ms = (time.perf_counter() - t_prep) * 1e3
     scene = Y.Scene(ctx, host, perm)
     grid = None
     if wl.get("grid"):
@@ -510,18 +528,10 @@ def run_ours(args):
             "warmup": args.warmup, "ms_per_step": round(ms_max / args.steps, 3), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded .ymtmp scene generated by ymrt_b200.scenes)",
-            "config": {"workload": f"{wl['scene']} {W}x{H} {spp}spp depth {wl['depth']}" +
-                       (" (~1.2M instanced triangles)" if wl["scene"] == "instanced" else ""),
-                       "sampler": "halton", "lights": "shape lights, NEE with MIS",
-                       "media": (("fog box + smoke box with a 128^3 fp16 density grid (fBm, 4 octaves, max "
-                                  "sigma_t 2.0), delta tracking") if wl.get("grid") else
-                                 ("noise-density medium sphere, delta tracking" if wl["scene"] == "textured" else
-                                  "fog box + fBm smoke box, delta tracking")) if wl.get("volume") else "none",
-                       "parallelism": f"replica x{world}" + (" + allreduce of frames" if world > 1 else ""),
-                       "l2": "256 MB buffer written between steps; path queues (>1 GB) exceed L2",
-                       "options": {"sort_hits": ctx.get_option("sort_hits"),
-                                   "defer_shadows": ctx.get_option("defer_shadows"),
-                                   "graph_loop": ctx.get_option("graph_loop")}},
+            "config": workload_config(wl, W, H, spp, world),
+            "wave_options": {"sort_hits": ctx.get_option("sort_hits"),
+                             "defer_shadows": ctx.get_option("defer_shadows"),
+                             "graph_loop": ctx.get_option("graph_loop")},
             "spp_per_s": round(W * H * spp * world * args.steps / (ms_max * 1e-3), 1),
             "rays": {"extension": ext, "shadow": shadow, "per_step": rays // max(args.steps, 1)},
             "frame_ms_device": round(frame_ms / args.steps, 3),
@@ -535,6 +545,7 @@ def run_ours(args):
                          "l2_bvh_gbs": dk["bvh_l2_gbs"]},
             "e2e": {"value": round(e2e_rays_all / e2e_wall_max / 1e6, 2) if e2e_wall_max > 0 else None,
                     "unit": "Mrays/s", "h2d_bytes_per_step": int(scene_bytes), "d2h_bytes_per_step": int(W * H * 16),
+                    "scene_prepare_host_ms": round(prep_ms, 2),
                     "ms_per_step": {"scene_upload": round(e2e_upload * 1e3 / max(1, min(args.steps, 3)), 2),
                                     "render_device": round(e2e_render_dev * 1e3 / max(1, min(args.steps, 3)), 2),
                                     "total": round(e2e_wall * 1e3 / max(1, min(args.steps, 3)), 2)}},
@@ -587,11 +598,13 @@ def fp64_check(path, perm, W, H, spp, depth, frame, image, volume=False, n_tiles
             "spp": spp, "sample": f"tiles {tb}..{te - 1} (16x16 each) of frame {frame}, same samples on all three"}
 
 
-def ref_cuda_timing(path, perm, W, H, spp, depth, pst, frames=2, volume=False):
+def ref_cuda_timing(path, perm, W, H, spp, depth, pst, frames=5, volume=False):
     """The reference's own wavefront kernels rebuilt for sm_100a
     (oracle/_ref/libymrt_refgpu.so, nvcc default floating-point flags), on
-    the same frame: device time of its wave loop. Its paths are the same
-    samples, so its query count is ours for the same frame index."""
+    the same frame: device time of its wave loop, the median of `frames`
+    frames after one warm-up, with the SM clocks sampled while they run. Its
+    paths are the same samples, so its query count is ours for the same frame
+    index."""
     try:
         from oracle import ref
         if not ref.gpu_available(exact=False):
@@ -599,10 +612,13 @@ def ref_cuda_timing(path, perm, W, H, spp, depth, pst, frames=2, volume=False):
         rg = ref.RefGpuScene(path, perm, W, H)
         rg.set_settings(spp=spp, ray_depth=depth, volume=int(volume))
         rg.render_frame(10_000, copy_out=False)  # warm-up (same frame as the profiled one)
+        clocks = ClockSampler(int(os.environ.get("LOCAL_RANK", "0")))
+        clocks.start()
         ms = []
         for _ in range(frames):
             rg.render_frame(10_000, copy_out=False)
             ms.append(rg.last_render_ms())
+        clk = clocks.stop()
         rg.set_profiling(True)
         rg.render_frame(10_000, copy_out=False)
         stages = rg.last_stage_ms()
@@ -610,9 +626,10 @@ def ref_cuda_timing(path, perm, W, H, spp, depth, pst, frames=2, volume=False):
     except Exception as e:  # noqa: BLE001 - reported, not fatal for our own measurement
         return {"unavailable": f"{type(e).__name__}: {e}"}
     rays = pst.extension_rays + pst.shadow_rays
-    best = min(ms)
-    return {"value": round(rays / (best * 1e-3) / 1e6, 2), "unit": "Mrays/s", "ms_per_frame": round(best, 2),
-            "frames": frames, "stage_ms": {k: round(v, 2) if isinstance(v, float) else v for k, v in stages.items()},
+    med = float(np.median(ms))
+    return {"value": round(rays / (med * 1e-3) / 1e6, 2), "unit": "Mrays/s", "ms_per_frame": round(med, 2),
+            "frames": frames, "ms_min_max": [round(min(ms), 2), round(max(ms), 2)], "clocks": clk,
+            "stage_ms": {k: round(v, 2) if isinstance(v, float) else v for k, v in stages.items()},
             "build": "reference src/Shading.cu stage kernels, nvcc -O3 sm_100a default FP flags, MAX_RAY_COUNT 1Mi",
             "rays_per_frame": int(rays)}
 
@@ -638,29 +655,52 @@ def scene_upload_bytes(host, perm) -> int:
                + perm.nbytes)
 
 
-def cpu_baseline(path, perm, W, H, spp, depth, budget_s=15.0, threads=None, volume=False):
-    """The reference's own path tracer built for the host, on a bounded tile
-    sample of the same frame (all host threads)."""
+def _reference_sample(path, perm, W, H, spp, depth, budget_s, threads, volume):
+    """The bounded tile sample the CPU legs time: tiles from the middle of
+    frame 1, as many as the timing build renders in about budget_s on
+    `threads` host threads. Returns the timing-build scene (settings made),
+    the tile range and the closest-hit + occlusion queries the reference makes
+    on it (counted by the counted build on the same tiles, untimed)."""
     from oracle import ref
-    threads = threads or os.cpu_count() or 1
-    rs = ref.RefScene(path, perm, W, H)
+    rs = ref.RefScene(path, perm, W, H, fast=True)
     rs.set_settings(spp=spp, ray_depth=depth, volume=int(volume))
     tiles_x, tiles_y = (W + 15) // 16, (H + 15) // 16
+    total = tiles_x * tiles_y
     mid = (tiles_y // 2) * tiles_x
-    # calibrate on a few tiles, then size the sample to the budget
+    # calibrate on growing samples from the same first tile (tiles differ in
+    # cost across the frame) until one takes an eighth of the budget
     n = max(threads // 4, 1)
+    while True:
+        rs.render_frame(1, mid, mid + n, wave_capacity=256 * spp * min(n, 64), threads=threads)
+        t1 = rs.last_render_seconds()
+        if t1 >= budget_s / 8 or mid + n >= total:
+            break
+        n = min(total - mid, max(n + 1, int(n * min(8.0, budget_s / 8 / max(t1, 1e-3)))))
+    n_tiles = int(max(1, min(total - mid, n * budget_s / max(t1, 1e-3))))
+    counted = ref.RefScene(path, perm, W, H)
+    counted.set_settings(spp=spp, ray_depth=depth, volume=int(volume))
     ref.query_counts(True)
-    rs.render_frame(1, mid, mid + n, wave_capacity=256 * spp * max(n, 1), threads=threads)
-    t1 = rs.last_render_seconds()
-    ref.query_counts(True)
-    n_tiles = int(max(1, min(tiles_x * tiles_y - mid, n * budget_s / max(t1, 1e-3))))
-    rs.render_frame(1, mid, mid + n_tiles, wave_capacity=256 * spp * min(n_tiles, 64), threads=threads)
-    secs = rs.last_render_seconds()
+    counted.render_frame(1, mid, mid + n_tiles, wave_capacity=256 * spp * min(n_tiles, 64), threads=threads)
     tq, sq = ref.query_counts(True)
+    counted.close()
+    return rs, (mid, mid + n_tiles), tq + sq, total
+
+
+def cpu_baseline(path, perm, W, H, spp, depth, budget_s=10.0, threads=None, volume=False):
+    """The reference's own path tracer built for the host (its timing build:
+    g++ -O3 -march, no query counters), on a bounded tile sample of the same
+    frame, all host threads."""
+    threads = threads or os.cpu_count() or 1
+    rs, (tb, te), rays, _ = _reference_sample(path, perm, W, H, spp, depth, budget_s, threads, volume)
+    rs.render_frame(1, tb, te, wave_capacity=256 * spp * min(te - tb, 64), threads=threads)
+    secs = rs.last_render_seconds()
+    isa = rs.isa
     rs.close()
-    return {"value": round((tq + sq) / secs / 1e6, 3), "unit": "Mrays/s", "cores": threads, "kind": "reference",
-            "sample": f"{n_tiles} tiles (16x16 px, {n_tiles * 256 * spp} paths at {spp} spp) from the middle of the frame, "
-                      f"{secs:.1f} s", "rays": tq + sq}
+    n_tiles = te - tb
+    return {"value": round(rays / secs / 1e6, 3), "unit": "Mrays/s", "cores": threads, "kind": "reference",
+            "build": f"g++ -O3 -march={isa} (oracle/build_ref.py build_timing)",
+            "sample": f"{n_tiles} tiles (16x16 px, {n_tiles * 256 * spp} paths at {spp} spp) from the middle of frame 1, "
+                      f"{secs:.1f} s; queries counted by the counted build on the same tiles", "rays": rays}
 
 
 def run_reference(args):
@@ -673,37 +713,31 @@ def run_reference(args):
     spp = args.spp or wl["spp"]
     perm = scenes.halton_permutations()
     path = scenes.scene_path(wl["scene"], 0)
-    from oracle import ref
     threads = os.cpu_count() or 1
-    rs = ref.RefScene(path, perm, W, H)
-    rs.set_settings(spp=spp, ray_depth=wl["depth"], volume=int(wl.get("volume", False)))
-    tiles_x, tiles_y = (W + 15) // 16, (H + 15) // 16
-    total_tiles = tiles_x * tiles_y
-    mid = (tiles_y // 2) * tiles_x
-    n = max(threads // 4, 1)
-    ref.query_counts(True)
-    rs.render_frame(1, mid, mid + n, wave_capacity=256 * spp * n, threads=threads)
-    t1 = rs.last_render_seconds()
-    n_tiles = int(max(1, min(total_tiles - mid, n * args.cpu_budget / max(t1, 1e-3))))
-    rays = 0
+    # each step a sample of about cpu_budget seconds, the whole run about two minutes at most
+    budget = min(args.cpu_budget, 120.0 / (args.warmup + args.steps))
+    rs, (tb, te), rays_per_step, total_tiles = _reference_sample(path, perm, W, H, spp, wl["depth"], budget,
+                                                                 threads, wl.get("volume", False))
     secs = 0.0
     for i in range(args.warmup + args.steps):
-        ref.query_counts(True)
-        rs.render_frame(i + 1, mid, mid + n_tiles, wave_capacity=256 * spp * min(n_tiles, 64), threads=threads)
-        tq, sq = ref.query_counts(True)
+        # every step renders the same sample (frame 1 of those tiles), whose
+        # queries the counted build counted
+        rs.render_frame(1, tb, te, wave_capacity=256 * spp * min(te - tb, 64), threads=threads)
         if i >= args.warmup:
-            rays += tq + sq
             secs += rs.last_render_seconds()
+    isa = rs.isa
     rs.close()
+    rays = rays_per_step * args.steps
     value = rays / secs / 1e6
-    sample = f"{n_tiles} of {total_tiles} tiles per step ({n_tiles * 256 * spp} paths at {spp} spp)"
+    n_tiles = te - tb
+    sample = (f"{n_tiles} of {total_tiles} tiles per step ({n_tiles * 256 * spp} paths at {spp} spp, frame 1), "
+              f"{threads} host threads, g++ -O3 -march={isa}")
     return {
         "impl": "reference", "metric": "Mrays/s", "value": round(value, 3), "unit": "Mrays/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(secs / args.steps * 1e3, 1),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded .ymtmp scene generated by ymrt_b200.scenes)",
-        "config": {"workload": f"{wl['scene']} {W}x{H} {spp}spp depth {wl['depth']}", "sampler": "halton",
-                   "parallelism": f"{threads} host threads"},
+        "config": workload_config(wl, W, H, spp, world),
         "cpu_baseline": {"value": round(value, 3), "unit": "Mrays/s", "cores": threads, "kind": "reference",
                          "sample": sample},
         "e2e": {"value": round(value, 3), "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -719,7 +753,7 @@ def main(argv=None):
     ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["batch", "diff", "diff_media"], default="instanced")
     ap.add_argument("--spp", type=int, default=0)
     ap.add_argument("--queue", type=int, default=0, help="path queue capacity (0 = library default)")
-    ap.add_argument("--cpu-budget", type=float, default=12.0, help="seconds of CPU work per reference sample")
+    ap.add_argument("--cpu-budget", type=float, default=10.0, help="seconds of CPU work per reference sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-ref-cuda", action="store_true", help="skip timing the reference's own CUDA kernels")
     ap.add_argument("--no-fp64", action="store_true", help="skip the image check against the FP64 oracle")

@@ -152,7 +152,11 @@ inline uint32_t ymrt_oracle_max_priority(const YMRT::RayTransfer& rt) {
 '''
 
 
-def shading_source(arg_order: str) -> str:
+def shading_source(arg_order: str, counted: bool = True, gen_name: str = "gen") -> str:
+    """Writes the build-time copy of src/Shading.cu (and its sampler and
+    media headers) into oracle/_ref/<gen_name>. counted=False leaves the
+    TraceRay / BVHTraverseShadow calls as the reference wrote them (the
+    counters are still defined, never incremented): the timing build."""
     src = os.path.join(REF, "src", "Shading.cu")
     with open(src, "r", encoding="utf-8", errors="replace") as f:
         text = f.read()
@@ -162,11 +166,13 @@ def shading_source(arg_order: str) -> str:
     # counting wrappers go after the includes, before the first namespace block
     first_ns = text.index("namespace YMRT")
     head, body = text[:first_ns], text[first_ns:]
-    body, n_trace = re.subn(r"\bTraceRay\(", "ymrt_oracle_counted_trace(", body)
-    body, n_shadow = re.subn(r"\bBVHTraverseShadow\(", "ymrt_oracle_counted_shadow(", body)
+    n_trace = n_shadow = 0
+    if counted:
+        body, n_trace = re.subn(r"\bTraceRay\(", "ymrt_oracle_counted_trace(", body)
+        body, n_shadow = re.subn(r"\bBVHTraverseShadow\(", "ymrt_oracle_counted_shadow(", body)
     body, n_prio = re.subn(r"\b(\w+)\.GetMaxPriorityRecord\(\)\.ior_priority", r"ymrt_oracle_max_priority(\1)", body)
     line_of_body = head.count("\n") + 1
-    gen_dir = os.path.join(OUT, "gen")
+    gen_dir = os.path.join(OUT, gen_name)
     os.makedirs(gen_dir, exist_ok=True)
     dst = os.path.join(gen_dir, "Shading.cu")
     out = (_HELPER + f'#line 1 "{src}"\n' + head + _COUNTERS + f'#line {line_of_body} "{src}"\n' + body)
@@ -470,6 +476,71 @@ def build(arg_order: str = "ltr", force: bool = False, jobs: int = 8) -> str:
 
 
 # ---------------------------------------------------------------------------
+# Timing build: the CPU baseline. The same sources (draws in the device's
+# order, the priority read made direct so the host build does not crash) with
+# g++ -O3 and an -march instruction set, glm's SIMD paths allowed, contraction
+# left at g++'s default, and no query counters in the stage kernels (shared
+# atomic counters would slow every query); the query count of a timed sample
+# comes from a run of the counted build on the same sample. The library is
+# built for two instruction sets (x86-64-v4: AVX-512; x86-64-v3: AVX2 + FMA)
+# because it is built here and run on another machine; oracle/ref.py loads
+# the widest one that machine supports.
+
+TIMING_ISAS = ("x86-64-v4", "x86-64-v3")
+TIMING_CXXFLAGS = ["-std=c++17", "-O3", "-DNDEBUG", "-fPIC", "-w", "-pthread"]
+
+
+def timing_lib_path(isa: str) -> str:
+    return os.path.join(OUT, f"libymrt_ref_fast_{isa.replace('x86-64-', '')}.so")
+
+
+def build_timing(isa: str = "x86-64-v4", force: bool = False, jobs: int = 8) -> str:
+    lib = timing_lib_path(isa)
+    if not os.path.isdir(os.path.join(REF, "src")):
+        if os.path.exists(lib):
+            return lib
+        raise FileNotFoundError(f"reference sources not found at {REF} and no prebuilt {lib}")
+    os.makedirs(OUT, exist_ok=True)
+    tag = isa.replace("x86-64-", "")
+    stamp_file = os.path.join(OUT, f"stamp_fast_{tag}")
+    h = hashlib.sha256(_stamp("ltr").encode())
+    h.update(" ".join(TIMING_CXXFLAGS + [isa]).encode())
+    stamp = h.hexdigest()
+    if not force and os.path.exists(lib) and os.path.exists(stamp_file):
+        with open(stamp_file) as f:
+            if f.read().strip() == stamp:
+                return lib
+    obj_dir = os.path.join(OUT, f"obj_fast_{tag}")
+    os.makedirs(obj_dir, exist_ok=True)
+    shading = shading_source("ltr", counted=False, gen_name="gen_fast")
+    flags = TIMING_CXXFLAGS + [f"-march={isa}"]
+    jobs_list = [(os.path.join(REF, s), os.path.join(obj_dir, os.path.basename(s) + ".o"), []) for s in HOST_SOURCES]
+    jobs_list.append((os.path.join(HERE, "ref_harness.cpp"), os.path.join(obj_dir, "ref_harness.o"),
+                      [f'-DYMRT_SHADING_SOURCE="{shading}"']))
+    jobs_list.append((os.path.join(HERE, "ref_stubs.cpp"), os.path.join(obj_dir, "ref_stubs.o"), []))
+    procs, objs = [], []
+    for src, obj, extra in jobs_list:
+        cmd = ["g++"] + flags + extra + _includes() + ["-c", src, "-o", obj]
+        procs.append((src, subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT)))
+        objs.append(obj)
+        while len([p for _, p in procs if p.poll() is None]) >= jobs:
+            procs[0][1].wait()
+    for src, p in procs:
+        out, _ = p.communicate()
+        if p.returncode != 0:
+            raise RuntimeError(f"timing build failed for {src}:\n{out.decode(errors='replace')[-4000:]}")
+    tmp = lib + ".tmp"
+    r = subprocess.run(["g++", "-shared", "-pthread", "-o", tmp] + objs + ["-Wl,--no-undefined", "-Wl,-Bsymbolic"],
+                       capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("timing build link failed:\n" + r.stdout[-4000:] + r.stderr[-4000:])
+    os.replace(tmp, lib)
+    with open(stamp_file, "w") as f:
+        f.write(stamp)
+    return lib
+
+
+# ---------------------------------------------------------------------------
 # FP64 oracle: the same reference sources and harness with every float
 # computation done in double precision, for the converged-image error of the
 # float renderers (the reference's and ymrt_b200's) at equal spp.
@@ -616,6 +687,8 @@ def main(argv=None):
     a = ap.parse_args(argv)
     print(build(a.arg_order, a.force))
     print(build_fp64(a.force))
+    for isa in TIMING_ISAS:
+        print(build_timing(isa, a.force))
     if a.gpu:
         print(build_gpu(a.force))
         print(build_gpu(a.force, exact=True))

@@ -92,6 +92,44 @@ def lib():
     return _lib
 
 
+_lib_fast = None
+
+
+def _cpu_flags() -> set:
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("flags"):
+                    return set(line.split(":", 1)[1].split())
+    except OSError:
+        pass
+    return set()
+
+
+def lib_fast():
+    """The timing build of the reference (build_ref.build_timing) for the
+    widest instruction set this machine runs, with its name; None when
+    neither is built."""
+    global _lib_fast
+    if _lib_fast is None:
+        from . import build_ref
+        flags = _cpu_flags()
+        isas = [i for i in build_ref.TIMING_ISAS
+                if i != "x86-64-v4" or {"avx512f", "avx512bw", "avx512cd", "avx512dq", "avx512vl"} <= flags]
+        for isa in isas:
+            path = build_ref.timing_lib_path(isa)
+            if not os.path.exists(path):
+                try:
+                    build_ref.build_timing(isa)
+                except Exception:  # noqa: BLE001 - no sources here: try the next one
+                    continue
+            L = ctypes.CDLL(path)
+            _bind(L, Settings)
+            _lib_fast = (L, isa)
+            break
+    return _lib_fast
+
+
 def available64() -> bool:
     return os.path.exists(LIB64_PATH)
 
@@ -125,9 +163,17 @@ def sobol_matrices() -> np.ndarray:
 class RefScene:
     """One scene loaded and prepared by the reference's own scene module."""
 
-    def __init__(self, path: str, halton_perm: np.ndarray, width: int, height: int, fp64: bool = False):
-        """fp64: load it into the FP64 build (renders return float64 images)."""
-        L = lib64() if fp64 else lib()
+    def __init__(self, path: str, halton_perm: np.ndarray, width: int, height: int, fp64: bool = False,
+                 fast: bool = False):
+        """fp64: load it into the FP64 build (renders return float64 images).
+        fast: into the timing build (no query counters; see lib_fast)."""
+        if fast:
+            lf = lib_fast()
+            if lf is None:
+                raise RuntimeError("the timing build of the reference is not available")
+            L, self.isa = lf
+        else:
+            L = lib64() if fp64 else lib()
         self._L = L
         self._f = np.float64 if fp64 else np.float32
         self._settings = Settings64 if fp64 else Settings
