@@ -1,12 +1,14 @@
 """Build recipe for the oracle: the YMRT reference compiled for the host.
 
 TEST INFRASTRUCTURE ONLY. Compiles the reference's own sources where they lie
-(``/root/reference/src``) with g++ into ``oracle/_ref/libymrt_ref.so``
+(``<reference>/src``) with g++ into ``oracle/_ref/libymrt_ref.so``
 (git-ignored, but shipped with the repository snapshot to GPU machines). The
 reference's CMake build is not used: the hot-path sources compile directly
 once a few MSVC/CUDA-runtime stand-ins are provided (``oracle/shims``,
 ``oracle/ref_stubs.cpp``). ``oracle/ref_harness.cpp`` is this project's
 headless driver around the reference's stage kernels.
+
+The reference root is taken from ``YMRT_REFERENCE_ROOT`` or ``--reference``.
 
 Floating point: ``-ffp-contract=off`` (no fused multiply-add), SSE2 scalar
 float, IEEE division and square root; glm is forced to its scalar code path.
@@ -26,7 +28,7 @@ occlusion queries, and reads the maximum-priority record of the nested-media
 stack directly where the reference reads it through a dangling reference
 (see ``_COUNTERS``).
 
-Usage: ``python oracle/build_ref.py [--arg-order ltr|native] [--force]``.
+Usage: ``python oracle/build_ref.py --reference <checkout> [--arg-order ltr|native] [--force] [--gpu]``.
 """
 from __future__ import annotations
 
@@ -38,7 +40,32 @@ import subprocess
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF = os.environ.get("YMRT_REFERENCE_ROOT", "/root/reference")
+# The reference checkout this recipe compiles: YMRT_REFERENCE_ROOT, or
+# --reference on the command line (set_reference). Without it only the
+# prebuilt libraries under oracle/_ref are used.
+REF = os.environ.get("YMRT_REFERENCE_ROOT", "")
+
+
+def set_reference(root: str) -> None:
+    global REF
+    REF = root
+
+
+def reference_root() -> str:
+    """The reference checkout: REF, else the one the prebuilt oracle was last
+    built from (recorded in oracle/_ref/reference_root), else ""."""
+    if REF:
+        return REF
+    try:
+        with open(os.path.join(OUT, "reference_root")) as f:
+            return f.read().strip()
+    except OSError:
+        return ""
+
+
+def _record_root() -> None:
+    with open(os.path.join(OUT, "reference_root"), "w") as f:
+        f.write(REF)
 OUT = os.path.join(HERE, "_ref")
 LIB = os.path.join(OUT, "libymrt_ref.so")
 
@@ -439,6 +466,7 @@ def build(arg_order: str = "ltr", force: bool = False, jobs: int = 8) -> str:
             return LIB
         raise FileNotFoundError(f"reference sources not found at {REF} and no prebuilt {LIB}")
     os.makedirs(OUT, exist_ok=True)
+    _record_root()
     stamp_file = os.path.join(OUT, "stamp")
     stamp = _stamp(arg_order)
     if not force and os.path.exists(LIB) and os.path.exists(stamp_file):
@@ -684,7 +712,10 @@ def main(argv=None):
     ap.add_argument("--arg-order", choices=["ltr", "native"], default="ltr")
     ap.add_argument("--force", action="store_true")
     ap.add_argument("--gpu", action="store_true", help="also build the reference's kernels for sm_100a")
+    ap.add_argument("--reference", default=None, help="the reference checkout (default: $YMRT_REFERENCE_ROOT)")
     a = ap.parse_args(argv)
+    if a.reference:
+        set_reference(a.reference)
     print(build(a.arg_order, a.force))
     print(build_fp64(a.force))
     for isa in TIMING_ISAS:

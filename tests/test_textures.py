@@ -56,7 +56,7 @@ def test_textured_scene_prepares_like_the_reference(scene_dir, halton_perm, orac
 def test_reference_test_scene_prepares_like_the_reference(halton_perm, oracle):
     """src/model/CornellBox_Test.ymtmp, read where the reference checkout is."""
     from oracle import build_ref
-    path = os.path.join(build_ref.REF, "src", "model", "CornellBox_Test.ymtmp")
+    path = os.path.join(build_ref.reference_root(), "src", "model", "CornellBox_Test.ymtmp")
     if not os.path.exists(path):
         pytest.skip("reference checkout absent")
     ours = Y.HostScene(path, 320, 240)
