@@ -262,6 +262,40 @@ int ymrt_scene_set_sobol_matrices(ymrt_scene* scene, const uint32_t* matrices, s
 /* Scenes must be freed before the context they were uploaded to. */
 void ymrt_scene_free(ymrt_scene* scene);
 
+/* ---- transform edits ----
+ * The reference's editor rebuilds its top-level BVH on the host after every
+ * transform edit, reordering the instances by the build, then uploads the
+ * whole scene again (GuiModule::UpdateScene, src/core/GuiModule.cpp:123-139;
+ * TopBVH.cpp:34-198, the instance reorder at :171-191).
+ *
+ * ymrt_scene_set_transforms does it where the uploaded scene lives: it
+ * replaces transforms first .. first+count-1 (16 floats each, column major,
+ * object to world; world_to_object NULL: inverted here as glm inverts;
+ * scales, 3 per transform, the Transform's own scale that sizes sphere
+ * lights: NULL keeps them) and rebuilds on the device the instance world
+ * boxes, the binary SAH build of them (which reorders the instances), the
+ * wide top-level BVH, the shape-light table and the camera's nested-media
+ * stack, bit for bit as ymrt_host_scene_set_transforms rebuilds a host scene.
+ * The meshes' own trees are in object space and are kept. Instance indices
+ * reported afterwards are the new order's (as in the reference). */
+int ymrt_scene_set_transforms(ymrt_scene* scene, uint32_t first, uint32_t count, const float* object_to_world,
+                              const float* world_to_object, const float* scales);
+int ymrt_host_scene_set_transforms(ymrt_host_scene* scene, uint32_t first, uint32_t count,
+                                   const float* object_to_world, const float* world_to_object, const float* scales);
+
+/* Device contents of an uploaded scene's top level, to compare with a host
+ * build: copies into `out` (cap_bytes) and returns the bytes, or the bytes
+ * needed when out is NULL, or a negative YMRT_ERR_*. */
+#define YMRT_SCENE_TLAS_NODES 1      /* wide top-level nodes, 80 bytes each */
+#define YMRT_SCENE_TLAS_PRIMS 2      /* uint32 instance per top-level leaf slot */
+#define YMRT_SCENE_INSTANCES 3       /* PrimitiveInstance, 32 bytes each, current order */
+#define YMRT_SCENE_SHAPE_LIGHTS 4    /* ShapeLight, 16 bytes each */
+#define YMRT_SCENE_LIGHT_TABLE 5     /* float power CDF */
+#define YMRT_SCENE_INSTANCE_BUCKETS 6 /* uint8 shading bucket per instance */
+#define YMRT_SCENE_CAMERA_MEDIA 7    /* the camera's RayTransfer, 104 bytes */
+#define YMRT_SCENE_FILE_INDEX 8      /* uint32 file index of each instance */
+long long ymrt_scene_download(const ymrt_scene* scene, int what, void* out, size_t cap_bytes);
+
 /* ---- rendering ---- */
 /* Renders one progressive frame (frame_index >= 1) of every tile into
  * out_rgba (width*height float4, linear radiance averaged over the frame's

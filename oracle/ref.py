@@ -68,6 +68,7 @@ def _bind(L, settings_type):
     L.ymref_occluded.argtypes = [vp, i, vp, vp, vp, vp]
     L.ymref_set_density_grid.argtypes = [vp, ctypes.c_uint32, i, i, i, vp]
     L.ymref_density.argtypes = [vp, ctypes.c_uint32, i, vp, vp]
+    L.ymref_set_transforms.argtypes = [vp, ctypes.c_uint32, ctypes.c_uint32, vp, vp]
     L.ymref_tracking_caps.restype = ctypes.c_ulonglong
     L.ymref_tracking_caps.argtypes = [i]
     if hasattr(L, "ymref_boundary_walk"):
@@ -348,6 +349,13 @@ class RefScene:
         v = np.ascontiguousarray(values, self._f)
         nz, ny, nx = v.shape
         assert self._L.ymref_set_density_grid(self.h, texture_index, nx, ny, nz, _p(v)) == 0
+
+    def set_transforms(self, first: int, object_to_world, scales=None) -> None:
+        """A transform edit and the reference editor's rebuild after it
+        (top level, instance order, lights, camera media)."""
+        m = np.ascontiguousarray(object_to_world, self._f).reshape(-1, 16)
+        sc = None if scales is None else np.ascontiguousarray(scales, self._f).reshape(-1, 3)
+        assert self._L.ymref_set_transforms(self.h, first, m.shape[0], _p(m), None if sc is None else _p(sc)) == 0
 
     def density(self, texture_index: int, points) -> np.ndarray:
         """A medium's density node (or attached grid) at object-space points

@@ -650,6 +650,29 @@ int ymref_set_density_grid(void* handle, uint32_t tex, int nx, int ny, int nz, c
   return 0;
 }
 
+// A transform edit as the reference's editor applies it: transforms
+// first .. first+count-1 replaced (16 floats each, column major, object to
+// world; the inverse by glm::inverse; scales, 3 per transform, the
+// TransformState scale that sizes sphere lights, when not null), then
+// GuiModule::UpdateScene's rebuild (src/core/GuiModule.cpp:123-170).
+int ymref_set_transforms(void* handle, uint32_t first, uint32_t count, const float* mats, const float* scales) {
+  auto ctx = static_cast<RefContext*>(handle);
+  auto& T = GuiModule::Transforms(*ctx->module);
+  auto& I = GuiModule::InvTransforms(*ctx->module);
+  auto& S = GuiModule::TransformStates(*ctx->module);
+  if (first > T.size() || count > T.size() - first) return -1;
+  for (uint32_t k = 0; k < count; ++k) {
+    glm::mat4 m;
+    std::memcpy(&m, mats + 16 * (size_t)k, sizeof(m));
+    T[first + k] = m;
+    I[first + k] = glm::inverse(m);
+    if (scales) S[first + k].scale_xyz = glm::vec3(scales[3 * k], scales[3 * k + 1], scales[3 * k + 2]);
+  }
+  GuiModule::RebuildAfterTransformEdit(*ctx->module, &ctx->instance_old_index);
+  ctx->scene = GuiModule::HostScene(*ctx->module);
+  return 0;
+}
+
 // A medium's density as the build-time copy of VolumeEval.cuh reads it
 // (the grid node when one is attached to `tex`, else the reference's
 // TextureEval), at n object-space points (3 floats each).

@@ -150,6 +150,10 @@ def library():
     L.ymrt_debug_occluded.argtypes = [vp, i, vp, vp, vp, vp]
     L.ymrt_debug_halton.argtypes = [vp, i, vp, vp, vp, i, vp, vp, vp]
     L.ymrt_debug_bound_record.argtypes = [vp, vp, sz, i]
+    L.ymrt_scene_set_transforms.argtypes = [vp, ctypes.c_uint32, ctypes.c_uint32, vp, vp, vp]
+    L.ymrt_host_scene_set_transforms.argtypes = [vp, ctypes.c_uint32, ctypes.c_uint32, vp, vp, vp]
+    L.ymrt_scene_download.restype = ctypes.c_longlong
+    L.ymrt_scene_download.argtypes = [vp, i, vp, sz]
     _lib = L
     return L
 
@@ -369,6 +373,13 @@ class HostScene:
         ids = raw[:, :2].copy().view(np.uint32)
         return ids, raw[:, 2:].copy(), self._query(QUERY_LIGHT_TABLE, np.float32)
 
+    def set_transforms(self, first: int, object_to_world, scales=None) -> None:
+        """Replaces transforms first.. of this prepared scene and rebuilds its
+        top level on the host (ymrt_host_scene_set_transforms)."""
+        m = np.ascontiguousarray(object_to_world, np.float32).reshape(-1, 16)
+        sc = None if scales is None else np.ascontiguousarray(scales, np.float32).reshape(-1, 3)
+        _check(library().ymrt_host_scene_set_transforms(self.h, first, m.shape[0], _p(m), None, _p(sc)))
+
     def transforms(self):
         t = self._query(QUERY_TRANSFORMS, np.float32).reshape(-1, 32)
         return t[:, :16].copy(), t[:, 16:].copy()
@@ -430,6 +441,28 @@ class Scene:
     def set_material_params(self, params: np.ndarray, first: int = 0) -> None:
         p = np.ascontiguousarray(params, dtype=np.float32).reshape(-1, 4)
         _check(library().ymrt_scene_set_material_params(self.h, first, p.shape[0], _p(p)), self.ctx.h)
+
+    SCENE_PARTS = {"tlas_nodes": (1, np.uint8), "tlas_prims": (2, np.uint32), "instances": (3, np.uint32),
+                   "shape_lights": (4, np.uint32), "light_table": (5, np.float32), "instance_buckets": (6, np.uint8),
+                   "camera_media": (7, np.uint32), "file_index": (8, np.uint32)}
+
+    def set_transforms(self, first: int, object_to_world, scales=None) -> None:
+        """Replaces transforms first.. (object-to-world 4x4 matrices, as
+        (count, 4, 4) arrays indexed [column][row] like glm) and rebuilds the
+        top level on the device (ymrt_scene_set_transforms)."""
+        m = np.ascontiguousarray(object_to_world, np.float32).reshape(-1, 16)
+        sc = None if scales is None else np.ascontiguousarray(scales, np.float32).reshape(-1, 3)
+        _check(library().ymrt_scene_set_transforms(self.h, first, m.shape[0], _p(m), None, _p(sc)), self.ctx.h)
+
+    def download(self, part: str) -> np.ndarray:
+        """Device contents of the scene's top level (ymrt_scene_download)."""
+        what, dt = self.SCENE_PARTS[part]
+        n = library().ymrt_scene_download(self.h, what, None, 0)
+        _check(0 if n >= 0 else int(n), self.ctx.h)
+        out = np.zeros(max(int(n), 1) // np.dtype(dt).itemsize, dt)
+        got = library().ymrt_scene_download(self.h, what, _p(out), out.nbytes)
+        _check(0 if got >= 0 else int(got), self.ctx.h)
+        return out[: int(n) // np.dtype(dt).itemsize]
 
     def set_density_grid(self, texture_index: int, values: np.ndarray, half: bool = False) -> None:
         """Attaches a density grid to texture node `texture_index`: values has

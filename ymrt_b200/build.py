@@ -35,7 +35,7 @@ NVCC_FLAGS = ARCH + [
 CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-fno-fast-math", "-I/usr/local/cuda/include",
              "-I" + os.path.join(ROOT, "include")]
 
-CU_SOURCES = ["kernels.cu", "wave_media.cu", "wave_adjoint.cu", "capi.cu"]
+CU_SOURCES = ["kernels.cu", "wave_media.cu", "wave_adjoint.cu", "tlas_build.cu", "capi.cu"]
 CXX_SOURCES = ["scene_host.cpp", "png_decode.cpp"]
 
 

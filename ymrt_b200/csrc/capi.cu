@@ -262,6 +262,17 @@ struct ymrt_scene {
   std::vector<std::unique_ptr<DeviceBuffer>> buffers;
   int width = 0, height = 0;
   uint64_t triangles = 0;
+  // top-level rebuilds on the device (ymrt_scene_set_transforms)
+  struct TopLevel {
+    uint32_t max_leaf = 3;
+    uint32_t node_count = 0;                 // top-level wide nodes
+    std::vector<uint32_t> file_index;        // file index of each instance (host copy)
+    std::vector<vec3> transform_scales;      // each transform's own scale (host copy)
+    bool prepared = false;
+    int cur = 0;                             // which of the pairs below holds the current order
+    DeviceBuffer inst[2], bucket[2], file_idx[2];
+    DeviceBuffer scales, items, nodes, mid, kind, left, stack, wide, prims, offsets, inside, camera, counts;
+  } top;
 
   template <typename T>
   cudaError_t upload(const std::vector<T>& v, const T** out) {
@@ -697,6 +708,10 @@ int ymrt_scene_upload(ymrt_context* ctx, const ymrt_host_scene* hs, const uint32
     D.halton_exp2 = exp2;
     D.halton_exp3 = exp3;
   }
+  sc->top.max_leaf = s.max_leaf_prims;
+  sc->top.node_count = (uint32_t)s.tlas_nodes.size();
+  sc->top.file_index = s.instance_file_index;
+  sc->top.transform_scales = s.transform_scales;
   *out = sc.release();
   return YMRT_OK;
 }
@@ -1225,6 +1240,170 @@ int ymrt_scene_set_material_params(ymrt_scene* scene, uint32_t first, uint32_t c
   if (e == cudaSuccess) e = cudaStreamSynchronize(scene->ctx->stream);
   if (e != cudaSuccess) return scene->ctx->cuda_fail(e, "updating materials");
   return YMRT_OK;
+}
+
+int ymrt_host_scene_set_transforms(ymrt_host_scene* hs, uint32_t first, uint32_t count, const float* object_to_world,
+                                   const float* world_to_object, const float* scales) {
+  if (!hs || !object_to_world) return YMRT_ERR_INVALID;
+  std::string err;
+  const int rc = set_transforms(&hs->s, first, count, object_to_world, world_to_object, scales, &err);
+  if (rc != YMRT_OK) g_last_error = err;
+  return rc;
+}
+
+int ymrt_scene_set_transforms(ymrt_scene* sc, uint32_t first, uint32_t count, const float* object_to_world,
+                              const float* world_to_object, const float* scales) {
+  if (!sc || !object_to_world) return YMRT_ERR_INVALID;
+  ymrt_context* ctx = sc->ctx;
+  DeviceScene& D = sc->dev;
+  auto& T = sc->top;
+  if (first > D.transform_count || count > D.transform_count - first)
+    return ctx->fail(YMRT_ERR_INVALID, "transform range out of bounds");
+  cudaSetDevice(ctx->device);
+  cudaStream_t st = ctx->stream;
+  const uint32_t n = D.instance_count;
+  std::vector<mat4> m(count), mi(count);
+  for (uint32_t k = 0; k < count; ++k) {
+    std::memcpy(&m[k], object_to_world + 16 * (size_t)k, sizeof(mat4));
+    if (world_to_object) std::memcpy(&mi[k], world_to_object + 16 * (size_t)k, sizeof(mat4));
+    else mi[k] = mat4_inverse(m[k]);
+    if (scales) {
+      const float* q = scales + 3 * (size_t)k;
+      T.transform_scales[first + k] = vmax(vec3(0.0001f), vec3(q[0], q[1], q[2]));
+    }
+  }
+  cudaError_t e = cudaSuccess;
+  if (count > 0) {
+    // the scene's own transform arrays (uploaded by ymrt_scene_upload)
+    e = cudaMemcpyAsync(const_cast<mat4*>(D.transforms) + first, m.data(), sizeof(mat4) * count,
+                        cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(const_cast<mat4*>(D.i_transforms) + first, mi.data(), sizeof(mat4) * count,
+                          cudaMemcpyHostToDevice, st);
+  }
+  const size_t nb = 2 * (size_t)n - 1;
+  if (!T.prepared) {
+    for (int k = 0; k < 2 && e == cudaSuccess; ++k) {
+      e = T.inst[k].ensure(sizeof(Instance) * n);
+      if (e == cudaSuccess) e = T.bucket[k].ensure(n);
+      if (e == cudaSuccess) e = T.file_idx[k].ensure(sizeof(uint32_t) * n);
+    }
+    if (e == cudaSuccess) e = T.items.ensure(sizeof(BuildItem) * n);
+    if (e == cudaSuccess) e = T.nodes.ensure(sizeof(BinNode) * nb);
+    if (e == cudaSuccess) e = T.mid.ensure(nb);
+    if (e == cudaSuccess) e = T.kind.ensure(nb);
+    if (e == cudaSuccess) e = T.left.ensure(sizeof(uint32_t) * nb);
+    if (e == cudaSuccess) e = T.stack.ensure(sizeof(uint32_t) * 2 * (7 * nb + 2));
+    if (e == cudaSuccess) e = T.wide.ensure(sizeof(WideNode) * std::max<size_t>(2 * (size_t)n, 2));
+    if (e == cudaSuccess) e = T.prims.ensure(sizeof(uint32_t) * n);
+    if (e == cudaSuccess) e = T.offsets.ensure(sizeof(uint32_t) * n);
+    if (e == cudaSuccess) e = T.inside.ensure(n);
+    if (e == cudaSuccess) e = T.camera.ensure(sizeof(RayTransfer));
+    if (e == cudaSuccess) e = T.counts.ensure(sizeof(uint32_t) * 4);
+    if (e == cudaSuccess) e = T.scales.ensure(sizeof(vec3) * std::max<size_t>(T.transform_scales.size(), 1));
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(T.inst[0].ptr, D.instances, sizeof(Instance) * n, cudaMemcpyDeviceToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(T.bucket[0].ptr, D.inst_bucket, n, cudaMemcpyDeviceToDevice, st);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(T.file_idx[0].ptr, T.file_index.data(), sizeof(uint32_t) * n, cudaMemcpyHostToDevice, st);
+    if (e != cudaSuccess) return ctx->cuda_fail(e, "preparing the top-level rebuild");
+    T.cur = 0;
+    T.prepared = true;
+  }
+  if (e == cudaSuccess && !T.transform_scales.empty())
+    e = cudaMemcpyAsync(T.scales.ptr, T.transform_scales.data(), sizeof(vec3) * T.transform_scales.size(),
+                        cudaMemcpyHostToDevice, st);
+  if (e != cudaSuccess) return ctx->cuda_fail(e, "uploading transforms");
+  const int c = T.cur, o = c ^ 1;
+  TlasBuild b{};
+  b.n = n;
+  b.instances = T.inst[c].as<Instance>();
+  b.instances_out = T.inst[o].as<Instance>();
+  b.bucket = T.bucket[c].as<uint8_t>();
+  b.bucket_out = T.bucket[o].as<uint8_t>();
+  b.file_index = T.file_idx[c].as<uint32_t>();
+  b.file_index_out = T.file_idx[o].as<uint32_t>();
+  b.transforms = D.transforms;
+  b.i_transforms = D.i_transforms;
+  b.transform_scales = T.scales.as<vec3>();
+  b.geometries = D.geometries;
+  b.materials = D.materials;
+  b.material_count = D.material_count;
+  b.tri_corners = D.tri_corners;
+  b.pos_idx = D.pos_idx;
+  b.positions = D.positions;
+  b.items = T.items.as<BuildItem>();
+  b.nodes = T.nodes.as<BinNode>();
+  b.mid = T.mid.as<uint8_t>();
+  b.split_kind = T.kind.as<uint8_t>();
+  b.split_left = T.left.as<uint32_t>();
+  b.stack = T.stack.as<uint32_t>();
+  b.wide = T.wide.as<WideNode>();
+  b.prims = T.prims.as<uint32_t>();
+  b.lights = const_cast<ShapeLight*>(D.shape_lights);
+  b.light_table = const_cast<float*>(D.shape_light_table);
+  b.light_count = D.shape_light_count;
+  b.light_offsets = T.offsets.as<uint32_t>();
+  b.inside = T.inside.as<uint8_t>();
+  b.camera_transfer = T.camera.as<RayTransfer>();
+  b.counts = T.counts.as<uint32_t>();
+  launch_tlas_rebuild(b, T.max_leaf, D.camera.position, camera_media_ray(D.camera), st);
+  uint32_t counts[4] = {};
+  RayTransfer rt{};
+  e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaMemcpyAsync(counts, T.counts.ptr, sizeof(counts), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&rt, T.camera.ptr, sizeof(rt), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return ctx->cuda_fail(e, "rebuilding the top level");
+  if (counts[2] != D.shape_light_count || counts[1] != n)
+    return ctx->fail(YMRT_ERR_INVALID, "top-level rebuild: light or leaf count changed");
+  T.cur = o;
+  T.node_count = counts[0];
+  D.instances = T.inst[o].as<Instance>();
+  D.inst_bucket = T.bucket[o].as<uint8_t>();
+  D.tlas_nodes = T.wide.as<WideNode>();
+  D.tlas_prims = T.prims.as<uint32_t>();
+  D.camera.transfer = rt;
+  return YMRT_OK;
+}
+
+long long ymrt_scene_download(const ymrt_scene* sc, int what, void* out, size_t cap_bytes) {
+  if (!sc) return YMRT_ERR_INVALID;
+  const DeviceScene& D = sc->dev;
+  const auto& T = sc->top;
+  const void* src = nullptr;
+  bool device = true;
+  size_t bytes = 0;
+  switch (what) {
+    case YMRT_SCENE_TLAS_NODES: src = D.tlas_nodes; bytes = sizeof(WideNode) * T.node_count; break;
+    case YMRT_SCENE_TLAS_PRIMS: src = D.tlas_prims; bytes = sizeof(uint32_t) * D.instance_count; break;
+    case YMRT_SCENE_INSTANCES: src = D.instances; bytes = sizeof(Instance) * D.instance_count; break;
+    case YMRT_SCENE_SHAPE_LIGHTS: src = D.shape_lights; bytes = sizeof(ShapeLight) * D.shape_light_count; break;
+    case YMRT_SCENE_LIGHT_TABLE: src = D.shape_light_table; bytes = sizeof(float) * D.shape_light_count; break;
+    case YMRT_SCENE_INSTANCE_BUCKETS: src = D.inst_bucket; bytes = D.instance_count; break;
+    case YMRT_SCENE_CAMERA_MEDIA: src = &D.camera.transfer; bytes = sizeof(RayTransfer); device = false; break;
+    case YMRT_SCENE_FILE_INDEX:
+      bytes = sizeof(uint32_t) * D.instance_count;
+      if (T.prepared) src = T.file_idx[T.cur].ptr;
+      else {
+        src = T.file_index.data();
+        device = false;
+      }
+      break;
+    default:
+      return YMRT_ERR_INVALID;
+  }
+  if (!out) return (long long)bytes;
+  if (cap_bytes < bytes) return YMRT_ERR_INVALID;
+  if (!device) {
+    std::memcpy(out, src, bytes);
+    return (long long)bytes;
+  }
+  cudaSetDevice(sc->ctx->device);
+  cudaError_t e = cudaMemcpyAsync(out, src, bytes, cudaMemcpyDeviceToHost, sc->ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(sc->ctx->stream);
+  if (e != cudaSuccess) return sc->ctx->cuda_fail(e, "downloading the scene");
+  return (long long)bytes;
 }
 
 int ymrt_scene_set_density_grid(ymrt_scene* scene, uint32_t texture_index, int nx, int ny, int nz,

@@ -191,6 +191,49 @@ struct BoundRecord;
 cudaError_t read_bound_media(BoundRecord* out, bool clear, cudaStream_t stream);
 cudaError_t read_bound_adjoint(BoundRecord* out, bool clear, cudaStream_t stream);
 
+// Device buffers of a top-level rebuild (tlas_build.cu). The instance
+// arrays are read in the current order and written in the build's order to
+// the *_out buffers; the lights, light table and camera stack are written in
+// place.
+struct BuildItem;
+struct BinNode;
+struct TlasBuild {
+  uint32_t n;  // instances
+  const Instance* instances;
+  Instance* instances_out;
+  const uint8_t* bucket;
+  uint8_t* bucket_out;
+  const uint32_t* file_index;
+  uint32_t* file_index_out;
+  const mat4* transforms;
+  const mat4* i_transforms;
+  const vec3* transform_scales;
+  const GeometryDesc* geometries;
+  const Material* materials;
+  uint32_t material_count;
+  const uint32_t* tri_corners;
+  const uint32_t* pos_idx;
+  const float* positions;
+  // build scratch
+  BuildItem* items;       // n
+  BinNode* nodes;         // 2n - 1
+  uint8_t* mid;           // 2n - 1
+  uint8_t* split_kind;    // 2n - 1
+  uint32_t* split_left;   // 2n - 1
+  uint32_t* stack;        // 2 * (7 * (2n - 1) + 2)
+  // outputs
+  WideNode* wide;         // top-level nodes (at most 2n)
+  uint32_t* prims;        // n: instance per top-level leaf slot
+  ShapeLight* lights;
+  float* light_table;
+  uint32_t light_count;   // entries the table holds (an edit keeps the count)
+  uint32_t* light_offsets;  // n
+  uint8_t* inside;          // n
+  RayTransfer* camera_transfer;
+  uint32_t* counts;         // [0] top-level nodes, [1] leaf slots, [2] light entries
+};
+void launch_tlas_rebuild(const TlasBuild& b, uint32_t max_leaf, vec3 cam_pos, vec3 cam_dir, cudaStream_t stream);
+
 uint32_t launch_wave(const PathPool& A, const PathPool& B, const HitPool& H, WaveControl* ctl, const JobDesc* jobs,
                      uint32_t n_jobs, WaveCounters* counters, const WaveOptions& opt, cudaEvent_t* ev,
                      cudaStream_t stream, unsigned long long graph_condition = 0);

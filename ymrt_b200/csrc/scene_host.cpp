@@ -145,169 +145,14 @@ mat4 compose_transform(vec3 t, vec3 s, vec3 r_deg) {
   return m;
 }
 
-// ------------------------------------------------------------ bounding ---
-// BBox3 helpers, src/BoundingBox.h:10-140.
+// --------------------------------------------------- BVH construction ---
+// The binary SAH build and the wide collapse are bvh_build.h (shared with the
+// device top-level rebuild); these drive them over host vectors.
 
 namespace {
-inline BBox box_extend(const BBox& b, vec3 p) {
-  BBox r;
-  r.pmin = vec3(gmin(b.pmin.x, p.x), gmin(b.pmin.y, p.y), gmin(b.pmin.z, p.z));
-  r.pmax = vec3(gmax(b.pmax.x, p.x), gmax(b.pmax.y, p.y), gmax(b.pmax.z, p.z));
-  return r;
-}
-inline BBox box_union(const BBox& a, const BBox& b) {
-  BBox r;
-  r.pmin = vec3(gmin(a.pmin.x, b.pmin.x), gmin(a.pmin.y, b.pmin.y), gmin(a.pmin.z, b.pmin.z));
-  r.pmax = vec3(gmax(a.pmax.x, b.pmax.x), gmax(a.pmax.y, b.pmax.y), gmax(a.pmax.z, b.pmax.z));
-  return r;
-}
-inline BBox bound_fix(const BBox& in) {
-  const float eps = 0.0005f;
-  BBox b = in;
-  for (int i = 0; i < 3; ++i) {
-    if (b.pmax[i] < b.pmin[i]) std::swap(b.pmax[i], b.pmin[i]);
-    if (std::fabs(b.pmax[i] - b.pmin[i]) < 2.0f * eps) {
-      b.pmax[i] += eps;
-      b.pmin[i] -= eps;
-    }
-  }
-  return b;
-}
-inline float box_area(const BBox& b) {
-  const vec3 e = b.pmax - b.pmin;
-  return 2.f * (e.x * e.y + e.y * e.z + e.x * e.z);
-}
-inline int box_longest_axis(const BBox& b) {
-  const vec3 d = b.pmax - b.pmin;
-  int a = 0;
-  if (d[1] > d[a]) a = 1;
-  if (d[2] > d[a]) a = 2;
-  return a;
-}
-inline vec3 box_center(const BBox& b) { return (b.pmax + b.pmin) * 0.5f; }
-inline BBox box_transform(const BBox& b, const mat4& M) {
-  BBox r;
-  for (int i = 0; i < 8; ++i) {
-    const vec3 c((i & 1) ? b.pmax.x : b.pmin.x, (i & 2) ? b.pmax.y : b.pmin.y, (i & 4) ? b.pmax.z : b.pmin.z);
-    r = box_extend(r, xform_point_glm(M, c));
-  }
-  return bound_fix(r);
-}
-
-// --------------------------------------------------- binary BVH (order) ---
-// The reference's top-down SAH builder (src/BottomBVH.cpp:34-166,
-// src/BottomBVH.h:40-190, src/TopBVH.cpp:34-198): 24 bins per axis, a
-// median split (heap selection) when SAH declines or partitioning fails,
-// one primitive per leaf, children flattened depth-first. Its partitioning
-// and selection steps are reproduced step for step, because the resulting
-// primitive order defines the triangle and instance indices (and the
-// shape-light order) that the rest of the pipeline reports.
-
-struct BuildItem {
-  BBox box;
-  vec3 center;
-  uint32_t idx;
-};
-
-struct BinNode {
-  BBox box;
-  uint32_t left = kEmpty, right = kEmpty;
-  uint32_t offset = 0, count = 0;
-};
-
-void heap_down(BuildItem* t, uint32_t i, uint32_t right, int axis) {
-  for (;;) {
-    const uint32_t lc = 2 * i + 1, rc = 2 * i + 2;
-    if (!(lc <= right)) return;
-    uint32_t target = lc;
-    if (rc <= right && t[rc].center[axis] > t[lc].center[axis]) target = rc;
-    if (t[i].center[axis] > t[target].center[axis]) return;
-    std::swap(t[i], t[target]);
-    i = target;
-  }
-}
-
-uint32_t find_mid_element(BuildItem* t, uint32_t count, int axis) {
-  const uint32_t n_th = (count - 1) / 2;
-  uint32_t n_pass = count - n_th;
-  for (uint32_t i = count / 2 - 1; i != kEmpty; --i) heap_down(t, i, count - 1, axis);
-  for (uint32_t i = count - 1; i > 0 && n_pass > 0; --i, --n_pass) {
-    std::swap(t[0], t[i]);
-    heap_down(t, 0, i - 1, axis);
-  }
-  return n_th;
-}
-
-uint32_t partition_items(BuildItem* t, uint32_t count, float pivot, int axis) {
-  uint32_t left = 0, right = count - 1;
-  while (left <= right && right != kEmpty) {
-    if (t[left].center[axis] <= pivot) ++left;
-    else std::swap(t[left], t[right--]);
-  }
-  return right;
-}
-
-bool eval_sah(const BuildItem* prims, uint32_t count, const BBox& cb, float parent_cost, float* split_pos,
-              int* split_axis) {
-  constexpr int kBins = 24;
-  int best_axis = -1;
-  float best_pos = 0.0f, best_cost = 1E36f;
-  struct Bin {
-    uint32_t count = 0;
-    BBox box;
-  };
-  bool valid[3] = {true, true, true};
-  vec3 ext = cb.pmax - cb.pmin;
-  for (int a = 0; a < 3; ++a)
-    if (ext[a] < kFloatEps) {
-      valid[a] = false;
-      ext[a] = kFloatEps;
-    }
-  Bin bins[kBins][3];
-  const vec3 i_ext = vec3(1.0f) / ext;
-  const vec3 bin_len = vmax(cb.pmax - cb.pmin, vec3(0.0f)) / float(kBins);
-  for (uint32_t i = 0; i < count; ++i) {
-    const vec3 ndc = (prims[i].center - cb.pmin) * i_ext;
-    for (int a = 0; a < 3; ++a) {
-      const int b = gmax(gmin((int)(ndc[a] * kBins), kBins - 1), 0);
-      bins[b][a].count++;
-      bins[b][a].box = box_union(bins[b][a].box, prims[i].box);
-    }
-  }
-  float la[kBins - 1][3], ra[kBins - 1][3];
-  uint32_t lc[kBins - 1][3], rc[kBins - 1][3];
-  for (int a = 0; a < 3; ++a) {
-    if (!valid[a]) continue;
-    BBox lb, rb;
-    uint32_t lcount = 0, rcount = 0;
-    for (int i = 0; i < kBins - 1; ++i) {
-      lcount += bins[i][a].count;
-      lb = box_union(lb, bins[i][a].box);
-      lc[i][a] = lcount;
-      la[i][a] = box_area(lb);
-      rcount += bins[kBins - 1 - i][a].count;
-      rb = box_union(rb, bins[kBins - 1 - i][a].box);
-      rc[kBins - 2 - i][a] = rcount;
-      ra[kBins - 2 - i][a] = box_area(rb);
-    }
-    for (int i = 0; i < kBins - 1; ++i) {
-      const float cost = lc[i][a] * la[i][a] + rc[i][a] * ra[i][a];
-      if (cost <= 0.0f) continue;
-      if (cost < best_cost) {
-        best_cost = cost;
-        best_axis = a;
-        best_pos = cb.pmin[a] + float(i + 1) * bin_len[a];
-      }
-    }
-  }
-  if (best_axis == -1 || best_cost >= parent_cost) return false;
-  *split_axis = best_axis;
-  *split_pos = best_pos;
-  return true;
-}
 
 // Builds the binary tree; reorders `items` in place. Returns the nodes in
-// build (breadth-first) order, root at 0.
+// build (level by level) order, root at 0.
 std::vector<BinNode> build_binary(std::vector<BuildItem>& items) {
   const uint32_t n = (uint32_t)items.size();
   std::vector<BinNode> nodes;
@@ -321,45 +166,10 @@ std::vector<BinNode> build_binary(std::vector<BuildItem>& items) {
     const uint32_t process = total - start;
     for (uint32_t ni = start; ni < start + process; ++ni) {
       BinNode& node = nodes[ni];
-      BuildItem* its = items.data() + node.offset;
-      BBox nb, cb;
-      for (uint32_t i = 0; i < node.count; ++i) {
-        nb = box_union(nb, its[i].box);
-        cb = box_extend(cb, its[i].center);
-      }
-      node.box = nb;
-      auto make_mid = [&]() {
-        const int axis = box_longest_axis(nb);
-        const uint32_t mid = find_mid_element(its, node.count, axis);
-        const uint32_t l = total;
-        total += 2;
-        node.left = l;
-        node.right = l + 1;
-        nodes[l].offset = node.offset;
-        nodes[l].count = mid + 1;
-        mid_split[l] = 1;
-        nodes[l + 1].offset = node.offset + mid + 1;
-        nodes[l + 1].count = node.count - 1 - mid;
-        mid_split[l + 1] = 1;
-      };
-      if (node.count <= 1) {
+      uint32_t left_count = 0;
+      const int kind = split_node(node, items.data() + node.offset, mid_split[ni] != 0, &left_count);
+      if (kind == kSplitLeaf) {
         node.left = node.right = kEmpty;
-        continue;
-      }
-      if (mid_split[ni]) {
-        make_mid();
-        continue;
-      }
-      const float parent_cost = node.count * box_area(node.box);
-      int axis = 0;
-      float pos = 0.0f;
-      if (!eval_sah(its, node.count, cb, parent_cost, &pos, &axis)) {
-        make_mid();
-        continue;
-      }
-      const uint32_t split = partition_items(its, node.count, pos, axis);
-      if (split == kEmpty || split == node.count - 1) {
-        make_mid();
         continue;
       }
       const uint32_t l = total;
@@ -367,9 +177,10 @@ std::vector<BinNode> build_binary(std::vector<BuildItem>& items) {
       node.left = l;
       node.right = l + 1;
       nodes[l].offset = node.offset;
-      nodes[l].count = split + 1;
-      nodes[l + 1].offset = node.offset + split + 1;
-      nodes[l + 1].count = node.count - 1 - split;
+      nodes[l].count = left_count;
+      nodes[l + 1].offset = node.offset + left_count;
+      nodes[l + 1].count = node.count - left_count;
+      mid_split[l] = mid_split[l + 1] = kind == kSplitMid ? 1 : 0;
     }
     start += process;
   }
@@ -377,136 +188,19 @@ std::vector<BinNode> build_binary(std::vector<BuildItem>& items) {
   return nodes;
 }
 
-// ------------------------------------------------------- wide BVH (8) ---
-
-constexpr int kWide = 8;
-
-struct WideBuilder {
-  const std::vector<BinNode>* bin;
-  std::vector<WideNode>* out;
-  std::vector<uint32_t>* prim_order;  // primitive (item position) per wide-leaf slot
-  uint32_t max_leaf;                  // a subtree of at most this many primitives becomes a leaf
-
-  static uint8_t quant_exp(float extent) {
-    // smallest e with extent / 2^e <= 250 (margin for outward rounding)
-    int e = -126;
-    if (extent > 0.0f) e = (int)std::ceil(std::log2(extent / 250.0f));
-    e = std::max(-126, std::min(127, e));
-    return (uint8_t)(e + 127);
-  }
-  static float exp_scale(uint8_t be) { return u2f((uint32_t)be << 23); }
-
-  // Grows a box by a relative margin so float rounding in the slab test can
-  // never reject a ray that touches the exact box.
-  static BBox pad(const BBox& b) {
-    BBox r = b;
-    for (int a = 0; a < 3; ++a) {
-      const float m = 2e-6f * std::max(std::fabs(b.pmin[a]), std::fabs(b.pmax[a])) + 1e-30f;
-      r.pmin[a] = b.pmin[a] - m;
-      r.pmax[a] = b.pmax[a] + m;
-    }
-    return r;
-  }
-
-  uint32_t subtree_prims(uint32_t ni) const { return (*bin)[ni].count; }
-
-  // Fills node `slot` of `out` from binary node `root`.
-  void build(uint32_t root, uint32_t slot) {
-    const auto& B = *bin;
-    std::vector<uint32_t> cand;
-    if (B[root].left == kEmpty) {
-      cand.push_back(root);  // single-leaf tree
-    } else {
-      cand.push_back(B[root].left);
-      cand.push_back(B[root].right);
-      while ((int)cand.size() < kWide) {
-        int best = -1;
-        float best_area = -1.0f;
-        for (int i = 0; i < (int)cand.size(); ++i) {
-          const BinNode& c = B[cand[i]];
-          if (c.left == kEmpty || c.count <= max_leaf) continue;
-          const float a = box_area(c.box);
-          if (a > best_area) {
-            best_area = a;
-            best = i;
-          }
-        }
-        if (best < 0) break;
-        const uint32_t e = cand[best];
-        cand[best] = B[e].left;
-        cand.insert(cand.begin() + best + 1, B[e].right);
-      }
-    }
-    WideNode node;
-    std::memset(&node, 0, sizeof(node));
-    BBox all;
-    std::vector<BBox> boxes;
-    for (uint32_t c : cand) {
-      boxes.push_back(pad(B[c].box));
-      all = box_union(all, boxes.back());
-    }
-    node.ox = all.pmin.x;
-    node.oy = all.pmin.y;
-    node.oz = all.pmin.z;
-    node.ex = quant_exp(all.pmax.x - all.pmin.x);
-    node.ey = quant_exp(all.pmax.y - all.pmin.y);
-    node.ez = quant_exp(all.pmax.z - all.pmin.z);
-    node.prim_base = (uint32_t)prim_order->size();
-    std::vector<uint32_t> internal;
-    for (size_t i = 0; i < cand.size(); ++i) {
-      const BinNode& c = B[cand[i]];
-      if (c.left == kEmpty || c.count <= max_leaf) {
-        const uint32_t off = (uint32_t)prim_order->size() - node.prim_base;
-        for (uint32_t k = 0; k < c.count; ++k) prim_order->push_back(c.offset + k);
-        node.meta[i] = (uint8_t)((c.count << 5) | off);
-      } else {
-        node.imask |= (uint8_t)(1u << i);
-        node.meta[i] = (uint8_t)internal.size();
-        internal.push_back(cand[i]);
-      }
-    }
-    // Quantise every child box on the node grid origin + q * 2^e, decoding
-    // exactly as the kernel does (one fmaf) and rounding outwards; widen the
-    // grid step if a bound does not fit in 8 bits.
-    const float org[3] = {node.ox, node.oy, node.oz};
-    uint8_t* exps[3] = {&node.ex, &node.ey, &node.ez};
-    uint8_t* qlo[3] = {node.qlo_x, node.qlo_y, node.qlo_z};
-    uint8_t* qhi[3] = {node.qhi_x, node.qhi_y, node.qhi_z};
-    for (int a = 0; a < 3; ++a) {
-      for (;;) {
-        const float sc = exp_scale(*exps[a]);
-        bool ok = true;
-        for (size_t i = 0; i < cand.size() && ok; ++i) {
-          int lo = (int)std::floor((boxes[i].pmin[a] - org[a]) / sc);
-          int hi = (int)std::ceil((boxes[i].pmax[a] - org[a]) / sc);
-          lo = std::max(0, std::min(255, lo));
-          hi = std::max(0, std::min(255, hi));
-          while (lo > 0 && std::fma((float)lo, sc, org[a]) > boxes[i].pmin[a]) --lo;
-          while (hi < 255 && std::fma((float)hi, sc, org[a]) < boxes[i].pmax[a]) ++hi;
-          if (std::fma((float)lo, sc, org[a]) > boxes[i].pmin[a] || std::fma((float)hi, sc, org[a]) < boxes[i].pmax[a])
-            ok = false;
-          qlo[a][i] = (uint8_t)lo;
-          qhi[a][i] = (uint8_t)hi;
-        }
-        if (ok || *exps[a] >= 254) break;
-        ++*exps[a];
-      }
-    }
-    node.child_base = (uint32_t)out->size();
-    out->resize(out->size() + internal.size());
-    (*out)[slot] = node;
-    for (size_t k = 0; k < internal.size(); ++k) build(internal[k], node.child_base + (uint32_t)k);
-  }
-};
-
 // Builds the wide BVH for a binary tree; appends nodes to `out` (root first)
 // and the primitive order of the leaves to `prim_order`.
 uint32_t build_wide(const std::vector<BinNode>& bin, std::vector<WideNode>* out, std::vector<uint32_t>* prim_order,
                     uint32_t max_leaf) {
   const uint32_t root = (uint32_t)out->size();
-  out->resize(out->size() + 1);
-  WideBuilder wb{&bin, out, prim_order, max_leaf};
-  wb.build(0, root);
+  uint32_t n_nodes = root + 1;
+  uint32_t n_prims = (uint32_t)prim_order->size();
+  out->resize(root + std::max<size_t>(bin.size(), 1));
+  prim_order->resize(n_prims + bin[0].count);
+  std::vector<uint32_t> stack(2 * (7 * bin.size() + 2));
+  build_wide_into(bin.data(), max_leaf, out->data(), root, &n_nodes, prim_order->data(), &n_prims, stack.data());
+  out->resize(n_nodes);
+  prim_order->resize(n_prims);
   return root;
 }
 
@@ -1270,50 +964,27 @@ int load_arrays(const ymrt_scene_desc* d, HostScene* scene, std::string* error) 
 
 namespace {
 
-// Watertight ray/triangle test, the reference's IntersectTri
-// (src/ShadingUtilities.cuh:54-134), host copy for camera set-up.
-bool host_intersect_tri(vec3 p0, vec3 p1, vec3 p2, vec3 o, vec3 d, float tmax, float* t_out) {
-  p0 = p0 - o;
-  p1 = p1 - o;
-  p2 = p2 - o;
-  const int kz = max_dimension(vabs(d));
-  int kx = kz + 1; if (kx == 3) kx = 0;
-  int ky = kx + 1; if (ky == 3) ky = 0;
-  const vec3 dd(d[kx], d[ky], d[kz]);
-  p0 = vec3(p0[kx], p0[ky], p0[kz]);
-  p1 = vec3(p1[kx], p1[ky], p1[kz]);
-  p2 = vec3(p2[kx], p2[ky], p2[kz]);
-  const float sx = -dd.x / dd.z, sy = -dd.y / dd.z, sz = 1.f / dd.z;
-  p0.x += sx * p0.z; p0.y += sy * p0.z;
-  p1.x += sx * p1.z; p1.y += sy * p1.z;
-  p2.x += sx * p2.z; p2.y += sy * p2.z;
-  const float e0 = p1.x * p2.y - p1.y * p2.x;
-  const float e1 = p2.x * p0.y - p2.y * p0.x;
-  const float e2 = p0.x * p1.y - p0.y * p1.x;
-  if ((e0 < 0 || e1 < 0 || e2 < 0) && (e0 > 0 || e1 > 0 || e2 > 0)) return false;
-  const float den = e0 + e1 + e2;
-  if (den == 0) return false;
-  p0.z *= sz; p1.z *= sz; p2.z *= sz;
-  const float inv = 1.0f / den;
-  float t = e0 * p0.z + e1 * p1.z + e2 * p2.z;
-  t *= inv;
-  if (t < kTMin || t > tmax) return false;
-  *t_out = t;
-  return true;
+}  // namespace
+
+vec3 camera_media_ray(const CameraDesc& cam) {
+  const float height = 2.0f * cam.tan_half_fov;
+  const float width = height * cam.aspect_ratio;
+  const vec3 dir = -cam.w + (0.5f - 0.5f) * width * cam.u + (0.5f - 0.5f) * height * cam.v;
+  return normalize(dir);
 }
+
+namespace {
 
 // Camera::InitCameraRayTransfer (src/Camera.cpp:15-78): instances the
 // camera sits inside (a ray from the camera hits them both forwards and
 // backwards) are pushed on the camera's ray-transfer stack.
 void init_camera_transfer(HostScene* s) {
   RayTransfer& rt = s->camera.transfer;
+  rt = RayTransfer{};  // records past record_count are zero
   rt.max_priority_record_index = -1;
   rt.record_count = 0;
   const CameraDesc& cam = s->camera;
-  const float height = 2.0f * cam.tan_half_fov;
-  const float width = height * cam.aspect_ratio;
-  vec3 dir = -cam.w + (0.5f - 0.5f) * width * cam.u + (0.5f - 0.5f) * height * cam.v;
-  dir = normalize(dir);
+  const vec3 dir = camera_media_ray(cam);
   auto hits_geometry = [&](uint32_t inst_idx, vec3 o_world, vec3 d_world) {
     const Instance& inst = s->instances[inst_idx];
     const mat4& wto = s->i_transforms[inst.transform_idx];
@@ -1331,7 +1002,7 @@ void init_camera_transfer(HostScene* s) {
         p[k] = vec3(m.pos[3 * vi], m.pos[3 * vi + 1], m.pos[3 * vi + 2]);
       }
       float th;
-      if (host_intersect_tri(p[0], p[1], p[2], o, d, kTMax, &th)) return true;
+      if (watertight_hit(p[0], p[1], p[2], o, d, kTMax, &th)) return true;
     }
     return false;
   };
@@ -1341,9 +1012,9 @@ void init_camera_transfer(HostScene* s) {
   for (uint32_t i : inside) {
     if (rt.record_count == kMaxBoundaryRecord) break;
     const Instance& inst = s->instances[i];
-    const Material& mat = s->materials[inst.material_idx];
-    const float ior = mat.material_type == kDefaultMtl ? mat.default_mtl.ior_n : 1.0f;
-    const uint32_t prio = mat.material_type == kDefaultMtl ? mat.default_mtl.ior_priority : 0u;
+    const bool dm = inst.material_idx < s->materials.size() && s->materials[inst.material_idx].material_type == kDefaultMtl;
+    const float ior = dm ? s->materials[inst.material_idx].default_mtl.ior_n : 1.0f;
+    const uint32_t prio = dm ? s->materials[inst.material_idx].default_mtl.ior_priority : 0u;
     BoundaryRecord& r = rt.records[rt.record_count++];
     r.prim_idx = i;
     r.ior = ior;
@@ -1355,6 +1026,109 @@ void init_camera_transfer(HostScene* s) {
 }
 
 }  // namespace
+
+// The top level: instance world boxes, the reference's binary SAH build of
+// them (which fixes the instance order), the wide top-level BVH, and the
+// shape-light table in the new instance order. prepare_scene runs it after
+// the meshes are built; set_transforms runs it again after an edit, starting
+// from the current instance order as the reference's editor does
+// (GuiModule::UpdateScene, src/core/GuiModule.cpp:123-139).
+int build_top_level(HostScene* s, std::string* error) {
+  const uint32_t ni = (uint32_t)s->instances.size();
+  if (ni == 0) {
+    if (error) *error = "scene has no instances";
+    return YMRT_ERR_INVALID;
+  }
+  std::vector<BuildItem> items(ni);
+  for (uint32_t i = 0; i < ni; ++i) {
+    const Instance& inst = s->instances[i];
+    items[i].box = box_transform(s->meshes[inst.geometry_idx].root_box, s->transforms[inst.transform_idx]);
+    items[i].center = box_center(items[i].box);
+    items[i].idx = i;
+  }
+  std::vector<BinNode> tbin = build_binary(items);
+  std::vector<Instance> reordered(ni);
+  std::vector<uint32_t> file_index(ni);
+  const bool ordered_before = s->instance_file_index.size() == ni;
+  for (uint32_t i = 0; i < ni; ++i) {
+    reordered[i] = s->instances[items[i].idx];
+    file_index[i] = ordered_before ? s->instance_file_index[items[i].idx] : items[i].idx;
+  }
+  s->instances.swap(reordered);
+  s->instance_file_index.swap(file_index);
+  s->tlas_nodes.clear();
+  s->tlas_prims.clear();
+  build_wide(tbin, &s->tlas_nodes, &s->tlas_prims, s->max_leaf_prims);
+  s->triangle_count_instanced = 0;
+  for (const Instance& inst : s->instances) s->triangle_count_instanced += s->meshes[inst.geometry_idx].tris.size() / 3;
+
+  // Shape lights: SceneModule::LoadShapeLight (src/core/SceneModule.cpp:1203-1304).
+  s->shape_lights.clear();
+  s->shape_light_table.clear();
+  for (uint32_t pi = 0; pi < ni; ++pi) {
+    const Instance& inst = s->instances[pi];
+    const Material& mat = s->materials[inst.material_idx];
+    if (mat.material_type != kLightMtl) continue;
+    const mat4& otw = s->transforms[inst.transform_idx];
+    const vec3 c = mat.light_mtl.light_color;
+    const float irradiance = (c.x + c.y + c.z) * mat.light_mtl.intensity * kPi;
+    const HostMesh& m = s->meshes[inst.geometry_idx];
+    if (m.kind == kGeoSphere) {
+      // the transform's own scale stretches the sphere into an ellipsoid;
+      // its area is approximated as (4/3) pi (ab + bc + ca)
+      const vec3 sc = s->transform_scales[inst.transform_idx];
+      const float a = m.radius * sc.x, b = m.radius * sc.y, c3 = m.radius * sc.z;
+      const float area = (4.0f / 3.0f) * kPi * (a * b + b * c3 + c3 * a);
+      s->shape_lights.push_back(ShapeLight{pi, kEmpty, irradiance * area, area});
+      continue;
+    }
+    for (uint32_t t = 0; t < m.tris.size() / 3; ++t) {
+      vec3 p[3];
+      for (int k = 0; k < 3; ++k) {
+        const uint32_t vi = m.pos_idx[m.tris[3 * t + k]];
+        p[k] = transform_position(otw, vec3(m.pos[3 * vi], m.pos[3 * vi + 1], m.pos[3 * vi + 2]));
+      }
+      const float area = length(cross(p[1] - p[0], p[2] - p[0]));
+      s->shape_lights.push_back(ShapeLight{pi, t, irradiance * area, 0.5f * area});
+    }
+  }
+  {
+    float total = 0.0f;
+    s->shape_light_table.resize(s->shape_lights.size());
+    for (size_t i = 0; i < s->shape_lights.size(); ++i) {
+      total += s->shape_lights[i].power;
+      s->shape_light_table[i] = total;
+    }
+    const float rcp = safe_rcp(total);
+    for (float& v : s->shape_light_table) v = total == 0.0f ? 0.0f : (v * rcp);
+  }
+
+  return YMRT_OK;
+}
+
+int set_transforms(HostScene* s, uint32_t first, uint32_t count, const float* object_to_world,
+                   const float* world_to_object, const float* scales, std::string* error) {
+  if (!object_to_world || first > s->transforms.size() || count > s->transforms.size() - first) {
+    if (error) *error = "transform range out of bounds";
+    return YMRT_ERR_INVALID;
+  }
+  for (uint32_t k = 0; k < count; ++k) {
+    mat4 m, mi;
+    std::memcpy(&m, object_to_world + 16 * (size_t)k, sizeof(mat4));
+    if (world_to_object) std::memcpy(&mi, world_to_object + 16 * (size_t)k, sizeof(mat4));
+    else mi = mat4_inverse(m);
+    s->transforms[first + k] = m;
+    s->i_transforms[first + k] = mi;
+    if (scales) {
+      const float* sc = scales + 3 * (size_t)k;
+      s->transform_scales[first + k] = vmax(vec3(0.0001f), vec3(sc[0], sc[1], sc[2]));
+    }
+  }
+  const int rc = build_top_level(s, error);
+  if (rc != YMRT_OK) return rc;
+  init_camera_transfer(s);
+  return YMRT_OK;
+}
 
 int prepare_scene(HostScene* s, int width, int height, std::string* error) {
   if (width <= 0 || height <= 0) {
@@ -1449,73 +1223,8 @@ int prepare_scene(HostScene* s, int width, int height, std::string* error) {
     s->geo_desc.push_back(gd);
   }
 
-  // Top level: the reference's instance order, then a wide BVH.
-  const uint32_t ni = (uint32_t)s->instances.size();
-  if (ni == 0) {
-    if (error) *error = "scene has no instances";
-    return YMRT_ERR_INVALID;
-  }
-  std::vector<BuildItem> items(ni);
-  for (uint32_t i = 0; i < ni; ++i) {
-    const Instance& inst = s->instances[i];
-    items[i].box = box_transform(s->meshes[inst.geometry_idx].root_box, s->transforms[inst.transform_idx]);
-    items[i].center = box_center(items[i].box);
-    items[i].idx = i;
-  }
-  std::vector<BinNode> tbin = build_binary(items);
-  std::vector<Instance> reordered(ni);
-  s->instance_file_index.assign(ni, 0);
-  for (uint32_t i = 0; i < ni; ++i) {
-    reordered[i] = s->instances[items[i].idx];
-    s->instance_file_index[i] = items[i].idx;
-  }
-  s->instances.swap(reordered);
-  s->tlas_nodes.clear();
-  s->tlas_prims.clear();
-  build_wide(tbin, &s->tlas_nodes, &s->tlas_prims, s->max_leaf_prims);
-  s->triangle_count_instanced = 0;
-  for (const Instance& inst : s->instances) s->triangle_count_instanced += s->meshes[inst.geometry_idx].tris.size() / 3;
-
-  // Shape lights: SceneModule::LoadShapeLight (src/core/SceneModule.cpp:1203-1304).
-  s->shape_lights.clear();
-  s->shape_light_table.clear();
-  for (uint32_t pi = 0; pi < ni; ++pi) {
-    const Instance& inst = s->instances[pi];
-    const Material& mat = s->materials[inst.material_idx];
-    if (mat.material_type != kLightMtl) continue;
-    const mat4& otw = s->transforms[inst.transform_idx];
-    const vec3 c = mat.light_mtl.light_color;
-    const float irradiance = (c.x + c.y + c.z) * mat.light_mtl.intensity * kPi;
-    const HostMesh& m = s->meshes[inst.geometry_idx];
-    if (m.kind == kGeoSphere) {
-      // the transform's own scale stretches the sphere into an ellipsoid;
-      // its area is approximated as (4/3) pi (ab + bc + ca)
-      const vec3 sc = s->transform_scales[inst.transform_idx];
-      const float a = m.radius * sc.x, b = m.radius * sc.y, c3 = m.radius * sc.z;
-      const float area = (4.0f / 3.0f) * kPi * (a * b + b * c3 + c3 * a);
-      s->shape_lights.push_back(ShapeLight{pi, kEmpty, irradiance * area, area});
-      continue;
-    }
-    for (uint32_t t = 0; t < m.tris.size() / 3; ++t) {
-      vec3 p[3];
-      for (int k = 0; k < 3; ++k) {
-        const uint32_t vi = m.pos_idx[m.tris[3 * t + k]];
-        p[k] = transform_position(otw, vec3(m.pos[3 * vi], m.pos[3 * vi + 1], m.pos[3 * vi + 2]));
-      }
-      const float area = length(cross(p[1] - p[0], p[2] - p[0]));
-      s->shape_lights.push_back(ShapeLight{pi, t, irradiance * area, 0.5f * area});
-    }
-  }
-  {
-    float total = 0.0f;
-    s->shape_light_table.resize(s->shape_lights.size());
-    for (size_t i = 0; i < s->shape_lights.size(); ++i) {
-      total += s->shape_lights[i].power;
-      s->shape_light_table[i] = total;
-    }
-    const float rcp = safe_rcp(total);
-    for (float& v : s->shape_light_table) v = total == 0.0f ? 0.0f : (v * rcp);
-  }
+  int rc = build_top_level(s, error);
+  if (rc != YMRT_OK) return rc;
 
   // Camera: SceneParser -> Camera::SetFov/SetPosition/SetDir (src/Camera.h:32,
   // 235-238, 301-311), then the rendering camera's aspect ratio.

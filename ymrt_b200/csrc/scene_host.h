@@ -14,17 +14,13 @@
 
 #include <vector_types.h>
 
+#include "bvh_build.h"
 #include "ymrt_scene.h"
 
 struct ymrt_scene_desc;
 struct ymrt_texture_desc;
 
 namespace ym {
-
-struct BBox {
-  vec3 pmax{kFloatMin, kFloatMin, kFloatMin};
-  vec3 pmin{kFloatMax, kFloatMax, kFloatMax};
-};
 
 // One geometry: a triangle mesh, or (kind kGeoSphere) an analytic sphere of
 // `radius` with no triangles.
@@ -80,6 +76,22 @@ int load_arrays(const ymrt_scene_desc* desc, HostScene* scene, std::string* erro
 // Builds BVHs, orders instances/triangles/lights like the reference, sets up
 // the rendering camera for a width x height image and flattens the arrays.
 int prepare_scene(HostScene* scene, int width, int height, std::string* error);
+
+// The top level of a prepared scene rebuilt from its current instance
+// order: instance boxes, the reference's binary SAH build of them (the new
+// instance order), the wide top-level BVH and the shape-light table.
+int build_top_level(HostScene* scene, std::string* error);
+
+// Replaces transforms first .. first+count-1 of a prepared scene (16 floats
+// each, column major; world_to_object NULL: inverted here; scales NULL: kept)
+// and rebuilds the top level and the camera's nested-media stack, as the
+// reference's editor does after a transform edit.
+int set_transforms(HostScene* scene, uint32_t first, uint32_t count, const float* object_to_world,
+                   const float* world_to_object, const float* scales, std::string* error);
+
+// The direction of the ray Camera::InitCameraRayTransfer casts from the
+// camera (through the image centre) to find the media it sits in.
+vec3 camera_media_ray(const CameraDesc& cam);
 
 // Texture nodes in the words of ymrt_texture_desc (include/ymrt.h).
 constexpr int kTextureWords = 20;
