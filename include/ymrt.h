@@ -464,6 +464,11 @@ int ymrt_debug_texture(ymrt_scene* scene, uint32_t texture_index, int n, const f
  * 6 records of prim, ior, priority, volume). words receives up to n_words
  * words (42 in all); clear != 0 resets the record afterwards. */
 int ymrt_debug_bound_record(ymrt_context* ctx, uint32_t* words, size_t n_words, int clear);
+/* Fault injection for tests of the error paths (no counterpart in the
+ * reference): the next `count` device allocations this library makes fail
+ * as out of memory (the call that needs them returns YMRT_ERR_OOM and leaves
+ * the context usable); 0 stops it. */
+void ymrt_debug_fail_allocations(int count);
 int ymrt_debug_occluded(ymrt_scene* scene, int n, const float* origin, const float* dir, const float* tmax,
                         int* occluded);
 int ymrt_debug_halton(ymrt_scene* scene, int n, const int* px, const int* py, const int* sample, int n_dims,

@@ -105,3 +105,18 @@ def test_reference_bvh_depth_fits_its_stack(name, scene_dir, halton_perm, oracle
     ref = oracle.RefScene(scenes.scene_path(name, 0, scene_dir), halton_perm, 64, 64)
     depths = ref.bvh_depths()
     assert depths.max() + 1 <= 32, depths
+
+
+def test_loader_rejects_malformed_values(tmp_path):
+    """Malformed values: a non-number in a vector, an unterminated block, a
+    reference to an undeclared name; each is YMRT_ERR_FORMAT with a message
+    naming the file, nothing thrown across the C ABI."""
+    cases = [
+        'Begin(Transform);\n\tname = "t";\n\ttranslate = <1,x,3>;\nEnd(Transform);\n',
+        'Begin(Transform);\n\tname = "t";\n\ttranslate = <1,2,3>;\n',
+        'Begin(PrimitiveInstance);\n\tname = "i";\n\tgeometry_index = "missing";\nEnd(PrimitiveInstance);\n',
+    ]
+    for k, text in enumerate(cases):
+        with pytest.raises(Y.YmrtError) as e:
+            Y.HostScene(write(tmp_path, text, f"bad{k}.ymtmp"), 8, 8)
+        assert e.value.code == -3, (k, e.value)

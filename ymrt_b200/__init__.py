@@ -150,6 +150,8 @@ def library():
     L.ymrt_debug_occluded.argtypes = [vp, i, vp, vp, vp, vp]
     L.ymrt_debug_halton.argtypes = [vp, i, vp, vp, vp, i, vp, vp, vp]
     L.ymrt_debug_bound_record.argtypes = [vp, vp, sz, i]
+    L.ymrt_debug_fail_allocations.argtypes = [i]
+    L.ymrt_debug_fail_allocations.restype = None
     L.ymrt_scene_set_transforms.argtypes = [vp, ctypes.c_uint32, ctypes.c_uint32, vp, vp, vp]
     L.ymrt_host_scene_set_transforms.argtypes = [vp, ctypes.c_uint32, ctypes.c_uint32, vp, vp, vp]
     L.ymrt_scene_download.restype = ctypes.c_longlong

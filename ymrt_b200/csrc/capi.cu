@@ -11,6 +11,7 @@
 #include <functional>
 #include <map>
 #include <memory>
+#include <atomic>
 #include <condition_variable>
 #include <mutex>
 #include <new>
@@ -32,6 +33,10 @@ namespace {
 
 thread_local std::string g_last_error;
 
+// Device allocations still to fail on purpose (ymrt_debug_fail_allocations):
+// a host-side fault injection for the error paths of allocation failures.
+std::atomic<int> g_failing_allocations{0};
+
 struct DeviceBuffer {
   void* ptr = nullptr;
   size_t bytes = 0;
@@ -44,6 +49,7 @@ struct DeviceBuffer {
   cudaError_t ensure(size_t n) {
     if (n <= bytes && ptr) return cudaSuccess;
     release();
+    if (g_failing_allocations.load() > 0 && g_failing_allocations.fetch_sub(1) > 0) return cudaErrorMemoryAllocation;
     cudaError_t e = cudaMalloc(&ptr, n ? n : 16);
     if (e == cudaSuccess) bytes = n;
     return e;
@@ -2086,6 +2092,8 @@ int ymrt_debug_occluded(ymrt_scene* sc, int n, const float* origin, const float*
   if (errs) return ctx->fail(YMRT_ERR_OVERFLOW, "traversal stack overflow");
   return YMRT_OK;
 }
+
+void ymrt_debug_fail_allocations(int count) { g_failing_allocations.store(count > 0 ? count : 0); }
 
 int ymrt_debug_bound_record(ymrt_context* ctx, uint32_t* words, size_t n_words, int clear) {
   if (!ctx || (!words && n_words > 0)) return YMRT_ERR_INVALID;
