@@ -126,6 +126,9 @@ int ymrt_set_profiling(ymrt_context* ctx, int enable);
 #define YMRT_OPT_SORT_HITS 1
 #define YMRT_OPT_DEFER_SHADOWS 2
 #define YMRT_OPT_GRAPH_LOOP 3
+/*   YMRT_OPT_TRACE_BLOCK   (default 128) threads per block of the closest-hit
+ *                          and shadow-ray kernels: 64, 128 or 256 */
+#define YMRT_OPT_TRACE_BLOCK 4
 int ymrt_set_option(ymrt_context* ctx, int option, int value);
 int ymrt_get_option(const ymrt_context* ctx, int option, int* value);
 

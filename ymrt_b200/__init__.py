@@ -170,7 +170,7 @@ def _check(rc: int, ctx=None):
         raise YmrtError(rc, msg)
 
 
-OPTIONS = {"sort_hits": 1, "defer_shadows": 2, "graph_loop": 3}
+OPTIONS = {"sort_hits": 1, "defer_shadows": 2, "graph_loop": 3, "trace_block": 4}
 
 
 class Context:

@@ -2,10 +2,12 @@
 
 Picks, by measuring on the GPU, the configuration that renders a workload
 fastest: path-queue capacity (paths in flight per wave), material-sorted
-shading on/off, deferred shadow rays on/off, the CUDA-graph wave loop on/off
-and the wide-BVH leaf size. The search is exhaustive over a small space
-(the defaults below: 3 x 2 x 2 x 3 = 36 points, two wave-loop kinds only when
-asked), each point timed on a sample of the workload (a band of tiles from
+shading on/off, deferred shadow rays on/off, the block shape of the
+closest-hit and shadow-ray kernels (threads per block), the CUDA-graph wave
+loop on/off and the wide-BVH leaf size. The search is exhaustive over a
+small space (the defaults below: 3 x 2 x 2 x 3 x 3 = 108 points, two
+wave-loop kinds only when asked), each point timed on a sample of the
+workload (a band of tiles from
 the middle of the frame, large enough to fill several waves) after one
 warm-up render; results are cached in a JSON file keyed by the workload.
 
@@ -25,10 +27,11 @@ DEFAULT_SPACE: Dict[str, List[int]] = {
     "queue_capacity": [1 << 20, 1 << 21, 1 << 22],
     "sort_hits": [0, 1],
     "defer_shadows": [0, 1],
+    "trace_block": [64, 128, 256],
     "max_leaf_triangles": [2, 3, 4],
 }
 
-WAVE_OPTIONS = ("sort_hits", "defer_shadows", "graph_loop")
+WAVE_OPTIONS = ("sort_hits", "defer_shadows", "graph_loop", "trace_block")
 
 
 def points(space: Dict[str, Iterable[int]]) -> List[Dict[str, int]]:
@@ -155,7 +158,7 @@ def tune_scene(path: str, width: int, height: int, setting, halton_perm, device:
 
 def tune_batch(ctx, renders, space: Optional[Dict[str, Iterable[int]]] = None, repeats: int = 2) -> Dict[str, object]:
     """Tunes the context-level choices (queue capacity, sorting, deferral,
-    graph loop) for a batch of renders as ymrt_b200.render_batch takes them;
+    block shape, graph loop) for a batch of renders as ymrt_b200.render_batch takes them;
     leaves the best configuration applied to `ctx`."""
     from . import render_batch
 

@@ -111,6 +111,7 @@ struct ymrt_context {
   WaveCounters batch_counters{};  // frame totals across the launch groups of one batch
   // wave options (ymrt_set_option)
   bool sort_hits = true;
+  uint32_t trace_block = 128;  // threads per block of k_extend / k_connect (YMRT_OPT_TRACE_BLOCK)
   bool defer_shadows = true;
   DeviceBuffer shadow_buf;
   ShadowQueue shadow_queue{};
@@ -408,6 +409,11 @@ int ymrt_set_option(ymrt_context* ctx, int option, int value) {
     case YMRT_OPT_SORT_HITS: ctx->sort_hits = value != 0; return YMRT_OK;
     case YMRT_OPT_DEFER_SHADOWS: ctx->defer_shadows = value != 0; return YMRT_OK;
     case YMRT_OPT_GRAPH_LOOP: ctx->graph_loop = value != 0; return YMRT_OK;
+    case YMRT_OPT_TRACE_BLOCK:
+      if (value != 64 && value != 128 && value != 256)
+        return ctx->fail(YMRT_ERR_INVALID, "YMRT_OPT_TRACE_BLOCK must be 64, 128 or 256");
+      ctx->trace_block = (uint32_t)value;
+      return YMRT_OK;
     default: return ctx->fail(YMRT_ERR_INVALID, "unknown option " + std::to_string(option));
   }
 }
@@ -418,6 +424,7 @@ int ymrt_get_option(const ymrt_context* ctx, int option, int* value) {
     case YMRT_OPT_SORT_HITS: *value = ctx->sort_hits ? 1 : 0; return YMRT_OK;
     case YMRT_OPT_DEFER_SHADOWS: *value = ctx->defer_shadows ? 1 : 0; return YMRT_OK;
     case YMRT_OPT_GRAPH_LOOP: *value = ctx->graph_loop ? 1 : 0; return YMRT_OK;
+    case YMRT_OPT_TRACE_BLOCK: *value = (int)ctx->trace_block; return YMRT_OK;
     default: return YMRT_ERR_INVALID;
   }
 }
@@ -859,6 +866,7 @@ int run_batch(ymrt_context* ctx, const BatchMemory& M, std::vector<JobDesc>& job
         (uintptr_t)M.pool[0].ray_o, (uintptr_t)M.pool[1].ray_o, (uintptr_t)M.hits.bary_t, (uintptr_t)M.ctl,
         (uintptr_t)M.jobs, (uintptr_t)M.counters, (uintptr_t)jobs.size(), (uintptr_t)o.volumes,
         (uintptr_t)o.sort_hits, (uintptr_t)o.defer_shadows, (uintptr_t)o.shadow_queue.o, M.capacity,
+        (uintptr_t)o.trace_block,
         (uintptr_t)o.features, (uintptr_t)o.grid_grads, (uintptr_t)o.grid_tex,
         (uintptr_t)o.adjoint, (uintptr_t)o.grads, o.grad_materials};
     if (ctx->graph_key != key) {
@@ -1002,6 +1010,7 @@ int batch_options(ymrt_context* ctx, const std::vector<JobDesc>& jobs, WaveOptio
     clamp = clamp || j.setting.enable_indirect_clamp;
   }
   opt->sort_hits = ctx->sort_hits;
+  opt->trace_block = ctx->trace_block;
   opt->defer_shadows = ctx->defer_shadows && !opt->volumes && !clamp;
   if (opt->defer_shadows) {
     int rc = ctx->ensure_shadow_queue();
@@ -1197,6 +1206,7 @@ int ymrt_render_backward_ex(ymrt_context* ctx, const ymrt_job* jobs_in, int n_jo
   WaveOptions opt;
   opt.adjoint = true;
   opt.volumes = volumes;
+  opt.trace_block = ctx->trace_block;
   opt.features = batch_features(slots.data(), slots.size());
   opt.grads = materials ? tg->material_grads_device : nullptr;
   opt.grad_materials = materials ? tg->n_materials : 0;

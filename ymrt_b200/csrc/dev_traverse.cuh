@@ -27,7 +27,8 @@ namespace ym {
 
 constexpr int kStackShared = 32;  // entries per thread in shared memory
 constexpr int kStackLocal = 64;   // further entries per thread in local memory
-constexpr int kTraceBlock = 128;  // threads per block of the traversal kernels
+constexpr int kTraceBlock = 128;  // threads per block of the traversal kernels (default)
+constexpr int kMaxTraceBlock = 256;  // largest block k_extend and k_connect are launched with
 
 // Stack entries carry the entry distance of the box that produced them, so a
 // pop can drop entries that lie beyond the current closest hit. An entry with
@@ -35,22 +36,24 @@ constexpr int kTraceBlock = 128;  // threads per block of the traversal kernels
 constexpr uint32_t kInstanceEntry = 0x80000000u;
 
 struct TraversalStack {
-  uint32_t* sh;   // shared-memory column of this thread: entries (stride kTraceBlock)
+  uint32_t* sh;   // shared-memory column of this thread: entries (stride: the block's threads)
   float* sht;     // shared-memory column of this thread: entry distances
   uint32_t loc[kStackLocal];
   float loct[kStackLocal];
   int sp;
+  int stride;
   bool overflow;
   __device__ __forceinline__ void bind(uint32_t* shared_entries, float* shared_t) {
     sh = shared_entries + threadIdx.x;
     sht = shared_t + threadIdx.x;
+    stride = (int)blockDim.x;
     sp = 0;
     overflow = false;
   }
   __device__ __forceinline__ void push(uint32_t v, float t = 0.0f) {
     if (sp < kStackShared) {
-      sh[sp * kTraceBlock] = v;
-      sht[sp * kTraceBlock] = t;
+      sh[sp * stride] = v;
+      sht[sp * stride] = t;
     } else if (sp < kStackShared + kStackLocal) {
       loc[sp - kStackShared] = v;
       loct[sp - kStackShared] = t;
@@ -63,8 +66,8 @@ struct TraversalStack {
   __device__ __forceinline__ uint32_t pop(float* t) {
     --sp;
     if (sp < kStackShared) {
-      *t = sht[sp * kTraceBlock];
-      return sh[sp * kTraceBlock];
+      *t = sht[sp * stride];
+      return sh[sp * stride];
     }
     *t = loct[sp - kStackShared];
     return loc[sp - kStackShared];
@@ -75,6 +78,13 @@ struct TraversalStack {
 #define YM_TRAVERSAL_SHARED(name)                                      \
   __shared__ uint32_t name##_entries[kStackShared * kTraceBlock];      \
   __shared__ float name##_t[kStackShared * kTraceBlock]
+// The same, in the dynamic shared memory of a kernel launched with any block
+// size up to kMaxTraceBlock (traversal_shared_bytes of it).
+#define YM_TRAVERSAL_SHARED_DYNAMIC(name)                                              \
+  extern __shared__ __align__(16) uint32_t name##_dyn[];                               \
+  uint32_t* name##_entries = name##_dyn;                                               \
+  float* name##_t = reinterpret_cast<float*>(name##_dyn + kStackShared * blockDim.x)
+constexpr size_t traversal_shared_bytes(uint32_t block) { return (size_t)kStackShared * block * 8u; }
 
 // The far end of the box-test interval for a ray whose closest hit so far is
 // at t: boxes are widened by 1e-6 relative, and so is this bound, so a box
@@ -662,20 +672,23 @@ __device__ __noinline__ bool trace_occluded_impl(uint32_t scene, TraversalStack&
 // the triangles of its leaf children tested. Stack entries need no entry
 // distance here, so the stack is entries only.
 constexpr int kOccStackShared = 32;  // entries per thread in shared memory
-constexpr int kConnectBlocksPerSm = 8;
+constexpr int kConnectBlocksPerSm = 8;  // at kTraceBlock threads (the register budget of the launch bounds)
+constexpr size_t occluded_shared_bytes(uint32_t block) { return (size_t)kOccStackShared * block * 4u; }
 
 struct OccStack {
-  uint32_t* sh;  // shared-memory column of this thread (stride kTraceBlock)
+  uint32_t* sh;  // shared-memory column of this thread (stride: the block's threads)
   uint32_t loc[kStackLocal];
   int sp;
+  int stride;
   bool overflow;
   __device__ __forceinline__ void bind(uint32_t* shared_entries) {
     sh = shared_entries + threadIdx.x;
+    stride = (int)blockDim.x;
     sp = 0;
     overflow = false;
   }
   __device__ __forceinline__ void push(uint32_t v) {
-    if (sp < kOccStackShared) sh[sp * kTraceBlock] = v;
+    if (sp < kOccStackShared) sh[sp * stride] = v;
     else if (sp < kOccStackShared + kStackLocal) loc[sp - kOccStackShared] = v;
     else {
       overflow = true;
@@ -685,7 +698,7 @@ struct OccStack {
   }
   __device__ __forceinline__ uint32_t pop() {
     --sp;
-    return sp < kOccStackShared ? sh[sp * kTraceBlock] : loc[sp - kOccStackShared];
+    return sp < kOccStackShared ? sh[sp * stride] : loc[sp - kOccStackShared];
   }
 };
 

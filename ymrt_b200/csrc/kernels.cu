@@ -455,7 +455,7 @@ namespace {
 // walks its queue grid-stride; the per-path kernels get one thread per slot.
 struct PersistentGrids {
   int device = -1;
-  uint32_t connect = 0;
+  uint32_t connect[3] = {0, 0, 0};  // k_connect blocks for 64-, 128- and 256-thread blocks
 };
 PersistentGrids g_grids;
 
@@ -473,7 +473,7 @@ uint32_t grid_for(K kernel, int block, int sms) {
 template <uint32_t kF>
 void launch_extend_surface(const WaveArgs& w) {
   const auto k = k_extend<false, kF & kFeatSpheres>;
-  k<<<w.blocks, kTraceBlock, 0, w.stream>>>(w.A, w.ctl, w.H, w.jobs, w.counters, nullptr,
+  k<<<w.trace_blocks, w.trace_block, traversal_shared_bytes(w.trace_block), w.stream>>>(w.A, w.ctl, w.H, w.jobs, w.counters, nullptr,
                                                                    kEmpty);
 }
 
@@ -499,7 +499,18 @@ void prepare_persistent_grids() {
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   PersistentGrids g;
   g.device = dev;
-  g.connect = grid_for(k_connect<0>, kTraceBlock, sms);
+  for (int b = 0; b < 3; ++b) {
+    const int block = 64 << b;
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_connect<0>, block, occluded_shared_bytes(block)) !=
+            cudaSuccess || per_sm < 1)
+      per_sm = 1;
+    g.connect[b] = (uint32_t)(per_sm * sms);
+  }
+  allow_trace_shared(k_extend<false, 0>);
+  allow_trace_shared(k_extend<false, kFeatSpheres>);
+  prepare_media_kernels();
+  prepare_adjoint_kernels();
   g_grids = g;
 }
 
@@ -523,7 +534,8 @@ uint32_t launch_wave(const PathPool& A, const PathPool& B, const HitPool& H, Wav
   if (ev) cudaEventRecord(ev[0], stream);
   k_generate<<<blocks_256, 256, 0, stream>>>(A, ctl, jobs, n_jobs);
   if (ev) cudaEventRecord(ev[1], stream);
-  const WaveArgs w{A, B, Hs, ctl, jobs, counters, blocks_trace, stream};
+  const uint32_t tb = (opt.trace_block == 64 || opt.trace_block == 256) ? opt.trace_block : (uint32_t)kTraceBlock;
+  const WaveArgs w{A, B, Hs, ctl, jobs, counters, blocks_trace, stream, tb, (cap + tb - 1) / tb};
   if (adjoint && opt.volumes) {
     launch_adjoint_extend_media(w, opt);
   } else if (opt.volumes) {
@@ -550,8 +562,11 @@ uint32_t launch_wave(const PathPool& A, const PathPool& B, const HitPool& H, Wav
     }
   }
   if (ev) cudaEventRecord(ev[4], stream);
-  if (defer && (feat & kFeatSpheres)) k_connect<kFeatSpheres><<<g.connect, kTraceBlock, 0, stream>>>(*defer, jobs, counters);
-  else if (defer) k_connect<0><<<g.connect, kTraceBlock, 0, stream>>>(*defer, jobs, counters);
+  const uint32_t conn_grid = g.connect[tb == 64 ? 0 : (tb == 128 ? 1 : 2)];
+  if (defer && (feat & kFeatSpheres))
+    k_connect<kFeatSpheres><<<conn_grid, tb, occluded_shared_bytes(tb), stream>>>(*defer, jobs, counters);
+  else if (defer)
+    k_connect<0><<<conn_grid, tb, occluded_shared_bytes(tb), stream>>>(*defer, jobs, counters);
   if (ev) cudaEventRecord(ev[5], stream);
   k_finish<<<1, 32, 0, stream>>>(ctl, counters, graph_condition);
   return 5u + (sort_hits ? 1u : 0u) + (defer ? 1u : 0u);

@@ -167,6 +167,7 @@ struct WaveOptions {
   uint32_t grad_materials = 0;
   float* grid_grads = nullptr; // adjoint: dLoss/d(value) of the density grid at texture node grid_tex
   uint32_t grid_tex = 0xFFFFFFFFu;
+  uint32_t trace_block = 128;  // threads per block of k_extend and k_connect (64, 128 or 256)
 };
 // One wave's pools, control block, jobs and launch shape, for the launchers
 // of the media (wave_media.cu) and adjoint (wave_adjoint.cu) kernels.
@@ -178,7 +179,14 @@ struct WaveArgs {
   WaveCounters* counters;
   uint32_t blocks;  // kTraceBlock-thread blocks (one thread per pool slot)
   cudaStream_t stream;
+  uint32_t trace_block;   // k_extend's threads per block
+  uint32_t trace_blocks;  // k_extend's blocks (one thread per pool slot)
 };
+// Before any launch (and before any stream capture) on the current device:
+// lets the k_extend instantiations of the media and adjoint units take a
+// kMaxTraceBlock-thread block's dynamic shared memory.
+void prepare_media_kernels();
+void prepare_adjoint_kernels();
 void launch_media_extend(uint32_t features, const WaveArgs& w);
 void launch_media_shade(uint32_t features, const WaveArgs& w);
 void launch_adjoint_extend_media(const WaveArgs& w, const WaveOptions& opt);

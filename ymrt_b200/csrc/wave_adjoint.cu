@@ -22,7 +22,7 @@ void surface_adjoint_shade(const WaveArgs& w, const WaveOptions& opt) {
 void launch_adjoint_extend_media(const WaveArgs& w, const WaveOptions& opt) {
   // free flight with the density-grid terms (one instantiation, all features)
   const auto k = k_extend<true, kFeatAll, true>;
-  k<<<w.blocks, kTraceBlock, 0, w.stream>>>(w.A, w.ctl, w.H, w.jobs, w.counters,
+  k<<<w.trace_blocks, w.trace_block, traversal_shared_bytes(w.trace_block), w.stream>>>(w.A, w.ctl, w.H, w.jobs, w.counters,
                                                                            opt.grid_grads, opt.grid_tex);
 }
 
@@ -40,6 +40,8 @@ void launch_adjoint_shade(bool volumes, uint32_t features, const WaveArgs& w, co
     default: surface_adjoint_shade<kFeatSpheres | kFeatTextures>(w, opt); break;
   }
 }
+
+void prepare_adjoint_kernels() { allow_trace_shared(k_extend<true, kFeatAll, true>); }
 
 cudaError_t upload_slots_adjoint(const DeviceScene* scenes, const uint32_t* slots, uint32_t n, const uint32_t* primes,
                                  const uint32_t* prime_sums, cudaStream_t stream) {

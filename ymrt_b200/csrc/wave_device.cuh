@@ -123,14 +123,17 @@ __device__ __forceinline__ void file_bucket(WaveCounters* counters, uint32_t buc
 // radiance the path gathers after the segment (its recorded total minus what
 // it gathered so far).
 //
-// Four resident blocks per SM (128 registers): on the 1080p instanced frame
-// 3.3% faster than five (102 registers, spills in the traversal loop) and
-// 15% faster than three; k_connect, with less live state, keeps five.
+// Launched with kTraceBlock threads by default, or any block size up to
+// kMaxTraceBlock (YMRT_OPT_TRACE_BLOCK, tuned by ymrt_b200.autotune); the
+// traversal stacks are in dynamic shared memory (traversal_shared_bytes).
+// The launch bounds give 128 registers, four resident 128-thread blocks per
+// SM: on the 1080p instanced frame 3.3% faster than five (102 registers,
+// spills in the traversal loop) and 15% faster than three.
 template <bool kVol, uint32_t kF, bool kAdj = false>
-__global__ void __launch_bounds__(kTraceBlock, 4) k_extend(PathPool P, const WaveControl* __restrict__ ctl, HitPool H,
+__global__ void __launch_bounds__(kMaxTraceBlock, 4 * kTraceBlock / kMaxTraceBlock) k_extend(PathPool P, const WaveControl* __restrict__ ctl, HitPool H,
                                                            const JobDesc* __restrict__ jobs, WaveCounters* counters,
                                                            float* grid_grads = nullptr, uint32_t grid_tex = kEmpty) {
-  YM_TRAVERSAL_SHARED(s_stack);
+  YM_TRAVERSAL_SHARED_DYNAMIC(s_stack);
   const uint32_t count = ctl->count;
   uint32_t tests = 0, nodes = 0, n_rays = 0;
   bool overflow = false;
@@ -1164,10 +1167,10 @@ __global__ void __launch_bounds__(kTraceBlock) k_shade(PathPool P, const WaveCon
 // waiting for the warp's slowest ray; each loop iteration advances every busy
 // lane by one step of its own walk (occluded_step).
 template <uint32_t kF>
-__global__ void __launch_bounds__(kTraceBlock, kConnectBlocksPerSm) k_connect(ShadowQueue Q,
+__global__ void __launch_bounds__(kMaxTraceBlock, kConnectBlocksPerSm * kTraceBlock / kMaxTraceBlock) k_connect(ShadowQueue Q,
                                                                              const JobDesc* __restrict__ jobs,
                                                                              WaveCounters* counters) {
-  __shared__ uint32_t s_stack[kOccStackShared * kTraceBlock];
+  extern __shared__ __align__(16) uint32_t s_stack[];  // occluded_shared_bytes(blockDim.x)
   OccStack st;
   st.bind(s_stack);
   OccWalk w;
@@ -1232,6 +1235,14 @@ __global__ void __launch_bounds__(kTraceBlock, kConnectBlocksPerSm) k_connect(Sh
 constexpr uint32_t surface_features(uint32_t f) { return f & (kFeatSpheres | kFeatTextures); }
 constexpr uint32_t media_features(uint32_t f) {
   return (f & (kFeatGrids | kFeatTextures)) ? (f | kFeatGrids | kFeatTextures) : (f & kFeatSpheres);
+}
+
+// Lets a k_extend instantiation take the dynamic shared memory of a
+// kMaxTraceBlock-thread block (more than the default 48 KB).
+template <typename K>
+static void allow_trace_shared(K kernel) {
+  cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)traversal_shared_bytes(kMaxTraceBlock));
 }
 
 // Writes scenes[k] into this translation unit's constant slot slots[k]

@@ -12,7 +12,7 @@ namespace {
 template <uint32_t kF>
 void media_extend(const WaveArgs& w) {
   const auto k = k_extend<true, kF>;
-  k<<<w.blocks, kTraceBlock, 0, w.stream>>>(w.A, w.ctl, w.H, w.jobs, w.counters, nullptr,
+  k<<<w.trace_blocks, w.trace_block, traversal_shared_bytes(w.trace_block), w.stream>>>(w.A, w.ctl, w.H, w.jobs, w.counters, nullptr,
                                                                    kEmpty);
 }
 
@@ -43,6 +43,13 @@ void launch_media_shade(uint32_t features, const WaveArgs& w) {
     case kAllNodes: media_shade<kAllNodes>(w); break;
     default: media_shade<kAllNodes | kFeatSpheres>(w); break;
   }
+}
+
+void prepare_media_kernels() {
+  allow_trace_shared(k_extend<true, 0>);
+  allow_trace_shared(k_extend<true, kFeatSpheres>);
+  allow_trace_shared(k_extend<true, kAllNodes>);
+  allow_trace_shared(k_extend<true, kAllNodes | kFeatSpheres>);
 }
 
 cudaError_t upload_slots_media(const DeviceScene* scenes, const uint32_t* slots, uint32_t n, const uint32_t* primes,
