@@ -18,6 +18,7 @@
 #include <unordered_map>
 
 #include "../../include/ymrt.h"
+#include "image_decode.h"
 #include "png_decode.h"
 #include "sphere.h"
 
@@ -666,23 +667,45 @@ float srgb_to_linear(float s) {
 
 int load_image_texture(const std::string& path, uint32_t color_space, Texture* t, std::vector<float>* pixels,
                        std::string* error) {
+  std::vector<uint8_t> bytes;
   {
     std::ifstream f(path, std::ios::binary);
     if (!f) {
       if (error) *error = "cannot open " + path;
       return YMRT_ERR_IO;
     }
-    char sig[8] = {0};
-    f.read(sig, 8);
-    static const unsigned char kPng[8] = {137, 80, 78, 71, 13, 10, 26, 10};
-    if (f.gcount() == 8 && std::memcmp(sig, kPng, 8) != 0) {
-      if (error) *error = path + ": only PNG images are supported";
-      return YMRT_ERR_UNSUPPORTED;
-    }
+    bytes.assign(std::istreambuf_iterator<char>(f), std::istreambuf_iterator<char>());
   }
   PngImage img;
   try {
-    if (!decode_png_file(path, &img, error)) return YMRT_ERR_IO;
+    const ImageFormat fmt = sniff_image(bytes.data(), bytes.size());
+    if (fmt == ImageFormat::kPng) {
+      if (!decode_png(bytes.data(), bytes.size(), &img, error)) {
+        if (error) *error = path + ": " + *error;
+        return YMRT_ERR_IO;
+      }
+    } else {
+      Image8 im;
+      bool unsupported = false, ok = false;
+      std::string msg;
+      if (fmt == ImageFormat::kJpeg) ok = decode_jpeg(bytes.data(), bytes.size(), &im, &msg, &unsupported);
+      else if (fmt == ImageFormat::kHdr) ok = decode_hdr(bytes.data(), bytes.size(), &im, &msg);
+      else if (fmt == ImageFormat::kBmp) ok = decode_bmp(bytes.data(), bytes.size(), &im, &msg, &unsupported);
+      else if (fmt == ImageFormat::kTga) ok = decode_tga(bytes.data(), bytes.size(), &im, &msg, &unsupported);
+      else {
+        unsupported = true;
+        msg = "unknown image format";
+      }
+      if (!ok) {
+        if (error) *error = path + ": " + msg;
+        return unsupported ? YMRT_ERR_UNSUPPORTED : YMRT_ERR_IO;
+      }
+      img.width = im.width;
+      img.height = im.height;
+      img.channels = im.channels;
+      img.sixteen = false;
+      img.samples.assign(im.samples.begin(), im.samples.end());
+    }
   } catch (const std::bad_alloc&) {
     if (error) *error = path + ": out of memory decoding the image";
     return YMRT_ERR_IO;

@@ -335,6 +335,364 @@ def write_png(path: str, samples, depth: int = 8, color_type: int = 2, palette=N
     return path
 
 
+# Baseline JPEG writer (this project's encoder, for test images; ITU-T T.81
+# Annex K example quantisation and Huffman tables).
+_K_LUM_Q = [16, 11, 10, 16, 24, 40, 51, 61, 12, 12, 14, 19, 26, 58, 60, 55, 14, 13, 16, 24, 40, 57, 69, 56,
+            14, 17, 22, 29, 51, 87, 80, 62, 18, 22, 37, 56, 68, 109, 103, 77, 24, 35, 55, 64, 81, 104, 113, 92,
+            49, 64, 78, 87, 103, 121, 120, 101, 72, 92, 95, 98, 112, 100, 103, 99]
+_K_CHR_Q = [17, 18, 24, 47, 99, 99, 99, 99, 18, 21, 26, 66, 99, 99, 99, 99, 24, 26, 56, 99, 99, 99, 99, 99,
+            47, 66, 99, 99, 99, 99, 99, 99] + [99] * 32
+_K_DC_LUM = ([0, 1, 5, 1, 1, 1, 1, 1, 1, 0, 0, 0, 0, 0, 0, 0], list(range(12)))
+_K_DC_CHR = ([0, 3, 1, 1, 1, 1, 1, 1, 1, 1, 1, 0, 0, 0, 0, 0], list(range(12)))
+_K_AC_LUM = ([0, 2, 1, 3, 3, 2, 4, 3, 5, 5, 4, 4, 0, 0, 1, 0x7d], bytes.fromhex(
+    "01020300041105122131410613516107227114328191a1082342b1c11552d1f02433627282090a161718191a25262728292a3435363738"
+    "393a434445464748494a535455565758595a636465666768696a737475767778797a838485868788898a92939495969798999aa2a3a4a5"
+    "a6a7a8a9aab2b3b4b5b6b7b8b9bac2c3c4c5c6c7c8c9cad2d3d4d5d6d7d8d9dae1e2e3e4e5e6e7e8e9eaf1f2f3f4f5f6f7f8f9fa"))
+_K_AC_CHR = ([0, 2, 1, 2, 4, 4, 3, 4, 7, 5, 4, 4, 0, 1, 2, 0x77], bytes.fromhex(
+    "000102031104052131061241510761711322328108144291a1b1c109233352f0156272d10a162434e125f11718191a262728292a35363738"
+    "393a434445464748494a535455565758595a636465666768696a737475767778797a82838485868788898a92939495969798999aa2a3a4a5"
+    "a6a7a8a9aab2b3b4b5b6b7b8b9bac2c3c4c5c6c7c8c9cad2d3d4d5d6d7d8d9dae2e3e4e5e6e7e8e9eaf2f3f4f5f6f7f8f9fa"))
+_ZIGZAG = [0, 1, 8, 16, 9, 2, 3, 10, 17, 24, 32, 25, 18, 11, 4, 5, 12, 19, 26, 33, 40, 48, 41, 34, 27, 20, 13, 6, 7, 14,
+           21, 28, 35, 42, 49, 56, 57, 50, 43, 36, 29, 22, 15, 23, 30, 37, 44, 51, 58, 59, 52, 45, 38, 31, 39, 46, 53,
+           60, 61, 54, 47, 55, 62, 63]
+
+
+def _huff_codes(counts, symbols):
+    codes, code, k = {}, 0, 0
+    for length in range(1, 17):
+        for _ in range(counts[length - 1]):
+            codes[symbols[k]] = (code, length)
+            code += 1
+            k += 1
+        code <<= 1
+    return codes
+
+
+class _BitWriter:
+    def __init__(self):
+        self.out = bytearray()
+        self.acc = 0
+        self.n = 0
+
+    def put(self, value, length):
+        for b in range(length - 1, -1, -1):
+            self.acc = (self.acc << 1) | ((value >> b) & 1)
+            self.n += 1
+            if self.n == 8:
+                self.out.append(self.acc)
+                if self.acc == 0xFF:
+                    self.out.append(0)
+                self.acc = self.n = 0
+
+    def flush(self):
+        while self.n:
+            self.put(1, 1)
+
+
+def write_jpeg(path: str, samples, quality: int = 75, subsampling: str = "420", restart: int = 0,
+               adobe_rgb: bool = False) -> str:
+    """Writes a baseline JPEG (this project's encoder, for test images):
+    samples (h, w) grey or (h, w, 3) RGB uint8, top row first; chroma
+    subsampling "444", "422" or "420"; a restart marker every `restart` MCUs
+    (0: none); adobe_rgb: store R, G, B without colour transform (Adobe APP14
+    transform 0, no JFIF marker)."""
+    import struct
+    img = np.asarray(samples, np.float64)
+    grey = img.ndim == 2
+    h, w = img.shape[:2]
+    scale = 5000 // quality if quality < 50 else 200 - 2 * quality
+    def qtab(base):
+        return [min(255, max(1, (b * scale + 50) // 100)) for b in base]
+    ql, qc = qtab(_K_LUM_Q), qtab(_K_CHR_Q)
+    if grey:
+        planes = [img]
+        sf = [(1, 1)]
+    else:
+        r, g, b = img[..., 0], img[..., 1], img[..., 2]
+        if adobe_rgb:
+            planes = [r, g, b]
+            sf = [(1, 1)] * 3
+        else:
+            y = 0.299 * r + 0.587 * g + 0.114 * b
+            cb = -0.168736 * r - 0.331264 * g + 0.5 * b + 128
+            cr = 0.5 * r - 0.418688 * g - 0.081312 * b + 128
+            hs, vs = {"444": (1, 1), "422": (2, 1), "420": (2, 2)}[subsampling]
+            planes = [y, cb, cr]
+            sf = [(hs, vs), (1, 1), (1, 1)]
+    hmax, vmax = max(f[0] for f in sf), max(f[1] for f in sf)
+    mx, my = -(-w // (8 * hmax)), -(-h // (8 * vmax))
+    n_comp = len(planes)
+    comp_planes = []
+    for k, pl in enumerate(planes):
+        ch, cv = sf[k]
+        dx, dy = hmax // ch, vmax // cv
+        pw, ph = mx * ch * 8, my * cv * 8
+        full = np.pad(pl, ((0, my * vmax * 8 - h), (0, mx * hmax * 8 - w)), mode="edge")
+        sub = full.reshape(ph, dy, pw, dx).mean(axis=(1, 3))
+        comp_planes.append(sub - 128.0)
+    # orthonormal 8-point DCT-II
+    n = np.arange(8)
+    C = np.cos((2 * n[None, :] + 1) * n[:, None] * np.pi / 16) * np.sqrt(2 / 8)
+    C[0] /= np.sqrt(2)
+    tabs = [ql] + [qc] * (n_comp - 1) if not adobe_rgb else [ql] * n_comp
+    dc_codes = [_huff_codes(*_K_DC_LUM), _huff_codes(*_K_DC_CHR)]
+    ac_codes = [_huff_codes(*_K_AC_LUM), _huff_codes(*_K_AC_CHR)]
+    tsel = [0] + [1] * (n_comp - 1) if not adobe_rgb else [0] * n_comp
+    bw = _BitWriter()
+    pred = [0] * n_comp
+
+    def bits_of(v):
+        m = abs(v)
+        nbits = m.bit_length()
+        return nbits, (v if v >= 0 else v + (1 << nbits) - 1)
+
+    def block(k, by, bx):
+        blk = comp_planes[k][by * 8:by * 8 + 8, bx * 8:bx * 8 + 8]
+        coef = C @ blk @ C.T
+        zz = coef.reshape(64)[_ZIGZAG]
+        qz = np.rint(zz / np.array(tabs[k], np.float64)).astype(int)
+        diff = int(qz[0]) - pred[k]
+        pred[k] = int(qz[0])
+        nb, v = bits_of(diff)
+        c, l = dc_codes[tsel[k]][nb]
+        bw.put(c, l)
+        if nb:
+            bw.put(v, nb)
+        run = 0
+        for i in range(1, 64):
+            a = int(qz[i])
+            if a == 0:
+                run += 1
+                continue
+            while run > 15:
+                c, l = ac_codes[tsel[k]][0xF0]
+                bw.put(c, l)
+                run -= 16
+            nb, v = bits_of(a)
+            c, l = ac_codes[tsel[k]][(run << 4) | nb]
+            bw.put(c, l)
+            bw.put(v, nb)
+            run = 0
+        if run:
+            c, l = ac_codes[tsel[k]][0x00]
+            bw.put(c, l)
+
+    data = bytearray()
+    mcu, rst = 0, 0
+    if n_comp == 1:
+        units = [(0, by, bx) for by in range(-(-h // 8)) for bx in range(-(-w // 8))]
+        groups = [[u] for u in units]
+    else:
+        groups = []
+        for j in range(my):
+            for i in range(mx):
+                groups.append([(k, j * sf[k][1] + y, i * sf[k][0] + x) for k in range(n_comp)
+                               for y in range(sf[k][1]) for x in range(sf[k][0])])
+    for g in groups:
+        if restart and mcu and mcu % restart == 0:
+            bw.flush()
+            data += bw.out + bytes([0xFF, 0xD0 + rst])
+            bw.out = bytearray()
+            rst = (rst + 1) & 7
+            pred = [0] * n_comp
+        for k, by, bx in g:
+            block(k, by, bx)
+        mcu += 1
+    bw.flush()
+    data += bw.out
+
+    def seg(marker, body):
+        return bytes([0xFF, marker]) + struct.pack(">H", len(body) + 2) + body
+
+    out = b"\xff\xd8"
+    if adobe_rgb:
+        out += seg(0xEE, b"Adobe" + bytes([0, 100, 0, 0, 0, 0, 0]))
+    else:
+        out += seg(0xE0, b"JFIF\x00\x01\x01\x00\x00\x01\x00\x01\x00\x00")
+    out += seg(0xDB, bytes([0]) + bytes(ql))
+    if n_comp > 1 and not adobe_rgb:
+        out += seg(0xDB, bytes([1]) + bytes(qc))
+    out += seg(0xC0, struct.pack(">BHHB", 8, h, w, n_comp) + b"".join(
+        bytes([k + 1, (sf[k][0] << 4) | sf[k][1], 0 if (k == 0 or adobe_rgb) else 1]) for k in range(n_comp)))
+    for cls, tabsel, spec in ((0, 0, _K_DC_LUM), (1, 0, _K_AC_LUM), (0, 1, _K_DC_CHR), (1, 1, _K_AC_CHR)):
+        if tabsel == 1 and (n_comp == 1 or adobe_rgb):
+            continue
+        out += seg(0xC4, bytes([(cls << 4) | tabsel]) + bytes(spec[0]) + bytes(spec[1]))
+    if restart:
+        out += seg(0xDD, struct.pack(">H", restart))
+    out += seg(0xDA, bytes([n_comp]) + b"".join(
+        bytes([k + 1, 0x00 if (k == 0 or adobe_rgb) else 0x11]) for k in range(n_comp)) + bytes([0, 63, 0]))
+    out += bytes(data) + b"\xff\xd9"
+    with open(path, "wb") as f:
+        f.write(out)
+    return path
+
+
+def write_hdr(path: str, rgb, rle: bool = True) -> str:
+    """Writes a Radiance RGBE file (this project's encoder, for test images):
+    rgb (h, w, 3) float, top row first; per-channel run-length scanlines when
+    rle (and 8 <= w < 32768), else flat pixels."""
+    img = np.asarray(rgb, np.float64)
+    h, w = img.shape[:2]
+    m = img.max(axis=2)
+    e = np.zeros((h, w), np.int64)
+    mant = np.zeros((h, w), np.float64)
+    nz = m > 1e-32
+    mant[nz], e[nz] = np.frexp(m[nz])
+    rgbe = np.zeros((h, w, 4), np.uint8)
+    f = np.where(nz, mant * 256.0 / np.where(nz, m, 1.0), 0.0)
+    rgbe[..., :3] = np.clip(np.floor(img * f[..., None]), 0, 255).astype(np.uint8)
+    rgbe[..., 3] = np.where(nz, e + 128, 0).astype(np.uint8)
+    out = bytearray(b"#?RADIANCE\nFORMAT=32-bit_rle_rgbe\n\n" + f"-Y {h} +X {w}\n".encode())
+    for y in range(h):
+        if not rle or w < 8 or w >= 32768:
+            out += rgbe[y].tobytes()
+            continue
+        out += bytes([2, 2, w >> 8, w & 255])
+        for c in range(4):
+            row = rgbe[y, :, c]
+            i = 0
+            while i < w:
+                run = 1
+                while i + run < w and run < 127 and row[i + run] == row[i]:
+                    run += 1
+                if run >= 3:
+                    out += bytes([128 + run, int(row[i])])
+                    i += run
+                    continue
+                j = i
+                while j < w and j - i < 128 and not (j + 2 < w and row[j] == row[j + 1] == row[j + 2]):
+                    j += 1
+                out += bytes([j - i]) + row[i:j].tobytes()
+                i = j
+    with open(path, "wb") as f:
+        f.write(bytes(out))
+    return path
+
+
+def write_bmp(path: str, samples, bpp: int = 24, header: int = 40, top_down: bool = False, masks=None,
+              palette=None) -> str:
+    """Writes a Windows bitmap (this project's encoder, for test images):
+    samples (h, w, n) top row first, or (h, w) palette indices with palette
+    (k, 3) RGB for bpp 1/4/8; header 12 (core), 40, 56, 108 or 124 bytes;
+    masks (r, g, b, a) pack 16/32-bit pixels as BI_BITFIELDS (header 40/56:
+    three masks after the header; 108/124: all four inside it), else the
+    default layouts (16: 5-5-5, 32: B, G, R, A bytes)."""
+    import struct
+    img = np.asarray(samples, np.uint8)
+    h, w = img.shape[:2]
+    compress = 3 if masks is not None else 0
+    dib = bytearray()
+    if header == 12:
+        dib += struct.pack("<IHHHH", 12, w, h, 1, bpp)
+    else:
+        dib += struct.pack("<IiiHHIIiiII", header, w, -h if top_down else h, 1, bpp, compress, 0, 2835, 2835, 0, 0)
+        if header == 56:
+            dib += struct.pack("<4I", *(masks or (0, 0, 0, 0)))
+        elif header in (108, 124):
+            dib += struct.pack("<4I", *(masks or (0, 0, 0, 0))) + struct.pack("<I", 0x73524742) + bytes(36 + 12)
+            if header == 124:
+                dib += bytes(16)
+        if masks is not None and header in (40, 56):
+            dib += struct.pack("<3I", *masks[:3])
+    pal = b""
+    if bpp < 16:
+        k = np.asarray(palette, np.uint8)
+        pal = b"".join(bytes([c[2], c[1], c[0]]) + (b"" if header == 12 else b"\0") for c in k)
+    offset = 14 + len(dib) + len(pal)
+    rows = []
+    for y in (range(h) if top_down else range(h - 1, -1, -1)):
+        r = img[y]
+        if bpp < 16:
+            idx = [int(v) for v in r]
+            if bpp == 8:
+                row = bytes(idx)
+            else:
+                per = 8 // bpp
+                row = bytearray((w + per - 1) // per)
+                for i, v in enumerate(idx):
+                    row[i // per] |= v << (8 - bpp * (1 + i % per))
+                row = bytes(row)
+        elif bpp == 24:
+            row = r[:, [2, 1, 0]].tobytes()
+        else:
+            m = masks or ((31 << 10, 31 << 5, 31, 0) if bpp == 16 else (0xFF0000, 0xFF00, 0xFF, 0xFF000000))
+            px = np.zeros(w, np.uint64)
+            for c, mask in enumerate(m):
+                if not mask or c >= r.shape[1]:
+                    continue
+                low = (mask & -mask).bit_length() - 1
+                bits = bin(mask).count("1")
+                px |= ((r[:, c].astype(np.uint64) >> np.uint64(8 - bits)) << np.uint64(low))
+            row = px.astype("<u2" if bpp == 16 else "<u4").tobytes()
+        rows.append(row + bytes((-len(row)) % 4))
+    body = b"".join(rows)
+    out = b"BM" + struct.pack("<IHHI", offset + len(body), 0, 0, offset) + bytes(dib) + pal + body
+    with open(path, "wb") as f:
+        f.write(out)
+    return path
+
+
+def write_tga(path: str, samples, image_type: int = 2, bpp: int | None = None, rle: bool = False,
+              top_down: bool = False, palette=None, palette_bits: int = 24, image_id: bytes = b"") -> str:
+    """Writes a Truevision TGA (this project's encoder, for test images):
+    samples (h, w, n) top row first, or (h, w) indices into palette (k, n)
+    for image_type 1; true-colour pixels stored B, G, R(, A), 15/16-bit
+    pixels as five bits per channel; rle packs run-length packets (runs and
+    literal spans, which may cross rows)."""
+    import struct
+    img = np.asarray(samples, np.uint8)
+    h, w = img.shape[:2]
+    n = 1 if img.ndim == 2 else img.shape[2]
+    if bpp is None:
+        bpp = 8 if image_type == 1 else 8 * n
+
+    def pixel_bytes(v, bits):
+        v = np.atleast_1d(v)
+        if bits in (15, 16) and len(v) == 3:
+            p = ((int(v[0]) >> 3) << 10) | ((int(v[1]) >> 3) << 5) | (int(v[2]) >> 3)
+            return struct.pack("<H", p)
+        if len(v) >= 3:
+            return bytes([v[2], v[1], v[0]]) + bytes(v[3:])
+        return bytes(int(x) for x in v)
+
+    pal = b""
+    if image_type == 1:
+        k = np.asarray(palette, np.uint8)
+        pal = b"".join(pixel_bytes(c, palette_bits) for c in k)
+        order = img if top_down else img[::-1]
+        pixels = [struct.pack("<B" if bpp == 8 else "<H", int(i)) for i in order.reshape(-1)]
+    else:
+        order = img if top_down else img[::-1]
+        flat = order.reshape(h * w, n)
+        pixels = [pixel_bytes(p, bpp) for p in flat]
+    if rle:
+        data = bytearray()
+        i = 0
+        while i < len(pixels):
+            run = 1
+            while i + run < len(pixels) and run < 128 and pixels[i + run] == pixels[i]:
+                run += 1
+            if run >= 2:
+                data += bytes([0x80 | (run - 1)]) + pixels[i]
+                i += run
+                continue
+            j = i
+            while j < len(pixels) and j - i < 128 and not (j + 1 < len(pixels) and pixels[j] == pixels[j + 1]):
+                j += 1
+            data += bytes([j - i - 1]) + b"".join(pixels[i:j])
+            i = j
+    else:
+        data = b"".join(pixels)
+    cmap = 1 if image_type == 1 else 0
+    hdr = struct.pack("<BBBHHBHHHHBB", len(image_id), cmap, image_type + (8 if rle else 0), 0,
+                      len(palette) if cmap else 0, palette_bits if cmap else 0, 0, 0, w, h, bpp,
+                      0x20 if top_down else 0)
+    with open(path, "wb") as f:
+        f.write(hdr + image_id + pal + bytes(data))
+    return path
+
+
 def texture_folder(path: str) -> str:
     """Where a scene file's image textures lie: texture_<stem>_<extension>
     beside it (get_texture_folder_from_scene_file, src/core/YMParser.cpp:20-30)."""
@@ -349,7 +707,9 @@ def write_scene(scene: Scene, path: str) -> str:
         folder = texture_folder(path)
         os.makedirs(folder, exist_ok=True)
         for fname, (samples, kw) in scene.image_files.items():
-            write_png(os.path.join(folder, fname), samples, **kw)
+            writer = {".jpg": write_jpeg, ".jpeg": write_jpeg, ".hdr": write_hdr, ".bmp": write_bmp,
+                      ".tga": write_tga}.get(os.path.splitext(fname)[1].lower(), write_png)
+            writer(os.path.join(folder, fname), samples, **kw)
     frm, look, fov = scene.camera
     out.append(f"Begin(Camera);\n\tfov = {_f(fov)};\n\tfrom = {_vec(frm)};\n\tlook = {_vec(look)};\nEnd(Camera);\n")
     for m in scene.meshes:
