@@ -407,6 +407,22 @@ int ymrt_accumulate(ymrt_scene* scene, const float* noise_rgba, float* acc_rgba,
 /* ---- known-answer entry points (host buffers) ---- */
 int ymrt_debug_trace(ymrt_scene* scene, int n, const float* origin, const float* dir, const uint32_t* last_hit,
                      uint32_t* inst, uint32_t* tri, float* t, float* bary, int* back, int* nearby);
+/* Renders one frame of tiles [tile_begin, tile_end) like ymrt_render_tiles
+ * (into out_rgba, a host array of width*height*4 floats; waves launched
+ * from the host) and records, after every closest-hit stage, the vertex of
+ * each path whose pixel has its bit set in watch_bits (host, one bit per
+ * pixel index y*width+x): 24 words per vertex -- pixel, depth (1 = camera
+ * ray), flags (1 hit, 2 volume scattering, 4 back face), instance, triangle,
+ * t, origin[3], direction[3], barycentrics or scattering position[3],
+ * throughput[3], light received so far[3], path index, 2 unused -- the
+ * state the reference's trace stage holds at the same point
+ * (Ray_trace_path_tracing, src/Shading.cu:1829-1854), so that paths can be
+ * compared vertex by vertex. *n_records = vertices recorded;
+ * YMRT_ERR_OVERFLOW when that exceeds `capacity` (the first `capacity` are
+ * returned). */
+int ymrt_debug_record_paths(ymrt_scene* scene, const ymrt_render_setting* setting, int frame_index, int tile_begin,
+                            int tile_end, const uint32_t* watch_bits, uint32_t* records, int capacity,
+                            int* n_records, float* out_rgba);
 /* Value of texture node `texture_index` at n object-space points (3 floats
  * each; host buffers), as the media read it: known-answer checks of grid and
  * fBm nodes. */

@@ -179,6 +179,118 @@ inline uint32_t ymrt_oracle_max_priority(const YMRT::RayTransfer& rt) {
 '''
 
 
+# Path-vertex recording, for parity diagnostics (the host parity build only:
+# the timing build stays as the reference wrote it, and the device builds
+# read the same vertices from the hit queue the trace stage writes, in
+# oracle/ref_gpu_harness.cu, without touching the reference's kernels).
+# After the trace stage's closest hit and volume free flight
+# (src/Shading.cu:1829-1854), the vertex of each watched pixel's path (the
+# ray, what it hit, the throughput and the light received so far) is written
+# to a record array, so that a path can be compared vertex by vertex with
+# ymrt_b200's (ymrt_debug_record_paths, the same 24-word layout).
+_RECORD_FILL = r'''
+struct YmrtOracleVertex {
+  uint32_t pixel, depth, flags, inst, tri;
+  float t, o[3], d[3], bary[3], tp[3], light[3];
+  uint32_t path, pad[2];
+};
+template <typename R, typename H, typename V>
+YMRT_ORACLE_FN void ymrt_oracle_fill(YmrtOracleVertex& v, uint32_t pixel, int depth, int sample, const R& ray, bool hit,
+                                     const H& rec, const V& tp, const V& light) {
+  v.pixel = pixel;
+  v.depth = (uint32_t)depth;
+  v.flags = (hit ? 1u : 0u) | (rec.volume_hit ? 2u : 0u) | (rec.hit_back ? 4u : 0u);
+  v.inst = rec.hit_instance_idx;
+  v.tri = rec.hit_triangle_idx;
+  v.t = rec.hit_t;
+  for (int c = 0; c < 3; ++c) {
+    v.o[c] = ray.origin[c];
+    v.d[c] = ray.direction[c];
+    v.bary[c] = rec.hit_barycentric[c];
+    v.tp[c] = tp[c];
+    v.light[c] = light[c];
+  }
+  v.path = (uint32_t)sample;
+  v.pad[0] = v.pad[1] = 0u;
+}
+'''
+_RECORD_HOST = ("\n// ---- inserted by oracle/build_ref.py: path-vertex recording ----\n#define YMRT_ORACLE_RECORDING 1\n"
+                "#define YMRT_ORACLE_FN inline\n" +
+                _RECORD_FILL + r'''
+struct YmrtOracleRecorder {
+  const uint32_t* watch = nullptr;
+  uint32_t n_pixels = 0;
+  YmrtOracleVertex* out = nullptr;
+  uint32_t capacity = 0;
+  std::atomic<uint32_t> count{0};
+};
+inline YmrtOracleRecorder& ymrt_oracle_recorder() {
+  static YmrtOracleRecorder r;
+  return r;
+}
+template <typename R, typename H, typename V>
+inline void ymrt_oracle_record(uint32_t pixel, int depth, int sample, const R& ray, bool hit, const H& rec, const V& tp,
+                               const V& light) {
+  YmrtOracleRecorder& q = ymrt_oracle_recorder();
+  if (!q.out || pixel >= q.n_pixels || !((q.watch[pixel >> 5] >> (pixel & 31u)) & 1u)) return;
+  const uint32_t k = q.count.fetch_add(1u, std::memory_order_relaxed);
+  if (k < q.capacity) ymrt_oracle_fill(q.out[k], pixel, depth, sample, ray, hit, rec, tp, light);
+}
+// ---- end of insertion ----
+''')
+_RECORD_CALL = ("ymrt_oracle_record(pixel_index, shading_ray_data_ray_depth[ray_index], "
+                "shading_ray_data_pixel_sample_index[ray_index], ray, hit_something, hit_record, ray_throughput, "
+                "ray_received_light);\n\t\t")
+
+
+# Material::FetchIOR (src/Material.h:262-277) writes the IOR priority only
+# for default materials; for a light material its callers go on with an
+# uninitialised priority (src/Shading.cu:694-697, 2146-2151,
+# src/ShadingUtilities.cuh:969-974, src/VolumeEval.cuh:460-461,
+# src/Camera.cpp:71-73), pushing it onto the nested-media stack when a light
+# lies within two ulps of a boundary hit. The parity builds declare those
+# variables zero-initialised (priority 0 for lights, the value ymrt_b200
+# uses), so that the oracle's results do not depend on leftover register or
+# stack contents. The timing build and the reference's default device build
+# keep the code as written.
+_PRIORITY_DECL = re.compile(r"\buint32_t\s+(mtl_ior_priority|material_ior_priority)\s*;")
+
+
+def _init_priorities(text: str) -> tuple[str, int]:
+    return _PRIORITY_DECL.subn(r"uint32_t \1 = 0u;", text)
+
+
+# Files besides Shading.cu that hold FetchIOR calls; the parity builds compile
+# copies of them (in the directory of the Shading.cu copy, so that its quoted
+# includes find them first), with the priorities initialised.
+_PRIORITY_FILES = {"ShadingUtilities.cuh": 1, "Camera.cpp": 1}
+
+
+def _priority_copies(gen_dir: str) -> None:
+    for name, expect in _PRIORITY_FILES.items():
+        src = os.path.join(REF, "src", name)
+        with open(src, "r", encoding="utf-8", errors="replace") as f:
+            text, n = _init_priorities(f.read())
+        if n != expect:
+            raise RuntimeError(f"{name}: {n} FetchIOR priority declarations (expected {expect})")
+        with open(os.path.join(gen_dir, name), "w") as f:
+            f.write(f'#line 1 "{src}"\n' + text)
+
+
+def _host_sources(gen_dir: str) -> list:
+    """HOST_SOURCES with Camera.cpp taken from the parity copy in gen_dir."""
+    return [os.path.join(gen_dir, "Camera.cpp") if s == "src/Camera.cpp" else os.path.join(REF, s)
+            for s in HOST_SOURCES]
+
+
+def _record_site(body: str) -> str:
+    """Inserts the recording call into Ray_trace_path_tracing, before its
+    miss branch (after the volume block)."""
+    k = body.index("__global__ void Ray_trace_path_tracing(")
+    j = body.index("if (!hit_something) {", k)
+    return body[:j] + _RECORD_CALL + body[j:]
+
+
 def shading_source(arg_order: str, counted: bool = True, gen_name: str = "gen") -> str:
     """Writes the build-time copy of src/Shading.cu (and its sampler and
     media headers) into oracle/_ref/<gen_name>. counted=False leaves the
@@ -198,25 +310,34 @@ def shading_source(arg_order: str, counted: bool = True, gen_name: str = "gen") 
         body, n_trace = re.subn(r"\bTraceRay\(", "ymrt_oracle_counted_trace(", body)
         body, n_shadow = re.subn(r"\bBVHTraverseShadow\(", "ymrt_oracle_counted_shadow(", body)
     body, n_prio = re.subn(r"\b(\w+)\.GetMaxPriorityRecord\(\)\.ior_priority", r"ymrt_oracle_max_priority(\1)", body)
+    n_init = 0
+    if counted:
+        body = _record_site(body)
+        body, n_init = _init_priorities(body)
+        if n_init != 2:
+            raise RuntimeError(f"Shading.cu: {n_init} FetchIOR priority declarations (expected 2)")
     line_of_body = head.count("\n") + 1
     gen_dir = os.path.join(OUT, gen_name)
     os.makedirs(gen_dir, exist_ok=True)
     dst = os.path.join(gen_dir, "Shading.cu")
-    out = (_HELPER + f'#line 1 "{src}"\n' + head + _COUNTERS + f'#line {line_of_body} "{src}"\n' + body)
+    out = (_HELPER + f'#line 1 "{src}"\n' + head + _COUNTERS + (_RECORD_HOST if counted else "") +
+           f'#line {line_of_body} "{src}"\n' + body)
     with open(dst, "w") as f:
         f.write(out)
-    n_pairs = _sampler_headers(arg_order, gen_dir)
+    n_pairs = _sampler_headers(arg_order, gen_dir, parity=counted)
+    if counted:
+        _priority_copies(gen_dir)
     with open(os.path.join(gen_dir, "Shading.cu.sites"), "w") as f:
         f.write(f"{n} argument lists sequenced, {n_trace} TraceRay and {n_shadow} BVHTraverseShadow calls counted, "
-                f"{n_prio} GetMaxPriorityRecord reads made direct, {n_pairs} two-draw constructors in "
-                f"RandomSampler.cuh sequenced\n")
+                f"{n_prio} GetMaxPriorityRecord reads made direct, {n_init} IOR priorities initialised, "
+                f"{n_pairs} two-draw constructors in RandomSampler.cuh sequenced\n")
     return dst
 
 
 _PAIR = re.compile(r"return glm::vec2\(Random1D\(\), Random1D\(\)\);")
 
 
-def _sampler_headers(arg_order: str, gen_dir: str) -> int:
+def _sampler_headers(arg_order: str, gen_dir: str, parity: bool = True) -> int:
     """The PCG and Sobol samplers' Random2D / SamplePixelOffset build a vec2
     from two Random1D() calls (src/RandomSampler.cuh:401-405, 544-548); the
     build-time copy of the header draws them first then second, as the
@@ -234,6 +355,10 @@ def _sampler_headers(arg_order: str, gen_dir: str) -> int:
     with open(os.path.join(src_dir, "VolumeEval.cuh"), "r", encoding="utf-8", errors="replace") as f:
         vol = f.read()
     vol = _media_hooks(vol)
+    if parity:
+        vol, n_init = _init_priorities(vol)
+        if n_init != 1:
+            raise RuntimeError(f"VolumeEval.cuh: {n_init} FetchIOR priority declarations (expected 1)")
     with open(os.path.join(gen_dir, "VolumeEval.cuh"), "w") as f:
         f.write(f'#line 1 "{os.path.join(src_dir, "VolumeEval.cuh")}"\n' + vol)
     return n
@@ -338,10 +463,14 @@ __host__ __device__ inline uint32_t ymrt_oracle_max_priority(const YMRT::RayTran
 '''
 
 
-def shading_source_gpu() -> str:
-    """Build-time copy of src/Shading.cu for the device build: only the
-    GetMaxPriorityRecord reads are rewritten; argument order and everything
-    else stay as the reference wrote them."""
+def shading_source_gpu(exact: bool = False) -> str:
+    """Build-time copy of src/Shading.cu for the device build, in a
+    directory of its own (oracle/_ref/gen_gpu, or gen_gpu_exact), so that it
+    includes the reference's own headers: the GetMaxPriorityRecord reads are
+    rewritten; argument order and everything else stay as the reference
+    wrote them. exact=True (the parity build) also initialises the IOR
+    priorities FetchIOR leaves unset, here and in copies of VolumeEval.cuh,
+    ShadingUtilities.cuh and Camera.cpp beside it."""
     src = os.path.join(REF, "src", "Shading.cu")
     with open(src, "r", encoding="utf-8", errors="replace") as f:
         text = f.read()
@@ -353,14 +482,28 @@ def shading_source_gpu() -> str:
     body, n_unroll = re.subn(r"#pragma unroll \(MAX_BOUNDARY_RECORD \+ 2\)", "#pragma unroll 8", body)
     body, n_unroll6 = re.subn(r"#pragma unroll MAX_BOUNDARY_RECORD\b", "#pragma unroll 6", body)
     n_unroll += n_unroll6
-    line_of_body = head.count("\n") + 1
-    gen_dir = os.path.join(OUT, "gen")
+    n_init = 0
+    gen_dir = os.path.join(OUT, "gen_gpu_exact" if exact else "gen_gpu")
     os.makedirs(gen_dir, exist_ok=True)
+    if exact:
+        body, n_init = _init_priorities(body)
+        if n_init != 2:
+            raise RuntimeError(f"Shading.cu: {n_init} FetchIOR priority declarations (expected 2)")
+        vsrc = os.path.join(REF, "src", "VolumeEval.cuh")
+        with open(vsrc, "r", encoding="utf-8", errors="replace") as f:
+            vol, nv = _init_priorities(f.read())
+        if nv != 1:
+            raise RuntimeError(f"VolumeEval.cuh: {nv} FetchIOR priority declarations (expected 1)")
+        with open(os.path.join(gen_dir, "VolumeEval.cuh"), "w") as f:
+            f.write(f'#line 1 "{vsrc}"\n' + vol)
+        _priority_copies(gen_dir)
+    line_of_body = head.count("\n") + 1
     dst = os.path.join(gen_dir, "Shading_gpu.cu")
     with open(dst, "w") as f:
         f.write(f'#line 1 "{src}"\n' + head + _GPU_FIX + f'#line {line_of_body} "{src}"\n' + body)
-    with open(os.path.join(gen_dir, "Shading_gpu.cu.sites"), "w") as f:
-        f.write(f"{n_prio} GetMaxPriorityRecord reads made direct, {n_unroll} unroll counts written as literals\n")
+    with open(dst + ".sites", "w") as f:
+        f.write(f"{n_prio} GetMaxPriorityRecord reads made direct, {n_init} IOR priorities initialised, "
+                f"{n_unroll} unroll counts written as literals\n")
     return dst
 
 
@@ -407,11 +550,12 @@ def build_gpu(force: bool = False, jobs: int = 8, exact: bool = False) -> str:
                 return lib
     obj_dir = os.path.join(OUT, "obj_gpu_exact" if exact else "obj_gpu")
     os.makedirs(obj_dir, exist_ok=True)
-    shading = shading_source_gpu()
+    shading = shading_source_gpu(exact)
     cmds, objs = [], []
-    for rel in HOST_SOURCES:
-        obj = os.path.join(obj_dir, os.path.basename(rel) + ".o")
-        cmds.append(["g++"] + CXXFLAGS + _gpu_includes() + ["-c", os.path.join(REF, rel), "-o", obj])
+    sources = _host_sources(os.path.dirname(shading)) if exact else [os.path.join(REF, s) for s in HOST_SOURCES]
+    for src in sources:
+        obj = os.path.join(obj_dir, os.path.basename(src) + ".o")
+        cmds.append(["g++"] + CXXFLAGS + _gpu_includes() + ["-c", src, "-o", obj])
         objs.append(obj)
     obj = os.path.join(obj_dir, "ref_stubs.o")
     cmds.append(["g++"] + CXXFLAGS + ["-DYMRT_ORACLE_REAL_CUDA"] + _gpu_includes() +
@@ -477,8 +621,9 @@ def build(arg_order: str = "ltr", force: bool = False, jobs: int = 8) -> str:
     procs = []
     obj_dir = os.path.join(OUT, "obj")
     os.makedirs(obj_dir, exist_ok=True)
-    jobs_list = [(os.path.join(REF, s), os.path.join(obj_dir, os.path.basename(s) + ".o"), []) for s in HOST_SOURCES]
     shading = shading_source(arg_order)
+    jobs_list = [(s, os.path.join(obj_dir, os.path.basename(s) + ".o"), [])
+                 for s in _host_sources(os.path.dirname(shading))]
     jobs_list.append((os.path.join(HERE, "ref_harness.cpp"), os.path.join(obj_dir, "ref_harness.o"),
                       [f'-DYMRT_SHADING_SOURCE="{shading}"']))
     jobs_list.append((os.path.join(HERE, "ref_stubs.cpp"), os.path.join(obj_dir, "ref_stubs.o"), []))
@@ -625,7 +770,7 @@ def _fp64_tree() -> str:
                 continue
             rel = os.path.relpath(os.path.join(d, name), src_root)
             origin = os.path.join(d, name)
-            if rel in ("Shading.cu", "RandomSampler.cuh", "VolumeEval.cuh"):
+            if rel in ("Shading.cu", "RandomSampler.cuh", "VolumeEval.cuh") + tuple(_PRIORITY_FILES):
                 origin = os.path.join(gen, rel)
             with open(origin, "r", encoding="utf-8", errors="replace") as f:
                 text, n = to_fp64(f.read())

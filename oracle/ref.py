@@ -34,6 +34,22 @@ class Settings64(ctypes.Structure):
     _fields_ = [(n, t) for n, t in Settings._fields_[:-1]] + [("indirect_limit", ctypes.c_double)]
 
 
+# One path vertex as the trace stage leaves it (24 words; the layout the
+# build-time recording hook writes and ymrt_debug_record_paths returns).
+VERTEX_DTYPE = np.dtype([("pixel", "<u4"), ("depth", "<u4"), ("flags", "<u4"), ("inst", "<u4"), ("tri", "<u4"),
+                         ("t", "<f4"), ("o", "<f4", 3), ("d", "<f4", 3), ("bary", "<f4", 3), ("tp", "<f4", 3),
+                         ("light", "<f4", 3), ("path", "<u4"), ("pad", "<u4", 2)])
+assert VERTEX_DTYPE.itemsize == 96
+
+
+def watch_bits(pixels, n_pixels: int) -> np.ndarray:
+    """One bit per pixel index, set for the given pixels."""
+    bits = np.zeros((n_pixels + 31) // 32, np.uint32)
+    px = np.asarray(pixels, np.int64).ravel()
+    np.bitwise_or.at(bits, px >> 5, (np.uint32(1) << (px & 31).astype(np.uint32)))
+    return bits
+
+
 def available() -> bool:
     return os.path.exists(LIB_PATH)
 
@@ -71,6 +87,9 @@ def _bind(L, settings_type):
     L.ymref_set_transforms.argtypes = [vp, ctypes.c_uint32, ctypes.c_uint32, vp, vp]
     L.ymref_tracking_caps.restype = ctypes.c_ulonglong
     L.ymref_tracking_caps.argtypes = [i]
+    if hasattr(L, "ymref_set_recorder"):
+        L.ymref_set_recorder.argtypes = [vp, vp, vp, i]
+        L.ymref_recorded.restype = ctypes.c_uint32
     if hasattr(L, "ymref_boundary_walk"):
         L.ymref_boundary_walk.argtypes = [vp, vp, vp, ctypes.c_float, ctypes.c_uint32, ctypes.c_uint32, vp, i, vp]
     L.ymref_halton.argtypes = [vp, i, vp, vp, vp, i, vp, vp, vp]
@@ -405,6 +424,25 @@ class RefScene:
     def last_render_seconds(self) -> float:
         return self._L.ymref_last_render_seconds(self.h)
 
+    def record_paths(self, pixels, frame_index: int = 1, tile_begin: int = 0, tile_end: int = 0,
+                     capacity: int = 1 << 16, threads: int | None = None):
+        """Renders a frame while recording the path vertices of the given
+        pixel indices (the trace stage's ray, hit, throughput and received
+        light at each depth); returns (records as VERTEX_DTYPE, image)."""
+        if self._f is not np.float32 or not hasattr(self._L, "ymref_set_recorder"):
+            raise RuntimeError("path recording needs the float parity build")
+        watch = watch_bits(pixels, self.width * self.height)
+        out = np.zeros(capacity, VERTEX_DTYPE)
+        self._L.ymref_set_recorder(self.h, _p(watch), _p(out), capacity)
+        try:
+            img = self.render_frame(frame_index, tile_begin, tile_end, threads=threads)
+            n = int(self._L.ymref_recorded())
+        finally:
+            self._L.ymref_set_recorder(self.h, None, None, 0)
+        if n > capacity:
+            raise RuntimeError(f"{n} vertices recorded, capacity {capacity}")
+        return out[:n].copy(), img
+
 
 def post_process(image, primitive_index, selected: int, gamma: float, exposure: float, outline: bool):
     """The reference's tone mapping (and outline) of an (H, W, 4) float32
@@ -460,6 +498,9 @@ def gpu_lib(exact: bool = False):
         for name in ("ymrefgpu_last_render_ms", "ymrefgpu_last_wall_ms"):
             getattr(L, name).restype = ctypes.c_double
             getattr(L, name).argtypes = [vp]
+        if hasattr(L, "ymrefgpu_set_recorder"):
+            L.ymrefgpu_set_recorder.argtypes = [vp, vp, i]
+            L.ymrefgpu_read_records.argtypes = [vp, vp, i]
         _gpu_libs[exact] = L
     return _gpu_libs[exact]
 
@@ -499,6 +540,24 @@ class RefGpuScene:
 
     def set_profiling(self, on: bool):
         self.L.ymrefgpu_set_profiling(self.h, int(on))
+
+    def record_paths(self, pixels, frame_index: int = 1, tile_begin: int = 0, tile_end: int = 0,
+                     capacity: int = 1 << 16):
+        """As RefScene.record_paths, on the device: the harness reads the
+        hit queue the reference's trace stage writes, so only vertices that
+        hit something are recorded (the reference's kernels are unchanged)."""
+        watch = watch_bits(pixels, self.width * self.height)
+        if self.L.ymrefgpu_set_recorder(self.h, _p(watch), capacity) != 0:
+            raise RuntimeError("ymrefgpu_set_recorder failed")
+        try:
+            img = self.render_frame(frame_index, tile_begin, tile_end)
+            out = np.zeros(capacity, VERTEX_DTYPE)
+            n = self.L.ymrefgpu_read_records(self.h, _p(out), capacity)
+        finally:
+            self.L.ymrefgpu_set_recorder(self.h, None, 0)
+        if n < 0 or n > capacity:
+            raise RuntimeError(f"recording failed or overflowed ({n} of {capacity})")
+        return out[:n].copy(), img
 
     def last_stage_ms(self) -> dict:
         out = np.zeros(3, np.float64)

@@ -34,6 +34,7 @@
 
 #include "ref_prepare.h"
 
+#include <algorithm>
 #include <chrono>
 #include <cstring>
 #include <string>
@@ -63,7 +64,47 @@ struct GpuContext {
   double stage_ms[3] = {0.0, 0.0, 0.0};  // generation, trace, shading (profiled frames only)
   uint32_t waves = 0;
   std::string error;
+  // path-vertex recording (ymrefgpu_set_recorder)
+  uint32_t* rec_watch = nullptr;
+  uint32_t* rec_out = nullptr;
+  uint32_t* rec_count = nullptr;
+  uint32_t rec_capacity = 0;
 };
+
+constexpr int kRecordWords = 24;
+
+// Appends the hit-queue entries of watched pixels to the record array (see
+// ymrefgpu_set_recorder): pixel, depth, flags (1 hit, 2 volume, 4 back),
+// instance, triangle, t, origin[3], direction[3], barycentrics[3],
+// throughput[3], received light[3], sample index, 2 unused.
+__global__ void k_record_hits(HitData hits, uint32_t n_hits, uint32_t width, uint32_t n_pixels,
+                              const uint32_t* __restrict__ watch, uint32_t* out, uint32_t* count, uint32_t capacity) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n_hits) return;
+  const uint32_t pixel = (uint32_t)hits.hit_data_pixel_position_y[i] * width + (uint32_t)hits.hit_data_pixel_position_x[i];
+  if (pixel >= n_pixels || !((watch[pixel >> 5] >> (pixel & 31u)) & 1u)) return;
+  const uint32_t k = atomicAdd(count, 1u);
+  if (k >= capacity) return;
+  const HitRecord h = hits.hit_data_hit_record[i];
+  const Ray ray = hits.hit_data_ray[i];
+  const glm::vec3 tp = hits.hit_data_throughput[i], light = hits.hit_data_received_light[i];
+  uint32_t* o = out + (size_t)k * kRecordWords;
+  o[0] = pixel;
+  o[1] = (uint32_t)hits.hit_data_ray_depth[i];
+  o[2] = 1u | (h.volume_hit ? 2u : 0u) | (h.hit_back ? 4u : 0u);
+  o[3] = h.hit_instance_idx;
+  o[4] = h.hit_triangle_idx;
+  o[5] = __float_as_uint(h.hit_t);
+  for (int c = 0; c < 3; ++c) {
+    o[6 + c] = __float_as_uint(ray.origin[c]);
+    o[9 + c] = __float_as_uint(ray.direction[c]);
+    o[12 + c] = __float_as_uint(h.hit_barycentric[c]);
+    o[15 + c] = __float_as_uint(tp[c]);
+    o[18 + c] = __float_as_uint(light[c]);
+  }
+  o[21] = (uint32_t)hits.hit_data_pixel_sample_index[i];
+  o[22] = o[23] = 0u;
+}
 
 template <typename T>
 bool upload(GpuContext* c, T** dst, const T* src, size_t count) {
@@ -177,6 +218,9 @@ void ymrefgpu_scene_free(void* handle) {
     ReleaseShadowRayData(c->shadow);
   } catch (...) {
   }
+  if (c->rec_watch) cudaFree(c->rec_watch);
+  if (c->rec_out) cudaFree(c->rec_out);
+  if (c->rec_count) cudaFree(c->rec_count);
   for (void* p : c->owned) cudaFree(p);
   if (c->image) cudaFree(c->image);
   if (c->ev0) cudaEventDestroy(c->ev0);
@@ -278,6 +322,13 @@ int ymrefgpu_render_frame(void* handle, int frame_index, int tile_begin, int til
       stage_end(1);
       CUDA_CHECK(cudaMemcpyAsync(counter_host, counter_device, sizeof(RayCounter), cudaMemcpyDeviceToHost, c->stream));
       CUDA_CHECK(cudaStreamSynchronize(c->stream));
+      if (c->rec_out && counter_host->hit_counter > 0) {
+        const uint32_t n_hits = counter_host->hit_counter;
+        k_record_hits<<<(n_hits + 255) / 256, 256, 0, c->stream>>>(c->hits, n_hits, w, w * h, c->rec_watch, c->rec_out,
+                                                                  c->rec_count, c->rec_capacity);
+        CUDA_CHECK(cudaGetLastError());
+        CUDA_CHECK(cudaStreamSynchronize(c->stream));
+      }
       counter_host->shading_ray_counter = 0;
       CUDA_CHECK(cudaMemcpyAsync(counter_device, counter_host, sizeof(RayCounter), cudaMemcpyHostToDevice, c->stream));
       CUDA_CHECK(cudaStreamSynchronize(c->stream));
@@ -318,6 +369,55 @@ double ymrefgpu_last_wall_ms(void* handle) { return static_cast<GpuContext*>(han
 // Per-stage device times of the last frame rendered with profiling on
 // (generation, trace, shading, in ms) and its wave count.
 void ymrefgpu_set_profiling(void* handle, int on) { static_cast<GpuContext*>(handle)->profile_stages = on != 0; }
+
+// Path-vertex recording for parity diagnostics: during the renders that
+// follow, after every trace stage a harness kernel reads the hit queue the
+// reference's trace stage wrote (hit record, ray, throughput, received light,
+// pixel, depth: src/Shading.cu:1880-1902) and appends the entries of watched
+// pixels (one bit per pixel in watch_bits, host memory, width*height bits)
+// to a device array of `capacity` records of 24 words, the layout
+// ymrt_debug_record_paths writes. The reference's kernels are not changed;
+// only vertices that hit something are queued there, so misses are not
+// recorded. capacity <= 0 stops recording and frees the arrays. Returns 0,
+// or -1 when the device arrays cannot be set up.
+int ymrefgpu_set_recorder(void* handle, const uint32_t* watch_bits, int capacity) {
+  auto c = static_cast<GpuContext*>(handle);
+  cudaSetDevice(c->device);
+  cudaDeviceSynchronize();
+  if (c->rec_watch) cudaFree(c->rec_watch);
+  if (c->rec_out) cudaFree(c->rec_out);
+  if (c->rec_count) cudaFree(c->rec_count);
+  c->rec_watch = nullptr;
+  c->rec_out = nullptr;
+  c->rec_count = nullptr;
+  c->rec_capacity = 0;
+  if (capacity <= 0 || !watch_bits) return 0;
+  const size_t words = ((size_t)c->width * c->height + 31) / 32;
+  if (cudaMalloc(&c->rec_watch, words * 4) != cudaSuccess ||
+      cudaMalloc(&c->rec_out, (size_t)kRecordWords * 4 * (size_t)capacity) != cudaSuccess ||
+      cudaMalloc(&c->rec_count, 4) != cudaSuccess ||
+      cudaMemcpy(c->rec_watch, watch_bits, words * 4, cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemset(c->rec_count, 0, 4) != cudaSuccess) {
+    ymrefgpu_set_recorder(handle, nullptr, 0);
+    return -1;
+  }
+  c->rec_capacity = (uint32_t)capacity;
+  return 0;
+}
+// Copies the records written so far (at most `capacity`) into out; returns
+// how many were recorded (those past the recorder's capacity are counted,
+// not written), or -1.
+int ymrefgpu_read_records(void* handle, void* out, int capacity) {
+  auto c = static_cast<GpuContext*>(handle);
+  cudaSetDevice(c->device);
+  if (cudaDeviceSynchronize() != cudaSuccess || !c->rec_count) return -1;
+  uint32_t n = 0;
+  if (cudaMemcpy(&n, c->rec_count, 4, cudaMemcpyDeviceToHost) != cudaSuccess) return -1;
+  const uint32_t kept = std::min<uint32_t>(std::min<uint32_t>(n, c->rec_capacity), (uint32_t)std::max(capacity, 0));
+  if (kept && cudaMemcpy(out, c->rec_out, (size_t)kRecordWords * 4 * kept, cudaMemcpyDeviceToHost) != cudaSuccess)
+    return -1;
+  return (int)n;
+}
 uint32_t ymrefgpu_last_stage_ms(void* handle, double* out3) {
   auto c = static_cast<GpuContext*>(handle);
   for (int k = 0; k < 3; ++k) out3[k] = c->stage_ms[k];

@@ -696,6 +696,27 @@ unsigned long long ymref_tracking_caps(int reset) {
   return reset ? ymrt_oracle_tracking_caps().exchange(0) : ymrt_oracle_tracking_caps().load();
 }
 
+#if defined(YMRT_ORACLE_RECORDING) && !defined(YMREF_FP64)
+// Path-vertex recording (parity build only): during the renders that follow,
+// the trace stage writes the vertex of every path of a watched pixel (one bit
+// per pixel in watch_bits, which must stay valid) into out, `capacity`
+// records of 24 words (YmrtOracleVertex). watch_bits == nullptr stops it.
+// Resets the count.
+void ymref_set_recorder(void* handle, const uint32_t* watch_bits, void* out, int capacity) {
+  auto ctx = static_cast<RefContext*>(handle);
+  YmrtOracleRecorder& q = ymrt_oracle_recorder();
+  q.out = nullptr;
+  q.watch = watch_bits;
+  q.n_pixels = watch_bits ? (uint32_t)(ctx->width * ctx->height) : 0u;
+  q.capacity = watch_bits ? (uint32_t)std::max(capacity, 0) : 0u;
+  q.count.store(0);
+  q.out = watch_bits ? static_cast<YmrtOracleVertex*>(out) : nullptr;
+}
+// Vertices recorded since the recorder was set (those past its capacity are
+// counted, not written).
+uint32_t ymref_recorded(void) { return ymrt_oracle_recorder().count.load(); }
+#endif
+
 // Halton sampler known-answer values: for each (px, py, sample) the global
 // sample index (src/HaltonEnumerator.h:43 GetIndex), the pixel offset as the
 // ray-generation stage computes it (src/Shading.cu:1698-1704) and the first

@@ -9,13 +9,12 @@ sampled from the scene's fBm node against that node in a converged image.
 import numpy as np
 import pytest
 
+import divergence as D
 import ymrt_b200 as Y
 
 pytestmark = pytest.mark.gpu
 
 FBM = 2  # texture index of the smoke's density node in the volumetric scenes
-REL_TOL = 1e-5
-ABS_TOL = 1e-7
 
 
 def trilinear(grid: np.ndarray, p: np.ndarray) -> np.ndarray:
@@ -106,14 +105,11 @@ def test_constant_grid_renders_as_constant_density(ctx, scene_dir, halton_perm, 
     ref.set_settings(spp=1, ray_depth=8, distant_light=1, volume=1)
     a, st = ours.render(s, frame)
     b = ref.render_frame(frame)
-    ours.close()
-    ref.close()
     assert st.device_errors == 0
     assert np.array_equal(a[..., 3], b[..., 3])
-    diff = np.abs(a[..., :3] - b[..., :3])
-    tol = REL_TOL * np.maximum(np.abs(a[..., :3]), np.abs(b[..., :3])) + ABS_TOL
-    bad = np.any(diff > tol, axis=-1)
-    assert bad.mean() <= 5e-3, f"{bad.sum()} of {bad.size} pixels differ beyond 1e-5 relative"
+    D.check_against_host(f"grid_const_h{int(half)}_f{frame}", ours, ref, s, frame, a, b)
+    ours.close()
+    ref.close()
 
 
 def test_fbm_grid_converges_to_fbm_node(ctx, scene_dir, halton_perm):

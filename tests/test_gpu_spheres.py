@@ -12,13 +12,12 @@ radiance per pixel, with and without the medium.
 import numpy as np
 import pytest
 
+import divergence as D
 import ymrt_b200 as Y
 from test_gpu_parity import _trace_case
 
 pytestmark = pytest.mark.gpu
 
-REL_TOL = 1e-5
-ABS_TOL = 1e-7
 W = H = 256
 
 
@@ -35,12 +34,6 @@ def spheres(ctx, spheres_path, halton_perm, oracle):
     yield ours, ref
     ours.close()
     ref.close()
-
-
-def _bad(a, b):
-    diff = np.abs(a[..., :3] - b[..., :3])
-    tol = REL_TOL * np.maximum(np.abs(a[..., :3]), np.abs(b[..., :3])) + ABS_TOL
-    return np.any(diff > tol, axis=-1)
 
 
 def test_trace_kat_spheres(spheres):
@@ -73,8 +66,7 @@ def test_per_sample_radiance_spheres(spheres, oracle, volume, frame):
     b = ref.render_frame(frame)
     ext, shadow = oracle.query_counts(reset=True)
     assert np.array_equal(a[..., 3], b[..., 3])
-    bad = _bad(a, b)
-    assert bad.mean() <= 5e-3, f"{bad.sum()} of {bad.size} pixels differ beyond 1e-5 relative"
+    D.check_against_host(f"spheres_v{volume}_f{frame}", ours, ref, s, frame, a, b)
     assert stats.device_errors == 0
     assert abs(int(stats.extension_rays) - ext) <= 0.01 * ext
     assert abs(int(stats.shadow_rays) - shadow) <= 0.01 * shadow
@@ -103,8 +95,7 @@ def test_wave_options_spheres(ctx, spheres, sort_hits, defer_shadows):
         ref.set_settings(spp=1, ray_depth=8)
         a, _ = ours.render(s, 3)
         b = ref.render_frame(3)
+        D.check_against_host("spheres_v0_f3", ours, ref, s, 3, a, b)
     finally:
         for k, v in before.items():
             ctx.set_option(k, v)
-    bad = _bad(a, b)
-    assert bad.mean() <= 5e-3, f"{bad.sum()} of {bad.size} pixels differ beyond 1e-5 relative"

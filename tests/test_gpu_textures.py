@@ -15,12 +15,11 @@ receives no gradient.
 import numpy as np
 import pytest
 
+import divergence as D
 import ymrt_b200 as Y
 
 pytestmark = pytest.mark.gpu
 
-REL_TOL = 1e-5
-ABS_TOL = 1e-7
 W = H = 256
 
 
@@ -37,12 +36,6 @@ def textured(ctx, textured_path, halton_perm, oracle):
     yield ours, ref
     ours.close()
     ref.close()
-
-
-def _bad(a, b):
-    diff = np.abs(a[..., :3] - b[..., :3])
-    tol = REL_TOL * np.maximum(np.abs(a[..., :3]), np.abs(b[..., :3])) + ABS_TOL
-    return np.any(diff > tol, axis=-1)
 
 
 def test_texture_nodes_match_reference(textured, textured_path):
@@ -84,8 +77,7 @@ def test_per_sample_radiance_textured(textured, oracle, volume, frame):
     ext, shadow = oracle.query_counts(reset=True)
     assert np.array_equal(a[..., 3], b[..., 3])
     assert a[..., :3].mean() > 0.01
-    bad = _bad(a, b)
-    assert bad.mean() <= 5e-3, f"{bad.sum()} of {bad.size} pixels differ beyond 1e-5 relative"
+    D.check_against_host(f"textured_v{volume}_f{frame}", ours, ref, s, frame, a, b)
     assert stats.device_errors == 0
     assert abs(int(stats.extension_rays) - ext) <= 0.01 * ext
     assert abs(int(stats.shadow_rays) - shadow) <= 0.01 * shadow
@@ -147,8 +139,10 @@ def test_per_sample_radiance_imaged(imaged, oracle, frame):
     device against the host's) into larger normal differences, so more
     pixels pass 1e-5 than in the other scenes, and a few paths take another
     branch (the frames themselves are pinned bit for bit by
-    test_shading_frames_match_reference): at most 2% of the pixels beyond
-    1e-5 relative, 0.2% beyond 1e-3, and the image means within 2e-4."""
+    test_shading_frames_match_reference). Every differing pixel is replayed
+    and classified (tests/divergence.py), their number bounded by the count
+    observed; at most 0.2% of the pixels beyond 1e-3, and the image means
+    within 2e-4."""
     ours, ref, _ = imaged
     s = Y.default_setting(spp=1, ray_depth=8)
     ref.set_settings(spp=1, ray_depth=8)
@@ -158,8 +152,7 @@ def test_per_sample_radiance_imaged(imaged, oracle, frame):
     ext, shadow = oracle.query_counts(reset=True)
     assert np.array_equal(a[..., 3], b[..., 3])
     assert a[..., :3].mean() > 0.01
-    bad = _bad(a, b)
-    assert bad.mean() <= 2e-2, f"{bad.sum()} of {bad.size} pixels differ beyond 1e-5 relative"
+    D.check_against_host(f"imaged_f{frame}", ours, ref, s, frame, a, b)
     diff = np.abs(a[..., :3] - b[..., :3]) / np.maximum(np.maximum(np.abs(a[..., :3]), np.abs(b[..., :3])), 1e-6)
     assert np.mean(np.any(diff > 1e-3, axis=-1)) <= 2e-3
     assert abs(float(a[..., :3].mean()) - float(b[..., :3].mean())) <= 2e-4 * float(b[..., :3].mean())

@@ -81,6 +81,13 @@ class Job(ctypes.Structure):
                 ("path_radiance_device", ctypes.c_void_p), ("dloss_device", ctypes.c_void_p)]
 
 
+# One path vertex as the closest-hit stage leaves it (ymrt_debug_record_paths).
+VERTEX_DTYPE = np.dtype([("pixel", "<u4"), ("depth", "<u4"), ("flags", "<u4"), ("inst", "<u4"), ("tri", "<u4"),
+                         ("t", "<f4"), ("o", "<f4", 3), ("d", "<f4", 3), ("bary", "<f4", 3), ("tp", "<f4", 3),
+                         ("light", "<f4", 3), ("path", "<u4"), ("pad", "<u4", 2)])
+VERTEX_HIT, VERTEX_VOLUME, VERTEX_BACK = 1, 2, 4
+
+
 class Stats(ctypes.Structure):
     _fields_ = [
         ("paths", ctypes.c_uint64), ("extension_rays", ctypes.c_uint64), ("shadow_rays", ctypes.c_uint64),
@@ -147,6 +154,7 @@ def library():
     L.ymrt_render_tiles.argtypes = [vp, ctypes.POINTER(RenderSetting), i, i, i, vp, i, ctypes.POINTER(Stats)]
     L.ymrt_accumulate.argtypes = [vp, vp, vp, i]
     L.ymrt_debug_trace.argtypes = [vp, i, vp, vp, vp, vp, vp, vp, vp, vp, vp]
+    L.ymrt_debug_record_paths.argtypes = [vp, ctypes.POINTER(RenderSetting), i, i, i, vp, vp, i, ctypes.POINTER(i), vp]
     L.ymrt_debug_occluded.argtypes = [vp, i, vp, vp, vp, vp]
     L.ymrt_debug_halton.argtypes = [vp, i, vp, vp, vp, i, vp, vp, vp]
     L.ymrt_debug_bound_record.argtypes = [vp, vp, sz, i]
@@ -551,6 +559,23 @@ class Scene:
                                          on_device, ctypes.byref(stats))
         _check(rc, self.ctx.h)
         return out, stats
+
+    def record_paths(self, setting: RenderSetting, pixels, frame_index: int = 1, tile_begin: int = 0,
+                     tile_end: int = 0, capacity: int = 1 << 16):
+        """Renders a frame (waves launched from the host) while recording,
+        after each closest-hit stage, the vertex of every path of the given
+        pixel indices: ray, hit, throughput and light received so far
+        (ymrt_debug_record_paths). Returns (records as VERTEX_DTYPE, image)."""
+        n_pix = self.width * self.height
+        watch = np.zeros((n_pix + 31) // 32, np.uint32)
+        px = np.asarray(pixels, np.int64).ravel()
+        np.bitwise_or.at(watch, px >> 5, (np.uint32(1) << (px & 31).astype(np.uint32)))
+        out = np.zeros(capacity, VERTEX_DTYPE)
+        img = np.zeros((self.height, self.width, 4), np.float32)
+        n = ctypes.c_int(0)
+        _check(library().ymrt_debug_record_paths(self.h, ctypes.byref(setting), frame_index, tile_begin, tile_end,
+                                                 _p(watch), _p(out), capacity, ctypes.byref(n), _p(img)), self.ctx.h)
+        return out[:n.value].copy(), img
 
     def trace(self, origins, dirs, last_hit=None) -> dict:
         o = np.ascontiguousarray(origins, np.float32)

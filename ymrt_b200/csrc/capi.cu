@@ -1928,6 +1928,65 @@ int ymrt_debug_trace(ymrt_scene* sc, int n, const float* origin, const float* di
   return YMRT_OK;
 }
 
+int ymrt_debug_record_paths(ymrt_scene* sc, const ymrt_render_setting* setting, int frame_index, int tile_begin,
+                            int tile_end, const uint32_t* watch_bits, uint32_t* records, int capacity, int* n_records,
+                            float* out_rgba) {
+  if (!sc || !setting || !watch_bits || !records || capacity < 0 || !n_records || !out_rgba) return YMRT_ERR_INVALID;
+  ymrt_context* ctx = sc->ctx;
+  cudaSetDevice(ctx->device);
+  cudaStream_t st = ctx->stream;
+  cudaError_t e;
+  const uint32_t n_pixels = (uint32_t)sc->width * sc->height;
+  const size_t watch_words = (n_pixels + 31) / 32, img_bytes = (size_t)n_pixels * sizeof(float4);
+  Staging sg{ctx};
+  const uint32_t* d_watch = sg.in(watch_bits, watch_words);
+  VertexRecord* d_rec = reinterpret_cast<VertexRecord*>(sg.out<uint32_t>((size_t)std::max(capacity, 1) * 24));
+  uint32_t* d_count = sg.out<uint32_t>(1);
+  float4* image = reinterpret_cast<float4*>(sg.out<float>(4 * (size_t)n_pixels));
+  if (sg.err != cudaSuccess) return ctx->cuda_fail(sg.err, "staging");
+  if ((e = cudaMemsetAsync(d_count, 0, sizeof(uint32_t), st)) != cudaSuccess) return ctx->cuda_fail(e, "clearing");
+  std::vector<JobDesc> jobs(1);
+  DeviceScene scene;
+  int rc = make_job(ctx, sc, setting, frame_index, tile_begin, tile_end, image, &jobs[0], &scene);
+  if (rc != YMRT_OK) return rc;
+  BatchMemory M;
+  if ((rc = context_memory(ctx, 1, &M)) != YMRT_OK) return rc;
+  WaveOptions opt;
+  if ((rc = batch_options(ctx, jobs, &opt)) != YMRT_OK) return rc;
+  opt.features = batch_features(&scene, 1);
+  // shadow rays traced in the shading stage, so that the light each path
+  // carries includes its next-event estimates, as the reference's does
+  opt.defer_shadows = false;
+  opt.recorder.watch = d_watch;
+  opt.recorder.n_pixels = n_pixels;
+  opt.recorder.out = d_rec;
+  opt.recorder.count = d_count;
+  opt.recorder.capacity = (uint32_t)capacity;
+  SlotLease lease(ctx, 1);
+  if (!lease.ok()) return ctx->fail(YMRT_ERR_INVALID, "no constant-memory scene slot for this device");
+  jobs[0].scene_slot = lease.slot(0);
+  if ((e = lease.upload(&scene, 1)) != cudaSuccess) return ctx->cuda_fail(e, "uploading constants");
+  if ((e = cudaMemsetAsync(image, 0, img_bytes, st)) != cudaSuccess) return ctx->cuda_fail(e, "clearing the image");
+  BatchResult r;
+  // waves launched from the host: the recorder is not part of the cached graph
+  if ((rc = run_batch(ctx, M, jobs, opt, false, false, &r)) != YMRT_OK) return rc;
+  uint32_t count = 0;
+  sg.back(&count, d_count, 1);
+  sg.back(out_rgba, reinterpret_cast<float*>(image), 4 * (size_t)n_pixels);
+  if ((e = cudaMemcpyAsync(ctx->counters_host, M.counters, sizeof(WaveCounters), cudaMemcpyDeviceToHost, st)) !=
+      cudaSuccess)
+    return ctx->cuda_fail(e, "reading counters");
+  if ((e = cudaStreamSynchronize(st)) != cudaSuccess || sg.err != cudaSuccess)
+    return ctx->cuda_fail(e != cudaSuccess ? e : sg.err, "recording paths");
+  const uint32_t kept = std::min<uint32_t>(count, (uint32_t)capacity);
+  if (kept && (e = cudaMemcpy(records, d_rec, (size_t)kept * sizeof(VertexRecord), cudaMemcpyDeviceToHost)) != cudaSuccess)
+    return ctx->cuda_fail(e, "reading records");
+  *n_records = (int)count;
+  rc = finish_batch(ctx, r, nullptr);
+  if (rc != YMRT_OK) return rc;
+  return count > (uint32_t)capacity ? ctx->fail(YMRT_ERR_OVERFLOW, "more path vertices than the record capacity") : YMRT_OK;
+}
+
 int ymrt_debug_density(ymrt_scene* sc, uint32_t texture_index, int n, const float* points, float* out) {
   if (!sc || n < 0 || !points || !out) return YMRT_ERR_INVALID;
   if (texture_index >= sc->textures.size()) return sc->ctx->fail(YMRT_ERR_INVALID, "texture index out of range");

@@ -104,6 +104,39 @@ __device__ __forceinline__ void generate_path(const PathPool& P, uint32_t base, 
 // (the miss branch of Ray_trace_path_tracing, src/Shading.cu:1855-1864), then
 // the path's radiance into its pixel (not in the adjoint pass, whose jobs
 // carry dLoss/dImage and only replay their paths). Misses are not listed.
+// Debug recording: the vertex each watched path of job 0 reached in this
+// wave's closest-hit stage (launched after k_extend only when a recorder is
+// set; the render's kernels are unchanged).
+__global__ void __launch_bounds__(256) k_record_vertices(PathPool P, const WaveControl* __restrict__ ctl, HitPool H,
+                                                         const JobDesc* __restrict__ jobs, PathRecorder R) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= ctl->count) return;
+  const uint2 pf = P.pixel_flags[i];
+  if ((pf.y & kFlagDead) || (pf.y >> kFlagJobShift) != 0u || pf.x >= R.n_pixels) return;
+  if (!((R.watch[pf.x >> 5] >> (pf.x & 31u)) & 1u)) return;
+  const uint32_t k = atomicAdd(R.count, 1u);
+  if (k >= R.capacity) return;
+  const uint4 ids = H.ids[i];
+  const bool volume = (ids.z & 2u) != 0u, hit = ids.x != kEmpty || volume;
+  VertexRecord v{};
+  v.pixel = pf.x;
+  v.depth = pf.y & kFlagDepthMask;
+  v.flags = (hit ? kVertexHit : 0u) | (volume ? kVertexVolume : 0u) | ((ids.z & 1u) ? kVertexBack : 0u);
+  v.inst = ids.x;
+  v.tri = ids.y;
+  const float4 o = P.ray_o[i], d = P.ray_d[i], tp = P.throughput[i], rad = P.radiance[i];
+  const float4 bt = hit ? H.bary_t[i] : make_float4(1.0f, 1.0f, 1.0f, kTMax);
+  v.t = bt.w;
+  v.o[0] = o.x; v.o[1] = o.y; v.o[2] = o.z;
+  v.d[0] = d.x; v.d[1] = d.y; v.d[2] = d.z;
+  v.bary[0] = bt.x; v.bary[1] = bt.y; v.bary[2] = bt.z;
+  v.throughput[0] = tp.x; v.throughput[1] = tp.y; v.throughput[2] = tp.z;
+  v.radiance[0] = rad.x; v.radiance[1] = rad.y; v.radiance[2] = rad.z;
+  v.path = P.path_id[i];
+  (void)jobs;
+  R.out[k] = v;
+}
+
 __global__ void __launch_bounds__(256) k_sort_hits(const WaveControl* __restrict__ ctl, HitPool H, PathPool P,
                                                    const JobDesc* __restrict__ jobs, WaveCounters* counters) {
   __shared__ uint32_t s_start[kShadeBuckets];
@@ -546,6 +579,7 @@ uint32_t launch_wave(const PathPool& A, const PathPool& B, const HitPool& H, Wav
       default: launch_extend_surface<kFeatSpheres>(w); break;
     }
   }
+  if (opt.recorder.out) k_record_vertices<<<blocks_256, 256, 0, stream>>>(A, ctl, H, jobs, opt.recorder);
   if (ev) cudaEventRecord(ev[2], stream);
   if (sort_hits) k_sort_hits<<<blocks_256, 256, 0, stream>>>(ctl, Hs, A, jobs, counters);
   if (ev) cudaEventRecord(ev[3], stream);

@@ -155,6 +155,35 @@ struct WaveControl {
 
 constexpr int kGradParams = 4;  // differentiated parameters per material: albedo r, g, b, roughness
 
+// One path vertex as the closest-hit stage leaves it: the ray, what it hit
+// (after volume free flight), the throughput and the light received so far.
+// The debug recorder writes one per watched path per wave, so that a
+// render's paths can be replayed vertex by vertex against another
+// renderer's (ymrt_debug_record_paths).
+struct VertexRecord {
+  uint32_t pixel, depth;  // pixel index in the job's image; 1 = camera ray
+  uint32_t flags;         // kVertexHit | kVertexVolume | kVertexBack
+  uint32_t inst, tri;
+  float t;
+  float o[3], d[3];
+  float bary[3];          // barycentrics, or the scattering position of a volume hit
+  float throughput[3];
+  float radiance[3];
+  uint32_t path;          // path index within the job
+  uint32_t pad[2];
+};
+static_assert(sizeof(VertexRecord) == 96, "VertexRecord is 24 words");
+constexpr uint32_t kVertexHit = 1u, kVertexVolume = 2u, kVertexBack = 4u;
+// Recording of the paths of watched pixels of job 0 (debug only; out ==
+// nullptr turns it off).
+struct PathRecorder {
+  const uint32_t* watch = nullptr;  // one bit per pixel of job 0's image
+  uint32_t n_pixels = 0;
+  VertexRecord* out = nullptr;
+  uint32_t* count = nullptr;        // records written (may exceed capacity: those past it are dropped)
+  uint32_t capacity = 0;
+};
+
 struct WaveOptions {
   uint32_t capacity = 0;       // path slots per pool (sizes the grids)
   bool volumes = false;        // volume scattering kernels
@@ -168,6 +197,7 @@ struct WaveOptions {
   float* grid_grads = nullptr; // adjoint: dLoss/d(value) of the density grid at texture node grid_tex
   uint32_t grid_tex = 0xFFFFFFFFu;
   uint32_t trace_block = 128;  // threads per block of k_extend and k_connect (64, 128 or 256)
+  PathRecorder recorder{};     // debug: vertices of watched paths after each closest-hit stage
 };
 // One wave's pools, control block, jobs and launch shape, for the launchers
 // of the media (wave_media.cu) and adjoint (wave_adjoint.cu) kernels.
