@@ -85,6 +85,7 @@ def _bind(L, settings_type):
     L.ymref_set_density_grid.argtypes = [vp, ctypes.c_uint32, i, i, i, vp]
     L.ymref_density.argtypes = [vp, ctypes.c_uint32, i, vp, vp]
     L.ymref_set_transforms.argtypes = [vp, ctypes.c_uint32, ctypes.c_uint32, vp, vp]
+    L.ymref_set_material_params.argtypes = [vp, ctypes.c_uint32, ctypes.c_uint32, vp]
     L.ymref_tracking_caps.restype = ctypes.c_ulonglong
     L.ymref_tracking_caps.argtypes = [i]
     if hasattr(L, "ymref_set_recorder"):
@@ -375,6 +376,13 @@ class RefScene:
         m = np.ascontiguousarray(object_to_world, self._f).reshape(-1, 16)
         sc = None if scales is None else np.ascontiguousarray(scales, self._f).reshape(-1, 3)
         assert self._L.ymref_set_transforms(self.h, first, m.shape[0], _p(m), None if sc is None else _p(sc)) == 0
+
+    def set_material_params(self, params, first: int = 0) -> None:
+        """(materials, 4): diffuse albedo rgb and roughness of each default
+        material, as ymrt_b200's Scene.set_material_params takes them."""
+        p = np.ascontiguousarray(params, self._f).reshape(-1, 4)
+        if self._L.ymref_set_material_params(self.h, first, p.shape[0], _p(p)) != 0:
+            raise ValueError("material range out of bounds")
 
     def density(self, texture_index: int, points) -> np.ndarray:
         """A medium's density node (or attached grid) at object-space points

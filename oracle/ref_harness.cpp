@@ -670,7 +670,28 @@ int ymref_set_transforms(void* handle, uint32_t first, uint32_t count, const flo
   }
   GuiModule::RebuildAfterTransformEdit(*ctx->module, &ctx->instance_old_index);
   ctx->scene = GuiModule::HostScene(*ctx->module);
+  ctx->scene.render_setting = &ctx->setting;  // as ymref_scene_load sets it
   return 0;
+}
+
+// Material parameters as ymrt_scene_set_material_params sets them (this
+// project's editing entry; the reference edits materials through its GUI):
+// for each default material in [first, first+count), 4 values -- diffuse
+// albedo r, g, b and roughness, written to both alphas; other materials are
+// left as they are. Returns 0, or -1 when the range is out of bounds.
+int ymref_set_material_params(void* handle, uint32_t first, uint32_t count, const float* params) {
+  auto ctx = static_cast<RefContext*>(handle);
+  auto& M = GuiModule::Materials(*ctx->module);
+  if (first > M.size() || count > M.size() - first) return -1;
+  for (uint32_t k = 0; k < count; ++k) {
+    Material& m = M[first + k];
+    if (m.material_type != DEFAULT_MTL) continue;
+    const float* q = params + 4 * (size_t)k;
+    m.default_mtl.diffuse_albedo = glm::vec3(q[0], q[1], q[2]);
+    m.default_mtl.alpha_x = q[3];
+    m.default_mtl.alpha_y = q[3];
+  }
+  return 0;  // edited in place: the scene's material array is the module's
 }
 
 // A medium's density as the build-time copy of VolumeEval.cuh reads it
