@@ -421,6 +421,9 @@ def run_ours(args):
     ctx = Y.Context(local_rank, queue_capacity=args.queue, profiling=False)
     if args.no_graph_loop:
         ctx.set_option("graph_loop", 0)
+    for item in args.option:
+        name, value = item.split("=")
+        ctx.set_option(name, int(value))
     # host scene preparation (parse, the reference's binary SAH builds, wide
     # collapse, light table), timed apart from the frames: the reference's
     # editor does it once per scene edit, not per frame
@@ -529,9 +532,7 @@ def run_ours(args):
             "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded .ymtmp scene generated by ymrt_b200.scenes)",
             "config": workload_config(wl, W, H, spp, world),
-            "wave_options": {"sort_hits": ctx.get_option("sort_hits"),
-                             "defer_shadows": ctx.get_option("defer_shadows"),
-                             "graph_loop": ctx.get_option("graph_loop")},
+            "wave_options": {name: ctx.get_option(name) for name in Y.OPTIONS},
             "spp_per_s": round(W * H * spp * world * args.steps / (ms_max * 1e-3), 1),
             "rays": {"extension": ext, "shadow": shadow, "per_step": rays // max(args.steps, 1)},
             "frame_ms_device": round(frame_ms / args.steps, 3),
@@ -759,6 +760,8 @@ def main(argv=None):
     ap.add_argument("--no-fp64", action="store_true", help="skip the image check against the FP64 oracle")
     ap.add_argument("--no-graph-loop", action="store_true",
                     help="launch the wave loop from the host instead of as one CUDA graph (for per-kernel profilers)")
+    ap.add_argument("--option", action="append", default=[], metavar="NAME=VALUE",
+                    help="wave option for the instanced-style workloads (ymrt_b200.OPTIONS), e.g. extend_refill=0")
     ap.add_argument("--autotune", action="store_true", help="batch workload: tune the wave options first")
     args = ap.parse_args(argv)
     if args.warmup < 3:

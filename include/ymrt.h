@@ -461,6 +461,14 @@ int ymrt_post_process(ymrt_context* ctx, float* image_rgba, const uint32_t* prim
                       uint32_t height, uint32_t selected, float gamma, float exposure, int outline,
                       int device_buffers);
 
+/* SavePngImage (src/FileIO.cpp:167-194): writes a host image of width x
+ * height float RGBA pixels, bottom row first (the order render output is in),
+ * as an 8-bit RGBA PNG with each channel (uint8)(clamp(v, 0, 1) * 255 + 0.5).
+ * The path's extension is replaced by .png and missing parent directories are
+ * created. YMRT_ERR_INVALID for bad arguments, YMRT_ERR_IO when the file
+ * cannot be written. No device is needed. */
+int ymrt_save_png(const char* path, const float* rgba, int width, int height);
+
 /* Pixels of image node `texture_index` of a host scene (from
  * ymrt_scene_from_arrays, or replacing a loaded image): count =
  * width * height * channels linear floats, channels interleaved, bottom row

@@ -76,6 +76,8 @@ def _bind(L, settings_type):
     L.ymref_post_process.argtypes = [vp, vp, i, i, ctypes.c_uint32, ctypes.c_float, ctypes.c_float, i]
     L.ymref_shading_frame.argtypes = [vp, i, vp, vp, vp, vp, vp, vp]
     L.ymref_image_pixels.restype = ctypes.c_longlong
+    if hasattr(L, "ymref_save_png"):
+        L.ymref_save_png.argtypes = [ctypes.c_char_p, vp, i, i]
     L.ymref_image_pixels.argtypes = [vp, ctypes.c_uint32, vp, ctypes.c_longlong]
     L.ymref_bvh_depths.argtypes = [vp, vp]
     L.ymref_sobol_matrices.restype = ctypes.c_size_t
@@ -450,6 +452,13 @@ class RefScene:
         if n > capacity:
             raise RuntimeError(f"{n} vertices recorded, capacity {capacity}")
         return out[:n].copy(), img
+
+
+def save_png(path: str, image) -> bool:
+    """The reference's SavePngImage of an (H, W, 4) float image, bottom row
+    first (float oracle)."""
+    img = np.ascontiguousarray(image, np.float32)
+    return lib().ymref_save_png(os.fsencode(path), _p(img), img.shape[1], img.shape[0]) == 1
 
 
 def post_process(image, primitive_index, selected: int, gamma: float, exposure: float, outline: bool):

@@ -24,6 +24,7 @@
 #include YMRT_SHADING_SOURCE
 
 #include "core/SceneModule.h"
+#include "FileIO.h"
 #include "core/YMParser.h"
 
 #include <atomic>
@@ -406,6 +407,16 @@ long long ymref_image_pixels(void* handle, uint32_t tex, float* out, long long c
       for (int c = 0; c < im.channel_count; ++c) out[((long long)y * im.width + x) * im.channel_count + c] = d[c];
     }
   return n;
+}
+
+// SavePngImage (src/FileIO.cpp:167-194) of a width x height RGBA image (rows
+// bottom first, as the renderer holds them). Returns 1 on success, 0 when the
+// reference's function reports failure.
+int ymref_save_png(const char* path, const float* rgba, int width, int height) {
+  std::vector<glm::vec4> image(width > 0 && height > 0 ? (size_t)width * height : 0);
+  for (size_t k = 0; k < image.size(); ++k)
+    image[k] = glm::vec4(rgba[4 * k], rgba[4 * k + 1], rgba[4 * k + 2], rgba[4 * k + 3]);
+  return SavePngImage(path ? std::string(path) : std::string(), image, width, height) ? 1 : 0;
 }
 
 // TextureEval (src/TextureEval.cuh:419-481) of texture node `tex` at n

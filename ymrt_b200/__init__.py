@@ -150,6 +150,7 @@ def library():
     L.ymrt_render_editor_view.argtypes = [vp, ctypes.POINTER(RenderSetting), ctypes.c_uint32, ctypes.c_uint32, vp, vp, i]
     L.ymrt_post_process.argtypes = [vp, vp, vp, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_float,
                                     ctypes.c_float, i, i]
+    L.ymrt_save_png.argtypes = [ctypes.c_char_p, vp, i, i]
     L.ymrt_render_forward.argtypes = [vp, ctypes.POINTER(RenderSetting), i, vp, i, ctypes.POINTER(Stats)]
     L.ymrt_render_tiles.argtypes = [vp, ctypes.POINTER(RenderSetting), i, i, i, vp, i, ctypes.POINTER(Stats)]
     L.ymrt_accumulate.argtypes = [vp, vp, vp, i]
@@ -661,6 +662,18 @@ def post_process(ctx: Context, image, primitive_index=None, selected: int = 0xFF
     _check(library().ymrt_post_process(ctx.h, _p(img), None if prim is None else _p(prim), img.shape[1], img.shape[0],
                                        selected, gamma, exposure, int(outline), 0), ctx.h)
     return img
+
+
+def save_png(path: str, image) -> None:
+    """Writes an (H, W, 4) float host image, bottom row first, as an 8-bit
+    RGBA PNG the way the reference's SavePngImage does (the extension becomes
+    .png; channels clamped to [0, 1], scaled by 255 and rounded)."""
+    img = np.ascontiguousarray(image, np.float32)
+    if img.ndim != 3 or img.shape[2] != 4:
+        raise ValueError("save_png: image must be (height, width, 4)")
+    rc = library().ymrt_save_png(os.fsencode(path), _p(img), img.shape[1], img.shape[0])
+    if rc != YMRT_OK:
+        raise YmrtError(rc, f"save_png: cannot write {path}")
 
 
 def render_backward_ex(ctx: Context, renders, records, dlosses, material_grads=None, grid_texture=None,

@@ -36,7 +36,7 @@ CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-fno-fast-math"
              "-I" + os.path.join(ROOT, "include")]
 
 CU_SOURCES = ["kernels.cu", "wave_media.cu", "wave_adjoint.cu", "tlas_build.cu", "capi.cu"]
-CXX_SOURCES = ["scene_host.cpp", "png_decode.cpp", "image_decode.cpp"]
+CXX_SOURCES = ["scene_host.cpp", "png_decode.cpp", "png_encode.cpp", "image_decode.cpp"]
 
 
 def _stamp() -> str:

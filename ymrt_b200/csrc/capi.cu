@@ -858,7 +858,8 @@ int run_batch(ymrt_context* ctx, const BatchMemory& M, std::vector<JobDesc>& job
     return ctx->cuda_fail(e, "uploading the wave control");
   WaveOptions o = opt;
   o.capacity = M.capacity;
-  cudaMemsetAsync(M.counters, 0, sizeof(WaveCounters), st);
+  if ((e = cudaMemsetAsync(M.counters, 0, sizeof(WaveCounters), st)) != cudaSuccess)
+    return ctx->cuda_fail(e, "clearing the wave counters");
   prepare_persistent_grids();
   cudaEventRecord(ctx->ev_start, st);
   if (use_graph && !profiling) {
@@ -1102,8 +1103,10 @@ int ymrt_render_batch(ymrt_context* ctx, const ymrt_job* jobs_in, int n_jobs, ym
   int rc = context_memory(ctx, all.size(), &M);
   if (rc != YMRT_OK) return rc;
   for (const JobDesc& j : all) {
-    cudaMemsetAsync(j.image, 0, (size_t)j.width * j.height * sizeof(float4), st);
-    if (j.path_radiance) cudaMemsetAsync(j.path_radiance, 0, (size_t)j.path_count * sizeof(float4), st);
+    e = cudaMemsetAsync(j.image, 0, (size_t)j.width * j.height * sizeof(float4), st);
+    if (e == cudaSuccess && j.path_radiance)
+      e = cudaMemsetAsync(j.path_radiance, 0, (size_t)j.path_count * sizeof(float4), st);
+    if (e != cudaSuccess) return ctx->cuda_fail(e, "clearing an image or its path records");
   }
   // Launch groups of jobs whose (scene, sampler) pairs fit the constant-memory slots.
   BatchResult total;
@@ -1217,8 +1220,12 @@ int ymrt_render_backward_ex(ymrt_context* ctx, const ymrt_job* jobs_in, int n_jo
   for (JobDesc& j : jobs) j.scene_slot = lease.slot(j.scene_slot);
   if ((e = lease.upload(slots.data(), (uint32_t)slots.size())) != cudaSuccess)
     return ctx->cuda_fail(e, "uploading constants");
-  if (materials) cudaMemsetAsync(tg->material_grads_device, 0, sizeof(float) * kGradParams * tg->n_materials, st);
-  if (grid) cudaMemsetAsync(tg->grid_grads_device, 0, sizeof(float) * tg->grid_values, st);
+  if (materials &&
+      (e = cudaMemsetAsync(tg->material_grads_device, 0, sizeof(float) * kGradParams * tg->n_materials, st)) !=
+          cudaSuccess)
+    return ctx->cuda_fail(e, "clearing the material gradients");
+  if (grid && (e = cudaMemsetAsync(tg->grid_grads_device, 0, sizeof(float) * tg->grid_values, st)) != cudaSuccess)
+    return ctx->cuda_fail(e, "clearing the grid gradients");
   BatchResult r;
   if ((rc = run_batch(ctx, M, jobs, opt, ctx->profiling, ctx->graph_loop, &r)) != YMRT_OK) return rc;
   if ((e = cudaMemcpyAsync(ctx->counters_host, M.counters, sizeof(WaveCounters), cudaMemcpyDeviceToHost, st)) !=
