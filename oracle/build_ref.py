@@ -238,6 +238,109 @@ inline void ymrt_oracle_record(uint32_t pixel, int depth, int sample, const R& r
 }
 // ---- end of insertion ----
 ''')
+# Radiance-event recording, for the double-precision albedo adjoint
+# (oracle/adjoint64.py; parity builds only). Every term a path adds to its
+# received light in the stage kernels (src/Shading.cu:1857 background,
+# 2084/2088 next-event estimation at a volume vertex, 2183 a light seen
+# before any scattering, 2218/2237 next-event estimation at a surface
+# vertex) is recorded with its pixel, sample, depth, kind and (surface
+# next-event estimation) the vertex's material, and so is every surface
+# scattering event (src/Shading.cu:2265, after the BSDF weight multiplies the
+# throughput) with its material. Values are stored in double whatever the
+# build's precision. Nothing the stages compute changes: the hooks return
+# their argument.
+_EVENT_HOST = r'''
+// ---- inserted by oracle/build_ref.py: radiance-event recording ----
+#define YMRT_ORACLE_EVENTS 1
+struct YmrtOracleEvent {
+  uint32_t pixel, sample, depth;
+  int32_t kind, material;  // kind: 0 surface scattering, 1 surface NEE, 2 volume NEE, 3 background, 4 light seen
+  uint32_t pad;
+  double value[3];
+};
+struct YmrtOracleEvents {
+  YmrtOracleEvent* out = nullptr;
+  uint32_t capacity = 0;
+  const uint32_t* watch = nullptr;  // one bit per pixel (null: every pixel)
+  uint32_t n_pixels = 0;
+  std::atomic<uint32_t> count{0};
+};
+inline YmrtOracleEvents& ymrt_oracle_events() {
+  static YmrtOracleEvents e;
+  return e;
+}
+inline void ymrt_oracle_event(int kind, uint32_t pixel, int sample, int depth, int material, double r, double g,
+                              double b) {
+  YmrtOracleEvents& q = ymrt_oracle_events();
+  if (!q.out) return;
+  if (q.watch && (pixel >= q.n_pixels || !((q.watch[pixel >> 5] >> (pixel & 31u)) & 1u))) return;
+  const uint32_t k = q.count.fetch_add(1u, std::memory_order_relaxed);
+  if (k >= q.capacity) return;
+  YmrtOracleEvent& e = q.out[k];
+  e.pixel = pixel;
+  e.sample = (uint32_t)sample;
+  e.depth = (uint32_t)depth;
+  e.kind = kind;
+  e.material = material;
+  e.pad = 0u;
+  e.value[0] = r;
+  e.value[1] = g;
+  e.value[2] = b;
+}
+template <typename V>
+inline V ymrt_oracle_contrib(int kind, uint32_t pixel, int sample, int depth, int material, const V& x) {
+  ymrt_oracle_event(kind, pixel, sample, depth, material, (double)x[0], (double)x[1], (double)x[2]);
+  return x;
+}
+inline void ymrt_oracle_scatter(uint32_t pixel, int sample, int depth, int material) {
+  ymrt_oracle_event(0, pixel, sample, depth, material, 0.0, 0.0, 0.0);
+}
+// ---- end of insertion ----
+'''
+_SCATTER_SITE = "ray_throughput *= bsdf_weight;"
+_SCATTER_CALL = ("ray_throughput *= bsdf_weight;\n\t\t"
+                 "ymrt_oracle_scatter(pixel_index, pixel_sample_index, ray_depth, (int)material_index);")
+
+
+def _event_sites(body: str) -> tuple[str, int, int]:
+    """Wraps each indirect_light_clamp(...) term added to ray_received_light
+    in ymrt_oracle_contrib (kind from the term's contents) and records the
+    surface scattering site. Returns (body, terms wrapped, scatter sites)."""
+    spans = []
+    for m in re.finditer(r"\bindirect_light_clamp\(", body):
+        start = body.rfind(";", 0, m.start())
+        if "ray_received_light +=" not in body[start:m.start()]:
+            continue  # the legacy kernel's `L +=` terms and the definition
+        depth_level, k = 0, m.end() - 1
+        while True:
+            c = body[k]
+            if c == "(":
+                depth_level += 1
+            elif c == ")":
+                depth_level -= 1
+                if depth_level == 0:
+                    break
+            k += 1
+        inner = body[m.start():k + 1]
+        if "EvalVolume" in inner:
+            args = "2, pixel_index, pixel_sample_index, ray_depth, -1"
+        elif "Background(" in inner:
+            args = ("3, pixel_index, shading_ray_data_pixel_sample_index[ray_index], "
+                    "shading_ray_data_ray_depth[ray_index], -1")
+        elif "light_mtl" in inner:
+            args = "4, pixel_index, pixel_sample_index, ray_depth, -1"
+        elif "EvalDistantLight(" in inner or "EvalShapeLight(" in inner:
+            args = "1, pixel_index, pixel_sample_index, ray_depth, (int)material_index"
+        else:
+            raise RuntimeError(f"Shading.cu: unclassified radiance term {inner[:80]!r}")
+        spans.append((m.start(), k + 1, args))
+    for a, b, args in reversed(spans):
+        body = body[:a] + f"ymrt_oracle_contrib({args}, " + body[a:b] + ")" + body[b:]
+    n_scatter = body.count(_SCATTER_SITE)
+    body = body.replace(_SCATTER_SITE, _SCATTER_CALL)
+    return body, len(spans), n_scatter
+
+
 _RECORD_CALL = ("ymrt_oracle_record(pixel_index, shading_ray_data_ray_depth[ray_index], "
                 "shading_ray_data_pixel_sample_index[ray_index], ray, hit_something, hit_record, ray_throughput, "
                 "ray_received_light);\n\t\t")
@@ -310,17 +413,20 @@ def shading_source(arg_order: str, counted: bool = True, gen_name: str = "gen") 
         body, n_trace = re.subn(r"\bTraceRay\(", "ymrt_oracle_counted_trace(", body)
         body, n_shadow = re.subn(r"\bBVHTraverseShadow\(", "ymrt_oracle_counted_shadow(", body)
     body, n_prio = re.subn(r"\b(\w+)\.GetMaxPriorityRecord\(\)\.ior_priority", r"ymrt_oracle_max_priority(\1)", body)
-    n_init = 0
+    n_init = n_terms = n_scatter = 0
     if counted:
         body = _record_site(body)
         body, n_init = _init_priorities(body)
         if n_init != 2:
             raise RuntimeError(f"Shading.cu: {n_init} FetchIOR priority declarations (expected 2)")
+        body, n_terms, n_scatter = _event_sites(body)
+        if (n_terms, n_scatter) != (6, 1):
+            raise RuntimeError(f"Shading.cu: {n_terms} radiance terms and {n_scatter} scattering sites (expected 6, 1)")
     line_of_body = head.count("\n") + 1
     gen_dir = os.path.join(OUT, gen_name)
     os.makedirs(gen_dir, exist_ok=True)
     dst = os.path.join(gen_dir, "Shading.cu")
-    out = (_HELPER + f'#line 1 "{src}"\n' + head + _COUNTERS + (_RECORD_HOST if counted else "") +
+    out = (_HELPER + f'#line 1 "{src}"\n' + head + _COUNTERS + (_RECORD_HOST + _EVENT_HOST if counted else "") +
            f'#line {line_of_body} "{src}"\n' + body)
     with open(dst, "w") as f:
         f.write(out)
@@ -330,6 +436,7 @@ def shading_source(arg_order: str, counted: bool = True, gen_name: str = "gen") 
     with open(os.path.join(gen_dir, "Shading.cu.sites"), "w") as f:
         f.write(f"{n} argument lists sequenced, {n_trace} TraceRay and {n_shadow} BVHTraverseShadow calls counted, "
                 f"{n_prio} GetMaxPriorityRecord reads made direct, {n_init} IOR priorities initialised, "
+                f"{n_terms} radiance terms and {n_scatter} scattering sites recorded, "
                 f"{n_pairs} two-draw constructors in RandomSampler.cuh sequenced\n")
     return dst
 

@@ -34,6 +34,14 @@ class Settings64(ctypes.Structure):
     _fields_ = [(n, t) for n, t in Settings._fields_[:-1]] + [("indirect_limit", ctypes.c_double)]
 
 
+# One radiance event of the parity builds' event recorder (YmrtOracleEvent):
+# kind 0 surface scattering (material: the vertex's), 1 next-event estimation
+# at a surface vertex (material: the vertex's), 2 next-event estimation at a
+# volume vertex, 3 background, 4 a light seen before any scattering; value:
+# the term added to the path's light (0 for scattering), in double.
+EVENT_DTYPE = np.dtype([("pixel", "<u4"), ("sample", "<u4"), ("depth", "<u4"), ("kind", "<i4"), ("material", "<i4"),
+                        ("pad", "<u4"), ("value", "<f8", 3)])
+assert EVENT_DTYPE.itemsize == 48
 # One path vertex as the trace stage leaves it (24 words; the layout the
 # build-time recording hook writes and ymrt_debug_record_paths returns).
 VERTEX_DTYPE = np.dtype([("pixel", "<u4"), ("depth", "<u4"), ("flags", "<u4"), ("inst", "<u4"), ("tri", "<u4"),
@@ -76,6 +84,9 @@ def _bind(L, settings_type):
     L.ymref_post_process.argtypes = [vp, vp, i, i, ctypes.c_uint32, ctypes.c_float, ctypes.c_float, i]
     L.ymref_shading_frame.argtypes = [vp, i, vp, vp, vp, vp, vp, vp]
     L.ymref_image_pixels.restype = ctypes.c_longlong
+    if hasattr(L, "ymref_set_events"):
+        L.ymref_set_events.argtypes = [vp, vp, i, vp]
+        L.ymref_events_recorded.restype = ctypes.c_uint32
     if hasattr(L, "ymref_save_png"):
         L.ymref_save_png.argtypes = [ctypes.c_char_p, vp, i, i]
     L.ymref_image_pixels.argtypes = [vp, ctypes.c_uint32, vp, ctypes.c_longlong]
@@ -88,6 +99,7 @@ def _bind(L, settings_type):
     L.ymref_density.argtypes = [vp, ctypes.c_uint32, i, vp, vp]
     L.ymref_set_transforms.argtypes = [vp, ctypes.c_uint32, ctypes.c_uint32, vp, vp]
     L.ymref_set_material_params.argtypes = [vp, ctypes.c_uint32, ctypes.c_uint32, vp]
+    L.ymref_get_material_params.argtypes = [vp, ctypes.c_uint32, ctypes.c_uint32, vp]
     L.ymref_tracking_caps.restype = ctypes.c_ulonglong
     L.ymref_tracking_caps.argtypes = [i]
     if hasattr(L, "ymref_set_recorder"):
@@ -379,6 +391,16 @@ class RefScene:
         sc = None if scales is None else np.ascontiguousarray(scales, self._f).reshape(-1, 3)
         assert self._L.ymref_set_transforms(self.h, first, m.shape[0], _p(m), None if sc is None else _p(sc)) == 0
 
+    def material_params(self) -> tuple[np.ndarray, np.ndarray]:
+        """((materials, 4) diffuse albedo rgb and alpha_x of each default
+        material, zeros for others; (materials,) bool: the material is
+        Lambertian, its diffuse lobe alone)."""
+        n = int(self.counts()["materials"])
+        out = np.zeros((n, 5), self._f)
+        if self._L.ymref_get_material_params(self.h, 0, n, _p(out)) != 0:
+            raise ValueError("material range out of bounds")
+        return out[:, :4].copy(), out[:, 4] != 0
+
     def set_material_params(self, params, first: int = 0) -> None:
         """(materials, 4): diffuse albedo rgb and roughness of each default
         material, as ymrt_b200's Scene.set_material_params takes them."""
@@ -433,6 +455,26 @@ class RefScene:
 
     def last_render_seconds(self) -> float:
         return self._L.ymref_last_render_seconds(self.h)
+
+    def record_events(self, frame_index: int = 1, tile_begin: int = 0, tile_end: int = 0, capacity: int = 1 << 22,
+                      pixels=None, threads: int | None = None):
+        """Renders a frame while recording its radiance events (EVENT_DTYPE:
+        every term added to a path's light and every surface scattering
+        event) of the given pixel indices (None: all); returns (events,
+        image). Parity builds, float or double."""
+        if not hasattr(self._L, "ymref_set_events"):
+            raise RuntimeError("event recording needs a parity build")
+        out = np.zeros(capacity, EVENT_DTYPE)
+        watch = None if pixels is None else watch_bits(pixels, self.width * self.height)
+        self._L.ymref_set_events(self.h, _p(out), capacity, None if watch is None else _p(watch))
+        try:
+            img = self.render_frame(frame_index, tile_begin, tile_end, threads=threads)
+            n = int(self._L.ymref_events_recorded())
+        finally:
+            self._L.ymref_set_events(self.h, None, 0, None)
+        if n > capacity:
+            raise RuntimeError(f"{n} events recorded, capacity {capacity}")
+        return out[:n].copy(), img
 
     def record_paths(self, pixels, frame_index: int = 1, tile_begin: int = 0, tile_end: int = 0,
                      capacity: int = 1 << 16, threads: int | None = None):

@@ -705,6 +705,33 @@ int ymref_set_material_params(void* handle, uint32_t first, uint32_t count, cons
   return 0;  // edited in place: the scene's material array is the module's
 }
 
+// The materials' (diffuse albedo r, g, b, alpha_x, lambertian) as 5 floats
+// each, zeros for other material types; lambertian is 1 for a default
+// material whose only lobe is the diffuse one (no specular, metal,
+// transmission or coat weight, no texture on those or on the albedo).
+int ymref_get_material_params(void* handle, uint32_t first, uint32_t count, float* out) {
+  auto ctx = static_cast<RefContext*>(handle);
+  const auto& M = GuiModule::Materials(*ctx->module);
+  if (first > M.size() || count > M.size() - first) return -1;
+  for (uint32_t k = 0; k < count; ++k) {
+    const Material& m = M[first + k];
+    float* q = out + 5 * (size_t)k;
+    for (int c = 0; c < 5; ++c) q[c] = 0.0f;
+    if (m.material_type != DEFAULT_MTL) continue;
+    const auto& d = m.default_mtl;
+    q[0] = d.diffuse_albedo.x;
+    q[1] = d.diffuse_albedo.y;
+    q[2] = d.diffuse_albedo.z;
+    q[3] = d.alpha_x;
+    const bool untextured = d.diffuse_albedo_tex == EMPTY_UINT32 && d.specular_weight_tex == EMPTY_UINT32 &&
+                            d.metalness_tex == EMPTY_UINT32 && d.transmission_weight_tex == EMPTY_UINT32 &&
+                            d.coat_weight_tex == EMPTY_UINT32;
+    q[4] = (untextured && d.specular_weight == 0.0f && d.metalness == 0.0f && d.transmission_weight == 0.0f &&
+            d.coat_weight == 0.0f) ? 1.0f : 0.0f;
+  }
+  return 0;
+}
+
 // A medium's density as the build-time copy of VolumeEval.cuh reads it
 // (the grid node when one is attached to `tex`, else the reference's
 // TextureEval), at n object-space points (3 floats each).
@@ -747,6 +774,27 @@ void ymref_set_recorder(void* handle, const uint32_t* watch_bits, void* out, int
 // Vertices recorded since the recorder was set (those past its capacity are
 // counted, not written).
 uint32_t ymref_recorded(void) { return ymrt_oracle_recorder().count.load(); }
+#endif
+
+#if defined(YMRT_ORACLE_EVENTS)
+// Radiance-event recording (parity builds, float and double): during the
+// renders that follow, every radiance term the stages add and every surface
+// scattering event of a watched pixel (one bit per pixel in watch_bits, which
+// must stay valid; null: every pixel) is written to out (YmrtOracleEvent, 48
+// bytes), up to `capacity`; out == nullptr stops it. Resets the count.
+void ymref_set_events(void* handle, void* out, int capacity, const uint32_t* watch_bits) {
+  auto ctx = static_cast<RefContext*>(handle);
+  YmrtOracleEvents& q = ymrt_oracle_events();
+  q.out = nullptr;
+  q.capacity = out ? (uint32_t)std::max(capacity, 0) : 0u;
+  q.watch = watch_bits;
+  q.n_pixels = (uint32_t)(ctx->width * ctx->height);
+  q.count.store(0);
+  q.out = static_cast<YmrtOracleEvent*>(out);
+}
+// Events since the recorder was set (those past its capacity are counted, not
+// written).
+uint32_t ymref_events_recorded(void) { return ymrt_oracle_events().count.load(); }
 #endif
 
 // Halton sampler known-answer values: for each (px, py, sample) the global

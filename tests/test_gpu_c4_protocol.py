@@ -119,6 +119,43 @@ def test_albedo_gradients_match_the_fp64_reference(ctx, volumetric_path, halton_
     ref.close()
 
 
+def test_albedo_gradients_match_the_fp64_host_adjoint_on_a_crop(ctx, volumetric_path, halton_perm, oracle):
+    """ymrt_render_backward on a 512x512 view (16 spp, media and sun on)
+    with dLoss/dImage nonzero only on a 64x64 crop, against the host adjoint
+    in double precision (oracle/adjoint64.py) over the FP64 oracle's
+    radiance terms of the same samples, for every Lambertian (material,
+    channel) pair: each within 1%."""
+    import torch
+    from oracle import adjoint64
+    if not oracle.available64():
+        pytest.skip("FP64 oracle not built")
+    view, crop, x0, y0, spp = 512, 64, 224, 192, 16
+    scene = Y.Scene(ctx, Y.HostScene(volumetric_path, view, view), halton_perm)
+    r = _Renderer(ctx, scene, Y.default_setting(spp=spp, ray_depth=8, distant_light=True, volume=True))
+    rng = np.random.default_rng(33)
+    w = np.zeros((view, view, 4), np.float32)
+    w[y0:y0 + crop, x0:x0 + crop] = rng.uniform(0.0, 1.0, (crop, crop, 4))
+    g, _ = r.adjoint(1, torch.as_tensor(w, device="cuda"))
+    ref = oracle.RefScene(volumetric_path, halton_perm, view, view, fp64=True)
+    ref.set_settings(spp=spp, ray_depth=8, distant_light=1, volume=1)
+    params, lam = ref.material_params()
+    tiles_x = view // 16
+    ys, xs = np.mgrid[y0:y0 + crop, x0:x0 + crop]
+    ev, _ = ref.record_events(1, tile_begin=(y0 // 16) * tiles_x, tile_end=((y0 + crop) // 16) * tiles_x,
+                              pixels=(ys * view + xs).ravel())
+    h = adjoint64.albedo_adjoint(ev, w.astype(np.float64), params, np.flatnonzero(lam), spp)
+    worst = 0.0
+    for m in np.flatnonzero(lam):
+        for k in range(3):
+            rel = abs(g[m, k] - h[m, k]) / abs(h[m, k])
+            worst = max(worst, rel)
+            assert rel <= 0.01, (m, k, g[m, k], h[m, k])
+    print(f"{len(np.flatnonzero(lam)) * 3} albedo gradients against the FP64 host adjoint: worst relative "
+          f"difference {worst:.2e}")
+    ref.close()
+    scene.close()
+
+
 def test_albedo_gradients_match_float_finite_differences_at_1e3(ctx, volumetric_path, halton_perm):
     """The same eight pairs against central differences (eps 1e-3) of
     ymrt_b200's own forward render with the same samples."""
