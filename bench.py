@@ -487,8 +487,8 @@ def run_ours(args):
     profiled_image = image.cpu().numpy() if rank == 0 else None
 
     # End to end through the C ABI: upload the scene from host memory, render,
-    # read the image back -- every step.
-    host_img = np.zeros((H, W, 4), np.float32)
+    # read the image back into pinned host memory -- every step.
+    host_img = torch.zeros((H, W, 4), dtype=torch.float32).pin_memory().numpy()
     e2e_rays, e2e_wall, e2e_upload, e2e_render_dev = 0, 0.0, 0.0, 0.0
     for i in range(max(1, min(args.steps, 3))):
         torch.cuda.synchronize()

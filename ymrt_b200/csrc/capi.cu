@@ -16,6 +16,7 @@
 #include <mutex>
 #include <new>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/ymrt.h"
@@ -115,6 +116,42 @@ struct ymrt_context {
   bool defer_shadows = true;
   DeviceBuffer shadow_buf;
   ShadowQueue shadow_queue{};
+  // pinned host staging of scene uploads (grown on demand, kept)
+  void* staging = nullptr;
+  size_t staging_bytes = 0;
+  // device buffers of freed scenes' packed uploads, kept for the next upload
+  // (at most kSpareSceneBuffers, the largest), so that replacing a scene
+  // does not allocate
+  static constexpr size_t kSpareSceneBuffers = 2;
+  std::vector<std::unique_ptr<DeviceBuffer>> spare_scene_buffers;
+  std::unique_ptr<DeviceBuffer> take_spare(size_t n) {
+    size_t best = spare_scene_buffers.size();
+    for (size_t k = 0; k < spare_scene_buffers.size(); ++k)
+      if (spare_scene_buffers[k]->bytes >= n &&
+          (best == spare_scene_buffers.size() || spare_scene_buffers[k]->bytes < spare_scene_buffers[best]->bytes))
+        best = k;
+    if (best == spare_scene_buffers.size()) return std::unique_ptr<DeviceBuffer>(new DeviceBuffer());
+    std::unique_ptr<DeviceBuffer> b = std::move(spare_scene_buffers[best]);
+    spare_scene_buffers.erase(spare_scene_buffers.begin() + (long)best);
+    return b;
+  }
+  void keep_spare(std::unique_ptr<DeviceBuffer> b) {
+    spare_scene_buffers.push_back(std::move(b));
+    std::sort(spare_scene_buffers.begin(), spare_scene_buffers.end(),
+              [](const std::unique_ptr<DeviceBuffer>& a, const std::unique_ptr<DeviceBuffer>& c) {
+                return a->bytes > c->bytes;
+              });
+    while (spare_scene_buffers.size() > kSpareSceneBuffers) spare_scene_buffers.pop_back();
+  }
+  cudaError_t ensure_staging(size_t n) {
+    if (n <= staging_bytes && staging) return cudaSuccess;
+    if (staging) cudaFreeHost(staging);
+    staging = nullptr;
+    staging_bytes = 0;
+    cudaError_t e = cudaMallocHost(&staging, n);
+    if (e == cudaSuccess) staging_bytes = n;
+    return e;
+  }
 
   int fail(int code, const std::string& msg) {
     error = msg;
@@ -291,6 +328,76 @@ struct ymrt_scene {
     *out = b.as<T>();
     return e;
   }
+
+  // Packed upload: arrays gathered with pack() go to the device with one
+  // allocation and one copy from the context's pinned staging buffer
+  // (pack_commit), instead of an allocation and a pageable copy each. The
+  // host arrays must stay unchanged until pack_commit returns; the device
+  // pointers are set by pack_commit.
+  struct PackItem {
+    const void* src;
+    size_t bytes;
+    const void** out;
+  };
+  std::vector<PackItem> packed;
+  std::vector<DeviceBuffer*> packed_buffers;  // the buffers pack_commit filled (returned to the context on free)
+  template <typename T>
+  void pack(const T* src, size_t count, const T** out) {
+    packed.push_back(PackItem{src, count * sizeof(T), reinterpret_cast<const void**>(out)});
+  }
+  template <typename T>
+  void pack(const std::vector<T>& v, const T** out) {
+    pack(v.data(), v.size(), out);
+  }
+  cudaError_t pack_commit() {
+    size_t total = 0;
+    for (const PackItem& p : packed) total += (std::max<size_t>(p.bytes, 16) + 255) & ~size_t(255);
+    cudaError_t e = cudaSuccess;
+    if (total) {
+      buffers.push_back(ctx->take_spare(total));
+      DeviceBuffer& b = *buffers.back();
+      packed_buffers.push_back(&b);
+      // the staging buffer is reused: the previous upload's copy must be done
+      if ((e = cudaStreamSynchronize(ctx->stream)) == cudaSuccess) e = b.ensure(total);
+      if (e == cudaSuccess) e = ctx->ensure_staging(total);
+      if (e == cudaSuccess) {
+        unsigned char* host = static_cast<unsigned char*>(ctx->staging);
+        // the host copies in pieces of at most 4 MiB, spread over a few
+        // threads (one thread copies well below the bus's rate)
+        struct Piece {
+          unsigned char* dst;
+          const unsigned char* src;
+          size_t bytes;
+        };
+        std::vector<Piece> pieces;
+        constexpr size_t kPiece = size_t(4) << 20;
+        size_t at = 0;
+        for (const PackItem& p : packed) {
+          for (size_t o = 0; o < p.bytes; o += kPiece)
+            pieces.push_back(Piece{host + at + o, static_cast<const unsigned char*>(p.src) + o,
+                                   std::min(kPiece, p.bytes - o)});
+          *p.out = b.as<unsigned char>() + at;
+          at += (std::max<size_t>(p.bytes, 16) + 255) & ~size_t(255);
+        }
+        const size_t n_threads =
+            std::min<size_t>({pieces.size(), (size_t)std::max(1u, std::thread::hardware_concurrency()), 8});
+        auto copy_share = [&](size_t t) {
+          for (size_t k = t; k < pieces.size(); k += n_threads) std::memcpy(pieces[k].dst, pieces[k].src, pieces[k].bytes);
+        };
+        if (n_threads <= 1 || total < (size_t(4) << 20)) {
+          for (size_t t = 0; t < std::max<size_t>(n_threads, 1); ++t) copy_share(t);
+        } else {
+          std::vector<std::thread> pool;
+          for (size_t t = 1; t < n_threads; ++t) pool.emplace_back(copy_share, t);
+          copy_share(0);
+          for (std::thread& th : pool) th.join();
+        }
+        e = cudaMemcpyAsync(b.ptr, host, total, cudaMemcpyHostToDevice, ctx->stream);
+      }
+    }
+    packed.clear();
+    return e;
+  }
 };
 
 namespace {
@@ -380,6 +487,8 @@ void ymrt_destroy(ymrt_context* ctx) {
   ctx->drop_graph();
   if (ctx->counters_host) cudaFreeHost(ctx->counters_host);
   if (ctx->ctl_host) cudaFreeHost(ctx->ctl_host);
+  if (ctx->staging) cudaFreeHost(ctx->staging);
+  ctx->spare_scene_buffers.clear();
   ctx->ctl_buf.release();
   if (ctx->ev_start) cudaEventDestroy(ctx->ev_start);
   if (ctx->ev_stop) cudaEventDestroy(ctx->ev_stop);
@@ -622,10 +731,19 @@ int ymrt_scene_upload(ymrt_context* ctx, const ymrt_host_scene* hs, const uint32
   sc->triangles = s.triangle_count_instanced;
   DeviceScene& D = sc->dev;
   cudaError_t e = cudaSuccess;
-#define UP(vec, field)                                          \
-  do {                                                          \
-    if (e == cudaSuccess) e = sc->upload(vec, &D.field);        \
-  } while (0)
+  // image pixels first (the texture nodes point at them), then every other
+  // array in one packed upload
+  std::vector<Texture> tex = s.textures;
+  for (size_t k = 0; k < tex.size(); ++k) {
+    if (tex[k].type != kTexImage) continue;
+    auto it = s.images.find((uint32_t)k);
+    const size_t n = (size_t)tex[k].width * tex[k].height * tex[k].channels;
+    if (it == s.images.end() || it->second.size() != n)
+      return ctx->fail(YMRT_ERR_INVALID, "image node " + std::to_string(k) + " has no pixels (ymrt_host_scene_set_image)");
+    sc->pack(it->second, &tex[k].image);
+  }
+  e = sc->pack_commit();
+#define UP(vec, field) sc->pack(vec, &D.field)
   UP(s.instances, instances);
   UP(s.transforms, transforms);
   UP(s.i_transforms, i_transforms);
@@ -647,33 +765,16 @@ int ymrt_scene_upload(ymrt_context* ctx, const ymrt_host_scene* hs, const uint32
   UP(s.shape_lights, shape_lights);
   UP(s.shape_light_table, shape_light_table);
   UP(s.volumes, volumes);
-  {
-    // image nodes: pixels into device buffers, the node pointing at them
-    std::vector<Texture> tex = s.textures;
-    for (size_t k = 0; k < tex.size() && e == cudaSuccess; ++k) {
-      if (tex[k].type != kTexImage) continue;
-      auto it = s.images.find((uint32_t)k);
-      const size_t n = (size_t)tex[k].width * tex[k].height * tex[k].channels;
-      if (it == s.images.end() || it->second.size() != n)
-        return ctx->fail(YMRT_ERR_INVALID, "image node " + std::to_string(k) + " has no pixels (ymrt_host_scene_set_image)");
-      const float* dev = nullptr;
-      e = sc->upload(it->second, &dev);
-      tex[k].image = dev;
-    }
-    UP(tex, textures);
-    sc->textures = tex;
-  }
-  {
-    std::vector<uint8_t> buckets(s.instances.size());
-    for (size_t i = 0; i < s.instances.size(); ++i) buckets[i] = (uint8_t)shading_bucket(s, s.instances[i]);
-    UP(buckets, inst_bucket);
-  }
+  UP(tex, textures);
+  sc->textures = tex;
+  std::vector<uint8_t> buckets(s.instances.size());
+  for (size_t i = 0; i < s.instances.size(); ++i) buckets[i] = (uint8_t)shading_bucket(s, s.instances[i]);
+  UP(buckets, inst_bucket);
 #undef UP
-  if (e == cudaSuccess) {
-    std::vector<uint32_t> perm(halton_perm, halton_perm + perm_len);
-    e = sc->upload(perm, &D.halton_perm);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
-  }
+  sc->pack(halton_perm, perm_len, &D.halton_perm);
+  if (e == cudaSuccess) e = sc->pack_commit();
+  else sc->packed.clear();
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
   if (e != cudaSuccess) return ctx->cuda_fail(e, "uploading scene");
   D.sampler_type = kSamplerHalton;
   D.instance_count = (uint32_t)s.instances.size();
@@ -745,6 +846,11 @@ void ymrt_scene_free(ymrt_scene* scene) {
   if (!scene) return;
   cudaSetDevice(scene->ctx->device);
   cudaStreamSynchronize(scene->ctx->stream);
+  // the packed upload's buffers go back to the context for the next upload
+  for (std::unique_ptr<DeviceBuffer>& b : scene->buffers)
+    if (b && b->ptr &&
+        std::find(scene->packed_buffers.begin(), scene->packed_buffers.end(), b.get()) != scene->packed_buffers.end())
+      scene->ctx->keep_spare(std::move(b));
   delete scene;
 }
 
