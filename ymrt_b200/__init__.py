@@ -179,7 +179,7 @@ def _check(rc: int, ctx=None):
         raise YmrtError(rc, msg)
 
 
-OPTIONS = {"sort_hits": 1, "defer_shadows": 2, "graph_loop": 3, "trace_block": 4}
+OPTIONS = {"sort_hits": 1, "defer_shadows": 2, "graph_loop": 3, "trace_block": 4, "sort_rays": 6}
 
 
 class Context:

@@ -114,6 +114,7 @@ struct ymrt_context {
   bool sort_hits = true;
   uint32_t trace_block = 128;  // threads per block of k_extend / k_connect (YMRT_OPT_TRACE_BLOCK)
   bool defer_shadows = true;
+  bool sort_rays = true;  // YMRT_OPT_SORT_RAYS
   DeviceBuffer shadow_buf;
   ShadowQueue shadow_queue{};
   // pinned host staging of scene uploads (grown on demand, kept)
@@ -187,7 +188,8 @@ struct ymrt_context {
       P.capacity = capacity;
     }
     const size_t hit_bytes = n * (sizeof(float4) + sizeof(uint4) + kMaxNearby * sizeof(uint4) +
-                                  kMaxBoundaryRecord * sizeof(float) + sizeof(uint32_t) + 1);
+                                  kMaxBoundaryRecord * sizeof(float) + sizeof(uint32_t) + 1) +
+                             2 * kRayBins * sizeof(uint32_t) + n * sizeof(uint16_t) + 16;
     cudaError_t e = hit_buf.ensure(hit_bytes);
     if (e != cudaSuccess) return cuda_fail(e, "allocating hit pool");
     char* h = hit_buf.as<char>();
@@ -196,6 +198,8 @@ struct ymrt_context {
     hits.nearby = reinterpret_cast<uint4*>(h); h += n * kMaxNearby * sizeof(uint4);
     hits.vol_w = reinterpret_cast<float*>(h); h += n * kMaxBoundaryRecord * sizeof(float);
     hits.order = reinterpret_cast<uint32_t*>(h); h += n * sizeof(uint32_t);
+    hits.ray_bins = reinterpret_cast<uint32_t*>(h); h += 2 * kRayBins * sizeof(uint32_t);
+    hits.ray_key = reinterpret_cast<uint16_t*>(h); h += n * sizeof(uint16_t);
     hits.bucket = reinterpret_cast<uint8_t*>(h);
     pool_capacity = capacity;
     shadow_queue = ShadowQueue{};
@@ -518,6 +522,7 @@ int ymrt_set_option(ymrt_context* ctx, int option, int value) {
     case YMRT_OPT_SORT_HITS: ctx->sort_hits = value != 0; return YMRT_OK;
     case YMRT_OPT_DEFER_SHADOWS: ctx->defer_shadows = value != 0; return YMRT_OK;
     case YMRT_OPT_GRAPH_LOOP: ctx->graph_loop = value != 0; return YMRT_OK;
+    case YMRT_OPT_SORT_RAYS: ctx->sort_rays = value != 0; return YMRT_OK;
     case YMRT_OPT_TRACE_BLOCK:
       if (value != 64 && value != 128 && value != 256)
         return ctx->fail(YMRT_ERR_INVALID, "YMRT_OPT_TRACE_BLOCK must be 64, 128 or 256");
@@ -534,6 +539,7 @@ int ymrt_get_option(const ymrt_context* ctx, int option, int* value) {
     case YMRT_OPT_DEFER_SHADOWS: *value = ctx->defer_shadows ? 1 : 0; return YMRT_OK;
     case YMRT_OPT_GRAPH_LOOP: *value = ctx->graph_loop ? 1 : 0; return YMRT_OK;
     case YMRT_OPT_TRACE_BLOCK: *value = (int)ctx->trace_block; return YMRT_OK;
+    case YMRT_OPT_SORT_RAYS: *value = ctx->sort_rays ? 1 : 0; return YMRT_OK;
     default: return YMRT_ERR_INVALID;
   }
 }
@@ -973,7 +979,7 @@ int run_batch(ymrt_context* ctx, const BatchMemory& M, std::vector<JobDesc>& job
         (uintptr_t)M.pool[0].ray_o, (uintptr_t)M.pool[1].ray_o, (uintptr_t)M.hits.bary_t, (uintptr_t)M.ctl,
         (uintptr_t)M.jobs, (uintptr_t)M.counters, (uintptr_t)jobs.size(), (uintptr_t)o.volumes,
         (uintptr_t)o.sort_hits, (uintptr_t)o.defer_shadows, (uintptr_t)o.shadow_queue.o, M.capacity,
-        (uintptr_t)o.trace_block,
+        (uintptr_t)o.trace_block, (uintptr_t)o.sort_rays,
         (uintptr_t)o.features, (uintptr_t)o.grid_grads, (uintptr_t)o.grid_tex,
         (uintptr_t)o.adjoint, (uintptr_t)o.grads, o.grad_materials};
     if (ctx->graph_key != key) {
@@ -1118,6 +1124,7 @@ int batch_options(ymrt_context* ctx, const std::vector<JobDesc>& jobs, WaveOptio
   }
   opt->sort_hits = ctx->sort_hits;
   opt->trace_block = ctx->trace_block;
+  opt->sort_rays = ctx->sort_rays;
   opt->defer_shadows = ctx->defer_shadows && !opt->volumes && !clamp;
   if (opt->defer_shadows) {
     int rc = ctx->ensure_shadow_queue();
@@ -1316,6 +1323,7 @@ int ymrt_render_backward_ex(ymrt_context* ctx, const ymrt_job* jobs_in, int n_jo
   opt.adjoint = true;
   opt.volumes = volumes;
   opt.trace_block = ctx->trace_block;
+  opt.sort_rays = ctx->sort_rays;
   opt.features = batch_features(slots.data(), slots.size());
   opt.grads = materials ? tg->material_grads_device : nullptr;
   opt.grad_materials = materials ? tg->n_materials : 0;
@@ -1684,6 +1692,8 @@ size_t carve(unsigned char* base, uint32_t n, PathPool pools[2], HitPool* hits, 
   hits->vol_w = nullptr;  // volume scattering is not rendered by this entry point
   hits->order = reinterpret_cast<uint32_t*>(take(n * sizeof(uint32_t)));
   hits->bucket = reinterpret_cast<uint8_t*>(take(n));
+  hits->ray_key = nullptr;  // continuing rays are traced in slot order here
+  hits->ray_bins = nullptr;
   return off;
 }
 

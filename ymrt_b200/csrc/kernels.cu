@@ -442,12 +442,14 @@ cudaError_t upload_constants(const DeviceScene* scenes, const uint32_t* slots, u
 
 // Start of a wave: the continuing paths left by the previous wave, the new
 // paths to generate (as many as fit), and the per-wave counters cleared.
-__global__ void k_plan(WaveControl* ctl, WaveCounters* counters) {
+__global__ void k_plan(WaveControl* ctl, WaveCounters* counters, uint32_t* ray_bins) {
   __shared__ uint32_t s_live;
   if (threadIdx.x == 0) s_live = counters->next_count;
   __syncthreads();
   uint32_t* words = reinterpret_cast<uint32_t*>(counters);
   for (uint32_t k = threadIdx.x; k < (uint32_t)(kWaveClearBytes / sizeof(uint32_t)); k += blockDim.x) words[k] = 0u;
+  if (ray_bins)
+    for (uint32_t k = threadIdx.x; k < kRayBins; k += blockDim.x) ray_bins[k] = 0u;
   if (threadIdx.x == 0) {
     const uint32_t live = ctl->more ? s_live : 0u;
     const unsigned long long left = ctl->more ? ctl->total - ctl->cursor : 0ull;
@@ -458,6 +460,107 @@ __global__ void k_plan(WaveControl* ctl, WaveCounters* counters) {
     ctl->count = live + gen;
     ctl->gen_cursor = ctl->cursor;
     ctl->cursor += gen;
+  }
+}
+
+// ------------------------------------------- continuing rays, grouped ---
+//
+// Continuing rays leave surfaces all over the scene in scattered directions;
+// k_shade writes them in shading order (grouped by material). Traced in that
+// order, the 32 lanes of a warp walk unrelated parts of the BVH. Before the
+// closest-hit stage, the wave's continuing slots are grouped by a key of the
+// ray's origin cell (an 8x8x8 grid over the scene's top-level bounds, Morton
+// order) and its direction (cube face and quadrant, 24 values) with one
+// counting sort (k_ray_hist, k_ray_scan, k_ray_scatter), and k_extend takes
+// them in that order. The hits are written to the rays' own slots, so nothing
+// after the closest-hit stage sees the order.
+
+__device__ __forceinline__ uint32_t spread3(uint32_t v) {  // 3 bits -> bits 0, 3, 6
+  return (v & 1u) | ((v & 2u) << 2) | ((v & 4u) << 4);
+}
+
+__device__ __forceinline__ uint32_t ray_group_key(const DeviceScene& S, float4 o, float4 d) {
+  // the scene's bounds: the top-level root's grid, origin + [0, 255] * 2^e
+  const uint4 w0 = __ldg(reinterpret_cast<const uint4*>(S.tlas_nodes));
+  const float lo[3] = {__uint_as_float(w0.x), __uint_as_float(w0.y), __uint_as_float(w0.z)};
+  const float ext[3] = {255.0f * __uint_as_float((w0.w & 0xFFu) << 23),
+                        255.0f * __uint_as_float(((w0.w >> 8) & 0xFFu) << 23),
+                        255.0f * __uint_as_float(((w0.w >> 16) & 0xFFu) << 23)};
+  const float p[3] = {o.x, o.y, o.z};
+  uint32_t cell[3];
+  for (int a = 0; a < 3; ++a) {
+    const float f = (p[a] - lo[a]) / ext[a] * 8.0f;
+    cell[a] = f > 0.0f ? min((uint32_t)f, 7u) : 0u;
+  }
+  const uint32_t morton = spread3(cell[0]) | (spread3(cell[1]) << 1) | (spread3(cell[2]) << 2);
+  const float ax = fabsf(d.x), ay = fabsf(d.y), az = fabsf(d.z);
+  uint32_t face, q;
+  if (ax >= ay && ax >= az) {
+    face = d.x < 0.0f ? 1u : 0u;
+    q = (d.y < 0.0f ? 1u : 0u) | (d.z < 0.0f ? 2u : 0u);
+  } else if (ay >= az) {
+    face = d.y < 0.0f ? 3u : 2u;
+    q = (d.x < 0.0f ? 1u : 0u) | (d.z < 0.0f ? 2u : 0u);
+  } else {
+    face = d.z < 0.0f ? 5u : 4u;
+    q = (d.x < 0.0f ? 1u : 0u) | (d.y < 0.0f ? 2u : 0u);
+  }
+  return (morton << 5) | (face * 4u + q);  // < kRayBins
+}
+
+__global__ void __launch_bounds__(256) k_ray_hist(PathPool P, const WaveControl* __restrict__ ctl, HitPool H,
+                                                  const JobDesc* __restrict__ jobs) {
+  const uint32_t live = ctl->live;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < live; i += gridDim.x * blockDim.x) {
+    const uint2 pf = P.pixel_flags[i];
+    const uint32_t key = ray_group_key(c_scenes[jobs[pf.y >> kFlagJobShift].scene_slot], P.ray_o[i], P.ray_d[i]);
+    H.ray_key[i] = (uint16_t)key;
+    atomicAdd(&H.ray_bins[key], 1u);
+  }
+}
+
+// Exclusive prefix sums of the kRayBins counts into the offsets (one block).
+__global__ void __launch_bounds__(1024) k_ray_scan(HitPool H) {
+  constexpr uint32_t kPer = kRayBins / 1024;
+  __shared__ uint32_t s_sum[1024];
+  const uint32_t t = threadIdx.x;
+  uint32_t v[kPer], acc = 0;
+  for (uint32_t k = 0; k < kPer; ++k) {
+    v[k] = H.ray_bins[t * kPer + k];
+    acc += v[k];
+  }
+  s_sum[t] = acc;
+  __syncthreads();
+  for (uint32_t off = 1; off < 1024; off <<= 1) {  // inclusive scan (Hillis-Steele)
+    const uint32_t x = t >= off ? s_sum[t - off] : 0u;
+    __syncthreads();
+    s_sum[t] += x;
+    __syncthreads();
+  }
+  uint32_t base = s_sum[t] - acc;
+  for (uint32_t k = 0; k < kPer; ++k) {
+    H.ray_bins[kRayBins + t * kPer + k] = base;
+    base += v[k];
+  }
+}
+
+__global__ void __launch_bounds__(256) k_ray_scatter(const WaveControl* __restrict__ ctl, HitPool H) {
+  const uint32_t live = ctl->live;
+  for (uint32_t warp_base = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); warp_base < live;
+       warp_base += gridDim.x * blockDim.x) {
+    const uint32_t i = warp_base + (threadIdx.x & 31u);
+    const bool has = i < live;
+    const uint32_t key = has ? (uint32_t)H.ray_key[i] : 0u;
+    const uint32_t act = __ballot_sync(0xFFFFFFFFu, has);
+    if (!has) continue;
+    // lanes with the same key take consecutive positions, in slot order
+    const int lane = threadIdx.x & 31;
+    const uint32_t peers = __match_any_sync(act, key);
+    const int leader = __ffs(peers) - 1;
+    uint32_t base = 0;
+    if (lane == leader) base = atomicAdd(&H.ray_bins[kRayBins + key], (uint32_t)__popc(peers));
+    base = __shfl_sync(peers, base, leader);
+    H.order[base + (uint32_t)__popc(peers & ((1u << lane) - 1u))] = i;
   }
 }
 
@@ -507,7 +610,7 @@ template <uint32_t kF>
 void launch_extend_surface(const WaveArgs& w) {
   const auto k = k_extend<false, kF & kFeatSpheres>;
   k<<<w.trace_blocks, w.trace_block, traversal_shared_bytes(w.trace_block), w.stream>>>(w.A, w.ctl, w.H, w.jobs, w.counters, nullptr,
-                                                                   kEmpty);
+                                                                   kEmpty, w.ray_order);
 }
 
 template <uint32_t kF>
@@ -563,12 +666,20 @@ uint32_t launch_wave(const PathPool& A, const PathPool& B, const HitPool& H, Wav
   // the uneven per-ray work; k_connect walks its queue with a GPU-sized grid.
   const uint32_t cap = std::max(opt.capacity, 1u);
   const uint32_t blocks_256 = (cap + 255) / 256, blocks_trace = (cap + kTraceBlock - 1) / kTraceBlock;
-  k_plan<<<1, 128, 0, stream>>>(ctl, counters);
+  // continuing rays grouped before tracing (surfaces; the pool must have the key arrays)
+  const bool sort_rays = opt.sort_rays && !opt.volumes && H.ray_key && H.ray_bins && H.order;
+  k_plan<<<1, 128, 0, stream>>>(ctl, counters, sort_rays ? H.ray_bins : nullptr);
+  if (sort_rays) {
+    k_ray_hist<<<blocks_256, 256, 0, stream>>>(A, ctl, H, jobs);
+    k_ray_scan<<<1, 1024, 0, stream>>>(H);
+    k_ray_scatter<<<blocks_256, 256, 0, stream>>>(ctl, H);
+  }
   if (ev) cudaEventRecord(ev[0], stream);
   k_generate<<<blocks_256, 256, 0, stream>>>(A, ctl, jobs, n_jobs);
   if (ev) cudaEventRecord(ev[1], stream);
   const uint32_t tb = (opt.trace_block == 64 || opt.trace_block == 256) ? opt.trace_block : (uint32_t)kTraceBlock;
-  const WaveArgs w{A, B, Hs, ctl, jobs, counters, blocks_trace, stream, tb, (cap + tb - 1) / tb};
+  const WaveArgs w{A, B, Hs, ctl, jobs, counters, blocks_trace, stream, tb, (cap + tb - 1) / tb,
+                   sort_rays ? H.order : nullptr};
   if (adjoint && opt.volumes) {
     launch_adjoint_extend_media(w, opt);
   } else if (opt.volumes) {
@@ -603,7 +714,7 @@ uint32_t launch_wave(const PathPool& A, const PathPool& B, const HitPool& H, Wav
     k_connect<0><<<conn_grid, tb, occluded_shared_bytes(tb), stream>>>(*defer, jobs, counters);
   if (ev) cudaEventRecord(ev[5], stream);
   k_finish<<<1, 32, 0, stream>>>(ctl, counters, graph_condition);
-  return 5u + (sort_hits ? 1u : 0u) + (defer ? 1u : 0u);
+  return 5u + (sort_hits ? 1u : 0u) + (defer ? 1u : 0u) + (sort_rays ? 3u : 0u);
 }
 
 cudaError_t read_bound_record(uint32_t* words, int n_words, bool clear, cudaStream_t stream) {

@@ -55,8 +55,12 @@ struct HitPool {
   uint4* nearby;    // kMaxNearby entries per slot: prim, t bits, back
   float* vol_w;     // kMaxBoundaryRecord medium-selection weights per slot (volume hits only)
   uint8_t* bucket;  // shading bucket per slot (kBucketNone: nothing to shade)
-  uint32_t* order;  // slots to shade, bucket by bucket
+  uint32_t* order;  // slots to shade, bucket by bucket (before the closest-hit stage: continuing rays, grouped)
+  uint16_t* ray_key;   // grouping key per continuing slot (null: rays are not grouped)
+  uint32_t* ray_bins;  // kRayBins counts, then kRayBins offsets
 };
+// Continuing rays are traced grouped by origin cell and direction (k_ray_*).
+constexpr uint32_t kRayBins = 1u << 14;
 
 // One render of a batch (a single render is a batch of one): its scene,
 // settings, output image and its range in the batch's path space (paths are
@@ -188,6 +192,7 @@ struct WaveOptions {
   uint32_t capacity = 0;       // path slots per pool (sizes the grids)
   bool volumes = false;        // volume scattering kernels
   bool sort_hits = true;       // shade hits listed by shading bucket
+  bool sort_rays = false;      // surfaces: trace continuing rays grouped by origin cell and direction
   bool defer_shadows = false;  // queue surface shadow rays for k_connect (ignored with volumes)
   uint32_t features = kFeatAll;  // scene features of the batch (kFeatSpheres | kFeatGrids | kFeatTextures)
   ShadowQueue shadow_queue{};
@@ -211,6 +216,7 @@ struct WaveArgs {
   cudaStream_t stream;
   uint32_t trace_block;   // k_extend's threads per block
   uint32_t trace_blocks;  // k_extend's blocks (one thread per pool slot)
+  const uint32_t* ray_order = nullptr;  // continuing slots in grouped order (null: slot order)
 };
 // Before any launch (and before any stream capture) on the current device:
 // lets the k_extend instantiations of the media and adjoint units take a

@@ -123,6 +123,10 @@ __device__ __forceinline__ void file_bucket(WaveCounters* counters, uint32_t buc
 // radiance the path gathers after the segment (its recorded total minus what
 // it gathered so far).
 //
+// ray_order (surfaces, optional): the continuing slots [0, live) in the order
+// to trace them (k_ray_scatter: grouped by origin cell and direction), so that
+// neighbouring lanes take similar walks; the new camera paths keep slot order.
+//
 // Launched with kTraceBlock threads by default, or any block size up to
 // kMaxTraceBlock (YMRT_OPT_TRACE_BLOCK, tuned by ymrt_b200.autotune); the
 // traversal stacks are in dynamic shared memory (traversal_shared_bytes).
@@ -132,15 +136,25 @@ __device__ __forceinline__ void file_bucket(WaveCounters* counters, uint32_t buc
 template <bool kVol, uint32_t kF, bool kAdj = false>
 __global__ void __launch_bounds__(kMaxTraceBlock, 4 * kTraceBlock / kMaxTraceBlock) k_extend(PathPool P, const WaveControl* __restrict__ ctl, HitPool H,
                                                            const JobDesc* __restrict__ jobs, WaveCounters* counters,
-                                                           float* grid_grads = nullptr, uint32_t grid_tex = kEmpty) {
+                                                           float* grid_grads = nullptr, uint32_t grid_tex = kEmpty,
+                                                           const uint32_t* __restrict__ ray_order = nullptr) {
   YM_TRAVERSAL_SHARED_DYNAMIC(s_stack);
   const uint32_t count = ctl->count;
+  const uint32_t live = ray_order ? ctl->live : 0u;
   uint32_t tests = 0, nodes = 0, n_rays = 0;
   bool overflow = false;
   for (uint32_t warp_base = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); warp_base < count;
        warp_base += gridDim.x * blockDim.x) {
-  const uint32_t i = warp_base + (threadIdx.x & 31u);
-  bool active = i < count;
+  const uint32_t j = warp_base + (threadIdx.x & 31u);
+  uint32_t i = j;
+  if (j < live) {
+    i = ray_order[j];
+    if (i >= live) {  // not a continuing slot: the order is broken (never expected)
+      atomicOr(&counters->errors, (uint32_t)kDevErrQueue);
+      i = j;
+    }
+  }
+  bool active = j < count;
   uint2 pf = active ? P.pixel_flags[i] : make_uint2(kEmpty, kFlagDead);
   if (active && (pf.y & kFlagDead)) active = false;
   uint32_t bucket = kBucketNone;
@@ -226,7 +240,7 @@ __global__ void __launch_bounds__(kMaxTraceBlock, 4 * kTraceBlock / kMaxTraceBlo
       bucket = volume_hit ? kBucketVolume : (uint32_t)S.inst_bucket[ch.inst];
     }
   }
-  if (i < count) H.bucket[i] = (uint8_t)bucket;
+  if (j < count) H.bucket[i] = (uint8_t)bucket;
   file_bucket(counters, bucket);
   n_rays += __popc(__ballot_sync(0xFFFFFFFFu, active));
   }
