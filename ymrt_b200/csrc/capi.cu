@@ -189,7 +189,7 @@ struct ymrt_context {
     }
     const size_t hit_bytes = n * (sizeof(float4) + sizeof(uint4) + kMaxNearby * sizeof(uint4) +
                                   kMaxBoundaryRecord * sizeof(float) + sizeof(uint32_t) + 1) +
-                             2 * kRayBins * sizeof(uint32_t) + n * sizeof(uint16_t) + 16;
+                             kRayBinWords * sizeof(uint32_t) + 2 * n * sizeof(uint32_t) + 16;
     cudaError_t e = hit_buf.ensure(hit_bytes);
     if (e != cudaSuccess) return cuda_fail(e, "allocating hit pool");
     char* h = hit_buf.as<char>();
@@ -198,8 +198,9 @@ struct ymrt_context {
     hits.nearby = reinterpret_cast<uint4*>(h); h += n * kMaxNearby * sizeof(uint4);
     hits.vol_w = reinterpret_cast<float*>(h); h += n * kMaxBoundaryRecord * sizeof(float);
     hits.order = reinterpret_cast<uint32_t*>(h); h += n * sizeof(uint32_t);
-    hits.ray_bins = reinterpret_cast<uint32_t*>(h); h += 2 * kRayBins * sizeof(uint32_t);
-    hits.ray_key = reinterpret_cast<uint16_t*>(h); h += n * sizeof(uint16_t);
+    hits.ray_bins = reinterpret_cast<uint32_t*>(h); h += kRayBinWords * sizeof(uint32_t);
+    hits.ray_key = reinterpret_cast<uint32_t*>(h); h += n * sizeof(uint32_t);
+    hits.ray_order = reinterpret_cast<uint32_t*>(h); h += n * sizeof(uint32_t);
     hits.bucket = reinterpret_cast<uint8_t*>(h);
     pool_capacity = capacity;
     shadow_queue = ShadowQueue{};
@@ -972,6 +973,8 @@ int run_batch(ymrt_context* ctx, const BatchMemory& M, std::vector<JobDesc>& job
   o.capacity = M.capacity;
   if ((e = cudaMemsetAsync(M.counters, 0, sizeof(WaveCounters), st)) != cudaSuccess)
     return ctx->cuda_fail(e, "clearing the wave counters");
+  if (M.hits.ray_bins && (e = cudaMemsetAsync(M.hits.ray_bins, 0, kRayBins * sizeof(uint32_t), st)) != cudaSuccess)
+    return ctx->cuda_fail(e, "clearing the ray-grouping counts");
   prepare_persistent_grids();
   cudaEventRecord(ctx->ev_start, st);
   if (use_graph && !profiling) {
@@ -1694,6 +1697,7 @@ size_t carve(unsigned char* base, uint32_t n, PathPool pools[2], HitPool* hits, 
   hits->bucket = reinterpret_cast<uint8_t*>(take(n));
   hits->ray_key = nullptr;  // continuing rays are traced in slot order here
   hits->ray_bins = nullptr;
+  hits->ray_order = nullptr;
   return off;
 }
 

@@ -138,9 +138,11 @@ __global__ void __launch_bounds__(256) k_record_vertices(PathPool P, const WaveC
 }
 
 __global__ void __launch_bounds__(256) k_sort_hits(const WaveControl* __restrict__ ctl, HitPool H, PathPool P,
-                                                   const JobDesc* __restrict__ jobs, WaveCounters* counters) {
+                                                   const JobDesc* __restrict__ jobs, WaveCounters* counters,
+                                                   const uint32_t* __restrict__ ray_order) {
   __shared__ uint32_t s_start[kShadeBuckets];
   const uint32_t count = ctl->count;
+  const uint32_t live = ray_order ? ctl->live : 0u;
   if (blockIdx.x * blockDim.x >= count) return;  // (uniform per block)
   if (threadIdx.x == 0) {
     uint32_t acc = 0;
@@ -152,8 +154,12 @@ __global__ void __launch_bounds__(256) k_sort_hits(const WaveControl* __restrict
   __syncthreads();
   for (uint32_t warp_base = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); warp_base < count;
        warp_base += gridDim.x * blockDim.x) {
-  const uint32_t i = warp_base + (threadIdx.x & 31u);
-  uint32_t b = i < count ? (uint32_t)H.bucket[i] : (uint32_t)kBucketNone;
+  // slots in the order they were traced (continuing rays grouped), so that
+  // each bucket lists its hits in that order too
+  const uint32_t j = warp_base + (threadIdx.x & 31u);
+  uint32_t i = j;
+  if (j < live && ray_order[j] < live) i = ray_order[j];
+  uint32_t b = j < count ? (uint32_t)H.bucket[i] : (uint32_t)kBucketNone;
   if (b == kBucketMiss) {
     const uint2 pf = P.pixel_flags[i];
     const JobDesc& J = jobs[pf.y >> kFlagJobShift];
@@ -442,14 +448,12 @@ cudaError_t upload_constants(const DeviceScene* scenes, const uint32_t* slots, u
 
 // Start of a wave: the continuing paths left by the previous wave, the new
 // paths to generate (as many as fit), and the per-wave counters cleared.
-__global__ void k_plan(WaveControl* ctl, WaveCounters* counters, uint32_t* ray_bins) {
+__global__ void k_plan(WaveControl* ctl, WaveCounters* counters) {
   __shared__ uint32_t s_live;
   if (threadIdx.x == 0) s_live = counters->next_count;
   __syncthreads();
   uint32_t* words = reinterpret_cast<uint32_t*>(counters);
   for (uint32_t k = threadIdx.x; k < (uint32_t)(kWaveClearBytes / sizeof(uint32_t)); k += blockDim.x) words[k] = 0u;
-  if (ray_bins)
-    for (uint32_t k = threadIdx.x; k < kRayBins; k += blockDim.x) ray_bins[k] = 0u;
   if (threadIdx.x == 0) {
     const uint32_t live = ctl->more ? s_live : 0u;
     const unsigned long long left = ctl->more ? ctl->total - ctl->cursor : 0ull;
@@ -471,12 +475,19 @@ __global__ void k_plan(WaveControl* ctl, WaveCounters* counters, uint32_t* ray_b
 // closest-hit stage, the wave's continuing slots are grouped by a key of the
 // ray's origin cell (an 8x8x8 grid over the scene's top-level bounds, Morton
 // order) and its direction (cube face and quadrant, 24 values) with one
-// counting sort (k_ray_hist, k_ray_scan, k_ray_scatter), and k_extend takes
+// counting sort (k_ray_hist, k_ray_scan_*, k_ray_scatter), and k_extend takes
 // them in that order. The hits are written to the rays' own slots, so nothing
 // after the closest-hit stage sees the order.
 
-__device__ __forceinline__ uint32_t spread3(uint32_t v) {  // 3 bits -> bits 0, 3, 6
-  return (v & 1u) | ((v & 2u) << 2) | ((v & 4u) << 4);
+__device__ __forceinline__ uint32_t spread3(uint32_t v) {  // bits 0, 1, 2, ... -> bits 0, 3, 6, ...
+  uint32_t r = 0;
+  for (uint32_t b = 0; b < kRayCellBits; ++b) r |= ((v >> b) & 1u) << (3 * b);
+  return r;
+}
+
+__device__ __forceinline__ uint32_t face_square(float u, float major) {  // u / |major| in [-1, 1] -> 0..kRayDirSplit-1
+  const float f = (u / major + 1.0f) * (0.5f * (float)kRayDirSplit);
+  return f > 0.0f ? min((uint32_t)f, kRayDirSplit - 1u) : 0u;
 }
 
 __device__ __forceinline__ uint32_t ray_group_key(const DeviceScene& S, float4 o, float4 d) {
@@ -487,25 +498,29 @@ __device__ __forceinline__ uint32_t ray_group_key(const DeviceScene& S, float4 o
                         255.0f * __uint_as_float(((w0.w >> 8) & 0xFFu) << 23),
                         255.0f * __uint_as_float(((w0.w >> 16) & 0xFFu) << 23)};
   const float p[3] = {o.x, o.y, o.z};
+  constexpr float kCells = (float)(1u << kRayCellBits);
   uint32_t cell[3];
   for (int a = 0; a < 3; ++a) {
-    const float f = (p[a] - lo[a]) / ext[a] * 8.0f;
-    cell[a] = f > 0.0f ? min((uint32_t)f, 7u) : 0u;
+    const float f = (p[a] - lo[a]) / ext[a] * kCells;
+    cell[a] = f > 0.0f ? min((uint32_t)f, (1u << kRayCellBits) - 1u) : 0u;
   }
   const uint32_t morton = spread3(cell[0]) | (spread3(cell[1]) << 1) | (spread3(cell[2]) << 2);
   const float ax = fabsf(d.x), ay = fabsf(d.y), az = fabsf(d.z);
-  uint32_t face, q;
+  uint32_t face, su, sv;
   if (ax >= ay && ax >= az) {
     face = d.x < 0.0f ? 1u : 0u;
-    q = (d.y < 0.0f ? 1u : 0u) | (d.z < 0.0f ? 2u : 0u);
+    su = face_square(d.y, ax);
+    sv = face_square(d.z, ax);
   } else if (ay >= az) {
     face = d.y < 0.0f ? 3u : 2u;
-    q = (d.x < 0.0f ? 1u : 0u) | (d.z < 0.0f ? 2u : 0u);
+    su = face_square(d.x, ay);
+    sv = face_square(d.z, ay);
   } else {
     face = d.z < 0.0f ? 5u : 4u;
-    q = (d.x < 0.0f ? 1u : 0u) | (d.y < 0.0f ? 2u : 0u);
+    su = face_square(d.x, az);
+    sv = face_square(d.y, az);
   }
-  return (morton << 5) | (face * 4u + q);  // < kRayBins
+  return morton * kRayDirs + (face * kRayDirSplit + su) * kRayDirSplit + sv;  // < kRayBins
 }
 
 __global__ void __launch_bounds__(256) k_ray_hist(PathPool P, const WaveControl* __restrict__ ctl, HitPool H,
@@ -514,34 +529,57 @@ __global__ void __launch_bounds__(256) k_ray_hist(PathPool P, const WaveControl*
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < live; i += gridDim.x * blockDim.x) {
     const uint2 pf = P.pixel_flags[i];
     const uint32_t key = ray_group_key(c_scenes[jobs[pf.y >> kFlagJobShift].scene_slot], P.ray_o[i], P.ray_d[i]);
-    H.ray_key[i] = (uint16_t)key;
+    H.ray_key[i] = key;
     atomicAdd(&H.ray_bins[key], 1u);
   }
 }
 
-// Exclusive prefix sums of the kRayBins counts into the offsets (one block).
-__global__ void __launch_bounds__(1024) k_ray_scan(HitPool H) {
-  constexpr uint32_t kPer = kRayBins / 1024;
-  __shared__ uint32_t s_sum[1024];
-  const uint32_t t = threadIdx.x;
-  uint32_t v[kPer], acc = 0;
-  for (uint32_t k = 0; k < kPer; ++k) {
-    v[k] = H.ray_bins[t * kPer + k];
-    acc += v[k];
+// Exclusive prefix sums of the kRayBins counts, in two steps: each
+// 1024-bin block's own prefix sums into the offsets and its total into
+// partial[block] (clearing the counts for the next wave), then the block
+// totals' prefix sums (one block); k_ray_scatter adds the two.
+__device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t* total) {
+  __shared__ uint32_t s_warp[32];
+  const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  uint32_t x = v;
+  for (uint32_t off = 1; off < 32; off <<= 1) {
+    const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, off);
+    if (lane >= off) x += y;
   }
-  s_sum[t] = acc;
+  if (lane == 31) s_warp[warp] = x;
   __syncthreads();
-  for (uint32_t off = 1; off < 1024; off <<= 1) {  // inclusive scan (Hillis-Steele)
-    const uint32_t x = t >= off ? s_sum[t - off] : 0u;
-    __syncthreads();
-    s_sum[t] += x;
-    __syncthreads();
+  if (warp == 0) {
+    const uint32_t n_warps = blockDim.x >> 5;
+    uint32_t w = lane < n_warps ? s_warp[lane] : 0u;
+    for (uint32_t off = 1; off < 32; off <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, w, off);
+      if (lane >= off) w += y;
+    }
+    s_warp[lane] = w;  // inclusive totals of warps 0..lane
   }
-  uint32_t base = s_sum[t] - acc;
-  for (uint32_t k = 0; k < kPer; ++k) {
-    H.ray_bins[kRayBins + t * kPer + k] = base;
-    base += v[k];
+  __syncthreads();
+  *total = s_warp[(blockDim.x >> 5) - 1];
+  return x - v + (warp > 0 ? s_warp[warp - 1] : 0u);
+}
+
+__global__ void __launch_bounds__(1024) k_ray_scan_blocks(HitPool H) {
+  const uint32_t k = blockIdx.x * 1024u + threadIdx.x;
+  const uint32_t v = k < kRayBins ? H.ray_bins[k] : 0u;
+  uint32_t total;
+  const uint32_t x = block_exclusive_scan(v, &total);
+  if (k < kRayBins) {
+    H.ray_bins[kRayBins + k] = x;
+    H.ray_bins[k] = 0u;
   }
+  if (threadIdx.x == 0) H.ray_bins[2 * kRayBins + blockIdx.x] = total;
+}
+
+__global__ void __launch_bounds__(1024) k_ray_scan_partials(HitPool H) {
+  const uint32_t k = threadIdx.x;
+  const uint32_t v = k < kRayScanBlocks ? H.ray_bins[2 * kRayBins + k] : 0u;
+  uint32_t total;
+  const uint32_t x = block_exclusive_scan(v, &total);
+  if (k < kRayScanBlocks) H.ray_bins[2 * kRayBins + k] = x;
 }
 
 __global__ void __launch_bounds__(256) k_ray_scatter(const WaveControl* __restrict__ ctl, HitPool H) {
@@ -558,9 +596,10 @@ __global__ void __launch_bounds__(256) k_ray_scatter(const WaveControl* __restri
     const uint32_t peers = __match_any_sync(act, key);
     const int leader = __ffs(peers) - 1;
     uint32_t base = 0;
-    if (lane == leader) base = atomicAdd(&H.ray_bins[kRayBins + key], (uint32_t)__popc(peers));
+    if (lane == leader)
+      base = H.ray_bins[2 * kRayBins + (key >> 10)] + atomicAdd(&H.ray_bins[kRayBins + key], (uint32_t)__popc(peers));
     base = __shfl_sync(peers, base, leader);
-    H.order[base + (uint32_t)__popc(peers & ((1u << lane) - 1u))] = i;
+    H.ray_order[base + (uint32_t)__popc(peers & ((1u << lane) - 1u))] = i;
   }
 }
 
@@ -667,11 +706,14 @@ uint32_t launch_wave(const PathPool& A, const PathPool& B, const HitPool& H, Wav
   const uint32_t cap = std::max(opt.capacity, 1u);
   const uint32_t blocks_256 = (cap + 255) / 256, blocks_trace = (cap + kTraceBlock - 1) / kTraceBlock;
   // continuing rays grouped before tracing (surfaces; the pool must have the key arrays)
-  const bool sort_rays = opt.sort_rays && !opt.volumes && H.ray_key && H.ray_bins && H.order;
-  k_plan<<<1, 128, 0, stream>>>(ctl, counters, sort_rays ? H.ray_bins : nullptr);
+  const bool sort_rays = opt.sort_rays && !opt.volumes && H.ray_key && H.ray_bins && H.ray_order;
+  k_plan<<<1, 128, 0, stream>>>(ctl, counters);
   if (sort_rays) {
+    // (the counts are zero: cleared when allocated, at the start of every
+    // frame and by each wave's k_ray_scan_blocks)
     k_ray_hist<<<blocks_256, 256, 0, stream>>>(A, ctl, H, jobs);
-    k_ray_scan<<<1, 1024, 0, stream>>>(H);
+    k_ray_scan_blocks<<<kRayScanBlocks, 1024, 0, stream>>>(H);
+    k_ray_scan_partials<<<1, 1024, 0, stream>>>(H);
     k_ray_scatter<<<blocks_256, 256, 0, stream>>>(ctl, H);
   }
   if (ev) cudaEventRecord(ev[0], stream);
@@ -679,7 +721,7 @@ uint32_t launch_wave(const PathPool& A, const PathPool& B, const HitPool& H, Wav
   if (ev) cudaEventRecord(ev[1], stream);
   const uint32_t tb = (opt.trace_block == 64 || opt.trace_block == 256) ? opt.trace_block : (uint32_t)kTraceBlock;
   const WaveArgs w{A, B, Hs, ctl, jobs, counters, blocks_trace, stream, tb, (cap + tb - 1) / tb,
-                   sort_rays ? H.order : nullptr};
+                   sort_rays ? H.ray_order : nullptr};
   if (adjoint && opt.volumes) {
     launch_adjoint_extend_media(w, opt);
   } else if (opt.volumes) {
@@ -692,7 +734,7 @@ uint32_t launch_wave(const PathPool& A, const PathPool& B, const HitPool& H, Wav
   }
   if (opt.recorder.out) k_record_vertices<<<blocks_256, 256, 0, stream>>>(A, ctl, H, jobs, opt.recorder);
   if (ev) cudaEventRecord(ev[2], stream);
-  if (sort_hits) k_sort_hits<<<blocks_256, 256, 0, stream>>>(ctl, Hs, A, jobs, counters);
+  if (sort_hits) k_sort_hits<<<blocks_256, 256, 0, stream>>>(ctl, Hs, A, jobs, counters, w.ray_order);
   if (ev) cudaEventRecord(ev[3], stream);
   if (adjoint) {
     launch_adjoint_shade(opt.volumes, feat, w, opt);
@@ -714,7 +756,7 @@ uint32_t launch_wave(const PathPool& A, const PathPool& B, const HitPool& H, Wav
     k_connect<0><<<conn_grid, tb, occluded_shared_bytes(tb), stream>>>(*defer, jobs, counters);
   if (ev) cudaEventRecord(ev[5], stream);
   k_finish<<<1, 32, 0, stream>>>(ctl, counters, graph_condition);
-  return 5u + (sort_hits ? 1u : 0u) + (defer ? 1u : 0u) + (sort_rays ? 3u : 0u);
+  return 5u + (sort_hits ? 1u : 0u) + (defer ? 1u : 0u) + (sort_rays ? 4u : 0u);
 }
 
 cudaError_t read_bound_record(uint32_t* words, int n_words, bool clear, cudaStream_t stream) {

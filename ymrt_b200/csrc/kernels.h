@@ -55,12 +55,21 @@ struct HitPool {
   uint4* nearby;    // kMaxNearby entries per slot: prim, t bits, back
   float* vol_w;     // kMaxBoundaryRecord medium-selection weights per slot (volume hits only)
   uint8_t* bucket;  // shading bucket per slot (kBucketNone: nothing to shade)
-  uint32_t* order;  // slots to shade, bucket by bucket (before the closest-hit stage: continuing rays, grouped)
-  uint16_t* ray_key;   // grouping key per continuing slot (null: rays are not grouped)
-  uint32_t* ray_bins;  // kRayBins counts, then kRayBins offsets
+  uint32_t* order;  // slots to shade, bucket by bucket
+  uint32_t* ray_order; // the continuing slots, grouped (null: rays are not grouped)
+  uint32_t* ray_key;   // grouping key per continuing slot
+  uint32_t* ray_bins;  // kRayBins counts, kRayBins offsets, kRayScanBlocks block offsets
 };
-// Continuing rays are traced grouped by origin cell and direction (k_ray_*).
-constexpr uint32_t kRayBins = 1u << 14;
+// Continuing rays are traced grouped by origin cell and direction (k_ray_*):
+// the origin's cell of a 2^kRayCellBits-per-axis grid over the scene, and the
+// direction's cube face split into kRayDirSplit x kRayDirSplit squares.
+constexpr uint32_t kRayCellBits = 4;
+constexpr uint32_t kRayDirSplit = 4;
+constexpr uint32_t kRayDirs = 6 * kRayDirSplit * kRayDirSplit;
+constexpr uint32_t kRayBins = (1u << (3 * kRayCellBits)) * kRayDirs;
+constexpr uint32_t kRayScanBlocks = (kRayBins + 1023) / 1024;  // at most 1024
+static_assert(kRayScanBlocks <= 1024, "the block totals are scanned by one block");
+constexpr size_t kRayBinWords = 2 * (size_t)kRayBins + kRayScanBlocks;
 
 // One render of a batch (a single render is a batch of one): its scene,
 // settings, output image and its range in the batch's path space (paths are
