@@ -129,9 +129,9 @@ int ymrt_set_profiling(ymrt_context* ctx, int enable);
 /*   YMRT_OPT_TRACE_BLOCK   (default 128) threads per block of the closest-hit
  *                          and shadow-ray kernels: 64, 128 or 256 */
 #define YMRT_OPT_TRACE_BLOCK 4
-/*   YMRT_OPT_SORT_RAYS     (default 1) surfaces: trace each wave's continuing
- *                          rays grouped by origin cell and direction instead
- *                          of in the order shading left them (same hits) */
+/*   YMRT_OPT_SORT_RAYS     (default 1) trace each wave's continuing rays
+ *                          grouped by origin cell and direction instead of
+ *                          in the order shading left them (same hits) */
 #define YMRT_OPT_SORT_RAYS 6
 int ymrt_set_option(ymrt_context* ctx, int option, int value);
 int ymrt_get_option(const ymrt_context* ctx, int option, int* value);

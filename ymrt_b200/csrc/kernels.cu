@@ -705,8 +705,8 @@ uint32_t launch_wave(const PathPool& A, const PathPool& B, const HitPool& H, Wav
   // the uneven per-ray work; k_connect walks its queue with a GPU-sized grid.
   const uint32_t cap = std::max(opt.capacity, 1u);
   const uint32_t blocks_256 = (cap + 255) / 256, blocks_trace = (cap + kTraceBlock - 1) / kTraceBlock;
-  // continuing rays grouped before tracing (surfaces; the pool must have the key arrays)
-  const bool sort_rays = opt.sort_rays && !opt.volumes && H.ray_key && H.ray_bins && H.ray_order;
+  // continuing rays grouped before tracing (the pool must have the key arrays)
+  const bool sort_rays = opt.sort_rays && H.ray_key && H.ray_bins && H.ray_order;
   k_plan<<<1, 128, 0, stream>>>(ctl, counters);
   if (sort_rays) {
     // (the counts are zero: cleared when allocated, at the start of every

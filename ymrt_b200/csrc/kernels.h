@@ -201,7 +201,7 @@ struct WaveOptions {
   uint32_t capacity = 0;       // path slots per pool (sizes the grids)
   bool volumes = false;        // volume scattering kernels
   bool sort_hits = true;       // shade hits listed by shading bucket
-  bool sort_rays = false;      // surfaces: trace continuing rays grouped by origin cell and direction
+  bool sort_rays = false;      // trace continuing rays grouped by origin cell and direction
   bool defer_shadows = false;  // queue surface shadow rays for k_connect (ignored with volumes)
   uint32_t features = kFeatAll;  // scene features of the batch (kFeatSpheres | kFeatGrids | kFeatTextures)
   ShadowQueue shadow_queue{};

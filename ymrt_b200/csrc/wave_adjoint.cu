@@ -23,7 +23,7 @@ void launch_adjoint_extend_media(const WaveArgs& w, const WaveOptions& opt) {
   // free flight with the density-grid terms (one instantiation, all features)
   const auto k = k_extend<true, kFeatAll, true>;
   k<<<w.trace_blocks, w.trace_block, traversal_shared_bytes(w.trace_block), w.stream>>>(w.A, w.ctl, w.H, w.jobs, w.counters,
-                                                                           opt.grid_grads, opt.grid_tex, nullptr);
+                                                                           opt.grid_grads, opt.grid_tex, w.ray_order);
 }
 
 void launch_adjoint_shade(bool volumes, uint32_t features, const WaveArgs& w, const WaveOptions& opt) {

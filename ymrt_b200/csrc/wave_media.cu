@@ -13,7 +13,7 @@ template <uint32_t kF>
 void media_extend(const WaveArgs& w) {
   const auto k = k_extend<true, kF>;
   k<<<w.trace_blocks, w.trace_block, traversal_shared_bytes(w.trace_block), w.stream>>>(w.A, w.ctl, w.H, w.jobs, w.counters, nullptr,
-                                                                   kEmpty, nullptr);
+                                                                   kEmpty, w.ray_order);
 }
 
 template <uint32_t kF>
