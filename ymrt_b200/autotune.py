@@ -2,10 +2,11 @@
 
 Picks, by measuring on the GPU, the configuration that renders a workload
 fastest: path-queue capacity (paths in flight per wave), material-sorted
-shading on/off, deferred shadow rays on/off, the block shape of the
+shading on/off, continuing rays grouped by origin and direction on/off,
+deferred shadow rays on/off, the block shape of the
 closest-hit and shadow-ray kernels (threads per block), the CUDA-graph wave
 loop on/off and the wide-BVH leaf size. The search is exhaustive over a
-small space (the defaults below: 3 x 2 x 2 x 3 x 3 = 108 points, two
+small space (the defaults below: 3 x 2 x 2 x 2 x 3 x 3 = 216 points, two
 wave-loop kinds only when asked), each point timed on a sample of the
 workload (a band of tiles from
 the middle of the frame, large enough to fill several waves) after one
@@ -26,12 +27,13 @@ from typing import Callable, Dict, Iterable, List, Optional
 DEFAULT_SPACE: Dict[str, List[int]] = {
     "queue_capacity": [1 << 20, 1 << 21, 1 << 22],
     "sort_hits": [0, 1],
+    "sort_rays": [0, 1],
     "defer_shadows": [0, 1],
     "trace_block": [64, 128, 256],
     "max_leaf_triangles": [2, 3, 4],
 }
 
-WAVE_OPTIONS = ("sort_hits", "defer_shadows", "graph_loop", "trace_block")
+WAVE_OPTIONS = ("sort_hits", "sort_rays", "defer_shadows", "graph_loop", "trace_block")
 
 
 def points(space: Dict[str, Iterable[int]]) -> List[Dict[str, int]]:

@@ -865,8 +865,12 @@ __device__ __noinline__ vec3 eval_volume_lights(uint32_t slot, TraversalStack& s
 // are shaded exactly as in the forward pass, nothing is added to the image,
 // and each material vertex adds its terms of dLoss/dParam (see AdjCtx) to
 // `grads` (per-block sums in shared memory, then one atomic per touched slot).
+//
+// The forward surface instantiations are held to four resident blocks per SM
+// (128 registers, a few spills) instead of three at 168 registers: the
+// 1080p 64-spp bench frame 220.4 -> 217.4 ms.
 template <bool kVol, bool kDefer, bool kAdj, uint32_t kF>
-__global__ void __launch_bounds__(kTraceBlock) k_shade(PathPool P, const WaveControl* __restrict__ ctl, HitPool H,
+__global__ void __launch_bounds__(kTraceBlock, (kVol || kAdj) ? 1 : 4) k_shade(PathPool P, const WaveControl* __restrict__ ctl, HitPool H,
                                                        PathPool Q, const JobDesc* __restrict__ jobs,
                                                        WaveCounters* counters, ShadowQueue shadow_q,
                                                        float* grads = nullptr, uint32_t grad_materials = 0,
