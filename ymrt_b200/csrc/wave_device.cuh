@@ -866,11 +866,24 @@ __device__ __noinline__ vec3 eval_volume_lights(uint32_t slot, TraversalStack& s
 // and each material vertex adds its terms of dLoss/dParam (see AdjCtx) to
 // `grads` (per-block sums in shared memory, then one atomic per touched slot).
 //
-// The forward surface instantiations are held to four resident blocks per SM
-// (128 registers, a few spills) instead of three at 168 registers: the
-// 1080p 64-spp bench frame 220.4 -> 217.4 ms.
+// Resident blocks per SM the register allocation is held to (measured on one
+// box, CUDA-event A/B): forward surfaces four (128 registers, a few spills;
+// the 1080p 64-spp bench frame 220.4 -> 217.4 ms against three at 168);
+// forward media without the texture nodes three (168 registers, 1-2 KB of
+// spills; the 1280x720 32-spp volumetric frame 925 -> 892 ms against two at
+// 255, four 903 ms); forward media with the texture nodes two (255
+// registers; three spill more and were slower, 892 -> 915 ms on the
+// textured frame); the surface adjoint three (backward pass of 16 views
+// 512² 16 spp 505 -> 487 ms); the media adjoint two.
 template <bool kVol, bool kDefer, bool kAdj, uint32_t kF>
-__global__ void __launch_bounds__(kTraceBlock, (kVol || kAdj) ? 1 : 4) k_shade(PathPool P, const WaveControl* __restrict__ ctl, HitPool H,
+constexpr int shade_blocks_per_sm() {
+  if (kAdj) return kVol ? 1 : 3;
+  if (kVol) return (kF & kFeatTextures) ? 1 : 3;
+  return 4;
+}
+
+template <bool kVol, bool kDefer, bool kAdj, uint32_t kF>
+__global__ void __launch_bounds__(kTraceBlock, shade_blocks_per_sm<kVol, kDefer, kAdj, kF>()) k_shade(PathPool P, const WaveControl* __restrict__ ctl, HitPool H,
                                                        PathPool Q, const JobDesc* __restrict__ jobs,
                                                        WaveCounters* counters, ShadowQueue shadow_q,
                                                        float* grads = nullptr, uint32_t grad_materials = 0,
