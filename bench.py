@@ -202,12 +202,26 @@ def kernel_table(pst):
     return out
 
 
-def batch_renders(seed: int = 0, n: int = 64):
+def batch_renders(seed: int = 0, n: int = 64, small: bool = False):
     """The batched workload: n renders, each a Cornell-like or instanced
     scene variant (per-render scene seed), at a resolution drawn from
     {256x256, 512x512, 640x480, 1024x1024} and U{4..64} spp, all seeded.
-    Instanced variants use two scene seeds (their BVH build dominates set-up)."""
+    Instanced variants use two scene seeds (their BVH build dominates set-up).
+
+    small=True: previews that each fill a small part of the GPU (2k-200k
+    paths against a 2 Mi-path queue): n renders over a pool of 48 scenes
+    (46 Cornell-like variants, each at one resolution of {64x64, 128x128,
+    160x120, 256x256}, and the two instanced seeds at 128x128), U{1..8} spp."""
     rng = np.random.default_rng(seed)
+    if small:
+        res = [(64, 64), (128, 128), (160, 120), (256, 256)]
+        pool = [("cornell", k, *res[k % len(res)]) for k in range(46)] + [("instanced", k, 128, 128) for k in range(2)]
+        out = []
+        for _ in range(n):
+            kind, scene_seed, W, H = pool[int(rng.integers(0, len(pool)))]
+            out.append({"scene": kind, "seed": scene_seed, "width": W, "height": H, "spp": int(rng.integers(1, 9)),
+                        "depth": 12 if kind == "instanced" else 8})
+        return out
     res = [(256, 256), (512, 512), (640, 480), (1024, 1024)]
     out = []
     for k in range(n):
@@ -222,7 +236,8 @@ def batch_renders(seed: int = 0, n: int = 64):
 
 def run_batch_workload(args):
     """64 renders in one batch (one CUDA-graph wave loop over all of them)
-    against the same renders made one after another."""
+    against the same renders made one after another; workload batch_small:
+    256 small previews (batch_renders(small=True)) the same way."""
     import torch
     import ymrt_b200 as Y
     from ymrt_b200 import scenes
@@ -230,7 +245,8 @@ def run_batch_workload(args):
     rank, world, local_rank = dist_env()
     torch.cuda.set_device(local_rank)
     perm = scenes.halton_permutations()
-    specs = batch_renders(seed=rank)
+    small = args.workload == "batch_small"
+    specs = batch_renders(seed=rank, n=256 if small else 64, small=small)
     ctx = Y.Context(local_rank)
     hosts, renders = {}, []
     for sp in specs:
@@ -273,11 +289,17 @@ def run_batch_workload(args):
     clk = clocks.stop()
     elapsed = ev0.elapsed_time(ev1)
     # the same renders one after another (frame 1 of each)
+    # (ms: the renders' own device times summed; loop_ms: CUDA events around
+    # the whole loop, host calls between the renders included)
     seq_ms, seq_rays = 0.0, 0
+    ev0.record()
     for sc, setting, _, out in renders:
         _, s1 = sc.render(setting, 1, out=out)
         seq_ms += s1.ms_total
         seq_rays += s1.extension_rays + s1.shadow_rays
+    ev1.record()
+    torch.cuda.synchronize()
+    seq_loop_ms = ev0.elapsed_time(ev1)
     batch_ms = elapsed / args.steps
     paths = sum(sp["width"] * sp["height"] * sp["spp"] for sp in specs)
     result = {
@@ -285,12 +307,14 @@ def run_batch_workload(args):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(batch_ms, 3), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded .ymtmp scenes generated by ymrt_b200.scenes)",
-        "config": {"workload": f"batch of {len(specs)} renders (Cornell-like and instanced variants, "
-                               "256x256..1024x1024, 4-64 spp)", "paths_per_step": paths,
+        "config": {"workload": f"batch of {len(specs)} renders (Cornell-like and instanced variants, " +
+                               ("64x64..256x256, 1-8 spp)" if small else "256x256..1024x1024, 4-64 spp)"),
+                   "paths_per_step": paths,
                    "l2": "256 MB buffer written between steps"},
         "spp_per_s": round(paths / (batch_ms * 1e-3), 1),
         "sequential": {"ms": round(seq_ms, 3), "mrays_s": round(seq_rays / (seq_ms * 1e-3) / 1e6, 2),
-                       "batch_speedup": round(seq_ms / batch_ms, 3)},
+                       "batch_speedup": round(seq_ms / batch_ms, 3), "loop_ms": round(seq_loop_ms, 3),
+                       "batch_speedup_loop": round(seq_loop_ms / batch_ms, 3)},
         "gpu_launches": int(launches), "device_errors": int(errors), "clocks": clk,
         "autotuned": tuned,
         "renders": specs,
@@ -751,7 +775,7 @@ def main(argv=None):
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["batch", "diff", "diff_media"], default="instanced")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["batch", "batch_small", "diff", "diff_media"], default="instanced")
     ap.add_argument("--spp", type=int, default=0)
     ap.add_argument("--queue", type=int, default=0, help="path queue capacity (0 = library default)")
     ap.add_argument("--cpu-budget", type=float, default=10.0, help="seconds of CPU work per reference sample")
@@ -769,7 +793,7 @@ def main(argv=None):
     if args.impl == "reference":
         with quiet_stdout():
             res = run_reference(args)
-    elif args.workload == "batch":
+    elif args.workload in ("batch", "batch_small"):
         res = run_batch_workload(args)
     elif args.workload in ("diff", "diff_media"):
         res = run_diff_workload(args, media=args.workload == "diff_media")

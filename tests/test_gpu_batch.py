@@ -44,3 +44,27 @@ def test_batch_equals_single_renders(ctx, cornell_path, volumetric_path, instanc
         assert _close(got[..., :3], want[..., :3]), f"render {k}: radiance differs"
     for c in cases:
         c[0].close()
+
+
+def test_batch_beyond_scene_slots(ctx, cornell_path, halton_perm):
+    """70 small renders of 68 distinct scenes: more (scene, sampler) pairs
+    than the 64 constant-memory scene slots, so the batch runs as two groups
+    of jobs; every render must still equal the same render made alone."""
+    import torch
+    sizes = [(32 + 16 * (k % 6), 32 + 16 * (k // 6 % 4)) for k in range(68)]
+    scenes = [Y.Scene(ctx, Y.HostScene(cornell_path, w, h), halton_perm) for w, h in sizes]
+    cases = [(scenes[k % 68], Y.default_setting(spp=1 + k % 3, ray_depth=6), 1 + k % 2) for k in range(70)]
+    singles, outs = [], []
+    for scene, setting, frame in cases:
+        single = torch.zeros((scene.height, scene.width, 4), dtype=torch.float32, device="cuda")
+        scene.render(setting, frame, out=single)
+        singles.append(single.cpu().numpy())
+        outs.append(torch.full((scene.height, scene.width, 4), float("nan"), dtype=torch.float32, device="cuda"))
+    stats = Y.render_batch(ctx, [(c[0], c[1], c[2], o) for c, o in zip(cases, outs)])
+    assert stats.device_errors == 0
+    for k, (o, want) in enumerate(zip(outs, singles)):
+        got = o.cpu().numpy()
+        assert np.array_equal(got[..., 3], want[..., 3]), f"render {k}: sample counts differ"
+        assert _close(got[..., :3], want[..., :3]), f"render {k}: radiance differs"
+    for s in scenes:
+        s.close()

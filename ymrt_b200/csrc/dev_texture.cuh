@@ -66,8 +66,13 @@ __device__ __forceinline__ float perlin_grad(int h, float x, float y, float z) {
 
 __device__ __forceinline__ float perlin_fade(float t) { return t * t * t * (t * (t * 6.0f - 15.0f) + 10.0f); }
 
-// PerlinNoiseEval (src/TextureEval.cuh:55-132).
-__device__ __forceinline__ float perlin_noise(vec3 p) {
+// PerlinNoiseEval (src/TextureEval.cuh:55-132). Out of line: the solid
+// nodes, fBm and turbulence call it from a dozen sites, and one shared copy
+// keeps the texture-enabled media shading kernel, which is bound by
+// instruction fetch, within its instruction cache (the 1280x720 32-spp
+// textured frame 889 -> 745 ms; the fBm media frame 892 -> 882 ms; fBm
+// itself out of line as well gained nothing more).
+static __device__ __noinline__ float perlin_noise(vec3 p) {
   int x0 = (int)floorf(p.x), y0 = (int)floorf(p.y), z0 = (int)floorf(p.z);
   const float tx = p.x - (float)x0, ty = p.y - (float)y0, tz = p.z - (float)z0;
   const int x1 = (x0 + 1) & 255, y1 = (y0 + 1) & 255, z1 = (z0 + 1) & 255;

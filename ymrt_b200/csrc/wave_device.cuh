@@ -873,7 +873,8 @@ __device__ __noinline__ vec3 eval_volume_lights(uint32_t slot, TraversalStack& s
 // spills; the 1280x720 32-spp volumetric frame 925 -> 892 ms against two at
 // 255, four 903 ms); forward media with the texture nodes two (255
 // registers; three spill more and were slower, 892 -> 915 ms on the
-// textured frame); the surface adjoint three (backward pass of 16 views
+// textured frame, and again with Perlin noise out of line, 745 -> 783 ms);
+// the surface adjoint three (backward pass of 16 views
 // 512² 16 spp 505 -> 487 ms); the media adjoint two.
 template <bool kVol, bool kDefer, bool kAdj, uint32_t kF>
 constexpr int shade_blocks_per_sm() {
